@@ -1,0 +1,306 @@
+#!/usr/bin/env python
+"""Benchmark of the QBVH closest-hit path: 1,310,720-triangle displaced icosphere, 16,777,216
+random rays (origins uniform in 1.5x the bounding box, directions uniform on the sphere).
+
+One step = one closest-hit launch over all rays, rays already resident in HBM (``value``).
+``e2e`` traces the same rays through the public C ABI entry point ``liar_gpu_trace`` from
+pinned host buffers, copies in and out included. ``--impl reference`` times the CPU
+restatement of the reference's path (oracle/) on the host cores instead.
+
+Multi-GPU (torchrun): rays are independent, so each rank traces its own ray set against its own
+replica of the mesh (weak scaling, no collective on the data path); rank 0 reports the total
+rays of all ranks over the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "QBVH closest-hit Mrays/s"
+WORKLOAD = "displaced icosphere 1,310,720 tris, 16,777,216 random rays, closest hit"
+LEVELS = 8
+N_RAYS = 1 << 24
+
+
+def load_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.samples: list[list[str]] = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.samples.append([x.strip() for x in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self) -> dict:
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if len(s) > 3 + k and "Active" in s[3 + k]
+                          and "Not" not in s[3 + k]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline_rays(v, f, rays, target_seconds=10.0):
+    """Times the oracle tree on a bounded sample of the workload's rays; returns (Mrays/s, info)."""
+    import oracle
+    threads = oracle.hardware_threads()
+    tree = oracle.Tree(v, f)
+    n = min(len(rays), 1 << 18)
+    t0 = time.perf_counter()
+    tree.trace(rays[:n], threads=threads)
+    dt = time.perf_counter() - t0
+    n2 = int(min(len(rays), max(n, n * target_seconds / max(dt, 1e-3))))
+    t0 = time.perf_counter()
+    tree.trace(rays[:n2], threads=threads)
+    dt2 = time.perf_counter() - t0
+    return n2 / dt2 / 1e6, {"cores": threads, "sample": f"first {n2} of the {len(rays)} workload rays, "
+                                                         f"{dt2:.1f} s on {threads} host threads"}
+
+
+def run_reference(args, world, rank):
+    """CPU restatement of the reference's path (oracle/), all host threads, bounded samples."""
+    if rank != 0:
+        return
+    import oracle
+    from liar_b200 import scenes
+    v, f = scenes.displaced_icosphere(LEVELS, seed=0)
+    rays = scenes.random_rays(v, N_RAYS, seed=0)
+    threads = oracle.hardware_threads()
+    tree = oracle.Tree(v, f)
+    sample = 1 << 20
+    for _ in range(args.warmup):
+        tree.trace(rays[:sample], threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        tree.trace(rays[:sample], threads=threads)
+        times.append(time.perf_counter() - t0)
+    dt = float(np.mean(times))
+    val = sample / dt / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt * 1e3 * (N_RAYS / sample), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural mesh and rays)",
+        "config": {"workload": WORKLOAD, "rays_per_step": sample, "sample_of": N_RAYS},
+        "cpu_baseline": {"value": val, "unit": "Mrays/s", "cores": threads, "kind": "port",
+                         "sample": f"first {sample} workload rays per step (CPU restatement; the reference's Lass core "
+                                   f"cannot be built)"},
+        "e2e": {"value": val, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        return run_reference(args, world, rank)
+
+    import torch
+    import torch.distributed as dist
+    from liar_b200 import scenes
+    from liar_b200.trace import Context, Mesh
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    v, f = scenes.displaced_icosphere(LEVELS, seed=0)
+    rays = scenes.random_rays(v, N_RAYS, seed=rank)
+    ctx = Context(local)
+    mesh = Mesh(ctx, v, f)
+    stats = mesh.stats
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    d_rays = torch.from_numpy(rays).to(f"cuda:{local}")
+    d_hits = torch.empty((N_RAYS, 2), dtype=torch.int32, device=f"cuda:{local}")
+    d_cnt = torch.zeros(2, dtype=torch.int64, device=f"cuda:{local}")
+    torch.cuda.synchronize()
+
+    # visit counts of this exact ray set (one counted launch, outside the timed region)
+    with torch.cuda.stream(stream):
+        mesh.trace_into(d_rays.data_ptr(), N_RAYS, d_hits.data_ptr(), stream=stream.cuda_stream,
+                        counters_ptr=d_cnt.data_ptr())
+    stream.synchronize()
+    ctx.synchronize()
+    nodes_visited, tris_tested = d_cnt.cpu().tolist()
+
+    def step(any_hit=False):
+        mesh.trace_into(d_rays.data_ptr(), N_RAYS, d_hits.data_ptr(), any_hit=any_hit, stream=stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    stream.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        stream.synchronize()
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * N_RAYS / (ms * 1e-3) / 1e6
+
+    # any hit (tmax = 0.5) on the same rays, same timing rules, reported beside the headline
+    d_rays_any = d_rays.clone()
+    d_rays_any[:, 7] = 0.5
+    def step_any():
+        mesh.trace_into(d_rays_any.data_ptr(), N_RAYS, d_hits.data_ptr(), any_hit=True, stream=stream.cuda_stream)
+    for _ in range(args.warmup):
+        step_any()
+    stream.synchronize()
+    a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a0.record(stream)
+    for _ in range(args.steps):
+        step_any()
+    a1.record(stream)
+    stream.synchronize()
+    ctx.synchronize()
+    ms_any = a0.elapsed_time(a1) / args.steps
+    del d_rays_any
+
+    # end to end through the C ABI with pinned host buffers, copies included
+    h_rays = torch.from_numpy(rays).pin_memory()
+    h_hits = torch.empty((N_RAYS, 2), dtype=torch.int32).pin_memory()
+    lib = ctx._lib
+    import ctypes as C
+
+    def e2e_step():
+        ctx.check(lib.liar_gpu_trace(ctx.handle, mesh.handle, C.c_void_p(h_rays.data_ptr()), N_RAYS,
+                                     C.c_void_p(h_hits.data_ptr()), 0))
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    e2e_steps = max(1, min(args.steps, 10))
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_s], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_val = world * N_RAYS / e2e_s / 1e6
+
+    peaks = load_peaks()
+    per_ray_model = 128.0 * nodes_visited / N_RAYS + 48.0 * tris_tested / N_RAYS + 40.0
+    achieved = per_ray_model * N_RAYS / (ms * 1e-3) / 1e9
+    traffic = None
+    prof = ROOT / "profiles" / "trace_closest_traffic.json"
+    if prof.exists():
+        traffic = json.loads(prof.read_text()).get("dram_bytes_per_launch")
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded procedural mesh and rays)",
+        "config": {"workload": WORKLOAD, "triangles": int(stats["n_triangles"]), "rays_per_step": N_RAYS,
+                   "parallelism": f"replicas{world}" if world > 1 else "single",
+                   "l2": "rays (512 MiB) stream through; larger than L2, no flush",
+                   "tree": {k: stats[k] for k in ("n_nodes", "n_leaves", "max_depth", "stack_needed", "sah_cost",
+                                                  "device_bytes", "build_seconds")}},
+        "any_hit": {"value": world * N_RAYS / (ms_any * 1e-3) / 1e6, "unit": "Mrays/s", "tmax": 0.5,
+                    "ms_per_step": ms_any},
+        "visits_per_ray": {"nodes": nodes_visited / N_RAYS, "triangles": tris_tested / N_RAYS},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                     "model": "128 B x nodes visited + 48 B x triangles tested + 40 B per ray, counted on device",
+                     "peak_source": peaks["source"]},
+        "e2e": {"value": e2e_val, "unit": "Mrays/s", "h2d_bytes_per_step": N_RAYS * 32,
+                "d2h_bytes_per_step": N_RAYS * 8, "api": "liar_gpu_trace (host buffers, pinned)"},
+        "gpu_launches": args.steps,
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        val, info = cpu_baseline_rays(v, f, rays)
+        line["cpu_baseline"] = {"value": val, "unit": "Mrays/s", "cores": info["cores"], "kind": "port",
+                                "sample": info["sample"]}
+    mesh.close()
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

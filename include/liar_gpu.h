@@ -1,0 +1,122 @@
+/* liar_gpu.h -- C ABI of the B200 (sm_100a) implementation of LiAR's per-sample hot path.
+ *
+ * Conventions
+ *   - Every function returns LIAR_OK (0) or a negative LIAR_ERR_* code and never throws.
+ *     liar_gpu_last_error(ctx) returns a readable message for the last failure on ctx.
+ *   - The caller owns every host buffer it passes. The library owns the device memory behind
+ *     the opaque handles (liar_gpu_ctx, liar_gpu_mesh, ...), released by the matching
+ *     *_destroy call.
+ *   - A context is bound to one CUDA device and is not re-entrant: use one context per host
+ *     thread. It replaces the reference's per-worker clone of tracer and sampler
+ *     (src/liar/kernel/render_engine.cpp:317-326).
+ *   - Functions without a "_device" suffix take HOST buffers and block until the result is
+ *     back in host memory. "_device" variants take device pointers and a cudaStream_t (passed
+ *     as void*, NULL = the context's stream) and return without synchronising.
+ */
+#ifndef LIAR_GPU_H
+#define LIAR_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LIAR_GPU_ABI_VERSION 1
+
+enum liar_status {
+    LIAR_OK = 0,
+    LIAR_ERR_INVALID = -1,     /* bad argument: null pointer, size, index out of range, NaN */
+    LIAR_ERR_CUDA = -2,        /* a CUDA runtime call failed */
+    LIAR_ERR_NO_DEVICE = -3,   /* no CUDA device, or the device is not sm_100 */
+    LIAR_ERR_OOM = -4,         /* device or host allocation failed */
+    LIAR_ERR_STACK = -5,       /* a traversal stack overflowed (tree deeper than the stack) */
+    LIAR_ERR_TIMEOUT = -6,     /* a bounded device-side wait gave up */
+    LIAR_ERR_CANCELLED = -7,   /* the host-mapped cancel flag was raised */
+    LIAR_ERR_UNSUPPORTED = -8  /* feature combination not implemented */
+};
+
+typedef struct liar_gpu_ctx liar_gpu_ctx;
+typedef struct liar_gpu_mesh liar_gpu_mesh;
+
+/* A ray with its parameter interval, 32 bytes: the BoundedRay of the reference
+ * (src/liar/kernel/bounded_ray.h:41-90). Direction need not be normalised; t is measured in
+ * units of |d|. */
+typedef struct liar_ray {
+    float ox, oy, oz, tmin;
+    float dx, dy, dz, tmax;
+} liar_ray;
+
+/* Result of one ray, 8 bytes. prim is the index of the triangle in the caller's triangle array
+ * (the reference's Intersection special field k, src/liar/scenery/triangle_mesh.cpp:309), or
+ * -1 on a miss. For any-hit queries prim is some occluding triangle and t its distance. */
+typedef struct liar_hit {
+    int32_t prim;
+    float t;
+} liar_hit;
+
+/* Options of the 4-wide SAH tree build. Zero-initialised options select the defaults. */
+typedef struct liar_build_opts {
+    int max_leaf_size;   /* triangles per leaf, 1..8 (default 4) */
+    int sah_bins;        /* 0 = full sweep SAH; else binned SAH with this many bins (default 0) */
+    float traversal_cost;/* SAH cost of one node visit relative to one triangle test (default 1.0) */
+    int threads;         /* host threads for the build, 0 = all cores */
+} liar_build_opts;
+
+typedef struct liar_mesh_stats {
+    uint64_t n_triangles;
+    uint64_t n_nodes;        /* 4-wide inner nodes, 128 bytes each */
+    uint64_t n_leaves;
+    uint32_t max_depth;      /* inner-node levels from the root to the deepest leaf */
+    uint32_t stack_needed;   /* traversal stack entries the deepest path can need */
+    double sah_cost;         /* SAH cost of the 4-wide tree (node visits + triangle tests) */
+    uint64_t device_bytes;   /* bytes of device memory held by the mesh */
+    double build_seconds;    /* host time of the build */
+} liar_mesh_stats;
+
+/* ---- context ------------------------------------------------------------------------------ */
+
+int liar_gpu_create(liar_gpu_ctx** out, int device);
+void liar_gpu_destroy(liar_gpu_ctx* ctx);
+const char* liar_gpu_last_error(const liar_gpu_ctx* ctx);
+int liar_gpu_abi_version(void);
+/* The stream used by the host-buffer entry points and by "_device" calls given stream NULL.
+ * NULL here selects the context's own non-blocking stream. */
+int liar_gpu_set_stream(liar_gpu_ctx* ctx, void* stream);
+/* Waits for the context's stream and reports device-side errors of the "_device" calls
+ * queued since the last check (stack overflow, bounded-wait timeout, cancel). */
+int liar_gpu_synchronize(liar_gpu_ctx* ctx);
+
+/* ---- triangle mesh: build + closest/any hit -----------------------------------------------
+ * Replaces TriangleMesh::TriangleMesh with its Lass QbvhTree<..., SAHSplitHeuristics> reset
+ * (src/liar/scenery/triangle_mesh.cpp:69-85, src/liar/scenery/triangle_mesh.h:53) and
+ * ObjectTree::doPreProcess (src/liar/scenery/object_trees.h:100-108). */
+int liar_gpu_mesh_build(liar_gpu_ctx* ctx, const float* vertices /* n_vertices x 3 */, size_t n_vertices,
+                        const uint32_t* triangles /* n_triangles x 3 vertex indices */, size_t n_triangles,
+                        const liar_build_opts* opts /* NULL = defaults */, liar_gpu_mesh** out);
+void liar_gpu_mesh_destroy(liar_gpu_mesh* mesh);
+int liar_gpu_mesh_stats(const liar_gpu_mesh* mesh, liar_mesh_stats* out);
+
+/* Closest hit (any_hit = 0) replaces TriangleMesh::doIntersect
+ * (src/liar/scenery/triangle_mesh.cpp:291-318): the nearest t > tmin, then accepted only if
+ * BoundedRay::inRange holds, t > tmin*(1+tol) && t < tmax*(1-tol) with tol = 1e-6
+ * (src/liar/kernel/bounded_ray.h:69-77, src/liar/kernel/kernel_common.cpp:32). Equal t is
+ * resolved to the lower triangle index.
+ * Any hit (any_hit = 1) replaces TriangleMesh::doIsIntersecting
+ * (src/liar/scenery/triangle_mesh.cpp:321-330): is there a triangle with tmin < t < tmax. */
+int liar_gpu_trace(liar_gpu_ctx* ctx, const liar_gpu_mesh* mesh, const liar_ray* rays, size_t n_rays,
+                   liar_hit* hits, int any_hit);
+int liar_gpu_trace_device(liar_gpu_ctx* ctx, const liar_gpu_mesh* mesh, const liar_ray* d_rays, size_t n_rays,
+                          liar_hit* d_hits, int any_hit, void* stream);
+/* Same as liar_gpu_trace_device, and adds per-ray node visits and triangle tests into
+ * d_counters[0] and d_counters[1] (two uint64 on the device, accumulated). */
+int liar_gpu_trace_counted_device(liar_gpu_ctx* ctx, const liar_gpu_mesh* mesh, const liar_ray* d_rays,
+                                  size_t n_rays, liar_hit* d_hits, int any_hit, unsigned long long* d_counters,
+                                  void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LIAR_GPU_H */

@@ -1,0 +1,106 @@
+"""ctypes binding of the sm_100a library ``libliar_gpu.so`` (C ABI in include/liar_gpu.h).
+
+There is no CPU fallback: importing this module raises if the library has not been built, and
+every entry point raises :class:`LiarGpuError` with the library's message when it fails.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = Path(os.environ.get("LIAR_GPU_LIB", _HERE / "libliar_gpu.so"))
+
+LIAR_OK = 0
+STATUS_NAMES = {
+    -1: "LIAR_ERR_INVALID",
+    -2: "LIAR_ERR_CUDA",
+    -3: "LIAR_ERR_NO_DEVICE",
+    -4: "LIAR_ERR_OOM",
+    -5: "LIAR_ERR_STACK",
+    -6: "LIAR_ERR_TIMEOUT",
+    -7: "LIAR_ERR_CANCELLED",
+    -8: "LIAR_ERR_UNSUPPORTED",
+}
+
+
+class LiarGpuError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {message}")
+        self.code = code
+
+
+class Ray(C.Structure):
+    _fields_ = [(n, C.c_float) for n in ("ox", "oy", "oz", "tmin", "dx", "dy", "dz", "tmax")]
+
+
+class Hit(C.Structure):
+    _fields_ = [("prim", C.c_int32), ("t", C.c_float)]
+
+
+class BuildOpts(C.Structure):
+    _fields_ = [("max_leaf_size", C.c_int), ("sah_bins", C.c_int), ("traversal_cost", C.c_float), ("threads", C.c_int)]
+
+
+class MeshStats(C.Structure):
+    _fields_ = [
+        ("n_triangles", C.c_uint64),
+        ("n_nodes", C.c_uint64),
+        ("n_leaves", C.c_uint64),
+        ("max_depth", C.c_uint32),
+        ("stack_needed", C.c_uint32),
+        ("sah_cost", C.c_double),
+        ("device_bytes", C.c_uint64),
+        ("build_seconds", C.c_double),
+    ]
+
+
+_vp = C.c_void_p
+_sz = C.c_size_t
+
+# name -> (restype, argtypes); every symbol declared in include/liar_gpu.h is listed here
+SIGNATURES: dict[str, tuple] = {
+    "liar_gpu_abi_version": (C.c_int, []),
+    "liar_gpu_create": (C.c_int, [C.POINTER(_vp), C.c_int]),
+    "liar_gpu_destroy": (None, [_vp]),
+    "liar_gpu_last_error": (C.c_char_p, [_vp]),
+    "liar_gpu_set_stream": (C.c_int, [_vp, _vp]),
+    "liar_gpu_synchronize": (C.c_int, [_vp]),
+    "liar_gpu_mesh_build": (C.c_int, [_vp, _vp, _sz, _vp, _sz, _vp, C.POINTER(_vp)]),
+    "liar_gpu_mesh_destroy": (None, [_vp]),
+    "liar_gpu_mesh_stats": (C.c_int, [_vp, C.POINTER(MeshStats)]),
+    "liar_gpu_trace": (C.c_int, [_vp, _vp, _vp, _sz, _vp, C.c_int]),
+    "liar_gpu_trace_device": (C.c_int, [_vp, _vp, _vp, _sz, _vp, C.c_int, _vp]),
+    "liar_gpu_trace_counted_device": (C.c_int, [_vp, _vp, _vp, _sz, _vp, C.c_int, _vp, _vp]),
+}
+
+
+def load(path: Path | str | None = None) -> C.CDLL:
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise ImportError(
+            f"{p} is missing: build it with `python -m liar_b200.build` (there is no CPU fallback)"
+        )
+    lib = C.CDLL(str(p))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+_LIB: C.CDLL | None = None
+
+
+def lib() -> C.CDLL:
+    global _LIB
+    if _LIB is None:
+        _LIB = load()
+    return _LIB
+
+
+def check(code: int, ctx=None) -> None:
+    if code != LIAR_OK:
+        msg = lib().liar_gpu_last_error(ctx).decode(errors="replace") if ctx else ""
+        raise LiarGpuError(code, msg)

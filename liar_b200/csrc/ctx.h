@@ -1,0 +1,81 @@
+// ctx.h -- the opaque context behind liar_gpu_ctx, shared by the .cu files of the library.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <functional>
+#include <string>
+#include <vector>
+
+#include "../../include/liar_gpu.h"
+#include "qbvh.h"
+
+namespace liar_gpu {
+
+// Scratch words of a context (device memory, allocated once per context):
+//   [kStatusWord]        device-side error bits, ORed by kernels, read and cleared by the host
+//   [kCounterWord + k]   work counters of persistent kernels (k = 0 device calls, 1..2 the
+//                        host-buffer pipeline slots, 3.. other kernels)
+constexpr int kScratchWords = 64;
+constexpr int kStatusWord = 0;
+constexpr int kCounterWord = 8;
+constexpr uint32_t kStatusTimeout = 1u << 8;
+constexpr uint32_t kStatusCancelled = 1u << 9;
+
+}  // namespace liar_gpu
+
+struct liar_gpu_ctx {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    uint32_t* d_scratch = nullptr;
+    // grow-only staging buffers of the host-buffer entry points
+    void* d_rays = nullptr;
+    size_t cap_rays = 0;
+    void* d_hits = nullptr;
+    size_t cap_hits = 0;
+    cudaStream_t pipe[2] = {nullptr, nullptr};
+    cudaEvent_t pipe_ev[3] = {nullptr, nullptr, nullptr};
+    // resources of other subsystems (renderer, photon maps) register their release here
+    std::vector<std::function<void()>> on_destroy;
+
+    void release_extensions() {
+        for (auto it = on_destroy.rbegin(); it != on_destroy.rend(); ++it) (*it)();
+        on_destroy.clear();
+        for (int k = 0; k < 2; ++k)
+            if (pipe[k]) cudaStreamDestroy(pipe[k]);
+        for (int k = 0; k < 3; ++k)
+            if (pipe_ev[k]) cudaEventDestroy(pipe_ev[k]);
+    }
+};
+
+namespace liar_gpu {
+
+int ctx_fail(liar_gpu_ctx* ctx, int code, const char* fmt, ...);
+int ctx_cuda(liar_gpu_ctx* ctx, cudaError_t e, const char* what);
+int ctx_activate(liar_gpu_ctx* ctx);
+int ctx_grow(liar_gpu_ctx* ctx, void** buf, size_t* cap, size_t bytes, const char* what);
+int ctx_check_status(liar_gpu_ctx* ctx);
+
+inline int ctx_ensure_pipeline(liar_gpu_ctx* ctx) {
+    for (int k = 0; k < 2; ++k)
+        if (!ctx->pipe[k]) {
+            cudaError_t e = cudaStreamCreateWithFlags(&ctx->pipe[k], cudaStreamNonBlocking);
+            if (e != cudaSuccess) return ctx_cuda(ctx, e, "create pipeline stream");
+        }
+    for (int k = 0; k < 3; ++k)
+        if (!ctx->pipe_ev[k]) {
+            cudaError_t e = cudaEventCreateWithFlags(&ctx->pipe_ev[k], cudaEventDisableTiming);
+            if (e != cudaSuccess) return ctx_cuda(ctx, e, "create pipeline event");
+        }
+    return LIAR_OK;
+}
+
+const QNode* mesh_nodes(const liar_gpu_mesh* m);
+const QTri* mesh_tris(const liar_gpu_mesh* m);
+uint32_t mesh_stack_needed(const liar_gpu_mesh* m);
+int mesh_device(const liar_gpu_mesh* m);
+
+}  // namespace liar_gpu

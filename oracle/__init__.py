@@ -1,0 +1,107 @@
+"""CPU oracle of the hot path -- TEST INFRASTRUCTURE ONLY.
+
+A plain C++ restatement of the reference's arithmetic (liboracle.so, built by oracle/build.py),
+used by tests/, by ``__graft_entry__.smoke()`` and by bench.py's CPU-baseline leg as the
+checker. The product (``liar_b200``) never imports it.
+
+Parity status: the reference's geometry core lives in the Lass library
+(lass/1.11.0-250+g078d9309, conanfile.py:39), which is not part of the reference tree and cannot
+be built here. The traversal restatement is therefore pinned by construction (the nearest-t rule
+with ties to the lower index is tree-independent) and by the brute-force definition, not by
+golden vectors of the reference, which ships none for this path. The spectral restatement is
+pinned by the known-answer test of test/test_spectrum.cpp:256-278 (tests/golden/).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+_LIB = None
+
+
+def lib() -> C.CDLL:
+    global _LIB
+    if _LIB is None:
+        path = _HERE / "liboracle.so"
+        if not path.exists():
+            from . import build as _b
+            _b.build()
+        L = C.CDLL(str(path))
+        vp, u64 = C.c_void_p, C.c_uint64
+        L.oracle_tri_intersect.restype = C.c_int
+        L.oracle_tri_intersect.argtypes = [vp] * 8
+        L.oracle_trace_bruteforce.restype = C.c_int
+        L.oracle_trace_bruteforce.argtypes = [vp, u64, vp, u64, vp, u64, vp, C.c_int, C.c_int]
+        L.oracle_tree_build.restype = vp
+        L.oracle_tree_build.argtypes = [vp, u64, vp, u64]
+        L.oracle_tree_trace.restype = C.c_int
+        L.oracle_tree_trace.argtypes = [vp, vp, u64, vp, C.c_int, C.c_int]
+        L.oracle_tree_free.restype = None
+        L.oracle_tree_free.argtypes = [vp]
+        L.oracle_hardware_threads.restype = C.c_int
+        _bind_extra(L)
+        _LIB = L
+    return _LIB
+
+
+def _bind_extra(L) -> None:
+    """Binds the optional restatements (spectra, shading, tracer, photons) when present."""
+    from . import _sigs
+    for name, (res, args) in _sigs.SIGNATURES.items():
+        fn = getattr(L, name, None)
+        if fn is not None:
+            fn.restype = res
+            fn.argtypes = args
+
+
+def hardware_threads() -> int:
+    return int(lib().oracle_hardware_threads())
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def tri_intersect(o, d, a, b, c):
+    """Moller-Trumbore on one ray/triangle; returns (t, u, v) or None."""
+    o, d, a, b, c = map(_f32, (o, d, a, b, c))
+    t, u, v = C.c_float(), C.c_float(), C.c_float()
+    hit = lib().oracle_tri_intersect(o.ctypes.data, d.ctypes.data, a.ctypes.data, b.ctypes.data, c.ctypes.data,
+                                     C.addressof(t), C.addressof(u), C.addressof(v))
+    return (t.value, u.value, v.value) if hit else None
+
+
+def trace_bruteforce(vertices, triangles, rays, any_hit=False, threads=0):
+    V = _f32(vertices).reshape(-1, 3)
+    T = np.ascontiguousarray(triangles, dtype=np.uint32).reshape(-1, 3)
+    R = _f32(rays).reshape(-1, 8)
+    H = np.empty((R.shape[0], 2), dtype=np.int32)
+    lib().oracle_trace_bruteforce(V.ctypes.data, V.shape[0], T.ctypes.data, T.shape[0], R.ctypes.data, R.shape[0],
+                                  H.ctypes.data, int(bool(any_hit)), int(threads))
+    return H[:, 0].copy(), H[:, 1].view(np.float32).copy()
+
+
+class Tree:
+    """Median-split binary tree over the mesh (CPU only)."""
+
+    def __init__(self, vertices, triangles):
+        self.V = _f32(vertices).reshape(-1, 3)
+        self.T = np.ascontiguousarray(triangles, dtype=np.uint32).reshape(-1, 3)
+        self.h = lib().oracle_tree_build(self.V.ctypes.data, self.V.shape[0], self.T.ctypes.data, self.T.shape[0])
+
+    def trace(self, rays, any_hit=False, threads=0):
+        R = _f32(rays).reshape(-1, 8)
+        H = np.empty((R.shape[0], 2), dtype=np.int32)
+        lib().oracle_tree_trace(self.h, R.ctypes.data, R.shape[0], H.ctypes.data, int(bool(any_hit)), int(threads))
+        return H[:, 0].copy(), H[:, 1].view(np.float32).copy()
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().oracle_tree_free(self.h)
+                self.h = None
+        except Exception:
+            pass
