@@ -115,6 +115,24 @@ int liar_gpu_trace_counted_device(liar_gpu_ctx* ctx, const liar_gpu_mesh* mesh, 
                                   size_t n_rays, liar_hit* d_hits, int any_hit, unsigned long long* d_counters,
                                   void* stream);
 
+/* Allocation-free closest hit / any hit. It has no counterpart in the reference; it exists for
+ * callers that must not call cudaMalloc while they trace: an application whose own pool
+ * allocator owns the device memory, a frame loop whose other streams would be stalled by the
+ * synchronisation cudaMalloc/cudaFree can cause, a plugin with a fixed memory budget.
+ * Results are those of liar_gpu_trace_device (same kernel, same rules), without a context: the
+ * work counter and status word live in a 256-byte device array compiled into the library.
+ *   - d_rays / d_hits are the caller's device buffers on the mesh's device (16- / 8-byte
+ *     aligned); at most 2^31 rays per call, more returns LIAR_ERR_INVALID.
+ *   - The call allocates nothing and blocks until the trace on `stream` (NULL = the legacy
+ *     default stream) has finished, so that it can return the kernel's status
+ *     (LIAR_ERR_STACK on a traversal stack overflow).
+ *   - The first call on a device looks up the array's device address (cudaGetSymbolAddress)
+ *     with that device current; make that first call before any stream capture.
+ *   - Every call shares the one array per device: calls that overlap on the GPU (from several
+ *     host threads or streams at once) race on it and must be serialised by the caller. */
+int liar_gpu_trace_device_noalloc(const liar_gpu_mesh* mesh, const liar_ray* d_rays, size_t n_rays,
+                                  liar_hit* d_hits, int any_hit, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -73,6 +73,7 @@ SIGNATURES: dict[str, tuple] = {
     "liar_gpu_trace": (C.c_int, [_vp, _vp, _vp, _sz, _vp, C.c_int]),
     "liar_gpu_trace_device": (C.c_int, [_vp, _vp, _vp, _sz, _vp, C.c_int, _vp]),
     "liar_gpu_trace_counted_device": (C.c_int, [_vp, _vp, _vp, _sz, _vp, C.c_int, _vp, _vp]),
+    "liar_gpu_trace_device_noalloc": (C.c_int, [_vp, _vp, _sz, _vp, C.c_int, _vp]),
 }
 
 
