@@ -18,7 +18,6 @@ import json
 import os
 import subprocess
 import sys
-import threading
 import time
 from pathlib import Path
 
@@ -42,49 +41,57 @@ def load_peaks() -> dict:
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+    """Samples SM clocks and throttle reasons every 100 ms (one nvidia-smi -lms process) while
+    the timed regions run."""
 
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
               "clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, device: int):
         self.device = device
-        self.samples: list[list[str]] = []
-        self._stop = threading.Event()
-        self._t = None
-
-    def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                if out.returncode == 0 and out.stdout.strip():
-                    self.samples.append([x.strip() for x in out.stdout.strip().split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+        self.proc = None
+        self.lines: list[str] = []
 
     def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
-        self._t.start()
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            time.sleep(0.3)  # let the first sample land before the timed work starts
+        except Exception:
+            self.proc = None
         return self
 
     def __exit__(self, *exc):
-        self._stop.set()
-        if self._t:
-            self._t.join(timeout=10)
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
 
     def summary(self) -> dict:
-        if not self.samples:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for s in self.samples for k in range(4) if len(s) > 3 + k and "Active" in s[3 + k]
-                          and "Not" not in s[3 + k]})
+        rows = [[x.strip() for x in ln.split(",")] for ln in self.lines]
+        rows = [r for r in rows if len(r) >= 7]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [num(r[0]) for r in rows if num(r[0]) is not None]
+        mx = [num(r[1]) for r in rows if num(r[1]) is not None]
+        pw = [num(r[2]) for r in rows if num(r[2]) is not None]
+        reasons = sorted({self.NAMES[k] for r in rows for k in range(4) if r[3 + k] == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+                "power_w_max": max(pw) if pw else None, "reasons": reasons, "samples": len(rows)}
 
 
 def dist_setup():
@@ -95,20 +102,25 @@ def dist_setup():
 
 
 def cpu_baseline_rays(v, f, rays, target_seconds=10.0):
-    """Times the oracle tree on a bounded sample of the workload's rays; returns (Mrays/s, info)."""
+    """Times the oracle tree on a bounded sample of the workload's rays (about target_seconds of
+    CPU work on all host threads); returns (Mrays/s, info)."""
     import oracle
     threads = oracle.hardware_threads()
     tree = oracle.Tree(v, f)
     n = min(len(rays), 1 << 18)
     t0 = time.perf_counter()
     tree.trace(rays[:n], threads=threads)
-    dt = time.perf_counter() - t0
-    n2 = int(min(len(rays), max(n, n * target_seconds / max(dt, 1e-3))))
-    t0 = time.perf_counter()
-    tree.trace(rays[:n2], threads=threads)
+    dt = max(time.perf_counter() - t0, 1e-3)
+    total = int(n * target_seconds / dt)
+    done, t0 = 0, time.perf_counter()
+    while done < total:
+        m = min(len(rays), total - done)
+        tree.trace(rays[:m], threads=threads)
+        done += m
     dt2 = time.perf_counter() - t0
-    return n2 / dt2 / 1e6, {"cores": threads, "sample": f"first {n2} of the {len(rays)} workload rays, "
-                                                         f"{dt2:.1f} s on {threads} host threads"}
+    return done / dt2 / 1e6, {"cores": threads, "sample": f"{done} rays of the workload distribution (first "
+                                                        f"{min(len(rays), total)} rays, repeated), {dt2:.1f} s "
+                                                        f"on {threads} host threads"}
 
 
 def run_reference(args, world, rank):
@@ -147,7 +159,7 @@ def run_reference(args, world, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -195,45 +207,11 @@ def main():
     def step(any_hit=False):
         mesh.trace_into(d_rays.data_ptr(), N_RAYS, d_hits.data_ptr(), any_hit=any_hit, stream=stream.cuda_stream)
 
-    for _ in range(args.warmup):
-        step()
-    stream.synchronize()
-    barrier()
-    torch.cuda.synchronize()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
-        ev0.record(stream)
-        for _ in range(args.steps):
-            step()
-        ev1.record(stream)
-        stream.synchronize()
-    ctx.synchronize()
-    torch.cuda.synchronize()
-    barrier()
-    ms = ev0.elapsed_time(ev1) / args.steps
-    if world > 1:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * N_RAYS / (ms * 1e-3) / 1e6
-
-    # any hit (tmax = 0.5) on the same rays, same timing rules, reported beside the headline
     d_rays_any = d_rays.clone()
     d_rays_any[:, 7] = 0.5
+
     def step_any():
         mesh.trace_into(d_rays_any.data_ptr(), N_RAYS, d_hits.data_ptr(), any_hit=True, stream=stream.cuda_stream)
-    for _ in range(args.warmup):
-        step_any()
-    stream.synchronize()
-    a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a0.record(stream)
-    for _ in range(args.steps):
-        step_any()
-    a1.record(stream)
-    stream.synchronize()
-    ctx.synchronize()
-    ms_any = a0.elapsed_time(a1) / args.steps
-    del d_rays_any
 
     # end to end through the C ABI with pinned host buffers, copies included
     h_rays = torch.from_numpy(rays).pin_memory()
@@ -245,20 +223,37 @@ def main():
         ctx.check(lib.liar_gpu_trace(ctx.handle, mesh.handle, C.c_void_p(h_rays.data_ptr()), N_RAYS,
                                      C.c_void_p(h_hits.data_ptr()), 0))
 
-    for _ in range(max(1, args.warmup)):
-        e2e_step()
-    e2e_steps = max(1, min(args.steps, 10))
-    barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        e2e_step()
-    torch.cuda.synchronize()
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    if world > 1:
-        t = torch.tensor([e2e_s], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    def timed(fn, steps):
+        """Device time per step of fn on the trace stream (CUDA events, synchronised both sides)."""
+        for _ in range(args.warmup):
+            fn()
+        stream.synchronize()
+        ctx.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        stream.synchronize()
+        ctx.synchronize()
+        torch.cuda.synchronize()
+        barrier()
+        ms_ = e0.elapsed_time(e1) / steps
+        if world > 1:
+            t = torch.tensor([ms_], device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_ = float(t.item())
+        return ms_
+
+    e2e_steps = max(1, min(args.steps, 20))
+    with ClockSampler(local) as clocks:
+        ms = timed(step, args.steps)
+        ms_any = timed(step_any, args.steps)
+        e2e_s = timed(e2e_step, e2e_steps) * 1e-3
+    del d_rays_any
+    value = world * N_RAYS / (ms * 1e-3) / 1e6
     e2e_val = world * N_RAYS / e2e_s / 1e6
 
     peaks = load_peaks()

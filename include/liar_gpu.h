@@ -75,6 +75,14 @@ typedef struct liar_mesh_stats {
     double build_seconds;    /* host time of the build */
 } liar_mesh_stats;
 
+/* Launch shape of the trace kernels of a context (no reference counterpart: tuning only; the
+ * results do not depend on it). */
+typedef struct liar_trace_config {
+    int block_size;   /* threads per block: 128 or 256 */
+    int smem_stack;   /* traversal stack entries per lane kept in shared memory: 8, 16 or 24
+                         (256-thread blocks: 8 or 16); deeper entries spill to local memory */
+} liar_trace_config;
+
 /* ---- context ------------------------------------------------------------------------------ */
 
 int liar_gpu_create(liar_gpu_ctx** out, int device);
@@ -87,6 +95,9 @@ int liar_gpu_set_stream(liar_gpu_ctx* ctx, void* stream);
 /* Waits for the context's stream and reports device-side errors of the "_device" calls
  * queued since the last check (stack overflow, bounded-wait timeout, cancel). */
 int liar_gpu_synchronize(liar_gpu_ctx* ctx);
+/* Selects / reads the trace kernels' launch shape (default 128 threads, 16 shared entries). */
+int liar_gpu_set_trace_config(liar_gpu_ctx* ctx, const liar_trace_config* cfg);
+int liar_gpu_get_trace_config(const liar_gpu_ctx* ctx, liar_trace_config* out);
 
 /* ---- triangle mesh: build + closest/any hit -----------------------------------------------
  * Replaces TriangleMesh::TriangleMesh with its Lass QbvhTree<..., SAHSplitHeuristics> reset

@@ -43,6 +43,10 @@ class BuildOpts(C.Structure):
     _fields_ = [("max_leaf_size", C.c_int), ("sah_bins", C.c_int), ("traversal_cost", C.c_float), ("threads", C.c_int)]
 
 
+class TraceConfig(C.Structure):
+    _fields_ = [("block_size", C.c_int), ("smem_stack", C.c_int)]
+
+
 class MeshStats(C.Structure):
     _fields_ = [
         ("n_triangles", C.c_uint64),
@@ -67,6 +71,8 @@ SIGNATURES: dict[str, tuple] = {
     "liar_gpu_last_error": (C.c_char_p, [_vp]),
     "liar_gpu_set_stream": (C.c_int, [_vp, _vp]),
     "liar_gpu_synchronize": (C.c_int, [_vp]),
+    "liar_gpu_set_trace_config": (C.c_int, [_vp, C.POINTER(TraceConfig)]),
+    "liar_gpu_get_trace_config": (C.c_int, [_vp, C.POINTER(TraceConfig)]),
     "liar_gpu_mesh_build": (C.c_int, [_vp, _vp, _sz, _vp, _sz, _vp, C.POINTER(_vp)]),
     "liar_gpu_mesh_destroy": (None, [_vp]),
     "liar_gpu_mesh_stats": (C.c_int, [_vp, C.POINTER(MeshStats)]),

@@ -5,6 +5,7 @@
 
 #include <functional>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/liar_gpu.h"
@@ -14,13 +15,14 @@ namespace liar_gpu {
 
 // Scratch words of a context (device memory, allocated once per context):
 //   [kStatusWord]        device-side error bits, ORed by kernels, read and cleared by the host
-//   [kCounterWord + k]   work counters of persistent kernels (k = 0 device calls, 1..2 the
-//                        host-buffer pipeline slots, 3.. other kernels)
+//   [kCounterWord + k]   work counters of persistent kernels (k = 0 device calls, 1..kPipeSlots
+//                        the host-buffer pipeline slots, above that other kernels)
 constexpr int kScratchWords = 64;
 constexpr int kStatusWord = 0;
 constexpr int kCounterWord = 8;
 constexpr uint32_t kStatusTimeout = 1u << 8;
 constexpr uint32_t kStatusCancelled = 1u << 9;
+constexpr int kPipeSlots = 3;  // staging slots of the host-buffer trace pipeline
 
 }  // namespace liar_gpu
 
@@ -36,17 +38,21 @@ struct liar_gpu_ctx {
     size_t cap_rays = 0;
     void* d_hits = nullptr;
     size_t cap_hits = 0;
-    cudaStream_t pipe[2] = {nullptr, nullptr};
-    cudaEvent_t pipe_ev[3] = {nullptr, nullptr, nullptr};
+    cudaStream_t pipe[kPipeSlots] = {};
+    // pipe_ev[k]: end of slot k's work; pipe_ev[kPipeSlots]: start (work queued before the call)
+    cudaEvent_t pipe_ev[kPipeSlots + 1] = {};
+    // launch shape of the trace kernels (liar_gpu_set_trace_config) and cached occupancy per kernel
+    liar_trace_config trace_cfg{128, 16};
+    std::unordered_map<const void*, int> occupancy;
     // resources of other subsystems (renderer, photon maps) register their release here
     std::vector<std::function<void()>> on_destroy;
 
     void release_extensions() {
         for (auto it = on_destroy.rbegin(); it != on_destroy.rend(); ++it) (*it)();
         on_destroy.clear();
-        for (int k = 0; k < 2; ++k)
+        for (int k = 0; k < kPipeSlots; ++k)
             if (pipe[k]) cudaStreamDestroy(pipe[k]);
-        for (int k = 0; k < 3; ++k)
+        for (int k = 0; k <= kPipeSlots; ++k)
             if (pipe_ev[k]) cudaEventDestroy(pipe_ev[k]);
     }
 };
@@ -60,12 +66,12 @@ int ctx_grow(liar_gpu_ctx* ctx, void** buf, size_t* cap, size_t bytes, const cha
 int ctx_check_status(liar_gpu_ctx* ctx);
 
 inline int ctx_ensure_pipeline(liar_gpu_ctx* ctx) {
-    for (int k = 0; k < 2; ++k)
+    for (int k = 0; k < kPipeSlots; ++k)
         if (!ctx->pipe[k]) {
             cudaError_t e = cudaStreamCreateWithFlags(&ctx->pipe[k], cudaStreamNonBlocking);
             if (e != cudaSuccess) return ctx_cuda(ctx, e, "create pipeline stream");
         }
-    for (int k = 0; k < 3; ++k)
+    for (int k = 0; k <= kPipeSlots; ++k)
         if (!ctx->pipe_ev[k]) {
             cudaError_t e = cudaEventCreateWithFlags(&ctx->pipe_ev[k], cudaEventDisableTiming);
             if (e != cudaSuccess) return ctx_cuda(ctx, e, "create pipeline event");

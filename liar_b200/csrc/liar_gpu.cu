@@ -71,55 +71,63 @@ int ctx_grow(liar_gpu_ctx* ctx, void** buf, size_t* cap, size_t bytes, const cha
 
 namespace {
 
-constexpr int kBlock = 128;
-
-template <bool ANY, int S, bool COUNT>
+template <bool ANY, int S, int BLOCK, bool COUNT>
 int launch_trace_t(liar_gpu_ctx* ctx, const liar_gpu_mesh* m, const liar_ray* d_rays, uint32_t n, liar_hit* d_hits,
                    TraceCounters* d_counters, cudaStream_t st, uint32_t* d_counter, uint32_t* d_status) {
-    auto kern = trace_kernel<ANY, S, kBlock, COUNT>;
-    const size_t smem = (size_t)S * kBlock * 8;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return ctx_cuda(ctx, e, "set trace shared memory");
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, smem);
-    if (e != cudaSuccess) return ctx_cuda(ctx, e, "occupancy query");
-    if (per_sm <= 0) per_sm = 1;
-    const uint64_t needed_blocks = ((uint64_t)n + kBlock - 1) / kBlock;
+    auto kern = trace_kernel<ANY, S, BLOCK, COUNT>;
+    const size_t smem = (size_t)S * BLOCK * 8;
+    int& per_sm = ctx->occupancy[(const void*)kern];
+    if (per_sm == 0) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return ctx_cuda(ctx, e, "set trace shared memory");
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BLOCK, smem);
+        if (e != cudaSuccess) return ctx_cuda(ctx, e, "occupancy query");
+        if (per_sm <= 0) per_sm = 1;
+    }
+    const uint64_t needed_blocks = ((uint64_t)n + BLOCK - 1) / BLOCK;
     uint64_t blocks = (uint64_t)ctx->num_sms * per_sm;
     if (blocks > needed_blocks) blocks = needed_blocks;
     if (blocks == 0) blocks = 1;
-    e = cudaMemsetAsync(d_counter, 0, sizeof(uint32_t), st);
+    cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "reset work counter");
-    kern<<<(unsigned)blocks, kBlock, smem, st>>>(m->d_nodes, m->d_tris, d_rays, d_hits, n, d_counter, d_status,
-                                              d_counters);
+    kern<<<(unsigned)blocks, BLOCK, smem, st>>>(m->d_nodes, m->d_tris, d_rays, d_hits, n, d_counter, d_status,
+                                             d_counters);
     return ctx_cuda(ctx, cudaGetLastError(), "trace kernel launch");
+}
+
+template <int S, int BLOCK>
+int launch_trace_sb(liar_gpu_ctx* ctx, const liar_gpu_mesh* m, const liar_ray* d_rays, uint32_t n, liar_hit* d_hits,
+                    int any_hit, TraceCounters* d_counters, cudaStream_t st, uint32_t* d_counter, uint32_t* d_status) {
+    const bool cnt = d_counters != nullptr;
+    if (any_hit)
+        return cnt ? launch_trace_t<true, S, BLOCK, true>(ctx, m, d_rays, n, d_hits, d_counters, st, d_counter, d_status)
+                   : launch_trace_t<true, S, BLOCK, false>(ctx, m, d_rays, n, d_hits, d_counters, st, d_counter, d_status);
+    return cnt ? launch_trace_t<false, S, BLOCK, true>(ctx, m, d_rays, n, d_hits, d_counters, st, d_counter, d_status)
+               : launch_trace_t<false, S, BLOCK, false>(ctx, m, d_rays, n, d_hits, d_counters, st, d_counter, d_status);
 }
 
 int launch_trace(liar_gpu_ctx* ctx, const liar_gpu_mesh* m, const liar_ray* d_rays, size_t n_rays, liar_hit* d_hits,
                  int any_hit, TraceCounters* d_counters, cudaStream_t st, uint32_t* d_counter, uint32_t* d_status) {
     if (n_rays == 0) return LIAR_OK;
-    // the work counter of the persistent warps overshoots n by 32 per warp; 2^31 keeps it far from wrapping
+    // the work counter of the persistent warps overshoots n by BATCH per warp; 2^31 keeps it far from wrapping
     if (n_rays > (1ull << 31)) return ctx_fail(ctx, LIAR_ERR_INVALID, "too many rays in one call (limit 2^31)");
     if (((uintptr_t)d_rays & 15) || ((uintptr_t)d_hits & 7))
         return ctx_fail(ctx, LIAR_ERR_INVALID, "ray buffer must be 16-byte aligned and hit buffer 8-byte aligned");
     const uint32_t need = m->stats.stack_needed;
+    if (need > (uint32_t)kTraceStackTotal)
+        return ctx_fail(ctx, LIAR_ERR_STACK, "tree needs %u stack entries, more than the %d the kernels hold", need,
+                        kTraceStackTotal);
     const uint32_t n = (uint32_t)n_rays;
-    const bool cnt = d_counters != nullptr;
-    if (need <= 24) {
-        if (any_hit)
-            return cnt ? launch_trace_t<true, 24, true>(ctx, m, d_rays, n, d_hits, d_counters, st, d_counter, d_status)
-                       : launch_trace_t<true, 24, false>(ctx, m, d_rays, n, d_hits, d_counters, st, d_counter, d_status);
-        return cnt ? launch_trace_t<false, 24, true>(ctx, m, d_rays, n, d_hits, d_counters, st, d_counter, d_status)
-                   : launch_trace_t<false, 24, false>(ctx, m, d_rays, n, d_hits, d_counters, st, d_counter, d_status);
-    }
-    if (need <= 64) {
-        if (any_hit)
-            return cnt ? launch_trace_t<true, 64, true>(ctx, m, d_rays, n, d_hits, d_counters, st, d_counter, d_status)
-                       : launch_trace_t<true, 64, false>(ctx, m, d_rays, n, d_hits, d_counters, st, d_counter, d_status);
-        return cnt ? launch_trace_t<false, 64, true>(ctx, m, d_rays, n, d_hits, d_counters, st, d_counter, d_status)
-                   : launch_trace_t<false, 64, false>(ctx, m, d_rays, n, d_hits, d_counters, st, d_counter, d_status);
-    }
-    return ctx_fail(ctx, LIAR_ERR_STACK, "tree needs %u stack entries, more than the 64 the kernels hold", need);
+    const int s = ctx->trace_cfg.smem_stack, b = ctx->trace_cfg.block_size;
+#define LIAR_TRACE_CASE(S_, B_) \
+    if (s == S_ && b == B_) return launch_trace_sb<S_, B_>(ctx, m, d_rays, n, d_hits, any_hit, d_counters, st, d_counter, d_status);
+    LIAR_TRACE_CASE(8, 128)
+    LIAR_TRACE_CASE(16, 128)
+    LIAR_TRACE_CASE(24, 128)
+    LIAR_TRACE_CASE(8, 256)
+    LIAR_TRACE_CASE(16, 256)
+#undef LIAR_TRACE_CASE
+    return ctx_fail(ctx, LIAR_ERR_INVALID, "no trace kernel for block %d, shared stack %d", b, s);
 }
 
 cudaStream_t pick_stream(liar_gpu_ctx* ctx, void* stream) {
@@ -330,9 +338,12 @@ extern "C" int liar_gpu_trace(liar_gpu_ctx* ctx, const liar_gpu_mesh* mesh, cons
     int rc = ctx_activate(ctx);
     if (rc) return rc;
     // Chunked pipeline: the copy in of chunk k+1 and the copy out of chunk k-1 overlap the
-    // traversal of chunk k. Two staging slots, each with its own stream and work counter.
-    const size_t chunk = n_rays < (size_t)(1u << 22) ? n_rays : (size_t)(1u << 22);
-    const int slots = n_rays > chunk ? 2 : 1;
+    // traversal of chunk k (PCIe, not the kernel, bounds this call). Up to kPipeSlots staging
+    // slots, each with its own stream and work counter; chunks of 1M rays keep the unoverlapped
+    // head (first copy in) and tail (last copy out) short.
+    const size_t chunk = n_rays < (size_t)(1u << 20) ? n_rays : (size_t)(1u << 20);
+    const size_t n_chunks = (n_rays + chunk - 1) / chunk;
+    const int slots = n_chunks < (size_t)kPipeSlots ? (int)n_chunks : kPipeSlots;
     rc = ctx_grow(ctx, &ctx->d_rays, &ctx->cap_rays, (size_t)slots * chunk * sizeof(liar_ray), "ray staging buffer");
     if (rc) return rc;
     rc = ctx_grow(ctx, &ctx->d_hits, &ctx->cap_hits, (size_t)slots * chunk * sizeof(liar_hit), "hit staging buffer");
@@ -342,11 +353,11 @@ extern "C" int liar_gpu_trace(liar_gpu_ctx* ctx, const liar_gpu_mesh* mesh, cons
     liar_ray* dr = (liar_ray*)ctx->d_rays;
     liar_hit* dh = (liar_hit*)ctx->d_hits;
     // the pipeline streams wait for work already queued on the context stream
-    cudaEventRecord(ctx->pipe_ev[2], ctx->stream);
-    for (int s = 0; s < slots; ++s) cudaStreamWaitEvent(ctx->pipe[s], ctx->pipe_ev[2], 0);
+    cudaEventRecord(ctx->pipe_ev[kPipeSlots], ctx->stream);
+    for (int s = 0; s < slots; ++s) cudaStreamWaitEvent(ctx->pipe[s], ctx->pipe_ev[kPipeSlots], 0);
     size_t k = 0;
     int slot = 0;
-    for (size_t base = 0; base < n_rays; base += chunk, ++k, slot ^= (slots - 1)) {
+    for (size_t base = 0; base < n_rays; base += chunk, ++k, slot = (slot + 1) % slots) {
         const size_t m = (n_rays - base) < chunk ? (n_rays - base) : chunk;
         cudaStream_t st = ctx->pipe[slot];
         cudaError_t e = cudaMemcpyAsync(dr + (size_t)slot * chunk, rays + base, m * sizeof(liar_ray),
@@ -358,9 +369,29 @@ extern "C" int liar_gpu_trace(liar_gpu_ctx* ctx, const liar_gpu_mesh* mesh, cons
         e = cudaMemcpyAsync(hits + base, dh + (size_t)slot * chunk, m * sizeof(liar_hit), cudaMemcpyDeviceToHost, st);
         if (e != cudaSuccess) return ctx_cuda(ctx, e, "copy hits out");
     }
+    // work queued on the context stream after this call is ordered after the whole trace
+    for (int s = 0; s < slots; ++s) {
+        cudaEventRecord(ctx->pipe_ev[s], ctx->pipe[s]);
+        cudaStreamWaitEvent(ctx->stream, ctx->pipe_ev[s], 0);
+    }
     for (int s = 0; s < slots; ++s) {
         rc = ctx_cuda(ctx, cudaStreamSynchronize(ctx->pipe[s]), "trace synchronize");
         if (rc) return rc;
     }
     return ctx_check_status(ctx);
+}
+
+extern "C" int liar_gpu_set_trace_config(liar_gpu_ctx* ctx, const liar_trace_config* cfg) {
+    if (!ctx || !cfg) return LIAR_ERR_INVALID;
+    const int b = cfg->block_size, s = cfg->smem_stack;
+    const bool ok = (b == 128 && (s == 8 || s == 16 || s == 24)) || (b == 256 && (s == 8 || s == 16));
+    if (!ok) return ctx_fail(ctx, LIAR_ERR_INVALID, "unsupported trace config: block %d, shared stack %d", b, s);
+    ctx->trace_cfg = *cfg;
+    return LIAR_OK;
+}
+
+extern "C" int liar_gpu_get_trace_config(const liar_gpu_ctx* ctx, liar_trace_config* out) {
+    if (!ctx || !out) return LIAR_ERR_INVALID;
+    *out = ctx->trace_cfg;
+    return LIAR_OK;
 }

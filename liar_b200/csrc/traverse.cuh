@@ -4,15 +4,20 @@
 // (src/liar/scenery/triangle_mesh.cpp:291-330) and ObjectTree::doIntersect / doIsIntersecting
 // (src/liar/scenery/object_trees.h:110-143).
 //
-// Organisation (one thread per ray):
-//   * persistent warps: a grid of (SM count x resident blocks) blocks whose warps pull batches of
-//     32 rays from an atomic counter until the ray array is exhausted;
-//   * a node is one 128-byte line read with seven 16-byte read-only loads; the four child boxes
-//     are slab-tested with the near/far planes chosen by the ray's direction signs;
-//   * hit children are ordered by entry distance; the farther ones are pushed with their entry
-//     distance onto a per-thread stack that lives in shared memory (column per thread, so the
-//     32 lanes of a warp hit 32 different banks), and popped entries farther than the current
-//     closest hit are dropped without touching the node;
+// Organisation (one lane per ray, persistent warps with per-lane refill):
+//   * a grid of (SM count x resident blocks) blocks; each warp takes batches of BATCH ray indices
+//     from one atomic work counter and hands them to its lanes one by one: whenever at least
+//     REFILL lanes have finished their ray, those lanes load the next rays of the batch, so short
+//     rays (most random rays miss the mesh after a node or two) do not leave lanes idle while a
+//     long ray of the same warp is still traversing (dynamic fetch, Aila & Laine 2009);
+//   * one loop turn per lane = descend through inner nodes to the next leaf, then test that leaf;
+//   * a node is one 128-byte line read with seven 16-byte loads that carry an L2 evict-last
+//     policy; rays and hits stream with evict-first, so the 512 MiB ray stream does not push the
+//     tree out of L2;
+//   * hit children are ordered by entry distance (5-comparator network on distance-bit keys);
+//     the farther ones are pushed with their entry distance onto a per-lane stack whose top S
+//     entries live in shared memory (column per lane: conflict-free) and whose deeper entries
+//     spill to local memory; popped entries farther than the current closest hit are dropped;
 //   * triangles are tested with the exact Moller-Trumbore of tri_exact.h, so t is bit-identical
 //     to the CPU restatement, and equal t resolves to the lower original triangle index.
 #pragma once
@@ -28,13 +33,42 @@ namespace liar_gpu {
 // device-side status bits (ORed into the status word of a launch)
 enum : uint32_t { STATUS_STACK_OVERFLOW = 1u, STATUS_BAD_NODE = 2u };
 
+// total stack entries per lane (shared top + local spill); the host refuses deeper trees
+constexpr int kTraceStackTotal = 64;
+
 struct TraceCounters {
     unsigned long long nodes;
     unsigned long long tris;
 };
 
-__device__ __forceinline__ float4 ldg4(const F4* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
-__device__ __forceinline__ int4 ldg4i(const I4* p) { return __ldg(reinterpret_cast<const int4*>(p)); }
+// ---- loads and stores with L2 eviction policies (PTX createpolicy / cache_hint)
+__device__ __forceinline__ uint64_t policy_evict_last() {
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t policy_evict_first() {
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ float4 ld_hint(const void* ptr, uint64_t pol) {
+    float4 v;
+    asm("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+        : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+        : "l"(ptr), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ int4 ld_hint_i(const void* ptr, uint64_t pol) {
+    int4 v;
+    asm("ld.global.nc.L2::cache_hint.v4.s32 {%0, %1, %2, %3}, [%4], %5;"
+        : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+        : "l"(ptr), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ void st_hint(void* ptr, int a, int b, uint64_t pol) {
+    asm volatile("st.global.L2::cache_hint.v2.s32 [%0], {%1, %2}, %3;" ::"l"(ptr), "r"(a), "r"(b), "l"(pol) : "memory");
+}
 
 __device__ __forceinline__ float safe_rcp(float d) {
     // keeps 1/d finite so that inverted (empty) boxes can never produce NaN slab distances
@@ -44,144 +78,155 @@ __device__ __forceinline__ float safe_rcp(float d) {
 
 __device__ __forceinline__ float max4f(float a, float b, float c, float d) { return fmaxf(fmaxf(a, b), fmaxf(c, d)); }
 __device__ __forceinline__ float min4f(float a, float b, float c, float d) { return fminf(fminf(a, b), fminf(c, d)); }
-
 __device__ __forceinline__ int sel4i(const int4& v, uint32_t s) { return s == 0 ? v.x : s == 1 ? v.y : s == 2 ? v.z : v.w; }
 __device__ __forceinline__ float sel4f(float a, float b, float c, float d, uint32_t s) {
     return s == 0 ? a : s == 1 ? b : s == 2 ? c : d;
 }
-
 __device__ __forceinline__ void cswap(uint32_t& a, uint32_t& b) {
     const uint32_t lo = min(a, b), hi = max(a, b);
     a = lo;
     b = hi;
 }
 
-// One ray against the tree. Returns hit prim (-1 on miss) and t. Template:
-//   ANY   : any-hit (early exit, tmin < t < tmax) instead of closest-hit
-//   S     : stack entries per thread
-//   COUNT : collect node-visit / triangle-test counters
+constexpr int kNodeNone = -1;  // "no node": 0xffffffff is never a real leaf (leaf counts are <= 8)
+
+// Per-lane traversal state.
+struct RayState {
+    float ox, oy, oz, tmin, dx, dy, dz, tmax;
+    float idx, idy, idz, oix, oiy, oiz;
+    float tbest;
+    int best;
+    int node;
+    int sp;
+};
+
+template <int S, int BLOCK>
+struct LaneStack {
+    static constexpr int L = kTraceStackTotal - S > 0 ? kTraceStackTotal - S : 1;
+    int* s_node;
+    float* s_t;
+    int l_node[L];
+    float l_t[L];
+
+    __device__ __forceinline__ void push(int sp, int node, float t) {
+        if (sp < S) {
+            s_node[sp * BLOCK + threadIdx.x] = node;
+            s_t[sp * BLOCK + threadIdx.x] = t;
+        } else {
+            l_node[sp - S] = node;
+            l_t[sp - S] = t;
+        }
+    }
+    __device__ __forceinline__ void get(int sp, int& node, float& t) const {
+        if (sp < S) {
+            node = s_node[sp * BLOCK + threadIdx.x];
+            t = s_t[sp * BLOCK + threadIdx.x];
+        } else {
+            node = l_node[sp - S];
+            t = l_t[sp - S];
+        }
+    }
+};
+
+// Traverses from st.node until one leaf has been tested (or the ray is finished).
+// Returns true when the ray is finished.
 template <bool ANY, int S, int BLOCK, bool COUNT>
-__device__ __forceinline__ void trace_one(const QNode* __restrict__ nodes, const QTri* __restrict__ tris, float ox, float oy,
-                                          float oz, float tmin, float dx, float dy, float dz, float tmax,
-                                          int* __restrict__ st_node, float* __restrict__ st_t, int& out_prim,
-                                          float& out_t, uint32_t& status, uint32_t& n_nodes, uint32_t& n_tris) {
-    const float idx = safe_rcp(dx), idy = safe_rcp(dy), idz = safe_rcp(dz);
-    const float ooxx = ox * idx, ooyy = oy * idy, oozz = oz * idz;
-    const bool nx = dx < 0.0f, ny = dy < 0.0f, nz = dz < 0.0f;
-
-    // closest hit keeps candidates strictly below range_far(tmax); any hit strictly below tmax
-    float tbest = ANY ? tmax : range_far(tmax);
-    int best = -1;
-    int sp = 0;
-    int node = 0;  // root
-    const int tid = threadIdx.x;
-
-    while (true) {
-        if (node >= 0) {
-            // ---- inner node: test four child boxes
-            if (COUNT) ++n_nodes;
-            const QNode* q = nodes + node;
-            const float4 lx = ldg4(&q->lo_x), hx = ldg4(&q->hi_x);
-            const float4 ly = ldg4(&q->lo_y), hy = ldg4(&q->hi_y);
-            const float4 lz = ldg4(&q->lo_z), hz = ldg4(&q->hi_z);
-            const int4 ch = ldg4i(&q->child);
-            const float4 nxp = nx ? hx : lx, fxp = nx ? lx : hx;
-            const float4 nyp = ny ? hy : ly, fyp = ny ? ly : hy;
-            const float4 nzp = nz ? hz : lz, fzp = nz ? lz : hz;
-            float tn[4], tf[4];
-            tn[0] = max4f(fmaf(nxp.x, idx, -ooxx), fmaf(nyp.x, idy, -ooyy), fmaf(nzp.x, idz, -oozz), tmin);
-            tn[1] = max4f(fmaf(nxp.y, idx, -ooxx), fmaf(nyp.y, idy, -ooyy), fmaf(nzp.y, idz, -oozz), tmin);
-            tn[2] = max4f(fmaf(nxp.z, idx, -ooxx), fmaf(nyp.z, idy, -ooyy), fmaf(nzp.z, idz, -oozz), tmin);
-            tn[3] = max4f(fmaf(nxp.w, idx, -ooxx), fmaf(nyp.w, idy, -ooyy), fmaf(nzp.w, idz, -oozz), tmin);
-            tf[0] = min4f(fmaf(fxp.x, idx, -ooxx), fmaf(fyp.x, idy, -ooyy), fmaf(fzp.x, idz, -oozz), tbest);
-            tf[1] = min4f(fmaf(fxp.y, idx, -ooxx), fmaf(fyp.y, idy, -ooyy), fmaf(fzp.y, idz, -oozz), tbest);
-            tf[2] = min4f(fmaf(fxp.z, idx, -ooxx), fmaf(fyp.z, idy, -ooyy), fmaf(fzp.z, idz, -oozz), tbest);
-            tf[3] = min4f(fmaf(fxp.w, idx, -ooxx), fmaf(fyp.w, idy, -ooyy), fmaf(fzp.w, idz, -oozz), tbest);
-            // sortable keys: entry distance bits (tn >= tmin >= 0 for valid rays) with the slot
-            // in the two low bits; misses become 0xffffffff
-            uint32_t key[4];
+__device__ __forceinline__ bool trace_step(const QNode* __restrict__ nodes, const QTri* __restrict__ tris, RayState& st,
+                                           LaneStack<S, BLOCK>& stack, uint64_t pol_tree, uint32_t& status,
+                                           uint32_t& n_nodes, uint32_t& n_tris) {
+    const bool nx = st.dx < 0.0f, ny = st.dy < 0.0f, nz = st.dz < 0.0f;
+    // ---- descend through inner nodes until the nearest candidate is a leaf
+    while (st.node >= 0) {
+        if (COUNT) ++n_nodes;
+        const QNode* q = nodes + st.node;
+        const float4 lx = ld_hint(&q->lo_x, pol_tree), hx = ld_hint(&q->hi_x, pol_tree);
+        const float4 ly = ld_hint(&q->lo_y, pol_tree), hy = ld_hint(&q->hi_y, pol_tree);
+        const float4 lz = ld_hint(&q->lo_z, pol_tree), hz = ld_hint(&q->hi_z, pol_tree);
+        const int4 ch = ld_hint_i(&q->child, pol_tree);
+        const float4 nxp = nx ? hx : lx, fxp = nx ? lx : hx;
+        const float4 nyp = ny ? hy : ly, fyp = ny ? ly : hy;
+        const float4 nzp = nz ? hz : lz, fzp = nz ? lz : hz;
+        float tn[4], tf[4];
+        tn[0] = max4f(fmaf(nxp.x, st.idx, -st.oix), fmaf(nyp.x, st.idy, -st.oiy), fmaf(nzp.x, st.idz, -st.oiz), st.tmin);
+        tn[1] = max4f(fmaf(nxp.y, st.idx, -st.oix), fmaf(nyp.y, st.idy, -st.oiy), fmaf(nzp.y, st.idz, -st.oiz), st.tmin);
+        tn[2] = max4f(fmaf(nxp.z, st.idx, -st.oix), fmaf(nyp.z, st.idy, -st.oiy), fmaf(nzp.z, st.idz, -st.oiz), st.tmin);
+        tn[3] = max4f(fmaf(nxp.w, st.idx, -st.oix), fmaf(nyp.w, st.idy, -st.oiy), fmaf(nzp.w, st.idz, -st.oiz), st.tmin);
+        tf[0] = min4f(fmaf(fxp.x, st.idx, -st.oix), fmaf(fyp.x, st.idy, -st.oiy), fmaf(fzp.x, st.idz, -st.oiz), st.tbest);
+        tf[1] = min4f(fmaf(fxp.y, st.idx, -st.oix), fmaf(fyp.y, st.idy, -st.oiy), fmaf(fzp.y, st.idz, -st.oiz), st.tbest);
+        tf[2] = min4f(fmaf(fxp.z, st.idx, -st.oix), fmaf(fyp.z, st.idy, -st.oiy), fmaf(fzp.z, st.idz, -st.oiz), st.tbest);
+        tf[3] = min4f(fmaf(fxp.w, st.idx, -st.oix), fmaf(fyp.w, st.idy, -st.oiy), fmaf(fzp.w, st.idz, -st.oiz), st.tbest);
+        // sortable keys: entry distance bits (tn >= tmin >= 0 for valid rays) with the slot in
+        // the two low bits; misses become 0xffffffff
+        uint32_t key[4];
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const bool h = tn[c] <= tf[c];
-                key[c] = h ? ((__float_as_uint(fmaxf(tn[c], 0.0f)) & ~3u) | (uint32_t)c) : 0xffffffffu;
-            }
-            if (!ANY) {
-                cswap(key[0], key[1]);
-                cswap(key[2], key[3]);
-                cswap(key[0], key[2]);
-                cswap(key[1], key[3]);
-                cswap(key[1], key[2]);
-            }
-            if (key[0] == 0xffffffffu && key[1] == 0xffffffffu && key[2] == 0xffffffffu && key[3] == 0xffffffffu) {
-                node = -1;  // nothing hit: pop below
-            } else {
-                // the nearest valid key is the smallest; for ANY the order does not matter,
-                // so take the first valid one
-                int first = 0;
-                if (ANY) first = key[0] != 0xffffffffu ? 0 : key[1] != 0xffffffffu ? 1 : key[2] != 0xffffffffu ? 2 : 3;
-                // push the others, farthest first
+        for (int c = 0; c < 4; ++c)
+            key[c] = tn[c] <= tf[c] ? ((__float_as_uint(fmaxf(tn[c], 0.0f)) & ~3u) | (uint32_t)c) : 0xffffffffu;
+        if (!ANY) {
+            cswap(key[0], key[1]);
+            cswap(key[2], key[3]);
+            cswap(key[0], key[2]);
+            cswap(key[1], key[3]);
+            cswap(key[1], key[2]);
+        }
+        const int first = key[0] != 0xffffffffu ? 0 : key[1] != 0xffffffffu ? 1 : key[2] != 0xffffffffu ? 2
+                                                                        : key[3] != 0xffffffffu ? 3 : -1;
+        if (first < 0) {
+            st.node = kNodeNone;  // nothing hit below this node
+            break;
+        }
+        // push the other hit children, farthest first
 #pragma unroll
-                for (int c = 3; c >= 0; --c) {
-                    if (c == first || key[c] == 0xffffffffu) continue;
-                    const uint32_t slot = key[c] & 3u;
-                    if (sp >= S) {
-                        status |= STATUS_STACK_OVERFLOW;
-                        continue;
-                    }
-                    st_node[sp * BLOCK + tid] = sel4i(ch, slot);
-                    st_t[sp * BLOCK + tid] = sel4f(tn[0], tn[1], tn[2], tn[3], slot);
-                    ++sp;
-                }
-                const uint32_t kf = first == 0 ? key[0] : first == 1 ? key[1] : first == 2 ? key[2] : key[3];
-                node = sel4i(ch, kf & 3u);  // a leaf is handled at the next loop turn
+        for (int c = 3; c >= 0; --c) {
+            if (c == first || key[c] == 0xffffffffu) continue;
+            const uint32_t slot = key[c] & 3u;
+            if (st.sp >= kTraceStackTotal) {
+                status |= STATUS_STACK_OVERFLOW;
                 continue;
             }
-        } else if (node != -1) {
-            // ---- leaf: packed 0x80000000 | count << 27 | first
-            const uint32_t packed = (uint32_t)node;
-            const uint32_t count = (packed >> 27) & 15u;
-            const uint32_t first = packed & 0x07ffffffu;
-            for (uint32_t k = 0; k < count; ++k) {
-                if (COUNT) ++n_tris;
-                const QTri* tp = tris + first + k;
-                const float4 a = ldg4(&tp->v0), e1 = ldg4(&tp->e1), e2 = ldg4(&tp->e2);
-                float t, u, v;
-                if (tri_intersect_exact(ox, oy, oz, dx, dy, dz, a.x, a.y, a.z, e1.x, e1.y, e1.z, e2.x, e2.y, e2.z, t, u,
-                                        v)) {
-                    const int prim = __float_as_int(a.w);
-                    if (ANY) {
-                        if (t > tmin && t < tmax) {
-                            out_prim = prim;
-                            out_t = t;
-                            return;
-                        }
-                    } else if (t > tmin && (t < tbest || (t == tbest && prim < best))) {
-                        tbest = t;
-                        best = prim;
+            stack.push(st.sp, sel4i(ch, slot), sel4f(tn[0], tn[1], tn[2], tn[3], slot));
+            ++st.sp;
+        }
+        const uint32_t kf = first == 0 ? key[0] : first == 1 ? key[1] : first == 2 ? key[2] : key[3];
+        st.node = sel4i(ch, kf & 3u);
+    }
+    // ---- test the leaf, if one was reached: packed 0x80000000 | count << 27 | first
+    if (st.node != kNodeNone) {
+        const uint32_t packed = (uint32_t)st.node;
+        const uint32_t count = (packed >> 27) & 15u;
+        const uint32_t first = packed & 0x07ffffffu;
+        for (uint32_t k = 0; k < count; ++k) {
+            if (COUNT) ++n_tris;
+            const QTri* tp = tris + first + k;
+            const float4 a = ld_hint(&tp->v0, pol_tree), e1 = ld_hint(&tp->e1, pol_tree), e2 = ld_hint(&tp->e2, pol_tree);
+            float t, u, v;
+            if (tri_intersect_exact(st.ox, st.oy, st.oz, st.dx, st.dy, st.dz, a.x, a.y, a.z, e1.x, e1.y, e1.z, e2.x,
+                                    e2.y, e2.z, t, u, v)) {
+                const int prim = __float_as_int(a.w);
+                if (ANY) {
+                    if (t > st.tmin && t < st.tmax) {
+                        st.best = prim;
+                        st.tbest = t;
+                        return true;
                     }
+                } else if (t > st.tmin && (t < st.tbest || (t == st.tbest && prim < st.best))) {
+                    st.tbest = t;
+                    st.best = prim;
                 }
             }
         }
-        // ---- pop the next entry that can still contain a closer hit
-        bool found = false;
-        while (sp > 0) {
-            --sp;
-            const float te = st_t[sp * BLOCK + tid];
-            if (ANY || te <= tbest) {
-                node = st_node[sp * BLOCK + tid];
-                found = true;
-                break;
-            }
+    }
+    // ---- pop the next entry that can still hold a closer hit
+    while (st.sp > 0) {
+        --st.sp;
+        int nd;
+        float te;
+        stack.get(st.sp, nd, te);
+        if (ANY || te <= st.tbest) {
+            st.node = nd;
+            return false;
         }
-        if (!found) break;
     }
-    if (!ANY && best >= 0 && !(tbest > range_near(tmin))) best = -1;  // BoundedRay::inRange near side
-    out_prim = best;
-    out_t = best >= 0 ? tbest : INFINITY;
-    if (ANY) {
-        out_prim = -1;
-        out_t = INFINITY;
-    }
+    return true;
 }
 
 template <bool ANY, int S, int BLOCK, bool COUNT>
@@ -190,28 +235,82 @@ __global__ void __launch_bounds__(BLOCK) trace_kernel(const QNode* __restrict__ 
                                                       uint32_t n_rays, uint32_t* __restrict__ work_counter,
                                                       uint32_t* __restrict__ status_word,
                                                       TraceCounters* __restrict__ counters) {
+    constexpr uint32_t BATCH = 256;   // ray indices a warp takes from the global counter at once
+    constexpr int REFILL = 8;         // refill once this many lanes are idle
     extern __shared__ int trace_smem[];  // S * BLOCK node entries, then S * BLOCK distances
-    int* st_node = trace_smem;
-    float* st_t = reinterpret_cast<float*>(trace_smem + S * BLOCK);
-    const int lane = threadIdx.x & 31;
+    LaneStack<S, BLOCK> stack;
+    stack.s_node = trace_smem;
+    stack.s_t = reinterpret_cast<float*>(trace_smem + S * BLOCK);
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    const uint64_t pol_tree = policy_evict_last();
+    const uint64_t pol_stream = policy_evict_first();
     uint32_t status = 0, n_nodes = 0, n_tris = 0;
+
+    uint32_t w_next = 0, w_end = 0;  // the warp's current batch [w_next, w_end), uniform
+    bool exhausted = false;          // uniform: the global counter has passed n_rays
+    int rid = -1;                    // this lane's ray, -1 when idle
+    RayState st;
+
     while (true) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(work_counter, 32u);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= n_rays) break;
-        const uint32_t i = base + (uint32_t)lane;
-        if (i < n_rays) {
-            const float4* rp = reinterpret_cast<const float4*>(rays + i);
-            const float4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
-            int prim = -1;
-            float t = INFINITY;
-            const bool finite = isfinite(r0.x) && isfinite(r0.y) && isfinite(r0.z) && isfinite(r1.x) &&
-                                isfinite(r1.y) && isfinite(r1.z) && !isnan(r0.w) && !isnan(r1.w);
-            if (finite)
-                trace_one<ANY, S, BLOCK, COUNT>(nodes, tris, r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, st_node,
-                                                st_t, prim, t, status, n_nodes, n_tris);
-            reinterpret_cast<int2*>(hits)[i] = make_int2(prim, __float_as_int(t));
+        const uint32_t idle = __ballot_sync(0xffffffffu, rid < 0);
+        if (exhausted) {
+            if (idle == 0xffffffffu) break;
+        } else if ((uint32_t)__popc(idle) >= (uint32_t)REFILL) {
+            if (w_next >= w_end) {
+                uint32_t b = 0;
+                if (lane == 0) b = atomicAdd(work_counter, BATCH);
+                b = __shfl_sync(0xffffffffu, b, 0);
+                if (b >= n_rays) {
+                    exhausted = true;
+                } else {
+                    w_next = b;
+                    w_end = min(b + BATCH, n_rays);
+                }
+            }
+            if (!exhausted) {
+                const uint32_t avail = w_end - w_next;
+                const uint32_t rank = __popc(idle & lt_mask);
+                if (rid < 0 && rank < avail) {
+                    rid = (int)(w_next + rank);
+                    const float4* rp = reinterpret_cast<const float4*>(rays + rid);
+                    const float4 r0 = ld_hint(rp, pol_stream), r1 = ld_hint(rp + 1, pol_stream);
+                    st.ox = r0.x;
+                    st.oy = r0.y;
+                    st.oz = r0.z;
+                    st.tmin = r0.w;
+                    st.dx = r1.x;
+                    st.dy = r1.y;
+                    st.dz = r1.z;
+                    st.tmax = r1.w;
+                    st.idx = safe_rcp(st.dx);
+                    st.idy = safe_rcp(st.dy);
+                    st.idz = safe_rcp(st.dz);
+                    st.oix = st.ox * st.idx;
+                    st.oiy = st.oy * st.idy;
+                    st.oiz = st.oz * st.idz;
+                    // closest hit keeps candidates strictly below range_far(tmax); any hit below tmax
+                    st.tbest = ANY ? st.tmax : range_far(st.tmax);
+                    st.best = -1;
+                    st.sp = 0;
+                    const bool finite = isfinite(r0.x) && isfinite(r0.y) && isfinite(r0.z) && isfinite(r1.x) &&
+                                        isfinite(r1.y) && isfinite(r1.z) && !isnan(r0.w) && !isnan(r1.w);
+                    st.node = finite ? 0 : kNodeNone;
+                }
+                w_next += min(avail, (uint32_t)__popc(idle));
+            }
+        }
+        if (rid >= 0) {
+            const bool done = st.node == kNodeNone ||
+                              trace_step<ANY, S, BLOCK, COUNT>(nodes, tris, st, stack, pol_tree, status, n_nodes, n_tris);
+            if (done) {
+                int prim = st.best;
+                float t = st.tbest;
+                if (!ANY && prim >= 0 && !(t > range_near(st.tmin))) prim = -1;  // BoundedRay::inRange near side
+                if (prim < 0) t = INFINITY;
+                st_hint(hits + rid, prim, __float_as_int(t), pol_stream);
+                rid = -1;
+            }
         }
     }
     if (status) atomicOr(status_word, status);

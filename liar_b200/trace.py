@@ -46,6 +46,18 @@ class Context:
     def set_stream(self, stream_ptr: int | None) -> None:
         N.check(self._lib.liar_gpu_set_stream(self.handle, C.c_void_p(stream_ptr or 0)), self.handle)
 
+    @property
+    def trace_config(self) -> tuple[int, int]:
+        """(threads per block, shared-memory stack entries per lane) of the trace kernels."""
+        c = N.TraceConfig()
+        N.check(self._lib.liar_gpu_get_trace_config(self.handle, C.byref(c)), self.handle)
+        return c.block_size, c.smem_stack
+
+    @trace_config.setter
+    def trace_config(self, value: tuple[int, int]) -> None:
+        c = N.TraceConfig(int(value[0]), int(value[1]))
+        N.check(self._lib.liar_gpu_set_trace_config(self.handle, C.byref(c)), self.handle)
+
     def synchronize(self) -> None:
         N.check(self._lib.liar_gpu_synchronize(self.handle), self.handle)
 

@@ -157,3 +157,31 @@ def test_full_size_properties(gpu_ctx):
     s = np.random.default_rng(1).choice(len(r), 1 << 20, replace=False)
     pr, tr = oracle.Tree(v, f).trace(r[s])
     assert_same(p[s], t[s], pr, tr)
+
+
+@pytest.mark.parametrize("cfg", [(128, 8), (128, 16), (128, 24), (256, 8), (256, 16)])
+def test_every_launch_shape_matches_oracle(gpu_ctx, cfg):
+    """All trace kernel variants give identical results; the 8-entry shared stack makes deep rays
+    spill to local memory on the 1.3M-triangle mesh."""
+    v, f = scenes.displaced_icosphere(levels=8, seed=0)
+    mesh = Mesh(gpu_ctx, v, f)
+    r = scenes.random_rays(v, 1 << 18, seed=21)
+    # rays from the centre cross the whole sphere's subtree: deep stacks
+    r[::2, 0:3] = 0.0
+    old = gpu_ctx.trace_config
+    try:
+        gpu_ctx.trace_config = cfg
+        assert gpu_ctx.trace_config == cfg
+        p, t = mesh.intersect(r)
+        pa, _ = mesh.intersect(r, any_hit=True)
+    finally:
+        gpu_ctx.trace_config = old
+    pr, tr = oracle.Tree(v, f).trace(r)
+    assert_same(p, t, pr, tr)
+    np.testing.assert_array_equal(pa >= 0, oracle.Tree(v, f).trace(r, any_hit=True)[0] >= 0)
+
+
+def test_unsupported_launch_shape_is_rejected(gpu_ctx):
+    with pytest.raises(LiarGpuError, match="INVALID"):
+        gpu_ctx.trace_config = (96, 16)
+    assert gpu_ctx.trace_config == (128, 16)
