@@ -38,9 +38,9 @@ struct liar_gpu_ctx {
     size_t cap_rays = 0;
     void* d_hits = nullptr;
     size_t cap_hits = 0;
-    cudaStream_t pipe[kPipeSlots] = {};
+    cudaStream_t pipe[liar_gpu::kPipeSlots] = {};
     // pipe_ev[k]: end of slot k's work; pipe_ev[kPipeSlots]: start (work queued before the call)
-    cudaEvent_t pipe_ev[kPipeSlots + 1] = {};
+    cudaEvent_t pipe_ev[liar_gpu::kPipeSlots + 1] = {};
     // launch shape of the trace kernels (liar_gpu_set_trace_config) and cached occupancy per kernel
     liar_trace_config trace_cfg{128, 16};
     std::unordered_map<const void*, int> occupancy;
@@ -50,9 +50,9 @@ struct liar_gpu_ctx {
     void release_extensions() {
         for (auto it = on_destroy.rbegin(); it != on_destroy.rend(); ++it) (*it)();
         on_destroy.clear();
-        for (int k = 0; k < kPipeSlots; ++k)
+        for (int k = 0; k < liar_gpu::kPipeSlots; ++k)
             if (pipe[k]) cudaStreamDestroy(pipe[k]);
-        for (int k = 0; k <= kPipeSlots; ++k)
+        for (int k = 0; k <= liar_gpu::kPipeSlots; ++k)
             if (pipe_ev[k]) cudaEventDestroy(pipe_ev[k]);
     }
 };
