@@ -126,6 +126,109 @@ int liar_gpu_trace_counted_device(liar_gpu_ctx* ctx, const liar_gpu_mesh* mesh, 
                                   size_t n_rays, liar_hit* d_hits, int any_hit, unsigned long long* d_counters,
                                   void* stream);
 
+/* ---- spectral path tracing ------------------------------------------------------------------
+ * A flattened scene: one triangle soup (parallelograms arrive as two triangles, meshes as their
+ * triangles) whose triangles carry an object index; objects carry a material and a light. */
+
+typedef struct liar_gpu_scene liar_gpu_scene;
+
+/* Spectrum evaluated at one wavelength (metres), the reference's Spectral `Single` mode
+ * (src/liar/kernel/spectral.cpp:178-220). */
+enum liar_spectrum_type {
+    LIAR_SPEC_CONSTANT = 0,  /* p[0] */
+    LIAR_SPEC_SAMPLED = 1,   /* piecewise linear: pool[offset .. +count) wavelengths, then count values
+                                (spectra/sampled.cpp:128, kernel/spectral.cpp:185-210) */
+    LIAR_SPEC_BLACKBODY = 2, /* p[0] temperature (K), p[1] scale; normalised at the peak (spectra/black_body.cpp:55-118) */
+    LIAR_SPEC_CAUCHY = 3     /* p[0] + p[1] / lambda_um^2 (spectra/cauchy.cpp:72-76) */
+};
+typedef struct liar_spectrum {
+    int32_t type, offset, count;
+    float p[3];
+} liar_spectrum;
+
+/* Shaders (src/liar/shaders/). spec[] holds spectrum indices (-1 = absent):
+ *   LAMBERT        spec[0] diffuse                                   (lambert.cpp:105-124)
+ *   CONDUCTOR      spec[0] eta, spec[1] kappa, spec[2] reflectance   (conductor.cpp:179-196)
+ *   COOK_TORRANCE  spec[0] eta, spec[1] kappa, spec[2] reflectance, rough_u/v, mdf (cook_torrance.cpp:189-295)
+ *   DIELECTRIC     spec[0] inner ior, spec[1] outer ior, spec[2] reflectance, spec[3] transmittance (dielectric.cpp:148-245)
+ *   WALTER         as DIELECTRIC plus rough_u/v, mdf                   (walter.cpp:215-415)
+ *   MIRROR         spec[0] reflectance                                 (mirror.cpp)
+ *   NONE           no BSDF: rays pass through (AdjointPhotonTracer's null-shader branch)
+ * emission: spectrum of an Unshaded component (shaders/unshaded.cpp:77), -1 if none. */
+enum liar_material_type {
+    LIAR_MAT_NONE = 0, LIAR_MAT_LAMBERT = 1, LIAR_MAT_CONDUCTOR = 2, LIAR_MAT_COOK_TORRANCE = 3,
+    LIAR_MAT_DIELECTRIC = 4, LIAR_MAT_WALTER = 5, LIAR_MAT_MIRROR = 6
+};
+enum liar_mdf_type { LIAR_MDF_BECKMANN = 0, LIAR_MDF_GGX = 1 };
+typedef struct liar_material {
+    int32_t type, mdf;
+    int32_t spec[4];
+    int32_t emission;
+    float rough_u, rough_v;
+} liar_material;
+
+/* Lights (src/liar/scenery/light_*.cpp). AREA_PARALLELOGRAM: pos = support, u/v = sizes
+ * (light_area.cpp + parallelogram.cpp); AREA_MESH: triangles [first_tri, first_tri + n_tris) of
+ * the soup, area-CDF sampling (triangle_mesh.cpp:414-443); POINT: pos (light_point.cpp:160-196);
+ * SKY: constant radiance at a fixed far distance (light_sky.cpp:140-363). power is the
+ * light's total power used for the selection CDF (kernel/light_context.cpp:272-333). */
+enum liar_light_type { LIAR_LIGHT_AREA_PARALLELOGRAM = 0, LIAR_LIGHT_AREA_MESH = 1, LIAR_LIGHT_POINT = 2, LIAR_LIGHT_SKY = 3 };
+typedef struct liar_light {
+    int32_t type, spectrum, object, double_sided;
+    int32_t first_tri, n_tris;
+    float pos[3], u[3], v[3];
+    float power;
+} liar_light;
+
+typedef struct liar_scene_desc {
+    const float* vertices; size_t n_vertices;            /* n x 3 */
+    const uint32_t* triangles; size_t n_triangles;       /* n x 3 */
+    const int32_t* triangle_object;                      /* n: object of each triangle */
+    const float* normals; size_t n_normals;              /* optional shading normals (n x 3) */
+    const int32_t* triangle_normals;                     /* optional, n_triangles x 3 indices into normals */
+    const int32_t* object_material; const int32_t* object_light; size_t n_objects;
+    const liar_material* materials; size_t n_materials;
+    const liar_spectrum* spectra; size_t n_spectra;
+    const float* spectrum_pool; size_t pool_size;
+    const liar_light* lights; size_t n_lights;
+    const float* observer; size_t n_observer;            /* n x 4: wavelength (m), xbar, ybar, zbar */
+    float scene_radius;                                  /* bounding sphere radius (sky distance) */
+} liar_scene_desc;
+
+/* PerspectiveCamera (src/liar/cameras/perspective_camera.cpp:406-434): direction/right/down are
+ * the scaled vectors direction_ = focalLength * d, right_ = width * r, down_ = height * dn. */
+typedef struct liar_camera {
+    float position[3], direction[3], right[3], down[3];
+    float direction_normal[3], right_normal[3], down_normal[3];
+    float lens_radius, focus_distance, near_limit, far_limit;
+} liar_camera;
+
+enum liar_tracer_type { LIAR_TRACER_ADJOINT_PHOTON = 0 };
+typedef struct liar_render_desc {
+    liar_camera camera;
+    int32_t width, height, spp;
+    int32_t tracer;
+    int32_t max_ray_generation;  /* Russian roulette (survival 0.5) from this generation on (ray_tracer.cpp:171) */
+    int32_t max_depth;           /* hard cap on generations, 0 = none */
+    uint64_t seed;
+    int32_t first_sample;        /* progressive rendering: index of the first sample of this pass */
+    int32_t wave_paths;          /* paths in flight per wave, 0 = automatic */
+} liar_render_desc;
+
+/* Uploads the scene (builds the triangle tree). */
+int liar_gpu_scene_upload(liar_gpu_ctx* ctx, const liar_scene_desc* desc, liar_gpu_scene** out);
+void liar_gpu_scene_destroy(liar_gpu_scene* scene);
+/* Renders `spp` samples per pixel (AdjointPhotonTracer, src/liar/tracers/adjoint_photon_tracer.cpp:84-292,
+ * driven like RenderEngine::render, src/liar/kernel/render_engine.cpp:170-358) and ADDS them to
+ * film: width x height x 8 floats = sums of X, Y, Z, alpha, X^2, Y^2, Z^2 and the sample count
+ * (the reference's Raster accumulation, src/liar/output/raster.cpp:547-606, before division). */
+int liar_gpu_render(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_render_desc* desc, float* film);
+/* Same on a device film buffer, asynchronous on `stream`. */
+int liar_gpu_render_device(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_render_desc* desc,
+                           float* d_film, void* stream);
+/* Path statistics of the last render on ctx: [0] paths, [1] path segments traced, [2] rays that hit. */
+int liar_gpu_render_stats(const liar_gpu_ctx* ctx, unsigned long long* out3);
+
 /* Allocation-free closest hit / any hit. It has no counterpart in the reference; it exists for
  * callers that must not call cudaMalloc while they trace: an application whose own pool
  * allocator owns the device memory, a frame loop whose other streams would be stalled by the

@@ -80,6 +80,12 @@ SIGNATURES: dict[str, tuple] = {
     "liar_gpu_trace_device": (C.c_int, [_vp, _vp, _vp, _sz, _vp, C.c_int, _vp]),
     "liar_gpu_trace_counted_device": (C.c_int, [_vp, _vp, _vp, _sz, _vp, C.c_int, _vp, _vp]),
     "liar_gpu_trace_device_noalloc": (C.c_int, [_vp, _vp, _sz, _vp, C.c_int, _vp]),
+    # renderer (liar_b200/render.py rebinds these with its struct types)
+    "liar_gpu_scene_upload": (C.c_int, [_vp, _vp, C.POINTER(_vp)]),
+    "liar_gpu_scene_destroy": (None, [_vp]),
+    "liar_gpu_render": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "liar_gpu_render_device": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "liar_gpu_render_stats": (C.c_int, [_vp, _vp]),
 }
 
 

@@ -46,6 +46,8 @@ struct liar_gpu_ctx {
     std::unordered_map<const void*, int> occupancy;
     // resources of other subsystems (renderer, photon maps) register their release here
     std::vector<std::function<void()>> on_destroy;
+    // per-subsystem state (work buffers of the renderer, photon maps), looked up by name
+    std::vector<std::pair<std::string, void*>> extensions;
 
     void release_extensions() {
         for (auto it = on_destroy.rbegin(); it != on_destroy.rend(); ++it) (*it)();
@@ -79,6 +81,8 @@ inline int ctx_ensure_pipeline(liar_gpu_ctx* ctx) {
     return LIAR_OK;
 }
 
+int trace_mesh_internal(liar_gpu_ctx* ctx, const liar_gpu_mesh* mesh, const liar_ray* d_rays, size_t n,
+                        liar_hit* d_hits, int any_hit, cudaStream_t st, int counter_word);
 const QNode* mesh_nodes(const liar_gpu_mesh* m);
 const QTri* mesh_tris(const liar_gpu_mesh* m);
 uint32_t mesh_stack_needed(const liar_gpu_mesh* m);

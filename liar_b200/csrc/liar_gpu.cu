@@ -137,6 +137,16 @@ cudaStream_t pick_stream(liar_gpu_ctx* ctx, void* stream) {
 
 }  // namespace
 
+namespace liar_gpu {
+// entry for the other subsystems of the library (renderer, photon tracer): one launch on a
+// device ray buffer with the context's launch shape and the given work-counter word
+int trace_mesh_internal(liar_gpu_ctx* ctx, const liar_gpu_mesh* mesh, const liar_ray* d_rays, size_t n,
+                        liar_hit* d_hits, int any_hit, cudaStream_t st, int counter_word) {
+    return launch_trace(ctx, mesh, d_rays, n, d_hits, any_hit, nullptr, st, ctx->d_scratch + counter_word,
+                        ctx->d_scratch + kStatusWord);
+}
+}  // namespace liar_gpu
+
 // ------------------------------------------------------------------------------------------------
 // context
 

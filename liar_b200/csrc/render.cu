@@ -1,0 +1,794 @@
+// render.cu -- wavefront spectral path tracer (the reference's AdjointPhotonTracer) on sm_100a.
+//
+// Replaces RenderEngine::render's per-sample loop (src/liar/kernel/render_engine.cpp:170-358)
+// driving AdjointPhotonTracer::tracePhoton / shadeSurface / scatterSurface
+// (src/liar/tracers/adjoint_photon_tracer.cpp:84-292). The recursion becomes a wavefront:
+//
+//   raygen   one thread per path: stratified screen / wavelength samples, camera ray
+//            (PerspectiveCamera::doGenerateRay, cameras/perspective_camera.cpp:406-434),
+//            Observer::sample for the wavelength (kernel/observer.cpp:283-317)
+//   extend   the closest-hit trace kernel over the compacted ray queue
+//   shade    one thread per queue entry: emission, BSDF set-up at the wavelength, one-sample MIS
+//            between BSDF and light sampling, Russian roulette, then the next ray is appended
+//            to the output queue (one atomicAdd per warp: ballot + popc compaction); finished
+//            paths add their XYZ to the film
+//
+// The estimator is the reference's: there are no shadow rays; the light-sampling branch
+// continues the path toward the light and the emission is picked up when that ray hits it.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/liar_gpu.h"
+#include "ctx.h"
+#include "render_dev.cuh"
+
+using namespace liar_gpu;
+using namespace liar_gpu::rt;
+
+struct liar_gpu_scene {
+    int device = -1;
+    liar_gpu_mesh* mesh = nullptr;
+    std::vector<void*> buffers;  // device allocations owned by the scene
+    DScene d{};
+    size_t n_triangles = 0;
+};
+
+namespace {
+
+template <class T>
+int upload(liar_gpu_ctx* ctx, liar_gpu_scene* s, const T* host, size_t n, const T** dev, const char* what) {
+    *dev = nullptr;
+    if (n == 0) return LIAR_OK;
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return ctx_cuda(ctx, e, what);
+    }
+    s->buffers.push_back(p);
+    e = cudaMemcpy(p, host, n * sizeof(T), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return ctx_cuda(ctx, e, what);
+    *dev = static_cast<const T*>(p);
+    return LIAR_OK;
+}
+
+// ---- path state (structure of arrays, one entry per path of the wave)
+struct Paths {
+    float* lam;        // wavelength (m)
+    float* lam_pdf;    // its pdf
+    float* T;          // throughput
+    float* L;          // radiance gathered so far
+    float* alpha;      // 1 once the camera ray hit something
+    int32_t* gen;      // generation of the ray in flight
+};
+
+struct Queue {
+    liar_ray* rays;
+    uint32_t* path;
+    uint32_t* count;   // device counter
+};
+
+struct WaveParams {
+    liar_camera cam;
+    int width, height, spp, max_gen, max_depth;
+    uint64_t seed;
+    uint64_t first_path;   // global index of the wave's first path
+};
+
+__device__ __forceinline__ SampleKey key_of(const WaveParams& W, uint64_t gpath) {
+    SampleKey k;
+    k.seed = W.seed;
+    k.pixel = (uint32_t)(gpath / (uint64_t)W.spp);
+    k.sample = (uint32_t)(gpath % (uint64_t)W.spp);
+    k.spp = (uint32_t)W.spp;
+    return k;
+}
+
+// appends (ray, path) to q with one atomic per warp
+__device__ __forceinline__ void queue_push(const Queue& q, bool want, const liar_ray& r, uint32_t path) {
+    const uint32_t mask = __ballot_sync(0xffffffffu, want);
+    if (mask == 0) return;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(q.count, (uint32_t)__popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (want) {
+        const uint32_t slot = base + __popc(mask & ((1u << lane) - 1u));
+        float4* dst = reinterpret_cast<float4*>(q.rays + slot);
+        dst[0] = make_float4(r.ox, r.oy, r.oz, r.tmin);
+        dst[1] = make_float4(r.dx, r.dy, r.dz, r.tmax);
+        q.path[slot] = path;
+    }
+}
+
+__device__ void splat(const DScene& S, const WaveParams& W, float* film, uint64_t gpath, float lam, float lam_pdf,
+                      float L, float alpha, unsigned long long* stats) {
+    const uint32_t pixel = (uint32_t)(gpath / (uint64_t)W.spp);
+    float3 xyz = mk(0, 0, 0);
+    if (lam_pdf > 0.0f) {
+        // Spectral::xyz in Single mode: v / pdf * sensitivity(lambda) (kernel/spectral.cpp:212-220)
+        const float s = L / lam_pdf;
+        const float3 c = observer_sensitivity(S, lam);
+        xyz = mk(s * c.x, s * c.y, s * c.z);
+    }
+    float* f = film + 8 * (size_t)pixel;
+    atomicAdd(f + 0, xyz.x);
+    atomicAdd(f + 1, xyz.y);
+    atomicAdd(f + 2, xyz.z);
+    atomicAdd(f + 3, alpha);
+    atomicAdd(f + 4, xyz.x * xyz.x);
+    atomicAdd(f + 5, xyz.y * xyz.y);
+    atomicAdd(f + 6, xyz.z * xyz.z);
+    atomicAdd(f + 7, 1.0f);
+}
+
+__global__ void __launch_bounds__(256) k_raygen(DScene S, WaveParams W, Paths P, Queue out, uint32_t n_paths,
+                                                float* film, unsigned long long* stats) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool want = false;
+    liar_ray r{};
+    if (i < n_paths) {
+        const uint64_t g = W.first_path + i;
+        const SampleKey k = key_of(W, g);
+        const uint32_t px = k.pixel % (uint32_t)W.width, py = k.pixel / (uint32_t)W.width;
+        const float sx = ((float)px + sample_dim(k, DIM_SCREEN, true)) / (float)W.width;
+        const float sy = ((float)py + sample_dim(k, DIM_SCREEN + 1, true)) / (float)W.height;
+        float lpdf;
+        const float lam = observer_sample(S, sample_dim(k, DIM_LAMBDA, true), lpdf);
+        const liar_camera& C = W.cam;
+        float3 pos = mk(C.position[0], C.position[1], C.position[2]);
+        float3 dir = mk(C.direction[0], C.direction[1], C.direction[2]) +
+                     (sx - 0.5f) * mk(C.right[0], C.right[1], C.right[2]) +
+                     (sy - 0.5f) * mk(C.down[0], C.down[1], C.down[2]);
+        dir = normal(dir);
+        const float3 dn = mk(C.direction_normal[0], C.direction_normal[1], C.direction_normal[2]);
+        float factor = 1.0f / dot(dir, dn);
+        if (C.lens_radius > 0.0f && C.focus_distance > 0.0f && C.focus_distance < 3.4e38f) {
+            const float2 lens = concentric_disk(sample_dim(k, DIM_LENS, true), sample_dim(k, DIM_LENS + 1, true));
+            const float3 lp = pos + (C.lens_radius * lens.x) * mk(C.right_normal[0], C.right_normal[1], C.right_normal[2]) +
+                              (C.lens_radius * lens.y) * mk(C.down_normal[0], C.down_normal[1], C.down_normal[2]);
+            const float3 fp = pos + (factor * C.focus_distance) * dir;
+            pos = lp;
+            dir = normal(fp - lp);
+            factor = 1.0f / dot(dir, dn);
+        }
+        P.lam[i] = lam;
+        P.lam_pdf[i] = lpdf;
+        P.T[i] = 1.0f;
+        P.L[i] = 0.0f;
+        P.alpha[i] = 0.0f;
+        P.gen[i] = 0;
+        r = liar_ray{pos.x, pos.y, pos.z, fmaxf(kTol, factor * C.near_limit),
+                     dir.x, dir.y, dir.z, factor * C.far_limit};
+        want = true;
+    }
+    queue_push(out, want, r, i);
+}
+
+// the whole of tracePhoton after the intersection, for one queue entry
+__global__ void __launch_bounds__(128) k_shade(DScene S, WaveParams W, Paths P, Queue in, const liar_hit* hits,
+                                               uint32_t n_in, Queue out, float* film,
+                                               unsigned long long* stats) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    bool want = false;
+    liar_ray nr{};
+    uint32_t p = 0;
+    uint32_t n_hit = 0;
+    if (q < n_in) {
+        p = in.path[q];
+        const float4 r0 = reinterpret_cast<const float4*>(in.rays + q)[0];
+        const float4 r1 = reinterpret_cast<const float4*>(in.rays + q)[1];
+        const float3 o = mk(r0.x, r0.y, r0.z), d = mk(r1.x, r1.y, r1.z);
+        const liar_hit h = hits[q];
+        const uint64_t g = W.first_path + p;
+        const SampleKey key = key_of(W, g);
+        const int gen = P.gen[p];
+        float T = P.T[p], L = P.L[p];
+        const float lam = P.lam[p];
+        bool alive = false;
+        float3 next_o = mk(0, 0, 0), next_d = mk(0, 0, 1);
+        float next_tmin = kTol, next_tmax = INFINITY;
+
+        if (h.prim < 0) {
+            // the sky is an object at a fixed distance (LightSky::doIntersect)
+            if (S.sky_light >= 0 && S.sky_distance > r0.w * (1.0f + kTol) && S.sky_distance < r1.w * (1.0f - kTol)) {
+                if (gen == 0) P.alpha[p] = 1.0f;
+                if (gen > 0) L += T * spec_eval(S, S.lights[S.sky_light].spectrum, lam, false);
+                // no shader: the ray continues past the sky and finds nothing
+            }
+        } else {
+            ++n_hit;
+            if (gen == 0) P.alpha[p] = 1.0f;
+            const uint32_t prim = (uint32_t)h.prim;
+            const int obj = S.tri_obj[prim];
+            const int light = S.obj_light[obj];
+            const int mi = S.obj_mat[obj];
+            // ---- IntersectionContext: re-intersect the hit triangle (TriangleMesh::doLocalContext)
+            const uint32_t i0 = S.tri_idx[3 * prim], i1 = S.tri_idx[3 * prim + 1], i2 = S.tri_idx[3 * prim + 2];
+            const float3 a = mk(S.verts[3 * i0], S.verts[3 * i0 + 1], S.verts[3 * i0 + 2]);
+            const float3 b = mk(S.verts[3 * i1], S.verts[3 * i1 + 1], S.verts[3 * i1 + 2]);
+            const float3 c = mk(S.verts[3 * i2], S.verts[3 * i2 + 1], S.verts[3 * i2 + 2]);
+            const float3 e1 = b - a, e2 = c - a;
+            float tt, bu, bv;
+            if (!tri_intersect_exact(o.x, o.y, o.z, d.x, d.y, d.z, a.x, a.y, a.z, e1.x, e1.y, e1.z, e2.x, e2.y, e2.z, tt,
+                                     bu, bv)) {
+                bu = bv = 0.0f;
+            }
+            const float3 target = a + bu * e1 + bv * e2;
+            const float3 ng0 = normal(cross(e1, e2));
+            float3 ns = ng0;
+            if (S.tri_nrm) {
+                const int n0 = S.tri_nrm[3 * prim], n1 = S.tri_nrm[3 * prim + 1], n2 = S.tri_nrm[3 * prim + 2];
+                if (n0 >= 0 && n1 >= 0 && n2 >= 0) {
+                    const float w0 = 1.0f - bu - bv;
+                    ns = normal(w0 * mk(S.normals[3 * n0], S.normals[3 * n0 + 1], S.normals[3 * n0 + 2]) +
+                                bu * mk(S.normals[3 * n1], S.normals[3 * n1 + 1], S.normals[3 * n1 + 2]) +
+                                bv * mk(S.normals[3 * n2], S.normals[3 * n2 + 1], S.normals[3 * n2 + 2]));
+                }
+            }
+            // solid event from the unflipped geometric normal (triangle_mesh.cpp:303-308)
+            const float dd = dot(d, ng0);
+            const bool leaving = dd > 0.0f;
+            // flipTo(-direction) (kernel/intersection_context.cpp:278-290)
+            const float3 ng = dot(ng0, -d) < 0.0f ? -ng0 : ng0;
+            const float3 N = dot(ns, -d) < 0.0f ? -ns : ns;
+            if (gen > 0 && light >= 0) {
+                // LightArea::doEmission: radiance of the light object that was hit
+                L += T * spec_eval(S, S.lights[light].spectrum, lam, false);
+            }
+            if (mi < 0 || S.mats[mi].type == LIAR_MAT_NONE) {
+                if (mi >= 0 && light < 0 && S.mats[mi].emission >= 0) L += T * spec_eval(S, S.mats[mi].emission, lam, false);
+                // no BSDF: continue through (bound(ray, t + tolerance, far))
+                alive = true;
+                next_o = o;
+                next_d = d;
+                next_tmin = h.t + kTol;
+                next_tmax = r1.w;
+            } else {
+                const liar_material M = S.mats[mi];
+                if (light < 0 && M.emission >= 0) L += T * spec_eval(S, M.emission, lam, false);
+                // ---- shading frame (IntersectionContext::bsdfToLocal, intersection_context.cpp:197-222)
+                float3 u = e1 - dot(e1, N) * N;
+                float3 v = e2 - dot(e2, N) * N;
+                const float su = dot(u, u), sv = dot(v, v);
+                if (fmaxf(su, sv) < 1e-3f * fmaxf(dot(e1, e1), dot(e2, e2))) {
+                    const float3 ax = fabsf(N.x) < 0.9f ? mk(1, 0, 0) : mk(0, 1, 0);
+                    u = cross(ax, N);
+                    v = cross(N, u);
+                }
+                if (su >= sv) {
+                    u = normal(u);
+                    v = cross(N, u);
+                } else {
+                    v = normal(v);
+                    u = cross(v, N);
+                }
+                // ---- the BSDF at this wavelength (Shader::bsdf)
+                Bsdf B;
+                B.type = (uint32_t)M.type;
+                B.mdf = M.mdf;
+                B.ng = mk(dot(ng, u), dot(ng, v), dot(ng, N));
+                B.r = B.t = 0.0f;
+                B.eta = B.kappa = B.ior = B.eta_i = B.eta_t = 1.0f;
+                B.au = sqr(fmaxf(M.rough_u, 1e-3f));
+                B.av = sqr(fmaxf(M.rough_v, 1e-3f));
+                switch (M.type) {
+                    case LIAR_MAT_LAMBERT:
+                        B.caps = CAP_REFL | CAP_DIFF;
+                        B.r = spec_eval(S, M.spec[0], lam, true);
+                        break;
+                    case LIAR_MAT_CONDUCTOR:
+                    case LIAR_MAT_COOK_TORRANCE:
+                        B.caps = M.type == LIAR_MAT_CONDUCTOR ? (CAP_REFL | CAP_SPEC) : (CAP_REFL | CAP_GLOSSY);
+                        B.eta = fmaxf(spec_eval(S, M.spec[0], lam, false), 1e-9f);
+                        B.kappa = fmaxf(spec_eval(S, M.spec[1], lam, false), 1e-9f);
+                        B.r = spec_eval(S, M.spec[2], lam, true);
+                        break;
+                    case LIAR_MAT_DIELECTRIC: {
+                        B.caps = CAP_REFL | CAP_TRANS | CAP_SPEC;
+                        const float ior1 = fmaxf(spec_eval(S, M.spec[1], lam, false), 1e-9f);
+                        const float ior2 = fmaxf(spec_eval(S, M.spec[0], lam, false), 1e-9f);
+                        B.ior = leaving ? ior2 / ior1 : ior1 / ior2;
+                        B.r = spec_eval(S, M.spec[2], lam, true);
+                        B.t = spec_eval(S, M.spec[3], lam, true);
+                        break;
+                    }
+                    case LIAR_MAT_WALTER: {
+                        B.caps = CAP_TRANS | CAP_GLOSSY;  // as constructed by Walter::Bsdf (walter.cpp:247)
+                        float ei = fmaxf(spec_eval(S, M.spec[1], lam, false), 1e-9f);
+                        float et = fmaxf(spec_eval(S, M.spec[0], lam, false), 1e-9f);
+                        if (leaving) {
+                            const float tmp = ei;
+                            ei = et;
+                            et = tmp;
+                        }
+                        B.eta_i = ei;
+                        B.eta_t = et;
+                        B.r = spec_eval(S, M.spec[2], lam, true);
+                        B.t = spec_eval(S, M.spec[3], lam, true);
+                        break;
+                    }
+                    case LIAR_MAT_MIRROR:
+                        B.caps = CAP_REFL | CAP_SPEC;
+                        B.r = spec_eval(S, M.spec[0], lam, true);
+                        break;
+                    default:
+                        B.caps = 0;
+                }
+                const float3 md = -d;
+                float3 wi = mk(dot(md, u), dot(md, v), dot(md, N));
+                wi.z = fmaxf(wi.z, kEps);
+                // ---- scatterSurface: one-sample MIS (adjoint_photon_tracer.cpp:212-292)
+                const bool strat = gen < W.max_gen;
+                const uint32_t base = DIM_GEN0 + DIMS_PER_GEN * (uint32_t)gen;
+                const float strategy_pdf = (has_caps(B.caps, CAP_DIFF) || has_caps(B.caps, CAP_GLOSSY)) ? 0.5f : 1.0f;
+                BsdfSample out{mk(0, 0, 0), 0.0f, 0.0f};
+                bool ok = false;
+                if (sample_dim(key, base + OFF_STRATEGY, strat) < strategy_pdf) {
+                    out = bsdf_sample(B, wi, sample_dim(key, base + OFF_BSDF, strat),
+                                      sample_dim(key, base + OFF_BSDF + 1, strat),
+                                      sample_dim(key, base + OFF_COMPONENT, strat), CAP_ALL);
+                    if (out.ok()) {
+                        out.pdf *= strategy_pdf;
+                        const float3 wd = out.wo.x * u + out.wo.y * v + out.wo.z * N;
+                        float pl = 0.0f;
+                        for (int l = 0; l < S.n_lights; ++l) {
+                            const LightEmission e = light_emission(S, l, target, wd, lam);
+                            if (e.pdf > 0.0f) pl += light_choice_pdf(S, l) * e.pdf;
+                        }
+                        pl *= (1.0f - strategy_pdf);
+                        out.value *= power_heuristic(out.pdf, pl);
+                        ok = out.ok();
+                    }
+                } else if (S.n_lights > 0) {
+                    const float uc = sample_dim(key, base + OFF_LIGHT_CHOICE, strat);
+                    int k = lower_bound_f(S.light_cdf, S.n_lights, uc);
+                    if (k > S.n_lights - 1) k = S.n_lights - 1;
+                    const float pc = light_choice_pdf(S, k);
+                    if (pc > 0.0f) {
+                        const LightSample ls = light_sample(S, k, target, sample_dim(key, base + OFF_LIGHT, strat),
+                                                            sample_dim(key, base + OFF_LIGHT + 1, strat), lam);
+                        if (ls.pdf > 0.0f) {
+                            float pdf = pc * ls.pdf;
+                            for (int l = 0; l < S.n_lights; ++l) {
+                                if (l == k) continue;
+                                const LightEmission e = light_emission(S, l, target, ls.dir, lam);
+                                if (e.pdf > 0.0f) pdf += light_choice_pdf(S, l) * e.pdf;
+                            }
+                            pdf *= (1.0f - strategy_pdf);
+                            const float3 wo = mk(dot(ls.dir, u), dot(ls.dir, v), dot(ls.dir, N));
+                            const BsdfOut be = bsdf_evaluate(B, wi, wo, CAP_ALL);
+                            if (be.pdf > 0.0f && be.value != 0.0f) {
+                                out.wo = wo;
+                                out.value = be.value * power_heuristic(pdf, be.pdf * strategy_pdf);
+                                out.pdf = pdf;
+                                ok = out.ok();
+                            }
+                        }
+                    }
+                }
+                if (ok) {
+                    // shadeSurface continues along the scattered direction (adjoint_photon_tracer.cpp:170-186)
+                    const float cos_t = out.wo.z;
+                    next_o = target + ((cos_t > 0.0f ? 10.0f : -10.0f) * kTol) * ng;
+                    next_d = out.wo.x * u + out.wo.y * v + out.wo.z * N;
+                    next_tmin = kTol;
+                    next_tmax = INFINITY;
+                    T *= out.value * (fabsf(cos_t) / out.pdf);
+                    alive = true;
+                }
+            }
+        }
+        if (alive) {
+            const int ng1 = gen + 1;
+            if (W.max_depth > 0 && ng1 >= W.max_depth) {
+                alive = false;
+            } else if (ng1 >= W.max_gen) {
+                // Russian roulette at the start of tracePhoton (adjoint_photon_tracer.cpp:86-100)
+                const float ur = sample_dim(key, DIM_GEN0 + DIMS_PER_GEN * (uint32_t)ng1 + OFF_RR, false);
+                if (ur < 0.5f) T /= 0.5f;
+                else alive = false;
+            }
+        }
+        if (alive) {
+            P.T[p] = T;
+            P.L[p] = L;
+            P.gen[p] = gen + 1;
+            nr = liar_ray{next_o.x, next_o.y, next_o.z, next_tmin, next_d.x, next_d.y, next_d.z, next_tmax};
+            want = true;
+        } else {
+            splat(S, W, film, g, lam, P.lam_pdf[p], L, P.alpha[p], stats);
+        }
+    }
+    queue_push(out, want, nr, p);
+    // statistics: segments traced and hits
+    const uint32_t lane = threadIdx.x & 31u;
+    unsigned long long segs = (q < n_in) ? 1ull : 0ull, hh = n_hit;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        segs += __shfl_down_sync(0xffffffffu, segs, o);
+        hh += __shfl_down_sync(0xffffffffu, hh, o);
+    }
+    if (lane == 0 && segs) {
+        atomicAdd(stats + 1, segs);
+        atomicAdd(stats + 2, hh);
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------------
+
+namespace {
+
+struct RenderBuffers {
+    size_t cap = 0;
+    void* mem = nullptr;
+    Paths P{};
+    Queue q[2]{};
+    liar_hit* hits = nullptr;
+    unsigned long long* stats = nullptr;  // [0] paths [1] segments [2] hits
+    uint32_t* h_count = nullptr;          // pinned
+};
+
+RenderBuffers* render_buffers(liar_gpu_ctx* ctx) {
+    static_assert(sizeof(liar_ray) == 32, "ray layout");
+    for (auto& ext : ctx->extensions)
+        if (ext.first == "render") return static_cast<RenderBuffers*>(ext.second);
+    RenderBuffers* rb = new RenderBuffers();
+    ctx->extensions.emplace_back("render", rb);
+    ctx->on_destroy.push_back([rb]() {
+        if (rb->mem) cudaFree(rb->mem);
+        if (rb->stats) cudaFree(rb->stats);
+        if (rb->h_count) cudaFreeHost(rb->h_count);
+        delete rb;
+    });
+    return rb;
+}
+
+int ensure_render_buffers(liar_gpu_ctx* ctx, RenderBuffers* rb, size_t n) {
+    if (!rb->stats) {
+        cudaError_t e = cudaMalloc((void**)&rb->stats, 4 * sizeof(unsigned long long));
+        if (e == cudaSuccess) e = cudaMallocHost((void**)&rb->h_count, 2 * sizeof(uint32_t));
+        if (e != cudaSuccess) return ctx_cuda(ctx, e, "render statistics buffers");
+    }
+    if (rb->cap >= n) return LIAR_OK;
+    if (rb->mem) cudaFree(rb->mem);
+    rb->mem = nullptr;
+    rb->cap = 0;
+    // per path: 6 state words; per queue slot (x2): 32 B ray + 4 B path; hits 8 B; 2 counters
+    const size_t bytes = n * (6 * 4 + 2 * (32 + 4) + 8) + 1024;
+    cudaError_t e = cudaMalloc(&rb->mem, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return ctx_cuda(ctx, e, "render wave buffers");
+    }
+    char* p = static_cast<char*>(rb->mem);
+    auto take = [&](size_t b) {
+        char* r = p;
+        p += (b + 255) & ~size_t(255);
+        return r;
+    };
+    rb->q[0].rays = reinterpret_cast<liar_ray*>(take(n * 32));
+    rb->q[1].rays = reinterpret_cast<liar_ray*>(take(n * 32));
+    rb->hits = reinterpret_cast<liar_hit*>(take(n * 8));
+    rb->q[0].path = reinterpret_cast<uint32_t*>(take(n * 4));
+    rb->q[1].path = reinterpret_cast<uint32_t*>(take(n * 4));
+    rb->P.lam = reinterpret_cast<float*>(take(n * 4));
+    rb->P.lam_pdf = reinterpret_cast<float*>(take(n * 4));
+    rb->P.T = reinterpret_cast<float*>(take(n * 4));
+    rb->P.L = reinterpret_cast<float*>(take(n * 4));
+    rb->P.alpha = reinterpret_cast<float*>(take(n * 4));
+    rb->P.gen = reinterpret_cast<int32_t*>(take(n * 4));
+    rb->q[0].count = reinterpret_cast<uint32_t*>(take(4));
+    rb->q[1].count = reinterpret_cast<uint32_t*>(take(4));
+    rb->cap = n;
+    return LIAR_OK;
+}
+
+}  // namespace
+
+extern "C" int liar_gpu_scene_upload(liar_gpu_ctx* ctx, const liar_scene_desc* desc, liar_gpu_scene** out) {
+    if (!ctx || !desc || !out) return LIAR_ERR_INVALID;
+    *out = nullptr;
+    const liar_scene_desc& D = *desc;
+    if (!D.vertices || !D.triangles || !D.triangle_object || D.n_triangles == 0)
+        return ctx_fail(ctx, LIAR_ERR_INVALID, "scene has no triangles");
+    if (!D.object_material || !D.object_light || D.n_objects == 0) return ctx_fail(ctx, LIAR_ERR_INVALID, "scene has no objects");
+    if (!D.observer || D.n_observer < 2) return ctx_fail(ctx, LIAR_ERR_INVALID, "observer table needs two or more rows");
+    if (D.n_lights > 4096) return ctx_fail(ctx, LIAR_ERR_INVALID, "too many lights (limit 4096)");
+    // validation of every index the kernels follow
+    for (size_t k = 0; k < D.n_triangles; ++k) {
+        const int32_t o = D.triangle_object[k];
+        if (o < 0 || (size_t)o >= D.n_objects) return ctx_fail(ctx, LIAR_ERR_INVALID, "triangle %zu: object index out of range", k);
+        if (D.triangle_normals)
+            for (int c = 0; c < 3; ++c) {
+                const int32_t ni = D.triangle_normals[3 * k + c];
+                if (ni >= 0 && (size_t)ni >= D.n_normals)
+                    return ctx_fail(ctx, LIAR_ERR_INVALID, "triangle %zu: normal index out of range", k);
+            }
+    }
+    for (size_t k = 0; k < D.n_objects; ++k) {
+        const int32_t m = D.object_material[k], l = D.object_light[k];
+        if (m >= 0 && (size_t)m >= D.n_materials) return ctx_fail(ctx, LIAR_ERR_INVALID, "object %zu: material out of range", k);
+        if (l >= 0 && (size_t)l >= D.n_lights) return ctx_fail(ctx, LIAR_ERR_INVALID, "object %zu: light out of range", k);
+    }
+    auto spec_ok = [&](int32_t s) { return s >= -1 && s < (int32_t)D.n_spectra; };
+    for (size_t k = 0; k < D.n_materials; ++k) {
+        const liar_material& m = D.materials[k];
+        if (m.type < LIAR_MAT_NONE || m.type > LIAR_MAT_MIRROR) return ctx_fail(ctx, LIAR_ERR_INVALID, "material %zu: bad type", k);
+        for (int c = 0; c < 4; ++c)
+            if (!spec_ok(m.spec[c])) return ctx_fail(ctx, LIAR_ERR_INVALID, "material %zu: spectrum out of range", k);
+        if (!spec_ok(m.emission)) return ctx_fail(ctx, LIAR_ERR_INVALID, "material %zu: emission out of range", k);
+    }
+    std::vector<float> spec_max(D.n_spectra, 0.0f);
+    for (size_t k = 0; k < D.n_spectra; ++k) {
+        const liar_spectrum& s = D.spectra[k];
+        if (s.type == LIAR_SPEC_SAMPLED) {
+            if (s.count < 2 || s.offset < 0 || (size_t)s.offset + 2 * (size_t)s.count > D.pool_size)
+                return ctx_fail(ctx, LIAR_ERR_INVALID, "spectrum %zu: sampled table out of range", k);
+            float mx = -INFINITY;
+            for (int i = 0; i < s.count; ++i) mx = std::max(mx, D.spectrum_pool[s.offset + s.count + i]);
+            spec_max[k] = mx;
+        } else if (s.type < 0 || s.type > LIAR_SPEC_CAUCHY) {
+            return ctx_fail(ctx, LIAR_ERR_INVALID, "spectrum %zu: bad type", k);
+        }
+    }
+    int sky = -1;
+    std::vector<float> cdf(D.n_lights), area(D.n_lights, 0.0f), tri_cdf(D.n_triangles, 0.0f);
+    double total = 0.0;
+    for (size_t k = 0; k < D.n_lights; ++k) {
+        const liar_light& L = D.lights[k];
+        if (!spec_ok(L.spectrum) || L.spectrum < 0) return ctx_fail(ctx, LIAR_ERR_INVALID, "light %zu: spectrum out of range", k);
+        if (L.type == LIAR_LIGHT_SKY) {
+            if (sky >= 0) return ctx_fail(ctx, LIAR_ERR_UNSUPPORTED, "more than one sky light");
+            sky = (int)k;
+        } else if (L.type == LIAR_LIGHT_AREA_PARALLELOGRAM) {
+            const double ux = L.u[0], uy = L.u[1], uz = L.u[2], vx = L.v[0], vy = L.v[1], vz = L.v[2];
+            const double cx = uy * vz - uz * vy, cy = uz * vx - ux * vz, cz = ux * vy - uy * vx;
+            area[k] = (float)std::sqrt(cx * cx + cy * cy + cz * cz);
+        } else if (L.type == LIAR_LIGHT_AREA_MESH) {
+            if (L.first_tri < 0 || L.n_tris <= 0 || (size_t)L.first_tri + (size_t)L.n_tris > D.n_triangles)
+                return ctx_fail(ctx, LIAR_ERR_INVALID, "light %zu: triangle range out of range", k);
+            if (L.n_tris > 1024) return ctx_fail(ctx, LIAR_ERR_UNSUPPORTED, "light %zu: mesh lights hold at most 1024 triangles", k);
+            double acc = 0.0;
+            std::vector<double> ar(L.n_tris);
+            for (int i = 0; i < L.n_tris; ++i) {
+                const uint32_t* t = D.triangles + 3 * (size_t)(L.first_tri + i);
+                const float* a = D.vertices + 3 * t[0];
+                const float* b = D.vertices + 3 * t[1];
+                const float* c = D.vertices + 3 * t[2];
+                const double e1[3] = {(double)b[0] - a[0], (double)b[1] - a[1], (double)b[2] - a[2]};
+                const double e2[3] = {(double)c[0] - a[0], (double)c[1] - a[1], (double)c[2] - a[2]};
+                const double nx = e1[1] * e2[2] - e1[2] * e2[1], ny = e1[2] * e2[0] - e1[0] * e2[2],
+                             nz = e1[0] * e2[1] - e1[1] * e2[0];
+                ar[i] = 0.5 * std::sqrt(nx * nx + ny * ny + nz * nz);
+                acc += ar[i];
+            }
+            double run = 0.0;
+            for (int i = 0; i < L.n_tris; ++i) {
+                run += ar[i];
+                tri_cdf[L.first_tri + i] = (float)(run / acc);
+            }
+            area[k] = (float)acc;
+        } else if (L.type != LIAR_LIGHT_POINT) {
+            return ctx_fail(ctx, LIAR_ERR_INVALID, "light %zu: bad type", k);
+        }
+        total += std::max(0.0f, L.power);
+        cdf[k] = (float)total;
+    }
+    for (size_t k = 0; k < D.n_lights; ++k) cdf[k] = total > 0 ? (float)(cdf[k] / total) : (float)(k + 1) / D.n_lights;
+    // observer: normalise so that the Y of the unit spectrum is 1 and build the sampling CDF
+    // (Observer::Observer, kernel/observer.cpp:57-129)
+    const size_t no = D.n_observer;
+    std::vector<float> ow(no), oxyz(3 * no), odxyz(3 * no, 0.0f), ocdf(no);
+    {
+        std::vector<double> dX(3 * no);
+        double prev = D.observer[0];
+        ocdf[0] = 0.0f;
+        double acc = 0.0;
+        std::vector<double> cd(no, 0.0);
+        for (size_t k = 0; k + 1 < no; ++k) {
+            const double w = D.observer[4 * k], wn = D.observer[4 * (k + 1)];
+            if (!(wn > w)) return ctx_fail(ctx, LIAR_ERR_INVALID, "observer wavelengths must increase");
+            for (int c = 0; c < 3; ++c) {
+                odxyz[3 * k + c] = (float)((D.observer[4 * (k + 1) + 1 + c] - D.observer[4 * k + 1 + c]) / (wn - w));
+                dX[3 * k + c] = D.observer[4 * k + 1 + c] * ((wn - prev) / 2);
+            }
+            prev = w;
+            acc += (std::fabs(D.observer[4 * k + 1]) + std::fabs(D.observer[4 * k + 2]) + std::fabs(D.observer[4 * k + 3]) +
+                    std::fabs(D.observer[4 * (k + 1) + 1]) + std::fabs(D.observer[4 * (k + 1) + 2]) +
+                    std::fabs(D.observer[4 * (k + 1) + 3])) * (wn - w);
+            cd[k + 1] = acc;
+        }
+        const double wl = D.observer[4 * (no - 1)];
+        for (int c = 0; c < 3; ++c) dX[3 * (no - 1) + c] = D.observer[4 * (no - 1) + 1 + c] * ((wl - prev) / 2);
+        double Y = 0.0;
+        for (size_t k = 0; k < no; ++k) Y += dX[3 * k + 1];
+        if (!(Y > 0)) return ctx_fail(ctx, LIAR_ERR_INVALID, "observer has no luminance");
+        for (size_t k = 0; k < no; ++k) {
+            ow[k] = D.observer[4 * k];
+            for (int c = 0; c < 3; ++c) {
+                oxyz[3 * k + c] = (float)(D.observer[4 * k + 1 + c] / Y);
+                odxyz[3 * k + c] = (float)(odxyz[3 * k + c] / Y);
+            }
+            ocdf[k] = (float)(cd[k] / acc);
+        }
+        ocdf[no - 1] = 1.0f;
+    }
+
+    int rc = ctx_activate(ctx);
+    if (rc) return rc;
+    liar_gpu_scene* s = new (std::nothrow) liar_gpu_scene();
+    if (!s) return ctx_fail(ctx, LIAR_ERR_OOM, "host allocation");
+    s->device = ctx->device;
+    rc = liar_gpu_mesh_build(ctx, D.vertices, D.n_vertices, D.triangles, D.n_triangles, nullptr, &s->mesh);
+    DScene& d = s->d;
+    if (!rc) rc = upload(ctx, s, D.vertices, 3 * D.n_vertices, &d.verts, "scene vertices");
+    if (!rc) rc = upload(ctx, s, D.triangles, 3 * D.n_triangles, &d.tri_idx, "scene triangles");
+    if (!rc) rc = upload(ctx, s, D.triangle_object, D.n_triangles, &d.tri_obj, "triangle objects");
+    if (!rc && D.normals && D.triangle_normals) {
+        rc = upload(ctx, s, D.normals, 3 * D.n_normals, &d.normals, "normals");
+        if (!rc) rc = upload(ctx, s, D.triangle_normals, 3 * D.n_triangles, &d.tri_nrm, "triangle normals");
+    }
+    if (!rc) rc = upload(ctx, s, D.object_material, D.n_objects, &d.obj_mat, "object materials");
+    if (!rc) rc = upload(ctx, s, D.object_light, D.n_objects, &d.obj_light, "object lights");
+    if (!rc) rc = upload(ctx, s, D.materials, D.n_materials, &d.mats, "materials");
+    if (!rc) rc = upload(ctx, s, D.spectra, D.n_spectra, &d.specs, "spectra");
+    if (!rc) rc = upload(ctx, s, D.spectrum_pool, D.pool_size, &d.pool, "spectrum pool");
+    if (!rc) rc = upload(ctx, s, spec_max.data(), spec_max.size(), &d.spec_max, "spectrum maxima");
+    if (!rc) rc = upload(ctx, s, D.lights, D.n_lights, &d.lights, "lights");
+    if (!rc) rc = upload(ctx, s, cdf.data(), cdf.size(), &d.light_cdf, "light cdf");
+    if (!rc) rc = upload(ctx, s, area.data(), area.size(), &d.light_area, "light areas");
+    if (!rc) rc = upload(ctx, s, tri_cdf.data(), tri_cdf.size(), &d.tri_cdf, "mesh light cdf");
+    if (!rc) rc = upload(ctx, s, ow.data(), no, &d.obs_w, "observer");
+    if (!rc) rc = upload(ctx, s, oxyz.data(), 3 * no, &d.obs_xyz, "observer");
+    if (!rc) rc = upload(ctx, s, odxyz.data(), 3 * no, &d.obs_dxyz, "observer");
+    if (!rc) rc = upload(ctx, s, ocdf.data(), no, &d.obs_cdf, "observer");
+    if (rc) {
+        liar_gpu_scene_destroy(s);
+        return rc;
+    }
+    d.nodes = mesh_nodes(s->mesh);
+    d.qtris = mesh_tris(s->mesh);
+    d.n_lights = (int)D.n_lights;
+    d.n_obs = (int)no;
+    d.sky_light = sky;
+    // LightSky::doSetSceneBound: intersections with the sky lie 1000 scene radii away
+    d.sky_distance = D.scene_radius > 0 ? 1e3f * D.scene_radius : 1e3f;
+    d.stack_needed = mesh_stack_needed(s->mesh);
+    s->n_triangles = D.n_triangles;
+    *out = s;
+    return LIAR_OK;
+}
+
+extern "C" void liar_gpu_scene_destroy(liar_gpu_scene* s) {
+    if (!s) return;
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (s->device >= 0) cudaSetDevice(s->device);
+    for (void* p : s->buffers) cudaFree(p);
+    if (s->mesh) liar_gpu_mesh_destroy(s->mesh);
+    if (cur >= 0) cudaSetDevice(cur);
+    delete s;
+}
+
+namespace {
+
+int render_impl(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_render_desc* desc, float* d_film,
+                cudaStream_t st) {
+    const liar_render_desc& R = *desc;
+    if (R.width <= 0 || R.height <= 0 || R.spp <= 0) return ctx_fail(ctx, LIAR_ERR_INVALID, "empty image or no samples");
+    if (R.max_ray_generation < 0) return ctx_fail(ctx, LIAR_ERR_INVALID, "max_ray_generation must be >= 0");
+    if (R.tracer != LIAR_TRACER_ADJOINT_PHOTON) return ctx_fail(ctx, LIAR_ERR_UNSUPPORTED, "tracer %d", R.tracer);
+    const uint64_t total = (uint64_t)R.width * R.height * R.spp;
+    if ((uint64_t)R.width * R.height >= (1ull << 32)) return ctx_fail(ctx, LIAR_ERR_INVALID, "image too large");
+    uint64_t wave = R.wave_paths > 0 ? (uint64_t)R.wave_paths : (1ull << 22);
+    if (wave > total) wave = total;
+    RenderBuffers* rb = render_buffers(ctx);
+    int rc = ensure_render_buffers(ctx, rb, (size_t)wave);
+    if (rc) return rc;
+    cudaError_t e = cudaMemsetAsync(rb->stats, 0, 4 * sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return ctx_cuda(ctx, e, "reset statistics");
+    WaveParams W;
+    W.cam = R.camera;
+    W.width = R.width;
+    W.height = R.height;
+    W.spp = R.spp;
+    W.max_gen = R.max_ray_generation;
+    W.max_depth = R.max_depth;
+    W.seed = mix64(R.seed ^ mix64(0x51ed270b27ad0e0dull + (uint64_t)(uint32_t)R.first_sample));
+    const DScene& S = scene->d;
+    for (uint64_t first = 0; first < total; first += wave) {
+        const uint32_t n = (uint32_t)std::min<uint64_t>(wave, total - first);
+        W.first_path = first;
+        int cur = 0;
+        e = cudaMemsetAsync(rb->q[0].count, 0, 4, st);
+        if (e != cudaSuccess) return ctx_cuda(ctx, e, "reset queue");
+        k_raygen<<<(n + 255) / 256, 256, 0, st>>>(S, W, rb->P, rb->q[0], n, d_film, rb->stats);
+        uint32_t n_in = n;
+        for (int bounce = 0; n_in > 0; ++bounce) {
+            if (bounce > 4096) return ctx_fail(ctx, LIAR_ERR_TIMEOUT, "paths did not terminate after 4096 bounces");
+            rc = trace_mesh_internal(ctx, scene->mesh, rb->q[cur].rays, n_in, rb->hits, 0, st, kCounterWord + 8);
+            if (rc) return rc;
+            e = cudaMemsetAsync(rb->q[cur ^ 1].count, 0, 4, st);
+            if (e != cudaSuccess) return ctx_cuda(ctx, e, "reset queue");
+            k_shade<<<(n_in + 127) / 128, 128, 0, st>>>(S, W, rb->P, rb->q[cur], rb->hits, n_in, rb->q[cur ^ 1], d_film,
+                                                        rb->stats);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return ctx_cuda(ctx, e, "shade launch");
+            cur ^= 1;
+            e = cudaMemcpyAsync(rb->h_count, rb->q[cur].count, 4, cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) return ctx_cuda(ctx, e, "queue size");
+            n_in = rb->h_count[0];
+        }
+    }
+    // path count
+    unsigned long long paths = total;
+    e = cudaMemcpyAsync(rb->stats, &paths, sizeof(paths), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return ctx_cuda(ctx, e, "statistics");
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return ctx_cuda(ctx, e, "render synchronize");
+    return ctx_check_status(ctx);
+}
+
+}  // namespace
+
+extern "C" int liar_gpu_render_device(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_render_desc* desc,
+                                      float* d_film, void* stream) {
+    if (!ctx) return LIAR_ERR_INVALID;
+    if (!scene || !desc || !d_film) return ctx_fail(ctx, LIAR_ERR_INVALID, "null scene, description or film");
+    if (scene->device != ctx->device) return ctx_fail(ctx, LIAR_ERR_INVALID, "scene lives on another device");
+    int rc = ctx_activate(ctx);
+    if (rc) return rc;
+    return render_impl(ctx, scene, desc, d_film, stream ? (cudaStream_t)stream : ctx->stream);
+}
+
+extern "C" int liar_gpu_render(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_render_desc* desc,
+                               float* film) {
+    if (!ctx) return LIAR_ERR_INVALID;
+    if (!scene || !desc || !film) return ctx_fail(ctx, LIAR_ERR_INVALID, "null scene, description or film");
+    if (desc->width <= 0 || desc->height <= 0) return ctx_fail(ctx, LIAR_ERR_INVALID, "empty image");
+    int rc = ctx_activate(ctx);
+    if (rc) return rc;
+    const size_t bytes = (size_t)desc->width * desc->height * 8 * sizeof(float);
+    float* d_film = nullptr;
+    cudaError_t e = cudaMalloc((void**)&d_film, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return ctx_cuda(ctx, e, "film");
+    }
+    e = cudaMemcpyAsync(d_film, film, bytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) rc = render_impl(ctx, scene, desc, d_film, ctx->stream);
+    else rc = ctx_cuda(ctx, e, "film copy in");
+    if (!rc) {
+        e = cudaMemcpyAsync(film, d_film, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) rc = ctx_cuda(ctx, e, "film copy out");
+    }
+    cudaFree(d_film);
+    return rc;
+}
+
+extern "C" int liar_gpu_render_stats(const liar_gpu_ctx* ctx, unsigned long long* out3) {
+    if (!ctx || !out3) return LIAR_ERR_INVALID;
+    for (auto& ext : ctx->extensions)
+        if (ext.first == "render") {
+            RenderBuffers* rb = static_cast<RenderBuffers*>(ext.second);
+            if (!rb->stats) break;
+            if (cudaMemcpy(out3, rb->stats, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost) != cudaSuccess) {
+                cudaGetLastError();
+                return LIAR_ERR_CUDA;
+            }
+            return LIAR_OK;
+        }
+    out3[0] = out3[1] = out3[2] = 0;
+    return LIAR_OK;
+}

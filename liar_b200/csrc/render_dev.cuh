@@ -1,0 +1,637 @@
+// render_dev.cuh -- device-side shading of the spectral path tracer: spectra at one wavelength,
+// the observer, the per-pixel stratified sampler, BSDFs, lights. Used by render.cu.
+//
+// Everything here restates the reference's per-sample arithmetic in single precision:
+//   spectra    src/liar/kernel/spectral.cpp:178-220, spectra/sampled.cpp:128,
+//              spectra/black_body.cpp:44-118, spectra/cauchy.cpp:72-76
+//   observer   src/liar/kernel/observer.cpp:57-171, 283-317
+//   BSDFs      src/liar/kernel/bsdf.cpp:52-98 (caps filtering), shaders/lambert.cpp:105-124,
+//              conductor.cpp:179-196, cook_torrance.cpp:234-295, dielectric.cpp:148-245,
+//              walter.cpp:215-415, mirror.cpp:142-160, kernel/microfacet.cpp:56-122,
+//              shaders/microfacet_trowbridge_reitz.cpp:47-80, microfacet_beckmann.cpp:53-124
+//   lights     src/liar/scenery/light_area.cpp:189-288, light_point.cpp:160-196,
+//              light_sky.cpp:140-363, scenery/parallelogram.cpp, triangle_mesh.cpp:414-443,
+//              kernel/scene_object.cpp (area to solid-angle pdf, angularPdf),
+//              kernel/light_context.cpp:272-333 (power CDF)
+// Lass routines the reference calls (cosineHemisphere, uniformSphere, uniformDisk) are restated
+// from published methods: Malley's method on the Shirley-Chiu concentric disk mapping, the
+// Archimedes cylinder map for the sphere.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/liar_gpu.h"
+#include "qbvh.h"
+#include "tri_exact.h"
+
+namespace liar_gpu {
+namespace rt {
+
+constexpr float kPi = 3.14159265358979323846f;
+constexpr float kTol = 1e-6f;  // liar::tolerance (src/liar/kernel/kernel_common.cpp:32)
+constexpr float kEps = 1.19209290e-07f;  // numeric_limits<float>::epsilon
+
+enum : uint32_t { CAP_EMISSION = 0x1, CAP_REFL = 0x2, CAP_TRANS = 0x4, CAP_DIFF = 0x10, CAP_SPEC = 0x20,
+                  CAP_GLOSSY = 0x40, CAP_ALL = 0xff };
+
+__host__ __device__ __forceinline__ bool has_caps(uint32_t caps, uint32_t wanted) { return (caps & wanted) == wanted; }
+__host__ __device__ __forceinline__ bool compatible_caps(uint32_t caps, uint32_t allowed) {
+    const uint32_t o = caps & allowed;
+    return (o & 0xf) > 0 && (o & 0xf0) > 0;
+}
+
+// ---- small vector helpers
+__device__ __forceinline__ float3 mk(float x, float y, float z) { return make_float3(x, y, z); }
+__device__ __forceinline__ float3 operator+(float3 a, float3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 operator-(float3 a, float3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 operator-(float3 a) { return mk(-a.x, -a.y, -a.z); }
+__device__ __forceinline__ float3 operator*(float s, float3 a) { return mk(s * a.x, s * a.y, s * a.z); }
+__device__ __forceinline__ float dot(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 cross(float3 a, float3 b) {
+    return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float norm(float3 a) { return sqrtf(dot(a, a)); }
+__device__ __forceinline__ float3 normal(float3 a) { return (1.0f / norm(a)) * a; }
+__device__ __forceinline__ float sqr(float x) { return x * x; }
+__device__ __forceinline__ float lerpf(float a, float b, float t) { return a + t * (b - a); }
+// Lass Vector3D::reflect: mirror `v` about this (unit) normal h
+__device__ __forceinline__ float3 reflect_about(float3 h, float3 v) { return (2.0f * dot(h, v)) * h - v; }
+
+// ---- scene as the kernels see it
+struct DScene {
+    const QNode* nodes;
+    const QTri* qtris;
+    const float* verts;          // n x 3
+    const uint32_t* tri_idx;     // n x 3
+    const int32_t* tri_obj;
+    const float* normals;        // optional
+    const int32_t* tri_nrm;      // optional, n x 3
+    const int32_t* obj_mat;
+    const int32_t* obj_light;
+    const liar_material* mats;
+    const liar_spectrum* specs;
+    const float* pool;
+    const float* spec_max;       // per spectrum: max of a sampled spectrum's values (reflectant rescale)
+    const liar_light* lights;
+    const float* light_cdf;      // n_lights, normalised cumulative power
+    const float* light_area;     // n_lights
+    const float* tri_cdf;        // per triangle: cumulative area within its mesh light (normalised)
+    int n_lights;
+    const float* obs_w;          // n_obs
+    const float* obs_xyz;        // n_obs x 3, normalised so that Y of the unit spectrum is 1
+    const float* obs_dxyz;       // n_obs x 3, slope to the next sample
+    const float* obs_cdf;        // n_obs
+    int n_obs;
+    float sky_distance;
+    int sky_light;
+    uint32_t stack_needed;
+};
+
+// ---- spectra
+__device__ __forceinline__ float planck(float w, float T) {
+    const float h = 6.626070040e-34f, c = 299792458.0f, kb = 1.3806488e-23f;
+    const float c1 = 2 * h * c * c, c2 = h * c / kb;
+    const float w5 = sqr(sqr(w)) * w;
+    return c1 / (w5 * expm1f(c2 / (w * T)));
+}
+
+__device__ __forceinline__ int upper_bound_f(const float* a, int n, float x) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (a[mid] > x) hi = mid; else lo = mid + 1;
+    }
+    return lo;
+}
+__device__ __forceinline__ int lower_bound_f(const float* a, int n, float x) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (a[mid] < x) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+// value of spectrum idx at wavelength w (m); reflectant spectra are clamped / rescaled to <= 1
+// like Spectral(..., SpectralType::Reflectant) (src/liar/kernel/spectral.cpp:47-70, 185-210)
+__device__ float spec_eval(const DScene& S, int idx, float w, bool reflectant) {
+    if (idx < 0) return 0.0f;
+    const liar_spectrum sp = S.specs[idx];
+    float v;
+    switch (sp.type) {
+        case LIAR_SPEC_SAMPLED: {
+            const float* ws = S.pool + sp.offset;
+            const float* vs = ws + sp.count;
+            const int i = upper_bound_f(ws, sp.count, w);
+            if (i == 0 || i == sp.count) return 0.0f;
+            const float t = (w - ws[i - 1]) / (ws[i] - ws[i - 1]);
+            v = lerpf(vs[i - 1], vs[i], t);
+            if (reflectant) {
+                const float mx = S.spec_max[idx];
+                if (mx > 1.0f) return v / mx;
+            }
+            return v;
+        }
+        case LIAR_SPEC_BLACKBODY: {
+            const float T = sp.p[0];
+            const float inv_norm = 1.0f / planck(2.897771955e-3f / T, T);
+            v = sp.p[1] * inv_norm * planck(w, T);
+            break;
+        }
+        case LIAR_SPEC_CAUCHY: {
+            const float wu = w * 1e6f;
+            v = sp.p[0] + sp.p[1] / sqr(wu);
+            break;
+        }
+        default:
+            v = sp.p[0];
+    }
+    return reflectant ? fminf(v, 1.0f) : v;
+}
+
+// ---- observer
+__device__ float observer_sample(const DScene& S, float u, float& pdf) {
+    const int n = S.n_obs;
+    const int i = upper_bound_f(S.obs_cdf, n, u);
+    if (i == 0 || i == n) {
+        pdf = 0.0f;
+        return i == 0 ? S.obs_w[0] : S.obs_w[n - 1];
+    }
+    const float c1 = S.obs_cdf[i - 1], c2 = S.obs_cdf[i];
+    const float dc = c2 - c1;
+    const float x = (u - c1) / dc;
+    const float w1 = S.obs_w[i - 1], w2 = S.obs_w[i];
+    pdf = dc / (w2 - w1);
+    return lerpf(w1, w2, x);
+}
+
+__device__ float3 observer_sensitivity(const DScene& S, float w) {
+    const int i = upper_bound_f(S.obs_w, S.n_obs, w);
+    if (i == 0 || i == S.n_obs) return mk(0, 0, 0);
+    const int k = i - 1;
+    const float dw = w - S.obs_w[k];
+    return mk(S.obs_xyz[3 * k] + S.obs_dxyz[3 * k] * dw, S.obs_xyz[3 * k + 1] + S.obs_dxyz[3 * k + 1] * dw,
+              S.obs_xyz[3 * k + 2] + S.obs_dxyz[3 * k + 2] * dw);
+}
+
+// ---- sampler: per-pixel stratified dimensions (see sampler.h for the definition)
+}  // namespace rt
+}  // namespace liar_gpu
+
+#include "sampler.h"
+
+namespace liar_gpu {
+namespace rt {
+
+// Malley's method on the concentric disk (Shirley & Chiu 1997): cosine-weighted hemisphere
+__device__ __forceinline__ float2 concentric_disk(float u1, float u2) {
+    const float a = 2.0f * u1 - 1.0f, b = 2.0f * u2 - 1.0f;
+    if (a == 0.0f && b == 0.0f) return make_float2(0.0f, 0.0f);
+    float r, phi;
+    if (fabsf(a) > fabsf(b)) {
+        r = a;
+        phi = (kPi / 4) * (b / a);
+    } else {
+        r = b;
+        phi = (kPi / 2) - (kPi / 4) * (a / b);
+    }
+    return make_float2(r * cosf(phi), r * sinf(phi));
+}
+__device__ __forceinline__ float3 cosine_hemisphere(float u1, float u2, float& pdf) {
+    const float2 d = concentric_disk(u1, u2);
+    const float z = sqrtf(fmaxf(0.0f, 1.0f - d.x * d.x - d.y * d.y));
+    pdf = z / kPi;
+    return mk(d.x, d.y, z);
+}
+// Archimedes: z uniform in [-1, 1], phi uniform
+__device__ __forceinline__ float3 uniform_sphere(float u1, float u2, float& pdf) {
+    const float z = 1.0f - 2.0f * u2;
+    const float r = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+    const float phi = 2.0f * kPi * u1;
+    pdf = 1.0f / (4.0f * kPi);
+    return mk(r * cosf(phi), r * sinf(phi), z);
+}
+
+// ---- BSDFs in the shading frame (z = shading normal)
+struct Bsdf {
+    uint32_t type;
+    uint32_t caps;
+    int mdf;
+    float3 ng;          // geometric normal in the BSDF frame
+    float r;            // diffuse / reflectance at the wavelength
+    float t;            // transmittance (dielectrics)
+    float eta, kappa;   // conductors
+    float ior;          // dielectric: ratio used by DielectricBsdf
+    float eta_i, eta_t; // Walter
+    float au, av;       // microfacet alphas (roughness squared)
+};
+
+struct BsdfOut {
+    float value, pdf;
+};
+struct BsdfSample {
+    float3 wo;
+    float value, pdf;
+    __device__ bool ok() const { return pdf > 0.0f && value != 0.0f; }
+};
+
+__device__ __forceinline__ float power_heuristic(float a, float b) { return sqr(a) / (sqr(a) + sqr(b)); }
+
+// microfacet distributions
+__device__ float mdf_sample_phi(float s, float au, float av) {
+    if (au == av) return 2 * kPi * s;
+    const float phi = atanf(av / au * tanf(2 * kPi * s));
+    if (s <= 0.25f) return phi;
+    if (s < 0.75f) return phi + kPi;
+    return phi + 2 * kPi;
+}
+__device__ float mdf_D(int mdf, float3 h, float au, float av, float& pdfH) {
+    if (mdf == LIAR_MDF_GGX) {
+        const float d = 1.0f / (kPi * au * av * sqr(sqr(h.x / au) + sqr(h.y / av) + sqr(h.z)));
+        pdfH = d * h.z;
+        return d;
+    }
+    const float c2 = sqr(h.z);
+    if (c2 == 0.0f) {
+        pdfH = 0.0f;  // the reference leaves pdfH untouched here; zero keeps the sample invalid
+        return 0.0f;
+    }
+    const float d = expf(-(sqr(h.x / au) + sqr(h.y / av)) / c2) / (kPi * au * av * sqr(c2));
+    pdfH = d * h.z;
+    return d;
+}
+__device__ float3 mdf_sample_h(int mdf, float sx, float sy, float au, float av) {
+    if (mdf == LIAR_MDF_GGX) {
+        const float phi = mdf_sample_phi(sx, au, av);
+        const float s = sqrtf(sy / (1.0f - sy));
+        return normal(mk(s * au * cosf(phi), s * av * sinf(phi), 1.0f));
+    }
+    const float s = logf(1.0f - sx);
+    float cp, sp, tan2;
+    if (au == av) {
+        const float phi = 2 * kPi * sy;
+        cp = cosf(phi);
+        sp = sinf(phi);
+        tan2 = -s * sqr(au);
+    } else {
+        const float phi = mdf_sample_phi(sx, au, av);  // the reference reuses sample.x here
+        cp = cosf(phi);
+        sp = sinf(phi);
+        tan2 = -s / (sqr(cp / au) + sqr(sp / av));
+    }
+    const float c2 = 1.0f / (1.0f + tan2);
+    const float ct = sqrtf(c2);
+    const float st = sqrtf(fmaxf(1.0f - c2, 0.0f));
+    return mk(cp * st, sp * st, ct);
+}
+__device__ float mdf_lambda(int mdf, float3 w, float au, float av) {
+    if (mdf == LIAR_MDF_GGX) {
+        const float inv_a2 = (sqr(w.x * au) + sqr(w.y * av)) / sqr(w.z);
+        return (sqrtf(1.0f + inv_a2) - 1.0f) / 2.0f;
+    }
+    // the reference's Beckmann Lambda returns this rational fit (microfacet_beckmann.cpp:110-124)
+    const float a2 = sqr(w.z) / (sqr(w.x * au) + sqr(w.y * av));
+    const float a = sqrtf(a2);
+    return a < 1.6f ? (3.535f * a + 2.181f * a2) / (1.0f + 2.276f * a + 2.577f * a2) : 1.0f;
+}
+__device__ float mdf_G1(int mdf, float3 w, float3 h, float au, float av) {
+    if (dot(w, h) * w.z <= 0.0f) return 0.0f;
+    return 1.0f / (1.0f + mdf_lambda(mdf, w, au, av));
+}
+
+__device__ float fresnel_conductor(float eta, float kappa, float cosI) {
+    const float c2 = sqr(cosI);
+    const float a = sqr(eta) + sqr(kappa);
+    const float b = (2 * cosI) * eta;
+    const float aO = a + c2, aP = a * c2 + 1;
+    return ((aO - b) / (aO + b) + (aP - b) / (aP + b)) / 2;
+}
+__device__ float fresnel_dielectric_walter(float ior, float3 wi, float3 h) {
+    const float cosI = fabsf(dot(wi, h));
+    const float sinT2 = sqr(ior) * (1 - sqr(cosI));
+    const float cosT = sqrtf(fmaxf(1 - sinT2, 0.0f));
+    const float rO = (ior * cosI - cosT) / (ior * cosI + cosT);
+    const float rP = (cosI - ior * cosT) / (cosI + ior * cosT);
+    return fminf((sqr(rO) + sqr(rP)) / 2, 1.0f);
+}
+__device__ float walter_pdf_reflection(const Bsdf& b, float rF, uint32_t allowed) {
+    const float pr = has_caps(allowed, CAP_REFL | CAP_GLOSSY) ? fabsf(b.r) * rF : 0.0f;
+    const float pt = has_caps(allowed, CAP_TRANS | CAP_GLOSSY) ? fabsf(b.t) * (1 - rF) : 0.0f;
+    const float tot = pr + pt;
+    if (tot == 0.0f) return -1.0f;
+    return pr / tot;
+}
+
+__device__ BsdfOut bsdf_do_evaluate(const Bsdf& b, float3 wi, float3 wo, uint32_t allowed) {
+    BsdfOut out{0.0f, 0.0f};
+    switch (b.type) {
+        case LIAR_MAT_LAMBERT: {
+            const float c = fabsf(wo.z);
+            if (c <= 0.0f) return out;
+            return BsdfOut{b.r / kPi, c / kPi};
+        }
+        case LIAR_MAT_COOK_TORRANCE: {
+            if (wo.z <= 0.0f) return out;
+            const float3 h = normal(wi + wo);
+            float pdfH;
+            const float d = mdf_D(b.mdf, h, b.au, b.av, pdfH);
+            const float dh = fabsf(dot(wi, h));
+            const float g = fminf(1.0f, fminf(2 * h.z * wi.z / dh, 2 * h.z * wo.z / dh));
+            const float pdf = pdfH / (4 * dot(wi, h));
+            float v = b.r * (d * g / (4 * wi.z * wo.z));
+            v *= fresnel_conductor(b.eta, b.kappa, fabsf(dot(wi, h)));
+            return BsdfOut{v, pdf};
+        }
+        case LIAR_MAT_WALTER: {
+            if (wo.z > 0.0f) {
+                const float3 h = normal(wi + wo);
+                const float rF = fresnel_dielectric_walter(b.eta_i / b.eta_t, wi, h);
+                const float pR = walter_pdf_reflection(b, rF, allowed);
+                if (pR < 0.0f) return out;
+                float pdfH;
+                const float d = mdf_D(b.mdf, h, b.au, b.av, pdfH);
+                const float g = mdf_G1(b.mdf, wi, h, b.au, b.av) * mdf_G1(b.mdf, wo, h, b.au, b.av);
+                const float dh = 1.0f / (4 * dot(wi, h));
+                return BsdfOut{b.r * (rF * d * g / (4 * wi.z * wo.z)), pR * pdfH * dh};
+            } else if (wo.z < 0.0f) {
+                const float3 h = normal(-(b.eta_i * wi) - b.eta_t * wo);
+                if (h.z <= 0.0f) return out;
+                const float cI = fabsf(dot(wi, h)), cT = fabsf(dot(wo, h));
+                const float rF = fresnel_dielectric_walter(b.eta_i / b.eta_t, wi, h);
+                const float pR = walter_pdf_reflection(b, rF, allowed);
+                if (pR < 0.0f) return out;
+                float pdfH;
+                const float d = mdf_D(b.mdf, h, b.au, b.av, pdfH);
+                const float g = mdf_G1(b.mdf, wi, h, b.au, b.av) * mdf_G1(b.mdf, wo, h, b.au, b.av);
+                const float dh = sqr(b.eta_t) * cT / sqr(b.eta_i * cI + b.eta_t * cT);
+                return BsdfOut{b.t * (((1 - rF) * d * g * (cI * dh)) / fabsf(wi.z * wo.z)), (1 - pR) * pdfH * dh};
+            }
+            return out;
+        }
+        default:  // specular BSDFs have no finite density
+            return out;
+    }
+}
+
+// Bsdf::evaluate: reject wo in the plane, drop the caps that the geometric normal rules out
+__device__ BsdfOut bsdf_evaluate(const Bsdf& b, float3 wi, float3 wo, uint32_t allowed) {
+    if (wo.z == 0.0f) return BsdfOut{0.0f, 0.0f};
+    const bool reflective = (dot(wi, b.ng) > 0.0f) == (dot(wo, b.ng) > 0.0f);
+    allowed &= ~(reflective ? CAP_TRANS : CAP_REFL);
+    if (!compatible_caps(b.caps, allowed)) return BsdfOut{0.0f, 0.0f};
+    return bsdf_do_evaluate(b, wi, wo, allowed);
+}
+
+__device__ BsdfSample bsdf_sample(const Bsdf& b, float3 wi, float sx, float sy, float comp, uint32_t allowed) {
+    BsdfSample out{mk(0, 0, 0), 0.0f, 0.0f};
+    if (!compatible_caps(b.caps, allowed)) return out;
+    switch (b.type) {
+        case LIAR_MAT_LAMBERT: {
+            float pdf;
+            out.wo = cosine_hemisphere(sx, sy, pdf);
+            out.pdf = pdf;
+            out.value = b.r / kPi;
+            return out;
+        }
+        case LIAR_MAT_CONDUCTOR: {
+            const float cosI = wi.z;
+            out.wo = mk(-wi.x, -wi.y, wi.z);
+            out.value = b.r * fresnel_conductor(b.eta, b.kappa, cosI) / cosI;
+            out.pdf = 1.0f;
+            return out;
+        }
+        case LIAR_MAT_MIRROR: {
+            out.wo = mk(-wi.x, -wi.y, wi.z);
+            out.value = b.r;
+            out.pdf = out.wo.z;
+            return out;
+        }
+        case LIAR_MAT_COOK_TORRANCE: {
+            const float3 h = mdf_sample_h(b.mdf, sx, sy, b.au, b.av);
+            const float3 wo = reflect_about(h, wi);
+            if (wo.z <= 0.0f) return out;
+            const BsdfOut e = bsdf_do_evaluate(b, wi, wo, allowed);
+            out.wo = wo;
+            out.value = e.value;
+            out.pdf = e.pdf;
+            return out;
+        }
+        case LIAR_MAT_DIELECTRIC: {
+            const float cosI = wi.z;
+            if (cosI <= 0.0f) return out;
+            const float ior = b.ior;
+            const float sinT2 = sqr(ior) * (1 - sqr(cosI));
+            const float cosT = sqrtf(fmaxf(1 - sinT2, 0.0f));
+            const float rO = (ior * cosI - cosT) / (ior * cosI + cosT);
+            const float rP = (cosI - ior * cosT) / (cosI + ior * cosT);
+            const float rF = (sqr(rO) + sqr(rP)) / 2;
+            const float pr = has_caps(allowed, CAP_REFL | CAP_SPEC) ? fabsf(b.r) * rF : 0.0f;
+            const float pt = has_caps(allowed, CAP_TRANS | CAP_SPEC) ? fabsf(b.t) * (1 - rF) : 0.0f;
+            if (pr + pt == 0.0f) return out;
+            const float probR = pr / (pr + pt);
+            if (comp < probR) {
+                out.wo = mk(-wi.x, -wi.y, wi.z);
+                out.value = b.r * rF / cosI;
+                out.pdf = probR;
+            } else {
+                out.wo = mk(-ior * wi.x, -ior * wi.y, -cosT);
+                out.value = b.t * (1 - rF) / cosT;
+                out.pdf = 1 - probR;
+            }
+            return out;
+        }
+        case LIAR_MAT_WALTER: {
+            const float3 h = mdf_sample_h(b.mdf, sx, sy, b.au, b.av);
+            float pdfH;
+            const float d = mdf_D(b.mdf, h, b.au, b.av, pdfH);
+            const float rF = fresnel_dielectric_walter(b.eta_i / b.eta_t, wi, h);
+            const float pR = walter_pdf_reflection(b, rF, allowed);
+            if (pR < 0.0f) return out;
+            if (comp < pR) {
+                const float3 wo = reflect_about(h, wi);
+                if (wo.z <= 0.0f) return out;
+                const float g = mdf_G1(b.mdf, wi, h, b.au, b.av) * mdf_G1(b.mdf, wo, h, b.au, b.av);
+                const float dh = 1.0f / (4 * dot(wo, h));
+                out.wo = wo;
+                out.pdf = pR * pdfH * dh;
+                out.value = b.r * (rF * d * g / (4 * wi.z * wo.z));
+            } else {
+                const float eta = b.eta_i / b.eta_t;
+                const float cI = fabsf(dot(wi, h));
+                const float s2 = sqr(eta) * (1 - sqr(cI));
+                const float cT = sqrtf(fmaxf(1 - s2, 0.0f));
+                const float3 wo = normal((-eta) * wi + (eta * cI - cT) * h);
+                if (wo.z >= 0.0f) return out;
+                const float g = mdf_G1(b.mdf, wi, h, b.au, b.av) * mdf_G1(b.mdf, wo, h, b.au, b.av);
+                const float dh = sqr(b.eta_t) * cT / sqr(b.eta_i * cI + b.eta_t * cT);
+                out.wo = wo;
+                out.pdf = (1 - pR) * pdfH * dh;
+                out.value = b.t * (((1 - rF) * d * g * (cI * dh)) / fabsf(wi.z * wo.z));
+            }
+            return out;
+        }
+        default:
+            return out;
+    }
+}
+
+// ---- lights
+struct LightEmission {
+    float value;   // radiance (unused by the light-sampling pdf sums)
+    float pdf;     // solid-angle pdf of sampling this direction on this light
+    float t;       // distance along the ray
+};
+
+// Parallelogram ray test (two-sided) for the light's surface; t in units of |d|, t > tmin
+__device__ bool parallelogram_hit(const liar_light& L, float3 o, float3 d, float tmin, float& t) {
+    const float3 p = mk(L.pos[0], L.pos[1], L.pos[2]), u = mk(L.u[0], L.u[1], L.u[2]), v = mk(L.v[0], L.v[1], L.v[2]);
+    const float3 n = cross(u, v);
+    const float den = dot(n, d);
+    if (den == 0.0f) return false;
+    const float th = dot(n, p - o) / den;
+    if (!(th > tmin)) return false;
+    const float3 x = o + th * d - p;
+    // coordinates in the (u, v) basis
+    const float uu = dot(u, u), uv = dot(u, v), vv = dot(v, v);
+    const float xu = dot(x, u), xv = dot(x, v);
+    const float det = uu * vv - uv * uv;
+    const float a = (xu * vv - xv * uv) / det, b = (xv * uu - xu * uv) / det;
+    if (a < 0.0f || a > 1.0f || b < 0.0f || b > 1.0f) return false;
+    t = th;
+    return true;
+}
+
+// SceneLight::emission for a ray leaving `o` along unit `d` (LightArea::doEmission ->
+// SceneObject::doAngularPdf: t^2 / |A cos|; the single-sided test sees a normal already flipped
+// toward the ray's origin, so hits are accepted from both sides)
+__device__ LightEmission light_emission(const DScene& S, int li, float3 o, float3 d, float lambda) {
+    LightEmission e{0.0f, 0.0f, INFINITY};
+    const liar_light L = S.lights[li];
+    if (L.type == LIAR_LIGHT_AREA_PARALLELOGRAM) {
+        float t;
+        if (!parallelogram_hit(L, o, d, kTol, t)) return e;
+        const float3 n = normal(cross(mk(L.u[0], L.u[1], L.u[2]), mk(L.v[0], L.v[1], L.v[2])));
+        e.pdf = sqr(t) / fabsf(S.light_area[li] * dot(d, n));
+        e.t = t;
+        e.value = spec_eval(S, L.spectrum, lambda, false);
+        return e;
+    }
+    if (L.type == LIAR_LIGHT_AREA_MESH) {
+        float tbest = INFINITY;
+        int best = -1;
+        for (int k = 0; k < L.n_tris; ++k) {
+            const int ti = L.first_tri + k;
+            const float* a = S.verts + 3 * S.tri_idx[3 * ti];
+            const float* b = S.verts + 3 * S.tri_idx[3 * ti + 1];
+            const float* c = S.verts + 3 * S.tri_idx[3 * ti + 2];
+            float t, uu, vv;
+            if (tri_intersect_exact(o.x, o.y, o.z, d.x, d.y, d.z, a[0], a[1], a[2], b[0] - a[0], b[1] - a[1],
+                                    b[2] - a[2], c[0] - a[0], c[1] - a[1], c[2] - a[2], t, uu, vv) &&
+                t > kTol && t < tbest) {
+                tbest = t;
+                best = ti;
+            }
+        }
+        if (best < 0) return e;
+        const float* a = S.verts + 3 * S.tri_idx[3 * best];
+        const float* b = S.verts + 3 * S.tri_idx[3 * best + 1];
+        const float* c = S.verts + 3 * S.tri_idx[3 * best + 2];
+        const float3 n = normal(cross(mk(b[0] - a[0], b[1] - a[1], b[2] - a[2]), mk(c[0] - a[0], c[1] - a[1], c[2] - a[2])));
+        e.pdf = sqr(tbest) / fabsf(S.light_area[li] * dot(d, n));
+        e.t = tbest;
+        e.value = spec_eval(S, L.spectrum, lambda, false);
+        return e;
+    }
+    if (L.type == LIAR_LIGHT_SKY) {
+        e.pdf = 1.0f / (4.0f * kPi);
+        e.t = S.sky_distance;
+        e.value = spec_eval(S, L.spectrum, lambda, false);
+        return e;
+    }
+    return e;  // point lights are never hit
+}
+
+struct LightSample {
+    float3 dir;
+    float dist;
+    float pdf;
+    float value;
+};
+
+// SceneLight::sampleEmission(sample, lightSample, target, shadowRay, pdf)
+__device__ LightSample light_sample(const DScene& S, int li, float3 target, float sx, float sy, float lambda) {
+    LightSample out{mk(0, 0, 1), 0.0f, 0.0f, 0.0f};
+    const liar_light L = S.lights[li];
+    if (L.type == LIAR_LIGHT_AREA_PARALLELOGRAM || L.type == LIAR_LIGHT_AREA_MESH) {
+        float3 p, n;
+        float pdf;
+        if (L.type == LIAR_LIGHT_AREA_PARALLELOGRAM) {
+            const float3 u = mk(L.u[0], L.u[1], L.u[2]), v = mk(L.v[0], L.v[1], L.v[2]);
+            p = mk(L.pos[0], L.pos[1], L.pos[2]) + sx * u + sy * v;
+            n = normal(cross(u, v));
+            pdf = 1.0f / S.light_area[li];
+        } else {
+            // TriangleMesh::doSampleSurface: pick a triangle by area, then a uniform point on it
+            const float* cdf = S.tri_cdf + L.first_tri;
+            int ii = lower_bound_f(cdf, L.n_tris, sx);
+            if (ii > L.n_tris - 1) ii = L.n_tris - 1;
+            const float i0 = ii > 0 ? cdf[ii - 1] : 0.0f;
+            const float tpdf = cdf[ii] - i0;
+            const float di = (sx - i0) / tpdf;
+            const int ti = L.first_tri + ii;
+            const float* a = S.verts + 3 * S.tri_idx[3 * ti];
+            const float* b = S.verts + 3 * S.tri_idx[3 * ti + 1];
+            const float* c = S.verts + 3 * S.tri_idx[3 * ti + 2];
+            const float3 A = mk(a[0], a[1], a[2]);
+            const float3 e1 = mk(b[0] - a[0], b[1] - a[1], b[2] - a[2]), e2 = mk(c[0] - a[0], c[1] - a[1], c[2] - a[2]);
+            const float3 nn = cross(e1, e2);
+            const float s = sqrtf(di);
+            const float uu = 1.0f - s, vv = s * sy;
+            const float nl = norm(nn);
+            n = (1.0f / nl) * nn;
+            pdf = tpdf / (nl / 2);
+            p = A + uu * e1 + vv * e2;
+        }
+        // SceneObject::doSampleSurface(sample, target, ...): area pdf to solid angle
+        float3 to = p - target;
+        const float d2 = dot(to, to);
+        to = (1.0f / sqrtf(d2)) * to;
+        pdf *= d2 / fabsf(dot(n, to));
+        // LightArea::doSampleEmission
+        float3 tl = p - target;
+        const float dist = norm(tl);
+        tl = (1.0f / dist) * tl;
+        out.dir = tl;
+        out.dist = dist;
+        if (!L.double_sided && dot(n, tl) > 0.0f) return out;  // target behind a single-sided light
+        out.pdf = pdf;
+        out.value = spec_eval(S, L.spectrum, lambda, false);
+        return out;
+    }
+    if (L.type == LIAR_LIGHT_POINT) {
+        float3 tl = mk(L.pos[0], L.pos[1], L.pos[2]) - target;
+        const float d2 = dot(tl, tl);
+        const float dist = sqrtf(d2);
+        out.dir = (1.0f / dist) * tl;
+        out.dist = dist;
+        out.pdf = 1.0f;
+        out.value = spec_eval(S, L.spectrum, lambda, false) / d2;  // default attenuation 1/d^2
+        return out;
+    }
+    if (L.type == LIAR_LIGHT_SKY) {
+        float pdf;
+        out.dir = uniform_sphere(sx, sy, pdf);
+        out.dist = S.sky_distance;
+        out.pdf = pdf;
+        out.value = spec_eval(S, L.spectrum, lambda, false);
+        return out;
+    }
+    return out;
+}
+
+__device__ __forceinline__ float light_choice_pdf(const DScene& S, int k) {
+    return k > 0 ? S.light_cdf[k] - S.light_cdf[k - 1] : S.light_cdf[0];
+}
+
+}  // namespace rt
+}  // namespace liar_gpu

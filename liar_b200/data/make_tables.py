@@ -1,0 +1,44 @@
+"""Regenerates ``liar_b200/data/tables.json`` from the reference's data files.
+
+The tables are public physical data, kept identical to the reference's so that spectral results
+can be compared with it:
+* ``observer``: the CIE 1931 2-degree colour matching functions (CVRL database), as shipped in the
+  reference's data/observer.tsv (loaded by src/liar/__init__.py:51-66, wavelengths in nm there,
+  stored here in metres like the reference's Observer).
+* ``spd``: complex refractive index n + ik of Ag, Al, Au, Cu (Hagemann, Gudat, Kunz 1974 and the
+  other sources named in each reference data/spd/*.spd header), wavelengths in metres.
+
+Run in a container that has the reference mounted: ``python liar_b200/data/make_tables.py
+/path/to/reference``. The product reads only the generated JSON.
+"""
+import json
+import sys
+from pathlib import Path
+
+
+def read_columns(path: Path):
+    rows = []
+    for line in path.read_text().splitlines():
+        line = line.strip()
+        if not line or line.startswith("#"):
+            continue
+        rows.append(line.split())
+    return rows
+
+
+def main(ref: Path) -> None:
+    rows = read_columns(ref / "data" / "observer.tsv")
+    header, body = rows[0], rows[1:]
+    assert header == ["w", "xbar", "ybar", "zbar"], header
+    observer = [[float(r[0]) * 1e-9, float(r[1]), float(r[2]), float(r[3])] for r in body]
+    spd = {}
+    for name in ("Ag", "Al", "Au", "Cu"):
+        body = read_columns(ref / "data" / "spd" / f"{name}.spd")
+        spd[name] = [[float(r[0]) * 1e-9, float(r[1]), float(r[2])] for r in body]
+    out = Path(__file__).resolve().parent / "tables.json"
+    out.write_text(json.dumps({"observer": observer, "spd": spd}, indent=None, separators=(",", ":")))
+    print(out, len(observer), {k: len(v) for k, v in spd.items()})
+
+
+if __name__ == "__main__":
+    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))

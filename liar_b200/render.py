@@ -1,0 +1,395 @@
+"""Flattening of the scene graph into the renderer's C ABI (include/liar_gpu.h) and the render call.
+
+RenderEngine (kernel.py) uses this to hand the whole scene to the GPU in one upload: every
+geometric object becomes triangles of one soup tagged with an object index; shaders become
+material records, spectra become spectrum records (their tables in one float pool), lights become
+light records with the total power that drives light selection (kernel/light_context.cpp:272-333).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native as N
+from . import _tables, scenery, shaders, spectra
+from .textures import as_scalar, as_spectrum
+
+# ---- C structs (mirrors of include/liar_gpu.h)
+
+
+class CSpectrum(C.Structure):
+    _fields_ = [("type", C.c_int32), ("offset", C.c_int32), ("count", C.c_int32), ("p", C.c_float * 3)]
+
+
+class CMaterial(C.Structure):
+    _fields_ = [("type", C.c_int32), ("mdf", C.c_int32), ("spec", C.c_int32 * 4), ("emission", C.c_int32),
+                ("rough_u", C.c_float), ("rough_v", C.c_float)]
+
+
+class CLight(C.Structure):
+    _fields_ = [("type", C.c_int32), ("spectrum", C.c_int32), ("object", C.c_int32), ("double_sided", C.c_int32),
+                ("first_tri", C.c_int32), ("n_tris", C.c_int32), ("pos", C.c_float * 3), ("u", C.c_float * 3),
+                ("v", C.c_float * 3), ("power", C.c_float)]
+
+
+_P = C.c_void_p
+_S = C.c_size_t
+
+
+class CSceneDesc(C.Structure):
+    _fields_ = [("vertices", _P), ("n_vertices", _S), ("triangles", _P), ("n_triangles", _S),
+                ("triangle_object", _P), ("normals", _P), ("n_normals", _S), ("triangle_normals", _P),
+                ("object_material", _P), ("object_light", _P), ("n_objects", _S),
+                ("materials", _P), ("n_materials", _S), ("spectra", _P), ("n_spectra", _S),
+                ("spectrum_pool", _P), ("pool_size", _S), ("lights", _P), ("n_lights", _S),
+                ("observer", _P), ("n_observer", _S), ("scene_radius", C.c_float)]
+
+
+class CCamera(C.Structure):
+    _fields_ = [("position", C.c_float * 3), ("direction", C.c_float * 3), ("right", C.c_float * 3),
+                ("down", C.c_float * 3), ("direction_normal", C.c_float * 3), ("right_normal", C.c_float * 3),
+                ("down_normal", C.c_float * 3), ("lens_radius", C.c_float), ("focus_distance", C.c_float),
+                ("near_limit", C.c_float), ("far_limit", C.c_float)]
+
+
+class CRenderDesc(C.Structure):
+    _fields_ = [("camera", CCamera), ("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32),
+                ("tracer", C.c_int32), ("max_ray_generation", C.c_int32), ("max_depth", C.c_int32),
+                ("seed", C.c_uint64), ("first_sample", C.c_int32), ("wave_paths", C.c_int32)]
+
+
+SPEC_CONSTANT, SPEC_SAMPLED, SPEC_BLACKBODY, SPEC_CAUCHY = 0, 1, 2, 3
+MAT_NONE, MAT_LAMBERT, MAT_CONDUCTOR, MAT_COOK_TORRANCE, MAT_DIELECTRIC, MAT_WALTER, MAT_MIRROR = range(7)
+LIGHT_PARA, LIGHT_MESH, LIGHT_POINT, LIGHT_SKY = 0, 1, 2, 3
+
+
+@dataclass
+class FlatScene:
+    vertices: np.ndarray
+    triangles: np.ndarray
+    triangle_object: np.ndarray
+    normals: np.ndarray | None
+    triangle_normals: np.ndarray | None
+    object_material: np.ndarray
+    object_light: np.ndarray
+    materials: C.Array
+    spectra: C.Array
+    pool: np.ndarray
+    lights: C.Array
+    observer: np.ndarray
+    scene_radius: float
+    keep: list = field(default_factory=list)
+
+    def desc(self) -> CSceneDesc:
+        d = CSceneDesc()
+        d.vertices = self.vertices.ctypes.data
+        d.n_vertices = self.vertices.shape[0]
+        d.triangles = self.triangles.ctypes.data
+        d.n_triangles = self.triangles.shape[0]
+        d.triangle_object = self.triangle_object.ctypes.data
+        if self.normals is not None and self.triangle_normals is not None:
+            d.normals = self.normals.ctypes.data
+            d.n_normals = self.normals.shape[0]
+            d.triangle_normals = self.triangle_normals.ctypes.data
+        d.object_material = self.object_material.ctypes.data
+        d.object_light = self.object_light.ctypes.data
+        d.n_objects = self.object_material.shape[0]
+        d.materials = C.addressof(self.materials) if len(self.materials) else None
+        d.n_materials = len(self.materials)
+        d.spectra = C.addressof(self.spectra) if len(self.spectra) else None
+        d.n_spectra = len(self.spectra)
+        d.spectrum_pool = self.pool.ctypes.data if self.pool.size else None
+        d.pool_size = self.pool.size
+        d.lights = C.addressof(self.lights) if len(self.lights) else None
+        d.n_lights = len(self.lights)
+        d.observer = self.observer.ctypes.data
+        d.n_observer = self.observer.shape[0]
+        d.scene_radius = self.scene_radius
+        return d
+
+
+class _Builder:
+    def __init__(self):
+        self.verts, self.tris, self.tri_obj, self.norms, self.tri_norms = [], [], [], [], []
+        self.n_verts = self.n_tris = self.n_norms = 0
+        self.has_normals = False
+        self.obj_mat, self.obj_light = [], []
+        self.materials, self.mat_ids = [], {}
+        self.spectra, self.spec_ids, self.pool = [], {}, []
+        self.lights = []
+
+    # -- spectra
+    def spectrum(self, x, reflectant_hint=False) -> int:
+        s = as_spectrum(x)
+        key = id(s)
+        if key in self.spec_ids:
+            return self.spec_ids[key][0]
+        rec = CSpectrum()
+        if isinstance(s, spectra.Sampled):
+            rec.type = SPEC_SAMPLED
+            rec.offset = len(self.pool)
+            rec.count = len(s.wavelengths)
+            self.pool.extend(s.wavelengths)
+            self.pool.extend(s.values)
+        elif isinstance(s, spectra.BlackBody):
+            rec.type = SPEC_BLACKBODY
+            rec.p[0], rec.p[1] = s.temperature, s.scale
+        elif isinstance(s, spectra.Cauchy):
+            rec.type = SPEC_CAUCHY
+            rec.p[0], rec.p[1] = s.a, s.b
+        elif type(s) is spectra.Spectrum:
+            rec.type = SPEC_CONSTANT
+            rec.p[0] = s.value
+        else:
+            raise TypeError(f"unsupported spectrum {type(s).__name__}")
+        idx = len(self.spectra)
+        self.spectra.append(rec)
+        self.spec_ids[key] = (idx, s)
+        return idx
+
+    # -- shaders
+    def material(self, shader) -> int:
+        if shader is None:
+            return -1
+        key = id(shader)
+        if key in self.mat_ids:
+            return self.mat_ids[key][0]
+        m = CMaterial()
+        m.spec[:] = [-1, -1, -1, -1]
+        m.emission = -1
+        bsdf = shader
+        if isinstance(shader, shaders.Sum):
+            emitters = [c for c in shader.children if isinstance(c, shaders.Unshaded)]
+            others = [c for c in shader.children if not isinstance(c, shaders.Unshaded)]
+            if len(emitters) > 1 or len(others) > 1:
+                raise NotImplementedError("Sum supports one BSDF and one Unshaded component on the GPU")
+            if emitters:
+                m.emission = self.spectrum(emitters[0].colour)
+            bsdf = others[0] if others else None
+        if isinstance(bsdf, shaders.Unshaded):
+            m.emission = self.spectrum(bsdf.colour)
+            bsdf = None
+        if bsdf is None:
+            m.type = MAT_NONE
+        elif isinstance(bsdf, shaders.Lambert):
+            m.type = MAT_LAMBERT
+            m.spec[0] = self.spectrum(bsdf.diffuse)
+        elif isinstance(bsdf, shaders.Mirror):
+            m.type = MAT_MIRROR
+            m.spec[0] = self.spectrum(bsdf.reflectance)
+        elif isinstance(bsdf, (shaders.Conductor, shaders.CookTorrance)):
+            m.type = MAT_CONDUCTOR if isinstance(bsdf, shaders.Conductor) else MAT_COOK_TORRANCE
+            m.spec[0] = self.spectrum(bsdf.refractionIndex)
+            m.spec[1] = self.spectrum(bsdf.absorptionCoefficient)
+            m.spec[2] = self.spectrum(bsdf.reflectance)
+            if isinstance(bsdf, shaders.CookTorrance):
+                m.rough_u = as_scalar(bsdf.roughnessU)
+                m.rough_v = as_scalar(bsdf.roughnessV)
+                m.mdf = bsdf.mdf.kind
+        elif isinstance(bsdf, shaders.Dielectric):
+            m.type = MAT_WALTER if isinstance(bsdf, shaders.Walter) else MAT_DIELECTRIC
+            m.spec[0] = self.spectrum(bsdf.innerRefractionIndex)
+            m.spec[1] = self.spectrum(bsdf.outerRefractionIndex)
+            m.spec[2] = self.spectrum(bsdf.reflectance)
+            m.spec[3] = self.spectrum(bsdf.transmittance)
+            if isinstance(bsdf, shaders.Walter):
+                m.rough_u = as_scalar(bsdf.roughnessU)
+                m.rough_v = as_scalar(bsdf.roughnessV)
+                m.mdf = bsdf.mdf.kind
+        else:
+            raise NotImplementedError(f"shader {type(bsdf).__name__} is not on the GPU path")
+        idx = len(self.materials)
+        self.materials.append(m)
+        self.mat_ids[key] = (idx, shader)
+        return idx
+
+    # -- geometry
+    def geometry(self, obj, shader, light: int) -> tuple[int, int]:
+        v, t, n, tn = obj.triangles()
+        obj_index = len(self.obj_mat)
+        self.obj_mat.append(self.material(shader))
+        self.obj_light.append(light)
+        first = self.n_tris
+        self.verts.append(np.asarray(v, dtype=np.float32))
+        self.tris.append(np.asarray(t, dtype=np.int64) + self.n_verts)
+        self.tri_obj.append(np.full(len(t), obj_index, dtype=np.int32))
+        if n is not None and tn is not None:
+            self.has_normals = True
+            self.norms.append(np.asarray(n, dtype=np.float32))
+            self.tri_norms.append(np.where(tn >= 0, tn + self.n_norms, -1).astype(np.int32))
+            self.n_norms += len(n)
+        else:
+            self.tri_norms.append(np.full((len(t), 3), -1, dtype=np.int32))
+        self.n_verts += len(v)
+        self.n_tris += len(t)
+        return first, len(t)
+
+    def visit(self, obj, inherited=None):
+        if isinstance(obj, scenery.List):
+            for c in obj.children:
+                self.visit(c, obj.shader or inherited)
+        elif isinstance(obj, scenery.LightArea):
+            surf = obj.surface
+            li = len(self.lights)
+            L = CLight()
+            L.spectrum = self.spectrum(obj.radiance)
+            L.double_sided = int(bool(obj.isDoubleSided))
+            first, count = self.geometry(surf, obj.shader or surf.shader or inherited, li)
+            L.object = len(self.obj_mat) - 1
+            if isinstance(surf, scenery.Parallelogram):
+                L.type = LIGHT_PARA
+                L.pos[:], L.u[:], L.v[:] = surf.support, surf.sizeU, surf.sizeV
+                area = surf.area
+            else:
+                L.type = LIGHT_MESH
+                L.first_tri, L.n_tris = first, count
+                v = self.verts[-1].astype(np.float64)
+                t = self.tris[-1] - (self.n_verts - len(self.verts[-1]))
+                area = float(0.5 * np.linalg.norm(np.cross(v[t[:, 1]] - v[t[:, 0]], v[t[:, 2]] - v[t[:, 0]]), axis=1).sum())
+            # LightArea::doTotalPower (light_area.cpp:290-294)
+            L.power = math.pi * area * as_spectrum(obj.radiance).luminance * (2 if obj.isDoubleSided else 1)
+            self.lights.append(L)
+        elif isinstance(obj, scenery.LightPoint):
+            L = CLight()
+            L.type = LIGHT_POINT
+            L.object = -1
+            L.spectrum = self.spectrum(obj.intensity)
+            L.pos[:] = obj.position
+            L.power = 4 * math.pi * as_spectrum(obj.intensity).luminance  # LightPoint::doTotalPower
+            self.lights.append(L)
+        elif isinstance(obj, scenery.LightSky):
+            L = CLight()
+            L.type = LIGHT_SKY
+            L.object = -1
+            L.spectrum = self.spectrum(obj.radiance)
+            self.lights.append(L)
+        elif hasattr(obj, "triangles"):
+            self.geometry(obj, obj.shader or inherited, -1)
+        else:
+            raise NotImplementedError(f"scene object {type(obj).__name__} is not on the GPU path")
+
+    def finish(self) -> FlatScene:
+        if not self.verts:
+            raise ValueError("the scene has no geometry")
+        V = np.ascontiguousarray(np.concatenate(self.verts), dtype=np.float32)
+        T = np.ascontiguousarray(np.concatenate(self.tris), dtype=np.uint32)
+        lo, hi = V.min(axis=0).astype(np.float64), V.max(axis=0).astype(np.float64)
+        radius = float(0.5 * np.linalg.norm(hi - lo))
+        for L in self.lights:
+            if L.type == LIGHT_SKY:
+                # power of a constant sky: pi * radiance * the area of the scene's bounding sphere
+                L.power = math.pi * 4 * math.pi * radius ** 2 * self.spec_ids_lum(L.spectrum)
+        return FlatScene(
+            vertices=V, triangles=T,
+            triangle_object=np.ascontiguousarray(np.concatenate(self.tri_obj), dtype=np.int32),
+            normals=np.ascontiguousarray(np.concatenate(self.norms), dtype=np.float32) if self.has_normals else None,
+            triangle_normals=np.ascontiguousarray(np.concatenate(self.tri_norms), dtype=np.int32) if self.has_normals else None,
+            object_material=np.asarray(self.obj_mat, dtype=np.int32),
+            object_light=np.asarray(self.obj_light, dtype=np.int32),
+            materials=(CMaterial * len(self.materials))(*self.materials),
+            spectra=(CSpectrum * len(self.spectra))(*self.spectra),
+            pool=np.asarray(self.pool, dtype=np.float32),
+            lights=(CLight * len(self.lights))(*self.lights),
+            observer=np.ascontiguousarray(_tables.observer(), dtype=np.float32),
+            scene_radius=radius,
+        )
+
+    def spec_ids_lum(self, idx: int) -> float:
+        for i, s in self.spec_ids.values():
+            if i == idx:
+                return s.luminance
+        return 1.0
+
+
+def flatten(scene) -> FlatScene:
+    b = _Builder()
+    b.visit(scene)
+    return b.finish()
+
+
+def render_desc(camera, width: int, height: int, spp: int, tracer, seed: int = 0, first_sample: int = 0,
+                wave_paths: int = 0) -> CRenderDesc:
+    r = CRenderDesc()
+    cam = camera.flatten()
+    for k in ("position", "direction", "right", "down", "direction_normal", "right_normal", "down_normal"):
+        getattr(r.camera, k)[:] = cam[k]
+    r.camera.lens_radius = cam["lens_radius"]
+    r.camera.focus_distance = min(cam["focus_distance"], 3.4028234663852886e38)
+    r.camera.near_limit = cam["near_limit"]
+    r.camera.far_limit = min(cam["far_limit"], 3.4028234663852886e38)
+    r.width, r.height, r.spp = int(width), int(height), int(spp)
+    r.tracer = getattr(tracer, "kind", 0)
+    r.max_ray_generation = int(tracer.maxRayGeneration)
+    r.max_depth = int(getattr(tracer, "maxDepth", 0))
+    r.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+    r.first_sample = int(first_sample)
+    r.wave_paths = int(wave_paths)
+    return r
+
+
+def resolve(film: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """(H, W, 8) sums -> mean XYZ + alpha (H, W, 4) and variance of the mean of XYZ (H, W, 3)."""
+    n = np.maximum(film[..., 7:8], 1.0).astype(np.float64)
+    mean = film[..., 0:4].astype(np.float64) / n
+    ex2 = film[..., 4:7].astype(np.float64) / n
+    var = np.maximum(ex2 - mean[..., 0:3] ** 2, 0.0) * n / np.maximum(n - 1, 1) / n
+    return mean, var
+
+
+# ---- GPU scene handle
+
+
+_RENDER_SIGS = {
+    "liar_gpu_scene_upload": (C.c_int, [C.c_void_p, C.POINTER(CSceneDesc), C.POINTER(C.c_void_p)]),
+    "liar_gpu_scene_destroy": (None, [C.c_void_p]),
+    "liar_gpu_render": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(CRenderDesc), C.c_void_p]),
+    "liar_gpu_render_device": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(CRenderDesc), C.c_void_p, C.c_void_p]),
+    "liar_gpu_render_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_ulonglong)]),
+}
+
+
+class GpuScene:
+    """A flattened scene resident on the device (liar_gpu_scene_upload)."""
+
+    def __init__(self, ctx, flat: FlatScene):
+        self.ctx = ctx
+        self.flat = flat
+        lib = ctx._lib
+        for name, (res, args) in _RENDER_SIGS.items():
+            fn = getattr(lib, name)
+            fn.restype, fn.argtypes = res, args
+        h = C.c_void_p()
+        d = flat.desc()
+        ctx.check(lib.liar_gpu_scene_upload(ctx.handle, C.byref(d), C.byref(h)))
+        self.handle = h
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.ctx._lib.liar_gpu_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def render(self, desc: CRenderDesc, film: np.ndarray | None = None) -> np.ndarray:
+        """Adds desc.spp samples per pixel to film ((H, W, 8) float32 sums); returns film."""
+        if film is None:
+            film = np.zeros((desc.height, desc.width, 8), dtype=np.float32)
+        assert film.dtype == np.float32 and film.flags.c_contiguous and film.shape == (desc.height, desc.width, 8)
+        self.ctx.check(self.ctx._lib.liar_gpu_render(self.ctx.handle, self.handle, C.byref(desc), film.ctypes.data))
+        return film
+
+    def render_device(self, desc: CRenderDesc, film_ptr: int, stream: int | None = None) -> None:
+        self.ctx.check(self.ctx._lib.liar_gpu_render_device(self.ctx.handle, self.handle, C.byref(desc),
+                                                            C.c_void_p(film_ptr), C.c_void_p(stream or 0)))
+
+    def stats(self) -> dict:
+        out = (C.c_ulonglong * 3)()
+        self.ctx.check(self.ctx._lib.liar_gpu_render_stats(self.ctx.handle, out))
+        return {"paths": out[0], "segments": out[1], "hits": out[2]}

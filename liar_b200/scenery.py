@@ -1,0 +1,153 @@
+"""Scene objects of the scene API (``liar.scenery``, src/liar/scenery/). They record geometry and
+shaders; RenderEngine flattens them into one triangle soup for the GPU."""
+from __future__ import annotations
+
+import numpy as np
+
+from .textures import Constant
+
+
+class SceneObject:
+    def __init__(self):
+        self.shader = None
+        self.interior = None
+
+
+class List(SceneObject):
+    """Group of children (scenery/list.cpp); the tree variants only change how the reference
+    finds the nearest child, which the GPU tree over the whole soup replaces."""
+
+    def __init__(self, children=()):
+        super().__init__()
+        self.children = list(children)
+
+    def add(self, child):
+        self.children.append(child)
+
+
+class QbvhTree(List):
+    pass
+
+
+class AabbTree(List):
+    pass
+
+
+class AabpTree(List):
+    pass
+
+
+class OctTree(List):
+    pass
+
+
+class Parallelogram(SceneObject):
+    def __init__(self, support, sizeU, sizeV):
+        super().__init__()
+        self.support = tuple(float(x) for x in support)
+        self.sizeU = tuple(float(x) for x in sizeU)
+        self.sizeV = tuple(float(x) for x in sizeV)
+
+    def triangles(self):
+        s, u, v = (np.asarray(x, dtype=np.float64) for x in (self.support, self.sizeU, self.sizeV))
+        verts = np.stack([s, s + u, s + u + v, s + v]).astype(np.float32)
+        return verts, np.array([[0, 1, 2], [0, 2, 3]], dtype=np.uint32), None, None
+
+    @property
+    def area(self) -> float:
+        return float(np.linalg.norm(np.cross(self.sizeU, self.sizeV)))
+
+
+class Triangle(SceneObject):
+    def __init__(self, a, b, c):
+        super().__init__()
+        self.vertices = (tuple(a), tuple(b), tuple(c))
+
+    def triangles(self):
+        return np.asarray(self.vertices, dtype=np.float32), np.array([[0, 1, 2]], dtype=np.uint32), None, None
+
+
+class TriangleMesh(SceneObject):
+    """TriangleMesh(vertices, normals, uvs, triangles) (scenery/triangle_mesh.cpp). A triangle is
+    three vertex indices, or three (vertex, normal[, uv]) index tuples."""
+
+    def __init__(self, vertices, normals=(), uvs=(), triangles=()):
+        super().__init__()
+        self.vertices = np.asarray(vertices, dtype=np.float32).reshape(-1, 3)
+        self.normals = np.asarray(normals, dtype=np.float32).reshape(-1, 3) if len(normals) else None
+        self.uvs = uvs
+        tri = list(triangles) if not isinstance(triangles, np.ndarray) else triangles
+        if isinstance(tri, np.ndarray) and tri.ndim == 2:
+            self._vi = tri.astype(np.uint32)
+            self._ni = None
+        else:
+            vi, ni = [], []
+            has_n = False
+            for t in tri:
+                row_v, row_n = [], []
+                for c in t:
+                    if isinstance(c, (tuple, list)):
+                        row_v.append(int(c[0]))
+                        n = int(c[1]) if len(c) > 1 and c[1] is not None else -1
+                        row_n.append(n)
+                        has_n |= n >= 0
+                    else:
+                        row_v.append(int(c))
+                        row_n.append(-1)
+                vi.append(row_v)
+                ni.append(row_n)
+            self._vi = np.asarray(vi, dtype=np.uint32).reshape(-1, 3)
+            self._ni = np.asarray(ni, dtype=np.int32).reshape(-1, 3) if has_n else None
+
+    def triangles(self):
+        return self.vertices, self._vi, self.normals, self._ni
+
+
+class Sphere(SceneObject):
+    """Sphere(center, radius), flattened into a geodesic triangle mesh with exact normals."""
+
+    def __init__(self, center=(0, 0, 0), radius=1.0, subdivisions: int = 5):
+        super().__init__()
+        self.center = tuple(float(x) for x in center)
+        self.radius = float(radius)
+        self.subdivisions = int(subdivisions)
+
+    def triangles(self):
+        from .scenes import icosahedron, subdivide
+        v, f = icosahedron()
+        for _ in range(self.subdivisions):
+            v, f = subdivide(v, f)
+        verts = (v * self.radius + np.asarray(self.center)).astype(np.float32)
+        return verts, f.astype(np.uint32), v.astype(np.float32), f.astype(np.int32)
+
+
+class SceneLight(SceneObject):
+    pass
+
+
+class LightArea(SceneLight):
+    """LightArea(surface) (scenery/light_area.cpp): a surface that emits radiance."""
+
+    def __init__(self, surface, radiance=None):
+        super().__init__()
+        self.surface = surface
+        self.radiance = radiance if radiance is not None else Constant(1.0).value
+        self.numberOfEmissionSamples = 9
+        self.isDoubleSided = False
+
+
+class LightPoint(SceneLight):
+    def __init__(self, position=(0, 0, 0), intensity=None):
+        super().__init__()
+        self.position = tuple(float(x) for x in position)
+        self.intensity = intensity if intensity is not None else Constant(1.0).value
+        self.numberOfEmissionSamples = 1
+
+
+class LightSky(SceneLight):
+    """Constant-radiance sky at a fixed distance of 1000 scene radii (scenery/light_sky.cpp)."""
+
+    def __init__(self, radiance=None):
+        super().__init__()
+        self.radiance = radiance if radiance is not None else Constant(1.0)
+        self.numberOfEmissionSamples = 1

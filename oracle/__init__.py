@@ -84,6 +84,39 @@ def trace_bruteforce(vertices, triangles, rays, any_hit=False, threads=0):
     return H[:, 0].copy(), H[:, 1].view(np.float32).copy()
 
 
+class RenderScene:
+    """The path-tracer restatement (oracle_render.cpp) over a flattened scene. ``flat`` is the
+    same ``liar_b200.render.FlatScene`` the GPU receives; it must outlive this object."""
+
+    def __init__(self, flat):
+        self.flat = flat
+        self._desc = flat.desc()
+        L = lib()
+        L.oracle_scene_create.restype = C.c_void_p
+        L.oracle_scene_create.argtypes = [C.c_void_p]
+        L.oracle_scene_free.restype = None
+        L.oracle_scene_free.argtypes = [C.c_void_p]
+        L.oracle_render.restype = C.c_int
+        L.oracle_render.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_int]
+        self.h = L.oracle_scene_create(C.addressof(self._desc))
+
+    def render(self, desc, film=None, pixels=None, threads=0):
+        """Adds desc.spp samples of pixels [begin, end) (all by default) to film (H, W, 8)."""
+        if film is None:
+            film = np.zeros((desc.height, desc.width, 8), dtype=np.float32)
+        b, e = pixels if pixels is not None else (0, desc.width * desc.height)
+        lib().oracle_render(self.h, C.addressof(desc), film.ctypes.data, int(b), int(e), int(threads))
+        return film
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().oracle_scene_free(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
 class Tree:
     """Median-split binary tree over the mesh (CPU only)."""
 

@@ -1,0 +1,933 @@
+// oracle_render.cpp -- CPU ORACLE (test infrastructure only) of the spectral path tracer.
+//
+// Loaded only by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference leg;
+// the product never calls it. A recursive restatement, in the reference's own structure and in
+// single precision, of:
+//   AdjointPhotonTracer::tracePhoton / shadeSurface / scatterSurface
+//        (src/liar/tracers/adjoint_photon_tracer.cpp:84-292)
+//   IntersectionContext flipTo / bsdfToLocal (src/liar/kernel/intersection_context.cpp:197-290)
+//   Bsdf::evaluate / sample caps rules (src/liar/kernel/bsdf.cpp:52-98, bsdf.h:141-145)
+//   Lambert, Conductor, CookTorrance, Dielectric, Walter, Mirror BSDFs and the GGX / Beckmann
+//        distributions (src/liar/shaders/*.cpp, src/liar/kernel/microfacet.cpp)
+//   LightArea / LightPoint / LightSky emission and sampling, LightContexts power CDF
+//        (src/liar/scenery/light_*.cpp, src/liar/kernel/light_context.cpp:272-333)
+//   Observer sample / sensitivity and Spectral::xyz in Single mode
+//        (src/liar/kernel/observer.cpp:57-171,283-317, src/liar/kernel/spectral.cpp:178-220)
+//   Sampled / BlackBody / Cauchy spectra (src/liar/spectra/*.cpp)
+// Scene intersection uses the oracle's own tree (oracle_trace.cpp) with the same hit rule.
+// The sample values come from the same stratified hash sampler definition as the product, so
+// both consume identical random numbers; results still differ where the libm
+// transcendentals (sin, cos, exp, log, tan, atan) round differently on the two machines.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+extern "C" int oracle_tri_intersect(const float* o, const float* d, const float* a, const float* b, const float* c,
+                                    float* t_out, float* u_out, float* v_out);
+extern "C" void* oracle_tree_build(const float* V, uint64_t nv, const uint32_t* T, uint64_t nt);
+extern "C" void oracle_tree_free(void* tree);
+
+namespace oracle_internal {
+struct Ray {
+    float ox, oy, oz, tmin, dx, dy, dz, tmax;
+};
+struct Hit {
+    int32_t prim;
+    float t;
+};
+Hit tree_closest(void* tree, const Ray& r);
+}  // namespace oracle_internal
+
+namespace {
+
+using oracle_internal::Hit;
+using oracle_internal::Ray;
+
+// ---- scene description (same memory layout as the library's C ABI structs)
+struct Spectrum {
+    int32_t type, offset, count;
+    float p[3];
+};
+struct Material {
+    int32_t type, mdf;
+    int32_t spec[4];
+    int32_t emission;
+    float rough_u, rough_v;
+};
+struct Light {
+    int32_t type, spectrum, object, double_sided;
+    int32_t first_tri, n_tris;
+    float pos[3], u[3], v[3];
+    float power;
+};
+struct Camera {
+    float position[3], direction[3], right[3], down[3];
+    float direction_normal[3], right_normal[3], down_normal[3];
+    float lens_radius, focus_distance, near_limit, far_limit;
+};
+struct SceneIn {
+    const float* vertices; uint64_t n_vertices;
+    const uint32_t* triangles; uint64_t n_triangles;
+    const int32_t* triangle_object;
+    const float* normals; uint64_t n_normals;
+    const int32_t* triangle_normals;
+    const int32_t* object_material; const int32_t* object_light; uint64_t n_objects;
+    const Material* materials; uint64_t n_materials;
+    const Spectrum* spectra; uint64_t n_spectra;
+    const float* pool; uint64_t pool_size;
+    const Light* lights; uint64_t n_lights;
+    const float* observer; uint64_t n_observer;
+    float scene_radius;
+};
+struct RenderIn {
+    Camera camera;
+    int32_t width, height, spp, tracer, max_ray_generation, max_depth;
+    uint64_t seed;
+    int32_t first_sample, wave_paths;
+};
+
+enum { SP_CONST = 0, SP_SAMPLED = 1, SP_BB = 2, SP_CAUCHY = 3 };
+enum { M_NONE = 0, M_LAMBERT = 1, M_CONDUCTOR = 2, M_CT = 3, M_DIELECTRIC = 4, M_WALTER = 5, M_MIRROR = 6 };
+enum { L_PARA = 0, L_MESH = 1, L_POINT = 2, L_SKY = 3 };
+enum { C_REFL = 0x2, C_TRANS = 0x4, C_DIFF = 0x10, C_SPEC = 0x20, C_GLOSSY = 0x40, C_ALL = 0xff };
+const float PI = 3.14159265358979323846f;
+const float TOL = 1e-6f;
+
+// ---- vectors
+struct V {
+    float x, y, z;
+};
+V operator+(V a, V b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+V operator-(V a, V b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+V operator-(V a) { return {-a.x, -a.y, -a.z}; }
+V operator*(float s, V a) { return {s * a.x, s * a.y, s * a.z}; }
+float dot(V a, V b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+V cross(V a, V b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+float len(V a) { return std::sqrt(dot(a, a)); }
+V unit(V a) { return (1.0f / len(a)) * a; }
+float sq(float x) { return x * x; }
+V reflect(V h, V v) { return (2.0f * dot(h, v)) * h - v; }  // Lass Vector3D::reflect
+
+// ---- sampler (the same definition as the library's sampler)
+uint64_t mix64(uint64_t z) {
+    z += 0x9e3779b97f4a7c15ull;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+float unitf(uint64_t h) { return (float)(uint32_t)(h >> 40) * (1.0f / 16777216.0f); }
+uint32_t permute(uint32_t i, uint32_t n, uint64_t key) {
+    if (n <= 1) return 0;
+    uint32_t bits = 0;
+    while ((1u << bits) < n) ++bits;
+    if (bits & 1u) ++bits;
+    const uint32_t half = bits / 2, mask = (1u << half) - 1u;
+    do {
+        uint32_t l = i >> half, r = i & mask;
+        for (uint32_t k = 0; k < 4; ++k) {
+            const uint32_t f = (uint32_t)mix64(key + 0x632be59bd9b4e019ull * (k + 1) + r) & mask;
+            const uint32_t nl = r;
+            r = l ^ f;
+            l = nl;
+        }
+        i = (l << half) | r;
+    } while (i >= n);
+    return i;
+}
+struct Sampler {
+    uint64_t seed;
+    uint32_t pixel, sample, spp;
+    float get(uint32_t dim, bool strat) const {
+        const uint64_t hd = mix64(seed ^ mix64(((uint64_t)pixel << 32) | (uint64_t)dim));
+        const float jit = unitf(mix64(hd + 0xd1b54a32d192ed03ull * ((uint64_t)sample + 1)));
+        if (!strat || spp <= 1) return jit;
+        const uint32_t s = permute(sample, spp, hd);
+        const float u = ((float)s + jit) / (float)spp;
+        return u < 1.0f ? u : 0.99999994f;
+    }
+};
+const uint32_t D_SCREEN = 0, D_LENS = 2, D_LAMBDA = 4, D_GEN0 = 8, D_PER_GEN = 8;
+const uint32_t O_STRAT = 0, O_BSDF = 1, O_COMP = 3, O_LCHOICE = 4, O_LIGHT = 5, O_RR = 7;
+
+// ---- scene
+struct Scene {
+    SceneIn in;
+    void* tree = nullptr;
+    std::vector<float> spec_max, light_cdf, light_area, tri_cdf;
+    std::vector<float> ow, oxyz, odxyz, ocdf;
+    int sky = -1;
+    float sky_distance = 1e3f;
+};
+
+float planck(float w, float T) {
+    const float h = 6.626070040e-34f, c = 299792458.0f, kb = 1.3806488e-23f;
+    const float c1 = 2 * h * c * c, c2 = h * c / kb;
+    const float w5 = sq(sq(w)) * w;
+    return c1 / (w5 * std::expm1(c2 / (w * T)));
+}
+
+float spectrum(const Scene& S, int idx, float w, bool reflectant) {
+    if (idx < 0) return 0.0f;
+    const Spectrum& sp = S.in.spectra[idx];
+    float v;
+    if (sp.type == SP_SAMPLED) {
+        const float* ws = S.in.pool + sp.offset;
+        const float* vs = ws + sp.count;
+        const float* it = std::upper_bound(ws, ws + sp.count, w);
+        if (it == ws || it == ws + sp.count) return 0.0f;
+        const int k = (int)(it - ws);
+        const float t = (w - ws[k - 1]) / (ws[k] - ws[k - 1]);
+        v = vs[k - 1] + t * (vs[k] - vs[k - 1]);
+        if (reflectant && S.spec_max[idx] > 1.0f) return v / S.spec_max[idx];
+        return v;
+    } else if (sp.type == SP_BB) {
+        const float T = sp.p[0];
+        v = sp.p[1] * (1.0f / planck(2.897771955e-3f / T, T)) * planck(w, T);
+    } else if (sp.type == SP_CAUCHY) {
+        const float wu = w * 1e6f;
+        v = sp.p[0] + sp.p[1] / sq(wu);
+    } else {
+        v = sp.p[0];
+    }
+    return reflectant ? std::min(v, 1.0f) : v;
+}
+
+float observer_sample(const Scene& S, float u, float& pdf) {
+    const int n = (int)S.ow.size();
+    const auto it = std::upper_bound(S.ocdf.begin(), S.ocdf.end(), u);
+    if (it == S.ocdf.begin() || it == S.ocdf.end()) {
+        pdf = 0;
+        return it == S.ocdf.begin() ? S.ow[0] : S.ow[n - 1];
+    }
+    const int k = (int)(it - S.ocdf.begin());
+    const float c1 = S.ocdf[k - 1], c2 = S.ocdf[k], dc = c2 - c1;
+    const float x = (u - c1) / dc;
+    pdf = dc / (S.ow[k] - S.ow[k - 1]);
+    return S.ow[k - 1] + x * (S.ow[k] - S.ow[k - 1]);
+}
+V observer_sensitivity(const Scene& S, float w) {
+    const auto it = std::upper_bound(S.ow.begin(), S.ow.end(), w);
+    if (it == S.ow.begin() || it == S.ow.end()) return {0, 0, 0};
+    const int k = (int)(it - S.ow.begin()) - 1;
+    const float dw = w - S.ow[k];
+    return {S.oxyz[3 * k] + S.odxyz[3 * k] * dw, S.oxyz[3 * k + 1] + S.odxyz[3 * k + 1] * dw,
+            S.oxyz[3 * k + 2] + S.odxyz[3 * k + 2] * dw};
+}
+
+// ---- warps restated from their published methods
+void concentric(float u1, float u2, float& x, float& y) {
+    const float a = 2 * u1 - 1, b = 2 * u2 - 1;
+    if (a == 0 && b == 0) {
+        x = y = 0;
+        return;
+    }
+    float r, phi;
+    if (std::fabs(a) > std::fabs(b)) {
+        r = a;
+        phi = (PI / 4) * (b / a);
+    } else {
+        r = b;
+        phi = (PI / 2) - (PI / 4) * (a / b);
+    }
+    x = r * std::cos(phi);
+    y = r * std::sin(phi);
+}
+V cosine_hemisphere(float u1, float u2, float& pdf) {
+    float x, y;
+    concentric(u1, u2, x, y);
+    const float z = std::sqrt(std::max(0.0f, 1 - x * x - y * y));
+    pdf = z / PI;
+    return {x, y, z};
+}
+V uniform_sphere(float u1, float u2, float& pdf) {
+    const float z = 1 - 2 * u2;
+    const float r = std::sqrt(std::max(0.0f, 1 - z * z));
+    const float phi = 2 * PI * u1;
+    pdf = 1 / (4 * PI);
+    return {r * std::cos(phi), r * std::sin(phi), z};
+}
+
+// ---- BSDF (in the shading frame)
+struct Bsdf {
+    int type, mdf;
+    uint32_t caps;
+    V ng;
+    float r, t, eta, kappa, ior, etaI, etaT, au, av;
+};
+struct Out {
+    V wo;
+    float value, pdf;
+    explicit operator bool() const { return pdf > 0 && value != 0; }
+};
+bool has(uint32_t c, uint32_t w) { return (c & w) == w; }
+bool compatible(uint32_t c, uint32_t a) {
+    const uint32_t o = c & a;
+    return (o & 0xf) > 0 && (o & 0xf0) > 0;
+}
+
+float sample_phi(float s, float au, float av) {
+    if (au == av) return 2 * PI * s;
+    const float phi = std::atan(av / au * std::tan(2 * PI * s));
+    if (s <= 0.25f) return phi;
+    if (s < 0.75f) return phi + PI;
+    return phi + 2 * PI;
+}
+float D(int mdf, V h, float au, float av, float& pdfH) {
+    if (mdf == 1) {  // Trowbridge-Reitz (GGX), microfacet_trowbridge_reitz.cpp:47-60
+        const float d = 1.0f / (PI * au * av * sq(sq(h.x / au) + sq(h.y / av) + sq(h.z)));
+        pdfH = d * h.z;
+        return d;
+    }
+    const float c2 = sq(h.z);  // Beckmann, microfacet_beckmann.cpp:53-74
+    if (c2 == 0) {
+        pdfH = 0;
+        return 0;
+    }
+    const float d = std::exp(-(sq(h.x / au) + sq(h.y / av)) / c2) / (PI * au * av * sq(c2));
+    pdfH = d * h.z;
+    return d;
+}
+V sample_h(int mdf, float sx, float sy, float au, float av) {
+    if (mdf == 1) {
+        const float phi = sample_phi(sx, au, av);
+        const float s = std::sqrt(sy / (1 - sy));
+        return unit({s * au * std::cos(phi), s * av * std::sin(phi), 1});
+    }
+    const float s = std::log(1 - sx);
+    float cp, sp, t2;
+    if (au == av) {
+        const float phi = 2 * PI * sy;
+        cp = std::cos(phi);
+        sp = std::sin(phi);
+        t2 = -s * sq(au);
+    } else {
+        const float phi = sample_phi(sx, au, av);
+        cp = std::cos(phi);
+        sp = std::sin(phi);
+        t2 = -s / (sq(cp / au) + sq(sp / av));
+    }
+    const float c2 = 1 / (1 + t2);
+    return {cp * std::sqrt(std::max(1 - c2, 0.0f)), sp * std::sqrt(std::max(1 - c2, 0.0f)), std::sqrt(c2)};
+}
+float lambda_(int mdf, V w, float au, float av) {
+    if (mdf == 1) return (std::sqrt(1 + (sq(w.x * au) + sq(w.y * av)) / sq(w.z)) - 1) / 2;
+    const float a2 = sq(w.z) / (sq(w.x * au) + sq(w.y * av));
+    const float a = std::sqrt(a2);
+    return a < 1.6f ? (3.535f * a + 2.181f * a2) / (1 + 2.276f * a + 2.577f * a2) : 1;
+}
+float G1(int mdf, V w, V h, float au, float av) {
+    if (dot(w, h) * w.z <= 0) return 0;
+    return 1 / (1 + lambda_(mdf, w, au, av));
+}
+float fresnel_cond(float eta, float kappa, float cosI) {
+    const float c2 = sq(cosI), a = sq(eta) + sq(kappa), b = 2 * cosI * eta;
+    const float aO = a + c2, aP = a * c2 + 1;
+    return ((aO - b) / (aO + b) + (aP - b) / (aP + b)) / 2;
+}
+float fresnel_walter(float ior, V wi, V h) {
+    const float cI = std::fabs(dot(wi, h));
+    const float s2 = sq(ior) * (1 - sq(cI));
+    const float cT = std::sqrt(std::max(1 - s2, 0.0f));
+    const float rO = (ior * cI - cT) / (ior * cI + cT), rP = (cI - ior * cT) / (cI + ior * cT);
+    return std::min((sq(rO) + sq(rP)) / 2, 1.0f);
+}
+float walter_pr(const Bsdf& b, float rF, uint32_t al) {
+    const float pr = has(al, C_REFL | C_GLOSSY) ? std::fabs(b.r) * rF : 0;
+    const float pt = has(al, C_TRANS | C_GLOSSY) ? std::fabs(b.t) * (1 - rF) : 0;
+    if (pr + pt == 0) return -1;
+    return pr / (pr + pt);
+}
+
+Out do_evaluate(const Bsdf& b, V wi, V wo, uint32_t al) {
+    Out o{{0, 0, 0}, 0, 0};
+    if (b.type == M_LAMBERT) {
+        const float c = std::fabs(wo.z);
+        if (c <= 0) return o;
+        return {wo, b.r / PI, c / PI};
+    }
+    if (b.type == M_CT) {
+        if (wo.z <= 0) return o;
+        const V h = unit(wi + wo);
+        float pdfH;
+        const float d = D(b.mdf, h, b.au, b.av, pdfH);
+        const float dh = std::fabs(dot(wi, h));
+        const float g = std::min(1.0f, std::min(2 * h.z * wi.z / dh, 2 * h.z * wo.z / dh));
+        const float pdf = pdfH / (4 * dot(wi, h));
+        float v = b.r * (d * g / (4 * wi.z * wo.z));
+        v *= fresnel_cond(b.eta, b.kappa, std::fabs(dot(wi, h)));
+        return {wo, v, pdf};
+    }
+    if (b.type == M_WALTER) {
+        if (wo.z > 0) {
+            const V h = unit(wi + wo);
+            const float rF = fresnel_walter(b.etaI / b.etaT, wi, h);
+            const float pR = walter_pr(b, rF, al);
+            if (pR < 0) return o;
+            float pdfH;
+            const float d = D(b.mdf, h, b.au, b.av, pdfH);
+            const float g = G1(b.mdf, wi, h, b.au, b.av) * G1(b.mdf, wo, h, b.au, b.av);
+            const float dh = 1 / (4 * dot(wi, h));
+            return {wo, b.r * (rF * d * g / (4 * wi.z * wo.z)), pR * pdfH * dh};
+        } else if (wo.z < 0) {
+            const V h = unit(-(b.etaI * wi) - b.etaT * wo);
+            if (h.z <= 0) return o;
+            const float cI = std::fabs(dot(wi, h)), cT = std::fabs(dot(wo, h));
+            const float rF = fresnel_walter(b.etaI / b.etaT, wi, h);
+            const float pR = walter_pr(b, rF, al);
+            if (pR < 0) return o;
+            float pdfH;
+            const float d = D(b.mdf, h, b.au, b.av, pdfH);
+            const float g = G1(b.mdf, wi, h, b.au, b.av) * G1(b.mdf, wo, h, b.au, b.av);
+            const float dh = sq(b.etaT) * cT / sq(b.etaI * cI + b.etaT * cT);
+            return {wo, b.t * (((1 - rF) * d * g * (cI * dh)) / std::fabs(wi.z * wo.z)), (1 - pR) * pdfH * dh};
+        }
+    }
+    return o;
+}
+Out evaluate(const Bsdf& b, V wi, V wo, uint32_t al) {
+    if (wo.z == 0) return {wo, 0, 0};
+    const bool refl = (dot(wi, b.ng) > 0) == (dot(wo, b.ng) > 0);
+    al &= ~(refl ? (uint32_t)C_TRANS : (uint32_t)C_REFL);
+    if (!compatible(b.caps, al)) return {wo, 0, 0};
+    return do_evaluate(b, wi, wo, al);
+}
+Out sample(const Bsdf& b, V wi, float sx, float sy, float comp, uint32_t al) {
+    Out o{{0, 0, 0}, 0, 0};
+    if (!compatible(b.caps, al)) return o;
+    switch (b.type) {
+        case M_LAMBERT: {
+            float pdf;
+            const V wo = cosine_hemisphere(sx, sy, pdf);
+            return {wo, b.r / PI, pdf};
+        }
+        case M_CONDUCTOR:
+            return {{-wi.x, -wi.y, wi.z}, b.r * fresnel_cond(b.eta, b.kappa, wi.z) / wi.z, 1};
+        case M_MIRROR:
+            return {{-wi.x, -wi.y, wi.z}, b.r, wi.z};
+        case M_CT: {
+            const V h = sample_h(b.mdf, sx, sy, b.au, b.av);
+            const V wo = reflect(h, wi);
+            if (wo.z <= 0) return o;
+            return do_evaluate(b, wi, wo, al);
+        }
+        case M_DIELECTRIC: {
+            const float cI = wi.z;
+            if (cI <= 0) return o;
+            const float ior = b.ior;
+            const float s2 = sq(ior) * (1 - sq(cI));
+            const float cT = std::sqrt(std::max(1 - s2, 0.0f));
+            const float rO = (ior * cI - cT) / (ior * cI + cT), rP = (cI - ior * cT) / (cI + ior * cT);
+            const float rF = (sq(rO) + sq(rP)) / 2;
+            const float pr = has(al, C_REFL | C_SPEC) ? std::fabs(b.r) * rF : 0;
+            const float pt = has(al, C_TRANS | C_SPEC) ? std::fabs(b.t) * (1 - rF) : 0;
+            if (pr + pt == 0) return o;
+            const float probR = pr / (pr + pt);
+            if (comp < probR) return {{-wi.x, -wi.y, wi.z}, b.r * rF / cI, probR};
+            return {{-ior * wi.x, -ior * wi.y, -cT}, b.t * (1 - rF) / cT, 1 - probR};
+        }
+        case M_WALTER: {
+            const V h = sample_h(b.mdf, sx, sy, b.au, b.av);
+            float pdfH;
+            const float d = D(b.mdf, h, b.au, b.av, pdfH);
+            const float rF = fresnel_walter(b.etaI / b.etaT, wi, h);
+            const float pR = walter_pr(b, rF, al);
+            if (pR < 0) return o;
+            if (comp < pR) {
+                const V wo = reflect(h, wi);
+                if (wo.z <= 0) return o;
+                const float g = G1(b.mdf, wi, h, b.au, b.av) * G1(b.mdf, wo, h, b.au, b.av);
+                const float dh = 1 / (4 * dot(wo, h));
+                return {wo, b.r * (rF * d * g / (4 * wi.z * wo.z)), pR * pdfH * dh};
+            }
+            const float eta = b.etaI / b.etaT;
+            const float cI = std::fabs(dot(wi, h));
+            const float s2 = sq(eta) * (1 - sq(cI));
+            const float cT = std::sqrt(std::max(1 - s2, 0.0f));
+            const V wo = unit((-eta) * wi + (eta * cI - cT) * h);
+            if (wo.z >= 0) return o;
+            const float g = G1(b.mdf, wi, h, b.au, b.av) * G1(b.mdf, wo, h, b.au, b.av);
+            const float dh = sq(b.etaT) * cT / sq(b.etaI * cI + b.etaT * cT);
+            return {wo, b.t * (((1 - rF) * d * g * (cI * dh)) / std::fabs(wi.z * wo.z)), (1 - pR) * pdfH * dh};
+        }
+    }
+    return o;
+}
+
+// ---- lights
+float light_pdf_choice(const Scene& S, int k) { return k > 0 ? S.light_cdf[k] - S.light_cdf[k - 1] : S.light_cdf[0]; }
+
+bool para_hit(const Light& L, V o, V d, float tmin, float& t) {
+    const V p{L.pos[0], L.pos[1], L.pos[2]}, u{L.u[0], L.u[1], L.u[2]}, v{L.v[0], L.v[1], L.v[2]};
+    const V n = cross(u, v);
+    const float den = dot(n, d);
+    if (den == 0) return false;
+    const float th = dot(n, p - o) / den;
+    if (!(th > tmin)) return false;
+    const V x = o + th * d - p;
+    const float uu = dot(u, u), uv = dot(u, v), vv = dot(v, v), xu = dot(x, u), xv = dot(x, v);
+    const float det = uu * vv - uv * uv;
+    const float a = (xu * vv - xv * uv) / det, b = (xv * uu - xu * uv) / det;
+    if (a < 0 || a > 1 || b < 0 || b > 1) return false;
+    t = th;
+    return true;
+}
+
+// SceneLight::emission(ray): radiance and solid-angle pdf of the direction
+float light_emission_pdf(const Scene& S, int li, V o, V d) {
+    const Light& L = S.in.lights[li];
+    if (L.type == L_PARA) {
+        float t;
+        if (!para_hit(L, o, d, TOL, t)) return 0;
+        const V n = unit(cross({L.u[0], L.u[1], L.u[2]}, {L.v[0], L.v[1], L.v[2]}));
+        return sq(t) / std::fabs(S.light_area[li] * dot(d, n));
+    }
+    if (L.type == L_MESH) {
+        float tb = INFINITY;
+        int best = -1;
+        for (int k = 0; k < L.n_tris; ++k) {
+            const uint32_t* tr = S.in.triangles + 3 * (size_t)(L.first_tri + k);
+            const float oo[3] = {o.x, o.y, o.z}, dd[3] = {d.x, d.y, d.z};
+            float t, u, v;
+            if (oracle_tri_intersect(oo, dd, S.in.vertices + 3 * tr[0], S.in.vertices + 3 * tr[1],
+                                     S.in.vertices + 3 * tr[2], &t, &u, &v) && t > TOL && t < tb) {
+                tb = t;
+                best = L.first_tri + k;
+            }
+        }
+        if (best < 0) return 0;
+        const uint32_t* tr = S.in.triangles + 3 * (size_t)best;
+        const float* a = S.in.vertices + 3 * tr[0];
+        const float* b = S.in.vertices + 3 * tr[1];
+        const float* c = S.in.vertices + 3 * tr[2];
+        const V n = unit(cross({b[0] - a[0], b[1] - a[1], b[2] - a[2]}, {c[0] - a[0], c[1] - a[1], c[2] - a[2]}));
+        return sq(tb) / std::fabs(S.light_area[li] * dot(d, n));
+    }
+    if (L.type == L_SKY) return 1 / (4 * PI);
+    return 0;
+}
+
+struct LS {
+    V dir;
+    float pdf;
+};
+LS light_sample(const Scene& S, int li, V target, float sx, float sy) {
+    const Light& L = S.in.lights[li];
+    if (L.type == L_PARA || L.type == L_MESH) {
+        V p, n;
+        float pdf;
+        if (L.type == L_PARA) {
+            const V u{L.u[0], L.u[1], L.u[2]}, v{L.v[0], L.v[1], L.v[2]};
+            p = V{L.pos[0], L.pos[1], L.pos[2]} + sx * u + sy * v;
+            n = unit(cross(u, v));
+            pdf = 1 / S.light_area[li];
+        } else {
+            const float* cdf = S.tri_cdf.data() + L.first_tri;
+            int ii = (int)(std::lower_bound(cdf, cdf + L.n_tris, sx) - cdf);
+            ii = std::min(ii, L.n_tris - 1);
+            const float i0 = ii > 0 ? cdf[ii - 1] : 0.0f;
+            const float tp = cdf[ii] - i0;
+            const float di = (sx - i0) / tp;
+            const uint32_t* tr = S.in.triangles + 3 * (size_t)(L.first_tri + ii);
+            const float* a = S.in.vertices + 3 * tr[0];
+            const float* b = S.in.vertices + 3 * tr[1];
+            const float* c = S.in.vertices + 3 * tr[2];
+            const V A{a[0], a[1], a[2]}, e1{b[0] - a[0], b[1] - a[1], b[2] - a[2]}, e2{c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+            const V nn = cross(e1, e2);
+            const float s = std::sqrt(di);
+            const float nl = len(nn);
+            n = (1 / nl) * nn;
+            pdf = tp / (nl / 2);
+            p = A + (1 - s) * e1 + (s * sy) * e2;
+        }
+        V to = p - target;
+        const float d2 = dot(to, to);
+        to = (1 / std::sqrt(d2)) * to;
+        pdf *= d2 / std::fabs(dot(n, to));
+        V tl = p - target;
+        tl = (1 / len(tl)) * tl;
+        if (!L.double_sided && dot(n, tl) > 0) return {tl, 0};
+        return {tl, pdf};
+    }
+    if (L.type == L_POINT) {
+        V tl = V{L.pos[0], L.pos[1], L.pos[2]} - target;
+        tl = (1 / len(tl)) * tl;
+        return {tl, 1};
+    }
+    if (L.type == L_SKY) {
+        float pdf;
+        const V d = uniform_sphere(sx, sy, pdf);
+        return {d, pdf};
+    }
+    return {{0, 0, 1}, 0};
+}
+
+float power_heuristic(float a, float b) { return sq(a) / (sq(a) + sq(b)); }
+
+struct Path {
+    const Scene* S;
+    const RenderIn* R;
+    Sampler smp;
+    float lam;
+    float alpha = 0;
+};
+
+float trace_photon(Path& P, V o, V d, float tmin, float tmax, int gen);
+
+// AdjointPhotonTracer::shadeSurface + scatterSurface for the hit `h` of ray (o, d)
+float shade_surface(Path& P, V o, V d, float tmin, float tmax, const Hit& h, int gen) {
+    const Scene& S = *P.S;
+    float result = 0;
+    const uint32_t prim = (uint32_t)h.prim;
+    const int obj = S.in.triangle_object[prim];
+    const int light = S.in.object_light[obj];
+    const int mi = S.in.object_material[obj];
+    const uint32_t* tr = S.in.triangles + 3 * (size_t)prim;
+    const float* pa = S.in.vertices + 3 * tr[0];
+    const float* pb = S.in.vertices + 3 * tr[1];
+    const float* pc = S.in.vertices + 3 * tr[2];
+    const V A{pa[0], pa[1], pa[2]};
+    const V e1 = V{pb[0], pb[1], pb[2]} - A, e2 = V{pc[0], pc[1], pc[2]} - A;
+    float tt, bu = 0, bv = 0;
+    const float oo[3] = {o.x, o.y, o.z}, dd[3] = {d.x, d.y, d.z};
+    if (!oracle_tri_intersect(oo, dd, pa, pb, pc, &tt, &bu, &bv)) bu = bv = 0;
+    const V target = A + bu * e1 + bv * e2;
+    const V ng0 = unit(cross(e1, e2));
+    V ns = ng0;
+    if (S.in.triangle_normals && S.in.normals) {
+        const int32_t* tn = S.in.triangle_normals + 3 * (size_t)prim;
+        if (tn[0] >= 0 && tn[1] >= 0 && tn[2] >= 0) {
+            const float* n0 = S.in.normals + 3 * tn[0];
+            const float* n1 = S.in.normals + 3 * tn[1];
+            const float* n2 = S.in.normals + 3 * tn[2];
+            const float w0 = 1 - bu - bv;
+            ns = unit(w0 * V{n0[0], n0[1], n0[2]} + bu * V{n1[0], n1[1], n1[2]} + bv * V{n2[0], n2[1], n2[2]});
+        }
+    }
+    const bool leaving = dot(d, ng0) > 0;
+    const V ng = dot(ng0, -d) < 0 ? -ng0 : ng0;  // flipTo(-direction)
+    const V N = dot(ns, -d) < 0 ? -ns : ns;
+    if (gen > 0 && light >= 0) result += spectrum(S, S.in.lights[light].spectrum, P.lam, false);
+    if (mi < 0 || S.in.materials[mi].type == M_NONE) {
+        if (mi >= 0 && light < 0 && S.in.materials[mi].emission >= 0)
+            result += spectrum(S, S.in.materials[mi].emission, P.lam, false);
+        return result + trace_photon(P, o, d, h.t + TOL, tmax, gen + 1);
+    }
+    const Material& M = S.in.materials[mi];
+    if (light < 0 && M.emission >= 0) result += spectrum(S, M.emission, P.lam, false);
+    // frame: IntersectionContext::bsdfToLocal
+    V u = e1 - dot(e1, N) * N, v = e2 - dot(e2, N) * N;
+    const float su = dot(u, u), sv = dot(v, v);
+    if (std::max(su, sv) < 1e-3f * std::max(dot(e1, e1), dot(e2, e2))) {
+        const V ax = std::fabs(N.x) < 0.9f ? V{1, 0, 0} : V{0, 1, 0};
+        u = cross(ax, N);
+        v = cross(N, u);
+    }
+    if (su >= sv) {
+        u = unit(u);
+        v = cross(N, u);
+    } else {
+        v = unit(v);
+        u = cross(v, N);
+    }
+    Bsdf B{};
+    B.type = M.type;
+    B.mdf = M.mdf;
+    B.ng = {dot(ng, u), dot(ng, v), dot(ng, N)};
+    B.eta = B.kappa = B.ior = B.etaI = B.etaT = 1;
+    B.au = sq(std::max(M.rough_u, 1e-3f));
+    B.av = sq(std::max(M.rough_v, 1e-3f));
+    switch (M.type) {
+        case M_LAMBERT:
+            B.caps = C_REFL | C_DIFF;
+            B.r = spectrum(S, M.spec[0], P.lam, true);
+            break;
+        case M_CONDUCTOR:
+        case M_CT:
+            B.caps = M.type == M_CONDUCTOR ? (C_REFL | C_SPEC) : (C_REFL | C_GLOSSY);
+            B.eta = std::max(spectrum(S, M.spec[0], P.lam, false), 1e-9f);
+            B.kappa = std::max(spectrum(S, M.spec[1], P.lam, false), 1e-9f);
+            B.r = spectrum(S, M.spec[2], P.lam, true);
+            break;
+        case M_DIELECTRIC: {
+            B.caps = C_REFL | C_TRANS | C_SPEC;
+            const float i1 = std::max(spectrum(S, M.spec[1], P.lam, false), 1e-9f);
+            const float i2 = std::max(spectrum(S, M.spec[0], P.lam, false), 1e-9f);
+            B.ior = leaving ? i2 / i1 : i1 / i2;
+            B.r = spectrum(S, M.spec[2], P.lam, true);
+            B.t = spectrum(S, M.spec[3], P.lam, true);
+            break;
+        }
+        case M_WALTER: {
+            B.caps = C_TRANS | C_GLOSSY;
+            float ei = std::max(spectrum(S, M.spec[1], P.lam, false), 1e-9f);
+            float et = std::max(spectrum(S, M.spec[0], P.lam, false), 1e-9f);
+            if (leaving) std::swap(ei, et);
+            B.etaI = ei;
+            B.etaT = et;
+            B.r = spectrum(S, M.spec[2], P.lam, true);
+            B.t = spectrum(S, M.spec[3], P.lam, true);
+            break;
+        }
+        case M_MIRROR:
+            B.caps = C_REFL | C_SPEC;
+            B.r = spectrum(S, M.spec[0], P.lam, true);
+            break;
+    }
+    const V md = -d;
+    V wi{dot(md, u), dot(md, v), dot(md, N)};
+    wi.z = std::max(wi.z, 1.19209290e-07f);
+    // scatterSurface
+    const bool strat = gen < P.R->max_ray_generation;
+    const uint32_t base = D_GEN0 + D_PER_GEN * (uint32_t)gen;
+    const float spdf = (has(B.caps, C_DIFF) || has(B.caps, C_GLOSSY)) ? 0.5f : 1.0f;
+    Out out{{0, 0, 0}, 0, 0};
+    if (P.smp.get(base + O_STRAT, strat) < spdf) {
+        out = sample(B, wi, P.smp.get(base + O_BSDF, strat), P.smp.get(base + O_BSDF + 1, strat),
+                     P.smp.get(base + O_COMP, strat), C_ALL);
+        if (!out) return result;
+        out.pdf *= spdf;
+        const V wd = out.wo.x * u + out.wo.y * v + out.wo.z * N;
+        float pl = 0;
+        for (int l = 0; l < (int)S.in.n_lights; ++l) {
+            const float p = light_emission_pdf(S, l, target, wd);
+            if (p > 0) pl += light_pdf_choice(S, l) * p;
+        }
+        pl *= (1 - spdf);
+        out.value *= power_heuristic(out.pdf, pl);
+    } else {
+        if (S.in.n_lights == 0) return result;
+        const float uc = P.smp.get(base + O_LCHOICE, strat);
+        int k = (int)(std::lower_bound(S.light_cdf.begin(), S.light_cdf.end(), uc) - S.light_cdf.begin());
+        k = std::min(k, (int)S.in.n_lights - 1);
+        const float pc = light_pdf_choice(S, k);
+        if (pc <= 0) return result;
+        const LS ls = light_sample(S, k, target, P.smp.get(base + O_LIGHT, strat), P.smp.get(base + O_LIGHT + 1, strat));
+        if (ls.pdf <= 0) return result;
+        float pdf = pc * ls.pdf;
+        for (int l = 0; l < (int)S.in.n_lights; ++l) {
+            if (l == k) continue;
+            const float p = light_emission_pdf(S, l, target, ls.dir);
+            if (p > 0) pdf += light_pdf_choice(S, l) * p;
+        }
+        pdf *= (1 - spdf);
+        const V wo{dot(ls.dir, u), dot(ls.dir, v), dot(ls.dir, N)};
+        const Out be = evaluate(B, wi, wo, C_ALL);
+        if (!be) return result;
+        out = {wo, be.value * power_heuristic(pdf, be.pdf * spdf), pdf};
+    }
+    if (!out) return result;
+    const float ct = out.wo.z;
+    const V start = target + ((ct > 0 ? 10.0f : -10.0f) * TOL) * ng;
+    const V nd = out.wo.x * u + out.wo.y * v + out.wo.z * N;
+    const float radiance = trace_photon(P, start, nd, TOL, INFINITY, gen + 1);
+    return result + (out.value * radiance) * (std::fabs(ct) / out.pdf);
+}
+
+float trace_photon(Path& P, V o, V d, float tmin, float tmax, int gen) {
+    const Scene& S = *P.S;
+    float power = 1;
+    if (P.R->max_depth > 0 && gen >= P.R->max_depth) return 0;
+    if (gen >= P.R->max_ray_generation) {
+        const float u = P.smp.get(D_GEN0 + D_PER_GEN * (uint32_t)gen + O_RR, false);
+        if (u < 0.5f) power /= 0.5f;
+        else return 0;
+    }
+    const Hit h = oracle_internal::tree_closest(S.tree, Ray{o.x, o.y, o.z, tmin, d.x, d.y, d.z, tmax});
+    if (h.prim < 0) {
+        if (S.sky >= 0 && S.sky_distance > tmin * (1 + TOL) && S.sky_distance < tmax * (1 - TOL)) {
+            if (gen == 0) P.alpha = 1;
+            if (gen > 0) return power * spectrum(S, S.in.lights[S.sky].spectrum, P.lam, false);
+        }
+        return 0;
+    }
+    if (gen == 0) P.alpha = 1;
+    return power * shade_surface(P, o, d, tmin, tmax, h, gen);
+}
+
+}  // namespace
+
+extern "C" {
+
+void* oracle_scene_create(const SceneIn* in) {
+    Scene* S = new Scene();
+    S->in = *in;
+    S->tree = oracle_tree_build(in->vertices, in->n_vertices, in->triangles, in->n_triangles);
+    S->spec_max.assign(in->n_spectra, 0);
+    for (uint64_t k = 0; k < in->n_spectra; ++k) {
+        const Spectrum& s = in->spectra[k];
+        if (s.type == SP_SAMPLED) {
+            float mx = -INFINITY;
+            for (int i = 0; i < s.count; ++i) mx = std::max(mx, in->pool[s.offset + s.count + i]);
+            S->spec_max[k] = mx;
+        }
+    }
+    const uint64_t nl = in->n_lights;
+    S->light_cdf.assign(nl, 0);
+    S->light_area.assign(nl, 0);
+    S->tri_cdf.assign(in->n_triangles, 0);
+    double tot = 0;
+    for (uint64_t k = 0; k < nl; ++k) {
+        const Light& L = in->lights[k];
+        if (L.type == L_SKY) S->sky = (int)k;
+        if (L.type == L_PARA) {
+            const double ux = L.u[0], uy = L.u[1], uz = L.u[2], vx = L.v[0], vy = L.v[1], vz = L.v[2];
+            const double cx = uy * vz - uz * vy, cy = uz * vx - ux * vz, cz = ux * vy - uy * vx;
+            S->light_area[k] = (float)std::sqrt(cx * cx + cy * cy + cz * cz);
+        } else if (L.type == L_MESH) {
+            std::vector<double> ar(L.n_tris);
+            double acc = 0;
+            for (int i = 0; i < L.n_tris; ++i) {
+                const uint32_t* t = in->triangles + 3 * (size_t)(L.first_tri + i);
+                const float* a = in->vertices + 3 * t[0];
+                const float* b = in->vertices + 3 * t[1];
+                const float* c = in->vertices + 3 * t[2];
+                const double e1[3] = {(double)b[0] - a[0], (double)b[1] - a[1], (double)b[2] - a[2]};
+                const double e2[3] = {(double)c[0] - a[0], (double)c[1] - a[1], (double)c[2] - a[2]};
+                const double nx = e1[1] * e2[2] - e1[2] * e2[1], ny = e1[2] * e2[0] - e1[0] * e2[2],
+                             nz = e1[0] * e2[1] - e1[1] * e2[0];
+                ar[i] = 0.5 * std::sqrt(nx * nx + ny * ny + nz * nz);
+                acc += ar[i];
+            }
+            double run = 0;
+            for (int i = 0; i < L.n_tris; ++i) {
+                run += ar[i];
+                S->tri_cdf[L.first_tri + i] = (float)(run / acc);
+            }
+            S->light_area[k] = (float)acc;
+        }
+        tot += std::max(0.0f, L.power);
+        S->light_cdf[k] = (float)tot;
+    }
+    for (uint64_t k = 0; k < nl; ++k) S->light_cdf[k] = tot > 0 ? (float)(S->light_cdf[k] / tot) : (float)(k + 1) / nl;
+    // observer (Observer::Observer)
+    const uint64_t n = in->n_observer;
+    const float* O = in->observer;
+    S->ow.resize(n);
+    S->oxyz.resize(3 * n);
+    S->odxyz.assign(3 * n, 0);
+    S->ocdf.resize(n);
+    std::vector<double> dX(3 * n), cd(n, 0);
+    double prev = O[0], acc = 0;
+    for (uint64_t k = 0; k + 1 < n; ++k) {
+        const double w = O[4 * k], wn = O[4 * (k + 1)];
+        for (int c = 0; c < 3; ++c) {
+            S->odxyz[3 * k + c] = (float)((O[4 * (k + 1) + 1 + c] - O[4 * k + 1 + c]) / (wn - w));
+            dX[3 * k + c] = O[4 * k + 1 + c] * ((wn - prev) / 2);
+        }
+        prev = w;
+        acc += (std::fabs(O[4 * k + 1]) + std::fabs(O[4 * k + 2]) + std::fabs(O[4 * k + 3]) + std::fabs(O[4 * (k + 1) + 1]) +
+                std::fabs(O[4 * (k + 1) + 2]) + std::fabs(O[4 * (k + 1) + 3])) * (wn - w);
+        cd[k + 1] = acc;
+    }
+    for (int c = 0; c < 3; ++c) dX[3 * (n - 1) + c] = O[4 * (n - 1) + 1 + c] * ((O[4 * (n - 1)] - prev) / 2);
+    double Y = 0;
+    for (uint64_t k = 0; k < n; ++k) Y += dX[3 * k + 1];
+    for (uint64_t k = 0; k < n; ++k) {
+        S->ow[k] = O[4 * k];
+        for (int c = 0; c < 3; ++c) {
+            S->oxyz[3 * k + c] = (float)(O[4 * k + 1 + c] / Y);
+            S->odxyz[3 * k + c] = (float)(S->odxyz[3 * k + c] / Y);
+        }
+        S->ocdf[k] = (float)(cd[k] / acc);
+    }
+    S->ocdf[n - 1] = 1;
+    S->sky_distance = in->scene_radius > 0 ? 1e3f * in->scene_radius : 1e3f;
+    return S;
+}
+
+void oracle_scene_free(void* s) {
+    Scene* S = static_cast<Scene*>(s);
+    if (S->tree) oracle_tree_free(S->tree);
+    delete S;
+}
+
+uint64_t oracle_mix64(uint64_t z) { return mix64(z); }
+
+// spectrum idx of the scene at wavelength w (Spectral Single-mode look-up)
+float oracle_spectrum_eval(void* s, int idx, float w, int reflectant) {
+    return spectrum(*static_cast<Scene*>(s), idx, w, reflectant != 0);
+}
+
+// Observer::sample and ::sensitivity of the scene's observer table
+float oracle_observer_sample(void* s, float u, float* pdf, float* xyz) {
+    const Scene& S = *static_cast<Scene*>(s);
+    const float w = observer_sample(S, u, *pdf);
+    const V c = observer_sensitivity(S, w);
+    xyz[0] = c.x;
+    xyz[1] = c.y;
+    xyz[2] = c.z;
+    return w;
+}
+
+// renders pixels [pixel_begin, pixel_end) of the image into film (8 floats per pixel, summed)
+int oracle_render(void* s, const RenderIn* R, float* film, int64_t pixel_begin, int64_t pixel_end, int threads) {
+    const Scene& S = *static_cast<Scene*>(s);
+    const int64_t npix = (int64_t)R->width * R->height;
+    if (pixel_end < 0 || pixel_end > npix) pixel_end = npix;
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    const uint64_t seed = mix64(R->seed ^ mix64(0x51ed270b27ad0e0dull + (uint64_t)(uint32_t)R->first_sample));
+    std::atomic<int64_t> next{pixel_begin};
+    auto work = [&]() {
+        while (true) {
+            const int64_t px = next.fetch_add(1);
+            if (px >= pixel_end) break;
+            float* f = film + 8 * px;
+            for (int smp = 0; smp < R->spp; ++smp) {
+                Path P;
+                P.S = &S;
+                P.R = R;
+                P.smp = Sampler{seed, (uint32_t)px, (uint32_t)smp, (uint32_t)R->spp};
+                const uint32_t ix = (uint32_t)(px % R->width), iy = (uint32_t)(px / R->width);
+                const float sx = ((float)ix + P.smp.get(D_SCREEN, true)) / (float)R->width;
+                const float sy = ((float)iy + P.smp.get(D_SCREEN + 1, true)) / (float)R->height;
+                float lpdf;
+                P.lam = observer_sample(S, P.smp.get(D_LAMBDA, true), lpdf);
+                const Camera& C = R->camera;
+                V pos{C.position[0], C.position[1], C.position[2]};
+                V dir = V{C.direction[0], C.direction[1], C.direction[2]} +
+                        (sx - 0.5f) * V{C.right[0], C.right[1], C.right[2]} + (sy - 0.5f) * V{C.down[0], C.down[1], C.down[2]};
+                dir = unit(dir);
+                const V dn{C.direction_normal[0], C.direction_normal[1], C.direction_normal[2]};
+                float factor = 1 / dot(dir, dn);
+                if (C.lens_radius > 0 && C.focus_distance > 0 && C.focus_distance < 3.4e38f) {
+                    float lx, ly;
+                    concentric(P.smp.get(D_LENS, true), P.smp.get(D_LENS + 1, true), lx, ly);
+                    const V lp = pos + (C.lens_radius * lx) * V{C.right_normal[0], C.right_normal[1], C.right_normal[2]} +
+                                 (C.lens_radius * ly) * V{C.down_normal[0], C.down_normal[1], C.down_normal[2]};
+                    const V fp = pos + (factor * C.focus_distance) * dir;
+                    pos = lp;
+                    dir = unit(fp - lp);
+                    factor = 1 / dot(dir, dn);
+                }
+                const float L = trace_photon(P, pos, dir, std::max(TOL, factor * C.near_limit), factor * C.far_limit, 0);
+                float X = 0, Yv = 0, Z = 0;
+                if (lpdf > 0) {
+                    const float sc = L / lpdf;
+                    const V c = observer_sensitivity(S, P.lam);
+                    X = sc * c.x;
+                    Yv = sc * c.y;
+                    Z = sc * c.z;
+                }
+                f[0] += X;
+                f[1] += Yv;
+                f[2] += Z;
+                f[3] += P.alpha;
+                f[4] += X * X;
+                f[5] += Yv * Yv;
+                f[6] += Z * Z;
+                f[7] += 1;
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int k = 1; k < threads; ++k) pool.emplace_back(work);
+    work();
+    for (auto& t : pool) t.join();
+    return 0;
+}
+
+}  // extern "C"

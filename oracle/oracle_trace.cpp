@@ -296,3 +296,21 @@ void oracle_tree_free(void* tree) { delete static_cast<Tree*>(tree); }
 int oracle_hardware_threads(void) { return (int)std::max(1u, std::thread::hardware_concurrency()); }
 
 }  // extern "C"
+
+// closest hit through the oracle tree, for the path-tracer restatement (oracle_render.cpp)
+namespace oracle_internal {
+struct Ray {
+    float ox, oy, oz, tmin, dx, dy, dz, tmax;
+};
+struct Hit {
+    int32_t prim;
+    float t;
+};
+Hit tree_closest(void* tree, const Ray& r) {
+    const Tree& t = *static_cast<Tree*>(tree);
+    if (t.nodes.empty()) return {-1, INFINITY};
+    const oracle_ray rr{r.ox, r.oy, r.oz, r.tmin, r.dx, r.dy, r.dz, r.tmax};
+    const oracle_hit h = trace_tree(t, rr, false);
+    return {h.prim, h.t};
+}
+}  // namespace oracle_internal
