@@ -123,6 +123,53 @@ def cpu_baseline_rays(v, f, rays, target_seconds=10.0):
                                                         f"on {threads} host threads"}
 
 
+def cornell_bench(ctx, stream, args, world, dist, local, cpu: bool) -> dict:
+    """Plain spectral path tracing of the Cornell workload (256 x 256, 16 spp, RR from generation 3,
+    depth cap 8): samples/s and path segments/s on the device, CPU restatement beside it."""
+    import torch
+    from liar_b200 import render as R, scenes_render
+    W, H, SPP = 256, 256, 16
+    e = scenes_render.cornell_engine(W, H, SPP)
+    flat = R.flatten(e.scene)
+    gs = R.GpuScene(ctx, flat)
+    desc = R.render_desc(e.camera, W, H, SPP, e.tracer, seed=0)
+    film = torch.zeros((H, W, 8), dtype=torch.float32, device=f"cuda:{local}")
+    for _ in range(max(3, args.warmup)):
+        gs.render_device(desc, film.data_ptr(), stream.cuda_stream)
+    stream.synchronize()
+    steps = max(1, min(args.steps, 20))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        gs.render_device(desc, film.data_ptr(), stream.cuda_stream)
+    e1.record(stream)
+    stream.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    st = gs.stats()
+    out = {"workload": "Cornell box 256x256, 16 spp, single wavelength, RR from generation 3, max depth 8",
+           "ms_per_frame": ms, "samples_per_s": world * st["paths"] / (ms * 1e-3),
+           "segments_per_s": world * st["segments"] / (ms * 1e-3), "segments_per_sample": st["segments"] / st["paths"],
+           "note": "device time of liar_gpu_render_device per frame; host waits for each bounce's queue size"}
+    if cpu:
+        import oracle
+        rows = 8
+        rs = oracle.RenderScene(flat)
+        cfilm = np.zeros((H, W, 8), np.float32)
+        t0 = time.perf_counter()
+        first_row = H // 2 - rows // 2
+        rs.render(desc, cfilm, pixels=(first_row * W, (first_row + rows) * W))
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": rows * W * SPP / dt, "unit": "samples/s", "cores": oracle.hardware_threads(),
+                               "kind": "port",
+                               "sample": f"{rows} middle image rows ({rows * W * SPP} samples), {dt:.1f} s"}
+    gs.close()
+    return out
+
+
 def run_reference(args, world, rank):
     """CPU restatement of the reference's path (oracle/), all host threads, bounded samples."""
     if rank != 0:
@@ -163,6 +210,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-workloads", action="store_true", help="only the traversal workload")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world, rank, local = dist_setup()
@@ -290,6 +338,9 @@ def main():
         line["cpu_baseline"] = {"value": val, "unit": "Mrays/s", "cores": info["cores"], "kind": "port",
                                 "sample": info["sample"]}
     mesh.close()
+    if not args.no_workloads:
+        line["cornell"] = cornell_bench(ctx, stream, args, world, dist, local, cpu=(rank == 0 and world == 1
+                                                                                 and not args.no_cpu_baseline))
     ctx.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
