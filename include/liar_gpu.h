@@ -229,6 +229,23 @@ int liar_gpu_render_device(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const
 /* Path statistics of the last render on ctx: [0] paths, [1] path segments traced, [2] rays that hit. */
 int liar_gpu_render_stats(const liar_gpu_ctx* ctx, unsigned long long* out3);
 
+/* ---- photon maps -------------------------------------------------------------------------------
+ * Replace the Lass KdTree<Photon> of PhotonMapper::buildPhotonMap (src/liar/tracers/photon_mapper.cpp:798-835)
+ * and its rangeSearch(point, maxRadius, maxCount) (photon_mapper.cpp:1097,1257,1312,1352): for each
+ * query point the (at most) k photons nearest to it with squared distance < r_max^2, in ascending
+ * distance (ties: lower photon index first). Photon positions are n x 3 floats. */
+typedef struct liar_gpu_photon_map liar_gpu_photon_map;
+int liar_gpu_photon_map_build(liar_gpu_ctx* ctx, const float* positions, size_t n, float r_max,
+                              liar_gpu_photon_map** out);
+int liar_gpu_photon_map_build_device(liar_gpu_ctx* ctx, const float* d_positions, size_t n, float r_max,
+                                     liar_gpu_photon_map** out, void* stream);
+void liar_gpu_photon_map_destroy(liar_gpu_photon_map* map);
+/* idx / d2: n_queries x k (unused slots: -1 / +inf); count (optional): neighbours found. k <= 64. */
+int liar_gpu_photon_gather(liar_gpu_ctx* ctx, const liar_gpu_photon_map* map, const float* queries, size_t n_queries,
+                           int k, int32_t* idx, float* d2, int32_t* count);
+int liar_gpu_photon_gather_device(liar_gpu_ctx* ctx, const liar_gpu_photon_map* map, const float* d_queries,
+                                  size_t n_queries, int k, int32_t* d_idx, float* d_d2, int32_t* d_count, void* stream);
+
 /* Allocation-free closest hit / any hit. It has no counterpart in the reference; it exists for
  * callers that must not call cudaMalloc while they trace: an application whose own pool
  * allocator owns the device memory, a frame loop whose other streams would be stalled by the

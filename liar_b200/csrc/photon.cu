@@ -1,0 +1,412 @@
+// photon.cu -- photon-map build and k-nearest gather on sm_100a.
+//
+// Replaces the Lass KdTree<Photon> that PhotonMapper::buildPhotonMap resets
+// (src/liar/tracers/photon_mapper.cpp:798-835, photon_mapper.h:153) and its rangeSearch(point,
+// maxRadius, maxCount) calls (photon_mapper.cpp:1097, 1257, 1312, 1352): the up to k photons
+// nearest to a point, all closer than r_max, the farthest first in the reference's heap.
+//
+// Build (hash grid; Teschner et al. 2003, "Optimized spatial hashing for collision detection"):
+//   cell = r_max * 1.001, cell key = floor((p - origin) / cell), bucket = hash(key) mod 2^m;
+//   counting sort of the photons by bucket (histogram, exclusive scan, scatter) into a
+//   bucket-ordered float4 array (x, y, z, original index).
+// Gather: one warp per query. The 27 cells around the query's cell are mapped to buckets, buckets
+// hit twice are visited once, and the warp streams their photons 32 at a time. The k = 64 nearest
+// are a sorted list of 64-bit keys (d^2 bits << 32 | photon index) spread over the warp (two per
+// lane); a batch of 32 candidates is sorted by a shuffle bitonic network and merged into the list
+// with half-cleaners, skipping batches in which no lane beats the current k-th key.
+// Distances use explicitly rounded IEEE operations in a fixed order, so the key of every
+// (query, photon) pair, and therefore the neighbour set including ties (equal d^2 resolve to the
+// lower index), equals the CPU restatement's.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <new>
+#include <vector>
+
+#include "../../include/liar_gpu.h"
+#include "ctx.h"
+
+using namespace liar_gpu;
+
+struct liar_gpu_photon_map {
+    int device = -1;
+    size_t n = 0;
+    float r_max = 0.0f, cell = 0.0f;
+    float origin[3] = {0, 0, 0};
+    uint32_t bucket_bits = 0;
+    float4* sorted = nullptr;      // bucket order: x, y, z, original index bits
+    uint32_t* bucket_start = nullptr;  // 2^bits + 1
+    void* scratch = nullptr;       // build scratch (bucket keys, counts), kept for rebuilds
+    size_t scratch_bytes = 0;
+};
+
+namespace {
+
+constexpr int kGatherK = 64;
+
+__host__ __device__ __forceinline__ uint32_t bucket_of(int ix, int iy, int iz, uint32_t mask) {
+    const uint32_t h = ((uint32_t)ix * 73856093u) ^ ((uint32_t)iy * 19349663u) ^ ((uint32_t)iz * 83492791u);
+    return h & mask;
+}
+
+__device__ __forceinline__ int cell_coord(float p, float o, float inv) { return (int)floorf((p - o) * inv); }
+
+// squared distance with fixed IEEE roundings (the CPU restatement performs the same operations)
+__device__ __forceinline__ float dist2_exact(float px, float py, float pz, float qx, float qy, float qz) {
+    const float dx = __fsub_rn(px, qx), dy = __fsub_rn(py, qy), dz = __fsub_rn(pz, qz);
+    return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+}
+
+struct BuildParams {
+    float ox, oy, oz, inv;
+    uint32_t mask;
+};
+
+__global__ void k_bucket_count(const float* __restrict__ pos, uint32_t n, BuildParams P, uint32_t* __restrict__ keys,
+                               uint32_t* __restrict__ counts) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
+    const uint32_t b = bucket_of(cell_coord(x, P.ox, P.inv), cell_coord(y, P.oy, P.inv), cell_coord(z, P.oz, P.inv), P.mask);
+    keys[i] = b;
+    atomicAdd(counts + b, 1u);
+}
+
+// exclusive scan of `counts` (n_buckets + 1 entries written to `start`), one block per 1024 x 4 entries
+constexpr int kScanBlock = 1024;
+constexpr int kScanItems = 4;
+
+__global__ void k_scan_local(const uint32_t* __restrict__ in, uint32_t n, uint32_t* __restrict__ out,
+                             uint32_t* __restrict__ block_sums) {
+    __shared__ uint32_t warp_sums[32];
+    const uint32_t base = blockIdx.x * kScanBlock * kScanItems + threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        v[k] = base + k < n ? in[base + k] : 0u;
+        s += v[k];
+    }
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t incl = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += t;
+    }
+    if (lane == 31) warp_sums[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < (kScanBlock / 32) ? warp_sums[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= (uint32_t)o) w += t;
+        }
+        warp_sums[lane] = w;
+    }
+    __syncthreads();
+    uint32_t run = incl - s + (warp > 0 ? warp_sums[warp - 1] : 0u);
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        if (base + k < n) out[base + k] = run;
+        run += v[k];
+    }
+    if (threadIdx.x == kScanBlock - 1) block_sums[blockIdx.x] = run;
+}
+
+__global__ void k_scan_add(uint32_t* __restrict__ out, uint32_t n, const uint32_t* __restrict__ block_offsets) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] += block_offsets[i / (kScanBlock * kScanItems)];
+}
+
+__global__ void k_scatter(const float* __restrict__ pos, uint32_t n, const uint32_t* __restrict__ keys,
+                          uint32_t* __restrict__ cursor, float4* __restrict__ sorted) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t slot = atomicAdd(cursor + keys[i], 1u);
+    sorted[slot] = make_float4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], __uint_as_float(i));
+}
+
+// ---- warp sorting helpers on 64-bit keys
+__device__ __forceinline__ uint64_t shfl_xor64(uint64_t v, int m) {
+    return __shfl_xor_sync(0xffffffffu, (unsigned long long)v, m);
+}
+// compare-exchange of lanes l and l^j; ascending where `up` holds for the pair's lower lane
+__device__ __forceinline__ uint64_t cmpx(uint64_t v, int j, bool up) {
+    const uint64_t o = shfl_xor64(v, j);
+    const bool lower = ((threadIdx.x & 31u) & (uint32_t)j) == 0u;
+    const bool take_min = lower == up;
+    return take_min ? (v < o ? v : o) : (v > o ? v : o);
+}
+// full ascending bitonic sort of one key per lane
+__device__ __forceinline__ uint64_t warp_sort32(uint64_t v) {
+    const uint32_t lane = threadIdx.x & 31u;
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) v = cmpx(v, j, (lane & (uint32_t)k) == 0u);
+    }
+    return v;
+}
+// sorts a bitonic sequence of one key per lane ascending
+__device__ __forceinline__ uint64_t warp_bitonic_merge32(uint64_t v) {
+#pragma unroll
+    for (int j = 16; j > 0; j >>= 1) v = cmpx(v, j, true);
+    return v;
+}
+__device__ __forceinline__ uint64_t reverse_lanes(uint64_t v) {
+    return __shfl_sync(0xffffffffu, (unsigned long long)v, 31 - (threadIdx.x & 31u));
+}
+
+__global__ void __launch_bounds__(256) k_gather(const float4* __restrict__ sorted, const uint32_t* __restrict__ start,
+                                                BuildParams P, float r2max, const float* __restrict__ queries,
+                                                uint32_t nq, int k_out, int32_t* __restrict__ out_idx,
+                                                float* __restrict__ out_d2, int32_t* __restrict__ out_count) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
+    constexpr uint64_t INF = ~0ull;
+    for (uint32_t q = warp_global; q < nq; q += n_warps) {
+        const float qx = queries[3 * q], qy = queries[3 * q + 1], qz = queries[3 * q + 2];
+        const int cx = cell_coord(qx, P.ox, P.inv), cy = cell_coord(qy, P.oy, P.inv), cz = cell_coord(qz, P.oz, P.inv);
+        // the 27 neighbour buckets, one per lane (lanes 27..31 idle); drop repeats
+        uint32_t my_bucket = 0xffffffffu;
+        if (lane < 27) {
+            const int dx = (int)(lane % 3) - 1, dy = (int)((lane / 3) % 3) - 1, dz = (int)(lane / 9) - 1;
+            my_bucket = bucket_of(cx + dx, cy + dy, cz + dz, P.mask);
+        }
+        bool first = lane < 27;
+#pragma unroll 1
+        for (int o = 0; o < 27; ++o) {
+            const uint32_t other = __shfl_sync(0xffffffffu, my_bucket, o);
+            if ((uint32_t)o < lane && other == my_bucket) first = false;
+        }
+        uint32_t todo = __ballot_sync(0xffffffffu, first);
+        // the k nearest so far, ascending: slot `lane` in lo, slot `32 + lane` in hi
+        uint64_t lo = INF, hi = INF;
+        uint64_t kth = INF;  // key of the current k-th (64th) nearest
+        while (todo) {
+            const int src = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const uint32_t b = __shfl_sync(0xffffffffu, my_bucket, src);
+            const uint32_t s0 = __ldg(start + b), s1 = __ldg(start + b + 1);
+            for (uint32_t base = s0; base < s1; base += 32) {
+                uint64_t key = INF;
+                const uint32_t i = base + lane;
+                if (i < s1) {
+                    const float4 p = __ldg(sorted + i);
+                    const float d2 = dist2_exact(p.x, p.y, p.z, qx, qy, qz);
+                    if (d2 < r2max) key = ((uint64_t)__float_as_uint(d2) << 32) | (uint64_t)__float_as_uint(p.w);
+                }
+                if (__ballot_sync(0xffffffffu, key < kth) == 0u) continue;
+                // merge the batch into the 64 nearest
+                uint64_t bsort = warp_sort32(key);
+                // smallest 32 of hi and the batch: half-cleaner against the reversed batch
+                uint64_t m = hi < reverse_lanes(bsort) ? hi : reverse_lanes(bsort);
+                m = warp_bitonic_merge32(m);
+                // lo (sorted) and m (sorted): split into the lower and upper 32
+                const uint64_t mr = reverse_lanes(m);
+                uint64_t nlo = lo < mr ? lo : mr;
+                uint64_t nhi = lo < mr ? mr : lo;
+                lo = warp_bitonic_merge32(nlo);
+                hi = warp_bitonic_merge32(nhi);
+                kth = __shfl_sync(0xffffffffu, (unsigned long long)hi, 31);
+            }
+        }
+        // write the first k_out entries (k_out <= 64) in ascending order
+        const uint32_t cnt_lo = __popc(__ballot_sync(0xffffffffu, lo != INF));
+        const uint32_t cnt_hi = __popc(__ballot_sync(0xffffffffu, hi != INF));
+        const int count = min((int)(cnt_lo + cnt_hi), k_out);
+        int32_t* oi = out_idx + (size_t)q * k_out;
+        float* od = out_d2 + (size_t)q * k_out;
+        if ((int)lane < k_out) {
+            oi[lane] = lo != INF ? (int32_t)(uint32_t)lo : -1;
+            od[lane] = lo != INF ? __uint_as_float((uint32_t)(lo >> 32)) : INFINITY;
+        }
+        if ((int)(32 + lane) < k_out) {
+            oi[32 + lane] = hi != INF ? (int32_t)(uint32_t)hi : -1;
+            od[32 + lane] = hi != INF ? __uint_as_float((uint32_t)(hi >> 32)) : INFINITY;
+        }
+        if (lane == 0 && out_count) out_count[q] = count;
+    }
+}
+
+int map_build_impl(liar_gpu_ctx* ctx, liar_gpu_photon_map* m, const float* d_pos, size_t n, cudaStream_t st) {
+    // bounding box on the host side of the caller's data is not available for device input: the
+    // origin only has to be consistent between build and gather, so a fixed origin is used
+    m->origin[0] = m->origin[1] = m->origin[2] = 0.0f;
+    // buckets: the next power of two >= 2n, at most 2^23 (the two-level scan covers 2^24 entries)
+    uint32_t bits = 10;
+    while (bits < 23 && (1ull << bits) < 2ull * n) ++bits;
+    m->bucket_bits = bits;
+    const size_t nb = (size_t)1 << bits;
+    const size_t scan_blocks = (nb + 1 + kScanBlock * kScanItems - 1) / (kScanBlock * kScanItems);
+    const size_t need = n * 4 + (nb + 1) * 4 + (nb + 1) * 4 + (scan_blocks + 1) * 8 + 1024;
+    if (m->scratch_bytes < need) {
+        if (m->scratch) cudaFree(m->scratch);
+        m->scratch = nullptr;
+        m->scratch_bytes = 0;
+        cudaError_t e = cudaMalloc(&m->scratch, need);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return ctx_cuda(ctx, e, "photon map build scratch");
+        }
+        m->scratch_bytes = need;
+    }
+    if (m->sorted) cudaFree(m->sorted);
+    if (m->bucket_start) cudaFree(m->bucket_start);
+    m->sorted = nullptr;
+    m->bucket_start = nullptr;
+    cudaError_t e = cudaMalloc((void**)&m->sorted, std::max<size_t>(n, 1) * sizeof(float4));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&m->bucket_start, (nb + 1) * sizeof(uint32_t));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return ctx_cuda(ctx, e, "photon map");
+    }
+    char* p = static_cast<char*>(m->scratch);
+    uint32_t* keys = reinterpret_cast<uint32_t*>(p);
+    p += ((n * 4 + 255) / 256) * 256;
+    uint32_t* counts = reinterpret_cast<uint32_t*>(p);
+    p += (((nb + 1) * 4 + 255) / 256) * 256;
+    uint32_t* cursor = reinterpret_cast<uint32_t*>(p);
+    p += (((nb + 1) * 4 + 255) / 256) * 256;
+    uint32_t* block_sums = reinterpret_cast<uint32_t*>(p);
+    uint32_t* block_offs = block_sums + scan_blocks + 1;
+    BuildParams P{m->origin[0], m->origin[1], m->origin[2], 1.0f / m->cell, (uint32_t)(nb - 1)};
+    e = cudaMemsetAsync(counts, 0, (nb + 1) * 4, st);
+    if (e != cudaSuccess) return ctx_cuda(ctx, e, "photon map counts");
+    if (n) k_bucket_count<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_pos, (uint32_t)n, P, keys, counts);
+    // exclusive scan of counts[0 .. nb] -> bucket_start (start[nb] = n)
+    k_scan_local<<<(unsigned)scan_blocks, kScanBlock, 0, st>>>(counts, (uint32_t)(nb + 1), m->bucket_start, block_sums);
+    if (scan_blocks > 1) {
+        // scan of the block sums (scan_blocks <= 2^26 / 4096 = 16384 entries: one more level)
+        const size_t blocks2 = (scan_blocks + kScanBlock * kScanItems - 1) / (kScanBlock * kScanItems);
+        if (blocks2 > 1) return ctx_fail(ctx, LIAR_ERR_UNSUPPORTED, "photon map too large to scan");
+        k_scan_local<<<1, kScanBlock, 0, st>>>(block_sums, (uint32_t)scan_blocks, block_offs, block_sums + scan_blocks);
+        k_scan_add<<<(unsigned)((nb + 1 + 255) / 256), 256, 0, st>>>(m->bucket_start, (uint32_t)(nb + 1), block_offs);
+    }
+    e = cudaMemcpyAsync(cursor, m->bucket_start, (nb + 1) * 4, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return ctx_cuda(ctx, e, "photon map cursor");
+    if (n) k_scatter<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_pos, (uint32_t)n, keys, cursor, m->sorted);
+    m->n = n;
+    return ctx_cuda(ctx, cudaGetLastError(), "photon map build");
+}
+
+}  // namespace
+
+extern "C" int liar_gpu_photon_map_build_device(liar_gpu_ctx* ctx, const float* d_positions, size_t n, float r_max,
+                                                liar_gpu_photon_map** out, void* stream) {
+    if (!ctx || !out) return LIAR_ERR_INVALID;
+    *out = nullptr;
+    if (n && !d_positions) return ctx_fail(ctx, LIAR_ERR_INVALID, "null photon positions");
+    if (!(r_max > 0.0f) || !std::isfinite(r_max)) return ctx_fail(ctx, LIAR_ERR_INVALID, "r_max must be positive");
+    if (n >= (1ull << 31)) return ctx_fail(ctx, LIAR_ERR_INVALID, "too many photons (limit 2^31)");
+    int rc = ctx_activate(ctx);
+    if (rc) return rc;
+    liar_gpu_photon_map* m = new (std::nothrow) liar_gpu_photon_map();
+    if (!m) return ctx_fail(ctx, LIAR_ERR_OOM, "host allocation");
+    m->device = ctx->device;
+    m->r_max = r_max;
+    m->cell = r_max * 1.001f;
+    rc = map_build_impl(ctx, m, d_positions, n, stream ? (cudaStream_t)stream : ctx->stream);
+    if (rc) {
+        liar_gpu_photon_map_destroy(m);
+        return rc;
+    }
+    *out = m;
+    return LIAR_OK;
+}
+
+extern "C" int liar_gpu_photon_map_build(liar_gpu_ctx* ctx, const float* positions, size_t n, float r_max,
+                                         liar_gpu_photon_map** out) {
+    if (!ctx || !out) return LIAR_ERR_INVALID;
+    *out = nullptr;
+    if (n && !positions) return ctx_fail(ctx, LIAR_ERR_INVALID, "null photon positions");
+    for (size_t i = 0; i < 3 * n; ++i)
+        if (!std::isfinite(positions[i])) return ctx_fail(ctx, LIAR_ERR_INVALID, "photon position is not finite");
+    int rc = ctx_activate(ctx);
+    if (rc) return rc;
+    float* d = nullptr;
+    cudaError_t e = cudaMalloc((void**)&d, std::max<size_t>(n, 1) * 12);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return ctx_cuda(ctx, e, "photon upload");
+    }
+    e = cudaMemcpyAsync(d, positions, n * 12, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) rc = liar_gpu_photon_map_build_device(ctx, d, n, r_max, out, ctx->stream);
+    else rc = ctx_cuda(ctx, e, "photon upload");
+    if (!rc) rc = ctx_cuda(ctx, cudaStreamSynchronize(ctx->stream), "photon map build");
+    cudaFree(d);
+    if (rc && *out) {
+        liar_gpu_photon_map_destroy(*out);
+        *out = nullptr;
+    }
+    return rc;
+}
+
+extern "C" void liar_gpu_photon_map_destroy(liar_gpu_photon_map* m) {
+    if (!m) return;
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (m->device >= 0) cudaSetDevice(m->device);
+    if (m->sorted) cudaFree(m->sorted);
+    if (m->bucket_start) cudaFree(m->bucket_start);
+    if (m->scratch) cudaFree(m->scratch);
+    if (cur >= 0) cudaSetDevice(cur);
+    delete m;
+}
+
+extern "C" int liar_gpu_photon_gather_device(liar_gpu_ctx* ctx, const liar_gpu_photon_map* m, const float* d_queries,
+                                             size_t n_queries, int k, int32_t* d_idx, float* d_d2, int32_t* d_count,
+                                             void* stream) {
+    if (!ctx) return LIAR_ERR_INVALID;
+    if (!m || (n_queries && (!d_queries || !d_idx || !d_d2))) return ctx_fail(ctx, LIAR_ERR_INVALID, "null map or buffer");
+    if (k < 1 || k > kGatherK) return ctx_fail(ctx, LIAR_ERR_INVALID, "k must be 1..%d", kGatherK);
+    if (m->device != ctx->device) return ctx_fail(ctx, LIAR_ERR_INVALID, "photon map lives on another device");
+    if (n_queries >= (1ull << 31)) return ctx_fail(ctx, LIAR_ERR_INVALID, "too many queries");
+    if (n_queries == 0) return LIAR_OK;
+    int rc = ctx_activate(ctx);
+    if (rc) return rc;
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    BuildParams P{m->origin[0], m->origin[1], m->origin[2], 1.0f / m->cell, (uint32_t)(((size_t)1 << m->bucket_bits) - 1)};
+    const float r2 = m->r_max * m->r_max;
+    const unsigned blocks = (unsigned)std::min<size_t>((n_queries + 7) / 8, (size_t)ctx->num_sms * 8);
+    k_gather<<<blocks, 256, 0, st>>>(m->sorted, m->bucket_start, P, r2, d_queries, (uint32_t)n_queries, k, d_idx, d_d2,
+                                     d_count);
+    return ctx_cuda(ctx, cudaGetLastError(), "photon gather launch");
+}
+
+extern "C" int liar_gpu_photon_gather(liar_gpu_ctx* ctx, const liar_gpu_photon_map* m, const float* queries,
+                                      size_t n_queries, int k, int32_t* idx, float* d2, int32_t* count) {
+    if (!ctx) return LIAR_ERR_INVALID;
+    if (!m || (n_queries && (!queries || !idx || !d2))) return ctx_fail(ctx, LIAR_ERR_INVALID, "null map or buffer");
+    if (k < 1 || k > kGatherK) return ctx_fail(ctx, LIAR_ERR_INVALID, "k must be 1..%d", kGatherK);
+    if (n_queries == 0) return LIAR_OK;
+    int rc = ctx_activate(ctx);
+    if (rc) return rc;
+    const size_t qb = n_queries * 12, ob = n_queries * (size_t)k * 4, cb = n_queries * 4;
+    char* d = nullptr;
+    cudaError_t e = cudaMalloc((void**)&d, qb + 2 * ob + cb + 64);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return ctx_cuda(ctx, e, "gather buffers");
+    }
+    float* dq = reinterpret_cast<float*>(d);
+    int32_t* di = reinterpret_cast<int32_t*>(d + qb);
+    float* dd = reinterpret_cast<float*>(d + qb + ob);
+    int32_t* dc = reinterpret_cast<int32_t*>(d + qb + 2 * ob);
+    e = cudaMemcpyAsync(dq, queries, qb, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) rc = liar_gpu_photon_gather_device(ctx, m, dq, n_queries, k, di, dd, dc, ctx->stream);
+    else rc = ctx_cuda(ctx, e, "query upload");
+    if (!rc) {
+        e = cudaMemcpyAsync(idx, di, ob, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(d2, dd, ob, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess && count) e = cudaMemcpyAsync(count, dc, cb, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) rc = ctx_cuda(ctx, e, "gather results");
+    }
+    cudaFree(d);
+    return rc;
+}

@@ -138,3 +138,19 @@ class Tree:
                 self.h = None
         except Exception:
             pass
+
+
+def knn(photons, queries, k, r_max, threads=0):
+    """Brute-force k nearest photons within r_max: (idx, d2, count) like liar_gpu_photon_gather."""
+    L = lib()
+    L.oracle_knn.restype = C.c_int
+    L.oracle_knn.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_int, C.c_float, C.c_void_p,
+                             C.c_void_p, C.c_void_p, C.c_int]
+    P = _f32(photons).reshape(-1, 3)
+    Q = _f32(queries).reshape(-1, 3)
+    idx = np.empty((Q.shape[0], k), np.int32)
+    d2 = np.empty((Q.shape[0], k), np.float32)
+    cnt = np.empty(Q.shape[0], np.int32)
+    L.oracle_knn(P.ctypes.data, P.shape[0], Q.ctypes.data, Q.shape[0], int(k), float(r_max), idx.ctypes.data,
+                 d2.ctypes.data, cnt.ctypes.data, int(threads))
+    return idx, d2, cnt

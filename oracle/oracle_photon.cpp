@@ -1,0 +1,49 @@
+// oracle_photon.cpp -- CPU ORACLE (test infrastructure only) of the photon-map gather.
+//
+// Restates KdTree::rangeSearch(point, maxRadius, maxCount) as the reference's PhotonMapper uses it
+// (src/liar/tracers/photon_mapper.cpp:1257, 1312, 1352; the tree is Lass's spat::KdTree, pinned
+// as lass/1.11.0-250+g078d9309 and absent from the reference tree): the at most k photons with
+// squared distance < r_max^2 nearest to the query. Exact brute force over all photons, squared
+// distances evaluated as ((dx*dx + dy*dy) + dz*dz) in IEEE single (compiled without
+// contraction), ordered by (distance, index). Neighbour sets are therefore exact; agreement
+// with Lass's own tie handling at equal distance is unpinned.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <thread>
+#include <utility>
+#include <vector>
+
+extern "C" int oracle_knn(const float* photons, uint64_t n, const float* queries, uint64_t nq, int k, float r_max,
+                          int32_t* idx, float* d2, int32_t* count, int threads) {
+    const float r2 = r_max * r_max;
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    std::atomic<uint64_t> next{0};
+    auto work = [&]() {
+        std::vector<std::pair<float, int32_t>> cand;
+        while (true) {
+            const uint64_t q = next.fetch_add(1);
+            if (q >= nq) break;
+            const float qx = queries[3 * q], qy = queries[3 * q + 1], qz = queries[3 * q + 2];
+            cand.clear();
+            for (uint64_t i = 0; i < n; ++i) {
+                const float dx = photons[3 * i] - qx, dy = photons[3 * i + 1] - qy, dz = photons[3 * i + 2] - qz;
+                const float dd = (dx * dx + dy * dy) + dz * dz;
+                if (dd < r2) cand.emplace_back(dd, (int32_t)i);
+            }
+            const size_t m = std::min<size_t>(cand.size(), (size_t)k);
+            std::partial_sort(cand.begin(), cand.begin() + m, cand.end());
+            for (int j = 0; j < k; ++j) {
+                idx[q * k + j] = (size_t)j < m ? cand[j].second : -1;
+                d2[q * k + j] = (size_t)j < m ? cand[j].first : INFINITY;
+            }
+            if (count) count[q] = (int32_t)m;
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < threads; ++t) pool.emplace_back(work);
+    work();
+    for (auto& t : pool) t.join();
+    return 0;
+}
