@@ -121,11 +121,18 @@ __global__ void k_scan_add(uint32_t* __restrict__ out, uint32_t n, const uint32_
     if (i < n) out[i] += block_offsets[i / (kScanBlock * kScanItems)];
 }
 
+// device-side status bits of the photon kernels (ORed into the context's status word)
+constexpr uint32_t kStatusBadBucket = 1u << 4;
+
 __global__ void k_scatter(const float* __restrict__ pos, uint32_t n, const uint32_t* __restrict__ keys,
-                          uint32_t* __restrict__ cursor, float4* __restrict__ sorted) {
+                          uint32_t* __restrict__ cursor, float4* __restrict__ sorted, uint32_t* __restrict__ status) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t slot = atomicAdd(cursor + keys[i], 1u);
+    if (slot >= n) {  // a bucket range past the photon array: record it, write nothing
+        atomicOr(status, kStatusBadBucket);
+        return;
+    }
     sorted[slot] = make_float4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], __uint_as_float(i));
 }
 
@@ -163,7 +170,8 @@ __device__ __forceinline__ uint64_t reverse_lanes(uint64_t v) {
 __global__ void __launch_bounds__(256) k_gather(const float4* __restrict__ sorted, const uint32_t* __restrict__ start,
                                                 BuildParams P, float r2max, const float* __restrict__ queries,
                                                 uint32_t nq, int k_out, int32_t* __restrict__ out_idx,
-                                                float* __restrict__ out_d2, int32_t* __restrict__ out_count) {
+                                                float* __restrict__ out_d2, int32_t* __restrict__ out_count,
+                                                uint32_t n_photons, uint32_t* __restrict__ status) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
@@ -192,6 +200,10 @@ __global__ void __launch_bounds__(256) k_gather(const float4* __restrict__ sorte
             todo &= todo - 1;
             const uint32_t b = __shfl_sync(0xffffffffu, my_bucket, src);
             const uint32_t s0 = __ldg(start + b), s1 = __ldg(start + b + 1);
+            if (s0 > s1 || s1 > n_photons) {  // a corrupt bucket range: record it and skip the bucket
+                if (lane == 0) atomicOr(status, kStatusBadBucket);
+                continue;
+            }
             for (uint32_t base = s0; base < s1; base += 32) {
                 uint64_t key = INF;
                 const uint32_t i = base + lane;
@@ -202,9 +214,11 @@ __global__ void __launch_bounds__(256) k_gather(const float4* __restrict__ sorte
                 }
                 if (__ballot_sync(0xffffffffu, key < kth) == 0u) continue;
                 // merge the batch into the 64 nearest
-                uint64_t bsort = warp_sort32(key);
-                // smallest 32 of hi and the batch: half-cleaner against the reversed batch
-                uint64_t m = hi < reverse_lanes(bsort) ? hi : reverse_lanes(bsort);
+                const uint64_t bsort = warp_sort32(key);
+                // smallest 32 of hi and the batch: half-cleaner against the reversed batch (every
+                // shuffle is executed by all 32 lanes, outside any lane-dependent branch)
+                const uint64_t brev = reverse_lanes(bsort);
+                uint64_t m = hi < brev ? hi : brev;
                 m = warp_bitonic_merge32(m);
                 // lo (sorted) and m (sorted): split into the lower and upper 32
                 const uint64_t mr = reverse_lanes(m);
@@ -289,7 +303,9 @@ int map_build_impl(liar_gpu_ctx* ctx, liar_gpu_photon_map* m, const float* d_pos
     }
     e = cudaMemcpyAsync(cursor, m->bucket_start, (nb + 1) * 4, cudaMemcpyDeviceToDevice, st);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "photon map cursor");
-    if (n) k_scatter<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_pos, (uint32_t)n, keys, cursor, m->sorted);
+    if (n)
+        k_scatter<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_pos, (uint32_t)n, keys, cursor, m->sorted,
+                                                              ctx->d_scratch + kStatusWord);
     m->n = n;
     return ctx_cuda(ctx, cudaGetLastError(), "photon map build");
 }
@@ -374,7 +390,7 @@ extern "C" int liar_gpu_photon_gather_device(liar_gpu_ctx* ctx, const liar_gpu_p
     const float r2 = m->r_max * m->r_max;
     const unsigned blocks = (unsigned)std::min<size_t>((n_queries + 7) / 8, (size_t)ctx->num_sms * 8);
     k_gather<<<blocks, 256, 0, st>>>(m->sorted, m->bucket_start, P, r2, d_queries, (uint32_t)n_queries, k, d_idx, d_d2,
-                                     d_count);
+                                     d_count, (uint32_t)m->n, ctx->d_scratch + kStatusWord);
     return ctx_cuda(ctx, cudaGetLastError(), "photon gather launch");
 }
 
