@@ -246,6 +246,38 @@ int liar_gpu_photon_gather(liar_gpu_ctx* ctx, const liar_gpu_photon_map* map, co
 int liar_gpu_photon_gather_device(liar_gpu_ctx* ctx, const liar_gpu_photon_map* map, const float* d_queries,
                                   size_t n_queries, int k, int32_t* d_idx, float* d_d2, int32_t* d_count, void* stream);
 
+/* ---- photon tracing ------------------------------------------------------------------------------
+ * PhotonMapper::fillPhotonMaps / emitPhoton / tracePhoton (src/liar/tracers/photon_mapper.cpp:573-796):
+ * photons leave the scene's lights (chosen by power), carry power at one wavelength, scatter by
+ * BSDF sampling with power-preserving Russian roulette (kernel/kernel_common.h:160) and are stored at
+ * hits on surfaces with a diffuse BSDF: into the caustic map when every bounce so far was specular
+ * or glossy, into the global map when not caustic and not a direct hit (isRayTracingDirect).
+ * Photons are emitted in waves of `wave` until the global map holds `global_target` photons or
+ * `max_emitted` photons have left the lights. Stored power is XYZ (the reference's Photon record),
+ * not yet divided by the number emitted. */
+enum liar_photon_map_kind { LIAR_PHOTON_GLOBAL = 1, LIAR_PHOTON_CAUSTIC = 2 };
+typedef struct liar_photon_desc {
+    int32_t max_ray_generation;  /* photon bounces (reference default 8) */
+    int32_t ray_traced_direct;   /* 1: direct photons are not stored in the global map */
+    uint64_t seed;
+    uint64_t global_target;      /* globalMapSize */
+    uint64_t max_emitted;        /* maxNumberOfPhotons */
+    uint64_t wave;               /* photons emitted per wave, 0 = automatic */
+} liar_photon_desc;
+typedef struct liar_photon_buffers {  /* device arrays of `capacity` photons */
+    float* position;   /* x 3 */
+    float* omega_in;   /* x 3: direction toward where the photon came from */
+    float* power;      /* x 3: XYZ */
+    uint32_t* path;    /* index of the emitted photon */
+    uint32_t* tag;     /* map kind (bits 0-1) | bounce << 8 */
+    uint64_t capacity;
+} liar_photon_buffers;
+typedef struct liar_photon_counts {
+    uint64_t stored, global, caustic, emitted;
+} liar_photon_counts;
+int liar_gpu_photon_trace(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_photon_desc* desc,
+                          const liar_photon_buffers* out, liar_photon_counts* counts, void* stream);
+
 /* Allocation-free closest hit / any hit. It has no counterpart in the reference; it exists for
  * callers that must not call cudaMalloc while they trace: an application whose own pool
  * allocator owns the device memory, a frame loop whose other streams would be stalled by the

@@ -205,39 +205,11 @@ __global__ void __launch_bounds__(128) k_shade(DScene S, WaveParams W, Paths P, 
         } else {
             ++n_hit;
             if (gen == 0) P.alpha[p] = 1.0f;
-            const uint32_t prim = (uint32_t)h.prim;
-            const int obj = S.tri_obj[prim];
-            const int light = S.obj_light[obj];
-            const int mi = S.obj_mat[obj];
-            // ---- IntersectionContext: re-intersect the hit triangle (TriangleMesh::doLocalContext)
-            const uint32_t i0 = S.tri_idx[3 * prim], i1 = S.tri_idx[3 * prim + 1], i2 = S.tri_idx[3 * prim + 2];
-            const float3 a = mk(S.verts[3 * i0], S.verts[3 * i0 + 1], S.verts[3 * i0 + 2]);
-            const float3 b = mk(S.verts[3 * i1], S.verts[3 * i1 + 1], S.verts[3 * i1 + 2]);
-            const float3 c = mk(S.verts[3 * i2], S.verts[3 * i2 + 1], S.verts[3 * i2 + 2]);
-            const float3 e1 = b - a, e2 = c - a;
-            float tt, bu, bv;
-            if (!tri_intersect_exact(o.x, o.y, o.z, d.x, d.y, d.z, a.x, a.y, a.z, e1.x, e1.y, e1.z, e2.x, e2.y, e2.z, tt,
-                                     bu, bv)) {
-                bu = bv = 0.0f;
-            }
-            const float3 target = a + bu * e1 + bv * e2;
-            const float3 ng0 = normal(cross(e1, e2));
-            float3 ns = ng0;
-            if (S.tri_nrm) {
-                const int n0 = S.tri_nrm[3 * prim], n1 = S.tri_nrm[3 * prim + 1], n2 = S.tri_nrm[3 * prim + 2];
-                if (n0 >= 0 && n1 >= 0 && n2 >= 0) {
-                    const float w0 = 1.0f - bu - bv;
-                    ns = normal(w0 * mk(S.normals[3 * n0], S.normals[3 * n0 + 1], S.normals[3 * n0 + 2]) +
-                                bu * mk(S.normals[3 * n1], S.normals[3 * n1 + 1], S.normals[3 * n1 + 2]) +
-                                bv * mk(S.normals[3 * n2], S.normals[3 * n2 + 1], S.normals[3 * n2 + 2]));
-                }
-            }
-            // solid event from the unflipped geometric normal (triangle_mesh.cpp:303-308)
-            const float dd = dot(d, ng0);
-            const bool leaving = dd > 0.0f;
-            // flipTo(-direction) (kernel/intersection_context.cpp:278-290)
-            const float3 ng = dot(ng0, -d) < 0.0f ? -ng0 : ng0;
-            const float3 N = dot(ns, -d) < 0.0f ? -ns : ns;
+            // ---- IntersectionContext of the hit (re-intersection, normals flipped toward -d, frame)
+            const HitContext H = hit_context(S, o, d, (uint32_t)h.prim);
+            const int light = H.light;
+            const int mi = H.mat;
+            const float3 target = H.target, ng = H.ng, N = H.N, u = H.u, v = H.v;
             if (gen > 0 && light >= 0) {
                 // LightArea::doEmission: radiance of the light object that was hit
                 L += T * spec_eval(S, S.lights[light].spectrum, lam, false);
@@ -253,74 +225,7 @@ __global__ void __launch_bounds__(128) k_shade(DScene S, WaveParams W, Paths P, 
             } else {
                 const liar_material M = S.mats[mi];
                 if (light < 0 && M.emission >= 0) L += T * spec_eval(S, M.emission, lam, false);
-                // ---- shading frame (IntersectionContext::bsdfToLocal, intersection_context.cpp:197-222)
-                float3 u = e1 - dot(e1, N) * N;
-                float3 v = e2 - dot(e2, N) * N;
-                const float su = dot(u, u), sv = dot(v, v);
-                if (fmaxf(su, sv) < 1e-3f * fmaxf(dot(e1, e1), dot(e2, e2))) {
-                    const float3 ax = fabsf(N.x) < 0.9f ? mk(1, 0, 0) : mk(0, 1, 0);
-                    u = cross(ax, N);
-                    v = cross(N, u);
-                }
-                if (su >= sv) {
-                    u = normal(u);
-                    v = cross(N, u);
-                } else {
-                    v = normal(v);
-                    u = cross(v, N);
-                }
-                // ---- the BSDF at this wavelength (Shader::bsdf)
-                Bsdf B;
-                B.type = (uint32_t)M.type;
-                B.mdf = M.mdf;
-                B.ng = mk(dot(ng, u), dot(ng, v), dot(ng, N));
-                B.r = B.t = 0.0f;
-                B.eta = B.kappa = B.ior = B.eta_i = B.eta_t = 1.0f;
-                B.au = sqr(fmaxf(M.rough_u, 1e-3f));
-                B.av = sqr(fmaxf(M.rough_v, 1e-3f));
-                switch (M.type) {
-                    case LIAR_MAT_LAMBERT:
-                        B.caps = CAP_REFL | CAP_DIFF;
-                        B.r = spec_eval(S, M.spec[0], lam, true);
-                        break;
-                    case LIAR_MAT_CONDUCTOR:
-                    case LIAR_MAT_COOK_TORRANCE:
-                        B.caps = M.type == LIAR_MAT_CONDUCTOR ? (CAP_REFL | CAP_SPEC) : (CAP_REFL | CAP_GLOSSY);
-                        B.eta = fmaxf(spec_eval(S, M.spec[0], lam, false), 1e-9f);
-                        B.kappa = fmaxf(spec_eval(S, M.spec[1], lam, false), 1e-9f);
-                        B.r = spec_eval(S, M.spec[2], lam, true);
-                        break;
-                    case LIAR_MAT_DIELECTRIC: {
-                        B.caps = CAP_REFL | CAP_TRANS | CAP_SPEC;
-                        const float ior1 = fmaxf(spec_eval(S, M.spec[1], lam, false), 1e-9f);
-                        const float ior2 = fmaxf(spec_eval(S, M.spec[0], lam, false), 1e-9f);
-                        B.ior = leaving ? ior2 / ior1 : ior1 / ior2;
-                        B.r = spec_eval(S, M.spec[2], lam, true);
-                        B.t = spec_eval(S, M.spec[3], lam, true);
-                        break;
-                    }
-                    case LIAR_MAT_WALTER: {
-                        B.caps = CAP_TRANS | CAP_GLOSSY;  // as constructed by Walter::Bsdf (walter.cpp:247)
-                        float ei = fmaxf(spec_eval(S, M.spec[1], lam, false), 1e-9f);
-                        float et = fmaxf(spec_eval(S, M.spec[0], lam, false), 1e-9f);
-                        if (leaving) {
-                            const float tmp = ei;
-                            ei = et;
-                            et = tmp;
-                        }
-                        B.eta_i = ei;
-                        B.eta_t = et;
-                        B.r = spec_eval(S, M.spec[2], lam, true);
-                        B.t = spec_eval(S, M.spec[3], lam, true);
-                        break;
-                    }
-                    case LIAR_MAT_MIRROR:
-                        B.caps = CAP_REFL | CAP_SPEC;
-                        B.r = spec_eval(S, M.spec[0], lam, true);
-                        break;
-                    default:
-                        B.caps = 0;
-                }
+                const Bsdf B = make_bsdf(S, M, H, lam);  // Shader::bsdf at this wavelength
                 const float3 md = -d;
                 float3 wi = mk(dot(md, u), dot(md, v), dot(md, N));
                 wi.z = fmaxf(wi.z, kEps);
@@ -667,6 +572,15 @@ extern "C" int liar_gpu_scene_upload(liar_gpu_ctx* ctx, const liar_scene_desc* d
     *out = s;
     return LIAR_OK;
 }
+
+namespace liar_gpu {
+namespace rt {
+// accessors for the other subsystems that shade against an uploaded scene (photon tracing)
+const DScene& scene_dscene(const liar_gpu_scene* s) { return s->d; }
+const liar_gpu_mesh* scene_mesh(const liar_gpu_scene* s) { return s->mesh; }
+int scene_device(const liar_gpu_scene* s) { return s->device; }
+}  // namespace rt
+}  // namespace liar_gpu
 
 extern "C" void liar_gpu_scene_destroy(liar_gpu_scene* s) {
     if (!s) return;

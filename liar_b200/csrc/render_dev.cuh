@@ -114,7 +114,7 @@ __device__ __forceinline__ int lower_bound_f(const float* a, int n, float x) {
 
 // value of spectrum idx at wavelength w (m); reflectant spectra are clamped / rescaled to <= 1
 // like Spectral(..., SpectralType::Reflectant) (src/liar/kernel/spectral.cpp:47-70, 185-210)
-__device__ float spec_eval(const DScene& S, int idx, float w, bool reflectant) {
+__device__ inline float spec_eval(const DScene& S, int idx, float w, bool reflectant) {
     if (idx < 0) return 0.0f;
     const liar_spectrum sp = S.specs[idx];
     float v;
@@ -150,7 +150,7 @@ __device__ float spec_eval(const DScene& S, int idx, float w, bool reflectant) {
 }
 
 // ---- observer
-__device__ float observer_sample(const DScene& S, float u, float& pdf) {
+__device__ inline float observer_sample(const DScene& S, float u, float& pdf) {
     const int n = S.n_obs;
     const int i = upper_bound_f(S.obs_cdf, n, u);
     if (i == 0 || i == n) {
@@ -165,7 +165,7 @@ __device__ float observer_sample(const DScene& S, float u, float& pdf) {
     return lerpf(w1, w2, x);
 }
 
-__device__ float3 observer_sensitivity(const DScene& S, float w) {
+__device__ inline float3 observer_sensitivity(const DScene& S, float w) {
     const int i = upper_bound_f(S.obs_w, S.n_obs, w);
     if (i == 0 || i == S.n_obs) return mk(0, 0, 0);
     const int k = i - 1;
@@ -238,14 +238,14 @@ struct BsdfSample {
 __device__ __forceinline__ float power_heuristic(float a, float b) { return sqr(a) / (sqr(a) + sqr(b)); }
 
 // microfacet distributions
-__device__ float mdf_sample_phi(float s, float au, float av) {
+__device__ inline float mdf_sample_phi(float s, float au, float av) {
     if (au == av) return 2 * kPi * s;
     const float phi = atanf(av / au * tanf(2 * kPi * s));
     if (s <= 0.25f) return phi;
     if (s < 0.75f) return phi + kPi;
     return phi + 2 * kPi;
 }
-__device__ float mdf_D(int mdf, float3 h, float au, float av, float& pdfH) {
+__device__ inline float mdf_D(int mdf, float3 h, float au, float av, float& pdfH) {
     if (mdf == LIAR_MDF_GGX) {
         const float d = 1.0f / (kPi * au * av * sqr(sqr(h.x / au) + sqr(h.y / av) + sqr(h.z)));
         pdfH = d * h.z;
@@ -260,7 +260,7 @@ __device__ float mdf_D(int mdf, float3 h, float au, float av, float& pdfH) {
     pdfH = d * h.z;
     return d;
 }
-__device__ float3 mdf_sample_h(int mdf, float sx, float sy, float au, float av) {
+__device__ inline float3 mdf_sample_h(int mdf, float sx, float sy, float au, float av) {
     if (mdf == LIAR_MDF_GGX) {
         const float phi = mdf_sample_phi(sx, au, av);
         const float s = sqrtf(sy / (1.0f - sy));
@@ -284,7 +284,7 @@ __device__ float3 mdf_sample_h(int mdf, float sx, float sy, float au, float av) 
     const float st = sqrtf(fmaxf(1.0f - c2, 0.0f));
     return mk(cp * st, sp * st, ct);
 }
-__device__ float mdf_lambda(int mdf, float3 w, float au, float av) {
+__device__ inline float mdf_lambda(int mdf, float3 w, float au, float av) {
     if (mdf == LIAR_MDF_GGX) {
         const float inv_a2 = (sqr(w.x * au) + sqr(w.y * av)) / sqr(w.z);
         return (sqrtf(1.0f + inv_a2) - 1.0f) / 2.0f;
@@ -294,19 +294,19 @@ __device__ float mdf_lambda(int mdf, float3 w, float au, float av) {
     const float a = sqrtf(a2);
     return a < 1.6f ? (3.535f * a + 2.181f * a2) / (1.0f + 2.276f * a + 2.577f * a2) : 1.0f;
 }
-__device__ float mdf_G1(int mdf, float3 w, float3 h, float au, float av) {
+__device__ inline float mdf_G1(int mdf, float3 w, float3 h, float au, float av) {
     if (dot(w, h) * w.z <= 0.0f) return 0.0f;
     return 1.0f / (1.0f + mdf_lambda(mdf, w, au, av));
 }
 
-__device__ float fresnel_conductor(float eta, float kappa, float cosI) {
+__device__ inline float fresnel_conductor(float eta, float kappa, float cosI) {
     const float c2 = sqr(cosI);
     const float a = sqr(eta) + sqr(kappa);
     const float b = (2 * cosI) * eta;
     const float aO = a + c2, aP = a * c2 + 1;
     return ((aO - b) / (aO + b) + (aP - b) / (aP + b)) / 2;
 }
-__device__ float fresnel_dielectric_walter(float ior, float3 wi, float3 h) {
+__device__ inline float fresnel_dielectric_walter(float ior, float3 wi, float3 h) {
     const float cosI = fabsf(dot(wi, h));
     const float sinT2 = sqr(ior) * (1 - sqr(cosI));
     const float cosT = sqrtf(fmaxf(1 - sinT2, 0.0f));
@@ -314,7 +314,7 @@ __device__ float fresnel_dielectric_walter(float ior, float3 wi, float3 h) {
     const float rP = (cosI - ior * cosT) / (cosI + ior * cosT);
     return fminf((sqr(rO) + sqr(rP)) / 2, 1.0f);
 }
-__device__ float walter_pdf_reflection(const Bsdf& b, float rF, uint32_t allowed) {
+__device__ inline float walter_pdf_reflection(const Bsdf& b, float rF, uint32_t allowed) {
     const float pr = has_caps(allowed, CAP_REFL | CAP_GLOSSY) ? fabsf(b.r) * rF : 0.0f;
     const float pt = has_caps(allowed, CAP_TRANS | CAP_GLOSSY) ? fabsf(b.t) * (1 - rF) : 0.0f;
     const float tot = pr + pt;
@@ -322,7 +322,7 @@ __device__ float walter_pdf_reflection(const Bsdf& b, float rF, uint32_t allowed
     return pr / tot;
 }
 
-__device__ BsdfOut bsdf_do_evaluate(const Bsdf& b, float3 wi, float3 wo, uint32_t allowed) {
+__device__ inline BsdfOut bsdf_do_evaluate(const Bsdf& b, float3 wi, float3 wo, uint32_t allowed) {
     BsdfOut out{0.0f, 0.0f};
     switch (b.type) {
         case LIAR_MAT_LAMBERT: {
@@ -374,7 +374,7 @@ __device__ BsdfOut bsdf_do_evaluate(const Bsdf& b, float3 wi, float3 wo, uint32_
 }
 
 // Bsdf::evaluate: reject wo in the plane, drop the caps that the geometric normal rules out
-__device__ BsdfOut bsdf_evaluate(const Bsdf& b, float3 wi, float3 wo, uint32_t allowed) {
+__device__ inline BsdfOut bsdf_evaluate(const Bsdf& b, float3 wi, float3 wo, uint32_t allowed) {
     if (wo.z == 0.0f) return BsdfOut{0.0f, 0.0f};
     const bool reflective = (dot(wi, b.ng) > 0.0f) == (dot(wo, b.ng) > 0.0f);
     allowed &= ~(reflective ? CAP_TRANS : CAP_REFL);
@@ -382,7 +382,7 @@ __device__ BsdfOut bsdf_evaluate(const Bsdf& b, float3 wi, float3 wo, uint32_t a
     return bsdf_do_evaluate(b, wi, wo, allowed);
 }
 
-__device__ BsdfSample bsdf_sample(const Bsdf& b, float3 wi, float sx, float sy, float comp, uint32_t allowed) {
+__device__ inline BsdfSample bsdf_sample(const Bsdf& b, float3 wi, float sx, float sy, float comp, uint32_t allowed) {
     BsdfSample out{mk(0, 0, 0), 0.0f, 0.0f};
     if (!compatible_caps(b.caps, allowed)) return out;
     switch (b.type) {
@@ -483,7 +483,7 @@ struct LightEmission {
 };
 
 // Parallelogram ray test (two-sided) for the light's surface; t in units of |d|, t > tmin
-__device__ bool parallelogram_hit(const liar_light& L, float3 o, float3 d, float tmin, float& t) {
+__device__ inline bool parallelogram_hit(const liar_light& L, float3 o, float3 d, float tmin, float& t) {
     const float3 p = mk(L.pos[0], L.pos[1], L.pos[2]), u = mk(L.u[0], L.u[1], L.u[2]), v = mk(L.v[0], L.v[1], L.v[2]);
     const float3 n = cross(u, v);
     const float den = dot(n, d);
@@ -504,7 +504,7 @@ __device__ bool parallelogram_hit(const liar_light& L, float3 o, float3 d, float
 // SceneLight::emission for a ray leaving `o` along unit `d` (LightArea::doEmission ->
 // SceneObject::doAngularPdf: t^2 / |A cos|; the single-sided test sees a normal already flipped
 // toward the ray's origin, so hits are accepted from both sides)
-__device__ LightEmission light_emission(const DScene& S, int li, float3 o, float3 d, float lambda) {
+__device__ inline LightEmission light_emission(const DScene& S, int li, float3 o, float3 d, float lambda) {
     LightEmission e{0.0f, 0.0f, INFINITY};
     const liar_light L = S.lights[li];
     if (L.type == LIAR_LIGHT_AREA_PARALLELOGRAM) {
@@ -559,7 +559,7 @@ struct LightSample {
 };
 
 // SceneLight::sampleEmission(sample, lightSample, target, shadowRay, pdf)
-__device__ LightSample light_sample(const DScene& S, int li, float3 target, float sx, float sy, float lambda) {
+__device__ inline LightSample light_sample(const DScene& S, int li, float3 target, float sx, float sy, float lambda) {
     LightSample out{mk(0, 0, 1), 0.0f, 0.0f, 0.0f};
     const liar_light L = S.lights[li];
     if (L.type == LIAR_LIGHT_AREA_PARALLELOGRAM || L.type == LIAR_LIGHT_AREA_MESH) {
@@ -631,6 +631,122 @@ __device__ LightSample light_sample(const DScene& S, int li, float3 target, floa
 
 __device__ __forceinline__ float light_choice_pdf(const DScene& S, int k) {
     return k > 0 ? S.light_cdf[k] - S.light_cdf[k - 1] : S.light_cdf[0];
+}
+
+// ---- the local context of a hit (IntersectionContext, kernel/intersection_context.cpp:55-290)
+struct HitContext {
+    float3 target;  // hit point on the triangle
+    float3 ng;      // geometric normal, flipped toward -d
+    float3 N;       // shading normal, flipped toward -d
+    float3 u, v;    // shading frame tangents
+    bool leaving;   // solid event from the unflipped geometric normal
+    int obj, light, mat;
+};
+
+__device__ inline HitContext hit_context(const DScene& S, float3 o, float3 d, uint32_t prim) {
+    HitContext H;
+    H.obj = S.tri_obj[prim];
+    H.light = S.obj_light[H.obj];
+    H.mat = S.obj_mat[H.obj];
+    // re-intersect the hit triangle for the barycentrics (TriangleMesh::doLocalContext)
+    const uint32_t i0 = S.tri_idx[3 * prim], i1 = S.tri_idx[3 * prim + 1], i2 = S.tri_idx[3 * prim + 2];
+    const float3 a = mk(S.verts[3 * i0], S.verts[3 * i0 + 1], S.verts[3 * i0 + 2]);
+    const float3 b = mk(S.verts[3 * i1], S.verts[3 * i1 + 1], S.verts[3 * i1 + 2]);
+    const float3 c = mk(S.verts[3 * i2], S.verts[3 * i2 + 1], S.verts[3 * i2 + 2]);
+    const float3 e1 = b - a, e2 = c - a;
+    float tt, bu, bv;
+    if (!tri_intersect_exact(o.x, o.y, o.z, d.x, d.y, d.z, a.x, a.y, a.z, e1.x, e1.y, e1.z, e2.x, e2.y, e2.z, tt, bu, bv))
+        bu = bv = 0.0f;
+    H.target = a + bu * e1 + bv * e2;
+    const float3 ng0 = normal(cross(e1, e2));
+    float3 ns = ng0;
+    if (S.tri_nrm) {
+        const int n0 = S.tri_nrm[3 * prim], n1 = S.tri_nrm[3 * prim + 1], n2 = S.tri_nrm[3 * prim + 2];
+        if (n0 >= 0 && n1 >= 0 && n2 >= 0) {
+            const float w0 = 1.0f - bu - bv;
+            ns = normal(w0 * mk(S.normals[3 * n0], S.normals[3 * n0 + 1], S.normals[3 * n0 + 2]) +
+                        bu * mk(S.normals[3 * n1], S.normals[3 * n1 + 1], S.normals[3 * n1 + 2]) +
+                        bv * mk(S.normals[3 * n2], S.normals[3 * n2 + 1], S.normals[3 * n2 + 2]));
+        }
+    }
+    H.leaving = dot(d, ng0) > 0.0f;  // triangle_mesh.cpp:303-308
+    H.ng = dot(ng0, -d) < 0.0f ? -ng0 : ng0;  // flipTo(-direction)
+    H.N = dot(ns, -d) < 0.0f ? -ns : ns;
+    // shading frame (IntersectionContext::bsdfToLocal)
+    float3 u = e1 - dot(e1, H.N) * H.N;
+    float3 v = e2 - dot(e2, H.N) * H.N;
+    const float su = dot(u, u), sv = dot(v, v);
+    if (fmaxf(su, sv) < 1e-3f * fmaxf(dot(e1, e1), dot(e2, e2))) {
+        const float3 ax = fabsf(H.N.x) < 0.9f ? mk(1, 0, 0) : mk(0, 1, 0);
+        u = cross(ax, H.N);
+        v = cross(H.N, u);
+    }
+    if (su >= sv) {
+        u = normal(u);
+        v = cross(H.N, u);
+    } else {
+        v = normal(v);
+        u = cross(v, H.N);
+    }
+    H.u = u;
+    H.v = v;
+    return H;
+}
+
+// Shader::bsdf at one wavelength
+__device__ inline Bsdf make_bsdf(const DScene& S, const liar_material& M, const HitContext& H, float lam) {
+    Bsdf B;
+    B.type = (uint32_t)M.type;
+    B.mdf = M.mdf;
+    B.ng = mk(dot(H.ng, H.u), dot(H.ng, H.v), dot(H.ng, H.N));
+    B.r = B.t = 0.0f;
+    B.eta = B.kappa = B.ior = B.eta_i = B.eta_t = 1.0f;
+    B.au = sqr(fmaxf(M.rough_u, 1e-3f));
+    B.av = sqr(fmaxf(M.rough_v, 1e-3f));
+    switch (M.type) {
+        case LIAR_MAT_LAMBERT:
+            B.caps = CAP_REFL | CAP_DIFF;
+            B.r = spec_eval(S, M.spec[0], lam, true);
+            break;
+        case LIAR_MAT_CONDUCTOR:
+        case LIAR_MAT_COOK_TORRANCE:
+            B.caps = M.type == LIAR_MAT_CONDUCTOR ? (CAP_REFL | CAP_SPEC) : (CAP_REFL | CAP_GLOSSY);
+            B.eta = fmaxf(spec_eval(S, M.spec[0], lam, false), 1e-9f);
+            B.kappa = fmaxf(spec_eval(S, M.spec[1], lam, false), 1e-9f);
+            B.r = spec_eval(S, M.spec[2], lam, true);
+            break;
+        case LIAR_MAT_DIELECTRIC: {
+            B.caps = CAP_REFL | CAP_TRANS | CAP_SPEC;
+            const float ior1 = fmaxf(spec_eval(S, M.spec[1], lam, false), 1e-9f);
+            const float ior2 = fmaxf(spec_eval(S, M.spec[0], lam, false), 1e-9f);
+            B.ior = H.leaving ? ior2 / ior1 : ior1 / ior2;
+            B.r = spec_eval(S, M.spec[2], lam, true);
+            B.t = spec_eval(S, M.spec[3], lam, true);
+            break;
+        }
+        case LIAR_MAT_WALTER: {
+            B.caps = CAP_TRANS | CAP_GLOSSY;  // as constructed by Walter::Bsdf (walter.cpp:247)
+            float ei = fmaxf(spec_eval(S, M.spec[1], lam, false), 1e-9f);
+            float et = fmaxf(spec_eval(S, M.spec[0], lam, false), 1e-9f);
+            if (H.leaving) {
+                const float tmp = ei;
+                ei = et;
+                et = tmp;
+            }
+            B.eta_i = ei;
+            B.eta_t = et;
+            B.r = spec_eval(S, M.spec[2], lam, true);
+            B.t = spec_eval(S, M.spec[3], lam, true);
+            break;
+        }
+        case LIAR_MAT_MIRROR:
+            B.caps = CAP_REFL | CAP_SPEC;
+            B.r = spec_eval(S, M.spec[0], lam, true);
+            break;
+        default:
+            B.caps = 0;
+    }
+    return B;
 }
 
 }  // namespace rt

@@ -66,3 +66,70 @@ class PhotonMap:
             self.close()
         except Exception:
             pass
+
+
+# ---- photon tracing (liar_gpu_photon_trace)
+
+class PhotonDesc(C.Structure):
+    _fields_ = [("max_ray_generation", C.c_int32), ("ray_traced_direct", C.c_int32), ("seed", C.c_uint64),
+                ("global_target", C.c_uint64), ("max_emitted", C.c_uint64), ("wave", C.c_uint64)]
+
+
+class PhotonBuffers(C.Structure):
+    _fields_ = [("position", C.c_void_p), ("omega_in", C.c_void_p), ("power", C.c_void_p), ("path", C.c_void_p),
+                ("tag", C.c_void_p), ("capacity", C.c_uint64)]
+
+
+class PhotonCounts(C.Structure):
+    _fields_ = [("stored", C.c_uint64), ("global_", C.c_uint64), ("caustic", C.c_uint64), ("emitted", C.c_uint64)]
+
+
+GLOBAL, CAUSTIC = 1, 2
+
+
+def photon_desc(global_target: int, max_emitted: int = 100_000_000, max_ray_generation: int = 8, seed: int = 0,
+                wave: int = 0, ray_traced_direct: bool = True) -> PhotonDesc:
+    d = PhotonDesc()
+    d.max_ray_generation = int(max_ray_generation)
+    d.ray_traced_direct = int(bool(ray_traced_direct))
+    d.seed = int(seed)
+    d.global_target = int(global_target)
+    d.max_emitted = int(max_emitted)
+    d.wave = int(wave)
+    return d
+
+
+def trace_photons(gpu_scene, desc: PhotonDesc, capacity: int, stream: int | None = None):
+    """Runs PhotonMapper::fillPhotonMaps on the GPU. Returns (dict of torch device tensors, counts)."""
+    import torch
+    ctx = gpu_scene.ctx
+    lib = ctx._lib
+    fn = lib.liar_gpu_photon_trace
+    fn.restype = C.c_int
+    fn.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(PhotonDesc), C.POINTER(PhotonBuffers), C.POINTER(PhotonCounts),
+                   C.c_void_p]
+    dev = f"cuda:{ctx.device}"
+    buf = {
+        "position": torch.empty((capacity, 3), dtype=torch.float32, device=dev),
+        "omega_in": torch.empty((capacity, 3), dtype=torch.float32, device=dev),
+        "power": torch.empty((capacity, 3), dtype=torch.float32, device=dev),
+        "path": torch.empty(capacity, dtype=torch.int32, device=dev),
+        "tag": torch.empty(capacity, dtype=torch.int32, device=dev),
+    }
+    b = PhotonBuffers(*(buf[k].data_ptr() for k in ("position", "omega_in", "power", "path", "tag")), int(capacity))
+    counts = PhotonCounts()
+    torch.cuda.synchronize()
+    ctx.check(fn(ctx.handle, gpu_scene.handle, C.byref(desc), C.byref(b), C.byref(counts), C.c_void_p(stream or 0)))
+    n = int(counts.stored)
+    out = {k: v[:n] for k, v in buf.items()}
+    return out, {"stored": n, "global": int(counts.global_), "caustic": int(counts.caustic),
+                 "emitted": int(counts.emitted)}
+
+
+def automatic_radius(power_xyz: np.ndarray, emitted: int, estimation_size: int = 50, tolerance: float = 0.05) -> float:
+    """PhotonMapper::buildPhotonMap's automatic estimation radius (photon_mapper.cpp:815-833): the
+    median photon power (|X|+|Y|+|Z| after scaling by 1 / photons emitted) sets the area."""
+    p = np.abs(np.asarray(power_xyz, dtype=np.float64)).sum(axis=1) / max(emitted, 1)
+    median = float(p[len(p) // 2]) if len(p) else 0.0
+    area = estimation_size * median / tolerance
+    return float(np.sqrt(area) / np.pi)

@@ -92,3 +92,27 @@ def white_furnace():
     cam.aspectRatio = 1
     cam.fovAngle = math.radians(30)
     return scene, cam
+
+
+def photon_scene(light_scale: float = 50.0):
+    """The photon-mapping workload: a glass sphere (Dielectric, Cauchy A = 1.5, B = 0.0042 um^2)
+    and a tilted GGX copper panel (CookTorrance with copper n, k) under a 5000 K point light. The
+    reference stores photons only on surfaces with a diffuse BSDF (photon_mapper.cpp:733), so the
+    two objects stand on a Lambert ground plane that receives the caustics."""
+    from . import scenery as sc
+    ground = sc.Parallelogram((-3, 0, -3), (6, 0, 0), (0, 0, 6))
+    ground.shader = shaders.Lambert(textures.Constant(0.7))
+    ball = sc.Sphere((-0.4, 0.5, 0.2), 0.5, subdivisions=5)
+    ball.shader = shaders.Dielectric(textures.Constant(spectra.Cauchy(1.5, 0.0042)))
+    panel = sc.Parallelogram((0.6, 0.0, -0.8), (0.5, 0.0, 0.9), (0.3, 1.2, 0.0))
+    cu = shaders.CookTorrance(textures.Constant(spectra.spd("Cu", "n")), textures.Constant(spectra.spd("Cu", "k")))
+    cu.mdf = shaders.MicrofacetTrowbridgeReitz()
+    cu.roughness = textures.Constant(0.15)
+    panel.shader = cu
+    light = sc.LightPoint((-0.2, 2.6, -0.6), spectra.BlackBody(5000.0, light_scale))
+    scene = sc.List([ground, ball, panel, light])
+    cam = cameras.PerspectiveCamera()
+    cam.position = (0.0, 2.2, -3.6)
+    cam.lookAt((0.0, 0.3, 0.0))
+    cam.aspectRatio = 16 / 9
+    return scene, cam

@@ -154,3 +154,19 @@ def knn(photons, queries, k, r_max, threads=0):
     L.oracle_knn(P.ctypes.data, P.shape[0], Q.ctypes.data, Q.shape[0], int(k), float(r_max), idx.ctypes.data,
                  d2.ctypes.data, cnt.ctypes.data, int(threads))
     return idx, d2, cnt
+
+
+def photon_trace(render_scene, desc, capacity, threads=0):
+    """The photon-tracing restatement over a RenderScene; photons sorted by (path, bounce).
+    Returns (records (n,) structured array, counts dict)."""
+    L = lib()
+    L.oracle_photon_trace.restype = C.c_int
+    L.oracle_photon_trace.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_int]
+    rec = np.zeros(capacity, dtype=[("pos", "<f4", 3), ("omega", "<f4", 3), ("power", "<f4", 3), ("path", "<u4"),
+                                    ("tag", "<u4")])
+    counts = np.zeros(4, np.uint64)
+    rc = L.oracle_photon_trace(render_scene.h, C.addressof(desc), rec.ctypes.data, capacity, counts.ctypes.data,
+                               int(threads))
+    n = int(min(counts[0], capacity))
+    return rec[:n], {"stored": int(counts[0]), "global": int(counts[1]), "caustic": int(counts[2]),
+                     "emitted": int(counts[3]), "rc": rc}

@@ -847,6 +847,235 @@ void oracle_scene_free(void* s) {
 
 uint64_t oracle_mix64(uint64_t z) { return mix64(z); }
 
+// ---- photon tracing: PhotonMapper::emitPhoton / tracePhoton (tracers/photon_mapper.cpp:628-796)
+struct PhotonIn {
+    int32_t max_ray_generation, ray_traced_direct;
+    uint64_t seed, global_target, max_emitted, wave;
+};
+struct PhotonRec {
+    float pos[3], omega[3], power[3];
+    uint32_t path, tag;
+};
+
+static void trace_photon_rec(const Scene& S, const PhotonIn& D, const Sampler& smp, uint32_t path, float lam,
+                             float lam_pdf, float power, V o, V d, float tmin, float tmax, int gen, bool caustic,
+                             std::vector<PhotonRec>& out) {
+    if (power == 0) return;
+    const Hit h = oracle_internal::tree_closest(S.tree, Ray{o.x, o.y, o.z, tmin, d.x, d.y, d.z, tmax});
+    if (h.prim < 0) return;
+    const V hit = o + h.t * d;
+    const uint32_t prim = (uint32_t)h.prim;
+    const int obj = S.in.triangle_object[prim];
+    const int mi = S.in.object_material[obj];
+    if (mi < 0 || S.in.materials[mi].type == M_NONE) {
+        if (gen >= D.max_ray_generation) return;
+        return trace_photon_rec(S, D, smp, path, lam, lam_pdf, power, o, d, h.t + TOL, tmax, gen + 1, caustic, out);
+    }
+    const Material& M = S.in.materials[mi];
+    if (M.type == M_LAMBERT) {
+        const bool to_caustic = caustic;
+        const bool to_global = (gen > 0 || !D.ray_traced_direct) && !caustic;
+        if (to_caustic || to_global) {
+            PhotonRec r;
+            r.pos[0] = hit.x;
+            r.pos[1] = hit.y;
+            r.pos[2] = hit.z;
+            r.omega[0] = -d.x;
+            r.omega[1] = -d.y;
+            r.omega[2] = -d.z;
+            const float sc = power / lam_pdf;  // Photon::Photon stores power.xyz(sample)
+            const V c = observer_sensitivity(S, lam);
+            r.power[0] = sc * c.x;
+            r.power[1] = sc * c.y;
+            r.power[2] = sc * c.z;
+            r.path = path;
+            r.tag = (to_caustic ? 2u : 1u) | ((uint32_t)gen << 8);
+            out.push_back(r);
+        }
+    }
+    if (gen >= D.max_ray_generation) return;
+    // the same local context as the path tracer
+    const uint32_t* tr = S.in.triangles + 3 * (size_t)prim;
+    const float* pa = S.in.vertices + 3 * tr[0];
+    const float* pb = S.in.vertices + 3 * tr[1];
+    const float* pc = S.in.vertices + 3 * tr[2];
+    const V A{pa[0], pa[1], pa[2]};
+    const V e1 = V{pb[0], pb[1], pb[2]} - A, e2 = V{pc[0], pc[1], pc[2]} - A;
+    const V ng0 = unit(cross(e1, e2));
+    V ns = ng0;
+    if (S.in.triangle_normals && S.in.normals) {
+        float tt, bu = 0, bv = 0;
+        const float oo[3] = {o.x, o.y, o.z}, dd[3] = {d.x, d.y, d.z};
+        if (!oracle_tri_intersect(oo, dd, pa, pb, pc, &tt, &bu, &bv)) bu = bv = 0;
+        const int32_t* tn = S.in.triangle_normals + 3 * (size_t)prim;
+        if (tn[0] >= 0 && tn[1] >= 0 && tn[2] >= 0) {
+            const float* n0 = S.in.normals + 3 * tn[0];
+            const float* n1 = S.in.normals + 3 * tn[1];
+            const float* n2 = S.in.normals + 3 * tn[2];
+            const float w0 = 1 - bu - bv;
+            ns = unit(w0 * V{n0[0], n0[1], n0[2]} + bu * V{n1[0], n1[1], n1[2]} + bv * V{n2[0], n2[1], n2[2]});
+        }
+    }
+    const bool leaving = dot(d, ng0) > 0;
+    const V ng = dot(ng0, -d) < 0 ? -ng0 : ng0;
+    const V N = dot(ns, -d) < 0 ? -ns : ns;
+    V u = e1 - dot(e1, N) * N, v = e2 - dot(e2, N) * N;
+    const float su = dot(u, u), sv = dot(v, v);
+    if (std::max(su, sv) < 1e-3f * std::max(dot(e1, e1), dot(e2, e2))) {
+        const V ax = std::fabs(N.x) < 0.9f ? V{1, 0, 0} : V{0, 1, 0};
+        u = cross(ax, N);
+        v = cross(N, u);
+    }
+    if (su >= sv) {
+        u = unit(u);
+        v = cross(N, u);
+    } else {
+        v = unit(v);
+        u = cross(v, N);
+    }
+    Bsdf B{};
+    B.type = M.type;
+    B.mdf = M.mdf;
+    B.ng = {dot(ng, u), dot(ng, v), dot(ng, N)};
+    B.eta = B.kappa = B.ior = B.etaI = B.etaT = 1;
+    B.au = sq(std::max(M.rough_u, 1e-3f));
+    B.av = sq(std::max(M.rough_v, 1e-3f));
+    switch (M.type) {
+        case M_LAMBERT:
+            B.caps = C_REFL | C_DIFF;
+            B.r = spectrum(S, M.spec[0], lam, true);
+            break;
+        case M_CONDUCTOR:
+        case M_CT:
+            B.caps = M.type == M_CONDUCTOR ? (C_REFL | C_SPEC) : (C_REFL | C_GLOSSY);
+            B.eta = std::max(spectrum(S, M.spec[0], lam, false), 1e-9f);
+            B.kappa = std::max(spectrum(S, M.spec[1], lam, false), 1e-9f);
+            B.r = spectrum(S, M.spec[2], lam, true);
+            break;
+        case M_DIELECTRIC: {
+            B.caps = C_REFL | C_TRANS | C_SPEC;
+            const float i1 = std::max(spectrum(S, M.spec[1], lam, false), 1e-9f);
+            const float i2 = std::max(spectrum(S, M.spec[0], lam, false), 1e-9f);
+            B.ior = leaving ? i2 / i1 : i1 / i2;
+            B.r = spectrum(S, M.spec[2], lam, true);
+            B.t = spectrum(S, M.spec[3], lam, true);
+            break;
+        }
+        case M_WALTER: {
+            B.caps = C_TRANS | C_GLOSSY;
+            float ei = std::max(spectrum(S, M.spec[1], lam, false), 1e-9f);
+            float et = std::max(spectrum(S, M.spec[0], lam, false), 1e-9f);
+            if (leaving) std::swap(ei, et);
+            B.etaI = ei;
+            B.etaT = et;
+            B.r = spectrum(S, M.spec[2], lam, true);
+            B.t = spectrum(S, M.spec[3], lam, true);
+            break;
+        }
+        case M_MIRROR:
+            B.caps = C_REFL | C_SPEC;
+            B.r = spectrum(S, M.spec[0], lam, true);
+            break;
+    }
+    const V md = -d;
+    V wi{dot(md, u), dot(md, v), dot(md, N)};
+    wi.z = std::max(wi.z, 1.19209290e-07f);
+    const uint32_t base = 8 + 8 * (uint32_t)gen;
+    const Out so = sample(B, wi, smp.get(base + 0, false), smp.get(base + 1, false), smp.get(base + 2, false), C_ALL);
+    if (!so) return;
+    const float ct = so.wo.z;
+    float np = power * so.value * (std::fabs(ct) / so.pdf);
+    const float prob = std::min(1.0f, np / power);
+    const float ur = smp.get(base + 3, false);
+    if (prob <= 0 || ur > prob) return;  // russianRoulette (kernel/kernel_common.h:160-168)
+    np /= std::min(prob, 1.0f);
+    const V nd = so.wo.x * u + so.wo.y * v + so.wo.z * N;
+    const V start = hit + ((ct > 0 ? 10.0f : -10.0f) * TOL) * ng;
+    const bool specular = M.type != M_LAMBERT;
+    trace_photon_rec(S, D, smp, path, lam, lam_pdf, np, start, nd, TOL, INFINITY, gen + 1,
+                     specular && (caustic || gen == 0), out);
+}
+
+static void emit_photon(const Scene& S, const PhotonIn& D, uint64_t seed, uint64_t path, std::vector<PhotonRec>& out) {
+    const Sampler smp{seed, (uint32_t)path, (uint32_t)(path >> 32), 1};
+    float lpdf;
+    const float lam = observer_sample(S, smp.get(5, false), lpdf);
+    const float ul = smp.get(0, false);
+    int k = (int)(std::lower_bound(S.light_cdf.begin(), S.light_cdf.end(), ul) - S.light_cdf.begin());
+    k = std::min(k, (int)S.in.n_lights - 1);
+    const float pc = light_pdf_choice(S, k);
+    const Light& L = S.in.lights[k];
+    const float ax = smp.get(1, false), ay = smp.get(2, false), bx = smp.get(3, false), by = smp.get(4, false);
+    V origin{0, 0, 0}, dir{0, 0, 1};
+    float pdf = 0, value = 0;
+    if (L.type == L_POINT) {
+        dir = uniform_sphere(ax, ay, pdf);
+        origin = {L.pos[0], L.pos[1], L.pos[2]};
+        value = spectrum(S, L.spectrum, lam, false);
+    } else if (L.type == L_PARA) {
+        const V u{L.u[0], L.u[1], L.u[2]}, v{L.v[0], L.v[1], L.v[2]};
+        origin = V{L.pos[0], L.pos[1], L.pos[2]} + ax * u + ay * v;
+        V n = unit(cross(u, v));
+        if (L.double_sided && 2 * bx >= 1) n = -n;
+        const V a = std::fabs(n.x) > std::fabs(n.y) ? V{-n.z, 0, n.x} : V{0, n.z, -n.y};
+        const V tu = unit(a), tv = cross(n, tu);
+        float dpdf;
+        const V ld = cosine_hemisphere(bx, by, dpdf);
+        dir = ld.x * tu + ld.y * tv + ld.z * n;
+        pdf = (1 / S.light_area[k]) * dpdf;
+        value = spectrum(S, L.spectrum, lam, false) * ld.z;
+    }
+    if (!(pdf > 0 && value != 0 && pc > 0 && lpdf > 0)) return;
+    trace_photon_rec(S, D, smp, (uint32_t)path, lam, lpdf, value / (pc * pdf), origin, dir, TOL, INFINITY, 0, false,
+                     out);
+}
+
+// photons of the whole emission, sorted by (path, bounce); counts = stored, global, caustic, emitted
+int oracle_photon_trace(void* s, const PhotonIn* D, PhotonRec* out, uint64_t capacity, uint64_t* counts, int threads) {
+    const Scene& S = *static_cast<Scene*>(s);
+    if (S.in.n_lights == 0) {
+        counts[0] = counts[1] = counts[2] = counts[3] = 0;
+        return 0;
+    }
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    const uint64_t seed = mix64(D->seed ^ 0x9a1d37c8e15b22f3ull);
+    const uint64_t wave = D->wave ? D->wave : (1ull << 21);
+    uint64_t emitted = 0, global = 0, caustic = 0, stored = 0;
+    while (emitted < D->max_emitted && global < D->global_target) {
+        const uint64_t n = std::min(wave, D->max_emitted - emitted);
+        std::vector<std::vector<PhotonRec>> parts(threads);
+        std::atomic<uint64_t> next{0};
+        auto work = [&](int t) {
+            while (true) {
+                const uint64_t b = next.fetch_add(1024);
+                if (b >= n) break;
+                for (uint64_t i = b; i < std::min(n, b + 1024); ++i) emit_photon(S, *D, seed, emitted + i, parts[t]);
+            }
+        };
+        std::vector<std::thread> pool;
+        for (int t = 1; t < threads; ++t) pool.emplace_back(work, t);
+        work(0);
+        for (auto& t : pool) t.join();
+        std::vector<PhotonRec> all;
+        for (auto& p : parts) all.insert(all.end(), p.begin(), p.end());
+        std::sort(all.begin(), all.end(), [](const PhotonRec& a, const PhotonRec& b) {
+            return a.path < b.path || (a.path == b.path && (a.tag >> 8) < (b.tag >> 8));
+        });
+        for (const PhotonRec& r : all) {
+            if (stored < capacity) out[stored] = r;
+            ++stored;
+            if ((r.tag & 3u) == 1u) ++global;
+            else ++caustic;
+        }
+        emitted += n;
+    }
+    counts[0] = stored;
+    counts[1] = global;
+    counts[2] = caustic;
+    counts[3] = emitted;
+    return stored > capacity ? -4 : 0;
+}
+
 // spectrum idx of the scene at wavelength w (Spectral Single-mode look-up)
 float oracle_spectrum_eval(void* s, int idx, float w, int reflectant) {
     return spectrum(*static_cast<Scene*>(s), idx, w, reflectant != 0);
