@@ -92,6 +92,7 @@ SIGNATURES: dict[str, tuple] = {
     "liar_gpu_photon_map_destroy": (None, [_vp]),
     "liar_gpu_photon_gather": (C.c_int, [_vp, _vp, _vp, _sz, C.c_int, _vp, _vp, _vp]),
     "liar_gpu_photon_gather_device": (C.c_int, [_vp, _vp, _vp, _sz, C.c_int, _vp, _vp, _vp, _vp]),
+    "liar_gpu_photon_trace": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
 }
 
 
