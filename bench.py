@@ -170,6 +170,127 @@ def cornell_bench(ctx, stream, args, world, dist, local, cpu: bool) -> dict:
     return out
 
 
+def camera_queries(flat, cam, width, height):
+    """Gather points of the photon workload: the first hits of the camera's pixel-centre rays on
+    surfaces with a diffuse (Lambert) BSDF, with their normals flipped toward the camera."""
+    from liar_b200 import render as R
+    from liar_b200.trace import Mesh
+    from liar_b200.kernel import default_context
+    c = cam.flatten()
+    ys, xs = np.mgrid[0:height, 0:width]
+    sx, sy = (xs + 0.5) / width - 0.5, (ys + 0.5) / height - 0.5
+    d = (np.asarray(c["direction"])[None, None] + sx[..., None] * np.asarray(c["right"])
+         + sy[..., None] * np.asarray(c["down"])).reshape(-1, 3)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    o = np.broadcast_to(np.asarray(c["position"]), d.shape)
+    rays = np.concatenate([o, np.full((len(d), 1), 1e-6), d, np.full((len(d), 1), np.inf)], axis=1).astype(np.float32)
+    mesh = Mesh(default_context(), flat.vertices, flat.triangles)
+    prim, t = mesh.intersect(rays)
+    mesh.close()
+    hit = prim >= 0
+    mats = flat.object_material[flat.triangle_object[np.maximum(prim, 0)]]
+    lam = np.array([m.type == R.MAT_LAMBERT for m in flat.materials])[np.maximum(mats, 0)] & (mats >= 0)
+    ok = hit & lam
+    pts = (o[ok] + t[ok, None] * d[ok]).astype(np.float32)
+    tri = flat.vertices[flat.triangles[prim[ok]]].astype(np.float64)
+    n = np.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0])
+    n /= np.linalg.norm(n, axis=1, keepdims=True)
+    n = np.where((n * d[ok]).sum(axis=1, keepdims=True) > 0, -n, n).astype(np.float32)
+    return np.ascontiguousarray(pts), np.ascontiguousarray(n)
+
+
+def photon_bench(ctx, stream, args, world, dist, local, cpu: bool, n_photons: int = 10_000_000) -> dict:
+    """Photon mapping workload: 10M photons in the global map, 1920 x 1080 gather points, k = 64."""
+    import ctypes as C
+    import torch
+    from liar_b200 import photons, render as R, scenes_render
+    K = 64
+    scene, cam = scenes_render.photon_scene()
+    flat = R.flatten(scene)
+    gs = R.GpuScene(ctx, flat)
+    desc = photons.photon_desc(n_photons, max_emitted=(1 << 32) - 1, ray_traced_direct=False, wave=1 << 22)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ph, counts = photons.trace_photons(gs, desc, capacity=n_photons + (3 << 22), stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    trace_s = time.perf_counter() - t0
+    glob = (ph["tag"] & 3) == photons.GLOBAL
+    pos = ph["position"][glob][:n_photons].contiguous()
+    power = ph["power"][glob][:n_photons].contiguous()
+    omega = ph["omega_in"][glob][:n_photons].contiguous()
+    n_map = pos.shape[0]
+    r = photons.automatic_radius(power.cpu().numpy(), counts["emitted"], K)
+    q, qn = camera_queries(flat, cam, 1920, 1080)
+    nq = q.shape[0]
+    dq = torch.from_numpy(q).to(f"cuda:{local}")
+    dqn = torch.from_numpy(qn).to(f"cuda:{local}")
+    didx = torch.empty((nq, K), dtype=torch.int32, device=f"cuda:{local}")
+    dd2 = torch.empty((nq, K), dtype=torch.float32, device=f"cuda:{local}")
+    dcnt = torch.empty(nq, dtype=torch.int32, device=f"cuda:{local}")
+    dest = torch.empty((nq, 3), dtype=torch.float32, device=f"cuda:{local}")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    pmap = photons.PhotonMap(ctx, device_ptr=pos.data_ptr(), n=n_map, r_max=r, stream=stream.cuda_stream)
+    e1.record(stream)
+    stream.synchronize()
+    build_ms = e0.elapsed_time(e1)
+    lib = ctx._lib
+
+    def gather():
+        pmap.gather_device(dq.data_ptr(), nq, K, didx.data_ptr(), dd2.data_ptr(), dcnt.data_ptr(), stream.cuda_stream)
+
+    def estimate():
+        ctx.check(lib.liar_gpu_photon_estimate_device(
+            ctx.handle, C.c_void_p(power.data_ptr()), C.c_void_p(omega.data_ptr()), n_map, C.c_void_p(dqn.data_ptr()),
+            nq, K, C.c_void_p(didx.data_ptr()), C.c_void_p(dd2.data_ptr()), C.c_void_p(dcnt.data_ptr()),
+            C.c_float(1.0 / counts["emitted"]), C.c_void_p(dest.data_ptr()), C.c_void_p(stream.cuda_stream)))
+
+    for _ in range(max(3, args.warmup)):
+        gather()
+        estimate()
+    stream.synchronize()
+    steps = max(1, min(args.steps, 20))
+    e0.record(stream)
+    for _ in range(steps):
+        gather()
+    e1.record(stream)
+    stream.synchronize()
+    g_ms = e0.elapsed_time(e1) / steps
+    e0.record(stream)
+    for _ in range(steps):
+        estimate()
+    e1.record(stream)
+    stream.synchronize()
+    est_ms = e0.elapsed_time(e1) / steps
+    ctx.synchronize()
+    found = dcnt.float().mean().item()
+    # algorithmic bytes per query: 12 B point + k x 36 B photon records (the reference's Photon) +
+    # 27 x 8 B bucket ranges + k x 8 B results + 4 B count
+    bytes_q = 12 + K * 36 + 27 * 8 + K * 8 + 4
+    out = {"workload": "glass sphere + GGX copper panel + Lambert ground, 5000 K point light; "
+                       f"{n_map} global photons, 1920x1080 gather points ({nq} on diffuse surfaces), k = {K}",
+           "photons_emitted": counts["emitted"], "photon_trace_s": trace_s,
+           "photons_stored_per_s": counts["stored"] / trace_s, "estimation_radius": r, "map_build_ms": build_ms,
+           "gather_ms": g_ms, "queries_per_s": world * nq / (g_ms * 1e-3), "mean_neighbours": found,
+           "gather_gbs_algorithmic": bytes_q * nq / (g_ms * 1e-3) / 1e9, "estimate_ms": est_ms}
+    if cpu:
+        import oracle
+        ns = min(nq, 20000)
+        sel = np.random.default_rng(0).choice(nq, ns, replace=False)
+        P = pos.cpu().numpy()
+        t0 = time.perf_counter()
+        ci, cd, cc = oracle.knn_grid(P, q[sel], K, r)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": ns / dt, "unit": "queries/s", "cores": oracle.hardware_threads(),
+                               "kind": "port", "sample": f"{ns} of the {nq} gather points (grid k-NN), {dt:.1f} s "
+                                                        "including the grid build"}
+        out["parity_sample"] = {"queries": ns, "identical_neighbour_sets":
+                                bool((didx.cpu().numpy()[sel] == ci).all() and (dcnt.cpu().numpy()[sel] == cc).all())}
+    pmap.close()
+    gs.close()
+    return out
+
+
 def run_reference(args, world, rank):
     """CPU restatement of the reference's path (oracle/), all host threads, bounded samples."""
     if rank != 0:
@@ -339,8 +460,9 @@ def main():
                                 "sample": info["sample"]}
     mesh.close()
     if not args.no_workloads:
-        line["cornell"] = cornell_bench(ctx, stream, args, world, dist, local, cpu=(rank == 0 and world == 1
-                                                                                 and not args.no_cpu_baseline))
+        cpu_leg = rank == 0 and world == 1 and not args.no_cpu_baseline
+        line["cornell"] = cornell_bench(ctx, stream, args, world, dist, local, cpu=cpu_leg)
+        line["photon"] = photon_bench(ctx, stream, args, world, dist, local, cpu=cpu_leg)
     ctx.close()
     if rank == 0:
         print(json.dumps(line), flush=True)

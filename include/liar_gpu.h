@@ -246,6 +246,15 @@ int liar_gpu_photon_gather(liar_gpu_ctx* ctx, const liar_gpu_photon_map* map, co
 int liar_gpu_photon_gather_device(liar_gpu_ctx* ctx, const liar_gpu_photon_map* map, const float* d_queries,
                                   size_t n_queries, int k, int32_t* d_idx, float* d_d2, int32_t* d_count, void* stream);
 
+/* PhotonMapper::estimateIrradianceImpl (src/liar/tracers/photon_mapper.cpp:1254-1279) over gather
+ * results: per query the XYZ power of the neighbours with omega_in . normal > 0, times
+ * power_scale (1 / photons emitted), over pi r^2 with r^2 the farthest neighbour's d2.
+ * d_power / d_omega_in: n_photons x 3; d_normals, d_out: n_queries x 3. */
+int liar_gpu_photon_estimate_device(liar_gpu_ctx* ctx, const float* d_power, const float* d_omega_in, size_t n_photons,
+                                    const float* d_normals, size_t n_queries, int k, const int32_t* d_idx,
+                                    const float* d_d2, const int32_t* d_count, float power_scale, float* d_out,
+                                    void* stream);
+
 /* ---- photon tracing ------------------------------------------------------------------------------
  * PhotonMapper::fillPhotonMaps / emitPhoton / tracePhoton (src/liar/tracers/photon_mapper.cpp:573-796):
  * photons leave the scene's lights (chosen by power), carry power at one wavelength, scatter by

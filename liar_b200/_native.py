@@ -93,6 +93,8 @@ SIGNATURES: dict[str, tuple] = {
     "liar_gpu_photon_gather": (C.c_int, [_vp, _vp, _vp, _sz, C.c_int, _vp, _vp, _vp]),
     "liar_gpu_photon_gather_device": (C.c_int, [_vp, _vp, _vp, _sz, C.c_int, _vp, _vp, _vp, _vp]),
     "liar_gpu_photon_trace": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "liar_gpu_photon_estimate_device": (C.c_int, [_vp, _vp, _vp, _sz, _vp, _sz, C.c_int, _vp, _vp, _vp, C.c_float,
+                                                  _vp, _vp]),
 }
 
 

@@ -247,6 +247,41 @@ __global__ void __launch_bounds__(256) k_gather(const float4* __restrict__ sorte
     }
 }
 
+// PhotonMapper::estimateIrradianceImpl (photon_mapper.cpp:1254-1279): sum of the powers of the
+// neighbours arriving from the normal's side, over pi r^2 with r the farthest neighbour's distance
+__global__ void k_estimate(const float* __restrict__ power, const float* __restrict__ omega_in,
+                           const float* __restrict__ normals, uint32_t nq, int k, const int32_t* __restrict__ idx,
+                           const float* __restrict__ d2, const int32_t* __restrict__ count, float power_scale,
+                           uint32_t n_photons, float* __restrict__ out, uint32_t* __restrict__ status) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nq) return;
+    const int c = count[q];
+    float x = 0.0f, y = 0.0f, z = 0.0f;
+    if (c > 0) {
+        const float nx = normals[3 * q], ny = normals[3 * q + 1], nz = normals[3 * q + 2];
+        for (int j = 0; j < c && j < k; ++j) {
+            const int32_t i = idx[(size_t)q * k + j];
+            if (i < 0 || (uint32_t)i >= n_photons) {
+                atomicOr(status, 1u << 4);
+                continue;
+            }
+            if (omega_in[3 * i] * nx + omega_in[3 * i + 1] * ny + omega_in[3 * i + 2] * nz > 0.0f) {
+                x += power[3 * i];
+                y += power[3 * i + 1];
+                z += power[3 * i + 2];
+            }
+        }
+        const float r2 = d2[(size_t)q * k + (c < k ? c : k) - 1];
+        const float s = r2 > 0.0f ? power_scale / (3.14159265358979323846f * r2) : 0.0f;
+        x *= s;
+        y *= s;
+        z *= s;
+    }
+    out[3 * q] = x;
+    out[3 * q + 1] = y;
+    out[3 * q + 2] = z;
+}
+
 int map_build_impl(liar_gpu_ctx* ctx, liar_gpu_photon_map* m, const float* d_pos, size_t n, cudaStream_t st) {
     // bounding box on the host side of the caller's data is not available for device input: the
     // origin only has to be consistent between build and gather, so a fixed origin is used
@@ -425,4 +460,24 @@ extern "C" int liar_gpu_photon_gather(liar_gpu_ctx* ctx, const liar_gpu_photon_m
     }
     cudaFree(d);
     return rc;
+}
+
+extern "C" int liar_gpu_photon_estimate_device(liar_gpu_ctx* ctx, const float* d_power, const float* d_omega_in,
+                                               size_t n_photons, const float* d_normals, size_t n_queries, int k,
+                                               const int32_t* d_idx, const float* d_d2, const int32_t* d_count,
+                                               float power_scale, float* d_out, void* stream) {
+    if (!ctx) return LIAR_ERR_INVALID;
+    if (n_queries && (!d_power || !d_omega_in || !d_normals || !d_idx || !d_d2 || !d_count || !d_out))
+        return ctx_fail(ctx, LIAR_ERR_INVALID, "null buffer");
+    if (k < 1 || k > kGatherK) return ctx_fail(ctx, LIAR_ERR_INVALID, "k must be 1..%d", kGatherK);
+    if (n_queries >= (1ull << 31) || n_photons >= (1ull << 31)) return ctx_fail(ctx, LIAR_ERR_INVALID, "too many items");
+    if (n_queries == 0) return LIAR_OK;
+    int rc = ctx_activate(ctx);
+    if (rc) return rc;
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    k_estimate<<<(unsigned)((n_queries + 255) / 256), 256, 0, st>>>(d_power, d_omega_in, d_normals, (uint32_t)n_queries, k,
+                                                                   d_idx, d_d2, d_count, power_scale,
+                                                                   (uint32_t)n_photons, d_out,
+                                                                   ctx->d_scratch + kStatusWord);
+    return ctx_cuda(ctx, cudaGetLastError(), "photon estimate launch");
 }

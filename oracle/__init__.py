@@ -156,6 +156,22 @@ def knn(photons, queries, k, r_max, threads=0):
     return idx, d2, cnt
 
 
+def knn_grid(photons, queries, k, r_max, threads=0):
+    """Grid-accelerated version of knn (identical results), for large photon counts."""
+    L = lib()
+    L.oracle_knn_grid.restype = C.c_int
+    L.oracle_knn_grid.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_int, C.c_float, C.c_void_p,
+                                  C.c_void_p, C.c_void_p, C.c_int]
+    P = _f32(photons).reshape(-1, 3)
+    Q = _f32(queries).reshape(-1, 3)
+    idx = np.empty((Q.shape[0], k), np.int32)
+    d2 = np.empty((Q.shape[0], k), np.float32)
+    cnt = np.empty(Q.shape[0], np.int32)
+    L.oracle_knn_grid(P.ctypes.data, P.shape[0], Q.ctypes.data, Q.shape[0], int(k), float(r_max), idx.ctypes.data,
+                      d2.ctypes.data, cnt.ctypes.data, int(threads))
+    return idx, d2, cnt
+
+
 def photon_trace(render_scene, desc, capacity, threads=0):
     """The photon-tracing restatement over a RenderScene; photons sorted by (path, bounce).
     Returns (records (n,) structured array, counts dict)."""
