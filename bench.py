@@ -279,11 +279,14 @@ def photon_bench(ctx, stream, args, world, dist, local, cpu: bool, n_photons: in
         sel = np.random.default_rng(0).choice(nq, ns, replace=False)
         P = pos.cpu().numpy()
         t0 = time.perf_counter()
+        oracle.knn_grid(P, q[sel[:1]], K, r)  # the grid build alone
+        t_build = time.perf_counter() - t0
+        t0 = time.perf_counter()
         ci, cd, cc = oracle.knn_grid(P, q[sel], K, r)
-        dt = time.perf_counter() - t0
+        dt = max(time.perf_counter() - t0 - t_build, 1e-6)
         out["cpu_baseline"] = {"value": ns / dt, "unit": "queries/s", "cores": oracle.hardware_threads(),
-                               "kind": "port", "sample": f"{ns} of the {nq} gather points (grid k-NN), {dt:.1f} s "
-                                                        "including the grid build"}
+                               "kind": "port", "sample": f"{ns} of the {nq} gather points (grid k-NN), {dt:.2f} s "
+                                                        f"after a {t_build:.1f} s grid build"}
         out["parity_sample"] = {"queries": ns, "identical_neighbour_sets":
                                 bool((didx.cpu().numpy()[sel] == ci).all() and (dcnt.cpu().numpy()[sel] == cc).all())}
     pmap.close()

@@ -5,22 +5,26 @@
 // maxRadius, maxCount) calls (photon_mapper.cpp:1097, 1257, 1312, 1352): the up to k photons
 // nearest to a point, all closer than r_max, the farthest first in the reference's heap.
 //
-// Build (hash grid; Teschner et al. 2003, "Optimized spatial hashing for collision detection"):
-//   cell = r_max * 1.001, cell key = floor((p - origin) / cell), bucket = hash(key) mod 2^m;
-//   counting sort of the photons by bucket (histogram, exclusive scan, scatter) into a
-//   bucket-ordered float4 array (x, y, z, original index).
-// Gather: one warp per query. The 27 cells around the query's cell are mapped to buckets, buckets
-// hit twice are visited once, and the warp streams their photons 32 at a time. The k = 64 nearest
-// are a sorted list of 64-bit keys (d^2 bits << 32 | photon index) spread over the warp (two per
-// lane); a batch of 32 candidates is sorted by a shuffle bitonic network and merged into the list
-// with half-cleaners, skipping batches in which no lane beats the current k-th key.
-// Distances use explicitly rounded IEEE operations in a fixed order, so the key of every
-// (query, photon) pair, and therefore the neighbour set including ties (equal d^2 resolve to the
-// lower index), equals the CPU restatement's.
+// Build (spatial hashing, Teschner et al. 2003): a bounding-box reduction fixes the grid origin;
+// cells are r_max / kRefine wide, cell = floor((p - origin) / cell_size), bucket =
+// hash(cell) mod 2^m; a counting sort (histogram, exclusive scan, scatter) orders the photons by
+// bucket into float4 (x, y, z, original index) records, each with its packed cell key beside it.
+// Gather: one warp per query visits the cells around the query in rings of growing Chebyshev
+// distance R and stops after ring R as soon as the current k-th distance is at most R cell
+// widths (every photon of a later ring is farther than that), or R cell widths reach r_max --
+// the grid form of the kd-tree search that shrinks its radius as it finds neighbours. Candidates
+// are filtered by their cell key, so buckets shared by colliding cells never yield a photon twice.
+// The k = 64 nearest are a sorted list of 64-bit keys (d^2 bits << 32 | photon index), two per
+// lane; a batch of 32 candidates is sorted by a shuffle bitonic network and merged in with
+// half-cleaners, batches with no key below the current k-th are skipped.
+// Distances use explicitly rounded IEEE operations in a fixed order, so every (query, photon) key
+// and therefore the neighbour set, ties included (equal d^2: lower index first), equals the CPU
+// restatement's.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <new>
 #include <vector>
 
@@ -34,22 +38,30 @@ struct liar_gpu_photon_map {
     size_t n = 0;
     float r_max = 0.0f, cell = 0.0f;
     float origin[3] = {0, 0, 0};
+    float extent = 0.0f;
     uint32_t bucket_bits = 0;
-    float4* sorted = nullptr;      // bucket order: x, y, z, original index bits
+    float4* sorted = nullptr;          // bucket order: x, y, z, original index bits
+    uint64_t* cell_key = nullptr;      // packed cell of each sorted photon
     uint32_t* bucket_start = nullptr;  // 2^bits + 1
-    void* scratch = nullptr;       // build scratch (bucket keys, counts), kept for rebuilds
+    void* scratch = nullptr;           // build scratch (bucket keys, counts, bounds), kept for rebuilds
     size_t scratch_bytes = 0;
 };
 
 namespace {
 
 constexpr int kGatherK = 64;
+constexpr float kRefine = 4.0f;              // cells per r_max
+constexpr int kCellBits = 21;                // per axis in the packed cell key
+constexpr int kCellLimit = (1 << kCellBits) - 2;
+constexpr uint32_t kStatusBadBucket = 1u << 4;  // device status bit of the photon kernels
 
 __host__ __device__ __forceinline__ uint32_t bucket_of(int ix, int iy, int iz, uint32_t mask) {
     const uint32_t h = ((uint32_t)ix * 73856093u) ^ ((uint32_t)iy * 19349663u) ^ ((uint32_t)iz * 83492791u);
     return h & mask;
 }
-
+__host__ __device__ __forceinline__ uint64_t pack_cell(int ix, int iy, int iz) {
+    return ((uint64_t)(uint32_t)ix << (2 * kCellBits)) | ((uint64_t)(uint32_t)iy << kCellBits) | (uint64_t)(uint32_t)iz;
+}
 __device__ __forceinline__ int cell_coord(float p, float o, float inv) { return (int)floorf((p - o) * inv); }
 
 // squared distance with fixed IEEE roundings (the CPU restatement performs the same operations)
@@ -62,6 +74,44 @@ struct BuildParams {
     float ox, oy, oz, inv;
     uint32_t mask;
 };
+
+// ---- bounding box (min x, y, z then max x, y, z as order-preserving integer keys)
+__device__ __forceinline__ uint32_t fkey(float f) {
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__host__ __forceinline__ float fkey_inv(uint32_t k) {
+    const uint32_t u = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+__global__ void k_bounds(const float* __restrict__ pos, uint32_t n, uint32_t* __restrict__ bounds) {
+    uint32_t lo[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, hi[3] = {0u, 0u, 0u};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const uint32_t k = fkey(pos[3 * i + a]);
+            lo[a] = min(lo[a], k);
+            hi[a] = max(hi[a], k);
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[a] = min(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
+            hi[a] = max(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
+        }
+    }
+    if ((threadIdx.x & 31u) == 0) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            atomicMin(bounds + a, lo[a]);
+            atomicMax(bounds + 3 + a, hi[a]);
+        }
+    }
+}
 
 __global__ void k_bucket_count(const float* __restrict__ pos, uint32_t n, BuildParams P, uint32_t* __restrict__ keys,
                                uint32_t* __restrict__ counts) {
@@ -121,11 +171,9 @@ __global__ void k_scan_add(uint32_t* __restrict__ out, uint32_t n, const uint32_
     if (i < n) out[i] += block_offsets[i / (kScanBlock * kScanItems)];
 }
 
-// device-side status bits of the photon kernels (ORed into the context's status word)
-constexpr uint32_t kStatusBadBucket = 1u << 4;
-
-__global__ void k_scatter(const float* __restrict__ pos, uint32_t n, const uint32_t* __restrict__ keys,
-                          uint32_t* __restrict__ cursor, float4* __restrict__ sorted, uint32_t* __restrict__ status) {
+__global__ void k_scatter(const float* __restrict__ pos, uint32_t n, BuildParams P, const uint32_t* __restrict__ keys,
+                          uint32_t* __restrict__ cursor, float4* __restrict__ sorted, uint64_t* __restrict__ cell_key,
+                          uint32_t* __restrict__ status) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t slot = atomicAdd(cursor + keys[i], 1u);
@@ -133,7 +181,9 @@ __global__ void k_scatter(const float* __restrict__ pos, uint32_t n, const uint3
         atomicOr(status, kStatusBadBucket);
         return;
     }
-    sorted[slot] = make_float4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], __uint_as_float(i));
+    const float x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
+    sorted[slot] = make_float4(x, y, z, __uint_as_float(i));
+    cell_key[slot] = pack_cell(cell_coord(x, P.ox, P.inv), cell_coord(y, P.oy, P.inv), cell_coord(z, P.oz, P.inv));
 }
 
 // ---- warp sorting helpers on 64-bit keys
@@ -167,67 +217,94 @@ __device__ __forceinline__ uint64_t reverse_lanes(uint64_t v) {
     return __shfl_sync(0xffffffffu, (unsigned long long)v, 31 - (threadIdx.x & 31u));
 }
 
-__global__ void __launch_bounds__(256) k_gather(const float4* __restrict__ sorted, const uint32_t* __restrict__ start,
-                                                BuildParams P, float r2max, const float* __restrict__ queries,
-                                                uint32_t nq, int k_out, int32_t* __restrict__ out_idx,
-                                                float* __restrict__ out_d2, int32_t* __restrict__ out_count,
-                                                uint32_t n_photons, uint32_t* __restrict__ status) {
+struct GatherParams {
+    BuildParams B;
+    float r2max;
+    float cell;
+    float slack;      // cell-assignment round-off allowance in the ring stopping rule
+    int max_ring;
+    uint32_t n_photons;
+};
+
+__global__ void __launch_bounds__(256) k_gather(const float4* __restrict__ sorted, const uint64_t* __restrict__ cell_key,
+                                                const uint32_t* __restrict__ start, GatherParams G,
+                                                const float* __restrict__ queries, uint32_t nq, int k_out,
+                                                int32_t* __restrict__ out_idx, float* __restrict__ out_d2,
+                                                int32_t* __restrict__ out_count, uint32_t* __restrict__ status) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
     constexpr uint64_t INF = ~0ull;
+    const BuildParams& P = G.B;
     for (uint32_t q = warp_global; q < nq; q += n_warps) {
         const float qx = queries[3 * q], qy = queries[3 * q + 1], qz = queries[3 * q + 2];
         const int cx = cell_coord(qx, P.ox, P.inv), cy = cell_coord(qy, P.oy, P.inv), cz = cell_coord(qz, P.oz, P.inv);
-        // the 27 neighbour buckets, one per lane (lanes 27..31 idle); drop repeats
-        uint32_t my_bucket = 0xffffffffu;
-        if (lane < 27) {
-            const int dx = (int)(lane % 3) - 1, dy = (int)((lane / 3) % 3) - 1, dz = (int)(lane / 9) - 1;
-            my_bucket = bucket_of(cx + dx, cy + dy, cz + dz, P.mask);
-        }
-        bool first = lane < 27;
-#pragma unroll 1
-        for (int o = 0; o < 27; ++o) {
-            const uint32_t other = __shfl_sync(0xffffffffu, my_bucket, o);
-            if ((uint32_t)o < lane && other == my_bucket) first = false;
-        }
-        uint32_t todo = __ballot_sync(0xffffffffu, first);
         // the k nearest so far, ascending: slot `lane` in lo, slot `32 + lane` in hi
         uint64_t lo = INF, hi = INF;
         uint64_t kth = INF;  // key of the current k-th (64th) nearest
-        while (todo) {
-            const int src = __ffs(todo) - 1;
-            todo &= todo - 1;
-            const uint32_t b = __shfl_sync(0xffffffffu, my_bucket, src);
-            const uint32_t s0 = __ldg(start + b), s1 = __ldg(start + b + 1);
-            if (s0 > s1 || s1 > n_photons) {  // a corrupt bucket range: record it and skip the bucket
-                if (lane == 0) atomicOr(status, kStatusBadBucket);
-                continue;
-            }
-            for (uint32_t base = s0; base < s1; base += 32) {
-                uint64_t key = INF;
-                const uint32_t i = base + lane;
-                if (i < s1) {
-                    const float4 p = __ldg(sorted + i);
-                    const float d2 = dist2_exact(p.x, p.y, p.z, qx, qy, qz);
-                    if (d2 < r2max) key = ((uint64_t)__float_as_uint(d2) << 32) | (uint64_t)__float_as_uint(p.w);
+        for (int R = 0; R <= G.max_ring; ++R) {
+            const int side = 2 * R + 1;
+            const int cube = side * side * side;
+            for (int c0 = 0; c0 < cube; c0 += 32) {
+                // lane: one cell of the cube around the query; keep the shell cells (Chebyshev = R)
+                const int c = c0 + (int)lane;
+                int dx = 0, dy = 0, dz = 0;
+                bool mine = false;
+                if (c < cube) {
+                    dx = c % side - R;
+                    dy = (c / side) % side - R;
+                    dz = c / (side * side) - R;
+                    mine = max(abs(dx), max(abs(dy), abs(dz))) == R;
                 }
-                if (__ballot_sync(0xffffffffu, key < kth) == 0u) continue;
-                // merge the batch into the 64 nearest
-                const uint64_t bsort = warp_sort32(key);
-                // smallest 32 of hi and the batch: half-cleaner against the reversed batch (every
-                // shuffle is executed by all 32 lanes, outside any lane-dependent branch)
-                const uint64_t brev = reverse_lanes(bsort);
-                uint64_t m = hi < brev ? hi : brev;
-                m = warp_bitonic_merge32(m);
-                // lo (sorted) and m (sorted): split into the lower and upper 32
-                const uint64_t mr = reverse_lanes(m);
-                uint64_t nlo = lo < mr ? lo : mr;
-                uint64_t nhi = lo < mr ? mr : lo;
-                lo = warp_bitonic_merge32(nlo);
-                hi = warp_bitonic_merge32(nhi);
-                kth = __shfl_sync(0xffffffffu, (unsigned long long)hi, 31);
+                const int ix = cx + dx, iy = cy + dy, iz = cz + dz;
+                mine = mine && ix >= 0 && iy >= 0 && iz >= 0 && ix <= kCellLimit && iy <= kCellLimit && iz <= kCellLimit;
+                uint32_t s0 = 0, s1 = 0;
+                if (mine) {
+                    const uint32_t b = bucket_of(ix, iy, iz, P.mask);
+                    s0 = __ldg(start + b);
+                    s1 = __ldg(start + b + 1);
+                    if (s0 > s1 || s1 > G.n_photons) {  // corrupt bucket range: record it, skip the cell
+                        atomicOr(status, kStatusBadBucket);
+                        s0 = s1 = 0;
+                    }
+                }
+                const uint64_t my_key = pack_cell(ix, iy, iz);
+                uint32_t todo = __ballot_sync(0xffffffffu, s1 > s0);
+                while (todo) {
+                    const int src = __ffs(todo) - 1;
+                    todo &= todo - 1;
+                    const uint32_t b0 = __shfl_sync(0xffffffffu, s0, src), b1 = __shfl_sync(0xffffffffu, s1, src);
+                    const uint64_t target = __shfl_sync(0xffffffffu, (unsigned long long)my_key, src);
+                    for (uint32_t base = b0; base < b1; base += 32) {
+                        uint64_t key = INF;
+                        const uint32_t i = base + lane;
+                        if (i < b1 && __ldg(reinterpret_cast<const unsigned long long*>(cell_key) + i) == target) {
+                            const float4 p = __ldg(sorted + i);
+                            const float d2 = dist2_exact(p.x, p.y, p.z, qx, qy, qz);
+                            if (d2 < G.r2max) key = ((uint64_t)__float_as_uint(d2) << 32) | (uint64_t)__float_as_uint(p.w);
+                        }
+                        if (__ballot_sync(0xffffffffu, key < kth) == 0u) continue;
+                        const uint64_t bsort = warp_sort32(key);
+                        // smallest 32 of hi and the batch: half-cleaner against the reversed batch
+                        // (every shuffle is executed by all 32 lanes, outside lane-dependent branches)
+                        const uint64_t brev = reverse_lanes(bsort);
+                        uint64_t m = hi < brev ? hi : brev;
+                        m = warp_bitonic_merge32(m);
+                        // lo (sorted) and m (sorted): split into the lower and upper 32
+                        const uint64_t mr = reverse_lanes(m);
+                        const uint64_t nlo = lo < mr ? lo : mr;
+                        const uint64_t nhi = lo < mr ? mr : lo;
+                        lo = warp_bitonic_merge32(nlo);
+                        hi = warp_bitonic_merge32(nhi);
+                        kth = __shfl_sync(0xffffffffu, (unsigned long long)hi, 31);
+                    }
+                }
             }
+            // every photon outside rings 0..R is farther than R cells (minus round-off)
+            const float reach = fmaxf((float)R * G.cell - G.slack, 0.0f);
+            const uint64_t kk = __shfl_sync(0xffffffffu, (unsigned long long)(k_out > 32 ? hi : lo), (k_out - 1) & 31);
+            if (kk != INF && __uint_as_float((uint32_t)(kk >> 32)) <= reach * reach) break;
+            if (reach * reach >= G.r2max) break;
         }
         // write the first k_out entries (k_out <= 64) in ascending order
         const uint32_t cnt_lo = __popc(__ballot_sync(0xffffffffu, lo != INF));
@@ -262,7 +339,7 @@ __global__ void k_estimate(const float* __restrict__ power, const float* __restr
         for (int j = 0; j < c && j < k; ++j) {
             const int32_t i = idx[(size_t)q * k + j];
             if (i < 0 || (uint32_t)i >= n_photons) {
-                atomicOr(status, 1u << 4);
+                atomicOr(status, kStatusBadBucket);
                 continue;
             }
             if (omega_in[3 * i] * nx + omega_in[3 * i + 1] * ny + omega_in[3 * i + 2] * nz > 0.0f) {
@@ -283,16 +360,13 @@ __global__ void k_estimate(const float* __restrict__ power, const float* __restr
 }
 
 int map_build_impl(liar_gpu_ctx* ctx, liar_gpu_photon_map* m, const float* d_pos, size_t n, cudaStream_t st) {
-    // bounding box on the host side of the caller's data is not available for device input: the
-    // origin only has to be consistent between build and gather, so a fixed origin is used
-    m->origin[0] = m->origin[1] = m->origin[2] = 0.0f;
     // buckets: the next power of two >= 2n, at most 2^23 (the two-level scan covers 2^24 entries)
     uint32_t bits = 10;
     while (bits < 23 && (1ull << bits) < 2ull * n) ++bits;
     m->bucket_bits = bits;
     const size_t nb = (size_t)1 << bits;
     const size_t scan_blocks = (nb + 1 + kScanBlock * kScanItems - 1) / (kScanBlock * kScanItems);
-    const size_t need = n * 4 + (nb + 1) * 4 + (nb + 1) * 4 + (scan_blocks + 1) * 8 + 1024;
+    const size_t need = n * 4 + 2 * (((nb + 1) * 4 + 255) / 256) * 256 + (scan_blocks + 1) * 8 + 4096;
     if (m->scratch_bytes < need) {
         if (m->scratch) cudaFree(m->scratch);
         m->scratch = nullptr;
@@ -305,10 +379,13 @@ int map_build_impl(liar_gpu_ctx* ctx, liar_gpu_photon_map* m, const float* d_pos
         m->scratch_bytes = need;
     }
     if (m->sorted) cudaFree(m->sorted);
+    if (m->cell_key) cudaFree(m->cell_key);
     if (m->bucket_start) cudaFree(m->bucket_start);
     m->sorted = nullptr;
+    m->cell_key = nullptr;
     m->bucket_start = nullptr;
     cudaError_t e = cudaMalloc((void**)&m->sorted, std::max<size_t>(n, 1) * sizeof(float4));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&m->cell_key, std::max<size_t>(n, 1) * sizeof(uint64_t));
     if (e == cudaSuccess) e = cudaMalloc((void**)&m->bucket_start, (nb + 1) * sizeof(uint32_t));
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -321,8 +398,34 @@ int map_build_impl(liar_gpu_ctx* ctx, liar_gpu_photon_map* m, const float* d_pos
     p += (((nb + 1) * 4 + 255) / 256) * 256;
     uint32_t* cursor = reinterpret_cast<uint32_t*>(p);
     p += (((nb + 1) * 4 + 255) / 256) * 256;
+    uint32_t* bounds = reinterpret_cast<uint32_t*>(p);
+    p += 256;
     uint32_t* block_sums = reinterpret_cast<uint32_t*>(p);
     uint32_t* block_offs = block_sums + scan_blocks + 1;
+    // grid origin and extent from the photons' bounding box
+    m->origin[0] = m->origin[1] = m->origin[2] = 0.0f;
+    m->extent = 0.0f;
+    if (n) {
+        const uint32_t init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+        e = cudaMemcpyAsync(bounds, init, sizeof(init), cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return ctx_cuda(ctx, e, "photon bounds");
+        const unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, (size_t)ctx->num_sms * 4);
+        k_bounds<<<blocks, 256, 0, st>>>(d_pos, (uint32_t)n, bounds);
+        uint32_t hb[6];
+        e = cudaMemcpyAsync(hb, bounds, sizeof(hb), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return ctx_cuda(ctx, e, "photon bounds");
+        for (int a = 0; a < 3; ++a) {
+            const float lo = fkey_inv(hb[a]), hi = fkey_inv(hb[3 + a]);
+            if (!std::isfinite(lo) || !std::isfinite(hi)) return ctx_fail(ctx, LIAR_ERR_INVALID, "photon position is not finite");
+            // one cell of margin below the lowest photon keeps every cell index positive
+            m->origin[a] = lo - m->cell;
+            m->extent = std::max(m->extent, hi - m->origin[a]);
+        }
+        if (m->extent / m->cell > (float)(kCellLimit - 4))
+            return ctx_fail(ctx, LIAR_ERR_UNSUPPORTED, "photons span more than %d grid cells per axis; raise r_max",
+                            kCellLimit - 4);
+    }
     BuildParams P{m->origin[0], m->origin[1], m->origin[2], 1.0f / m->cell, (uint32_t)(nb - 1)};
     e = cudaMemsetAsync(counts, 0, (nb + 1) * 4, st);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "photon map counts");
@@ -330,7 +433,6 @@ int map_build_impl(liar_gpu_ctx* ctx, liar_gpu_photon_map* m, const float* d_pos
     // exclusive scan of counts[0 .. nb] -> bucket_start (start[nb] = n)
     k_scan_local<<<(unsigned)scan_blocks, kScanBlock, 0, st>>>(counts, (uint32_t)(nb + 1), m->bucket_start, block_sums);
     if (scan_blocks > 1) {
-        // scan of the block sums (scan_blocks <= 2^26 / 4096 = 16384 entries: one more level)
         const size_t blocks2 = (scan_blocks + kScanBlock * kScanItems - 1) / (kScanBlock * kScanItems);
         if (blocks2 > 1) return ctx_fail(ctx, LIAR_ERR_UNSUPPORTED, "photon map too large to scan");
         k_scan_local<<<1, kScanBlock, 0, st>>>(block_sums, (uint32_t)scan_blocks, block_offs, block_sums + scan_blocks);
@@ -339,8 +441,8 @@ int map_build_impl(liar_gpu_ctx* ctx, liar_gpu_photon_map* m, const float* d_pos
     e = cudaMemcpyAsync(cursor, m->bucket_start, (nb + 1) * 4, cudaMemcpyDeviceToDevice, st);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "photon map cursor");
     if (n)
-        k_scatter<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_pos, (uint32_t)n, keys, cursor, m->sorted,
-                                                              ctx->d_scratch + kStatusWord);
+        k_scatter<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_pos, (uint32_t)n, P, keys, cursor, m->sorted,
+                                                              m->cell_key, ctx->d_scratch + kStatusWord);
     m->n = n;
     return ctx_cuda(ctx, cudaGetLastError(), "photon map build");
 }
@@ -360,7 +462,7 @@ extern "C" int liar_gpu_photon_map_build_device(liar_gpu_ctx* ctx, const float* 
     if (!m) return ctx_fail(ctx, LIAR_ERR_OOM, "host allocation");
     m->device = ctx->device;
     m->r_max = r_max;
-    m->cell = r_max * 1.001f;
+    m->cell = r_max / kRefine;
     rc = map_build_impl(ctx, m, d_positions, n, stream ? (cudaStream_t)stream : ctx->stream);
     if (rc) {
         liar_gpu_photon_map_destroy(m);
@@ -394,6 +496,7 @@ extern "C" int liar_gpu_photon_map_build(liar_gpu_ctx* ctx, const float* positio
         liar_gpu_photon_map_destroy(*out);
         *out = nullptr;
     }
+    if (!rc) rc = ctx_check_status(ctx);
     return rc;
 }
 
@@ -403,6 +506,7 @@ extern "C" void liar_gpu_photon_map_destroy(liar_gpu_photon_map* m) {
     cudaGetDevice(&cur);
     if (m->device >= 0) cudaSetDevice(m->device);
     if (m->sorted) cudaFree(m->sorted);
+    if (m->cell_key) cudaFree(m->cell_key);
     if (m->bucket_start) cudaFree(m->bucket_start);
     if (m->scratch) cudaFree(m->scratch);
     if (cur >= 0) cudaSetDevice(cur);
@@ -421,11 +525,17 @@ extern "C" int liar_gpu_photon_gather_device(liar_gpu_ctx* ctx, const liar_gpu_p
     int rc = ctx_activate(ctx);
     if (rc) return rc;
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
-    BuildParams P{m->origin[0], m->origin[1], m->origin[2], 1.0f / m->cell, (uint32_t)(((size_t)1 << m->bucket_bits) - 1)};
-    const float r2 = m->r_max * m->r_max;
+    GatherParams G;
+    G.B = BuildParams{m->origin[0], m->origin[1], m->origin[2], 1.0f / m->cell,
+                      (uint32_t)(((size_t)1 << m->bucket_bits) - 1)};
+    G.r2max = m->r_max * m->r_max;
+    G.cell = m->cell;
+    G.slack = std::max(1e-3f * m->cell, 8.0f * 1.1920929e-07f * std::max(m->extent, 1.0f));
+    G.max_ring = (int)std::ceil(m->r_max / m->cell) + 1;
+    G.n_photons = (uint32_t)m->n;
     const unsigned blocks = (unsigned)std::min<size_t>((n_queries + 7) / 8, (size_t)ctx->num_sms * 8);
-    k_gather<<<blocks, 256, 0, st>>>(m->sorted, m->bucket_start, P, r2, d_queries, (uint32_t)n_queries, k, d_idx, d_d2,
-                                     d_count, (uint32_t)m->n, ctx->d_scratch + kStatusWord);
+    k_gather<<<blocks, 256, 0, st>>>(m->sorted, m->cell_key, m->bucket_start, G, d_queries, (uint32_t)n_queries, k, d_idx,
+                                     d_d2, d_count, ctx->d_scratch + kStatusWord);
     return ctx_cuda(ctx, cudaGetLastError(), "photon gather launch");
 }
 
@@ -435,6 +545,8 @@ extern "C" int liar_gpu_photon_gather(liar_gpu_ctx* ctx, const liar_gpu_photon_m
     if (!m || (n_queries && (!queries || !idx || !d2))) return ctx_fail(ctx, LIAR_ERR_INVALID, "null map or buffer");
     if (k < 1 || k > kGatherK) return ctx_fail(ctx, LIAR_ERR_INVALID, "k must be 1..%d", kGatherK);
     if (n_queries == 0) return LIAR_OK;
+    for (size_t i = 0; i < 3 * n_queries; ++i)
+        if (!std::isfinite(queries[i])) return ctx_fail(ctx, LIAR_ERR_INVALID, "query position is not finite");
     int rc = ctx_activate(ctx);
     if (rc) return rc;
     const size_t qb = n_queries * 12, ob = n_queries * (size_t)k * 4, cb = n_queries * 4;
@@ -459,6 +571,7 @@ extern "C" int liar_gpu_photon_gather(liar_gpu_ctx* ctx, const liar_gpu_photon_m
         if (e != cudaSuccess) rc = ctx_cuda(ctx, e, "gather results");
     }
     cudaFree(d);
+    if (!rc) rc = ctx_check_status(ctx);
     return rc;
 }
 
