@@ -170,6 +170,81 @@ def cornell_bench(ctx, stream, args, world, dist, local, cpu: bool) -> dict:
     return out
 
 
+def batch_bench(ctx, stream, args, world, dist, local, cpu: bool, n_scenes: int = 64) -> dict:
+    """Batched rendering: 64 seeded procedural scenes (10k-2M triangles, 128^2-1024^2, 4-64 spp,
+    log-uniform), 4 hero wavelengths, max depth 8, the whole batch as one CUDA-graph launch with
+    launch shapes chosen by the autotuner. samples/s counts camera paths (each carries 4 wavelengths)."""
+    import torch
+    from liar_b200 import batch as B, render as R, scenes_batch as SB
+    t0 = time.perf_counter()
+    work = SB.batch_workload(n_scenes, seed=0)
+    tracer = SB.batch_tracer()
+    flats = [R.flatten(w.scene) for w in work]
+    scenes = [R.GpuScene(ctx, f) for f in flats]
+    entries = [(gs, R.render_desc(w.camera, w.width, w.height, w.spp, tracer, seed=k))
+               for k, (gs, w) in enumerate(zip(scenes, work))]
+    setup_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    cfg, tune = B.tune_batch(ctx, entries, hero=4, probe_spp=2, stream=stream.cuda_stream)
+    tune_s = time.perf_counter() - t0
+    br = B.BatchRenderer(ctx, entries, cfg)
+    br.launch(stream.cuda_stream)                    # warm-up: the whole batch once
+    stream.synchronize()
+    steps = 2
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        br.launch(stream.cuda_stream)
+    e1.record(stream)
+    stream.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    st = br.stats()
+    tris = [w.n_triangles for w in work]
+    out = {"workload": f"{n_scenes} procedural scenes, {min(tris)}-{max(tris)} triangles ({sum(tris)} total), "
+                       "128^2-1024^2, 4-64 spp, 4 hero wavelengths, RR from generation 3, max depth 8",
+           "ms_per_batch": ms, "samples_per_s": world * st["paths"] / (ms * 1e-3),
+           "segments_per_s": world * st["segments"] / (ms * 1e-3), "samples_per_batch": st["paths"],
+           "segments_per_sample": st["segments"] / st["paths"], "waves": st["waves"],
+           "graph_launches_per_batch": 1,
+           "tuned": {"trace": [cfg.trace.block_size, cfg.trace.smem_stack],
+                     "wave_paths": cfg.wave_paths, "shade_blocks_per_sm": cfg.shade_blocks_per_sm,
+                     "cached": tune.get("cached", False), "seconds": tune_s},
+           "setup_seconds": setup_s,
+           "note": "device time of one cudaGraphLaunch per batch (WHILE node over waves, queue sizes on device)"}
+    br.close()
+    if cpu:
+        import oracle
+        # the CPU restatement (one wavelength per sample) on the middle rows of the smallest, the
+        # median and the largest scene, about 4 s each
+        order = np.argsort(tris)
+        done, dt = 0, 0.0
+        picked = []
+        for k in (int(order[0]), int(order[len(order) // 2]), int(order[-1])):
+            w, d = work[k], entries[k][1]
+            rs = oracle.RenderScene(flats[k])
+            film = np.zeros((d.height, d.width, 8), np.float32)
+            row, t_scene = d.height // 2, 0.0
+            while t_scene < 4.0 and row < d.height:
+                rows = min(4, d.height - row)
+                t1 = time.perf_counter()
+                rs.render(d, film, pixels=(row * d.width, (row + rows) * d.width))
+                t_scene += time.perf_counter() - t1
+                done += rows * d.width * d.spp
+                row += rows
+            dt += t_scene
+            picked.append(f"scene {k} ({w.n_triangles} tris, {w.width}^2, {w.spp} spp)")
+        out["cpu_baseline"] = {"value": done / dt, "unit": "samples/s", "cores": oracle.hardware_threads(),
+                               "kind": "port", "sample": f"{done} samples of {', '.join(picked)}, one wavelength "
+                                                         f"per sample, {dt:.1f} s"}
+    for gs in scenes:
+        gs.close()
+    return out
+
+
 def camera_queries(flat, cam, width, height):
     """Gather points of the photon workload: the first hits of the camera's pixel-centre rays on
     surfaces with a diffuse (Lambert) BSDF, with their normals flipped toward the camera."""
@@ -335,6 +410,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-workloads", action="store_true", help="only the traversal workload")
+    ap.add_argument("--batch-scenes", type=int, default=64, help="scenes in the batched-rendering workload")
+    ap.add_argument("--only", default="", help="comma list of workloads to run (cornell,photon,batch); default all")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world, rank, local = dist_setup()
@@ -464,8 +541,13 @@ def main():
     mesh.close()
     if not args.no_workloads:
         cpu_leg = rank == 0 and world == 1 and not args.no_cpu_baseline
-        line["cornell"] = cornell_bench(ctx, stream, args, world, dist, local, cpu=cpu_leg)
-        line["photon"] = photon_bench(ctx, stream, args, world, dist, local, cpu=cpu_leg)
+        only = set(filter(None, args.only.split(",")))
+        if not only or "cornell" in only:
+            line["cornell"] = cornell_bench(ctx, stream, args, world, dist, local, cpu=cpu_leg)
+        if not only or "photon" in only:
+            line["photon"] = photon_bench(ctx, stream, args, world, dist, local, cpu=cpu_leg)
+        if not only or "batch" in only:
+            line["batch"] = batch_bench(ctx, stream, args, world, dist, local, cpu=cpu_leg, n_scenes=args.batch_scenes)
     ctx.close()
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -229,6 +229,35 @@ int liar_gpu_render_device(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const
 /* Path statistics of the last render on ctx: [0] paths, [1] path segments traced, [2] rays that hit. */
 int liar_gpu_render_stats(const liar_gpu_ctx* ctx, unsigned long long* out3);
 
+/* ---- batched rendering (no reference counterpart: the reference renders one scene per process)
+ * Many scenes, resolutions and sample counts rendered by one CUDA-graph launch: a scene table,
+ * the paths of all items in one index space cut into waves, and a device-side WHILE loop over the
+ * waves (conditional graph node), each wave running raygen and `max_bounces` x (trace, shade) with
+ * queue sizes that stay on the device. hero_wavelengths = 4 carries four wavelengths per path
+ * (hero wavelength spectral sampling: the first is sampled from the observer, the others are
+ * rotations of it over the observer's range, combined with the balance heuristic); secondary
+ * wavelengths end at a dispersive (non-constant index) dielectric. */
+typedef struct liar_gpu_batch liar_gpu_batch;
+typedef struct liar_batch_item {
+    const liar_gpu_scene* scene;
+    liar_render_desc render;   /* tracer must be LIAR_TRACER_ADJOINT_PHOTON; wave_paths is ignored */
+    float* d_film;             /* device film, width x height x 8 floats; samples are added */
+} liar_batch_item;
+typedef struct liar_batch_config {
+    int32_t hero_wavelengths;  /* 1 or 4 */
+    int32_t max_bounces;       /* bounces per wave; must be >= the items' max_depth (0 = that max_depth) */
+    int32_t wave_paths;        /* paths in flight per wave, 0 = 4M */
+    int32_t shade_blocks_per_sm; /* grid of the shade kernel: 4, 8 or 16 blocks of 128 per SM, 0 = 16 */
+    liar_trace_config trace;   /* zero = the context's trace config */
+} liar_batch_config;
+int liar_gpu_batch_create(liar_gpu_ctx* ctx, const liar_batch_item* items, size_t n_items,
+                          const liar_batch_config* cfg, liar_gpu_batch** out);
+/* one cudaGraphLaunch on `stream` (NULL = the context's stream) renders every item */
+int liar_gpu_batch_launch(liar_gpu_ctx* ctx, liar_gpu_batch* batch, void* stream);
+/* after a launch has finished: [0] paths, [1] path segments traced, [2] segments that hit, [3] waves */
+int liar_gpu_batch_stats(const liar_gpu_batch* batch, unsigned long long* out4);
+void liar_gpu_batch_destroy(liar_gpu_batch* batch);
+
 /* ---- photon maps -------------------------------------------------------------------------------
  * Replace the Lass KdTree<Photon> of PhotonMapper::buildPhotonMap (src/liar/tracers/photon_mapper.cpp:798-835)
  * and its rangeSearch(point, maxRadius, maxCount) (photon_mapper.cpp:1097,1257,1312,1352): for each

@@ -95,6 +95,11 @@ SIGNATURES: dict[str, tuple] = {
     "liar_gpu_photon_trace": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "liar_gpu_photon_estimate_device": (C.c_int, [_vp, _vp, _vp, _sz, _vp, _sz, C.c_int, _vp, _vp, _vp, C.c_float,
                                                   _vp, _vp]),
+    # batched rendering (liar_b200/batch.py)
+    "liar_gpu_batch_create": (C.c_int, [_vp, _vp, _sz, _vp, C.POINTER(_vp)]),
+    "liar_gpu_batch_launch": (C.c_int, [_vp, _vp, _vp]),
+    "liar_gpu_batch_stats": (C.c_int, [_vp, _vp]),
+    "liar_gpu_batch_destroy": (None, [_vp]),
 }
 
 

@@ -328,4 +328,103 @@ __global__ void __launch_bounds__(BLOCK) trace_kernel(const QNode* __restrict__ 
     }
 }
 
+// ---- many trees in one launch (batched rendering): each ray names its scene, whose tree comes
+// from a table; the ray count is read from device memory, so the launch can sit in a CUDA graph
+// whose queue sizes are only known on the device
+struct TreeRoot {
+    const QNode* nodes;
+    const QTri* tris;
+};
+
+template <int S, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) trace_multi_kernel(const TreeRoot* __restrict__ roots,
+                                                            const liar_ray* __restrict__ rays,
+                                                            const uint32_t* __restrict__ ray_scene,
+                                                            liar_hit* __restrict__ hits, const uint32_t* __restrict__ n_dev,
+                                                            uint32_t* __restrict__ work_counter,
+                                                            uint32_t* __restrict__ status_word) {
+    constexpr uint32_t BATCH = 256;
+    constexpr int REFILL = 8;
+    extern __shared__ int trace_smem[];
+    LaneStack<S, BLOCK> stack;
+    stack.s_node = trace_smem;
+    stack.s_t = reinterpret_cast<float*>(trace_smem + S * BLOCK);
+    const uint32_t n_rays = *n_dev;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    const uint64_t pol_tree = policy_evict_last();
+    const uint64_t pol_stream = policy_evict_first();
+    uint32_t status = 0, n_nodes = 0, n_tris = 0;
+    uint32_t w_next = 0, w_end = 0;
+    bool exhausted = false;
+    int rid = -1;
+    RayState st;
+    const QNode* nodes = nullptr;
+    const QTri* tris = nullptr;
+    while (true) {
+        const uint32_t idle = __ballot_sync(0xffffffffu, rid < 0);
+        if (exhausted) {
+            if (idle == 0xffffffffu) break;
+        } else if ((uint32_t)__popc(idle) >= (uint32_t)REFILL) {
+            if (w_next >= w_end) {
+                uint32_t b = 0;
+                if (lane == 0) b = atomicAdd(work_counter, BATCH);
+                b = __shfl_sync(0xffffffffu, b, 0);
+                if (b >= n_rays) {
+                    exhausted = true;
+                } else {
+                    w_next = b;
+                    w_end = min(b + BATCH, n_rays);
+                }
+            }
+            if (!exhausted) {
+                const uint32_t avail = w_end - w_next;
+                const uint32_t rank = __popc(idle & lt_mask);
+                if (rid < 0 && rank < avail) {
+                    rid = (int)(w_next + rank);
+                    const TreeRoot root = roots[ray_scene[rid]];
+                    nodes = root.nodes;
+                    tris = root.tris;
+                    const float4* rp = reinterpret_cast<const float4*>(rays + rid);
+                    const float4 r0 = ld_hint(rp, pol_stream), r1 = ld_hint(rp + 1, pol_stream);
+                    st.ox = r0.x;
+                    st.oy = r0.y;
+                    st.oz = r0.z;
+                    st.tmin = r0.w;
+                    st.dx = r1.x;
+                    st.dy = r1.y;
+                    st.dz = r1.z;
+                    st.tmax = r1.w;
+                    st.idx = safe_rcp(st.dx);
+                    st.idy = safe_rcp(st.dy);
+                    st.idz = safe_rcp(st.dz);
+                    st.oix = st.ox * st.idx;
+                    st.oiy = st.oy * st.idy;
+                    st.oiz = st.oz * st.idz;
+                    st.tbest = range_far(st.tmax);
+                    st.best = -1;
+                    st.sp = 0;
+                    const bool finite = isfinite(r0.x) && isfinite(r0.y) && isfinite(r0.z) && isfinite(r1.x) &&
+                                        isfinite(r1.y) && isfinite(r1.z) && !isnan(r0.w) && !isnan(r1.w);
+                    st.node = finite ? 0 : kNodeNone;
+                }
+                w_next += min(avail, (uint32_t)__popc(idle));
+            }
+        }
+        if (rid >= 0) {
+            const bool done = st.node == kNodeNone ||
+                              trace_step<false, S, BLOCK, false>(nodes, tris, st, stack, pol_tree, status, n_nodes, n_tris);
+            if (done) {
+                int prim = st.best;
+                float t = st.tbest;
+                if (prim >= 0 && !(t > range_near(st.tmin))) prim = -1;
+                if (prim < 0) t = INFINITY;
+                st_hint(hits + rid, prim, __float_as_int(t), pol_stream);
+                rid = -1;
+            }
+        }
+    }
+    if (status) atomicOr(status_word, status);
+}
+
 }  // namespace liar_gpu
