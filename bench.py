@@ -36,8 +36,9 @@ def load_peaks() -> dict:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
         d = json.loads(p.read_text())
-        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
-    return {"hbm_gbs": 6650.0, "source": "fallback"}
+        return {"hbm_gbs": float(d["hbm_gbs"]), "bf16_tflops": float(d.get("bf16_tflops", 1590.0)),
+                "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
 
 
 class ClockSampler:
@@ -245,6 +246,134 @@ def batch_bench(ctx, stream, args, world, dist, local, cpu: bool, n_scenes: int 
     return out
 
 
+def guided_bench(ctx, stream, args, world, dist, local, cpu: bool) -> dict:
+    """Learned path guiding on the slit room (200k clutter triangles, 1024^2): time for guided
+    rendering (online training included) to reach the error of a plain 1024-spp render, against a
+    plain reference at args.guided_ref_spp (the reference's own variance is subtracted from each MSE).
+    Also the guide network's tensor-core throughput (inference and one training step)."""
+    import torch
+    from liar_b200 import guiding as GD, render as R, scenes_guiding as SG
+    res, ref_spp, plain_spp, chunk = args.guided_res, args.guided_ref_spp, 1024, 16
+    dev = f"cuda:{local}"
+    scene, cam = SG.slit_room(200_000)
+    flat = R.flatten(scene)
+    gs = R.GpuScene(ctx, flat)
+    tracer = SG.guiding_tracer()
+    st = stream.cuda_stream
+
+    def film():
+        return torch.zeros((res, res, 8), dtype=torch.float32, device=dev)
+
+    def resolve(f):
+        n = f[..., 7:8].clamp(min=1.0)
+        mean = f[..., 0:3] / n
+        var = (f[..., 4:7] / n - mean ** 2).clamp(min=0.0) / (n - 1).clamp(min=1.0)
+        return mean, var
+
+    ref = film()
+    t0 = time.perf_counter()
+    for k in range(0, ref_spp, 256):
+        gs.render_device(R.render_desc(cam, res, res, min(256, ref_spp - k), tracer, seed=1_000_000, first_sample=k),
+                         ref.data_ptr(), st)
+    stream.synchronize()
+    ref_s = time.perf_counter() - t0
+    ref_mean, ref_var = resolve(ref)
+    ref_var_term = float(ref_var.mean())
+
+    def mse(f):
+        m, _ = resolve(f)
+        return float(((m - ref_mean) ** 2).mean()) - ref_var_term
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    plain = film()
+    gs.render_device(R.render_desc(cam, res, res, 16, tracer, seed=5), film().data_ptr(), st)  # warm-up
+    e0.record(stream)
+    gs.render_device(R.render_desc(cam, res, res, plain_spp, tracer, seed=7), plain.data_ptr(), st)
+    e1.record(stream)
+    stream.synchronize()
+    plain_s = e0.elapsed_time(e1) * 1e-3
+    plain_mse = mse(plain)
+    plain_stats = gs.stats()
+    # guided: chunks of 16 spp, training during the first 8 chunks
+    g = GD.Guide(ctx, GD.scene_bounds(flat), guide_probability=0.3, learning_rate=5e-3, steps_per_pass=4,
+                 batch_records=65536, seed=0)
+    gf = film()
+    curve, t_cum, spp, t_hit = [], 0.0, 0, None
+    while spp < 4 * plain_spp:
+        d = R.render_desc(cam, res, res, chunk, tracer, seed=11, first_sample=spp)
+        e0.record(stream)
+        g.render(gs, d, gf.data_ptr(), train=spp < 8 * chunk, stream=st)
+        e1.record(stream)
+        stream.synchronize()
+        dt = e0.elapsed_time(e1) * 1e-3
+        prev_t, prev_m = t_cum, (curve[-1][2] if curve else None)
+        t_cum += dt
+        spp += chunk
+        m = mse(gf)
+        curve.append((round(t_cum, 4), spp, m))
+        if m <= plain_mse and t_hit is None:
+            # linear interpolation of the crossing inside the last chunk
+            if prev_m is not None and prev_m > m:
+                t_hit = prev_t + dt * (prev_m - plain_mse) / (prev_m - m)
+            else:
+                t_hit = t_cum
+            break
+    gstats = g.stats()
+    # the network alone: inference over 1M vertices, one training step over 65,536 records
+    x = torch.rand((1 << 20, 9), device=dev) * 2 - 1
+    rec = torch.cat([torch.rand((65536, 9), device=dev) * 2 - 1, torch.nn.functional.normalize(
+        torch.randn((65536, 3), device=dev), dim=1), torch.rand((65536, 1), device=dev)], 1).contiguous()
+    g.eval(x, stream=st)
+    g.train_step(rec, apply=True, stream=st)
+    e0.record(stream)
+    for _ in range(5):
+        g.eval(x, stream=st)
+    e1.record(stream)
+    stream.synchronize()
+    eval_s = e0.elapsed_time(e1) * 1e-3 / 5
+    t0 = time.perf_counter()
+    for _ in range(5):
+        g.train_step(rec, apply=True, stream=st)
+    train_s = (time.perf_counter() - t0) / 5
+    flop_fwd = 2 * (225 * 64 + 4 * 64 * 64 + 64 * 40)
+    peaks = load_peaks()
+    out = {"workload": f"slit room {res}x{res}, 200k box triangles, GGX floor, 6500 K light through a 0.2x2 slit; "
+                       f"MLP 9 -> 225 (12 frequencies) -> 5x64 -> 8 vMF lobes, bf16",
+           "reference_spp": ref_spp, "reference_seconds": ref_s,
+           "plain": {"spp": plain_spp, "seconds": plain_s, "mse": plain_mse,
+                     "samples_per_s": plain_spp * res * res / plain_s,
+                     "segments_per_sample": plain_stats["segments"] / max(plain_stats["paths"], 1)},
+           "guided": {"seconds_to_plain_mse": t_hit, "spp_at_crossing": spp if t_hit else None,
+                      "training_chunks": 8, "chunk_spp": chunk, "adam_steps": gstats["steps"],
+                      "curve_t_spp_mse": curve[:: max(1, len(curve) // 24)]},
+           "time_ratio_guided_over_plain": (t_hit / plain_s) if t_hit else None,
+           "network": {"inference_queries_per_s": (1 << 20) / eval_s,
+                       "inference_tflops": flop_fwd * (1 << 20) / eval_s / 1e12,
+                       "train_step_ms_65536": train_s * 1e3,
+                       "train_tflops": 3 * flop_fwd * 65536 / train_s / 1e12,
+                       "peak_bf16_tflops": peaks["bf16_tflops"],
+                       "inference_frac_of_peak": flop_fwd * (1 << 20) / eval_s / 1e12 / peaks["bf16_tflops"]},
+           "note": "MSE over XYZ against the plain reference, reference variance subtracted; guided time includes "
+                   "online training (8 chunks x 4 Adam steps x 65,536 records)"}
+    if cpu:
+        import oracle
+        rs = oracle.RenderScene(flat)
+        cres = 256
+        d = R.render_desc(cam, cres, cres, 16, tracer, seed=3)
+        cfilm = np.zeros((cres, cres, 8), np.float32)
+        rows, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < 8.0 and rows < cres:
+            rs.render(d, cfilm, pixels=(rows * cres, (rows + 4) * cres))
+            rows += 4
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": rows * cres * 16 / dt, "unit": "samples/s", "cores": oracle.hardware_threads(),
+                               "kind": "port", "sample": f"plain path tracing, {rows} rows of a {cres}^2 16-spp "
+                                                         f"render of the slit room, {dt:.1f} s"}
+    g.close()
+    gs.close()
+    return out
+
+
 def camera_queries(flat, cam, width, height):
     """Gather points of the photon workload: the first hits of the camera's pixel-centre rays on
     surfaces with a diffuse (Lambert) BSDF, with their normals flipped toward the camera."""
@@ -411,7 +540,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-workloads", action="store_true", help="only the traversal workload")
     ap.add_argument("--batch-scenes", type=int, default=64, help="scenes in the batched-rendering workload")
-    ap.add_argument("--only", default="", help="comma list of workloads to run (cornell,photon,batch); default all")
+    ap.add_argument("--only", default="", help="comma list of workloads to run (cornell,photon,batch,guided); default all")
+    ap.add_argument("--guided-res", type=int, default=1024, help="image side of the guiding workload")
+    ap.add_argument("--guided-ref-spp", type=int, default=4096, help="samples per pixel of its plain reference")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world, rank, local = dist_setup()
@@ -546,6 +677,8 @@ def main():
             line["cornell"] = cornell_bench(ctx, stream, args, world, dist, local, cpu=cpu_leg)
         if not only or "photon" in only:
             line["photon"] = photon_bench(ctx, stream, args, world, dist, local, cpu=cpu_leg)
+        if not only or "guided" in only:
+            line["guided"] = guided_bench(ctx, stream, args, world, dist, local, cpu=cpu_leg)
         if not only or "batch" in only:
             line["batch"] = batch_bench(ctx, stream, args, world, dist, local, cpu=cpu_leg, n_scenes=args.batch_scenes)
     ctx.close()

@@ -258,6 +258,57 @@ int liar_gpu_batch_launch(liar_gpu_ctx* ctx, liar_gpu_batch* batch, void* stream
 int liar_gpu_batch_stats(const liar_gpu_batch* batch, unsigned long long* out4);
 void liar_gpu_batch_destroy(liar_gpu_batch* batch);
 
+/* ---- learned path guiding (no reference counterpart: the reference's AdjointPhotonTracer samples
+ * the BSDF and the lights only, src/liar/tracers/adjoint_photon_tracer.cpp:212-292)
+ * A small MLP maps (position, shading normal, direction to the previous vertex) to a mixture of 8
+ * von Mises-Fisher lobes over outgoing directions. Network: the 9 inputs (position normalised to
+ * the config's box) -> sin/cos(pi 2^(f/2) x) for f = 0..11 plus the raw inputs (225 features) ->
+ * 5 ReLU layers of 64 -> 40 outputs; bf16 weights, f32 accumulation, no biases. Trained online with
+ * Adam on the renderer's own samples (KL divergence of the guide from the sampled integrand). */
+typedef struct liar_gpu_guide liar_gpu_guide;
+typedef struct liar_guide_config {
+    float bounds_lo[3], bounds_hi[3]; /* position normalisation box (the scene's bounds) */
+    float learning_rate;              /* Adam step size, 0 = 5e-3 */
+    float guide_probability;          /* chance of sampling the guide at a diffuse/glossy vertex, [0, 1) */
+    int32_t batch_records;            /* training records per Adam step, 0 = 65536 */
+    int32_t steps_per_pass;           /* Adam steps after each rendered pass when training, 0 = 4 */
+    uint64_t seed;                    /* weight initialisation */
+} liar_guide_config;
+int liar_gpu_guide_create(liar_gpu_ctx* ctx, const liar_guide_config* cfg, liar_gpu_guide** out);
+void liar_gpu_guide_destroy(liar_gpu_guide* guide);
+/* number of f32 parameters: W0 256x64, W1..W4 64x64, W5 64x48, row-major [in][out], concatenated
+ * (rows 225..255 of W0 and columns 40..47 of W5 are padding and stay zero) */
+size_t liar_gpu_guide_param_count(void);
+int liar_gpu_guide_get_params(liar_gpu_ctx* ctx, const liar_gpu_guide* guide, float* host, size_t n);
+/* replaces the weights and resets the optimiser state */
+int liar_gpu_guide_set_params(liar_gpu_ctx* ctx, liar_gpu_guide* guide, const float* host, size_t n);
+/* d_inputs: n x 9 floats (position, normal, direction); d_mixture: n x 40 floats = 8 lobes x
+ * (mean x, y, z, concentration) then the 8 lobe weights */
+int liar_gpu_guide_eval_device(liar_gpu_ctx* ctx, const liar_gpu_guide* guide, const float* d_inputs, size_t n,
+                               float* d_mixture, void* stream);
+/* One training step on n records of 13 floats: position, normal, direction to the previous vertex,
+ * sampled direction, weight (integrand / sampling density, >= 0). apply = 0 computes the gradient
+ * only. d_grad (optional) receives the gradient (param_count floats), d_loss (optional) the loss. */
+int liar_gpu_guide_train_device(liar_gpu_ctx* ctx, liar_gpu_guide* guide, const float* d_records, size_t n, int apply,
+                                float* d_grad, float* d_loss, void* stream);
+/* draws one direction per mixture (d_mixture n x 40 as above) from uniforms d_u (n x 3: lobe
+ * choice, cosine, azimuth) -> d_dirs (n x 3), d_pdf (n): the mixture density there */
+int liar_gpu_guide_sample_device(liar_gpu_ctx* ctx, const float* d_mixture, const float* d_u, size_t n, float* d_dirs,
+                                 float* d_pdf, void* stream);
+/* [0] Adam steps taken, [1] training records produced by guided renders, [2] guided vertices,
+ * [3] passes rendered */
+int liar_gpu_guide_stats(const liar_gpu_guide* guide, unsigned long long* out4);
+/* The AdjointPhotonTracer estimator with the guide as a third sampling technique: at a diffuse or
+ * glossy vertex the directional strategy draws from the guide with probability guide_probability,
+ * else from the BSDF (one-sample MIS of the mixed density against light sampling). Renders the
+ * desc's spp as passes of one sample per pixel; with train != 0 every pass records (vertex,
+ * direction, integrand / density) and takes steps_per_pass Adam steps before the next pass. */
+int liar_gpu_render_guided_device(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, liar_gpu_guide* guide,
+                                  const liar_render_desc* desc, int train, float* d_film, void* stream);
+/* statistics of the last guided render on ctx: [0] paths, [1] path segments, [2] segments that
+ * hit, [3] directions drawn from the guide */
+int liar_gpu_render_guided_stats(const liar_gpu_ctx* ctx, unsigned long long* out4);
+
 /* ---- photon maps -------------------------------------------------------------------------------
  * Replace the Lass KdTree<Photon> of PhotonMapper::buildPhotonMap (src/liar/tracers/photon_mapper.cpp:798-835)
  * and its rangeSearch(point, maxRadius, maxCount) (photon_mapper.cpp:1097,1257,1312,1352): for each

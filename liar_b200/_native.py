@@ -100,6 +100,18 @@ SIGNATURES: dict[str, tuple] = {
     "liar_gpu_batch_launch": (C.c_int, [_vp, _vp, _vp]),
     "liar_gpu_batch_stats": (C.c_int, [_vp, _vp]),
     "liar_gpu_batch_destroy": (None, [_vp]),
+    # learned path guiding (liar_b200/guiding.py)
+    "liar_gpu_guide_create": (C.c_int, [_vp, _vp, C.POINTER(_vp)]),
+    "liar_gpu_guide_destroy": (None, [_vp]),
+    "liar_gpu_guide_param_count": (_sz, []),
+    "liar_gpu_guide_get_params": (C.c_int, [_vp, _vp, _vp, _sz]),
+    "liar_gpu_guide_set_params": (C.c_int, [_vp, _vp, _vp, _sz]),
+    "liar_gpu_guide_eval_device": (C.c_int, [_vp, _vp, _vp, _sz, _vp, _vp]),
+    "liar_gpu_guide_train_device": (C.c_int, [_vp, _vp, _vp, _sz, C.c_int, _vp, _vp, _vp]),
+    "liar_gpu_guide_sample_device": (C.c_int, [_vp, _vp, _vp, _sz, _vp, _vp, _vp]),
+    "liar_gpu_guide_stats": (C.c_int, [_vp, _vp]),
+    "liar_gpu_render_guided_device": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, _vp, _vp]),
+    "liar_gpu_render_guided_stats": (C.c_int, [_vp, _vp]),
 }
 
 

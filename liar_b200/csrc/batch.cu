@@ -179,29 +179,9 @@ __global__ void __launch_bounds__(256) k_b_raygen(BParams P, BState<H> st, BQueu
             k.pixel = (uint32_t)(local / (uint64_t)it.spp);
             k.sample = (uint32_t)(local % (uint64_t)it.spp);
             k.spp = (uint32_t)it.spp;
-            const uint32_t px = k.pixel % (uint32_t)it.width, py = k.pixel / (uint32_t)it.width;
-            const float sx = ((float)px + sample_dim(k, DIM_SCREEN, true)) / (float)it.width;
-            const float sy = ((float)py + sample_dim(k, DIM_SCREEN + 1, true)) / (float)it.height;
             float lam[H], pdfsum;
             hero_wavelengths<H>(S, sample_dim(k, DIM_LAMBDA, true), lam, pdfsum);
-            const liar_camera& cam = it.cam;
-            float3 pos = mk(cam.position[0], cam.position[1], cam.position[2]);
-            float3 dir = mk(cam.direction[0], cam.direction[1], cam.direction[2]) +
-                         (sx - 0.5f) * mk(cam.right[0], cam.right[1], cam.right[2]) +
-                         (sy - 0.5f) * mk(cam.down[0], cam.down[1], cam.down[2]);
-            dir = normal(dir);
-            const float3 dn = mk(cam.direction_normal[0], cam.direction_normal[1], cam.direction_normal[2]);
-            float factor = 1.0f / dot(dir, dn);
-            if (cam.lens_radius > 0.0f && cam.focus_distance > 0.0f && cam.focus_distance < 3.4e38f) {
-                const float2 lens = concentric_disk(sample_dim(k, DIM_LENS, true), sample_dim(k, DIM_LENS + 1, true));
-                const float3 lp =
-                    pos + (cam.lens_radius * lens.x) * mk(cam.right_normal[0], cam.right_normal[1], cam.right_normal[2]) +
-                    (cam.lens_radius * lens.y) * mk(cam.down_normal[0], cam.down_normal[1], cam.down_normal[2]);
-                const float3 fp = pos + (factor * cam.focus_distance) * dir;
-                pos = lp;
-                dir = normal(fp - lp);
-                factor = 1.0f / dot(dir, dn);
-            }
+            r = camera_ray(it.cam, k, it.width, it.height);
             st.item[i] = ii;
             for (int h = 0; h < H; ++h) {
                 st.lam[(size_t)H * i + h] = lam[h];
@@ -211,8 +191,6 @@ __global__ void __launch_bounds__(256) k_b_raygen(BParams P, BState<H> st, BQueu
             st.pdfsum[i] = pdfsum;
             st.alpha[i] = 0.0f;
             st.gen[i] = 0;
-            r = liar_ray{pos.x, pos.y, pos.z, fmaxf(kTol, factor * cam.near_limit), dir.x, dir.y, dir.z,
-                         factor * cam.far_limit};
             sc = (uint32_t)it.scene;
             want = true;
         }

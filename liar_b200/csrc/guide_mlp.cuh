@@ -1,0 +1,313 @@
+// guide_mlp.cuh -- the path-guiding network on the tensor cores (no reference counterpart).
+//
+// Network: 9 inputs (position normalised to the scene box, shading normal, direction to the
+// previous vertex) -> frequency encoding (per input: sin and cos of pi * 2^(f/2) * x, f = 0..11, then
+// the 9 raw inputs; 225 features, padded to 256) -> 5 ReLU layers of 64 -> 48 outputs (40 used):
+// 8 von Mises-Fisher lobes, each (mean direction m 3, log concentration 1, logit 1). No biases.
+// Weights are bf16, accumulation f32 (mma.sync m16n8k16); activations stay in registers between
+// layers: the f32 accumulator fragment of two adjacent 8-column tiles is, element for element, the
+// A fragment of the next layer's 16-column k tile, so a layer costs no shared-memory round trip.
+//
+// Parameters (f32 master copy, row-major [in][out]): W0 256x64, W1..W4 64x64, W5 64x48.
+// For the kernels they are repacked as bf16 B fragments in lane order ("fwd": B = W_l,
+// "bwd": B = W_l^T for l = 1..5), one uint2 per lane per 16x8 tile, so a warp loads a tile
+// with one conflict-free 64-bit shared-memory access.
+#pragma once
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+namespace liar_gpu {
+namespace guide {
+
+constexpr int kIn = 9;
+constexpr int kFreq = 12;
+constexpr int kEncUsed = kIn * 2 * kFreq + kIn;  // 225
+constexpr int kEnc = 256;
+constexpr int kWidth = 64;
+constexpr int kOut = 48;
+constexpr int kOutUsed = 40;
+constexpr int kLobes = 8;
+constexpr int kLayers = 6;  // W0..W5
+
+__host__ __device__ constexpr int layer_k(int l) { return l == 0 ? kEnc : kWidth; }
+__host__ __device__ constexpr int layer_n(int l) { return l == 5 ? kOut : kWidth; }
+__host__ __device__ constexpr int param_offset(int l) {
+    return l == 0 ? 0 : (l <= 5 ? kEnc * kWidth + (l - 1) * kWidth * kWidth : kEnc * kWidth + 4 * kWidth * kWidth + kWidth * kOut);
+}
+constexpr int kParams = param_offset(6);  // 35840
+
+// fragment tile counts and offsets (in tiles of 32 uint2): W0 has 16 x 8 tiles, W1..W4 4 x 8, W5 4 x 6
+__host__ __device__ constexpr int fwd_tiles(int l) { return (layer_k(l) / 16) * (layer_n(l) / 8); }
+__host__ __device__ constexpr int fwd_tile_offset(int l) {
+    return l == 0 ? 0 : (l <= 5 ? 128 + 32 * (l - 1) : 128 + 32 * 4 + 24);
+}
+constexpr int kFwdTiles = fwd_tile_offset(6);  // 280
+// backward: B = W_l^T (k = out features of W_l, n = its 64 in features), l = 1..5: 4 x 8 tiles
+// for W1..W4, 3 x 8 for W5
+__host__ __device__ constexpr int bwd_tiles(int l) { return (layer_n(l) / 16) * (kWidth / 8); }
+__host__ __device__ constexpr int bwd_tile_offset(int l) { return l <= 5 ? 32 * (l - 1) : 32 * 4 + 24; }
+constexpr int kBwdTiles = bwd_tile_offset(6);  // 152
+static_assert(fwd_tile_offset(5) + fwd_tiles(5) == kFwdTiles, "forward fragment table");
+static_assert(bwd_tile_offset(5) + bwd_tiles(5) == kBwdTiles, "backward fragment table");
+constexpr size_t kFwdBytes = (size_t)kFwdTiles * 32 * 8;
+constexpr size_t kBwdBytes = (size_t)kBwdTiles * 32 * 8;
+
+#ifdef __CUDACC__
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+__device__ __forceinline__ float bf16_lo(uint32_t v) { return __uint_as_float(v << 16); }
+__device__ __forceinline__ float bf16_hi(uint32_t v) { return __uint_as_float(v & 0xffff0000u); }
+
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint2 b) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b.x), "r"(b.y));
+}
+
+// frequency f of the encoding: pi * 2^(f / 2), f = 0..11 (a half-octave ladder up to 45.25 pi:
+// features down to about a twentieth of the scene box, fine enough for radiance and coarse
+// enough to generalise from tens of thousands of training records)
+__device__ __forceinline__ float enc_scale(int f) {
+    const float s = (f & 1) ? 1.41421356237309515f : 1.0f;  // sqrt(2) rounded to float
+    return s * (float)(1 << (f >> 1));
+}
+
+// the encoded features (c, c + 1) of one input row, c even
+__device__ __forceinline__ void enc_pair(const float* x, int c, float& a, float& b) {
+    if (c < kIn * 2 * kFreq) {
+        const int d = c / (2 * kFreq), f = (c % (2 * kFreq)) >> 1;
+        sincospif(x[d] * enc_scale(f), &a, &b);
+    } else if (c < kEncUsed) {
+        a = x[c - kIn * 2 * kFreq];
+        b = c + 1 < kEncUsed ? x[c + 1 - kIn * 2 * kFreq] : 0.0f;
+    } else {
+        a = b = 0.0f;
+    }
+}
+
+// one warp, 32 rows = two m16 tiles. xr[mt][h]: the 9 inputs of row 16 mt + g + 8 h
+// (g = lane / 4). Returns the output-layer accumulators acc[mt][nt][4] (6 n tiles of 8).
+// If h_out is given, stores the bf16 activations h_1..h_5 at h_out[(l-1) * ld_layer + row * 64 + col]
+// for rows < n_rows (row relative to the warp's first row).
+struct ActStore {
+    __nv_bfloat16* base;  // null: no store
+    size_t ld_layer;      // elements between layers
+    uint32_t row0;        // first row of this warp in the store
+    uint32_t n_valid;     // rows of this warp that exist
+};
+
+__device__ __forceinline__ void store_frag_row(const ActStore& S, int layer, uint32_t row, int col, uint32_t v) {
+    if (S.base && row < S.n_valid)
+        *reinterpret_cast<uint32_t*>(S.base + (size_t)(layer - 1) * S.ld_layer + (size_t)(S.row0 + row) * kWidth + col) = v;
+}
+
+__device__ __forceinline__ void mlp_forward_warp(const float (&xr)[2][2][kIn], const uint2* __restrict__ wf,
+                                                 float (&out)[2][6][4], const ActStore& S) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    float acc[2][8][4];
+    uint32_t a[2][4][4];  // next layer's A fragments [mt][kk][reg]
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) acc[mt][nt][r] = 0.0f;
+    // layer 0: A fragments straight from the encoding
+#pragma unroll 1
+    for (int kk = 0; kk < kEnc / 16; ++kk) {
+        uint32_t a0[2][4];
+        const int c0 = 16 * kk + 2 * t, c1 = c0 + 8;
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+            float p, q;
+            enc_pair(xr[mt][0], c0, p, q);
+            a0[mt][0] = pack_bf16(p, q);
+            enc_pair(xr[mt][1], c0, p, q);
+            a0[mt][1] = pack_bf16(p, q);
+            enc_pair(xr[mt][0], c1, p, q);
+            a0[mt][2] = pack_bf16(p, q);
+            enc_pair(xr[mt][1], c1, p, q);
+            a0[mt][3] = pack_bf16(p, q);
+        }
+        const uint2* wt = wf + (size_t)(kk * 8) * 32 + lane;
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) {
+            const uint2 b = wt[nt * 32];
+            mma_bf16(acc[0][nt], a0[0], b);
+            mma_bf16(acc[1][nt], a0[1], b);
+        }
+    }
+    // hidden layers 1..4 and the output layer 5
+#pragma unroll 1
+    for (int l = 1; l <= 5; ++l) {
+        // ReLU, round to bf16, regroup as A fragments (and store h_l)
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) {
+                const float* e = acc[mt][2 * kk];
+                const float* o = acc[mt][2 * kk + 1];
+                a[mt][kk][0] = pack_bf16(fmaxf(e[0], 0.0f), fmaxf(e[1], 0.0f));
+                a[mt][kk][1] = pack_bf16(fmaxf(e[2], 0.0f), fmaxf(e[3], 0.0f));
+                a[mt][kk][2] = pack_bf16(fmaxf(o[0], 0.0f), fmaxf(o[1], 0.0f));
+                a[mt][kk][3] = pack_bf16(fmaxf(o[2], 0.0f), fmaxf(o[3], 0.0f));
+                if (S.base) {
+                    const uint32_t r0 = 16 * mt + g;
+                    store_frag_row(S, l, r0, 16 * kk + 2 * t, a[mt][kk][0]);
+                    store_frag_row(S, l, r0 + 8, 16 * kk + 2 * t, a[mt][kk][1]);
+                    store_frag_row(S, l, r0, 16 * kk + 8 + 2 * t, a[mt][kk][2]);
+                    store_frag_row(S, l, r0 + 8, 16 * kk + 8 + 2 * t, a[mt][kk][3]);
+                }
+            }
+        const int n_nt = l == 5 ? kOut / 8 : 8;
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt)
+#pragma unroll
+                for (int r = 0; r < 4; ++r) acc[mt][nt][r] = 0.0f;
+        const uint2* wl = wf + (size_t)fwd_tile_offset(l) * 32 + lane;
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk)
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt) {
+                if (nt < n_nt) {
+                    const uint2 b = wl[(kk * n_nt + nt) * 32];
+                    uint32_t (&a0)[4] = a[0][kk];
+                    uint32_t (&a1)[4] = a[1][kk];
+                    mma_bf16(acc[0][nt], a0, b);
+                    mma_bf16(acc[1][nt], a1, b);
+                }
+            }
+    }
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 6; ++nt)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) out[mt][nt][r] = acc[mt][nt][r];
+}
+
+// writes the warp's raw outputs to a per-warp [32][kOutStride] f32 scratch
+constexpr int kOutStride = kOut + 1;
+__device__ __forceinline__ void scatter_out(const float (&out)[2][6][4], float* s) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 6; ++nt) {
+            const int r = 16 * mt + g, c = 8 * nt + 2 * t;
+            s[r * kOutStride + c] = out[mt][nt][0];
+            s[r * kOutStride + c + 1] = out[mt][nt][1];
+            s[(r + 8) * kOutStride + c] = out[mt][nt][2];
+            s[(r + 8) * kOutStride + c + 1] = out[mt][nt][3];
+        }
+}
+
+#endif  // __CUDACC__
+
+// ---- the mixture (host and device)
+
+#ifdef __CUDACC__
+#define GM_HD __host__ __device__ __forceinline__
+#else
+#define GM_HD inline
+#endif
+
+// concentration exp(clamp(s)); the mean's gradient uses 1 / max(|m|, kMeanNormMin)
+constexpr float kLogKappaMin = -6.0f, kLogKappaMax = 7.0f, kMeanNormMin = 1e-3f;
+
+struct Lobe {
+    float mx, my, mz, kappa;
+};
+
+// raw outputs (40) -> lobes (unit mean, concentration) and weights (softmax)
+GM_HD void mixture_from_raw(const float* o, Lobe* lobes, float* w) {
+    float mx = -3.0e38f;
+    for (int l = 0; l < kLobes; ++l) mx = fmaxf(mx, o[5 * l + 4]);
+    float sum = 0.0f;
+    for (int l = 0; l < kLobes; ++l) {
+        const float x = o[5 * l], y = o[5 * l + 1], z = o[5 * l + 2];
+        const float n = sqrtf(x * x + y * y + z * z);
+        if (n > 0.0f) {
+            const float inv = 1.0f / n;
+            lobes[l].mx = x * inv;
+            lobes[l].my = y * inv;
+            lobes[l].mz = z * inv;
+        } else {
+            lobes[l].mx = lobes[l].my = 0.0f;
+            lobes[l].mz = 1.0f;
+        }
+        lobes[l].kappa = expf(fminf(fmaxf(o[5 * l + 3], kLogKappaMin), kLogKappaMax));
+        w[l] = expf(o[5 * l + 4] - mx);
+        sum += w[l];
+    }
+    for (int l = 0; l < kLobes; ++l) w[l] /= sum;
+}
+
+// log of the vMF density on the unit sphere: kappa / (2 pi (1 - e^{-2 kappa})) e^{kappa (mu.w - 1)}
+GM_HD float vmf_log_pdf(float kappa, float cos_t) {
+    return logf(kappa / (-expm1f(-2.0f * kappa))) - 1.8378770664093453f /* log 2 pi */ + kappa * (cos_t - 1.0f);
+}
+
+#ifdef __CUDACC__
+// ---- the mixture as stored by the network's inference: m[0..31] = 8 x (mu x, y, z, kappa),
+// m[32..39] = the 8 weights
+
+__device__ __forceinline__ float mixture_pdf(const float* m, float dx, float dy, float dz) {
+    float p = 0.0f;
+#pragma unroll
+    for (int l = 0; l < kLobes; ++l) {
+        const float c = m[4 * l] * dx + m[4 * l + 1] * dy + m[4 * l + 2] * dz;
+        p += m[32 + l] * expf(vmf_log_pdf(m[4 * l + 3], c));
+    }
+    return p;
+}
+
+// lobe by weight (u0), then the vMF's cosine by its inverse CDF, w = 1 + log(u1 + (1 - u1) e^{-2k}) / k
+// (Jakob 2012), azimuth 2 pi u2 in the frame of Duff et al. 2017 around the mean
+__device__ __forceinline__ void mixture_sample(const float* m, float u0, float u1, float u2, float& dx, float& dy,
+                                               float& dz) {
+    int lobe = kLobes - 1;
+    float acc = 0.0f;
+#pragma unroll
+    for (int l = 0; l < kLobes; ++l) {
+        acc += m[32 + l];
+        if (u0 < acc && lobe == kLobes - 1 && l < kLobes - 1) lobe = l;
+    }
+    // (the first l with u0 < acc; the last lobe takes the rounding remainder)
+    float mx = m[0], my = m[1], mz = m[2], k = m[3];
+#pragma unroll
+    for (int l = 1; l < kLobes; ++l)
+        if (l == lobe) {
+            mx = m[4 * l];
+            my = m[4 * l + 1];
+            mz = m[4 * l + 2];
+            k = m[4 * l + 3];
+        }
+    float w = 1.0f + logf(u1 + (1.0f - u1) * expf(-2.0f * k)) / k;
+    w = fminf(1.0f, fmaxf(-1.0f, w));
+    const float s = sqrtf(fmaxf(0.0f, 1.0f - w * w));
+    const float sign = copysignf(1.0f, mz);
+    const float a = -1.0f / (sign + mz);
+    const float b = mx * my * a;
+    const float tx = 1.0f + sign * mx * mx * a, ty = sign * b, tz = -sign * mx;
+    const float bx = b, by = sign + my * my * a, bz = -my;
+    float sp, cp;
+    sincospif(2.0f * u2, &sp, &cp);
+    dx = w * mx + s * (cp * tx + sp * bx);
+    dy = w * my + s * (cp * ty + sp * by);
+    dz = w * mz + s * (cp * tz + sp * bz);
+}
+#endif
+
+#undef GM_HD
+
+}  // namespace guide
+}  // namespace liar_gpu

@@ -1,0 +1,669 @@
+// guided.cu -- the AdjointPhotonTracer estimator with a learned guide as a third sampling
+// technique, trained online on its own samples (no reference counterpart; the estimator without
+// the guide is src/liar/tracers/adjoint_photon_tracer.cpp:84-292, as in render.cu).
+//
+// Per pass (one sample per pixel): raygen -> per bounce [trace, shade]; the shade kernel is one
+// warp per 32 queue entries: hit context per lane, then (when the guide is on and a lane of the
+// warp sits on a diffuse or glossy surface) the guide network for the 32 vertices on the tensor
+// cores, then the scattering decision per lane:
+//   directional strategy (probability s = 0.5 at diffuse/glossy vertices): guide with probability
+//   c, else BSDF; density p_d = c q + (1 - c) p_bsdf
+//   light strategy (probability 1 - s): as the reference
+// weighted by the power heuristic between s p_d and (1 - s) p_light (one-sample MIS). With c = 0
+// every float operation is the one of render.cu, so the images agree to rounding.
+// Training records (vertex, direction, integrand / density) are written per scattering event and
+// completed when the pass ends: weight = (L_end - L_at_vertex) * p_chosen / (w_mis T_vertex p_mix),
+// the sampled integrand f cos L_in over the density p_mix of the whole one-sample mixture.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <new>
+#include <vector>
+
+#include "../../include/liar_gpu.h"
+#include "ctx.h"
+#include "guide_mlp.cuh"
+#include "render_dev.cuh"
+
+using namespace liar_gpu;
+using namespace liar_gpu::rt;
+using namespace liar_gpu::guide;
+
+namespace liar_gpu {
+namespace rt {
+const DScene& scene_dscene(const liar_gpu_scene* s);
+const liar_gpu_mesh* scene_mesh(const liar_gpu_scene* s);
+int scene_device(const liar_gpu_scene* s);
+}  // namespace rt
+namespace guide {
+const uint2* guide_frag_fwd(const liar_gpu_guide* g);
+const liar_guide_config& guide_config(const liar_gpu_guide* g);
+int guide_device(const liar_gpu_guide* g);
+int guide_train(liar_gpu_ctx* ctx, liar_gpu_guide* g, const float* d_records, const uint32_t* d_count, size_t n_max,
+                int apply, float* d_grad_out, float* d_loss_out, cudaStream_t st);
+void guide_count(liar_gpu_guide* g, unsigned long long records, unsigned long long guided, unsigned long long passes);
+unsigned long long guide_steps(const liar_gpu_guide* g);
+}  // namespace guide
+}  // namespace liar_gpu
+
+namespace {
+
+constexpr int kRawRecord = 15;  // position 3, normal 3, direction to the previous vertex 3, sampled direction 3,
+                                // path slot, radiance before, scale
+constexpr int kTrainRecord = 13;
+constexpr uint32_t kDimGuide = 0x100000u;  // per generation g: kDimGuide + 4 g + {choice, lobe, cosine, azimuth}
+
+struct GPaths {
+    float* lam;
+    float* lam_pdf;
+    float* T;
+    float* L;
+    float* alpha;
+    int32_t* gen;
+};
+
+struct GQueue {
+    liar_ray* rays;
+    uint32_t* path;
+    uint32_t* count;
+};
+
+struct GParams {
+    liar_camera cam;
+    int width, height, spp, max_gen, max_depth;
+    uint64_t seed;
+    uint32_t sample;        // the pass: sample index of every pixel
+    float guide_prob;       // c (0: guide off)
+    int train;
+    float box_lo[3], box_inv[3];
+    float* records;         // raw records
+    uint32_t* rec_count;
+    uint32_t rec_cap;
+    unsigned long long* stats;  // [0] paths [1] segments [2] hits [3] guided vertices
+};
+
+__device__ __forceinline__ SampleKey gkey(const GParams& W, uint32_t pixel) {
+    SampleKey k;
+    k.seed = W.seed;
+    k.pixel = pixel;
+    k.sample = W.sample;
+    k.spp = (uint32_t)W.spp;
+    return k;
+}
+
+__device__ __forceinline__ void gqueue_push(const GQueue& q, bool want, const liar_ray& r, uint32_t path) {
+    const uint32_t mask = __ballot_sync(0xffffffffu, want);
+    if (mask == 0) return;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(q.count, (uint32_t)__popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (want) {
+        const uint32_t slot = base + __popc(mask & ((1u << lane) - 1u));
+        float4* dst = reinterpret_cast<float4*>(q.rays + slot);
+        dst[0] = make_float4(r.ox, r.oy, r.oz, r.tmin);
+        dst[1] = make_float4(r.dx, r.dy, r.dz, r.tmax);
+        q.path[slot] = path;
+    }
+}
+
+__device__ void gsplat(const DScene& S, float* film, uint32_t pixel, float lam, float lam_pdf, float L, float alpha) {
+    float3 xyz = mk(0, 0, 0);
+    if (lam_pdf > 0.0f) {
+        const float s = L / lam_pdf;
+        const float3 c = observer_sensitivity(S, lam);
+        xyz = mk(s * c.x, s * c.y, s * c.z);
+    }
+    float* f = film + 8 * (size_t)pixel;
+    atomicAdd(f + 0, xyz.x);
+    atomicAdd(f + 1, xyz.y);
+    atomicAdd(f + 2, xyz.z);
+    atomicAdd(f + 3, alpha);
+    atomicAdd(f + 4, xyz.x * xyz.x);
+    atomicAdd(f + 5, xyz.y * xyz.y);
+    atomicAdd(f + 6, xyz.z * xyz.z);
+    atomicAdd(f + 7, 1.0f);
+}
+
+__global__ void __launch_bounds__(256) k_g_raygen(DScene S, GParams W, GPaths P, GQueue out, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool want = false;
+    liar_ray r{};
+    if (i < n) {
+        const SampleKey k = gkey(W, i);
+        float lpdf;
+        const float lam = observer_sample(S, sample_dim(k, DIM_LAMBDA, true), lpdf);
+        r = camera_ray(W.cam, k, W.width, W.height);
+        P.lam[i] = lam;
+        P.lam_pdf[i] = lpdf;
+        P.T[i] = 1.0f;
+        P.L[i] = 0.0f;
+        P.alpha[i] = 0.0f;
+        P.gen[i] = 0;
+        want = true;
+    }
+    gqueue_push(out, want, r, i);
+}
+
+constexpr int kShadeThreads = 128;
+constexpr size_t kShadeSmem = kFwdBytes + 4 * (32 * kIn + 32 * kOutStride) * sizeof(float);
+
+__global__ void __launch_bounds__(kShadeThreads) k_g_shade(DScene S, GParams W, GPaths P, GQueue in,
+                                                           const liar_hit* __restrict__ hits, uint32_t n_in, GQueue out,
+                                                           float* film, const uint2* __restrict__ frag) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint2* wf = reinterpret_cast<uint2*>(smem);
+    const bool guide_on = W.guide_prob > 0.0f;
+    if (guide_on) {
+        const uint4* s = reinterpret_cast<const uint4*>(frag);
+        uint4* d = reinterpret_cast<uint4*>(wf);
+        for (size_t i = threadIdx.x; i < kFwdBytes / 16; i += blockDim.x) d[i] = s[i];
+        __syncthreads();
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float* xs = reinterpret_cast<float*>(smem + kFwdBytes) + warp * (32 * kIn + 32 * kOutStride);
+    float* os = xs + 32 * kIn;
+    const uint32_t n_tiles = (n_in + 31) / 32;
+    unsigned long long segs = 0, n_hit = 0, n_guided = 0;
+    for (uint32_t tile = blockIdx.x * 4 + warp; tile < n_tiles; tile += gridDim.x * 4) {
+        const uint32_t q = tile * 32 + lane;
+        const bool valid = q < n_in;
+        uint32_t p = 0;
+        float4 r0 = make_float4(0, 0, 0, 0), r1 = make_float4(0, 0, 1, 0);
+        liar_hit h{-1, 0.0f};
+        HitContext HC;
+        HC.mat = -1;
+        HC.light = -1;
+        bool surface = false, guidable = false;
+        liar_material M{};
+        if (valid) {
+            p = in.path[q];
+            r0 = reinterpret_cast<const float4*>(in.rays + q)[0];
+            r1 = reinterpret_cast<const float4*>(in.rays + q)[1];
+            h = hits[q];
+            if (h.prim >= 0) {
+                HC = hit_context(S, mk(r0.x, r0.y, r0.z), mk(r1.x, r1.y, r1.z), (uint32_t)h.prim);
+                surface = HC.mat >= 0 && S.mats[HC.mat].type != LIAR_MAT_NONE;
+                if (surface) {
+                    M = S.mats[HC.mat];
+                    guidable = M.type == LIAR_MAT_LAMBERT || M.type == LIAR_MAT_COOK_TORRANCE ||
+                               M.type == LIAR_MAT_WALTER;
+                }
+            }
+        }
+        // ---- the guide network for the warp's vertices
+        float mix[kOutUsed];
+        const bool run_net = guide_on && __any_sync(0xffffffffu, guidable);
+        if (run_net) {
+            float x[kIn];
+            if (guidable) {
+                x[0] = (HC.target.x - W.box_lo[0]) * W.box_inv[0];
+                x[1] = (HC.target.y - W.box_lo[1]) * W.box_inv[1];
+                x[2] = (HC.target.z - W.box_lo[2]) * W.box_inv[2];
+                x[3] = HC.N.x;
+                x[4] = HC.N.y;
+                x[5] = HC.N.z;
+                x[6] = -r1.x;
+                x[7] = -r1.y;
+                x[8] = -r1.z;
+            } else {
+                for (int c = 0; c < kIn; ++c) x[c] = 0.0f;
+            }
+            for (int c = 0; c < kIn; ++c) xs[lane * kIn + c] = x[c];
+            __syncwarp();
+            float xr[2][2][kIn];
+            const int g = lane >> 2;
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+                for (int hh = 0; hh < 2; ++hh)
+#pragma unroll
+                    for (int c = 0; c < kIn; ++c) xr[mt][hh][c] = xs[(16 * mt + g + 8 * hh) * kIn + c];
+            float o[2][6][4];
+            mlp_forward_warp(xr, wf, o, ActStore{nullptr, 0, 0, 0});
+            scatter_out(o, os);
+            __syncwarp();
+            if (guidable) {
+                Lobe lobes[kLobes];
+                float w[kLobes];
+                mixture_from_raw(os + lane * kOutStride, lobes, w);
+#pragma unroll
+                for (int l = 0; l < kLobes; ++l) {
+                    mix[4 * l] = lobes[l].mx;
+                    mix[4 * l + 1] = lobes[l].my;
+                    mix[4 * l + 2] = lobes[l].mz;
+                    mix[4 * l + 3] = lobes[l].kappa;
+                    mix[32 + l] = w[l];
+                }
+            }
+            __syncwarp();
+        }
+        // ---- shading (render.cu's k_shade with the guide as a third technique)
+        bool want = false;
+        liar_ray nr{};
+        bool rec_want = false;
+        float rec[kRawRecord];
+        if (valid) {
+            ++segs;
+            const float3 o = mk(r0.x, r0.y, r0.z), d = mk(r1.x, r1.y, r1.z);
+            const SampleKey key = gkey(W, p);
+            const int gen = P.gen[p];
+            float T = P.T[p], L = P.L[p];
+            const float lam = P.lam[p];
+            bool alive = false;
+            float3 next_o = mk(0, 0, 0), next_d = mk(0, 0, 1);
+            float next_tmin = kTol, next_tmax = INFINITY;
+            if (h.prim < 0) {
+                if (S.sky_light >= 0 && S.sky_distance > r0.w * (1.0f + kTol) && S.sky_distance < r1.w * (1.0f - kTol)) {
+                    if (gen == 0) P.alpha[p] = 1.0f;
+                    if (gen > 0) L += T * spec_eval(S, S.lights[S.sky_light].spectrum, lam, false);
+                }
+            } else {
+                ++n_hit;
+                if (gen == 0) P.alpha[p] = 1.0f;
+                const int light = HC.light, mi = HC.mat;
+                const float3 target = HC.target, ng = HC.ng, N = HC.N, u = HC.u, v = HC.v;
+                if (gen > 0 && light >= 0) L += T * spec_eval(S, S.lights[light].spectrum, lam, false);
+                if (!surface) {
+                    if (mi >= 0 && light < 0 && S.mats[mi].emission >= 0) L += T * spec_eval(S, S.mats[mi].emission, lam, false);
+                    alive = true;
+                    next_o = o;
+                    next_d = d;
+                    next_tmin = h.t + kTol;
+                    next_tmax = r1.w;
+                } else {
+                    if (light < 0 && M.emission >= 0) L += T * spec_eval(S, M.emission, lam, false);
+                    const Bsdf B = make_bsdf(S, M, HC, lam);
+                    const float3 md = -d;
+                    float3 wi = mk(dot(md, u), dot(md, v), dot(md, N));
+                    wi.z = fmaxf(wi.z, kEps);
+                    const bool strat = gen < W.max_gen;
+                    const uint32_t base = DIM_GEN0 + DIMS_PER_GEN * (uint32_t)gen;
+                    const float strategy_pdf =
+                        (has_caps(B.caps, CAP_DIFF) || has_caps(B.caps, CAP_GLOSSY)) ? 0.5f : 1.0f;
+                    const float c = (guide_on && guidable && strategy_pdf < 1.0f) ? W.guide_prob : 0.0f;
+                    const uint32_t gbase = kDimGuide + 4u * (uint32_t)gen;
+                    float3 wo = mk(0, 0, 1);
+                    float3 wd = mk(0, 0, 1);
+                    float value = 0.0f, pdf_s = 0.0f, w_mis = 0.0f, p_mix = 0.0f;
+                    bool ok = false;
+                    if (sample_dim(key, base + OFF_STRATEGY, strat) < strategy_pdf) {
+                        float p_dir = 0.0f;
+                        if (c > 0.0f && sample_dim(key, gbase, false) < c) {
+                            // the guide
+                            ++n_guided;
+                            float gx, gy, gz;
+                            mixture_sample(mix, sample_dim(key, gbase + 1, false), sample_dim(key, gbase + 2, false),
+                                           sample_dim(key, gbase + 3, false), gx, gy, gz);
+                            wd = mk(gx, gy, gz);
+                            wo = mk(dot(wd, u), dot(wd, v), dot(wd, N));
+                            const BsdfOut be = bsdf_evaluate(B, wi, wo, CAP_ALL);
+                            p_dir = c * mixture_pdf(mix, gx, gy, gz) + (1.0f - c) * be.pdf;
+                            value = be.value;
+                            ok = p_dir > 0.0f && value != 0.0f;
+                        } else {
+                            const BsdfSample bs = bsdf_sample(B, wi, sample_dim(key, base + OFF_BSDF, strat),
+                                                              sample_dim(key, base + OFF_BSDF + 1, strat),
+                                                              sample_dim(key, base + OFF_COMPONENT, strat), CAP_ALL);
+                            if (bs.ok()) {
+                                wo = bs.wo;
+                                wd = bs.wo.x * u + bs.wo.y * v + bs.wo.z * N;
+                                const float qd = c > 0.0f ? mixture_pdf(mix, wd.x, wd.y, wd.z) : 0.0f;
+                                p_dir = c > 0.0f ? c * qd + (1.0f - c) * bs.pdf : bs.pdf;
+                                value = bs.value;
+                                ok = true;
+                            }
+                        }
+                        if (ok) {
+                            pdf_s = p_dir * strategy_pdf;
+                            float pl = 0.0f;
+                            for (int l = 0; l < S.n_lights; ++l) {
+                                const LightEmission e = light_emission(S, l, target, wd, lam);
+                                if (e.pdf > 0.0f) pl += light_choice_pdf(S, l) * e.pdf;
+                            }
+                            pl *= (1.0f - strategy_pdf);
+                            w_mis = power_heuristic(pdf_s, pl);
+                            value *= w_mis;
+                            ok = pdf_s > 0.0f && value != 0.0f;
+                            p_mix = pdf_s + pl;
+                        }
+                    } else if (S.n_lights > 0) {
+                        const float uc = sample_dim(key, base + OFF_LIGHT_CHOICE, strat);
+                        int k = lower_bound_f(S.light_cdf, S.n_lights, uc);
+                        if (k > S.n_lights - 1) k = S.n_lights - 1;
+                        const float pc = light_choice_pdf(S, k);
+                        if (pc > 0.0f) {
+                            const LightSample ls = light_sample(S, k, target, sample_dim(key, base + OFF_LIGHT, strat),
+                                                                sample_dim(key, base + OFF_LIGHT + 1, strat), lam);
+                            if (ls.pdf > 0.0f) {
+                                float pdf = pc * ls.pdf;
+                                for (int l = 0; l < S.n_lights; ++l) {
+                                    if (l == k) continue;
+                                    const LightEmission e = light_emission(S, l, target, ls.dir, lam);
+                                    if (e.pdf > 0.0f) pdf += light_choice_pdf(S, l) * e.pdf;
+                                }
+                                pdf *= (1.0f - strategy_pdf);
+                                const float3 lwo = mk(dot(ls.dir, u), dot(ls.dir, v), dot(ls.dir, N));
+                                const BsdfOut be = bsdf_evaluate(B, wi, lwo, CAP_ALL);
+                                if (be.pdf > 0.0f && be.value != 0.0f) {
+                                    const float p_dir =
+                                        c > 0.0f ? c * mixture_pdf(mix, ls.dir.x, ls.dir.y, ls.dir.z) + (1.0f - c) * be.pdf
+                                                 : be.pdf;
+                                    wo = lwo;
+                                    wd = ls.dir;
+                                    w_mis = power_heuristic(pdf, p_dir * strategy_pdf);
+                                    value = be.value * w_mis;
+                                    pdf_s = pdf;
+                                    ok = pdf_s > 0.0f && value != 0.0f;
+                                    p_mix = pdf + p_dir * strategy_pdf;
+                                }
+                            }
+                        }
+                    }
+                    if (ok) {
+                        const float cos_t = wo.z;
+                        next_o = target + ((cos_t > 0.0f ? 10.0f : -10.0f) * kTol) * ng;
+                        next_d = wo.x * u + wo.y * v + wo.z * N;
+                        next_tmin = kTol;
+                        next_tmax = INFINITY;
+                        if (W.train && guidable && strategy_pdf < 1.0f && T > 0.0f && w_mis > 0.0f && p_mix > 0.0f) {
+                            rec_want = true;
+                            rec[0] = target.x;
+                            rec[1] = target.y;
+                            rec[2] = target.z;
+                            rec[3] = N.x;
+                            rec[4] = N.y;
+                            rec[5] = N.z;
+                            rec[6] = -d.x;
+                            rec[7] = -d.y;
+                            rec[8] = -d.z;
+                            rec[9] = wd.x;
+                            rec[10] = wd.y;
+                            rec[11] = wd.z;
+                            rec[12] = __uint_as_float(p);
+                            rec[13] = L;
+                            rec[14] = pdf_s / (w_mis * T * p_mix);
+                        }
+                        T *= value * (fabsf(cos_t) / pdf_s);
+                        alive = true;
+                    }
+                }
+            }
+            if (alive) {
+                const int ng1 = gen + 1;
+                if (W.max_depth > 0 && ng1 >= W.max_depth) {
+                    alive = false;
+                } else if (ng1 >= W.max_gen) {
+                    const float ur = sample_dim(key, DIM_GEN0 + DIMS_PER_GEN * (uint32_t)ng1 + OFF_RR, false);
+                    if (ur < 0.5f) T /= 0.5f;
+                    else alive = false;
+                }
+            }
+            if (alive) {
+                P.T[p] = T;
+                P.L[p] = L;
+                P.gen[p] = gen + 1;
+                nr = liar_ray{next_o.x, next_o.y, next_o.z, next_tmin, next_d.x, next_d.y, next_d.z, next_tmax};
+                want = true;
+            } else {
+                P.L[p] = L;  // the radiance at the end of the path completes its training records
+                gsplat(S, film, p, lam, P.lam_pdf[p], L, P.alpha[p]);
+            }
+        }
+        gqueue_push(out, want, nr, p);
+        // training records, one atomic per warp
+        const uint32_t rmask = __ballot_sync(0xffffffffu, rec_want);
+        if (rmask) {
+            const uint32_t leader = __ffs(rmask) - 1;
+            uint32_t rb = 0;
+            if ((uint32_t)lane == leader) rb = atomicAdd(W.rec_count, (uint32_t)__popc(rmask));
+            rb = __shfl_sync(0xffffffffu, rb, leader);
+            if (rec_want) {
+                const uint32_t slot = rb + __popc(rmask & ((1u << lane) - 1u));
+                if (slot < W.rec_cap) {
+                    float* dst = W.records + (size_t)slot * kRawRecord;
+                    for (int c = 0; c < kRawRecord; ++c) dst[c] = rec[c];
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        segs += __shfl_down_sync(0xffffffffu, segs, o);
+        n_hit += __shfl_down_sync(0xffffffffu, n_hit, o);
+        n_guided += __shfl_down_sync(0xffffffffu, n_guided, o);
+    }
+    if (lane == 0 && segs) {
+        atomicAdd(W.stats + 1, segs);
+        atomicAdd(W.stats + 2, n_hit);
+        if (n_guided) atomicAdd(W.stats + 3, n_guided);
+    }
+}
+
+// completes the pass's records: weight = (L_end - L_vertex) * scale; keeps the positive ones
+__global__ void k_g_finalize(const float* __restrict__ raw, const uint32_t* __restrict__ raw_count, uint32_t raw_cap,
+                             const float* __restrict__ L_end, float* __restrict__ train, uint32_t* train_count,
+                             uint32_t train_cap) {
+    const uint32_t n = min(*raw_count, raw_cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float* r = raw + (size_t)i * kRawRecord;
+        const uint32_t p = __float_as_uint(r[12]);
+        const float w = (L_end[p] - r[13]) * r[14];
+        if (w > 0.0f && isfinite(w)) {
+            const uint32_t slot = atomicAdd(train_count, 1u);
+            if (slot < train_cap) {
+                float* d = train + (size_t)slot * kTrainRecord;
+                for (int c = 0; c < 12; ++c) d[c] = r[c];
+                d[12] = w;
+            }
+        }
+    }
+}
+
+struct GuidedBuffers {
+    size_t cap = 0;       // paths per wave
+    size_t rec_cap = 0;   // raw records per pass
+    void* mem = nullptr;
+    GPaths P{};
+    GQueue q[2]{};
+    liar_hit* hits = nullptr;
+    float* raw = nullptr;
+    float* train = nullptr;
+    uint32_t* counters = nullptr;            // [0] raw records [1] training records
+    unsigned long long* stats = nullptr;     // [0..3]
+    uint32_t* h_count = nullptr;             // pinned, 4 words
+};
+
+GuidedBuffers* guided_buffers(liar_gpu_ctx* ctx) {
+    for (auto& ext : ctx->extensions)
+        if (ext.first == "guided") return static_cast<GuidedBuffers*>(ext.second);
+    GuidedBuffers* gb = new GuidedBuffers();
+    ctx->extensions.emplace_back("guided", gb);
+    ctx->on_destroy.push_back([gb]() {
+        if (gb->mem) cudaFree(gb->mem);
+        if (gb->h_count) cudaFreeHost(gb->h_count);
+        delete gb;
+    });
+    return gb;
+}
+
+int ensure_guided_buffers(liar_gpu_ctx* ctx, GuidedBuffers* gb, size_t n, size_t rec_cap) {
+    if (!gb->h_count) {
+        cudaError_t e = cudaMallocHost((void**)&gb->h_count, 4 * sizeof(uint32_t));
+        if (e != cudaSuccess) return ctx_cuda(ctx, e, "guided render host buffers");
+    }
+    if (gb->cap >= n && gb->rec_cap >= rec_cap) return LIAR_OK;
+    if (gb->mem) cudaFree(gb->mem);
+    gb->mem = nullptr;
+    gb->cap = gb->rec_cap = 0;
+    const size_t bytes = n * (6 * 4 + 2 * (32 + 4) + 8) + rec_cap * (kRawRecord + kTrainRecord) * 4 + 4096;
+    cudaError_t e = cudaMalloc(&gb->mem, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return ctx_cuda(ctx, e, "guided render buffers");
+    }
+    char* p = static_cast<char*>(gb->mem);
+    auto take = [&](size_t b) {
+        char* r = p;
+        p += (b + 255) & ~size_t(255);
+        return r;
+    };
+    gb->q[0].rays = reinterpret_cast<liar_ray*>(take(n * 32));
+    gb->q[1].rays = reinterpret_cast<liar_ray*>(take(n * 32));
+    gb->hits = reinterpret_cast<liar_hit*>(take(n * 8));
+    gb->q[0].path = reinterpret_cast<uint32_t*>(take(n * 4));
+    gb->q[1].path = reinterpret_cast<uint32_t*>(take(n * 4));
+    gb->P.lam = reinterpret_cast<float*>(take(n * 4));
+    gb->P.lam_pdf = reinterpret_cast<float*>(take(n * 4));
+    gb->P.T = reinterpret_cast<float*>(take(n * 4));
+    gb->P.L = reinterpret_cast<float*>(take(n * 4));
+    gb->P.alpha = reinterpret_cast<float*>(take(n * 4));
+    gb->P.gen = reinterpret_cast<int32_t*>(take(n * 4));
+    gb->raw = reinterpret_cast<float*>(take(rec_cap * kRawRecord * 4));
+    gb->train = reinterpret_cast<float*>(take(rec_cap * kTrainRecord * 4));
+    gb->q[0].count = reinterpret_cast<uint32_t*>(take(4));
+    gb->q[1].count = reinterpret_cast<uint32_t*>(take(4));
+    gb->counters = reinterpret_cast<uint32_t*>(take(8));
+    gb->stats = reinterpret_cast<unsigned long long*>(take(4 * 8));
+    gb->cap = n;
+    gb->rec_cap = rec_cap;
+    return LIAR_OK;
+}
+
+int attrs_done_device = -1;
+
+}  // namespace
+
+extern "C" int liar_gpu_render_guided_device(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, liar_gpu_guide* guide,
+                                             const liar_render_desc* desc, int train, float* d_film, void* stream) {
+    if (!ctx) return LIAR_ERR_INVALID;
+    if (!scene || !guide || !desc || !d_film) return ctx_fail(ctx, LIAR_ERR_INVALID, "null scene, guide, description or film");
+    if (scene_device(scene) != ctx->device || guide_device(guide) != ctx->device)
+        return ctx_fail(ctx, LIAR_ERR_INVALID, "scene or guide lives on another device");
+    const liar_render_desc& R = *desc;
+    if (R.width <= 0 || R.height <= 0 || R.spp <= 0) return ctx_fail(ctx, LIAR_ERR_INVALID, "empty image or no samples");
+    if (R.max_ray_generation < 0) return ctx_fail(ctx, LIAR_ERR_INVALID, "max_ray_generation must be >= 0");
+    if (R.tracer != LIAR_TRACER_ADJOINT_PHOTON) return ctx_fail(ctx, LIAR_ERR_UNSUPPORTED, "tracer %d", R.tracer);
+    const uint64_t npix = (uint64_t)R.width * R.height;
+    if (npix > (1ull << 26)) return ctx_fail(ctx, LIAR_ERR_INVALID, "guided rendering takes at most 2^26 pixels");
+    int rc = ctx_activate(ctx);
+    if (rc) return rc;
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    const liar_guide_config& cfg = guide_config(guide);
+    const uint32_t batch = cfg.batch_records > 0 ? (uint32_t)cfg.batch_records : 65536u;
+    const int steps = cfg.steps_per_pass > 0 ? cfg.steps_per_pass : 4;
+    const size_t rec_cap = train ? std::max<size_t>((size_t)batch * steps, 1 << 16) : 0;
+    GuidedBuffers* gb = guided_buffers(ctx);
+    rc = ensure_guided_buffers(ctx, gb, (size_t)npix, rec_cap);
+    if (rc) return rc;
+    if (attrs_done_device != ctx->device) {
+        cudaError_t e = cudaFuncSetAttribute(k_g_shade, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kShadeSmem);
+        if (e != cudaSuccess) return ctx_cuda(ctx, e, "guided shade attributes");
+        attrs_done_device = ctx->device;
+    }
+    cudaError_t e = cudaMemsetAsync(gb->stats, 0, 4 * sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return ctx_cuda(ctx, e, "reset statistics");
+    GParams W;
+    W.cam = R.camera;
+    W.width = R.width;
+    W.height = R.height;
+    W.spp = R.spp;
+    W.max_gen = R.max_ray_generation;
+    W.max_depth = R.max_depth;
+    W.seed = mix64(R.seed ^ mix64(0x51ed270b27ad0e0dull + (uint64_t)(uint32_t)R.first_sample));
+    W.train = train ? 1 : 0;
+    for (int k = 0; k < 3; ++k) {
+        W.box_lo[k] = cfg.bounds_lo[k];
+        W.box_inv[k] = 1.0f / (cfg.bounds_hi[k] - cfg.bounds_lo[k]);
+    }
+    W.records = gb->raw;
+    W.rec_count = gb->counters;
+    W.rec_cap = (uint32_t)rec_cap;
+    W.stats = gb->stats;
+    const DScene& S = scene_dscene(scene);
+    const liar_gpu_mesh* mesh = scene_mesh(scene);
+    const uint32_t n = (uint32_t)npix;
+    // the shade kernel holds the guide's weights in shared memory only while the guide is sampled
+    int per_sm_guided = 0, per_sm_plain = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_guided, k_g_shade, kShadeThreads, kShadeSmem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_plain, k_g_shade, kShadeThreads, 0);
+    if (e != cudaSuccess) return ctx_cuda(ctx, e, "guided shade occupancy");
+    unsigned long long records_total = 0;
+    for (int pass = 0; pass < R.spp; ++pass) {
+        W.sample = (uint32_t)pass;
+        // an untrained guide is not sampled: the first training pass renders with BSDF and lights only
+        W.guide_prob = (train && guide_steps(guide) == 0) ? 0.0f : cfg.guide_probability;
+        const bool guide_on = W.guide_prob > 0.0f;
+        const size_t smem = guide_on ? kShadeSmem : 0;
+        const unsigned shade_grid = (unsigned)(ctx->num_sms * std::max(guide_on ? per_sm_guided : per_sm_plain, 1));
+        e = cudaMemsetAsync(gb->q[0].count, 0, 4, st);
+        if (e == cudaSuccess && train) e = cudaMemsetAsync(gb->counters, 0, 8, st);
+        if (e != cudaSuccess) return ctx_cuda(ctx, e, "reset queue");
+        k_g_raygen<<<(n + 255) / 256, 256, 0, st>>>(S, W, gb->P, gb->q[0], n);
+        uint32_t n_in = n;
+        int cur = 0;
+        for (int bounce = 0; n_in > 0; ++bounce) {
+            if (bounce > 4096) return ctx_fail(ctx, LIAR_ERR_TIMEOUT, "paths did not terminate after 4096 bounces");
+            rc = trace_mesh_internal(ctx, mesh, gb->q[cur].rays, n_in, gb->hits, 0, st, kCounterWord + 8);
+            if (rc) return rc;
+            e = cudaMemsetAsync(gb->q[cur ^ 1].count, 0, 4, st);
+            if (e != cudaSuccess) return ctx_cuda(ctx, e, "reset queue");
+            const unsigned grid = std::min<unsigned>(shade_grid, (n_in + kShadeThreads - 1) / kShadeThreads);
+            k_g_shade<<<grid, kShadeThreads, smem, st>>>(S, W, gb->P, gb->q[cur], gb->hits, n_in, gb->q[cur ^ 1],
+                                                               d_film, guide_frag_fwd(guide));
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return ctx_cuda(ctx, e, "guided shade launch");
+            cur ^= 1;
+            e = cudaMemcpyAsync(gb->h_count, gb->q[cur].count, 4, cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) return ctx_cuda(ctx, e, "queue size");
+            n_in = gb->h_count[0];
+        }
+        if (train) {
+            k_g_finalize<<<ctx->num_sms * 4, 256, 0, st>>>(gb->raw, gb->counters, (uint32_t)rec_cap, gb->P.L, gb->train,
+                                                           gb->counters + 1, (uint32_t)rec_cap);
+            e = cudaMemcpyAsync(gb->h_count, gb->counters, 8, cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) return ctx_cuda(ctx, e, "training records");
+            const uint32_t n_train = std::min<uint32_t>(gb->h_count[1], (uint32_t)rec_cap);
+            records_total += n_train;
+            if (n_train > 0) {
+                for (int s = 0; s < steps; ++s) {
+                    const uint32_t first = (uint32_t)(((uint64_t)s * batch) % n_train);
+                    const uint32_t cnt = std::min<uint32_t>(batch, n_train - first);
+                    rc = guide_train(ctx, guide, gb->train + (size_t)first * kTrainRecord, nullptr, cnt, 1, nullptr,
+                                     nullptr, st);
+                    if (rc) return rc;
+                }
+            }
+        }
+    }
+    unsigned long long stats[4];
+    e = cudaMemcpyAsync(stats, gb->stats, sizeof(stats), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return ctx_cuda(ctx, e, "guided render statistics");
+    guide_count(guide, records_total, stats[3], (unsigned long long)R.spp);
+    stats[0] = npix * (uint64_t)R.spp;
+    e = cudaMemcpyAsync(gb->stats, stats, 8, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return ctx_cuda(ctx, e, "guided render statistics");
+    return ctx_check_status(ctx);
+}
+
+extern "C" int liar_gpu_render_guided_stats(const liar_gpu_ctx* ctx, unsigned long long* out4) {
+    if (!ctx || !out4) return LIAR_ERR_INVALID;
+    for (auto& ext : ctx->extensions)
+        if (ext.first == "guided") {
+            GuidedBuffers* gb = static_cast<GuidedBuffers*>(ext.second);
+            if (!gb->stats) break;
+            if (cudaMemcpy(out4, gb->stats, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost) != cudaSuccess) {
+                cudaGetLastError();
+                return LIAR_ERR_CUDA;
+            }
+            return LIAR_OK;
+        }
+    for (int k = 0; k < 4; ++k) out4[k] = 0;
+    return LIAR_OK;
+}

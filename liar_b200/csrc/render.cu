@@ -136,36 +136,15 @@ __global__ void __launch_bounds__(256) k_raygen(DScene S, WaveParams W, Paths P,
     if (i < n_paths) {
         const uint64_t g = W.first_path + i;
         const SampleKey k = key_of(W, g);
-        const uint32_t px = k.pixel % (uint32_t)W.width, py = k.pixel / (uint32_t)W.width;
-        const float sx = ((float)px + sample_dim(k, DIM_SCREEN, true)) / (float)W.width;
-        const float sy = ((float)py + sample_dim(k, DIM_SCREEN + 1, true)) / (float)W.height;
         float lpdf;
         const float lam = observer_sample(S, sample_dim(k, DIM_LAMBDA, true), lpdf);
-        const liar_camera& C = W.cam;
-        float3 pos = mk(C.position[0], C.position[1], C.position[2]);
-        float3 dir = mk(C.direction[0], C.direction[1], C.direction[2]) +
-                     (sx - 0.5f) * mk(C.right[0], C.right[1], C.right[2]) +
-                     (sy - 0.5f) * mk(C.down[0], C.down[1], C.down[2]);
-        dir = normal(dir);
-        const float3 dn = mk(C.direction_normal[0], C.direction_normal[1], C.direction_normal[2]);
-        float factor = 1.0f / dot(dir, dn);
-        if (C.lens_radius > 0.0f && C.focus_distance > 0.0f && C.focus_distance < 3.4e38f) {
-            const float2 lens = concentric_disk(sample_dim(k, DIM_LENS, true), sample_dim(k, DIM_LENS + 1, true));
-            const float3 lp = pos + (C.lens_radius * lens.x) * mk(C.right_normal[0], C.right_normal[1], C.right_normal[2]) +
-                              (C.lens_radius * lens.y) * mk(C.down_normal[0], C.down_normal[1], C.down_normal[2]);
-            const float3 fp = pos + (factor * C.focus_distance) * dir;
-            pos = lp;
-            dir = normal(fp - lp);
-            factor = 1.0f / dot(dir, dn);
-        }
+        r = camera_ray(W.cam, k, W.width, W.height);
         P.lam[i] = lam;
         P.lam_pdf[i] = lpdf;
         P.T[i] = 1.0f;
         P.L[i] = 0.0f;
         P.alpha[i] = 0.0f;
         P.gen[i] = 0;
-        r = liar_ray{pos.x, pos.y, pos.z, fmaxf(kTol, factor * C.near_limit),
-                     dir.x, dir.y, dir.z, factor * C.far_limit};
         want = true;
     }
     queue_push(out, want, r, i);

@@ -749,5 +749,30 @@ __device__ inline Bsdf make_bsdf(const DScene& S, const liar_material& M, const 
     return B;
 }
 
+// PerspectiveCamera::doGenerateRay (cameras/perspective_camera.cpp:406-434) for the pixel and
+// sample of key k: stratified jitter in the pixel, thin-lens when the lens radius and focus
+// distance are set; the ray's limits scale the camera's near/far planes by 1 / cos(axis angle)
+__device__ inline liar_ray camera_ray(const liar_camera& C, const SampleKey& k, int width, int height) {
+    const uint32_t px = k.pixel % (uint32_t)width, py = k.pixel / (uint32_t)width;
+    const float sx = ((float)px + sample_dim(k, DIM_SCREEN, true)) / (float)width;
+    const float sy = ((float)py + sample_dim(k, DIM_SCREEN + 1, true)) / (float)height;
+    float3 pos = mk(C.position[0], C.position[1], C.position[2]);
+    float3 dir = mk(C.direction[0], C.direction[1], C.direction[2]) + (sx - 0.5f) * mk(C.right[0], C.right[1], C.right[2]) +
+                 (sy - 0.5f) * mk(C.down[0], C.down[1], C.down[2]);
+    dir = normal(dir);
+    const float3 dn = mk(C.direction_normal[0], C.direction_normal[1], C.direction_normal[2]);
+    float factor = 1.0f / dot(dir, dn);
+    if (C.lens_radius > 0.0f && C.focus_distance > 0.0f && C.focus_distance < 3.4e38f) {
+        const float2 lens = concentric_disk(sample_dim(k, DIM_LENS, true), sample_dim(k, DIM_LENS + 1, true));
+        const float3 lp = pos + (C.lens_radius * lens.x) * mk(C.right_normal[0], C.right_normal[1], C.right_normal[2]) +
+                          (C.lens_radius * lens.y) * mk(C.down_normal[0], C.down_normal[1], C.down_normal[2]);
+        const float3 fp = pos + (factor * C.focus_distance) * dir;
+        pos = lp;
+        dir = normal(fp - lp);
+        factor = 1.0f / dot(dir, dn);
+    }
+    return liar_ray{pos.x, pos.y, pos.z, fmaxf(kTol, factor * C.near_limit), dir.x, dir.y, dir.z, factor * C.far_limit};
+}
+
 }  // namespace rt
 }  // namespace liar_gpu

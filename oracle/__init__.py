@@ -186,3 +186,59 @@ def photon_trace(render_scene, desc, capacity, threads=0):
     n = int(min(counts[0], capacity))
     return rec[:n], {"stored": int(counts[0]), "global": int(counts[1]), "caustic": int(counts[2]),
                      "emitted": int(counts[3]), "rc": rc}
+
+
+# ---- path-guiding network (oracle_guide.cpp)
+
+GUIDE_PARAMS = 256 * 64 + 4 * 64 * 64 + 64 * 48
+
+
+def _guide_lib():
+    L = lib()
+    vp = C.c_void_p
+    L.oracle_guide_forward.restype = C.c_int
+    L.oracle_guide_forward.argtypes = [vp, vp, C.c_uint64, vp, vp, C.c_int, vp, vp]
+    L.oracle_guide_grad.restype = C.c_int
+    L.oracle_guide_grad.argtypes = [vp, vp, C.c_uint64, vp, vp, C.c_int, vp, vp]
+    L.oracle_vmf_pdf.restype = C.c_int
+    L.oracle_vmf_pdf.argtypes = [vp, vp, C.c_uint64, vp]
+    L.oracle_vmf_sample.restype = C.c_int
+    L.oracle_vmf_sample.argtypes = [vp, vp, C.c_uint64, vp, vp]
+    return L
+
+
+def guide_forward(params, inputs, lo, hi, emulate=True):
+    """(raw outputs (n, 48), mixtures (n, 40)) of the guiding network on raw inputs (n, 9)."""
+    p, x = _f32(params), _f32(inputs).reshape(-1, 9)
+    lo, hi = _f32(lo), _f32(hi)
+    raw = np.zeros((x.shape[0], 48), np.float32)
+    mix = np.zeros((x.shape[0], 40), np.float32)
+    _guide_lib().oracle_guide_forward(p.ctypes.data, x.ctypes.data, x.shape[0], lo.ctypes.data, hi.ctypes.data,
+                                      int(emulate), raw.ctypes.data, mix.ctypes.data)
+    return raw, mix
+
+
+def guide_grad(params, records, lo, hi, emulate=True):
+    """(gradient (GUIDE_PARAMS,) float64, loss) of the mean training loss over records (n, 13)."""
+    p, r = _f32(params), _f32(records).reshape(-1, 13)
+    lo, hi = _f32(lo), _f32(hi)
+    g = np.zeros(GUIDE_PARAMS, np.float64)
+    loss = C.c_double()
+    _guide_lib().oracle_guide_grad(p.ctypes.data, r.ctypes.data, r.shape[0], lo.ctypes.data, hi.ctypes.data,
+                                   int(emulate), g.ctypes.data, C.addressof(loss))
+    return g, loss.value
+
+
+def vmf_pdf(mix, dirs):
+    m, d = _f32(mix).reshape(-1, 40), _f32(dirs).reshape(-1, 3)
+    out = np.zeros(d.shape[0], np.float32)
+    _guide_lib().oracle_vmf_pdf(m.ctypes.data, d.ctypes.data, d.shape[0], out.ctypes.data)
+    return out
+
+
+def vmf_sample(mix, u):
+    m, uu = _f32(mix).reshape(-1, 40), _f32(u).reshape(-1, 3)
+    dirs = np.zeros((uu.shape[0], 3), np.float32)
+    pdf = np.zeros(uu.shape[0], np.float32)
+    _guide_lib().oracle_vmf_sample(m.ctypes.data, uu.ctypes.data, uu.shape[0], dirs.ctypes.data, pdf.ctypes.data)
+    return dirs, pdf
