@@ -90,8 +90,9 @@ int launch_trace_t(liar_gpu_ctx* ctx, const liar_gpu_mesh* m, const liar_ray* d_
     if (blocks == 0) blocks = 1;
     cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "reset work counter");
+    const uint32_t batch = trace_batch(n, (uint32_t)blocks * (BLOCK / 32));
     kern<<<(unsigned)blocks, BLOCK, smem, st>>>(m->d_nodes, m->d_tris, d_rays, d_hits, n, d_counter, d_status,
-                                             d_counters);
+                                             d_counters, batch);
     return ctx_cuda(ctx, cudaGetLastError(), "trace kernel launch");
 }
 

@@ -6,6 +6,7 @@
 //
 // Organisation (one lane per ray, persistent warps with per-lane refill):
 //   * a grid of (SM count x resident blocks) blocks; each warp takes batches of BATCH ray indices
+//     (32..256, sized so that the n rays cover every resident warp)
 //     from one atomic work counter and hands them to its lanes one by one: whenever at least
 //     REFILL lanes have finished their ray, those lanes load the next rays of the batch, so short
 //     rays (most random rays miss the mesh after a node or two) do not leave lanes idle while a
@@ -229,13 +230,22 @@ __device__ __forceinline__ bool trace_step(const QNode* __restrict__ nodes, cons
     return true;
 }
 
+// rays per warp fetch: the n rays spread evenly over the launch's warps, rounded up to a multiple
+// of 32 and kept within [32, 256] (fewer fetches for large waves, full occupancy for small ones)
+__host__ __device__ __forceinline__ uint32_t trace_batch(uint32_t n, uint32_t warps) {
+    const uint32_t per = warps ? (n + warps - 1) / warps : n;
+    const uint32_t b = (per + 31u) & ~31u;
+    return b < 32u ? 32u : (b > 256u ? 256u : b);
+}
+
 template <bool ANY, int S, int BLOCK, bool COUNT>
 __global__ void __launch_bounds__(BLOCK) trace_kernel(const QNode* __restrict__ nodes, const QTri* __restrict__ tris,
                                                       const liar_ray* __restrict__ rays, liar_hit* __restrict__ hits,
                                                       uint32_t n_rays, uint32_t* __restrict__ work_counter,
                                                       uint32_t* __restrict__ status_word,
-                                                      TraceCounters* __restrict__ counters) {
-    constexpr uint32_t BATCH = 256;   // ray indices a warp takes from the global counter at once
+                                                      TraceCounters* __restrict__ counters, uint32_t BATCH) {
+    // BATCH: ray indices a warp takes from the global counter at once (trace_batch: n spread over
+    // all resident warps, 32..256, so that a small wave still keeps every warp busy)
     constexpr int REFILL = 8;         // refill once this many lanes are idle
     extern __shared__ int trace_smem[];  // S * BLOCK node entries, then S * BLOCK distances
     LaneStack<S, BLOCK> stack;
@@ -343,13 +353,13 @@ __global__ void __launch_bounds__(BLOCK) trace_multi_kernel(const TreeRoot* __re
                                                             liar_hit* __restrict__ hits, const uint32_t* __restrict__ n_dev,
                                                             uint32_t* __restrict__ work_counter,
                                                             uint32_t* __restrict__ status_word) {
-    constexpr uint32_t BATCH = 256;
     constexpr int REFILL = 8;
     extern __shared__ int trace_smem[];
     LaneStack<S, BLOCK> stack;
     stack.s_node = trace_smem;
     stack.s_t = reinterpret_cast<float*>(trace_smem + S * BLOCK);
     const uint32_t n_rays = *n_dev;
+    const uint32_t BATCH = trace_batch(n_rays, gridDim.x * (BLOCK / 32));
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
     const uint64_t pol_tree = policy_evict_last();
