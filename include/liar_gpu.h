@@ -165,6 +165,9 @@ typedef struct liar_material {
     int32_t spec[4];
     int32_t emission;
     float rough_u, rough_v;
+    int32_t samples;   /* DirectLighting: reflection (and transmission) samples per vertex, the shader's
+                          numReflectionSamples (conductor.cpp:118, dielectric.cpp:134-144,
+                          cook_torrance.cpp:182); 0 = 1 */
 } liar_material;
 
 /* Lights (src/liar/scenery/light_*.cpp). AREA_PARALLELOGRAM: pos = support, u/v = sizes
@@ -178,6 +181,8 @@ typedef struct liar_light {
     int32_t first_tri, n_tris;
     float pos[3], u[3], v[3];
     float power;
+    int32_t emission_samples;  /* numberOfEmissionSamples (light_context.cpp:66-72): DirectLighting's
+                                  light and BSDF samples per light per vertex; 0 = 1 */
 } liar_light;
 
 typedef struct liar_scene_desc {
@@ -203,7 +208,11 @@ typedef struct liar_camera {
     float lens_radius, focus_distance, near_limit, far_limit;
 } liar_camera;
 
-enum liar_tracer_type { LIAR_TRACER_ADJOINT_PHOTON = 0 };
+/* ADJOINT_PHOTON: src/liar/tracers/adjoint_photon_tracer.cpp (unidirectional path tracing);
+ * DIRECT_LIGHTING: src/liar/tracers/direct_lighting.cpp (direct light by
+ * RayTracer::estimateLightContribution, kernel/ray_tracer.cpp:188-276, plus recursive specular
+ * and glossy reflection/transmission up to max_ray_generation) */
+enum liar_tracer_type { LIAR_TRACER_ADJOINT_PHOTON = 0, LIAR_TRACER_DIRECT_LIGHTING = 1 };
 typedef struct liar_render_desc {
     liar_camera camera;
     int32_t width, height, spp;
@@ -213,6 +222,8 @@ typedef struct liar_render_desc {
     uint64_t seed;
     int32_t first_sample;        /* progressive rendering: index of the first sample of this pass */
     int32_t wave_paths;          /* paths in flight per wave, 0 = automatic */
+    int32_t secondary_light_samples; /* DirectLighting.numberOfSecondaryLightSamples (0 = 1) */
+    int32_t trace_glossy;        /* DirectLighting.traceGlossy: -1 = false, otherwise true */
 } liar_render_desc;
 
 /* Uploads the scene (builds the triangle tree). */

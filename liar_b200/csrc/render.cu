@@ -36,6 +36,8 @@ struct liar_gpu_scene {
     std::vector<void*> buffers;  // device allocations owned by the scene
     DScene d{};
     size_t n_triangles = 0;
+    std::vector<liar_light> h_lights;        // host copies for launch planning
+    std::vector<liar_material> h_materials;
 };
 
 namespace {
@@ -539,6 +541,8 @@ extern "C" int liar_gpu_scene_upload(liar_gpu_ctx* ctx, const liar_scene_desc* d
         liar_gpu_scene_destroy(s);
         return rc;
     }
+    s->h_lights.assign(D.lights, D.lights + D.n_lights);
+    s->h_materials.assign(D.materials, D.materials + D.n_materials);
     d.nodes = mesh_nodes(s->mesh);
     d.qtris = mesh_tris(s->mesh);
     d.n_lights = (int)D.n_lights;
@@ -556,6 +560,13 @@ namespace liar_gpu {
 namespace rt {
 // accessors for the other subsystems that shade against an uploaded scene (photon tracing)
 const DScene& scene_dscene(const liar_gpu_scene* s) { return s->d; }
+const std::vector<liar_light>& scene_lights(const liar_gpu_scene* s) { return s->h_lights; }
+const std::vector<liar_material>& scene_materials(const liar_gpu_scene* s) { return s->h_materials; }
+unsigned long long* render_stats_device(liar_gpu_ctx* ctx, cudaStream_t st) {
+    RenderBuffers* rb = render_buffers(ctx);
+    if (!rb->stats && ensure_render_buffers(ctx, rb, 0)) return nullptr;
+    return rb->stats;
+}
 const liar_gpu_mesh* scene_mesh(const liar_gpu_scene* s) { return s->mesh; }
 int scene_device(const liar_gpu_scene* s) { return s->device; }
 }  // namespace rt
@@ -572,6 +583,14 @@ extern "C" void liar_gpu_scene_destroy(liar_gpu_scene* s) {
     delete s;
 }
 
+namespace liar_gpu {
+namespace rt {
+// DirectLighting (direct.cu)
+int render_direct(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_render_desc& R, float* d_film,
+                  cudaStream_t st);
+}  // namespace rt
+}  // namespace liar_gpu
+
 namespace {
 
 int render_impl(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_render_desc* desc, float* d_film,
@@ -579,6 +598,7 @@ int render_impl(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_rende
     const liar_render_desc& R = *desc;
     if (R.width <= 0 || R.height <= 0 || R.spp <= 0) return ctx_fail(ctx, LIAR_ERR_INVALID, "empty image or no samples");
     if (R.max_ray_generation < 0) return ctx_fail(ctx, LIAR_ERR_INVALID, "max_ray_generation must be >= 0");
+    if (R.tracer == LIAR_TRACER_DIRECT_LIGHTING) return render_direct(ctx, scene, R, d_film, st);
     if (R.tracer != LIAR_TRACER_ADJOINT_PHOTON) return ctx_fail(ctx, LIAR_ERR_UNSUPPORTED, "tracer %d", R.tracer);
     const uint64_t total = (uint64_t)R.width * R.height * R.spp;
     if ((uint64_t)R.width * R.height >= (1ull << 32)) return ctx_fail(ctx, LIAR_ERR_INVALID, "image too large");

@@ -26,13 +26,13 @@ class CSpectrum(C.Structure):
 
 class CMaterial(C.Structure):
     _fields_ = [("type", C.c_int32), ("mdf", C.c_int32), ("spec", C.c_int32 * 4), ("emission", C.c_int32),
-                ("rough_u", C.c_float), ("rough_v", C.c_float)]
+                ("rough_u", C.c_float), ("rough_v", C.c_float), ("samples", C.c_int32)]
 
 
 class CLight(C.Structure):
     _fields_ = [("type", C.c_int32), ("spectrum", C.c_int32), ("object", C.c_int32), ("double_sided", C.c_int32),
                 ("first_tri", C.c_int32), ("n_tris", C.c_int32), ("pos", C.c_float * 3), ("u", C.c_float * 3),
-                ("v", C.c_float * 3), ("power", C.c_float)]
+                ("v", C.c_float * 3), ("power", C.c_float), ("emission_samples", C.c_int32)]
 
 
 _P = C.c_void_p
@@ -58,7 +58,8 @@ class CCamera(C.Structure):
 class CRenderDesc(C.Structure):
     _fields_ = [("camera", CCamera), ("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32),
                 ("tracer", C.c_int32), ("max_ray_generation", C.c_int32), ("max_depth", C.c_int32),
-                ("seed", C.c_uint64), ("first_sample", C.c_int32), ("wave_paths", C.c_int32)]
+                ("seed", C.c_uint64), ("first_sample", C.c_int32), ("wave_paths", C.c_int32),
+                ("secondary_light_samples", C.c_int32), ("trace_glossy", C.c_int32)]
 
 
 SPEC_CONSTANT, SPEC_SAMPLED, SPEC_BLACKBODY, SPEC_CAUCHY = 0, 1, 2, 3
@@ -160,6 +161,7 @@ class _Builder:
         m = CMaterial()
         m.spec[:] = [-1, -1, -1, -1]
         m.emission = -1
+        m.samples = 1
         bsdf = shader
         if isinstance(shader, shaders.Sum):
             emitters = [c for c in shader.children if isinstance(c, shaders.Unshaded)]
@@ -186,6 +188,7 @@ class _Builder:
             m.spec[1] = self.spectrum(bsdf.absorptionCoefficient)
             m.spec[2] = self.spectrum(bsdf.reflectance)
             if isinstance(bsdf, shaders.CookTorrance):
+                m.samples = int(getattr(bsdf, "numberOfSamples", 1))
                 m.rough_u = as_scalar(bsdf.roughnessU)
                 m.rough_v = as_scalar(bsdf.roughnessV)
                 m.mdf = bsdf.mdf.kind
@@ -196,6 +199,7 @@ class _Builder:
             m.spec[2] = self.spectrum(bsdf.reflectance)
             m.spec[3] = self.spectrum(bsdf.transmittance)
             if isinstance(bsdf, shaders.Walter):
+                m.samples = int(getattr(bsdf, "numberOfSamples", 1))
                 m.rough_u = as_scalar(bsdf.roughnessU)
                 m.rough_v = as_scalar(bsdf.roughnessV)
                 m.mdf = bsdf.mdf.kind
@@ -237,6 +241,7 @@ class _Builder:
             L = CLight()
             L.spectrum = self.spectrum(obj.radiance)
             L.double_sided = int(bool(obj.isDoubleSided))
+            L.emission_samples = int(obj.numberOfEmissionSamples)
             first, count = self.geometry(surf, obj.shader or surf.shader or inherited, li)
             L.object = len(self.obj_mat) - 1
             if isinstance(surf, scenery.Parallelogram):
@@ -256,6 +261,7 @@ class _Builder:
             L = CLight()
             L.type = LIGHT_POINT
             L.object = -1
+            L.emission_samples = int(obj.numberOfEmissionSamples)
             L.spectrum = self.spectrum(obj.intensity)
             L.pos[:] = obj.position
             L.power = 4 * math.pi * as_spectrum(obj.intensity).luminance  # LightPoint::doTotalPower
@@ -264,6 +270,7 @@ class _Builder:
             L = CLight()
             L.type = LIGHT_SKY
             L.object = -1
+            L.emission_samples = int(obj.numberOfEmissionSamples)
             L.spectrum = self.spectrum(obj.radiance)
             self.lights.append(L)
         elif hasattr(obj, "triangles"):
@@ -327,6 +334,8 @@ def render_desc(camera, width: int, height: int, spp: int, tracer, seed: int = 0
     r.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
     r.first_sample = int(first_sample)
     r.wave_paths = int(wave_paths)
+    r.secondary_light_samples = int(getattr(tracer, "numberOfSecondaryLightSamples", 1))
+    r.trace_glossy = 1 if getattr(tracer, "traceGlossy", True) else -1
     return r
 
 

@@ -11,3 +11,14 @@ class RayTracer:
 
 class AdjointPhotonTracer(RayTracer):
     kind = 0
+
+
+class DirectLighting(RayTracer):
+    """Whitted-style direct lighting (src/liar/tracers/direct_lighting.cpp): direct light by light
+    and BSDF sampling per light, recursive specular (and glossy) reflection and transmission."""
+    kind = 1
+
+    def __init__(self):
+        super().__init__()
+        self.numberOfSecondaryLightSamples = 1   # direct_lighting.cpp:46-49
+        self.traceGlossy = True

@@ -40,6 +40,7 @@ struct Hit {
     float t;
 };
 Hit tree_closest(void* tree, const Ray& r);
+bool tree_any(void* tree, const Ray& r);
 }  // namespace oracle_internal
 
 namespace {
@@ -57,12 +58,14 @@ struct Material {
     int32_t spec[4];
     int32_t emission;
     float rough_u, rough_v;
+    int32_t samples;
 };
 struct Light {
     int32_t type, spectrum, object, double_sided;
     int32_t first_tri, n_tris;
     float pos[3], u[3], v[3];
     float power;
+    int32_t emission_samples;
 };
 struct Camera {
     float position[3], direction[3], right[3], down[3];
@@ -88,6 +91,7 @@ struct RenderIn {
     int32_t width, height, spp, tracer, max_ray_generation, max_depth;
     uint64_t seed;
     int32_t first_sample, wave_paths;
+    int32_t secondary_light_samples, trace_glossy;
 };
 
 enum { SP_CONST = 0, SP_SAMPLED = 1, SP_BB = 2, SP_CAUCHY = 3 };
@@ -577,14 +581,18 @@ struct Path {
 
 float trace_photon(Path& P, V o, V d, float tmin, float tmax, int gen);
 
-// AdjointPhotonTracer::shadeSurface + scatterSurface for the hit `h` of ray (o, d)
-float shade_surface(Path& P, V o, V d, float tmin, float tmax, const Hit& h, int gen) {
-    const Scene& S = *P.S;
-    float result = 0;
+// IntersectionContext of a hit (intersection_context.cpp:55-290): point, flipped normals, frame
+struct Ctx {
+    V target, ng, N, u, v;
+    bool leaving;
+    int obj, light, mi;
+};
+Ctx hit_ctx(const Scene& S, V o, V d, const Hit& h) {
+    Ctx c;
     const uint32_t prim = (uint32_t)h.prim;
-    const int obj = S.in.triangle_object[prim];
-    const int light = S.in.object_light[obj];
-    const int mi = S.in.object_material[obj];
+    c.obj = S.in.triangle_object[prim];
+    c.light = S.in.object_light[c.obj];
+    c.mi = S.in.object_material[c.obj];
     const uint32_t* tr = S.in.triangles + 3 * (size_t)prim;
     const float* pa = S.in.vertices + 3 * tr[0];
     const float* pb = S.in.vertices + 3 * tr[1];
@@ -594,7 +602,7 @@ float shade_surface(Path& P, V o, V d, float tmin, float tmax, const Hit& h, int
     float tt, bu = 0, bv = 0;
     const float oo[3] = {o.x, o.y, o.z}, dd[3] = {d.x, d.y, d.z};
     if (!oracle_tri_intersect(oo, dd, pa, pb, pc, &tt, &bu, &bv)) bu = bv = 0;
-    const V target = A + bu * e1 + bv * e2;
+    c.target = A + bu * e1 + bv * e2;
     const V ng0 = unit(cross(e1, e2));
     V ns = ng0;
     if (S.in.triangle_normals && S.in.normals) {
@@ -607,9 +615,85 @@ float shade_surface(Path& P, V o, V d, float tmin, float tmax, const Hit& h, int
             ns = unit(w0 * V{n0[0], n0[1], n0[2]} + bu * V{n1[0], n1[1], n1[2]} + bv * V{n2[0], n2[1], n2[2]});
         }
     }
-    const bool leaving = dot(d, ng0) > 0;
-    const V ng = dot(ng0, -d) < 0 ? -ng0 : ng0;  // flipTo(-direction)
-    const V N = dot(ns, -d) < 0 ? -ns : ns;
+    c.leaving = dot(d, ng0) > 0;
+    c.ng = dot(ng0, -d) < 0 ? -ng0 : ng0;  // flipTo(-direction)
+    c.N = dot(ns, -d) < 0 ? -ns : ns;
+    // frame: IntersectionContext::bsdfToLocal
+    V u = e1 - dot(e1, c.N) * c.N, v = e2 - dot(e2, c.N) * c.N;
+    const float su = dot(u, u), sv = dot(v, v);
+    if (std::max(su, sv) < 1e-3f * std::max(dot(e1, e1), dot(e2, e2))) {
+        const V ax = std::fabs(c.N.x) < 0.9f ? V{1, 0, 0} : V{0, 1, 0};
+        u = cross(ax, c.N);
+        v = cross(c.N, u);
+    }
+    if (su >= sv) {
+        u = unit(u);
+        v = cross(c.N, u);
+    } else {
+        v = unit(v);
+        u = cross(v, c.N);
+    }
+    c.u = u;
+    c.v = v;
+    return c;
+}
+
+// Shader::bsdf at one wavelength
+Bsdf make_bsdf(const Scene& S, const Material& M, const Ctx& c, float lam) {
+    Bsdf B{};
+    B.type = M.type;
+    B.mdf = M.mdf;
+    B.ng = {dot(c.ng, c.u), dot(c.ng, c.v), dot(c.ng, c.N)};
+    B.eta = B.kappa = B.ior = B.etaI = B.etaT = 1;
+    B.au = sq(std::max(M.rough_u, 1e-3f));
+    B.av = sq(std::max(M.rough_v, 1e-3f));
+    switch (M.type) {
+        case M_LAMBERT:
+            B.caps = C_REFL | C_DIFF;
+            B.r = spectrum(S, M.spec[0], lam, true);
+            break;
+        case M_CONDUCTOR:
+        case M_CT:
+            B.caps = M.type == M_CONDUCTOR ? (C_REFL | C_SPEC) : (C_REFL | C_GLOSSY);
+            B.eta = std::max(spectrum(S, M.spec[0], lam, false), 1e-9f);
+            B.kappa = std::max(spectrum(S, M.spec[1], lam, false), 1e-9f);
+            B.r = spectrum(S, M.spec[2], lam, true);
+            break;
+        case M_DIELECTRIC: {
+            B.caps = C_REFL | C_TRANS | C_SPEC;
+            const float i1 = std::max(spectrum(S, M.spec[1], lam, false), 1e-9f);
+            const float i2 = std::max(spectrum(S, M.spec[0], lam, false), 1e-9f);
+            B.ior = c.leaving ? i2 / i1 : i1 / i2;
+            B.r = spectrum(S, M.spec[2], lam, true);
+            B.t = spectrum(S, M.spec[3], lam, true);
+            break;
+        }
+        case M_WALTER: {
+            B.caps = C_TRANS | C_GLOSSY;
+            float ei = std::max(spectrum(S, M.spec[1], lam, false), 1e-9f);
+            float et = std::max(spectrum(S, M.spec[0], lam, false), 1e-9f);
+            if (c.leaving) std::swap(ei, et);
+            B.etaI = ei;
+            B.etaT = et;
+            B.r = spectrum(S, M.spec[2], lam, true);
+            B.t = spectrum(S, M.spec[3], lam, true);
+            break;
+        }
+        case M_MIRROR:
+            B.caps = C_REFL | C_SPEC;
+            B.r = spectrum(S, M.spec[0], lam, true);
+            break;
+    }
+    return B;
+}
+
+// AdjointPhotonTracer::shadeSurface + scatterSurface for the hit `h` of ray (o, d)
+float shade_surface(Path& P, V o, V d, float tmin, float tmax, const Hit& h, int gen) {
+    const Scene& S = *P.S;
+    float result = 0;
+    const Ctx c = hit_ctx(S, o, d, h);
+    const int light = c.light, mi = c.mi;
+    const V target = c.target, ng = c.ng, N = c.N, u = c.u, v = c.v;
     if (gen > 0 && light >= 0) result += spectrum(S, S.in.lights[light].spectrum, P.lam, false);
     if (mi < 0 || S.in.materials[mi].type == M_NONE) {
         if (mi >= 0 && light < 0 && S.in.materials[mi].emission >= 0)
@@ -618,65 +702,7 @@ float shade_surface(Path& P, V o, V d, float tmin, float tmax, const Hit& h, int
     }
     const Material& M = S.in.materials[mi];
     if (light < 0 && M.emission >= 0) result += spectrum(S, M.emission, P.lam, false);
-    // frame: IntersectionContext::bsdfToLocal
-    V u = e1 - dot(e1, N) * N, v = e2 - dot(e2, N) * N;
-    const float su = dot(u, u), sv = dot(v, v);
-    if (std::max(su, sv) < 1e-3f * std::max(dot(e1, e1), dot(e2, e2))) {
-        const V ax = std::fabs(N.x) < 0.9f ? V{1, 0, 0} : V{0, 1, 0};
-        u = cross(ax, N);
-        v = cross(N, u);
-    }
-    if (su >= sv) {
-        u = unit(u);
-        v = cross(N, u);
-    } else {
-        v = unit(v);
-        u = cross(v, N);
-    }
-    Bsdf B{};
-    B.type = M.type;
-    B.mdf = M.mdf;
-    B.ng = {dot(ng, u), dot(ng, v), dot(ng, N)};
-    B.eta = B.kappa = B.ior = B.etaI = B.etaT = 1;
-    B.au = sq(std::max(M.rough_u, 1e-3f));
-    B.av = sq(std::max(M.rough_v, 1e-3f));
-    switch (M.type) {
-        case M_LAMBERT:
-            B.caps = C_REFL | C_DIFF;
-            B.r = spectrum(S, M.spec[0], P.lam, true);
-            break;
-        case M_CONDUCTOR:
-        case M_CT:
-            B.caps = M.type == M_CONDUCTOR ? (C_REFL | C_SPEC) : (C_REFL | C_GLOSSY);
-            B.eta = std::max(spectrum(S, M.spec[0], P.lam, false), 1e-9f);
-            B.kappa = std::max(spectrum(S, M.spec[1], P.lam, false), 1e-9f);
-            B.r = spectrum(S, M.spec[2], P.lam, true);
-            break;
-        case M_DIELECTRIC: {
-            B.caps = C_REFL | C_TRANS | C_SPEC;
-            const float i1 = std::max(spectrum(S, M.spec[1], P.lam, false), 1e-9f);
-            const float i2 = std::max(spectrum(S, M.spec[0], P.lam, false), 1e-9f);
-            B.ior = leaving ? i2 / i1 : i1 / i2;
-            B.r = spectrum(S, M.spec[2], P.lam, true);
-            B.t = spectrum(S, M.spec[3], P.lam, true);
-            break;
-        }
-        case M_WALTER: {
-            B.caps = C_TRANS | C_GLOSSY;
-            float ei = std::max(spectrum(S, M.spec[1], P.lam, false), 1e-9f);
-            float et = std::max(spectrum(S, M.spec[0], P.lam, false), 1e-9f);
-            if (leaving) std::swap(ei, et);
-            B.etaI = ei;
-            B.etaT = et;
-            B.r = spectrum(S, M.spec[2], P.lam, true);
-            B.t = spectrum(S, M.spec[3], P.lam, true);
-            break;
-        }
-        case M_MIRROR:
-            B.caps = C_REFL | C_SPEC;
-            B.r = spectrum(S, M.spec[0], P.lam, true);
-            break;
-    }
+    const Bsdf B = make_bsdf(S, M, c, P.lam);
     const V md = -d;
     V wi{dot(md, u), dot(md, v), dot(md, N)};
     wi.z = std::max(wi.z, 1.19209290e-07f);
@@ -746,6 +772,222 @@ float trace_photon(Path& P, V o, V d, float tmin, float tmax, int gen) {
     }
     if (gen == 0) P.alpha = 1;
     return power * shade_surface(P, o, d, tmin, tmax, h, gen);
+}
+
+// ---- DirectLighting (tracers/direct_lighting.cpp) with RayTracer::estimateLightContribution
+// (kernel/ray_tracer.cpp:188-276): the recursive form of the library's wavefront (csrc/direct.cu),
+// with the same sample dimensions, branch keys and shadow-ray bounds.
+const float SHADOW_SHRINK = 1e-4f;
+
+uint32_t dl_dim_light(int l, int k, int axis) { return 0x200000u + ((uint32_t)l * 1024u + (uint32_t)k) * 8u + (uint32_t)axis; }
+uint32_t dl_dim_scatter(int i, int axis) { return 0x400000u + (uint32_t)i * 8u + (uint32_t)axis; }
+uint32_t dl_dim_branch(uint32_t key, uint32_t j) {
+    return 0x80000000u | (uint32_t)(mix64(((uint64_t)key << 20) ^ j) & 0x7fffffffu);
+}
+uint32_t dl_child_key(uint32_t key, uint32_t c) { return (uint32_t)mix64(((uint64_t)key << 8) | (c + 1u)) | 1u; }
+
+// SceneLight::sampleEmission: direction, distance, solid-angle pdf, radiance
+struct LSF {
+    V dir;
+    float dist, pdf, value;
+};
+LSF light_sample_full(const Scene& S, int li, V target, float sx, float sy, float lam) {
+    const Light& L = S.in.lights[li];
+    const LS ls = light_sample(S, li, target, sx, sy);
+    LSF out{ls.dir, 0, ls.pdf, 0};
+    if (L.type == L_PARA || L.type == L_MESH) {
+        // the sampled point again, for the distance (light_sample normalised the direction)
+        V p;
+        if (L.type == L_PARA) {
+            p = V{L.pos[0], L.pos[1], L.pos[2]} + sx * V{L.u[0], L.u[1], L.u[2]} + sy * V{L.v[0], L.v[1], L.v[2]};
+        } else {
+            const float* cdf = S.tri_cdf.data() + L.first_tri;
+            int ii = (int)(std::lower_bound(cdf, cdf + L.n_tris, sx) - cdf);
+            ii = std::min(ii, L.n_tris - 1);
+            const float i0 = ii > 0 ? cdf[ii - 1] : 0.0f;
+            const float di = (sx - i0) / (cdf[ii] - i0);
+            const uint32_t* tr = S.in.triangles + 3 * (size_t)(L.first_tri + ii);
+            const float* a = S.in.vertices + 3 * tr[0];
+            const float* b = S.in.vertices + 3 * tr[1];
+            const float* c = S.in.vertices + 3 * tr[2];
+            const float sr = std::sqrt(di);
+            p = V{a[0], a[1], a[2]} + (1 - sr) * V{b[0] - a[0], b[1] - a[1], b[2] - a[2]} +
+                (sr * sy) * V{c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+        }
+        out.dist = len(p - target);
+        if (out.pdf > 0) out.value = spectrum(S, L.spectrum, lam, false);
+    } else if (L.type == L_POINT) {
+        const V tl = V{L.pos[0], L.pos[1], L.pos[2]} - target;
+        const float d2 = dot(tl, tl);
+        out.dist = std::sqrt(d2);
+        out.value = spectrum(S, L.spectrum, lam, false) / d2;
+    } else if (L.type == L_SKY) {
+        out.dist = S.sky_distance;
+        out.value = spectrum(S, L.spectrum, lam, false);
+    }
+    return out;
+}
+
+// SceneLight::emission(ray): pdf, radiance and distance of the light along a direction
+struct LEF {
+    float pdf, value, t;
+};
+LEF light_emission_full(const Scene& S, int li, V o, V d, float lam) {
+    const Light& L = S.in.lights[li];
+    LEF e{0, 0, INFINITY};
+    if (L.type == L_PARA) {
+        float t;
+        if (!para_hit(L, o, d, TOL, t)) return e;
+        e.t = t;
+    } else if (L.type == L_MESH) {
+        float tb = INFINITY;
+        for (int k = 0; k < L.n_tris; ++k) {
+            const uint32_t* tr = S.in.triangles + 3 * (size_t)(L.first_tri + k);
+            const float oo[3] = {o.x, o.y, o.z}, dd[3] = {d.x, d.y, d.z};
+            float t, uu, vv;
+            if (oracle_tri_intersect(oo, dd, S.in.vertices + 3 * tr[0], S.in.vertices + 3 * tr[1],
+                                     S.in.vertices + 3 * tr[2], &t, &uu, &vv) && t > TOL && t < tb)
+                tb = t;
+        }
+        if (!(tb < INFINITY)) return e;
+        e.t = tb;
+    } else if (L.type == L_SKY) {
+        e.t = S.sky_distance;
+    } else {
+        return e;
+    }
+    e.pdf = light_emission_pdf(S, li, o, d);
+    if (e.pdf > 0) e.value = spectrum(S, L.spectrum, lam, false);
+    return e;
+}
+
+struct DLPath {
+    const Scene* S;
+    const RenderIn* R;
+    Sampler smp;
+    float lam;
+    float alpha = 0;
+};
+
+bool occluded(const Scene& S, V o, V d, float tmax) {
+    return oracle_internal::tree_any(S.tree, Ray{o.x, o.y, o.z, TOL, d.x, d.y, d.z, tmax});
+}
+
+bool is_specular(const Bsdf& B) { return B.type == M_MIRROR || B.type == M_CONDUCTOR || B.type == M_DIELECTRIC; }
+
+template <class U>
+float estimate_light(const Scene& S, const Bsdf& B, const Ctx& c, V wi, V start, int l, int nl, int nb, float lam,
+                     const U& u) {
+    const Light& L = S.in.lights[l];
+    const bool singular = L.type == L_POINT;
+    uint32_t caps = C_REFL | C_TRANS | C_DIFF | C_GLOSSY;
+    if (!singular) caps |= C_SPEC;
+    const float fnl = (float)nl, fnb = (float)nb;
+    float result = 0;
+    for (int k = 0; k < nl; ++k) {
+        const LSF ls = light_sample_full(S, l, start, u(0, k, 0), u(0, k, 1), lam);
+        if (ls.pdf <= 0 || ls.value == 0) continue;
+        if ((L.type == L_PARA || L.type == L_MESH) && dot(c.N, ls.dir) <= 0) continue;
+        const V wo{dot(ls.dir, c.u), dot(ls.dir, c.v), dot(ls.dir, c.N)};
+        const Out be = evaluate(B, wi, wo, caps);
+        if (be.value == 0 || !(be.pdf > 0)) continue;
+        if (occluded(S, start, ls.dir, ls.dist * (1 - SHADOW_SHRINK))) continue;
+        const float w = power_heuristic(fnl * ls.pdf, fnb * be.pdf);
+        result += be.value * ls.value * (w * std::fabs(wo.z) / (fnl * ls.pdf));
+    }
+    for (int k = 0; k < nb; ++k) {
+        const Out bs = sample(B, wi, u(1, k, 0), u(1, k, 1), u(2, k, 0), caps);
+        if (!bs) continue;
+        const V wd = bs.wo.x * c.u + bs.wo.y * c.v + bs.wo.z * c.N;
+        const LEF e = light_emission_full(S, l, start, wd, lam);
+        if (!(e.pdf > 0) || e.value == 0) continue;
+        if (occluded(S, start, wd, e.t * (1 - SHADOW_SHRINK))) continue;
+        const float w = is_specular(B) ? 1.0f : power_heuristic(fnb * bs.pdf, fnl * e.pdf);
+        result += bs.value * e.value * (w * std::fabs(bs.wo.z) / (fnb * bs.pdf));
+    }
+    return result;
+}
+
+float dl_cast(DLPath& P, V o, V d, float tmin, float tmax, int gen, bool hq, uint32_t key) {
+    const Scene& S = *P.S;
+    const RenderIn& R = *P.R;
+    if (gen > R.max_ray_generation) return 0;
+    const Hit h = oracle_internal::tree_closest(S.tree, Ray{o.x, o.y, o.z, tmin, d.x, d.y, d.z, tmax});
+    if (h.prim < 0) {
+        if (gen == 0 && S.sky >= 0 && S.sky_distance > tmin * (1 + TOL) && S.sky_distance < tmax * (1 - TOL)) P.alpha = 1;
+        return 0;
+    }
+    if (gen == 0) P.alpha = 1;
+    const Ctx c = hit_ctx(S, o, d, h);
+    if (c.mi < 0) return dl_cast(P, o, d, h.t + TOL, tmax, gen + 1, hq, dl_child_key(key, 0));
+    const Material& M = S.in.materials[c.mi];
+    float result = 0;
+    if ((gen == 0 || c.light < 0) && M.emission >= 0) result += spectrum(S, M.emission, P.lam, false);
+    if (M.type == M_NONE) return result;
+    const Bsdf B = make_bsdf(S, M, c, P.lam);
+    const V md = -d;
+    V wi{dot(md, c.u), dot(md, c.v), dot(md, c.N)};
+    wi.z = std::max(wi.z, 1.19209290e-07f);
+    const V start = c.target + (10.0f * TOL) * c.N;
+    const int nlights = (int)S.in.n_lights;
+    if (hq) {
+        for (int l = 0; l < nlights; ++l) {
+            const Light& L = S.in.lights[l];
+            const int nl = L.emission_samples > 0 ? L.emission_samples : 1;
+            const int nb = L.type == L_POINT ? 0 : nl;
+            auto u = [&](int kind, int k, int axis) {
+                const int ax = kind == 0 ? axis : (kind == 1 ? 2 + axis : 4);
+                return P.smp.get(dl_dim_light(l, k, ax), true);
+            };
+            result += estimate_light(S, B, c, wi, start, l, nl, nb, P.lam, u);
+        }
+    } else if (nlights > 0) {
+        const int n = R.secondary_light_samples > 0 ? R.secondary_light_samples : 1;
+        for (int k = 0; k < n; ++k) {
+            const uint32_t j0 = 16u * (uint32_t)k;
+            const float uc = P.smp.get(dl_dim_branch(key, j0), false);
+            int l = (int)(std::lower_bound(S.light_cdf.begin(), S.light_cdf.end(), uc) - S.light_cdf.begin());
+            l = std::min(l, nlights - 1);
+            const float pc = light_pdf_choice(S, l);
+            if (!(pc > 0)) continue;
+            const int nb = S.in.lights[l].type == L_POINT ? 0 : 1;
+            auto u = [&](int kind, int, int axis) {
+                return P.smp.get(dl_dim_branch(key, j0 + 1u + 2u * (uint32_t)kind + (uint32_t)axis), false);
+            };
+            result += estimate_light(S, B, c, wi, start, l, 1, nb, P.lam, u) / ((float)n * pc);
+        }
+    }
+    // traced specular and glossy scattering
+    const uint32_t glossy = R.trace_glossy < 0 ? 0u : (uint32_t)C_GLOSSY;
+    const uint32_t sg = C_REFL | C_TRANS | C_SPEC | glossy;
+    if (compatible(B.caps, sg) && gen + 1 <= R.max_ray_generation) {
+        const int ns = hq ? (M.samples > 0 ? M.samples : 1) : 1;
+        for (int side = 0; side < 2; ++side) {
+            const uint32_t dir_cap = side == 0 ? C_REFL : C_TRANS;
+            if (!has(B.caps, dir_cap)) continue;
+            for (int i = 0; i < ns; ++i) {
+                float u0, u1, uc;
+                if (hq) {
+                    u0 = P.smp.get(dl_dim_scatter(i, 3 * side), true);
+                    u1 = P.smp.get(dl_dim_scatter(i, 3 * side + 1), true);
+                    uc = P.smp.get(dl_dim_scatter(i, 3 * side + 2), true);
+                } else {
+                    const uint32_t j0 = 0x1000u + 8u * (uint32_t)side;
+                    u0 = P.smp.get(dl_dim_branch(key, j0), false);
+                    u1 = P.smp.get(dl_dim_branch(key, j0 + 1u), false);
+                    uc = P.smp.get(dl_dim_branch(key, j0 + 2u), false);
+                }
+                const Out bs = sample(B, wi, u0, u1, uc, dir_cap | C_SPEC | glossy);
+                if (!bs || (side == 0 ? !(bs.wo.z > 0) : !(bs.wo.z < 0))) continue;
+                const V wd = bs.wo.x * c.u + bs.wo.y * c.v + bs.wo.z * c.N;
+                const V begin = c.target + ((side == 0 ? 10.0f : -10.0f) * TOL) * c.N;
+                const float child = dl_cast(P, begin, wd, TOL, INFINITY, gen + 1, hq && is_specular(B),
+                                            dl_child_key(key, 2u * (uint32_t)i + (uint32_t)side));
+                result += bs.value * child * (std::fabs(bs.wo.z) / ((float)ns * bs.pdf));
+            }
+        }
+    }
+    return result;
 }
 
 }  // namespace
@@ -1132,7 +1374,14 @@ int oracle_render(void* s, const RenderIn* R, float* film, int64_t pixel_begin, 
                     dir = unit(fp - lp);
                     factor = 1 / dot(dir, dn);
                 }
-                const float L = trace_photon(P, pos, dir, std::max(TOL, factor * C.near_limit), factor * C.far_limit, 0);
+                float L;
+                if (R->tracer == 1) {
+                    DLPath D{&S, R, P.smp, P.lam};
+                    L = dl_cast(D, pos, dir, std::max(TOL, factor * C.near_limit), factor * C.far_limit, 0, true, 1u);
+                    P.alpha = D.alpha;
+                } else {
+                    L = trace_photon(P, pos, dir, std::max(TOL, factor * C.near_limit), factor * C.far_limit, 0);
+                }
                 float X = 0, Yv = 0, Z = 0;
                 if (lpdf > 0) {
                     const float sc = L / lpdf;

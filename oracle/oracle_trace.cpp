@@ -306,6 +306,12 @@ struct Hit {
     int32_t prim;
     float t;
 };
+bool tree_any(void* tree, const Ray& r) {
+    const Tree& t = *static_cast<Tree*>(tree);
+    if (t.nodes.empty()) return false;
+    const oracle_ray rr{r.ox, r.oy, r.oz, r.tmin, r.dx, r.dy, r.dz, r.tmax};
+    return trace_tree(t, rr, true).prim >= 0;
+}
 Hit tree_closest(void* tree, const Ray& r) {
     const Tree& t = *static_cast<Tree*>(tree);
     if (t.nodes.empty()) return {-1, INFINITY};
