@@ -155,6 +155,27 @@ def cornell_bench(ctx, stream, args, world, dist, local, cpu: bool) -> dict:
            "ms_per_frame": ms, "samples_per_s": world * st["paths"] / (ms * 1e-3),
            "segments_per_s": world * st["segments"] / (ms * 1e-3), "segments_per_sample": st["segments"] / st["paths"],
            "note": "device time of liar_gpu_render_device per frame; host waits for each bounce's queue size"}
+    # the same frame with the DirectLighting tracer (16 light + 16 BSDF samples per camera vertex)
+    from liar_b200 import tracers
+    dl = tracers.DirectLighting()
+    ddesc = R.render_desc(e.camera, W, H, SPP, dl, seed=0)
+    for _ in range(2):
+        gs.render_device(ddesc, film.data_ptr(), stream.cuda_stream)
+    stream.synchronize()
+    dsteps = max(1, min(args.steps, 10))
+    e0.record(stream)
+    for _ in range(dsteps):
+        gs.render_device(ddesc, film.data_ptr(), stream.cuda_stream)
+    e1.record(stream)
+    stream.synchronize()
+    dms = e0.elapsed_time(e1) / dsteps
+    if world > 1:
+        t = torch.tensor([dms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dms = float(t.item())
+    out["direct_lighting"] = {"ms_per_frame": dms, "samples_per_s": world * W * H * SPP / (dms * 1e-3),
+                              "shadow_rays_per_sample": 32,
+                              "shadow_rays_per_s": world * W * H * SPP * 32 / (dms * 1e-3)}
     if cpu:
         import oracle
         rows = 8
@@ -167,6 +188,13 @@ def cornell_bench(ctx, stream, args, world, dist, local, cpu: bool) -> dict:
         out["cpu_baseline"] = {"value": rows * W * SPP / dt, "unit": "samples/s", "cores": oracle.hardware_threads(),
                                "kind": "port",
                                "sample": f"{rows} middle image rows ({rows * W * SPP} samples), {dt:.1f} s"}
+        drows = 2
+        t0 = time.perf_counter()
+        rs.render(ddesc, cfilm, pixels=(first_row * W, (first_row + drows) * W))
+        dt = time.perf_counter() - t0
+        out["direct_lighting"]["cpu_baseline"] = {
+            "value": drows * W * SPP / dt, "unit": "samples/s", "cores": oracle.hardware_threads(), "kind": "port",
+            "sample": f"{drows} middle image rows ({drows * W * SPP} samples) with DirectLighting, {dt:.1f} s"}
     gs.close()
     return out
 
