@@ -323,13 +323,16 @@ def guided_bench(ctx, stream, args, world, dist, local, cpu: bool) -> dict:
     plain_mse = mse(plain)
     plain_stats = gs.stats()
     # guided: chunks of 16 spp, training during the first 8 chunks
-    g = GD.Guide(ctx, GD.scene_bounds(flat), guide_probability=0.3, learning_rate=5e-3, steps_per_pass=4,
-                 batch_records=65536, seed=0)
+    g = GD.Guide(ctx, GD.scene_bounds(flat), guide_probability=0.7, light_probability=0.1, learning_rate=5e-3,
+                 steps_per_pass=4, batch_records=65536, seed=0)
     gf = film()
     curve, t_cum, spp, t_hit = [], 0.0, 0, None
     while spp < 4 * plain_spp:
         d = R.render_desc(cam, res, res, chunk, tracer, seed=11, first_sample=spp)
         e0.record(stream)
+        # training: one round per pass over the image for the first 8 chunks
+        if spp < 8 * chunk:
+            d.wave_paths = res * res
         g.render(gs, d, gf.data_ptr(), train=spp < 8 * chunk, stream=st)
         e1.record(stream)
         stream.synchronize()
@@ -373,6 +376,7 @@ def guided_bench(ctx, stream, args, world, dist, local, cpu: bool) -> dict:
                      "segments_per_sample": plain_stats["segments"] / max(plain_stats["paths"], 1)},
            "guided": {"seconds_to_plain_mse": t_hit, "spp_at_crossing": spp if t_hit else None,
                       "training_chunks": 8, "chunk_spp": chunk, "adam_steps": gstats["steps"],
+                      "guide_probability": 0.7, "light_probability": 0.1,
                       "curve_t_spp_mse": curve[:: max(1, len(curve) // 24)]},
            "time_ratio_guided_over_plain": (t_hit / plain_s) if t_hit else None,
            "network": {"inference_queries_per_s": (1 << 20) / eval_s,

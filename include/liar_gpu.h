@@ -281,6 +281,8 @@ typedef struct liar_guide_config {
     float bounds_lo[3], bounds_hi[3]; /* position normalisation box (the scene's bounds) */
     float learning_rate;              /* Adam step size, 0 = 5e-3 */
     float guide_probability;          /* chance of sampling the guide at a diffuse/glossy vertex, [0, 1) */
+    float light_probability;          /* chance of light sampling at a guided vertex (the reference's
+                                         one-sample MIS uses 0.5), [0, 1); 0 = 0.5 */
     int32_t batch_records;            /* training records per Adam step, 0 = 65536 */
     int32_t steps_per_pass;           /* Adam steps after each rendered pass when training, 0 = 4 */
     uint64_t seed;                    /* weight initialisation */

@@ -36,6 +36,7 @@ struct liar_gpu_guide {
     uint2* frag_bwd = nullptr;
     // training scratch, sized for cap records
     size_t cap = 0;
+    __nv_bfloat16* enc = nullptr;    // h_0 (the encodings): [cap][256]
     __nv_bfloat16* act = nullptr;    // h_1..h_5: [5][cap][64]
     __nv_bfloat16* delta = nullptr;  // delta_1..delta_5: [5][cap][64]
     __nv_bfloat16* gout = nullptr;   // [cap][48]
@@ -69,7 +70,11 @@ constexpr int kRecordFloats = 13;
 // normalised record weights are clipped here: radiance estimates are heavy-tailed and a handful of
 // records would otherwise set the whole gradient (the renderer stays unbiased whatever the guide)
 constexpr float kWeightClip = 20.0f;
-constexpr size_t kEvalSmem = kFwdBytes + 4 * (32 * kIn + 32 * kOutStride) * sizeof(float);
+constexpr int kFwdWarps = 8;  // forward kernels: 8 warps share one copy of the weights
+constexpr int kFwdThreads = 32 * kFwdWarps;
+// per warp: the encodings of its 32 rows; the raw outputs reuse the same bytes afterwards
+static_assert((size_t)32 * kOutStride * sizeof(float) <= kEncWarpBytes, "output scratch fits the encodings");
+constexpr size_t kEvalSmem = kFwdBytes + kFwdWarps * kEncWarpBytes;
 
 __device__ __forceinline__ void normalise_input(const float* raw, const float* lo, const float* inv_ext, float* x) {
     for (int c = 0; c < 3; ++c) x[c] = (raw[c] - lo[c]) * inv_ext[c];
@@ -132,18 +137,6 @@ int launch_pack(liar_gpu_guide* G, cudaStream_t st, int bump) {
     return cudaGetLastError() == cudaSuccess ? LIAR_OK : LIAR_ERR_CUDA;
 }
 
-// ---- per-warp input gather: xs[32][kIn] (normalised rows) -> xr[mt][h][kIn] of rows 16 mt + g + 8 h
-
-__device__ __forceinline__ void gather_rows(const float* xs, float (&xr)[2][2][kIn]) {
-    const int g = (threadIdx.x & 31) >> 2;
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-        for (int h = 0; h < 2; ++h)
-#pragma unroll
-            for (int c = 0; c < kIn; ++c) xr[mt][h][c] = xs[(16 * mt + g + 8 * h) * kIn + c];
-}
-
 __device__ __forceinline__ void load_frags(uint2* dst, const uint2* __restrict__ src, size_t bytes) {
     const uint4* s = reinterpret_cast<const uint4*>(src);
     uint4* d = reinterpret_cast<uint4*>(dst);
@@ -152,28 +145,26 @@ __device__ __forceinline__ void load_frags(uint2* dst, const uint2* __restrict__
 }
 
 // ---- inference: raw inputs [n][9] -> mixtures [n][40] = 8 x (mu xyz, kappa), then 8 weights
-__global__ void __launch_bounds__(kThreads) k_eval(const uint2* __restrict__ frag, const float* __restrict__ in, size_t n,
-                                                   Box box, float* __restrict__ mix) {
+__global__ void __launch_bounds__(kFwdThreads) k_eval(const uint2* __restrict__ frag, const float* __restrict__ in,
+                                                      size_t n, Box box, float* __restrict__ mix) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint2* wf = reinterpret_cast<uint2*>(smem);
-    float* xs_all = reinterpret_cast<float*>(smem + kFwdBytes);
     load_frags(wf, frag, kFwdBytes);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float* xs = xs_all + warp * (32 * kIn + 32 * kOutStride);
-    float* os = xs + 32 * kIn;
+    __nv_bfloat16* enc = reinterpret_cast<__nv_bfloat16*>(smem + kFwdBytes + warp * kEncWarpBytes);
+    float* os = reinterpret_cast<float*>(enc);
     const size_t n_tiles = (n + 31) / 32;
-    for (size_t tile = (size_t)blockIdx.x * 4 + warp; tile < n_tiles; tile += (size_t)gridDim.x * 4) {
+    for (size_t tile = (size_t)blockIdx.x * kFwdWarps + warp; tile < n_tiles; tile += (size_t)gridDim.x * kFwdWarps) {
         const size_t row = tile * 32 + lane;
         float x[kIn];
         if (row < n) normalise_input(in + row * kIn, box.lo, box.inv_ext, x);
         else
             for (int c = 0; c < kIn; ++c) x[c] = 0.0f;
-        for (int c = 0; c < kIn; ++c) xs[lane * kIn + c] = x[c];
+        encode_row(x, enc + lane * kEncLd);
         __syncwarp();
-        float xr[2][2][kIn];
-        gather_rows(xs, xr);
         float out[2][6][4];
-        mlp_forward_warp(xr, wf, out, ActStore{nullptr, 0, 0, 0});
+        mlp_forward_warp(enc, wf, out, ActStore{nullptr, 0, 0, 0});
+        __syncwarp();
         scatter_out(out, os);
         __syncwarp();
         if (row < n) {
@@ -238,25 +229,25 @@ __device__ float record_gradient(const float* o, float wx, float wy, float wz, f
 }
 
 // forward over a batch of records with the activations stored, then the output gradient
-__global__ void __launch_bounds__(kThreads) k_train_forward(const uint2* __restrict__ frag, const float* __restrict__ rec,
-                                                            const uint32_t* __restrict__ n_dev, size_t n_max, Box box,
-                                                            const float* __restrict__ scalars_in,
-                                                            __nv_bfloat16* __restrict__ act, __nv_bfloat16* __restrict__ gout,
-                                                            float* __restrict__ loss) {
+__global__ void __launch_bounds__(kFwdThreads) k_train_forward(const uint2* __restrict__ frag, const float* __restrict__ rec,
+                                                               const uint32_t* __restrict__ n_dev, size_t n_max, Box box,
+                                                               const float* __restrict__ scalars_in,
+                                                               __nv_bfloat16* __restrict__ enc_out,
+                                                               __nv_bfloat16* __restrict__ act,
+                                                               __nv_bfloat16* __restrict__ gout, float* __restrict__ loss) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint2* wf = reinterpret_cast<uint2*>(smem);
-    float* xs_all = reinterpret_cast<float*>(smem + kFwdBytes);
     load_frags(wf, frag, kFwdBytes);
     const size_t n = n_dev ? min((size_t)*n_dev, n_max) : n_max;
     const float wsum = scalars_in[0];
     const float inv_mean = (wsum > 0.0f && n > 0) ? (float)n / wsum : 0.0f;
     const float inv_b = n > 0 ? 1.0f / (float)n : 0.0f;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float* xs = xs_all + warp * (32 * kIn + 32 * kOutStride);
-    float* os = xs + 32 * kIn;
+    __nv_bfloat16* enc = reinterpret_cast<__nv_bfloat16*>(smem + kFwdBytes + warp * kEncWarpBytes);
+    float* os = reinterpret_cast<float*>(enc);
     const size_t n_tiles = (n + 31) / 32;
     float lsum = 0.0f;
-    for (size_t tile = (size_t)blockIdx.x * 4 + warp; tile < n_tiles; tile += (size_t)gridDim.x * 4) {
+    for (size_t tile = (size_t)blockIdx.x * kFwdWarps + warp; tile < n_tiles; tile += (size_t)gridDim.x * kFwdWarps) {
         const size_t row = tile * 32 + lane;
         float x[kIn];
         float wx = 0, wy = 0, wz = 1, weight = 0;
@@ -271,13 +262,16 @@ __global__ void __launch_bounds__(kThreads) k_train_forward(const uint2* __restr
         } else {
             for (int c = 0; c < kIn; ++c) x[c] = 0.0f;
         }
-        for (int c = 0; c < kIn; ++c) xs[lane * kIn + c] = x[c];
+        encode_row(x, enc + lane * kEncLd);
         __syncwarp();
-        float xr[2][2][kIn];
-        gather_rows(xs, xr);
-        float out[2][6][4];
         const uint32_t valid = (uint32_t)min((size_t)32, n - tile * 32);
-        mlp_forward_warp(xr, wf, out, ActStore{act, n_max * kWidth, (uint32_t)(tile * 32), valid});
+        // h_0 for the weight gradient of W0: the warp writes its rows, 512 contiguous bytes each
+        for (uint32_t r = 0; r < valid; ++r)
+            reinterpret_cast<uint4*>(enc_out + (tile * 32 + r) * kEnc)[lane] =
+                reinterpret_cast<const uint4*>(enc + r * kEncLd)[lane];
+        float out[2][6][4];
+        mlp_forward_warp(enc, wf, out, ActStore{act, n_max * kWidth, (uint32_t)(tile * 32), valid});
+        __syncwarp();
         scatter_out(out, os);
         __syncwarp();
         if (row < n) {
@@ -385,8 +379,9 @@ constexpr int kDwChunk = 2048;
 constexpr int kDwStage = 64;
 constexpr int kDwLd = 72;  // padded bf16 row stride of the staged tiles
 
-__global__ void __launch_bounds__(kThreads) k_train_dw(const float* __restrict__ rec, const uint32_t* __restrict__ n_dev,
-                                                       size_t n_max, Box box, const __nv_bfloat16* __restrict__ act,
+__global__ void __launch_bounds__(kThreads) k_train_dw(const uint32_t* __restrict__ n_dev, size_t n_max,
+                                                       const __nv_bfloat16* __restrict__ enc,
+                                                       const __nv_bfloat16* __restrict__ act,
                                                        const __nv_bfloat16* __restrict__ delta,
                                                        const __nv_bfloat16* __restrict__ gout, float* __restrict__ grads) {
     __shared__ __align__(16) uint16_t Hs[kDwStage * kDwLd];
@@ -409,27 +404,15 @@ __global__ void __launch_bounds__(kThreads) k_train_dw(const float* __restrict__
         for (int r = 0; r < 4; ++r) acc[nt][r] = 0.0f;
     for (size_t s0 = c0; s0 < c1; s0 += kDwStage) {
         __syncthreads();
-        // stage H (64 records x 64 features) and D (64 records x N)
-        if (layer == 0) {
-            for (int i = threadIdx.x; i < kDwStage * 32; i += kThreads) {
-                const int r = i >> 5, cp = (i & 31) * 2;
-                const size_t row = s0 + r;
-                float a = 0.0f, b = 0.0f;
-                if (row < c1) {
-                    float x[kIn];
-                    normalise_input(rec + row * kRecordFloats, box.lo, box.inv_ext, x);
-                    enc_pair(x, 64 * job + cp, a, b);
-                }
-                *reinterpret_cast<uint32_t*>(&Hs[r * kDwLd + cp]) = pack_bf16(a, b);
-            }
-        } else {
-            for (int i = threadIdx.x; i < kDwStage * 8; i += kThreads) {
-                const int r = i >> 3, ch = i & 7;
-                const size_t row = s0 + r;
-                uint4 v = make_uint4(0, 0, 0, 0);
-                if (row < c1) v = *reinterpret_cast<const uint4*>(H + row * kWidth + ch * 8);
-                *reinterpret_cast<uint4*>(&Hs[r * kDwLd + ch * 8]) = v;
-            }
+        // stage H (64 records x 64 features; for W0 the job's 64 columns of the encodings) and D
+        const __nv_bfloat16* Hs_src = layer == 0 ? enc + 64 * job : H;
+        const int ldH = layer == 0 ? kEnc : kWidth;
+        for (int i = threadIdx.x; i < kDwStage * 8; i += kThreads) {
+            const int r = i >> 3, ch = i & 7;
+            const size_t row = s0 + r;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (row < c1) v = *reinterpret_cast<const uint4*>(Hs_src + row * ldH + ch * 8);
+            *reinterpret_cast<uint4*>(&Hs[r * kDwLd + ch * 8]) = v;
         }
         const int chunks = ldD / 8;
         for (int i = threadIdx.x; i < kDwStage * chunks; i += kThreads) {
@@ -505,15 +488,18 @@ int g_alloc(liar_gpu_ctx* ctx, liar_gpu_guide* G, size_t bytes, void** p, const 
 
 int ensure_train_buffers(liar_gpu_ctx* ctx, liar_gpu_guide* G, size_t n) {
     if (G->cap >= n) return LIAR_OK;
-    for (void* p : {(void*)G->act, (void*)G->delta, (void*)G->gout}) {
+    for (void* p : {(void*)G->enc, (void*)G->act, (void*)G->delta, (void*)G->gout}) {
         if (!p) continue;
         cudaFree(p);
         G->buffers.erase(std::remove(G->buffers.begin(), G->buffers.end(), p), G->buffers.end());
     }
-    G->act = G->delta = G->gout = nullptr;
+    G->enc = G->act = G->delta = G->gout = nullptr;
     G->cap = 0;
     void* p = nullptr;
-    int rc = g_alloc(ctx, G, n * 5 * kWidth * 2, &p, "guide activations");
+    int rc = g_alloc(ctx, G, n * kEnc * 2, &p, "guide encodings");
+    if (rc) return rc;
+    G->enc = static_cast<__nv_bfloat16*>(p);
+    rc = g_alloc(ctx, G, n * 5 * kWidth * 2, &p, "guide activations");
     if (rc) return rc;
     G->act = static_cast<__nv_bfloat16*>(p);
     rc = g_alloc(ctx, G, n * 5 * kWidth * 2, &p, "guide deltas");
@@ -578,12 +564,14 @@ int guide_train(liar_gpu_ctx* ctx, liar_gpu_guide* G, const float* d_records, co
     const int sms = ctx->num_sms;
     k_weight_sum<<<sms * 4, 256, 0, st>>>(d_records, d_count, n_max, G->scalars);
     const unsigned tiles = (unsigned)((n_max + 31) / 32);
+    const unsigned fgrid = std::max(1u, std::min<unsigned>((tiles + kFwdWarps - 1) / kFwdWarps, (unsigned)sms));
     const unsigned grid = std::max(1u, std::min<unsigned>((tiles + 3) / 4, (unsigned)sms * 2));
-    k_train_forward<<<grid, kThreads, kEvalSmem, st>>>(G->frag_fwd, d_records, d_count, n_max, box, G->scalars, G->act,
+    k_train_forward<<<fgrid, kFwdThreads, kEvalSmem, st>>>(G->frag_fwd, d_records, d_count, n_max, box, G->scalars, G->enc,
+                                                           G->act,
                                                         G->gout, G->scalars + 1);
     k_train_backward<<<grid, kThreads, kBwdBytes, st>>>(G->frag_bwd, d_count, n_max, G->act, G->gout, G->delta);
     const dim3 dwg((unsigned)((n_max + kDwChunk - 1) / kDwChunk), 9);
-    k_train_dw<<<dwg, kThreads, 0, st>>>(d_records, d_count, n_max, box, G->act, G->delta, G->gout, G->grads);
+    k_train_dw<<<dwg, kThreads, 0, st>>>(d_count, n_max, G->enc, G->act, G->delta, G->gout, G->grads);
     const float lr = apply ? (G->cfg.learning_rate > 0 ? G->cfg.learning_rate : 5e-3f) : 0.0f;
     k_adam<<<(kParams + 255) / 256, 256, 0, st>>>(G->params, G->grads, G->adam_m, G->adam_v, G->step, lr, 0.9f, 0.99f,
                                                   1e-8f, d_grad_out);
@@ -614,6 +602,8 @@ extern "C" int liar_gpu_guide_create(liar_gpu_ctx* ctx, const liar_guide_config*
             return ctx_fail(ctx, LIAR_ERR_INVALID, "guide bounds must be finite with hi > lo");
     if (cfg->guide_probability < 0.0f || cfg->guide_probability >= 1.0f)
         return ctx_fail(ctx, LIAR_ERR_INVALID, "guide_probability must lie in [0, 1)");
+    if (cfg->light_probability < 0.0f || cfg->light_probability >= 1.0f)
+        return ctx_fail(ctx, LIAR_ERR_INVALID, "light_probability must lie in [0, 1)");
     if (cfg->learning_rate < 0.0f || cfg->batch_records < 0 || cfg->steps_per_pass < 0)
         return ctx_fail(ctx, LIAR_ERR_INVALID, "negative learning rate, batch or step count");
     int rc = ctx_activate(ctx);
@@ -703,8 +693,9 @@ extern "C" int liar_gpu_guide_eval_device(liar_gpu_ctx* ctx, const liar_gpu_guid
     if (rc) return rc;
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
     const size_t tiles = (n + 31) / 32;
-    const unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>((tiles + 3) / 4, (size_t)ctx->num_sms * 2));
-    k_eval<<<grid, kThreads, kEvalSmem, st>>>(G->frag_fwd, d_inputs, n, make_box(G->cfg), d_mixture);
+    const unsigned grid =
+        (unsigned)std::max<size_t>(1, std::min<size_t>((tiles + kFwdWarps - 1) / kFwdWarps, (size_t)ctx->num_sms));
+    k_eval<<<grid, kFwdThreads, kEvalSmem, st>>>(G->frag_fwd, d_inputs, n, make_box(G->cfg), d_mixture);
     return ctx_cuda(ctx, cudaGetLastError(), "guide evaluation");
 }
 

@@ -70,31 +70,52 @@ __device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], 
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b.x), "r"(b.y));
 }
 
-// frequency f of the encoding: pi * 2^(f / 2), f = 0..11 (a half-octave ladder up to 45.25 pi:
-// features down to about a twentieth of the scene box, fine enough for radiance and coarse
-// enough to generalise from tens of thousands of training records)
-__device__ __forceinline__ float enc_scale(int f) {
-    const float s = (f & 1) ? 1.41421356237309515f : 1.0f;  // sqrt(2) rounded to float
-    return s * (float)(1 << (f >> 1));
-}
+// The encoding of one row, written by its lane into the warp's shared buffer (row stride kEncLd
+// bf16, padded so that the eight 16-byte rows an ldmatrix reads fall on distinct banks). Per input
+// two sincospif calls (pi x and pi x sqrt(2)); the other frequencies by the doubling formulas
+// sin 2a = 2 sin a cos a, cos 2a = cos^2 a - sin^2 a (x fl(sqrt 2) 2^k is exactly fl(x fl(sqrt 2)) 2^k,
+// so these are the angles of the definition; the recurrence adds ~1e-6 absolute error, far below bf16).
+constexpr int kEncLd = kEnc + 8;
+constexpr size_t kEncWarpBytes = (size_t)32 * kEncLd * 2;
 
-// the encoded features (c, c + 1) of one input row, c even
-__device__ __forceinline__ void enc_pair(const float* x, int c, float& a, float& b) {
-    if (c < kIn * 2 * kFreq) {
-        const int d = c / (2 * kFreq), f = (c % (2 * kFreq)) >> 1;
-        sincospif(x[d] * enc_scale(f), &a, &b);
-    } else if (c < kEncUsed) {
-        a = x[c - kIn * 2 * kFreq];
-        b = c + 1 < kEncUsed ? x[c + 1 - kIn * 2 * kFreq] : 0.0f;
-    } else {
-        a = b = 0.0f;
+__device__ __forceinline__ void encode_row(const float* x, __nv_bfloat16* row) {
+    uint32_t* dst = reinterpret_cast<uint32_t*>(row);
+#pragma unroll
+    for (int d = 0; d < kIn; ++d) {
+        float s0, c0, s1, c1;
+        sincospif(x[d], &s0, &c0);
+        sincospif(x[d] * 1.41421356237309515f, &s1, &c1);
+        uint32_t* w = dst + d * kFreq;  // pair index (d * 24 + 2 f) / 2
+#pragma unroll
+        for (int k = 0; k < kFreq / 2; ++k) {
+            w[2 * k] = pack_bf16(s0, c0);
+            w[2 * k + 1] = pack_bf16(s1, c1);
+            const float ns0 = 2.0f * s0 * c0, nc0 = c0 * c0 - s0 * s0;
+            const float ns1 = 2.0f * s1 * c1, nc1 = c1 * c1 - s1 * s1;
+            s0 = ns0;
+            c0 = nc0;
+            s1 = ns1;
+            c1 = nc1;
+        }
     }
+    uint32_t* raw = dst + kIn * kFreq;  // columns 216..255
+#pragma unroll
+    for (int c = 0; c < 4; ++c) raw[c] = pack_bf16(x[2 * c], x[2 * c + 1]);
+    raw[4] = pack_bf16(x[8], 0.0f);
+#pragma unroll
+    for (int c = 5; c < (kEnc - kIn * 2 * kFreq) / 2; ++c) raw[c] = 0u;
 }
 
-// one warp, 32 rows = two m16 tiles. xr[mt][h]: the 9 inputs of row 16 mt + g + 8 h
-// (g = lane / 4). Returns the output-layer accumulators acc[mt][nt][4] (6 n tiles of 8).
-// If h_out is given, stores the bf16 activations h_1..h_5 at h_out[(l-1) * ld_layer + row * 64 + col]
-// for rows < n_rows (row relative to the warp's first row).
+__device__ __forceinline__ void ldmatrix_x4(uint32_t (&r)[4], const void* smem_ptr) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(smem_ptr);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(a));
+}
+
+// one warp, 32 rows = two m16 tiles. enc: the warp's [32][kEncLd] bf16 encodings (encode_row).
+// Returns the output-layer accumulators out[mt][nt][4] (6 n tiles of 8). If S.base is set, stores
+// the bf16 activations h_1..h_5 at S.base[(l-1) * ld_layer + row * 64 + col] for valid rows.
 struct ActStore {
     __nv_bfloat16* base;  // null: no store
     size_t ld_layer;      // elements between layers
@@ -107,7 +128,7 @@ __device__ __forceinline__ void store_frag_row(const ActStore& S, int layer, uin
         *reinterpret_cast<uint32_t*>(S.base + (size_t)(layer - 1) * S.ld_layer + (size_t)(S.row0 + row) * kWidth + col) = v;
 }
 
-__device__ __forceinline__ void mlp_forward_warp(const float (&xr)[2][2][kIn], const uint2* __restrict__ wf,
+__device__ __forceinline__ void mlp_forward_warp(const __nv_bfloat16* enc, const uint2* __restrict__ wf,
                                                  float (&out)[2][6][4], const ActStore& S) {
     const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     float acc[2][8][4];
@@ -118,23 +139,14 @@ __device__ __forceinline__ void mlp_forward_warp(const float (&xr)[2][2][kIn], c
         for (int nt = 0; nt < 8; ++nt)
 #pragma unroll
             for (int r = 0; r < 4; ++r) acc[mt][nt][r] = 0.0f;
-    // layer 0: A fragments straight from the encoding
-#pragma unroll 1
+    // layer 0: A fragments by ldmatrix from the encodings (lane l addresses row l % 16, column
+    // half 8 (l / 16) of the 16 x 16 tile)
+    const __nv_bfloat16* arow = enc + (lane & 15) * kEncLd + 8 * (lane >> 4);
+#pragma unroll 2
     for (int kk = 0; kk < kEnc / 16; ++kk) {
         uint32_t a0[2][4];
-        const int c0 = 16 * kk + 2 * t, c1 = c0 + 8;
-#pragma unroll
-        for (int mt = 0; mt < 2; ++mt) {
-            float p, q;
-            enc_pair(xr[mt][0], c0, p, q);
-            a0[mt][0] = pack_bf16(p, q);
-            enc_pair(xr[mt][1], c0, p, q);
-            a0[mt][1] = pack_bf16(p, q);
-            enc_pair(xr[mt][0], c1, p, q);
-            a0[mt][2] = pack_bf16(p, q);
-            enc_pair(xr[mt][1], c1, p, q);
-            a0[mt][3] = pack_bf16(p, q);
-        }
+        ldmatrix_x4(a0[0], arow + 16 * kk);
+        ldmatrix_x4(a0[1], arow + 16 * kEncLd + 16 * kk);
         const uint2* wt = wf + (size_t)(kk * 8) * 32 + lane;
 #pragma unroll
         for (int nt = 0; nt < 8; ++nt) {
@@ -179,10 +191,8 @@ __device__ __forceinline__ void mlp_forward_warp(const float (&xr)[2][2][kIn], c
             for (int nt = 0; nt < 8; ++nt) {
                 if (nt < n_nt) {
                     const uint2 b = wl[(kk * n_nt + nt) * 32];
-                    uint32_t (&a0)[4] = a[0][kk];
-                    uint32_t (&a1)[4] = a[1][kk];
-                    mma_bf16(acc[0][nt], a0, b);
-                    mma_bf16(acc[1][nt], a1, b);
+                    mma_bf16(acc[0][nt], a[0][kk], b);
+                    mma_bf16(acc[1][nt], a[1][kk], b);
                 }
             }
     }

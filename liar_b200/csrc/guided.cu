@@ -2,17 +2,16 @@
 // technique, trained online on its own samples (no reference counterpart; the estimator without
 // the guide is src/liar/tracers/adjoint_photon_tracer.cpp:84-292, as in render.cu).
 //
-// Per pass (one sample per pixel): raygen -> per bounce [trace, shade]; the shade kernel is one
-// warp per 32 queue entries: hit context per lane, then (when the guide is on and a lane of the
-// warp sits on a diffuse or glossy surface) the guide network for the 32 vertices on the tensor
-// cores, then the scattering decision per lane:
+// Per wave of paths: raygen -> per bounce [trace, (guide inputs of the diffuse and glossy
+// vertices, guide network over the queue on the tensor cores), shade]; the shade kernel is one
+// thread per queue entry and reads its vertex's mixture when it makes the scattering decision:
 //   directional strategy (probability s = 0.5 at diffuse/glossy vertices): guide with probability
 //   c, else BSDF; density p_d = c q + (1 - c) p_bsdf
 //   light strategy (probability 1 - s): as the reference
 // weighted by the power heuristic between s p_d and (1 - s) p_light (one-sample MIS). With c = 0
 // every float operation is the one of render.cu, so the images agree to rounding.
 // Training records (vertex, direction, integrand / density) are written per scattering event and
-// completed when the pass ends: weight = (L_end - L_at_vertex) * p_chosen / (w_mis T_vertex p_mix),
+// completed when the wave ends: weight = (L_end - L_at_vertex) * p_chosen / (w_mis T_vertex p_mix),
 // the sampled integrand f cos L_in over the density p_mix of the whole one-sample mixture.
 #include <cuda_runtime.h>
 
@@ -73,8 +72,9 @@ struct GParams {
     liar_camera cam;
     int width, height, spp, max_gen, max_depth;
     uint64_t seed;
-    uint32_t sample;        // the pass: sample index of every pixel
+    uint64_t first_path;    // global index (pixel * spp + sample) of the wave's first path
     float guide_prob;       // c (0: guide off)
+    float light_prob;       // light-sampling share at guided vertices
     int train;
     float box_lo[3], box_inv[3];
     float* records;         // raw records
@@ -83,11 +83,12 @@ struct GParams {
     unsigned long long* stats;  // [0] paths [1] segments [2] hits [3] guided vertices
 };
 
-__device__ __forceinline__ SampleKey gkey(const GParams& W, uint32_t pixel) {
+__device__ __forceinline__ SampleKey gkey(const GParams& W, uint32_t slot) {
+    const uint64_t g = W.first_path + slot;
     SampleKey k;
     k.seed = W.seed;
-    k.pixel = pixel;
-    k.sample = W.sample;
+    k.pixel = (uint32_t)(g / (uint64_t)W.spp);
+    k.sample = (uint32_t)(g % (uint64_t)W.spp);
     k.spp = (uint32_t)W.spp;
     return k;
 }
@@ -148,27 +149,49 @@ __global__ void __launch_bounds__(256) k_g_raygen(DScene S, GParams W, GPaths P,
 }
 
 constexpr int kShadeThreads = 128;
-constexpr size_t kShadeSmem = kFwdBytes + 4 * (32 * kIn + 32 * kOutStride) * sizeof(float);
+
+// the guide's inputs for every queue entry that sits on a diffuse or glossy surface (position,
+// shading normal, direction to the previous vertex; zeros elsewhere)
+__global__ void __launch_bounds__(128) k_g_prep(DScene S, GQueue in, const liar_hit* __restrict__ hits, uint32_t n_in,
+                                                float* __restrict__ gin) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n_in) return;
+    float x[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const liar_hit h = hits[q];
+    if (h.prim >= 0) {
+        const float4 r0 = reinterpret_cast<const float4*>(in.rays + q)[0];
+        const float4 r1 = reinterpret_cast<const float4*>(in.rays + q)[1];
+        const int obj = S.tri_obj[h.prim];
+        const int mi = S.obj_mat[obj];
+        if (mi >= 0) {
+            const int type = S.mats[mi].type;
+            if (type == LIAR_MAT_LAMBERT || type == LIAR_MAT_COOK_TORRANCE || type == LIAR_MAT_WALTER) {
+                const HitContext HC = hit_context(S, mk(r0.x, r0.y, r0.z), mk(r1.x, r1.y, r1.z), (uint32_t)h.prim);
+                x[0] = HC.target.x;
+                x[1] = HC.target.y;
+                x[2] = HC.target.z;
+                x[3] = HC.N.x;
+                x[4] = HC.N.y;
+                x[5] = HC.N.z;
+                x[6] = -r1.x;
+                x[7] = -r1.y;
+                x[8] = -r1.z;
+            }
+        }
+    }
+    float* dst = gin + (size_t)q * 9;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) dst[c] = x[c];
+}
 
 __global__ void __launch_bounds__(kShadeThreads) k_g_shade(DScene S, GParams W, GPaths P, GQueue in,
                                                            const liar_hit* __restrict__ hits, uint32_t n_in, GQueue out,
-                                                           float* film, const uint2* __restrict__ frag) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    uint2* wf = reinterpret_cast<uint2*>(smem);
+                                                           float* film, const float* __restrict__ gmix) {
+    const int lane = threadIdx.x & 31;
     const bool guide_on = W.guide_prob > 0.0f;
-    if (guide_on) {
-        const uint4* s = reinterpret_cast<const uint4*>(frag);
-        uint4* d = reinterpret_cast<uint4*>(wf);
-        for (size_t i = threadIdx.x; i < kFwdBytes / 16; i += blockDim.x) d[i] = s[i];
-        __syncthreads();
-    }
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float* xs = reinterpret_cast<float*>(smem + kFwdBytes) + warp * (32 * kIn + 32 * kOutStride);
-    float* os = xs + 32 * kIn;
-    const uint32_t n_tiles = (n_in + 31) / 32;
     unsigned long long segs = 0, n_hit = 0, n_guided = 0;
-    for (uint32_t tile = blockIdx.x * 4 + warp; tile < n_tiles; tile += gridDim.x * 4) {
-        const uint32_t q = tile * 32 + lane;
+    {
+        const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
         const bool valid = q < n_in;
         uint32_t p = 0;
         float4 r0 = make_float4(0, 0, 0, 0), r1 = make_float4(0, 0, 1, 0);
@@ -193,52 +216,18 @@ __global__ void __launch_bounds__(kShadeThreads) k_g_shade(DScene S, GParams W, 
                 }
             }
         }
-        // ---- the guide network for the warp's vertices
+        // the guide's mixture at this vertex (computed by the network for the whole queue)
         float mix[kOutUsed];
-        const bool run_net = guide_on && __any_sync(0xffffffffu, guidable);
-        if (run_net) {
-            float x[kIn];
-            if (guidable) {
-                x[0] = (HC.target.x - W.box_lo[0]) * W.box_inv[0];
-                x[1] = (HC.target.y - W.box_lo[1]) * W.box_inv[1];
-                x[2] = (HC.target.z - W.box_lo[2]) * W.box_inv[2];
-                x[3] = HC.N.x;
-                x[4] = HC.N.y;
-                x[5] = HC.N.z;
-                x[6] = -r1.x;
-                x[7] = -r1.y;
-                x[8] = -r1.z;
-            } else {
-                for (int c = 0; c < kIn; ++c) x[c] = 0.0f;
+        if (guide_on && guidable) {
+            const float4* src = reinterpret_cast<const float4*>(gmix + (size_t)q * kOutUsed);
+#pragma unroll
+            for (int c = 0; c < kOutUsed / 4; ++c) {
+                const float4 v = src[c];
+                mix[4 * c] = v.x;
+                mix[4 * c + 1] = v.y;
+                mix[4 * c + 2] = v.z;
+                mix[4 * c + 3] = v.w;
             }
-            for (int c = 0; c < kIn; ++c) xs[lane * kIn + c] = x[c];
-            __syncwarp();
-            float xr[2][2][kIn];
-            const int g = lane >> 2;
-#pragma unroll
-            for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-                for (int hh = 0; hh < 2; ++hh)
-#pragma unroll
-                    for (int c = 0; c < kIn; ++c) xr[mt][hh][c] = xs[(16 * mt + g + 8 * hh) * kIn + c];
-            float o[2][6][4];
-            mlp_forward_warp(xr, wf, o, ActStore{nullptr, 0, 0, 0});
-            scatter_out(o, os);
-            __syncwarp();
-            if (guidable) {
-                Lobe lobes[kLobes];
-                float w[kLobes];
-                mixture_from_raw(os + lane * kOutStride, lobes, w);
-#pragma unroll
-                for (int l = 0; l < kLobes; ++l) {
-                    mix[4 * l] = lobes[l].mx;
-                    mix[4 * l + 1] = lobes[l].my;
-                    mix[4 * l + 2] = lobes[l].mz;
-                    mix[4 * l + 3] = lobes[l].kappa;
-                    mix[32 + l] = w[l];
-                }
-            }
-            __syncwarp();
         }
         // ---- shading (render.cu's k_shade with the guide as a third technique)
         bool want = false;
@@ -281,9 +270,10 @@ __global__ void __launch_bounds__(kShadeThreads) k_g_shade(DScene S, GParams W, 
                     wi.z = fmaxf(wi.z, kEps);
                     const bool strat = gen < W.max_gen;
                     const uint32_t base = DIM_GEN0 + DIMS_PER_GEN * (uint32_t)gen;
-                    const float strategy_pdf =
-                        (has_caps(B.caps, CAP_DIFF) || has_caps(B.caps, CAP_GLOSSY)) ? 0.5f : 1.0f;
-                    const float c = (guide_on && guidable && strategy_pdf < 1.0f) ? W.guide_prob : 0.0f;
+                    const bool smooth = has_caps(B.caps, CAP_DIFF) || has_caps(B.caps, CAP_GLOSSY);
+                    const bool guided = guide_on && guidable && smooth;
+                    const float strategy_pdf = smooth ? (guided ? 1.0f - W.light_prob : 0.5f) : 1.0f;
+                    const float c = guided ? W.guide_prob : 0.0f;
                     const uint32_t gbase = kDimGuide + 4u * (uint32_t)gen;
                     float3 wo = mk(0, 0, 1);
                     float3 wd = mk(0, 0, 1);
@@ -409,7 +399,7 @@ __global__ void __launch_bounds__(kShadeThreads) k_g_shade(DScene S, GParams W, 
                 want = true;
             } else {
                 P.L[p] = L;  // the radiance at the end of the path completes its training records
-                gsplat(S, film, p, lam, P.lam_pdf[p], L, P.alpha[p]);
+                gsplat(S, film, (uint32_t)((W.first_path + p) / (uint64_t)W.spp), lam, P.lam_pdf[p], L, P.alpha[p]);
             }
         }
         gqueue_push(out, want, nr, p);
@@ -442,7 +432,7 @@ __global__ void __launch_bounds__(kShadeThreads) k_g_shade(DScene S, GParams W, 
     }
 }
 
-// completes the pass's records: weight = (L_end - L_vertex) * scale; keeps the positive ones
+// completes the wave's records: weight = (L_end - L_vertex) * scale; keeps the positive ones
 __global__ void k_g_finalize(const float* __restrict__ raw, const uint32_t* __restrict__ raw_count, uint32_t raw_cap,
                              const float* __restrict__ L_end, float* __restrict__ train, uint32_t* train_count,
                              uint32_t train_cap) {
@@ -464,13 +454,15 @@ __global__ void k_g_finalize(const float* __restrict__ raw, const uint32_t* __re
 
 struct GuidedBuffers {
     size_t cap = 0;       // paths per wave
-    size_t rec_cap = 0;   // raw records per pass
+    size_t rec_cap = 0;   // raw records per wave
     void* mem = nullptr;
     GPaths P{};
     GQueue q[2]{};
     liar_hit* hits = nullptr;
     float* raw = nullptr;
     float* train = nullptr;
+    float* gin = nullptr;   // guide inputs per queue entry (9 floats)
+    float* gmix = nullptr;  // guide mixtures per queue entry (40 floats)
     uint32_t* counters = nullptr;            // [0] raw records [1] training records
     unsigned long long* stats = nullptr;     // [0..3]
     uint32_t* h_count = nullptr;             // pinned, 4 words
@@ -498,7 +490,7 @@ int ensure_guided_buffers(liar_gpu_ctx* ctx, GuidedBuffers* gb, size_t n, size_t
     if (gb->mem) cudaFree(gb->mem);
     gb->mem = nullptr;
     gb->cap = gb->rec_cap = 0;
-    const size_t bytes = n * (6 * 4 + 2 * (32 + 4) + 8) + rec_cap * (kRawRecord + kTrainRecord) * 4 + 4096;
+    const size_t bytes = n * (6 * 4 + 2 * (32 + 4) + 8 + (9 + kOutUsed) * 4) + rec_cap * (kRawRecord + kTrainRecord) * 4 + 8192;
     cudaError_t e = cudaMalloc(&gb->mem, bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -521,6 +513,8 @@ int ensure_guided_buffers(liar_gpu_ctx* ctx, GuidedBuffers* gb, size_t n, size_t
     gb->P.L = reinterpret_cast<float*>(take(n * 4));
     gb->P.alpha = reinterpret_cast<float*>(take(n * 4));
     gb->P.gen = reinterpret_cast<int32_t*>(take(n * 4));
+    gb->gin = reinterpret_cast<float*>(take(n * 9 * 4));
+    gb->gmix = reinterpret_cast<float*>(take(n * kOutUsed * 4));
     gb->raw = reinterpret_cast<float*>(take(rec_cap * kRawRecord * 4));
     gb->train = reinterpret_cast<float*>(take(rec_cap * kTrainRecord * 4));
     gb->q[0].count = reinterpret_cast<uint32_t*>(take(4));
@@ -531,8 +525,6 @@ int ensure_guided_buffers(liar_gpu_ctx* ctx, GuidedBuffers* gb, size_t n, size_t
     gb->rec_cap = rec_cap;
     return LIAR_OK;
 }
-
-int attrs_done_device = -1;
 
 }  // namespace
 
@@ -547,7 +539,15 @@ extern "C" int liar_gpu_render_guided_device(liar_gpu_ctx* ctx, const liar_gpu_s
     if (R.max_ray_generation < 0) return ctx_fail(ctx, LIAR_ERR_INVALID, "max_ray_generation must be >= 0");
     if (R.tracer != LIAR_TRACER_ADJOINT_PHOTON) return ctx_fail(ctx, LIAR_ERR_UNSUPPORTED, "tracer %d", R.tracer);
     const uint64_t npix = (uint64_t)R.width * R.height;
-    if (npix > (1ull << 26)) return ctx_fail(ctx, LIAR_ERR_INVALID, "guided rendering takes at most 2^26 pixels");
+    if (npix >= (1ull << 32)) return ctx_fail(ctx, LIAR_ERR_INVALID, "image too large");
+    const uint64_t total = npix * (uint64_t)R.spp;
+    // paths per wave: without training as many as fit (4M); when training, the guide learns after
+    // every wave, so a wave is a whole number of passes over the image, about 2M paths
+    uint64_t wave;
+    if (R.wave_paths > 0) wave = (uint64_t)R.wave_paths;
+    else if (train) wave = npix * std::max<uint64_t>(1, (1ull << 21) / npix);
+    else wave = 1ull << 22;
+    wave = std::min<uint64_t>(std::min<uint64_t>(wave, total), 1ull << 26);
     int rc = ctx_activate(ctx);
     if (rc) return rc;
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
@@ -556,13 +556,8 @@ extern "C" int liar_gpu_render_guided_device(liar_gpu_ctx* ctx, const liar_gpu_s
     const int steps = cfg.steps_per_pass > 0 ? cfg.steps_per_pass : 4;
     const size_t rec_cap = train ? std::max<size_t>((size_t)batch * steps, 1 << 16) : 0;
     GuidedBuffers* gb = guided_buffers(ctx);
-    rc = ensure_guided_buffers(ctx, gb, (size_t)npix, rec_cap);
+    rc = ensure_guided_buffers(ctx, gb, (size_t)wave, rec_cap);
     if (rc) return rc;
-    if (attrs_done_device != ctx->device) {
-        cudaError_t e = cudaFuncSetAttribute(k_g_shade, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kShadeSmem);
-        if (e != cudaSuccess) return ctx_cuda(ctx, e, "guided shade attributes");
-        attrs_done_device = ctx->device;
-    }
     cudaError_t e = cudaMemsetAsync(gb->stats, 0, 4 * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "reset statistics");
     GParams W;
@@ -584,20 +579,14 @@ extern "C" int liar_gpu_render_guided_device(liar_gpu_ctx* ctx, const liar_gpu_s
     W.stats = gb->stats;
     const DScene& S = scene_dscene(scene);
     const liar_gpu_mesh* mesh = scene_mesh(scene);
-    const uint32_t n = (uint32_t)npix;
-    // the shade kernel holds the guide's weights in shared memory only while the guide is sampled
-    int per_sm_guided = 0, per_sm_plain = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_guided, k_g_shade, kShadeThreads, kShadeSmem);
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_plain, k_g_shade, kShadeThreads, 0);
-    if (e != cudaSuccess) return ctx_cuda(ctx, e, "guided shade occupancy");
     unsigned long long records_total = 0;
-    for (int pass = 0; pass < R.spp; ++pass) {
-        W.sample = (uint32_t)pass;
-        // an untrained guide is not sampled: the first training pass renders with BSDF and lights only
+    for (uint64_t first = 0; first < total; first += wave) {
+        const uint32_t n = (uint32_t)std::min<uint64_t>(wave, total - first);
+        W.first_path = first;
+        // an untrained guide is not sampled: the first training wave renders with BSDF and lights only
         W.guide_prob = (train && guide_steps(guide) == 0) ? 0.0f : cfg.guide_probability;
+        W.light_prob = cfg.light_probability > 0.0f ? cfg.light_probability : 0.5f;
         const bool guide_on = W.guide_prob > 0.0f;
-        const size_t smem = guide_on ? kShadeSmem : 0;
-        const unsigned shade_grid = (unsigned)(ctx->num_sms * std::max(guide_on ? per_sm_guided : per_sm_plain, 1));
         e = cudaMemsetAsync(gb->q[0].count, 0, 4, st);
         if (e == cudaSuccess && train) e = cudaMemsetAsync(gb->counters, 0, 8, st);
         if (e != cudaSuccess) return ctx_cuda(ctx, e, "reset queue");
@@ -610,9 +599,14 @@ extern "C" int liar_gpu_render_guided_device(liar_gpu_ctx* ctx, const liar_gpu_s
             if (rc) return rc;
             e = cudaMemsetAsync(gb->q[cur ^ 1].count, 0, 4, st);
             if (e != cudaSuccess) return ctx_cuda(ctx, e, "reset queue");
-            const unsigned grid = std::min<unsigned>(shade_grid, (n_in + kShadeThreads - 1) / kShadeThreads);
-            k_g_shade<<<grid, kShadeThreads, smem, st>>>(S, W, gb->P, gb->q[cur], gb->hits, n_in, gb->q[cur ^ 1],
-                                                               d_film, guide_frag_fwd(guide));
+            if (guide_on) {
+                // the guide network over the queue's diffuse and glossy vertices
+                k_g_prep<<<(n_in + 127) / 128, 128, 0, st>>>(S, gb->q[cur], gb->hits, n_in, gb->gin);
+                rc = liar_gpu_guide_eval_device(ctx, guide, gb->gin, n_in, gb->gmix, st);
+                if (rc) return rc;
+            }
+            k_g_shade<<<(n_in + kShadeThreads - 1) / kShadeThreads, kShadeThreads, 0, st>>>(
+                S, W, gb->P, gb->q[cur], gb->hits, n_in, gb->q[cur ^ 1], d_film, gb->gmix);
             e = cudaGetLastError();
             if (e != cudaSuccess) return ctx_cuda(ctx, e, "guided shade launch");
             cur ^= 1;

@@ -15,7 +15,8 @@ INPUTS, MIXTURE, RECORD = 9, 40, 13
 
 class GuideConfig(C.Structure):
     _fields_ = [("bounds_lo", C.c_float * 3), ("bounds_hi", C.c_float * 3), ("learning_rate", C.c_float),
-                ("guide_probability", C.c_float), ("batch_records", C.c_int32), ("steps_per_pass", C.c_int32),
+                ("guide_probability", C.c_float), ("light_probability", C.c_float), ("batch_records", C.c_int32),
+                ("steps_per_pass", C.c_int32),
                 ("seed", C.c_uint64)]
 
 
@@ -45,13 +46,14 @@ def _stream(stream) -> C.c_void_p:
 
 class Guide:
     def __init__(self, ctx, bounds, learning_rate: float = 0.0, guide_probability: float = 0.5,
-                 batch_records: int = 0, steps_per_pass: int = 0, seed: int = 0):
+                 batch_records: int = 0, steps_per_pass: int = 0, seed: int = 0, light_probability: float = 0.0):
         self.ctx = ctx
         c = GuideConfig()
         c.bounds_lo[:] = [float(x) for x in bounds[0]]
         c.bounds_hi[:] = [float(x) for x in bounds[1]]
         c.learning_rate = float(learning_rate)
         c.guide_probability = float(guide_probability)
+        c.light_probability = float(light_probability)
         c.batch_records = int(batch_records)
         c.steps_per_pass = int(steps_per_pass)
         c.seed = int(seed) & 0xFFFFFFFFFFFFFFFF

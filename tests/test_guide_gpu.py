@@ -224,7 +224,7 @@ def test_guided_render_is_unbiased():
     gs = R.GpuScene(default_context(), flat)
     g = GD.Guide(default_context(), GD.scene_bounds(flat), guide_probability=0.5, learning_rate=5e-3,
                  steps_per_pass=4, batch_records=32768, seed=1)
-    warm = R.render_desc(cam, 64, 64, 8, _tracer(), seed=99)
+    warm = R.render_desc(cam, 64, 64, 8, _tracer(), seed=99, wave_paths=64 * 64)  # one pass per training round
     g.render(gs, warm, _film(warm).data_ptr(), train=True)
     st = g.stats()
     assert st["steps"] >= 8 * 4 - 4 and st["records"] > 0
@@ -248,7 +248,7 @@ def test_slit_room_guide_learns_the_slit():
     gs = R.GpuScene(default_context(), flat)
     g = GD.Guide(default_context(), GD.scene_bounds(flat), guide_probability=0.3, learning_rate=5e-3,
                  steps_per_pass=8, batch_records=65536, seed=0)
-    train_d = R.render_desc(cam, 256, 256, 32, _tracer(), seed=7)
+    train_d = R.render_desc(cam, 256, 256, 32, _tracer(), seed=7, wave_paths=256 * 256)
     g.render(gs, train_d, _film(train_d).data_ptr(), train=True)
     assert g.stats()["records"] > 20000
     rng = np.random.default_rng(0)
