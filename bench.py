@@ -563,6 +563,42 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_case(name: str) -> None:
+    """Small single-kernel workloads for profiling captures (ncu -k ... python bench.py --case NAME):
+    guide-eval (the guide network over 1M random vertices, 3 launches), direct (DirectLighting on
+    the Cornell frame, 256^2 x 4 spp, twice), shade (the Cornell path-tracing frame, twice),
+    gather (k = 64 over 4M uniform photons for 256k uniform queries, twice)."""
+    import torch
+    from liar_b200.kernel import default_context
+    ctx = default_context()
+    if name == "guide-eval":
+        from liar_b200 import guiding as GD
+        g = GD.Guide(ctx, (np.array([-1, -1, -1], np.float32), np.array([1, 1, 1], np.float32)))
+        x = torch.rand((1 << 20, 9), device="cuda", generator=torch.Generator("cuda").manual_seed(0)) * 2 - 1
+        for _ in range(3):
+            g.eval(x)
+    elif name in ("direct", "shade"):
+        from liar_b200 import render as R, scenes_render, tracers
+        e = scenes_render.cornell_engine(256, 256, 16)
+        gs = R.GpuScene(ctx, R.flatten(e.scene))
+        film = torch.zeros((256, 256, 8), device="cuda")
+        d = (R.render_desc(e.camera, 256, 256, 4, tracers.DirectLighting()) if name == "direct"
+             else R.render_desc(e.camera, 256, 256, 16, e.tracer))
+        for _ in range(2):
+            gs.render_device(d, film.data_ptr())
+    elif name == "gather":
+        from liar_b200 import photons as PH
+        rng = np.random.default_rng(0)
+        m = PH.PhotonMap(ctx, rng.random((1 << 22, 3)).astype(np.float32), 0.02)
+        q = rng.random((1 << 18, 3)).astype(np.float32)
+        for _ in range(2):
+            m.gather(q, 64)
+    else:
+        raise SystemExit(f"unknown case {name}")
+    torch.cuda.synchronize()
+    print(json.dumps({"case": name, "ok": True}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -575,7 +611,10 @@ def main():
     ap.add_argument("--only", default="", help="comma list of workloads to run (cornell,photon,batch,guided); default all")
     ap.add_argument("--guided-res", type=int, default=1024, help="image side of the guiding workload")
     ap.add_argument("--guided-ref-spp", type=int, default=4096, help="samples per pixel of its plain reference")
+    ap.add_argument("--case", default="", help="run one small profiling workload instead (see run_case)")
     args = ap.parse_args()
+    if args.case:
+        return run_case(args.case)
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world, rank, local = dist_setup()
     if args.impl == "reference":

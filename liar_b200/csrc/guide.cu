@@ -19,6 +19,7 @@
 #include "../../include/liar_gpu.h"
 #include "ctx.h"
 #include "guide_mlp.cuh"
+#include "guide_umma.cuh"
 #include "sampler.h"
 
 using namespace liar_gpu;
@@ -34,6 +35,8 @@ struct liar_gpu_guide {
     uint32_t* step = nullptr;  // Adam step count (device)
     uint2* frag_fwd = nullptr;
     uint2* frag_bwd = nullptr;
+    unsigned char* umma_w = nullptr;  // B-operand images of the six layers for the tcgen05 inference
+    uint32_t* status = nullptr;       // device status word of the tcgen05 inference (bounded waits)
     // training scratch, sized for cap records
     size_t cap = 0;
     __nv_bfloat16* enc = nullptr;    // h_0 (the encodings): [cap][256]
@@ -131,9 +134,22 @@ __global__ void k_pack(const float* __restrict__ P, uint2* __restrict__ fwd, uin
     }
 }
 
+// the tcgen05 B operands: layer l's element (n, k) = W_l[k][n] at umma_offset(n, k, K_l)
+__global__ void k_pack_umma(const float* __restrict__ P, unsigned char* __restrict__ img) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;  // one parameter (k, n) per thread
+    if (i >= kParams) return;
+    int l = 0;
+    while (l < 5 && i >= param_offset(l + 1)) ++l;
+    const int loc = i - param_offset(l), N = layer_n(l), K = layer_k(l);
+    const int k = loc / N, n = loc % N;
+    *reinterpret_cast<__nv_bfloat16*>(img + umma_w_offset(l) + umma_offset((uint32_t)n, (uint32_t)k, (uint32_t)K)) =
+        __float2bfloat16_rn(P[i]);
+}
+
 int launch_pack(liar_gpu_guide* G, cudaStream_t st, int bump) {
     const int total = (kFwdTiles + kBwdTiles) * 32;
     k_pack<<<(total + 255) / 256, 256, 0, st>>>(G->params, G->frag_fwd, G->frag_bwd, G->step, bump);
+    k_pack_umma<<<(kParams + 255) / 256, 256, 0, st>>>(G->params, G->umma_w);
     return cudaGetLastError() == cudaSuccess ? LIAR_OK : LIAR_ERR_CUDA;
 }
 
@@ -144,40 +160,110 @@ __device__ __forceinline__ void load_frags(uint2* dst, const uint2* __restrict__
     __syncthreads();
 }
 
-// ---- inference: raw inputs [n][9] -> mixtures [n][40] = 8 x (mu xyz, kappa), then 8 weights
-__global__ void __launch_bounds__(kFwdThreads) k_eval(const uint2* __restrict__ frag, const float* __restrict__ in,
-                                                      size_t n, Box box, float* __restrict__ mix) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    uint2* wf = reinterpret_cast<uint2*>(smem);
-    load_frags(wf, frag, kFwdBytes);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    __nv_bfloat16* enc = reinterpret_cast<__nv_bfloat16*>(smem + kFwdBytes + warp * kEncWarpBytes);
-    float* os = reinterpret_cast<float*>(enc);
-    const size_t n_tiles = (n + 31) / 32;
-    for (size_t tile = (size_t)blockIdx.x * kFwdWarps + warp; tile < n_tiles; tile += (size_t)gridDim.x * kFwdWarps) {
-        const size_t row = tile * 32 + lane;
+// ---- inference on tcgen05: two slots of 128 rows per CTA (guide_umma.cuh)
+__global__ void __launch_bounds__(kTcThreads, 1) k_eval_tc(const unsigned char* __restrict__ w_img,
+                                                           const float* __restrict__ in, size_t n, Box box,
+                                                           float* __restrict__ mix, uint32_t* __restrict__ status) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    unsigned char* sw = smem;
+    uint64_t* mbar_all = reinterpret_cast<uint64_t*>(sw + kUmmaWBytes + (size_t)kTcSlots * kUmmaA0Bytes);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar_all + kTcSlots);
+    volatile uint32_t* failed = tmem_slot + 1;  // one flag per slot
+    const uint32_t tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t slot = tid >> 7, r = tid & 127u;  // this thread's slot and row within the slot's tile
+    unsigned char* buf = sw + kUmmaWBytes + slot * kUmmaA0Bytes;
+    {
+        const uint4* s = reinterpret_cast<const uint4*>(w_img);
+        uint4* d = reinterpret_cast<uint4*>(sw);
+        for (uint32_t i = tid; i < kUmmaWBytes / 16; i += kTcThreads) d[i] = s[i];
+    }
+    if (tid == 0) {
+        for (int k = 0; k < kTcSlots; ++k)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(mbar_all + k)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        failed[0] = failed[1] = 0u;
+    }
+    if (warp == 0) {
+        const uint32_t sa = (uint32_t)__cvta_generic_to_shared(tmem_slot);
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sa), "r"(kTcTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot + 64u * slot;                 // the slot's accumulator columns
+    const uint32_t taddr = tmem + ((32u * (warp & 3u)) << 16);     // the warp's lane quarter
+    const uint32_t mbar_addr = (uint32_t)__cvta_generic_to_shared(mbar_all + slot);
+    const uint32_t sw_addr = (uint32_t)__cvta_generic_to_shared(sw);
+    const uint32_t buf_addr = (uint32_t)__cvta_generic_to_shared(buf);
+    auto slot_sync = [&]() { asm volatile("bar.sync %0, 128;" ::"r"(1u + slot) : "memory"); };
+    constexpr uint32_t kMaxTries = 1u << 24;
+    uint32_t phase = 0;
+    const size_t n_tiles = (n + kTcRows - 1) / kTcRows;
+    for (size_t tile = (size_t)blockIdx.x * kTcSlots + slot; tile < n_tiles; tile += (size_t)gridDim.x * kTcSlots) {
+        const size_t row = tile * kTcRows + r;
         float x[kIn];
         if (row < n) normalise_input(in + row * kIn, box.lo, box.inv_ext, x);
         else
             for (int c = 0; c < kIn; ++c) x[c] = 0.0f;
-        encode_row(x, enc + lane * kEncLd);
-        __syncwarp();
-        float out[2][6][4];
-        mlp_forward_warp(enc, wf, out, ActStore{nullptr, 0, 0, 0});
-        __syncwarp();
-        scatter_out(out, os);
-        __syncwarp();
+        encode_row_umma(x, buf, r);
+        float v[64];
+        bool ok = true;
+        for (int l = 0; l < kLayers; ++l) {
+            // the layer's A operand is in shared memory and the slot's last accumulator reads are
+            // done: hand the operand to the tensor core
+            fence_async_smem();
+            tc_fence_before();
+            slot_sync();
+            tc_fence_after();
+            if (r == 0) {
+                const uint32_t K = (uint32_t)layer_k(l), N = (uint32_t)layer_n(l);
+                const uint32_t b_base = sw_addr + umma_w_offset(l);
+                const uint32_t idesc = umma_idesc(N);
+                for (uint32_t j = 0; j < K / 16; ++j)
+                    umma_bf16(tmem, umma_smem_desc(buf_addr + 256u * j, (K / 8) * 128u),
+                              umma_smem_desc(b_base + 256u * j, (K / 8) * 128u), idesc, j > 0 ? 1u : 0u);
+                umma_commit(mbar_addr);
+            }
+            if (!mbar_wait(mbar_addr, phase, kMaxTries)) failed[slot] = 1u;
+            phase ^= 1u;
+            slot_sync();  // the slot agrees on completion before anyone reads the accumulator
+            if (failed[slot]) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            tmem_ld_x64(taddr, v);
+            if (l < kLayers - 1) {
+                // ReLU, bf16, the next layer's A operand (row r, 8 chunks of 8 columns) in the slot's
+                // buffer, whose encodings the finished layer-0 MMA no longer needs
+                unsigned char* dst = buf + (r >> 3) * (kWidth / 8) * 128u + (r & 7u) * 16u;
+#pragma unroll
+                for (int c = 0; c < kWidth / 8; ++c) {
+                    const float* q = v + 8 * c;
+                    *reinterpret_cast<uint4*>(dst + c * 128u) =
+                        make_uint4(pack_bf16(fmaxf(q[0], 0.0f), fmaxf(q[1], 0.0f)), pack_bf16(fmaxf(q[2], 0.0f), fmaxf(q[3], 0.0f)),
+                                   pack_bf16(fmaxf(q[4], 0.0f), fmaxf(q[5], 0.0f)), pack_bf16(fmaxf(q[6], 0.0f), fmaxf(q[7], 0.0f)));
+                }
+            }
+        }
+        if (!ok) break;
         if (row < n) {
             Lobe lobes[kLobes];
             float w[kLobes];
-            mixture_from_raw(os + lane * kOutStride, lobes, w);
+            mixture_from_raw(v, lobes, w);
             float4* dst = reinterpret_cast<float4*>(mix + row * kOutUsed);
             for (int l = 0; l < kLobes; ++l) dst[l] = make_float4(lobes[l].mx, lobes[l].my, lobes[l].mz, lobes[l].kappa);
             dst[8] = make_float4(w[0], w[1], w[2], w[3]);
             dst[9] = make_float4(w[4], w[5], w[6], w[7]);
         }
-        __syncwarp();
     }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tmem_slot), "r"(kTcTmemCols));
+    if (tid == 0 && (failed[0] | failed[1])) atomicOr(status, kStatusTimeout);
 }
 
 // ---- training
@@ -515,11 +601,11 @@ int ensure_train_buffers(liar_gpu_ctx* ctx, liar_gpu_guide* G, size_t n) {
 int smem_attrs(liar_gpu_ctx* ctx) {
     static int done_device = -1;
     if (done_device == ctx->device) return LIAR_OK;
-    cudaError_t e = cudaFuncSetAttribute(k_eval, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEvalSmem);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_train_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEvalSmem);
+    cudaError_t e = cudaFuncSetAttribute(k_train_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEvalSmem);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_train_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBwdBytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_eval_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUmmaSmem);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "guide kernel attributes");
     done_device = ctx->device;
     return LIAR_OK;
@@ -627,6 +713,14 @@ extern "C" int liar_gpu_guide_create(liar_gpu_ctx* ctx, const liar_guide_config*
     if (!rc) G->frag_fwd = static_cast<uint2*>(p);
     if (!rc) rc = g_alloc(ctx, G, kBwdBytes, &p, "guide fragments");
     if (!rc) G->frag_bwd = static_cast<uint2*>(p);
+    if (!rc) rc = g_alloc(ctx, G, kUmmaWBytes, &p, "guide operand images");
+    if (!rc) G->umma_w = static_cast<unsigned char*>(p);
+    if (!rc) rc = g_alloc(ctx, G, 16, &p, "guide status");
+    if (!rc) {
+        G->status = static_cast<uint32_t*>(p);
+        cudaError_t e = cudaMemset(G->status, 0, 16);
+        if (e != cudaSuccess) rc = ctx_cuda(ctx, e, "guide status");
+    }
     if (!rc) {
         std::vector<float> P;
         init_params(P, cfg->seed);
@@ -692,10 +786,10 @@ extern "C" int liar_gpu_guide_eval_device(liar_gpu_ctx* ctx, const liar_gpu_guid
     rc = smem_attrs(ctx);
     if (rc) return rc;
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
-    const size_t tiles = (n + 31) / 32;
-    const unsigned grid =
-        (unsigned)std::max<size_t>(1, std::min<size_t>((tiles + kFwdWarps - 1) / kFwdWarps, (size_t)ctx->num_sms));
-    k_eval<<<grid, kFwdThreads, kEvalSmem, st>>>(G->frag_fwd, d_inputs, n, make_box(G->cfg), d_mixture);
+    // inference: raw inputs [n][9] -> mixtures [n][40] = 8 x (mu xyz, kappa), then the 8 weights
+    const size_t tiles = (n + kTcRows - 1) / kTcRows;
+    const unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>((tiles + kTcSlots - 1) / kTcSlots, (size_t)ctx->num_sms));
+    k_eval_tc<<<grid, kTcThreads, kUmmaSmem, st>>>(G->umma_w, d_inputs, n, make_box(G->cfg), d_mixture, G->status);
     return ctx_cuda(ctx, cudaGetLastError(), "guide evaluation");
 }
 

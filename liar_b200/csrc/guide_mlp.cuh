@@ -4,9 +4,11 @@
 // previous vertex) -> frequency encoding (per input: sin and cos of pi * 2^(f/2) * x, f = 0..11, then
 // the 9 raw inputs; 225 features, padded to 256) -> 5 ReLU layers of 64 -> 48 outputs (40 used):
 // 8 von Mises-Fisher lobes, each (mean direction m 3, log concentration 1, logit 1). No biases.
-// Weights are bf16, accumulation f32 (mma.sync m16n8k16); activations stay in registers between
-// layers: the f32 accumulator fragment of two adjacent 8-column tiles is, element for element, the
-// A fragment of the next layer's 16-column k tile, so a layer costs no shared-memory round trip.
+// Weights are bf16, accumulation f32. Inference runs on tcgen05 (guide_umma.cuh); the training
+// forward and backward here run per warp on mma.sync m16n8k16, with the activations in registers
+// between layers: the f32 accumulator fragment of two adjacent 8-column tiles is, element for
+// element, the A fragment of the next layer's 16-column k tile (no shared-memory round trip), and
+// the bf16 activations are stored for the backward pass.
 //
 // Parameters (f32 master copy, row-major [in][out]): W0 256x64, W1..W4 64x64, W5 64x48.
 // For the kernels they are repacked as bf16 B fragments in lane order ("fwd": B = W_l,

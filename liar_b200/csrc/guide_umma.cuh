@@ -1,0 +1,157 @@
+// guide_umma.cuh -- the guide network's inference on the 5th-generation tensor cores (tcgen05).
+//
+// A CTA runs two independent 4-warp slots, each evaluating 128 rows at a time (M = 128; thread r
+// of the slot owns row r), so that one slot's SIMT work overlaps the other's tensor-core work.
+//   * the weights live in shared memory as the B operands of every layer, bf16, K-major, in the
+//     canonical no-swizzle layout: element (n, k) of a layer with K inputs at
+//     (n / 8) * (K / 8) * 128 + (k / 8) * 128 + (n % 8) * 16 + (k % 8) * 2 bytes, i.e. 8x16-byte core
+//     matrices with the K-adjacent ones 128 B apart (leading byte offset) and the 8-row groups
+//     (K / 8) * 128 B apart (stride byte offset);
+//   * the activations (A operands) use the same layout: 128 x 256 for the encodings, 128 x 64 for
+//     the hidden layers;
+//   * a slot's accumulator is 128 lanes x 64 f32 columns of tensor memory; its thread 0 issues each layer
+//     as K / 16 tcgen05.mma (kind::f16, bf16 inputs, f32 accumulation) and commits them to an
+//     mbarrier; every warp then reads its 32 lanes (tcgen05.ld 32x32b.x64), applies ReLU, and
+//     writes the next layer's A operand back to shared memory.
+// Every wait on the mbarrier is bounded; on a timeout the CTA records kStatusTimeout, frees its
+// tensor memory and returns.
+#pragma once
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include "guide_mlp.cuh"
+
+namespace liar_gpu {
+namespace guide {
+
+constexpr int kTcRows = 128;
+constexpr int kTcSlots = 2;                    // tiles in flight per CTA, one per 4-warp slot
+constexpr int kTcThreads = 128 * kTcSlots;
+constexpr uint32_t kTcTmemCols = 64 * kTcSlots;  // slot s accumulates in columns [64 s, 64 s + 64)
+
+// B-operand images of the six layers (bytes from the start of the image)
+__host__ __device__ constexpr uint32_t umma_w_offset(int l) {
+    return l == 0 ? 0u : (l <= 5 ? 32768u + 8192u * (uint32_t)(l - 1) : 32768u + 4u * 8192u + 6144u);
+}
+constexpr uint32_t kUmmaWBytes = umma_w_offset(6);  // 71680
+constexpr uint32_t kUmmaA0Bytes = (uint32_t)kTcRows * kEnc * 2;    // 65536
+constexpr uint32_t kUmmaA1Bytes = (uint32_t)kTcRows * kWidth * 2;  // 16384
+// per slot one operand buffer: the encodings for layer 0, then (once layer 0 has finished) the
+// hidden activations in its first kUmmaA1Bytes
+constexpr size_t kUmmaSmem = 1024 + kUmmaWBytes + (size_t)kTcSlots * kUmmaA0Bytes + 128;
+
+// byte offset of element (row, k) in a K-major no-swizzle operand with K columns
+__host__ __device__ __forceinline__ uint32_t umma_offset(uint32_t row, uint32_t k, uint32_t K) {
+    return (row >> 3) * (K >> 3) * 128u + (k >> 3) * 128u + (row & 7u) * 16u + (k & 7u) * 2u;
+}
+
+#ifdef __CUDACC__
+
+// shared-memory matrix descriptor: start >> 4 [0,14), leading byte offset >> 4 [16,30),
+// stride byte offset >> 4 [32,46), version 1 [46,48), no swizzle [61,64)
+__device__ __forceinline__ uint64_t umma_smem_desc(uint32_t smem_addr, uint32_t sbo_bytes) {
+    return (uint64_t)((smem_addr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) |
+           ((uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// instruction descriptor of kind::f16: f32 accumulator, bf16 A and B, both K-major, N, M = 128
+__host__ __device__ constexpr uint32_t umma_idesc(uint32_t n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((uint32_t)(kTcRows >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t"
+        "}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t mbar_addr) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar_addr)
+                 : "memory");
+}
+
+// bounded wait for the mbarrier phase: true when it completed
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar_addr, uint32_t phase, uint32_t max_tries) {
+    for (uint32_t i = 0; i < max_tries; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t"
+            ".reg .pred P1;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t"
+            "}"
+            : "=r"(done)
+            : "r"(mbar_addr), "r"(phase)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tmem_ld_x64(uint32_t taddr, float (&v)[64]) {
+    uint32_t r[64];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x64.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,"
+        "%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,"
+        "%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]),
+          "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]),
+          "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]),
+          "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]),
+          "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 64; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// the encodings of row r into the 128 x 256 A operand: per input 12 sin/cos pairs = 3 chunks of
+// 16 bytes (angle doubling as encode_row), then the raw inputs and zero padding
+__device__ __forceinline__ void encode_row_umma(const float* x, unsigned char* a0, uint32_t r) {
+    unsigned char* row = a0 + (r >> 3) * (kEnc / 8) * 128u + (r & 7u) * 16u;
+#pragma unroll
+    for (int d = 0; d < kIn; ++d) {
+        float s0, c0, s1, c1;
+        sincospif(x[d], &s0, &c0);
+        sincospif(x[d] * 1.41421356237309515f, &s1, &c1);
+        uint32_t w[12];
+#pragma unroll
+        for (int k = 0; k < kFreq / 2; ++k) {
+            w[2 * k] = pack_bf16(s0, c0);
+            w[2 * k + 1] = pack_bf16(s1, c1);
+            const float ns0 = 2.0f * s0 * c0, nc0 = c0 * c0 - s0 * s0;
+            const float ns1 = 2.0f * s1 * c1, nc1 = c1 * c1 - s1 * s1;
+            s0 = ns0;
+            c0 = nc0;
+            s1 = ns1;
+            c1 = nc1;
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            *reinterpret_cast<uint4*>(row + (3 * d + c) * 128u) = make_uint4(w[4 * c], w[4 * c + 1], w[4 * c + 2], w[4 * c + 3]);
+    }
+    *reinterpret_cast<uint4*>(row + 27 * 128u) =
+        make_uint4(pack_bf16(x[0], x[1]), pack_bf16(x[2], x[3]), pack_bf16(x[4], x[5]), pack_bf16(x[6], x[7]));
+    *reinterpret_cast<uint4*>(row + 28 * 128u) = make_uint4(pack_bf16(x[8], 0.0f), 0u, 0u, 0u);
+#pragma unroll
+    for (int c = 29; c < kEnc / 8; ++c) *reinterpret_cast<uint4*>(row + c * 128u) = make_uint4(0u, 0u, 0u, 0u);
+}
+
+#endif  // __CUDACC__
+
+}  // namespace guide
+}  // namespace liar_gpu
