@@ -102,6 +102,26 @@ def dist_setup():
     return world, rank, local
 
 
+def replica_seed(rank: int) -> int:
+    """Replicas trace their own ray sets: rank k draws the workload's rays with seed k."""
+    return rank
+
+
+def max_over_ranks(ms: float, world: int, dist, device) -> float:
+    """A timed region's duration as the slowest rank saw it (one all-reduce, MAX)."""
+    if world <= 1:
+        return ms
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world: int, units_per_rank: int, ms: float) -> float:
+    """Units of all ranks over the slowest rank's time, per second (weak scaling: fixed units per rank)."""
+    return world * units_per_rank / (ms * 1e-3)
+
+
 def cpu_baseline_rays(v, f, rays, target_seconds=10.0):
     """Times the oracle tree on a bounded sample of the workload's rays (about target_seconds of
     CPU work on all host threads); returns (Mrays/s, info)."""
@@ -146,10 +166,7 @@ def cornell_bench(ctx, stream, args, world, dist, local, cpu: bool) -> dict:
     e1.record(stream)
     stream.synchronize()
     ms = e0.elapsed_time(e1) / steps
-    if world > 1:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, world, dist, f"cuda:{local}")
     st = gs.stats()
     out = {"workload": "Cornell box 256x256, 16 spp, single wavelength, RR from generation 3, max depth 8",
            "ms_per_frame": ms, "samples_per_s": world * st["paths"] / (ms * 1e-3),
@@ -169,10 +186,7 @@ def cornell_bench(ctx, stream, args, world, dist, local, cpu: bool) -> dict:
     e1.record(stream)
     stream.synchronize()
     dms = e0.elapsed_time(e1) / dsteps
-    if world > 1:
-        t = torch.tensor([dms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dms = float(t.item())
+    dms = max_over_ranks(dms, world, dist, f"cuda:{local}")
     out["direct_lighting"] = {"ms_per_frame": dms, "samples_per_s": world * W * H * SPP / (dms * 1e-3),
                               "shadow_rays_per_sample": 32,
                               "shadow_rays_per_s": world * W * H * SPP * 32 / (dms * 1e-3)}
@@ -227,10 +241,7 @@ def batch_bench(ctx, stream, args, world, dist, local, cpu: bool, n_scenes: int 
     e1.record(stream)
     stream.synchronize()
     ms = e0.elapsed_time(e1) / steps
-    if world > 1:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, world, dist, f"cuda:{local}")
     st = br.stats()
     tris = [w.n_triangles for w in work]
     out = {"workload": f"{n_scenes} procedural scenes, {min(tris)}-{max(tris)} triangles ({sum(tris)} total), "
@@ -636,7 +647,7 @@ def main():
             dist.barrier()
 
     v, f = scenes.displaced_icosphere(LEVELS, seed=0)
-    rays = scenes.random_rays(v, N_RAYS, seed=rank)
+    rays = scenes.random_rays(v, N_RAYS, seed=replica_seed(rank))
     ctx = Context(local)
     mesh = Mesh(ctx, v, f)
     stats = mesh.stats
@@ -691,12 +702,7 @@ def main():
         ctx.synchronize()
         torch.cuda.synchronize()
         barrier()
-        ms_ = e0.elapsed_time(e1) / steps
-        if world > 1:
-            t = torch.tensor([ms_], device=f"cuda:{local}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms_ = float(t.item())
-        return ms_
+        return max_over_ranks(e0.elapsed_time(e1) / steps, world, dist, f"cuda:{local}")
 
     e2e_steps = max(1, min(args.steps, 20))
     with ClockSampler(local) as clocks:
@@ -704,8 +710,8 @@ def main():
         ms_any = timed(step_any, args.steps)
         e2e_s = timed(e2e_step, e2e_steps) * 1e-3
     del d_rays_any
-    value = world * N_RAYS / (ms * 1e-3) / 1e6
-    e2e_val = world * N_RAYS / e2e_s / 1e6
+    value = whole_job_rate(world, N_RAYS, ms) / 1e6
+    e2e_val = whole_job_rate(world, N_RAYS, e2e_s * 1e3) / 1e6
 
     peaks = load_peaks()
     per_ray_model = 128.0 * nodes_visited / N_RAYS + 48.0 * tris_tested / N_RAYS + 40.0
