@@ -578,7 +578,8 @@ def run_case(name: str) -> None:
     """Small single-kernel workloads for profiling captures (ncu -k ... python bench.py --case NAME):
     guide-eval (the guide network over 1M random vertices, 3 launches), direct (DirectLighting on
     the Cornell frame, 256^2 x 4 spp, twice), shade (the Cornell path-tracing frame, twice),
-    gather (k = 64 over 4M uniform photons for 256k uniform queries, twice)."""
+    gather (k = 64 over 4M uniform photons for 256k uniform queries, twice), guided (the slit
+    room at 256^2: 4 training passes, then 16 guided samples per pixel)."""
     import torch
     from liar_b200.kernel import default_context
     ctx = default_context()
@@ -597,6 +598,18 @@ def run_case(name: str) -> None:
              else R.render_desc(e.camera, 256, 256, 16, e.tracer))
         for _ in range(2):
             gs.render_device(d, film.data_ptr())
+    elif name == "guided":
+        from liar_b200 import guiding as GD, render as R, scenes_guiding as SG
+        scene, cam = SG.slit_room(200_000)
+        flat = R.flatten(scene)
+        gs = R.GpuScene(ctx, flat)
+        g = GD.Guide(ctx, GD.scene_bounds(flat), guide_probability=0.7, light_probability=0.1, learning_rate=5e-3,
+                     steps_per_pass=4, batch_records=16384, seed=0)
+        film = torch.zeros((256, 256, 8), device="cuda")
+        d = R.render_desc(cam, 256, 256, 4, SG.guiding_tracer(), seed=1)
+        d.wave_paths = 256 * 256
+        g.render(gs, d, film.data_ptr(), train=True)
+        g.render(gs, R.render_desc(cam, 256, 256, 16, SG.guiding_tracer(), seed=2), film.data_ptr(), train=False)
     elif name == "gather":
         from liar_b200 import photons as PH
         rng = np.random.default_rng(0)

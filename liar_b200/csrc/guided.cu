@@ -12,7 +12,10 @@
 // every float operation is the one of render.cu, so the images agree to rounding.
 // Training records (vertex, direction, integrand / density) are written per scattering event and
 // completed when the wave ends: weight = (L_end - L_at_vertex) * p_chosen / (w_mis T_vertex p_mix),
-// the sampled integrand f cos L_in over the density p_mix of the whole one-sample mixture.
+// the sampled integrand f cos L_in over the density p_mix of the whole one-sample mixture. Paths
+// are numbered sample-major, so a training wave of whole passes covers the whole image; when the
+// record buffer cannot hold every candidate, a random subset is kept; the records with a positive
+// weight are stride-permuted before the Adam steps so that each batch mixes all generations.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -72,25 +75,36 @@ struct GParams {
     liar_camera cam;
     int width, height, spp, max_gen, max_depth;
     uint64_t seed;
-    uint64_t first_path;    // global index (pixel * spp + sample) of the wave's first path
+    uint64_t first_path;    // global index (sample * pixels + pixel) of the wave's first path
+    uint32_t npix;
     float guide_prob;       // c (0: guide off)
     float light_prob;       // light-sampling share at guided vertices
     int train;
+    float rec_keep;         // probability that a candidate training record is kept
     float box_lo[3], box_inv[3];
     float* records;         // raw records
-    uint32_t* rec_count;
+    uint32_t* rec_count;    // [0] kept records [2] candidates
     uint32_t rec_cap;
     unsigned long long* stats;  // [0] paths [1] segments [2] hits [3] guided vertices
 };
 
+// Paths are numbered sample-major: a run of npix consecutive paths is one sample of every pixel,
+// so a training wave of whole passes sees the whole image.
 __device__ __forceinline__ SampleKey gkey(const GParams& W, uint32_t slot) {
     const uint64_t g = W.first_path + slot;
     SampleKey k;
     k.seed = W.seed;
-    k.pixel = (uint32_t)(g / (uint64_t)W.spp);
-    k.sample = (uint32_t)(g % (uint64_t)W.spp);
+    k.pixel = (uint32_t)(g % (uint64_t)W.npix);
+    k.sample = (uint32_t)(g / (uint64_t)W.npix);
     k.spp = (uint32_t)W.spp;
     return k;
+}
+
+// a uniform number in [0, 1) per (path, generation) that decides whether a candidate training
+// record is kept: the kept records are an unbiased thinning of all of the wave's vertices
+__device__ __forceinline__ float record_lottery(const GParams& W, uint32_t slot, int gen) {
+    const uint64_t h = mix64(W.seed ^ mix64(((W.first_path + slot) << 8) | (uint64_t)(gen & 0xff)) ^ 0x7f4a7c159e3779b9ull);
+    return (float)(h >> 40) * (1.0f / 16777216.0f);
 }
 
 __device__ __forceinline__ void gqueue_push(const GQueue& q, bool want, const liar_ray& r, uint32_t path) {
@@ -232,7 +246,7 @@ __global__ void __launch_bounds__(kShadeThreads) k_g_shade(DScene S, GParams W, 
         // ---- shading (render.cu's k_shade with the guide as a third technique)
         bool want = false;
         liar_ray nr{};
-        bool rec_want = false;
+        bool rec_want = false, rec_cand = false;
         float rec[kRawRecord];
         if (valid) {
             ++segs;
@@ -359,7 +373,8 @@ __global__ void __launch_bounds__(kShadeThreads) k_g_shade(DScene S, GParams W, 
                         next_tmin = kTol;
                         next_tmax = INFINITY;
                         if (W.train && guidable && strategy_pdf < 1.0f && T > 0.0f && w_mis > 0.0f && p_mix > 0.0f) {
-                            rec_want = true;
+                            rec_cand = true;
+                            rec_want = record_lottery(W, p, gen) < W.rec_keep;
                             rec[0] = target.x;
                             rec[1] = target.y;
                             rec[2] = target.z;
@@ -399,11 +414,13 @@ __global__ void __launch_bounds__(kShadeThreads) k_g_shade(DScene S, GParams W, 
                 want = true;
             } else {
                 P.L[p] = L;  // the radiance at the end of the path completes its training records
-                gsplat(S, film, (uint32_t)((W.first_path + p) / (uint64_t)W.spp), lam, P.lam_pdf[p], L, P.alpha[p]);
+                gsplat(S, film, (uint32_t)((W.first_path + p) % (uint64_t)W.npix), lam, P.lam_pdf[p], L, P.alpha[p]);
             }
         }
         gqueue_push(out, want, nr, p);
         // training records, one atomic per warp
+        const uint32_t cmask = __ballot_sync(0xffffffffu, rec_cand);
+        if (cmask && (uint32_t)lane == __ffs(cmask) - 1) atomicAdd(W.rec_count + 2, (uint32_t)__popc(cmask));
         const uint32_t rmask = __ballot_sync(0xffffffffu, rec_want);
         if (rmask) {
             const uint32_t leader = __ffs(rmask) - 1;
@@ -452,6 +469,18 @@ __global__ void k_g_finalize(const float* __restrict__ raw, const uint32_t* __re
     }
 }
 
+// out[(i * A) mod m] = in[i]: a stride permutation of the training records (A prime and > m, so it
+// is a bijection), which spreads every batch over all generations of the wave; the raw records are
+// in order of generation
+__global__ void k_g_shuffle(const float* __restrict__ in, float* __restrict__ out, uint32_t m, uint32_t A) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        const uint32_t j = (uint32_t)(((uint64_t)i * A) % m);
+        const float* s = in + (size_t)i * kTrainRecord;
+        float* d = out + (size_t)j * kTrainRecord;
+        for (int c = 0; c < kTrainRecord; ++c) d[c] = s[c];
+    }
+}
+
 struct GuidedBuffers {
     size_t cap = 0;       // paths per wave
     size_t rec_cap = 0;   // raw records per wave
@@ -461,9 +490,10 @@ struct GuidedBuffers {
     liar_hit* hits = nullptr;
     float* raw = nullptr;
     float* train = nullptr;
+    float* shuffled = nullptr;  // the training records in stride-permuted order
     float* gin = nullptr;   // guide inputs per queue entry (9 floats)
     float* gmix = nullptr;  // guide mixtures per queue entry (40 floats)
-    uint32_t* counters = nullptr;            // [0] raw records [1] training records
+    uint32_t* counters = nullptr;            // [0] raw records [1] training records [2] candidates
     unsigned long long* stats = nullptr;     // [0..3]
     uint32_t* h_count = nullptr;             // pinned, 4 words
 };
@@ -490,7 +520,8 @@ int ensure_guided_buffers(liar_gpu_ctx* ctx, GuidedBuffers* gb, size_t n, size_t
     if (gb->mem) cudaFree(gb->mem);
     gb->mem = nullptr;
     gb->cap = gb->rec_cap = 0;
-    const size_t bytes = n * (6 * 4 + 2 * (32 + 4) + 8 + (9 + kOutUsed) * 4) + rec_cap * (kRawRecord + kTrainRecord) * 4 + 8192;
+    const size_t bytes =
+        n * (6 * 4 + 2 * (32 + 4) + 8 + (9 + kOutUsed) * 4) + rec_cap * (kRawRecord + 2 * kTrainRecord) * 4 + 8192;
     cudaError_t e = cudaMalloc(&gb->mem, bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -517,9 +548,10 @@ int ensure_guided_buffers(liar_gpu_ctx* ctx, GuidedBuffers* gb, size_t n, size_t
     gb->gmix = reinterpret_cast<float*>(take(n * kOutUsed * 4));
     gb->raw = reinterpret_cast<float*>(take(rec_cap * kRawRecord * 4));
     gb->train = reinterpret_cast<float*>(take(rec_cap * kTrainRecord * 4));
+    gb->shuffled = reinterpret_cast<float*>(take(rec_cap * kTrainRecord * 4));
     gb->q[0].count = reinterpret_cast<uint32_t*>(take(4));
     gb->q[1].count = reinterpret_cast<uint32_t*>(take(4));
-    gb->counters = reinterpret_cast<uint32_t*>(take(8));
+    gb->counters = reinterpret_cast<uint32_t*>(take(16));
     gb->stats = reinterpret_cast<unsigned long long*>(take(4 * 8));
     gb->cap = n;
     gb->rec_cap = rec_cap;
@@ -554,7 +586,12 @@ extern "C" int liar_gpu_render_guided_device(liar_gpu_ctx* ctx, const liar_gpu_s
     const liar_guide_config& cfg = guide_config(guide);
     const uint32_t batch = cfg.batch_records > 0 ? (uint32_t)cfg.batch_records : 65536u;
     const int steps = cfg.steps_per_pass > 0 ? cfg.steps_per_pass : 4;
-    const size_t rec_cap = train ? std::max<size_t>((size_t)batch * steps, 1 << 16) : 0;
+    // raw records: room for about 2.5 candidates per path (at most 2^25 records); only the records
+    // whose path found light after the vertex train the guide, usually a few percent, so every
+    // candidate is kept while the buffer has room, and when it has not, a random subset (the keep
+    // probability follows the previous wave's candidates per path, with 20% slack)
+    const size_t rec_cap = train ? std::min<size_t>(std::max<size_t>((size_t)wave * 5 / 2, (size_t)batch * steps), 1ull << 25) : 0;
+    const size_t rec_target = rec_cap - rec_cap / 5;
     GuidedBuffers* gb = guided_buffers(ctx);
     rc = ensure_guided_buffers(ctx, gb, (size_t)wave, rec_cap);
     if (rc) return rc;
@@ -568,6 +605,7 @@ extern "C" int liar_gpu_render_guided_device(liar_gpu_ctx* ctx, const liar_gpu_s
     W.max_gen = R.max_ray_generation;
     W.max_depth = R.max_depth;
     W.seed = mix64(R.seed ^ mix64(0x51ed270b27ad0e0dull + (uint64_t)(uint32_t)R.first_sample));
+    W.npix = (uint32_t)npix;
     W.train = train ? 1 : 0;
     for (int k = 0; k < 3; ++k) {
         W.box_lo[k] = cfg.bounds_lo[k];
@@ -580,15 +618,17 @@ extern "C" int liar_gpu_render_guided_device(liar_gpu_ctx* ctx, const liar_gpu_s
     const DScene& S = scene_dscene(scene);
     const liar_gpu_mesh* mesh = scene_mesh(scene);
     unsigned long long records_total = 0;
+    double candidates_per_path = 2.0;
     for (uint64_t first = 0; first < total; first += wave) {
         const uint32_t n = (uint32_t)std::min<uint64_t>(wave, total - first);
         W.first_path = first;
+        W.rec_keep = (float)std::min(1.0, (double)rec_target / ((double)n * candidates_per_path));
         // an untrained guide is not sampled: the first training wave renders with BSDF and lights only
         W.guide_prob = (train && guide_steps(guide) == 0) ? 0.0f : cfg.guide_probability;
         W.light_prob = cfg.light_probability > 0.0f ? cfg.light_probability : 0.5f;
         const bool guide_on = W.guide_prob > 0.0f;
         e = cudaMemsetAsync(gb->q[0].count, 0, 4, st);
-        if (e == cudaSuccess && train) e = cudaMemsetAsync(gb->counters, 0, 8, st);
+        if (e == cudaSuccess && train) e = cudaMemsetAsync(gb->counters, 0, 12, st);
         if (e != cudaSuccess) return ctx_cuda(ctx, e, "reset queue");
         k_g_raygen<<<(n + 255) / 256, 256, 0, st>>>(S, W, gb->P, gb->q[0], n);
         uint32_t n_in = n;
@@ -618,16 +658,20 @@ extern "C" int liar_gpu_render_guided_device(liar_gpu_ctx* ctx, const liar_gpu_s
         if (train) {
             k_g_finalize<<<ctx->num_sms * 4, 256, 0, st>>>(gb->raw, gb->counters, (uint32_t)rec_cap, gb->P.L, gb->train,
                                                            gb->counters + 1, (uint32_t)rec_cap);
-            e = cudaMemcpyAsync(gb->h_count, gb->counters, 8, cudaMemcpyDeviceToHost, st);
+            e = cudaMemcpyAsync(gb->h_count, gb->counters, 12, cudaMemcpyDeviceToHost, st);
             if (e == cudaSuccess) e = cudaStreamSynchronize(st);
             if (e != cudaSuccess) return ctx_cuda(ctx, e, "training records");
             const uint32_t n_train = std::min<uint32_t>(gb->h_count[1], (uint32_t)rec_cap);
+            if (gb->h_count[2] > 0) candidates_per_path = (double)gb->h_count[2] / (double)n;
             records_total += n_train;
             if (n_train > 0) {
+                k_g_shuffle<<<ctx->num_sms * 4, 256, 0, st>>>(gb->train, gb->shuffled, n_train, 2147483647u);
+                e = cudaGetLastError();
+                if (e != cudaSuccess) return ctx_cuda(ctx, e, "shuffle launch");
                 for (int s = 0; s < steps; ++s) {
                     const uint32_t first = (uint32_t)(((uint64_t)s * batch) % n_train);
                     const uint32_t cnt = std::min<uint32_t>(batch, n_train - first);
-                    rc = guide_train(ctx, guide, gb->train + (size_t)first * kTrainRecord, nullptr, cnt, 1, nullptr,
+                    rc = guide_train(ctx, guide, gb->shuffled + (size_t)first * kTrainRecord, nullptr, cnt, 1, nullptr,
                                      nullptr, st);
                     if (rc) return rc;
                 }
