@@ -121,6 +121,16 @@ class _Builder:
         self.materials, self.mat_ids = [], {}
         self.spectra, self.spec_ids, self.pool = [], {}, []
         self.lights = []
+        self.M = None  # current local-to-world affine matrix (None: identity)
+
+    # -- transformations (scenery/transformation.cpp, translation.cpp)
+    def point(self, p) -> np.ndarray:
+        p = np.asarray(p, dtype=np.float64)
+        return p if self.M is None else p @ self.M[:3, :3].T + self.M[:3, 3]
+
+    def vector(self, v) -> np.ndarray:
+        v = np.asarray(v, dtype=np.float64)
+        return v if self.M is None else v @ self.M[:3, :3].T
 
     # -- spectra
     def spectrum(self, x, reflectant_hint=False) -> int:
@@ -213,6 +223,17 @@ class _Builder:
     # -- geometry
     def geometry(self, obj, shader, light: int) -> tuple[int, int]:
         v, t, n, tn = obj.triangles()
+        if self.M is not None:
+            v = self.point(v).astype(np.float32)
+            if n is not None:
+                nn = np.asarray(n, dtype=np.float64) @ np.linalg.inv(self.M[:3, :3])  # inverse transpose
+                n = (nn / np.maximum(np.linalg.norm(nn, axis=1, keepdims=True), 1e-300)).astype(np.float32)
+            if np.linalg.det(self.M[:3, :3]) < 0:
+                # a mirroring transformation: keep the geometric normal the transformed local one,
+                # as the reference transforms the local context's normal
+                t = np.asarray(t)[:, [0, 2, 1]]
+                if tn is not None:
+                    tn = np.asarray(tn)[:, [0, 2, 1]]
         obj_index = len(self.obj_mat)
         self.obj_mat.append(self.material(shader))
         self.obj_light.append(light)
@@ -235,6 +256,14 @@ class _Builder:
         if isinstance(obj, scenery.List):
             for c in obj.children:
                 self.visit(c, obj.shader or inherited)
+        elif isinstance(obj, (scenery.Transformation, scenery.Translation)):
+            saved = self.M
+            local = obj.matrix()
+            self.M = local if saved is None else saved @ local
+            try:
+                self.visit(obj.child, obj.shader or inherited)
+            finally:
+                self.M = saved
         elif isinstance(obj, scenery.LightArea):
             surf = obj.surface
             li = len(self.lights)
@@ -246,8 +275,11 @@ class _Builder:
             L.object = len(self.obj_mat) - 1
             if isinstance(surf, scenery.Parallelogram):
                 L.type = LIGHT_PARA
-                L.pos[:], L.u[:], L.v[:] = surf.support, surf.sizeU, surf.sizeV
-                area = surf.area
+                pos, u, v = self.point(surf.support), self.vector(surf.sizeU), self.vector(surf.sizeV)
+                if self.M is not None and np.linalg.det(self.M[:3, :3]) < 0:
+                    u, v = v, u  # the same surface, facing like its (re-wound) triangles
+                L.pos[:], L.u[:], L.v[:] = (tuple(float(x) for x in a) for a in (pos, u, v))
+                area = float(np.linalg.norm(np.cross(u, v)))
             else:
                 L.type = LIGHT_MESH
                 L.first_tri, L.n_tris = first, count
@@ -263,7 +295,7 @@ class _Builder:
             L.object = -1
             L.emission_samples = int(obj.numberOfEmissionSamples)
             L.spectrum = self.spectrum(obj.intensity)
-            L.pos[:] = obj.position
+            L.pos[:] = tuple(float(x) for x in self.point(obj.position))
             L.power = 4 * math.pi * as_spectrum(obj.intensity).luminance  # LightPoint::doTotalPower
             self.lights.append(L)
         elif isinstance(obj, scenery.LightSky):

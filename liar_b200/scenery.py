@@ -121,6 +121,117 @@ class Sphere(SceneObject):
         return verts, f.astype(np.uint32), v.astype(np.float32), f.astype(np.int32)
 
 
+class Box(SceneObject):
+    """Box(), Box((min, max)) or Box(min, max) (scenery/box.cpp; the default is [-1, 1]^3),
+    flattened into 12 outward-wound triangles."""
+
+    def __init__(self, *args):
+        super().__init__()
+        if not args:
+            lo, hi = (-1.0, -1.0, -1.0), (1.0, 1.0, 1.0)
+        elif len(args) == 1:
+            lo, hi = args[0]
+        elif len(args) == 2:
+            lo, hi = args
+        else:
+            raise TypeError("Box(), Box((min, max)) or Box(min, max)")
+        self.min = tuple(float(x) for x in lo)
+        self.max = tuple(float(x) for x in hi)
+
+    @property
+    def bounds(self):
+        return (self.min, self.max)
+
+    @bounds.setter
+    def bounds(self, value):
+        self.min, self.max = (tuple(float(x) for x in v) for v in value)
+
+    def triangles(self):
+        lo, hi = np.asarray(self.min, dtype=np.float64), np.asarray(self.max, dtype=np.float64)
+        # corner k = (x bit 0, y bit 1, z bit 2)
+        corners = np.array([[hi[0] if k & 1 else lo[0], hi[1] if k & 2 else lo[1], hi[2] if k & 4 else lo[2]]
+                            for k in range(8)], dtype=np.float32)
+        quads = [(0, 4, 6, 2), (1, 3, 7, 5),   # -x, +x
+                 (0, 1, 5, 4), (2, 6, 7, 3),   # -y, +y
+                 (0, 2, 3, 1), (4, 5, 7, 6)]   # -z, +z
+        tris = []
+        for a, b, c, d in quads:
+            tris += [(a, b, c), (a, c, d)]
+        return corners, np.asarray(tris, dtype=np.uint32), None, None
+
+
+def as_matrix(m) -> np.ndarray:
+    """A 4 x 4 float64 affine matrix from a 4 x 4 or 3 x 4 nested sequence (row-major, the last
+    column the translation), 16 or 12 numbers, or an object with a `matrix` attribute."""
+    if hasattr(m, "matrix"):
+        m = m.matrix
+    a = np.asarray(m, dtype=np.float64)
+    if a.size == 16:
+        a = a.reshape(4, 4)
+    elif a.size == 12:
+        a = np.vstack([a.reshape(3, 4), [0.0, 0.0, 0.0, 1.0]])
+    else:
+        raise ValueError("a transformation is a 4 x 4 or 3 x 4 matrix")
+    if not np.allclose(a[3], [0.0, 0.0, 0.0, 1.0]):
+        raise ValueError("only affine transformations are supported (last row 0, 0, 0, 1)")
+    return a
+
+
+class Transformation(SceneObject):
+    """Transformation(child, localToWorld) (scenery/transformation.cpp): the child in a local frame.
+    The flattening applies localToWorld to the child's vertices and light geometry and the inverse
+    transpose to its normals."""
+
+    def __init__(self, child, localToWorld):
+        super().__init__()
+        self.child = child
+        self.localToWorld = localToWorld
+
+    @property
+    def localToWorld(self) -> np.ndarray:
+        return self._m
+
+    @localToWorld.setter
+    def localToWorld(self, m):
+        a = as_matrix(m)
+        if abs(np.linalg.det(a[:3, :3])) < 1e-300:
+            raise ValueError("singular transformation")
+        self._m = a
+
+    @property
+    def worldToLocal(self) -> np.ndarray:
+        return np.linalg.inv(self._m)
+
+    def matrix(self) -> np.ndarray:
+        return self._m
+
+
+class Translation(SceneObject):
+    """Translation(child, offset) (scenery/translation.cpp): localToWorld is the offset vector."""
+
+    def __init__(self, child, localToWorld=(0.0, 0.0, 0.0)):
+        super().__init__()
+        self.child = child
+        self.localToWorld = localToWorld
+
+    @property
+    def localToWorld(self):
+        return self._t
+
+    @localToWorld.setter
+    def localToWorld(self, v):
+        self._t = tuple(float(x) for x in v)
+
+    @property
+    def worldToLocal(self):
+        return tuple(-x for x in self._t)
+
+    def matrix(self) -> np.ndarray:
+        a = np.eye(4)
+        a[:3, 3] = self._t
+        return a
+
+
 class SceneLight(SceneObject):
     pass
 
