@@ -224,15 +224,26 @@ typedef struct liar_render_desc {
     int32_t wave_paths;          /* paths in flight per wave, 0 = automatic */
     int32_t secondary_light_samples; /* DirectLighting.numberOfSecondaryLightSamples (0 = 1) */
     int32_t trace_glossy;        /* DirectLighting.traceGlossy: -1 = false, otherwise true */
+    /* reconstruction filter between the tracer and the film (a RenderTarget wrapper in the
+     * reference): LIAR_FILTER_BOX = the sample's own pixel with weight 1 (Raster alone),
+     * LIAR_FILTER_TRIANGLE = FilterTriangle (output/filter_triangle.cpp:100-145, 169),
+     * LIAR_FILTER_MITCHELL = FilterMitchell (output/filter_mitchell.cpp:84-150) */
+    int32_t filter;
+    float filter_param;          /* triangle: width (0 = 1); Mitchell: B (0 = 1/3) */
+    float max_sample_luminance;  /* Raster.maxSampleLuminance (output/raster.cpp:572-575); 0 = no clamp */
 } liar_render_desc;
+
+enum liar_filter { LIAR_FILTER_BOX = 0, LIAR_FILTER_TRIANGLE = 1, LIAR_FILTER_MITCHELL = 2 };
 
 /* Uploads the scene (builds the triangle tree). */
 int liar_gpu_scene_upload(liar_gpu_ctx* ctx, const liar_scene_desc* desc, liar_gpu_scene** out);
 void liar_gpu_scene_destroy(liar_gpu_scene* scene);
 /* Renders `spp` samples per pixel (AdjointPhotonTracer, src/liar/tracers/adjoint_photon_tracer.cpp:84-292,
  * driven like RenderEngine::render, src/liar/kernel/render_engine.cpp:170-358) and ADDS them to
- * film: width x height x 8 floats = sums of X, Y, Z, alpha, X^2, Y^2, Z^2 and the sample count
- * (the reference's Raster accumulation, src/liar/output/raster.cpp:547-606, before division). */
+ * film: width x height x 8 floats = sums of w a X, w a Y, w a Z, w a, w X^2, w Y^2, w Z^2 and w
+ * over the samples that reach the pixel, w the filter weight (1 for the box filter) and a the
+ * sample's alpha (the reference's Raster accumulation, src/liar/output/raster.cpp:547-606, before
+ * division: the pixel is the first four sums over the last). */
 int liar_gpu_render(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_render_desc* desc, float* film);
 /* Same on a device film buffer, asynchronous on `stream`. */
 int liar_gpu_render_device(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_render_desc* desc,

@@ -39,7 +39,7 @@ struct BItem {
     int width, height, spp, max_gen, max_depth;
     uint64_t seed;
     uint64_t path_begin;
-    float* film;
+    FilmSpec film;
     liar_camera cam;
 };
 
@@ -145,15 +145,12 @@ __device__ void bsplat(const DScene& S, const BItem& it, uint64_t local, const f
             xyz = xyz + mk(s * c.x, s * c.y, s * c.z);
         }
     }
-    float* f = it.film + 8 * (size_t)(local / (uint64_t)it.spp);
-    atomicAdd(f + 0, xyz.x);
-    atomicAdd(f + 1, xyz.y);
-    atomicAdd(f + 2, xyz.z);
-    atomicAdd(f + 3, alpha);
-    atomicAdd(f + 4, xyz.x * xyz.x);
-    atomicAdd(f + 5, xyz.y * xyz.y);
-    atomicAdd(f + 6, xyz.z * xyz.z);
-    atomicAdd(f + 7, 1.0f);
+    SampleKey k;
+    k.seed = it.seed;
+    k.pixel = (uint32_t)(local / (uint64_t)it.spp);
+    k.sample = (uint32_t)(local % (uint64_t)it.spp);
+    k.spp = (uint32_t)it.spp;
+    film_splat(it.film, k, xyz, alpha);
 }
 
 template <int H>
@@ -665,7 +662,11 @@ extern "C" int liar_gpu_batch_create(liar_gpu_ctx* ctx, const liar_batch_item* i
         h.max_gen = R.max_ray_generation;
         h.max_depth = R.max_depth;
         h.seed = mix64(R.seed ^ mix64(0x51ed270b27ad0e0dull + (uint64_t)(uint32_t)R.first_sample));
-        h.film = it.d_film;
+        h.film = film_spec(it.d_film, R);
+        if (const char* m = film_desc_error(R)) {
+            delete b;
+            return ctx_fail(ctx, LIAR_ERR_INVALID, "batch item %zu: %s", i, m);
+        }
         h.cam = R.camera;
         h.path_begin = begin[i];
         begin[i + 1] = begin[i] + (uint64_t)R.width * R.height * R.spp;

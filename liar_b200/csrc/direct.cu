@@ -75,6 +75,7 @@ struct DParams {
     int n_secondary;
     uint32_t glossy;  // CAP_GLOSSY when glossy reflection/transmission is traced
     unsigned long long* stats;
+    FilmSpec film;
 };
 
 // sampler dimensions (disjoint from the path tracer's and from each other)
@@ -378,10 +379,9 @@ __global__ void k_dl_shadow_add(DShadows sh, uint32_t n, const liar_hit* __restr
     if (v != 0.0f && hits[i].prim < 0) atomicAdd(&L[sh.slot[i]], v);
 }
 
-__global__ void k_dl_splat(DScene S, DParams W, DSamples P, uint32_t n, float* film) {
+__global__ void k_dl_splat(DScene S, DParams W, DSamples P, uint32_t n) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const uint32_t pixel = (uint32_t)((W.first_path + i) / (uint64_t)W.spp);
     const float lam_pdf = P.lam_pdf[i], L = P.L[i];
     float3 xyz = mk(0, 0, 0);
     if (lam_pdf > 0.0f) {
@@ -389,15 +389,7 @@ __global__ void k_dl_splat(DScene S, DParams W, DSamples P, uint32_t n, float* f
         const float3 c = observer_sensitivity(S, P.lam[i]);
         xyz = mk(s * c.x, s * c.y, s * c.z);
     }
-    float* f = film + 8 * (size_t)pixel;
-    atomicAdd(f + 0, xyz.x);
-    atomicAdd(f + 1, xyz.y);
-    atomicAdd(f + 2, xyz.z);
-    atomicAdd(f + 3, P.alpha[i]);
-    atomicAdd(f + 4, xyz.x * xyz.x);
-    atomicAdd(f + 5, xyz.y * xyz.y);
-    atomicAdd(f + 6, xyz.z * xyz.z);
-    atomicAdd(f + 7, 1.0f);
+    film_splat(W.film, dkey(W, W.first_path + i), xyz, P.alpha[i]);
 }
 
 struct DirectBuffers {
@@ -503,6 +495,7 @@ int render_direct(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_ren
     W.width = R.width;
     W.height = R.height;
     W.spp = R.spp;
+    W.film = film_spec(d_film, R);
     W.max_gen = R.max_ray_generation;
     W.seed = mix64(R.seed ^ mix64(0x51ed270b27ad0e0dull + (uint64_t)(uint32_t)R.first_sample));
     W.n_secondary = n_sec;
@@ -575,7 +568,7 @@ int render_direct(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_ren
             cur ^= 1;
             n_in = b->h_counters[cur];
         }
-        k_dl_splat<<<(n + 255) / 256, 256, 0, st>>>(S, W, P, n, d_film);
+        k_dl_splat<<<(n + 255) / 256, 256, 0, st>>>(S, W, P, n);
         e = cudaGetLastError();
         if (e != cudaSuccess) return ctx_cuda(ctx, e, "direct lighting splat");
     }

@@ -86,6 +86,7 @@ struct GParams {
     uint32_t* rec_count;    // [0] kept records [2] candidates
     uint32_t rec_cap;
     unsigned long long* stats;  // [0] paths [1] segments [2] hits [3] guided vertices
+    FilmSpec film;
 };
 
 // Paths are numbered sample-major: a run of npix consecutive paths is one sample of every pixel,
@@ -124,22 +125,14 @@ __device__ __forceinline__ void gqueue_push(const GQueue& q, bool want, const li
     }
 }
 
-__device__ void gsplat(const DScene& S, float* film, uint32_t pixel, float lam, float lam_pdf, float L, float alpha) {
+__device__ void gsplat(const DScene& S, const GParams& W, uint32_t slot, float lam, float lam_pdf, float L, float alpha) {
     float3 xyz = mk(0, 0, 0);
     if (lam_pdf > 0.0f) {
         const float s = L / lam_pdf;
         const float3 c = observer_sensitivity(S, lam);
         xyz = mk(s * c.x, s * c.y, s * c.z);
     }
-    float* f = film + 8 * (size_t)pixel;
-    atomicAdd(f + 0, xyz.x);
-    atomicAdd(f + 1, xyz.y);
-    atomicAdd(f + 2, xyz.z);
-    atomicAdd(f + 3, alpha);
-    atomicAdd(f + 4, xyz.x * xyz.x);
-    atomicAdd(f + 5, xyz.y * xyz.y);
-    atomicAdd(f + 6, xyz.z * xyz.z);
-    atomicAdd(f + 7, 1.0f);
+    film_splat(W.film, gkey(W, slot), xyz, alpha);
 }
 
 __global__ void __launch_bounds__(256) k_g_raygen(DScene S, GParams W, GPaths P, GQueue out, uint32_t n) {
@@ -200,7 +193,7 @@ __global__ void __launch_bounds__(128) k_g_prep(DScene S, GQueue in, const liar_
 
 __global__ void __launch_bounds__(kShadeThreads) k_g_shade(DScene S, GParams W, GPaths P, GQueue in,
                                                            const liar_hit* __restrict__ hits, uint32_t n_in, GQueue out,
-                                                           float* film, const float* __restrict__ gmix) {
+                                                           const float* __restrict__ gmix) {
     const int lane = threadIdx.x & 31;
     const bool guide_on = W.guide_prob > 0.0f;
     unsigned long long segs = 0, n_hit = 0, n_guided = 0;
@@ -230,19 +223,9 @@ __global__ void __launch_bounds__(kShadeThreads) k_g_shade(DScene S, GParams W, 
                 }
             }
         }
-        // the guide's mixture at this vertex (computed by the network for the whole queue)
-        float mix[kOutUsed];
-        if (guide_on && guidable) {
-            const float4* src = reinterpret_cast<const float4*>(gmix + (size_t)q * kOutUsed);
-#pragma unroll
-            for (int c = 0; c < kOutUsed / 4; ++c) {
-                const float4 v = src[c];
-                mix[4 * c] = v.x;
-                mix[4 * c + 1] = v.y;
-                mix[4 * c + 2] = v.z;
-                mix[4 * c + 3] = v.w;
-            }
-        }
+        // the guide's mixture at this vertex (computed by the network for the whole queue), read
+        // where it is used (only when the vertex is guided) rather than held in registers
+        const float* __restrict__ mix = gmix + (size_t)q * kOutUsed;
         // ---- shading (render.cu's k_shade with the guide as a third technique)
         bool want = false;
         liar_ray nr{};
@@ -414,7 +397,7 @@ __global__ void __launch_bounds__(kShadeThreads) k_g_shade(DScene S, GParams W, 
                 want = true;
             } else {
                 P.L[p] = L;  // the radiance at the end of the path completes its training records
-                gsplat(S, film, (uint32_t)((W.first_path + p) % (uint64_t)W.npix), lam, P.lam_pdf[p], L, P.alpha[p]);
+                gsplat(S, W, p, lam, P.lam_pdf[p], L, P.alpha[p]);
             }
         }
         gqueue_push(out, want, nr, p);
@@ -570,6 +553,7 @@ extern "C" int liar_gpu_render_guided_device(liar_gpu_ctx* ctx, const liar_gpu_s
     if (R.width <= 0 || R.height <= 0 || R.spp <= 0) return ctx_fail(ctx, LIAR_ERR_INVALID, "empty image or no samples");
     if (R.max_ray_generation < 0) return ctx_fail(ctx, LIAR_ERR_INVALID, "max_ray_generation must be >= 0");
     if (R.tracer != LIAR_TRACER_ADJOINT_PHOTON) return ctx_fail(ctx, LIAR_ERR_UNSUPPORTED, "tracer %d", R.tracer);
+    if (const char* m = film_desc_error(R)) return ctx_fail(ctx, LIAR_ERR_INVALID, "%s", m);
     const uint64_t npix = (uint64_t)R.width * R.height;
     if (npix >= (1ull << 32)) return ctx_fail(ctx, LIAR_ERR_INVALID, "image too large");
     const uint64_t total = npix * (uint64_t)R.spp;
@@ -606,6 +590,7 @@ extern "C" int liar_gpu_render_guided_device(liar_gpu_ctx* ctx, const liar_gpu_s
     W.max_depth = R.max_depth;
     W.seed = mix64(R.seed ^ mix64(0x51ed270b27ad0e0dull + (uint64_t)(uint32_t)R.first_sample));
     W.npix = (uint32_t)npix;
+    W.film = film_spec(d_film, R);
     W.train = train ? 1 : 0;
     for (int k = 0; k < 3; ++k) {
         W.box_lo[k] = cfg.bounds_lo[k];
@@ -646,7 +631,7 @@ extern "C" int liar_gpu_render_guided_device(liar_gpu_ctx* ctx, const liar_gpu_s
                 if (rc) return rc;
             }
             k_g_shade<<<(n_in + kShadeThreads - 1) / kShadeThreads, kShadeThreads, 0, st>>>(
-                S, W, gb->P, gb->q[cur], gb->hits, n_in, gb->q[cur ^ 1], d_film, gb->gmix);
+                S, W, gb->P, gb->q[cur], gb->hits, n_in, gb->q[cur ^ 1], gb->gmix);
             e = cudaGetLastError();
             if (e != cudaSuccess) return ctx_cuda(ctx, e, "guided shade launch");
             cur ^= 1;

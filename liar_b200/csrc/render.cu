@@ -80,6 +80,7 @@ struct WaveParams {
     int width, height, spp, max_gen, max_depth;
     uint64_t seed;
     uint64_t first_path;   // global index of the wave's first path
+    FilmSpec film;
 };
 
 __device__ __forceinline__ SampleKey key_of(const WaveParams& W, uint64_t gpath) {
@@ -109,9 +110,8 @@ __device__ __forceinline__ void queue_push(const Queue& q, bool want, const liar
     }
 }
 
-__device__ void splat(const DScene& S, const WaveParams& W, float* film, uint64_t gpath, float lam, float lam_pdf,
-                      float L, float alpha, unsigned long long* stats) {
-    const uint32_t pixel = (uint32_t)(gpath / (uint64_t)W.spp);
+__device__ void splat(const DScene& S, const WaveParams& W, uint64_t gpath, float lam, float lam_pdf, float L,
+                      float alpha) {
     float3 xyz = mk(0, 0, 0);
     if (lam_pdf > 0.0f) {
         // Spectral::xyz in Single mode: v / pdf * sensitivity(lambda) (kernel/spectral.cpp:212-220)
@@ -119,19 +119,11 @@ __device__ void splat(const DScene& S, const WaveParams& W, float* film, uint64_
         const float3 c = observer_sensitivity(S, lam);
         xyz = mk(s * c.x, s * c.y, s * c.z);
     }
-    float* f = film + 8 * (size_t)pixel;
-    atomicAdd(f + 0, xyz.x);
-    atomicAdd(f + 1, xyz.y);
-    atomicAdd(f + 2, xyz.z);
-    atomicAdd(f + 3, alpha);
-    atomicAdd(f + 4, xyz.x * xyz.x);
-    atomicAdd(f + 5, xyz.y * xyz.y);
-    atomicAdd(f + 6, xyz.z * xyz.z);
-    atomicAdd(f + 7, 1.0f);
+    film_splat(W.film, key_of(W, gpath), xyz, alpha);
 }
 
 __global__ void __launch_bounds__(256) k_raygen(DScene S, WaveParams W, Paths P, Queue out, uint32_t n_paths,
-                                                float* film, unsigned long long* stats) {
+                                                unsigned long long* stats) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     bool want = false;
     liar_ray r{};
@@ -154,8 +146,7 @@ __global__ void __launch_bounds__(256) k_raygen(DScene S, WaveParams W, Paths P,
 
 // the whole of tracePhoton after the intersection, for one queue entry
 __global__ void __launch_bounds__(128) k_shade(DScene S, WaveParams W, Paths P, Queue in, const liar_hit* hits,
-                                               uint32_t n_in, Queue out, float* film,
-                                               unsigned long long* stats) {
+                                               uint32_t n_in, Queue out, unsigned long long* stats) {
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     bool want = false;
     liar_ray nr{};
@@ -289,7 +280,7 @@ __global__ void __launch_bounds__(128) k_shade(DScene S, WaveParams W, Paths P, 
             nr = liar_ray{next_o.x, next_o.y, next_o.z, next_tmin, next_d.x, next_d.y, next_d.z, next_tmax};
             want = true;
         } else {
-            splat(S, W, film, g, lam, P.lam_pdf[p], L, P.alpha[p], stats);
+            splat(S, W, g, lam, P.lam_pdf[p], L, P.alpha[p]);
         }
     }
     queue_push(out, want, nr, p);
@@ -598,6 +589,7 @@ int render_impl(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_rende
     const liar_render_desc& R = *desc;
     if (R.width <= 0 || R.height <= 0 || R.spp <= 0) return ctx_fail(ctx, LIAR_ERR_INVALID, "empty image or no samples");
     if (R.max_ray_generation < 0) return ctx_fail(ctx, LIAR_ERR_INVALID, "max_ray_generation must be >= 0");
+    if (const char* m = film_desc_error(R)) return ctx_fail(ctx, LIAR_ERR_INVALID, "%s", m);
     if (R.tracer == LIAR_TRACER_DIRECT_LIGHTING) return render_direct(ctx, scene, R, d_film, st);
     if (R.tracer != LIAR_TRACER_ADJOINT_PHOTON) return ctx_fail(ctx, LIAR_ERR_UNSUPPORTED, "tracer %d", R.tracer);
     const uint64_t total = (uint64_t)R.width * R.height * R.spp;
@@ -617,6 +609,7 @@ int render_impl(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_rende
     W.max_gen = R.max_ray_generation;
     W.max_depth = R.max_depth;
     W.seed = mix64(R.seed ^ mix64(0x51ed270b27ad0e0dull + (uint64_t)(uint32_t)R.first_sample));
+    W.film = film_spec(d_film, R);
     const DScene& S = scene->d;
     for (uint64_t first = 0; first < total; first += wave) {
         const uint32_t n = (uint32_t)std::min<uint64_t>(wave, total - first);
@@ -624,7 +617,7 @@ int render_impl(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_rende
         int cur = 0;
         e = cudaMemsetAsync(rb->q[0].count, 0, 4, st);
         if (e != cudaSuccess) return ctx_cuda(ctx, e, "reset queue");
-        k_raygen<<<(n + 255) / 256, 256, 0, st>>>(S, W, rb->P, rb->q[0], n, d_film, rb->stats);
+        k_raygen<<<(n + 255) / 256, 256, 0, st>>>(S, W, rb->P, rb->q[0], n, rb->stats);
         uint32_t n_in = n;
         for (int bounce = 0; n_in > 0; ++bounce) {
             if (bounce > 4096) return ctx_fail(ctx, LIAR_ERR_TIMEOUT, "paths did not terminate after 4096 bounces");
@@ -632,7 +625,7 @@ int render_impl(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_rende
             if (rc) return rc;
             e = cudaMemsetAsync(rb->q[cur ^ 1].count, 0, 4, st);
             if (e != cudaSuccess) return ctx_cuda(ctx, e, "reset queue");
-            k_shade<<<(n_in + 127) / 128, 128, 0, st>>>(S, W, rb->P, rb->q[cur], rb->hits, n_in, rb->q[cur ^ 1], d_film,
+            k_shade<<<(n_in + 127) / 128, 128, 0, st>>>(S, W, rb->P, rb->q[cur], rb->hits, n_in, rb->q[cur ^ 1],
                                                         rb->stats);
             e = cudaGetLastError();
             if (e != cudaSuccess) return ctx_cuda(ctx, e, "shade launch");

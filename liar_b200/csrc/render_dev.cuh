@@ -774,5 +774,95 @@ __device__ inline liar_ray camera_ray(const liar_camera& C, const SampleKey& k, 
     return liar_ray{pos.x, pos.y, pos.z, fmaxf(kTol, factor * C.near_limit), dir.x, dir.y, dir.z, factor * C.far_limit};
 }
 
+// ---- the film (output/raster.cpp:547-606, output/filter_triangle.cpp, output/filter_mitchell.cpp)
+
+struct FilmSpec {
+    float* film;         // width x height x 8 sums
+    int width, height;
+    int filter;          // liar_filter
+    float param;         // triangle width / Mitchell B
+    float max_lum;       // Raster.maxSampleLuminance, <= 0: none
+};
+
+// the filter settings of a render description, or nullptr when they are valid
+__host__ inline const char* film_desc_error(const liar_render_desc& R) {
+    if (R.filter != LIAR_FILTER_BOX && R.filter != LIAR_FILTER_TRIANGLE && R.filter != LIAR_FILTER_MITCHELL)
+        return "unknown reconstruction filter";
+    if (R.filter == LIAR_FILTER_TRIANGLE && !(R.filter_param >= 0.0f && R.filter_param <= 8.0f))
+        return "triangle filter width must be in (0, 8] (0 selects 1)";
+    if (R.filter == LIAR_FILTER_MITCHELL && !(R.filter_param >= -8.0f && R.filter_param <= 8.0f))
+        return "Mitchell filter B out of range";
+    if (!(R.max_sample_luminance >= 0.0f)) return "max_sample_luminance must be >= 0 (0: no clamp)";
+    return nullptr;
+}
+
+__host__ inline FilmSpec film_spec(float* film, const liar_render_desc& R) {
+    FilmSpec F;
+    F.film = film;
+    F.width = R.width;
+    F.height = R.height;
+    F.filter = R.filter;
+    F.param = R.filter == LIAR_FILTER_TRIANGLE ? (R.filter_param > 0.0f ? R.filter_param : 1.0f)
+                                               : (R.filter_param != 0.0f ? R.filter_param : 1.0f / 3.0f);
+    F.max_lum = R.max_sample_luminance;
+    return F;
+}
+
+// FilterMitchell::filterKernel (filter_mitchell.cpp:133-146), C = (1 - B) / 2
+__device__ __forceinline__ float mitchell_kernel(float x, float B) {
+    const float C = (1.0f - B) / 2.0f;
+    x = fabsf(x);
+    if (x < 1.0f)
+        return ((12.0f - 9.0f * B - 6.0f * C) * (x * x * x) + (-18.0f + 12.0f * B + 6.0f * C) * (x * x) + (6.0f - 2.0f * B)) / 6.0f;
+    if (x < 2.0f)
+        return ((-B - 6.0f * C) * (x * x * x) + (6.0f * B + 30.0f * C) * (x * x) + (-12.0f * B - 48.0f * C) * x +
+                (8.0f * B + 24.0f * C)) / 6.0f;
+    return 0.0f;
+}
+
+__device__ __forceinline__ void film_add(float* f, float3 xyz, float alpha, float w) {
+    const float wa = w * alpha;
+    atomicAdd(f + 0, wa * xyz.x);
+    atomicAdd(f + 1, wa * xyz.y);
+    atomicAdd(f + 2, wa * xyz.z);
+    atomicAdd(f + 3, wa);
+    atomicAdd(f + 4, w * (xyz.x * xyz.x));
+    atomicAdd(f + 5, w * (xyz.y * xyz.y));
+    atomicAdd(f + 6, w * (xyz.z * xyz.z));
+    atomicAdd(f + 7, w);
+}
+
+// One sample into the film. The box filter adds it to its own pixel with weight 1. The triangle
+// and Mitchell filters spread it over the pixels within their radius with the weights the
+// reference's filters give: the pixel at offset (i, j) gets k(dx + i) k(dy + j), with (dx, dy) the
+// sample's offset from its pixel's centre (the reference adds the offset, so the footprint is
+// mirrored about the pixel centre); pixels outside the image are dropped, as Raster drops them.
+// A sample brighter than max_lum in Y is scaled down to it first.
+__device__ inline void film_splat(const FilmSpec& F, const SampleKey& k, float3 xyz, float alpha) {
+    if (F.max_lum > 0.0f && xyz.y > F.max_lum) {
+        const float s = F.max_lum / xyz.y;
+        xyz = mk(xyz.x * s, xyz.y * s, xyz.z * s);
+    }
+    if (F.filter == LIAR_FILTER_BOX) {
+        film_add(F.film + 8 * (size_t)k.pixel, xyz, alpha, 1.0f);
+        return;
+    }
+    const int px = (int)(k.pixel % (uint32_t)F.width), py = (int)(k.pixel / (uint32_t)F.width);
+    const float dx = sample_dim(k, DIM_SCREEN, true) - 0.5f, dy = sample_dim(k, DIM_SCREEN + 1, true) - 0.5f;
+    const bool mitchell = F.filter == LIAR_FILTER_MITCHELL;
+    const int r = mitchell ? 2 : (int)ceilf(F.param);
+    for (int j = -r; j <= r; ++j) {
+        const int y = py + j;
+        if (y < 0 || y >= F.height) continue;
+        const float fy = mitchell ? mitchell_kernel(dy + (float)j, F.param) : fmaxf(0.0f, F.param - fabsf(dy + (float)j));
+        for (int i = -r; i <= r; ++i) {
+            const int x = px + i;
+            if (x < 0 || x >= F.width) continue;
+            const float fx = mitchell ? mitchell_kernel(dx + (float)i, F.param) : fmaxf(0.0f, F.param - fabsf(dx + (float)i));
+            film_add(F.film + 8 * ((size_t)y * F.width + x), xyz, alpha, fx * fy);
+        }
+    }
+}
+
 }  // namespace rt
 }  // namespace liar_gpu

@@ -45,8 +45,9 @@ class RenderEngine:
             # the reference throws here (render_engine.cpp:172-193)
             raise RuntimeError("RenderEngine needs a camera, a tracer, a sampler and a scene before render()")
         w, h = self.sampler.resolution
+        from .output import film_settings
         desc = R.render_desc(self.camera, w, h, self.sampler.samplesPerPixel, self.tracer,
-                             seed=self.seed or getattr(self.sampler, "seed_", 0))
+                             seed=self.seed or getattr(self.sampler, "seed_", 0), **film_settings(self.target))
         film = self._scene().render(desc)
         xyza, var = R.resolve(film)
         self.film = film

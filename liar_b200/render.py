@@ -59,7 +59,11 @@ class CRenderDesc(C.Structure):
     _fields_ = [("camera", CCamera), ("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32),
                 ("tracer", C.c_int32), ("max_ray_generation", C.c_int32), ("max_depth", C.c_int32),
                 ("seed", C.c_uint64), ("first_sample", C.c_int32), ("wave_paths", C.c_int32),
-                ("secondary_light_samples", C.c_int32), ("trace_glossy", C.c_int32)]
+                ("secondary_light_samples", C.c_int32), ("trace_glossy", C.c_int32),
+                ("filter", C.c_int32), ("filter_param", C.c_float), ("max_sample_luminance", C.c_float)]
+
+
+FILTER_BOX, FILTER_TRIANGLE, FILTER_MITCHELL = 0, 1, 2
 
 
 SPEC_CONSTANT, SPEC_SAMPLED, SPEC_BLACKBODY, SPEC_CAUCHY = 0, 1, 2, 3
@@ -350,7 +354,11 @@ def flatten(scene) -> FlatScene:
 
 
 def render_desc(camera, width: int, height: int, spp: int, tracer, seed: int = 0, first_sample: int = 0,
-                wave_paths: int = 0) -> CRenderDesc:
+                wave_paths: int = 0, filter: int = FILTER_BOX, filter_param: float = 0.0,
+                max_sample_luminance: float = 0.0) -> CRenderDesc:
+    """The C render description. filter / filter_param select the reconstruction filter (box;
+    triangle of the given width, default 1; Mitchell with the given B, default 1/3);
+    max_sample_luminance > 0 clamps each sample's Y (Raster.maxSampleLuminance)."""
     r = CRenderDesc()
     cam = camera.flatten()
     for k in ("position", "direction", "right", "down", "direction_normal", "right_normal", "down_normal"):
@@ -368,15 +376,25 @@ def render_desc(camera, width: int, height: int, spp: int, tracer, seed: int = 0
     r.wave_paths = int(wave_paths)
     r.secondary_light_samples = int(getattr(tracer, "numberOfSecondaryLightSamples", 1))
     r.trace_glossy = 1 if getattr(tracer, "traceGlossy", True) else -1
+    r.filter = int(filter)
+    r.filter_param = float(filter_param)
+    r.max_sample_luminance = float(max_sample_luminance) if math.isfinite(max_sample_luminance) else 0.0
     return r
 
 
 def resolve(film: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
-    """(H, W, 8) sums -> mean XYZ + alpha (H, W, 4) and variance of the mean of XYZ (H, W, 3)."""
-    n = np.maximum(film[..., 7:8], 1.0).astype(np.float64)
-    mean = film[..., 0:4].astype(np.float64) / n
-    ex2 = film[..., 4:7].astype(np.float64) / n
-    var = np.maximum(ex2 - mean[..., 0:3] ** 2, 0.0) * n / np.maximum(n - 1, 1) / n
+    """(H, W, 8) sums -> mean XYZ + alpha (H, W, 4) and variance of the mean of XYZ (H, W, 3).
+
+    The mean is the reference's pixel (Raster::weighted, output/raster.cpp:645-651): the weighted
+    sums over the sum of the filter weights (the sample count for the box filter), zero where no
+    weight arrived. The variance is the sample variance of the mean for the box filter and an
+    estimate of it with the filter weights otherwise."""
+    w = film[..., 7:8].astype(np.float64)
+    ok = w > 0
+    n = np.where(ok, w, 1.0)
+    mean = np.where(ok, film[..., 0:4].astype(np.float64) / n, 0.0)
+    ex2 = np.where(ok, film[..., 4:7].astype(np.float64) / n, 0.0)
+    var = np.maximum(ex2 - mean[..., 0:3] ** 2, 0.0) / np.maximum(n - 1, 1)
     return mean, var
 
 

@@ -92,6 +92,8 @@ struct RenderIn {
     uint64_t seed;
     int32_t first_sample, wave_paths;
     int32_t secondary_light_samples, trace_glossy;
+    int32_t filter;
+    float filter_param, max_sample_luminance;
 };
 
 enum { SP_CONST = 0, SP_SAMPLED = 1, SP_BB = 2, SP_CAUCHY = 3 };
@@ -1334,6 +1336,64 @@ float oracle_observer_sample(void* s, float u, float* pdf, float* xyz) {
     return w;
 }
 
+// ---- the film: Raster::doWriteRender (output/raster.cpp:547-606) behind FilterTriangle
+// (output/filter_triangle.cpp:100-145, kernel :167-170) or FilterMitchell
+// (output/filter_mitchell.cpp:84-146): the pixel at offset (i, j) from the sample's pixel gets
+// weight k(dx + i) k(dy + j), (dx, dy) the sample's offset from its pixel centre; pixels outside
+// the image are dropped; a sample brighter than maxSampleLuminance in Y is scaled down to it.
+static float mitchell_kernel(float x, float B) {
+    const float C = (1.0f - B) / 2.0f;
+    x = std::fabs(x);
+    if (x < 1.0f)
+        return ((12.0f - 9.0f * B - 6.0f * C) * (x * x * x) + (-18.0f + 12.0f * B + 6.0f * C) * (x * x) + (6.0f - 2.0f * B)) / 6.0f;
+    if (x < 2.0f)
+        return ((-B - 6.0f * C) * (x * x * x) + (6.0f * B + 30.0f * C) * (x * x) + (-12.0f * B - 48.0f * C) * x +
+                (8.0f * B + 24.0f * C)) / 6.0f;
+    return 0.0f;
+}
+
+static void film_add(float* f, float X, float Y, float Z, float alpha, float w) {
+    const float wa = w * alpha;
+    f[0] += wa * X;
+    f[1] += wa * Y;
+    f[2] += wa * Z;
+    f[3] += wa;
+    f[4] += w * (X * X);
+    f[5] += w * (Y * Y);
+    f[6] += w * (Z * Z);
+    f[7] += w;
+}
+
+static void film_splat(const RenderIn& R, float* film, int px, int py, float jx, float jy, float X, float Y, float Z,
+                       float alpha) {
+    if (R.max_sample_luminance > 0.0f && Y > R.max_sample_luminance) {
+        const float s = R.max_sample_luminance / Y;
+        X *= s;
+        Y *= s;
+        Z *= s;
+    }
+    if (R.filter == 0) {
+        film_add(film + 8 * ((int64_t)py * R.width + px), X, Y, Z, alpha, 1.0f);
+        return;
+    }
+    const bool mitchell = R.filter == 2;
+    const float param = mitchell ? (R.filter_param != 0.0f ? R.filter_param : 1.0f / 3.0f)
+                                 : (R.filter_param > 0.0f ? R.filter_param : 1.0f);
+    const int r = mitchell ? 2 : (int)std::ceil(param);
+    const float dx = jx - 0.5f, dy = jy - 0.5f;
+    for (int j = -r; j <= r; ++j) {
+        const int y = py + j;
+        if (y < 0 || y >= R.height) continue;
+        const float fy = mitchell ? mitchell_kernel(dy + (float)j, param) : std::max(0.0f, param - std::fabs(dy + (float)j));
+        for (int i = -r; i <= r; ++i) {
+            const int x = px + i;
+            if (x < 0 || x >= R.width) continue;
+            const float fx = mitchell ? mitchell_kernel(dx + (float)i, param) : std::max(0.0f, param - std::fabs(dx + (float)i));
+            film_add(film + 8 * ((int64_t)y * R.width + x), X, Y, Z, alpha, fx * fy);
+        }
+    }
+}
+
 // renders pixels [pixel_begin, pixel_end) of the image into film (8 floats per pixel, summed)
 int oracle_render(void* s, const RenderIn* R, float* film, int64_t pixel_begin, int64_t pixel_end, int threads) {
     const Scene& S = *static_cast<Scene*>(s);
@@ -1342,11 +1402,20 @@ int oracle_render(void* s, const RenderIn* R, float* film, int64_t pixel_begin, 
     if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
     const uint64_t seed = mix64(R->seed ^ mix64(0x51ed270b27ad0e0dull + (uint64_t)(uint32_t)R->first_sample));
     std::atomic<int64_t> next{pixel_begin};
+    // with a filter, a sample reaches its neighbours' pixels too: every thread sums into a film of
+    // its own, added to the caller's at the end
+    std::vector<std::vector<float>> own(R->filter != 0 ? (size_t)threads : 0);
+    std::atomic<int> slot{0};
     auto work = [&]() {
+        float* target = film;
+        if (R->filter != 0) {
+            auto& v = own[(size_t)slot.fetch_add(1)];
+            v.assign((size_t)npix * 8, 0.0f);
+            target = v.data();
+        }
         while (true) {
             const int64_t px = next.fetch_add(1);
             if (px >= pixel_end) break;
-            float* f = film + 8 * px;
             for (int smp = 0; smp < R->spp; ++smp) {
                 Path P;
                 P.S = &S;
@@ -1390,14 +1459,8 @@ int oracle_render(void* s, const RenderIn* R, float* film, int64_t pixel_begin, 
                     Yv = sc * c.y;
                     Z = sc * c.z;
                 }
-                f[0] += X;
-                f[1] += Yv;
-                f[2] += Z;
-                f[3] += P.alpha;
-                f[4] += X * X;
-                f[5] += Yv * Yv;
-                f[6] += Z * Z;
-                f[7] += 1;
+                film_splat(*R, target, (int)ix, (int)iy, P.smp.get(D_SCREEN, true), P.smp.get(D_SCREEN + 1, true), X, Yv,
+                           Z, P.alpha);
             }
         }
     };
@@ -1405,6 +1468,8 @@ int oracle_render(void* s, const RenderIn* R, float* film, int64_t pixel_begin, 
     for (int k = 1; k < threads; ++k) pool.emplace_back(work);
     work();
     for (auto& t : pool) t.join();
+    for (const auto& v : own)
+        for (size_t k = 0; k < v.size(); ++k) film[k] += v[k];
     return 0;
 }
 
