@@ -333,18 +333,20 @@ def guided_bench(ctx, stream, args, world, dist, local, cpu: bool) -> dict:
     plain_s = e0.elapsed_time(e1) * 1e-3
     plain_mse = mse(plain)
     plain_stats = gs.stats()
-    # guided: chunks of 16 spp, training during the first 8 chunks
-    g = GD.Guide(ctx, GD.scene_bounds(flat), guide_probability=0.7, light_probability=0.1, learning_rate=5e-3,
-                 steps_per_pass=4, batch_records=65536, seed=0)
+    # guided: chunks of 16 spp; during the first train_chunks chunks the guide trains after every
+    # pass over the image (4 Adam steps of 16,384 records)
+    c_guide, lp_guide, train_chunks = 0.4, 0.1, 4
+    g = GD.Guide(ctx, GD.scene_bounds(flat), guide_probability=c_guide, light_probability=lp_guide,
+                 learning_rate=5e-3, steps_per_pass=4, batch_records=16384, seed=0)
     gf = film()
     curve, t_cum, spp, t_hit = [], 0.0, 0, None
     while spp < 4 * plain_spp:
         d = R.render_desc(cam, res, res, chunk, tracer, seed=11, first_sample=spp)
         e0.record(stream)
-        # training: one round per pass over the image for the first 8 chunks
-        if spp < 8 * chunk:
-            d.wave_paths = res * res
-        g.render(gs, d, gf.data_ptr(), train=spp < 8 * chunk, stream=st)
+        training = spp < train_chunks * chunk
+        if training:
+            d.wave_paths = res * res  # one training round per pass over the image
+        g.render(gs, d, gf.data_ptr(), train=training, stream=st)
         e1.record(stream)
         stream.synchronize()
         dt = e0.elapsed_time(e1) * 1e-3
@@ -386,8 +388,8 @@ def guided_bench(ctx, stream, args, world, dist, local, cpu: bool) -> dict:
                      "samples_per_s": plain_spp * res * res / plain_s,
                      "segments_per_sample": plain_stats["segments"] / max(plain_stats["paths"], 1)},
            "guided": {"seconds_to_plain_mse": t_hit, "spp_at_crossing": spp if t_hit else None,
-                      "training_chunks": 8, "chunk_spp": chunk, "adam_steps": gstats["steps"],
-                      "guide_probability": 0.7, "light_probability": 0.1,
+                      "training_chunks": train_chunks, "chunk_spp": chunk, "adam_steps": gstats["steps"],
+                      "batch_records": 16384, "guide_probability": c_guide, "light_probability": lp_guide,
                       "curve_t_spp_mse": curve[:: max(1, len(curve) // 24)]},
            "time_ratio_guided_over_plain": (t_hit / plain_s) if t_hit else None,
            "network": {"inference_queries_per_s": (1 << 20) / eval_s,
@@ -397,7 +399,7 @@ def guided_bench(ctx, stream, args, world, dist, local, cpu: bool) -> dict:
                        "peak_bf16_tflops": peaks["bf16_tflops"],
                        "inference_frac_of_peak": flop_fwd * (1 << 20) / eval_s / 1e12 / peaks["bf16_tflops"]},
            "note": "MSE over XYZ against the plain reference, reference variance subtracted; guided time includes "
-                   "online training (8 chunks x 4 Adam steps x 65,536 records)"}
+                   f"online training ({train_chunks} chunks x {chunk} passes x 4 Adam steps x 16,384 records)"}
     if cpu:
         import oracle
         rs = oracle.RenderScene(flat)
