@@ -163,7 +163,8 @@ __device__ __forceinline__ void load_frags(uint2* dst, const uint2* __restrict__
 // ---- inference on tcgen05: two slots of 128 rows per CTA (guide_umma.cuh)
 __global__ void __launch_bounds__(kTcThreads, 1) k_eval_tc(const unsigned char* __restrict__ w_img,
                                                            const float* __restrict__ in, size_t n, Box box,
-                                                           float* __restrict__ mix, uint32_t* __restrict__ status) {
+                                                           float* __restrict__ mix, int stride,
+                                                           uint32_t* __restrict__ status) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     unsigned char* sw = smem;
@@ -254,10 +255,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_eval_tc(const unsigned char* 
             Lobe lobes[kLobes];
             float w[kLobes];
             mixture_from_raw(v, lobes, w);
-            float4* dst = reinterpret_cast<float4*>(mix + row * kOutUsed);
+            float4* dst = reinterpret_cast<float4*>(mix + row * (size_t)stride);
             for (int l = 0; l < kLobes; ++l) dst[l] = make_float4(lobes[l].mx, lobes[l].my, lobes[l].mz, lobes[l].kappa);
             dst[8] = make_float4(w[0], w[1], w[2], w[3]);
             dst[9] = make_float4(w[4], w[5], w[6], w[7]);
+            if (stride == kMixRender) {
+                float a[kLobes];
+                for (int l = 0; l < kLobes; ++l) a[l] = w[l] * vmf_norm(lobes[l].kappa);
+                dst[10] = make_float4(a[0], a[1], a[2], a[3]);
+                dst[11] = make_float4(a[4], a[5], a[6], a[7]);
+            }
         }
     }
     tc_fence_before();
@@ -775,8 +782,23 @@ extern "C" int liar_gpu_guide_set_params(liar_gpu_ctx* ctx, liar_gpu_guide* G, c
     return ctx_cuda(ctx, cudaStreamSynchronize(ctx->stream), "guide parameters");
 }
 
+namespace liar_gpu {
+namespace guide {
+int guide_eval(liar_gpu_ctx* ctx, const liar_gpu_guide* G, const float* d_inputs, size_t n, float* d_mixture,
+               int stride, cudaStream_t st);
+}  // namespace guide
+}  // namespace liar_gpu
+
 extern "C" int liar_gpu_guide_eval_device(liar_gpu_ctx* ctx, const liar_gpu_guide* G, const float* d_inputs, size_t n,
                                           float* d_mixture, void* stream) {
+    if (!ctx) return LIAR_ERR_INVALID;
+    return guide_eval(ctx, G, d_inputs, n, d_mixture, kOutUsed, stream ? (cudaStream_t)stream : ctx->stream);
+}
+
+// inference: raw inputs [n][9] -> mixtures [n][stride] = 8 x (mu xyz, kappa), the 8 weights and,
+// with stride kMixRender, the 8 weights times their lobe's normalisation
+int liar_gpu::guide::guide_eval(liar_gpu_ctx* ctx, const liar_gpu_guide* G, const float* d_inputs, size_t n,
+                                float* d_mixture, int stride, cudaStream_t st) {
     if (!ctx || !G) return LIAR_ERR_INVALID;
     if (n == 0) return LIAR_OK;
     if (!d_inputs || !d_mixture) return ctx_fail(ctx, LIAR_ERR_INVALID, "null inputs or outputs");
@@ -785,11 +807,11 @@ extern "C" int liar_gpu_guide_eval_device(liar_gpu_ctx* ctx, const liar_gpu_guid
     if (rc) return rc;
     rc = smem_attrs(ctx);
     if (rc) return rc;
-    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
-    // inference: raw inputs [n][9] -> mixtures [n][40] = 8 x (mu xyz, kappa), then the 8 weights
+    if (stride != kOutUsed && stride != kMixRender) return ctx_fail(ctx, LIAR_ERR_INVALID, "mixture stride %d", stride);
     const size_t tiles = (n + kTcRows - 1) / kTcRows;
     const unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>((tiles + kTcSlots - 1) / kTcSlots, (size_t)ctx->num_sms));
-    k_eval_tc<<<grid, kTcThreads, kUmmaSmem, st>>>(G->umma_w, d_inputs, n, make_box(G->cfg), d_mixture, G->status);
+    k_eval_tc<<<grid, kTcThreads, kUmmaSmem, st>>>(G->umma_w, d_inputs, n, make_box(G->cfg), d_mixture, stride,
+                                                   G->status);
     return ctx_cuda(ctx, cudaGetLastError(), "guide evaluation");
 }
 

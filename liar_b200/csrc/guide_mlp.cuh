@@ -268,9 +268,26 @@ GM_HD float vmf_log_pdf(float kappa, float cos_t) {
     return logf(kappa / (-expm1f(-2.0f * kappa))) - 1.8378770664093453f /* log 2 pi */ + kappa * (cos_t - 1.0f);
 }
 
+// the vMF normalisation kappa / (2 pi (1 - e^{-2 kappa}))
+GM_HD float vmf_norm(float kappa) { return kappa / (6.283185307179586f * -expm1f(-2.0f * kappa)); }
+
+// the renderer's copy of a mixture carries each lobe's weight times its normalisation as well
+constexpr int kMixRender = 48;
+
 #ifdef __CUDACC__
 // ---- the mixture as stored by the network's inference: m[0..31] = 8 x (mu x, y, z, kappa),
-// m[32..39] = the 8 weights
+// m[32..39] = the 8 weights (and, in the renderer's copy, m[40..47] = weight x vmf_norm(kappa))
+
+// the density from the renderer's copy: one exponential per lobe
+__device__ __forceinline__ float mixture_pdf_render(const float* m, float dx, float dy, float dz) {
+    float p = 0.0f;
+#pragma unroll
+    for (int l = 0; l < kLobes; ++l) {
+        const float c = m[4 * l] * dx + m[4 * l + 1] * dy + m[4 * l + 2] * dz;
+        p += m[40 + l] * expf(m[4 * l + 3] * (c - 1.0f));
+    }
+    return p;
+}
 
 __device__ __forceinline__ float mixture_pdf(const float* m, float dx, float dy, float dz) {
     float p = 0.0f;

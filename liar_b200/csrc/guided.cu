@@ -46,6 +46,8 @@ int guide_train(liar_gpu_ctx* ctx, liar_gpu_guide* g, const float* d_records, co
                 int apply, float* d_grad_out, float* d_loss_out, cudaStream_t st);
 void guide_count(liar_gpu_guide* g, unsigned long long records, unsigned long long guided, unsigned long long passes);
 unsigned long long guide_steps(const liar_gpu_guide* g);
+int guide_eval(liar_gpu_ctx* ctx, const liar_gpu_guide* G, const float* d_inputs, size_t n, float* d_mixture,
+               int stride, cudaStream_t st);
 }  // namespace guide
 }  // namespace liar_gpu
 
@@ -225,7 +227,7 @@ __global__ void __launch_bounds__(kShadeThreads) k_g_shade(DScene S, GParams W, 
         }
         // the guide's mixture at this vertex (computed by the network for the whole queue), read
         // where it is used (only when the vertex is guided) rather than held in registers
-        const float* __restrict__ mix = gmix + (size_t)q * kOutUsed;
+        const float* __restrict__ mix = gmix + (size_t)q * kMixRender;
         // ---- shading (render.cu's k_shade with the guide as a third technique)
         bool want = false;
         liar_ray nr{};
@@ -287,7 +289,7 @@ __global__ void __launch_bounds__(kShadeThreads) k_g_shade(DScene S, GParams W, 
                             wd = mk(gx, gy, gz);
                             wo = mk(dot(wd, u), dot(wd, v), dot(wd, N));
                             const BsdfOut be = bsdf_evaluate(B, wi, wo, CAP_ALL);
-                            p_dir = c * mixture_pdf(mix, gx, gy, gz) + (1.0f - c) * be.pdf;
+                            p_dir = c * mixture_pdf_render(mix, gx, gy, gz) + (1.0f - c) * be.pdf;
                             value = be.value;
                             ok = p_dir > 0.0f && value != 0.0f;
                         } else {
@@ -297,7 +299,7 @@ __global__ void __launch_bounds__(kShadeThreads) k_g_shade(DScene S, GParams W, 
                             if (bs.ok()) {
                                 wo = bs.wo;
                                 wd = bs.wo.x * u + bs.wo.y * v + bs.wo.z * N;
-                                const float qd = c > 0.0f ? mixture_pdf(mix, wd.x, wd.y, wd.z) : 0.0f;
+                                const float qd = c > 0.0f ? mixture_pdf_render(mix, wd.x, wd.y, wd.z) : 0.0f;
                                 p_dir = c > 0.0f ? c * qd + (1.0f - c) * bs.pdf : bs.pdf;
                                 value = bs.value;
                                 ok = true;
@@ -336,7 +338,7 @@ __global__ void __launch_bounds__(kShadeThreads) k_g_shade(DScene S, GParams W, 
                                 const BsdfOut be = bsdf_evaluate(B, wi, lwo, CAP_ALL);
                                 if (be.pdf > 0.0f && be.value != 0.0f) {
                                     const float p_dir =
-                                        c > 0.0f ? c * mixture_pdf(mix, ls.dir.x, ls.dir.y, ls.dir.z) + (1.0f - c) * be.pdf
+                                        c > 0.0f ? c * mixture_pdf_render(mix, ls.dir.x, ls.dir.y, ls.dir.z) + (1.0f - c) * be.pdf
                                                  : be.pdf;
                                     wo = lwo;
                                     wd = ls.dir;
@@ -500,11 +502,14 @@ int ensure_guided_buffers(liar_gpu_ctx* ctx, GuidedBuffers* gb, size_t n, size_t
         if (e != cudaSuccess) return ctx_cuda(ctx, e, "guided render host buffers");
     }
     if (gb->cap >= n && gb->rec_cap >= rec_cap) return LIAR_OK;
+    // grow, keeping what earlier calls needed (training and rendering calls alternate)
+    n = std::max(n, gb->cap);
+    rec_cap = std::max(rec_cap, gb->rec_cap);
     if (gb->mem) cudaFree(gb->mem);
     gb->mem = nullptr;
     gb->cap = gb->rec_cap = 0;
     const size_t bytes =
-        n * (6 * 4 + 2 * (32 + 4) + 8 + (9 + kOutUsed) * 4) + rec_cap * (kRawRecord + 2 * kTrainRecord) * 4 + 8192;
+        n * (6 * 4 + 2 * (32 + 4) + 8 + (9 + kMixRender) * 4) + rec_cap * (kRawRecord + 2 * kTrainRecord) * 4 + 8192;
     cudaError_t e = cudaMalloc(&gb->mem, bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -528,7 +533,7 @@ int ensure_guided_buffers(liar_gpu_ctx* ctx, GuidedBuffers* gb, size_t n, size_t
     gb->P.alpha = reinterpret_cast<float*>(take(n * 4));
     gb->P.gen = reinterpret_cast<int32_t*>(take(n * 4));
     gb->gin = reinterpret_cast<float*>(take(n * 9 * 4));
-    gb->gmix = reinterpret_cast<float*>(take(n * kOutUsed * 4));
+    gb->gmix = reinterpret_cast<float*>(take(n * kMixRender * 4));
     gb->raw = reinterpret_cast<float*>(take(rec_cap * kRawRecord * 4));
     gb->train = reinterpret_cast<float*>(take(rec_cap * kTrainRecord * 4));
     gb->shuffled = reinterpret_cast<float*>(take(rec_cap * kTrainRecord * 4));
@@ -559,10 +564,11 @@ extern "C" int liar_gpu_render_guided_device(liar_gpu_ctx* ctx, const liar_gpu_s
     const uint64_t total = npix * (uint64_t)R.spp;
     // paths per wave: without training as many as fit (4M); when training, the guide learns after
     // every wave, so a wave is a whole number of passes over the image, about 2M paths
+    GuidedBuffers* gb = guided_buffers(ctx);
     uint64_t wave;
     if (R.wave_paths > 0) wave = (uint64_t)R.wave_paths;
     else if (train) wave = npix * std::max<uint64_t>(1, (1ull << 21) / npix);
-    else wave = 1ull << 22;
+    else wave = gb->cap >= (1u << 20) ? gb->cap : (1ull << 22);  // reuse the buffers of earlier waves
     wave = std::min<uint64_t>(std::min<uint64_t>(wave, total), 1ull << 26);
     int rc = ctx_activate(ctx);
     if (rc) return rc;
@@ -576,7 +582,6 @@ extern "C" int liar_gpu_render_guided_device(liar_gpu_ctx* ctx, const liar_gpu_s
     // probability follows the previous wave's candidates per path, with 20% slack)
     const size_t rec_cap = train ? std::min<size_t>(std::max<size_t>((size_t)wave * 5 / 2, (size_t)batch * steps), 1ull << 25) : 0;
     const size_t rec_target = rec_cap - rec_cap / 5;
-    GuidedBuffers* gb = guided_buffers(ctx);
     rc = ensure_guided_buffers(ctx, gb, (size_t)wave, rec_cap);
     if (rc) return rc;
     cudaError_t e = cudaMemsetAsync(gb->stats, 0, 4 * sizeof(unsigned long long), st);
@@ -627,7 +632,7 @@ extern "C" int liar_gpu_render_guided_device(liar_gpu_ctx* ctx, const liar_gpu_s
             if (guide_on) {
                 // the guide network over the queue's diffuse and glossy vertices
                 k_g_prep<<<(n_in + 127) / 128, 128, 0, st>>>(S, gb->q[cur], gb->hits, n_in, gb->gin);
-                rc = liar_gpu_guide_eval_device(ctx, guide, gb->gin, n_in, gb->gmix, st);
+                rc = guide_eval(ctx, guide, gb->gin, n_in, gb->gmix, kMixRender, st);
                 if (rc) return rc;
             }
             k_g_shade<<<(n_in + kShadeThreads - 1) / kShadeThreads, kShadeThreads, 0, st>>>(
