@@ -137,7 +137,9 @@ typedef struct liar_gpu_scene liar_gpu_scene;
 enum liar_spectrum_type {
     LIAR_SPEC_CONSTANT = 0,  /* p[0] */
     LIAR_SPEC_SAMPLED = 1,   /* piecewise linear: pool[offset .. +count) wavelengths, then count values
-                                (spectra/sampled.cpp:128, kernel/spectral.cpp:185-210) */
+                                (spectra/sampled.cpp:128, kernel/spectral.cpp:185-210); as a reflectance
+                                divided by its maximum when above 1, or by p[0] when p[0] > 0 (a colour
+                                recovered from XYZ, spectra/recovery_meng_simon.cpp:151-166) */
     LIAR_SPEC_BLACKBODY = 2, /* p[0] temperature (K), p[1] scale; normalised at the peak (spectra/black_body.cpp:55-118) */
     LIAR_SPEC_CAUCHY = 3     /* p[0] + p[1] / lambda_um^2 (spectra/cauchy.cpp:72-76) */
 };

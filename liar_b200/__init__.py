@@ -8,5 +8,8 @@ shading and photon work runs on the GPU behind the C ABI of include/liar_gpu.h
 """
 from . import cameras, output, samplers, scenery, shaders, spectra, textures, tracers  # noqa: F401
 from .kernel import RenderEngine  # noqa: F401
+from .recovery import RgbSpace, sRGB  # noqa: F401
+from .spectra import rgb  # noqa: F401
 
-__all__ = ["cameras", "output", "samplers", "scenery", "shaders", "spectra", "textures", "tracers", "RenderEngine"]
+__all__ = ["cameras", "output", "samplers", "scenery", "shaders", "spectra", "textures", "tracers", "RenderEngine",
+           "rgb", "RgbSpace", "sRGB"]

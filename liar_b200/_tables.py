@@ -1,4 +1,5 @@
-"""Access to the spectral data tables in liar_b200/data/tables.json (CIE 1931 observer, metal n, k)."""
+"""Access to the spectral data tables in liar_b200/data/tables.json (CIE 1931 observer, metal n, k,
+Meng-Simon recovery spectra)."""
 from __future__ import annotations
 
 import functools
@@ -38,3 +39,8 @@ def observer_y_weights() -> tuple[np.ndarray, np.ndarray]:
 
 def spd(name: str) -> list:
     return _load()["spd"][name]
+
+
+def recovery() -> dict:
+    """{"wavelengths": [m], "xy": [[x, y]], "spectra": [[values]]}."""
+    return _load()["recovery"]

@@ -412,7 +412,7 @@ extern "C" int liar_gpu_scene_upload(liar_gpu_ctx* ctx, const liar_scene_desc* d
                 return ctx_fail(ctx, LIAR_ERR_INVALID, "spectrum %zu: sampled table out of range", k);
             float mx = -INFINITY;
             for (int i = 0; i < s.count; ++i) mx = std::max(mx, D.spectrum_pool[s.offset + s.count + i]);
-            spec_max[k] = mx;
+            spec_max[k] = s.p[0] > 0.0f ? s.p[0] : mx;  // p[0] > 0: the reflectance bound of a recovered colour
         } else if (s.type < 0 || s.type > LIAR_SPEC_CAUCHY) {
             return ctx_fail(ctx, LIAR_ERR_INVALID, "spectrum %zu: bad type", k);
         }

@@ -7,6 +7,10 @@ can be compared with it:
   stored here in metres like the reference's Observer).
 * ``spd``: complex refractive index n + ik of Ag, Al, Au, Cu (Hagemann, Gudat, Kunz 1974 and the
   other sources named in each reference data/spd/*.spd header), wavelengths in metres.
+* ``recovery``: the spectra of the tristimulus-to-spectrum recovery of Meng, Simon, Hanika and
+  Dachsbacher, "Physically Meaningful Rendering using Tristimulus Colours" (EGSR 2015), sampled
+  at chromaticities xy, as shipped in the reference's data/recovery_meng_simon.json (loaded by
+  src/liar/__init__.py:72-79); wavelengths in metres.
 
 Run in a container that has the reference mounted: ``python liar_b200/data/make_tables.py
 /path/to/reference``. The product reads only the generated JSON.
@@ -35,9 +39,14 @@ def main(ref: Path) -> None:
     for name in ("Ag", "Al", "Au", "Cu"):
         body = read_columns(ref / "data" / "spd" / f"{name}.spd")
         spd[name] = [[float(r[0]) * 1e-9, float(r[1]), float(r[2])] for r in body]
+    rec = json.loads((ref / "data" / "recovery_meng_simon.json").read_text())
+    recovery = {"wavelengths": [float(w) * 1e-9 for w in rec["wavelengths"]],
+                "xy": [[float(v) for v in s["xy"]] for s in rec["spectra"]],
+                "spectra": [[float(v) for v in s["spectrum"]] for s in rec["spectra"]]}
     out = Path(__file__).resolve().parent / "tables.json"
-    out.write_text(json.dumps({"observer": observer, "spd": spd}, indent=None, separators=(",", ":")))
-    print(out, len(observer), {k: len(v) for k, v in spd.items()})
+    out.write_text(json.dumps({"observer": observer, "spd": spd, "recovery": recovery}, indent=None,
+                              separators=(",", ":")))
+    print(out, len(observer), {k: len(v) for k, v in spd.items()}, len(recovery["xy"]))
 
 
 if __name__ == "__main__":

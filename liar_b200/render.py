@@ -149,6 +149,17 @@ class _Builder:
             rec.count = len(s.wavelengths)
             self.pool.extend(s.wavelengths)
             self.pool.extend(s.values)
+        elif isinstance(s, spectra.Xyz):
+            # the recovered spectrum at the recovery's wavelengths, with the recovery's bound for
+            # the reflectance rescale (RecoveryMengSimon::doRecover, Single mode)
+            from .recovery import standard
+            ws, vs, mx = standard().sampled(s.xyz)
+            rec.type = SPEC_SAMPLED
+            rec.offset = len(self.pool)
+            rec.count = len(ws)
+            rec.p[0] = mx
+            self.pool.extend(float(w) for w in ws)
+            self.pool.extend(float(v) for v in vs)
         elif isinstance(s, spectra.BlackBody):
             rec.type = SPEC_BLACKBODY
             rec.p[0], rec.p[1] = s.temperature, s.scale

@@ -112,6 +112,39 @@ class Cauchy(Spectrum):
         return self.b != 0.0
 
 
+class Xyz(Spectrum):
+    """A spectrum given by its tristimulus value (the reference's SpectrumXYZ,
+    kernel/spectrum.cpp:232-252), evaluated through the standard recovery (liar_b200.recovery)."""
+
+    def __init__(self, xyz):
+        self.xyz = tuple(float(v) for v in xyz)
+        if len(self.xyz) != 3:
+            raise ValueError("Xyz needs three values")
+
+    def __call__(self, wavelength):
+        from .recovery import standard
+        rec = standard()
+        w = np.asarray(wavelength, dtype=np.float64)
+        return np.vectorize(lambda x: rec.recover(self.xyz, x))(w).astype(np.float64)
+
+    @property
+    def luminance(self) -> float:
+        return self.xyz[1]
+
+    def isChromatic(self) -> bool:
+        return True
+
+
+def rgb(r, g=None, b=None, space=None) -> Xyz:
+    """rgb(r, g, b[, space]) or rgb((r, g, b)[, space]) (kernel/rgb_space.cpp:402-419): the colour in
+    the RGB space (sRGB by default) as a tristimulus spectrum."""
+    from .recovery import sRGB, RgbSpace
+    if g is None or isinstance(g, RgbSpace):
+        space = g if isinstance(g, RgbSpace) else space
+        r, g, b = tuple(r)[:3]
+    return Xyz((space or sRGB).toXYZ((r, g, b)))
+
+
 def spd(name: str, component: str = "n") -> Sampled:
     """Complex refractive index table of a metal (Ag, Al, Au, Cu) as a Sampled spectrum of n or k,
     the data the reference ships as data/spd/*.spd (read by src/liar/tools/spd.py)."""

@@ -1006,7 +1006,7 @@ void* oracle_scene_create(const SceneIn* in) {
         if (s.type == SP_SAMPLED) {
             float mx = -INFINITY;
             for (int i = 0; i < s.count; ++i) mx = std::max(mx, in->pool[s.offset + s.count + i]);
-            S->spec_max[k] = mx;
+            S->spec_max[k] = s.p[0] > 0.0f ? s.p[0] : mx;
         }
     }
     const uint64_t nl = in->n_lights;
