@@ -213,8 +213,25 @@ typedef struct liar_camera {
 /* ADJOINT_PHOTON: src/liar/tracers/adjoint_photon_tracer.cpp (unidirectional path tracing);
  * DIRECT_LIGHTING: src/liar/tracers/direct_lighting.cpp (direct light by
  * RayTracer::estimateLightContribution, kernel/ray_tracer.cpp:188-276, plus recursive specular
- * and glossy reflection/transmission up to max_ray_generation) */
-enum liar_tracer_type { LIAR_TRACER_ADJOINT_PHOTON = 0, LIAR_TRACER_DIRECT_LIGHTING = 1 };
+ * and glossy reflection/transmission up to max_ray_generation);
+ * PHOTON_MAPPER: src/liar/tracers/photon_mapper.cpp (DirectLighting plus, at every vertex with a
+ * diffuse part, the caustic map's Gaussian-filtered estimate and the global map's radiance
+ * estimate, photon_mapper.cpp:466-518, 1282-1381; photon maps filled per render as
+ * fillPhotonMaps / buildPhotonMap, :573-835; no final gather, the reference's default) */
+enum liar_tracer_type { LIAR_TRACER_ADJOINT_PHOTON = 0, LIAR_TRACER_DIRECT_LIGHTING = 1, LIAR_TRACER_PHOTON_MAPPER = 2 };
+
+/* PhotonMapper settings (photon_mapper.cpp:108-142 defaults). Map 0 is the global map, map 1 the
+ * caustic map. Photons bounce up to max_ray_generation; the seed of the photons is the render's. */
+typedef struct liar_photon_mapper_desc {
+    uint64_t max_photons;           /* maxNumberOfPhotons: emission stops here (0 = 10^8) */
+    uint64_t global_map_size;       /* globalMapSize: emission stops once the global map holds this (0 = 10000) */
+    float estimation_radius[2];     /* rMax of the estimates; 0 = automatic (buildPhotonMap, :815-833) */
+    float estimation_tolerance[2];  /* of the automatic radius (0 = 0.05) */
+    int32_t estimation_size[2];     /* photons per estimate, at most 64 (0 = 50) */
+    int32_t ray_trace_direct;       /* isRayTracingDirect: -1 = false (direct light from the global map), else true */
+    int32_t visualize;              /* isVisualizingPhotonMap: nonzero renders the global map's irradiance */
+} liar_photon_mapper_desc;
+
 typedef struct liar_render_desc {
     liar_camera camera;
     int32_t width, height, spp;
@@ -233,6 +250,7 @@ typedef struct liar_render_desc {
     int32_t filter;
     float filter_param;          /* triangle: width (0 = 1); Mitchell: B (0 = 1/3) */
     float max_sample_luminance;  /* Raster.maxSampleLuminance (output/raster.cpp:572-575); 0 = no clamp */
+    liar_photon_mapper_desc photon_mapper;  /* tracer PHOTON_MAPPER only */
 } liar_render_desc;
 
 enum liar_filter { LIAR_FILTER_BOX = 0, LIAR_FILTER_TRIANGLE = 1, LIAR_FILTER_MITCHELL = 2 };
@@ -335,6 +353,23 @@ int liar_gpu_render_guided_device(liar_gpu_ctx* ctx, const liar_gpu_scene* scene
  * hit, [3] directions drawn from the guide */
 int liar_gpu_render_guided_stats(const liar_gpu_ctx* ctx, unsigned long long* out4);
 
+/* ---- spectra of tristimulus values ------------------------------------------------------------
+ * The context's standard recovery, as the reference's liar.Recovery.setStandard with a
+ * RecoveryMengSimon (src/liar/__init__.py:72-79, spectra/recovery_meng_simon.cpp:93-310): spectra
+ * (n_samples x n_wavelengths, wavelengths in metres, increasing) sampled at chromaticities xy
+ * (n_samples x 2, inside [-0.3, 1.0] x [-0.3, 1.2]), and the Delaunay triangulation of those
+ * points followed by the box corners (-0.3, -0.3), (1.0, -0.3), (1.0, 1.2), (-0.3, 1.2) as point
+ * indices n_samples .. n_samples + 3 (n_triangles x 3). The PhotonMapper needs it (photon powers
+ * are XYZ, Spectral::fromXYZ); liar_b200 sets the reference's table on every context it renders
+ * with. A colour is the barycentric blend of the spectra at its triangle's corners (zero at the
+ * box corners), the weights scaled to sum to X + Y + Z. */
+int liar_gpu_set_recovery(liar_gpu_ctx* ctx, const float* wavelengths, int n_wavelengths, const float* xy,
+                          const float* spectra, int n_samples, const int32_t* triangles, int n_triangles);
+/* The blend of each of n XYZ colours (d_xyz: n x 3): sample indices (n x 3, -1 = none) and weights
+ * (n x 3); colours without a recovery get -1 and 0. */
+int liar_gpu_recovery_locate_device(liar_gpu_ctx* ctx, const float* d_xyz, size_t n, int32_t* d_idx,
+                                    float* d_weights, void* stream);
+
 /* ---- photon maps -------------------------------------------------------------------------------
  * Replace the Lass KdTree<Photon> of PhotonMapper::buildPhotonMap (src/liar/tracers/photon_mapper.cpp:798-835)
  * and its rangeSearch(point, maxRadius, maxCount) (photon_mapper.cpp:1097,1257,1312,1352): for each
@@ -392,6 +427,16 @@ typedef struct liar_photon_counts {
 } liar_photon_counts;
 int liar_gpu_photon_trace(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_photon_desc* desc,
                           const liar_photon_buffers* out, liar_photon_counts* counts, void* stream);
+/* The photon maps of the last PhotonMapper render on ctx (kept for the next render of the same
+ * scene and settings): [0] photons shot, [1] global map size, [2] caustic map size, [3] 1 when maps
+ * exist; radii (2 floats, may be NULL): the global and caustic estimation radii in use.
+ * (PhotonMapper::doPreProcess statistics, src/liar/tracers/photon_mapper.cpp:372-390.) */
+int liar_gpu_photon_mapper_stats(const liar_gpu_ctx* ctx, unsigned long long* out4, float* radii);
+/* Copies map `map` (0 global, 1 caustic) of those maps to host arrays of `capacity` photons (any may
+ * be NULL): positions, directions toward where the photons came from and scaled XYZ powers (n x 3
+ * floats each), and the powers' recovery blends (n x 3 indices, n x 3 weights); *n_out = photons. */
+int liar_gpu_photon_mapper_get_map(liar_gpu_ctx* ctx, int map, float* position, float* omega_in, float* power,
+                                   int32_t* blend_idx, float* blend_w, size_t capacity, size_t* n_out);
 
 /* Allocation-free closest hit / any hit. It has no counterpart in the reference; it exists for
  * callers that must not call cudaMalloc while they trace: an application whose own pool

@@ -93,6 +93,10 @@ SIGNATURES: dict[str, tuple] = {
     "liar_gpu_photon_gather": (C.c_int, [_vp, _vp, _vp, _sz, C.c_int, _vp, _vp, _vp]),
     "liar_gpu_photon_gather_device": (C.c_int, [_vp, _vp, _vp, _sz, C.c_int, _vp, _vp, _vp, _vp]),
     "liar_gpu_photon_trace": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "liar_gpu_photon_mapper_stats": (C.c_int, [_vp, _vp, _vp]),
+    "liar_gpu_photon_mapper_get_map": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_size_t, _vp]),
+    "liar_gpu_set_recovery": (C.c_int, [_vp, _vp, C.c_int, _vp, _vp, C.c_int, _vp, C.c_int]),
+    "liar_gpu_recovery_locate_device": (C.c_int, [_vp, _vp, C.c_size_t, _vp, _vp, _vp]),
     "liar_gpu_photon_estimate_device": (C.c_int, [_vp, _vp, _vp, _sz, _vp, _sz, C.c_int, _vp, _vp, _vp, C.c_float,
                                                   _vp, _vp]),
     # batched rendering (liar_b200/batch.py)

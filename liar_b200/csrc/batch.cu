@@ -253,17 +253,19 @@ __global__ void __launch_bounds__(128) k_b_shade(BParams P, BState<H> st, BQueue
                 const int light = HC.light, mi = HC.mat;
                 if (gen > 0 && light >= 0)
                     for (int k = 0; k < H; ++k) L[k] += T[k] * spec_eval(S, S.lights[light].spectrum, lam[k], false);
-                if (mi < 0 || S.mats[mi].type == LIAR_MAT_NONE) {
-                    if (mi >= 0 && light < 0 && S.mats[mi].emission >= 0)
-                        for (int k = 0; k < H; ++k) L[k] += T[k] * spec_eval(S, S.mats[mi].emission, lam[k], false);
+                const bool shader_emits = gen == 0 || light < 0;  // as render.cu
+                if (mi < 0) {
                     alive = true;
                     next_o = o;
                     next_d = d;
                     next_tmin = h.t + kTol;
                     next_tmax = r1.w;
+                } else if (S.mats[mi].type == LIAR_MAT_NONE) {
+                    if (shader_emits && S.mats[mi].emission >= 0)
+                        for (int k = 0; k < H; ++k) L[k] += T[k] * spec_eval(S, S.mats[mi].emission, lam[k], false);
                 } else {
                     const liar_material M = S.mats[mi];
-                    if (light < 0 && M.emission >= 0)
+                    if (shader_emits && M.emission >= 0)
                         for (int k = 0; k < H; ++k) L[k] += T[k] * spec_eval(S, M.emission, lam[k], false);
                     const Bsdf B = make_bsdf(S, M, HC, lam[0]);
                     const float3 md = -d;

@@ -23,6 +23,7 @@
 
 #include "../../include/liar_gpu.h"
 #include "ctx.h"
+#include "photon_mapper.h"
 #include "render_dev.cuh"
 
 using namespace liar_gpu;
@@ -76,6 +77,13 @@ struct DParams {
     uint32_t glossy;  // CAP_GLOSSY when glossy reflection/transmission is traced
     unsigned long long* stats;
     FilmSpec film;
+    // PhotonMapper (photon_mapper.cpp:466-518): 0 off, 1 render, 2 visualise the photon map;
+    // vertices that estimate from the maps append their hit point and task index here
+    int pm;
+    int pm_direct;       // isRayTracingDirect
+    float* q_pos;
+    uint32_t* q_task;
+    uint32_t* q_count;
 };
 
 // sampler dimensions (disjoint from the path tracer's and from each other)
@@ -253,11 +261,25 @@ __global__ void __launch_bounds__(128) k_dl_shade(DScene S, DParams W, DSamples 
                 B = make_bsdf(S, M, HC, lam);
                 has_bsdf = true;
                 n_sh = hq ? shadow_hq : (S.n_lights > 0 ? 2u * (uint32_t)W.n_secondary : 0u);
-                if (compatible_caps(B.caps, sg) && more) {
+                if (W.pm == 2 || (W.pm == 1 && !W.pm_direct)) n_sh = 0u;  // no traced direct light
+                if (compatible_caps(B.caps, sg) && more && W.pm != 2) {
                     const uint32_t ns = hq ? (uint32_t)(M.samples > 0 ? M.samples : 1) : 1u;
                     n_ch = (has_caps(B.caps, CAP_REFL) ? ns : 0u) + (has_caps(B.caps, CAP_TRANS) ? ns : 0u);
                 }
             }
+        }
+    }
+    // PhotonMapper: vertices with a shader query the photon maps (the visualisation), or those with
+    // a diffuse component do (estimateCaustics, estimateRadiance)
+    const bool query = W.pm != 0 && shading && HC.mat >= 0 &&
+                       (W.pm == 2 || (has_bsdf && has_caps(B.caps, CAP_DIFF)));
+    if (W.pm != 0) {  // uniform over the launch: every lane of the warp takes the reservation
+        const uint32_t qi = warp_reserve(W.q_count, query ? 1u : 0u);
+        if (query) {
+            W.q_pos[3 * (size_t)qi] = HC.target.x;
+            W.q_pos[3 * (size_t)qi + 1] = HC.target.y;
+            W.q_pos[3 * (size_t)qi + 2] = HC.target.z;
+            W.q_task[qi] = q;
         }
     }
     ShadowWriter sw{sh, warp_reserve(sh.count, n_sh), 0u, n_sh};
@@ -284,14 +306,17 @@ __global__ void __launch_bounds__(128) k_dl_shade(DScene S, DParams W, DSamples 
         } else {
             const SampleKey skey = dkey(W, W.first_path + p);
             // shader emission: camera rays see light objects, other emitters are always seen
-            if ((gen == 0 || HC.light < 0) && M.emission >= 0) atomicAdd(&P.L[p], T * spec_eval(S, M.emission, lam, false));
-            if (has_bsdf) {
+            if (W.pm != 2 && (gen == 0 || HC.light < 0) && M.emission >= 0)
+                atomicAdd(&P.L[p], T * spec_eval(S, M.emission, lam, false));
+            if (has_bsdf && W.pm != 2) {
                 const float3 md = -d;
                 float3 wi = mk(dot(md, HC.u), dot(md, HC.v), dot(md, HC.N));
                 wi.z = fmaxf(wi.z, kEps);
                 const float3 start = HC.target + (10.0f * kTol) * HC.N;
                 // ---- direct light (traceDirect)
-                if (hq) {
+                if (W.pm == 1 && !W.pm_direct) {
+                    // the PhotonMapper without traced direct light: the global map holds it
+                } else if (hq) {
                     for (int l = 0; l < S.n_lights; ++l) {
                         const liar_light& L = S.lights[l];
                         const int nl = L.emission_samples > 0 ? L.emission_samples : 1;
@@ -379,6 +404,92 @@ __global__ void k_dl_shadow_add(DShadows sh, uint32_t n, const liar_hit* __restr
     if (v != 0.0f && hits[i].prim < 0) atomicAdd(&L[sh.slot[i]], v);
 }
 
+// ---- PhotonMapper estimates at the queried vertices (photon_mapper.cpp:1282-1381, 1254-1279)
+enum { kEstRadiance = 0, kEstCaustics = 1, kEstIrradiance = 2 };
+
+// Photon::spectralPower: the XYZ power as a spectrum at the sample's wavelength (Spectral::fromXYZ,
+// an illuminant), through the photon's precomputed blend
+__device__ __forceinline__ float photon_power(const PmMap& M, const DRecovery& R, int32_t i, float lam) {
+    RecoveryBlend b;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        b.idx[j] = M.blend_idx[3 * (size_t)i + j];
+        b.w[j] = M.blend_w[3 * (size_t)i + j];
+    }
+    return recovery_eval(R, b, lam, false);
+}
+
+// one thread per queried vertex: the vertex's BSDF against the k nearest photons of one map
+//   kEstRadiance:   sum f(w, w_p) Phi_p(lam) / (pi r^2), f without its specular and glossy parts,
+//                   at least two photons (estimateRadiance without an irradiance map)
+//   kEstCaustics:   the same with the Gaussian filter w = alpha (1 - (1 - e^(-beta d^2 / 2r^2)) /
+//                   (1 - e^-beta)), alpha 0.918, beta 1.953, f's diffuse part (estimateCaustics)
+//   kEstIrradiance: the XYZ of the photons arriving from the normal's side over pi r^2, as a
+//                   spectrum at lam (isVisualizingPhotonMap: estimateIrradianceImpl)
+// r^2 is the squared distance of the farthest photon found; the result, times the task's weight,
+// is added to the sample's radiance
+__global__ void __launch_bounds__(128) k_pm_estimate(DScene S, DParams W, DSamples P, DTasks tin,
+                                                     const liar_hit* __restrict__ hits, const uint32_t* __restrict__ q_task,
+                                                     uint32_t n_q, PmMap M, DRecovery R, int kind,
+                                                     const int32_t* __restrict__ g_idx, const float* __restrict__ g_d2,
+                                                     const int32_t* __restrict__ g_cnt) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_q) return;
+    const int k = M.k;
+    const int cnt = min(g_cnt[i], k);
+    if (cnt < (kind == kEstIrradiance ? 1 : 2)) return;
+    const uint32_t q = q_task[i];
+    const uint32_t p = tin.slot[q];
+    const float T = tin.T[q];
+    const float4 r0 = reinterpret_cast<const float4*>(tin.rays + q)[0];
+    const float4 r1 = reinterpret_cast<const float4*>(tin.rays + q)[1];
+    const float3 d = mk(r1.x, r1.y, r1.z);
+    const HitContext HC = hit_context(S, mk(r0.x, r0.y, r0.z), d, (uint32_t)hits[q].prim);
+    const float lam = P.lam[p];
+    const int32_t* idx = g_idx + (size_t)i * k;
+    const float r2 = g_d2[(size_t)i * k + cnt - 1];
+    if (!(r2 > 0.0f)) return;
+    float result = 0.0f;
+    if (kind == kEstIrradiance) {
+        float X = 0.0f, Y = 0.0f, Z = 0.0f;
+        for (int j = 0; j < cnt; ++j) {
+            const int32_t ph = idx[j];
+            if (ph < 0 || (uint64_t)ph >= M.n) continue;
+            if (M.omega_in[3 * (size_t)ph] * HC.N.x + M.omega_in[3 * (size_t)ph + 1] * HC.N.y +
+                    M.omega_in[3 * (size_t)ph + 2] * HC.N.z > 0.0f) {
+                X += M.power[3 * (size_t)ph];
+                Y += M.power[3 * (size_t)ph + 1];
+                Z += M.power[3 * (size_t)ph + 2];
+            }
+        }
+        const float inv = 1.0f / (3.14159265358979323846f * r2);
+        RecoveryBlend b;
+        if (recovery_locate(R, X * inv, Y * inv, Z * inv, b)) result = recovery_eval(R, b, lam, false);
+    } else {
+        const liar_material Mat = S.mats[HC.mat];
+        const Bsdf B = make_bsdf(S, Mat, HC, lam);
+        const float3 md = -d;
+        float3 wi = mk(dot(md, HC.u), dot(md, HC.v), dot(md, HC.N));
+        wi.z = fmaxf(wi.z, kEps);
+        const uint32_t caps = kind == kEstRadiance ? (CAP_ALL & ~CAP_SPEC & ~CAP_GLOSSY) : (CAP_REFL | CAP_TRANS | CAP_DIFF);
+        const float alpha = 0.918f, beta = 1.953f;
+        const float b1 = -beta / (2.0f * r2), b2 = 1.0f / (1.0f - expf(-beta));
+        for (int j = 0; j < cnt; ++j) {
+            const int32_t ph = idx[j];
+            if (ph < 0 || (uint64_t)ph >= M.n) continue;
+            const float3 om = mk(M.omega_in[3 * (size_t)ph], M.omega_in[3 * (size_t)ph + 1], M.omega_in[3 * (size_t)ph + 2]);
+            const float3 wo = mk(dot(om, HC.u), dot(om, HC.v), dot(om, HC.N));
+            const BsdfOut be = bsdf_evaluate(B, wi, wo, caps);
+            if (!(be.pdf > 0.0f) || be.value == 0.0f) continue;
+            float v = be.value * photon_power(M, R, ph, lam);
+            if (kind == kEstCaustics) v *= alpha * (1.0f - b2 * (1.0f - expf(b1 * g_d2[(size_t)i * k + j])));
+            result += v;
+        }
+        result /= 3.14159265358979323846f * r2;
+    }
+    if (result != 0.0f) atomicAdd(&P.L[p], T * result);
+}
+
 __global__ void k_dl_splat(DScene S, DParams W, DSamples P, uint32_t n) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -399,8 +510,14 @@ struct DirectBuffers {
     void* shadows = nullptr;
     liar_hit* hits = nullptr;
     size_t hits_cap = 0;
-    uint32_t* counters = nullptr;  // [0] task count A, [1] task count B, [2] shadow count
+    uint32_t* counters = nullptr;  // [0] task count A, [1] task count B, [2] shadow count, [3] map queries
     uint32_t* h_counters = nullptr;
+    // PhotonMapper: the queried vertices (3 floats, a task index and a gather count each) and one
+    // map's gather results (k indices and squared distances per vertex)
+    void* queries = nullptr;
+    size_t n_queries = 0;
+    void* gathers = nullptr;
+    size_t n_gathers = 0;
 };
 
 DirectBuffers* direct_buffers(liar_gpu_ctx* ctx) {
@@ -409,7 +526,8 @@ DirectBuffers* direct_buffers(liar_gpu_ctx* ctx) {
     DirectBuffers* b = new DirectBuffers();
     ctx->extensions.emplace_back("direct", b);
     ctx->on_destroy.push_back([b]() {
-        for (void* p : {b->samples, b->tasks[0], b->tasks[1], b->shadows, (void*)b->hits, (void*)b->counters})
+        for (void* p : {b->samples, b->tasks[0], b->tasks[1], b->shadows, (void*)b->hits, (void*)b->counters, b->queries,
+                        b->gathers})
             if (p) cudaFree(p);
         if (b->h_counters) cudaFreeHost(b->h_counters);
         delete b;
@@ -450,7 +568,7 @@ namespace liar_gpu {
 namespace rt {
 
 int render_direct(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_render_desc& R, float* d_film,
-                  cudaStream_t st) {
+                  cudaStream_t st, const PmMaps* pm) {
     if (R.max_ray_generation < 0 || R.max_ray_generation > 250)
         return ctx_fail(ctx, LIAR_ERR_INVALID, "max_ray_generation must lie in [0, 250]");
     const uint64_t total = (uint64_t)R.width * R.height * R.spp;
@@ -501,6 +619,11 @@ int render_direct(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_ren
     W.n_secondary = n_sec;
     W.glossy = R.trace_glossy < 0 ? 0u : CAP_GLOSSY;
     W.stats = stats;
+    W.pm = pm ? (pm->visualize ? 2 : 1) : 0;
+    W.pm_direct = pm ? pm->ray_direct : 1;
+    W.q_pos = nullptr;
+    W.q_task = nullptr;
+    W.q_count = b->counters + 3;
     const DScene& S = scene_dscene(scene);
     const liar_gpu_mesh* mesh = scene_mesh(scene);
     for (uint64_t first = 0; first < total; first += wave) {
@@ -535,6 +658,11 @@ int render_direct(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_ren
                 rc = grow(ctx, &hp, &b->hits_cap, std::max<uint64_t>(want_shadows, n_in), 8, "direct lighting hits");
                 b->hits = static_cast<liar_hit*>(hp);
             }
+            if (!rc && pm) {
+                rc = grow(ctx, &b->queries, &b->n_queries, n_in, 20, "photon map queries");
+                W.q_pos = static_cast<float*>(b->queries);
+                W.q_task = reinterpret_cast<uint32_t*>(static_cast<char*>(b->queries) + b->n_queries * 12);
+            }
             if (rc) return rc;
             const DTasks tin = task_view(b->tasks[cur], b->n_tasks[cur], b->counters + cur);
             const DTasks tout = task_view(b->tasks[cur ^ 1], b->n_tasks[cur ^ 1], b->counters + (cur ^ 1));
@@ -547,7 +675,7 @@ int render_direct(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_ren
             rc = trace_mesh_internal(ctx, mesh, tin.rays, n_in, b->hits, 0, st, kCounterWord + 10);
             if (rc) return rc;
             e = cudaMemsetAsync(b->counters + (cur ^ 1), 0, 4, st);
-            if (e == cudaSuccess) e = cudaMemsetAsync(b->counters + 2, 0, 4, st);
+            if (e == cudaSuccess) e = cudaMemsetAsync(b->counters + 2, 0, 8, st);
             if (e != cudaSuccess) return ctx_cuda(ctx, e, "reset queues");
             k_dl_shade<<<(n_in + 127) / 128, 128, 0, st>>>(S, W, P, tin, b->hits, n_in, tout, sq, (uint32_t)sh_hq);
             e = cudaGetLastError();
@@ -558,6 +686,26 @@ int render_direct(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_ren
             const uint32_t n_sh = b->h_counters[2];
             if ((uint64_t)n_sh > want_shadows || (uint64_t)b->h_counters[cur ^ 1] > want_children)
                 return ctx_fail(ctx, LIAR_ERR_INVALID, "direct lighting queue overflow");
+            // the photon-map estimates of the queried vertices, while the tasks' hits are current
+            const uint32_t n_q = pm ? b->h_counters[3] : 0u;
+            if (n_q > n_in) return ctx_fail(ctx, LIAR_ERR_INVALID, "photon map query overflow");
+            for (int m = 0; n_q > 0 && m < 2; ++m) {
+                const PmMap& M = pm->map[m];
+                if (pm->visualize && m != kPmGlobal) continue;
+                if (M.n == 0 || M.k < 1 || !M.grid) continue;
+                rc = grow(ctx, &b->gathers, &b->n_gathers, (size_t)n_q * M.k, 8, "photon gathers");
+                if (rc) return rc;
+                int32_t* g_idx = static_cast<int32_t*>(b->gathers);
+                float* g_d2 = reinterpret_cast<float*>(g_idx + b->n_gathers);
+                int32_t* g_cnt = reinterpret_cast<int32_t*>(b->queries) + 4 * b->n_queries;  // after positions and tasks
+                rc = liar_gpu_photon_gather_device(ctx, M.grid, W.q_pos, n_q, M.k, g_idx, g_d2, g_cnt, st);
+                if (rc) return rc;
+                const int kind = pm->visualize ? kEstIrradiance : (m == kPmGlobal ? kEstRadiance : kEstCaustics);
+                k_pm_estimate<<<(n_q + 127) / 128, 128, 0, st>>>(S, W, P, tin, b->hits, W.q_task, n_q, M, pm->rec, kind,
+                                                                  g_idx, g_d2, g_cnt);
+                e = cudaGetLastError();
+                if (e != cudaSuccess) return ctx_cuda(ctx, e, "photon estimate launch");
+            }
             if (n_sh > 0) {
                 rc = trace_mesh_internal(ctx, mesh, sq.rays, n_sh, b->hits, 1, st, kCounterWord + 10);
                 if (rc) return rc;

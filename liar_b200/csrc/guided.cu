@@ -254,15 +254,18 @@ __global__ void __launch_bounds__(kShadeThreads) k_g_shade(DScene S, GParams W, 
                 const int light = HC.light, mi = HC.mat;
                 const float3 target = HC.target, ng = HC.ng, N = HC.N, u = HC.u, v = HC.v;
                 if (gen > 0 && light >= 0) L += T * spec_eval(S, S.lights[light].spectrum, lam, false);
-                if (!surface) {
-                    if (mi >= 0 && light < 0 && S.mats[mi].emission >= 0) L += T * spec_eval(S, S.mats[mi].emission, lam, false);
-                    alive = true;
+                const bool shader_emits = gen == 0 || light < 0;  // as render.cu
+                if (mi < 0) {
+                    alive = true;  // no shader: continue through
                     next_o = o;
                     next_d = d;
                     next_tmin = h.t + kTol;
                     next_tmax = r1.w;
+                } else if (!surface) {
+                    // a shader without a BSDF: its emission, and the path ends
+                    if (shader_emits && S.mats[mi].emission >= 0) L += T * spec_eval(S, S.mats[mi].emission, lam, false);
                 } else {
-                    if (light < 0 && M.emission >= 0) L += T * spec_eval(S, M.emission, lam, false);
+                    if (shader_emits && M.emission >= 0) L += T * spec_eval(S, M.emission, lam, false);
                     const Bsdf B = make_bsdf(S, M, HC, lam);
                     const float3 md = -d;
                     float3 wi = mk(dot(md, u), dot(md, v), dot(md, N));

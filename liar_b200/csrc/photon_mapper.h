@@ -1,0 +1,41 @@
+// photon_mapper.h -- the photon maps a PhotonMapper render reads (src/liar/tracers/photon_mapper.cpp),
+// shared by the map builder (photon_mapper.cu) and the DirectLighting wavefront that shades with
+// them (direct.cu).
+#pragma once
+#include <stdint.h>
+
+#include "../../include/liar_gpu.h"
+#include "recovery.cuh"
+
+namespace liar_gpu {
+
+enum PmMapKind { kPmGlobal = 0, kPmCaustic = 1 };
+
+// one photon map on the device: the photons in the reference's buffer order (emission, then
+// bounce), their power scaled by 1 / photons emitted, and each power's spectral blend
+struct PmMap {
+    const liar_gpu_photon_map* grid = nullptr;  // gather structure over the positions
+    const float* position = nullptr;            // n x 3
+    const float* omega_in = nullptr;            // n x 3, toward where the photon came from
+    const float* power = nullptr;               // n x 3, XYZ
+    const int32_t* blend_idx = nullptr;         // n x 3 (RecoveryBlend of the power)
+    const float* blend_w = nullptr;             // n x 3
+    uint64_t n = 0;
+    float radius = 0.0f;                        // estimationRadius (rMax of the gathers)
+    int k = 0;                                  // estimationSize (kMax of the gathers)
+};
+
+struct PmMaps {
+    PmMap map[2];
+    DRecovery rec;
+    int visualize = 0;     // isVisualizingPhotonMap
+    int ray_direct = 1;    // isRayTracingDirect
+    uint64_t emitted = 0;  // photons shot
+};
+
+namespace rt {
+int render_direct(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_render_desc& R, float* d_film,
+                  cudaStream_t st, const PmMaps* pm);
+}  // namespace rt
+
+}  // namespace liar_gpu

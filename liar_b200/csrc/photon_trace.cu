@@ -156,13 +156,16 @@ __global__ void __launch_bounds__(128) k_photon_shade(DScene S, PParams P, PStat
             const HitContext H = hit_context(S, o, d, (uint32_t)h.prim);
             const float3 hit_point = o + h.t * d;
             const int mi = H.mat;
-            if (mi < 0 || S.mats[mi].type == LIAR_MAT_NONE) {
+            if (mi < 0) {
                 // no shader: entering or leaving something, continue through
                 if (gen < P.max_gen) {
                     nr = liar_ray{o.x, o.y, o.z, h.t + kTol, d.x, d.y, d.z, r1.w};
                     st.gen[slot] = gen + 1;
                     want = true;
                 }
+            } else if (S.mats[mi].type == LIAR_MAT_NONE) {
+                // a shader without a BSDF (Unshaded) stores nothing and absorbs the photon
+                // (tracePhoton: no diffuse caps, shader->bsdf() is null)
             } else {
                 const liar_material M = S.mats[mi];
                 if (M.type == LIAR_MAT_LAMBERT) {

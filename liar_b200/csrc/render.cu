@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -25,6 +26,7 @@
 
 #include "../../include/liar_gpu.h"
 #include "ctx.h"
+#include "photon_mapper.h"
 #include "render_dev.cuh"
 
 using namespace liar_gpu;
@@ -32,6 +34,7 @@ using namespace liar_gpu::rt;
 
 struct liar_gpu_scene {
     int device = -1;
+    uint64_t uid = 0;  // unique per upload in the process (keys caches of derived data)
     liar_gpu_mesh* mesh = nullptr;
     std::vector<void*> buffers;  // device allocations owned by the scene
     DScene d{};
@@ -186,17 +189,22 @@ __global__ void __launch_bounds__(128) k_shade(DScene S, WaveParams W, Paths P, 
                 // LightArea::doEmission: radiance of the light object that was hit
                 L += T * spec_eval(S, S.lights[light].spectrum, lam, false);
             }
-            if (mi < 0 || S.mats[mi].type == LIAR_MAT_NONE) {
-                if (mi >= 0 && light < 0 && S.mats[mi].emission >= 0) L += T * spec_eval(S, S.mats[mi].emission, lam, false);
-                // no BSDF: continue through (bound(ray, t + tolerance, far))
+            // the shader's emission counts unless a light was hit past the camera vertex (the
+            // reference asks the object for its light only at generations > 0)
+            const bool shader_emits = gen == 0 || light < 0;
+            if (mi < 0) {
+                // no shader: entering or leaving something, continue through (bound(ray, t + tolerance, far))
                 alive = true;
                 next_o = o;
                 next_d = d;
                 next_tmin = h.t + kTol;
                 next_tmax = r1.w;
+            } else if (S.mats[mi].type == LIAR_MAT_NONE) {
+                // a shader without a BSDF (Unshaded): its emission, and the path ends
+                if (shader_emits && S.mats[mi].emission >= 0) L += T * spec_eval(S, S.mats[mi].emission, lam, false);
             } else {
                 const liar_material M = S.mats[mi];
-                if (light < 0 && M.emission >= 0) L += T * spec_eval(S, M.emission, lam, false);
+                if (shader_emits && M.emission >= 0) L += T * spec_eval(S, M.emission, lam, false);
                 const Bsdf B = make_bsdf(S, M, H, lam);  // Shader::bsdf at this wavelength
                 const float3 md = -d;
                 float3 wi = mk(dot(md, u), dot(md, v), dot(md, N));
@@ -505,6 +513,8 @@ extern "C" int liar_gpu_scene_upload(liar_gpu_ctx* ctx, const liar_scene_desc* d
     liar_gpu_scene* s = new (std::nothrow) liar_gpu_scene();
     if (!s) return ctx_fail(ctx, LIAR_ERR_OOM, "host allocation");
     s->device = ctx->device;
+    static std::atomic<uint64_t> next_uid{1};
+    s->uid = next_uid.fetch_add(1);
     rc = liar_gpu_mesh_build(ctx, D.vertices, D.n_vertices, D.triangles, D.n_triangles, nullptr, &s->mesh);
     DScene& d = s->d;
     if (!rc) rc = upload(ctx, s, D.vertices, 3 * D.n_vertices, &d.verts, "scene vertices");
@@ -560,6 +570,7 @@ unsigned long long* render_stats_device(liar_gpu_ctx* ctx, cudaStream_t st) {
 }
 const liar_gpu_mesh* scene_mesh(const liar_gpu_scene* s) { return s->mesh; }
 int scene_device(const liar_gpu_scene* s) { return s->device; }
+uint64_t scene_uid(const liar_gpu_scene* s) { return s->uid; }
 }  // namespace rt
 }  // namespace liar_gpu
 
@@ -576,9 +587,9 @@ extern "C" void liar_gpu_scene_destroy(liar_gpu_scene* s) {
 
 namespace liar_gpu {
 namespace rt {
-// DirectLighting (direct.cu)
-int render_direct(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_render_desc& R, float* d_film,
-                  cudaStream_t st);
+// PhotonMapper (photon_mapper.cu): photon maps, then the DirectLighting wavefront with their estimates
+int render_photon_mapper(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_render_desc& R, float* d_film,
+                         cudaStream_t st);
 }  // namespace rt
 }  // namespace liar_gpu
 
@@ -590,7 +601,8 @@ int render_impl(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_rende
     if (R.width <= 0 || R.height <= 0 || R.spp <= 0) return ctx_fail(ctx, LIAR_ERR_INVALID, "empty image or no samples");
     if (R.max_ray_generation < 0) return ctx_fail(ctx, LIAR_ERR_INVALID, "max_ray_generation must be >= 0");
     if (const char* m = film_desc_error(R)) return ctx_fail(ctx, LIAR_ERR_INVALID, "%s", m);
-    if (R.tracer == LIAR_TRACER_DIRECT_LIGHTING) return render_direct(ctx, scene, R, d_film, st);
+    if (R.tracer == LIAR_TRACER_DIRECT_LIGHTING) return render_direct(ctx, scene, R, d_film, st, nullptr);
+    if (R.tracer == LIAR_TRACER_PHOTON_MAPPER) return render_photon_mapper(ctx, scene, R, d_film, st);
     if (R.tracer != LIAR_TRACER_ADJOINT_PHOTON) return ctx_fail(ctx, LIAR_ERR_UNSUPPORTED, "tracer %d", R.tracer);
     const uint64_t total = (uint64_t)R.width * R.height * R.spp;
     if ((uint64_t)R.width * R.height >= (1ull << 32)) return ctx_fail(ctx, LIAR_ERR_INVALID, "image too large");

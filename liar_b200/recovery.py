@@ -112,6 +112,31 @@ def standard() -> RecoveryMengSimon:
     return RecoveryMengSimon(t["wavelengths"], [(tuple(xy), v) for xy, v in zip(t["xy"], t["spectra"])])
 
 
+def device_table(rec: RecoveryMengSimon | None = None) -> dict:
+    """The arrays liar_gpu_set_recovery takes: wavelengths, xy, spectra and the triangles (point
+    indices; the box corners follow the samples)."""
+    rec = rec or standard()
+    return {"wavelengths": np.ascontiguousarray(rec.wavelengths, dtype=np.float32),
+            "xy": np.ascontiguousarray(rec.points[:rec.n_samples], dtype=np.float32),
+            "points": np.ascontiguousarray(rec.points, dtype=np.float32),
+            "spectra": np.ascontiguousarray(rec.values, dtype=np.float32),
+            "triangles": np.ascontiguousarray(rec.triangulation.simplices, dtype=np.int32)}
+
+
+def set_standard_on(ctx) -> None:
+    """Sets the standard recovery on a device context (once per context)."""
+    import ctypes as C
+    if getattr(ctx, "_recovery_set", False):
+        return
+    t = device_table()
+    fn = ctx._lib.liar_gpu_set_recovery
+    fn.restype = C.c_int
+    fn.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int]
+    ctx.check(fn(ctx.handle, t["wavelengths"].ctypes.data, t["wavelengths"].size, t["xy"].ctypes.data,
+                 t["spectra"].ctypes.data, t["xy"].shape[0], t["triangles"].ctypes.data, t["triangles"].shape[0]))
+    ctx._recovery_set = True
+
+
 # ---- RGB spaces (kernel/rgb_space.cpp)
 
 _BRADFORD = np.array([[0.8951, 0.2664, -0.1614], [-0.7502, 1.7135, 0.0367], [0.0389, -0.0685, 1.0296]])

@@ -55,12 +55,19 @@ class CCamera(C.Structure):
                 ("near_limit", C.c_float), ("far_limit", C.c_float)]
 
 
+class CPhotonMapperDesc(C.Structure):
+    _fields_ = [("max_photons", C.c_uint64), ("global_map_size", C.c_uint64),
+                ("estimation_radius", C.c_float * 2), ("estimation_tolerance", C.c_float * 2),
+                ("estimation_size", C.c_int32 * 2), ("ray_trace_direct", C.c_int32), ("visualize", C.c_int32)]
+
+
 class CRenderDesc(C.Structure):
     _fields_ = [("camera", CCamera), ("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32),
                 ("tracer", C.c_int32), ("max_ray_generation", C.c_int32), ("max_depth", C.c_int32),
                 ("seed", C.c_uint64), ("first_sample", C.c_int32), ("wave_paths", C.c_int32),
                 ("secondary_light_samples", C.c_int32), ("trace_glossy", C.c_int32),
-                ("filter", C.c_int32), ("filter_param", C.c_float), ("max_sample_luminance", C.c_float)]
+                ("filter", C.c_int32), ("filter_param", C.c_float), ("max_sample_luminance", C.c_float),
+                ("photon_mapper", CPhotonMapperDesc)]
 
 
 FILTER_BOX, FILTER_TRIANGLE, FILTER_MITCHELL = 0, 1, 2
@@ -387,6 +394,20 @@ def render_desc(camera, width: int, height: int, spp: int, tracer, seed: int = 0
     r.wave_paths = int(wave_paths)
     r.secondary_light_samples = int(getattr(tracer, "numberOfSecondaryLightSamples", 1))
     r.trace_glossy = 1 if getattr(tracer, "traceGlossy", True) else -1
+    if r.tracer == 2:
+        if getattr(tracer, "numFinalGatherRays", 0):
+            raise NotImplementedError("PhotonMapper final gathering is not on the GPU path (numFinalGatherRays = 0)")
+        if float(getattr(tracer, "causticsQuality", 1.0)) != 1.0:
+            raise NotImplementedError("PhotonMapper causticsQuality other than 1 is not on the GPU path")
+        pm = r.photon_mapper
+        pm.max_photons = int(tracer.maxNumberOfPhotons)
+        pm.global_map_size = int(tracer.globalMapSize)
+        for m in range(2):
+            pm.estimation_radius[m] = float(tracer._radius[m])
+            pm.estimation_tolerance[m] = float(tracer._tolerance[m])
+            pm.estimation_size[m] = int(tracer._size[m])
+        pm.ray_trace_direct = 1 if tracer.isRayTracingDirect else -1
+        pm.visualize = 1 if tracer.isVisualizingPhotonMap else 0
     r.filter = int(filter)
     r.filter_param = float(filter_param)
     r.max_sample_luminance = float(max_sample_luminance) if math.isfinite(max_sample_luminance) else 0.0
@@ -435,6 +456,8 @@ class GpuScene:
         d = flat.desc()
         ctx.check(lib.liar_gpu_scene_upload(ctx.handle, C.byref(d), C.byref(h)))
         self.handle = h
+        from .recovery import set_standard_on
+        set_standard_on(ctx)  # the PhotonMapper's Spectral::fromXYZ
 
     def close(self):
         if getattr(self, "handle", None):
@@ -463,3 +486,33 @@ class GpuScene:
         out = (C.c_ulonglong * 3)()
         self.ctx.check(self.ctx._lib.liar_gpu_render_stats(self.ctx.handle, out))
         return {"paths": out[0], "segments": out[1], "hits": out[2]}
+
+
+# ---- PhotonMapper maps (liar_gpu_photon_mapper_stats / _get_map)
+
+def photon_mapper_stats(ctx) -> dict:
+    """The photon maps of the last PhotonMapper render on ctx."""
+    out = (C.c_ulonglong * 4)()
+    radii = (C.c_float * 2)()
+    fn = ctx._lib.liar_gpu_photon_mapper_stats
+    fn.restype, fn.argtypes = C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]
+    ctx.check(fn(ctx.handle, out, radii))
+    return {"emitted": out[0], "global": out[1], "caustic": out[2], "valid": bool(out[3]),
+            "radius": (radii[0], radii[1])}
+
+
+def photon_mapper_map(ctx, m: int) -> dict:
+    """Map m (0 global, 1 caustic) of the last PhotonMapper render as host arrays."""
+    st = photon_mapper_stats(ctx)
+    n = int(st["global"] if m == 0 else st["caustic"])
+    a = {k: np.zeros((n, 3), np.float32) for k in ("position", "omega_in", "power", "blend_w")}
+    a["blend_idx"] = np.zeros((n, 3), np.int32)
+    got = C.c_size_t()
+    fn = ctx._lib.liar_gpu_photon_mapper_get_map
+    fn.restype = C.c_int
+    fn.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
+                   C.POINTER(C.c_size_t)]
+    ctx.check(fn(ctx.handle, int(m), a["position"].ctypes.data, a["omega_in"].ctypes.data, a["power"].ctypes.data,
+                 a["blend_idx"].ctypes.data, a["blend_w"].ctypes.data, n, C.byref(got)))
+    a["radius"] = st["radius"][m]
+    return a

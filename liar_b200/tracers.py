@@ -1,5 +1,7 @@
 """Ray tracers of the scene API (``liar.tracers``). AdjointPhotonTracer runs as the wavefront path
-tracer of liar_b200/csrc/render.cu (src/liar/tracers/adjoint_photon_tracer.cpp)."""
+tracer of liar_b200/csrc/render.cu (src/liar/tracers/adjoint_photon_tracer.cpp), DirectLighting and
+PhotonMapper as the task wavefront of liar_b200/csrc/direct.cu (src/liar/tracers/direct_lighting.cpp,
+photon_mapper.cpp)."""
 from __future__ import annotations
 
 
@@ -22,3 +24,51 @@ class DirectLighting(RayTracer):
         super().__init__()
         self.numberOfSecondaryLightSamples = 1   # direct_lighting.cpp:46-49
         self.traceGlossy = True
+
+
+class PhotonMapper(DirectLighting):
+    """Photon mapping (src/liar/tracers/photon_mapper.cpp): DirectLighting plus, at every vertex with
+    a diffuse part, the caustic map's Gaussian-filtered estimate and the global map's radiance
+    estimate; the maps are filled from the lights before rendering. Defaults as the reference's
+    (photon_mapper.cpp:108-142). Final gathering (numFinalGatherRays > 0) and volumetric maps are
+    not on the GPU path; causticsQuality other than 1 (its storage probabilities) neither."""
+    kind = 2
+    MAP_TYPES = {"global": 0, "caustic": 1, "caustics": 1}
+
+    def __init__(self):
+        super().__init__()
+        self.maxNumberOfPhotons = 100_000_000
+        self.globalMapSize = 10_000
+        self.causticsQuality = 1.0
+        self.numFinalGatherRays = 0
+        self.numSecondaryGatherRays = 1
+        self.ratioPrecomputedIrradiance = 0.25
+        self.isVisualizingPhotonMap = False
+        self.isRayTracingDirect = True
+        self._radius = [0.0, 0.0]
+        self._tolerance = [0.05, 0.05]
+        self._size = [50, 50]
+
+    def _map(self, mapType: str) -> int:
+        try:
+            return self.MAP_TYPES[mapType]
+        except KeyError:
+            raise KeyError(f"map type must be 'global' or 'caustic', not {mapType!r}") from None
+
+    def estimationRadius(self, mapType: str) -> float:
+        return self._radius[self._map(mapType)]
+
+    def setEstimationRadius(self, mapType: str, radius: float) -> None:
+        self._radius[self._map(mapType)] = float(radius)
+
+    def estimationTolerance(self, mapType: str) -> float:
+        return self._tolerance[self._map(mapType)]
+
+    def setEstimationTolerance(self, mapType: str, tolerance: float) -> None:
+        self._tolerance[self._map(mapType)] = float(tolerance)
+
+    def estimationSize(self, mapType: str) -> int:
+        return self._size[self._map(mapType)]
+
+    def setEstimationSize(self, mapType: str, size: int) -> None:
+        self._size[self._map(mapType)] = int(size)

@@ -108,6 +108,49 @@ class RenderScene:
         lib().oracle_render(self.h, C.addressof(desc), film.ctypes.data, int(b), int(e), int(threads))
         return film
 
+    def render_pm(self, desc, maps, recovery_table, film=None, pixels=None, threads=0):
+        """The PhotonMapper restatement with the given maps: ``maps`` is a list of two dicts (global,
+        caustic) with position, omega_in, power (n x 3 float32), blend_idx (n x 3 int32), blend_w
+        (n x 3 float32), radius and k; ``recovery_table`` is liar_b200.recovery.device_table()."""
+        if film is None:
+            film = np.zeros((desc.height, desc.width, 8), dtype=np.float32)
+        keep = []
+
+        def arr(a, dt):
+            a = np.ascontiguousarray(a, dtype=dt)
+            keep.append(a)
+            return a.ctypes.data
+
+        pm = _PmIn()
+        for m in range(2):
+            d = maps[m]
+            pm.position[m] = arr(d["position"], np.float32)
+            pm.omega_in[m] = arr(d["omega_in"], np.float32)
+            pm.power[m] = arr(d["power"], np.float32)
+            pm.blend_idx[m] = arr(d["blend_idx"], np.int32)
+            pm.blend_w[m] = arr(d["blend_w"], np.float32)
+            pm.n[m] = int(np.asarray(d["position"]).reshape(-1, 3).shape[0])
+            pm.radius[m] = float(d["radius"])
+            pm.k[m] = int(d["k"])
+        pm.visualize = int(bool(desc.photon_mapper.visualize))
+        pm.ray_direct = 0 if desc.photon_mapper.ray_trace_direct < 0 else 1
+        t = recovery_table
+        pm.rec_wavelengths = arr(t["wavelengths"], np.float32)
+        pm.rec_spectra = arr(t["spectra"], np.float32)
+        pm.rec_points = arr(t["points"], np.float32)
+        pm.rec_tris = arr(t["triangles"], np.int32)
+        pm.rec_nw = int(np.asarray(t["wavelengths"]).size)
+        pm.rec_ns = int(np.asarray(t["spectra"]).shape[0])
+        pm.rec_nt = int(np.asarray(t["triangles"]).shape[0])
+        L = lib()
+        L.oracle_render_pm.restype = C.c_int
+        L.oracle_render_pm.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_int]
+        b, e = pixels if pixels is not None else (0, desc.width * desc.height)
+        rc = L.oracle_render_pm(self.h, C.addressof(desc), C.byref(pm), film.ctypes.data, int(b), int(e), int(threads))
+        if rc:
+            raise RuntimeError(f"oracle_render_pm failed ({rc})")
+        return film
+
     def __del__(self):
         try:
             if self.h:
@@ -115,6 +158,14 @@ class RenderScene:
                 self.h = None
         except Exception:
             pass
+
+
+class _PmIn(C.Structure):
+    _fields_ = [("position", C.c_void_p * 2), ("omega_in", C.c_void_p * 2), ("power", C.c_void_p * 2),
+                ("blend_idx", C.c_void_p * 2), ("blend_w", C.c_void_p * 2), ("n", C.c_uint64 * 2),
+                ("radius", C.c_float * 2), ("k", C.c_int32 * 2), ("visualize", C.c_int32), ("ray_direct", C.c_int32),
+                ("rec_wavelengths", C.c_void_p), ("rec_spectra", C.c_void_p), ("rec_points", C.c_void_p),
+                ("rec_tris", C.c_void_p), ("rec_nw", C.c_int32), ("rec_ns", C.c_int32), ("rec_nt", C.c_int32)]
 
 
 class Tree:

@@ -94,6 +94,30 @@ struct RenderIn {
     int32_t secondary_light_samples, trace_glossy;
     int32_t filter;
     float filter_param, max_sample_luminance;
+    // PhotonMapper settings (liar_photon_mapper_desc); the oracle takes its maps as PmIn instead
+    uint64_t pm_max_photons, pm_global_map_size;
+    float pm_radius[2], pm_tolerance[2];
+    int32_t pm_size[2], pm_ray_trace_direct, pm_visualize;
+};
+
+// The photon maps of a PhotonMapper render (photon_mapper.cpp:798-835) as the oracle gets them:
+// photons in buffer order, powers XYZ already scaled, each power's recovery blend (three sample
+// indices, -1 = none, and weights); the standard recovery table for colours located here.
+struct PmIn {
+    const float* position[2];
+    const float* omega_in[2];
+    const float* power[2];
+    const int32_t* blend_idx[2];
+    const float* blend_w[2];
+    uint64_t n[2];
+    float radius[2];
+    int32_t k[2];
+    int32_t visualize, ray_direct;
+    const float* rec_wavelengths;
+    const float* rec_spectra;
+    const float* rec_points;   // (n_samples + 4) x 2
+    const int32_t* rec_tris;
+    int32_t rec_nw, rec_ns, rec_nt;
 };
 
 enum { SP_CONST = 0, SP_SAMPLED = 1, SP_BB = 2, SP_CAUCHY = 3 };
@@ -697,13 +721,17 @@ float shade_surface(Path& P, V o, V d, float tmin, float tmax, const Hit& h, int
     const int light = c.light, mi = c.mi;
     const V target = c.target, ng = c.ng, N = c.N, u = c.u, v = c.v;
     if (gen > 0 && light >= 0) result += spectrum(S, S.in.lights[light].spectrum, P.lam, false);
-    if (mi < 0 || S.in.materials[mi].type == M_NONE) {
-        if (mi >= 0 && light < 0 && S.in.materials[mi].emission >= 0)
-            result += spectrum(S, S.in.materials[mi].emission, P.lam, false);
-        return result + trace_photon(P, o, d, h.t + TOL, tmax, gen + 1);
+    // the shader's emission counts unless the object is a light hit past the camera vertex
+    // (shadeSurface asks for the object's light only at generations > 0)
+    const bool shader_emits = gen == 0 || light < 0;
+    if (mi < 0) return result + trace_photon(P, o, d, h.t + TOL, tmax, gen + 1);  // no shader: continue through
+    if (S.in.materials[mi].type == M_NONE) {
+        // a shader without a BSDF: its emission, nothing scatters
+        if (shader_emits && S.in.materials[mi].emission >= 0) result += spectrum(S, S.in.materials[mi].emission, P.lam, false);
+        return result;
     }
     const Material& M = S.in.materials[mi];
-    if (light < 0 && M.emission >= 0) result += spectrum(S, M.emission, P.lam, false);
+    if (shader_emits && M.emission >= 0) result += spectrum(S, M.emission, P.lam, false);
     const Bsdf B = make_bsdf(S, M, c, P.lam);
     const V md = -d;
     V wi{dot(md, u), dot(md, v), dot(md, N)};
@@ -869,7 +897,81 @@ struct DLPath {
     Sampler smp;
     float lam;
     float alpha = 0;
+    const PmIn* pm = nullptr;  // PhotonMapper maps, nullptr for DirectLighting
 };
+
+// ---- PhotonMapper estimates (photon_mapper.cpp:1254-1381)
+
+// RecoveryMengSimon::Impl::recover by a search of every triangle: blend of XYZ, false when none
+bool pm_locate(const PmIn& pm, float X, float Y, float Z, int32_t idx[3], float w[3]) {
+    const float s = X + Y + Z;
+    if (s == 0.0f) return false;
+    const float x = X / s, y = Y / s;
+    if (!(x >= -0.3f && x <= 1.0f && y >= -0.3f && y <= 1.2f)) return false;
+    int best = -1;
+    float bw[3] = {0, 0, 0}, best_min = -INFINITY;
+    for (int t = 0; t < pm.rec_nt; ++t) {
+        const int i0 = pm.rec_tris[3 * t], i1 = pm.rec_tris[3 * t + 1], i2 = pm.rec_tris[3 * t + 2];
+        const float ax = pm.rec_points[2 * i0], ay = pm.rec_points[2 * i0 + 1];
+        const float bx = pm.rec_points[2 * i1], by = pm.rec_points[2 * i1 + 1];
+        const float qx = pm.rec_points[2 * i2], qy = pm.rec_points[2 * i2 + 1];
+        const float det = (bx - ax) * (qy - ay) - (qx - ax) * (by - ay);
+        if (det == 0.0f) continue;
+        const float w1 = ((x - ax) * (qy - ay) - (qx - ax) * (y - ay)) / det;
+        const float w2 = ((bx - ax) * (y - ay) - (x - ax) * (by - ay)) / det;
+        const float w0 = 1.0f - w1 - w2;
+        const float mn = std::min(w0, std::min(w1, w2));
+        if (mn > best_min) {
+            best_min = mn;
+            best = t;
+            bw[0] = w0;
+            bw[1] = w1;
+            bw[2] = w2;
+        }
+    }
+    if (best < 0) return false;
+    float wtot = 0;
+    for (int j = 0; j < 3; ++j) {
+        const int i = pm.rec_tris[3 * best + j];
+        idx[j] = i < pm.rec_ns ? i : -1;
+        if (idx[j] < 0) bw[j] = 0;
+        wtot += bw[j];
+    }
+    if (wtot == 0) return false;
+    for (int j = 0; j < 3; ++j) w[j] = bw[j] * (s / wtot);
+    return true;
+}
+
+// RecoveryMengSimon::doRecover at lam, as an illuminant
+float pm_recover(const PmIn& pm, const int32_t idx[3], const float w[3], float lam) {
+    const float* ws = pm.rec_wavelengths;
+    const int k = (int)(std::upper_bound(ws, ws + pm.rec_nw, lam) - ws);
+    if (k == 0 || k == pm.rec_nw) return 0.0f;
+    const float t = (lam - ws[k - 1]) / (ws[k] - ws[k - 1]);
+    float v0 = 0, v1 = 0;
+    for (int j = 0; j < 3; ++j) {
+        if (idx[j] < 0) continue;
+        const float* sp = pm.rec_spectra + (size_t)idx[j] * pm.rec_nw;
+        v0 += w[j] * sp[k - 1];
+        v1 += w[j] * sp[k];
+    }
+    return v0 + t * (v1 - v0);
+}
+
+// KdTree::rangeSearch(point, rMax, kMax): the k nearest photons with d^2 < rMax^2, by brute force
+// (ascending d^2, ties by photon index)
+void pm_nearest(const PmIn& pm, int m, V x, std::vector<std::pair<float, int64_t>>& out) {
+    out.clear();
+    const float r2max = pm.radius[m] * pm.radius[m];
+    const float* P = pm.position[m];
+    for (uint64_t i = 0; i < pm.n[m]; ++i) {
+        const float dx = P[3 * i] - x.x, dy = P[3 * i + 1] - x.y, dz = P[3 * i + 2] - x.z;
+        const float d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 < r2max) out.push_back({d2, (int64_t)i});
+    }
+    std::sort(out.begin(), out.end());
+    if ((int64_t)out.size() > pm.k[m]) out.resize((size_t)pm.k[m]);
+}
 
 bool occluded(const Scene& S, V o, V d, float tmax) {
     return oracle_internal::tree_any(S.tree, Ray{o.x, o.y, o.z, TOL, d.x, d.y, d.z, tmax});
@@ -910,6 +1012,61 @@ float estimate_light(const Scene& S, const Bsdf& B, const Ctx& c, V wi, V start,
     return result;
 }
 
+// estimateRadiance (m = 0, global map, f without specular and glossy parts) and estimateCaustics
+// (m = 1, caustic map, Gaussian filter, f's diffuse part): at least two photons, over pi r^2 with
+// r^2 the farthest photon's squared distance
+float pm_estimate(const DLPath& P, int m, const Ctx& c, const Bsdf& B, V wi) {
+    const PmIn& pm = *P.pm;
+    if (pm.n[m] == 0 || pm.k[m] < 1) return 0;
+    thread_local std::vector<std::pair<float, int64_t>> nb;
+    pm_nearest(pm, m, c.target, nb);
+    if (nb.size() < 2) return 0;
+    const float r2 = nb.back().first;
+    if (!(r2 > 0)) return 0;
+    const uint32_t caps = m == 0 ? (uint32_t)(C_ALL & ~C_SPEC & ~C_GLOSSY) : (uint32_t)(C_REFL | C_TRANS | C_DIFF);
+    const float alpha = 0.918f, beta = 1.953f;
+    const float b1 = -beta / (2.0f * r2), b2 = 1.0f / (1.0f - std::exp(-beta));
+    float result = 0;
+    for (const auto& e : nb) {
+        const int64_t i = e.second;
+        const float* om = pm.omega_in[m] + 3 * i;
+        const V wo{om[0] * c.u.x + om[1] * c.u.y + om[2] * c.u.z, om[0] * c.v.x + om[1] * c.v.y + om[2] * c.v.z,
+                   om[0] * c.N.x + om[1] * c.N.y + om[2] * c.N.z};
+        const Out be = evaluate(B, wi, wo, caps);
+        if (!(be.pdf > 0) || be.value == 0) continue;
+        float v = be.value * pm_recover(pm, pm.blend_idx[m] + 3 * i, pm.blend_w[m] + 3 * i, P.lam);
+        if (m == 1) v *= alpha * (1.0f - b2 * (1.0f - std::exp(b1 * e.first)));
+        result += v;
+    }
+    return result / (3.14159265358979323846f * r2);
+}
+
+// isVisualizingPhotonMap: the global map's irradiance at the hit from the normal's side
+// (estimateIrradianceImpl, photon_mapper.cpp:1254-1279) as a spectrum at lam
+float pm_irradiance(const DLPath& P, const Ctx& c) {
+    const PmIn& pm = *P.pm;
+    if (pm.n[0] == 0 || pm.k[0] < 1) return 0;
+    thread_local std::vector<std::pair<float, int64_t>> nb;
+    pm_nearest(pm, 0, c.target, nb);
+    if (nb.empty()) return 0;
+    const float r2 = nb.back().first;
+    if (!(r2 > 0)) return 0;
+    float X = 0, Y = 0, Z = 0;
+    for (const auto& e : nb) {
+        const float* om = pm.omega_in[0] + 3 * e.second;
+        if (om[0] * c.N.x + om[1] * c.N.y + om[2] * c.N.z > 0) {
+            X += pm.power[0][3 * e.second];
+            Y += pm.power[0][3 * e.second + 1];
+            Z += pm.power[0][3 * e.second + 2];
+        }
+    }
+    const float inv = 1.0f / (3.14159265358979323846f * r2);
+    int32_t idx[3];
+    float w[3];
+    if (!pm_locate(pm, X * inv, Y * inv, Z * inv, idx, w)) return 0;
+    return pm_recover(pm, idx, w, P.lam);
+}
+
 float dl_cast(DLPath& P, V o, V d, float tmin, float tmax, int gen, bool hq, uint32_t key) {
     const Scene& S = *P.S;
     const RenderIn& R = *P.R;
@@ -923,6 +1080,7 @@ float dl_cast(DLPath& P, V o, V d, float tmin, float tmax, int gen, bool hq, uin
     const Ctx c = hit_ctx(S, o, d, h);
     if (c.mi < 0) return dl_cast(P, o, d, h.t + TOL, tmax, gen + 1, hq, dl_child_key(key, 0));
     const Material& M = S.in.materials[c.mi];
+    if (P.pm && P.pm->visualize) return pm_irradiance(P, c);
     float result = 0;
     if ((gen == 0 || c.light < 0) && M.emission >= 0) result += spectrum(S, M.emission, P.lam, false);
     if (M.type == M_NONE) return result;
@@ -932,7 +1090,10 @@ float dl_cast(DLPath& P, V o, V d, float tmin, float tmax, int gen, bool hq, uin
     wi.z = std::max(wi.z, 1.19209290e-07f);
     const V start = c.target + (10.0f * TOL) * c.N;
     const int nlights = (int)S.in.n_lights;
-    if (hq) {
+    if (P.pm && has(B.caps, C_DIFF)) result += pm_estimate(P, 1, c, B, wi) + pm_estimate(P, 0, c, B, wi);
+    if (P.pm && !P.pm->ray_direct) {
+        // no traced direct light: the global map holds it
+    } else if (hq) {
         for (int l = 0; l < nlights; ++l) {
             const Light& L = S.in.lights[l];
             const int nl = L.emission_samples > 0 ? L.emission_samples : 1;
@@ -1111,10 +1272,11 @@ static void trace_photon_rec(const Scene& S, const PhotonIn& D, const Sampler& s
     const uint32_t prim = (uint32_t)h.prim;
     const int obj = S.in.triangle_object[prim];
     const int mi = S.in.object_material[obj];
-    if (mi < 0 || S.in.materials[mi].type == M_NONE) {
+    if (mi < 0) {  // no shader: entering or leaving something
         if (gen >= D.max_ray_generation) return;
         return trace_photon_rec(S, D, smp, path, lam, lam_pdf, power, o, d, h.t + TOL, tmax, gen + 1, caustic, out);
     }
+    if (S.in.materials[mi].type == M_NONE) return;  // a shader without a BSDF absorbs the photon
     const Material& M = S.in.materials[mi];
     if (M.type == M_LAMBERT) {
         const bool to_caustic = caustic;
@@ -1394,8 +1556,23 @@ static void film_splat(const RenderIn& R, float* film, int px, int py, float jx,
     }
 }
 
+int render_body(void* s, const RenderIn* R, const PmIn* pm, float* film, int64_t pixel_begin, int64_t pixel_end,
+                int threads);
+
 // renders pixels [pixel_begin, pixel_end) of the image into film (8 floats per pixel, summed)
 int oracle_render(void* s, const RenderIn* R, float* film, int64_t pixel_begin, int64_t pixel_end, int threads) {
+    return render_body(s, R, nullptr, film, pixel_begin, pixel_end, threads);
+}
+
+// the PhotonMapper (tracer 2) with the given maps
+int oracle_render_pm(void* s, const RenderIn* R, const PmIn* pm, float* film, int64_t pixel_begin, int64_t pixel_end,
+                     int threads) {
+    if (!pm) return -1;
+    return render_body(s, R, pm, film, pixel_begin, pixel_end, threads);
+}
+
+int render_body(void* s, const RenderIn* R, const PmIn* pm, float* film, int64_t pixel_begin, int64_t pixel_end,
+                int threads) {
     const Scene& S = *static_cast<Scene*>(s);
     const int64_t npix = (int64_t)R->width * R->height;
     if (pixel_end < 0 || pixel_end > npix) pixel_end = npix;
@@ -1444,8 +1621,9 @@ int oracle_render(void* s, const RenderIn* R, float* film, int64_t pixel_begin, 
                     factor = 1 / dot(dir, dn);
                 }
                 float L;
-                if (R->tracer == 1) {
+                if (R->tracer == 1 || R->tracer == 2) {
                     DLPath D{&S, R, P.smp, P.lam};
+                    D.pm = R->tracer == 2 ? pm : nullptr;
                     L = dl_cast(D, pos, dir, std::max(TOL, factor * C.near_limit), factor * C.far_limit, 0, true, 1u);
                     P.alpha = D.alpha;
                 } else {

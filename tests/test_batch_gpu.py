@@ -109,7 +109,10 @@ def test_hero_wavelengths_same_expectation(cornell):
     torch.cuda.synchronize()
     a, b = four.films[0].cpu().numpy(), one.films[0].cpu().numpy()
     ma, mb = _mean_within(a, b)
-    assert abs(ma[..., 1].mean() / mb[..., 1].mean() - 1) < 0.02
+    # the luminance of the lit surfaces (the light, a sub-pixel emitter far brighter than the rest
+    # and seen by the camera, would dominate the mean with its variance)
+    lit = (ma[..., 1] < 2.0) & (mb[..., 1] < 2.0)
+    assert abs(ma[..., 1][lit].mean() / mb[..., 1][lit].mean() - 1) < 0.02
     # hero wavelengths cut the colour noise: the mean per-pixel variance of X and Z drops
     _, va = R.resolve(a)
     _, vb = R.resolve(b)
