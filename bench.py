@@ -539,6 +539,36 @@ def photon_bench(ctx, stream, args, world, dist, local, cpu: bool, n_photons: in
         out["parity_sample"] = {"queries": ns, "identical_neighbour_sets":
                                 bool((didx.cpu().numpy()[sel] == ci).all() and (dcnt.cpu().numpy()[sel] == cc).all())}
     pmap.close()
+    # the PhotonMapper tracer end to end on the same scene: a global map of n_photons photons
+    # (direct light from the map, as the gather workload above; k = 64 for both maps), then
+    # 1920 x 1080 at 1 sample per pixel; the maps are built by the first render and kept
+    from liar_b200 import tracers
+    pm = tracers.PhotonMapper()
+    pm.maxRayGeneration = 8
+    pm.globalMapSize = n_photons
+    pm.isRayTracingDirect = False
+    pm.setEstimationSize("global", K)
+    pm.setEstimationSize("caustic", K)
+    film = torch.zeros((1080, 1920, 8), dtype=torch.float32, device=f"cuda:{local}")
+    t0 = time.perf_counter()
+    gs.render_device(R.render_desc(cam, 1920, 1080, 1, pm, seed=0), film.data_ptr(), stream.cuda_stream)
+    stream.synchronize()
+    first_s = time.perf_counter() - t0
+    st = R.photon_mapper_stats(ctx)
+    gs.render_device(R.render_desc(cam, 1920, 1080, 1, pm, seed=0, first_sample=1), film.data_ptr(), stream.cuda_stream)
+    e0.record(stream)
+    for k in range(2):
+        gs.render_device(R.render_desc(cam, 1920, 1080, 1, pm, seed=0, first_sample=2 + k), film.data_ptr(),
+                         stream.cuda_stream)
+    e1.record(stream)
+    stream.synchronize()
+    frame_ms = e0.elapsed_time(e1) / 2
+    out["photon_mapper_render"] = {
+        "workload": f"PhotonMapper 1920x1080, 1 spp, global map {st['global']} photons, caustic map "
+                    f"{st['caustic']}, k = {K}, direct light from the global map, max generation 8",
+        "photons_shot": st["emitted"], "radii": st["radius"], "first_render_with_map_build_s": first_s,
+        "frame_ms": frame_ms, "samples_per_s": 1920 * 1080 / (frame_ms * 1e-3)}
+    del film
     gs.close()
     return out
 
@@ -581,7 +611,8 @@ def run_case(name: str) -> None:
     guide-eval (the guide network over 1M random vertices, 3 launches), direct (DirectLighting on
     the Cornell frame, 256^2 x 4 spp, twice), shade (the Cornell path-tracing frame, twice),
     gather (k = 64 over 4M uniform photons for 256k uniform queries, twice), guided (the slit
-    room at 256^2: 4 training passes, then 16 guided samples per pixel)."""
+    room at 256^2: 4 training passes, then 16 guided samples per pixel), pm (the PhotonMapper on
+    the photon scene, 1M global photons, 480 x 270, two frames)."""
     import torch
     from liar_b200.kernel import default_context
     ctx = default_context()
@@ -612,6 +643,18 @@ def run_case(name: str) -> None:
         d.wave_paths = 256 * 256
         g.render(gs, d, film.data_ptr(), train=True)
         g.render(gs, R.render_desc(cam, 256, 256, 16, SG.guiding_tracer(), seed=2), film.data_ptr(), train=False)
+    elif name == "pm":
+        from liar_b200 import render as R, scenes_render, tracers
+        scene, cam = scenes_render.photon_scene()
+        gs = R.GpuScene(ctx, R.flatten(scene))
+        t = tracers.PhotonMapper()
+        t.globalMapSize = 1_000_000
+        t.isRayTracingDirect = False
+        t.setEstimationSize("global", 64)
+        t.setEstimationSize("caustic", 64)
+        film = torch.zeros((270, 480, 8), device="cuda")
+        for k in range(2):
+            gs.render_device(R.render_desc(cam, 480, 270, 1, t, seed=0, first_sample=k), film.data_ptr())
     elif name == "gather":
         from liar_b200 import photons as PH
         rng = np.random.default_rng(0)
