@@ -463,7 +463,7 @@ def photon_bench(ctx, stream, args, world, dist, local, cpu: bool, n_photons: in
     ph, counts = photons.trace_photons(gs, desc, capacity=n_photons + (3 << 22), stream=stream.cuda_stream)
     torch.cuda.synchronize()
     trace_s = time.perf_counter() - t0
-    glob = (ph["tag"] & 3) == photons.GLOBAL
+    glob = (ph["tag"] & photons.GLOBAL) != 0
     pos = ph["position"][glob][:n_photons].contiguous()
     power = ph["power"][glob][:n_photons].contiguous()
     omega = ph["omega_in"][glob][:n_photons].contiguous()
@@ -568,6 +568,35 @@ def photon_bench(ctx, stream, args, world, dist, local, cpu: bool, n_photons: in
                     f"{st['caustic']}, k = {K}, direct light from the global map, max generation 8",
         "photons_shot": st["emitted"], "radii": st["radius"], "first_render_with_map_build_s": first_s,
         "frame_ms": frame_ms, "samples_per_s": 1920 * 1080 / (frame_ms * 1e-3)}
+    del film
+    gs.close()
+    # the reference's classic photon-mapping example (examples/cornell_box/photon_mapper_classic.py):
+    # the Cornell box, 200,000 global photons, 36 final gather rays over the precomputed irradiance
+    # map (ratio 0.25), traced direct light, 800 x 800 x 4 spp
+    scene, cam = scenes_render.cornell_box()
+    gs = R.GpuScene(ctx, R.flatten(scene))
+    pm = tracers.PhotonMapper()
+    pm.maxNumberOfPhotons = 10_000_000
+    pm.globalMapSize = 200_000
+    pm.numFinalGatherRays = 36
+    pm.ratioPrecomputedIrradiance = 0.25
+    film = torch.zeros((800, 800, 8), dtype=torch.float32, device=f"cuda:{local}")
+    t0 = time.perf_counter()
+    gs.render_device(R.render_desc(cam, 800, 800, 1, pm, seed=0), film.data_ptr(), stream.cuda_stream)
+    stream.synchronize()
+    first_s = time.perf_counter() - t0
+    st = R.photon_mapper_stats(ctx)
+    e0.record(stream)
+    gs.render_device(R.render_desc(cam, 800, 800, 4, pm, seed=0, first_sample=1), film.data_ptr(), stream.cuda_stream)
+    e1.record(stream)
+    stream.synchronize()
+    frame_ms = e0.elapsed_time(e1)
+    out["photon_mapper_classic"] = {
+        "workload": f"Cornell box, PhotonMapper with 36 final gather rays, global map {st['global']} photons, "
+                    f"caustic map {st['caustic']}, irradiance ratio 0.25, 800x800 x 4 spp",
+        "photons_shot": st["emitted"], "first_render_with_maps_s": first_s, "frame_ms": frame_ms,
+        "samples_per_s": 800 * 800 * 4 / (frame_ms * 1e-3),
+        "gather_rays_per_s": 800 * 800 * 4 * 36 / (frame_ms * 1e-3)}
     del film
     gs.close()
     return out

@@ -217,7 +217,9 @@ typedef struct liar_camera {
  * PHOTON_MAPPER: src/liar/tracers/photon_mapper.cpp (DirectLighting plus, at every vertex with a
  * diffuse part, the caustic map's Gaussian-filtered estimate and the global map's radiance
  * estimate, photon_mapper.cpp:466-518, 1282-1381; photon maps filled per render as
- * fillPhotonMaps / buildPhotonMap, :573-835; no final gather, the reference's default) */
+ * fillPhotonMaps / buildPhotonMap, :573-835; with final gathering at high-quality diffuse vertices,
+ * gatherIndirect / traceGatherRay / gatherSecondary, :1060-1251, over the precomputed irradiance
+ * map, :943-995) */
 enum liar_tracer_type { LIAR_TRACER_ADJOINT_PHOTON = 0, LIAR_TRACER_DIRECT_LIGHTING = 1, LIAR_TRACER_PHOTON_MAPPER = 2 };
 
 /* PhotonMapper settings (photon_mapper.cpp:108-142 defaults). Map 0 is the global map, map 1 the
@@ -230,6 +232,10 @@ typedef struct liar_photon_mapper_desc {
     int32_t estimation_size[2];     /* photons per estimate, at most 64 (0 = 50) */
     int32_t ray_trace_direct;       /* isRayTracingDirect: -1 = false (direct light from the global map), else true */
     int32_t visualize;              /* isVisualizingPhotonMap: nonzero renders the global map's irradiance */
+    int32_t final_gather_rays;      /* numFinalGatherRays, used with traced direct light (0 = no final gather) */
+    int32_t secondary_gather_rays;  /* numSecondaryGatherRays: 0 = the reference's 1, -1 = none */
+    float ratio_precomputed_irradiance; /* ratioPrecomputedIrradiance: 0 = the reference's 0.25, < 0 = none */
+    int32_t reserved;
 } liar_photon_mapper_desc;
 
 typedef struct liar_render_desc {
@@ -401,7 +407,9 @@ int liar_gpu_photon_estimate_device(liar_gpu_ctx* ctx, const float* d_power, con
  * photons leave the scene's lights (chosen by power), carry power at one wavelength, scatter by
  * BSDF sampling with power-preserving Russian roulette (kernel/kernel_common.h:160) and are stored at
  * hits on surfaces with a diffuse BSDF: into the caustic map when every bounce so far was specular
- * or glossy, into the global map when not caustic and not a direct hit (isRayTracingDirect).
+ * or glossy, into the global map when not caustic and not a direct hit (isRayTracingDirect), or
+ * always with final gathering (photon_mapper.cpp:742); one record per stored hit, tagged with
+ * every map it belongs to.
  * Photons are emitted in waves of `wave` until the global map holds `global_target` photons or
  * `max_emitted` photons have left the lights. Stored power is XYZ (the reference's Photon record),
  * not yet divided by the number emitted. */
@@ -413,14 +421,17 @@ typedef struct liar_photon_desc {
     uint64_t global_target;      /* globalMapSize */
     uint64_t max_emitted;        /* maxNumberOfPhotons */
     uint64_t wave;               /* photons emitted per wave, 0 = automatic */
+    int32_t final_gather;        /* 1: every diffuse hit goes to the global map (hasFinalGather) */
+    int32_t reserved;
 } liar_photon_desc;
 typedef struct liar_photon_buffers {  /* device arrays of `capacity` photons */
     float* position;   /* x 3 */
     float* omega_in;   /* x 3: direction toward where the photon came from */
     float* power;      /* x 3: XYZ */
     uint32_t* path;    /* index of the emitted photon */
-    uint32_t* tag;     /* map kind (bits 0-1) | bounce << 8 */
+    uint32_t* tag;     /* map kinds (bits 0-1: LIAR_PHOTON_GLOBAL | LIAR_PHOTON_CAUSTIC) | bounce << 8 */
     uint64_t capacity;
+    float* normal;     /* x 3, may be NULL: the shading normal on the side the photon came from */
 } liar_photon_buffers;
 typedef struct liar_photon_counts {
     uint64_t stored, global, caustic, emitted;
@@ -437,6 +448,12 @@ int liar_gpu_photon_mapper_stats(const liar_gpu_ctx* ctx, unsigned long long* ou
  * floats each), and the powers' recovery blends (n x 3 indices, n x 3 weights); *n_out = photons. */
 int liar_gpu_photon_mapper_get_map(liar_gpu_ctx* ctx, int map, float* position, float* omega_in, float* power,
                                    int32_t* blend_idx, float* blend_w, size_t capacity, size_t* n_out);
+/* Copies the irradiance map of those maps (final gathering, buildIrradianceMap,
+ * src/liar/tracers/photon_mapper.cpp:970-995): positions, normals, irradiances (XYZ), their recovery
+ * blends (n x 3 each) and squared estimation radii (n); any may be NULL; *n_out = points. */
+int liar_gpu_photon_mapper_get_irradiance(liar_gpu_ctx* ctx, float* position, float* normal, float* xyz,
+                                          int32_t* blend_idx, float* blend_w, float* r2, size_t capacity,
+                                          size_t* n_out);
 
 /* Allocation-free closest hit / any hit. It has no counterpart in the reference; it exists for
  * callers that must not call cudaMalloc while they trace: an application whose own pool

@@ -95,6 +95,7 @@ SIGNATURES: dict[str, tuple] = {
     "liar_gpu_photon_trace": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "liar_gpu_photon_mapper_stats": (C.c_int, [_vp, _vp, _vp]),
     "liar_gpu_photon_mapper_get_map": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_size_t, _vp]),
+    "liar_gpu_photon_mapper_get_irradiance": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_size_t, _vp]),
     "liar_gpu_set_recovery": (C.c_int, [_vp, _vp, C.c_int, _vp, _vp, C.c_int, _vp, C.c_int]),
     "liar_gpu_recovery_locate_device": (C.c_int, [_vp, _vp, C.c_size_t, _vp, _vp, _vp]),
     "liar_gpu_photon_estimate_device": (C.c_int, [_vp, _vp, _vp, _sz, _vp, _sz, C.c_int, _vp, _vp, _vp, C.c_float,

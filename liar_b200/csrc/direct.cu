@@ -82,9 +82,15 @@ struct DParams {
     int pm;
     int pm_direct;       // isRayTracingDirect
     float* q_pos;
-    uint32_t* q_task;
+    uint32_t* q_task;    // bit 31: the vertex gathers its indirect light (no radiance estimate)
     uint32_t* q_count;
+    int fg_rays;         // final gathering: rays per high-quality diffuse vertex (0: none)
+    int fg_secondary;    // numSecondaryGatherRays
+    DTasks fg;           // the gather rays of this generation (meta: stage in bit 9)
 };
+
+constexpr uint32_t kNoRadiance = 0x80000000u;
+constexpr uint32_t kStage1 = 1u << 9;
 
 // sampler dimensions (disjoint from the path tracer's and from each other)
 __host__ __device__ __forceinline__ uint32_t dim_light(int l, int k, int axis) {  // axis 0,1 light 2D; 2,3 BSDF 2D; 4 component
@@ -92,6 +98,9 @@ __host__ __device__ __forceinline__ uint32_t dim_light(int l, int k, int axis) {
 }
 __host__ __device__ __forceinline__ uint32_t dim_scatter(int i, int axis) {  // 0,1,2 reflection; 3,4,5 transmission
     return 0x400000u + (uint32_t)i * 8u + (uint32_t)axis;
+}
+__host__ __device__ __forceinline__ uint32_t dim_final_gather(int i, int axis) {  // 0,1 BSDF 2D; 2 component
+    return 0x600000u + (uint32_t)i * 4u + (uint32_t)axis;
 }
 __host__ __device__ __forceinline__ uint32_t dim_branch(uint32_t key, uint32_t j) {
     return 0x80000000u | (uint32_t)(mix64(((uint64_t)key << 20) ^ j) & 0x7fffffffu);
@@ -217,6 +226,27 @@ __device__ void estimate_light(const DScene& S, const Bsdf& B, const HitContext&
     }
 }
 
+// traceDirect with highQuality false (direct_lighting.cpp:236-262): n lights chosen by power, one
+// light and one BSDF sample each, from the branch key's streams
+__device__ void direct_low_quality(const DScene& S, int n, const Bsdf& B, const HitContext& HC, float3 wi, float3 start,
+                                   float lam, float T, uint32_t slot, uint32_t key, const SampleKey& skey,
+                                   ShadowWriter& sw) {
+    if (S.n_lights <= 0) return;
+    for (int k = 0; k < n; ++k) {
+        const uint32_t j0 = 16u * (uint32_t)k;
+        const float uc = sample_dim(skey, dim_branch(key, j0), false);
+        int l = lower_bound_f(S.light_cdf, S.n_lights, uc);
+        if (l > S.n_lights - 1) l = S.n_lights - 1;
+        const float pc = light_choice_pdf(S, l);
+        if (!(pc > 0.0f)) continue;
+        const int nb = S.lights[l].type == LIAR_LIGHT_POINT ? 0 : 1;
+        auto u = [&](int kind, int, int axis) {
+            return sample_dim(skey, dim_branch(key, j0 + 1u + 2u * (uint32_t)kind + (uint32_t)axis), false);
+        };
+        estimate_light(S, B, HC, wi, start, l, 1, nb, lam, T / ((float)n * pc), slot, sw, u);
+    }
+}
+
 __global__ void __launch_bounds__(128) k_dl_shade(DScene S, DParams W, DSamples P, DTasks in,
                                                   const liar_hit* __restrict__ hits, uint32_t n_in, DTasks out,
                                                   DShadows sh, uint32_t shadow_hq) {
@@ -270,16 +300,46 @@ __global__ void __launch_bounds__(128) k_dl_shade(DScene S, DParams W, DSamples 
         }
     }
     // PhotonMapper: vertices with a shader query the photon maps (the visualisation), or those with
-    // a diffuse component do (estimateCaustics, estimateRadiance)
+    // a diffuse component do (estimateCaustics, estimateRadiance); high-quality ones gather their
+    // indirect light with final gather rays instead of the radiance estimate (photon_mapper.cpp:490-507)
     const bool query = W.pm != 0 && shading && HC.mat >= 0 &&
                        (W.pm == 2 || (has_bsdf && has_caps(B.caps, CAP_DIFF)));
+    const uint32_t n_fg = (query && W.pm == 1 && hq && W.fg_rays > 0) ? (uint32_t)W.fg_rays : 0u;
     if (W.pm != 0) {  // uniform over the launch: every lane of the warp takes the reservation
         const uint32_t qi = warp_reserve(W.q_count, query ? 1u : 0u);
         if (query) {
             W.q_pos[3 * (size_t)qi] = HC.target.x;
             W.q_pos[3 * (size_t)qi + 1] = HC.target.y;
             W.q_pos[3 * (size_t)qi + 2] = HC.target.z;
-            W.q_task[qi] = q;
+            W.q_task[qi] = q | (n_fg > 0 ? kNoRadiance : 0u);
+        }
+    }
+    if (W.fg_rays > 0) {  // uniform as well
+        const uint32_t gbase = warp_reserve(W.fg.count, n_fg);
+        if (n_fg > 0) {
+            // gatherIndirect (photon_mapper.cpp:1060-1146): BSDF samples of the reflective diffuse part
+            const SampleKey skey = dkey(W, W.first_path + p);
+            const float3 md = -d;
+            float3 wi = mk(dot(md, HC.u), dot(md, HC.v), dot(md, HC.N));
+            wi.z = fmaxf(wi.z, kEps);
+            const float3 start = HC.target + (10.0f * kTol) * HC.N;
+            for (uint32_t i = 0; i < n_fg; ++i) {
+                const uint32_t gi = gbase + i;
+                const BsdfSample bs = bsdf_sample(B, wi, sample_dim(skey, dim_final_gather((int)i, 0), true),
+                                                  sample_dim(skey, dim_final_gather((int)i, 1), true),
+                                                  sample_dim(skey, dim_final_gather((int)i, 2), true), CAP_REFL | CAP_DIFF);
+                W.fg.slot[gi] = p;
+                W.fg.meta[gi] = (uint32_t)(gen + 1);
+                W.fg.key[gi] = child_key(key, 0x200u + i);
+                if (bs.ok()) {
+                    const float3 wd = bs.wo.x * HC.u + bs.wo.y * HC.v + bs.wo.z * HC.N;
+                    put_ray(W.fg.rays, gi, start, wd, kTol, INFINITY);
+                    W.fg.T[gi] = T * bs.value * (fabsf(bs.wo.z) / ((float)n_fg * bs.pdf));
+                } else {
+                    put_void_ray(W.fg.rays, gi);
+                    W.fg.T[gi] = 0.0f;
+                }
+            }
         }
     }
     ShadowWriter sw{sh, warp_reserve(sh.count, n_sh), 0u, n_sh};
@@ -327,21 +387,8 @@ __global__ void __launch_bounds__(128) k_dl_shade(DScene S, DParams W, DSamples 
                         };
                         estimate_light(S, B, HC, wi, start, l, nl, nb, lam, T, p, sw, u);
                     }
-                } else if (S.n_lights > 0) {
-                    const int n = W.n_secondary;
-                    for (int k = 0; k < n; ++k) {
-                        const uint32_t j0 = 16u * (uint32_t)k;
-                        const float uc = sample_dim(skey, dim_branch(key, j0), false);
-                        int l = lower_bound_f(S.light_cdf, S.n_lights, uc);
-                        if (l > S.n_lights - 1) l = S.n_lights - 1;
-                        const float pc = light_choice_pdf(S, l);
-                        if (!(pc > 0.0f)) continue;
-                        const int nb = S.lights[l].type == LIAR_LIGHT_POINT ? 0 : 1;
-                        auto u = [&](int kind, int, int axis) {
-                            return sample_dim(skey, dim_branch(key, j0 + 1u + 2u * (uint32_t)kind + (uint32_t)axis), false);
-                        };
-                        estimate_light(S, B, HC, wi, start, l, 1, nb, lam, T / ((float)n * pc), p, sw, u);
-                    }
+                } else {
+                    direct_low_quality(S, W.n_secondary, B, HC, wi, start, lam, T, p, key, skey, sw);
                 }
                 // ---- traced specular and glossy scattering (traceSpecularAndGlossy)
                 if (n_ch > 0) {
@@ -405,7 +452,7 @@ __global__ void k_dl_shadow_add(DShadows sh, uint32_t n, const liar_hit* __restr
 }
 
 // ---- PhotonMapper estimates at the queried vertices (photon_mapper.cpp:1282-1381, 1254-1279)
-enum { kEstRadiance = 0, kEstCaustics = 1, kEstIrradiance = 2 };
+enum { kEstRadiance = 0, kEstCaustics = 1, kEstIrradiance = 2, kEstIrradianceMap = 3 };
 
 // Photon::spectralPower: the XYZ power as a spectrum at the sample's wavelength (Spectral::fromXYZ,
 // an illuminant), through the photon's precomputed blend
@@ -419,6 +466,30 @@ __device__ __forceinline__ float photon_power(const PmMap& M, const DRecovery& R
     return recovery_eval(R, b, lam, false);
 }
 
+// estimateRadiance from the nearest irradiance point j (photon_mapper.cpp:1290-1304): the BSDF
+// from the viewer toward the point's normal times the point's irradiance at lam
+__device__ float irradiance_map_radiance(const DScene& S, const PmIrradiance& I, const DRecovery& R,
+                                         const HitContext& HC, float3 d, float lam, int32_t j) {
+    if (j < 0 || (uint64_t)j >= I.n) return 0.0f;
+    const liar_material Mat = S.mats[HC.mat];
+    if (Mat.type == LIAR_MAT_NONE) return 0.0f;
+    const Bsdf B = make_bsdf(S, Mat, HC, lam);
+    if (!has_caps(B.caps, CAP_DIFF)) return 0.0f;
+    const float3 md = -d;
+    float3 wi = mk(dot(md, HC.u), dot(md, HC.v), dot(md, HC.N));
+    wi.z = fmaxf(wi.z, kEps);
+    const float3 n = mk(I.normal[3 * (size_t)j], I.normal[3 * (size_t)j + 1], I.normal[3 * (size_t)j + 2]);
+    const BsdfOut be = bsdf_evaluate(B, wi, mk(dot(n, HC.u), dot(n, HC.v), dot(n, HC.N)), CAP_ALL);
+    if (!(be.pdf > 0.0f) || be.value == 0.0f) return 0.0f;
+    RecoveryBlend b;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        b.idx[c] = I.blend_idx[3 * (size_t)j + c];
+        b.w[c] = I.blend_w[3 * (size_t)j + c];
+    }
+    return be.value * recovery_eval(R, b, lam, false);
+}
+
 // one thread per queried vertex: the vertex's BSDF against the k nearest photons of one map
 //   kEstRadiance:   sum f(w, w_p) Phi_p(lam) / (pi r^2), f without its specular and glossy parts,
 //                   at least two photons (estimateRadiance without an irradiance map)
@@ -426,19 +497,22 @@ __device__ __forceinline__ float photon_power(const PmMap& M, const DRecovery& R
 //                   (1 - e^-beta)), alpha 0.918, beta 1.953, f's diffuse part (estimateCaustics)
 //   kEstIrradiance: the XYZ of the photons arriving from the normal's side over pi r^2, as a
 //                   spectrum at lam (isVisualizingPhotonMap: estimateIrradianceImpl)
+//   kEstIrradianceMap: f(w, n_i) E_i(lam) of the nearest irradiance point i within the radius
+//                   (estimateRadiance with the precomputed irradiance map, :1290-1304)
 // r^2 is the squared distance of the farthest photon found; the result, times the task's weight,
 // is added to the sample's radiance
 __global__ void __launch_bounds__(128) k_pm_estimate(DScene S, DParams W, DSamples P, DTasks tin,
                                                      const liar_hit* __restrict__ hits, const uint32_t* __restrict__ q_task,
-                                                     uint32_t n_q, PmMap M, DRecovery R, int kind,
+                                                     uint32_t n_q, PmMap M, PmIrradiance I, DRecovery R, int kind,
                                                      const int32_t* __restrict__ g_idx, const float* __restrict__ g_d2,
                                                      const int32_t* __restrict__ g_cnt) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_q) return;
-    const int k = M.k;
+    if ((kind == kEstRadiance || kind == kEstIrradianceMap) && (q_task[i] & kNoRadiance)) return;
+    const int k = kind == kEstIrradianceMap ? 1 : M.k;
     const int cnt = min(g_cnt[i], k);
-    if (cnt < (kind == kEstIrradiance ? 1 : 2)) return;
-    const uint32_t q = q_task[i];
+    if (cnt < (kind == kEstIrradiance || kind == kEstIrradianceMap ? 1 : 2)) return;
+    const uint32_t q = q_task[i] & ~kNoRadiance;
     const uint32_t p = tin.slot[q];
     const float T = tin.T[q];
     const float4 r0 = reinterpret_cast<const float4*>(tin.rays + q)[0];
@@ -465,6 +539,8 @@ __global__ void __launch_bounds__(128) k_pm_estimate(DScene S, DParams W, DSampl
         const float inv = 1.0f / (3.14159265358979323846f * r2);
         RecoveryBlend b;
         if (recovery_locate(R, X * inv, Y * inv, Z * inv, b)) result = recovery_eval(R, b, lam, false);
+    } else if (kind == kEstIrradianceMap) {
+        result = irradiance_map_radiance(S, I, R, HC, d, lam, idx[0]);
     } else {
         const liar_material Mat = S.mats[HC.mat];
         const Bsdf B = make_bsdf(S, Mat, HC, lam);
@@ -488,6 +564,159 @@ __global__ void __launch_bounds__(128) k_pm_estimate(DScene S, DParams W, DSampl
         result /= 3.14159265358979323846f * r2;
     }
     if (result != 0.0f) atomicAdd(&P.L[p], T * result);
+}
+
+// ---- final gathering (photon_mapper.cpp:1060-1251)
+
+// the hits of the gather rays: a hit on an object without a shader continues through it
+// (traceGatherRay's "entering or leaving something"); every other hit becomes a query of the map
+// that answers estimateRadiance there (the irradiance map, else the global map)
+__global__ void __launch_bounds__(128) k_fg_prep(DScene S, DTasks g, const liar_hit* __restrict__ hits, uint32_t n_g,
+                                                 DTasks next, float* q_pos, uint32_t* q_task, uint32_t* q_count) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < n_g;
+    bool cont = false, query = false;
+    float3 point = mk(0, 0, 0);
+    float4 r0 = make_float4(0, 0, 0, 0), r1 = make_float4(0, 0, 1, 0);
+    liar_hit h{-1, 0.0f};
+    if (valid && g.T[i] != 0.0f) {
+        h = hits[i];
+        if (h.prim >= 0) {
+            r0 = reinterpret_cast<const float4*>(g.rays + i)[0];
+            r1 = reinterpret_cast<const float4*>(g.rays + i)[1];
+            const int mi = S.obj_mat[S.tri_obj[h.prim]];
+            if (mi < 0) cont = true;
+            else {
+                query = true;
+                point = mk(r0.x, r0.y, r0.z) + h.t * mk(r1.x, r1.y, r1.z);
+            }
+        }
+    }
+    const uint32_t qi = warp_reserve(q_count, query ? 1u : 0u);
+    if (query) {
+        q_pos[3 * (size_t)qi] = point.x;
+        q_pos[3 * (size_t)qi + 1] = point.y;
+        q_pos[3 * (size_t)qi + 2] = point.z;
+        q_task[qi] = i;
+    }
+    const uint32_t ci = warp_reserve(next.count, cont ? 1u : 0u);
+    if (cont) {
+        put_ray(next.rays, ci, mk(r0.x, r0.y, r0.z), mk(r1.x, r1.y, r1.z), h.t + kTol, r1.w);
+        next.slot[ci] = g.slot[i];
+        next.T[ci] = g.T[i];
+        next.meta[ci] = g.meta[i];
+        next.key[ci] = g.key[i];
+    }
+}
+
+// the radiance a gather ray brings back (traceGatherRay, photon_mapper.cpp:1150-1190): the map
+// estimate at its hit, or, where the hit is closer than that estimate's radius at the first gather
+// stage, numSecondaryGatherRays more gather rays and the low-quality direct light from there
+// (gatherSecondary, :1195-1219)
+__global__ void __launch_bounds__(128) k_fg_shade(DScene S, DParams W, DSamples P, DTasks g,
+                                                  const liar_hit* __restrict__ hits, const uint32_t* __restrict__ q_task,
+                                                  uint32_t n_q, PmMap M, PmIrradiance I, DRecovery R,
+                                                  const int32_t* __restrict__ g_idx, const float* __restrict__ g_d2,
+                                                  const int32_t* __restrict__ g_cnt, DTasks next, DShadows sh) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < n_q;
+    uint32_t gi = 0, p = 0, meta = 0, key = 0;
+    float Tg = 0.0f, lam = 0.0f;
+    float3 o = mk(0, 0, 0), d = mk(0, 0, 1);
+    float t = 0.0f;
+    HitContext HC;
+    HC.mat = -1;
+    HC.light = -1;
+    Bsdf B{};
+    bool bsdf_ok = false, secondary = false;
+    float radiance = 0.0f;
+    if (valid) {
+        gi = q_task[i];
+        p = g.slot[gi];
+        Tg = g.T[gi];
+        meta = g.meta[gi];
+        key = g.key[gi];
+        const float4 r0 = reinterpret_cast<const float4*>(g.rays + gi)[0];
+        const float4 r1 = reinterpret_cast<const float4*>(g.rays + gi)[1];
+        o = mk(r0.x, r0.y, r0.z);
+        d = mk(r1.x, r1.y, r1.z);
+        const liar_hit h = hits[gi];
+        t = h.t;
+        HC = hit_context(S, o, d, (uint32_t)h.prim);
+        lam = P.lam[p];
+        const liar_material Mat = S.mats[HC.mat];
+        if (Mat.type != LIAR_MAT_NONE) {
+            B = make_bsdf(S, Mat, HC, lam);
+            bsdf_ok = true;
+        }
+        // estimateRadiance: nothing without a diffuse part (and its radius stays infinite)
+        float sqr = INFINITY;
+        if (bsdf_ok && has_caps(B.caps, CAP_DIFF)) {
+            if (I.n > 0) {
+                const int32_t j = g_cnt[i] > 0 ? g_idx[i] : -1;
+                if (j < 0) {
+                    sqr = M.radius;  // the reference assigns the radius, not its square (:1295)
+                } else {
+                    sqr = I.r2[j];
+                    radiance = irradiance_map_radiance(S, I, R, HC, d, lam, j);
+                }
+            } else {
+                const int k = M.k, cnt = min(g_cnt[i], k);
+                if (cnt < 2) {
+                    sqr = M.radius;  // as above (:1316)
+                } else {
+                    sqr = g_d2[(size_t)i * k + cnt - 1];
+                    const float3 md = -d;
+                    float3 wi = mk(dot(md, HC.u), dot(md, HC.v), dot(md, HC.N));
+                    wi.z = fmaxf(wi.z, kEps);
+                    for (int j = 0; j < cnt; ++j) {
+                        const int32_t ph = g_idx[(size_t)i * k + j];
+                        if (ph < 0 || (uint64_t)ph >= M.n) continue;
+                        const float3 om = mk(M.omega_in[3 * (size_t)ph], M.omega_in[3 * (size_t)ph + 1],
+                                             M.omega_in[3 * (size_t)ph + 2]);
+                        const BsdfOut be = bsdf_evaluate(B, wi, mk(dot(om, HC.u), dot(om, HC.v), dot(om, HC.N)),
+                                                         CAP_ALL & ~CAP_SPEC & ~CAP_GLOSSY);
+                        if (!(be.pdf > 0.0f) || be.value == 0.0f) continue;
+                        radiance += be.value * photon_power(M, R, ph, lam);
+                    }
+                    radiance /= 3.14159265358979323846f * sqr;
+                }
+            }
+        }
+        secondary = t * t < sqr && !(meta & kStage1) && W.fg_secondary > 0;
+    }
+    // gatherSecondary: the second stage's rays and shadow rays, reserved exactly
+    const uint32_t n_ch = (secondary && bsdf_ok) ? (uint32_t)W.fg_secondary : 0u;
+    const uint32_t n_sh = (secondary && bsdf_ok && S.n_lights > 0) ? 2u * (uint32_t)W.n_secondary : 0u;
+    ShadowWriter sw{sh, warp_reserve(sh.count, n_sh), 0u, n_sh};
+    const uint32_t cbase = warp_reserve(next.count, n_ch);
+    if (valid && !secondary && radiance != 0.0f) atomicAdd(&P.L[p], Tg * radiance);
+    if (n_ch > 0) {
+        const SampleKey skey = dkey(W, W.first_path + p);
+        const float3 md = -d;
+        float3 wi = mk(dot(md, HC.u), dot(md, HC.v), dot(md, HC.N));
+        wi.z = fmaxf(wi.z, kEps);
+        const float3 target = o + t * d;
+        for (uint32_t c = 0; c < n_ch; ++c) {
+            const uint32_t ci = cbase + c;
+            const uint32_t ck = child_key(key, 0x300u + c);
+            const BsdfSample bs = bsdf_sample(B, wi, sample_dim(skey, dim_branch(ck, 0x2000u), false),
+                                              sample_dim(skey, dim_branch(ck, 0x2001u), false),
+                                              sample_dim(skey, dim_branch(ck, 0x2002u), false), CAP_REFL | CAP_DIFF);
+            next.slot[ci] = p;
+            next.meta[ci] = (meta & 0xffu) + 1u | kStage1;
+            next.key[ci] = ck;
+            if (bs.ok()) {
+                put_ray(next.rays, ci, target, bs.wo.x * HC.u + bs.wo.y * HC.v + bs.wo.z * HC.N, kTol, INFINITY);
+                next.T[ci] = Tg * bs.value * (fabsf(bs.wo.z) / ((float)n_ch * bs.pdf));
+            } else {
+                put_void_ray(next.rays, ci);
+                next.T[ci] = 0.0f;
+            }
+        }
+        direct_low_quality(S, W.n_secondary, B, HC, wi, HC.target + (10.0f * kTol) * HC.N, lam, Tg, p, key, skey, sw);
+    }
+    sw.finish(p);
 }
 
 __global__ void k_dl_splat(DScene S, DParams W, DSamples P, uint32_t n) {
@@ -518,6 +747,11 @@ struct DirectBuffers {
     size_t n_queries = 0;
     void* gathers = nullptr;
     size_t n_gathers = 0;
+    // final gathering: two queues of gather rays (48 B each, as tasks) and their hits
+    void* fg[2] = {nullptr, nullptr};
+    size_t n_fg[2] = {0, 0};
+    liar_hit* fg_hits = nullptr;
+    size_t fg_hits_cap = 0;
 };
 
 DirectBuffers* direct_buffers(liar_gpu_ctx* ctx) {
@@ -527,7 +761,7 @@ DirectBuffers* direct_buffers(liar_gpu_ctx* ctx) {
     ctx->extensions.emplace_back("direct", b);
     ctx->on_destroy.push_back([b]() {
         for (void* p : {b->samples, b->tasks[0], b->tasks[1], b->shadows, (void*)b->hits, (void*)b->counters, b->queries,
-                        b->gathers})
+                        b->gathers, b->fg[0], b->fg[1], (void*)b->fg_hits})
             if (p) cudaFree(p);
         if (b->h_counters) cudaFreeHost(b->h_counters);
         delete b;
@@ -562,6 +796,84 @@ DTasks task_view(void* base, size_t cap, uint32_t* count) {
     return t;
 }
 
+// the gather rays of one generation (n0 in queue 0): per stage trace them, let hits without a
+// shader pass, query the map that estimates the radiance at the other hits, shade (estimate or
+// second stage), then trace and add the shadow rays of the second stage; rays that pass and second
+// stage rays form the next queue
+int final_gather(liar_gpu_ctx* ctx, const liar_gpu_mesh* mesh, const DScene& S, DParams& W, const DSamples& P,
+                 DirectBuffers* b, const PmMaps* pm, uint32_t n0, cudaStream_t st) {
+    const PmMap& M = pm->map[kPmGlobal];
+    const bool irr = pm->irr.n > 0;
+    const int k = irr ? 1 : M.k;
+    uint32_t n_g = n0;
+    int cur = 0;
+    for (int pass = 0; n_g > 0; ++pass) {
+        if (pass > 32) return ctx_fail(ctx, LIAR_ERR_TIMEOUT, "final gather rays did not end after 32 passes");
+        const uint64_t want_next = (uint64_t)n_g * (uint64_t)std::max(1, W.fg_secondary);
+        const uint64_t want_sh = (uint64_t)n_g * 2ull * (uint64_t)W.n_secondary;
+        if (want_next > (1ull << 31) || want_sh > (1ull << 31))
+            return ctx_fail(ctx, LIAR_ERR_UNSUPPORTED, "final gather wave too large: set render.wave_paths lower");
+        int rc = grow(ctx, &b->fg[cur ^ 1], &b->n_fg[cur ^ 1], want_next, 48, "final gather rays");
+        if (!rc) rc = grow(ctx, &b->queries, &b->n_queries, n_g, 20, "final gather queries");
+        if (!rc) rc = grow(ctx, &b->gathers, &b->n_gathers, (size_t)n_g * k, 8, "final gather neighbours");
+        if (!rc) rc = grow(ctx, &b->shadows, &b->n_shadows, std::max<uint64_t>(want_sh, 1), 40, "final gather shadows");
+        if (!rc && b->fg_hits_cap < std::max<uint64_t>(std::max<uint64_t>(want_sh, n_g), 1)) {
+            void* hp = b->fg_hits;
+            rc = grow(ctx, &hp, &b->fg_hits_cap, std::max<uint64_t>(want_sh, n_g), 8, "final gather hits");
+            b->fg_hits = static_cast<liar_hit*>(hp);
+        }
+        if (rc) return rc;
+        const DTasks g = task_view(b->fg[cur], b->n_fg[cur], b->counters + 4 + cur);
+        const DTasks next = task_view(b->fg[cur ^ 1], b->n_fg[cur ^ 1], b->counters + 4 + (cur ^ 1));
+        float* q_pos = static_cast<float*>(b->queries);
+        uint32_t* q_task = reinterpret_cast<uint32_t*>(static_cast<char*>(b->queries) + b->n_queries * 12);
+        int32_t* g_cnt = reinterpret_cast<int32_t*>(b->queries) + 4 * b->n_queries;
+        int32_t* g_idx = static_cast<int32_t*>(b->gathers);
+        float* g_d2 = reinterpret_cast<float*>(g_idx + b->n_gathers);
+        DShadows sq;
+        char* sc = static_cast<char*>(b->shadows);
+        sq.rays = reinterpret_cast<liar_ray*>(sc);
+        sq.slot = reinterpret_cast<uint32_t*>(sc + b->n_shadows * 32);
+        sq.value = reinterpret_cast<float*>(sc + b->n_shadows * 36);
+        sq.count = b->counters + 2;
+        rc = trace_mesh_internal(ctx, mesh, g.rays, n_g, b->fg_hits, 0, st, kCounterWord + 10);
+        if (rc) return rc;
+        cudaError_t e = cudaMemsetAsync(b->counters + 4 + (cur ^ 1), 0, 4, st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(b->counters + 2, 0, 8, st);  // shadows, queries
+        if (e != cudaSuccess) return ctx_cuda(ctx, e, "final gather counters");
+        k_fg_prep<<<(n_g + 127) / 128, 128, 0, st>>>(S, g, b->fg_hits, n_g, next, q_pos, q_task, b->counters + 3);
+        e = cudaMemcpyAsync(b->h_counters + 8, b->counters + 3, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return ctx_cuda(ctx, e, "final gather queries");
+        const uint32_t n_q = b->h_counters[8];
+        if (n_q > 0) {
+            rc = liar_gpu_photon_gather_device(ctx, irr ? pm->irr.grid : M.grid, q_pos, n_q, k, g_idx, g_d2, g_cnt, st);
+            if (rc) return rc;
+            k_fg_shade<<<(n_q + 127) / 128, 128, 0, st>>>(S, W, P, g, b->fg_hits, q_task, n_q, M, pm->irr, pm->rec, g_idx,
+                                                          g_d2, g_cnt, next, sq);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return ctx_cuda(ctx, e, "final gather shade launch");
+        }
+        e = cudaMemcpyAsync(b->h_counters + 8, b->counters, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return ctx_cuda(ctx, e, "final gather queue sizes");
+        const uint32_t n_sh = b->h_counters[8 + 2];
+        const uint32_t n_next = b->h_counters[8 + 4 + (cur ^ 1)];
+        if ((uint64_t)n_sh > want_sh || (uint64_t)n_next > want_next)
+            return ctx_fail(ctx, LIAR_ERR_INVALID, "final gather queue overflow");
+        if (n_sh > 0) {
+            rc = trace_mesh_internal(ctx, mesh, sq.rays, n_sh, b->fg_hits, 1, st, kCounterWord + 10);
+            if (rc) return rc;
+            k_dl_shadow_add<<<(n_sh + 255) / 256, 256, 0, st>>>(sq, n_sh, b->fg_hits, P.L);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return ctx_cuda(ctx, e, "final gather shadow launch");
+        }
+        cur ^= 1;
+        n_g = n_next;
+    }
+    return LIAR_OK;
+}
+
 }  // namespace
 
 namespace liar_gpu {
@@ -593,7 +905,8 @@ int render_direct(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_ren
     }
     // samples per wave: keep the first generation's shadow queue near 1 GiB
     uint64_t wave = R.wave_paths > 0 ? (uint64_t)R.wave_paths
-                                     : std::max<uint64_t>(4096, (1ull << 30) / (40ull * shadow_per_task + 64));
+                                     : std::max<uint64_t>(4096, (1ull << 30) / (40ull * shadow_per_task + 64 +
+                                                                                (pm ? 48ull * (uint64_t)pm->fg_rays : 0)));
     wave = std::min<uint64_t>(std::min<uint64_t>(wave, total), 1ull << 22);
     DirectBuffers* b = direct_buffers(ctx);
     int rc = LIAR_OK;
@@ -624,6 +937,10 @@ int render_direct(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_ren
     W.q_pos = nullptr;
     W.q_task = nullptr;
     W.q_count = b->counters + 3;
+    W.fg_rays = (pm && !pm->visualize) ? pm->fg_rays : 0;
+    W.fg_secondary = pm ? pm->fg_secondary : 0;
+    W.fg = DTasks{};
+    W.fg.count = b->counters + 4;
     const DScene& S = scene_dscene(scene);
     const liar_gpu_mesh* mesh = scene_mesh(scene);
     for (uint64_t first = 0; first < total; first += wave) {
@@ -663,6 +980,10 @@ int render_direct(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_ren
                 W.q_pos = static_cast<float*>(b->queries);
                 W.q_task = reinterpret_cast<uint32_t*>(static_cast<char*>(b->queries) + b->n_queries * 12);
             }
+            if (!rc && W.fg_rays > 0) {
+                rc = grow(ctx, &b->fg[0], &b->n_fg[0], (uint64_t)n_in * W.fg_rays, 48, "final gather rays");
+                W.fg = task_view(b->fg[0], b->n_fg[0], b->counters + 4);
+            }
             if (rc) return rc;
             const DTasks tin = task_view(b->tasks[cur], b->n_tasks[cur], b->counters + cur);
             const DTasks tout = task_view(b->tasks[cur ^ 1], b->n_tasks[cur ^ 1], b->counters + (cur ^ 1));
@@ -675,14 +996,15 @@ int render_direct(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_ren
             rc = trace_mesh_internal(ctx, mesh, tin.rays, n_in, b->hits, 0, st, kCounterWord + 10);
             if (rc) return rc;
             e = cudaMemsetAsync(b->counters + (cur ^ 1), 0, 4, st);
-            if (e == cudaSuccess) e = cudaMemsetAsync(b->counters + 2, 0, 8, st);
+            if (e == cudaSuccess) e = cudaMemsetAsync(b->counters + 2, 0, 12, st);
             if (e != cudaSuccess) return ctx_cuda(ctx, e, "reset queues");
             k_dl_shade<<<(n_in + 127) / 128, 128, 0, st>>>(S, W, P, tin, b->hits, n_in, tout, sq, (uint32_t)sh_hq);
             e = cudaGetLastError();
             if (e != cudaSuccess) return ctx_cuda(ctx, e, "direct lighting shade launch");
-            e = cudaMemcpyAsync(b->h_counters, b->counters, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+            e = cudaMemcpyAsync(b->h_counters, b->counters, 5 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
             if (e == cudaSuccess) e = cudaStreamSynchronize(st);
             if (e != cudaSuccess) return ctx_cuda(ctx, e, "direct lighting queue sizes");
+            const uint32_t n_fg0 = W.fg_rays > 0 ? b->h_counters[4] : 0u;
             const uint32_t n_sh = b->h_counters[2];
             if ((uint64_t)n_sh > want_shadows || (uint64_t)b->h_counters[cur ^ 1] > want_children)
                 return ctx_fail(ctx, LIAR_ERR_INVALID, "direct lighting queue overflow");
@@ -693,16 +1015,21 @@ int render_direct(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_ren
                 const PmMap& M = pm->map[m];
                 if (pm->visualize && m != kPmGlobal) continue;
                 if (M.n == 0 || M.k < 1 || !M.grid) continue;
-                rc = grow(ctx, &b->gathers, &b->n_gathers, (size_t)n_q * M.k, 8, "photon gathers");
+                // the global estimate reads the irradiance map when there is one
+                const bool irr = m == kPmGlobal && !pm->visualize && pm->irr.n > 0;
+                const int k = irr ? 1 : M.k;
+                rc = grow(ctx, &b->gathers, &b->n_gathers, (size_t)n_q * k, 8, "photon gathers");
                 if (rc) return rc;
                 int32_t* g_idx = static_cast<int32_t*>(b->gathers);
                 float* g_d2 = reinterpret_cast<float*>(g_idx + b->n_gathers);
                 int32_t* g_cnt = reinterpret_cast<int32_t*>(b->queries) + 4 * b->n_queries;  // after positions and tasks
-                rc = liar_gpu_photon_gather_device(ctx, M.grid, W.q_pos, n_q, M.k, g_idx, g_d2, g_cnt, st);
+                rc = liar_gpu_photon_gather_device(ctx, irr ? pm->irr.grid : M.grid, W.q_pos, n_q, k, g_idx, g_d2,
+                                                   g_cnt, st);
                 if (rc) return rc;
-                const int kind = pm->visualize ? kEstIrradiance : (m == kPmGlobal ? kEstRadiance : kEstCaustics);
-                k_pm_estimate<<<(n_q + 127) / 128, 128, 0, st>>>(S, W, P, tin, b->hits, W.q_task, n_q, M, pm->rec, kind,
-                                                                  g_idx, g_d2, g_cnt);
+                const int kind = pm->visualize ? kEstIrradiance
+                                               : (m == kPmGlobal ? (irr ? kEstIrradianceMap : kEstRadiance) : kEstCaustics);
+                k_pm_estimate<<<(n_q + 127) / 128, 128, 0, st>>>(S, W, P, tin, b->hits, W.q_task, n_q, M, pm->irr,
+                                                                  pm->rec, kind, g_idx, g_d2, g_cnt);
                 e = cudaGetLastError();
                 if (e != cudaSuccess) return ctx_cuda(ctx, e, "photon estimate launch");
             }
@@ -712,6 +1039,10 @@ int render_direct(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_ren
                 k_dl_shadow_add<<<(n_sh + 255) / 256, 256, 0, st>>>(sq, n_sh, b->hits, P.L);
                 e = cudaGetLastError();
                 if (e != cudaSuccess) return ctx_cuda(ctx, e, "direct lighting shadow launch");
+            }
+            if (n_fg0 > 0) {
+                rc = final_gather(ctx, mesh, S, W, P, b, pm, n_fg0, st);
+                if (rc) return rc;
             }
             cur ^= 1;
             n_in = b->h_counters[cur];

@@ -22,6 +22,7 @@
 #include "../../include/liar_gpu.h"
 #include "ctx.h"
 #include "photon_mapper.h"
+#include "sampler.h"
 
 using namespace liar_gpu;
 
@@ -43,7 +44,9 @@ struct PmCache {
     uint64_t seed = 0;
     bool valid = false;
     void* mem = nullptr;
+    void* irr_mem = nullptr;
     liar_gpu_photon_map* grid[2] = {nullptr, nullptr};
+    liar_gpu_photon_map* irr_grid = nullptr;
     PmMaps maps;
 
     void release() {
@@ -51,8 +54,11 @@ struct PmCache {
             if (g) liar_gpu_photon_map_destroy(g);
             g = nullptr;
         }
+        if (irr_grid) liar_gpu_photon_map_destroy(irr_grid);
+        irr_grid = nullptr;
         if (mem) cudaFree(mem);
-        mem = nullptr;
+        if (irr_mem) cudaFree(irr_mem);
+        mem = irr_mem = nullptr;
         valid = false;
     }
 };
@@ -75,7 +81,7 @@ bool same_desc(const liar_photon_mapper_desc& a, const liar_photon_mapper_desc& 
 
 // the stored photons of one trace, on the host
 struct Traced {
-    std::vector<float> position, omega, power;
+    std::vector<float> position, omega, power, normal;
     std::vector<uint32_t> path, tag;
     uint64_t emitted = 0, stored = 0;
 };
@@ -84,7 +90,7 @@ int trace(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_photon_desc
           cudaStream_t st, Traced& out) {
     for (int attempt = 0; attempt < 6; ++attempt, capacity *= 4) {
         void* mem = nullptr;
-        cudaError_t e = cudaMalloc(&mem, capacity * 44 + 1024);
+        cudaError_t e = cudaMalloc(&mem, capacity * 56 + 1024);
         if (e != cudaSuccess) {
             cudaGetLastError();
             return ctx_cuda(ctx, e, "photon buffers");
@@ -96,6 +102,7 @@ int trace(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_photon_desc
         B.power = reinterpret_cast<float*>(p + capacity * 24);
         B.path = reinterpret_cast<uint32_t*>(p + capacity * 36);
         B.tag = reinterpret_cast<uint32_t*>(p + capacity * 40);
+        B.normal = reinterpret_cast<float*>(p + capacity * 44);
         B.capacity = capacity;
         liar_photon_counts counts{};
         int rc = liar_gpu_photon_trace(ctx, scene, &pd, &B, &counts, st);
@@ -108,6 +115,7 @@ int trace(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_photon_desc
             out.position.resize(3 * n);
             out.omega.resize(3 * n);
             out.power.resize(3 * n);
+            out.normal.resize(3 * n);
             out.path.resize(n);
             out.tag.resize(n);
             out.emitted = counts.emitted;
@@ -118,6 +126,7 @@ int trace(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_photon_desc
                 if (e == cudaSuccess) e = cudaMemcpyAsync(out.power.data(), B.power, n * 12, cudaMemcpyDeviceToHost, st);
                 if (e == cudaSuccess) e = cudaMemcpyAsync(out.path.data(), B.path, n * 4, cudaMemcpyDeviceToHost, st);
                 if (e == cudaSuccess) e = cudaMemcpyAsync(out.tag.data(), B.tag, n * 4, cudaMemcpyDeviceToHost, st);
+                if (e == cudaSuccess) e = cudaMemcpyAsync(out.normal.data(), B.normal, n * 12, cudaMemcpyDeviceToHost, st);
                 if (e == cudaSuccess) e = cudaStreamSynchronize(st);
                 if (e != cudaSuccess) rc = ctx_cuda(ctx, e, "photon download");
             }
@@ -126,6 +135,87 @@ int trace(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_photon_desc
         return rc;
     }
     return ctx_fail(ctx, LIAR_ERR_OOM, "photon buffer still too small");
+}
+
+__global__ void k_irr_r2(const float* __restrict__ d2, const int32_t* __restrict__ cnt, uint32_t n, int k,
+                         float* __restrict__ r2) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int c = min(cnt[i], k);
+    r2[i] = c > 0 ? d2[(size_t)i * k + c - 1] : 0.0f;
+}
+
+// the points of the irradiance map: global photons chosen with probability `ratio` (the reference
+// draws uniform(rng) <= ratio per stored global photon; here a hash of the photon's emission and
+// bounce), each with the photon's position and normal; their irradiance is estimateIrradianceImpl
+// over the global map (liar_gpu_photon_estimate_device), and a gather grid over them answers the
+// nearest-neighbour queries of estimateRadiance
+int build_irradiance(liar_gpu_ctx* ctx, cudaStream_t st, PmCache* C, const Traced& T,
+                     const std::vector<uint32_t>& global, float ratio) {
+    PmMaps& M = C->maps;
+    const PmMap& G = M.map[kPmGlobal];
+    std::vector<float> host;  // positions, then normals
+    std::vector<uint32_t> chosen;
+    for (uint32_t i : global) {
+        const uint64_t h = mix64(0x6972726164ull ^ mix64(((uint64_t)T.path[i] << 8) | ((T.tag[i] >> 8) & 0xffu)));
+        const float u = (float)(h >> 40) * (1.0f / 16777216.0f);
+        if (u <= ratio) chosen.push_back(i);
+    }
+    const size_t n = chosen.size();
+    if (n == 0) return LIAR_OK;
+    host.resize(6 * n);
+    for (size_t j = 0; j < n; ++j)
+        for (int c = 0; c < 3; ++c) {
+            host[3 * j + c] = T.position[3 * chosen[j] + c];
+            host[3 * n + 3 * j + c] = T.normal[3 * chosen[j] + c];
+        }
+    const int k = G.k;
+    // per point: position, normal, xyz, blend (idx, w) = 60 B and r2 4 B; gather scratch k x 8 B + 4 B
+    const size_t keep = n * 64 + 1024, scratch = n * ((size_t)k * 8 + 4) + 256;
+    cudaError_t e = cudaMalloc(&C->irr_mem, keep);
+    void* tmp = nullptr;
+    if (e == cudaSuccess) e = cudaMalloc(&tmp, scratch);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        if (tmp) cudaFree(tmp);
+        return ctx_cuda(ctx, e, "irradiance map");
+    }
+    float* pos = static_cast<float*>(C->irr_mem);
+    float* nrm = pos + 3 * n;
+    float* xyz = pos + 6 * n;
+    int32_t* bidx = reinterpret_cast<int32_t*>(pos + 9 * n);
+    float* bw = pos + 12 * n;
+    float* r2 = pos + 15 * n;
+    int32_t* g_idx = static_cast<int32_t*>(tmp);
+    float* g_d2 = reinterpret_cast<float*>(g_idx + (size_t)n * k);
+    int32_t* g_cnt = reinterpret_cast<int32_t*>(g_d2 + (size_t)n * k);
+    int rc = LIAR_OK;
+    e = cudaMemcpyAsync(pos, host.data(), 6 * n * sizeof(float), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) rc = ctx_cuda(ctx, e, "irradiance points");
+    if (!rc) rc = liar_gpu_photon_gather_device(ctx, G.grid, pos, n, k, g_idx, g_d2, g_cnt, st);
+    if (!rc)
+        rc = liar_gpu_photon_estimate_device(ctx, G.power, G.omega_in, (size_t)G.n, nrm, n, k, g_idx, g_d2, g_cnt, 1.0f,
+                                             xyz, st);
+    if (!rc) {
+        k_irr_r2<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g_d2, g_cnt, (uint32_t)n, k, r2);
+        rc = ctx_cuda(ctx, cudaGetLastError(), "irradiance radii");
+    }
+    if (!rc) rc = recovery_locate_device(ctx, xyz, n, bidx, bw, st);
+    if (!rc) rc = liar_gpu_photon_map_build_device(ctx, pos, n, G.radius, &C->irr_grid, st);
+    e = cudaStreamSynchronize(st);
+    cudaFree(tmp);
+    if (rc) return rc;
+    if (e != cudaSuccess) return ctx_cuda(ctx, e, "irradiance map");
+    PmIrradiance& I = M.irr;
+    I.grid = C->irr_grid;
+    I.position = pos;
+    I.normal = nrm;
+    I.xyz = xyz;
+    I.blend_idx = bidx;
+    I.blend_w = bw;
+    I.r2 = r2;
+    I.n = n;
+    return LIAR_OK;
 }
 
 int build_maps(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_render_desc& R, cudaStream_t st,
@@ -140,6 +230,8 @@ int build_maps(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_render
     pd.global_target = target;
     pd.max_emitted = max_photons;
     pd.wave = std::min<uint64_t>(std::max<uint64_t>(2 * target, 1u << 14), 1u << 21);
+    const bool fg = D.ray_trace_direct >= 0 && D.final_gather_rays > 0;  // hasFinalGather
+    pd.final_gather = fg ? 1 : 0;
     Traced T;
     int rc = trace(ctx, scene, pd, (target + pd.wave) * 4, st, T);
     if (rc) return rc;
@@ -164,6 +256,8 @@ int build_maps(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_render
     M.emitted = shot;
     M.visualize = D.visualize != 0;
     M.ray_direct = D.ray_trace_direct < 0 ? 0 : 1;
+    M.fg_rays = fg ? D.final_gather_rays : 0;
+    M.fg_secondary = fg ? (D.secondary_gather_rays == 0 ? 1 : std::max(0, D.secondary_gather_rays)) : 0;
     std::vector<uint32_t> members[2];
     for (uint32_t i : order)
         if (T.path[i] < shot) {
@@ -226,6 +320,12 @@ int build_maps(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_render
         P.grid = C->grid[m];
         e = cudaStreamSynchronize(st);  // the host copy of the photons goes out of scope
         if (e != cudaSuccess) return ctx_cuda(ctx, e, "photon map build");
+    }
+    // ---- the irradiance map of final gathering (photon_mapper.cpp:745-749, 970-995)
+    const float ratio = D.ratio_precomputed_irradiance == 0.0f ? 0.25f : D.ratio_precomputed_irradiance;
+    if (fg && ratio > 0.0f && M.map[kPmGlobal].n > 0) {
+        rc = build_irradiance(ctx, st, C, T, members[kPmGlobal], ratio);
+        if (rc) return rc;
     }
     C->scene = rt::scene_uid(scene);
     C->desc = D;
@@ -312,4 +412,29 @@ extern "C" int liar_gpu_photon_mapper_get_map(liar_gpu_ctx* ctx, int map, float*
     if (n && e == cudaSuccess && blend_idx) e = cudaMemcpy(blend_idx, M.blend_idx, n * 12, cudaMemcpyDeviceToHost);
     if (n && e == cudaSuccess && blend_w) e = cudaMemcpy(blend_w, M.blend_w, n * 12, cudaMemcpyDeviceToHost);
     return e == cudaSuccess ? LIAR_OK : ctx_cuda(ctx, e, "photon map download");
+}
+
+extern "C" int liar_gpu_photon_mapper_get_irradiance(liar_gpu_ctx* ctx, float* position, float* normal, float* xyz,
+                                                     int32_t* blend_idx, float* blend_w, float* r2, size_t capacity,
+                                                     size_t* n_out) {
+    if (!ctx || !n_out) return LIAR_ERR_INVALID;
+    *n_out = 0;
+    const PmCache* c = nullptr;
+    for (auto& ext : ctx->extensions)
+        if (ext.first == "photon_mapper") c = static_cast<const PmCache*>(ext.second);
+    if (!c || !c->valid) return ctx_fail(ctx, LIAR_ERR_INVALID, "no photon maps on this context");
+    const PmIrradiance& I = c->maps.irr;
+    *n_out = (size_t)I.n;
+    if (I.n > capacity) return ctx_fail(ctx, LIAR_ERR_INVALID, "irradiance map holds %llu points, more than capacity",
+                                        (unsigned long long)I.n);
+    int rc = ctx_activate(ctx);
+    if (rc) return rc;
+    const size_t n = (size_t)I.n;
+    cudaError_t e = cudaSuccess;
+    const void* src[6] = {I.position, I.normal, I.xyz, I.blend_idx, I.blend_w, I.r2};
+    void* dst[6] = {position, normal, xyz, blend_idx, blend_w, r2};
+    const size_t bytes[6] = {n * 12, n * 12, n * 12, n * 12, n * 12, n * 4};
+    for (int k = 0; k < 6 && e == cudaSuccess; ++k)
+        if (n && dst[k]) e = cudaMemcpy(dst[k], src[k], bytes[k], cudaMemcpyDeviceToHost);
+    return e == cudaSuccess ? LIAR_OK : ctx_cuda(ctx, e, "irradiance map download");
 }

@@ -25,11 +25,28 @@ struct PmMap {
     int k = 0;                                  // estimationSize (kMax of the gathers)
 };
 
+// the precomputed irradiance map of final gathering (buildIrradianceMap, photon_mapper.cpp:970-995):
+// points at a random subset of the global photons, each with its normal, its irradiance
+// (estimateIrradianceImpl over the global map) as a recovery blend, and its squared radius
+struct PmIrradiance {
+    const liar_gpu_photon_map* grid = nullptr;  // nearest-neighbour structure over the points
+    const float* position = nullptr;            // n x 3
+    const float* normal = nullptr;              // n x 3
+    const float* xyz = nullptr;                 // n x 3
+    const int32_t* blend_idx = nullptr;         // n x 3
+    const float* blend_w = nullptr;             // n x 3
+    const float* r2 = nullptr;                  // n: squaredEstimationRadius (0: no photon found)
+    uint64_t n = 0;
+};
+
 struct PmMaps {
     PmMap map[2];
+    PmIrradiance irr;
     DRecovery rec;
     int visualize = 0;     // isVisualizingPhotonMap
     int ray_direct = 1;    // isRayTracingDirect
+    int fg_rays = 0;       // numFinalGatherRays when final gathering is on (hasFinalGather), else 0
+    int fg_secondary = 0;  // numSecondaryGatherRays
     uint64_t emitted = 0;  // photons shot
 };
 

@@ -53,6 +53,7 @@ struct PParams {
     uint64_t first_path;
     int max_gen;
     int rt_direct;
+    int final_gather;  // every diffuse hit is a global photon
 };
 
 __device__ __forceinline__ float psample(const PParams& P, uint64_t path, uint32_t dim) {
@@ -171,7 +172,7 @@ __global__ void __launch_bounds__(128) k_photon_shade(DScene S, PParams P, PStat
                 if (M.type == LIAR_MAT_LAMBERT) {
                     // Shader::hasCaps(diffuse): store (photon_mapper.cpp:733-748)
                     const bool to_caustic = caustic;
-                    const bool to_global = (gen > 0 || !P.rt_direct) && !caustic;
+                    const bool to_global = ((gen > 0 || !P.rt_direct) && !caustic) || P.final_gather;
                     if (to_caustic || to_global) {
                         const unsigned long long s = atomicAdd(counters + 0, 1ull);
                         if (s < B.capacity) {
@@ -187,9 +188,15 @@ __global__ void __launch_bounds__(128) k_photon_shade(DScene S, PParams P, PStat
                             B.power[3 * s + 1] = sc * c.y;
                             B.power[3 * s + 2] = sc * c.z;
                             B.path[s] = (uint32_t)path;
-                            B.tag[s] = (to_caustic ? (uint32_t)LIAR_PHOTON_CAUSTIC : (uint32_t)LIAR_PHOTON_GLOBAL) |
-                                       ((uint32_t)gen << 8);
-                            atomicAdd(counters + (to_caustic ? 2 : 1), 1ull);
+                            B.tag[s] = (to_caustic ? (uint32_t)LIAR_PHOTON_CAUSTIC : 0u) |
+                                       (to_global ? (uint32_t)LIAR_PHOTON_GLOBAL : 0u) | ((uint32_t)gen << 8);
+                            if (B.normal) {
+                                B.normal[3 * s] = H.N.x;
+                                B.normal[3 * s + 1] = H.N.y;
+                                B.normal[3 * s + 2] = H.N.z;
+                            }
+                            if (to_global) atomicAdd(counters + 1, 1ull);
+                            if (to_caustic) atomicAdd(counters + 2, 1ull);
                         } else {
                             atomicOr(status, 1u << 5);  // buffer full: the photon is lost, the host reports it
                         }
@@ -324,6 +331,7 @@ extern "C" int liar_gpu_photon_trace(liar_gpu_ctx* ctx, const liar_gpu_scene* sc
     P.seed = mix64(desc->seed ^ 0x9a1d37c8e15b22f3ull);
     P.max_gen = desc->max_ray_generation;
     P.rt_direct = desc->ray_traced_direct;
+    P.final_gather = desc->final_gather ? 1 : 0;
     uint64_t emitted = 0;
     counts->stored = counts->global = counts->caustic = 0;
     while (emitted < desc->max_emitted && counts->global < desc->global_target) {

@@ -72,12 +72,13 @@ class PhotonMap:
 
 class PhotonDesc(C.Structure):
     _fields_ = [("max_ray_generation", C.c_int32), ("ray_traced_direct", C.c_int32), ("seed", C.c_uint64),
-                ("global_target", C.c_uint64), ("max_emitted", C.c_uint64), ("wave", C.c_uint64)]
+                ("global_target", C.c_uint64), ("max_emitted", C.c_uint64), ("wave", C.c_uint64),
+                ("final_gather", C.c_int32), ("reserved", C.c_int32)]
 
 
 class PhotonBuffers(C.Structure):
     _fields_ = [("position", C.c_void_p), ("omega_in", C.c_void_p), ("power", C.c_void_p), ("path", C.c_void_p),
-                ("tag", C.c_void_p), ("capacity", C.c_uint64)]
+                ("tag", C.c_void_p), ("capacity", C.c_uint64), ("normal", C.c_void_p)]
 
 
 class PhotonCounts(C.Structure):
@@ -88,7 +89,7 @@ GLOBAL, CAUSTIC = 1, 2
 
 
 def photon_desc(global_target: int, max_emitted: int = 100_000_000, max_ray_generation: int = 8, seed: int = 0,
-                wave: int = 0, ray_traced_direct: bool = True) -> PhotonDesc:
+                wave: int = 0, ray_traced_direct: bool = True, final_gather: bool = False) -> PhotonDesc:
     d = PhotonDesc()
     d.max_ray_generation = int(max_ray_generation)
     d.ray_traced_direct = int(bool(ray_traced_direct))
@@ -96,6 +97,7 @@ def photon_desc(global_target: int, max_emitted: int = 100_000_000, max_ray_gene
     d.global_target = int(global_target)
     d.max_emitted = int(max_emitted)
     d.wave = int(wave)
+    d.final_gather = int(bool(final_gather))
     return d
 
 

@@ -58,7 +58,9 @@ class CCamera(C.Structure):
 class CPhotonMapperDesc(C.Structure):
     _fields_ = [("max_photons", C.c_uint64), ("global_map_size", C.c_uint64),
                 ("estimation_radius", C.c_float * 2), ("estimation_tolerance", C.c_float * 2),
-                ("estimation_size", C.c_int32 * 2), ("ray_trace_direct", C.c_int32), ("visualize", C.c_int32)]
+                ("estimation_size", C.c_int32 * 2), ("ray_trace_direct", C.c_int32), ("visualize", C.c_int32),
+                ("final_gather_rays", C.c_int32), ("secondary_gather_rays", C.c_int32),
+                ("ratio_precomputed_irradiance", C.c_float), ("reserved", C.c_int32)]
 
 
 class CRenderDesc(C.Structure):
@@ -395,8 +397,6 @@ def render_desc(camera, width: int, height: int, spp: int, tracer, seed: int = 0
     r.secondary_light_samples = int(getattr(tracer, "numberOfSecondaryLightSamples", 1))
     r.trace_glossy = 1 if getattr(tracer, "traceGlossy", True) else -1
     if r.tracer == 2:
-        if getattr(tracer, "numFinalGatherRays", 0):
-            raise NotImplementedError("PhotonMapper final gathering is not on the GPU path (numFinalGatherRays = 0)")
         if float(getattr(tracer, "causticsQuality", 1.0)) != 1.0:
             raise NotImplementedError("PhotonMapper causticsQuality other than 1 is not on the GPU path")
         pm = r.photon_mapper
@@ -408,6 +408,10 @@ def render_desc(camera, width: int, height: int, spp: int, tracer, seed: int = 0
             pm.estimation_size[m] = int(tracer._size[m])
         pm.ray_trace_direct = 1 if tracer.isRayTracingDirect else -1
         pm.visualize = 1 if tracer.isVisualizingPhotonMap else 0
+        pm.final_gather_rays = int(tracer.numFinalGatherRays)
+        pm.secondary_gather_rays = int(tracer.numSecondaryGatherRays) or -1
+        ratio = float(tracer.ratioPrecomputedIrradiance)
+        pm.ratio_precomputed_irradiance = ratio if ratio > 0 else -1.0
     r.filter = int(filter)
     r.filter_param = float(filter_param)
     r.max_sample_luminance = float(max_sample_luminance) if math.isfinite(max_sample_luminance) else 0.0
@@ -515,4 +519,24 @@ def photon_mapper_map(ctx, m: int) -> dict:
     ctx.check(fn(ctx.handle, int(m), a["position"].ctypes.data, a["omega_in"].ctypes.data, a["power"].ctypes.data,
                  a["blend_idx"].ctypes.data, a["blend_w"].ctypes.data, n, C.byref(got)))
     a["radius"] = st["radius"][m]
+    return a
+
+
+def photon_mapper_irradiance(ctx) -> dict:
+    """The irradiance map of the last PhotonMapper render with final gathering, as host arrays."""
+    got = C.c_size_t()
+    fn = ctx._lib.liar_gpu_photon_mapper_get_irradiance
+    fn.restype = C.c_int
+    fn.argtypes = [C.c_void_p] + [C.c_void_p] * 6 + [C.c_size_t, C.POINTER(C.c_size_t)]
+    # the size first (a call with capacity 0 reports it, refusing the copy when there are points)
+    rc = fn(ctx.handle, None, None, None, None, None, None, 0, C.byref(got))
+    n = int(got.value)
+    a = {k: np.zeros((n, 3), np.float32) for k in ("position", "normal", "xyz", "blend_w")}
+    a["blend_idx"] = np.zeros((n, 3), np.int32)
+    a["r2"] = np.zeros(n, np.float32)
+    if n:
+        ctx.check(fn(ctx.handle, a["position"].ctypes.data, a["normal"].ctypes.data, a["xyz"].ctypes.data,
+                     a["blend_idx"].ctypes.data, a["blend_w"].ctypes.data, a["r2"].ctypes.data, n, C.byref(got)))
+    elif rc:
+        ctx.check(rc)  # no maps at all
     return a

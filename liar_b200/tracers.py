@@ -29,9 +29,13 @@ class DirectLighting(RayTracer):
 class PhotonMapper(DirectLighting):
     """Photon mapping (src/liar/tracers/photon_mapper.cpp): DirectLighting plus, at every vertex with
     a diffuse part, the caustic map's Gaussian-filtered estimate and the global map's radiance
-    estimate; the maps are filled from the lights before rendering. Defaults as the reference's
-    (photon_mapper.cpp:108-142). Final gathering (numFinalGatherRays > 0) and volumetric maps are
-    not on the GPU path; causticsQuality other than 1 (its storage probabilities) neither."""
+    estimate; the maps are filled from the lights before rendering. With numFinalGatherRays > 0
+    (and isRayTracingDirect) high-quality diffuse vertices gather the indirect light with that many
+    BSDF-sampled rays, evaluated at their hits from the precomputed irradiance map
+    (ratioPrecomputedIrradiance of the global photons), with numSecondaryGatherRays more rays where a
+    hit lies closer than the estimation radius. Defaults as the reference's
+    (photon_mapper.cpp:108-142). Volumetric maps and causticsQuality other than 1 (its storage
+    probabilities) are not on the GPU path."""
     kind = 2
     MAP_TYPES = {"global": 0, "caustic": 1, "caustics": 1}
 

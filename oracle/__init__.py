@@ -108,10 +108,12 @@ class RenderScene:
         lib().oracle_render(self.h, C.addressof(desc), film.ctypes.data, int(b), int(e), int(threads))
         return film
 
-    def render_pm(self, desc, maps, recovery_table, film=None, pixels=None, threads=0):
+    def render_pm(self, desc, maps, recovery_table, film=None, pixels=None, threads=0, irradiance=None):
         """The PhotonMapper restatement with the given maps: ``maps`` is a list of two dicts (global,
         caustic) with position, omega_in, power (n x 3 float32), blend_idx (n x 3 int32), blend_w
-        (n x 3 float32), radius and k; ``recovery_table`` is liar_b200.recovery.device_table()."""
+        (n x 3 float32), radius and k; ``recovery_table`` is liar_b200.recovery.device_table();
+        ``irradiance`` the irradiance map of final gathering (position, normal, blend_idx, blend_w,
+        r2) or None. Final gathering follows desc.photon_mapper."""
         if film is None:
             film = np.zeros((desc.height, desc.width, 8), dtype=np.float32)
         keep = []
@@ -142,6 +144,17 @@ class RenderScene:
         pm.rec_nw = int(np.asarray(t["wavelengths"]).size)
         pm.rec_ns = int(np.asarray(t["spectra"]).shape[0])
         pm.rec_nt = int(np.asarray(t["triangles"]).shape[0])
+        D = desc.photon_mapper
+        fg = D.ray_trace_direct >= 0 and D.final_gather_rays > 0
+        pm.fg_rays = int(D.final_gather_rays) if fg else 0
+        pm.fg_secondary = (1 if D.secondary_gather_rays == 0 else max(0, int(D.secondary_gather_rays))) if fg else 0
+        if irradiance is not None and len(irradiance["position"]):
+            pm.irr_position = arr(irradiance["position"], np.float32)
+            pm.irr_normal = arr(irradiance["normal"], np.float32)
+            pm.irr_blend_idx = arr(irradiance["blend_idx"], np.int32)
+            pm.irr_blend_w = arr(irradiance["blend_w"], np.float32)
+            pm.irr_r2 = arr(irradiance["r2"], np.float32)
+            pm.n_irr = int(np.asarray(irradiance["position"]).reshape(-1, 3).shape[0])
         L = lib()
         L.oracle_render_pm.restype = C.c_int
         L.oracle_render_pm.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_int]
@@ -165,7 +178,10 @@ class _PmIn(C.Structure):
                 ("blend_idx", C.c_void_p * 2), ("blend_w", C.c_void_p * 2), ("n", C.c_uint64 * 2),
                 ("radius", C.c_float * 2), ("k", C.c_int32 * 2), ("visualize", C.c_int32), ("ray_direct", C.c_int32),
                 ("rec_wavelengths", C.c_void_p), ("rec_spectra", C.c_void_p), ("rec_points", C.c_void_p),
-                ("rec_tris", C.c_void_p), ("rec_nw", C.c_int32), ("rec_ns", C.c_int32), ("rec_nt", C.c_int32)]
+                ("rec_tris", C.c_void_p), ("rec_nw", C.c_int32), ("rec_ns", C.c_int32), ("rec_nt", C.c_int32),
+                ("fg_rays", C.c_int32), ("fg_secondary", C.c_int32), ("irr_position", C.c_void_p),
+                ("irr_normal", C.c_void_p), ("irr_blend_idx", C.c_void_p), ("irr_blend_w", C.c_void_p),
+                ("irr_r2", C.c_void_p), ("n_irr", C.c_uint64)]
 
 
 class Tree:

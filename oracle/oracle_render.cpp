@@ -98,6 +98,9 @@ struct RenderIn {
     uint64_t pm_max_photons, pm_global_map_size;
     float pm_radius[2], pm_tolerance[2];
     int32_t pm_size[2], pm_ray_trace_direct, pm_visualize;
+    int32_t pm_final_gather_rays, pm_secondary_gather_rays;
+    float pm_ratio_precomputed_irradiance;
+    int32_t pm_reserved;
 };
 
 // The photon maps of a PhotonMapper render (photon_mapper.cpp:798-835) as the oracle gets them:
@@ -118,6 +121,15 @@ struct PmIn {
     const float* rec_points;   // (n_samples + 4) x 2
     const int32_t* rec_tris;
     int32_t rec_nw, rec_ns, rec_nt;
+    // final gathering: rays per high-quality diffuse vertex (0: none), secondary rays, and the
+    // irradiance map (points, normals, blends of the irradiance, squared radii)
+    int32_t fg_rays, fg_secondary;
+    const float* irr_position;
+    const float* irr_normal;
+    const int32_t* irr_blend_idx;
+    const float* irr_blend_w;
+    const float* irr_r2;
+    uint64_t n_irr;
 };
 
 enum { SP_CONST = 0, SP_SAMPLED = 1, SP_BB = 2, SP_CAUCHY = 3 };
@@ -1067,6 +1079,131 @@ float pm_irradiance(const DLPath& P, const Ctx& c) {
     return pm_recover(pm, idx, w, P.lam);
 }
 
+// traceDirect with highQuality false (direct_lighting.cpp:236-262)
+float dl_direct_lq(const DLPath& P, const Bsdf& B, const Ctx& c, V wi, V start, uint32_t key) {
+    const Scene& S = *P.S;
+    const int nlights = (int)S.in.n_lights;
+    if (nlights <= 0) return 0;
+    const int n = P.R->secondary_light_samples > 0 ? P.R->secondary_light_samples : 1;
+    float result = 0;
+    for (int k = 0; k < n; ++k) {
+        const uint32_t j0 = 16u * (uint32_t)k;
+        const float uc = P.smp.get(dl_dim_branch(key, j0), false);
+        int l = (int)(std::lower_bound(S.light_cdf.begin(), S.light_cdf.end(), uc) - S.light_cdf.begin());
+        l = std::min(l, nlights - 1);
+        const float pc = light_pdf_choice(S, l);
+        if (!(pc > 0)) continue;
+        const int nb = S.in.lights[l].type == L_POINT ? 0 : 1;
+        auto u = [&](int kind, int, int axis) {
+            return P.smp.get(dl_dim_branch(key, j0 + 1u + 2u * (uint32_t)kind + (uint32_t)axis), false);
+        };
+        result += estimate_light(S, B, c, wi, start, l, 1, nb, P.lam, u) / ((float)n * pc);
+    }
+    return result;
+}
+
+uint32_t dl_dim_final_gather(int i, int axis) { return 0x600000u + (uint32_t)i * 4u + (uint32_t)axis; }
+
+// estimateRadiance (photon_mapper.cpp:1282-1336): from the irradiance map's nearest point within
+// the global radius when there is a map, else the global map's k nearest photons; *sqr gets the
+// estimate's squared radius (the radius itself, as the reference assigns it, when nothing is found;
+// infinity without a diffuse part)
+float pm_radiance(const DLPath& P, const Ctx& c, const Bsdf& B, V wi, float* sqr) {
+    const PmIn& pm = *P.pm;
+    *sqr = INFINITY;
+    if (!has(B.caps, C_DIFF)) return 0;
+    if (pm.n_irr > 0) {
+        const float r2max = pm.radius[0] * pm.radius[0];
+        int64_t best = -1;
+        float bd = INFINITY;
+        for (uint64_t i = 0; i < pm.n_irr; ++i) {
+            const float dx = pm.irr_position[3 * i] - c.target.x, dy = pm.irr_position[3 * i + 1] - c.target.y,
+                        dz = pm.irr_position[3 * i + 2] - c.target.z;
+            const float d2 = dx * dx + dy * dy + dz * dz;
+            if (d2 < r2max && d2 < bd) {
+                bd = d2;
+                best = (int64_t)i;
+            }
+        }
+        if (best < 0) {
+            *sqr = pm.radius[0];
+            return 0;
+        }
+        *sqr = pm.irr_r2[best];
+        const float* n = pm.irr_normal + 3 * best;
+        const V wo{n[0] * c.u.x + n[1] * c.u.y + n[2] * c.u.z, n[0] * c.v.x + n[1] * c.v.y + n[2] * c.v.z,
+                   n[0] * c.N.x + n[1] * c.N.y + n[2] * c.N.z};
+        const Out be = evaluate(B, wi, wo, C_ALL);
+        if (!(be.pdf > 0) || be.value == 0) return 0;
+        return be.value * pm_recover(pm, pm.irr_blend_idx + 3 * best, pm.irr_blend_w + 3 * best, P.lam);
+    }
+    if (pm.n[0] == 0 || pm.k[0] < 1) return 0;
+    thread_local std::vector<std::pair<float, int64_t>> nb;
+    pm_nearest(pm, 0, c.target, nb);
+    if (nb.size() < 2) {
+        *sqr = pm.radius[0];
+        return 0;
+    }
+    *sqr = nb.back().first;
+    return pm_estimate(P, 0, c, B, wi);
+}
+
+float pm_gather_indirect(const DLPath& P, const Ctx& c, const Bsdf& B, V wi, V origin, int n, int stage,
+                         uint32_t key);
+
+// traceGatherRay (photon_mapper.cpp:1150-1190)
+float pm_trace_gather(const DLPath& P, V o, V d, float tmin, int stage, uint32_t key) {
+    const Scene& S = *P.S;
+    const Hit h = oracle_internal::tree_closest(S.tree, Ray{o.x, o.y, o.z, tmin, d.x, d.y, d.z, INFINITY});
+    if (h.prim < 0) return 0;
+    const Ctx c = hit_ctx(S, o, d, h);
+    if (c.mi < 0) return pm_trace_gather(P, o, d, h.t + TOL, stage, key);  // entering or leaving something
+    const Material& M = S.in.materials[c.mi];
+    if (M.type == M_NONE) return 0;
+    const Bsdf B = make_bsdf(S, M, c, P.lam);
+    const V md = -d;
+    V wi{dot(md, c.u), dot(md, c.v), dot(md, c.N)};
+    wi.z = std::max(wi.z, 1.19209290e-07f);
+    float sqr;
+    const float radiance = pm_radiance(P, c, B, wi, &sqr);
+    if (h.t * h.t < sqr && stage == 0 && P.pm->fg_secondary > 0) {
+        // gatherSecondary (:1195-1219)
+        const V point = o + h.t * d;
+        return pm_gather_indirect(P, c, B, wi, point, P.pm->fg_secondary, 1, key) +
+               dl_direct_lq(P, B, c, wi, c.target + (10.0f * TOL) * c.N, key);
+    }
+    return radiance;
+}
+
+// gatherIndirect (:1060-1146): n BSDF samples of the reflective diffuse part, each traced as a
+// gather ray; the first stage's samples are per-sample dimensions, the second stage's hashes of
+// the ray's key
+float pm_gather_indirect(const DLPath& P, const Ctx& c, const Bsdf& B, V wi, V origin, int n, int stage,
+                         uint32_t key) {
+    float result = 0;
+    for (int i = 0; i < n; ++i) {
+        float u0, u1, uc;
+        uint32_t gk;
+        if (stage == 0) {
+            u0 = P.smp.get(dl_dim_final_gather(i, 0), true);
+            u1 = P.smp.get(dl_dim_final_gather(i, 1), true);
+            uc = P.smp.get(dl_dim_final_gather(i, 2), true);
+            gk = dl_child_key(key, 0x200u + (uint32_t)i);
+        } else {
+            gk = dl_child_key(key, 0x300u + (uint32_t)i);
+            u0 = P.smp.get(dl_dim_branch(gk, 0x2000u), false);
+            u1 = P.smp.get(dl_dim_branch(gk, 0x2001u), false);
+            uc = P.smp.get(dl_dim_branch(gk, 0x2002u), false);
+        }
+        const Out out = sample(B, wi, u0, u1, uc, C_REFL | C_DIFF);
+        if (!out) continue;
+        const V wd = out.wo.x * c.u + out.wo.y * c.v + out.wo.z * c.N;
+        const float radiance = pm_trace_gather(P, origin, wd, TOL, stage, gk);
+        result += radiance * (out.value * (std::fabs(out.wo.z) / ((float)n * out.pdf)));
+    }
+    return result;
+}
+
 float dl_cast(DLPath& P, V o, V d, float tmin, float tmax, int gen, bool hq, uint32_t key) {
     const Scene& S = *P.S;
     const RenderIn& R = *P.R;
@@ -1090,7 +1227,15 @@ float dl_cast(DLPath& P, V o, V d, float tmin, float tmax, int gen, bool hq, uin
     wi.z = std::max(wi.z, 1.19209290e-07f);
     const V start = c.target + (10.0f * TOL) * c.N;
     const int nlights = (int)S.in.n_lights;
-    if (P.pm && has(B.caps, C_DIFF)) result += pm_estimate(P, 1, c, B, wi) + pm_estimate(P, 0, c, B, wi);
+    if (P.pm && has(B.caps, C_DIFF)) {
+        result += pm_estimate(P, 1, c, B, wi);  // estimateCaustics
+        if (hq && P.pm->fg_rays > 0) {
+            result += pm_gather_indirect(P, c, B, wi, start, P.pm->fg_rays, 0, key);
+        } else {
+            float sqr;
+            result += pm_radiance(P, c, B, wi, &sqr);
+        }
+    }
     if (P.pm && !P.pm->ray_direct) {
         // no traced direct light: the global map holds it
     } else if (hq) {
@@ -1104,21 +1249,8 @@ float dl_cast(DLPath& P, V o, V d, float tmin, float tmax, int gen, bool hq, uin
             };
             result += estimate_light(S, B, c, wi, start, l, nl, nb, P.lam, u);
         }
-    } else if (nlights > 0) {
-        const int n = R.secondary_light_samples > 0 ? R.secondary_light_samples : 1;
-        for (int k = 0; k < n; ++k) {
-            const uint32_t j0 = 16u * (uint32_t)k;
-            const float uc = P.smp.get(dl_dim_branch(key, j0), false);
-            int l = (int)(std::lower_bound(S.light_cdf.begin(), S.light_cdf.end(), uc) - S.light_cdf.begin());
-            l = std::min(l, nlights - 1);
-            const float pc = light_pdf_choice(S, l);
-            if (!(pc > 0)) continue;
-            const int nb = S.in.lights[l].type == L_POINT ? 0 : 1;
-            auto u = [&](int kind, int, int axis) {
-                return P.smp.get(dl_dim_branch(key, j0 + 1u + 2u * (uint32_t)kind + (uint32_t)axis), false);
-            };
-            result += estimate_light(S, B, c, wi, start, l, 1, nb, P.lam, u) / ((float)n * pc);
-        }
+    } else {
+        result += dl_direct_lq(P, B, c, wi, start, key);
     }
     // traced specular and glossy scattering
     const uint32_t glossy = R.trace_glossy < 0 ? 0u : (uint32_t)C_GLOSSY;
@@ -1256,6 +1388,7 @@ uint64_t oracle_mix64(uint64_t z) { return mix64(z); }
 struct PhotonIn {
     int32_t max_ray_generation, ray_traced_direct;
     uint64_t seed, global_target, max_emitted, wave;
+    int32_t final_gather, reserved;
 };
 struct PhotonRec {
     float pos[3], omega[3], power[3];
@@ -1280,7 +1413,8 @@ static void trace_photon_rec(const Scene& S, const PhotonIn& D, const Sampler& s
     const Material& M = S.in.materials[mi];
     if (M.type == M_LAMBERT) {
         const bool to_caustic = caustic;
-        const bool to_global = (gen > 0 || !D.ray_traced_direct) && !caustic;
+        // photon_mapper.cpp:742: with final gathering every diffuse hit is a global photon
+        const bool to_global = ((gen > 0 || !D.ray_traced_direct) && !caustic) || D.final_gather;
         if (to_caustic || to_global) {
             PhotonRec r;
             r.pos[0] = hit.x;
@@ -1295,7 +1429,7 @@ static void trace_photon_rec(const Scene& S, const PhotonIn& D, const Sampler& s
             r.power[1] = sc * c.y;
             r.power[2] = sc * c.z;
             r.path = path;
-            r.tag = (to_caustic ? 2u : 1u) | ((uint32_t)gen << 8);
+            r.tag = (to_caustic ? 2u : 0u) | (to_global ? 1u : 0u) | ((uint32_t)gen << 8);
             out.push_back(r);
         }
     }
@@ -1470,8 +1604,8 @@ int oracle_photon_trace(void* s, const PhotonIn* D, PhotonRec* out, uint64_t cap
         for (const PhotonRec& r : all) {
             if (stored < capacity) out[stored] = r;
             ++stored;
-            if ((r.tag & 3u) == 1u) ++global;
-            else ++caustic;
+            if (r.tag & 1u) ++global;
+            if (r.tag & 2u) ++caustic;
         }
         emitted += n;
     }

@@ -54,7 +54,9 @@ def _run(tracer, w=32, h=32, spp=4, seed=3):
     maps = [R.photon_mapper_map(ctx, m) for m in (0, 1)]
     for m in range(2):
         maps[m]["k"] = tracer.estimationSize("global" if m == 0 else "caustic")
-    c = oracle.RenderScene(flat).render_pm(d, maps, recovery.device_table())
+    irr = R.photon_mapper_irradiance(ctx)
+    st["irradiance"] = irr
+    c = oracle.RenderScene(flat).render_pm(d, maps, recovery.device_table(), irradiance=irr)
     return g, c, st, maps
 
 
@@ -112,6 +114,34 @@ def test_visualised_photon_map():
     assert mg[..., 1].mean() > 1e-3
 
 
+def _fg(rays=8, ratio=0.25, secondary=1, global_size=20_000):
+    t = _pm(global_size=global_size)
+    t.numFinalGatherRays = rays
+    t.ratioPrecomputedIrradiance = ratio
+    t.numSecondaryGatherRays = secondary
+    return t
+
+
+def test_final_gathering_matches_oracle():
+    """numFinalGatherRays > 0: camera (and specular-chain) diffuse vertices gather the indirect
+    light with BSDF-sampled rays evaluated from the precomputed irradiance map, with a secondary
+    gather and low-quality direct light where a gather hit is closer than the estimate's radius."""
+    g, c, st, maps = _run(_fg(), w=24, h=24, spp=2, seed=9)
+    irr = st["irradiance"]
+    # with final gathering every diffuse hit is a global photon, a quarter of them irradiance points
+    assert 20_000 <= st["global"] <= 20_004
+    assert 0.2 * st["global"] < len(irr["position"]) < 0.3 * st["global"]
+    assert (irr["r2"] > 0).mean() > 0.99 and np.allclose(np.linalg.norm(irr["normal"], axis=1), 1, atol=1e-3)
+    mg, _ = _close(g, c)
+    assert mg[..., 1].mean() > 1e-3
+
+
+def test_final_gathering_without_irradiance_map_or_secondary_rays():
+    g, c, st, _ = _run(_fg(rays=6, ratio=0.0, secondary=0), w=20, h=20, spp=2, seed=11)
+    assert len(st["irradiance"]["position"]) == 0
+    _close(g, c)
+
+
 def test_maps_are_kept_for_the_same_scene_and_settings():
     scene, cam = _scene()
     flat = R.flatten(scene)
@@ -147,9 +177,26 @@ def test_photon_mapper_agrees_with_path_tracing_on_average():
     assert abs(ya / yb - 1) < 0.1, (ya, yb)
 
 
+def test_final_gathering_agrees_with_path_tracing_on_average():
+    scene, cam = scenes_render.cornell_box()
+    flat = R.flatten(scene)
+    gs = R.GpuScene(default_context(), flat)
+    t = _fg(rays=16, global_size=100_000)
+    t.maxRayGeneration = 8
+    pm = gs.render(R.render_desc(cam, 40, 40, 4, t, seed=4))
+    pt_tracer = tracers.AdjointPhotonTracer()
+    pt_tracer.maxRayGeneration = 8
+    pt = gs.render(R.render_desc(cam, 40, 40, 256, pt_tracer, seed=4))
+    a, _ = R.resolve(pm)
+    b, _ = R.resolve(pt)
+    lit = (a[..., 1] < 2.0) & (b[..., 1] < 2.0)
+    ya, yb = a[..., 1][lit].mean(), b[..., 1][lit].mean()
+    assert abs(ya / yb - 1) < 0.1, (ya, yb)
+
+
 def test_unsupported_settings_fail_loudly():
     t = _pm()
-    t.numFinalGatherRays = 16
+    t.causticsQuality = 2.0
     scene, cam = _scene()
     with pytest.raises(NotImplementedError):
         R.render_desc(cam, 8, 8, 1, t)

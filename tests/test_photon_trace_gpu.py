@@ -47,7 +47,7 @@ def test_trace_build_gather_pipeline():
     d = photons.photon_desc(50_000, max_emitted=2_000_000, wave=65536, ray_traced_direct=False)
     g, gc = photons.trace_photons(gs, d, capacity=500_000)
     assert gc["global"] >= 50_000
-    glob = (g["tag"] & 3) == photons.GLOBAL
+    glob = (g["tag"] & photons.GLOBAL) != 0
     pos = g["position"][glob].contiguous()
     r = photons.automatic_radius(g["power"][glob].cpu().numpy(), gc["emitted"], 64)
     m = photons.PhotonMap(ctx, device_ptr=pos.data_ptr(), n=pos.shape[0], r_max=r)
