@@ -170,7 +170,23 @@ typedef struct liar_material {
     int32_t samples;   /* DirectLighting: reflection (and transmission) samples per vertex, the shader's
                           numReflectionSamples (conductor.cpp:118, dielectric.cpp:134-144,
                           cook_torrance.cpp:182); 0 = 1 */
+    int32_t tex[4];    /* texture of parameter spec[k] (index into the scene's textures), -1 = the constant
+                          spectrum spec[k] */
 } liar_material;
+
+/* Textures of spectral material parameters (src/liar/textures/): a tree of nodes looked up at a
+ * hit's (u, v) coordinates.
+ *   CONSTANT      spectrum                                    (textures/constant.cpp)
+ *   CHECKER       a where the fractional (u, v) lie on the same side of split p[0], p[1], else b
+ *                 (CheckerBoard, checker_board.cpp:154-190 with anti-aliasing "none")
+ *   GRID          a on the lines of half thickness p[0] (u, and v from below) and p[1] (v from
+ *                 above), else b (GridBoard, grid_board.cpp:60-67)
+ *   UV_TRANSFORM  child a at (p[0] u + p[1] v + p[2], p[3] u + p[4] v + p[5]) (TransformationUv) */
+enum liar_texture_type { LIAR_TEX_CONSTANT = 0, LIAR_TEX_CHECKER = 1, LIAR_TEX_GRID = 2, LIAR_TEX_UV_TRANSFORM = 3 };
+typedef struct liar_texture {
+    int32_t type, a, b, spectrum;
+    float p[6];
+} liar_texture;
 
 /* Lights (src/liar/scenery/light_*.cpp). AREA_PARALLELOGRAM: pos = support, u/v = sizes
  * (light_area.cpp + parallelogram.cpp); AREA_MESH: triangles [first_tri, first_tri + n_tris) of
@@ -200,6 +216,9 @@ typedef struct liar_scene_desc {
     const liar_light* lights; size_t n_lights;
     const float* observer; size_t n_observer;            /* n x 4: wavelength (m), xbar, ybar, zbar */
     float scene_radius;                                  /* bounding sphere radius (sky distance) */
+    const liar_texture* textures; size_t n_textures;     /* optional */
+    const float* triangle_uvs;                           /* optional, n_triangles x 6: (u, v) per corner;
+                                                            NULL: the barycentric coordinates of the hit */
 } liar_scene_desc;
 
 /* PerspectiveCamera (src/liar/cameras/perspective_camera.cpp:406-434): direction/right/down are

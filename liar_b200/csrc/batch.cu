@@ -327,7 +327,8 @@ __global__ void __launch_bounds__(128) k_b_shade(BParams P, BState<H> st, BQueue
                     if (ok) {
                         // the BSDF value at every hero wavelength along the chosen direction
                         const bool dispersive = (M.type == LIAR_MAT_DIELECTRIC || M.type == LIAR_MAT_WALTER) &&
-                                                ((M.spec[0] >= 0 && S.specs[M.spec[0]].type != LIAR_SPEC_CONSTANT) ||
+                                                (M.tex[0] >= 0 || M.tex[1] >= 0 ||
+                                                 (M.spec[0] >= 0 && S.specs[M.spec[0]].type != LIAR_SPEC_CONSTANT) ||
                                                  (M.spec[1] >= 0 && S.specs[M.spec[1]].type != LIAR_SPEC_CONSTANT));
                         float val[H];
                         for (int k = 0; k < H; ++k) {

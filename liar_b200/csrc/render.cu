@@ -21,6 +21,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <new>
 #include <vector>
 
@@ -411,7 +412,41 @@ extern "C" int liar_gpu_scene_upload(liar_gpu_ctx* ctx, const liar_scene_desc* d
         for (int c = 0; c < 4; ++c)
             if (!spec_ok(m.spec[c])) return ctx_fail(ctx, LIAR_ERR_INVALID, "material %zu: spectrum out of range", k);
         if (!spec_ok(m.emission)) return ctx_fail(ctx, LIAR_ERR_INVALID, "material %zu: emission out of range", k);
+        for (int c = 0; c < 4; ++c)
+            if (m.tex[c] < -1 || (m.tex[c] >= 0 && (size_t)m.tex[c] >= D.n_textures))
+                return ctx_fail(ctx, LIAR_ERR_INVALID, "material %zu: texture out of range", k);
     }
+    if (D.n_textures > 0 && !D.textures) return ctx_fail(ctx, LIAR_ERR_INVALID, "textures missing");
+    if (D.n_textures > (1u << 20)) return ctx_fail(ctx, LIAR_ERR_INVALID, "too many textures (limit 2^20)");
+    // every texture node must end at constants within 32 nodes (the lookup's bound), without cycles
+    std::vector<int> tex_depth(D.n_textures, 0);  // 0: not visited, -1: being visited, else its depth
+    const char* tex_err = nullptr;
+    int tex_bad = -1;
+    std::function<int(int, int)> depth_of = [&](int t, int level) -> int {
+        if (t < 0 || (size_t)t >= D.n_textures) return tex_err = "child out of range", -1;
+        if (tex_depth[t] > 0) return tex_depth[t];
+        if (tex_depth[t] < 0) return tex_err = "cycle", tex_bad = t, -1;
+        if (level > 32) return tex_err = "more than 32 nested textures", tex_bad = t, -1;
+        const liar_texture& T = D.textures[t];
+        int d = 0;
+        if (T.type == LIAR_TEX_CONSTANT) {
+            if (T.spectrum < 0 || T.spectrum >= (int32_t)D.n_spectra) return tex_err = "spectrum out of range", tex_bad = t, -1;
+            d = 1;
+        } else if (T.type == LIAR_TEX_CHECKER || T.type == LIAR_TEX_GRID || T.type == LIAR_TEX_UV_TRANSFORM) {
+            tex_depth[t] = -1;
+            const int da = depth_of(T.a, level + 1);
+            if (da < 0) return -1;
+            int db = 0;
+            if (T.type != LIAR_TEX_UV_TRANSFORM && (db = depth_of(T.b, level + 1)) < 0) return -1;
+            d = std::max(da, db) + 1;
+        } else {
+            return tex_err = "bad type", tex_bad = t, -1;
+        }
+        if (d > 32) return tex_err = "more than 32 nested textures", tex_bad = t, -1;
+        return tex_depth[t] = d;
+    };
+    for (size_t k = 0; k < D.n_textures; ++k)
+        if (depth_of((int)k, 1) < 0) return ctx_fail(ctx, LIAR_ERR_INVALID, "texture %d: %s", tex_bad < 0 ? (int)k : tex_bad, tex_err);
     std::vector<float> spec_max(D.n_spectra, 0.0f);
     for (size_t k = 0; k < D.n_spectra; ++k) {
         const liar_spectrum& s = D.spectra[k];
@@ -524,6 +559,8 @@ extern "C" int liar_gpu_scene_upload(liar_gpu_ctx* ctx, const liar_scene_desc* d
         rc = upload(ctx, s, D.normals, 3 * D.n_normals, &d.normals, "normals");
         if (!rc) rc = upload(ctx, s, D.triangle_normals, 3 * D.n_triangles, &d.tri_nrm, "triangle normals");
     }
+    if (!rc && D.triangle_uvs) rc = upload(ctx, s, D.triangle_uvs, 6 * D.n_triangles, &d.tri_uv, "triangle uvs");
+    if (!rc) rc = upload(ctx, s, D.textures, D.n_textures, &d.texs, "textures");
     if (!rc) rc = upload(ctx, s, D.object_material, D.n_objects, &d.obj_mat, "object materials");
     if (!rc) rc = upload(ctx, s, D.object_light, D.n_objects, &d.obj_light, "object lights");
     if (!rc) rc = upload(ctx, s, D.materials, D.n_materials, &d.mats, "materials");
@@ -547,6 +584,7 @@ extern "C" int liar_gpu_scene_upload(liar_gpu_ctx* ctx, const liar_scene_desc* d
     d.nodes = mesh_nodes(s->mesh);
     d.qtris = mesh_tris(s->mesh);
     d.n_lights = (int)D.n_lights;
+    d.n_tex = (int)D.n_textures;
     d.n_obs = (int)no;
     d.sky_light = sky;
     // LightSky::doSetSceneBound: intersections with the sky lie 1000 scene radii away

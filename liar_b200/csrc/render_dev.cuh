@@ -85,6 +85,9 @@ struct DScene {
     float sky_distance;
     int sky_light;
     uint32_t stack_needed;
+    const liar_texture* texs;    // optional texture nodes
+    int n_tex;
+    const float* tri_uv;         // optional, per triangle 3 x (u, v)
 };
 
 // ---- spectra
@@ -641,6 +644,7 @@ struct HitContext {
     float3 u, v;    // shading frame tangents
     bool leaving;   // solid event from the unflipped geometric normal
     int obj, light, mat;
+    float uv_u, uv_v;  // surface coordinates: the triangle corners' (u, v) at the barycentrics, or those
 };
 
 __device__ inline HitContext hit_context(const DScene& S, float3 o, float3 d, uint32_t prim) {
@@ -658,6 +662,15 @@ __device__ inline HitContext hit_context(const DScene& S, float3 o, float3 d, ui
     if (!tri_intersect_exact(o.x, o.y, o.z, d.x, d.y, d.z, a.x, a.y, a.z, e1.x, e1.y, e1.z, e2.x, e2.y, e2.z, tt, bu, bv))
         bu = bv = 0.0f;
     H.target = a + bu * e1 + bv * e2;
+    if (S.tri_uv) {
+        const float* t = S.tri_uv + 6 * (size_t)prim;
+        const float w0 = 1.0f - bu - bv;
+        H.uv_u = w0 * t[0] + bu * t[2] + bv * t[4];
+        H.uv_v = w0 * t[1] + bu * t[3] + bv * t[5];
+    } else {
+        H.uv_u = bu;
+        H.uv_v = bv;
+    }
     const float3 ng0 = normal(cross(e1, e2));
     float3 ns = ng0;
     if (S.tri_nrm) {
@@ -693,6 +706,45 @@ __device__ inline HitContext hit_context(const DScene& S, float3 o, float3 d, ui
     return H;
 }
 
+// Texture::lookUp of a tree of uv textures: the transforms move (u, v), the boards pick a child
+// (without anti-aliasing a board always picks one), the leaf is a spectrum
+__device__ inline float texture_eval(const DScene& S, int t, float u, float v, float lam, bool reflectant) {
+    for (int depth = 0; depth < 32 && t >= 0 && t < S.n_tex; ++depth) {
+        const liar_texture T = S.texs[t];
+        switch (T.type) {
+            case LIAR_TEX_CHECKER: {
+                const float fu = u - floorf(u), fv = v - floorf(v);
+                t = ((fu < T.p[0]) == (fv < T.p[1])) ? T.a : T.b;
+                break;
+            }
+            case LIAR_TEX_GRID: {
+                const float fu = u - floorf(u), fv = v - floorf(v);
+                const bool on = fu < T.p[0] || fv < T.p[0] || fu > 1.0f - T.p[0] || fv > 1.0f - T.p[1];
+                t = on ? T.a : T.b;
+                break;
+            }
+            case LIAR_TEX_UV_TRANSFORM: {
+                const float nu = T.p[0] * u + T.p[1] * v + T.p[2];
+                const float nv = T.p[3] * u + T.p[4] * v + T.p[5];
+                u = nu;
+                v = nv;
+                t = T.a;
+                break;
+            }
+            default:
+                return spec_eval(S, T.spectrum, lam, reflectant);
+        }
+    }
+    return 0.0f;
+}
+
+// a material parameter: its texture at the hit, else its constant spectrum
+__device__ __forceinline__ float param_eval(const DScene& S, const liar_material& M, int k, const HitContext& H,
+                                            float lam, bool reflectant) {
+    return M.tex[k] >= 0 ? texture_eval(S, M.tex[k], H.uv_u, H.uv_v, lam, reflectant)
+                         : spec_eval(S, M.spec[k], lam, reflectant);
+}
+
 // Shader::bsdf at one wavelength
 __device__ inline Bsdf make_bsdf(const DScene& S, const liar_material& M, const HitContext& H, float lam) {
     Bsdf B;
@@ -706,28 +758,28 @@ __device__ inline Bsdf make_bsdf(const DScene& S, const liar_material& M, const 
     switch (M.type) {
         case LIAR_MAT_LAMBERT:
             B.caps = CAP_REFL | CAP_DIFF;
-            B.r = spec_eval(S, M.spec[0], lam, true);
+            B.r = param_eval(S, M, 0, H, lam, true);
             break;
         case LIAR_MAT_CONDUCTOR:
         case LIAR_MAT_COOK_TORRANCE:
             B.caps = M.type == LIAR_MAT_CONDUCTOR ? (CAP_REFL | CAP_SPEC) : (CAP_REFL | CAP_GLOSSY);
-            B.eta = fmaxf(spec_eval(S, M.spec[0], lam, false), 1e-9f);
-            B.kappa = fmaxf(spec_eval(S, M.spec[1], lam, false), 1e-9f);
-            B.r = spec_eval(S, M.spec[2], lam, true);
+            B.eta = fmaxf(param_eval(S, M, 0, H, lam, false), 1e-9f);
+            B.kappa = fmaxf(param_eval(S, M, 1, H, lam, false), 1e-9f);
+            B.r = param_eval(S, M, 2, H, lam, true);
             break;
         case LIAR_MAT_DIELECTRIC: {
             B.caps = CAP_REFL | CAP_TRANS | CAP_SPEC;
-            const float ior1 = fmaxf(spec_eval(S, M.spec[1], lam, false), 1e-9f);
-            const float ior2 = fmaxf(spec_eval(S, M.spec[0], lam, false), 1e-9f);
+            const float ior1 = fmaxf(param_eval(S, M, 1, H, lam, false), 1e-9f);
+            const float ior2 = fmaxf(param_eval(S, M, 0, H, lam, false), 1e-9f);
             B.ior = H.leaving ? ior2 / ior1 : ior1 / ior2;
-            B.r = spec_eval(S, M.spec[2], lam, true);
-            B.t = spec_eval(S, M.spec[3], lam, true);
+            B.r = param_eval(S, M, 2, H, lam, true);
+            B.t = param_eval(S, M, 3, H, lam, true);
             break;
         }
         case LIAR_MAT_WALTER: {
             B.caps = CAP_TRANS | CAP_GLOSSY;  // as constructed by Walter::Bsdf (walter.cpp:247)
-            float ei = fmaxf(spec_eval(S, M.spec[1], lam, false), 1e-9f);
-            float et = fmaxf(spec_eval(S, M.spec[0], lam, false), 1e-9f);
+            float ei = fmaxf(param_eval(S, M, 1, H, lam, false), 1e-9f);
+            float et = fmaxf(param_eval(S, M, 0, H, lam, false), 1e-9f);
             if (H.leaving) {
                 const float tmp = ei;
                 ei = et;
@@ -735,13 +787,13 @@ __device__ inline Bsdf make_bsdf(const DScene& S, const liar_material& M, const 
             }
             B.eta_i = ei;
             B.eta_t = et;
-            B.r = spec_eval(S, M.spec[2], lam, true);
-            B.t = spec_eval(S, M.spec[3], lam, true);
+            B.r = param_eval(S, M, 2, H, lam, true);
+            B.t = param_eval(S, M, 3, H, lam, true);
             break;
         }
         case LIAR_MAT_MIRROR:
             B.caps = CAP_REFL | CAP_SPEC;
-            B.r = spec_eval(S, M.spec[0], lam, true);
+            B.r = param_eval(S, M, 0, H, lam, true);
             break;
         default:
             B.caps = 0;

@@ -15,6 +15,7 @@ import numpy as np
 
 from . import _native as N
 from . import _tables, scenery, shaders, spectra
+from . import textures as tx
 from .textures import as_scalar, as_spectrum
 
 # ---- C structs (mirrors of include/liar_gpu.h)
@@ -26,7 +27,11 @@ class CSpectrum(C.Structure):
 
 class CMaterial(C.Structure):
     _fields_ = [("type", C.c_int32), ("mdf", C.c_int32), ("spec", C.c_int32 * 4), ("emission", C.c_int32),
-                ("rough_u", C.c_float), ("rough_v", C.c_float), ("samples", C.c_int32)]
+                ("rough_u", C.c_float), ("rough_v", C.c_float), ("samples", C.c_int32), ("tex", C.c_int32 * 4)]
+
+
+class CTexture(C.Structure):
+    _fields_ = [("type", C.c_int32), ("a", C.c_int32), ("b", C.c_int32), ("spectrum", C.c_int32), ("p", C.c_float * 6)]
 
 
 class CLight(C.Structure):
@@ -45,7 +50,8 @@ class CSceneDesc(C.Structure):
                 ("object_material", _P), ("object_light", _P), ("n_objects", _S),
                 ("materials", _P), ("n_materials", _S), ("spectra", _P), ("n_spectra", _S),
                 ("spectrum_pool", _P), ("pool_size", _S), ("lights", _P), ("n_lights", _S),
-                ("observer", _P), ("n_observer", _S), ("scene_radius", C.c_float)]
+                ("observer", _P), ("n_observer", _S), ("scene_radius", C.c_float),
+                ("textures", _P), ("n_textures", _S), ("triangle_uvs", _P)]
 
 
 class CCamera(C.Structure):
@@ -75,6 +81,7 @@ class CRenderDesc(C.Structure):
 FILTER_BOX, FILTER_TRIANGLE, FILTER_MITCHELL = 0, 1, 2
 
 
+TEX_CONSTANT, TEX_CHECKER, TEX_GRID, TEX_UV_TRANSFORM = range(4)
 SPEC_CONSTANT, SPEC_SAMPLED, SPEC_BLACKBODY, SPEC_CAUCHY = 0, 1, 2, 3
 MAT_NONE, MAT_LAMBERT, MAT_CONDUCTOR, MAT_COOK_TORRANCE, MAT_DIELECTRIC, MAT_WALTER, MAT_MIRROR = range(7)
 LIGHT_PARA, LIGHT_MESH, LIGHT_POINT, LIGHT_SKY = 0, 1, 2, 3
@@ -95,6 +102,8 @@ class FlatScene:
     lights: C.Array
     observer: np.ndarray
     scene_radius: float
+    textures: C.Array | None = None
+    triangle_uvs: np.ndarray | None = None  # n_triangles x 3 x 2, when a texture needs them
     keep: list = field(default_factory=list)
 
     def desc(self) -> CSceneDesc:
@@ -122,6 +131,11 @@ class FlatScene:
         d.observer = self.observer.ctypes.data
         d.n_observer = self.observer.shape[0]
         d.scene_radius = self.scene_radius
+        if self.textures is not None and len(self.textures):
+            d.textures = C.addressof(self.textures)
+            d.n_textures = len(self.textures)
+        if self.triangle_uvs is not None:
+            d.triangle_uvs = self.triangle_uvs.ctypes.data
         return d
 
 
@@ -134,6 +148,8 @@ class _Builder:
         self.materials, self.mat_ids = [], {}
         self.spectra, self.spec_ids, self.pool = [], {}, []
         self.lights = []
+        self.textures, self.tex_ids = [], {}
+        self.tri_uvs = []  # per object: n x 3 x 2 corner uvs, or None for the barycentric ones
         self.M = None  # current local-to-world affine matrix (None: identity)
 
     # -- transformations (scenery/transformation.cpp, translation.cpp)
@@ -185,6 +201,44 @@ class _Builder:
         self.spec_ids[key] = (idx, s)
         return idx
 
+    # -- textures (src/liar/textures/): a tree of nodes per textured material parameter
+    def texture(self, t) -> int:
+        key = id(t)
+        if key in self.tex_ids:
+            return self.tex_ids[key][0]
+        rec = CTexture()
+        rec.a = rec.b = rec.spectrum = -1
+        if isinstance(t, tx.CheckerBoard):
+            tx.warn_point_lookup(t)
+            rec.type = TEX_CHECKER
+            rec.p[0], rec.p[1] = t.split
+        elif isinstance(t, tx.GridBoard):
+            rec.type = TEX_GRID
+            rec.p[0], rec.p[1] = t.thickness[0] / 2, t.thickness[1] / 2  # GridBoard's halfThickness
+        elif isinstance(t, tx.TransformationUv):
+            rec.type = TEX_UV_TRANSFORM
+            m = t.transformation
+            rec.p[:] = [float(m[0, 0]), float(m[0, 1]), float(m[0, 2]), float(m[1, 0]), float(m[1, 1]), float(m[1, 2])]
+        else:
+            rec.type = TEX_CONSTANT
+            rec.spectrum = self.spectrum(t)
+        idx = len(self.textures)
+        self.textures.append(rec)
+        self.tex_ids[key] = (idx, t)
+        if isinstance(t, tx.BinaryOperator):
+            self.textures[idx].a = self.texture(t.textureA)
+            self.textures[idx].b = self.texture(t.textureB)
+        elif isinstance(t, tx.UnaryOperator):
+            self.textures[idx].a = self.texture(t.texture)
+        return idx
+
+    def param(self, m, k: int, value):
+        """Material parameter k: a uv texture as a texture tree, else a constant spectrum."""
+        if tx.is_uv_texture(value):
+            m.tex[k] = self.texture(value)
+        else:
+            m.spec[k] = self.spectrum(value)
+
     # -- shaders
     def material(self, shader) -> int:
         if shader is None:
@@ -194,6 +248,7 @@ class _Builder:
             return self.mat_ids[key][0]
         m = CMaterial()
         m.spec[:] = [-1, -1, -1, -1]
+        m.tex[:] = [-1, -1, -1, -1]
         m.emission = -1
         m.samples = 1
         bsdf = shader
@@ -212,15 +267,15 @@ class _Builder:
             m.type = MAT_NONE
         elif isinstance(bsdf, shaders.Lambert):
             m.type = MAT_LAMBERT
-            m.spec[0] = self.spectrum(bsdf.diffuse)
+            self.param(m, 0, bsdf.diffuse)
         elif isinstance(bsdf, shaders.Mirror):
             m.type = MAT_MIRROR
-            m.spec[0] = self.spectrum(bsdf.reflectance)
+            self.param(m, 0, bsdf.reflectance)
         elif isinstance(bsdf, (shaders.Conductor, shaders.CookTorrance)):
             m.type = MAT_CONDUCTOR if isinstance(bsdf, shaders.Conductor) else MAT_COOK_TORRANCE
-            m.spec[0] = self.spectrum(bsdf.refractionIndex)
-            m.spec[1] = self.spectrum(bsdf.absorptionCoefficient)
-            m.spec[2] = self.spectrum(bsdf.reflectance)
+            self.param(m, 0, bsdf.refractionIndex)
+            self.param(m, 1, bsdf.absorptionCoefficient)
+            self.param(m, 2, bsdf.reflectance)
             if isinstance(bsdf, shaders.CookTorrance):
                 m.samples = int(getattr(bsdf, "numberOfSamples", 1))
                 m.rough_u = as_scalar(bsdf.roughnessU)
@@ -228,10 +283,10 @@ class _Builder:
                 m.mdf = bsdf.mdf.kind
         elif isinstance(bsdf, shaders.Dielectric):
             m.type = MAT_WALTER if isinstance(bsdf, shaders.Walter) else MAT_DIELECTRIC
-            m.spec[0] = self.spectrum(bsdf.innerRefractionIndex)
-            m.spec[1] = self.spectrum(bsdf.outerRefractionIndex)
-            m.spec[2] = self.spectrum(bsdf.reflectance)
-            m.spec[3] = self.spectrum(bsdf.transmittance)
+            self.param(m, 0, bsdf.innerRefractionIndex)
+            self.param(m, 1, bsdf.outerRefractionIndex)
+            self.param(m, 2, bsdf.reflectance)
+            self.param(m, 3, bsdf.transmittance)
             if isinstance(bsdf, shaders.Walter):
                 m.samples = int(getattr(bsdf, "numberOfSamples", 1))
                 m.rough_u = as_scalar(bsdf.roughnessU)
@@ -247,6 +302,7 @@ class _Builder:
     # -- geometry
     def geometry(self, obj, shader, light: int) -> tuple[int, int]:
         v, t, n, tn = obj.triangles()
+        uv = obj.corner_uvs() if hasattr(obj, "corner_uvs") else None
         if self.M is not None:
             v = self.point(v).astype(np.float32)
             if n is not None:
@@ -256,6 +312,8 @@ class _Builder:
                 # a mirroring transformation: keep the geometric normal the transformed local one,
                 # as the reference transforms the local context's normal
                 t = np.asarray(t)[:, [0, 2, 1]]
+                if uv is not None:
+                    uv = np.asarray(uv)[:, [0, 2, 1]]
                 if tn is not None:
                     tn = np.asarray(tn)[:, [0, 2, 1]]
         obj_index = len(self.obj_mat)
@@ -265,6 +323,7 @@ class _Builder:
         self.verts.append(np.asarray(v, dtype=np.float32))
         self.tris.append(np.asarray(t, dtype=np.int64) + self.n_verts)
         self.tri_obj.append(np.full(len(t), obj_index, dtype=np.int32))
+        self.tri_uvs.append(None if uv is None else np.asarray(uv, dtype=np.float32).reshape(len(t), 3, 2))
         if n is not None and tn is not None:
             self.has_normals = True
             self.norms.append(np.asarray(n, dtype=np.float32))
@@ -358,7 +417,19 @@ class _Builder:
             lights=(CLight * len(self.lights))(*self.lights),
             observer=np.ascontiguousarray(_tables.observer(), dtype=np.float32),
             scene_radius=radius,
+            textures=(CTexture * len(self.textures))(*self.textures) if self.textures else None,
+            triangle_uvs=self.triangle_uvs(),
         )
+
+    def triangle_uvs(self) -> np.ndarray | None:
+        """Corner uvs of every triangle when a texture reads them and an object has its own; the
+        others keep the barycentric ones (corners (0, 0), (1, 0), (0, 1))."""
+        if not self.textures or all(u is None for u in self.tri_uvs):
+            return None
+        bary = np.array([[0, 0], [1, 0], [0, 1]], dtype=np.float32)
+        parts = [u if u is not None else np.broadcast_to(bary, (len(o), 3, 2))
+                 for u, o in zip(self.tri_uvs, self.tri_obj)]
+        return np.ascontiguousarray(np.concatenate(parts).reshape(-1, 6), dtype=np.float32)
 
     def spec_ids_lum(self, idx: int) -> float:
         for i, s in self.spec_ids.values():

@@ -53,6 +53,10 @@ class Parallelogram(SceneObject):
         verts = np.stack([s, s + u, s + u + v, s + v]).astype(np.float32)
         return verts, np.array([[0, 1, 2], [0, 2, 3]], dtype=np.uint32), None, None
 
+    def corner_uvs(self):
+        """The parametric (u, v) of support + u sizeU + v sizeV at the corners (parallelogram.cpp:77-89)."""
+        return np.array([[[0, 0], [1, 0], [1, 1]], [[0, 0], [1, 1], [0, 1]]], dtype=np.float32)
+
     @property
     def area(self) -> float:
         return float(np.linalg.norm(np.cross(self.sizeU, self.sizeV)))
@@ -80,27 +84,46 @@ class TriangleMesh(SceneObject):
         if isinstance(tri, np.ndarray) and tri.ndim == 2:
             self._vi = tri.astype(np.uint32)
             self._ni = None
+            self._ti = None
         else:
-            vi, ni = [], []
-            has_n = False
+            vi, ni, ti = [], [], []
+            has_n = has_t = False
             for t in tri:
-                row_v, row_n = [], []
+                row_v, row_n, row_t = [], [], []
                 for c in t:
                     if isinstance(c, (tuple, list)):
                         row_v.append(int(c[0]))
                         n = int(c[1]) if len(c) > 1 and c[1] is not None else -1
+                        u = int(c[2]) if len(c) > 2 and c[2] is not None else -1
                         row_n.append(n)
+                        row_t.append(u)
                         has_n |= n >= 0
+                        has_t |= u >= 0
                     else:
                         row_v.append(int(c))
                         row_n.append(-1)
+                        row_t.append(-1)
                 vi.append(row_v)
                 ni.append(row_n)
+                ti.append(row_t)
             self._vi = np.asarray(vi, dtype=np.uint32).reshape(-1, 3)
             self._ni = np.asarray(ni, dtype=np.int32).reshape(-1, 3) if has_n else None
+            self._ti = np.asarray(ti, dtype=np.int32).reshape(-1, 3) if has_t else None
 
     def triangles(self):
         return self.vertices, self._vi, self.normals, self._ni
+
+    def corner_uvs(self):
+        """The corners' uvs of triangles that index them; a triangle without has the barycentric
+        coordinates of the hit as its uv (corners (0, 0), (1, 0), (0, 1))."""
+        if self._ti is None or len(self.uvs) == 0:
+            return None
+        table = np.asarray(self.uvs, dtype=np.float32).reshape(-1, 2)
+        if (self._ti >= len(table)).any():
+            raise IndexError("TriangleMesh: uv index out of range")
+        bary = np.array([[0, 0], [1, 0], [0, 1]], dtype=np.float32)
+        full = (self._ti >= 0).all(axis=1, keepdims=True)[..., None]
+        return np.where(full, table[np.maximum(self._ti, 0)], bary[None]).astype(np.float32)
 
 
 class Sphere(SceneObject):
@@ -119,6 +142,25 @@ class Sphere(SceneObject):
             v, f = subdivide(v, f)
         verts = (v * self.radius + np.asarray(self.center)).astype(np.float32)
         return verts, f.astype(np.uint32), v.astype(np.float32), f.astype(np.int32)
+
+    def corner_uvs(self):
+        """(phi / 2 pi, theta / pi) of the corners' normals (sphere.cpp:130-152), phi unwrapped per
+        triangle across the seam and taken from the other corners at the poles."""
+        from .scenes import icosahedron, subdivide
+        v, f = icosahedron()
+        for _ in range(self.subdivisions):
+            v, f = subdivide(v, f)
+        n = v / np.linalg.norm(v, axis=1, keepdims=True)
+        u = np.arctan2(n[:, 1], n[:, 0]) / (2 * np.pi)
+        w = np.arccos(np.clip(n[:, 2], -1.0, 1.0)) / np.pi
+        cu, cw = u[f], w[f]                                   # n_tris x 3
+        cu = np.where(cu < cu.max(axis=1, keepdims=True) - 0.5, cu + 1.0, cu)
+        pole = np.hypot(n[:, 0], n[:, 1])[f] < 1e-6
+        if pole.any():
+            other = np.where(pole, np.nan, cu)
+            fill = np.nanmean(other, axis=1, keepdims=True)
+            cu = np.where(pole, fill, cu)
+        return np.stack([cu, cw], axis=-1).astype(np.float32)
 
 
 class Box(SceneObject):
@@ -158,6 +200,23 @@ class Box(SceneObject):
         for a, b, c, d in quads:
             tris += [(a, b, c), (a, c, d)]
         return corners, np.asarray(tris, dtype=np.uint32), None, None
+
+    def corner_uvs(self):
+        """Box::doLocalContext (box.cpp:216-250): on the face of axis k, u and v run over the
+        axes k + 1 and k + 2 from the minimum, v mirrored on the faces that look down the axis."""
+        corners, tris, _, _ = self.triangles()
+        lo, size = np.asarray(self.min, dtype=np.float64), np.asarray(self.max, dtype=np.float64) - np.asarray(self.min)
+        out = np.zeros((len(tris), 3, 2), dtype=np.float32)
+        for k, t in enumerate(tris):
+            axis = k // 4
+            positive = (k // 2) % 2 == 1
+            i, j = (axis + 1) % 3, (axis + 2) % 3
+            for c in range(3):
+                p = corners[t[c]].astype(np.float64)
+                uu = (p[i] - lo[i]) / size[i] if size[i] else 0.0
+                vv = (p[j] - lo[j]) / size[j] if size[j] else 0.0
+                out[k, c] = (uu, vv if positive else 1.0 - vv)
+        return out
 
 
 def as_matrix(m) -> np.ndarray:

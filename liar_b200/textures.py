@@ -1,6 +1,16 @@
-"""Textures of the scene API (``liar.textures``). Only constant textures are on the hot path
-(src/liar/textures/constant.cpp); a Constant wraps a spectrum or a number."""
+"""Textures of the scene API (``liar.textures``, src/liar/textures/).
+
+On the GPU path: Constant (textures/constant.cpp), a spectrum or a number; and the uv textures
+CheckerBoard (checker_board.cpp), GridBoard (grid_board.cpp) and TransformationUv
+(transformation_uv.cpp), which pick or move between other textures by the hit's (u, v)
+coordinates. A material parameter that is a uv texture becomes a tree of liar_texture nodes
+(include/liar_gpu.h) that the kernels walk at every hit; emission and roughness slots take
+constant textures only."""
 from __future__ import annotations
+
+import warnings
+
+import numpy as np
 
 from .spectra import Spectrum
 
@@ -18,15 +28,151 @@ class Constant(Texture):
         return self.value
 
 
+def _texture(x) -> Texture:
+    """A texture slot's value as a texture: textures as they are, spectra and numbers as Constant."""
+    if isinstance(x, Texture):
+        return x
+    if isinstance(x, (Spectrum, int, float)):
+        return Constant(x)
+    raise TypeError(f"expected a texture, a spectrum or a number, got {type(x).__name__}")
+
+
+class BinaryOperator(Texture):
+    """Base of the textures that mix two inputs (binary_operator.cpp): textureA, textureB."""
+
+    def __init__(self, a, b):
+        self.textureA = _texture(a)
+        self.textureB = _texture(b)
+
+
+class UnaryOperator(Texture):
+    """Base of the textures with one input (unary_operator.cpp): texture."""
+
+    def __init__(self, texture):
+        self.texture = _texture(texture)
+
+
+class CheckerBoard(BinaryOperator):
+    """CheckerBoard(a, b): a where the fractional u and v lie on the same side of ``split``
+    (default (0.5, 0.5)), else b (checker_board.cpp:113-157).
+
+    antiAliasing "none" is the reference's point lookup. "bilinear" (the reference's default)
+    averages the board over the pixel footprint that ray differentials give; the GPU path carries
+    no ray differentials, so it renders "bilinear" as "none", the footprint's zero-size limit: the
+    pixel filter then does the averaging over the camera samples."""
+
+    AA_NONE = "none"
+    AA_BILINEAR = "bilinear"
+    _default_aa = "bilinear"
+    _warned = False
+
+    def __init__(self, a, b):
+        super().__init__(a, b)
+        self.split = (0.5, 0.5)
+        self.antiAliasing = CheckerBoard._default_aa
+
+    @property
+    def split(self):
+        return self._split
+
+    @split.setter
+    def split(self, value):
+        u, v = value
+        self._split = (float(u), float(v))
+
+    @property
+    def antiAliasing(self) -> str:
+        return self._aa
+
+    @antiAliasing.setter
+    def antiAliasing(self, mode: str):
+        mode = str(mode).lower()
+        if mode not in (self.AA_NONE, self.AA_BILINEAR):
+            raise KeyError(f"antiAliasing must be 'none' or 'bilinear', not {mode!r}")
+        self._aa = mode
+
+    @staticmethod
+    def setDefaultAntiAliasing(mode: str):
+        mode = str(mode).lower()
+        if mode not in (CheckerBoard.AA_NONE, CheckerBoard.AA_BILINEAR):
+            raise KeyError(f"antiAliasing must be 'none' or 'bilinear', not {mode!r}")
+        CheckerBoard._default_aa = mode
+
+
+class GridBoard(BinaryOperator):
+    """GridBoard(a, b): a on grid lines of ``thickness`` (default (0.1, 0.1)) around the integer u
+    and v, else b. As in grid_board.cpp:80-87, the first thickness bounds u at both sides and v
+    from below, the second v from above."""
+
+    def __init__(self, a, b):
+        super().__init__(a, b)
+        self.thickness = (0.1, 0.1)
+
+    @property
+    def thickness(self):
+        return self._thickness
+
+    @thickness.setter
+    def thickness(self, value):
+        u, v = value
+        self._thickness = (float(u), float(v))
+
+
+def as_matrix2d(m) -> np.ndarray:
+    """A 3 x 3 float64 matrix of a 2D affine transformation: 3 x 3 or 2 x 3 (row-major, the last
+    column the translation), 9 or 6 numbers, or an object with a `matrix` attribute."""
+    if hasattr(m, "matrix"):
+        m = m.matrix
+    a = np.asarray(m, dtype=np.float64)
+    if a.size == 9:
+        a = a.reshape(3, 3)
+    elif a.size == 6:
+        a = np.vstack([a.reshape(2, 3), [0.0, 0.0, 1.0]])
+    else:
+        raise ValueError("a 2D transformation is a 3 x 3 or 2 x 3 matrix")
+    if not np.allclose(a[2], [0.0, 0.0, 1.0]):
+        raise NotImplementedError("projective uv transformations are not on the GPU path")
+    return a
+
+
+class TransformationUv(UnaryOperator):
+    """TransformationUv(texture, transformation): texture looked up at the transformed (u, v)
+    (transformation_uv.cpp:67-70)."""
+
+    def __init__(self, texture, transformation):
+        super().__init__(texture)
+        self.transformation = transformation
+
+    @property
+    def transformation(self) -> np.ndarray:
+        return self._matrix
+
+    @transformation.setter
+    def transformation(self, value):
+        self._matrix = as_matrix2d(value)
+
+
+def is_uv_texture(x) -> bool:
+    return isinstance(x, (CheckerBoard, GridBoard, TransformationUv))
+
+
+def warn_point_lookup(tex: CheckerBoard):
+    if tex.antiAliasing == CheckerBoard.AA_BILINEAR and not CheckerBoard._warned:
+        CheckerBoard._warned = True
+        warnings.warn("CheckerBoard antiAliasing 'bilinear' is rendered as 'none' (no ray differentials on the GPU path)",
+                      stacklevel=3)
+
+
 def as_spectrum(x) -> Spectrum:
-    """Spectrum of a texture, a spectrum or a number (the shaders' texture slots)."""
+    """Spectrum of a constant texture, a spectrum or a number (the texture slots that take
+    constants only)."""
     if isinstance(x, Constant):
         return x.value
     if isinstance(x, Spectrum):
         return x
     if isinstance(x, (int, float)):
         return Spectrum(float(x))
-    raise TypeError(f"unsupported texture {type(x).__name__}: only constant textures are implemented")
+    raise TypeError(f"unsupported texture {type(x).__name__} in this slot: it takes constant textures only")
 
 
 def as_scalar(x) -> float:

@@ -28,7 +28,8 @@ def sources() -> list[Path]:
 
 def _digest() -> str:
     h = hashlib.sha256()
-    for p in sources() + sorted(HERE.glob("*.h")):
+    # the sources, and the C ABI header whose struct layouts they check
+    for p in sources() + sorted(HERE.glob("*.h")) + sorted((HERE.parent / "include").glob("*.h")):
         h.update(p.name.encode())
         h.update(p.read_bytes())
     h.update(" ".join(FLAGS).encode())

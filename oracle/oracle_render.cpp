@@ -21,10 +21,13 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstddef>
 #include <cstdint>
 #include <cstring>
 #include <thread>
 #include <vector>
+
+#include "../include/liar_gpu.h"
 
 extern "C" int oracle_tri_intersect(const float* o, const float* d, const float* a, const float* b, const float* c,
                                     float* t_out, float* u_out, float* v_out);
@@ -59,6 +62,11 @@ struct Material {
     int32_t emission;
     float rough_u, rough_v;
     int32_t samples;
+    int32_t tex[4];
+};
+struct Texture {
+    int32_t type, a, b, spectrum;
+    float p[6];
 };
 struct Light {
     int32_t type, spectrum, object, double_sided;
@@ -85,6 +93,8 @@ struct SceneIn {
     const Light* lights; uint64_t n_lights;
     const float* observer; uint64_t n_observer;
     float scene_radius;
+    const Texture* textures; uint64_t n_textures;
+    const float* triangle_uvs;
 };
 struct RenderIn {
     Camera camera;
@@ -102,6 +112,18 @@ struct RenderIn {
     float pm_ratio_precomputed_irradiance;
     int32_t pm_reserved;
 };
+
+// the mirrors above have the C ABI's layout
+static_assert(sizeof(Spectrum) == sizeof(liar_spectrum) && sizeof(Material) == sizeof(liar_material) &&
+                  sizeof(Texture) == sizeof(liar_texture) && sizeof(Light) == sizeof(liar_light) &&
+                  sizeof(Camera) == sizeof(liar_camera) && sizeof(SceneIn) == sizeof(liar_scene_desc) &&
+                  sizeof(RenderIn) == sizeof(liar_render_desc),
+              "oracle mirrors out of step with include/liar_gpu.h");
+static_assert(offsetof(Material, tex) == offsetof(liar_material, tex) &&
+                  offsetof(SceneIn, triangle_uvs) == offsetof(liar_scene_desc, triangle_uvs) &&
+                  offsetof(RenderIn, pm_max_photons) == offsetof(liar_render_desc, photon_mapper) &&
+                  offsetof(RenderIn, filter) == offsetof(liar_render_desc, filter),
+              "oracle mirrors out of step with include/liar_gpu.h");
 
 // The photon maps of a PhotonMapper render (photon_mapper.cpp:798-835) as the oracle gets them:
 // photons in buffer order, powers XYZ already scaled, each power's recovery blend (three sample
@@ -624,7 +646,53 @@ struct Ctx {
     V target, ng, N, u, v;
     bool leaving;
     int obj, light, mi;
+    float uv_u, uv_v;
 };
+
+// IntersectionContext::uv of a triangle hit (TriangleMesh::doLocalContext, triangle_mesh.cpp:334-356):
+// the corners' (u, v) interpolated at the barycentrics, or the barycentrics themselves
+void hit_uv(const Scene& S, uint32_t prim, float bu, float bv, float& u, float& v) {
+    if (!S.in.triangle_uvs) {
+        u = bu;
+        v = bv;
+        return;
+    }
+    const float* t = S.in.triangle_uvs + 6 * (size_t)prim;
+    const float w0 = 1 - bu - bv;
+    u = w0 * t[0] + bu * t[2] + bv * t[4];
+    v = w0 * t[1] + bu * t[3] + bv * t[5];
+}
+
+float frac(float x) { return x - std::floor(x); }
+
+// Texture::lookUp of the uv textures (src/liar/textures/): TransformationUv moves the context's uv
+// (transformation_uv.cpp:67-70), CheckerBoard without anti-aliasing picks A where the fractional u
+// and v lie on the same side of the split (checker_board.cpp:113-124, 149-157), GridBoard picks A
+// on the lines (grid_board.cpp:80-87), Constant is its spectrum
+float texture(const Scene& S, int t, float u, float v, float lam, bool reflectant) {
+    for (int depth = 0; depth < 32; ++depth) {
+        const Texture& T = S.in.textures[t];
+        if (T.type == 1) {
+            t = ((frac(u) < T.p[0]) == (frac(v) < T.p[1])) ? T.a : T.b;
+        } else if (T.type == 2) {
+            const float fu = frac(u), fv = frac(v);
+            t = (fu < T.p[0] || fv < T.p[0] || fu > 1 - T.p[0] || fv > 1 - T.p[1]) ? T.a : T.b;
+        } else if (T.type == 3) {
+            const float nu = T.p[0] * u + T.p[1] * v + T.p[2];
+            const float nv = T.p[3] * u + T.p[4] * v + T.p[5];
+            u = nu;
+            v = nv;
+            t = T.a;
+        } else {
+            return spectrum(S, T.spectrum, lam, reflectant);
+        }
+    }
+    return 0;
+}
+
+float param(const Scene& S, const Material& M, int k, float u, float v, float lam, bool reflectant) {
+    return M.tex[k] >= 0 ? texture(S, M.tex[k], u, v, lam, reflectant) : spectrum(S, M.spec[k], lam, reflectant);
+}
 Ctx hit_ctx(const Scene& S, V o, V d, const Hit& h) {
     Ctx c;
     const uint32_t prim = (uint32_t)h.prim;
@@ -641,6 +709,7 @@ Ctx hit_ctx(const Scene& S, V o, V d, const Hit& h) {
     const float oo[3] = {o.x, o.y, o.z}, dd[3] = {d.x, d.y, d.z};
     if (!oracle_tri_intersect(oo, dd, pa, pb, pc, &tt, &bu, &bv)) bu = bv = 0;
     c.target = A + bu * e1 + bv * e2;
+    hit_uv(S, prim, bu, bv, c.uv_u, c.uv_v);
     const V ng0 = unit(cross(e1, e2));
     V ns = ng0;
     if (S.in.triangle_normals && S.in.normals) {
@@ -688,38 +757,38 @@ Bsdf make_bsdf(const Scene& S, const Material& M, const Ctx& c, float lam) {
     switch (M.type) {
         case M_LAMBERT:
             B.caps = C_REFL | C_DIFF;
-            B.r = spectrum(S, M.spec[0], lam, true);
+            B.r = param(S, M, 0, c.uv_u, c.uv_v, lam, true);
             break;
         case M_CONDUCTOR:
         case M_CT:
             B.caps = M.type == M_CONDUCTOR ? (C_REFL | C_SPEC) : (C_REFL | C_GLOSSY);
-            B.eta = std::max(spectrum(S, M.spec[0], lam, false), 1e-9f);
-            B.kappa = std::max(spectrum(S, M.spec[1], lam, false), 1e-9f);
-            B.r = spectrum(S, M.spec[2], lam, true);
+            B.eta = std::max(param(S, M, 0, c.uv_u, c.uv_v, lam, false), 1e-9f);
+            B.kappa = std::max(param(S, M, 1, c.uv_u, c.uv_v, lam, false), 1e-9f);
+            B.r = param(S, M, 2, c.uv_u, c.uv_v, lam, true);
             break;
         case M_DIELECTRIC: {
             B.caps = C_REFL | C_TRANS | C_SPEC;
-            const float i1 = std::max(spectrum(S, M.spec[1], lam, false), 1e-9f);
-            const float i2 = std::max(spectrum(S, M.spec[0], lam, false), 1e-9f);
+            const float i1 = std::max(param(S, M, 1, c.uv_u, c.uv_v, lam, false), 1e-9f);
+            const float i2 = std::max(param(S, M, 0, c.uv_u, c.uv_v, lam, false), 1e-9f);
             B.ior = c.leaving ? i2 / i1 : i1 / i2;
-            B.r = spectrum(S, M.spec[2], lam, true);
-            B.t = spectrum(S, M.spec[3], lam, true);
+            B.r = param(S, M, 2, c.uv_u, c.uv_v, lam, true);
+            B.t = param(S, M, 3, c.uv_u, c.uv_v, lam, true);
             break;
         }
         case M_WALTER: {
             B.caps = C_TRANS | C_GLOSSY;
-            float ei = std::max(spectrum(S, M.spec[1], lam, false), 1e-9f);
-            float et = std::max(spectrum(S, M.spec[0], lam, false), 1e-9f);
+            float ei = std::max(param(S, M, 1, c.uv_u, c.uv_v, lam, false), 1e-9f);
+            float et = std::max(param(S, M, 0, c.uv_u, c.uv_v, lam, false), 1e-9f);
             if (c.leaving) std::swap(ei, et);
             B.etaI = ei;
             B.etaT = et;
-            B.r = spectrum(S, M.spec[2], lam, true);
-            B.t = spectrum(S, M.spec[3], lam, true);
+            B.r = param(S, M, 2, c.uv_u, c.uv_v, lam, true);
+            B.t = param(S, M, 3, c.uv_u, c.uv_v, lam, true);
             break;
         }
         case M_MIRROR:
             B.caps = C_REFL | C_SPEC;
-            B.r = spectrum(S, M.spec[0], lam, true);
+            B.r = param(S, M, 0, c.uv_u, c.uv_v, lam, true);
             break;
     }
     return B;
@@ -1390,6 +1459,7 @@ struct PhotonIn {
     uint64_t seed, global_target, max_emitted, wave;
     int32_t final_gather, reserved;
 };
+static_assert(sizeof(PhotonIn) == sizeof(liar_photon_desc), "oracle mirror out of step with include/liar_gpu.h");
 struct PhotonRec {
     float pos[3], omega[3], power[3];
     uint32_t path, tag;
@@ -1443,10 +1513,12 @@ static void trace_photon_rec(const Scene& S, const PhotonIn& D, const Sampler& s
     const V e1 = V{pb[0], pb[1], pb[2]} - A, e2 = V{pc[0], pc[1], pc[2]} - A;
     const V ng0 = unit(cross(e1, e2));
     V ns = ng0;
+    float tt, bu = 0, bv = 0;
+    const float oo[3] = {o.x, o.y, o.z}, dd[3] = {d.x, d.y, d.z};
+    if (!oracle_tri_intersect(oo, dd, pa, pb, pc, &tt, &bu, &bv)) bu = bv = 0;
+    float uv_u, uv_v;
+    hit_uv(S, prim, bu, bv, uv_u, uv_v);
     if (S.in.triangle_normals && S.in.normals) {
-        float tt, bu = 0, bv = 0;
-        const float oo[3] = {o.x, o.y, o.z}, dd[3] = {d.x, d.y, d.z};
-        if (!oracle_tri_intersect(oo, dd, pa, pb, pc, &tt, &bu, &bv)) bu = bv = 0;
         const int32_t* tn = S.in.triangle_normals + 3 * (size_t)prim;
         if (tn[0] >= 0 && tn[1] >= 0 && tn[2] >= 0) {
             const float* n0 = S.in.normals + 3 * tn[0];
@@ -1483,38 +1555,38 @@ static void trace_photon_rec(const Scene& S, const PhotonIn& D, const Sampler& s
     switch (M.type) {
         case M_LAMBERT:
             B.caps = C_REFL | C_DIFF;
-            B.r = spectrum(S, M.spec[0], lam, true);
+            B.r = param(S, M, 0, uv_u, uv_v, lam, true);
             break;
         case M_CONDUCTOR:
         case M_CT:
             B.caps = M.type == M_CONDUCTOR ? (C_REFL | C_SPEC) : (C_REFL | C_GLOSSY);
-            B.eta = std::max(spectrum(S, M.spec[0], lam, false), 1e-9f);
-            B.kappa = std::max(spectrum(S, M.spec[1], lam, false), 1e-9f);
-            B.r = spectrum(S, M.spec[2], lam, true);
+            B.eta = std::max(param(S, M, 0, uv_u, uv_v, lam, false), 1e-9f);
+            B.kappa = std::max(param(S, M, 1, uv_u, uv_v, lam, false), 1e-9f);
+            B.r = param(S, M, 2, uv_u, uv_v, lam, true);
             break;
         case M_DIELECTRIC: {
             B.caps = C_REFL | C_TRANS | C_SPEC;
-            const float i1 = std::max(spectrum(S, M.spec[1], lam, false), 1e-9f);
-            const float i2 = std::max(spectrum(S, M.spec[0], lam, false), 1e-9f);
+            const float i1 = std::max(param(S, M, 1, uv_u, uv_v, lam, false), 1e-9f);
+            const float i2 = std::max(param(S, M, 0, uv_u, uv_v, lam, false), 1e-9f);
             B.ior = leaving ? i2 / i1 : i1 / i2;
-            B.r = spectrum(S, M.spec[2], lam, true);
-            B.t = spectrum(S, M.spec[3], lam, true);
+            B.r = param(S, M, 2, uv_u, uv_v, lam, true);
+            B.t = param(S, M, 3, uv_u, uv_v, lam, true);
             break;
         }
         case M_WALTER: {
             B.caps = C_TRANS | C_GLOSSY;
-            float ei = std::max(spectrum(S, M.spec[1], lam, false), 1e-9f);
-            float et = std::max(spectrum(S, M.spec[0], lam, false), 1e-9f);
+            float ei = std::max(param(S, M, 1, uv_u, uv_v, lam, false), 1e-9f);
+            float et = std::max(param(S, M, 0, uv_u, uv_v, lam, false), 1e-9f);
             if (leaving) std::swap(ei, et);
             B.etaI = ei;
             B.etaT = et;
-            B.r = spectrum(S, M.spec[2], lam, true);
-            B.t = spectrum(S, M.spec[3], lam, true);
+            B.r = param(S, M, 2, uv_u, uv_v, lam, true);
+            B.t = param(S, M, 3, uv_u, uv_v, lam, true);
             break;
         }
         case M_MIRROR:
             B.caps = C_REFL | C_SPEC;
-            B.r = spectrum(S, M.spec[0], lam, true);
+            B.r = param(S, M, 0, uv_u, uv_v, lam, true);
             break;
     }
     const V md = -d;

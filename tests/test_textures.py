@@ -1,0 +1,150 @@
+"""uv textures of the scene API (src/liar/textures/checker_board.cpp, grid_board.cpp,
+transformation_uv.cpp): their flattening into liar_texture trees, the surface coordinates of the
+shapes, and the oracle's renders of a checker board lit by a uniform sky, whose quadrants show the
+board's reflectances."""
+import numpy as np
+import pytest
+
+import oracle
+from liar_b200 import cameras, render as R, scenery, shaders, spectra, textures as tx, tracers
+
+
+def test_checker_tree_is_flattened_once_per_node():
+    white, black = tx.Constant(0.8), tx.Constant(0.2)
+    board = tx.CheckerBoard(white, black)
+    board.split = (0.25, 0.75)
+    board.antiAliasing = tx.CheckerBoard.AA_NONE
+    moved = tx.TransformationUv(board, [[4, 0, 0.5], [0, 4, 0], [0, 0, 1]])
+    grid = tx.GridBoard(moved, black)
+    grid.thickness = (0.2, 0.4)
+    a = scenery.Parallelogram((0, 0, 0), (1, 0, 0), (0, 1, 0))
+    a.shader = shaders.Lambert(grid)
+    b = scenery.Parallelogram((0, 0, 1), (1, 0, 0), (0, 1, 0))
+    b.shader = shaders.Lambert(board)   # shares the board's nodes
+    flat = R.flatten(scenery.List([a, b]))
+    T = list(flat.textures)
+    kinds = [t.type for t in T]
+    assert kinds.count(R.TEX_CHECKER) == 1 and kinds.count(R.TEX_GRID) == 1 and kinds.count(R.TEX_UV_TRANSFORM) == 1
+    assert kinds.count(R.TEX_CONSTANT) == 2
+    m0, m1 = flat.materials[0], flat.materials[1]
+    assert m0.spec[0] == -1 and m1.spec[0] == -1
+    g = T[m0.tex[0]]
+    assert g.type == R.TEX_GRID and tuple(g.p[:2]) == pytest.approx((0.1, 0.2))   # half thickness
+    tr = T[g.a]
+    assert tr.type == R.TEX_UV_TRANSFORM and list(tr.p) == pytest.approx([4, 0, 0.5, 0, 4, 0])
+    assert tr.a == m1.tex[0] and T[tr.a].type == R.TEX_CHECKER and tuple(T[tr.a].p[:2]) == (0.25, 0.75)
+    assert T[T[tr.a].b].spectrum == T[g.b].spectrum
+    # parallelogram uvs: (u, v) of support + u sizeU + v sizeV at the corners
+    np.testing.assert_array_equal(flat.triangle_uvs[:2].reshape(2, 3, 2), a.corner_uvs())
+
+
+def test_constant_only_scenes_carry_no_uvs_and_constants_stay_spectra():
+    p = scenery.Parallelogram((0, 0, 0), (1, 0, 0), (0, 1, 0))
+    p.shader = shaders.Lambert(tx.Constant(0.5))
+    flat = R.flatten(p)
+    assert flat.triangle_uvs is None and flat.textures is None
+    assert flat.materials[0].tex[0] == -1 and flat.materials[0].spec[0] >= 0
+
+
+def test_shape_uvs():
+    box = scenery.Box((0, 0, 0), (2, 1, 4))
+    v, t, _, _ = box.triangles()
+    uv = box.corner_uvs()
+    for k in range(12):
+        axis, positive = k // 4, (k // 2) % 2 == 1
+        i, j = (axis + 1) % 3, (axis + 2) % 3
+        for c in range(3):
+            p = v[t[k][c]]
+            expect_v = p[j] / (2, 1, 4)[j]
+            assert uv[k, c, 0] == pytest.approx(p[i] / (2, 1, 4)[i])
+            assert uv[k, c, 1] == pytest.approx(expect_v if positive else 1 - expect_v)
+    sphere = scenery.Sphere((1, 2, 3), 2.0, subdivisions=2)
+    sv, st, _, _ = sphere.triangles()
+    suv = sphere.corner_uvs()
+    n = (sv.astype(np.float64) - (1, 2, 3)) / 2.0
+    theta = np.arccos(np.clip(n[:, 2], -1, 1)) / np.pi
+    np.testing.assert_allclose(suv[..., 1], theta[st], atol=1e-6)
+    assert (np.ptp(suv[..., 0], axis=1) < 0.3).all()      # unwrapped across the seam
+    mesh = scenery.TriangleMesh([(0, 0, 0), (1, 0, 0), (0, 1, 0), (1, 1, 0)], (), [(0.1, 0.2), (0.3, 0.4), (0.5, 0.6)],
+                                [((0, None, 0), (1, None, 1), (2, None, 2)), (1, 3, 2)])
+    muv = mesh.corner_uvs()
+    np.testing.assert_allclose(muv[0], [[0.1, 0.2], [0.3, 0.4], [0.5, 0.6]])
+    np.testing.assert_allclose(muv[1], [[0, 0], [1, 0], [0, 1]])   # no uvs: the barycentrics
+
+
+def test_mirroring_transformation_rewinds_uvs_with_the_triangles():
+    p = scenery.Parallelogram((0, 0, 0), (1, 0, 0), (0, 1, 0))
+    p.shader = shaders.Lambert(tx.CheckerBoard(0.1, 0.9))
+    with pytest.warns(UserWarning, match="bilinear"):
+        tx.CheckerBoard._warned = False
+        m = scenery.Transformation(p, [[-1, 0, 0, 0], [0, 1, 0, 0], [0, 0, 1, 0], [0, 0, 0, 1]])
+        flat = R.flatten(m)
+    uv = flat.triangle_uvs.reshape(-1, 3, 2)
+    np.testing.assert_array_equal(uv, p.corner_uvs()[:, [0, 2, 1]])
+    assert (flat.triangles == np.array([[0, 2, 1], [0, 3, 2]])).all()
+
+
+def test_bad_texture_uses_fail_loudly():
+    with pytest.raises(NotImplementedError):
+        tx.TransformationUv(tx.Constant(1), [[1, 0, 0], [0, 1, 0], [0.5, 0, 1]])
+    with pytest.raises(KeyError):
+        tx.CheckerBoard(0, 1).antiAliasing = "trilinear"
+    light = scenery.Parallelogram((0, 0, 0), (1, 0, 0), (0, 1, 0))
+    light.shader = shaders.Unshaded(tx.CheckerBoard(0, 1))
+    with pytest.raises(TypeError):
+        R.flatten(light)
+
+
+def _board_scene(texture):
+    """A unit checker plane z = 0 (uv = (x, y)) under a uniform sky of radiance 1, seen from above
+    with x to the right of the image and y up: the view covers x in [0.1, 0.9], y in [0.2, 0.8]."""
+    plane = scenery.Parallelogram((0, 0, 0), (1, 0, 0), (0, 1, 0))
+    plane.shader = shaders.Lambert(texture)
+    sky = scenery.LightSky(tx.Constant(1.0))
+    cam = cameras.PerspectiveCamera()
+    cam.position = (0.5, 0.5, 0.4)
+    cam.sky = (0, 1, 0)
+    cam.lookAt((0.5, 0.5, 0.0))
+    return scenery.List([plane, sky]), cam
+
+
+def _quadrants(img, w, h, band=3):
+    """Mean luminance of the image's top-left, top-right, bottom-left and bottom-right quadrants,
+    leaving out a band around the middle lines."""
+    Y = img[..., 1]
+    cx, cy = w // 2, h // 2
+    return (Y[:cy - band, :cx - band].mean(), Y[:cy - band, cx + band:].mean(),
+            Y[cy + band:, :cx - band].mean(), Y[cy + band:, cx + band:].mean())
+
+
+@pytest.mark.parametrize("shift", [False, True])
+def test_oracle_checker_board_quadrants(shift):
+    a, b = 0.8, 0.2
+    board = tx.CheckerBoard(tx.Constant(a), tx.Constant(b))
+    board.antiAliasing = "none"
+    tex = tx.TransformationUv(board, [[1, 0, 0.5], [0, 1, 0], [0, 0, 1]]) if shift else board
+    scene, cam = _board_scene(tex)
+    t = tracers.DirectLighting()
+    t.maxRayGeneration = 1
+    w, h = 40, 30
+    flat = R.flatten(scene)
+    img, _ = R.resolve(oracle.RenderScene(flat).render(R.render_desc(cam, w, h, 16, t, seed=1)))
+    tl, tr, bl, br = _quadrants(img, w, h)
+    # A where u and v lie on the same side of the split: (u > 0.5, v > 0.5) is the top right
+    expect = (b, a, a, b) if not shift else (a, b, b, a)
+    np.testing.assert_allclose((tl, tr, bl, br), expect, rtol=0.05)
+
+
+def test_oracle_grid_board_lines():
+    grid = tx.GridBoard(tx.Constant(0.9), tx.Constant(0.1))
+    grid.thickness = (0.2, 0.2)
+    # 2 cells per unit: lines (0.1 wide in uv) at x = 0.5 and y = 0.5 cross the image's middle
+    scene, cam = _board_scene(tx.TransformationUv(grid, [[2, 0, 0], [0, 2, 0], [0, 0, 1]]))
+    t = tracers.DirectLighting()
+    t.maxRayGeneration = 1
+    w, h = 40, 30
+    img, _ = R.resolve(oracle.RenderScene(R.flatten(scene)).render(R.render_desc(cam, w, h, 8, t, seed=2)))
+    Y = img[..., 1]
+    assert Y[h // 2 - 1:h // 2 + 1, :].mean() == pytest.approx(0.9, rel=0.05)    # the line y = 0.5
+    assert Y[:, w // 2 - 1:w // 2 + 1].mean() == pytest.approx(0.9, rel=0.05)    # the line x = 0.5
+    assert Y[4:10, 6:12].mean() == pytest.approx(0.1, rel=0.1)                    # inside a cell

@@ -1,0 +1,141 @@
+"""uv textures on the GPU (render_dev.cuh texture_eval / param_eval) against the oracle's
+restatement (oracle_render.cpp texture / param) in every renderer that shades surfaces: the path
+tracer, DirectLighting, the batched renderer and photon tracing; and the scene upload's checks of
+texture trees."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from liar_b200 import batch as B, cameras, photons, render as R, scenery, shaders, spectra, textures as tx, tracers
+from liar_b200._native import LiarGpuError
+from liar_b200.kernel import default_context
+
+pytestmark = pytest.mark.gpu
+
+
+def _scene():
+    a, b = tx.Constant(0.85), tx.Constant(spectra.Sampled([380e-9, 550e-9, 720e-9], [0.1, 0.3, 0.6]))
+    board = tx.CheckerBoard(a, b)
+    board.antiAliasing = "none"
+    floor = scenery.Parallelogram((-2, 0, -2), (4, 0, 0), (0, 0, 4))
+    floor.shader = shaders.Lambert(tx.TransformationUv(board, [[4, 0, 0.25], [0, 4, 0], [0, 0, 1]]))
+    grid = tx.GridBoard(tx.Constant(0.05), tx.Constant(0.6))
+    grid.thickness = (0.15, 0.3)
+    back = scenery.Parallelogram((-2, 0, 2), (4, 0, 0), (0, 3, 0))
+    back.shader = shaders.Lambert(tx.TransformationUv(grid, [[3, 1, 0], [0, 3, 0], [0, 0, 1]]))
+    ball = scenery.Sphere((-0.7, 0.6, 0.2), 0.6, subdivisions=3)
+    ct = shaders.CookTorrance(tx.Constant(spectra.Spectrum(1.5)), tx.Constant(spectra.Spectrum(3.0)))
+    stripes = tx.CheckerBoard(tx.Constant(1.0), tx.Constant(0.2))
+    stripes.split = (0.5, 2.0)        # v always below the split: stripes along u
+    stripes.antiAliasing = "none"
+    ct.reflectance = tx.TransformationUv(stripes, [[8, 0, 0], [0, 1, 0], [0, 0, 1]])
+    ct.roughness = tx.Constant(0.3)
+    ball.shader = ct
+    box = scenery.Box((0.3, 0, -0.5), (1.1, 0.8, 0.3))
+    box.shader = shaders.Lambert(tx.CheckerBoard(0.7, 0.15))
+    mirrored = scenery.Transformation(box, [[-1, 0, 0, 0.6], [0, 1, 0, 0], [0, 0, 1, 0], [0, 0, 0, 1]])
+    surf = scenery.Parallelogram((-0.5, 2.5, -0.5), (1, 0, 0), (0, 0, 1))
+    light = scenery.LightArea(surf)
+    light.radiance = spectra.BlackBody(5000, 20)
+    cam = cameras.PerspectiveCamera()
+    cam.position = (0, 1.5, -4)
+    cam.lookAt((0, 0.8, 0))
+    return scenery.List([floor, back, ball, mirrored, light]), cam
+
+
+def _within_3_sigma(g, c, min_fraction=0.99):
+    mg, vg = R.resolve(g)
+    mc, vc = R.resolve(c)
+    sig = np.sqrt(vg + vc)
+    ok = np.abs(mg[..., :3] - mc[..., :3]) <= 3 * sig + 1e-6 * np.maximum(np.abs(mc[..., :3]), 1.0)
+    assert ok.mean() >= min_fraction, f"only {ok.mean():.4f} of pixel channels within 3 sigma"
+    np.testing.assert_array_equal(g[..., 7], c[..., 7])
+    assert abs(mg[..., 1].mean() / mc[..., 1].mean() - 1) < 0.02
+    return mg, mc
+
+
+@pytest.fixture(scope="module")
+def textured():
+    import warnings
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        scene, cam = _scene()
+        flat = R.flatten(scene)
+    assert flat.triangle_uvs is not None and len(flat.textures) >= 10
+    return flat, R.GpuScene(default_context(), flat), cam
+
+
+@pytest.mark.parametrize("kind", ["path", "direct"])
+def test_textured_scene_matches_oracle(textured, kind):
+    flat, gs, cam = textured
+    if kind == "path":
+        t = tracers.AdjointPhotonTracer()
+    else:
+        t = tracers.DirectLighting()
+    t.maxRayGeneration = 3
+    d = R.render_desc(cam, 48, 40, 16, t, seed=5)
+    g = gs.render(d)
+    c = oracle.RenderScene(flat).render(d)
+    mg, _ = _within_3_sigma(g, c)
+    # the board shows: the floor's pixels take both checker values
+    assert np.ptp(mg[-8:, :, 1]) > 0.05
+
+
+def test_textured_batch_matches_single_render(textured):
+    _, gs, cam = textured
+    t = tracers.AdjointPhotonTracer()
+    t.maxRayGeneration = 3
+    t.maxDepth = 8                      # the batched renderer's bounded path length
+    d = R.render_desc(cam, 40, 32, 8, t, seed=2)
+    film = torch.zeros((d.height, d.width, 8), dtype=torch.float32, device="cuda:0")
+    gs.render_device(d, film.data_ptr())
+    br = B.BatchRenderer(default_context(), [(gs, d)], B.make_config(hero=1))
+    br.launch()
+    torch.cuda.synchronize()
+    a, b = br.films[0].cpu().numpy(), film.cpu().numpy()
+    scale = max(float(np.abs(b[..., :7]).max()), 1e-6)
+    np.testing.assert_allclose(a[..., :7], b[..., :7], rtol=2e-5, atol=2e-6 * scale)
+    br.close()
+
+
+def test_textured_photon_trace_matches_oracle(textured):
+    flat, gs, _ = textured
+    d = photons.photon_desc(3000, max_emitted=400_000, wave=8192, ray_traced_direct=False, seed=6)
+    g, gc = photons.trace_photons(gs, d, capacity=400_000)
+    c, cc = oracle.photon_trace(oracle.RenderScene(flat), d, 400_000)
+    g = {k: v.cpu().numpy() for k, v in g.items()}
+    assert gc["emitted"] == cc["emitted"]
+    gkey = (g["path"].astype(np.int64) << 8) | ((g["tag"] >> 8) & 0xFF)
+    ckey = (c["path"].astype(np.int64) << 8) | ((c["tag"] >> 8) & 0xFF)
+    common, gi, ci = np.intersect1d(gkey, ckey, return_indices=True)
+    assert len(common) >= 0.98 * len(ckey)
+    np.testing.assert_allclose(g["power"][gi], c["power"][ci], rtol=2e-3, atol=1e-3)
+
+
+def _upload(flat):
+    return R.GpuScene(default_context(), flat)
+
+
+def test_upload_refuses_bad_texture_trees():
+    p = scenery.Parallelogram((0, 0, 0), (1, 0, 0), (0, 1, 0))
+    board = tx.CheckerBoard(0.1, 0.9)
+    board.antiAliasing = "none"
+    p.shader = shaders.Lambert(board)
+    flat = R.flatten(p)
+    _upload(flat)                                       # the tree as flattened is fine
+    root = flat.materials[0].tex[0]
+    flat.textures[flat.textures[root].a].type = R.TEX_UV_TRANSFORM
+    flat.textures[flat.textures[root].a].a = root       # a cycle
+    with pytest.raises(LiarGpuError):
+        _upload(flat)
+    flat = R.flatten(p)
+    flat.materials[0].tex[0] = len(flat.textures)       # out of range
+    with pytest.raises(LiarGpuError):
+        _upload(flat)
+    deep = tx.Constant(0.5)
+    for _ in range(40):
+        deep = tx.TransformationUv(deep, [[1, 0, 0.01], [0, 1, 0], [0, 0, 1]])
+    p.shader = shaders.Lambert(deep)
+    with pytest.raises(LiarGpuError):
+        _upload(R.flatten(p))
