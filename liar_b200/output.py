@@ -1,13 +1,32 @@
-"""Render targets (``liar.output``). Image keeps the reference's name; with no image codecs in this
-build it writes the linear XYZ film as .npy (or a 3-channel .pfm when the name ends in .pfm).
-Display, an X11 window in the reference, is unavailable on this box and is replaced by a headless
-buffer that keeps the last frame."""
+"""Render targets (``liar.output``). Image keeps the reference's name and writes its file through
+the reference's Raster tone mapping (output/raster.cpp) and image codecs (``codecs.py``: .png,
+.hdr, .pfm, .exr); a name ending in .npy keeps the linear XYZA film itself. Display, an X11
+window in the reference, is unavailable on this box and is replaced by a headless buffer that
+keeps the last frame."""
 from __future__ import annotations
 
 import math
 from pathlib import Path
 
 import numpy as np
+
+from . import codecs
+
+TONE_MAPPINGS = ("Linear", "CompressY", "CompressRGB", "Reinhard2002Y", "Reinhard2002RGB", "ExponentialY",
+                 "ExponentialRGB", "DuikerY", "DuikerRGB")
+
+
+def _filmic(x):
+    """Duiker's filmic curve with the display gamma undone (raster.cpp:60-67)."""
+    x = np.maximum(np.float32(0), x - np.float32(0.004))
+    y = (x * (np.float32(6.2) * x + np.float32(0.5))) / (x * (np.float32(6.2) * x + np.float32(1.7)) + np.float32(0.06))
+    return np.power(y, np.float32(2.2))
+
+
+def _inv_filmic(y: float) -> float:
+    y = min(max(y, 0.0), 0.99999) ** (1.0 / 2.2)
+    a, b, c = 6.2 * y - 6.2, 1.7 * y - 0.5, 0.06 * y
+    return (-b - math.sqrt(b * b - 4 * a * c)) / (2 * a) + 0.004
 
 
 class RenderTarget:
@@ -24,21 +43,141 @@ class RenderTarget:
         self.variance = variance
 
 
-class Image(RenderTarget):
-    def __init__(self, filename: str = "image.npy", resolution=(320, 240)):
+class Raster(RenderTarget):
+    """The reference's Raster settings and tone mapping (output/raster.cpp:45-500): rgbSpace,
+    toneMapping, exposureStops (setting it turns autoExposure off), exposureCorrectionStops,
+    autoExposure (default on), middleGrey (0.184)."""
+
+    def __init__(self, resolution=(320, 240)):
         super().__init__(resolution)
-        self.filename = filename
+        self.rgbSpace = codecs.default_space()
+        self._tone = "Linear"
+        self._stops = 0.0
+        self.exposureCorrectionStops = 0.0
+        self.autoExposure = True
+        self.middleGrey = 0.184
+
+    @property
+    def toneMapping(self) -> str:
+        return self._tone
+
+    @toneMapping.setter
+    def toneMapping(self, mode: str):
+        for t in TONE_MAPPINGS:
+            if t.lower() == str(mode).lower():
+                self._tone = t
+                return
+        raise KeyError(f"unknown tone mapping {mode!r}; one of {TONE_MAPPINGS}")
+
+    @property
+    def exposureStops(self) -> float:
+        if self.autoExposure and self.xyza is not None:
+            return self._auto_stops()
+        return self._stops
+
+    @exposureStops.setter
+    def exposureStops(self, stops: float):
+        self.autoExposure = False
+        self._stops = float(stops)
+
+    def _auto_stops(self) -> float:
+        """Raster::exposureStops with autoExposure (raster.cpp:99-150): the gain that maps the
+        log-average luminance of the covered pixels to middleGrey, in thirds of a stop."""
+        y = self.xyza[..., 1].astype(np.float64)
+        cov = y > 0
+        if not cov.any():
+            gain = 1.0
+        else:
+            avg = math.exp(float(np.log(y[cov]).mean()))
+            g = self.middleGrey
+            if self._tone == "Linear":
+                gain = g / avg
+            elif self._tone in ("CompressY", "CompressRGB", "Reinhard2002Y", "Reinhard2002RGB"):
+                gain = g / (avg * (1 - g))
+            elif self._tone in ("ExponentialY", "ExponentialRGB"):
+                gain = -math.log1p(-g) / avg
+            else:
+                gain = _inv_filmic(g) / avg
+        self._stops = round(3.0 * math.log2(gain)) / 3.0
+        return self._stops
+
+    def tonemap(self, space) -> np.ndarray:
+        """Raster::tonemap(destSpace) (raster.cpp:309-496): (H, W, 4) RGBA in `space`; a NaN
+        pixel becomes pink."""
+        gain = np.float32(2.0 ** (self.exposureStops + self.exposureCorrectionStops))
+        lin = self.xyza[..., :3].astype(np.float32) * gain
+        alpha = self.xyza[..., 3:4].astype(np.float32)
+        t = self._tone
+        with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
+            if t == "Linear":
+                rgb = space.toRGB(lin)
+            elif t == "CompressY":
+                rgb = space.toRGB(lin / (1 + lin[..., 1:2]))
+            elif t == "ExponentialY":
+                Y = lin[..., 1:2]
+                scale = np.where(Y < 1e-8, 1 - Y / 2, -np.expm1(-Y) / Y)
+                rgb = space.toRGB(lin * scale)
+            elif t == "DuikerY":
+                Y = lin[..., 1:2]
+                rgb = space.toRGB(lin * (_filmic(Y) / np.maximum(Y, np.float32(0.004))))
+            elif t == "Reinhard2002Y":
+                Lw = gain * np.float32(self.max_scene_luminance())
+                inv = np.float32(1.0) / (Lw * Lw)
+                Y = lin[..., 1:2]
+                rgb = space.toRGB(lin * ((1 + Y * inv) / (1 + Y)))
+            else:
+                c = space.toRGBlinear(lin)
+                if t == "CompressRGB":
+                    c = c / (1 + c)
+                elif t == "Reinhard2002RGB":
+                    Lw = gain * np.float32(self.max_scene_luminance())
+                    inv = np.float32(1.0) / (Lw * Lw)
+                    c = c * (1 + c * inv) / (1 + c)
+                elif t == "ExponentialRGB":
+                    c = -np.expm1(-c)
+                else:  # DuikerRGB
+                    c = _filmic(c)
+                rgb = space.toGamma(c)
+        out = np.concatenate([rgb, alpha], axis=-1).astype(np.float32)
+        bad = np.isnan(out).any(axis=-1)
+        out[bad] = (1.0, 0.0, 1.0, 1.0)
+        return out
+
+    def max_scene_luminance(self) -> float:
+        """The brightest pixel's mean luminance (the reference tracks it while splatting,
+        raster.cpp:594-598)."""
+        y = self.xyza[..., 1]
+        return float(max(y.max(), 0.0)) if y.size else 0.0
+
+
+class Image(Raster):
+    """Image(path, resolution) (output/image.cpp): on writing, the film tone-mapped into the codec's
+    colour space and saved (Image::save); a .npy path keeps the linear XYZA film."""
+
+    def __init__(self, path: str = "image.npy", resolution=(320, 240)):
+        super().__init__(resolution)
+        self.path = path
+        self.options = ""
+
+    @property
+    def filename(self) -> str:
+        return str(self.path)
+
+    @filename.setter
+    def filename(self, value: str):
+        self.path = value
 
     def write(self, xyza, variance):
         super().write(xyza, variance)
-        p = Path(self.filename)
-        if p.suffix.lower() == ".pfm":
-            h, w = xyza.shape[:2]
-            with open(p, "wb") as f:
-                f.write(f"PF\n{w} {h}\n-1.0\n".encode())
-                f.write(np.ascontiguousarray(xyza[::-1, :, :3], dtype="<f4").tobytes())
-        else:
-            np.save(p.with_suffix(".npy") if p.suffix != ".npy" else p, xyza.astype(np.float32))
+        self.save()
+
+    def save(self):
+        p = Path(self.path)
+        if p.suffix.lower() == ".npy":
+            np.save(p, self.xyza.astype(np.float32))
+            return
+        space = codecs.writer_space(p, self.rgbSpace)
+        codecs.write(p, self.tonemap(space), space)
 
 
 class Display(RenderTarget):

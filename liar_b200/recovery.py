@@ -160,6 +160,7 @@ class RgbSpace:
         cs, cd = _BRADFORD @ W, _BRADFORD @ np.ones(3)
         m_cat = np.linalg.inv(_BRADFORD) @ np.diag(cd / cs) @ _BRADFORD   # white W -> illuminant E
         self.matrix = (m_cat @ m_xyz).astype(np.float32)  # columns: XYZ of the red, green, blue primaries
+        self.inverse = np.linalg.inv(m_cat @ m_xyz).astype(np.float32)  # columns: RGB of X, Y, Z
 
     def toXYZ(self, rgb) -> tuple[float, float, float]:
         r = np.asarray(rgb[:3], dtype=np.float32)
@@ -167,6 +168,44 @@ class RgbSpace:
             r = (np.sign(r) * np.power(np.abs(r), np.float32(self.gamma))).astype(np.float32)  # tonecurve
         x = self.matrix[:, 0] * r[0] + self.matrix[:, 1] * r[1] + self.matrix[:, 2] * r[2]
         return tuple(float(v) for v in x.astype(np.float32))
+
+    # array forms (..., 3) of RgbSpace::toXYZ / toRGBA / toRGBAlinear / toGamma / toLinear
+    # (rgb_space.cpp:82-189); the tonecurve is sign(x) |x|^gamma
+    def _curve(self, a: np.ndarray, g: float) -> np.ndarray:
+        if g == 1.0:
+            return a
+        return (np.sign(a) * np.power(np.abs(a), np.float32(g))).astype(np.float32)
+
+    def toLinear(self, rgb) -> np.ndarray:
+        return self._curve(np.asarray(rgb, dtype=np.float32), self.gamma)
+
+    def toGamma(self, rgb) -> np.ndarray:
+        return self._curve(np.asarray(rgb, dtype=np.float32), 1.0 / self.gamma)
+
+    def toXYZlinear(self, rgb) -> np.ndarray:
+        return (np.asarray(rgb, dtype=np.float32) @ self.matrix.T).astype(np.float32)
+
+    def toXYZarray(self, rgb) -> np.ndarray:
+        return self.toXYZlinear(self.toLinear(rgb))
+
+    def toRGBlinear(self, xyz) -> np.ndarray:
+        return (np.asarray(xyz, dtype=np.float32) @ self.inverse.T).astype(np.float32)
+
+    def toRGB(self, xyz) -> np.ndarray:
+        return self.toGamma(self.toRGBlinear(xyz))
+
+    def withGamma(self, gamma: float) -> "RgbSpace":
+        return RgbSpace(self.red, self.green, self.blue, self.white, gamma)
+
+    def linearSpace(self) -> "RgbSpace":
+        return self.withGamma(1.0)
+
+    def __eq__(self, other) -> bool:
+        return isinstance(other, RgbSpace) and (self.red, self.green, self.blue, self.white, self.gamma) == \
+            (other.red, other.green, other.blue, other.white, other.gamma)
+
+    def __hash__(self) -> int:
+        return hash((self.red, self.green, self.blue, self.white, self.gamma))
 
 
 sRGB = RgbSpace((0.6400, 0.3300), (0.3000, 0.6000), (0.1500, 0.0600), (0.3127, 0.3290), 2.2)
