@@ -181,11 +181,19 @@ typedef struct liar_material {
  *                 (CheckerBoard, checker_board.cpp:154-190 with anti-aliasing "none")
  *   GRID          a on the lines of half thickness p[0] (u, and v from below) and p[1] (v from
  *                 above), else b (GridBoard, grid_board.cpp:60-67)
- *   UV_TRANSFORM  child a at (p[0] u + p[1] v + p[2], p[3] u + p[4] v + p[5]) (TransformationUv) */
-enum liar_texture_type { LIAR_TEX_CONSTANT = 0, LIAR_TEX_CHECKER = 1, LIAR_TEX_GRID = 2, LIAR_TEX_UV_TRANSFORM = 3 };
+ *   UV_TRANSFORM  child a at (p[0] u + p[1] v + p[2], p[3] u + p[4] v + p[5]) (TransformationUv)
+ *   IMAGE         an a x b image of XYZ pixels (rows from the top) starting at pixel `pixels` of the
+ *                 scene's texture_pixels, looked up at (u, 1 - v) by nearest pixel (p[0] = 0) or
+ *                 bilinearly (p[0] = 1) with wrap-around (Image, textures/image.cpp:279-718 at mip
+ *                 level 0); the XYZ becomes a spectrum through the context's recovery table
+ *                 (Spectral::fromXYZ), so scenes with images need liar_gpu_set_recovery first */
+enum liar_texture_type {
+    LIAR_TEX_CONSTANT = 0, LIAR_TEX_CHECKER = 1, LIAR_TEX_GRID = 2, LIAR_TEX_UV_TRANSFORM = 3, LIAR_TEX_IMAGE = 4
+};
 typedef struct liar_texture {
     int32_t type, a, b, spectrum;
     float p[6];
+    int64_t pixels;
 } liar_texture;
 
 /* Lights (src/liar/scenery/light_*.cpp). AREA_PARALLELOGRAM: pos = support, u/v = sizes
@@ -219,6 +227,7 @@ typedef struct liar_scene_desc {
     const liar_texture* textures; size_t n_textures;     /* optional */
     const float* triangle_uvs;                           /* optional, n_triangles x 6: (u, v) per corner;
                                                             NULL: the barycentric coordinates of the hit */
+    const float* texture_pixels; size_t n_texture_pixels; /* image textures: n x 4 (X, Y, Z, unused) */
 } liar_scene_desc;
 
 /* PerspectiveCamera (src/liar/cameras/perspective_camera.cpp:406-434): direction/right/down are
@@ -387,7 +396,9 @@ int liar_gpu_render_guided_stats(const liar_gpu_ctx* ctx, unsigned long long* ou
  * indices n_samples .. n_samples + 3 (n_triangles x 3). The PhotonMapper needs it (photon powers
  * are XYZ, Spectral::fromXYZ); liar_b200 sets the reference's table on every context it renders
  * with. A colour is the barycentric blend of the spectra at its triangle's corners (zero at the
- * box corners), the weights scaled to sum to X + Y + Z. */
+ * box corners), the weights scaled to sum to X + Y + Z. Image textures need it too. A table
+ * replaced by a later call stays allocated until the context is destroyed: scenes uploaded and
+ * photon maps built with it keep using it. */
 int liar_gpu_set_recovery(liar_gpu_ctx* ctx, const float* wavelengths, int n_wavelengths, const float* xy,
                           const float* spectra, int n_samples, const int32_t* triangles, int n_triangles);
 /* The blend of each of n XYZ colours (d_xyz: n x 3): sample indices (n x 3, -1 = none) and weights

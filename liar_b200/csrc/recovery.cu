@@ -19,6 +19,7 @@ struct RecoveryTable {
     void* mem = nullptr;
     DRecovery d{};
     bool set = false;
+    std::vector<void*> retired;  // replaced tables, still read by the scenes and maps built with them
 };
 
 RecoveryTable* recovery_table(liar_gpu_ctx* ctx) {
@@ -28,6 +29,7 @@ RecoveryTable* recovery_table(liar_gpu_ctx* ctx) {
     ctx->extensions.emplace_back("recovery", t);
     ctx->on_destroy.push_back([t]() {
         if (t->mem) cudaFree(t->mem);
+        for (void* p : t->retired) cudaFree(p);
         delete t;
     });
     return t;
@@ -130,11 +132,9 @@ extern "C" int liar_gpu_set_recovery(liar_gpu_ctx* ctx, const float* wavelengths
     if (rc) return rc;
     RecoveryTable* T = recovery_table(ctx);
     if (T->mem) {
-        cudaError_t e = cudaStreamSynchronize(ctx->stream);
-        if (e == cudaSuccess) e = cudaFree(T->mem);
+        T->retired.push_back(T->mem);
         T->mem = nullptr;
         T->set = false;
-        if (e != cudaSuccess) return ctx_cuda(ctx, e, "recovery table");
     }
     const size_t nw = (size_t)n_wavelengths, ns = (size_t)n_samples;
     const size_t sizes[7] = {nw * 4, ns * nw * 4, ns * 4, pts.size() * 4, (size_t)n_triangles * 12, first.size() * 4,

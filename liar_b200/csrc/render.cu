@@ -30,6 +30,10 @@
 #include "photon_mapper.h"
 #include "render_dev.cuh"
 
+namespace liar_gpu {
+const DRecovery* ctx_recovery(liar_gpu_ctx* ctx);  // recovery.cu
+}
+
 using namespace liar_gpu;
 using namespace liar_gpu::rt;
 
@@ -422,6 +426,7 @@ extern "C" int liar_gpu_scene_upload(liar_gpu_ctx* ctx, const liar_scene_desc* d
     std::vector<int> tex_depth(D.n_textures, 0);  // 0: not visited, -1: being visited, else its depth
     const char* tex_err = nullptr;
     int tex_bad = -1;
+    bool has_images = false;
     std::function<int(int, int)> depth_of = [&](int t, int level) -> int {
         if (t < 0 || (size_t)t >= D.n_textures) return tex_err = "child out of range", -1;
         if (tex_depth[t] > 0) return tex_depth[t];
@@ -431,6 +436,13 @@ extern "C" int liar_gpu_scene_upload(liar_gpu_ctx* ctx, const liar_scene_desc* d
         int d = 0;
         if (T.type == LIAR_TEX_CONSTANT) {
             if (T.spectrum < 0 || T.spectrum >= (int32_t)D.n_spectra) return tex_err = "spectrum out of range", tex_bad = t, -1;
+            d = 1;
+        } else if (T.type == LIAR_TEX_IMAGE) {
+            if (T.a <= 0 || T.b <= 0 || T.pixels < 0 || !D.texture_pixels ||
+                (uint64_t)T.pixels + (uint64_t)T.a * (uint64_t)T.b > (uint64_t)D.n_texture_pixels)
+                return tex_err = "image pixels out of range", tex_bad = t, -1;
+            if (!(T.p[0] == 0.0f || T.p[0] == 1.0f)) return tex_err = "image filter must be 0 or 1", tex_bad = t, -1;
+            has_images = true;
             d = 1;
         } else if (T.type == LIAR_TEX_CHECKER || T.type == LIAR_TEX_GRID || T.type == LIAR_TEX_UV_TRANSFORM) {
             tex_depth[t] = -1;
@@ -447,6 +459,9 @@ extern "C" int liar_gpu_scene_upload(liar_gpu_ctx* ctx, const liar_scene_desc* d
     };
     for (size_t k = 0; k < D.n_textures; ++k)
         if (depth_of((int)k, 1) < 0) return ctx_fail(ctx, LIAR_ERR_INVALID, "texture %d: %s", tex_bad < 0 ? (int)k : tex_bad, tex_err);
+    const DRecovery* rec = has_images ? ctx_recovery(ctx) : nullptr;
+    if (has_images && !rec)
+        return ctx_fail(ctx, LIAR_ERR_INVALID, "image textures need the context's recovery table (liar_gpu_set_recovery)");
     std::vector<float> spec_max(D.n_spectra, 0.0f);
     for (size_t k = 0; k < D.n_spectra; ++k) {
         const liar_spectrum& s = D.spectra[k];
@@ -561,6 +576,12 @@ extern "C" int liar_gpu_scene_upload(liar_gpu_ctx* ctx, const liar_scene_desc* d
     }
     if (!rc && D.triangle_uvs) rc = upload(ctx, s, D.triangle_uvs, 6 * D.n_triangles, &d.tri_uv, "triangle uvs");
     if (!rc) rc = upload(ctx, s, D.textures, D.n_textures, &d.texs, "textures");
+    if (!rc && has_images) {
+        const float* px = nullptr;
+        rc = upload(ctx, s, D.texture_pixels, 4 * D.n_texture_pixels, &px, "texture pixels");
+        d.tex_pixels = reinterpret_cast<const float4*>(px);
+        d.rec = *rec;
+    }
     if (!rc) rc = upload(ctx, s, D.object_material, D.n_objects, &d.obj_mat, "object materials");
     if (!rc) rc = upload(ctx, s, D.object_light, D.n_objects, &d.obj_light, "object lights");
     if (!rc) rc = upload(ctx, s, D.materials, D.n_materials, &d.mats, "materials");

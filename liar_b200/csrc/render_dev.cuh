@@ -21,6 +21,7 @@
 #include <stdint.h>
 
 #include "../../include/liar_gpu.h"
+#include "recovery.cuh"
 #include "qbvh.h"
 #include "tri_exact.h"
 
@@ -88,6 +89,8 @@ struct DScene {
     const liar_texture* texs;    // optional texture nodes
     int n_tex;
     const float* tri_uv;         // optional, per triangle 3 x (u, v)
+    const float4* tex_pixels;    // image textures' XYZ pixels
+    DRecovery rec;               // the recovery of image pixels (set when the scene has images)
 };
 
 // ---- spectra
@@ -706,6 +709,37 @@ __device__ inline HitContext hit_context(const DScene& S, float3 o, float3 d, ui
     return H;
 }
 
+// Image::lookUp at mip level 0 (textures/image.cpp:654-718, 598-609): (u, 1 - v) over the
+// pixels with wrap-around, nearest or bilinear between pixel centres; the indices are clamped
+// where float rounding puts a wrapped coordinate on the image's far edge
+__device__ inline float3 image_lookup(const DScene& S, const liar_texture& T, float u, float v) {
+    const int nx = T.a, ny = T.b;
+    const float4* px = S.tex_pixels + T.pixels;
+    const float fx = (float)nx, fy = (float)ny;
+    if (T.p[0] == 0.0f) {
+        int x0 = (int)floorf((u - floorf(u)) * fx);
+        const float w = 1.0f - v;
+        int y0 = (int)floorf((w - floorf(w)) * fy);
+        x0 = min(max(x0, 0), nx - 1);
+        y0 = min(max(y0, 0), ny - 1);
+        const float4 p = px[(size_t)y0 * nx + x0];
+        return make_float3(p.x, p.y, p.z);
+    }
+    float x = u * fx - 0.5f, y = (1.0f - v) * fy - 0.5f;
+    x -= floorf(x / fx) * fx;  // num::mod into [0, n)
+    y -= floorf(y / fy) * fy;
+    const float x0 = floorf(x), y0 = floorf(y);
+    const float dx = x - x0, dy = y - y0;
+    const int i0 = min(max((int)x0, 0), nx - 1), j0 = min(max((int)y0, 0), ny - 1);
+    const int i1 = i0 + 1 == nx ? 0 : i0 + 1, j1 = j0 + 1 == ny ? 0 : j0 + 1;
+    const float4 p00 = px[(size_t)j0 * nx + i0], p10 = px[(size_t)j0 * nx + i1];
+    const float4 p01 = px[(size_t)j1 * nx + i0], p11 = px[(size_t)j1 * nx + i1];
+    const float ex = 1.0f - dx, ey = 1.0f - dy;
+    return make_float3((p00.x * ex + p10.x * dx) * ey + (p01.x * ex + p11.x * dx) * dy,
+                       (p00.y * ex + p10.y * dx) * ey + (p01.y * ex + p11.y * dx) * dy,
+                       (p00.z * ex + p10.z * dx) * ey + (p01.z * ex + p11.z * dx) * dy);
+}
+
 // Texture::lookUp of a tree of uv textures: the transforms move (u, v), the boards pick a child
 // (without anti-aliasing a board always picks one), the leaf is a spectrum
 __device__ inline float texture_eval(const DScene& S, int t, float u, float v, float lam, bool reflectant) {
@@ -730,6 +764,13 @@ __device__ inline float texture_eval(const DScene& S, int t, float u, float v, f
                 v = nv;
                 t = T.a;
                 break;
+            }
+            case LIAR_TEX_IMAGE: {
+                // Image::doLookUp: Spectral::fromXYZ of the looked-up colour
+                const float3 c = image_lookup(S, T, u, v);
+                RecoveryBlend b;
+                if (!recovery_locate(S.rec, c.x, c.y, c.z, b)) return 0.0f;
+                return recovery_eval(S.rec, b, lam, reflectant);
             }
             default:
                 return spec_eval(S, T.spectrum, lam, reflectant);

@@ -31,7 +31,8 @@ class CMaterial(C.Structure):
 
 
 class CTexture(C.Structure):
-    _fields_ = [("type", C.c_int32), ("a", C.c_int32), ("b", C.c_int32), ("spectrum", C.c_int32), ("p", C.c_float * 6)]
+    _fields_ = [("type", C.c_int32), ("a", C.c_int32), ("b", C.c_int32), ("spectrum", C.c_int32), ("p", C.c_float * 6),
+                ("pixels", C.c_int64)]
 
 
 class CLight(C.Structure):
@@ -51,7 +52,8 @@ class CSceneDesc(C.Structure):
                 ("materials", _P), ("n_materials", _S), ("spectra", _P), ("n_spectra", _S),
                 ("spectrum_pool", _P), ("pool_size", _S), ("lights", _P), ("n_lights", _S),
                 ("observer", _P), ("n_observer", _S), ("scene_radius", C.c_float),
-                ("textures", _P), ("n_textures", _S), ("triangle_uvs", _P)]
+                ("textures", _P), ("n_textures", _S), ("triangle_uvs", _P),
+                ("texture_pixels", _P), ("n_texture_pixels", _S)]
 
 
 class CCamera(C.Structure):
@@ -81,7 +83,7 @@ class CRenderDesc(C.Structure):
 FILTER_BOX, FILTER_TRIANGLE, FILTER_MITCHELL = 0, 1, 2
 
 
-TEX_CONSTANT, TEX_CHECKER, TEX_GRID, TEX_UV_TRANSFORM = range(4)
+TEX_CONSTANT, TEX_CHECKER, TEX_GRID, TEX_UV_TRANSFORM, TEX_IMAGE = range(5)
 SPEC_CONSTANT, SPEC_SAMPLED, SPEC_BLACKBODY, SPEC_CAUCHY = 0, 1, 2, 3
 MAT_NONE, MAT_LAMBERT, MAT_CONDUCTOR, MAT_COOK_TORRANCE, MAT_DIELECTRIC, MAT_WALTER, MAT_MIRROR = range(7)
 LIGHT_PARA, LIGHT_MESH, LIGHT_POINT, LIGHT_SKY = 0, 1, 2, 3
@@ -104,6 +106,7 @@ class FlatScene:
     scene_radius: float
     textures: C.Array | None = None
     triangle_uvs: np.ndarray | None = None  # n_triangles x 3 x 2, when a texture needs them
+    texture_pixels: np.ndarray | None = None  # image textures' pixels, n x 4 (X, Y, Z, 0)
     keep: list = field(default_factory=list)
 
     def desc(self) -> CSceneDesc:
@@ -136,6 +139,9 @@ class FlatScene:
             d.n_textures = len(self.textures)
         if self.triangle_uvs is not None:
             d.triangle_uvs = self.triangle_uvs.ctypes.data
+        if self.texture_pixels is not None:
+            d.texture_pixels = self.texture_pixels.ctypes.data
+            d.n_texture_pixels = self.texture_pixels.shape[0]
         return d
 
 
@@ -149,6 +155,7 @@ class _Builder:
         self.spectra, self.spec_ids, self.pool = [], {}, []
         self.lights = []
         self.textures, self.tex_ids = [], {}
+        self.tex_pixels, self.n_tex_pixels = [], 0
         self.tri_uvs = []  # per object: n x 3 x 2 corner uvs, or None for the barycentric ones
         self.M = None  # current local-to-world affine matrix (None: identity)
 
@@ -215,6 +222,17 @@ class _Builder:
         elif isinstance(t, tx.GridBoard):
             rec.type = TEX_GRID
             rec.p[0], rec.p[1] = t.thickness[0] / 2, t.thickness[1] / 2  # GridBoard's halfThickness
+        elif isinstance(t, tx.Image):
+            t.warn_if_filtered()
+            h, w = t.xyz.shape[:2]
+            rec.type = TEX_IMAGE
+            rec.a, rec.b = w, h
+            rec.p[0] = 0.0 if t.antiAliasing == "none" else 1.0
+            rec.pixels = self.n_tex_pixels
+            px = np.zeros((h * w, 4), np.float32)
+            px[:, :3] = t.xyz.reshape(-1, 3)
+            self.tex_pixels.append(px)
+            self.n_tex_pixels += h * w
         elif isinstance(t, tx.TransformationUv):
             rec.type = TEX_UV_TRANSFORM
             m = t.transformation
@@ -419,6 +437,7 @@ class _Builder:
             scene_radius=radius,
             textures=(CTexture * len(self.textures))(*self.textures) if self.textures else None,
             triangle_uvs=self.triangle_uvs(),
+            texture_pixels=np.ascontiguousarray(np.concatenate(self.tex_pixels)) if self.tex_pixels else None,
         )
 
     def triangle_uvs(self) -> np.ndarray | None:
@@ -527,12 +546,12 @@ class GpuScene:
         for name, (res, args) in _RENDER_SIGS.items():
             fn = getattr(lib, name)
             fn.restype, fn.argtypes = res, args
+        from .recovery import set_standard_on
+        set_standard_on(ctx)  # Spectral::fromXYZ of image textures and of the PhotonMapper's photons
         h = C.c_void_p()
         d = flat.desc()
         ctx.check(lib.liar_gpu_scene_upload(ctx.handle, C.byref(d), C.byref(h)))
         self.handle = h
-        from .recovery import set_standard_on
-        set_standard_on(ctx)  # the PhotonMapper's Spectral::fromXYZ
 
     def close(self):
         if getattr(self, "handle", None):

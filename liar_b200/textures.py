@@ -1,9 +1,9 @@
 """Textures of the scene API (``liar.textures``, src/liar/textures/).
 
 On the GPU path: Constant (textures/constant.cpp), a spectrum or a number; and the uv textures
-CheckerBoard (checker_board.cpp), GridBoard (grid_board.cpp) and TransformationUv
-(transformation_uv.cpp), which pick or move between other textures by the hit's (u, v)
-coordinates. A material parameter that is a uv texture becomes a tree of liar_texture nodes
+CheckerBoard (checker_board.cpp), GridBoard (grid_board.cpp), TransformationUv
+(transformation_uv.cpp) and Image (image.cpp), which pick, move between or look up colours by
+the hit's (u, v) coordinates. A material parameter that is a uv texture becomes a tree of liar_texture nodes
 (include/liar_gpu.h) that the kernels walk at every hit; emission and roughness slots take
 constant textures only."""
 from __future__ import annotations
@@ -152,8 +152,97 @@ class TransformationUv(UnaryOperator):
         self._matrix = as_matrix2d(value)
 
 
+class Image(Texture):
+    """Image(path[, antiAliasing, mipMapping][, rgbSpace]) (textures/image.cpp): the picture read
+    as XYZ (codecs.read) and looked up at (u, 1 - v) with wrap-around; its colour becomes a
+    spectrum through the standard recovery (Spectral::fromXYZ).
+
+    antiAliasing "none" takes the nearest pixel, "bilinear" blends the four around. "trilinear"
+    (the reference's default) and mip-mapping blend mip levels chosen by the ray differentials'
+    footprint, which this path does not carry: with a zero footprint the reference's lookup is the
+    bilinear one at level 0 (image.cpp:279-356, mipMapLevel), which is what is rendered."""
+
+    AA_NONE, AA_BILINEAR, AA_TRILINEAR = "none", "bilinear", "trilinear"
+    MM_NONE, MM_ISOTROPIC, MM_ANISOTROPIC = "none", "isotropic", "anisotropic"
+    _default_aa = "trilinear"
+    _default_mm = "anisotropic"
+    _warned = False
+
+    def __init__(self, path=None, *args):
+        aa, mm, space = Image._default_aa, Image._default_mm, None
+        if len(args) == 1:
+            space = args[0]
+        elif len(args) >= 2:
+            aa, mm = args[0], args[1]
+            space = args[2] if len(args) > 2 else None
+        self.antiAliasing = aa
+        self.mipMapping = mm
+        self.filename = None
+        self.rgbSpace = None
+        self.xyz = None
+        if path is not None:
+            self.loadFile(path, space)
+
+    def loadFile(self, path, rgbSpace=None):
+        from . import codecs
+        xyza, space = codecs.read(path, rgbSpace)
+        if xyza.shape[0] == 0 or xyza.shape[1] == 0:
+            raise ValueError("bad image resolution")
+        self.filename, self.rgbSpace = str(path), space
+        self.xyz = np.ascontiguousarray(xyza[..., :3], dtype=np.float32)
+
+    @classmethod
+    def from_xyz(cls, xyz, antiAliasing="bilinear"):
+        """An image texture of XYZ pixels (H, W, 3), row 0 at the top."""
+        t = cls(None, antiAliasing, "none")
+        t.xyz = np.ascontiguousarray(np.asarray(xyz, dtype=np.float32).reshape(*np.shape(xyz)[:2], 3))
+        return t
+
+    @property
+    def resolution(self):
+        return (self.xyz.shape[1], self.xyz.shape[0]) if self.xyz is not None else (0, 0)
+
+    @property
+    def antiAliasing(self) -> str:
+        return self._aa
+
+    @antiAliasing.setter
+    def antiAliasing(self, mode):
+        mode = str(mode).lower()
+        if mode not in (self.AA_NONE, self.AA_BILINEAR, self.AA_TRILINEAR):
+            raise KeyError(f"antiAliasing must be 'none', 'bilinear' or 'trilinear', not {mode!r}")
+        self._aa = mode
+
+    @property
+    def mipMapping(self) -> str:
+        return self._mm
+
+    @mipMapping.setter
+    def mipMapping(self, mode):
+        mode = str(mode).lower()
+        if mode not in (self.MM_NONE, self.MM_ISOTROPIC, self.MM_ANISOTROPIC):
+            raise KeyError(f"mipMapping must be 'none', 'isotropic' or 'anisotropic', not {mode!r}")
+        self._mm = mode
+
+    @staticmethod
+    def setDefaultAntiAliasing(mode):
+        Image._default_aa = str(mode).lower()
+
+    @staticmethod
+    def setDefaultMipMapping(mode):
+        Image._default_mm = str(mode).lower()
+
+    def warn_if_filtered(self):
+        if self.xyz is None:
+            raise ValueError("Image texture has no pixels (loadFile first)")
+        if self._aa == self.AA_TRILINEAR and not Image._warned:
+            Image._warned = True
+            warnings.warn("Image antiAliasing 'trilinear' is rendered as 'bilinear' at mip level 0 "
+                          "(no ray differentials on the GPU path)", stacklevel=4)
+
+
 def is_uv_texture(x) -> bool:
-    return isinstance(x, (CheckerBoard, GridBoard, TransformationUv))
+    return isinstance(x, (CheckerBoard, GridBoard, TransformationUv, Image))
 
 
 def warn_point_lookup(tex: CheckerBoard):

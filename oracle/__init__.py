@@ -99,6 +99,17 @@ class RenderScene:
         L.oracle_render.restype = C.c_int
         L.oracle_render.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_int]
         self.h = L.oracle_scene_create(C.addressof(self._desc))
+        if getattr(flat, "texture_pixels", None) is not None:
+            # image textures turn their colours into spectra with the standard recovery
+            from liar_b200.recovery import device_table
+            t = device_table()
+            self._rec = t
+            L.oracle_scene_set_recovery.restype = None
+            L.oracle_scene_set_recovery.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
+                                                    C.c_void_p, C.c_int]
+            L.oracle_scene_set_recovery(self.h, t["wavelengths"].ctypes.data, t["wavelengths"].size,
+                                        t["points"].ctypes.data, t["spectra"].ctypes.data, t["spectra"].shape[0],
+                                        t["triangles"].ctypes.data, t["triangles"].shape[0])
 
     def render(self, desc, film=None, pixels=None, threads=0):
         """Adds desc.spp samples of pixels [begin, end) (all by default) to film (H, W, 8)."""

@@ -67,6 +67,7 @@ struct Material {
 struct Texture {
     int32_t type, a, b, spectrum;
     float p[6];
+    int64_t pixels;
 };
 struct Light {
     int32_t type, spectrum, object, double_sided;
@@ -95,6 +96,7 @@ struct SceneIn {
     float scene_radius;
     const Texture* textures; uint64_t n_textures;
     const float* triangle_uvs;
+    const float* texture_pixels; uint64_t n_texture_pixels;
 };
 struct RenderIn {
     Camera camera;
@@ -122,7 +124,9 @@ static_assert(sizeof(Spectrum) == sizeof(liar_spectrum) && sizeof(Material) == s
 static_assert(offsetof(Material, tex) == offsetof(liar_material, tex) &&
                   offsetof(SceneIn, triangle_uvs) == offsetof(liar_scene_desc, triangle_uvs) &&
                   offsetof(RenderIn, pm_max_photons) == offsetof(liar_render_desc, photon_mapper) &&
-                  offsetof(RenderIn, filter) == offsetof(liar_render_desc, filter),
+                  offsetof(RenderIn, filter) == offsetof(liar_render_desc, filter) &&
+                  offsetof(Texture, pixels) == offsetof(liar_texture, pixels) &&
+                  offsetof(SceneIn, texture_pixels) == offsetof(liar_scene_desc, texture_pixels),
               "oracle mirrors out of step with include/liar_gpu.h");
 
 // The photon maps of a PhotonMapper render (photon_mapper.cpp:798-835) as the oracle gets them:
@@ -218,8 +222,21 @@ const uint32_t D_SCREEN = 0, D_LENS = 2, D_LAMBDA = 4, D_GEN0 = 8, D_PER_GEN = 8
 const uint32_t O_STRAT = 0, O_BSDF = 1, O_COMP = 3, O_LCHOICE = 4, O_LIGHT = 5, O_RR = 7;
 
 // ---- scene
+// a recovery table (RecoveryMengSimon, recovery_meng_simon.cpp:93-310): spectra at chromaticity
+// points, the triangulation of the points and the four box corners that follow them
+struct RecView {
+    const float* wavelengths = nullptr;
+    const float* spectra = nullptr;
+    const float* points = nullptr;   // (ns + 4) x 2
+    const int32_t* tris = nullptr;
+    int nw = 0, ns = 0, nt = 0;
+};
+
 struct Scene {
     SceneIn in;
+    RecView rec;                     // for image textures (Spectral::fromXYZ)
+    std::vector<float> rec_w, rec_s, rec_p;
+    std::vector<int32_t> rec_t;
     void* tree = nullptr;
     std::vector<float> spec_max, light_cdf, light_area, tri_cdf;
     std::vector<float> ow, oxyz, odxyz, ocdf;
@@ -665,6 +682,91 @@ void hit_uv(const Scene& S, uint32_t prim, float bu, float bv, float& u, float& 
 
 float frac(float x) { return x - std::floor(x); }
 
+// RecoveryMengSimon::Impl::recover by a search of every triangle: blend of XYZ (three sample
+// indices, -1 for a box corner, and weights scaled to X + Y + Z), false when there is none
+bool rec_locate(const RecView& R, float X, float Y, float Z, int32_t idx[3], float w[3]) {
+    const float s = X + Y + Z;
+    if (s == 0.0f || R.nt == 0) return false;
+    const float x = X / s, y = Y / s;
+    if (!(x >= -0.3f && x <= 1.0f && y >= -0.3f && y <= 1.2f)) return false;
+    int best = -1;
+    float bw[3] = {0, 0, 0}, best_min = -INFINITY;
+    for (int t = 0; t < R.nt; ++t) {
+        const int i0 = R.tris[3 * t], i1 = R.tris[3 * t + 1], i2 = R.tris[3 * t + 2];
+        const float ax = R.points[2 * i0], ay = R.points[2 * i0 + 1];
+        const float bx = R.points[2 * i1], by = R.points[2 * i1 + 1];
+        const float qx = R.points[2 * i2], qy = R.points[2 * i2 + 1];
+        const float det = (bx - ax) * (qy - ay) - (qx - ax) * (by - ay);
+        if (det == 0.0f) continue;
+        const float w1 = ((x - ax) * (qy - ay) - (qx - ax) * (y - ay)) / det;
+        const float w2 = ((bx - ax) * (y - ay) - (x - ax) * (by - ay)) / det;
+        const float w0 = 1.0f - w1 - w2;
+        const float mn = std::min(w0, std::min(w1, w2));
+        if (mn > best_min) {
+            best_min = mn;
+            best = t;
+            bw[0] = w0;
+            bw[1] = w1;
+            bw[2] = w2;
+        }
+    }
+    if (best < 0) return false;
+    float wtot = 0;
+    for (int j = 0; j < 3; ++j) {
+        const int i = R.tris[3 * best + j];
+        idx[j] = i < R.ns ? i : -1;
+        if (idx[j] < 0) bw[j] = 0;
+        wtot += bw[j];
+    }
+    if (wtot == 0) return false;
+    for (int j = 0; j < 3; ++j) w[j] = bw[j] * (s / wtot);
+    return true;
+}
+
+// RecoveryMengSimon::doRecover (Single mode) at lam: the blend interpolated between the table's
+// wavelengths; as a reflectance divided by the blend of the spectra's maxima when that exceeds 1
+float rec_eval(const RecView& R, const int32_t idx[3], const float w[3], float lam, bool reflectant) {
+    const float* ws = R.wavelengths;
+    const int k = (int)(std::upper_bound(ws, ws + R.nw, lam) - ws);
+    if (k == 0 || k == R.nw) return 0.0f;
+    const float t = (lam - ws[k - 1]) / (ws[k] - ws[k - 1]);
+    float v0 = 0, v1 = 0, mx = 0;
+    for (int j = 0; j < 3; ++j) {
+        if (idx[j] < 0) continue;
+        const float* sp = R.spectra + (size_t)idx[j] * R.nw;
+        v0 += w[j] * sp[k - 1];
+        v1 += w[j] * sp[k];
+        mx += w[j] * *std::max_element(sp, sp + R.nw);
+    }
+    const float v = v0 + t * (v1 - v0);
+    return reflectant && mx > 1.0f ? v / mx : v;
+}
+
+// Image::lookUp at mip level 0 (textures/image.cpp:598-609 nearest, 690-713 bilinear): (u, 1 - v)
+// over the pixels with wrap-around; indices clamped where rounding lands on the far edge
+void image_lookup(const Scene& S, const Texture& T, float u, float v, float out[3]) {
+    const int nx = T.a, ny = T.b;
+    const float* px = S.in.texture_pixels + 4 * T.pixels;
+    if (T.p[0] == 0.0f) {
+        int x0 = (int)std::floor(frac(u) * (float)nx), y0 = (int)std::floor(frac(1.0f - v) * (float)ny);
+        x0 = std::min(std::max(x0, 0), nx - 1);
+        y0 = std::min(std::max(y0, 0), ny - 1);
+        for (int c = 0; c < 3; ++c) out[c] = px[4 * ((size_t)y0 * nx + x0) + c];
+        return;
+    }
+    float x = u * (float)nx - 0.5f, y = (1.0f - v) * (float)ny - 0.5f;
+    x -= std::floor(x / (float)nx) * (float)nx;
+    y -= std::floor(y / (float)ny) * (float)ny;
+    const float x0 = std::floor(x), y0 = std::floor(y), dx = x - x0, dy = y - y0;
+    const int i0 = std::min(std::max((int)x0, 0), nx - 1), j0 = std::min(std::max((int)y0, 0), ny - 1);
+    const int i1 = (i0 + 1) % nx, j1 = (j0 + 1) % ny;
+    for (int c = 0; c < 3; ++c) {
+        const float p00 = px[4 * ((size_t)j0 * nx + i0) + c], p10 = px[4 * ((size_t)j0 * nx + i1) + c];
+        const float p01 = px[4 * ((size_t)j1 * nx + i0) + c], p11 = px[4 * ((size_t)j1 * nx + i1) + c];
+        out[c] = (p00 * (1 - dx) + p10 * dx) * (1 - dy) + (p01 * (1 - dx) + p11 * dx) * dy;
+    }
+}
+
 // Texture::lookUp of the uv textures (src/liar/textures/): TransformationUv moves the context's uv
 // (transformation_uv.cpp:67-70), CheckerBoard without anti-aliasing picks A where the fractional u
 // and v lie on the same side of the split (checker_board.cpp:113-124, 149-157), GridBoard picks A
@@ -683,6 +785,14 @@ float texture(const Scene& S, int t, float u, float v, float lam, bool reflectan
             u = nu;
             v = nv;
             t = T.a;
+        } else if (T.type == 4) {
+            // Image::doLookUp: Spectral::fromXYZ of the colour
+            float c[3];
+            image_lookup(S, T, u, v, c);
+            int32_t idx[3];
+            float w[3];
+            if (!rec_locate(S.rec, c[0], c[1], c[2], idx, w)) return 0;
+            return rec_eval(S.rec, idx, w, lam, reflectant);
         } else {
             return spectrum(S, T.spectrum, lam, reflectant);
         }
@@ -983,60 +1093,23 @@ struct DLPath {
 
 // ---- PhotonMapper estimates (photon_mapper.cpp:1254-1381)
 
-// RecoveryMengSimon::Impl::recover by a search of every triangle: blend of XYZ, false when none
-bool pm_locate(const PmIn& pm, float X, float Y, float Z, int32_t idx[3], float w[3]) {
-    const float s = X + Y + Z;
-    if (s == 0.0f) return false;
-    const float x = X / s, y = Y / s;
-    if (!(x >= -0.3f && x <= 1.0f && y >= -0.3f && y <= 1.2f)) return false;
-    int best = -1;
-    float bw[3] = {0, 0, 0}, best_min = -INFINITY;
-    for (int t = 0; t < pm.rec_nt; ++t) {
-        const int i0 = pm.rec_tris[3 * t], i1 = pm.rec_tris[3 * t + 1], i2 = pm.rec_tris[3 * t + 2];
-        const float ax = pm.rec_points[2 * i0], ay = pm.rec_points[2 * i0 + 1];
-        const float bx = pm.rec_points[2 * i1], by = pm.rec_points[2 * i1 + 1];
-        const float qx = pm.rec_points[2 * i2], qy = pm.rec_points[2 * i2 + 1];
-        const float det = (bx - ax) * (qy - ay) - (qx - ax) * (by - ay);
-        if (det == 0.0f) continue;
-        const float w1 = ((x - ax) * (qy - ay) - (qx - ax) * (y - ay)) / det;
-        const float w2 = ((bx - ax) * (y - ay) - (x - ax) * (by - ay)) / det;
-        const float w0 = 1.0f - w1 - w2;
-        const float mn = std::min(w0, std::min(w1, w2));
-        if (mn > best_min) {
-            best_min = mn;
-            best = t;
-            bw[0] = w0;
-            bw[1] = w1;
-            bw[2] = w2;
-        }
-    }
-    if (best < 0) return false;
-    float wtot = 0;
-    for (int j = 0; j < 3; ++j) {
-        const int i = pm.rec_tris[3 * best + j];
-        idx[j] = i < pm.rec_ns ? i : -1;
-        if (idx[j] < 0) bw[j] = 0;
-        wtot += bw[j];
-    }
-    if (wtot == 0) return false;
-    for (int j = 0; j < 3; ++j) w[j] = bw[j] * (s / wtot);
-    return true;
+RecView pm_rec(const PmIn& pm) {
+    RecView R;
+    R.wavelengths = pm.rec_wavelengths;
+    R.spectra = pm.rec_spectra;
+    R.points = pm.rec_points;
+    R.tris = pm.rec_tris;
+    R.nw = pm.rec_nw;
+    R.ns = pm.rec_ns;
+    R.nt = pm.rec_nt;
+    return R;
 }
-
-// RecoveryMengSimon::doRecover at lam, as an illuminant
+bool pm_locate(const PmIn& pm, float X, float Y, float Z, int32_t idx[3], float w[3]) {
+    return rec_locate(pm_rec(pm), X, Y, Z, idx, w);
+}
+// Spectral::fromXYZ as an illuminant
 float pm_recover(const PmIn& pm, const int32_t idx[3], const float w[3], float lam) {
-    const float* ws = pm.rec_wavelengths;
-    const int k = (int)(std::upper_bound(ws, ws + pm.rec_nw, lam) - ws);
-    if (k == 0 || k == pm.rec_nw) return 0.0f;
-    const float t = (lam - ws[k - 1]) / (ws[k] - ws[k - 1]);
-    float v0 = 0, v1 = 0;
-    for (int j = 0; j < 3; ++j) {
-        if (idx[j] < 0) continue;
-        const float* sp = pm.rec_spectra + (size_t)idx[j] * pm.rec_nw;
-        v0 += w[j] * sp[k - 1];
-        v1 += w[j] * sp[k];
-    }
-    return v0 + t * (v1 - v0);
+    return rec_eval(pm_rec(pm), idx, w, lam, false);
 }
 
 // KdTree::rangeSearch(point, rMax, kMax): the k nearest photons with d^2 < rMax^2, by brute force
@@ -1357,6 +1430,24 @@ float dl_cast(DLPath& P, V o, V d, float tmin, float tmax, int gen, bool hq, uin
 }  // namespace
 
 extern "C" {
+
+// the recovery table of image textures (copied): wavelengths, chromaticity points of the samples
+// and the box corners after them, spectra, triangles
+void oracle_scene_set_recovery(void* scene, const float* wavelengths, int nw, const float* points, const float* spectra,
+                               int ns, const int32_t* tris, int nt) {
+    Scene* S = static_cast<Scene*>(scene);
+    S->rec_w.assign(wavelengths, wavelengths + nw);
+    S->rec_p.assign(points, points + 2 * (size_t)(ns + 4));
+    S->rec_s.assign(spectra, spectra + (size_t)ns * nw);
+    S->rec_t.assign(tris, tris + 3 * (size_t)nt);
+    S->rec.wavelengths = S->rec_w.data();
+    S->rec.points = S->rec_p.data();
+    S->rec.spectra = S->rec_s.data();
+    S->rec.tris = S->rec_t.data();
+    S->rec.nw = nw;
+    S->rec.ns = ns;
+    S->rec.nt = nt;
+}
 
 void* oracle_scene_create(const SceneIn* in) {
     Scene* S = new Scene();

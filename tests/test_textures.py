@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 import oracle
-from liar_b200 import cameras, render as R, scenery, shaders, spectra, textures as tx, tracers
+from liar_b200 import cameras, output, render as R, scenery, shaders, spectra, textures as tx, tracers
 
 
 def test_checker_tree_is_flattened_once_per_node():
@@ -148,3 +148,59 @@ def test_oracle_grid_board_lines():
     assert Y[h // 2 - 1:h // 2 + 1, :].mean() == pytest.approx(0.9, rel=0.05)    # the line y = 0.5
     assert Y[:, w // 2 - 1:w // 2 + 1].mean() == pytest.approx(0.9, rel=0.05)    # the line x = 0.5
     assert Y[4:10, 6:12].mean() == pytest.approx(0.1, rel=0.1)                    # inside a cell
+
+
+def _grey_xyz(levels):
+    """XYZ of equal-energy greys (x = y = 1/3) of the given luminances."""
+    lv = np.asarray(levels, dtype=np.float32)
+    return np.stack([lv, lv, lv], axis=-1)
+
+
+def test_image_texture_is_flattened_into_the_pixel_pool(tmp_path):
+    a = tx.Image.from_xyz(_grey_xyz([[0.2, 0.4, 0.3], [0.6, 0.8, 0.5]]), antiAliasing="none")
+    b = tx.Image.from_xyz(_grey_xyz([[0.1], [0.9]]))
+    p = scenery.Parallelogram((0, 0, 0), (1, 0, 0), (0, 1, 0))
+    p.shader = shaders.Lambert(a)
+    q = scenery.Parallelogram((0, 0, 1), (1, 0, 0), (0, 1, 0))
+    q.shader = shaders.Lambert(tx.TransformationUv(b, [[2, 0, 0], [0, 1, 0], [0, 0, 1]]))
+    flat = R.flatten(scenery.List([p, q]))
+    T = list(flat.textures)
+    ia = T[flat.materials[0].tex[0]]
+    ib = T[T[flat.materials[1].tex[0]].a]
+    assert (ia.type, ia.a, ia.b, ia.pixels, ia.p[0]) == (R.TEX_IMAGE, 3, 2, 0, 0.0)
+    assert (ib.type, ib.a, ib.b, ib.pixels, ib.p[0]) == (R.TEX_IMAGE, 1, 2, 6, 1.0)
+    assert flat.texture_pixels.shape == (8, 4)
+    np.testing.assert_array_equal(flat.texture_pixels[:6, 1], np.float32([0.2, 0.4, 0.3, 0.6, 0.8, 0.5]))
+    # a file is read in its codec's colour space
+    img = output.Image(str(tmp_path / "t.pfm"), (3, 2))
+    img.exposureStops = 0.0
+    xyza = np.concatenate([_grey_xyz([[0.2, 0.4, 0.3], [0.6, 0.8, 0.5]]), np.ones((2, 3, 1), np.float32)], -1)
+    img.write(xyza, None)
+    t = tx.Image(str(tmp_path / "t.pfm"))
+    assert t.resolution == (3, 2) and t.antiAliasing == "trilinear" and t.rgbSpace.gamma == 1.0
+    np.testing.assert_allclose(t.xyz, xyza[..., :3], rtol=1e-5, atol=1e-6)
+    with pytest.warns(UserWarning, match="trilinear"):
+        tx.Image._warned = False
+        p.shader = shaders.Lambert(t)
+        R.flatten(p)
+
+
+@pytest.mark.parametrize("filter", ["none", "bilinear"])
+def test_oracle_image_quadrants(filter):
+    levels = np.array([[0.2, 0.7], [0.45, 0.1]], np.float32)
+    tex = tx.Image.from_xyz(_grey_xyz(levels), antiAliasing=filter)
+    scene, cam = _board_scene(tex)
+    t = tracers.DirectLighting()
+    t.maxRayGeneration = 1
+    w, h = 40, 30
+    img, _ = R.resolve(oracle.RenderScene(R.flatten(scene)).render(R.render_desc(cam, w, h, 16, t, seed=3)))
+    tl, tr, bl, br = _quadrants(img, w, h, band=5 if filter == "none" else 1)
+    if filter == "none":
+        # the image's top row at the top of the plane (v up), its pixels filling the quadrants
+        np.testing.assert_allclose((tl, tr, bl, br), levels.ravel(), rtol=0.05)
+    else:
+        # bilinear between pixel centres (u, v = 0.25, 0.75) with wrap-around: at the view's
+        # corners the nearest pixel dominates, in the middle all four blend equally
+        Y = img[..., 1]
+        assert Y[h // 2 - 1:h // 2 + 1, w // 2 - 1:w // 2 + 1].mean() == pytest.approx(levels.mean(), rel=0.05)
+        assert list(np.argsort([tl, tr, bl, br])) == list(np.argsort(levels.ravel()))

@@ -10,6 +10,7 @@ import oracle
 from liar_b200 import batch as B, cameras, photons, render as R, scenery, shaders, spectra, textures as tx, tracers
 from liar_b200._native import LiarGpuError
 from liar_b200.kernel import default_context
+from liar_b200.recovery import sRGB
 
 pytestmark = pytest.mark.gpu
 
@@ -33,15 +34,21 @@ def _scene():
     ct.roughness = tx.Constant(0.3)
     ball.shader = ct
     box = scenery.Box((0.3, 0, -0.5), (1.1, 0.8, 0.3))
-    box.shader = shaders.Lambert(tx.CheckerBoard(0.7, 0.15))
     mirrored = scenery.Transformation(box, [[-1, 0, 0, 0.6], [0, 1, 0, 0], [0, 0, 1, 0], [0, 0, 0, 1]])
+    rng = np.random.default_rng(11)
+    rgb = rng.uniform(0.05, 0.9, size=(5, 7, 3)).astype(np.float32)
+    photo = tx.Image.from_xyz(sRGB.linearSpace().toXYZlinear(rgb), antiAliasing="bilinear")
+    panel = scenery.Parallelogram((1.9, 0, -1.5), (0, 0, 3), (0, 2, 0))
+    panel.shader = shaders.Lambert(tx.TransformationUv(photo, [[2, 0, 0.1], [0, 1.5, 0], [0, 0, 1]]))
+    tiles = tx.Image.from_xyz(sRGB.linearSpace().toXYZlinear(rgb[:2, :3]), antiAliasing="none")
+    box.shader = shaders.Lambert(tiles)
     surf = scenery.Parallelogram((-0.5, 2.5, -0.5), (1, 0, 0), (0, 0, 1))
     light = scenery.LightArea(surf)
     light.radiance = spectra.BlackBody(5000, 20)
     cam = cameras.PerspectiveCamera()
     cam.position = (0, 1.5, -4)
     cam.lookAt((0, 0.8, 0))
-    return scenery.List([floor, back, ball, mirrored, light]), cam
+    return scenery.List([floor, back, ball, mirrored, panel, light]), cam
 
 
 def _within_3_sigma(g, c, min_fraction=0.99):
@@ -62,7 +69,7 @@ def textured():
         warnings.simplefilter("ignore")
         scene, cam = _scene()
         flat = R.flatten(scene)
-    assert flat.triangle_uvs is not None and len(flat.textures) >= 10
+    assert flat.triangle_uvs is not None and len(flat.textures) >= 10 and flat.texture_pixels is not None
     return flat, R.GpuScene(default_context(), flat), cam
 
 
@@ -131,6 +138,13 @@ def test_upload_refuses_bad_texture_trees():
         _upload(flat)
     flat = R.flatten(p)
     flat.materials[0].tex[0] = len(flat.textures)       # out of range
+    with pytest.raises(LiarGpuError):
+        _upload(flat)
+    img = tx.Image.from_xyz(np.full((2, 2, 3), 0.5, np.float32))
+    p.shader = shaders.Lambert(img)
+    flat = R.flatten(p)
+    _upload(flat)
+    flat.textures[flat.materials[0].tex[0]].pixels = 2     # runs past the pool's end
     with pytest.raises(LiarGpuError):
         _upload(flat)
     deep = tx.Constant(0.5)
