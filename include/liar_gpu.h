@@ -186,9 +186,18 @@ typedef struct liar_material {
  *                 scene's texture_pixels, looked up at (u, 1 - v) by nearest pixel (p[0] = 0) or
  *                 bilinearly (p[0] = 1) with wrap-around (Image, textures/image.cpp:279-718 at mip
  *                 level 0); the XYZ becomes a spectrum through the context's recovery table
- *                 (Spectral::fromXYZ), so scenes with images need liar_gpu_set_recovery first */
+ *                 (Spectral::fromXYZ), so scenes with images need liar_gpu_set_recovery first
+ *   NOISE         Perlin noise of the hit point (p[0] = 0: Perlin, perlin.cpp:60-205) or its fractal
+ *                 sum over p[0] octaves with falloff p[1] (FBm, fbm.cpp:62-90), a flat spectrum;
+ *                 permutation tables: 3 x 257 bytes at `pixels` of the scene's noise_tables
+ *   ABS           |child a| (Abs, abs.cpp:26-35)
+ *   AFFINE        p[0] child a + p[1], the child looked up as an illuminant and the result
+ *                 clamped to 1 as a reflectance (Product / Sum with one non-constant input,
+ *                 product.cpp:90-99, sum.cpp:90-105)
+ * A lookup applies at most 8 ABS / AFFINE nodes along its path. */
 enum liar_texture_type {
-    LIAR_TEX_CONSTANT = 0, LIAR_TEX_CHECKER = 1, LIAR_TEX_GRID = 2, LIAR_TEX_UV_TRANSFORM = 3, LIAR_TEX_IMAGE = 4
+    LIAR_TEX_CONSTANT = 0, LIAR_TEX_CHECKER = 1, LIAR_TEX_GRID = 2, LIAR_TEX_UV_TRANSFORM = 3, LIAR_TEX_IMAGE = 4,
+    LIAR_TEX_NOISE = 5, LIAR_TEX_ABS = 6, LIAR_TEX_AFFINE = 7
 };
 typedef struct liar_texture {
     int32_t type, a, b, spectrum;
@@ -228,6 +237,7 @@ typedef struct liar_scene_desc {
     const float* triangle_uvs;                           /* optional, n_triangles x 6: (u, v) per corner;
                                                             NULL: the barycentric coordinates of the hit */
     const float* texture_pixels; size_t n_texture_pixels; /* image textures: n x 4 (X, Y, Z, unused) */
+    const uint8_t* noise_tables; size_t n_noise_tables;   /* noise textures' permutation tables (bytes) */
 } liar_scene_desc;
 
 /* PerspectiveCamera (src/liar/cameras/perspective_camera.cpp:406-434): direction/right/down are

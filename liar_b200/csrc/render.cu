@@ -424,9 +424,10 @@ extern "C" int liar_gpu_scene_upload(liar_gpu_ctx* ctx, const liar_scene_desc* d
     if (D.n_textures > (1u << 20)) return ctx_fail(ctx, LIAR_ERR_INVALID, "too many textures (limit 2^20)");
     // every texture node must end at constants within 32 nodes (the lookup's bound), without cycles
     std::vector<int> tex_depth(D.n_textures, 0);  // 0: not visited, -1: being visited, else its depth
+    std::vector<int> tex_post(D.n_textures, 0);   // the most ABS / AFFINE nodes on a path down from it
     const char* tex_err = nullptr;
     int tex_bad = -1;
-    bool has_images = false;
+    bool has_images = false, has_noise = false;
     std::function<int(int, int)> depth_of = [&](int t, int level) -> int {
         if (t < 0 || (size_t)t >= D.n_textures) return tex_err = "child out of range", -1;
         if (tex_depth[t] > 0) return tex_depth[t];
@@ -444,6 +445,21 @@ extern "C" int liar_gpu_scene_upload(liar_gpu_ctx* ctx, const liar_scene_desc* d
             if (!(T.p[0] == 0.0f || T.p[0] == 1.0f)) return tex_err = "image filter must be 0 or 1", tex_bad = t, -1;
             has_images = true;
             d = 1;
+        } else if (T.type == LIAR_TEX_NOISE) {
+            if (T.pixels < 0 || !D.noise_tables || (uint64_t)T.pixels + 771 > (uint64_t)D.n_noise_tables)
+                return tex_err = "noise tables out of range", tex_bad = t, -1;
+            if (!(T.p[0] >= 0.0f && T.p[0] <= 64.0f && T.p[0] == std::floor(T.p[0])) || !std::isfinite(T.p[1]))
+                return tex_err = "noise octaves must be an integer in 0..64 with a finite falloff", tex_bad = t, -1;
+            has_noise = true;
+            d = 1;
+        } else if (T.type == LIAR_TEX_ABS || T.type == LIAR_TEX_AFFINE) {
+            if (!std::isfinite(T.p[0]) || !std::isfinite(T.p[1])) return tex_err = "non-finite parameters", tex_bad = t, -1;
+            tex_depth[t] = -1;
+            const int da = depth_of(T.a, level + 1);
+            if (da < 0) return -1;
+            if (tex_post[T.a] + 1 > 8) return tex_err = "more than 8 Abs / Product / Sum nodes on a path", tex_bad = t, -1;
+            tex_post[t] = tex_post[T.a] + 1;
+            d = da + 1;
         } else if (T.type == LIAR_TEX_CHECKER || T.type == LIAR_TEX_GRID || T.type == LIAR_TEX_UV_TRANSFORM) {
             tex_depth[t] = -1;
             const int da = depth_of(T.a, level + 1);
@@ -451,6 +467,7 @@ extern "C" int liar_gpu_scene_upload(liar_gpu_ctx* ctx, const liar_scene_desc* d
             int db = 0;
             if (T.type != LIAR_TEX_UV_TRANSFORM && (db = depth_of(T.b, level + 1)) < 0) return -1;
             d = std::max(da, db) + 1;
+            tex_post[t] = std::max(tex_post[T.a], T.type != LIAR_TEX_UV_TRANSFORM ? tex_post[T.b] : 0);
         } else {
             return tex_err = "bad type", tex_bad = t, -1;
         }
@@ -582,6 +599,7 @@ extern "C" int liar_gpu_scene_upload(liar_gpu_ctx* ctx, const liar_scene_desc* d
         d.tex_pixels = reinterpret_cast<const float4*>(px);
         d.rec = *rec;
     }
+    if (!rc && has_noise) rc = upload(ctx, s, D.noise_tables, D.n_noise_tables, &d.noise_tables, "noise tables");
     if (!rc) rc = upload(ctx, s, D.object_material, D.n_objects, &d.obj_mat, "object materials");
     if (!rc) rc = upload(ctx, s, D.object_light, D.n_objects, &d.obj_light, "object lights");
     if (!rc) rc = upload(ctx, s, D.materials, D.n_materials, &d.mats, "materials");

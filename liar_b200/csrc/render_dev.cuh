@@ -90,6 +90,7 @@ struct DScene {
     int n_tex;
     const float* tri_uv;         // optional, per triangle 3 x (u, v)
     const float4* tex_pixels;    // image textures' XYZ pixels
+    const uint8_t* noise_tables; // noise textures' permutation tables
     DRecovery rec;               // the recovery of image pixels (set when the scene has images)
 };
 
@@ -740,9 +741,93 @@ __device__ inline float3 image_lookup(const DScene& S, const liar_texture& T, fl
                        (p00.z * ex + p10.z * dx) * ey + (p01.z * ex + p11.z * dx) * dy);
 }
 
+// Perlin::noise (perlin.cpp:60-90, 170-205): improved Perlin noise over a 256-periodic lattice,
+// gradients picked by the xor of three permutation tables (257 entries each, the last repeating
+// the first), quintic fade, trilinear blend
+__device__ inline float perlin_gradient(const uint8_t* tab, int x, int y, int z, float dx, float dy, float dz) {
+    switch ((tab[x] ^ tab[257 + y] ^ tab[514 + z]) & 15) {
+        case 0: return dx + dy;
+        case 1: return dy - dx;
+        case 2: return dx - dy;
+        case 3: return -dx - dy;
+        case 4: return dx + dz;
+        case 5: return dz - dx;
+        case 6: return dx - dz;
+        case 7: return -dx - dz;
+        case 8: return dy + dz;
+        case 9: return dz - dy;
+        case 10: return dy - dz;
+        case 11: return -dy - dz;
+        case 12: return dx + dy;
+        case 13: return dy - dx;
+        case 14: return dz - dy;
+        default: return -dy - dz;
+    }
+}
+
+__device__ __forceinline__ float perlin_fade(float d) {
+    const float d2 = d * d;
+    return (6.0f * d2 * d - 15.0f * d2 + 10.0f * d) * d2;
+}
+
+__device__ inline float perlin_noise(const uint8_t* tab, float3 q) {
+    float c[3] = {q.x, q.y, q.z}, d[3];
+    int i[3];
+    for (int k = 0; k < 3; ++k) {
+        const float m = c[k] - floorf(c[k] * (1.0f / 256.0f)) * 256.0f;  // num::mod(x, 256)
+        const float f = floorf(m);
+        i[k] = (int)f;
+        d[k] = m - f;
+        if (i[k] >= 256) i[k] = 0;  // rounding onto the period: the same lattice point as 0
+        if (i[k] < 0) i[k] = 0;
+    }
+    const float g0 = perlin_gradient(tab, i[0], i[1], i[2], d[0], d[1], d[2]);
+    const float g1 = perlin_gradient(tab, i[0] + 1, i[1], i[2], d[0] - 1, d[1], d[2]);
+    const float g2 = perlin_gradient(tab, i[0], i[1] + 1, i[2], d[0], d[1] - 1, d[2]);
+    const float g3 = perlin_gradient(tab, i[0] + 1, i[1] + 1, i[2], d[0] - 1, d[1] - 1, d[2]);
+    const float g4 = perlin_gradient(tab, i[0], i[1], i[2] + 1, d[0], d[1], d[2] - 1);
+    const float g5 = perlin_gradient(tab, i[0] + 1, i[1], i[2] + 1, d[0] - 1, d[1], d[2] - 1);
+    const float g6 = perlin_gradient(tab, i[0], i[1] + 1, i[2] + 1, d[0], d[1] - 1, d[2] - 1);
+    const float g7 = perlin_gradient(tab, i[0] + 1, i[1] + 1, i[2] + 1, d[0] - 1, d[1] - 1, d[2] - 1);
+    const float sx = perlin_fade(d[0]), sy = perlin_fade(d[1]), sz = perlin_fade(d[2]);
+    auto lerp = [](float a, float b, float t) { return a + t * (b - a); };
+    return lerp(lerp(lerp(g0, g1, sx), lerp(g2, g3, sx), sy), lerp(lerp(g4, g5, sx), lerp(g6, g7, sx), sy), sz);
+}
+
+// FBm::doScalarLookUp (fbm.cpp:62-90) with a zero footprint (every octave): octaves of noise at
+// doubling frequencies, each weighed by falloff^k; p[0] = 0 is plain Perlin noise
+__device__ inline float noise_texture(const DScene& S, const liar_texture& T, float3 x) {
+    const uint8_t* tab = S.noise_tables + T.pixels;
+    const int octaves = (int)T.p[0];
+    if (octaves <= 0) return perlin_noise(tab, x);
+    float result = 0.0f, freq = 1.0f, weight = 1.0f;
+    for (int k = 0; k < octaves; ++k) {
+        result += weight * perlin_noise(tab, freq * x);
+        freq *= 2.0f;
+        weight *= T.p[1];
+    }
+    return result;
+}
+
 // Texture::lookUp of a tree of uv textures: the transforms move (u, v), the boards pick a child
 // (without anti-aliasing a board always picks one), the leaf is a spectrum
-__device__ inline float texture_eval(const DScene& S, int t, float u, float v, float lam, bool reflectant) {
+__device__ inline float texture_eval(const DScene& S, int t, float u, float v, float3 x, float lam, bool reflectant) {
+    // ABS / AFFINE nodes on the way down, applied to the leaf's value on the way back
+    int post_type[8];
+    float post_a[8], post_b[8];
+    bool post_refl[8];
+    int n_post = 0;
+    auto finish = [&](float val) {
+        for (int k = n_post - 1; k >= 0; --k) {
+            if (post_type[k] == LIAR_TEX_ABS) {
+                val = fabsf(val);
+            } else {
+                val = post_a[k] * val + post_b[k];
+                if (post_refl[k]) val = fminf(val, 1.0f);
+            }
+        }
+        return val;
+    };
     for (int depth = 0; depth < 32 && t >= 0 && t < S.n_tex; ++depth) {
         const liar_texture T = S.texs[t];
         switch (T.type) {
@@ -769,11 +854,27 @@ __device__ inline float texture_eval(const DScene& S, int t, float u, float v, f
                 // Image::doLookUp: Spectral::fromXYZ of the looked-up colour
                 const float3 c = image_lookup(S, T, u, v);
                 RecoveryBlend b;
-                if (!recovery_locate(S.rec, c.x, c.y, c.z, b)) return 0.0f;
-                return recovery_eval(S.rec, b, lam, reflectant);
+                if (!recovery_locate(S.rec, c.x, c.y, c.z, b)) return finish(0.0f);
+                return finish(recovery_eval(S.rec, b, lam, reflectant));
+            }
+            case LIAR_TEX_NOISE: {
+                const float n = noise_texture(S, T, x);  // Spectral(value, type): min(value, 1) as a reflectance
+                return finish(reflectant ? fminf(n, 1.0f) : n);
+            }
+            case LIAR_TEX_ABS:
+            case LIAR_TEX_AFFINE: {
+                if (n_post == 8) return 0.0f;
+                post_type[n_post] = T.type;
+                post_a[n_post] = T.p[0];
+                post_b[n_post] = T.p[1];
+                post_refl[n_post] = reflectant;
+                ++n_post;
+                if (T.type == LIAR_TEX_AFFINE) reflectant = false;  // inputs looked up as illuminants
+                t = T.a;
+                break;
             }
             default:
-                return spec_eval(S, T.spectrum, lam, reflectant);
+                return finish(spec_eval(S, T.spectrum, lam, reflectant));
         }
     }
     return 0.0f;
@@ -782,7 +883,7 @@ __device__ inline float texture_eval(const DScene& S, int t, float u, float v, f
 // a material parameter: its texture at the hit, else its constant spectrum
 __device__ __forceinline__ float param_eval(const DScene& S, const liar_material& M, int k, const HitContext& H,
                                             float lam, bool reflectant) {
-    return M.tex[k] >= 0 ? texture_eval(S, M.tex[k], H.uv_u, H.uv_v, lam, reflectant)
+    return M.tex[k] >= 0 ? texture_eval(S, M.tex[k], H.uv_u, H.uv_v, H.target, lam, reflectant)
                          : spec_eval(S, M.spec[k], lam, reflectant);
 }
 

@@ -53,7 +53,7 @@ class CSceneDesc(C.Structure):
                 ("spectrum_pool", _P), ("pool_size", _S), ("lights", _P), ("n_lights", _S),
                 ("observer", _P), ("n_observer", _S), ("scene_radius", C.c_float),
                 ("textures", _P), ("n_textures", _S), ("triangle_uvs", _P),
-                ("texture_pixels", _P), ("n_texture_pixels", _S)]
+                ("texture_pixels", _P), ("n_texture_pixels", _S), ("noise_tables", _P), ("n_noise_tables", _S)]
 
 
 class CCamera(C.Structure):
@@ -83,7 +83,7 @@ class CRenderDesc(C.Structure):
 FILTER_BOX, FILTER_TRIANGLE, FILTER_MITCHELL = 0, 1, 2
 
 
-TEX_CONSTANT, TEX_CHECKER, TEX_GRID, TEX_UV_TRANSFORM, TEX_IMAGE = range(5)
+TEX_CONSTANT, TEX_CHECKER, TEX_GRID, TEX_UV_TRANSFORM, TEX_IMAGE, TEX_NOISE, TEX_ABS, TEX_AFFINE = range(8)
 SPEC_CONSTANT, SPEC_SAMPLED, SPEC_BLACKBODY, SPEC_CAUCHY = 0, 1, 2, 3
 MAT_NONE, MAT_LAMBERT, MAT_CONDUCTOR, MAT_COOK_TORRANCE, MAT_DIELECTRIC, MAT_WALTER, MAT_MIRROR = range(7)
 LIGHT_PARA, LIGHT_MESH, LIGHT_POINT, LIGHT_SKY = 0, 1, 2, 3
@@ -107,6 +107,7 @@ class FlatScene:
     textures: C.Array | None = None
     triangle_uvs: np.ndarray | None = None  # n_triangles x 3 x 2, when a texture needs them
     texture_pixels: np.ndarray | None = None  # image textures' pixels, n x 4 (X, Y, Z, 0)
+    noise_tables: np.ndarray | None = None    # noise textures' permutation tables, bytes
     keep: list = field(default_factory=list)
 
     def desc(self) -> CSceneDesc:
@@ -142,6 +143,9 @@ class FlatScene:
         if self.texture_pixels is not None:
             d.texture_pixels = self.texture_pixels.ctypes.data
             d.n_texture_pixels = self.texture_pixels.shape[0]
+        if self.noise_tables is not None:
+            d.noise_tables = self.noise_tables.ctypes.data
+            d.n_noise_tables = self.noise_tables.size
         return d
 
 
@@ -156,6 +160,7 @@ class _Builder:
         self.lights = []
         self.textures, self.tex_ids = [], {}
         self.tex_pixels, self.n_tex_pixels = [], 0
+        self.noise_tables, self.n_noise = [], 0
         self.tri_uvs = []  # per object: n x 3 x 2 corner uvs, or None for the barycentric ones
         self.M = None  # current local-to-world affine matrix (None: identity)
 
@@ -233,6 +238,28 @@ class _Builder:
             px[:, :3] = t.xyz.reshape(-1, 3)
             self.tex_pixels.append(px)
             self.n_tex_pixels += h * w
+        elif isinstance(t, tx.Perlin):
+            rec.type = TEX_NOISE
+            rec.p[0] = float(t.numOctaves) if isinstance(t, tx.FBm) else 0.0
+            rec.p[1] = float(t.falloff) if isinstance(t, tx.FBm) else 0.0
+            rec.pixels = self.n_noise
+            self.noise_tables.append(t.tables.reshape(-1))
+            self.n_noise += t.tables.size
+        elif isinstance(t, tx.Abs):
+            rec.type = TEX_ABS
+        elif isinstance(t, (tx.Product, tx.Sum)):
+            parts = t.factors if isinstance(t, tx.Product) else t.terms
+            varying = [f for f in parts if tx.flat_value(f) is None]
+            consts = [tx.flat_value(f) for f in parts if tx.flat_value(f) is not None]
+            if len(varying) > 1:
+                raise NotImplementedError(f"{type(t).__name__} of more than one non-constant texture is not on the GPU path")
+            if not varying:
+                raise NotImplementedError(f"a {type(t).__name__} of constants: use a Constant")
+            rec.type = TEX_AFFINE
+            if isinstance(t, tx.Product):
+                rec.p[0], rec.p[1] = float(np.prod(consts)) if consts else 1.0, 0.0
+            else:
+                rec.p[0], rec.p[1] = 1.0, float(np.sum(consts)) if consts else 0.0
         elif isinstance(t, tx.TransformationUv):
             rec.type = TEX_UV_TRANSFORM
             m = t.transformation
@@ -248,6 +275,9 @@ class _Builder:
             self.textures[idx].b = self.texture(t.textureB)
         elif isinstance(t, tx.UnaryOperator):
             self.textures[idx].a = self.texture(t.texture)
+        elif isinstance(t, (tx.Product, tx.Sum)):
+            parts = t.factors if isinstance(t, tx.Product) else t.terms
+            self.textures[idx].a = self.texture(next(f for f in parts if tx.flat_value(f) is None))
         return idx
 
     def param(self, m, k: int, value):
@@ -438,6 +468,7 @@ class _Builder:
             textures=(CTexture * len(self.textures))(*self.textures) if self.textures else None,
             triangle_uvs=self.triangle_uvs(),
             texture_pixels=np.ascontiguousarray(np.concatenate(self.tex_pixels)) if self.tex_pixels else None,
+            noise_tables=np.ascontiguousarray(np.concatenate(self.noise_tables)) if self.noise_tables else None,
         )
 
     def triangle_uvs(self) -> np.ndarray | None:

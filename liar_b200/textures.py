@@ -241,8 +241,77 @@ class Image(Texture):
                           "(no ray differentials on the GPU path)", stacklevel=4)
 
 
+class Perlin(Texture):
+    """Perlin([seed]) (textures/perlin.cpp): improved Perlin noise of the hit point, a flat
+    spectrum. The lattice's three permutation tables are shuffled from the seed by this package's
+    own generator (numpy's PCG64, one permutation per axis); the reference shuffles with pcg-cpp's
+    pcg32_k2_fast through std::shuffle, so the same seed gives a differently placed but identically
+    constructed noise field."""
+
+    def __init__(self, seed: int = 0):
+        self.seed = int(seed)
+
+    @property
+    def seed(self) -> int:
+        return self._seed
+
+    @seed.setter
+    def seed(self, value: int):
+        self._seed = int(value) & 0xFFFFFFFF
+        rng = np.random.Generator(np.random.PCG64(self._seed))
+        tables = np.zeros((3, 257), np.uint8)
+        for k in range(3):
+            perm = rng.permutation(256)
+            tables[k, :256] = perm
+            tables[k, 256] = perm[0]          # the padding entry repeats the first
+        self.tables = tables
+
+
+class FBm(Perlin):
+    """FBm(numOctaves[, falloff]) (textures/fbm.cpp): octaves of Perlin noise (seed 0) at doubling
+    frequencies, weighed by falloff^k (default 0.5). The reference lowers the octave count where
+    the ray differentials' footprint is wide; this path has no differentials, so every octave
+    counts (the reference's zero-footprint case)."""
+
+    def __init__(self, numOctaves: int, falloff: float = 0.5):
+        super().__init__(0)
+        if int(numOctaves) < 1 or int(numOctaves) > 64:
+            raise ValueError("numOctaves must be in 1..64")
+        self.numOctaves = int(numOctaves)
+        self.falloff = float(falloff)
+
+
+class Abs(UnaryOperator):
+    """Abs(texture) (textures/abs.cpp): the absolute value of its input."""
+
+
+class Product(Texture):
+    """Product(factors) or Product(a, b) (textures/product.cpp). On the GPU path at most one factor
+    may vary; the others must be flat constants (numbers or constant spectra of one value)."""
+
+    def __init__(self, *args):
+        factors = args[0] if len(args) == 1 and isinstance(args[0], (list, tuple)) else args
+        self.factors = [_texture(f) for f in factors]
+
+
+class Sum(Texture):
+    """Sum(terms) or Sum(a, b) (textures/sum.cpp). On the GPU path at most one term may vary; the
+    others must be flat constants."""
+
+    def __init__(self, *args):
+        terms = args[0] if len(args) == 1 and isinstance(args[0], (list, tuple)) else args
+        self.terms = [_texture(t) for t in terms]
+
+
+def flat_value(t) -> float | None:
+    """The value of a flat constant texture (a number or a constant spectrum), else None."""
+    if isinstance(t, Constant) and type(t.value) is Spectrum:
+        return float(t.value.value)
+    return None
+
+
 def is_uv_texture(x) -> bool:
-    return isinstance(x, (CheckerBoard, GridBoard, TransformationUv, Image))
+    return isinstance(x, (CheckerBoard, GridBoard, TransformationUv, Image, Perlin, Abs, Product, Sum))
 
 
 def warn_point_lookup(tex: CheckerBoard):

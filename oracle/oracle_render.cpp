@@ -97,6 +97,7 @@ struct SceneIn {
     const Texture* textures; uint64_t n_textures;
     const float* triangle_uvs;
     const float* texture_pixels; uint64_t n_texture_pixels;
+    const uint8_t* noise_tables; uint64_t n_noise_tables;
 };
 struct RenderIn {
     Camera camera;
@@ -126,7 +127,8 @@ static_assert(offsetof(Material, tex) == offsetof(liar_material, tex) &&
                   offsetof(RenderIn, pm_max_photons) == offsetof(liar_render_desc, photon_mapper) &&
                   offsetof(RenderIn, filter) == offsetof(liar_render_desc, filter) &&
                   offsetof(Texture, pixels) == offsetof(liar_texture, pixels) &&
-                  offsetof(SceneIn, texture_pixels) == offsetof(liar_scene_desc, texture_pixels),
+                  offsetof(SceneIn, texture_pixels) == offsetof(liar_scene_desc, texture_pixels) &&
+                  offsetof(SceneIn, noise_tables) == offsetof(liar_scene_desc, noise_tables),
               "oracle mirrors out of step with include/liar_gpu.h");
 
 // The photon maps of a PhotonMapper render (photon_mapper.cpp:798-835) as the oracle gets them:
@@ -771,8 +773,71 @@ void image_lookup(const Scene& S, const Texture& T, float u, float v, float out[
 // (transformation_uv.cpp:67-70), CheckerBoard without anti-aliasing picks A where the fractional u
 // and v lie on the same side of the split (checker_board.cpp:113-124, 149-157), GridBoard picks A
 // on the lines (grid_board.cpp:80-87), Constant is its spectrum
-float texture(const Scene& S, int t, float u, float v, float lam, bool reflectant) {
-    for (int depth = 0; depth < 32; ++depth) {
+// Perlin::noise and FBm::doScalarLookUp (perlin.cpp:60-90, 170-205; fbm.cpp:62-90 with a zero
+// footprint, so every octave): improved Perlin noise on a 256-periodic lattice
+float perlin_gradient(const uint8_t* tab, int x, int y, int z, float dx, float dy, float dz) {
+    static const int8_t G[16][3] = {{1, 1, 0}, {-1, 1, 0}, {1, -1, 0}, {-1, -1, 0}, {1, 0, 1}, {-1, 0, 1},
+                                    {1, 0, -1}, {-1, 0, -1}, {0, 1, 1}, {0, -1, 1}, {0, 1, -1}, {0, -1, -1},
+                                    {1, 1, 0}, {-1, 1, 0}, {0, -1, 1}, {0, -1, -1}};
+    const int8_t* g = G[(tab[x] ^ tab[257 + y] ^ tab[514 + z]) & 15];
+    float r = 0;  // the reference's sums, term by term in its order
+    const float c[3] = {dx, dy, dz};
+    int first = -1;
+    for (int k = 0; k < 3; ++k)
+        if (g[k] != 0 && first < 0) first = k;
+    r = g[first] * c[first];
+    for (int k = first + 1; k < 3; ++k)
+        if (g[k] != 0) r = r + g[k] * c[k];
+    return r;
+}
+
+float perlin_noise(const uint8_t* tab, V q) {
+    const float c[3] = {q.x, q.y, q.z};
+    float d[3];
+    int i[3];
+    for (int k = 0; k < 3; ++k) {
+        const float m = c[k] - std::floor(c[k] * (1.0f / 256.0f)) * 256.0f;
+        const float f = std::floor(m);
+        i[k] = (int)f;
+        d[k] = m - f;
+        if (i[k] >= 256 || i[k] < 0) i[k] = 0;
+    }
+    float g[8];
+    for (int n = 0; n < 8; ++n) {
+        const int a = n & 1, b = (n >> 1) & 1, e = (n >> 2) & 1;
+        g[n] = perlin_gradient(tab, i[0] + a, i[1] + b, i[2] + e, d[0] - a, d[1] - b, d[2] - e);
+    }
+    auto fade = [](float x) { const float x2 = x * x; return (6 * x2 * x - 15 * x2 + 10 * x) * x2; };
+    auto lerp = [](float a, float b, float t) { return a + t * (b - a); };
+    const float sx = fade(d[0]), sy = fade(d[1]), sz = fade(d[2]);
+    return lerp(lerp(lerp(g[0], g[1], sx), lerp(g[2], g[3], sx), sy), lerp(lerp(g[4], g[5], sx), lerp(g[6], g[7], sx), sy),
+                sz);
+}
+
+float noise_texture(const Scene& S, const Texture& T, V x) {
+    const uint8_t* tab = S.in.noise_tables + T.pixels;
+    const int octaves = (int)T.p[0];
+    if (octaves <= 0) return perlin_noise(tab, x);
+    float result = 0, freq = 1, weight = 1;
+    for (int k = 0; k < octaves; ++k) {
+        result += weight * perlin_noise(tab, freq * x);
+        freq *= 2;
+        weight *= T.p[1];
+    }
+    return result;
+}
+
+// Abs (abs.cpp:26-35) looks its input up as the caller does; Product / Sum of one texture with
+// constants (product.cpp:90-99, sum.cpp:90-105) as illuminants, the result clamped as a
+// reflectance; applied to the value found below them
+float texture_rec(const Scene& S, int t, float u, float v, V x, float lam, bool reflectant, int depth);
+
+float texture(const Scene& S, int t, float u, float v, V x, float lam, bool reflectant) {
+    return texture_rec(S, t, u, v, x, lam, reflectant, 0);
+}
+
+float texture_rec(const Scene& S, int t, float u, float v, V x, float lam, bool reflectant, int depth0) {
+    for (int depth = depth0; depth < 32; ++depth) {
         const Texture& T = S.in.textures[t];
         if (T.type == 1) {
             t = ((frac(u) < T.p[0]) == (frac(v) < T.p[1])) ? T.a : T.b;
@@ -785,6 +850,14 @@ float texture(const Scene& S, int t, float u, float v, float lam, bool reflectan
             u = nu;
             v = nv;
             t = T.a;
+        } else if (T.type == 5) {
+            const float n = noise_texture(S, T, x);
+            return reflectant ? std::min(n, 1.0f) : n;
+        } else if (T.type == 6) {
+            return std::fabs(texture_rec(S, T.a, u, v, x, lam, reflectant, depth + 1));
+        } else if (T.type == 7) {
+            const float r = T.p[0] * texture_rec(S, T.a, u, v, x, lam, false, depth + 1) + T.p[1];
+            return reflectant ? std::min(r, 1.0f) : r;
         } else if (T.type == 4) {
             // Image::doLookUp: Spectral::fromXYZ of the colour
             float c[3];
@@ -800,8 +873,8 @@ float texture(const Scene& S, int t, float u, float v, float lam, bool reflectan
     return 0;
 }
 
-float param(const Scene& S, const Material& M, int k, float u, float v, float lam, bool reflectant) {
-    return M.tex[k] >= 0 ? texture(S, M.tex[k], u, v, lam, reflectant) : spectrum(S, M.spec[k], lam, reflectant);
+float param(const Scene& S, const Material& M, int k, float u, float v, V x, float lam, bool reflectant) {
+    return M.tex[k] >= 0 ? texture(S, M.tex[k], u, v, x, lam, reflectant) : spectrum(S, M.spec[k], lam, reflectant);
 }
 Ctx hit_ctx(const Scene& S, V o, V d, const Hit& h) {
     Ctx c;
@@ -867,38 +940,38 @@ Bsdf make_bsdf(const Scene& S, const Material& M, const Ctx& c, float lam) {
     switch (M.type) {
         case M_LAMBERT:
             B.caps = C_REFL | C_DIFF;
-            B.r = param(S, M, 0, c.uv_u, c.uv_v, lam, true);
+            B.r = param(S, M, 0, c.uv_u, c.uv_v, c.target, lam, true);
             break;
         case M_CONDUCTOR:
         case M_CT:
             B.caps = M.type == M_CONDUCTOR ? (C_REFL | C_SPEC) : (C_REFL | C_GLOSSY);
-            B.eta = std::max(param(S, M, 0, c.uv_u, c.uv_v, lam, false), 1e-9f);
-            B.kappa = std::max(param(S, M, 1, c.uv_u, c.uv_v, lam, false), 1e-9f);
-            B.r = param(S, M, 2, c.uv_u, c.uv_v, lam, true);
+            B.eta = std::max(param(S, M, 0, c.uv_u, c.uv_v, c.target, lam, false), 1e-9f);
+            B.kappa = std::max(param(S, M, 1, c.uv_u, c.uv_v, c.target, lam, false), 1e-9f);
+            B.r = param(S, M, 2, c.uv_u, c.uv_v, c.target, lam, true);
             break;
         case M_DIELECTRIC: {
             B.caps = C_REFL | C_TRANS | C_SPEC;
-            const float i1 = std::max(param(S, M, 1, c.uv_u, c.uv_v, lam, false), 1e-9f);
-            const float i2 = std::max(param(S, M, 0, c.uv_u, c.uv_v, lam, false), 1e-9f);
+            const float i1 = std::max(param(S, M, 1, c.uv_u, c.uv_v, c.target, lam, false), 1e-9f);
+            const float i2 = std::max(param(S, M, 0, c.uv_u, c.uv_v, c.target, lam, false), 1e-9f);
             B.ior = c.leaving ? i2 / i1 : i1 / i2;
-            B.r = param(S, M, 2, c.uv_u, c.uv_v, lam, true);
-            B.t = param(S, M, 3, c.uv_u, c.uv_v, lam, true);
+            B.r = param(S, M, 2, c.uv_u, c.uv_v, c.target, lam, true);
+            B.t = param(S, M, 3, c.uv_u, c.uv_v, c.target, lam, true);
             break;
         }
         case M_WALTER: {
             B.caps = C_TRANS | C_GLOSSY;
-            float ei = std::max(param(S, M, 1, c.uv_u, c.uv_v, lam, false), 1e-9f);
-            float et = std::max(param(S, M, 0, c.uv_u, c.uv_v, lam, false), 1e-9f);
+            float ei = std::max(param(S, M, 1, c.uv_u, c.uv_v, c.target, lam, false), 1e-9f);
+            float et = std::max(param(S, M, 0, c.uv_u, c.uv_v, c.target, lam, false), 1e-9f);
             if (c.leaving) std::swap(ei, et);
             B.etaI = ei;
             B.etaT = et;
-            B.r = param(S, M, 2, c.uv_u, c.uv_v, lam, true);
-            B.t = param(S, M, 3, c.uv_u, c.uv_v, lam, true);
+            B.r = param(S, M, 2, c.uv_u, c.uv_v, c.target, lam, true);
+            B.t = param(S, M, 3, c.uv_u, c.uv_v, c.target, lam, true);
             break;
         }
         case M_MIRROR:
             B.caps = C_REFL | C_SPEC;
-            B.r = param(S, M, 0, c.uv_u, c.uv_v, lam, true);
+            B.r = param(S, M, 0, c.uv_u, c.uv_v, c.target, lam, true);
             break;
     }
     return B;
@@ -1646,38 +1719,38 @@ static void trace_photon_rec(const Scene& S, const PhotonIn& D, const Sampler& s
     switch (M.type) {
         case M_LAMBERT:
             B.caps = C_REFL | C_DIFF;
-            B.r = param(S, M, 0, uv_u, uv_v, lam, true);
+            B.r = param(S, M, 0, uv_u, uv_v, hit, lam, true);
             break;
         case M_CONDUCTOR:
         case M_CT:
             B.caps = M.type == M_CONDUCTOR ? (C_REFL | C_SPEC) : (C_REFL | C_GLOSSY);
-            B.eta = std::max(param(S, M, 0, uv_u, uv_v, lam, false), 1e-9f);
-            B.kappa = std::max(param(S, M, 1, uv_u, uv_v, lam, false), 1e-9f);
-            B.r = param(S, M, 2, uv_u, uv_v, lam, true);
+            B.eta = std::max(param(S, M, 0, uv_u, uv_v, hit, lam, false), 1e-9f);
+            B.kappa = std::max(param(S, M, 1, uv_u, uv_v, hit, lam, false), 1e-9f);
+            B.r = param(S, M, 2, uv_u, uv_v, hit, lam, true);
             break;
         case M_DIELECTRIC: {
             B.caps = C_REFL | C_TRANS | C_SPEC;
-            const float i1 = std::max(param(S, M, 1, uv_u, uv_v, lam, false), 1e-9f);
-            const float i2 = std::max(param(S, M, 0, uv_u, uv_v, lam, false), 1e-9f);
+            const float i1 = std::max(param(S, M, 1, uv_u, uv_v, hit, lam, false), 1e-9f);
+            const float i2 = std::max(param(S, M, 0, uv_u, uv_v, hit, lam, false), 1e-9f);
             B.ior = leaving ? i2 / i1 : i1 / i2;
-            B.r = param(S, M, 2, uv_u, uv_v, lam, true);
-            B.t = param(S, M, 3, uv_u, uv_v, lam, true);
+            B.r = param(S, M, 2, uv_u, uv_v, hit, lam, true);
+            B.t = param(S, M, 3, uv_u, uv_v, hit, lam, true);
             break;
         }
         case M_WALTER: {
             B.caps = C_TRANS | C_GLOSSY;
-            float ei = std::max(param(S, M, 1, uv_u, uv_v, lam, false), 1e-9f);
-            float et = std::max(param(S, M, 0, uv_u, uv_v, lam, false), 1e-9f);
+            float ei = std::max(param(S, M, 1, uv_u, uv_v, hit, lam, false), 1e-9f);
+            float et = std::max(param(S, M, 0, uv_u, uv_v, hit, lam, false), 1e-9f);
             if (leaving) std::swap(ei, et);
             B.etaI = ei;
             B.etaT = et;
-            B.r = param(S, M, 2, uv_u, uv_v, lam, true);
-            B.t = param(S, M, 3, uv_u, uv_v, lam, true);
+            B.r = param(S, M, 2, uv_u, uv_v, hit, lam, true);
+            B.t = param(S, M, 3, uv_u, uv_v, hit, lam, true);
             break;
         }
         case M_MIRROR:
             B.caps = C_REFL | C_SPEC;
-            B.r = param(S, M, 0, uv_u, uv_v, lam, true);
+            B.r = param(S, M, 0, uv_u, uv_v, hit, lam, true);
             break;
     }
     const V md = -d;

@@ -204,3 +204,72 @@ def test_oracle_image_quadrants(filter):
         Y = img[..., 1]
         assert Y[h // 2 - 1:h // 2 + 1, w // 2 - 1:w // 2 + 1].mean() == pytest.approx(levels.mean(), rel=0.05)
         assert list(np.argsort([tl, tr, bl, br])) == list(np.argsort(levels.ravel()))
+
+
+def _noise(tables, p):
+    """Improved Perlin noise as perlin.cpp:60-90, 170-205 states it, in numpy (float64)."""
+    G = np.array([[1, 1, 0], [-1, 1, 0], [1, -1, 0], [-1, -1, 0], [1, 0, 1], [-1, 0, 1], [1, 0, -1], [-1, 0, -1],
+                  [0, 1, 1], [0, -1, 1], [0, 1, -1], [0, -1, -1], [1, 1, 0], [-1, 1, 0], [0, -1, 1], [0, -1, -1]])
+    q = np.mod(p, 256.0)
+    i = np.floor(q).astype(int)
+    d = q - i
+    fade = lambda t: (6 * t ** 3 - 15 * t ** 2 + 10 * t) * t ** 2
+    s = fade(d)
+    g = {}
+    for a in (0, 1):
+        for b in (0, 1):
+            for c in (0, 1):
+                h = tables[0][i[..., 0] + a] ^ tables[1][i[..., 1] + b] ^ tables[2][i[..., 2] + c]
+                grad = G[h % 16]
+                g[a, b, c] = (grad * (d - (a, b, c))).sum(-1)
+    lerp = lambda x, y, t: x + t * (y - x)
+    return lerp(lerp(lerp(g[0, 0, 0], g[1, 0, 0], s[..., 0]), lerp(g[0, 1, 0], g[1, 1, 0], s[..., 0]), s[..., 1]),
+                lerp(lerp(g[0, 0, 1], g[1, 0, 1], s[..., 0]), lerp(g[0, 1, 1], g[1, 1, 1], s[..., 0]), s[..., 1]), s[..., 2])
+
+
+def test_noise_tables_and_flattening():
+    p = tx.Perlin(7)
+    assert p.tables.shape == (3, 257) and (p.tables[:, 256] == p.tables[:, 0]).all()
+    assert all(sorted(t[:256]) == list(range(256)) for t in p.tables)
+    assert (tx.Perlin(7).tables == p.tables).all() and not (tx.Perlin(8).tables == p.tables).all()
+    f = tx.FBm(5, 0.6)
+    tex = tx.Sum([tx.Constant(0.25), 0.25, tx.Product(tx.Constant(0.5), tx.Abs(f))])
+    plane = scenery.Parallelogram((0, 0, 0), (1, 0, 0), (0, 1, 0))
+    plane.shader = shaders.Lambert(tex)
+    flat = R.flatten(plane)
+    T = list(flat.textures)
+    s = T[flat.materials[0].tex[0]]
+    assert s.type == R.TEX_AFFINE and tuple(s.p[:2]) == (1.0, 0.5)
+    m = T[s.a]
+    assert m.type == R.TEX_AFFINE and tuple(m.p[:2]) == (0.5, 0.0)
+    a = T[m.a]
+    n = T[a.a]
+    assert a.type == R.TEX_ABS and n.type == R.TEX_NOISE and tuple(n.p[:2]) == pytest.approx((5.0, 0.6))
+    np.testing.assert_array_equal(flat.noise_tables[n.pixels:n.pixels + 771], f.tables.reshape(-1))
+    with pytest.raises(NotImplementedError):
+        plane.shader = shaders.Lambert(tx.Product(tx.Perlin(), tx.Perlin(1)))
+        R.flatten(plane)
+
+
+@pytest.mark.parametrize("octaves", [0, 3])
+def test_oracle_noise_follows_the_hit_point(octaves):
+    """A plane shaded with 0.5 + 0.4 noise(x) under a uniform sky shows that reflectance at every
+    pixel: the oracle's noise against the numpy statement above, at the pixel centres' hits."""
+    noise = tx.FBm(octaves, 0.5) if octaves else tx.Perlin(3)
+    scene, cam = _board_scene(tx.Sum(0.5, tx.Product(0.4, noise)))
+    t = tracers.DirectLighting()
+    t.maxRayGeneration = 1
+    w, h = 40, 30
+    img, var = R.resolve(oracle.RenderScene(R.flatten(scene)).render(R.render_desc(cam, w, h, 64, t, seed=4)))
+    # pixel centres on the plane: x right over [0.1, 0.9], y up over [0.2, 0.8]
+    xs = 0.5 + 0.4 * (2 * (np.arange(w) + 0.5) / w - 1)
+    ys = 0.5 - 0.3 * (2 * (np.arange(h) + 0.5) / h - 1)
+    P = np.stack(list(np.meshgrid(xs, ys)) + [np.zeros((h, w))], axis=-1)
+    n = np.zeros((h, w))
+    for k in range(max(octaves, 1)):
+        n += 0.5 ** k * _noise(noise.tables, P * 2.0 ** k)
+    expect = 0.5 + 0.4 * n
+    err = np.abs(img[..., 1] - expect)
+    # within the sky estimate's noise (and the noise's change across a pixel)
+    assert (err <= 4 * np.sqrt(var[..., 1]) + 0.01).mean() > 0.99 and np.ptp(expect) > 0.1
+    assert np.corrcoef(img[..., 1].ravel(), expect.ravel())[0, 1] > 0.95

@@ -25,6 +25,9 @@ def _scene():
     grid.thickness = (0.15, 0.3)
     back = scenery.Parallelogram((-2, 0, 2), (4, 0, 0), (0, 3, 0))
     back.shader = shaders.Lambert(tx.TransformationUv(grid, [[3, 1, 0], [0, 3, 0], [0, 0, 1]]))
+    marble = scenery.Parallelogram((-1.9, 0, 1.9), (0, 0, -3), (0, 2.5, 0))    # the left wall
+    marble.shader = shaders.Lambert(tx.Sum(0.3, tx.Product(0.6, tx.Abs(tx.FBm(4, 0.55)))))
+    ball_noise = tx.Sum([0.5, tx.Product([0.45, tx.Perlin(9)])])
     ball = scenery.Sphere((-0.7, 0.6, 0.2), 0.6, subdivisions=3)
     ct = shaders.CookTorrance(tx.Constant(spectra.Spectrum(1.5)), tx.Constant(spectra.Spectrum(3.0)))
     stripes = tx.CheckerBoard(tx.Constant(1.0), tx.Constant(0.2))
@@ -32,6 +35,7 @@ def _scene():
     stripes.antiAliasing = "none"
     ct.reflectance = tx.TransformationUv(stripes, [[8, 0, 0], [0, 1, 0], [0, 0, 1]])
     ct.roughness = tx.Constant(0.3)
+    ct.absorptionCoefficient = ball_noise       # a noisy absorption: textures on non-reflectance slots too
     ball.shader = ct
     box = scenery.Box((0.3, 0, -0.5), (1.1, 0.8, 0.3))
     mirrored = scenery.Transformation(box, [[-1, 0, 0, 0.6], [0, 1, 0, 0], [0, 0, 1, 0], [0, 0, 0, 1]])
@@ -48,7 +52,7 @@ def _scene():
     cam = cameras.PerspectiveCamera()
     cam.position = (0, 1.5, -4)
     cam.lookAt((0, 0.8, 0))
-    return scenery.List([floor, back, ball, mirrored, panel, light]), cam
+    return scenery.List([floor, back, marble, ball, mirrored, panel, light]), cam
 
 
 def _within_3_sigma(g, c, min_fraction=0.99):
