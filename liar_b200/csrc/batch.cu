@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(256) k_b_raygen(BParams P, BState<H> st, BQueu
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&C->stats[0], (unsigned long long)n);
 }
 
-template <int H>
+template <int H, bool TEX>
 __global__ void __launch_bounds__(128) k_b_shade(BParams P, BState<H> st, BQueue in, const liar_hit* __restrict__ hits,
                                                  int cur, BQueue out) {
     BControl* C = P.ctrl;
@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(128) k_b_shade(BParams P, BState<H> st, BQueue
                     const liar_material M = S.mats[mi];
                     if (shader_emits && M.emission >= 0)
                         for (int k = 0; k < H; ++k) L[k] += T[k] * spec_eval(S, M.emission, lam[k], false);
-                    const Bsdf B = make_bsdf(S, M, HC, lam[0]);
+                    const Bsdf B = make_bsdf<TEX>(S, M, HC, lam[0]);
                     const float3 md = -d;
                     float3 wi = mk(dot(md, HC.u), dot(md, HC.v), dot(md, HC.N));
                     wi.z = fmaxf(wi.z, kEps);
@@ -336,7 +336,7 @@ __global__ void __launch_bounds__(128) k_b_shade(BParams P, BState<H> st, BQueue
                                 val[k] = 0.0f;  // secondary wavelengths end at a dispersive interface
                                 continue;
                             }
-                            const Bsdf Bk = k == 0 ? B : make_bsdf(S, M, HC, lam[k]);
+                            const Bsdf Bk = k == 0 ? B : make_bsdf<TEX>(S, M, HC, lam[k]);
                             if (from_bsdf) {
                                 if (k == 0) {
                                     val[k] = bs.value;
@@ -457,6 +457,7 @@ struct liar_gpu_batch {
     uint32_t n_waves = 0;
     uint64_t total = 0;
     int shade_blocks_per_sm = 16;
+    bool textured = false;  // some scene has textures: the shading kernel with texture lookups
     liar_trace_config trace{128, 16};
     std::vector<void*> buffers;
     BParams params{};
@@ -525,7 +526,7 @@ int capture_body(liar_gpu_ctx* ctx, liar_gpu_batch* b, cudaStream_t cs, BState<H
         cudaError_t e = cudaLaunchKernel(tl.kern, dim3(tl.grid), dim3(tl.block), args, tl.smem, cs);
         if (e != cudaSuccess) return ctx_cuda(ctx, e, "batch trace launch");
         k_b_clear_queue<<<1, 1, 0, cs>>>(b->ctrl, cur ^ 1);
-        k_b_shade<H><<<sms * b->shade_blocks_per_sm, 128, 0, cs>>>(P, st, q[cur], hits, cur, q[cur ^ 1]);
+        (b->textured ? k_b_shade<H, true> : k_b_shade<H, false>)<<<sms * b->shade_blocks_per_sm, 128, 0, cs>>>(P, st, q[cur], hits, cur, q[cur ^ 1]);
         cur ^= 1;
     }
     k_b_flush<H><<<sms * 4, 256, 0, cs>>>(P, st, q[cur], cur);
@@ -703,6 +704,7 @@ extern "C" int liar_gpu_batch_create(liar_gpu_ctx* ctx, const liar_batch_item* i
     std::vector<TreeRoot> roots(scenes.size());
     for (size_t s = 0; s < scenes.size(); ++s) {
         hs[s] = scene_dscene(scenes[s]);
+        b->textured |= hs[s].n_tex > 0;
         roots[s] = TreeRoot{hs[s].nodes, hs[s].qtris};
         if (hs[s].stack_needed > (uint32_t)kTraceStackTotal) {
             delete b;

@@ -247,6 +247,7 @@ __device__ void direct_low_quality(const DScene& S, int n, const Bsdf& B, const 
     }
 }
 
+template <bool TEX>
 __global__ void __launch_bounds__(128) k_dl_shade(DScene S, DParams W, DSamples P, DTasks in,
                                                   const liar_hit* __restrict__ hits, uint32_t n_in, DTasks out,
                                                   DShadows sh, uint32_t shadow_hq) {
@@ -288,7 +289,7 @@ __global__ void __launch_bounds__(128) k_dl_shade(DScene S, DParams W, DSamples 
             M = S.mats[HC.mat];
             lam = P.lam[p];
             if (M.type != LIAR_MAT_NONE) {
-                B = make_bsdf(S, M, HC, lam);
+                B = make_bsdf<TEX>(S, M, HC, lam);
                 has_bsdf = true;
                 n_sh = hq ? shadow_hq : (S.n_lights > 0 ? 2u * (uint32_t)W.n_secondary : 0u);
                 if (W.pm == 2 || (W.pm == 1 && !W.pm_direct)) n_sh = 0u;  // no traced direct light
@@ -998,7 +999,7 @@ int render_direct(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_ren
             e = cudaMemsetAsync(b->counters + (cur ^ 1), 0, 4, st);
             if (e == cudaSuccess) e = cudaMemsetAsync(b->counters + 2, 0, 12, st);
             if (e != cudaSuccess) return ctx_cuda(ctx, e, "reset queues");
-            k_dl_shade<<<(n_in + 127) / 128, 128, 0, st>>>(S, W, P, tin, b->hits, n_in, tout, sq, (uint32_t)sh_hq);
+            (S.n_tex > 0 ? k_dl_shade<true> : k_dl_shade<false>)<<<(n_in + 127) / 128, 128, 0, st>>>(S, W, P, tin, b->hits, n_in, tout, sq, (uint32_t)sh_hq);
             e = cudaGetLastError();
             if (e != cudaSuccess) return ctx_cuda(ctx, e, "direct lighting shade launch");
             e = cudaMemcpyAsync(b->h_counters, b->counters, 5 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);

@@ -193,6 +193,7 @@ __global__ void __launch_bounds__(128) k_g_prep(DScene S, GQueue in, const liar_
     for (int c = 0; c < 9; ++c) dst[c] = x[c];
 }
 
+template <bool TEX>
 __global__ void __launch_bounds__(kShadeThreads) k_g_shade(DScene S, GParams W, GPaths P, GQueue in,
                                                            const liar_hit* __restrict__ hits, uint32_t n_in, GQueue out,
                                                            const float* __restrict__ gmix) {
@@ -266,7 +267,7 @@ __global__ void __launch_bounds__(kShadeThreads) k_g_shade(DScene S, GParams W, 
                     if (shader_emits && S.mats[mi].emission >= 0) L += T * spec_eval(S, S.mats[mi].emission, lam, false);
                 } else {
                     if (shader_emits && M.emission >= 0) L += T * spec_eval(S, M.emission, lam, false);
-                    const Bsdf B = make_bsdf(S, M, HC, lam);
+                    const Bsdf B = make_bsdf<TEX>(S, M, HC, lam);
                     const float3 md = -d;
                     float3 wi = mk(dot(md, u), dot(md, v), dot(md, N));
                     wi.z = fmaxf(wi.z, kEps);
@@ -638,7 +639,7 @@ extern "C" int liar_gpu_render_guided_device(liar_gpu_ctx* ctx, const liar_gpu_s
                 rc = guide_eval(ctx, guide, gb->gin, n_in, gb->gmix, kMixRender, st);
                 if (rc) return rc;
             }
-            k_g_shade<<<(n_in + kShadeThreads - 1) / kShadeThreads, kShadeThreads, 0, st>>>(
+            (S.n_tex > 0 ? k_g_shade<true> : k_g_shade<false>)<<<(n_in + kShadeThreads - 1) / kShadeThreads, kShadeThreads, 0, st>>>(
                 S, W, gb->P, gb->q[cur], gb->hits, n_in, gb->q[cur ^ 1], gb->gmix);
             e = cudaGetLastError();
             if (e != cudaSuccess) return ctx_cuda(ctx, e, "guided shade launch");

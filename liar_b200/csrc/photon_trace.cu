@@ -135,6 +135,7 @@ __global__ void __launch_bounds__(256) k_photon_emit(DScene S, PParams P, uint32
     pqueue_push(out, want, r, i);
 }
 
+template <bool TEX>
 __global__ void __launch_bounds__(128) k_photon_shade(DScene S, PParams P, PState st, PQueue in, const liar_hit* hits,
                                                       uint32_t n_in, PQueue out, liar_photon_buffers B,
                                                       unsigned long long* counters, uint32_t* status) {
@@ -203,7 +204,7 @@ __global__ void __launch_bounds__(128) k_photon_shade(DScene S, PParams P, PStat
                     }
                 }
                 if (gen < P.max_gen) {
-                    const Bsdf Bs = make_bsdf(S, M, H, lam);
+                    const Bsdf Bs = make_bsdf<TEX>(S, M, H, lam);
                     const float3 md = -d;
                     float3 wi = mk(dot(md, H.u), dot(md, H.v), dot(md, H.N));
                     wi.z = fmaxf(wi.z, kEps);
@@ -351,7 +352,7 @@ extern "C" int liar_gpu_photon_trace(liar_gpu_ctx* ctx, const liar_gpu_scene* sc
             if (rc) return rc;
             e = cudaMemsetAsync(w->q[cur ^ 1].count, 0, 4, st);
             if (e != cudaSuccess) return ctx_cuda(ctx, e, "photon queue");
-            k_photon_shade<<<(n_in + 127) / 128, 128, 0, st>>>(S, P, w->st, w->q[cur], w->hits, n_in, w->q[cur ^ 1], *out,
+            (S.n_tex > 0 ? k_photon_shade<true> : k_photon_shade<false>)<<<(n_in + 127) / 128, 128, 0, st>>>(S, P, w->st, w->q[cur], w->hits, n_in, w->q[cur ^ 1], *out,
                                                                w->counters, ctx->d_scratch + kStatusWord);
             cur ^= 1;
             e = cudaMemcpyAsync(w->h_count, w->q[cur].count, 4, cudaMemcpyDeviceToHost, st);

@@ -153,6 +153,7 @@ __global__ void __launch_bounds__(256) k_raygen(DScene S, WaveParams W, Paths P,
 }
 
 // the whole of tracePhoton after the intersection, for one queue entry
+template <bool TEX>
 __global__ void __launch_bounds__(128) k_shade(DScene S, WaveParams W, Paths P, Queue in, const liar_hit* hits,
                                                uint32_t n_in, Queue out, unsigned long long* stats) {
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -210,7 +211,7 @@ __global__ void __launch_bounds__(128) k_shade(DScene S, WaveParams W, Paths P, 
             } else {
                 const liar_material M = S.mats[mi];
                 if (shader_emits && M.emission >= 0) L += T * spec_eval(S, M.emission, lam, false);
-                const Bsdf B = make_bsdf(S, M, H, lam);  // Shader::bsdf at this wavelength
+                const Bsdf B = make_bsdf<TEX>(S, M, H, lam);  // Shader::bsdf at this wavelength
                 const float3 md = -d;
                 float3 wi = mk(dot(md, u), dot(md, v), dot(md, N));
                 wi.z = fmaxf(wi.z, kEps);
@@ -629,6 +630,22 @@ extern "C" int liar_gpu_scene_upload(liar_gpu_ctx* ctx, const liar_scene_desc* d
     // LightSky::doSetSceneBound: intersections with the sky lie 1000 scene radii away
     d.sky_distance = D.scene_radius > 0 ? 1e3f * D.scene_radius : 1e3f;
     d.stack_needed = mesh_stack_needed(s->mesh);
+    {
+        // the description's own device copy, which out-of-line device code reads it through
+        void* p = nullptr;
+        cudaError_t e = cudaMalloc(&p, sizeof(DScene));
+        if (e == cudaSuccess) {
+            s->buffers.push_back(p);
+            d.self = static_cast<const DScene*>(p);
+            e = cudaMemcpy(p, &d, sizeof(DScene), cudaMemcpyHostToDevice);
+        }
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            const int r = ctx_cuda(ctx, e, "scene description");
+            liar_gpu_scene_destroy(s);
+            return r;
+        }
+    }
     s->n_triangles = D.n_triangles;
     *out = s;
     return LIAR_OK;
@@ -714,7 +731,7 @@ int render_impl(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_rende
             if (rc) return rc;
             e = cudaMemsetAsync(rb->q[cur ^ 1].count, 0, 4, st);
             if (e != cudaSuccess) return ctx_cuda(ctx, e, "reset queue");
-            k_shade<<<(n_in + 127) / 128, 128, 0, st>>>(S, W, rb->P, rb->q[cur], rb->hits, n_in, rb->q[cur ^ 1],
+            (S.n_tex > 0 ? k_shade<true> : k_shade<false>)<<<(n_in + 127) / 128, 128, 0, st>>>(S, W, rb->P, rb->q[cur], rb->hits, n_in, rb->q[cur ^ 1],
                                                         rb->stats);
             e = cudaGetLastError();
             if (e != cudaSuccess) return ctx_cuda(ctx, e, "shade launch");

@@ -92,6 +92,7 @@ struct DScene {
     const float4* tex_pixels;    // image textures' XYZ pixels
     const uint8_t* noise_tables; // noise textures' permutation tables
     DRecovery rec;               // the recovery of image pixels (set when the scene has images)
+    const DScene* self;          // this description in device memory (for out-of-line lookups)
 };
 
 // ---- spectra
@@ -811,7 +812,11 @@ __device__ inline float noise_texture(const DScene& S, const liar_texture& T, fl
 
 // Texture::lookUp of a tree of uv textures: the transforms move (u, v), the boards pick a child
 // (without anti-aliasing a board always picks one), the leaf is a spectrum
-__device__ inline float texture_eval(const DScene& S, int t, float u, float v, float3 x, float lam, bool reflectant) {
+// kept out of line, reading the scene from its device copy: the shading kernels carry one call
+// instead of the lookup's registers and frame
+static __device__ __noinline__ float texture_eval(const DScene* __restrict__ G, int t, float u, float v, float3 x, float lam,
+                                           bool reflectant) {
+    const DScene& S = *G;
     // ABS / AFFINE nodes on the way down, applied to the leaf's value on the way back
     int post_type[8];
     float post_a[8], post_b[8];
@@ -881,13 +886,16 @@ __device__ inline float texture_eval(const DScene& S, int t, float u, float v, f
 }
 
 // a material parameter: its texture at the hit, else its constant spectrum
+// (TEX false: a kernel instance for scenes without textures, which carries no lookup)
+template <bool TEX>
 __device__ __forceinline__ float param_eval(const DScene& S, const liar_material& M, int k, const HitContext& H,
                                             float lam, bool reflectant) {
-    return M.tex[k] >= 0 ? texture_eval(S, M.tex[k], H.uv_u, H.uv_v, H.target, lam, reflectant)
-                         : spec_eval(S, M.spec[k], lam, reflectant);
+    if (TEX && M.tex[k] >= 0) return texture_eval(S.self, M.tex[k], H.uv_u, H.uv_v, H.target, lam, reflectant);
+    return spec_eval(S, M.spec[k], lam, reflectant);
 }
 
 // Shader::bsdf at one wavelength
+template <bool TEX = true>
 __device__ inline Bsdf make_bsdf(const DScene& S, const liar_material& M, const HitContext& H, float lam) {
     Bsdf B;
     B.type = (uint32_t)M.type;
@@ -900,28 +908,28 @@ __device__ inline Bsdf make_bsdf(const DScene& S, const liar_material& M, const 
     switch (M.type) {
         case LIAR_MAT_LAMBERT:
             B.caps = CAP_REFL | CAP_DIFF;
-            B.r = param_eval(S, M, 0, H, lam, true);
+            B.r = param_eval<TEX>(S, M, 0, H, lam, true);
             break;
         case LIAR_MAT_CONDUCTOR:
         case LIAR_MAT_COOK_TORRANCE:
             B.caps = M.type == LIAR_MAT_CONDUCTOR ? (CAP_REFL | CAP_SPEC) : (CAP_REFL | CAP_GLOSSY);
-            B.eta = fmaxf(param_eval(S, M, 0, H, lam, false), 1e-9f);
-            B.kappa = fmaxf(param_eval(S, M, 1, H, lam, false), 1e-9f);
-            B.r = param_eval(S, M, 2, H, lam, true);
+            B.eta = fmaxf(param_eval<TEX>(S, M, 0, H, lam, false), 1e-9f);
+            B.kappa = fmaxf(param_eval<TEX>(S, M, 1, H, lam, false), 1e-9f);
+            B.r = param_eval<TEX>(S, M, 2, H, lam, true);
             break;
         case LIAR_MAT_DIELECTRIC: {
             B.caps = CAP_REFL | CAP_TRANS | CAP_SPEC;
-            const float ior1 = fmaxf(param_eval(S, M, 1, H, lam, false), 1e-9f);
-            const float ior2 = fmaxf(param_eval(S, M, 0, H, lam, false), 1e-9f);
+            const float ior1 = fmaxf(param_eval<TEX>(S, M, 1, H, lam, false), 1e-9f);
+            const float ior2 = fmaxf(param_eval<TEX>(S, M, 0, H, lam, false), 1e-9f);
             B.ior = H.leaving ? ior2 / ior1 : ior1 / ior2;
-            B.r = param_eval(S, M, 2, H, lam, true);
-            B.t = param_eval(S, M, 3, H, lam, true);
+            B.r = param_eval<TEX>(S, M, 2, H, lam, true);
+            B.t = param_eval<TEX>(S, M, 3, H, lam, true);
             break;
         }
         case LIAR_MAT_WALTER: {
             B.caps = CAP_TRANS | CAP_GLOSSY;  // as constructed by Walter::Bsdf (walter.cpp:247)
-            float ei = fmaxf(param_eval(S, M, 1, H, lam, false), 1e-9f);
-            float et = fmaxf(param_eval(S, M, 0, H, lam, false), 1e-9f);
+            float ei = fmaxf(param_eval<TEX>(S, M, 1, H, lam, false), 1e-9f);
+            float et = fmaxf(param_eval<TEX>(S, M, 0, H, lam, false), 1e-9f);
             if (H.leaving) {
                 const float tmp = ei;
                 ei = et;
@@ -929,13 +937,13 @@ __device__ inline Bsdf make_bsdf(const DScene& S, const liar_material& M, const 
             }
             B.eta_i = ei;
             B.eta_t = et;
-            B.r = param_eval(S, M, 2, H, lam, true);
-            B.t = param_eval(S, M, 3, H, lam, true);
+            B.r = param_eval<TEX>(S, M, 2, H, lam, true);
+            B.t = param_eval<TEX>(S, M, 3, H, lam, true);
             break;
         }
         case LIAR_MAT_MIRROR:
             B.caps = CAP_REFL | CAP_SPEC;
-            B.r = param_eval(S, M, 0, H, lam, true);
+            B.r = param_eval<TEX>(S, M, 0, H, lam, true);
             break;
         default:
             B.caps = 0;
