@@ -238,6 +238,10 @@ typedef struct liar_scene_desc {
                                                             NULL: the barycentric coordinates of the hit */
     const float* texture_pixels; size_t n_texture_pixels; /* image textures: n x 4 (X, Y, Z, unused) */
     const uint8_t* noise_tables; size_t n_noise_tables;   /* noise textures' permutation tables (bytes) */
+    /* analytic spheres (Sphere, scenery/sphere.cpp): n x 4 (centre, radius) and each one's object;
+       sphere k is primitive n_triangles + k in hits. Their surface coordinates are
+       (phi / 2 pi, theta / pi) of the outward normal (sphere.cpp:130-152). */
+    const float* spheres; size_t n_spheres; const int32_t* sphere_object;
 } liar_scene_desc;
 
 /* PerspectiveCamera (src/liar/cameras/perspective_camera.cpp:406-434): direction/right/down are

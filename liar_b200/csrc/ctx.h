@@ -87,5 +87,8 @@ const QNode* mesh_nodes(const liar_gpu_mesh* m);
 const QTri* mesh_tris(const liar_gpu_mesh* m);
 uint32_t mesh_stack_needed(const liar_gpu_mesh* m);
 int mesh_device(const liar_gpu_mesh* m);
+int mesh_build_with_spheres(liar_gpu_ctx* ctx, const float* vertices, size_t n_vertices, const uint32_t* triangles,
+                            size_t n_triangles, const float* spheres, size_t n_spheres, const liar_build_opts* opts,
+                            liar_gpu_mesh** out);
 
 }  // namespace liar_gpu

@@ -282,7 +282,7 @@ __global__ void __launch_bounds__(128) k_dl_shade(DScene S, DParams W, DSamples 
     uint32_t n_sh = 0, n_ch = 0;
     const uint32_t sg = CAP_REFL | CAP_TRANS | CAP_SPEC | W.glossy;
     if (shading) {
-        HC = hit_context(S, o, d, (uint32_t)h.prim);
+        HC = hit_context(S, o, d, (uint32_t)h.prim, h.t);
         if (HC.mat < 0) {
             n_ch = more ? 1u : 0u;  // no shader: continue through the surface
         } else {
@@ -519,7 +519,7 @@ __global__ void __launch_bounds__(128) k_pm_estimate(DScene S, DParams W, DSampl
     const float4 r0 = reinterpret_cast<const float4*>(tin.rays + q)[0];
     const float4 r1 = reinterpret_cast<const float4*>(tin.rays + q)[1];
     const float3 d = mk(r1.x, r1.y, r1.z);
-    const HitContext HC = hit_context(S, mk(r0.x, r0.y, r0.z), d, (uint32_t)hits[q].prim);
+    const HitContext HC = hit_context(S, mk(r0.x, r0.y, r0.z), d, (uint32_t)hits[q].prim, hits[q].t);
     const float lam = P.lam[p];
     const int32_t* idx = g_idx + (size_t)i * k;
     const float r2 = g_d2[(size_t)i * k + cnt - 1];
@@ -585,7 +585,7 @@ __global__ void __launch_bounds__(128) k_fg_prep(DScene S, DTasks g, const liar_
         if (h.prim >= 0) {
             r0 = reinterpret_cast<const float4*>(g.rays + i)[0];
             r1 = reinterpret_cast<const float4*>(g.rays + i)[1];
-            const int mi = S.obj_mat[S.tri_obj[h.prim]];
+            const int mi = S.obj_mat[prim_object(S, (uint32_t)h.prim)];
             if (mi < 0) cont = true;
             else {
                 query = true;
@@ -643,7 +643,7 @@ __global__ void __launch_bounds__(128) k_fg_shade(DScene S, DParams W, DSamples 
         d = mk(r1.x, r1.y, r1.z);
         const liar_hit h = hits[gi];
         t = h.t;
-        HC = hit_context(S, o, d, (uint32_t)h.prim);
+        HC = hit_context(S, o, d, (uint32_t)h.prim, h.t);
         lam = P.lam[p];
         const liar_material Mat = S.mats[HC.mat];
         if (Mat.type != LIAR_MAT_NONE) {

@@ -170,12 +170,12 @@ __global__ void __launch_bounds__(128) k_g_prep(DScene S, GQueue in, const liar_
     if (h.prim >= 0) {
         const float4 r0 = reinterpret_cast<const float4*>(in.rays + q)[0];
         const float4 r1 = reinterpret_cast<const float4*>(in.rays + q)[1];
-        const int obj = S.tri_obj[h.prim];
+        const int obj = prim_object(S, (uint32_t)h.prim);
         const int mi = S.obj_mat[obj];
         if (mi >= 0) {
             const int type = S.mats[mi].type;
             if (type == LIAR_MAT_LAMBERT || type == LIAR_MAT_COOK_TORRANCE || type == LIAR_MAT_WALTER) {
-                const HitContext HC = hit_context(S, mk(r0.x, r0.y, r0.z), mk(r1.x, r1.y, r1.z), (uint32_t)h.prim);
+                const HitContext HC = hit_context(S, mk(r0.x, r0.y, r0.z), mk(r1.x, r1.y, r1.z), (uint32_t)h.prim, h.t);
                 x[0] = HC.target.x;
                 x[1] = HC.target.y;
                 x[2] = HC.target.z;
@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(kShadeThreads) k_g_shade(DScene S, GParams W, 
             r1 = reinterpret_cast<const float4*>(in.rays + q)[1];
             h = hits[q];
             if (h.prim >= 0) {
-                HC = hit_context(S, mk(r0.x, r0.y, r0.z), mk(r1.x, r1.y, r1.z), (uint32_t)h.prim);
+                HC = hit_context(S, mk(r0.x, r0.y, r0.z), mk(r1.x, r1.y, r1.z), (uint32_t)h.prim, h.t);
                 surface = HC.mat >= 0 && S.mats[HC.mat].type != LIAR_MAT_NONE;
                 if (surface) {
                     M = S.mats[HC.mat];

@@ -243,6 +243,15 @@ extern "C" int liar_gpu_mesh_build(liar_gpu_ctx* ctx, const float* vertices, siz
     if (!ctx || !out) return LIAR_ERR_INVALID;
     *out = nullptr;
     if (!vertices || !triangles) return ctx_fail(ctx, LIAR_ERR_INVALID, "null vertex or triangle array");
+    return liar_gpu::mesh_build_with_spheres(ctx, vertices, n_vertices, triangles, n_triangles, nullptr, 0, opts, out);
+}
+
+// the tree over a scene's triangles and analytic spheres (sphere k is primitive n_triangles + k)
+int liar_gpu::mesh_build_with_spheres(liar_gpu_ctx* ctx, const float* vertices, size_t n_vertices,
+                                      const uint32_t* triangles, size_t n_triangles, const float* spheres,
+                                      size_t n_spheres, const liar_build_opts* opts, liar_gpu_mesh** out) {
+    if (!ctx || !out) return LIAR_ERR_INVALID;
+    *out = nullptr;
     int rc = ctx_activate(ctx);
     if (rc) return rc;
     BuildOptions bo;
@@ -255,7 +264,7 @@ extern "C" int liar_gpu_mesh_build(liar_gpu_ctx* ctx, const float* vertices, siz
     const auto t0 = std::chrono::steady_clock::now();
     QBVHHost q;
     char msg[256] = {0};
-    rc = build_qbvh(vertices, n_vertices, triangles, n_triangles, bo, q, msg, sizeof(msg));
+    rc = build_qbvh(vertices, n_vertices, triangles, n_triangles, spheres, n_spheres, bo, q, msg, sizeof(msg));
     if (rc) return ctx_fail(ctx, rc, "mesh build: %s", msg);
     const auto t1 = std::chrono::steady_clock::now();
     liar_gpu_mesh* m = new (std::nothrow) liar_gpu_mesh();

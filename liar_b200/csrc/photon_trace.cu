@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(128) k_photon_shade(DScene S, PParams P, PStat
         float power = st.power[slot];
         bool caustic = st.caustic[slot] != 0;
         if (h.prim >= 0 && power != 0.0f) {
-            const HitContext H = hit_context(S, o, d, (uint32_t)h.prim);
+            const HitContext H = hit_context(S, o, d, (uint32_t)h.prim, h.t);
             const float3 hit_point = o + h.t * d;
             const int mi = H.mat;
             if (mi < 0) {

@@ -15,7 +15,8 @@
 //     count[c]      : the leaf's triangle count again (0 for inner nodes), kept for tools
 //
 //   QTri (48 B): v0, e1 = v1 - v0, e2 = v2 - v0 as three float4, the original triangle index in
-//   the w lane of the first. e1/e2 are the same IEEE single subtractions that the
+//   the w lane of the first; e1.w = 0. A sphere primitive has its centre in v0, its radius in
+//   e1.x and e1.w = 1. e1/e2 are the same IEEE single subtractions that the
 //   Moller-Trumbore test performs, so precomputing them changes no bit of the result.
 #pragma once
 #include <stddef.h>
@@ -69,6 +70,11 @@ struct BuildOptions {
 // Builds the tree; returns 0 on success, a negative LIAR_ERR_* otherwise (msg filled).
 int build_qbvh(const float* vertices, uint64_t n_vertices, const uint32_t* triangles, uint64_t n_triangles,
                const BuildOptions& opts, QBVHHost& out, char* msg, size_t msg_len);
+// The same over triangles and spheres (n_spheres x 4: centre, radius); sphere k is primitive
+// n_triangles + k, its QTri holding the centre in v0, the radius in e1.x and 1 in e1.w
+int build_qbvh(const float* vertices, uint64_t n_vertices, const uint32_t* triangles, uint64_t n_triangles,
+               const float* spheres, uint64_t n_spheres, const BuildOptions& opts, QBVHHost& out, char* msg,
+               size_t msg_len);
 void free_qbvh(QBVHHost& q);
 
 }  // namespace liar_gpu

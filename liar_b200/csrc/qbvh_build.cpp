@@ -271,13 +271,24 @@ struct Collapser {
 
 int build_qbvh(const float* V, uint64_t nv, const uint32_t* T, uint64_t nt, const BuildOptions& opts, QBVHHost& out,
                char* msg, size_t msg_len) {
+    return build_qbvh(V, nv, T, nt, nullptr, 0, opts, out, msg, msg_len);
+}
+
+int build_qbvh(const float* V, uint64_t nv, const uint32_t* T, uint64_t nt, const float* S, uint64_t ns,
+               const BuildOptions& opts, QBVHHost& out, char* msg, size_t msg_len) {
     auto fail = [&](int code, const char* what) {
         if (msg && msg_len) std::snprintf(msg, msg_len, "%s", what);
         return code;
     };
-    if (nt == 0) return fail(LIAR_ERR_INVALID, "mesh has no triangles");
-    if (nt >= (1ull << 27)) return fail(LIAR_ERR_INVALID, "too many triangles (limit 2^27 - 1 per mesh)");
-    if (!V || !T) return fail(LIAR_ERR_INVALID, "null vertex or triangle array");
+    if (nt + ns == 0) return fail(LIAR_ERR_INVALID, "mesh has no triangles");
+    if (nt + ns >= (1ull << 27)) return fail(LIAR_ERR_INVALID, "too many primitives (limit 2^27 - 1 per mesh)");
+    if (nt > 0 && (!V || !T)) return fail(LIAR_ERR_INVALID, "null vertex or triangle array");
+    if (ns > 0 && !S) return fail(LIAR_ERR_INVALID, "null sphere array");
+    for (uint64_t k = 0; k < ns; ++k)
+        if (!std::isfinite(S[4 * k]) || !std::isfinite(S[4 * k + 1]) || !std::isfinite(S[4 * k + 2]) ||
+            !(S[4 * k + 3] > 0.0f) || !std::isfinite(S[4 * k + 3]))
+            return fail(LIAR_ERR_INVALID, "sphere centre not finite or radius not positive");
+    const uint64_t np = nt + ns;
     const int max_leaf = opts.max_leaf_size <= 0 ? 4 : opts.max_leaf_size;
     if (max_leaf > 8) return fail(LIAR_ERR_INVALID, "max_leaf_size must be 1..8");
     const int bins = opts.sah_bins <= 0 ? 32 : std::min(opts.sah_bins, 256);
@@ -288,7 +299,7 @@ int build_qbvh(const float* V, uint64_t nv, const uint32_t* T, uint64_t nt, cons
     for (uint64_t k = 0; k < nt * 3; ++k)
         if (T[k] >= nv) return fail(LIAR_ERR_INVALID, "triangle vertex index out of range");
 
-    std::vector<PrimRef> prims(nt);
+    std::vector<PrimRef> prims(np);
     Box root;
     for (uint64_t i = 0; i < nt; ++i) {
         PrimRef& p = prims[i];
@@ -300,12 +311,25 @@ int build_qbvh(const float* V, uint64_t nv, const uint32_t* T, uint64_t nt, cons
         }
         root.grow(p.lo, p.hi);
     }
-    std::vector<uint32_t> idx(nt);
-    for (uint64_t i = 0; i < nt; ++i) idx[i] = (uint32_t)i;
-    std::vector<BNode> bnodes(2 * nt);
+    for (uint64_t k = 0; k < ns; ++k) {
+        // a sphere's box, rounded outward by the relative error of centre +- radius
+        PrimRef& p = prims[nt + k];
+        const float r = S[4 * k + 3];
+        for (int a = 0; a < 3; ++a) {
+            const float c = S[4 * k + a];
+            const float slack = (std::fabs(c) + r) * 2.4e-7f;
+            p.lo[a] = (c - r) - slack;
+            p.hi[a] = (c + r) + slack;
+            p.c[a] = c;
+        }
+        root.grow(p.lo, p.hi);
+    }
+    std::vector<uint32_t> idx(np);
+    for (uint64_t i = 0; i < np; ++i) idx[i] = (uint32_t)i;
+    std::vector<BNode> bnodes(2 * np);
     Builder b(prims, idx, bnodes, threads, max_leaf, bins, opts.traversal_cost > 0 ? opts.traversal_cost : 1.0);
     const int32_t r = b.alloc();
-    b.build(r, 0, (uint32_t)nt, 0);
+    b.build(r, 0, (uint32_t)np, 0);
     bnodes.resize((size_t)b.next_node.load());
 
     // conservative padding of every child box (absolute, relative to the scene's magnitude)
@@ -325,22 +349,30 @@ int build_qbvh(const float* V, uint64_t nv, const uint32_t* T, uint64_t nt, cons
     out.nodes = (QNode*)std::aligned_alloc(128, out.n_nodes * sizeof(QNode));
     if (!out.nodes) return fail(LIAR_ERR_OOM, "host allocation of nodes failed");
     std::memcpy(out.nodes, col.qnodes.data(), out.n_nodes * sizeof(QNode));
-    out.n_tris = nt;
-    out.tris = (QTri*)std::aligned_alloc(128, ((nt * sizeof(QTri) + 127) / 128) * 128);
+    out.n_tris = np;
+    out.tris = (QTri*)std::aligned_alloc(128, ((np * sizeof(QTri) + 127) / 128) * 128);
     if (!out.tris) {
         std::free(out.nodes);
         out.nodes = nullptr;
         return fail(LIAR_ERR_OOM, "host allocation of triangles failed");
     }
-    for (uint64_t k = 0; k < nt; ++k) {
+    for (uint64_t k = 0; k < np; ++k) {
         const uint32_t i = idx[k];
-        const float* a = V + 3 * T[3 * i + 0];
-        const float* bb = V + 3 * T[3 * i + 1];
-        const float* c = V + 3 * T[3 * i + 2];
         QTri& q = out.tris[k];
         int32_t ii = (int32_t)i;
         float wbits;
         std::memcpy(&wbits, &ii, 4);
+        if (i >= nt) {
+            // a sphere: centre and index bits, then the radius with the sphere flag in e1.w
+            const float* sp = S + 4 * (i - nt);
+            q.v0 = {sp[0], sp[1], sp[2], wbits};
+            q.e1 = {sp[3], 0.0f, 0.0f, 1.0f};
+            q.e2 = {0.0f, 0.0f, 0.0f, 0.0f};
+            continue;
+        }
+        const float* a = V + 3 * T[3 * i + 0];
+        const float* bb = V + 3 * T[3 * i + 1];
+        const float* c = V + 3 * T[3 * i + 2];
         q.v0 = {a[0], a[1], a[2], wbits};
         q.e1 = {bb[0] - a[0], bb[1] - a[1], bb[2] - a[2], 0.0f};
         q.e2 = {c[0] - a[0], c[1] - a[1], c[2] - a[2], 0.0f};

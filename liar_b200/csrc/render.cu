@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(128) k_shade(DScene S, WaveParams W, Paths P, 
             ++n_hit;
             if (gen == 0) P.alpha[p] = 1.0f;
             // ---- IntersectionContext of the hit (re-intersection, normals flipped toward -d, frame)
-            const HitContext H = hit_context(S, o, d, (uint32_t)h.prim);
+            const HitContext H = hit_context(S, o, d, (uint32_t)h.prim, h.t);
             const int light = H.light;
             const int mi = H.mat;
             const float3 target = H.target, ng = H.ng, N = H.N, u = H.u, v = H.v;
@@ -389,8 +389,17 @@ extern "C" int liar_gpu_scene_upload(liar_gpu_ctx* ctx, const liar_scene_desc* d
     if (!ctx || !desc || !out) return LIAR_ERR_INVALID;
     *out = nullptr;
     const liar_scene_desc& D = *desc;
-    if (!D.vertices || !D.triangles || !D.triangle_object || D.n_triangles == 0)
+    if (D.n_triangles == 0 && D.n_spheres == 0) return ctx_fail(ctx, LIAR_ERR_INVALID, "scene has no triangles");
+    if (D.n_triangles > 0 && (!D.vertices || !D.triangles || !D.triangle_object))
         return ctx_fail(ctx, LIAR_ERR_INVALID, "scene has no triangles");
+    if (D.n_spheres > 0 && (!D.spheres || !D.sphere_object)) return ctx_fail(ctx, LIAR_ERR_INVALID, "spheres missing");
+    for (size_t k = 0; k < D.n_spheres; ++k) {
+        const int32_t o = D.sphere_object[k];
+        if (o < 0 || (size_t)o >= D.n_objects) return ctx_fail(ctx, LIAR_ERR_INVALID, "sphere %zu: object index out of range", k);
+        const float* sp = D.spheres + 4 * k;
+        if (!std::isfinite(sp[0]) || !std::isfinite(sp[1]) || !std::isfinite(sp[2]) || !(sp[3] > 0.0f) || !std::isfinite(sp[3]))
+            return ctx_fail(ctx, LIAR_ERR_INVALID, "sphere %zu: centre not finite or radius not positive", k);
+    }
     if (!D.object_material || !D.object_light || D.n_objects == 0) return ctx_fail(ctx, LIAR_ERR_INVALID, "scene has no objects");
     if (!D.observer || D.n_observer < 2) return ctx_fail(ctx, LIAR_ERR_INVALID, "observer table needs two or more rows");
     if (D.n_lights > 4096) return ctx_fail(ctx, LIAR_ERR_INVALID, "too many lights (limit 4096)");
@@ -583,11 +592,19 @@ extern "C" int liar_gpu_scene_upload(liar_gpu_ctx* ctx, const liar_scene_desc* d
     s->device = ctx->device;
     static std::atomic<uint64_t> next_uid{1};
     s->uid = next_uid.fetch_add(1);
-    rc = liar_gpu_mesh_build(ctx, D.vertices, D.n_vertices, D.triangles, D.n_triangles, nullptr, &s->mesh);
+    rc = mesh_build_with_spheres(ctx, D.vertices, D.n_vertices, D.triangles, D.n_triangles, D.spheres, D.n_spheres,
+                                 nullptr, &s->mesh);
     DScene& d = s->d;
     if (!rc) rc = upload(ctx, s, D.vertices, 3 * D.n_vertices, &d.verts, "scene vertices");
     if (!rc) rc = upload(ctx, s, D.triangles, 3 * D.n_triangles, &d.tri_idx, "scene triangles");
     if (!rc) rc = upload(ctx, s, D.triangle_object, D.n_triangles, &d.tri_obj, "triangle objects");
+    if (!rc && D.n_spheres) {
+        const float* sp = nullptr;
+        rc = upload(ctx, s, D.spheres, 4 * D.n_spheres, &sp, "spheres");
+        d.spheres = reinterpret_cast<const float4*>(sp);
+        if (!rc) rc = upload(ctx, s, D.sphere_object, D.n_spheres, &d.sphere_obj, "sphere objects");
+    }
+    d.n_tris = (uint32_t)D.n_triangles;
     if (!rc && D.normals && D.triangle_normals) {
         rc = upload(ctx, s, D.normals, 3 * D.n_normals, &d.normals, "normals");
         if (!rc) rc = upload(ctx, s, D.triangle_normals, 3 * D.n_triangles, &d.tri_nrm, "triangle normals");

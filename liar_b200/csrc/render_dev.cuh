@@ -93,7 +93,15 @@ struct DScene {
     const uint8_t* noise_tables; // noise textures' permutation tables
     DRecovery rec;               // the recovery of image pixels (set when the scene has images)
     const DScene* self;          // this description in device memory (for out-of-line lookups)
+    const float4* spheres;       // analytic spheres: centre, radius; primitive n_tris + k
+    const int32_t* sphere_obj;
+    uint32_t n_tris;
 };
+
+// the object of a hit primitive (a triangle, or an analytic sphere past the triangles)
+__device__ __forceinline__ int prim_object(const DScene& S, uint32_t prim) {
+    return prim < S.n_tris ? S.tri_obj[prim] : S.sphere_obj[prim - S.n_tris];
+}
 
 // ---- spectra
 __device__ __forceinline__ float planck(float w, float T) {
@@ -652,8 +660,33 @@ struct HitContext {
     float uv_u, uv_v;  // surface coordinates: the triangle corners' (u, v) at the barycentrics, or those
 };
 
-__device__ inline HitContext hit_context(const DScene& S, float3 o, float3 d, uint32_t prim) {
+__device__ inline HitContext hit_context(const DScene& S, float3 o, float3 d, uint32_t prim, float t) {
     HitContext H;
+    if (prim >= S.n_tris) {
+        // Sphere::doLocalContext (sphere.cpp:130-175): the point reprojected onto the surface, the
+        // outward normal, uv from its spherical angles, dPoint/du along (-n.y, n.x, 0)
+        const float4 sp = S.spheres[prim - S.n_tris];
+        H.obj = S.sphere_obj[prim - S.n_tris];
+        H.light = S.obj_light[H.obj];
+        H.mat = S.obj_mat[H.obj];
+        const float3 c = mk(sp.x, sp.y, sp.z);
+        const float3 n0 = normal(o + t * d - c);
+        H.target = c + sp.w * n0;
+        H.uv_u = atan2f(n0.y, n0.x) * (0.5f / 3.14159265358979323846f);
+        H.uv_v = acosf(fminf(fmaxf(n0.z, -1.0f), 1.0f)) * (1.0f / 3.14159265358979323846f);
+        H.leaving = dot(d, n0) > 0.0f;
+        H.ng = dot(n0, -1.0f * d) < 0.0f ? -1.0f * n0 : n0;
+        H.N = H.ng;
+        float3 u = mk(-n0.y, n0.x, 0.0f);
+        u = u - dot(u, H.N) * H.N;
+        if (dot(u, u) < 1e-12f) {
+            const float3 ax = fabsf(H.N.x) < 0.9f ? mk(1, 0, 0) : mk(0, 1, 0);
+            u = cross(ax, H.N);
+        }
+        H.u = normal(u);
+        H.v = cross(H.N, H.u);
+        return H;
+    }
     H.obj = S.tri_obj[prim];
     H.light = S.obj_light[H.obj];
     H.mat = S.obj_mat[H.obj];

@@ -200,8 +200,17 @@ __device__ __forceinline__ bool trace_step(const QNode* __restrict__ nodes, cons
             const QTri* tp = tris + first + k;
             const float4 a = ld_hint(&tp->v0, pol_tree), e1 = ld_hint(&tp->e1, pol_tree), e2 = ld_hint(&tp->e2, pol_tree);
             float t, u, v;
-            if (tri_intersect_exact(st.ox, st.oy, st.oz, st.dx, st.dy, st.dz, a.x, a.y, a.z, e1.x, e1.y, e1.z, e2.x,
-                                    e2.y, e2.z, t, u, v)) {
+            bool hit;
+            if (e1.w != 0.0f) {
+                // a sphere: its nearer root beyond tmin, else the farther one
+                float t1;
+                hit = sphere_intersect_exact(st.ox, st.oy, st.oz, st.dx, st.dy, st.dz, a.x, a.y, a.z, e1.x, t, t1);
+                if (hit && !(t > st.tmin)) t = t1;
+            } else {
+                hit = tri_intersect_exact(st.ox, st.oy, st.oz, st.dx, st.dy, st.dz, a.x, a.y, a.z, e1.x, e1.y, e1.z,
+                                          e2.x, e2.y, e2.z, t, u, v);
+            }
+            if (hit) {
                 const int prim = __float_as_int(a.w);
                 if (ANY) {
                     if (t > st.tmin && t < st.tmax) {

@@ -23,11 +23,18 @@
 #define TX_SUB(a, b) __fsub_rn((a), (b))
 #define TX_MUL(a, b) __fmul_rn((a), (b))
 #define TX_RCP(a) __frcp_rn(a)
+#define TX_DIV(a, b) __fdiv_rn((a), (b))
+#define TX_SQRT(a) __fsqrt_rn(a)
 #else
 #define TX_ADD(a, b) ((a) + (b))
 #define TX_SUB(a, b) ((a) - (b))
 #define TX_MUL(a, b) ((a) * (b))
 #define TX_RCP(a) (1.0f / (a))
+#define TX_DIV(a, b) ((a) / (b))
+#define TX_SQRT(a) std::sqrt(a)
+#endif
+#ifndef __CUDA_ARCH__
+#include <cmath>
 #endif
 
 namespace liar_gpu {
@@ -56,6 +63,29 @@ TX_HD bool tri_intersect_exact(float ox, float oy, float oz, float dx, float dy,
     t_out = TX_MUL(TX_ADD(TX_ADD(TX_MUL(e2x, qx), TX_MUL(e2y, qy)), TX_MUL(e2z, qz)), inv);
     u_out = u;
     v_out = v;
+    return true;
+}
+
+// The ray o + t d against the sphere |p - c| = r (Sphere::doIntersect, scenery/sphere.cpp:100-128,
+// through Lass's intersect(sphere, ray), whose source is not part of the reference): the roots of
+// a t^2 + 2 b t + c = 0 with a = d.d, b = (o - c).d, c = |o - c|^2 - r^2, taken in the cancellation-
+// free form q = -(b + sign(b) sqrt(b^2 - a c)), t = q / a and c / q (Press et al., Numerical Recipes
+// 5.6). Returns the roots in increasing order; false when the ray misses. Correctly rounded
+// operations in a fixed order, as in the triangle test.
+TX_HD bool sphere_intersect_exact(float ox, float oy, float oz, float dx, float dy, float dz, float cx, float cy,
+                                  float cz, float r, float& t0, float& t1) {
+    const float sx = TX_SUB(ox, cx), sy = TX_SUB(oy, cy), sz = TX_SUB(oz, cz);
+    const float a = TX_ADD(TX_ADD(TX_MUL(dx, dx), TX_MUL(dy, dy)), TX_MUL(dz, dz));
+    const float b = TX_ADD(TX_ADD(TX_MUL(sx, dx), TX_MUL(sy, dy)), TX_MUL(sz, dz));
+    const float c = TX_SUB(TX_ADD(TX_ADD(TX_MUL(sx, sx), TX_MUL(sy, sy)), TX_MUL(sz, sz)), TX_MUL(r, r));
+    const float disc = TX_SUB(TX_MUL(b, b), TX_MUL(a, c));
+    if (!(disc >= 0.0f) || !(a > 0.0f)) return false;
+    const float root = TX_SQRT(disc);
+    const float q = b >= 0.0f ? -TX_ADD(b, root) : TX_SUB(root, b);
+    if (q == 0.0f) return false;
+    const float ta = TX_DIV(q, a), tb = TX_DIV(c, q);
+    t0 = ta < tb ? ta : tb;
+    t1 = ta < tb ? tb : ta;
     return true;
 }
 

@@ -53,7 +53,8 @@ class CSceneDesc(C.Structure):
                 ("spectrum_pool", _P), ("pool_size", _S), ("lights", _P), ("n_lights", _S),
                 ("observer", _P), ("n_observer", _S), ("scene_radius", C.c_float),
                 ("textures", _P), ("n_textures", _S), ("triangle_uvs", _P),
-                ("texture_pixels", _P), ("n_texture_pixels", _S), ("noise_tables", _P), ("n_noise_tables", _S)]
+                ("texture_pixels", _P), ("n_texture_pixels", _S), ("noise_tables", _P), ("n_noise_tables", _S),
+                ("spheres", _P), ("n_spheres", _S), ("sphere_object", _P)]
 
 
 class CCamera(C.Structure):
@@ -108,15 +109,18 @@ class FlatScene:
     triangle_uvs: np.ndarray | None = None  # n_triangles x 3 x 2, when a texture needs them
     texture_pixels: np.ndarray | None = None  # image textures' pixels, n x 4 (X, Y, Z, 0)
     noise_tables: np.ndarray | None = None    # noise textures' permutation tables, bytes
+    spheres: np.ndarray | None = None         # analytic spheres, n x 4 (centre, radius)
+    sphere_object: np.ndarray | None = None
     keep: list = field(default_factory=list)
 
     def desc(self) -> CSceneDesc:
         d = CSceneDesc()
-        d.vertices = self.vertices.ctypes.data
-        d.n_vertices = self.vertices.shape[0]
-        d.triangles = self.triangles.ctypes.data
-        d.n_triangles = self.triangles.shape[0]
-        d.triangle_object = self.triangle_object.ctypes.data
+        if self.triangles.shape[0]:
+            d.vertices = self.vertices.ctypes.data
+            d.n_vertices = self.vertices.shape[0]
+            d.triangles = self.triangles.ctypes.data
+            d.n_triangles = self.triangles.shape[0]
+            d.triangle_object = self.triangle_object.ctypes.data
         if self.normals is not None and self.triangle_normals is not None:
             d.normals = self.normals.ctypes.data
             d.n_normals = self.normals.shape[0]
@@ -146,6 +150,10 @@ class FlatScene:
         if self.noise_tables is not None:
             d.noise_tables = self.noise_tables.ctypes.data
             d.n_noise_tables = self.noise_tables.size
+        if self.spheres is not None and len(self.spheres):
+            d.spheres = self.spheres.ctypes.data
+            d.n_spheres = self.spheres.shape[0]
+            d.sphere_object = self.sphere_object.ctypes.data
         return d
 
 
@@ -162,6 +170,7 @@ class _Builder:
         self.tex_pixels, self.n_tex_pixels = [], 0
         self.noise_tables, self.n_noise = [], 0
         self.tri_uvs = []  # per object: n x 3 x 2 corner uvs, or None for the barycentric ones
+        self.spheres, self.sphere_obj = [], []
         self.M = None  # current local-to-world affine matrix (None: identity)
 
     # -- transformations (scenery/transformation.cpp, translation.cpp)
@@ -436,17 +445,41 @@ class _Builder:
             L.emission_samples = int(obj.numberOfEmissionSamples)
             L.spectrum = self.spectrum(obj.radiance)
             self.lights.append(L)
+        elif isinstance(obj, scenery.Sphere) and obj.analytic and self.similarity() is not None:
+            # an analytic sphere: centre and radius through the similarity (uniform scale)
+            scale = self.similarity()
+            obj_index = len(self.obj_mat)
+            self.obj_mat.append(self.material(obj.shader or inherited))
+            self.obj_light.append(-1)
+            c = self.point(obj.center)
+            self.spheres.append((float(c[0]), float(c[1]), float(c[2]), obj.radius * scale))
+            self.sphere_obj.append(obj_index)
         elif hasattr(obj, "triangles"):
             self.geometry(obj, obj.shader or inherited, -1)
         else:
             raise NotImplementedError(f"scene object {type(obj).__name__} is not on the GPU path")
 
+    def similarity(self) -> float | None:
+        """The uniform scale of the current transformation when it is a similarity (rotation or
+        mirror times a uniform scale, plus a translation), else None."""
+        if self.M is None:
+            return 1.0
+        A = self.M[:3, :3]
+        G = A.T @ A
+        s2 = G[0, 0]
+        if s2 <= 0 or not np.allclose(G, s2 * np.eye(3), rtol=1e-9, atol=1e-12 * s2):
+            return None
+        return float(np.sqrt(s2))
+
     def finish(self) -> FlatScene:
-        if not self.verts:
+        if not self.verts and not self.spheres:
             raise ValueError("the scene has no geometry")
-        V = np.ascontiguousarray(np.concatenate(self.verts), dtype=np.float32)
-        T = np.ascontiguousarray(np.concatenate(self.tris), dtype=np.uint32)
-        lo, hi = V.min(axis=0).astype(np.float64), V.max(axis=0).astype(np.float64)
+        V = np.ascontiguousarray(np.concatenate(self.verts), dtype=np.float32) if self.verts else np.zeros((0, 3), np.float32)
+        T = np.ascontiguousarray(np.concatenate(self.tris), dtype=np.uint32) if self.tris else np.zeros((0, 3), np.uint32)
+        SP = np.asarray(self.spheres, dtype=np.float32).reshape(-1, 4)
+        ext = [V] + ([SP[:, :3] - SP[:, 3:], SP[:, :3] + SP[:, 3:]] if len(SP) else [])
+        E = np.concatenate([e for e in ext if len(e)])
+        lo, hi = E.min(axis=0).astype(np.float64), E.max(axis=0).astype(np.float64)
         radius = float(0.5 * np.linalg.norm(hi - lo))
         for L in self.lights:
             if L.type == LIGHT_SKY:
@@ -454,7 +487,7 @@ class _Builder:
                 L.power = math.pi * 4 * math.pi * radius ** 2 * self.spec_ids_lum(L.spectrum)
         return FlatScene(
             vertices=V, triangles=T,
-            triangle_object=np.ascontiguousarray(np.concatenate(self.tri_obj), dtype=np.int32),
+            triangle_object=np.ascontiguousarray(np.concatenate(self.tri_obj), dtype=np.int32) if self.tri_obj else np.zeros(0, np.int32),
             normals=np.ascontiguousarray(np.concatenate(self.norms), dtype=np.float32) if self.has_normals else None,
             triangle_normals=np.ascontiguousarray(np.concatenate(self.tri_norms), dtype=np.int32) if self.has_normals else None,
             object_material=np.asarray(self.obj_mat, dtype=np.int32),
@@ -469,6 +502,8 @@ class _Builder:
             triangle_uvs=self.triangle_uvs(),
             texture_pixels=np.ascontiguousarray(np.concatenate(self.tex_pixels)) if self.tex_pixels else None,
             noise_tables=np.ascontiguousarray(np.concatenate(self.noise_tables)) if self.noise_tables else None,
+            spheres=np.ascontiguousarray(SP) if len(SP) else None,
+            sphere_object=np.asarray(self.sphere_obj, dtype=np.int32) if len(SP) else None,
         )
 
     def triangle_uvs(self) -> np.ndarray | None:

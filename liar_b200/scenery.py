@@ -127,18 +127,25 @@ class TriangleMesh(SceneObject):
 
 
 class Sphere(SceneObject):
-    """Sphere(center, radius), flattened into a geodesic triangle mesh with exact normals."""
+    """Sphere(center, radius) (scenery/sphere.cpp): an analytic sphere, intersected exactly on
+    the GPU. With ``subdivisions`` it is flattened into a geodesic triangle mesh with exact normals
+    instead; a sphere that is an area light's surface, or that sits under a transformation that is
+    not a similarity, always is (with 5 subdivisions unless given)."""
 
-    def __init__(self, center=(0, 0, 0), radius=1.0, subdivisions: int = 5):
+    def __init__(self, center=(0, 0, 0), radius=1.0, subdivisions: int | None = None):
         super().__init__()
         self.center = tuple(float(x) for x in center)
         self.radius = float(radius)
-        self.subdivisions = int(subdivisions)
+        self.subdivisions = None if subdivisions is None else int(subdivisions)
+
+    @property
+    def analytic(self) -> bool:
+        return self.subdivisions is None
 
     def triangles(self):
         from .scenes import icosahedron, subdivide
         v, f = icosahedron()
-        for _ in range(self.subdivisions):
+        for _ in range(self.subdivisions if self.subdivisions is not None else 5):
             v, f = subdivide(v, f)
         verts = (v * self.radius + np.asarray(self.center)).astype(np.float32)
         return verts, f.astype(np.uint32), v.astype(np.float32), f.astype(np.int32)
@@ -148,7 +155,7 @@ class Sphere(SceneObject):
         triangle across the seam and taken from the other corners at the poles."""
         from .scenes import icosahedron, subdivide
         v, f = icosahedron()
-        for _ in range(self.subdivisions):
+        for _ in range(self.subdivisions if self.subdivisions is not None else 5):
             v, f = subdivide(v, f)
         n = v / np.linalg.norm(v, axis=1, keepdims=True)
         u = np.arctan2(n[:, 1], n[:, 0]) / (2 * np.pi)

@@ -33,6 +33,7 @@ extern "C" int oracle_tri_intersect(const float* o, const float* d, const float*
                                     float* t_out, float* u_out, float* v_out);
 extern "C" void* oracle_tree_build(const float* V, uint64_t nv, const uint32_t* T, uint64_t nt);
 extern "C" void oracle_tree_free(void* tree);
+extern "C" void oracle_tree_set_spheres(void* tree, const float* spheres, uint64_t n, uint64_t n_tris);
 
 namespace oracle_internal {
 struct Ray {
@@ -98,6 +99,7 @@ struct SceneIn {
     const float* triangle_uvs;
     const float* texture_pixels; uint64_t n_texture_pixels;
     const uint8_t* noise_tables; uint64_t n_noise_tables;
+    const float* spheres; uint64_t n_spheres; const int32_t* sphere_object;
 };
 struct RenderIn {
     Camera camera;
@@ -128,7 +130,8 @@ static_assert(offsetof(Material, tex) == offsetof(liar_material, tex) &&
                   offsetof(RenderIn, filter) == offsetof(liar_render_desc, filter) &&
                   offsetof(Texture, pixels) == offsetof(liar_texture, pixels) &&
                   offsetof(SceneIn, texture_pixels) == offsetof(liar_scene_desc, texture_pixels) &&
-                  offsetof(SceneIn, noise_tables) == offsetof(liar_scene_desc, noise_tables),
+                  offsetof(SceneIn, noise_tables) == offsetof(liar_scene_desc, noise_tables) &&
+                  offsetof(SceneIn, sphere_object) == offsetof(liar_scene_desc, sphere_object),
               "oracle mirrors out of step with include/liar_gpu.h");
 
 // The photon maps of a PhotonMapper render (photon_mapper.cpp:798-835) as the oracle gets them:
@@ -879,6 +882,29 @@ float param(const Scene& S, const Material& M, int k, float u, float v, V x, flo
 Ctx hit_ctx(const Scene& S, V o, V d, const Hit& h) {
     Ctx c;
     const uint32_t prim = (uint32_t)h.prim;
+    if (prim >= S.in.n_triangles) {
+        // Sphere::doLocalContext (sphere.cpp:130-175): the point reprojected onto the surface, the
+        // outward normal, uv of its spherical angles, dPoint/du along (-n.y, n.x, 0)
+        const uint64_t k = prim - S.in.n_triangles;
+        const float* sp = S.in.spheres + 4 * k;
+        const V C{sp[0], sp[1], sp[2]};
+        c.obj = S.in.sphere_object[k];
+        c.light = S.in.object_light[c.obj];
+        c.mi = S.in.object_material[c.obj];
+        const V n0 = unit((o + h.t * d) - C);
+        c.target = C + sp[3] * n0;
+        c.uv_u = std::atan2(n0.y, n0.x) * (0.5f / 3.14159265358979323846f);
+        c.uv_v = std::acos(std::min(std::max(n0.z, -1.0f), 1.0f)) * (1.0f / 3.14159265358979323846f);
+        c.leaving = dot(d, n0) > 0;
+        c.ng = dot(n0, -d) < 0 ? -n0 : n0;
+        c.N = c.ng;
+        V u{-n0.y, n0.x, 0.0f};
+        u = u - dot(u, c.N) * c.N;
+        if (dot(u, u) < 1e-12f) u = cross(std::fabs(c.N.x) < 0.9f ? V{1, 0, 0} : V{0, 1, 0}, c.N);
+        c.u = unit(u);
+        c.v = cross(c.N, c.u);
+        return c;
+    }
     c.obj = S.in.triangle_object[prim];
     c.light = S.in.object_light[c.obj];
     c.mi = S.in.object_material[c.obj];
@@ -1526,6 +1552,7 @@ void* oracle_scene_create(const SceneIn* in) {
     Scene* S = new Scene();
     S->in = *in;
     S->tree = oracle_tree_build(in->vertices, in->n_vertices, in->triangles, in->n_triangles);
+    if (in->n_spheres) oracle_tree_set_spheres(S->tree, in->spheres, in->n_spheres, in->n_triangles);
     S->spec_max.assign(in->n_spectra, 0);
     for (uint64_t k = 0; k < in->n_spectra; ++k) {
         const Spectrum& s = in->spectra[k];
@@ -1637,7 +1664,7 @@ static void trace_photon_rec(const Scene& S, const PhotonIn& D, const Sampler& s
     if (h.prim < 0) return;
     const V hit = o + h.t * d;
     const uint32_t prim = (uint32_t)h.prim;
-    const int obj = S.in.triangle_object[prim];
+    const int obj = prim < S.in.n_triangles ? S.in.triangle_object[prim] : S.in.sphere_object[prim - S.in.n_triangles];
     const int mi = S.in.object_material[obj];
     if (mi < 0) {  // no shader: entering or leaving something
         if (gen >= D.max_ray_generation) return;
@@ -1669,46 +1696,10 @@ static void trace_photon_rec(const Scene& S, const PhotonIn& D, const Sampler& s
     }
     if (gen >= D.max_ray_generation) return;
     // the same local context as the path tracer
-    const uint32_t* tr = S.in.triangles + 3 * (size_t)prim;
-    const float* pa = S.in.vertices + 3 * tr[0];
-    const float* pb = S.in.vertices + 3 * tr[1];
-    const float* pc = S.in.vertices + 3 * tr[2];
-    const V A{pa[0], pa[1], pa[2]};
-    const V e1 = V{pb[0], pb[1], pb[2]} - A, e2 = V{pc[0], pc[1], pc[2]} - A;
-    const V ng0 = unit(cross(e1, e2));
-    V ns = ng0;
-    float tt, bu = 0, bv = 0;
-    const float oo[3] = {o.x, o.y, o.z}, dd[3] = {d.x, d.y, d.z};
-    if (!oracle_tri_intersect(oo, dd, pa, pb, pc, &tt, &bu, &bv)) bu = bv = 0;
-    float uv_u, uv_v;
-    hit_uv(S, prim, bu, bv, uv_u, uv_v);
-    if (S.in.triangle_normals && S.in.normals) {
-        const int32_t* tn = S.in.triangle_normals + 3 * (size_t)prim;
-        if (tn[0] >= 0 && tn[1] >= 0 && tn[2] >= 0) {
-            const float* n0 = S.in.normals + 3 * tn[0];
-            const float* n1 = S.in.normals + 3 * tn[1];
-            const float* n2 = S.in.normals + 3 * tn[2];
-            const float w0 = 1 - bu - bv;
-            ns = unit(w0 * V{n0[0], n0[1], n0[2]} + bu * V{n1[0], n1[1], n1[2]} + bv * V{n2[0], n2[1], n2[2]});
-        }
-    }
-    const bool leaving = dot(d, ng0) > 0;
-    const V ng = dot(ng0, -d) < 0 ? -ng0 : ng0;
-    const V N = dot(ns, -d) < 0 ? -ns : ns;
-    V u = e1 - dot(e1, N) * N, v = e2 - dot(e2, N) * N;
-    const float su = dot(u, u), sv = dot(v, v);
-    if (std::max(su, sv) < 1e-3f * std::max(dot(e1, e1), dot(e2, e2))) {
-        const V ax = std::fabs(N.x) < 0.9f ? V{1, 0, 0} : V{0, 1, 0};
-        u = cross(ax, N);
-        v = cross(N, u);
-    }
-    if (su >= sv) {
-        u = unit(u);
-        v = cross(N, u);
-    } else {
-        v = unit(v);
-        u = cross(v, N);
-    }
+    const Ctx lc = hit_ctx(S, o, d, h);
+    const bool leaving = lc.leaving;
+    const V ng = lc.ng, N = lc.N, u = lc.u, v = lc.v;
+    const float uv_u = lc.uv_u, uv_v = lc.uv_v;
     Bsdf B{};
     B.type = M.type;
     B.mdf = M.mdf;

@@ -64,6 +64,24 @@ int oracle_tri_intersect(const float* o, const float* d, const float* a, const f
     return 1;
 }
 
+// ray / sphere: the roots of a t^2 + 2 b t + c = 0 (a = d.d, b = (o - c).d, c = |o - c|^2 - r^2)
+// by q = -(b + sign(b) sqrt(b^2 - a c)), t = q / a, c / q (Numerical Recipes 5.6), in increasing order
+int oracle_sphere_intersect(const float* o, const float* d, const float* center, float r, float* t0, float* t1) {
+    const float sx = o[0] - center[0], sy = o[1] - center[1], sz = o[2] - center[2];
+    const float a = (d[0] * d[0] + d[1] * d[1]) + d[2] * d[2];
+    const float b = (sx * d[0] + sy * d[1]) + sz * d[2];
+    const float c = ((sx * sx + sy * sy) + sz * sz) - r * r;
+    const float disc = b * b - a * c;
+    if (!(disc >= 0.0f) || !(a > 0.0f)) return 0;
+    const float root = std::sqrt(disc);
+    const float q = b >= 0.0f ? -(b + root) : root - b;
+    if (q == 0.0f) return 0;
+    const float ta = q / a, tb = c / q;
+    *t0 = std::min(ta, tb);
+    *t1 = std::max(ta, tb);
+    return 1;
+}
+
 }  // extern "C"
 
 namespace {
@@ -125,6 +143,8 @@ struct Tree {
     std::vector<BNode> nodes;
     std::vector<uint32_t> idx;
     Mesh mesh;
+    std::vector<float> spheres;  // n x 4: centre, radius; primitive index n_tris + k
+    uint32_t n_tris = 0;
 };
 
 void tri_bounds(const Mesh& m, uint32_t i, float* lo, float* hi) {
@@ -200,9 +220,21 @@ oracle_hit trace_tree(const Tree& t, const oracle_ray& r, bool any) {
     }
     int32_t best = -1;
     float tbest = any ? r.tmax : r.tmax * (1.0f - kTol);
+    // spheres, by brute force: the nearer root beyond tmin, else the farther one
+    for (size_t k = 0; 4 * k < t.spheres.size(); ++k) {
+        float t0, t1;
+        if (!oracle_sphere_intersect(o, d, &t.spheres[4 * k], t.spheres[4 * k + 3], &t0, &t1)) continue;
+        const float th = t0 > r.tmin ? t0 : t1;
+        const int32_t prim = (int32_t)(t.n_tris + k);
+        if (any) {
+            if (th > r.tmin && th < r.tmax) return {prim, th};
+        } else {
+            offer(prim, th, r, best, tbest);
+        }
+    }
     int32_t stack[128];
     int sp = 0;
-    stack[sp++] = 0;
+    if (!t.nodes.empty()) stack[sp++] = 0;
     while (sp > 0) {
         const BNode& n = t.nodes[stack[--sp]];
         float tn;
@@ -293,6 +325,13 @@ int oracle_tree_trace(void* tree, const oracle_ray* rays, uint64_t n, oracle_hit
 
 void oracle_tree_free(void* tree) { delete static_cast<Tree*>(tree); }
 
+// analytic spheres (n x 4: centre, radius) beside the tree's n_tris triangles
+void oracle_tree_set_spheres(void* tree, const float* spheres, uint64_t n, uint64_t n_tris) {
+    Tree& t = *static_cast<Tree*>(tree);
+    t.spheres.assign(spheres, spheres + 4 * n);
+    t.n_tris = (uint32_t)n_tris;
+}
+
 int oracle_hardware_threads(void) { return (int)std::max(1u, std::thread::hardware_concurrency()); }
 
 }  // extern "C"
@@ -308,13 +347,13 @@ struct Hit {
 };
 bool tree_any(void* tree, const Ray& r) {
     const Tree& t = *static_cast<Tree*>(tree);
-    if (t.nodes.empty()) return false;
+    if (t.nodes.empty() && t.spheres.empty()) return false;
     const oracle_ray rr{r.ox, r.oy, r.oz, r.tmin, r.dx, r.dy, r.dz, r.tmax};
     return trace_tree(t, rr, true).prim >= 0;
 }
 Hit tree_closest(void* tree, const Ray& r) {
     const Tree& t = *static_cast<Tree*>(tree);
-    if (t.nodes.empty()) return {-1, INFINITY};
+    if (t.nodes.empty() && t.spheres.empty()) return {-1, INFINITY};
     const oracle_ray rr{r.ox, r.oy, r.oz, r.tmin, r.dx, r.dy, r.dz, r.tmax};
     const oracle_hit h = trace_tree(t, rr, false);
     return {h.prim, h.t};
