@@ -81,8 +81,10 @@ inline int ctx_ensure_pipeline(liar_gpu_ctx* ctx) {
     return LIAR_OK;
 }
 
+// n_dev: when given, the ray count in device memory (at most n, which sizes the launch)
 int trace_mesh_internal(liar_gpu_ctx* ctx, const liar_gpu_mesh* mesh, const liar_ray* d_rays, size_t n,
-                        liar_hit* d_hits, int any_hit, cudaStream_t st, int counter_word);
+                        liar_hit* d_hits, int any_hit, cudaStream_t st, int counter_word,
+                        const uint32_t* n_dev = nullptr);
 const QNode* mesh_nodes(const liar_gpu_mesh* m);
 const QTri* mesh_tris(const liar_gpu_mesh* m);
 uint32_t mesh_stack_needed(const liar_gpu_mesh* m);

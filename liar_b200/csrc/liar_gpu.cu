@@ -73,7 +73,8 @@ namespace {
 
 template <bool ANY, int S, int BLOCK, bool COUNT>
 int launch_trace_t(liar_gpu_ctx* ctx, const liar_gpu_mesh* m, const liar_ray* d_rays, uint32_t n, liar_hit* d_hits,
-                   TraceCounters* d_counters, cudaStream_t st, uint32_t* d_counter, uint32_t* d_status) {
+                   TraceCounters* d_counters, cudaStream_t st, uint32_t* d_counter, uint32_t* d_status,
+                   const uint32_t* n_dev) {
     auto kern = trace_kernel<ANY, S, BLOCK, COUNT>;
     const size_t smem = (size_t)S * BLOCK * 8;
     int& per_sm = ctx->occupancy[(const void*)kern];
@@ -92,23 +93,25 @@ int launch_trace_t(liar_gpu_ctx* ctx, const liar_gpu_mesh* m, const liar_ray* d_
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "reset work counter");
     const uint32_t batch = trace_batch(n, (uint32_t)blocks * (BLOCK / 32));
     kern<<<(unsigned)blocks, BLOCK, smem, st>>>(m->d_nodes, m->d_tris, d_rays, d_hits, n, d_counter, d_status,
-                                             d_counters, batch);
+                                             d_counters, batch, n_dev);
     return ctx_cuda(ctx, cudaGetLastError(), "trace kernel launch");
 }
 
 template <int S, int BLOCK>
 int launch_trace_sb(liar_gpu_ctx* ctx, const liar_gpu_mesh* m, const liar_ray* d_rays, uint32_t n, liar_hit* d_hits,
-                    int any_hit, TraceCounters* d_counters, cudaStream_t st, uint32_t* d_counter, uint32_t* d_status) {
+                    int any_hit, TraceCounters* d_counters, cudaStream_t st, uint32_t* d_counter, uint32_t* d_status,
+                    const uint32_t* n_dev) {
     const bool cnt = d_counters != nullptr;
     if (any_hit)
-        return cnt ? launch_trace_t<true, S, BLOCK, true>(ctx, m, d_rays, n, d_hits, d_counters, st, d_counter, d_status)
-                   : launch_trace_t<true, S, BLOCK, false>(ctx, m, d_rays, n, d_hits, d_counters, st, d_counter, d_status);
-    return cnt ? launch_trace_t<false, S, BLOCK, true>(ctx, m, d_rays, n, d_hits, d_counters, st, d_counter, d_status)
-               : launch_trace_t<false, S, BLOCK, false>(ctx, m, d_rays, n, d_hits, d_counters, st, d_counter, d_status);
+        return cnt ? launch_trace_t<true, S, BLOCK, true>(ctx, m, d_rays, n, d_hits, d_counters, st, d_counter, d_status, n_dev)
+                   : launch_trace_t<true, S, BLOCK, false>(ctx, m, d_rays, n, d_hits, d_counters, st, d_counter, d_status, n_dev);
+    return cnt ? launch_trace_t<false, S, BLOCK, true>(ctx, m, d_rays, n, d_hits, d_counters, st, d_counter, d_status, n_dev)
+               : launch_trace_t<false, S, BLOCK, false>(ctx, m, d_rays, n, d_hits, d_counters, st, d_counter, d_status, n_dev);
 }
 
 int launch_trace(liar_gpu_ctx* ctx, const liar_gpu_mesh* m, const liar_ray* d_rays, size_t n_rays, liar_hit* d_hits,
-                 int any_hit, TraceCounters* d_counters, cudaStream_t st, uint32_t* d_counter, uint32_t* d_status) {
+                 int any_hit, TraceCounters* d_counters, cudaStream_t st, uint32_t* d_counter, uint32_t* d_status,
+                 const uint32_t* n_dev = nullptr) {
     if (n_rays == 0) return LIAR_OK;
     // the work counter of the persistent warps overshoots n by BATCH per warp; 2^31 keeps it far from wrapping
     if (n_rays > (1ull << 31)) return ctx_fail(ctx, LIAR_ERR_INVALID, "too many rays in one call (limit 2^31)");
@@ -121,7 +124,7 @@ int launch_trace(liar_gpu_ctx* ctx, const liar_gpu_mesh* m, const liar_ray* d_ra
     const uint32_t n = (uint32_t)n_rays;
     const int s = ctx->trace_cfg.smem_stack, b = ctx->trace_cfg.block_size;
 #define LIAR_TRACE_CASE(S_, B_) \
-    if (s == S_ && b == B_) return launch_trace_sb<S_, B_>(ctx, m, d_rays, n, d_hits, any_hit, d_counters, st, d_counter, d_status);
+    if (s == S_ && b == B_) return launch_trace_sb<S_, B_>(ctx, m, d_rays, n, d_hits, any_hit, d_counters, st, d_counter, d_status, n_dev);
     LIAR_TRACE_CASE(8, 128)
     LIAR_TRACE_CASE(16, 128)
     LIAR_TRACE_CASE(24, 128)
@@ -142,9 +145,9 @@ namespace liar_gpu {
 // entry for the other subsystems of the library (renderer, photon tracer): one launch on a
 // device ray buffer with the context's launch shape and the given work-counter word
 int trace_mesh_internal(liar_gpu_ctx* ctx, const liar_gpu_mesh* mesh, const liar_ray* d_rays, size_t n,
-                        liar_hit* d_hits, int any_hit, cudaStream_t st, int counter_word) {
+                        liar_hit* d_hits, int any_hit, cudaStream_t st, int counter_word, const uint32_t* n_dev) {
     return launch_trace(ctx, mesh, d_rays, n, d_hits, any_hit, nullptr, st, ctx->d_scratch + counter_word,
-                        ctx->d_scratch + kStatusWord);
+                        ctx->d_scratch + kStatusWord, n_dev);
 }
 }  // namespace liar_gpu
 

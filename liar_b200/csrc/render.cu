@@ -155,7 +155,10 @@ __global__ void __launch_bounds__(256) k_raygen(DScene S, WaveParams W, Paths P,
 // the whole of tracePhoton after the intersection, for one queue entry
 template <bool TEX>
 __global__ void __launch_bounds__(128) k_shade(DScene S, WaveParams W, Paths P, Queue in, const liar_hit* hits,
-                                               uint32_t n_in, Queue out, unsigned long long* stats) {
+                                               uint32_t n_in, const uint32_t* __restrict__ n_dev, Queue out,
+                                               unsigned long long* stats) {
+    // n_dev: the queue's size in device memory when the host launched with an upper bound
+    if (n_dev) n_in = min(n_in, *n_dev);
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     bool want = false;
     liar_ray nr{};
@@ -325,7 +328,8 @@ struct RenderBuffers {
     Queue q[2]{};
     liar_hit* hits = nullptr;
     unsigned long long* stats = nullptr;  // [0] paths [1] segments [2] hits
-    uint32_t* h_count = nullptr;          // pinned
+    uint32_t* h_count = nullptr;          // pinned, two slots
+    cudaEvent_t ev[2] = {nullptr, nullptr};  // the copies into them
 };
 
 RenderBuffers* render_buffers(liar_gpu_ctx* ctx) {
@@ -338,6 +342,8 @@ RenderBuffers* render_buffers(liar_gpu_ctx* ctx) {
         if (rb->mem) cudaFree(rb->mem);
         if (rb->stats) cudaFree(rb->stats);
         if (rb->h_count) cudaFreeHost(rb->h_count);
+        for (cudaEvent_t e : rb->ev)
+            if (e) cudaEventDestroy(e);
         delete rb;
     });
     return rb;
@@ -347,6 +353,8 @@ int ensure_render_buffers(liar_gpu_ctx* ctx, RenderBuffers* rb, size_t n) {
     if (!rb->stats) {
         cudaError_t e = cudaMalloc((void**)&rb->stats, 4 * sizeof(unsigned long long));
         if (e == cudaSuccess) e = cudaMallocHost((void**)&rb->h_count, 2 * sizeof(uint32_t));
+        for (int k = 0; k < 2 && e == cudaSuccess; ++k)
+            if (!rb->ev[k]) e = cudaEventCreateWithFlags(&rb->ev[k], cudaEventDisableTiming);
         if (e != cudaSuccess) return ctx_cuda(ctx, e, "render statistics buffers");
     }
     if (rb->cap >= n) return LIAR_OK;
@@ -741,22 +749,32 @@ int render_impl(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_rende
         e = cudaMemsetAsync(rb->q[0].count, 0, 4, st);
         if (e != cudaSuccess) return ctx_cuda(ctx, e, "reset queue");
         k_raygen<<<(n + 255) / 256, 256, 0, st>>>(S, W, rb->P, rb->q[0], n, rb->stats);
-        uint32_t n_in = n;
-        for (int bounce = 0; n_in > 0; ++bounce) {
+        // Bounce b reads queue c_b and writes c_{b+1} <= c_b. The host launches bounce b sized for
+        // c_{b-1}, the kernels read c_b on the device, and the host waits for c_b only after
+        // bounce b is queued, so the GPU never idles on the round trip; the bounce launched
+        // after the last non-empty one finds an empty queue and ends at once.
+        uint32_t bound = n;  // c_{b-1}: an upper bound of the queue bounce b reads
+        for (int bounce = 0; bound > 0; ++bounce) {
             if (bounce > 4096) return ctx_fail(ctx, LIAR_ERR_TIMEOUT, "paths did not terminate after 4096 bounces");
-            rc = trace_mesh_internal(ctx, scene->mesh, rb->q[cur].rays, n_in, rb->hits, 0, st, kCounterWord + 8);
+            const uint32_t* n_dev = bounce == 0 ? nullptr : rb->q[cur].count;
+            rc = trace_mesh_internal(ctx, scene->mesh, rb->q[cur].rays, bound, rb->hits, 0, st, kCounterWord + 8, n_dev);
             if (rc) return rc;
             e = cudaMemsetAsync(rb->q[cur ^ 1].count, 0, 4, st);
             if (e != cudaSuccess) return ctx_cuda(ctx, e, "reset queue");
-            (S.n_tex > 0 ? k_shade<true> : k_shade<false>)<<<(n_in + 127) / 128, 128, 0, st>>>(S, W, rb->P, rb->q[cur], rb->hits, n_in, rb->q[cur ^ 1],
-                                                        rb->stats);
+            (S.n_tex > 0 ? k_shade<true> : k_shade<false>)<<<(bound + 127) / 128, 128, 0, st>>>(
+                S, W, rb->P, rb->q[cur], rb->hits, bound, n_dev, rb->q[cur ^ 1], rb->stats);
             e = cudaGetLastError();
             if (e != cudaSuccess) return ctx_cuda(ctx, e, "shade launch");
             cur ^= 1;
-            e = cudaMemcpyAsync(rb->h_count, rb->q[cur].count, 4, cudaMemcpyDeviceToHost, st);
-            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            const int slot = (bounce + 1) & 1;  // c_{b+1}
+            e = cudaMemcpyAsync(rb->h_count + slot, rb->q[cur].count, 4, cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaEventRecord(rb->ev[slot], st);
             if (e != cudaSuccess) return ctx_cuda(ctx, e, "queue size");
-            n_in = rb->h_count[0];
+            if (bounce == 0) continue;  // c_0 = n is known: bounce 1 is launched for n
+            // c_b, copied after bounce b - 1, bounds bounce b + 1
+            e = cudaEventSynchronize(rb->ev[bounce & 1]);
+            if (e != cudaSuccess) return ctx_cuda(ctx, e, "queue size");
+            bound = rb->h_count[bounce & 1];
         }
     }
     // path count

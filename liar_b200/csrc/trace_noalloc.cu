@@ -88,7 +88,7 @@ int launch_noalloc(const QNode* nodes, const QTri* tris, const liar_ray* rays, u
         return LIAR_ERR_CUDA;
     }
     kern<<<(unsigned)blocks, kBlockNA, smem, st>>>(nodes, tris, rays, hits, n, scratch, scratch + 1, nullptr,
-                                                   trace_batch(n, (uint32_t)blocks * (kBlockNA / 32)));
+                                                   trace_batch(n, (uint32_t)blocks * (kBlockNA / 32)), nullptr);
     if (cudaGetLastError() != cudaSuccess) return LIAR_ERR_CUDA;
     return LIAR_OK;
 }

@@ -252,9 +252,16 @@ __global__ void __launch_bounds__(BLOCK) trace_kernel(const QNode* __restrict__ 
                                                       const liar_ray* __restrict__ rays, liar_hit* __restrict__ hits,
                                                       uint32_t n_rays, uint32_t* __restrict__ work_counter,
                                                       uint32_t* __restrict__ status_word,
-                                                      TraceCounters* __restrict__ counters, uint32_t BATCH) {
+                                                      TraceCounters* __restrict__ counters, uint32_t BATCH,
+                                                      const uint32_t* __restrict__ n_dev) {
     // BATCH: ray indices a warp takes from the global counter at once (trace_batch: n spread over
-    // all resident warps, 32..256, so that a small wave still keeps every warp busy)
+    // all resident warps, 32..256, so that a small wave still keeps every warp busy).
+    // n_dev: the ray count in device memory, at most n_rays (a queue whose size the host does not
+    // wait for); the launch was sized for n_rays
+    if (n_dev) {
+        n_rays = min(*n_dev, n_rays);
+        BATCH = trace_batch(n_rays, gridDim.x * (BLOCK / 32));
+    }
     constexpr int REFILL = 8;         // refill once this many lanes are idle
     extern __shared__ int trace_smem[];  // S * BLOCK node entries, then S * BLOCK distances
     LaneStack<S, BLOCK> stack;
