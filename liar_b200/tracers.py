@@ -8,7 +8,9 @@ from __future__ import annotations
 class RayTracer:
     def __init__(self):
         self.maxRayGeneration = 8  # kernel/ray_tracer.cpp:171
-        self.maxDepth = 0          # hard cap on generations (0 = none), see DESIGN.md
+        # hard cap on generations (0 = none), an extension: with Russian roulette from generation
+        # maxRayGeneration it bounds the path length, as a fixed-depth workload asks
+        self.maxDepth = 0
 
 
 class AdjointPhotonTracer(RayTracer):
