@@ -484,10 +484,9 @@ def photon_bench(ctx, stream, args, world, dist, local, cpu: bool, n_photons: in
     stream.synchronize()
     first_build_ms = e0.elapsed_time(e1)  # includes the first allocation of the map's buffers
     build_ms = 0.0
-    for _ in range(3):
-        pmap.close()
+    for _ in range(3):  # rebuilds in the map's own buffers, as a render after the first one does
         e0.record(stream)
-        pmap = photons.PhotonMap(ctx, device_ptr=pos.data_ptr(), n=n_map, r_max=r, stream=stream.cuda_stream)
+        pmap.rebuild(pos.data_ptr(), n_map, r, stream=stream.cuda_stream)
         e1.record(stream)
         stream.synchronize()
         build_ms += e0.elapsed_time(e1) / 3

@@ -430,6 +430,10 @@ int liar_gpu_photon_map_build(liar_gpu_ctx* ctx, const float* positions, size_t 
                               liar_gpu_photon_map** out);
 int liar_gpu_photon_map_build_device(liar_gpu_ctx* ctx, const float* d_positions, size_t n, float r_max,
                                      liar_gpu_photon_map** out, void* stream);
+/* The same into an existing map (buildPhotonMap runs once per PhotonMapper::doPreProcess): its
+ * device buffers are kept and grown only when the new photons need more. */
+int liar_gpu_photon_map_rebuild_device(liar_gpu_ctx* ctx, liar_gpu_photon_map* map, const float* d_positions, size_t n,
+                                       float r_max, void* stream);
 void liar_gpu_photon_map_destroy(liar_gpu_photon_map* map);
 /* idx / d2: n_queries x k (unused slots: -1 / +inf); count (optional): neighbours found. k <= 64. */
 int liar_gpu_photon_gather(liar_gpu_ctx* ctx, const liar_gpu_photon_map* map, const float* queries, size_t n_queries,

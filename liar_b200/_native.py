@@ -89,6 +89,7 @@ SIGNATURES: dict[str, tuple] = {
     # photon maps (liar_b200/photons.py)
     "liar_gpu_photon_map_build": (C.c_int, [_vp, _vp, _sz, C.c_float, C.POINTER(_vp)]),
     "liar_gpu_photon_map_build_device": (C.c_int, [_vp, _vp, _sz, C.c_float, C.POINTER(_vp), _vp]),
+    "liar_gpu_photon_map_rebuild_device": (C.c_int, [_vp, _vp, _vp, _sz, C.c_float, _vp]),
     "liar_gpu_photon_map_destroy": (None, [_vp]),
     "liar_gpu_photon_gather": (C.c_int, [_vp, _vp, _vp, _sz, C.c_int, _vp, _vp, _vp]),
     "liar_gpu_photon_gather_device": (C.c_int, [_vp, _vp, _vp, _sz, C.c_int, _vp, _vp, _vp, _vp]),

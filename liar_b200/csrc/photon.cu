@@ -45,6 +45,7 @@ struct liar_gpu_photon_map {
     uint32_t* bucket_start = nullptr;  // 2^bits + 1
     void* scratch = nullptr;           // build scratch (bucket keys, counts, bounds), kept for rebuilds
     size_t scratch_bytes = 0;
+    size_t cap_n = 0, cap_buckets = 0; // capacities of sorted / cell_key and of bucket_start
 };
 
 namespace {
@@ -378,15 +379,25 @@ int map_build_impl(liar_gpu_ctx* ctx, liar_gpu_photon_map* m, const float* d_pos
         }
         m->scratch_bytes = need;
     }
-    if (m->sorted) cudaFree(m->sorted);
-    if (m->cell_key) cudaFree(m->cell_key);
-    if (m->bucket_start) cudaFree(m->bucket_start);
-    m->sorted = nullptr;
-    m->cell_key = nullptr;
-    m->bucket_start = nullptr;
-    cudaError_t e = cudaMalloc((void**)&m->sorted, std::max<size_t>(n, 1) * sizeof(float4));
-    if (e == cudaSuccess) e = cudaMalloc((void**)&m->cell_key, std::max<size_t>(n, 1) * sizeof(uint64_t));
-    if (e == cudaSuccess) e = cudaMalloc((void**)&m->bucket_start, (nb + 1) * sizeof(uint32_t));
+    cudaError_t e = cudaSuccess;
+    if (m->cap_n < std::max<size_t>(n, 1)) {
+        // photons beyond the buffers' capacity (a first build, or a rebuild with more photons)
+        if (m->sorted) cudaFree(m->sorted);
+        if (m->cell_key) cudaFree(m->cell_key);
+        m->sorted = nullptr;
+        m->cell_key = nullptr;
+        m->cap_n = 0;
+        e = cudaMalloc((void**)&m->sorted, std::max<size_t>(n, 1) * sizeof(float4));
+        if (e == cudaSuccess) e = cudaMalloc((void**)&m->cell_key, std::max<size_t>(n, 1) * sizeof(uint64_t));
+        if (e == cudaSuccess) m->cap_n = std::max<size_t>(n, 1);
+    }
+    if (e == cudaSuccess && m->cap_buckets < nb + 1) {
+        if (m->bucket_start) cudaFree(m->bucket_start);
+        m->bucket_start = nullptr;
+        m->cap_buckets = 0;
+        e = cudaMalloc((void**)&m->bucket_start, (nb + 1) * sizeof(uint32_t));
+        if (e == cudaSuccess) m->cap_buckets = nb + 1;
+    }
     if (e != cudaSuccess) {
         cudaGetLastError();
         return ctx_cuda(ctx, e, "photon map");
@@ -470,6 +481,20 @@ extern "C" int liar_gpu_photon_map_build_device(liar_gpu_ctx* ctx, const float* 
     }
     *out = m;
     return LIAR_OK;
+}
+
+extern "C" int liar_gpu_photon_map_rebuild_device(liar_gpu_ctx* ctx, liar_gpu_photon_map* m, const float* d_positions,
+                                                  size_t n, float r_max, void* stream) {
+    if (!ctx || !m) return LIAR_ERR_INVALID;
+    if (n && !d_positions) return ctx_fail(ctx, LIAR_ERR_INVALID, "null photon positions");
+    if (!(r_max > 0.0f) || !std::isfinite(r_max)) return ctx_fail(ctx, LIAR_ERR_INVALID, "r_max must be positive");
+    if (n >= (1ull << 31)) return ctx_fail(ctx, LIAR_ERR_INVALID, "too many photons (limit 2^31)");
+    if (m->device != ctx->device) return ctx_fail(ctx, LIAR_ERR_INVALID, "photon map belongs to another device");
+    int rc = ctx_activate(ctx);
+    if (rc) return rc;
+    m->r_max = r_max;
+    m->cell = r_max / kRefine;
+    return map_build_impl(ctx, m, d_positions, n, stream ? (cudaStream_t)stream : ctx->stream);
 }
 
 extern "C" int liar_gpu_photon_map_build(liar_gpu_ctx* ctx, const float* positions, size_t n, float r_max,

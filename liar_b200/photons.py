@@ -13,6 +13,8 @@ _SIGS = {
     "liar_gpu_photon_map_build": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_float, C.POINTER(C.c_void_p)]),
     "liar_gpu_photon_map_build_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_float,
                                                    C.POINTER(C.c_void_p), C.c_void_p]),
+    "liar_gpu_photon_map_rebuild_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_float,
+                                                     C.c_void_p]),
     "liar_gpu_photon_map_destroy": (None, [C.c_void_p]),
     "liar_gpu_photon_gather": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_int, C.c_void_p,
                                          C.c_void_p, C.c_void_p]),
@@ -40,6 +42,14 @@ class PhotonMap:
             self.n = P.shape[0]
         self.handle = h
         self.r_max = float(r_max)
+
+    def rebuild(self, device_ptr: int, n: int, r_max: float | None = None, stream: int | None = None):
+        """Builds the map again over n device positions, in its existing buffers (grown when needed)."""
+        r = self.r_max if r_max is None else float(r_max)
+        self.ctx.check(self.ctx._lib.liar_gpu_photon_map_rebuild_device(self.ctx.handle, self.handle,
+                                                                        C.c_void_p(device_ptr), int(n), r,
+                                                                        C.c_void_p(stream or 0)))
+        self.n, self.r_max = int(n), r
 
     def gather(self, queries, k: int = 64):
         Q = np.ascontiguousarray(queries, dtype=np.float32).reshape(-1, 3)

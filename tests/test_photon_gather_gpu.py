@@ -71,3 +71,24 @@ def test_gather_rejects_bad_arguments():
     m = PhotonMap(ctx, np.ones((3, 3), np.float32), r_max=1.0)
     with pytest.raises(LiarGpuError, match="INVALID"):
         m.gather(np.zeros((2, 3), np.float32), 65)
+
+
+def test_rebuild_in_place_matches_a_fresh_map():
+    """A map rebuilt over other photons (fewer, then more than its buffers hold, and another
+    radius) answers exactly like a map built fresh over them."""
+    import torch
+    ctx = default_context()
+    rng = np.random.default_rng(9)
+    Q = rng.uniform(-2, 2, size=(2000, 3)).astype(np.float32)
+    first = torch.from_numpy(surface_photons(40000, seed=3)).cuda()
+    m = PhotonMap(ctx, device_ptr=first.data_ptr(), n=40000, r_max=0.1)
+    for n, r, seed in ((20000, 0.1, 4), (80000, 0.15, 5)):
+        P = surface_photons(n, seed=seed)
+        d = torch.from_numpy(P).cuda()
+        m.rebuild(d.data_ptr(), n, r)
+        torch.cuda.synchronize()
+        gi, gd, gc = m.gather(Q, 32)
+        ci, cd, cc = oracle.knn(P, Q, 32, r)
+        np.testing.assert_array_equal(gc, cc)
+        np.testing.assert_array_equal(gi, ci)
+        np.testing.assert_array_equal(gd.view(np.int32), cd.view(np.int32))
