@@ -110,3 +110,28 @@ def test_bad_spheres_are_refused():
     flat.sphere_object[0] = 5
     with pytest.raises(LiarGpuError):
         R.GpuScene(default_context(), flat)
+
+
+def test_scene_of_spheres_only():
+    """No triangles at all: the tree holds the spheres alone."""
+    from liar_b200 import cameras
+    a = scenery.Sphere((0, 0, 0), 1.0)
+    a.shader = shaders.Lambert(tx.Constant(0.6))
+    b = scenery.Sphere((2.5, 0, 0), 0.7)
+    b.shader = shaders.Mirror(tx.Constant(0.9))
+    scene = scenery.List([a, b, scenery.LightSky(tx.Constant(1.0))])
+    cam = cameras.PerspectiveCamera()
+    cam.position = (1, -6, 0.5)
+    cam.lookAt((1, 0, 0))
+    flat = R.flatten(scene)
+    assert flat.triangles.shape[0] == 0
+    t = tracers.AdjointPhotonTracer()
+    t.maxRayGeneration = 3
+    d = R.render_desc(cam, 40, 30, 8, t, seed=1)
+    g = R.GpuScene(default_context(), flat).render(d)
+    c = oracle.RenderScene(flat).render(d)
+    np.testing.assert_array_equal(g[..., 3], c[..., 3])
+    mg, _ = R.resolve(g)
+    mc, _ = R.resolve(c)
+    assert mg[..., 1].mean() > 0.01 and np.ptp(mg[..., 1]) > 0.1
+    assert abs(mg[..., 1].mean() / mc[..., 1].mean() - 1) < 0.03
