@@ -172,6 +172,50 @@ __global__ void k_scan_add(uint32_t* __restrict__ out, uint32_t n, const uint32_
     if (i < n) out[i] += block_offsets[i / (kScanBlock * kScanItems)];
 }
 
+// ---- spatial order of gather queries: a counting sort by the Morton code of a 64^3 grid over the
+// map, so that the warps running at the same time gather from overlapping cells
+constexpr int kOrderBits = 6;
+constexpr uint32_t kOrderCells = 1u << (3 * kOrderBits);
+
+__device__ __forceinline__ uint32_t spread3(uint32_t v) {  // bit k of v to bit 3k
+    uint32_t r = 0;
+#pragma unroll
+    for (int k = 0; k < kOrderBits; ++k) r |= ((v >> k) & 1u) << (3 * k);
+    return r;
+}
+
+__device__ __forceinline__ uint32_t order_key(float x, float y, float z, float ox, float oy, float oz, float inv) {
+    const float c[3] = {(x - ox) * inv, (y - oy) * inv, (z - oz) * inv};
+    uint32_t k = 0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float f = fminf(fmaxf(c[a], 0.0f), (float)((1 << kOrderBits) - 1));  // NaN -> 0
+        k |= spread3((uint32_t)f) << a;
+    }
+    return k;
+}
+
+__global__ void k_order_count(const float* __restrict__ q, uint32_t n, float ox, float oy, float oz, float inv,
+                              uint32_t* __restrict__ keys, uint32_t* __restrict__ counts) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t k = order_key(q[3 * i], q[3 * i + 1], q[3 * i + 2], ox, oy, oz, inv);
+    keys[i] = k;
+    atomicAdd(counts + k, 1u);
+}
+
+__global__ void k_order_scatter(const float* __restrict__ q, uint32_t n, const uint32_t* __restrict__ keys,
+                                uint32_t* __restrict__ cursor, float4* __restrict__ ordered, uint32_t* __restrict__ status) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t slot = atomicAdd(cursor + keys[i], 1u);
+    if (slot >= n) {  // cannot happen with consistent counts: record, write nothing
+        atomicOr(status, kStatusBadBucket);
+        return;
+    }
+    ordered[slot] = make_float4(q[3 * i], q[3 * i + 1], q[3 * i + 2], __uint_as_float(i));
+}
+
 __global__ void k_scatter(const float* __restrict__ pos, uint32_t n, BuildParams P, const uint32_t* __restrict__ keys,
                           uint32_t* __restrict__ cursor, float4* __restrict__ sorted, uint64_t* __restrict__ cell_key,
                           uint32_t* __restrict__ status) {
@@ -231,14 +275,28 @@ __global__ void __launch_bounds__(256) k_gather(const float4* __restrict__ sorte
                                                 const uint32_t* __restrict__ start, GatherParams G,
                                                 const float* __restrict__ queries, uint32_t nq, int k_out,
                                                 int32_t* __restrict__ out_idx, float* __restrict__ out_d2,
-                                                int32_t* __restrict__ out_count, uint32_t* __restrict__ status) {
+                                                int32_t* __restrict__ out_count, uint32_t* __restrict__ status,
+                                                const float4* __restrict__ ordered) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
     constexpr uint64_t INF = ~0ull;
     const BuildParams& P = G.B;
-    for (uint32_t q = warp_global; q < nq; q += n_warps) {
-        const float qx = queries[3 * q], qy = queries[3 * q + 1], qz = queries[3 * q + 2];
+    for (uint32_t w = warp_global; w < nq; w += n_warps) {
+        // ordered: the queries in spatial order, each with its own index in w (results go there)
+        uint32_t q = w;
+        float qx, qy, qz;
+        if (ordered) {
+            const float4 o = ordered[w];
+            qx = o.x;
+            qy = o.y;
+            qz = o.z;
+            q = __float_as_uint(o.w);
+        } else {
+            qx = queries[3 * q];
+            qy = queries[3 * q + 1];
+            qz = queries[3 * q + 2];
+        }
         const int cx = cell_coord(qx, P.ox, P.inv), cy = cell_coord(qy, P.oy, P.inv), cz = cell_coord(qz, P.oz, P.inv);
         // the k nearest so far, ascending: slot `lane` in lo, slot `32 + lane` in hi
         uint64_t lo = INF, hi = INF;
@@ -538,6 +596,64 @@ extern "C" void liar_gpu_photon_map_destroy(liar_gpu_photon_map* m) {
     delete m;
 }
 
+namespace {
+
+constexpr size_t kOrderMinQueries = 1u << 15;  // below this the sort costs more than it saves
+
+struct GatherOrder {
+    void* mem = nullptr;
+    size_t cap = 0;
+};
+
+// the queries as float4 (x, y, z, own index) in the Morton order of a 64^3 grid over the map
+int order_queries(liar_gpu_ctx* ctx, const liar_gpu_photon_map* m, const float* d_q, uint32_t n, cudaStream_t st,
+                  const float4** out) {
+    GatherOrder* g = nullptr;
+    for (auto& ext : ctx->extensions)
+        if (ext.first == "gather_order") g = static_cast<GatherOrder*>(ext.second);
+    if (!g) {
+        g = new GatherOrder();
+        ctx->extensions.emplace_back("gather_order", g);
+        ctx->on_destroy.push_back([g]() {
+            if (g->mem) cudaFree(g->mem);
+            delete g;
+        });
+    }
+    const size_t nb = kOrderCells;
+    const size_t scan_blocks = (nb + 1 + kScanBlock * kScanItems - 1) / (kScanBlock * kScanItems);
+    const size_t a_ord = ((size_t)n * 16 + 255) / 256 * 256, a_keys = ((size_t)n * 4 + 255) / 256 * 256;
+    const size_t a_cnt = ((nb + 1) * 4 + 255) / 256 * 256;
+    int rc = ctx_grow(ctx, &g->mem, &g->cap, a_ord + a_keys + 3 * a_cnt + (scan_blocks + 1) * 8 + 256, "gather order");
+    if (rc) return rc;
+    char* p = static_cast<char*>(g->mem);
+    float4* ordered = reinterpret_cast<float4*>(p);
+    uint32_t* keys = reinterpret_cast<uint32_t*>(p + a_ord);
+    uint32_t* counts = reinterpret_cast<uint32_t*>(p + a_ord + a_keys);
+    uint32_t* start = reinterpret_cast<uint32_t*>(p + a_ord + a_keys + a_cnt);
+    uint32_t* cursor = reinterpret_cast<uint32_t*>(p + a_ord + a_keys + 2 * a_cnt);
+    uint32_t* block_sums = reinterpret_cast<uint32_t*>(p + a_ord + a_keys + 3 * a_cnt);
+    uint32_t* block_offs = block_sums + scan_blocks + 1;
+    cudaError_t e = cudaMemsetAsync(counts, 0, (nb + 1) * 4, st);
+    if (e != cudaSuccess) return ctx_cuda(ctx, e, "gather order");
+    const float inv = (float)(1 << kOrderBits) / std::max(m->extent, 1e-30f);
+    const unsigned blocks = (n + 255) / 256;
+    k_order_count<<<blocks, 256, 0, st>>>(d_q, n, m->origin[0], m->origin[1], m->origin[2], inv, keys, counts);
+    k_scan_local<<<(unsigned)scan_blocks, kScanBlock, 0, st>>>(counts, (uint32_t)(nb + 1), start, block_sums);
+    if (scan_blocks > 1) {
+        k_scan_local<<<1, kScanBlock, 0, st>>>(block_sums, (uint32_t)scan_blocks, block_offs, block_sums + scan_blocks);
+        k_scan_add<<<(unsigned)((nb + 1 + 255) / 256), 256, 0, st>>>(start, (uint32_t)(nb + 1), block_offs);
+    }
+    e = cudaMemcpyAsync(cursor, start, (nb + 1) * 4, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return ctx_cuda(ctx, e, "gather order");
+    k_order_scatter<<<blocks, 256, 0, st>>>(d_q, n, keys, cursor, ordered, ctx->d_scratch + kStatusWord);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return ctx_cuda(ctx, e, "gather order");
+    *out = ordered;
+    return LIAR_OK;
+}
+
+}  // namespace
+
 extern "C" int liar_gpu_photon_gather_device(liar_gpu_ctx* ctx, const liar_gpu_photon_map* m, const float* d_queries,
                                              size_t n_queries, int k, int32_t* d_idx, float* d_d2, int32_t* d_count,
                                              void* stream) {
@@ -558,9 +674,14 @@ extern "C" int liar_gpu_photon_gather_device(liar_gpu_ctx* ctx, const liar_gpu_p
     G.slack = std::max(1e-3f * m->cell, 8.0f * 1.1920929e-07f * std::max(m->extent, 1.0f));
     G.max_ring = (int)std::ceil(m->r_max / m->cell) + 1;
     G.n_photons = (uint32_t)m->n;
+    const float4* ordered = nullptr;
+    if (n_queries >= kOrderMinQueries && m->n > 0) {
+        rc = order_queries(ctx, m, d_queries, (uint32_t)n_queries, st, &ordered);
+        if (rc) return rc;
+    }
     const unsigned blocks = (unsigned)std::min<size_t>((n_queries + 7) / 8, (size_t)ctx->num_sms * 8);
     k_gather<<<blocks, 256, 0, st>>>(m->sorted, m->cell_key, m->bucket_start, G, d_queries, (uint32_t)n_queries, k, d_idx,
-                                     d_d2, d_count, ctx->d_scratch + kStatusWord);
+                                     d_d2, d_count, ctx->d_scratch + kStatusWord, ordered);
     return ctx_cuda(ctx, cudaGetLastError(), "photon gather launch");
 }
 

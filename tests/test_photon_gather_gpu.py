@@ -92,3 +92,20 @@ def test_rebuild_in_place_matches_a_fresh_map():
         np.testing.assert_array_equal(gc, cc)
         np.testing.assert_array_equal(gi, ci)
         np.testing.assert_array_equal(gd.view(np.int32), cd.view(np.int32))
+
+
+def test_many_queries_take_the_spatially_ordered_path():
+    """From 32,768 queries on, the gather orders them along a Morton curve first; the answers stay
+    those of each query, in the caller's order."""
+    ctx = default_context()
+    P = surface_photons(100000, seed=11)
+    rng = np.random.default_rng(12)
+    Q = np.concatenate([P[rng.choice(len(P), 30000, replace=False)] + rng.normal(scale=0.02, size=(30000, 3)),
+                        rng.uniform(-2.5, 2.5, size=(10000, 3))]).astype(np.float32)
+    rng.shuffle(Q)
+    m = PhotonMap(ctx, P, r_max=0.08)
+    gi, gd, gc = m.gather(Q, 48)
+    ci, cd, cc = oracle.knn_grid(P, Q, 48, 0.08)
+    np.testing.assert_array_equal(gc, cc)
+    np.testing.assert_array_equal(gi, ci)
+    np.testing.assert_array_equal(gd.view(np.int32), cd.view(np.int32))
