@@ -12,6 +12,10 @@
  *   - Functions without a "_device" suffix take HOST buffers and block until the result is
  *     back in host memory. "_device" variants take device pointers and a cudaStream_t (passed
  *     as void*, NULL = the context's stream) and return without synchronising.
+ *   - "_device" calls of one context share its device scratch (work counters, status word,
+ *     reorder buffers): give them one stream, or order their streams with events. The photon
+ *     gather additionally orders itself after the previous gather of the same context, whatever
+ *     the streams, because its reorder buffer decides where results are written.
  */
 #ifndef LIAR_GPU_H
 #define LIAR_GPU_H
@@ -511,11 +515,14 @@ int liar_gpu_photon_mapper_get_irradiance(liar_gpu_ctx* ctx, float* position, fl
  * work counter and status word live in a 256-byte device array compiled into the library.
  *   - d_rays / d_hits are the caller's device buffers on the mesh's device (16- / 8-byte
  *     aligned); at most 2^31 rays per call, more returns LIAR_ERR_INVALID.
- *   - The call allocates nothing and blocks until the trace on `stream` (NULL = the legacy
- *     default stream) has finished, so that it can return the kernel's status
- *     (LIAR_ERR_STACK on a traversal stack overflow).
- *   - The first call on a device looks up the array's device address (cudaGetSymbolAddress)
- *     with that device current; make that first call before any stream capture.
+ *   - The call allocates nothing. It reads the kernel's status word back on `stream` (NULL =
+ *     the legacy default stream) and waits for that stream alone, so that it can return the
+ *     status (LIAR_ERR_STACK on a traversal stack overflow); other streams are not waited for.
+ *   - The first call on a device does the set-up: it looks up the array's device address
+ *     (cudaGetSymbolAddress) with that device current and sizes the kernel's grid from its
+ *     occupancy; later calls make no such queries. Make that first call before any stream
+ *     capture. The kernel is the one the context path runs with its default launch shape, so
+ *     once the program has traced through a context, the CUDA driver has its code loaded.
  *   - Every call shares the one array per device: calls that overlap on the GPU (from several
  *     host threads or streams at once) race on it and must be serialised by the caller. */
 int liar_gpu_trace_device_noalloc(const liar_gpu_mesh* mesh, const liar_ray* d_rays, size_t n_rays,

@@ -292,6 +292,10 @@ __global__ void __launch_bounds__(256) k_gather(const float4* __restrict__ sorte
             qy = o.y;
             qz = o.z;
             q = __float_as_uint(o.w);
+            if (q >= nq) {  // a slot the reorder pass did not fill: record it, write nothing
+                if (lane == 0) atomicOr(status, kStatusBadBucket);
+                continue;
+            }
         } else {
             qx = queries[3 * q];
             qy = queries[3 * q + 1];
@@ -603,11 +607,15 @@ constexpr size_t kOrderMinQueries = 1u << 15;  // below this the sort costs more
 struct GatherOrder {
     void* mem = nullptr;
     size_t cap = 0;
+    // end of the last gather that read the buffer: a gather on another stream waits for it, since
+    // the buffer's entries decide where k_gather writes its results
+    cudaEvent_t last_use = nullptr;
+    bool used = false;
 };
 
 // the queries as float4 (x, y, z, own index) in the Morton order of a 64^3 grid over the map
 int order_queries(liar_gpu_ctx* ctx, const liar_gpu_photon_map* m, const float* d_q, uint32_t n, cudaStream_t st,
-                  const float4** out) {
+                  const float4** out, GatherOrder** order) {
     GatherOrder* g = nullptr;
     for (auto& ext : ctx->extensions)
         if (ext.first == "gather_order") g = static_cast<GatherOrder*>(ext.second);
@@ -616,8 +624,17 @@ int order_queries(liar_gpu_ctx* ctx, const liar_gpu_photon_map* m, const float* 
         ctx->extensions.emplace_back("gather_order", g);
         ctx->on_destroy.push_back([g]() {
             if (g->mem) cudaFree(g->mem);
+            if (g->last_use) cudaEventDestroy(g->last_use);
             delete g;
         });
+    }
+    if (!g->last_use) {
+        cudaError_t e = cudaEventCreateWithFlags(&g->last_use, cudaEventDisableTiming);
+        if (e != cudaSuccess) return ctx_cuda(ctx, e, "gather order event");
+    }
+    if (g->used) {
+        cudaError_t e = cudaStreamWaitEvent(st, g->last_use, 0);
+        if (e != cudaSuccess) return ctx_cuda(ctx, e, "gather order wait");
     }
     const size_t nb = kOrderCells;
     const size_t scan_blocks = (nb + 1 + kScanBlock * kScanItems - 1) / (kScanBlock * kScanItems);
@@ -649,6 +666,7 @@ int order_queries(liar_gpu_ctx* ctx, const liar_gpu_photon_map* m, const float* 
     e = cudaGetLastError();
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "gather order");
     *out = ordered;
+    *order = g;
     return LIAR_OK;
 }
 
@@ -675,14 +693,20 @@ extern "C" int liar_gpu_photon_gather_device(liar_gpu_ctx* ctx, const liar_gpu_p
     G.max_ring = (int)std::ceil(m->r_max / m->cell) + 1;
     G.n_photons = (uint32_t)m->n;
     const float4* ordered = nullptr;
+    GatherOrder* order = nullptr;
     if (n_queries >= kOrderMinQueries && m->n > 0) {
-        rc = order_queries(ctx, m, d_queries, (uint32_t)n_queries, st, &ordered);
+        rc = order_queries(ctx, m, d_queries, (uint32_t)n_queries, st, &ordered, &order);
         if (rc) return rc;
     }
     const unsigned blocks = (unsigned)std::min<size_t>((n_queries + 7) / 8, (size_t)ctx->num_sms * 8);
     k_gather<<<blocks, 256, 0, st>>>(m->sorted, m->cell_key, m->bucket_start, G, d_queries, (uint32_t)n_queries, k, d_idx,
                                      d_d2, d_count, ctx->d_scratch + kStatusWord, ordered);
-    return ctx_cuda(ctx, cudaGetLastError(), "photon gather launch");
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && order) {
+        e = cudaEventRecord(order->last_use, st);
+        order->used = e == cudaSuccess;
+    }
+    return ctx_cuda(ctx, e, "photon gather launch");
 }
 
 extern "C" int liar_gpu_photon_gather(liar_gpu_ctx* ctx, const liar_gpu_photon_map* m, const float* queries,

@@ -33,15 +33,35 @@ constexpr int kNoAllocWords = 64;
 __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocWords];
 
 constexpr int kMaxDevices = 64;
-std::mutex g_setup_mutex;
-uint32_t* g_scratch_ptr[kMaxDevices] = {};
-int g_num_sms[kMaxDevices] = {};
-std::atomic<bool> g_ready[kMaxDevices] = {};
-
 constexpr int kBlockNA = 128;
+// the context path's default launch shape: 16 stack entries per lane in shared memory, the rest
+// (up to 64) in local memory; a program that has traced through a context has this kernel loaded
+constexpr int kStackNA = 16;
 constexpr size_t kNoAllocMaxRays = (size_t)1 << 31;
 
-// once per device, with that device current
+struct NoAllocDevice {
+    uint32_t* scratch = nullptr;  // device address of g_noalloc_scratch on this device
+    unsigned blocks[2] = {};      // persistent grid of the closest-hit [0] and any-hit [1] kernel
+};
+std::mutex g_setup_mutex;
+NoAllocDevice g_dev[kMaxDevices];
+std::atomic<bool> g_ready[kMaxDevices] = {};
+
+template <bool ANY>
+int resident_blocks(int sms, unsigned* out) {
+    auto kern = trace_kernel<ANY, kStackNA, kBlockNA, false>;
+    const size_t smem = (size_t)kStackNA * kBlockNA * 8;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlockNA, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return LIAR_ERR_CUDA;
+    }
+    *out = (unsigned)sms * (unsigned)(per_sm > 0 ? per_sm : 1);
+    return LIAR_OK;
+}
+
+// once per device, with that device current: the scratch array's device address and the grid
+// sizes, so that later calls make no driver queries
 int noalloc_setup(int device) {
     if (g_ready[device].load(std::memory_order_acquire)) return LIAR_OK;
     std::lock_guard<std::mutex> lock(g_setup_mutex);
@@ -58,37 +78,31 @@ int noalloc_setup(int device) {
         cudaGetLastError();
         return LIAR_ERR_CUDA;
     }
-    g_scratch_ptr[device] = static_cast<uint32_t*>(ptr);
-    g_num_sms[device] = sms;
+    NoAllocDevice d;
+    d.scratch = static_cast<uint32_t*>(ptr);
+    int rc = resident_blocks<false>(sms, &d.blocks[0]);
+    if (rc == LIAR_OK) rc = resident_blocks<true>(sms, &d.blocks[1]);
+    if (rc != LIAR_OK) return rc;
+    g_dev[device] = d;
     g_ready[device].store(true, std::memory_order_release);
     return LIAR_OK;
 }
 
-template <bool ANY, int S>
+template <bool ANY>
 int launch_noalloc(const QNode* nodes, const QTri* tris, const liar_ray* rays, uint32_t n, liar_hit* hits,
-                   cudaStream_t st, uint32_t* scratch, int num_sms) {
-    auto kern = trace_kernel<ANY, S, kBlockNA, false>;
-    const size_t smem = (size_t)S * kBlockNA * 8;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
-        cudaGetLastError();
-        return LIAR_ERR_CUDA;
-    }
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlockNA, smem) != cudaSuccess) {
-        cudaGetLastError();
-        return LIAR_ERR_CUDA;
-    }
-    if (per_sm <= 0) per_sm = 1;
-    uint64_t blocks = (uint64_t)num_sms * per_sm;
+                   cudaStream_t st, const NoAllocDevice& d) {
+    const size_t smem = (size_t)kStackNA * kBlockNA * 8;
+    uint64_t blocks = d.blocks[ANY ? 1 : 0];
     const uint64_t needed = ((uint64_t)n + kBlockNA - 1) / kBlockNA;
     if (blocks > needed) blocks = needed;
     // the array keeps whatever the previous call left: the counter and the status start at zero
-    if (cudaMemsetAsync(scratch, 0, 2 * sizeof(uint32_t), st) != cudaSuccess) {
+    if (cudaMemsetAsync(d.scratch, 0, 2 * sizeof(uint32_t), st) != cudaSuccess) {
         cudaGetLastError();
         return LIAR_ERR_CUDA;
     }
-    kern<<<(unsigned)blocks, kBlockNA, smem, st>>>(nodes, tris, rays, hits, n, scratch, scratch + 1, nullptr,
-                                                   trace_batch(n, (uint32_t)blocks * (kBlockNA / 32)), nullptr);
+    trace_kernel<ANY, kStackNA, kBlockNA, false><<<(unsigned)blocks, kBlockNA, smem, st>>>(
+        nodes, tris, rays, hits, n, d.scratch, d.scratch + 1, nullptr,
+        trace_batch(n, (uint32_t)blocks * (kBlockNA / 32)), nullptr);
     if (cudaGetLastError() != cudaSuccess) return LIAR_ERR_CUDA;
     return LIAR_OK;
 }
@@ -115,27 +129,20 @@ extern "C" int liar_gpu_trace_device_noalloc(const liar_gpu_mesh* mesh, const li
     int rc = noalloc_setup(device);
     const uint32_t need = mesh_stack_needed(mesh);
     cudaStream_t st = (cudaStream_t)stream;
-    uint32_t* scratch = g_scratch_ptr[device];
     const uint32_t n = (uint32_t)n_rays;
     if (rc == LIAR_OK) {
-        if (need <= 24)
-            rc = any_hit ? launch_noalloc<true, 24>(mesh_nodes(mesh), mesh_tris(mesh), d_rays, n, d_hits, st, scratch,
-                                                    g_num_sms[device])
-                         : launch_noalloc<false, 24>(mesh_nodes(mesh), mesh_tris(mesh), d_rays, n, d_hits, st, scratch,
-                                                     g_num_sms[device]);
-        else if (need <= 64)
-            rc = any_hit ? launch_noalloc<true, 64>(mesh_nodes(mesh), mesh_tris(mesh), d_rays, n, d_hits, st, scratch,
-                                                    g_num_sms[device])
-                         : launch_noalloc<false, 64>(mesh_nodes(mesh), mesh_tris(mesh), d_rays, n, d_hits, st, scratch,
-                                                     g_num_sms[device]);
-        else
+        if (need > (uint32_t)kTraceStackTotal)
             rc = LIAR_ERR_STACK;
+        else
+            rc = any_hit ? launch_noalloc<true>(mesh_nodes(mesh), mesh_tris(mesh), d_rays, n, d_hits, st, g_dev[device])
+                         : launch_noalloc<false>(mesh_nodes(mesh), mesh_tris(mesh), d_rays, n, d_hits, st, g_dev[device]);
     }
     if (rc == LIAR_OK) {
-        // wait, then report the kernel's status word (a stack overflow makes the result invalid)
+        // read the kernel's status word on the caller's stream, then wait for that stream only
+        // (a stack overflow makes the result invalid)
         uint32_t status = 0;
-        cudaError_t e = cudaStreamSynchronize(st);
-        if (e == cudaSuccess) e = cudaMemcpy(&status, scratch + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+        cudaError_t e = cudaMemcpyAsync(&status, g_dev[device].scratch + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) {
             cudaGetLastError();
             rc = LIAR_ERR_CUDA;
