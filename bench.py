@@ -95,6 +95,57 @@ class ClockSampler:
                 "power_w_max": max(pw) if pw else None, "reasons": reasons, "samples": len(rows)}
 
 
+def ctx_sms(ctx) -> int:
+    import torch
+    return torch.cuda.get_device_properties(ctx.device).multi_processor_count
+
+
+def workload_config(world: int, n_triangles: int) -> dict:
+    """The traversal workload's config, identical in both arms."""
+    return {"workload": WORKLOAD, "triangles": int(n_triangles), "rays_per_step": N_RAYS,
+            "parallelism": f"replicas{world}" if world > 1 else "single",
+            "l2": "rays (512 MiB) stream through; larger than L2, no flush"}
+
+
+def l2_read_peak(stream, device: str, sms: int) -> dict:
+    """L2 read bandwidth of this GPU, measured by the project's probe kernel
+    (liar_b200/probe/l2_read.cu): buffers of 16-64 MiB (inside the 126 MB L2) read 16 B at a time
+    by 4 blocks of 512 threads per SM, many passes per launch; the best size's GB/s."""
+    import ctypes as C
+    import torch
+    from liar_b200 import build
+    lib = C.CDLL(str(build.PROBE_LIB))
+    lib.liar_probe_l2_read.restype = C.c_int
+    lib.liar_probe_l2_read.argtypes = [C.c_void_p, C.c_uint64, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+    blocks = 4 * sms
+    sink = torch.empty(blocks * 512, dtype=torch.int32, device=device)
+    best, rows = 0.0, []
+    for mib in (16, 32, 48, 64):
+        buf = torch.randint(0, 1 << 30, (mib << 18,), dtype=torch.int32, device=device)  # mib MiB
+        n_vec = buf.numel() // 4
+        passes = max(1, (4 << 30) // buf.numel() // 4)  # about 4 GiB read per launch
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+        def launch():
+            rc = lib.liar_probe_l2_read(C.c_void_p(buf.data_ptr()), n_vec, passes, blocks, C.c_void_p(sink.data_ptr()),
+                                        C.c_void_p(stream.cuda_stream))
+            if rc:
+                raise RuntimeError(f"L2 probe launch failed: CUDA error {rc}")
+
+        for _ in range(3):
+            launch()
+        e0.record(stream)
+        for _ in range(5):
+            launch()
+        e1.record(stream)
+        stream.synchronize()
+        gbs = 5 * passes * buf.numel() * 4 / (e0.elapsed_time(e1) * 1e-3) / 1e9
+        rows.append([mib, round(gbs, 1)])
+        best = max(best, gbs)
+        del buf
+    return {"gbs": best, "by_buffer_mib": rows, "source": "measured (liar_b200/probe/l2_read.cu)"}
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -168,10 +219,21 @@ def cornell_bench(ctx, stream, args, world, dist, local, cpu: bool) -> dict:
     ms = e0.elapsed_time(e1) / steps
     ms = max_over_ranks(ms, world, dist, f"cuda:{local}")
     st = gs.stats()
+    peaks = load_peaks()
+    seg_s = world * st["segments"] / (ms * 1e-3)
+    # per path segment through HBM: the trace kernel reads the queued ray (32 B + 4 B path index)
+    # and writes its hit (8 B); the shade kernel reads ray, index and hit, reads and writes the
+    # 24 B path state, and appends the next ray (36 B): 172 B. The 36-triangle tree stays in L1/L2.
+    seg_bytes = 36 + 8 + 44 + 48 + 36
     out = {"workload": "Cornell box 256x256, 16 spp, single wavelength, RR from generation 3, max depth 8",
            "ms_per_frame": ms, "samples_per_s": world * st["paths"] / (ms * 1e-3),
-           "segments_per_s": world * st["segments"] / (ms * 1e-3), "segments_per_sample": st["segments"] / st["paths"],
-           "note": "device time of liar_gpu_render_device per frame; host waits for each bounce's queue size"}
+           "segments_per_s": seg_s, "segments_per_sample": st["segments"] / st["paths"],
+           "roofline": {"bound": "hbm", "achieved": seg_bytes * seg_s / world / 1e9, "peak": peaks["hbm_gbs"],
+                        "unit": "GB/s", "frac": seg_bytes * seg_s / world / 1e9 / peaks["hbm_gbs"], "traffic": None,
+                        "model": f"{seg_bytes} B per path segment (queued ray, hit, path state, next ray)",
+                        "note": "a 36-triangle scene: latency- and issue-bound, far below the memory roofline"},
+           "note": "device time of liar_gpu_render_device per frame; each bounce is launched against the queue "
+                   "length on the device, the host reads a length only after the next bounce is queued"}
     # the same frame with the DirectLighting tracer (16 light + 16 BSDF samples per camera vertex)
     from liar_b200 import tracers
     dl = tracers.DirectLighting()
@@ -192,23 +254,28 @@ def cornell_bench(ctx, stream, args, world, dist, local, cpu: bool) -> dict:
                               "shadow_rays_per_s": world * W * H * SPP * 32 / (dms * 1e-3)}
     if cpu:
         import oracle
-        rows = 8
         rs = oracle.RenderScene(flat)
-        cfilm = np.zeros((H, W, 8), np.float32)
-        t0 = time.perf_counter()
-        first_row = H // 2 - rows // 2
-        rs.render(desc, cfilm, pixels=(first_row * W, (first_row + rows) * W))
-        dt = time.perf_counter() - t0
-        out["cpu_baseline"] = {"value": rows * W * SPP / dt, "unit": "samples/s", "cores": oracle.hardware_threads(),
-                               "kind": "port",
-                               "sample": f"{rows} middle image rows ({rows * W * SPP} samples), {dt:.1f} s"}
-        drows = 2
-        t0 = time.perf_counter()
-        rs.render(ddesc, cfilm, pixels=(first_row * W, (first_row + drows) * W))
-        dt = time.perf_counter() - t0
+
+        def cpu_rate(d, seconds=2.0):
+            """Whole frames (then rows, wrapping around) of d on all host threads for at least
+            `seconds` of wall time; returns (samples/s, samples, s)."""
+            cfilm = np.zeros((H, W, 8), np.float32)
+            done, row, t0 = 0, 0, time.perf_counter()
+            while time.perf_counter() - t0 < seconds:
+                rows = min(16, H - row)
+                rs.render(d, cfilm, pixels=(row * W, (row + rows) * W))
+                done += rows * W * SPP
+                row = (row + rows) % H
+            dt = time.perf_counter() - t0
+            return done / dt, done, dt
+
+        val, n, dt = cpu_rate(desc)
+        out["cpu_baseline"] = {"value": val, "unit": "samples/s", "cores": oracle.hardware_threads(), "kind": "port",
+                               "sample": f"{n} samples ({n // (W * SPP)} image rows of 16 spp), {dt:.1f} s"}
+        val, n, dt = cpu_rate(ddesc)
         out["direct_lighting"]["cpu_baseline"] = {
-            "value": drows * W * SPP / dt, "unit": "samples/s", "cores": oracle.hardware_threads(), "kind": "port",
-            "sample": f"{drows} middle image rows ({drows * W * SPP} samples) with DirectLighting, {dt:.1f} s"}
+            "value": val, "unit": "samples/s", "cores": oracle.hardware_threads(), "kind": "port",
+            "sample": f"{n} samples ({n // (W * SPP)} image rows of 16 spp) with DirectLighting, {dt:.1f} s"}
     gs.close()
     return out
 
@@ -243,6 +310,12 @@ def batch_bench(ctx, stream, args, world, dist, local, cpu: bool, n_scenes: int 
     ms = e0.elapsed_time(e1) / steps
     ms = max_over_ranks(ms, world, dist, f"cuda:{local}")
     st = br.stats()
+    peaks = load_peaks()
+    seg_s = world * st["segments"] / (ms * 1e-3)
+    # per path segment through HBM: trace reads the queued ray (36 B) and writes its hit (8 B);
+    # shade reads ray and hit, reads and writes the path state of 4 hero wavelengths (16 + 12 x 4
+    # = 64 B) and appends the next ray (36 B): 252 B; tree nodes and triangles are not counted
+    seg_bytes = 36 + 8 + 44 + 128 + 36
     tris = [w.n_triangles for w in work]
     out = {"workload": f"{n_scenes} procedural scenes, {min(tris)}-{max(tris)} triangles ({sum(tris)} total), "
                        "128^2-1024^2, 4-64 spp, 4 hero wavelengths, RR from generation 3, max depth 8",
@@ -250,6 +323,11 @@ def batch_bench(ctx, stream, args, world, dist, local, cpu: bool, n_scenes: int 
            "segments_per_s": world * st["segments"] / (ms * 1e-3), "samples_per_batch": st["paths"],
            "segments_per_sample": st["segments"] / st["paths"], "waves": st["waves"],
            "graph_launches_per_batch": 1,
+           "roofline": {"bound": "hbm", "achieved": seg_bytes * seg_s / world / 1e9, "peak": peaks["hbm_gbs"],
+                        "unit": "GB/s", "frac": seg_bytes * seg_s / world / 1e9 / peaks["hbm_gbs"], "traffic": None,
+                        "model": f"{seg_bytes} B per path segment (queued ray, hit, 4-wavelength path state, next "
+                                 "ray); the trees' node and triangle reads are not counted, so this is a lower "
+                                 "bound of the memory work"},
            "tuned": {"trace": [cfg.trace.block_size, cfg.trace.smem_stack],
                      "wave_paths": cfg.wave_paths, "shade_blocks_per_sm": cfg.shade_blocks_per_sm,
                      "cached": tune.get("cached", False), "seconds": tune_s},
@@ -523,12 +601,19 @@ def photon_bench(ctx, stream, args, world, dist, local, cpu: bool, n_photons: in
     # algorithmic bytes per query: 12 B point + k x 36 B photon records (the reference's Photon) +
     # 27 x 8 B bucket ranges + k x 8 B results + 4 B count
     bytes_q = 12 + K * 36 + 27 * 8 + K * 8 + 4
+    peaks = load_peaks()
+    gbs = bytes_q * nq / (g_ms * 1e-3) / 1e9
     out = {"workload": "glass sphere + GGX copper panel + Lambert ground, 5000 K point light; "
                        f"{n_map} global photons, 1920x1080 gather points ({nq} on diffuse surfaces), k = {K}",
            "photons_emitted": counts["emitted"], "photon_trace_s": trace_s,
            "photons_stored_per_s": counts["stored"] / trace_s, "estimation_radius": r, "map_build_ms": build_ms, "first_map_build_ms": first_build_ms,
            "gather_ms": g_ms, "queries_per_s": world * nq / (g_ms * 1e-3), "mean_neighbours": found,
-           "gather_gbs_algorithmic": bytes_q * nq / (g_ms * 1e-3) / 1e9, "estimate_ms": est_ms}
+           "gather_gbs_algorithmic": gbs, "estimate_ms": est_ms,
+           "roofline": {"bound": "hbm", "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                        "frac": gbs / peaks["hbm_gbs"], "traffic": None,
+                        "model": f"{bytes_q} B per query: 12 B point, {K} x 36 B photon records, 27 x 8 B bucket "
+                                 f"ranges, {K} x 8 B results, 4 B count",
+                        "kernel": "k_gather"}}
     if cpu:
         import oracle
         ns = min(nq, 20000)
@@ -610,7 +695,9 @@ def photon_bench(ctx, stream, args, world, dist, local, cpu: bool, n_photons: in
 
 
 def run_reference(args, world, rank):
-    """CPU restatement of the reference's path (oracle/), all host threads, bounded samples."""
+    """The reference arm: the CPU restatement of the reference's path (oracle/: the same 4-wide
+    SAH tree restated on the host and the exact triangle test) on all host threads, tracing all
+    16,777,216 workload rays per step, through the same timed-step structure as our arm."""
     if rank != 0:
         return
     import oracle
@@ -619,24 +706,23 @@ def run_reference(args, world, rank):
     rays = scenes.random_rays(v, N_RAYS, seed=0)
     threads = oracle.hardware_threads()
     tree = oracle.Tree(v, f)
-    sample = 1 << 20
     for _ in range(args.warmup):
-        tree.trace(rays[:sample], threads=threads)
+        tree.trace(rays, threads=threads)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        tree.trace(rays[:sample], threads=threads)
+        tree.trace(rays, threads=threads)
         times.append(time.perf_counter() - t0)
     dt = float(np.mean(times))
-    val = sample / dt / 1e6
+    val = N_RAYS / dt / 1e6
     line = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": dt * 1e3 * (N_RAYS / sample), "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural mesh and rays)",
-        "config": {"workload": WORKLOAD, "rays_per_step": sample, "sample_of": N_RAYS},
+        "config": workload_config(world, f.shape[0]),
         "cpu_baseline": {"value": val, "unit": "Mrays/s", "cores": threads, "kind": "port",
-                         "sample": f"first {sample} workload rays per step (CPU restatement; the reference's Lass core "
-                                   f"cannot be built)"},
+                         "sample": f"all {N_RAYS} workload rays per step, closest hit (CPU restatement; the "
+                                   f"reference's Lass core cannot be built)"},
         "e2e": {"value": val, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -808,6 +894,7 @@ def main():
     e2e_val = whole_job_rate(world, N_RAYS, e2e_s * 1e3) / 1e6
 
     peaks = load_peaks()
+    l2 = l2_read_peak(stream, f"cuda:{local}", ctx_sms(ctx))
     per_ray_model = 128.0 * nodes_visited / N_RAYS + 48.0 * tris_tested / N_RAYS + 40.0
     achieved = per_ray_model * N_RAYS / (ms * 1e-3) / 1e9
     traffic = None
@@ -819,18 +906,18 @@ def main():
         "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded procedural mesh and rays)",
-        "config": {"workload": WORKLOAD, "triangles": int(stats["n_triangles"]), "rays_per_step": N_RAYS,
-                   "parallelism": f"replicas{world}" if world > 1 else "single",
-                   "l2": "rays (512 MiB) stream through; larger than L2, no flush",
-                   "tree": {k: stats[k] for k in ("n_nodes", "n_leaves", "max_depth", "stack_needed", "sah_cost",
-                                                  "device_bytes", "build_seconds")}},
+        "config": workload_config(world, stats["n_triangles"]),
+        "tree": {k: stats[k] for k in ("n_nodes", "n_leaves", "max_depth", "stack_needed", "sah_cost",
+                                       "device_bytes", "build_seconds")},
         "any_hit": {"value": world * N_RAYS / (ms_any * 1e-3) / 1e6, "unit": "Mrays/s", "tmax": 0.5,
                     "ms_per_step": ms_any},
         "visits_per_ray": {"nodes": nodes_visited / N_RAYS, "triangles": tris_tested / N_RAYS},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                      "model": "128 B x nodes visited + 48 B x triangles tested + 40 B per ray, counted on device",
-                     "peak_source": peaks["source"]},
+                     "peak_source": peaks["source"],
+                     "l2": {"peak": l2["gbs"], "frac": achieved / l2["gbs"], "unit": "GB/s",
+                            "peak_by_buffer_mib": l2["by_buffer_mib"], "peak_source": l2["source"]}},
         "e2e": {"value": e2e_val, "unit": "Mrays/s", "h2d_bytes_per_step": N_RAYS * 32,
                 "d2h_bytes_per_step": N_RAYS * 8, "api": "liar_gpu_trace (host buffers, pinned)"},
         "gpu_launches": args.steps,

@@ -99,6 +99,13 @@ int liar_gpu_set_stream(liar_gpu_ctx* ctx, void* stream);
 /* Waits for the context's stream and reports device-side errors of the "_device" calls
  * queued since the last check (stack overflow, bounded-wait timeout, cancel). */
 int liar_gpu_synchronize(liar_gpu_ctx* ctx);
+/* Cancellation, the counterpart of RenderEngine::isCanceling (src/liar/kernel/render_engine.cpp:
+ * 239-242, 294-297, 342): the renders of ctx read *flag between waves and bounces and, once it is
+ * non-zero, queue no more work, wait for the work in flight and return LIAR_ERR_CANCELLED. The film
+ * then holds the samples of the paths that finished (a partial image, like the reference's
+ * cancelled render, not an estimate to keep). flag is the caller's host memory (any thread may
+ * set it) and must stay valid until it is replaced; NULL removes it. */
+int liar_gpu_set_cancel_flag(liar_gpu_ctx* ctx, const volatile int32_t* flag);
 /* Selects / reads the trace kernels' launch shape (default 128 threads, 16 shared entries). */
 int liar_gpu_set_trace_config(liar_gpu_ctx* ctx, const liar_trace_config* cfg);
 int liar_gpu_get_trace_config(const liar_gpu_ctx* ctx, liar_trace_config* out);
@@ -303,9 +310,16 @@ typedef struct liar_render_desc {
     float filter_param;          /* triangle: width (0 = 1); Mitchell: B (0 = 1/3) */
     float max_sample_luminance;  /* Raster.maxSampleLuminance (output/raster.cpp:572-575); 0 = no clamp */
     liar_photon_mapper_desc photon_mapper;  /* tracer PHOTON_MAPPER only */
+    /* the sample pattern of the reference's sampler class: LIAR_SAMPLER_STRATIFIER (0;
+     * samplers/stratifier.cpp: screen and lens samples on a sqrt(spp) x sqrt(spp) grid when spp is
+     * a square) or LIAR_SAMPLER_LATIN_HYPERCUBE (samplers/latin_hypercube.cpp: every axis
+     * stratified on its own), ORed with LIAR_SAMPLER_NOT_JITTERED for `jittered = False` (every
+     * stratified value at its stratum's centre, samplers/stratifier.h:90) */
+    int32_t sampler;
 } liar_render_desc;
 
 enum liar_filter { LIAR_FILTER_BOX = 0, LIAR_FILTER_TRIANGLE = 1, LIAR_FILTER_MITCHELL = 2 };
+enum liar_sampler { LIAR_SAMPLER_STRATIFIER = 0, LIAR_SAMPLER_LATIN_HYPERCUBE = 1, LIAR_SAMPLER_NOT_JITTERED = 2 };
 
 /* Uploads the scene (builds the triangle tree). */
 int liar_gpu_scene_upload(liar_gpu_ctx* ctx, const liar_scene_desc* desc, liar_gpu_scene** out);

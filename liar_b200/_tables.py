@@ -1,5 +1,5 @@
 """Access to the spectral data tables in liar_b200/data/tables.json (CIE 1931 observer, metal n, k,
-Meng-Simon recovery spectra)."""
+Meng-Simon recovery spectra, the Cornell box's measured spectra)."""
 from __future__ import annotations
 
 import functools
@@ -44,3 +44,9 @@ def spd(name: str) -> list:
 def recovery() -> dict:
     """{"wavelengths": [m], "xy": [[x, y]], "spectra": [[values]]}."""
     return _load()["recovery"]
+
+
+def cornell_box() -> dict:
+    """{"wavelengths": [m], "white", "red", "green", "light": [values]}: the measured Cornell box
+    spectra (the table of the reference's src/liar/tools/cornell_box.py)."""
+    return _load()["cornell_box"]

@@ -18,6 +18,9 @@ CSRC = HERE / "csrc"
 INCLUDE = HERE.parent / "include"
 LIB = HERE / "libliar_gpu.so"
 STAMP = HERE / ".libliar_gpu.stamp"
+# the benchmark's L2 bandwidth probe, a separate library outside the C ABI
+PROBE_SRC = HERE / "probe" / "l2_read.cu"
+PROBE_LIB = HERE / "libliar_probe.so"
 
 NVCC_FLAGS = [
     "-O3",
@@ -50,8 +53,22 @@ def _digest() -> str:
     return h.hexdigest()
 
 
+def build_probe(force: bool = False, verbose: bool = False) -> Path:
+    """Compiles the L2 bandwidth probe library unless it is newer than its source."""
+    if not force and PROBE_LIB.exists() and PROBE_LIB.stat().st_mtime >= PROBE_SRC.stat().st_mtime:
+        return PROBE_LIB
+    tmp = PROBE_LIB.with_suffix(".so.tmp")
+    cmd = [_nvcc(), *NVCC_FLAGS, "-shared", str(PROBE_SRC), "-o", str(tmp)]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, PROBE_LIB)
+    return PROBE_LIB
+
+
 def build(force: bool = False, verbose: bool = False, extra_flags: list[str] | None = None) -> Path:
     """Compiles the library unless it is up to date; returns its path."""
+    build_probe(force=force, verbose=verbose)
     digest = _digest()
     if not force and LIB.exists() and STAMP.exists() and STAMP.read_text().strip() == digest and not extra_flags:
         return LIB

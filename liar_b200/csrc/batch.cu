@@ -37,6 +37,7 @@ namespace {
 struct BItem {
     int scene;
     int width, height, spp, max_gen, max_depth;
+    uint32_t sampler;  // SAMPLER_* mode bits (sampler.h)
     uint64_t seed;
     uint64_t path_begin;
     FilmSpec film;
@@ -150,6 +151,7 @@ __device__ void bsplat(const DScene& S, const BItem& it, uint64_t local, const f
     k.pixel = (uint32_t)(local / (uint64_t)it.spp);
     k.sample = (uint32_t)(local % (uint64_t)it.spp);
     k.spp = (uint32_t)it.spp;
+    k.mode = it.sampler;
     film_splat(it.film, k, xyz, alpha);
 }
 
@@ -176,6 +178,7 @@ __global__ void __launch_bounds__(256) k_b_raygen(BParams P, BState<H> st, BQueu
             k.pixel = (uint32_t)(local / (uint64_t)it.spp);
             k.sample = (uint32_t)(local % (uint64_t)it.spp);
             k.spp = (uint32_t)it.spp;
+            k.mode = it.sampler;
             float lam[H], pdfsum;
             hero_wavelengths<H>(S, sample_dim(k, DIM_LAMBDA, true), lam, pdfsum);
             r = camera_ray(it.cam, k, it.width, it.height);
@@ -226,6 +229,7 @@ __global__ void __launch_bounds__(128) k_b_shade(BParams P, BState<H> st, BQueue
             key.pixel = (uint32_t)(local / (uint64_t)it.spp);
             key.sample = (uint32_t)(local % (uint64_t)it.spp);
             key.spp = (uint32_t)it.spp;
+            key.mode = it.sampler;
             // low 16 bits: ray generation; bit 16: the path crossed a dispersive interface and
             // carries lam[0] alone
             const int gen_word = st.gen[p];
@@ -665,6 +669,7 @@ extern "C" int liar_gpu_batch_create(liar_gpu_ctx* ctx, const liar_batch_item* i
         h.spp = R.spp;
         h.max_gen = R.max_ray_generation;
         h.max_depth = R.max_depth;
+        h.sampler = (uint32_t)R.sampler;
         h.seed = mix64(R.seed ^ mix64(0x51ed270b27ad0e0dull + (uint64_t)(uint32_t)R.first_sample));
         h.film = film_spec(it.d_film, R);
         if (const char* m = film_desc_error(R)) {

@@ -21,7 +21,6 @@ constexpr int kScratchWords = 64;
 constexpr int kStatusWord = 0;
 constexpr int kCounterWord = 8;
 constexpr uint32_t kStatusTimeout = 1u << 8;
-constexpr uint32_t kStatusCancelled = 1u << 9;
 constexpr int kPipeSlots = 3;  // staging slots of the host-buffer trace pipeline
 
 }  // namespace liar_gpu
@@ -44,6 +43,8 @@ struct liar_gpu_ctx {
     // launch shape of the trace kernels (liar_gpu_set_trace_config) and cached occupancy per kernel
     liar_trace_config trace_cfg{128, 16};
     std::unordered_map<const void*, int> occupancy;
+    // the caller's cancel flag (liar_gpu_set_cancel_flag), read between waves and bounces
+    const volatile int32_t* cancel_flag = nullptr;
     // resources of other subsystems (renderer, photon maps) register their release here
     std::vector<std::function<void()>> on_destroy;
     // per-subsystem state (work buffers of the renderer, photon maps), looked up by name
@@ -66,6 +67,10 @@ int ctx_cuda(liar_gpu_ctx* ctx, cudaError_t e, const char* what);
 int ctx_activate(liar_gpu_ctx* ctx);
 int ctx_grow(liar_gpu_ctx* ctx, void** buf, size_t* cap, size_t bytes, const char* what);
 int ctx_check_status(liar_gpu_ctx* ctx);
+
+inline bool ctx_cancel_requested(const liar_gpu_ctx* ctx) { return ctx->cancel_flag && *ctx->cancel_flag != 0; }
+// ends a cancelled render: waits for the work queued on st, then reports LIAR_ERR_CANCELLED
+int ctx_cancelled(liar_gpu_ctx* ctx, cudaStream_t st);
 
 inline int ctx_ensure_pipeline(liar_gpu_ctx* ctx) {
     for (int k = 0; k < kPipeSlots; ++k)

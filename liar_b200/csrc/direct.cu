@@ -71,6 +71,7 @@ struct DSamples {
 struct DParams {
     liar_camera cam;
     int width, height, spp, max_gen;
+    uint32_t sampler;  // SAMPLER_* mode bits (sampler.h)
     uint64_t seed;
     uint64_t first_path;
     int n_secondary;
@@ -115,6 +116,7 @@ __device__ __forceinline__ SampleKey dkey(const DParams& W, uint64_t g) {
     k.pixel = (uint32_t)(g / (uint64_t)W.spp);
     k.sample = (uint32_t)(g % (uint64_t)W.spp);
     k.spp = (uint32_t)W.spp;
+    k.mode = W.sampler;
     return k;
 }
 
@@ -929,6 +931,7 @@ int render_direct(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_ren
     W.spp = R.spp;
     W.film = film_spec(d_film, R);
     W.max_gen = R.max_ray_generation;
+    W.sampler = (uint32_t)R.sampler;
     W.seed = mix64(R.seed ^ mix64(0x51ed270b27ad0e0dull + (uint64_t)(uint32_t)R.first_sample));
     W.n_secondary = n_sec;
     W.glossy = R.trace_glossy < 0 ? 0u : CAP_GLOSSY;
@@ -945,6 +948,7 @@ int render_direct(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_ren
     const DScene& S = scene_dscene(scene);
     const liar_gpu_mesh* mesh = scene_mesh(scene);
     for (uint64_t first = 0; first < total; first += wave) {
+        if (ctx_cancel_requested(ctx)) return ctx_cancelled(ctx, st);
         const uint32_t n = (uint32_t)std::min<uint64_t>(wave, total - first);
         DSamples P;
         P.lam = static_cast<float*>(b->samples);
@@ -960,6 +964,7 @@ int render_direct(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_ren
         uint32_t n_in = n;
         int cur = 0;
         for (int gen = 0; n_in > 0 && gen <= W.max_gen; ++gen) {
+            if (ctx_cancel_requested(ctx)) return ctx_cancelled(ctx, st);
             // the next generation's queue and this generation's shadow rays at their worst case
             const uint64_t want_children = gen + 1 <= W.max_gen ? (uint64_t)n_in * children : 0;
             const uint64_t want_shadows = (uint64_t)n_in * shadow_per_task;

@@ -76,6 +76,7 @@ struct GQueue {
 struct GParams {
     liar_camera cam;
     int width, height, spp, max_gen, max_depth;
+    uint32_t sampler;       // SAMPLER_* mode bits (sampler.h)
     uint64_t seed;
     uint64_t first_path;    // global index (sample * pixels + pixel) of the wave's first path
     uint32_t npix;
@@ -100,6 +101,7 @@ __device__ __forceinline__ SampleKey gkey(const GParams& W, uint32_t slot) {
     k.pixel = (uint32_t)(g % (uint64_t)W.npix);
     k.sample = (uint32_t)(g / (uint64_t)W.npix);
     k.spp = (uint32_t)W.spp;
+    k.mode = W.sampler;
     return k;
 }
 
@@ -597,6 +599,7 @@ extern "C" int liar_gpu_render_guided_device(liar_gpu_ctx* ctx, const liar_gpu_s
     W.spp = R.spp;
     W.max_gen = R.max_ray_generation;
     W.max_depth = R.max_depth;
+    W.sampler = (uint32_t)R.sampler;
     W.seed = mix64(R.seed ^ mix64(0x51ed270b27ad0e0dull + (uint64_t)(uint32_t)R.first_sample));
     W.npix = (uint32_t)npix;
     W.film = film_spec(d_film, R);
@@ -614,6 +617,7 @@ extern "C" int liar_gpu_render_guided_device(liar_gpu_ctx* ctx, const liar_gpu_s
     unsigned long long records_total = 0;
     double candidates_per_path = 2.0;
     for (uint64_t first = 0; first < total; first += wave) {
+        if (ctx_cancel_requested(ctx)) return ctx_cancelled(ctx, st);
         const uint32_t n = (uint32_t)std::min<uint64_t>(wave, total - first);
         W.first_path = first;
         W.rec_keep = (float)std::min(1.0, (double)rec_target / ((double)n * candidates_per_path));
@@ -629,6 +633,7 @@ extern "C" int liar_gpu_render_guided_device(liar_gpu_ctx* ctx, const liar_gpu_s
         int cur = 0;
         for (int bounce = 0; n_in > 0; ++bounce) {
             if (bounce > 4096) return ctx_fail(ctx, LIAR_ERR_TIMEOUT, "paths did not terminate after 4096 bounces");
+            if (ctx_cancel_requested(ctx)) return ctx_cancelled(ctx, st);
             rc = trace_mesh_internal(ctx, mesh, gb->q[cur].rays, n_in, gb->hits, 0, st, kCounterWord + 8);
             if (rc) return rc;
             e = cudaMemsetAsync(gb->q[cur ^ 1].count, 0, 4, st);

@@ -231,8 +231,15 @@ int ctx_check_status(liar_gpu_ctx* ctx) {
     if (status & STATUS_STACK_OVERFLOW)
         return ctx_fail(ctx, LIAR_ERR_STACK, "device traversal stack overflowed (status 0x%x)", status);
     if (status & kStatusTimeout) return ctx_fail(ctx, LIAR_ERR_TIMEOUT, "a bounded device wait gave up (status 0x%x)", status);
-    if (status & kStatusCancelled) return ctx_fail(ctx, LIAR_ERR_CANCELLED, "cancelled (status 0x%x)", status);
     return ctx_fail(ctx, LIAR_ERR_CUDA, "device reported status 0x%x", status);
+}
+
+int ctx_cancelled(liar_gpu_ctx* ctx, cudaStream_t st) {
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return ctx_cuda(ctx, e, "cancel: wait for the queued work");
+    const int rc = ctx_check_status(ctx);  // a device error of the finished work takes precedence
+    if (rc) return rc;
+    return ctx_fail(ctx, LIAR_ERR_CANCELLED, "render cancelled by the cancel flag");
 }
 
 }  // namespace liar_gpu
@@ -402,6 +409,12 @@ extern "C" int liar_gpu_trace(liar_gpu_ctx* ctx, const liar_gpu_mesh* mesh, cons
         if (rc) return rc;
     }
     return ctx_check_status(ctx);
+}
+
+extern "C" int liar_gpu_set_cancel_flag(liar_gpu_ctx* ctx, const volatile int32_t* flag) {
+    if (!ctx) return LIAR_ERR_INVALID;
+    ctx->cancel_flag = flag;
+    return LIAR_OK;
 }
 
 extern "C" int liar_gpu_set_trace_config(liar_gpu_ctx* ctx, const liar_trace_config* cfg) {

@@ -86,6 +86,7 @@ struct Queue {
 struct WaveParams {
     liar_camera cam;
     int width, height, spp, max_gen, max_depth;
+    uint32_t sampler;      // SAMPLER_* mode bits (sampler.h)
     uint64_t seed;
     uint64_t first_path;   // global index of the wave's first path
     FilmSpec film;
@@ -97,6 +98,7 @@ __device__ __forceinline__ SampleKey key_of(const WaveParams& W, uint64_t gpath)
     k.pixel = (uint32_t)(gpath / (uint64_t)W.spp);
     k.sample = (uint32_t)(gpath % (uint64_t)W.spp);
     k.spp = (uint32_t)W.spp;
+    k.mode = W.sampler;
     return k;
 }
 
@@ -720,6 +722,8 @@ int render_impl(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_rende
     if (R.width <= 0 || R.height <= 0 || R.spp <= 0) return ctx_fail(ctx, LIAR_ERR_INVALID, "empty image or no samples");
     if (R.max_ray_generation < 0) return ctx_fail(ctx, LIAR_ERR_INVALID, "max_ray_generation must be >= 0");
     if (const char* m = film_desc_error(R)) return ctx_fail(ctx, LIAR_ERR_INVALID, "%s", m);
+    if (R.sampler & ~(LIAR_SAMPLER_LATIN_HYPERCUBE | LIAR_SAMPLER_NOT_JITTERED))
+        return ctx_fail(ctx, LIAR_ERR_INVALID, "unknown sampler bits 0x%x", (unsigned)R.sampler);
     if (R.tracer == LIAR_TRACER_DIRECT_LIGHTING) return render_direct(ctx, scene, R, d_film, st, nullptr);
     if (R.tracer == LIAR_TRACER_PHOTON_MAPPER) return render_photon_mapper(ctx, scene, R, d_film, st);
     if (R.tracer != LIAR_TRACER_ADJOINT_PHOTON) return ctx_fail(ctx, LIAR_ERR_UNSUPPORTED, "tracer %d", R.tracer);
@@ -739,10 +743,12 @@ int render_impl(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_rende
     W.spp = R.spp;
     W.max_gen = R.max_ray_generation;
     W.max_depth = R.max_depth;
+    W.sampler = (uint32_t)R.sampler;
     W.seed = mix64(R.seed ^ mix64(0x51ed270b27ad0e0dull + (uint64_t)(uint32_t)R.first_sample));
     W.film = film_spec(d_film, R);
     const DScene& S = scene->d;
     for (uint64_t first = 0; first < total; first += wave) {
+        if (ctx_cancel_requested(ctx)) return ctx_cancelled(ctx, st);
         const uint32_t n = (uint32_t)std::min<uint64_t>(wave, total - first);
         W.first_path = first;
         int cur = 0;
@@ -756,6 +762,7 @@ int render_impl(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_rende
         uint32_t bound = n;  // c_{b-1}: an upper bound of the queue bounce b reads
         for (int bounce = 0; bound > 0; ++bounce) {
             if (bounce > 4096) return ctx_fail(ctx, LIAR_ERR_TIMEOUT, "paths did not terminate after 4096 bounces");
+            if (ctx_cancel_requested(ctx)) return ctx_cancelled(ctx, st);
             const uint32_t* n_dev = bounce == 0 ? nullptr : rb->q[cur].count;
             rc = trace_mesh_internal(ctx, scene->mesh, rb->q[cur].rays, bound, rb->hits, 0, st, kCounterWord + 8, n_dev);
             if (rc) return rc;
@@ -815,7 +822,7 @@ extern "C" int liar_gpu_render(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, c
     e = cudaMemcpyAsync(d_film, film, bytes, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) rc = render_impl(ctx, scene, desc, d_film, ctx->stream);
     else rc = ctx_cuda(ctx, e, "film copy in");
-    if (!rc) {
+    if (!rc || rc == LIAR_ERR_CANCELLED) {  // a cancelled render hands back its partial film
         e = cudaMemcpyAsync(film, d_film, bytes, cudaMemcpyDeviceToHost, ctx->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
         if (e != cudaSuccess) rc = ctx_cuda(ctx, e, "film copy out");

@@ -989,8 +989,10 @@ __device__ inline Bsdf make_bsdf(const DScene& S, const liar_material& M, const 
 // distance are set; the ray's limits scale the camera's near/far planes by 1 / cos(axis angle)
 __device__ inline liar_ray camera_ray(const liar_camera& C, const SampleKey& k, int width, int height) {
     const uint32_t px = k.pixel % (uint32_t)width, py = k.pixel / (uint32_t)width;
-    const float sx = ((float)px + sample_dim(k, DIM_SCREEN, true)) / (float)width;
-    const float sy = ((float)py + sample_dim(k, DIM_SCREEN + 1, true)) / (float)height;
+    float jx, jy;
+    sample_2d(k, DIM_SCREEN, jx, jy);
+    const float sx = ((float)px + jx) / (float)width;
+    const float sy = ((float)py + jy) / (float)height;
     float3 pos = mk(C.position[0], C.position[1], C.position[2]);
     float3 dir = mk(C.direction[0], C.direction[1], C.direction[2]) + (sx - 0.5f) * mk(C.right[0], C.right[1], C.right[2]) +
                  (sy - 0.5f) * mk(C.down[0], C.down[1], C.down[2]);
@@ -998,7 +1000,9 @@ __device__ inline liar_ray camera_ray(const liar_camera& C, const SampleKey& k, 
     const float3 dn = mk(C.direction_normal[0], C.direction_normal[1], C.direction_normal[2]);
     float factor = 1.0f / dot(dir, dn);
     if (C.lens_radius > 0.0f && C.focus_distance > 0.0f && C.focus_distance < 3.4e38f) {
-        const float2 lens = concentric_disk(sample_dim(k, DIM_LENS, true), sample_dim(k, DIM_LENS + 1, true));
+        float lu, lv;
+        sample_2d(k, DIM_LENS, lu, lv);
+        const float2 lens = concentric_disk(lu, lv);
         const float3 lp = pos + (C.lens_radius * lens.x) * mk(C.right_normal[0], C.right_normal[1], C.right_normal[2]) +
                           (C.lens_radius * lens.y) * mk(C.down_normal[0], C.down_normal[1], C.down_normal[2]);
         const float3 fp = pos + (factor * C.focus_distance) * dir;
@@ -1083,7 +1087,9 @@ __device__ inline void film_splat(const FilmSpec& F, const SampleKey& k, float3 
         return;
     }
     const int px = (int)(k.pixel % (uint32_t)F.width), py = (int)(k.pixel / (uint32_t)F.width);
-    const float dx = sample_dim(k, DIM_SCREEN, true) - 0.5f, dy = sample_dim(k, DIM_SCREEN + 1, true) - 0.5f;
+    float jx, jy;
+    sample_2d(k, DIM_SCREEN, jx, jy);
+    const float dx = jx - 0.5f, dy = jy - 0.5f;
     const bool mitchell = F.filter == LIAR_FILTER_MITCHELL;
     const int r = mitchell ? 2 : (int)ceilf(F.param);
     for (int j = -r; j <= r; ++j) {

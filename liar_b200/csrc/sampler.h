@@ -14,6 +14,7 @@
 //   stratum= a bijection of [0, spp) keyed by h: a 4-round Feistel network on the next even
 //            power of two, cycle-walked into [0, spp) (Black & Rogaway 2002)
 //   value  = (stratum + jitter) / spp
+// Screen and lens samples are 2D-stratified (sample_2d), as the reference's Stratifier does.
 #pragma once
 #include <stdint.h>
 
@@ -68,18 +69,62 @@ enum : uint32_t {
     OFF_RR = 7
 };
 
+// sampler modes (liar_render_desc.sampler, include/liar_gpu.h)
+//   default        Stratifier (samplers/stratifier.cpp:163-180): screen and lens samples on the
+//                  sqrt(spp) x sqrt(spp) grid of 2D strata when spp is a square
+//   LATIN          LatinHypercube (samplers/latin_hypercube.cpp): screen and lens axes stratified
+//                  separately over the spp samples, like every other dimension
+//   NOT_JITTERED   `jittered = False`: every stratified value sits at its stratum's centre (the
+//                  reference's jitter() returns 0.5, stratifier.h:90)
+enum : uint32_t { SAMPLER_LATIN = 1u, SAMPLER_NOT_JITTERED = 2u };
+
 struct SampleKey {
     uint64_t seed;
     uint32_t pixel, sample, spp;
+    uint32_t mode = 0;
 };
 
+LS_HD uint64_t dim_hash(const SampleKey& k, uint32_t dim) {
+    return mix64(k.seed ^ mix64(((uint64_t)k.pixel << 32) | (uint64_t)dim));
+}
+LS_HD float dim_jitter(const SampleKey& k, uint64_t hd) {
+    return to_unit(mix64(hd + 0xd1b54a32d192ed03ull * ((uint64_t)k.sample + 1)));
+}
+
 LS_HD float sample_dim(const SampleKey& k, uint32_t dim, bool stratified) {
-    const uint64_t hd = mix64(k.seed ^ mix64(((uint64_t)k.pixel << 32) | (uint64_t)dim));
-    const float jitter = to_unit(mix64(hd + 0xd1b54a32d192ed03ull * ((uint64_t)k.sample + 1)));
-    if (!stratified || k.spp <= 1) return jitter;
+    const uint64_t hd = dim_hash(k, dim);
+    if (!stratified) return dim_jitter(k, hd);
+    const float jitter = (k.mode & SAMPLER_NOT_JITTERED) ? 0.5f : dim_jitter(k, hd);
+    if (k.spp <= 1) return jitter;
     const uint32_t s = permute_index(k.sample, k.spp, hd);
     const float u = ((float)s + jitter) / (float)k.spp;
     return u < 1.0f ? u : 0.99999994f;
+}
+
+// exact integer square root of small counts
+LS_HD uint32_t isqrt_u32(uint32_t n) {
+    uint32_t r = 0;
+    while ((r + 1) * (r + 1) <= n) ++r;
+    return r;
+}
+
+// the 2D sample of dimensions (dim, dim + 1): one of the spp = n^2 cells of the n x n grid per
+// sample (a bijection keyed by the pixel and dim), jittered within the cell; LatinHypercube
+// mode, or a count that is not a square, stratifies the two axes separately
+LS_HD void sample_2d(const SampleKey& k, uint32_t dim, float& x, float& y) {
+    const uint32_t n = k.spp > 1 ? isqrt_u32(k.spp) : 1u;
+    if ((k.mode & SAMPLER_LATIN) || k.spp <= 1 || n * n != k.spp) {
+        x = sample_dim(k, dim, true);
+        y = sample_dim(k, dim + 1, true);
+        return;
+    }
+    const uint64_t hx = dim_hash(k, dim), hy = dim_hash(k, dim + 1);
+    const uint32_t s = permute_index(k.sample, k.spp, hx);
+    const bool jit = !(k.mode & SAMPLER_NOT_JITTERED);
+    const float jx = jit ? dim_jitter(k, hx) : 0.5f, jy = jit ? dim_jitter(k, hy) : 0.5f;
+    const float u = ((float)(s % n) + jx) / (float)n, v = ((float)(s / n) + jy) / (float)n;
+    x = u < 1.0f ? u : 0.99999994f;
+    y = v < 1.0f ? v : 0.99999994f;
 }
 
 }  // namespace liar_gpu

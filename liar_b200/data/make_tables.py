@@ -11,6 +11,10 @@ can be compared with it:
   Dachsbacher, "Physically Meaningful Rendering using Tristimulus Colours" (EGSR 2015), sampled
   at chromaticities xy, as shipped in the reference's data/recovery_meng_simon.json (loaded by
   src/liar/__init__.py:72-79); wavelengths in metres.
+* ``cornell_box``: the measured spectra of the Cornell box (Cornell University Program of Computer
+  Graphics, "The Cornell Box" data): white, red and green wall reflectances and the light's
+  emission, 400-700 nm in 4 nm steps, as embedded in the reference's src/liar/tools/cornell_box.py
+  (the table passed to spd.loads there); wavelengths in metres.
 
 Run in a container that has the reference mounted: ``python liar_b200/data/make_tables.py
 /path/to/reference``. The product reads only the generated JSON.
@@ -43,10 +47,17 @@ def main(ref: Path) -> None:
     recovery = {"wavelengths": [float(w) * 1e-9 for w in rec["wavelengths"]],
                 "xy": [[float(v) for v in s["xy"]] for s in rec["spectra"]],
                 "spectra": [[float(v) for v in s["spectrum"]] for s in rec["spectra"]]}
+    # the numeric table of the spd.loads("""...""") literal in tools/cornell_box.py
+    text = (ref / "src" / "liar" / "tools" / "cornell_box.py").read_text()
+    body = text.split('spd.loads("""', 1)[1].split('"""', 1)[0]
+    cols = [[float(v) for v in line.split()] for line in body.splitlines() if line.strip()]
+    assert all(len(c) == 5 for c in cols), "expected wavelength, white, red, green, light columns"
+    cornell = {"wavelengths": [c[0] * 1e-9 for c in cols], "white": [c[1] for c in cols],
+               "red": [c[2] for c in cols], "green": [c[3] for c in cols], "light": [c[4] for c in cols]}
     out = Path(__file__).resolve().parent / "tables.json"
-    out.write_text(json.dumps({"observer": observer, "spd": spd, "recovery": recovery}, indent=None,
-                              separators=(",", ":")))
-    print(out, len(observer), {k: len(v) for k, v in spd.items()}, len(recovery["xy"]))
+    out.write_text(json.dumps({"observer": observer, "spd": spd, "recovery": recovery, "cornell_box": cornell},
+                              indent=None, separators=(",", ":")))
+    print(out, len(observer), {k: len(v) for k, v in spd.items()}, len(recovery["xy"]), len(cols))
 
 
 if __name__ == "__main__":

@@ -5,6 +5,7 @@ window in the reference, is unavailable on this box and is replaced by a headles
 keeps the last frame."""
 from __future__ import annotations
 
+import enum
 import math
 from pathlib import Path
 
@@ -14,6 +15,20 @@ from . import codecs
 
 TONE_MAPPINGS = ("Linear", "CompressY", "CompressRGB", "Reinhard2002Y", "Reinhard2002RGB", "ExponentialY",
                  "ExponentialRGB", "DuikerY", "DuikerRGB")
+
+
+class ToneMapping(str, enum.Enum):
+    """Raster.ToneMapping, a string enum as in the reference (output/raster.cpp:29-41)."""
+
+    Linear = "Linear"
+    CompressY = "CompressY"
+    CompressRGB = "CompressRGB"
+    Reinhard2002Y = "Reinhard2002Y"
+    Reinhard2002RGB = "Reinhard2002RGB"
+    ExponentialY = "ExponentialY"
+    ExponentialRGB = "ExponentialRGB"
+    DuikerY = "DuikerY"
+    DuikerRGB = "DuikerRGB"
 
 
 def _filmic(x):
@@ -42,6 +57,11 @@ class RenderTarget:
         self.xyza = xyza
         self.variance = variance
 
+    def isCanceling(self) -> bool:
+        """RenderTarget::isCanceling (kernel/render_target.h:59): True asks the engine to stop the
+        render in progress. The base target never cancels; a subclass may override it."""
+        return False
+
 
 class Raster(RenderTarget):
     """The reference's Raster settings and tone mapping (output/raster.cpp:45-500): rgbSpace,
@@ -61,10 +81,13 @@ class Raster(RenderTarget):
     def toneMapping(self) -> str:
         return self._tone
 
+    ToneMapping = ToneMapping
+
     @toneMapping.setter
     def toneMapping(self, mode: str):
+        name = str(getattr(mode, "value", mode))
         for t in TONE_MAPPINGS:
-            if t.lower() == str(mode).lower():
+            if t.lower() == name.lower():
                 self._tone = t
                 return
         raise KeyError(f"unknown tone mapping {mode!r}; one of {TONE_MAPPINGS}")
@@ -180,10 +203,62 @@ class Image(Raster):
         codecs.write(p, self.tonemap(space), space)
 
 
-class Display(RenderTarget):
+class Display(Raster):
+    """Display(title, resolution): the reference's window (output/display.cpp, PixelToaster) is
+    unavailable on this box; this headless raster keeps the last frame (``xyza``, and
+    ``tonemap(space)`` for its pixels) with the window's settings."""
+
     def __init__(self, title: str = "", resolution=(320, 240)):
         super().__init__(resolution)
-        self.title = title
+        self._title = str(title)
+        self.autoUpdate = True
+        self.showHistogram = False
+
+    @property
+    def title(self) -> str:
+        return self._title
+
+
+class Splitter(RenderTarget):
+    """Splitter([children]) (output/splitter.cpp): hands every render to each child; its resolution
+    is the children's largest; it is cancelling when any child is."""
+
+    def __init__(self, children=()):
+        self.children = list(children)
+        super().__init__(self.resolution)
+
+    @property
+    def resolution(self) -> tuple[int, int]:
+        w, h = 1, 1
+        for c in getattr(self, "_children", []):
+            w, h = max(w, c.resolution[0]), max(h, c.resolution[1])
+        return (w, h)
+
+    @resolution.setter
+    def resolution(self, value) -> None:  # derived from the children
+        pass
+
+    @property
+    def children(self) -> list:
+        return list(self._children)
+
+    @children.setter
+    def children(self, children) -> None:
+        self._children = list(children)
+
+    def add(self, child) -> None:
+        if isinstance(child, (list, tuple)):
+            self._children.extend(child)
+        else:
+            self._children.append(child)
+
+    def write(self, xyza, variance):
+        super().write(xyza, variance)
+        for c in self._children:
+            c.write(xyza, variance)
+
+    def isCanceling(self) -> bool:
+        return any(c.isCanceling() for c in self._children)
 
 
 class FilterTriangle(RenderTarget):
@@ -237,7 +312,14 @@ class FilterMitchell(RenderTarget):
 
 def film_settings(target) -> dict:
     """The GPU film settings of a render target chain: the outermost reconstruction filter and the
-    maxSampleLuminance of the raster at the end of the chain."""
+    maxSampleLuminance of the raster at the end of the chain. A Splitter's children share the one
+    GPU film, so they must agree on these settings."""
+    if isinstance(target, Splitter):
+        settings = [film_settings(c) for c in target.children] or [film_settings(None)]
+        if any(st != settings[0] for st in settings[1:]):
+            raise NotImplementedError("the children of a Splitter render into one film: give them the same filter "
+                                      "and maxSampleLuminance")
+        return settings[0]
     filt, param = 0, 0.0
     t = target
     while isinstance(t, (FilterTriangle, FilterMitchell)):

@@ -209,3 +209,5 @@ class RgbSpace:
 
 
 sRGB = RgbSpace((0.6400, 0.3300), (0.3000, 0.6000), (0.1500, 0.0600), (0.3127, 0.3290), 2.2)
+# the identity space of the reference (kernel/rgb_space.h:126-130): X, Y, Z as R, G, B, white E
+CIEXYZ = RgbSpace((1.0, 0.0), (0.0, 1.0), (0.0, 0.0), (1.0 / 3, 1.0 / 3), 1.0)

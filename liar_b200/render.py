@@ -14,7 +14,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _native as N
-from . import _tables, scenery, shaders, spectra
+from . import _tables, mediums, scenery, shaders, spectra
 from . import textures as tx
 from .textures import as_scalar, as_spectrum
 
@@ -78,7 +78,7 @@ class CRenderDesc(C.Structure):
                 ("seed", C.c_uint64), ("first_sample", C.c_int32), ("wave_paths", C.c_int32),
                 ("secondary_light_samples", C.c_int32), ("trace_glossy", C.c_int32),
                 ("filter", C.c_int32), ("filter_param", C.c_float), ("max_sample_luminance", C.c_float),
-                ("photon_mapper", CPhotonMapperDesc)]
+                ("photon_mapper", CPhotonMapperDesc), ("sampler", C.c_int32)]
 
 
 FILTER_BOX, FILTER_TRIANGLE, FILTER_MITCHELL = 0, 1, 2
@@ -393,6 +393,9 @@ class _Builder:
         return first, len(t)
 
     def visit(self, obj, inherited=None):
+        if not mediums.is_vacuum(getattr(obj, "interior", None)):
+            raise NotImplementedError(f"{type(obj).__name__}.interior is a {type(obj.interior).__name__}: "
+                                      "participating media are not on the GPU path")
         if isinstance(obj, scenery.List):
             for c in obj.children:
                 self.visit(c, obj.shader or inherited)
@@ -531,10 +534,11 @@ def flatten(scene) -> FlatScene:
 
 def render_desc(camera, width: int, height: int, spp: int, tracer, seed: int = 0, first_sample: int = 0,
                 wave_paths: int = 0, filter: int = FILTER_BOX, filter_param: float = 0.0,
-                max_sample_luminance: float = 0.0) -> CRenderDesc:
+                max_sample_luminance: float = 0.0, sampler: int = 0) -> CRenderDesc:
     """The C render description. filter / filter_param select the reconstruction filter (box;
     triangle of the given width, default 1; Mitchell with the given B, default 1/3);
-    max_sample_luminance > 0 clamps each sample's Y (Raster.maxSampleLuminance)."""
+    max_sample_luminance > 0 clamps each sample's Y (Raster.maxSampleLuminance); sampler holds
+    the LIAR_SAMPLER_* bits of the sampler (samplers.Stratifier.mode)."""
     r = CRenderDesc()
     cam = camera.flatten()
     for k in ("position", "direction", "right", "down", "direction_normal", "right_normal", "down_normal"):
@@ -571,6 +575,7 @@ def render_desc(camera, width: int, height: int, spp: int, tracer, seed: int = 0
     r.filter = int(filter)
     r.filter_param = float(filter_param)
     r.max_sample_luminance = float(max_sample_luminance) if math.isfinite(max_sample_luminance) else 0.0
+    r.sampler = int(sampler)
     return r
 
 

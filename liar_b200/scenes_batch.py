@@ -160,15 +160,21 @@ def _log_uniform_int(rng, lo: float, hi: float, size: int) -> np.ndarray:
     return np.round(np.exp(rng.uniform(math.log(lo), math.log(hi), size=size))).astype(np.int64)
 
 
-def batch_workload(n_scenes: int = 64, seed: int = 0, tris=(10_000, 2_000_000), side=(128, 1024), spp=(4, 64)):
-    """The batched-rendering workload: n_scenes scenes, triangle count, square image side and
-    samples per pixel log-uniform in their ranges (all seeded)."""
+def batch_workload_params(n_scenes: int = 64, seed: int = 0, tris=(10_000, 2_000_000), side=(128, 1024),
+                          spp=(4, 64)) -> list[tuple[int, int, int, int]]:
+    """(scene seed, triangle count, image side, samples per pixel) of each scene of the workload:
+    triangle count, square image side and samples per pixel log-uniform in their ranges."""
     rng = np.random.default_rng(seed)
     nt = _log_uniform_int(rng, *tris, n_scenes)
     sd = _log_uniform_int(rng, *side, n_scenes)
     sp = _log_uniform_int(rng, *spp, n_scenes)
     seeds = rng.integers(0, 2**31, size=n_scenes)
-    return [batch_scene(int(seeds[k]), int(nt[k]), int(sd[k]), int(sp[k])) for k in range(n_scenes)]
+    return [(int(seeds[k]), int(nt[k]), int(sd[k]), int(sp[k])) for k in range(n_scenes)]
+
+
+def batch_workload(n_scenes: int = 64, seed: int = 0, tris=(10_000, 2_000_000), side=(128, 1024), spp=(4, 64)):
+    """The batched-rendering workload: n_scenes scenes of batch_workload_params (all seeded)."""
+    return [batch_scene(*p) for p in batch_workload_params(n_scenes, seed, tris, side, spp)]
 
 
 def batch_tracer(max_ray_generation: int = 3, max_depth: int = 8):

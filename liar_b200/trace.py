@@ -46,6 +46,14 @@ class Context:
     def set_stream(self, stream_ptr: int | None) -> None:
         N.check(self._lib.liar_gpu_set_stream(self.handle, C.c_void_p(stream_ptr or 0)), self.handle)
 
+    def set_cancel_flag(self, flag: C.c_int32 | None) -> None:
+        """Renders on this context stop between waves and bounces once flag.value != 0 and raise
+        LiarGpuError(LIAR_ERR_CANCELLED) (liar_gpu_set_cancel_flag). The caller keeps flag alive;
+        None removes it."""
+        self._cancel = flag
+        N.check(self._lib.liar_gpu_set_cancel_flag(self.handle, C.byref(flag) if flag is not None else None),
+                self.handle)
+
     @property
     def trace_config(self) -> tuple[int, int]:
         """(threads per block, shared-memory stack entries per lane) of the trace kernels."""

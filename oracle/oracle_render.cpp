@@ -116,6 +116,7 @@ struct RenderIn {
     int32_t pm_final_gather_rays, pm_secondary_gather_rays;
     float pm_ratio_precomputed_irradiance;
     int32_t pm_reserved;
+    int32_t sampler;  // LIAR_SAMPLER_* bits
 };
 
 // the mirrors above have the C ABI's layout
@@ -128,6 +129,7 @@ static_assert(offsetof(Material, tex) == offsetof(liar_material, tex) &&
                   offsetof(SceneIn, triangle_uvs) == offsetof(liar_scene_desc, triangle_uvs) &&
                   offsetof(RenderIn, pm_max_photons) == offsetof(liar_render_desc, photon_mapper) &&
                   offsetof(RenderIn, filter) == offsetof(liar_render_desc, filter) &&
+                  offsetof(RenderIn, sampler) == offsetof(liar_render_desc, sampler) &&
                   offsetof(Texture, pixels) == offsetof(liar_texture, pixels) &&
                   offsetof(SceneIn, texture_pixels) == offsetof(liar_scene_desc, texture_pixels) &&
                   offsetof(SceneIn, noise_tables) == offsetof(liar_scene_desc, noise_tables) &&
@@ -211,16 +213,40 @@ uint32_t permute(uint32_t i, uint32_t n, uint64_t key) {
     } while (i >= n);
     return i;
 }
+// mode bits: LIAR_SAMPLER_LATIN_HYPERCUBE (screen and lens axes stratified one by one, the
+// LatinHypercube, samplers/latin_hypercube.cpp) and LIAR_SAMPLER_NOT_JITTERED (stratum centres,
+// samplers/stratifier.h:90); without them the Stratifier's 2D grid of screen and lens strata
+// (samplers/stratifier.cpp:163-180)
 struct Sampler {
     uint64_t seed;
     uint32_t pixel, sample, spp;
+    uint32_t mode = 0;
+    uint64_t hash(uint32_t dim) const { return mix64(seed ^ mix64(((uint64_t)pixel << 32) | (uint64_t)dim)); }
+    float jitter(uint64_t hd) const { return unitf(mix64(hd + 0xd1b54a32d192ed03ull * ((uint64_t)sample + 1))); }
     float get(uint32_t dim, bool strat) const {
-        const uint64_t hd = mix64(seed ^ mix64(((uint64_t)pixel << 32) | (uint64_t)dim));
-        const float jit = unitf(mix64(hd + 0xd1b54a32d192ed03ull * ((uint64_t)sample + 1)));
-        if (!strat || spp <= 1) return jit;
+        const uint64_t hd = hash(dim);
+        if (!strat) return jitter(hd);
+        const float jit = (mode & LIAR_SAMPLER_NOT_JITTERED) ? 0.5f : jitter(hd);
+        if (spp <= 1) return jit;
         const uint32_t s = permute(sample, spp, hd);
         const float u = ((float)s + jit) / (float)spp;
         return u < 1.0f ? u : 0.99999994f;
+    }
+    void get2(uint32_t dim, float& x, float& y) const {
+        uint32_t n = 0;
+        while ((n + 1) * (n + 1) <= spp) ++n;
+        if ((mode & LIAR_SAMPLER_LATIN_HYPERCUBE) || spp <= 1 || n * n != spp) {
+            x = get(dim, true);
+            y = get(dim + 1, true);
+            return;
+        }
+        const uint64_t hx = hash(dim), hy = hash(dim + 1);
+        const uint32_t s = permute(sample, spp, hx);
+        const bool jit = !(mode & LIAR_SAMPLER_NOT_JITTERED);
+        const float jx = jit ? jitter(hx) : 0.5f, jy = jit ? jitter(hy) : 0.5f;
+        const float u = ((float)(s % n) + jx) / (float)n, v = ((float)(s / n) + jy) / (float)n;
+        x = u < 1.0f ? u : 0.99999994f;
+        y = v < 1.0f ? v : 0.99999994f;
     }
 };
 const uint32_t D_SCREEN = 0, D_LENS = 2, D_LAMBDA = 4, D_GEN0 = 8, D_PER_GEN = 8;
@@ -1958,10 +1984,12 @@ int render_body(void* s, const RenderIn* R, const PmIn* pm, float* film, int64_t
                 Path P;
                 P.S = &S;
                 P.R = R;
-                P.smp = Sampler{seed, (uint32_t)px, (uint32_t)smp, (uint32_t)R->spp};
+                P.smp = Sampler{seed, (uint32_t)px, (uint32_t)smp, (uint32_t)R->spp, (uint32_t)R->sampler};
                 const uint32_t ix = (uint32_t)(px % R->width), iy = (uint32_t)(px / R->width);
-                const float sx = ((float)ix + P.smp.get(D_SCREEN, true)) / (float)R->width;
-                const float sy = ((float)iy + P.smp.get(D_SCREEN + 1, true)) / (float)R->height;
+                float jx, jy;
+                P.smp.get2(D_SCREEN, jx, jy);
+                const float sx = ((float)ix + jx) / (float)R->width;
+                const float sy = ((float)iy + jy) / (float)R->height;
                 float lpdf;
                 P.lam = observer_sample(S, P.smp.get(D_LAMBDA, true), lpdf);
                 const Camera& C = R->camera;
@@ -1973,7 +2001,9 @@ int render_body(void* s, const RenderIn* R, const PmIn* pm, float* film, int64_t
                 float factor = 1 / dot(dir, dn);
                 if (C.lens_radius > 0 && C.focus_distance > 0 && C.focus_distance < 3.4e38f) {
                     float lx, ly;
-                    concentric(P.smp.get(D_LENS, true), P.smp.get(D_LENS + 1, true), lx, ly);
+                    float lu, lv;
+                    P.smp.get2(D_LENS, lu, lv);
+                    concentric(lu, lv, lx, ly);
                     const V lp = pos + (C.lens_radius * lx) * V{C.right_normal[0], C.right_normal[1], C.right_normal[2]} +
                                  (C.lens_radius * ly) * V{C.down_normal[0], C.down_normal[1], C.down_normal[2]};
                     const V fp = pos + (factor * C.focus_distance) * dir;
@@ -1998,8 +2028,7 @@ int render_body(void* s, const RenderIn* R, const PmIn* pm, float* film, int64_t
                     Yv = sc * c.y;
                     Z = sc * c.z;
                 }
-                film_splat(*R, target, (int)ix, (int)iy, P.smp.get(D_SCREEN, true), P.smp.get(D_SCREEN + 1, true), X, Yv,
-                           Z, P.alpha);
+                film_splat(*R, target, (int)ix, (int)iy, jx, jy, X, Yv, Z, P.alpha);
             }
         }
     };

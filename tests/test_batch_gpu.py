@@ -1,4 +1,5 @@
-"""Batched rendering (one CUDA-graph launch over many scenes) against single-scene renders.
+"""Batched rendering (one CUDA-graph launch over many scenes) against single-scene renders and,
+for scenes of the batched workload itself, against the CPU restatement of the reference.
 
 With one hero wavelength the batch draws exactly the samples liar_gpu_render_device draws for each
 item on its own, so the films agree to float rounding (only the order of the per-pixel atomic adds
@@ -12,6 +13,7 @@ import numpy as np
 import pytest
 import torch
 
+import oracle
 from liar_b200 import (batch as B, cameras, render as R, scenery, scenes_batch, scenes_render, shaders, spectra,
                        textures, tracers)
 from liar_b200._native import LiarGpuError
@@ -184,6 +186,35 @@ def test_procedural_batch_matches_single_renders():
     for film, ref in zip(br.films, refs):
         _close(film.cpu().numpy(), ref)
         assert film[..., 1].sum().item() > 0
+
+
+def test_workload_scenes_through_the_batch_match_the_oracle():
+    """The smallest, the median and the largest scene of the 64-scene workload (by triangles: 10k
+    to 2M), rendered together in one 4-hero-wavelength graph launch at 40 x 40 x 16 spp, against
+    the oracle's one-wavelength restatement of the reference's path tracer on the same scenes."""
+    ctx = default_context()
+    params = scenes_batch.batch_workload_params(64, seed=0)
+    order = np.argsort([p[1] for p in params])
+    picks = [int(order[0]), int(order[len(order) // 2]), int(order[-1])]
+    assert params[picks[0]][1] < 12_000 and params[picks[-1]][1] > 1_500_000
+    flats, entries = [], []
+    for k in picks:
+        bs = scenes_batch.batch_scene(params[k][0], params[k][1], 40, 16)
+        flats.append(R.flatten(bs.scene))
+        gs = R.GpuScene(ctx, flats[-1])
+        entries.append((gs, R.render_desc(bs.camera, 40, 40, 16, scenes_batch.batch_tracer(), seed=100 + k)))
+    br = B.BatchRenderer(ctx, entries, B.make_config(hero=4))
+    br.launch()
+    torch.cuda.synchronize()
+    for film, flat, (gs, d) in zip(br.films, flats, entries):
+        c = oracle.RenderScene(flat).render(d)
+        g = film.cpu().numpy()
+        ma, mc = _mean_within(g, c, min_fraction=0.98)
+        np.testing.assert_array_equal(g[..., 7], c[..., 7])
+        assert mc[..., 1].mean() > 0.01
+        assert abs(ma[..., 1].mean() / mc[..., 1].mean() - 1) < 0.03
+        gs.close()
+    br.close()
 
 
 def test_invalid_batches_fail_loudly(cornell):

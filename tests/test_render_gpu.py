@@ -50,6 +50,20 @@ def test_cornell_matches_oracle():
     assert mg[..., 1].mean() > 0.01
 
 
+def test_cornell_workload_at_full_size():
+    """The plain path-tracing workload exactly: 256 x 256, 16 spp, Russian roulette from
+    generation 3, depth cap 8, seed 0 (the Cornell engine of scenes_render)."""
+    e = scenes_render.cornell_engine()
+    assert e.sampler.resolution == (256, 256) and e.sampler.samplesPerPixel == 16
+    assert (e.tracer.maxRayGeneration, e.tracer.maxDepth, e.seed) == (3, 8, 0)
+    g, c, stats = run_both(e.scene, e.camera, 256, 256, 16, max_gen=3, max_depth=8, seed=0)
+    assert stats["paths"] == 256 * 256 * 16
+    mg, mc = within_3_sigma(g, c)
+    np.testing.assert_array_equal(g[..., 7], c[..., 7])
+    np.testing.assert_array_equal(g[..., 3], c[..., 3])
+    assert abs(mg[..., 1].mean() / mc[..., 1].mean() - 1) < 0.005
+
+
 def test_cornell_without_depth_cap_and_other_rr_start():
     scene, cam = scenes_render.cornell_box()
     g, c, _ = run_both(scene, cam, 48, 48, 8, max_gen=8, max_depth=0, seed=7)
