@@ -241,12 +241,139 @@ class Image(Texture):
                           "(no ray differentials on the GPU path)", stacklevel=4)
 
 
+_U32, _U64 = 0xFFFFFFFF, 0xFFFFFFFFFFFFFFFF
+# PCG constants (O'Neill 2014, pcg-random.org): the default 64-bit and 32-bit LCG multipliers and
+# increments, and the 32-bit MCG multiplier of the RXS M XS output with its inverse mod 2^32
+_PCG_MUL64, _PCG_INC64 = 6364136223846793005, 1442695040888963407
+_PCG_MUL32, _PCG_INC32 = 747796405, 2891336453
+_RXS_MUL32, _RXS_UNMUL32 = 277803737, 2897767785
+
+
+def _xsh_rs_64_32(state: int) -> int:
+    """PCG's XSH RS output, 64-bit state to 32 bits: xorshift by 22, then a shift of 22 to 29
+    chosen by the top 3 bits."""
+    rshift = state >> 61
+    state ^= state >> 22
+    return (state >> (22 + rshift)) & _U32
+
+
+def _rxs_m_xs_32(state: int) -> int:
+    """PCG's RXS M XS output on 32 bits (a bijection): random xorshift, multiply, xorshift by 22."""
+    state ^= state >> (4 + (state >> 28))
+    state = (state * _RXS_MUL32) & _U32
+    return state ^ (state >> 22)
+
+
+def _unxorshift32(y: int, shift: int) -> int:
+    x = y
+    for _ in range(32 // shift + 1):
+        x = y ^ (x >> shift)
+    return x & _U32
+
+
+def _rxs_m_xs_32_inverse(value: int) -> int:
+    x = _unxorshift32(value, 22)
+    x = (x * _RXS_UNMUL32) & _U32
+    return _unxorshift32(x, 4 + (x >> 28))
+
+
+class Pcg32K2Fast:
+    """pcg32_k2_fast of pcg-cpp (O'Neill, "PCG: A Family of Simple Fast Space-Efficient
+    Statistically Good Algorithms for Random Number Generation", 2014): a 64-bit one-stream LCG
+    with the XSH RS output, extended by a 2-entry table of 32-bit values XORed into every output
+    (entry picked by the state's low bit; the table advances, as a 32-bit RXS M XS generator run
+    inside out, whenever the state's low 32 bits are all zero). The reference seeds one with the
+    Perlin seed (src/liar/textures/perlin.cpp:140)."""
+
+    def __init__(self, seed: int):
+        self.state = (((seed & _U64) + _PCG_INC64) * _PCG_MUL64 + _PCG_INC64) & _U64
+        # the table starts from the base generator's outputs, offset by the difference of two
+        a, b = self._base(), self._base()
+        diff = (a - b) & _U32
+        self.table = [self._base() ^ diff for _ in range(2)]
+
+    def _base(self) -> int:
+        old = self.state
+        self.state = (old * _PCG_MUL64 + _PCG_INC64) & _U64
+        return _xsh_rs_64_32(old)
+
+    def _advance_table(self) -> None:
+        carry = False
+        for i in range(len(self.table)):
+            if carry:
+                carry = self._step_entry(i)
+            carry = self._step_entry(i) or carry
+
+    def _step_entry(self, i: int) -> bool:
+        st = _rxs_m_xs_32_inverse(self.table[i])
+        st = (st * _PCG_MUL32 + _PCG_INC32 + 2 * (i + 1)) & _U32
+        self.table[i] = _rxs_m_xs_32(st)
+        return self.table[i] == 0
+
+    def __call__(self) -> int:
+        if (self.state & _U32) == 0:
+            self._advance_table()
+        ext = self.table[self.state & 1]
+        return self._base() ^ ext
+
+
+def _uniform_below(g, n: int) -> int:
+    """A uniform integer in [0, n) from a 32-bit generator, as libstdc++'s
+    uniform_int_distribution draws it: Lemire's multiply-and-reject ("Fast Random Integer
+    Generation in an Interval", 2019) on a 64-bit product."""
+    product = g() * n
+    low = product & _U32
+    if low < n:
+        threshold = ((1 << 32) - n) % n
+        while low < threshold:
+            product = g() * n
+            low = product & _U32
+    return product >> 32
+
+
+def std_shuffle(values: list, g) -> None:
+    """std::shuffle of libstdc++ (GCC 11 and later) with a 32-bit generator: Fisher-Yates from the
+    front, one draw per element, except that while i * (i + 1) fits the generator's range two
+    positions come from one draw of [0, (i + 1)(i + 2)) (its quotient and remainder by i + 2), after
+    a first single swap when the length is even."""
+    n = len(values)
+    if n < 2:
+        return
+    if (1 << 32) - 1 < n * n:
+        raise NotImplementedError("ranges beyond the paired draws are not needed here")
+    i = 1
+    if n % 2 == 0:
+        j = _uniform_below(g, 2)
+        values[1], values[j] = values[j], values[1]
+        i = 2
+    while i < n:
+        r = i + 1
+        x = _uniform_below(g, r * (r + 1))
+        a, b = x // (r + 1), x % (r + 1)
+        values[i], values[a] = values[a], values[i]
+        values[i + 1], values[b] = values[b], values[i + 1]
+        i += 2
+
+
+def perlin_tables(seed: int) -> np.ndarray:
+    """The reference's three lattice permutation tables of Perlin(seed) (perlin.cpp:137-152): one
+    pcg32_k2_fast seeded with the seed shuffles 0..255 for x, then y, then z; a padding entry
+    repeats each table's first value. (3, 257) uint8."""
+    g = Pcg32K2Fast(int(seed) & _U32)
+    out = np.zeros((3, 257), np.uint8)
+    for k in range(3):
+        t = list(range(256))
+        std_shuffle(t, g)
+        out[k, :256] = t
+        out[k, 256] = t[0]
+    return out
+
+
 class Perlin(Texture):
     """Perlin([seed]) (textures/perlin.cpp): improved Perlin noise of the hit point, a flat
-    spectrum. The lattice's three permutation tables are shuffled from the seed by this package's
-    own generator (numpy's PCG64, one permutation per axis); the reference shuffles with pcg-cpp's
-    pcg32_k2_fast through std::shuffle, so the same seed gives a differently placed but identically
-    constructed noise field."""
+    spectrum. The lattice's three permutation tables are the reference's for the same seed
+    (perlin_tables: pcg32_k2_fast through libstdc++'s std::shuffle, as a Linux build of the
+    reference draws them)."""
 
     def __init__(self, seed: int = 0):
         self.seed = int(seed)
@@ -258,13 +385,7 @@ class Perlin(Texture):
     @seed.setter
     def seed(self, value: int):
         self._seed = int(value) & 0xFFFFFFFF
-        rng = np.random.Generator(np.random.PCG64(self._seed))
-        tables = np.zeros((3, 257), np.uint8)
-        for k in range(3):
-            perm = rng.permutation(256)
-            tables[k, :256] = perm
-            tables[k, 256] = perm[0]          # the padding entry repeats the first
-        self.tables = tables
+        self.tables = perlin_tables(self._seed)
 
 
 class FBm(Perlin):

@@ -273,3 +273,35 @@ def test_oracle_noise_follows_the_hit_point(octaves):
     # within the sky estimate's noise (and the noise's change across a pixel)
     assert (err <= 4 * np.sqrt(var[..., 1]) + 0.01).mean() > 0.99 and np.ptp(expect) > 0.1
     assert np.corrcoef(img[..., 1].ravel(), expect.ravel())[0, 1] > 0.95
+
+
+def test_perlin_tables_are_the_references_for_the_seed():
+    """pcg32_k2_fast and std::shuffle as restated in textures.py against the vectors of
+    tests/golden/make_perlin_golden.py (pcg-cpp's generator and libstdc++'s std::shuffle, compiled):
+    the generator's first outputs, the three lattice tables of Perlin(seed) (perlin.cpp:137-152),
+    and shuffles of both parities."""
+    import json
+    from pathlib import Path
+    gold = json.loads((Path(__file__).resolve().parent / "golden" / "perlin_tables.json").read_text())
+    for seed, v in gold["seeds"].items():
+        g = tx.Pcg32K2Fast(int(seed))
+        assert [g() for _ in range(20)] == v["outputs"]
+        t = tx.Perlin(int(seed)).tables
+        assert (t[:, :256] == np.asarray(v["tables"])).all()
+        assert (t[:, 256] == t[:, 0]).all()
+        for n, ref in v["shuffles"].items():
+            vals = list(range(int(n)))
+            tx.std_shuffle(vals, tx.Pcg32K2Fast(int(seed)))
+            assert vals == ref
+
+
+def test_pcg_extension_table_advances_like_an_inside_out_generator():
+    """The table step (taken when the state's low 32 bits are zero) inverts the RXS M XS output,
+    steps the 32-bit LCG with increment + 2(i + 1) and outputs again."""
+    g = tx.Pcg32K2Fast(0)
+    for v in (0, 1, 0xDEADBEEF, 0xFFFFFFFF):
+        assert tx._rxs_m_xs_32_inverse(tx._rxs_m_xs_32(v)) == v
+    before = list(g.table)
+    g._advance_table()
+    st = (tx._rxs_m_xs_32_inverse(before[0]) * tx._PCG_MUL32 + tx._PCG_INC32 + 2) & 0xFFFFFFFF
+    assert g.table[0] == tx._rxs_m_xs_32(st)
