@@ -106,6 +106,13 @@ int liar_gpu_synchronize(liar_gpu_ctx* ctx);
  * cancelled render, not an estimate to keep). flag is the caller's host memory (any thread may
  * set it) and must stay valid until it is replaced; NULL removes it. */
 int liar_gpu_set_cancel_flag(liar_gpu_ctx* ctx, const volatile int32_t* flag);
+/* Failure injection for tests of the device-side timeout path (no reference counterpart). With
+ * LIAR_FAULT_TEST_GUIDE_WAIT the guide network kernels of ctx issue no tensor-core work and wait,
+ * with a short limit, for a completion that nothing signals: every such launch records a timeout,
+ * frees its tensor memory and returns, and the next liar_gpu_synchronize reports
+ * LIAR_ERR_TIMEOUT with the context still usable. 0 turns it off. */
+enum liar_fault_test { LIAR_FAULT_TEST_NONE = 0, LIAR_FAULT_TEST_GUIDE_WAIT = 1 };
+int liar_gpu_set_fault_test(liar_gpu_ctx* ctx, int mode);
 /* Selects / reads the trace kernels' launch shape (default 128 threads, 16 shared entries). */
 int liar_gpu_set_trace_config(liar_gpu_ctx* ctx, const liar_trace_config* cfg);
 int liar_gpu_get_trace_config(const liar_gpu_ctx* ctx, liar_trace_config* out);

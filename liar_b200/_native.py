@@ -72,6 +72,7 @@ SIGNATURES: dict[str, tuple] = {
     "liar_gpu_set_stream": (C.c_int, [_vp, _vp]),
     "liar_gpu_synchronize": (C.c_int, [_vp]),
     "liar_gpu_set_cancel_flag": (C.c_int, [_vp, _vp]),
+    "liar_gpu_set_fault_test": (C.c_int, [_vp, C.c_int]),
     "liar_gpu_set_trace_config": (C.c_int, [_vp, C.POINTER(TraceConfig)]),
     "liar_gpu_get_trace_config": (C.c_int, [_vp, C.POINTER(TraceConfig)]),
     "liar_gpu_mesh_build": (C.c_int, [_vp, _vp, _sz, _vp, _sz, _vp, C.POINTER(_vp)]),

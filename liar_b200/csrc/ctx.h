@@ -45,6 +45,8 @@ struct liar_gpu_ctx {
     std::unordered_map<const void*, int> occupancy;
     // the caller's cancel flag (liar_gpu_set_cancel_flag), read between waves and bounces
     const volatile int32_t* cancel_flag = nullptr;
+    // LIAR_FAULT_TEST_* mode of liar_gpu_set_fault_test (0: off)
+    int fault_test = 0;
     // resources of other subsystems (renderer, photon maps) register their release here
     std::vector<std::function<void()>> on_destroy;
     // per-subsystem state (work buffers of the renderer, photon maps), looked up by name

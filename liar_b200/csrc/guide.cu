@@ -36,7 +36,6 @@ struct liar_gpu_guide {
     uint2* frag_fwd = nullptr;
     uint2* frag_bwd = nullptr;
     unsigned char* umma_w = nullptr;  // B-operand images of the six layers for the tcgen05 inference
-    uint32_t* status = nullptr;       // device status word of the tcgen05 inference (bounded waits)
     // training scratch, sized for cap records
     size_t cap = 0;
     __nv_bfloat16* enc = nullptr;    // h_0 (the encodings): [cap][256]
@@ -161,10 +160,15 @@ __device__ __forceinline__ void load_frags(uint2* dst, const uint2* __restrict__
 }
 
 // ---- inference on tcgen05: two slots of 128 rows per CTA (guide_umma.cuh)
+// Every mbarrier wait is bounded by max_tries polls. A wait that runs out records the timeout,
+// waits once more (bounded again) for the commit it was waiting for, so that no MMA still writes
+// the accumulator, and the CTA frees its TMEM and leaves. issue_mma = 0 is the timeout test: no
+// MMA and no commit are issued, so the first wait runs out with nothing in flight.
 __global__ void __launch_bounds__(kTcThreads, 1) k_eval_tc(const unsigned char* __restrict__ w_img,
                                                            const float* __restrict__ in, size_t n, Box box,
                                                            float* __restrict__ mix, int stride,
-                                                           uint32_t* __restrict__ status) {
+                                                           uint32_t* __restrict__ status, uint32_t max_tries,
+                                                           int issue_mma) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     unsigned char* sw = smem;
@@ -200,7 +204,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_eval_tc(const unsigned char* 
     const uint32_t sw_addr = (uint32_t)__cvta_generic_to_shared(sw);
     const uint32_t buf_addr = (uint32_t)__cvta_generic_to_shared(buf);
     auto slot_sync = [&]() { asm volatile("bar.sync %0, 128;" ::"r"(1u + slot) : "memory"); };
-    constexpr uint32_t kMaxTries = 1u << 24;
     uint32_t phase = 0;
     const size_t n_tiles = (n + kTcRows - 1) / kTcRows;
     for (size_t tile = (size_t)blockIdx.x * kTcSlots + slot; tile < n_tiles; tile += (size_t)gridDim.x * kTcSlots) {
@@ -219,7 +222,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_eval_tc(const unsigned char* 
             tc_fence_before();
             slot_sync();
             tc_fence_after();
-            if (r == 0) {
+            if (r == 0 && issue_mma) {
                 const uint32_t K = (uint32_t)layer_k(l), N = (uint32_t)layer_n(l);
                 const uint32_t b_base = sw_addr + umma_w_offset(l);
                 const uint32_t idesc = umma_idesc(N);
@@ -228,13 +231,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_eval_tc(const unsigned char* 
                               umma_smem_desc(b_base + 256u * j, (K / 8) * 128u), idesc, j > 0 ? 1u : 0u);
                 umma_commit(mbar_addr);
             }
-            if (!mbar_wait(mbar_addr, phase, kMaxTries)) failed[slot] = 1u;
-            phase ^= 1u;
+            if (!mbar_wait(mbar_addr, phase, max_tries)) failed[slot] = 1u;
             slot_sync();  // the slot agrees on completion before anyone reads the accumulator
             if (failed[slot]) {
+                // drain: the commit this slot gave up on, if any, before the TMEM is freed
+                if (issue_mma) mbar_wait(mbar_addr, phase, max_tries);
                 ok = false;
                 break;
             }
+            phase ^= 1u;
             tc_fence_after();
             tmem_ld_x64(taddr, v);
             if (l < kLayers - 1) {
@@ -722,12 +727,6 @@ extern "C" int liar_gpu_guide_create(liar_gpu_ctx* ctx, const liar_guide_config*
     if (!rc) G->frag_bwd = static_cast<uint2*>(p);
     if (!rc) rc = g_alloc(ctx, G, kUmmaWBytes, &p, "guide operand images");
     if (!rc) G->umma_w = static_cast<unsigned char*>(p);
-    if (!rc) rc = g_alloc(ctx, G, 16, &p, "guide status");
-    if (!rc) {
-        G->status = static_cast<uint32_t*>(p);
-        cudaError_t e = cudaMemset(G->status, 0, 16);
-        if (e != cudaSuccess) rc = ctx_cuda(ctx, e, "guide status");
-    }
     if (!rc) {
         std::vector<float> P;
         init_params(P, cfg->seed);
@@ -810,8 +809,12 @@ int liar_gpu::guide::guide_eval(liar_gpu_ctx* ctx, const liar_gpu_guide* G, cons
     if (stride != kOutUsed && stride != kMixRender) return ctx_fail(ctx, LIAR_ERR_INVALID, "mixture stride %d", stride);
     const size_t tiles = (n + kTcRows - 1) / kTcRows;
     const unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>((tiles + kTcSlots - 1) / kTcSlots, (size_t)ctx->num_sms));
+    // the bounded waits' limit: 2^24 polls, far beyond a layer's MMAs; the timeout test
+    // (liar_gpu_set_fault_test) issues no MMA and gives up after 2^16 polls
+    const bool wait_test = ctx->fault_test == LIAR_FAULT_TEST_GUIDE_WAIT;
     k_eval_tc<<<grid, kTcThreads, kUmmaSmem, st>>>(G->umma_w, d_inputs, n, make_box(G->cfg), d_mixture, stride,
-                                                   G->status);
+                                                   ctx->d_scratch + kStatusWord, wait_test ? 1u << 16 : 1u << 24,
+                                                   wait_test ? 0 : 1);
     return ctx_cuda(ctx, cudaGetLastError(), "guide evaluation");
 }
 

@@ -411,6 +411,13 @@ extern "C" int liar_gpu_trace(liar_gpu_ctx* ctx, const liar_gpu_mesh* mesh, cons
     return ctx_check_status(ctx);
 }
 
+extern "C" int liar_gpu_set_fault_test(liar_gpu_ctx* ctx, int mode) {
+    if (!ctx) return LIAR_ERR_INVALID;
+    if (mode != 0 && mode != LIAR_FAULT_TEST_GUIDE_WAIT) return ctx_fail(ctx, LIAR_ERR_INVALID, "fault test %d", mode);
+    ctx->fault_test = mode;
+    return LIAR_OK;
+}
+
 extern "C" int liar_gpu_set_cancel_flag(liar_gpu_ctx* ctx, const volatile int32_t* flag) {
     if (!ctx) return LIAR_ERR_INVALID;
     ctx->cancel_flag = flag;

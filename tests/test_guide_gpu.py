@@ -262,3 +262,30 @@ def test_slit_room_guide_learns_the_slit():
     ratio = np.median(q) * 2 * np.pi  # against a uniform density over the hemisphere
     print(f"slit room: guide density toward the slit / uniform hemisphere = {ratio:.1f}")
     assert ratio > 5.0
+
+
+def test_bounded_wait_times_out_and_the_context_stays_usable():
+    """The tcgen05 inference kernel's mbarrier waits are bounded. Under the fault test mode no MMA
+    is issued, so every wait runs out: the launch records a timeout, frees its tensor memory and
+    returns; liar_gpu_synchronize reports LIAR_ERR_TIMEOUT, and afterwards the same guide on the
+    same context evaluates normally."""
+    import ctypes as C
+    from liar_b200._native import LiarGpuError
+    ctx = default_context()
+    g = GD.Guide(ctx, (np.array([-1, -1, -1], np.float32), np.array([1, 1, 1], np.float32)), seed=3)
+    x = torch.rand((3000, 9), device="cuda", generator=torch.Generator("cuda").manual_seed(1)) * 2 - 1
+    ref = g.eval(x)
+    ctx.synchronize()
+    ref = ref.clone()
+    ctx.check(ctx._lib.liar_gpu_set_fault_test(ctx.handle, C.c_int(1)))
+    try:
+        g.eval(x)
+        with pytest.raises(LiarGpuError) as err:
+            ctx.synchronize()
+        assert err.value.code == -6  # LIAR_ERR_TIMEOUT
+    finally:
+        ctx.check(ctx._lib.liar_gpu_set_fault_test(ctx.handle, C.c_int(0)))
+    again = g.eval(x)
+    ctx.synchronize()
+    torch.testing.assert_close(again, ref, rtol=0, atol=0)
+    g.close()
