@@ -226,3 +226,32 @@ def test_unknown_extension_fails_loudly(tmp_path):
     xyza, _ = _film(np.random.default_rng(4))
     with pytest.raises(ValueError):
         _save(tmp_path, "x.bmp", xyza)
+
+
+@pytest.mark.parametrize("fname", ["colors-srgb.png", "colors-adobergb.png"])
+def test_png_decoder_meets_the_references_codec_test(fname):
+    """The reference's own known answers (test/test_codecs.cpp, lodepng_srgb and lodepng_adobergb,
+    extracted to tests/golden/codec_colors.json): the space each test image reports and the XYZ
+    (illuminant E) at the centres of its 24 colour patches within the test's tolerance. The images
+    are read from a reference checkout (LIAR_REFERENCE_DIR, or a `reference` folder beside this
+    repository); without one the test is skipped."""
+    import json
+    import os
+    from pathlib import Path
+    here = Path(__file__).resolve().parent
+    ref = Path(os.environ.get("LIAR_REFERENCE_DIR", here.parents[1] / "reference"))
+    path = ref / "test" / fname
+    if not path.exists():
+        pytest.skip("no reference checkout")
+    gold = json.loads((here / "golden" / "codec_colors.json").read_text())
+    xyza, space = codecs.read(path)
+    assert xyza.shape == (400, 600, 4)
+    want = gold["files"][fname]
+    for name in ("red", "green", "blue", "white"):
+        assert np.allclose(getattr(space, name), want["chromaticities"][name], atol=gold["chromaticity_tolerance"])
+    assert abs(space.gamma - want["gamma"]) < gold["gamma_tolerance"]
+    for y in range(4):
+        for x in range(6):
+            px = xyza[100 * y + 50, 100 * x + 50]
+            assert np.all(np.abs(px[:3] - np.asarray(gold["xyz"][y][x])) < gold["xyz_tolerance"]), (y, x, px)
+            assert abs(px[3] - 1.0) < 1e-3
