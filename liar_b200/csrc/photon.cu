@@ -332,35 +332,55 @@ __global__ void __launch_bounds__(256) k_gather(const float4* __restrict__ sorte
                     }
                 }
                 const uint64_t my_key = pack_cell(ix, iy, iz);
-                uint32_t todo = __ballot_sync(0xffffffffu, s1 > s0);
-                while (todo) {
-                    const int src = __ffs(todo) - 1;
-                    todo &= todo - 1;
-                    const uint32_t b0 = __shfl_sync(0xffffffffu, s0, src), b1 = __shfl_sync(0xffffffffu, s1, src);
-                    const uint64_t target = __shfl_sync(0xffffffffu, (unsigned long long)my_key, src);
-                    for (uint32_t base = b0; base < b1; base += 32) {
-                        uint64_t key = INF;
-                        const uint32_t i = base + lane;
-                        if (i < b1 && __ldg(reinterpret_cast<const unsigned long long*>(cell_key) + i) == target) {
+                // the chunk's photons as one list: lane j's cell owns items [excl_j, excl_j + cnt_j)
+                // of it, so that a batch of 32 candidates spans as many cells as it takes (cells
+                // hold a photon or two on average; one batch per cell would leave most lanes idle)
+                // (64-bit counts: 32 colliding cells of one huge bucket must not wrap)
+                const uint64_t cnt = s1 - s0;
+                uint64_t incl = cnt;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint64_t t = __shfl_up_sync(0xffffffffu, (unsigned long long)incl, o);
+                    if ((int)lane >= o) incl += t;
+                }
+                const uint64_t total = __shfl_sync(0xffffffffu, (unsigned long long)incl, 31);
+                const uint64_t excl = incl - cnt;
+                for (uint64_t base = 0; base < total; base += 32) {
+                    const uint64_t item = base + lane;
+                    // the owning cell: the last lane whose list starts at or before the item
+                    // (every lane runs the same shuffles)
+                    uint32_t owner = 0;
+#pragma unroll
+                    for (uint32_t step = 16; step > 0; step >>= 1) {
+                        const uint64_t e = __shfl_sync(0xffffffffu, (unsigned long long)excl, (int)(owner + step));
+                        if (e <= item) owner += step;
+                    }
+                    const uint32_t o_s0 = __shfl_sync(0xffffffffu, s0, (int)owner);
+                    const uint64_t o_excl = __shfl_sync(0xffffffffu, (unsigned long long)excl, (int)owner);
+                    const uint64_t target = __shfl_sync(0xffffffffu, (unsigned long long)my_key, (int)owner);
+                    uint64_t key = INF;
+                    if (item < total) {
+                        const uint32_t i = o_s0 + (uint32_t)(item - o_excl);
+                        if (__ldg(reinterpret_cast<const unsigned long long*>(cell_key) + i) == target) {
                             const float4 p = __ldg(sorted + i);
                             const float d2 = dist2_exact(p.x, p.y, p.z, qx, qy, qz);
                             if (d2 < G.r2max) key = ((uint64_t)__float_as_uint(d2) << 32) | (uint64_t)__float_as_uint(p.w);
                         }
-                        if (__ballot_sync(0xffffffffu, key < kth) == 0u) continue;
-                        const uint64_t bsort = warp_sort32(key);
-                        // smallest 32 of hi and the batch: half-cleaner against the reversed batch
-                        // (every shuffle is executed by all 32 lanes, outside lane-dependent branches)
-                        const uint64_t brev = reverse_lanes(bsort);
-                        uint64_t m = hi < brev ? hi : brev;
-                        m = warp_bitonic_merge32(m);
-                        // lo (sorted) and m (sorted): split into the lower and upper 32
-                        const uint64_t mr = reverse_lanes(m);
-                        const uint64_t nlo = lo < mr ? lo : mr;
-                        const uint64_t nhi = lo < mr ? mr : lo;
-                        lo = warp_bitonic_merge32(nlo);
-                        hi = warp_bitonic_merge32(nhi);
-                        kth = __shfl_sync(0xffffffffu, (unsigned long long)hi, 31);
                     }
+                    if (__ballot_sync(0xffffffffu, key < kth) == 0u) continue;
+                    const uint64_t bsort = warp_sort32(key);
+                    // smallest 32 of hi and the batch: half-cleaner against the reversed batch
+                    // (every shuffle is executed by all 32 lanes, outside lane-dependent branches)
+                    const uint64_t brev = reverse_lanes(bsort);
+                    uint64_t m = hi < brev ? hi : brev;
+                    m = warp_bitonic_merge32(m);
+                    // lo (sorted) and m (sorted): split into the lower and upper 32
+                    const uint64_t mr = reverse_lanes(m);
+                    const uint64_t nlo = lo < mr ? lo : mr;
+                    const uint64_t nhi = lo < mr ? mr : lo;
+                    lo = warp_bitonic_merge32(nlo);
+                    hi = warp_bitonic_merge32(nhi);
+                    kth = __shfl_sync(0xffffffffu, (unsigned long long)hi, 31);
                 }
             }
             // every photon outside rings 0..R is farther than R cells (minus round-off)
