@@ -193,26 +193,34 @@ typedef struct liar_material {
 } liar_material;
 
 /* Textures of spectral material parameters (src/liar/textures/): a tree of nodes looked up at a
- * hit's (u, v) coordinates.
+ * hit's (u, v) coordinates. A camera hit carries the screen-space footprint of the camera's ray
+ * differentials (kernel/camera.cpp:53-60, intersection_context.cpp:295-324): the derivatives of
+ * (u, v) and of the hit point; every other hit has a zero footprint.
  *   CONSTANT      spectrum                                    (textures/constant.cpp)
  *   CHECKER       a where the fractional (u, v) lie on the same side of split p[0], p[1], else b
- *                 (CheckerBoard, checker_board.cpp:154-190 with anti-aliasing "none")
+ *                 (CheckerBoard, checker_board.cpp:113-207); p[2] = 1: bilinear anti-aliasing, the
+ *                 share of a over the footprint's (u, v) box blends a and b
  *   GRID          a on the lines of half thickness p[0] (u, and v from below) and p[1] (v from
  *                 above), else b (GridBoard, grid_board.cpp:60-67)
  *   UV_TRANSFORM  child a at (p[0] u + p[1] v + p[2], p[3] u + p[4] v + p[5]) (TransformationUv)
- *   IMAGE         an a x b image of XYZ pixels (rows from the top) starting at pixel `pixels` of the
- *                 scene's texture_pixels, looked up at (u, 1 - v) by nearest pixel (p[0] = 0) or
- *                 bilinearly (p[0] = 1) with wrap-around (Image, textures/image.cpp:279-718 at mip
- *                 level 0); the XYZ becomes a spectrum through the context's recovery table
- *                 (Spectral::fromXYZ), so scenes with images need liar_gpu_set_recovery first
+ *   IMAGE         an a x b image of XYZ pixels (rows from the top) with its mip levels, looked up
+ *                 at (u, 1 - v) with wrap-around by nearest pixel (p[0] = 0), bilinearly (p[0] = 1)
+ *                 or trilinearly across levels (p[0] = 2) (Image, textures/image.cpp:249-718); the
+ *                 XYZ becomes a spectrum through the context's recovery table (Spectral::fromXYZ),
+ *                 so scenes with images need liar_gpu_set_recovery first. texture_pixels[pixels]
+ *                 holds int32 bits {levels along u, levels along v, mip mode (0 none, 1 isotropic,
+ *                 2 anisotropic), 0}; the next levels_u x levels_v entries hold {offset low 31 bits,
+ *                 offset high bits, width, height} of level (iu, iv) at index iv x levels_u + iu,
+ *                 its pixels at texture_pixels[pixels + offset]
  *   NOISE         Perlin noise of the hit point (p[0] = 0: Perlin, perlin.cpp:60-205) or its fractal
- *                 sum over p[0] octaves with falloff p[1] (FBm, fbm.cpp:62-90), a flat spectrum;
- *                 permutation tables: 3 x 257 bytes at `pixels` of the scene's noise_tables
+ *                 sum over up to p[0] octaves with falloff p[1], fewer for a wide footprint (FBm,
+ *                 fbm.cpp:62-101), a flat spectrum; permutation tables: 3 x 257 bytes at `pixels`
+ *                 of the scene's noise_tables
  *   ABS           |child a| (Abs, abs.cpp:26-35)
  *   AFFINE        p[0] child a + p[1], the child looked up as an illuminant and the result
  *                 clamped to 1 as a reflectance (Product / Sum with one non-constant input,
  *                 product.cpp:90-99, sum.cpp:90-105)
- * A lookup applies at most 8 ABS / AFFINE nodes along its path. */
+ * A lookup applies at most 8 ABS / AFFINE / anti-aliased CHECKER nodes along any path. */
 enum liar_texture_type {
     LIAR_TEX_CONSTANT = 0, LIAR_TEX_CHECKER = 1, LIAR_TEX_GRID = 2, LIAR_TEX_UV_TRANSFORM = 3, LIAR_TEX_IMAGE = 4,
     LIAR_TEX_NOISE = 5, LIAR_TEX_ABS = 6, LIAR_TEX_AFFINE = 7

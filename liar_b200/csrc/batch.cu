@@ -253,7 +253,9 @@ __global__ void __launch_bounds__(128) k_b_shade(BParams P, BState<H> st, BQueue
             } else {
                 ++n_hit;
                 if (gen == 0) st.alpha[p] = 1.0f;
-                const HitContext HC = hit_context(S, o, d, (uint32_t)h.prim, h.t);
+                HitContext HC = hit_context(S, o, d, (uint32_t)h.prim, h.t);
+                // the camera vertex carries the camera's ray differentials (texture filtering)
+                if (S.n_tex > 0 && gen == 0) camera_footprint(S, HC, (uint32_t)h.prim, it.cam, key, it.width, it.height);
                 const int light = HC.light, mi = HC.mat;
                 if (gen > 0 && light >= 0)
                     for (int k = 0; k < H; ++k) L[k] += T[k] * spec_eval(S, S.lights[light].spectrum, lam[k], false);

@@ -285,6 +285,9 @@ __global__ void __launch_bounds__(128) k_dl_shade(DScene S, DParams W, DSamples 
     const uint32_t sg = CAP_REFL | CAP_TRANS | CAP_SPEC | W.glossy;
     if (shading) {
         HC = hit_context(S, o, d, (uint32_t)h.prim, h.t);
+        // the camera vertex carries the camera's ray differentials (texture filtering); reflected
+        // and transmitted tasks carry none
+        if (TEX && gen == 0) camera_footprint(S, HC, (uint32_t)h.prim, W.cam, dkey(W, W.first_path + p), W.width, W.height);
         if (HC.mat < 0) {
             n_ch = more ? 1u : 0u;  // no shader: continue through the surface
         } else {
@@ -521,7 +524,9 @@ __global__ void __launch_bounds__(128) k_pm_estimate(DScene S, DParams W, DSampl
     const float4 r0 = reinterpret_cast<const float4*>(tin.rays + q)[0];
     const float4 r1 = reinterpret_cast<const float4*>(tin.rays + q)[1];
     const float3 d = mk(r1.x, r1.y, r1.z);
-    const HitContext HC = hit_context(S, mk(r0.x, r0.y, r0.z), d, (uint32_t)hits[q].prim, hits[q].t);
+    HitContext HC = hit_context(S, mk(r0.x, r0.y, r0.z), d, (uint32_t)hits[q].prim, hits[q].t);
+    if (S.n_tex > 0 && (tin.meta[q] & 0xffu) == 0u)  // a camera vertex: its footprint, as k_dl_shade
+        camera_footprint(S, HC, (uint32_t)hits[q].prim, W.cam, dkey(W, W.first_path + p), W.width, W.height);
     const float lam = P.lam[p];
     const int32_t* idx = g_idx + (size_t)i * k;
     const float r2 = g_d2[(size_t)i * k + cnt - 1];

@@ -241,6 +241,8 @@ __global__ void __launch_bounds__(kShadeThreads) k_g_shade(DScene S, GParams W, 
             const float3 o = mk(r0.x, r0.y, r0.z), d = mk(r1.x, r1.y, r1.z);
             const SampleKey key = gkey(W, p);
             const int gen = P.gen[p];
+            // the camera vertex carries the camera's ray differentials (texture filtering)
+            if (TEX && surface && gen == 0) camera_footprint(S, HC, (uint32_t)h.prim, W.cam, key, W.width, W.height);
             float T = P.T[p], L = P.L[p];
             const float lam = P.lam[p];
             bool alive = false;

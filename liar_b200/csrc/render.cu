@@ -192,7 +192,9 @@ __global__ void __launch_bounds__(128) k_shade(DScene S, WaveParams W, Paths P, 
             ++n_hit;
             if (gen == 0) P.alpha[p] = 1.0f;
             // ---- IntersectionContext of the hit (re-intersection, normals flipped toward -d, frame)
-            const HitContext H = hit_context(S, o, d, (uint32_t)h.prim, h.t);
+            HitContext H = hit_context(S, o, d, (uint32_t)h.prim, h.t);
+            // the camera vertex carries the camera's ray differentials (texture filtering)
+            if (TEX && gen == 0) camera_footprint(S, H, (uint32_t)h.prim, W.cam, key, W.width, W.height);
             const int light = H.light;
             const int mi = H.mat;
             const float3 target = H.target, ng = H.ng, N = H.N, u = H.u, v = H.v;
@@ -459,10 +461,28 @@ extern "C" int liar_gpu_scene_upload(liar_gpu_ctx* ctx, const liar_scene_desc* d
             if (T.spectrum < 0 || T.spectrum >= (int32_t)D.n_spectra) return tex_err = "spectrum out of range", tex_bad = t, -1;
             d = 1;
         } else if (T.type == LIAR_TEX_IMAGE) {
-            if (T.a <= 0 || T.b <= 0 || T.pixels < 0 || !D.texture_pixels ||
-                (uint64_t)T.pixels + (uint64_t)T.a * (uint64_t)T.b > (uint64_t)D.n_texture_pixels)
+            // the mip table at `pixels` (see include/liar_gpu.h): level counts and mode, then per level
+            // the offset of its pixels (from `pixels`) and its size, every level inside the pool
+            const uint64_t np = D.n_texture_pixels;
+            if (T.a <= 0 || T.b <= 0 || T.pixels < 0 || !D.texture_pixels || (uint64_t)T.pixels >= np)
                 return tex_err = "image pixels out of range", tex_bad = t, -1;
-            if (!(T.p[0] == 0.0f || T.p[0] == 1.0f)) return tex_err = "image filter must be 0 or 1", tex_bad = t, -1;
+            const float* hp = D.texture_pixels + 4 * (size_t)T.pixels;
+            int32_t hdr[4];
+            std::memcpy(hdr, hp, sizeof(hdr));
+            const int n_u = hdr[0], n_v = hdr[1], mip = hdr[2];
+            if (n_u < 1 || n_u > 32 || n_v < 1 || n_v > 32 || mip < 0 || mip > 2 || (mip != 2 && n_v != 1) ||
+                (mip == 0 && n_u != 1) || (uint64_t)T.pixels + 1 + (uint64_t)n_u * n_v > np)
+                return tex_err = "bad image mip table", tex_bad = t, -1;
+            for (int lv = 0; lv < n_u * n_v; ++lv) {
+                int32_t e[4];
+                std::memcpy(e, hp + 4 * (1 + lv), sizeof(e));
+                const uint64_t off = ((uint64_t)(uint32_t)e[1] << 31) | (uint64_t)(uint32_t)e[0];
+                if (e[2] <= 0 || e[3] <= 0 || off < 1 + (uint64_t)n_u * n_v ||
+                    (uint64_t)T.pixels + off + (uint64_t)e[2] * (uint64_t)e[3] > np)
+                    return tex_err = "image mip level out of range", tex_bad = t, -1;
+            }
+            if (!(T.p[0] == 0.0f || T.p[0] == 1.0f || T.p[0] == 2.0f))
+                return tex_err = "image anti-aliasing must be 0, 1 or 2", tex_bad = t, -1;
             has_images = true;
             d = 1;
         } else if (T.type == LIAR_TEX_NOISE) {
@@ -477,7 +497,8 @@ extern "C" int liar_gpu_scene_upload(liar_gpu_ctx* ctx, const liar_scene_desc* d
             tex_depth[t] = -1;
             const int da = depth_of(T.a, level + 1);
             if (da < 0) return -1;
-            if (tex_post[T.a] + 1 > 8) return tex_err = "more than 8 Abs / Product / Sum nodes on a path", tex_bad = t, -1;
+            if (tex_post[T.a] + 1 > 8)
+                return tex_err = "more than 8 Abs, Product, Sum or anti-aliased CheckerBoard nodes on a path", tex_bad = t, -1;
             tex_post[t] = tex_post[T.a] + 1;
             d = da + 1;
         } else if (T.type == LIAR_TEX_CHECKER || T.type == LIAR_TEX_GRID || T.type == LIAR_TEX_UV_TRANSFORM) {
@@ -487,7 +508,11 @@ extern "C" int liar_gpu_scene_upload(liar_gpu_ctx* ctx, const liar_scene_desc* d
             int db = 0;
             if (T.type != LIAR_TEX_UV_TRANSFORM && (db = depth_of(T.b, level + 1)) < 0) return -1;
             d = std::max(da, db) + 1;
-            tex_post[t] = std::max(tex_post[T.a], T.type != LIAR_TEX_UV_TRANSFORM ? tex_post[T.b] : 0);
+            // an anti-aliased CheckerBoard waits for both children: one more pending operator
+            const int own = (T.type == LIAR_TEX_CHECKER && T.p[2] != 0.0f) ? 1 : 0;
+            tex_post[t] = std::max(tex_post[T.a], T.type != LIAR_TEX_UV_TRANSFORM ? tex_post[T.b] : 0) + own;
+            if (tex_post[t] > 8)
+                return tex_err = "more than 8 Abs, Product, Sum or anti-aliased CheckerBoard nodes on a path", tex_bad = t, -1;
         } else {
             return tex_err = "bad type", tex_bad = t, -1;
         }

@@ -658,6 +658,9 @@ struct HitContext {
     bool leaving;   // solid event from the unflipped geometric normal
     int obj, light, mat;
     float uv_u, uv_v;  // surface coordinates: the triangle corners' (u, v) at the barycentrics, or those
+    // screen-space footprint (IntersectionContext::dUv_dI / dUv_dJ and the larger squared norm of
+    // dPoint_dI, dPoint_dJ): zero unless the hit carries ray differentials (hit_footprint)
+    float du_i = 0.0f, dv_i = 0.0f, du_j = 0.0f, dv_j = 0.0f, fp2 = 0.0f;
 };
 
 __device__ inline HitContext hit_context(const DScene& S, float3 o, float3 d, uint32_t prim, float t) {
@@ -747,34 +750,6 @@ __device__ inline HitContext hit_context(const DScene& S, float3 o, float3 d, ui
 // Image::lookUp at mip level 0 (textures/image.cpp:654-718, 598-609): (u, 1 - v) over the
 // pixels with wrap-around, nearest or bilinear between pixel centres; the indices are clamped
 // where float rounding puts a wrapped coordinate on the image's far edge
-__device__ inline float3 image_lookup(const DScene& S, const liar_texture& T, float u, float v) {
-    const int nx = T.a, ny = T.b;
-    const float4* px = S.tex_pixels + T.pixels;
-    const float fx = (float)nx, fy = (float)ny;
-    if (T.p[0] == 0.0f) {
-        int x0 = (int)floorf((u - floorf(u)) * fx);
-        const float w = 1.0f - v;
-        int y0 = (int)floorf((w - floorf(w)) * fy);
-        x0 = min(max(x0, 0), nx - 1);
-        y0 = min(max(y0, 0), ny - 1);
-        const float4 p = px[(size_t)y0 * nx + x0];
-        return make_float3(p.x, p.y, p.z);
-    }
-    float x = u * fx - 0.5f, y = (1.0f - v) * fy - 0.5f;
-    x -= floorf(x / fx) * fx;  // num::mod into [0, n)
-    y -= floorf(y / fy) * fy;
-    const float x0 = floorf(x), y0 = floorf(y);
-    const float dx = x - x0, dy = y - y0;
-    const int i0 = min(max((int)x0, 0), nx - 1), j0 = min(max((int)y0, 0), ny - 1);
-    const int i1 = i0 + 1 == nx ? 0 : i0 + 1, j1 = j0 + 1 == ny ? 0 : j0 + 1;
-    const float4 p00 = px[(size_t)j0 * nx + i0], p10 = px[(size_t)j0 * nx + i1];
-    const float4 p01 = px[(size_t)j1 * nx + i0], p11 = px[(size_t)j1 * nx + i1];
-    const float ex = 1.0f - dx, ey = 1.0f - dy;
-    return make_float3((p00.x * ex + p10.x * dx) * ey + (p01.x * ex + p11.x * dx) * dy,
-                       (p00.y * ex + p10.y * dx) * ey + (p01.y * ex + p11.y * dx) * dy,
-                       (p00.z * ex + p10.z * dx) * ey + (p01.z * ex + p11.z * dx) * dy);
-}
-
 // Perlin::noise (perlin.cpp:60-90, 170-205): improved Perlin noise over a 256-periodic lattice,
 // gradients picked by the xor of three permutation tables (257 entries each, the last repeating
 // the first), quintic fade, trilinear blend
@@ -828,94 +803,264 @@ __device__ inline float perlin_noise(const uint8_t* tab, float3 q) {
     return lerp(lerp(lerp(g0, g1, sx), lerp(g2, g3, sx), sy), lerp(lerp(g4, g5, sx), lerp(g6, g7, sx), sy), sz);
 }
 
-// FBm::doScalarLookUp (fbm.cpp:62-90) with a zero footprint (every octave): octaves of noise at
-// doubling frequencies, each weighed by falloff^k; p[0] = 0 is plain Perlin noise
-__device__ inline float noise_texture(const DScene& S, const liar_texture& T, float3 x) {
+// the point a texture is looked up at: (u, v) with its screen-space derivatives, the squared
+// footprint on the surface (FBm's octave count) and the hit point (noise textures)
+struct TexPoint {
+    float u, v, du_i, dv_i, du_j, dv_j, fp2;
+    float3 x;
+};
+
+// CheckerBoard::weightA (checker_board.cpp:149-181): 1 or 0 without anti-aliasing; with bilinear
+// anti-aliasing the share of A over the footprint's (u, v) box, half a derivative to each side
+// (CheckerBoard::integrate, checker_board.cpp:185-207), the point rule where the box is empty
+__device__ inline float checker_weight(const liar_texture& T, const TexPoint& q) {
+    const float sx = T.p[0], sy = T.p[1];
+    const float fu = q.u - floorf(q.u), fv = q.v - floorf(q.v);
+    const float point = (fu < sx) == (fv < sy) ? 1.0f : 0.0f;
+    if (T.p[2] == 0.0f) return point;
+    const float du = fmaxf(fabsf(q.du_i), fabsf(q.du_j)), dv = fmaxf(fabsf(q.dv_i), fabsf(q.dv_j));
+    const float area = du * dv;
+    if (!(area > 0.0f)) return point;
+    const float mnu = fu - du / 2, mnv = fv - dv / 2, mxu = fu + du / 2, mxv = fv + dv / 2;
+    const float mn0u = floorf(mnu), mn0v = floorf(mnv), mx0u = floorf(mxu), mx0v = floorf(mxv);
+    const float d0u = mx0u - mn0u, d0v = mx0v - mn0v;
+    const float dmnu = mnu - mn0u, dmnv = mnv - mn0v, dmxu = mxu - mx0u, dmxv = mxv - mx0v;
+    // (min(d, split), max(d - split, 0)) per corner and axis
+    const float mnU0 = fminf(dmnu, sx), mnU1 = fmaxf(dmnu - sx, 0.0f);
+    const float mnV0 = fminf(dmnv, sy), mnV1 = fmaxf(dmnv - sy, 0.0f);
+    const float mxU0 = fminf(dmxu, sx), mxU1 = fmaxf(dmxu - sx, 0.0f);
+    const float mxV0 = fminf(dmxv, sy), mxV1 = fmaxf(dmxv - sy, 0.0f);
+    const float oneU0 = sx, oneU1 = 1.0f - sx, oneV0 = sy, oneV1 = 1.0f - sy;
+    float r = (sx * sy + (1.0f - sx) * (1.0f - sy)) * d0u * d0v;
+    r += ((oneU0 * mxV0 + oneU1 * mxV1) - (oneU0 * mnV0 + oneU1 * mnV1)) * d0u;
+    r += ((mxU0 * oneV0 + mxU1 * oneV1) - (mnU0 * oneV0 + mnU1 * oneV1)) * d0v;
+    r += (mxU0 * mxV0 + mxU1 * mxV1) - (mxU0 * mnV0 + mxU1 * mnV1);
+    r += (mnU0 * mnV0 + mnU1 * mnV1) - (mnU0 * mxV0 + mnU1 * mxV1);
+    return fminf(fmaxf(r / area, 0.0f), 1.0f);
+}
+
+// Image::mipMapLevel (image.cpp:580-612): the level of a footprint `width` in (u or v) units is
+// maxLevel + log2(width), its fraction from the significand (log2(m) ~ m - 1 for 1 <= m < 2)
+__device__ inline void mip_level(float width, int n_levels, int& l0, int& l1, float& frac) {
+    const int max_level = n_levels - 1;
+    const float w = fmaxf(width, 1e-9f);
+    const int i = __float_as_int(w);
+    const int level = max_level + ((i >> 23) - 127);
+    if (level < 0) {
+        l0 = l1 = 0;
+        frac = 0.0f;
+    } else if (level >= max_level) {
+        l0 = l1 = max_level;
+        frac = 0.0f;
+    } else {
+        l0 = level;
+        l1 = level + 1;
+        frac = __int_as_float((127 << 23) | (i & 0x7fffff)) - 1.0f;
+    }
+}
+
+// one level of an image's mip table (the header at `pixels`: level counts, then per level the
+// offset of its pixels and its size; textures.Image lays it out)
+struct MipLevel {
+    const float4* px;
+    int w, h;
+};
+__device__ __forceinline__ MipLevel mip_get(const DScene& S, const liar_texture& T, int n_u, int iu, int iv) {
+    const float4* base = S.tex_pixels + T.pixels;
+    const float4 e = base[1 + iv * n_u + iu];
+    MipLevel m;
+    m.px = base + ((int64_t)__float_as_int(e.y) << 31 | (int64_t)(uint32_t)__float_as_int(e.x));
+    m.w = __float_as_int(e.z);
+    m.h = __float_as_int(e.w);
+    return m;
+}
+
+// Image::nearest (image.cpp:618-631): the pixel under (u, 1 - v), wrapped
+__device__ inline float3 image_nearest(const MipLevel& m, float u, float v) {
+    const float w = 1.0f - v;
+    int x0 = (int)floorf((u - floorf(u)) * (float)m.w);
+    int y0 = (int)floorf((w - floorf(w)) * (float)m.h);
+    x0 = min(max(x0, 0), m.w - 1);
+    y0 = min(max(y0, 0), m.h - 1);
+    const float4 p = m.px[(size_t)y0 * m.w + x0];
+    return mk(p.x, p.y, p.z);
+}
+
+// Image::bilinear (image.cpp:636-690, the vectorised build): the fractional (u, 1 - v) scaled to
+// the level, half a pixel back, the four neighbours with wrap-around
+__device__ inline float3 image_bilinear(const MipLevel& m, float u, float v) {
+    const float w = 1.0f - v;
+    const float x = (u - floorf(u)) * (float)m.w - 0.5f, y = (w - floorf(w)) * (float)m.h - 0.5f;
+    const float x0 = floorf(x), y0 = floorf(y);
+    const float dx = x - x0, dy = y - y0;
+    int i0 = (int)x0, j0 = (int)y0;
+    if (i0 < 0) i0 += m.w;
+    if (j0 < 0) j0 += m.h;
+    i0 = min(max(i0, 0), m.w - 1);
+    j0 = min(max(j0, 0), m.h - 1);
+    const int i1 = i0 + 1 < m.w ? i0 + 1 : 0, j1 = j0 + 1 < m.h ? j0 + 1 : 0;
+    const float4 p00 = m.px[(size_t)j0 * m.w + i0], p10 = m.px[(size_t)j0 * m.w + i1];
+    const float4 p01 = m.px[(size_t)j1 * m.w + i0], p11 = m.px[(size_t)j1 * m.w + i1];
+    const float ex = 1.0f - dx, ey = 1.0f - dy;
+    const float3 a = mk(ex * p00.x + dx * p10.x, ex * p00.y + dx * p10.y, ex * p00.z + dx * p10.z);
+    const float3 b = mk(ex * p01.x + dx * p11.x, ex * p01.y + dx * p11.y, ex * p01.z + dx * p11.z);
+    return mk(ey * a.x + dy * b.x, ey * a.y + dy * b.y, ey * a.z + dy * b.z);
+}
+
+// Image::lookUp (image.cpp:249-330): mip levels from the footprint (none: level 0; isotropic: the
+// largest derivative over one chain of levels; anisotropic: u and v derivatives over a table of
+// levels), then nearest, bilinear, or trilinear (bilinear lookups blended across the levels)
+__device__ inline float3 image_lookup(const DScene& S, const liar_texture& T, const TexPoint& q) {
+    const float4 hdr = S.tex_pixels[T.pixels];
+    const int n_u = __float_as_int(hdr.x), n_v = __float_as_int(hdr.y), mip = __float_as_int(hdr.z);
+    int u0 = 0, u1 = 0, v0 = 0, v1 = 0;
+    float fu = 0.0f, fv = 0.0f;
+    const float wu = fmaxf(fabsf(q.du_i), fabsf(q.du_j)), wv = fmaxf(fabsf(q.dv_i), fabsf(q.dv_j));
+    if (mip == 1) {
+        mip_level(fmaxf(wu, wv), n_u, u0, u1, fu);
+    } else if (mip == 2) {
+        mip_level(wu, n_u, u0, u1, fu);
+        mip_level(wv, n_v, v0, v1, fv);
+    }
+    const int aa = (int)T.p[0];
+    if (aa == 0) return image_nearest(mip_get(S, T, n_u, u0, v0), q.u, q.v);
+    if (aa == 1) return image_bilinear(mip_get(S, T, n_u, u0, v0), q.u, q.v);
+    const float3 p00 = image_bilinear(mip_get(S, T, n_u, u0, v0), q.u, q.v);
+    const float3 p10 = image_bilinear(mip_get(S, T, n_u, u1, v0), q.u, q.v);
+    const float eu = 1.0f - fu;
+    float3 r = mk(eu * p00.x + fu * p10.x, eu * p00.y + fu * p10.y, eu * p00.z + fu * p10.z);
+    if (v0 != v1) {
+        const float3 p01 = image_bilinear(mip_get(S, T, n_u, u0, v1), q.u, q.v);
+        const float3 p11 = image_bilinear(mip_get(S, T, n_u, u1, v1), q.u, q.v);
+        const float3 r1 = mk(eu * p01.x + fu * p11.x, eu * p01.y + fu * p11.y, eu * p01.z + fu * p11.z);
+        const float ev = 1.0f - fv;
+        r = mk(ev * r.x + fv * r1.x, ev * r.y + fv * r1.y, ev * r.z + fv * r1.z);
+    }
+    return r;
+}
+
+// FBm::doScalarLookUp (fbm.cpp:76-101): 1 - log2(footprint^2) / 2 octaves, clamped to [1, octaves],
+// the fraction of the last one blended in; p[0] = 0 is plain Perlin noise (perlin.cpp:60-90)
+__device__ inline float noise_texture(const DScene& S, const liar_texture& T, const TexPoint& q) {
     const uint8_t* tab = S.noise_tables + T.pixels;
     const int octaves = (int)T.p[0];
-    if (octaves <= 0) return perlin_noise(tab, x);
+    if (octaves <= 0) return perlin_noise(tab, q.x);
+    const float ideal = 1.0f - log2f(q.fp2) / 2.0f;  // +inf for a zero footprint
+    const float real = fminf(fmaxf(ideal, 1.0f), (float)octaves);
+    const int n = (int)floorf(real);
     float result = 0.0f, freq = 1.0f, weight = 1.0f;
-    for (int k = 0; k < octaves; ++k) {
-        result += weight * perlin_noise(tab, freq * x);
+    for (int k = 0; k < n; ++k) {
+        result += weight * perlin_noise(tab, freq * q.x);
         freq *= 2.0f;
         weight *= T.p[1];
     }
+    const float frac = real - (float)n;
+    if (frac > 0.0f) result += frac * weight * perlin_noise(tab, freq * q.x);
     return result;
 }
 
-// Texture::lookUp of a tree of uv textures: the transforms move (u, v), the boards pick a child
-// (without anti-aliasing a board always picks one), the leaf is a spectrum
-// kept out of line, reading the scene from its device copy: the shading kernels carry one call
-// instead of the lookup's registers and frame
-static __device__ __noinline__ float texture_eval(const DScene* __restrict__ G, int t, float u, float v, float3 x, float lam,
-                                           bool reflectant) {
+// Texture::lookUp of a texture tree (src/liar/textures/): transforms move (u, v) and its
+// derivatives, boards pick a child or (anti-aliased CheckerBoard) blend both, images and noise are
+// leaves, ABS / AFFINE apply to the value below them (abs.cpp:26-35; Product / Sum with constants,
+// product.cpp:90-99, sum.cpp:90-105, look their input up as an illuminant and clamp as a
+// reflectance), anything else is its spectrum. The operators waiting for values below them sit on a
+// frame stack of at most kTexOps entries (the scene upload refuses trees with more on one path).
+// Kept out of line, reading the scene from its device copy, so the shading kernels carry one call
+// instead of the lookup's registers and frame.
+constexpr int kTexOps = 8;
+struct TexFrame {
+    int op;        // LIAR_TEX_ABS, LIAR_TEX_AFFINE, or LIAR_TEX_CHECKER (a blend)
+    float a, b;    // AFFINE: a v + b; CHECKER: the weight of child A in a
+    bool refl;     // the caller's spectral type
+    bool second;   // CHECKER: child A's value is in va, child B is being looked up
+    float va;
+    int tb;        // CHECKER: child B, looked up at q
+    TexPoint q;
+};
+static __device__ __noinline__ float texture_eval(const DScene* __restrict__ G, int t, TexPoint q, float lam,
+                                                  bool reflectant) {
     const DScene& S = *G;
-    // ABS / AFFINE nodes on the way down, applied to the leaf's value on the way back
-    int post_type[8];
-    float post_a[8], post_b[8];
-    bool post_refl[8];
-    int n_post = 0;
-    auto finish = [&](float val) {
-        for (int k = n_post - 1; k >= 0; --k) {
-            if (post_type[k] == LIAR_TEX_ABS) {
-                val = fabsf(val);
-            } else {
-                val = post_a[k] * val + post_b[k];
-                if (post_refl[k]) val = fminf(val, 1.0f);
-            }
-        }
-        return val;
-    };
-    for (int depth = 0; depth < 32 && t >= 0 && t < S.n_tex; ++depth) {
-        const liar_texture T = S.texs[t];
-        switch (T.type) {
-            case LIAR_TEX_CHECKER: {
-                const float fu = u - floorf(u), fv = v - floorf(v);
-                t = ((fu < T.p[0]) == (fv < T.p[1])) ? T.a : T.b;
-                break;
-            }
-            case LIAR_TEX_GRID: {
-                const float fu = u - floorf(u), fv = v - floorf(v);
+    TexFrame fr[kTexOps];
+    int n = 0;
+    while (true) {
+        // ---- down: from node t to a leaf value, pushing the operators met on the way
+        float val = 0.0f;
+        for (int steps = 0;; ++steps) {
+            if (steps >= 64 || t < 0 || t >= S.n_tex) return 0.0f;
+            const liar_texture T = S.texs[t];
+            if (T.type == LIAR_TEX_CHECKER) {
+                const float wa = checker_weight(T, q);
+                if (wa >= 1.0f) {
+                    t = T.a;
+                } else if (wa <= 0.0f) {
+                    t = T.b;
+                } else {
+                    // Spectral(wA A + (1 - wA) B, type) of the two looked up as illuminants
+                    if (n == kTexOps) return 0.0f;
+                    fr[n++] = TexFrame{LIAR_TEX_CHECKER, wa, 0.0f, reflectant, false, 0.0f, T.b, q};
+                    reflectant = false;
+                    t = T.a;
+                }
+            } else if (T.type == LIAR_TEX_GRID) {
+                const float fu = q.u - floorf(q.u), fv = q.v - floorf(q.v);
                 const bool on = fu < T.p[0] || fv < T.p[0] || fu > 1.0f - T.p[0] || fv > 1.0f - T.p[1];
                 t = on ? T.a : T.b;
-                break;
-            }
-            case LIAR_TEX_UV_TRANSFORM: {
-                const float nu = T.p[0] * u + T.p[1] * v + T.p[2];
-                const float nv = T.p[3] * u + T.p[4] * v + T.p[5];
-                u = nu;
-                v = nv;
+            } else if (T.type == LIAR_TEX_UV_TRANSFORM) {
+                TexPoint m = q;
+                m.u = T.p[0] * q.u + T.p[1] * q.v + T.p[2];
+                m.v = T.p[3] * q.u + T.p[4] * q.v + T.p[5];
+                m.du_i = T.p[0] * q.du_i + T.p[1] * q.dv_i;
+                m.dv_i = T.p[3] * q.du_i + T.p[4] * q.dv_i;
+                m.du_j = T.p[0] * q.du_j + T.p[1] * q.dv_j;
+                m.dv_j = T.p[3] * q.du_j + T.p[4] * q.dv_j;
+                q = m;
                 t = T.a;
-                break;
-            }
-            case LIAR_TEX_IMAGE: {
+            } else if (T.type == LIAR_TEX_ABS || T.type == LIAR_TEX_AFFINE) {
+                if (n == kTexOps) return 0.0f;
+                fr[n++] = TexFrame{T.type, T.p[0], T.p[1], reflectant, false, 0.0f, -1, q};
+                if (T.type == LIAR_TEX_AFFINE) reflectant = false;  // the input looked up as an illuminant
+                t = T.a;
+            } else if (T.type == LIAR_TEX_IMAGE) {
                 // Image::doLookUp: Spectral::fromXYZ of the looked-up colour
-                const float3 c = image_lookup(S, T, u, v);
+                const float3 c = image_lookup(S, T, q);
                 RecoveryBlend b;
-                if (!recovery_locate(S.rec, c.x, c.y, c.z, b)) return finish(0.0f);
-                return finish(recovery_eval(S.rec, b, lam, reflectant));
-            }
-            case LIAR_TEX_NOISE: {
-                const float n = noise_texture(S, T, x);  // Spectral(value, type): min(value, 1) as a reflectance
-                return finish(reflectant ? fminf(n, 1.0f) : n);
-            }
-            case LIAR_TEX_ABS:
-            case LIAR_TEX_AFFINE: {
-                if (n_post == 8) return 0.0f;
-                post_type[n_post] = T.type;
-                post_a[n_post] = T.p[0];
-                post_b[n_post] = T.p[1];
-                post_refl[n_post] = reflectant;
-                ++n_post;
-                if (T.type == LIAR_TEX_AFFINE) reflectant = false;  // inputs looked up as illuminants
-                t = T.a;
+                val = recovery_locate(S.rec, c.x, c.y, c.z, b) ? recovery_eval(S.rec, b, lam, reflectant) : 0.0f;
+                break;
+            } else if (T.type == LIAR_TEX_NOISE) {
+                const float v = noise_texture(S, T, q);  // Spectral(value, type): min(value, 1) as a reflectance
+                val = reflectant ? fminf(v, 1.0f) : v;
+                break;
+            } else {
+                val = spec_eval(S, T.spectrum, lam, reflectant);
                 break;
             }
-            default:
-                return finish(spec_eval(S, T.spectrum, lam, reflectant));
         }
+        // ---- up: apply the waiting operators; a blend whose first child is done looks up its second
+        bool descend = false;
+        while (n > 0 && !descend) {
+            TexFrame& f = fr[n - 1];
+            if (f.op == LIAR_TEX_ABS) {
+                val = fabsf(val);
+                --n;
+            } else if (f.op == LIAR_TEX_AFFINE) {
+                val = f.a * val + f.b;
+                if (f.refl) val = fminf(val, 1.0f);
+                --n;
+            } else if (!f.second) {
+                f.second = true;
+                f.va = val;
+                t = f.tb;
+                q = f.q;
+                reflectant = false;
+                descend = true;
+            } else {
+                val = f.a * f.va + (1.0f - f.a) * val;
+                if (f.refl) val = fminf(val, 1.0f);
+                --n;
+            }
+        }
+        if (!descend) return val;
     }
-    return 0.0f;
 }
 
 // a material parameter: its texture at the hit, else its constant spectrum
@@ -923,7 +1068,9 @@ static __device__ __noinline__ float texture_eval(const DScene* __restrict__ G, 
 template <bool TEX>
 __device__ __forceinline__ float param_eval(const DScene& S, const liar_material& M, int k, const HitContext& H,
                                             float lam, bool reflectant) {
-    if (TEX && M.tex[k] >= 0) return texture_eval(S.self, M.tex[k], H.uv_u, H.uv_v, H.target, lam, reflectant);
+    if (TEX && M.tex[k] >= 0)
+        return texture_eval(S.self, M.tex[k], TexPoint{H.uv_u, H.uv_v, H.du_i, H.dv_i, H.du_j, H.dv_j, H.fp2, H.target},
+                            lam, reflectant);
     return spec_eval(S, M.spec[k], lam, reflectant);
 }
 
@@ -987,21 +1134,16 @@ __device__ inline Bsdf make_bsdf(const DScene& S, const liar_material& M, const 
 // PerspectiveCamera::doGenerateRay (cameras/perspective_camera.cpp:406-434) for the pixel and
 // sample of key k: stratified jitter in the pixel, thin-lens when the lens radius and focus
 // distance are set; the ray's limits scale the camera's near/far planes by 1 / cos(axis angle)
-__device__ inline liar_ray camera_ray(const liar_camera& C, const SampleKey& k, int width, int height) {
-    const uint32_t px = k.pixel % (uint32_t)width, py = k.pixel / (uint32_t)width;
-    float jx, jy;
-    sample_2d(k, DIM_SCREEN, jx, jy);
-    const float sx = ((float)px + jx) / (float)width;
-    const float sy = ((float)py + jy) / (float)height;
-    float3 pos = mk(C.position[0], C.position[1], C.position[2]);
-    float3 dir = mk(C.direction[0], C.direction[1], C.direction[2]) + (sx - 0.5f) * mk(C.right[0], C.right[1], C.right[2]) +
-                 (sy - 0.5f) * mk(C.down[0], C.down[1], C.down[2]);
+// PerspectiveCamera::doGenerateRay at screen point (sx, sy) and lens sample (lu, lv)
+__device__ inline void camera_ray_at(const liar_camera& C, float sx, float sy, float lu, float lv, float3& pos,
+                                     float3& dir, float& factor) {
+    pos = mk(C.position[0], C.position[1], C.position[2]);
+    dir = mk(C.direction[0], C.direction[1], C.direction[2]) + (sx - 0.5f) * mk(C.right[0], C.right[1], C.right[2]) +
+          (sy - 0.5f) * mk(C.down[0], C.down[1], C.down[2]);
     dir = normal(dir);
     const float3 dn = mk(C.direction_normal[0], C.direction_normal[1], C.direction_normal[2]);
-    float factor = 1.0f / dot(dir, dn);
+    factor = 1.0f / dot(dir, dn);
     if (C.lens_radius > 0.0f && C.focus_distance > 0.0f && C.focus_distance < 3.4e38f) {
-        float lu, lv;
-        sample_2d(k, DIM_LENS, lu, lv);
         const float2 lens = concentric_disk(lu, lv);
         const float3 lp = pos + (C.lens_radius * lens.x) * mk(C.right_normal[0], C.right_normal[1], C.right_normal[2]) +
                           (C.lens_radius * lens.y) * mk(C.down_normal[0], C.down_normal[1], C.down_normal[2]);
@@ -1010,7 +1152,133 @@ __device__ inline liar_ray camera_ray(const liar_camera& C, const SampleKey& k, 
         dir = normal(fp - lp);
         factor = 1.0f / dot(dir, dn);
     }
+}
+
+// screen and lens samples of key k
+__device__ __forceinline__ void camera_samples(const SampleKey& k, int width, int height, float& sx, float& sy,
+                                               float& lu, float& lv) {
+    const uint32_t px = k.pixel % (uint32_t)width, py = k.pixel / (uint32_t)width;
+    float jx, jy;
+    sample_2d(k, DIM_SCREEN, jx, jy);
+    sx = ((float)px + jx) / (float)width;
+    sy = ((float)py + jy) / (float)height;
+    lu = lv = 0.5f;
+    sample_2d(k, DIM_LENS, lu, lv);
+}
+
+// PerspectiveCamera::doGenerateRay (cameras/perspective_camera.cpp:406-434) for the pixel and
+// sample of key k: stratified jitter in the pixel, thin-lens when the lens radius and focus
+// distance are set; the ray's limits scale the camera's near/far planes by 1 / cos(axis angle)
+__device__ inline liar_ray camera_ray(const liar_camera& C, const SampleKey& k, int width, int height) {
+    float sx, sy, lu, lv;
+    camera_samples(k, width, height, sx, sy, lu, lv);
+    float3 pos, dir;
+    float factor;
+    camera_ray_at(C, sx, sy, lu, lv, pos, dir, factor);
     return liar_ray{pos.x, pos.y, pos.z, fmaxf(kTol, factor * C.near_limit), dir.x, dir.y, dir.z, factor * C.far_limit};
+}
+
+// Camera::primaryRay's two differential rays (kernel/camera.cpp:53-60): the same lens sample at the
+// screen point moved by one sample spacing along x and along y; RenderEngine spaces them
+// 1 / (resolution sqrt(samples per pixel)) apart (render_engine.cpp:211-215)
+__device__ inline void camera_differentials(const liar_camera& C, const SampleKey& k, int width, int height,
+                                            float3& oi, float3& di, float3& oj, float3& dj) {
+    float sx, sy, lu, lv, f;
+    camera_samples(k, width, height, sx, sy, lu, lv);
+    const float root = sqrtf((float)k.spp);
+    const float dsx = 1.0f / ((float)width * root), dsy = 1.0f / ((float)height * root);
+    camera_ray_at(C, sx + dsx, sy, lu, lv, oi, di, f);
+    camera_ray_at(C, sx, sy + dsy, lu, lv, oj, dj, f);
+}
+
+// dPoint/du and dPoint/dv of a hit's surface parametrisation: a triangle's corner uvs (without
+// them its barycentrics, so the edges), a sphere's spherical angles (sphere.cpp:150-172)
+__device__ inline bool hit_dpduv(const DScene& S, uint32_t prim, float3 n_out, float3& dpdu, float3& dpdv) {
+    if (prim >= S.n_tris) {
+        const float r = S.spheres[prim - S.n_tris].w;
+        constexpr float kPi = 3.14159265358979323846f;
+        const float theta = acosf(fminf(fmaxf(n_out.z, -1.0f), 1.0f));
+        const float st = sinf(theta);
+        dpdu = (r * 2.0f * kPi) * mk(-n_out.y, n_out.x, 0.0f);
+        if (st != 0.0f) {
+            const float cs = n_out.z / st;
+            dpdv = (r * kPi) * mk(cs * n_out.x, cs * n_out.y, -st);
+        } else {
+            const float phi = atan2f(n_out.y, n_out.x);
+            dpdv = (r * kPi) * mk(cosf(phi), sinf(phi), 0.0f);
+        }
+        return true;
+    }
+    const uint32_t i0 = S.tri_idx[3 * prim], i1 = S.tri_idx[3 * prim + 1], i2 = S.tri_idx[3 * prim + 2];
+    const float3 a = mk(S.verts[3 * i0], S.verts[3 * i0 + 1], S.verts[3 * i0 + 2]);
+    const float3 e1 = mk(S.verts[3 * i1], S.verts[3 * i1 + 1], S.verts[3 * i1 + 2]) - a;
+    const float3 e2 = mk(S.verts[3 * i2], S.verts[3 * i2 + 1], S.verts[3 * i2 + 2]) - a;
+    if (!S.tri_uv) {
+        dpdu = e1;
+        dpdv = e2;
+        return true;
+    }
+    const float* t = S.tri_uv + 6 * (size_t)prim;
+    const float du1 = t[2] - t[0], dv1 = t[3] - t[1], du2 = t[4] - t[0], dv2 = t[5] - t[1];
+    const float det = du1 * dv2 - dv1 * du2;
+    if (det == 0.0f) return false;
+    const float inv = 1.0f / det;
+    dpdu = inv * (dv2 * e1 - dv1 * e2);
+    dpdv = inv * (du1 * e2 - du2 * e1);
+    return true;
+}
+
+// IntersectionContext::setScreenSpaceDifferentialsI (intersection_context.cpp:295-324) for both
+// differential rays: each meets the tangent plane of the hit (shading normal, hit point); dPoint
+// is the offset of that point, dUv solves dPoint = dPdU du + dPdV dv on the two axes other than the
+// plane's major axis (Cramer's rule); a ray parallel to the plane, or a degenerate
+// parametrisation, leaves a zero footprint
+__device__ inline void hit_footprint(const DScene& S, HitContext& H, uint32_t prim, float3 oi, float3 di, float3 oj,
+                                     float3 dj) {
+    float3 n_out = H.N;
+    if (prim >= S.n_tris) {
+        const float4 sp = S.spheres[prim - S.n_tris];
+        n_out = normal(H.target - mk(sp.x, sp.y, sp.z));
+    }
+    float3 dpdu, dpdv;
+    if (!hit_dpduv(S, prim, n_out, dpdu, dpdv)) return;
+    const float3 N = H.N, P = H.target;
+    const float ax = fabsf(N.x), ay = fabsf(N.y), az = fabsf(N.z);
+    const int major = ax >= ay ? (ax >= az ? 0 : 2) : (ay >= az ? 1 : 2);
+    const int a = (major + 1) % 3, b = (major + 2) % 3;
+    auto comp = [](float3 v, int i) { return i == 0 ? v.x : (i == 1 ? v.y : v.z); };
+    const float m00 = comp(dpdu, a), m01 = comp(dpdv, a), m10 = comp(dpdu, b), m11 = comp(dpdv, b);
+    const float det = m00 * m11 - m01 * m10;
+    float fp2 = 0.0f;
+    for (int side = 0; side < 2; ++side) {
+        const float3 o = side ? oj : oi, d = side ? dj : di;
+        const float nd = dot(N, d);
+        if (nd == 0.0f) continue;
+        const float t = dot(N, P - o) / nd;
+        if (!(t >= 0.0f)) continue;
+        const float3 dp = (o + t * d) - P;
+        fp2 = fmaxf(fp2, dot(dp, dp));
+        if (det == 0.0f) continue;
+        const float ra = comp(dp, a), rb = comp(dp, b);
+        const float du = (ra * m11 - m01 * rb) / det, dv = (m00 * rb - ra * m10) / det;
+        if (side) {
+            H.du_j = du;
+            H.dv_j = dv;
+        } else {
+            H.du_i = du;
+            H.dv_i = dv;
+        }
+    }
+    H.fp2 = fp2;
+}
+
+// the footprint of a camera hit: the camera's differential rays for key k (the camera vertex only;
+// rays past it carry none, as the reference's DifferentialRay(BoundedRay) does)
+__device__ inline void camera_footprint(const DScene& S, HitContext& H, uint32_t prim, const liar_camera& C,
+                                        const SampleKey& k, int width, int height) {
+    float3 oi, di, oj, dj;
+    camera_differentials(C, k, width, height, oi, di, oj, dj);
+    hit_footprint(S, H, prim, oi, di, oj, dj);
 }
 
 // ---- the film (output/raster.cpp:547-606, output/filter_triangle.cpp, output/filter_mitchell.cpp)

@@ -230,23 +230,23 @@ class _Builder:
         rec = CTexture()
         rec.a = rec.b = rec.spectrum = -1
         if isinstance(t, tx.CheckerBoard):
-            tx.warn_point_lookup(t)
             rec.type = TEX_CHECKER
             rec.p[0], rec.p[1] = t.split
+            rec.p[2] = 1.0 if t.antiAliasing == tx.CheckerBoard.AA_BILINEAR else 0.0
         elif isinstance(t, tx.GridBoard):
             rec.type = TEX_GRID
             rec.p[0], rec.p[1] = t.thickness[0] / 2, t.thickness[1] / 2  # GridBoard's halfThickness
         elif isinstance(t, tx.Image):
-            t.warn_if_filtered()
+            if t.xyz is None:
+                raise ValueError("Image texture has no pixels (loadFile first)")
             h, w = t.xyz.shape[:2]
             rec.type = TEX_IMAGE
             rec.a, rec.b = w, h
-            rec.p[0] = 0.0 if t.antiAliasing == "none" else 1.0
+            rec.p[0] = {"none": 0.0, "bilinear": 1.0, "trilinear": 2.0}[t.antiAliasing]
             rec.pixels = self.n_tex_pixels
-            px = np.zeros((h * w, 4), np.float32)
-            px[:, :3] = t.xyz.reshape(-1, 3)
-            self.tex_pixels.append(px)
-            self.n_tex_pixels += h * w
+            block = tx.image_pool_block(t)
+            self.tex_pixels.append(block)
+            self.n_tex_pixels += block.shape[0]
         elif isinstance(t, tx.Perlin):
             rec.type = TEX_NOISE
             rec.p[0] = float(t.numOctaves) if isinstance(t, tx.FBm) else 0.0

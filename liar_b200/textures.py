@@ -10,6 +10,8 @@ from __future__ import annotations
 
 import warnings
 
+import math
+
 import numpy as np
 
 from .spectra import Spectrum
@@ -54,17 +56,16 @@ class UnaryOperator(Texture):
 
 class CheckerBoard(BinaryOperator):
     """CheckerBoard(a, b): a where the fractional u and v lie on the same side of ``split``
-    (default (0.5, 0.5)), else b (checker_board.cpp:113-157).
+    (default (0.5, 0.5)), else b (checker_board.cpp:113-207).
 
     antiAliasing "none" is the reference's point lookup. "bilinear" (the reference's default)
-    averages the board over the pixel footprint that ray differentials give; the GPU path carries
-    no ray differentials, so it renders "bilinear" as "none", the footprint's zero-size limit: the
-    pixel filter then does the averaging over the camera samples."""
+    blends a and b by a's share of the pixel footprint that the camera's ray differentials give
+    (CheckerBoard::integrate); hits without differentials (past the camera vertex) look up the
+    point."""
 
     AA_NONE = "none"
     AA_BILINEAR = "bilinear"
     _default_aa = "bilinear"
-    _warned = False
 
     def __init__(self, a, b):
         super().__init__(a, b)
@@ -152,21 +153,91 @@ class TransformationUv(UnaryOperator):
         self._matrix = as_matrix2d(value)
 
 
+def _mip_compress(level: np.ndarray, axis: int, new_size: int) -> np.ndarray:
+    """Image::makeMipMap (image.cpp:428-560): one level halved along axis (1 = x, 0 = y) of an
+    (h, w, 4) float32 level. An even size averages pairs; an odd size 2 n + 1 weighs three
+    neighbours (n - k, n, k + 1) / (2 n + 1). Along x the weights are those of the reference's
+    vectorised build (the default, LIAR_HAVE_AVX), which multiplies the middle pixel by itself
+    instead of by its weight (image.cpp:528-531); along y it uses the weight. A zero size keeps
+    the parent."""
+    old = level.shape[axis]
+    if new_size == 0 or level.shape[1 - axis] == 0:
+        return level
+    a = np.moveaxis(level, axis, 0)
+    if 2 * new_size == old:
+        out = (a[0::2] + a[1::2]) * np.float32(0.5)
+    else:
+        if 2 * new_size + 1 != old:
+            raise ValueError("mip level sizes must halve")
+        scale = np.float32(1.0) / np.float32(old)
+        k = np.arange(new_size, dtype=np.float32)
+        w0 = (scale * (np.float32(new_size) - k))[:, None, None]
+        w1 = scale * np.float32(new_size)
+        w2 = (scale * (k + np.float32(1)))[:, None, None]
+        p0, p1, p2 = a[0:2 * new_size:2], a[1:2 * new_size:2], a[2:2 * new_size + 1:2]
+        mid = p1 * p1 if axis == 1 else w1 * p1
+        out = (w0 * p0 + mid) + w2 * p2
+    return np.ascontiguousarray(np.moveaxis(out.astype(np.float32), 0, axis))
+
+
+def mip_levels(pixels: np.ndarray, mode: str) -> tuple[int, int, list]:
+    """Image::makeMipMaps (image.cpp:365-425): (levels along u, levels along v, [levels]) of an
+    (h, w, 4) image, level (iu, iv) at index iv * levels_u + iu. "none": the image alone;
+    "isotropic": floor(log2(max(w, h))) + 1 levels, each halving x then y; "anisotropic":
+    (floor(log2 w) + 1) x (floor(log2 h) + 1) levels, row iv the image halved iv times along y and
+    then iu times along x."""
+    h, w = pixels.shape[:2]
+    base = np.ascontiguousarray(pixels, dtype=np.float32)
+    if mode == Image.MM_NONE:
+        return 1, 1, [base]
+    if mode == Image.MM_ISOTROPIC:
+        n = int(math.floor(math.log2(max(w, h)))) + 1
+        levels = [base]
+        for i in range(1, n):
+            tmp = _mip_compress(levels[-1], 1, w >> i)
+            levels.append(_mip_compress(tmp, 0, h >> i))
+        return n, 1, levels
+    nu, nv = int(math.floor(math.log2(w))) + 1, int(math.floor(math.log2(h))) + 1
+    levels = [base]
+    for j in range(nv):
+        if j > 0:
+            levels.append(_mip_compress(levels[(j - 1) * nu], 0, h >> j))
+        for i in range(1, nu):
+            levels.append(_mip_compress(levels[-1], 1, w >> i))
+    return nu, nv, levels
+
+
+def image_pool_block(t) -> np.ndarray:
+    """The texture_pixels block of an image texture (include/liar_gpu.h, LIAR_TEX_IMAGE): the mip
+    table's header {levels u, levels v, mip mode, 0} and one entry {offset low 31 bits, offset
+    high bits, width, height} per level, as int32 bits in float32, then every level's pixels."""
+    px = np.zeros(t.xyz.shape[:2] + (4,), np.float32)
+    px[..., :3] = t.xyz
+    nu, nv, levels = mip_levels(px, t.mipMapping)
+    head = np.zeros((1 + nu * nv, 4), np.int32)
+    head[0] = (nu, nv, {Image.MM_NONE: 0, Image.MM_ISOTROPIC: 1, Image.MM_ANISOTROPIC: 2}[t.mipMapping], 0)
+    off = 1 + nu * nv
+    for k, lv in enumerate(levels):
+        head[1 + k] = (off & 0x7FFFFFFF, off >> 31, lv.shape[1], lv.shape[0])
+        off += lv.shape[0] * lv.shape[1]
+    return np.concatenate([head.view(np.float32)] + [lv.reshape(-1, 4) for lv in levels])
+
+
 class Image(Texture):
     """Image(path[, antiAliasing, mipMapping][, rgbSpace]) (textures/image.cpp): the picture read
     as XYZ (codecs.read) and looked up at (u, 1 - v) with wrap-around; its colour becomes a
     spectrum through the standard recovery (Spectral::fromXYZ).
 
-    antiAliasing "none" takes the nearest pixel, "bilinear" blends the four around. "trilinear"
-    (the reference's default) and mip-mapping blend mip levels chosen by the ray differentials'
-    footprint, which this path does not carry: with a zero footprint the reference's lookup is the
-    bilinear one at level 0 (image.cpp:279-356, mipMapLevel), which is what is rendered."""
+    antiAliasing "none" takes the nearest pixel, "bilinear" blends the four around, "trilinear"
+    (the reference's default) blends bilinear lookups of the two mip levels around the level that
+    the camera's ray differentials' footprint picks (mipMapping "anisotropic", the default, per
+    axis; "isotropic" by the larger; "none" always the image itself). Hits without differentials
+    (past the camera vertex) look up level 0."""
 
     AA_NONE, AA_BILINEAR, AA_TRILINEAR = "none", "bilinear", "trilinear"
     MM_NONE, MM_ISOTROPIC, MM_ANISOTROPIC = "none", "isotropic", "anisotropic"
     _default_aa = "trilinear"
     _default_mm = "anisotropic"
-    _warned = False
 
     def __init__(self, path=None, *args):
         aa, mm, space = Image._default_aa, Image._default_mm, None
@@ -192,9 +263,9 @@ class Image(Texture):
         self.xyz = np.ascontiguousarray(xyza[..., :3], dtype=np.float32)
 
     @classmethod
-    def from_xyz(cls, xyz, antiAliasing="bilinear"):
+    def from_xyz(cls, xyz, antiAliasing="bilinear", mipMapping="none"):
         """An image texture of XYZ pixels (H, W, 3), row 0 at the top."""
-        t = cls(None, antiAliasing, "none")
+        t = cls(None, antiAliasing, mipMapping)
         t.xyz = np.ascontiguousarray(np.asarray(xyz, dtype=np.float32).reshape(*np.shape(xyz)[:2], 3))
         return t
 
@@ -231,14 +302,6 @@ class Image(Texture):
     @staticmethod
     def setDefaultMipMapping(mode):
         Image._default_mm = str(mode).lower()
-
-    def warn_if_filtered(self):
-        if self.xyz is None:
-            raise ValueError("Image texture has no pixels (loadFile first)")
-        if self._aa == self.AA_TRILINEAR and not Image._warned:
-            Image._warned = True
-            warnings.warn("Image antiAliasing 'trilinear' is rendered as 'bilinear' at mip level 0 "
-                          "(no ray differentials on the GPU path)", stacklevel=4)
 
 
 _U32, _U64 = 0xFFFFFFFF, 0xFFFFFFFFFFFFFFFF
@@ -433,13 +496,6 @@ def flat_value(t) -> float | None:
 
 def is_uv_texture(x) -> bool:
     return isinstance(x, (CheckerBoard, GridBoard, TransformationUv, Image, Perlin, Abs, Product, Sum))
-
-
-def warn_point_lookup(tex: CheckerBoard):
-    if tex.antiAliasing == CheckerBoard.AA_BILINEAR and not CheckerBoard._warned:
-        CheckerBoard._warned = True
-        warnings.warn("CheckerBoard antiAliasing 'bilinear' is rendered as 'none' (no ray differentials on the GPU path)",
-                      stacklevel=3)
 
 
 def as_spectrum(x) -> Spectrum:

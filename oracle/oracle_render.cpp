@@ -695,6 +695,8 @@ struct Ctx {
     bool leaving;
     int obj, light, mi;
     float uv_u, uv_v;
+    // the screen-space footprint (dUv_dI, dUv_dJ, max |dPoint|^2): zero without ray differentials
+    float du_i = 0, dv_i = 0, du_j = 0, dv_j = 0, fp2 = 0;
 };
 
 // IntersectionContext::uv of a triangle hit (TriangleMesh::doLocalContext, triangle_mesh.cpp:334-356):
@@ -773,29 +775,136 @@ float rec_eval(const RecView& R, const int32_t idx[3], const float w[3], float l
     return reflectant && mx > 1.0f ? v / mx : v;
 }
 
-// Image::lookUp at mip level 0 (textures/image.cpp:598-609 nearest, 690-713 bilinear): (u, 1 - v)
-// over the pixels with wrap-around; indices clamped where rounding lands on the far edge
-void image_lookup(const Scene& S, const Texture& T, float u, float v, float out[3]) {
-    const int nx = T.a, ny = T.b;
-    const float* px = S.in.texture_pixels + 4 * T.pixels;
-    if (T.p[0] == 0.0f) {
-        int x0 = (int)std::floor(frac(u) * (float)nx), y0 = (int)std::floor(frac(1.0f - v) * (float)ny);
-        x0 = std::min(std::max(x0, 0), nx - 1);
-        y0 = std::min(std::max(y0, 0), ny - 1);
-        for (int c = 0; c < 3; ++c) out[c] = px[4 * ((size_t)y0 * nx + x0) + c];
-        return;
+// the point a texture is looked up at: (u, v), its screen-space derivatives, the squared surface
+// footprint and the hit point
+struct TexPoint {
+    float u, v, du_i, dv_i, du_j, dv_j, fp2;
+    V x;
+};
+TexPoint tp(const Ctx& c) { return TexPoint{c.uv_u, c.uv_v, c.du_i, c.dv_i, c.du_j, c.dv_j, c.fp2, c.target}; }
+
+// Image::mipMapLevel (image.cpp:580-612): level maxLevel + log2(width), the fraction from the
+// significand
+void mip_level(float width, int n_levels, int& l0, int& l1, float& frac_) {
+    const int max_level = n_levels - 1;
+    const float w = std::max(width, 1e-9f);
+    int32_t i;
+    std::memcpy(&i, &w, 4);
+    const int level = max_level + ((i >> 23) - 127);
+    if (level < 0) {
+        l0 = l1 = 0;
+        frac_ = 0;
+    } else if (level >= max_level) {
+        l0 = l1 = max_level;
+        frac_ = 0;
+    } else {
+        l0 = level;
+        l1 = level + 1;
+        const int32_t mi = (127 << 23) | (i & 0x7fffff);
+        float m;
+        std::memcpy(&m, &mi, 4);
+        frac_ = m - 1.0f;
     }
-    float x = u * (float)nx - 0.5f, y = (1.0f - v) * (float)ny - 0.5f;
-    x -= std::floor(x / (float)nx) * (float)nx;
-    y -= std::floor(y / (float)ny) * (float)ny;
+}
+
+// level (iu, iv) of an image's mip table at texture_pixels[T.pixels] (include/liar_gpu.h)
+struct MipLevel {
+    const float* px;
+    int w, h;
+};
+MipLevel mip_get(const Scene& S, const Texture& T, int n_u, int iu, int iv) {
+    const float* base = S.in.texture_pixels + 4 * T.pixels;
+    int32_t e[4];
+    std::memcpy(e, base + 4 * (1 + iv * n_u + iu), sizeof(e));
+    const uint64_t off = ((uint64_t)(uint32_t)e[1] << 31) | (uint64_t)(uint32_t)e[0];
+    return MipLevel{base + 4 * off, e[2], e[3]};
+}
+
+// Image::nearest (image.cpp:618-631) and Image::bilinear (image.cpp:636-690, the vectorised
+// build): (u, 1 - v) with wrap-around
+void image_nearest(const MipLevel& m, float u, float v, float out[3]) {
+    int x0 = (int)std::floor(frac(u) * (float)m.w), y0 = (int)std::floor(frac(1.0f - v) * (float)m.h);
+    x0 = std::min(std::max(x0, 0), m.w - 1);
+    y0 = std::min(std::max(y0, 0), m.h - 1);
+    for (int c = 0; c < 3; ++c) out[c] = m.px[4 * ((size_t)y0 * m.w + x0) + c];
+}
+void image_bilinear(const MipLevel& m, float u, float v, float out[3]) {
+    const float x = frac(u) * (float)m.w - 0.5f, y = frac(1.0f - v) * (float)m.h - 0.5f;
     const float x0 = std::floor(x), y0 = std::floor(y), dx = x - x0, dy = y - y0;
-    const int i0 = std::min(std::max((int)x0, 0), nx - 1), j0 = std::min(std::max((int)y0, 0), ny - 1);
-    const int i1 = (i0 + 1) % nx, j1 = (j0 + 1) % ny;
+    int i0 = (int)x0, j0 = (int)y0;
+    if (i0 < 0) i0 += m.w;
+    if (j0 < 0) j0 += m.h;
+    i0 = std::min(std::max(i0, 0), m.w - 1);
+    j0 = std::min(std::max(j0, 0), m.h - 1);
+    const int i1 = i0 + 1 < m.w ? i0 + 1 : 0, j1 = j0 + 1 < m.h ? j0 + 1 : 0;
     for (int c = 0; c < 3; ++c) {
-        const float p00 = px[4 * ((size_t)j0 * nx + i0) + c], p10 = px[4 * ((size_t)j0 * nx + i1) + c];
-        const float p01 = px[4 * ((size_t)j1 * nx + i0) + c], p11 = px[4 * ((size_t)j1 * nx + i1) + c];
-        out[c] = (p00 * (1 - dx) + p10 * dx) * (1 - dy) + (p01 * (1 - dx) + p11 * dx) * dy;
+        const float p00 = m.px[4 * ((size_t)j0 * m.w + i0) + c], p10 = m.px[4 * ((size_t)j0 * m.w + i1) + c];
+        const float p01 = m.px[4 * ((size_t)j1 * m.w + i0) + c], p11 = m.px[4 * ((size_t)j1 * m.w + i1) + c];
+        const float a = (1 - dx) * p00 + dx * p10, b = (1 - dx) * p01 + dx * p11;
+        out[c] = (1 - dy) * a + dy * b;
     }
+}
+
+// Image::lookUp (image.cpp:249-330): levels from the footprint, then nearest, bilinear, or
+// trilinear across the levels
+void image_lookup(const Scene& S, const Texture& T, const TexPoint& q, float out[3]) {
+    int32_t hdr[4];
+    std::memcpy(hdr, S.in.texture_pixels + 4 * T.pixels, sizeof(hdr));
+    const int n_u = hdr[0], n_v = hdr[1], mip = hdr[2];
+    int u0 = 0, u1 = 0, v0 = 0, v1 = 0;
+    float fu = 0, fv = 0;
+    const float wu = std::max(std::fabs(q.du_i), std::fabs(q.du_j)), wv = std::max(std::fabs(q.dv_i), std::fabs(q.dv_j));
+    if (mip == 1) {
+        mip_level(std::max(wu, wv), n_u, u0, u1, fu);
+    } else if (mip == 2) {
+        mip_level(wu, n_u, u0, u1, fu);
+        mip_level(wv, n_v, v0, v1, fv);
+    }
+    const int aa = (int)T.p[0];
+    if (aa == 0) return image_nearest(mip_get(S, T, n_u, u0, v0), q.u, q.v, out);
+    if (aa == 1) return image_bilinear(mip_get(S, T, n_u, u0, v0), q.u, q.v, out);
+    float p00[3], p10[3];
+    image_bilinear(mip_get(S, T, n_u, u0, v0), q.u, q.v, p00);
+    image_bilinear(mip_get(S, T, n_u, u1, v0), q.u, q.v, p10);
+    for (int c = 0; c < 3; ++c) out[c] = (1 - fu) * p00[c] + fu * p10[c];
+    if (v0 != v1) {
+        float p01[3], p11[3];
+        image_bilinear(mip_get(S, T, n_u, u0, v1), q.u, q.v, p01);
+        image_bilinear(mip_get(S, T, n_u, u1, v1), q.u, q.v, p11);
+        for (int c = 0; c < 3; ++c) out[c] = (1 - fv) * out[c] + fv * ((1 - fu) * p01[c] + fu * p11[c]);
+    }
+}
+
+// CheckerBoard::weightA and ::integrate (checker_board.cpp:149-207): the share of A over the
+// footprint's (u, v) box with bilinear anti-aliasing, else (or for an empty box) the point rule
+float checker_weight(const Texture& T, const TexPoint& q) {
+    const float sx = T.p[0], sy = T.p[1];
+    const float fu = frac(q.u), fv = frac(q.v);
+    const float point = (fu < sx) == (fv < sy) ? 1.0f : 0.0f;
+    if (T.p[2] == 0.0f) return point;
+    const float du = std::max(std::fabs(q.du_i), std::fabs(q.du_j)), dv = std::max(std::fabs(q.dv_i), std::fabs(q.dv_j));
+    const float area = du * dv;
+    if (!(area > 0.0f)) return point;
+    const float mn[2] = {fu - du / 2, fv - dv / 2}, mx[2] = {fu + du / 2, fv + dv / 2};
+    const float split[2] = {sx, sy};
+    float d0[2], cmin[2][2], cmax[2][2];  // cmin[axis] = (min(d, split), max(d - split, 0)) of the low corner
+    for (int k = 0; k < 2; ++k) {
+        const float a0 = std::floor(mn[k]), b0 = std::floor(mx[k]);
+        d0[k] = b0 - a0;
+        const float dmn = mn[k] - a0, dmx = mx[k] - b0;
+        cmin[k][0] = std::min(dmn, split[k]);
+        cmin[k][1] = std::max(dmn - split[k], 0.0f);
+        cmax[k][0] = std::min(dmx, split[k]);
+        cmax[k][1] = std::max(dmx - split[k], 0.0f);
+    }
+    const float oneU[2] = {sx, 1 - sx}, oneV[2] = {sy, 1 - sy};
+    auto dot2 = [](const float* a, const float* b) { return a[0] * b[0] + a[1] * b[1]; };
+    float r = (sx * sy + (1 - sx) * (1 - sy)) * d0[0] * d0[1];
+    r += (dot2(oneU, cmax[1]) - dot2(oneU, cmin[1])) * d0[0];
+    r += (dot2(cmax[0], oneV) - dot2(cmin[0], oneV)) * d0[1];
+    r += dot2(cmax[0], cmax[1]) - dot2(cmax[0], cmin[1]);
+    r += dot2(cmin[0], cmin[1]) - dot2(cmin[0], cmax[1]);
+    return std::min(std::max(r / area, 0.0f), 1.0f);
 }
 
 // Texture::lookUp of the uv textures (src/liar/textures/): TransformationUv moves the context's uv
@@ -843,54 +952,71 @@ float perlin_noise(const uint8_t* tab, V q) {
                 sz);
 }
 
-float noise_texture(const Scene& S, const Texture& T, V x) {
+// FBm::doScalarLookUp (fbm.cpp:76-101): 1 - log2(footprint^2) / 2 octaves clamped to [1, octaves],
+// the last one's fraction blended in; Perlin when p[0] = 0
+float noise_texture(const Scene& S, const Texture& T, const TexPoint& q) {
     const uint8_t* tab = S.in.noise_tables + T.pixels;
     const int octaves = (int)T.p[0];
-    if (octaves <= 0) return perlin_noise(tab, x);
+    if (octaves <= 0) return perlin_noise(tab, q.x);
+    const float ideal = 1.0f - std::log2(q.fp2) / 2.0f;
+    const float real = std::min(std::max(ideal, 1.0f), (float)octaves);
+    const int n = (int)std::floor(real);
     float result = 0, freq = 1, weight = 1;
-    for (int k = 0; k < octaves; ++k) {
-        result += weight * perlin_noise(tab, freq * x);
+    for (int k = 0; k < n; ++k) {
+        result += weight * perlin_noise(tab, freq * q.x);
         freq *= 2;
         weight *= T.p[1];
     }
+    const float fr = real - (float)n;
+    if (fr > 0) result += fr * weight * perlin_noise(tab, freq * q.x);
     return result;
 }
 
 // Abs (abs.cpp:26-35) looks its input up as the caller does; Product / Sum of one texture with
 // constants (product.cpp:90-99, sum.cpp:90-105) as illuminants, the result clamped as a
 // reflectance; applied to the value found below them
-float texture_rec(const Scene& S, int t, float u, float v, V x, float lam, bool reflectant, int depth);
-
-float texture(const Scene& S, int t, float u, float v, V x, float lam, bool reflectant) {
-    return texture_rec(S, t, u, v, x, lam, reflectant, 0);
-}
-
-float texture_rec(const Scene& S, int t, float u, float v, V x, float lam, bool reflectant, int depth0) {
-    for (int depth = depth0; depth < 32; ++depth) {
+float texture_rec(const Scene& S, int t, TexPoint q, float lam, bool reflectant, int depth0) {
+    for (int depth = depth0; depth < 64; ++depth) {
         const Texture& T = S.in.textures[t];
         if (T.type == 1) {
-            t = ((frac(u) < T.p[0]) == (frac(v) < T.p[1])) ? T.a : T.b;
+            const float wa = checker_weight(T, q);
+            if (wa >= 1) {
+                t = T.a;
+            } else if (wa <= 0) {
+                t = T.b;
+            } else {
+                // Spectral(wA A + (1 - wA) B, type) of the two looked up as illuminants
+                const float va = texture_rec(S, T.a, q, lam, false, depth + 1);
+                const float vb = texture_rec(S, T.b, q, lam, false, depth + 1);
+                const float r = wa * va + (1 - wa) * vb;
+                return reflectant ? std::min(r, 1.0f) : r;
+            }
         } else if (T.type == 2) {
-            const float fu = frac(u), fv = frac(v);
+            const float fu = frac(q.u), fv = frac(q.v);
             t = (fu < T.p[0] || fv < T.p[0] || fu > 1 - T.p[0] || fv > 1 - T.p[1]) ? T.a : T.b;
         } else if (T.type == 3) {
-            const float nu = T.p[0] * u + T.p[1] * v + T.p[2];
-            const float nv = T.p[3] * u + T.p[4] * v + T.p[5];
-            u = nu;
-            v = nv;
+            // TransformationUv (transformation_uv.cpp:67-70): (u, v) and its derivatives
+            TexPoint n = q;
+            n.u = T.p[0] * q.u + T.p[1] * q.v + T.p[2];
+            n.v = T.p[3] * q.u + T.p[4] * q.v + T.p[5];
+            n.du_i = T.p[0] * q.du_i + T.p[1] * q.dv_i;
+            n.dv_i = T.p[3] * q.du_i + T.p[4] * q.dv_i;
+            n.du_j = T.p[0] * q.du_j + T.p[1] * q.dv_j;
+            n.dv_j = T.p[3] * q.du_j + T.p[4] * q.dv_j;
+            q = n;
             t = T.a;
         } else if (T.type == 5) {
-            const float n = noise_texture(S, T, x);
+            const float n = noise_texture(S, T, q);
             return reflectant ? std::min(n, 1.0f) : n;
         } else if (T.type == 6) {
-            return std::fabs(texture_rec(S, T.a, u, v, x, lam, reflectant, depth + 1));
+            return std::fabs(texture_rec(S, T.a, q, lam, reflectant, depth + 1));
         } else if (T.type == 7) {
-            const float r = T.p[0] * texture_rec(S, T.a, u, v, x, lam, false, depth + 1) + T.p[1];
+            const float r = T.p[0] * texture_rec(S, T.a, q, lam, false, depth + 1) + T.p[1];
             return reflectant ? std::min(r, 1.0f) : r;
         } else if (T.type == 4) {
             // Image::doLookUp: Spectral::fromXYZ of the colour
             float c[3];
-            image_lookup(S, T, u, v, c);
+            image_lookup(S, T, q, c);
             int32_t idx[3];
             float w[3];
             if (!rec_locate(S.rec, c[0], c[1], c[2], idx, w)) return 0;
@@ -902,8 +1028,8 @@ float texture_rec(const Scene& S, int t, float u, float v, V x, float lam, bool 
     return 0;
 }
 
-float param(const Scene& S, const Material& M, int k, float u, float v, V x, float lam, bool reflectant) {
-    return M.tex[k] >= 0 ? texture(S, M.tex[k], u, v, x, lam, reflectant) : spectrum(S, M.spec[k], lam, reflectant);
+float param(const Scene& S, const Material& M, int k, const TexPoint& q, float lam, bool reflectant) {
+    return M.tex[k] >= 0 ? texture_rec(S, M.tex[k], q, lam, reflectant, 0) : spectrum(S, M.spec[k], lam, reflectant);
 }
 Ctx hit_ctx(const Scene& S, V o, V d, const Hit& h) {
     Ctx c;
@@ -992,48 +1118,162 @@ Bsdf make_bsdf(const Scene& S, const Material& M, const Ctx& c, float lam) {
     switch (M.type) {
         case M_LAMBERT:
             B.caps = C_REFL | C_DIFF;
-            B.r = param(S, M, 0, c.uv_u, c.uv_v, c.target, lam, true);
+            B.r = param(S, M, 0, tp(c), lam, true);
             break;
         case M_CONDUCTOR:
         case M_CT:
             B.caps = M.type == M_CONDUCTOR ? (C_REFL | C_SPEC) : (C_REFL | C_GLOSSY);
-            B.eta = std::max(param(S, M, 0, c.uv_u, c.uv_v, c.target, lam, false), 1e-9f);
-            B.kappa = std::max(param(S, M, 1, c.uv_u, c.uv_v, c.target, lam, false), 1e-9f);
-            B.r = param(S, M, 2, c.uv_u, c.uv_v, c.target, lam, true);
+            B.eta = std::max(param(S, M, 0, tp(c), lam, false), 1e-9f);
+            B.kappa = std::max(param(S, M, 1, tp(c), lam, false), 1e-9f);
+            B.r = param(S, M, 2, tp(c), lam, true);
             break;
         case M_DIELECTRIC: {
             B.caps = C_REFL | C_TRANS | C_SPEC;
-            const float i1 = std::max(param(S, M, 1, c.uv_u, c.uv_v, c.target, lam, false), 1e-9f);
-            const float i2 = std::max(param(S, M, 0, c.uv_u, c.uv_v, c.target, lam, false), 1e-9f);
+            const float i1 = std::max(param(S, M, 1, tp(c), lam, false), 1e-9f);
+            const float i2 = std::max(param(S, M, 0, tp(c), lam, false), 1e-9f);
             B.ior = c.leaving ? i2 / i1 : i1 / i2;
-            B.r = param(S, M, 2, c.uv_u, c.uv_v, c.target, lam, true);
-            B.t = param(S, M, 3, c.uv_u, c.uv_v, c.target, lam, true);
+            B.r = param(S, M, 2, tp(c), lam, true);
+            B.t = param(S, M, 3, tp(c), lam, true);
             break;
         }
         case M_WALTER: {
             B.caps = C_TRANS | C_GLOSSY;
-            float ei = std::max(param(S, M, 1, c.uv_u, c.uv_v, c.target, lam, false), 1e-9f);
-            float et = std::max(param(S, M, 0, c.uv_u, c.uv_v, c.target, lam, false), 1e-9f);
+            float ei = std::max(param(S, M, 1, tp(c), lam, false), 1e-9f);
+            float et = std::max(param(S, M, 0, tp(c), lam, false), 1e-9f);
             if (c.leaving) std::swap(ei, et);
             B.etaI = ei;
             B.etaT = et;
-            B.r = param(S, M, 2, c.uv_u, c.uv_v, c.target, lam, true);
-            B.t = param(S, M, 3, c.uv_u, c.uv_v, c.target, lam, true);
+            B.r = param(S, M, 2, tp(c), lam, true);
+            B.t = param(S, M, 3, tp(c), lam, true);
             break;
         }
         case M_MIRROR:
             B.caps = C_REFL | C_SPEC;
-            B.r = param(S, M, 0, c.uv_u, c.uv_v, c.target, lam, true);
+            B.r = param(S, M, 0, tp(c), lam, true);
             break;
     }
     return B;
+}
+
+// PerspectiveCamera::doGenerateRay (perspective_camera.cpp:406-434) at screen point (sx, sy) and
+// lens sample (lu, lv)
+void camera_at(const Camera& C, float sx, float sy, float lu, float lv, V& pos, V& dir, float& factor) {
+    pos = V{C.position[0], C.position[1], C.position[2]};
+    dir = V{C.direction[0], C.direction[1], C.direction[2]} + (sx - 0.5f) * V{C.right[0], C.right[1], C.right[2]} +
+          (sy - 0.5f) * V{C.down[0], C.down[1], C.down[2]};
+    dir = unit(dir);
+    const V dn{C.direction_normal[0], C.direction_normal[1], C.direction_normal[2]};
+    factor = 1 / dot(dir, dn);
+    if (C.lens_radius > 0 && C.focus_distance > 0 && C.focus_distance < 3.4e38f) {
+        float lx, ly;
+        concentric(lu, lv, lx, ly);
+        const V lp = pos + (C.lens_radius * lx) * V{C.right_normal[0], C.right_normal[1], C.right_normal[2]} +
+                     (C.lens_radius * ly) * V{C.down_normal[0], C.down_normal[1], C.down_normal[2]};
+        const V fp = pos + (factor * C.focus_distance) * dir;
+        pos = lp;
+        dir = unit(fp - lp);
+        factor = 1 / dot(dir, dn);
+    }
+}
+
+void camera_samples(const RenderIn& R, const Sampler& smp, float& sx, float& sy, float& lu, float& lv) {
+    const uint32_t ix = smp.pixel % (uint32_t)R.width, iy = smp.pixel / (uint32_t)R.width;
+    float jx, jy;
+    smp.get2(D_SCREEN, jx, jy);
+    sx = ((float)ix + jx) / (float)R.width;
+    sy = ((float)iy + jy) / (float)R.height;
+    smp.get2(D_LENS, lu, lv);
+}
+
+// dPoint/du and dPoint/dv of the hit's parametrisation (corner uvs, else the barycentrics; a
+// sphere's spherical angles, sphere.cpp:150-172)
+bool hit_dpduv(const Scene& S, uint32_t prim, V n_out, V& dpdu, V& dpdv) {
+    if (prim >= S.in.n_triangles) {
+        const float r = S.in.spheres[4 * (prim - S.in.n_triangles) + 3];
+        const float pi = 3.14159265358979323846f;
+        const float theta = std::acos(std::min(std::max(n_out.z, -1.0f), 1.0f));
+        const float st = std::sin(theta);
+        dpdu = (r * 2.0f * pi) * V{-n_out.y, n_out.x, 0.0f};
+        if (st != 0.0f) {
+            const float cs = n_out.z / st;
+            dpdv = (r * pi) * V{cs * n_out.x, cs * n_out.y, -st};
+        } else {
+            const float phi = std::atan2(n_out.y, n_out.x);
+            dpdv = (r * pi) * V{std::cos(phi), std::sin(phi), 0.0f};
+        }
+        return true;
+    }
+    const uint32_t* tr = S.in.triangles + 3 * (size_t)prim;
+    const float* pa = S.in.vertices + 3 * tr[0];
+    const float* pb = S.in.vertices + 3 * tr[1];
+    const float* pc = S.in.vertices + 3 * tr[2];
+    const V A{pa[0], pa[1], pa[2]};
+    const V e1 = V{pb[0], pb[1], pb[2]} - A, e2 = V{pc[0], pc[1], pc[2]} - A;
+    if (!S.in.triangle_uvs) {
+        dpdu = e1;
+        dpdv = e2;
+        return true;
+    }
+    const float* t = S.in.triangle_uvs + 6 * (size_t)prim;
+    const float du1 = t[2] - t[0], dv1 = t[3] - t[1], du2 = t[4] - t[0], dv2 = t[5] - t[1];
+    const float det = du1 * dv2 - dv1 * du2;
+    if (det == 0.0f) return false;
+    const float inv = 1.0f / det;
+    dpdu = inv * (dv2 * e1 - dv1 * e2);
+    dpdv = inv * (du1 * e2 - du2 * e1);
+    return true;
+}
+
+// IntersectionContext::setScreenSpaceDifferentialsI (intersection_context.cpp:295-324) for the
+// camera's two differential rays (Camera::primaryRay, camera.cpp:53-60: the screen point moved by
+// 1 / (resolution sqrt(spp)), render_engine.cpp:211-215): where each meets the tangent plane, and
+// the (u, v) step of that offset on the plane's two minor axes (Cramer's rule)
+void camera_footprint(const Scene& S, const RenderIn& R, const Sampler& smp, uint32_t prim, Ctx& c) {
+    float sx, sy, lu, lv, f;
+    camera_samples(R, smp, sx, sy, lu, lv);
+    const float root = std::sqrt((float)smp.spp);
+    const float dsx = 1.0f / ((float)R.width * root), dsy = 1.0f / ((float)R.height * root);
+    V oi, di, oj, dj;
+    camera_at(R.camera, sx + dsx, sy, lu, lv, oi, di, f);
+    camera_at(R.camera, sx, sy + dsy, lu, lv, oj, dj, f);
+    V n_out = c.N;
+    if (prim >= S.in.n_triangles) {
+        const float* sp = S.in.spheres + 4 * (prim - S.in.n_triangles);
+        n_out = unit(c.target - V{sp[0], sp[1], sp[2]});
+    }
+    V dpdu, dpdv;
+    if (!hit_dpduv(S, prim, n_out, dpdu, dpdv)) return;
+    const V N = c.N, P = c.target;
+    const float ax = std::fabs(N.x), ay = std::fabs(N.y), az = std::fabs(N.z);
+    const int major = ax >= ay ? (ax >= az ? 0 : 2) : (ay >= az ? 1 : 2);
+    const int a = (major + 1) % 3, b = (major + 2) % 3;
+    auto comp = [](V v, int i) { return i == 0 ? v.x : (i == 1 ? v.y : v.z); };
+    const float m00 = comp(dpdu, a), m01 = comp(dpdv, a), m10 = comp(dpdu, b), m11 = comp(dpdv, b);
+    const float det = m00 * m11 - m01 * m10;
+    float fp2 = 0;
+    for (int side = 0; side < 2; ++side) {
+        const V o = side ? oj : oi, d = side ? dj : di;
+        const float nd = dot(N, d);
+        if (nd == 0.0f) continue;
+        const float t = dot(N, P - o) / nd;
+        if (!(t >= 0.0f)) continue;
+        const V dp = (o + t * d) - P;
+        fp2 = std::max(fp2, dot(dp, dp));
+        if (det == 0.0f) continue;
+        const float ra = comp(dp, a), rb = comp(dp, b);
+        const float du = (ra * m11 - m01 * rb) / det, dv = (m00 * rb - ra * m10) / det;
+        (side ? c.du_j : c.du_i) = du;
+        (side ? c.dv_j : c.dv_i) = dv;
+    }
+    c.fp2 = fp2;
 }
 
 // AdjointPhotonTracer::shadeSurface + scatterSurface for the hit `h` of ray (o, d)
 float shade_surface(Path& P, V o, V d, float tmin, float tmax, const Hit& h, int gen) {
     const Scene& S = *P.S;
     float result = 0;
-    const Ctx c = hit_ctx(S, o, d, h);
+    Ctx c = hit_ctx(S, o, d, h);
+    if (gen == 0 && S.in.n_textures > 0) camera_footprint(S, *P.R, P.smp, (uint32_t)h.prim, c);  // the camera vertex
     const int light = c.light, mi = c.mi;
     const V target = c.target, ng = c.ng, N = c.N, u = c.u, v = c.v;
     if (gen > 0 && light >= 0) result += spectrum(S, S.in.lights[light].spectrum, P.lam, false);
@@ -1481,7 +1721,8 @@ float dl_cast(DLPath& P, V o, V d, float tmin, float tmax, int gen, bool hq, uin
         return 0;
     }
     if (gen == 0) P.alpha = 1;
-    const Ctx c = hit_ctx(S, o, d, h);
+    Ctx c = hit_ctx(S, o, d, h);
+    if (gen == 0 && S.in.n_textures > 0) camera_footprint(S, R, P.smp, (uint32_t)h.prim, c);  // the camera vertex
     if (c.mi < 0) return dl_cast(P, o, d, h.t + TOL, tmax, gen + 1, hq, dl_child_key(key, 0));
     const Material& M = S.in.materials[c.mi];
     if (P.pm && P.pm->visualize) return pm_irradiance(P, c);
@@ -1736,38 +1977,38 @@ static void trace_photon_rec(const Scene& S, const PhotonIn& D, const Sampler& s
     switch (M.type) {
         case M_LAMBERT:
             B.caps = C_REFL | C_DIFF;
-            B.r = param(S, M, 0, uv_u, uv_v, hit, lam, true);
+            B.r = param(S, M, 0, TexPoint{uv_u, uv_v, 0, 0, 0, 0, 0, hit}, lam, true);
             break;
         case M_CONDUCTOR:
         case M_CT:
             B.caps = M.type == M_CONDUCTOR ? (C_REFL | C_SPEC) : (C_REFL | C_GLOSSY);
-            B.eta = std::max(param(S, M, 0, uv_u, uv_v, hit, lam, false), 1e-9f);
-            B.kappa = std::max(param(S, M, 1, uv_u, uv_v, hit, lam, false), 1e-9f);
-            B.r = param(S, M, 2, uv_u, uv_v, hit, lam, true);
+            B.eta = std::max(param(S, M, 0, TexPoint{uv_u, uv_v, 0, 0, 0, 0, 0, hit}, lam, false), 1e-9f);
+            B.kappa = std::max(param(S, M, 1, TexPoint{uv_u, uv_v, 0, 0, 0, 0, 0, hit}, lam, false), 1e-9f);
+            B.r = param(S, M, 2, TexPoint{uv_u, uv_v, 0, 0, 0, 0, 0, hit}, lam, true);
             break;
         case M_DIELECTRIC: {
             B.caps = C_REFL | C_TRANS | C_SPEC;
-            const float i1 = std::max(param(S, M, 1, uv_u, uv_v, hit, lam, false), 1e-9f);
-            const float i2 = std::max(param(S, M, 0, uv_u, uv_v, hit, lam, false), 1e-9f);
+            const float i1 = std::max(param(S, M, 1, TexPoint{uv_u, uv_v, 0, 0, 0, 0, 0, hit}, lam, false), 1e-9f);
+            const float i2 = std::max(param(S, M, 0, TexPoint{uv_u, uv_v, 0, 0, 0, 0, 0, hit}, lam, false), 1e-9f);
             B.ior = leaving ? i2 / i1 : i1 / i2;
-            B.r = param(S, M, 2, uv_u, uv_v, hit, lam, true);
-            B.t = param(S, M, 3, uv_u, uv_v, hit, lam, true);
+            B.r = param(S, M, 2, TexPoint{uv_u, uv_v, 0, 0, 0, 0, 0, hit}, lam, true);
+            B.t = param(S, M, 3, TexPoint{uv_u, uv_v, 0, 0, 0, 0, 0, hit}, lam, true);
             break;
         }
         case M_WALTER: {
             B.caps = C_TRANS | C_GLOSSY;
-            float ei = std::max(param(S, M, 1, uv_u, uv_v, hit, lam, false), 1e-9f);
-            float et = std::max(param(S, M, 0, uv_u, uv_v, hit, lam, false), 1e-9f);
+            float ei = std::max(param(S, M, 1, TexPoint{uv_u, uv_v, 0, 0, 0, 0, 0, hit}, lam, false), 1e-9f);
+            float et = std::max(param(S, M, 0, TexPoint{uv_u, uv_v, 0, 0, 0, 0, 0, hit}, lam, false), 1e-9f);
             if (leaving) std::swap(ei, et);
             B.etaI = ei;
             B.etaT = et;
-            B.r = param(S, M, 2, uv_u, uv_v, hit, lam, true);
-            B.t = param(S, M, 3, uv_u, uv_v, hit, lam, true);
+            B.r = param(S, M, 2, TexPoint{uv_u, uv_v, 0, 0, 0, 0, 0, hit}, lam, true);
+            B.t = param(S, M, 3, TexPoint{uv_u, uv_v, 0, 0, 0, 0, 0, hit}, lam, true);
             break;
         }
         case M_MIRROR:
             B.caps = C_REFL | C_SPEC;
-            B.r = param(S, M, 0, uv_u, uv_v, hit, lam, true);
+            B.r = param(S, M, 0, TexPoint{uv_u, uv_v, 0, 0, 0, 0, 0, hit}, lam, true);
             break;
     }
     const V md = -d;
@@ -1988,29 +2229,13 @@ int render_body(void* s, const RenderIn* R, const PmIn* pm, float* film, int64_t
                 const uint32_t ix = (uint32_t)(px % R->width), iy = (uint32_t)(px / R->width);
                 float jx, jy;
                 P.smp.get2(D_SCREEN, jx, jy);
-                const float sx = ((float)ix + jx) / (float)R->width;
-                const float sy = ((float)iy + jy) / (float)R->height;
                 float lpdf;
                 P.lam = observer_sample(S, P.smp.get(D_LAMBDA, true), lpdf);
                 const Camera& C = R->camera;
-                V pos{C.position[0], C.position[1], C.position[2]};
-                V dir = V{C.direction[0], C.direction[1], C.direction[2]} +
-                        (sx - 0.5f) * V{C.right[0], C.right[1], C.right[2]} + (sy - 0.5f) * V{C.down[0], C.down[1], C.down[2]};
-                dir = unit(dir);
-                const V dn{C.direction_normal[0], C.direction_normal[1], C.direction_normal[2]};
-                float factor = 1 / dot(dir, dn);
-                if (C.lens_radius > 0 && C.focus_distance > 0 && C.focus_distance < 3.4e38f) {
-                    float lx, ly;
-                    float lu, lv;
-                    P.smp.get2(D_LENS, lu, lv);
-                    concentric(lu, lv, lx, ly);
-                    const V lp = pos + (C.lens_radius * lx) * V{C.right_normal[0], C.right_normal[1], C.right_normal[2]} +
-                                 (C.lens_radius * ly) * V{C.down_normal[0], C.down_normal[1], C.down_normal[2]};
-                    const V fp = pos + (factor * C.focus_distance) * dir;
-                    pos = lp;
-                    dir = unit(fp - lp);
-                    factor = 1 / dot(dir, dn);
-                }
+                float sx, sy, lu, lv, factor;
+                camera_samples(*R, P.smp, sx, sy, lu, lv);
+                V pos, dir;
+                camera_at(C, sx, sy, lu, lv, pos, dir, factor);
                 float L;
                 if (R->tracer == 1 || R->tracer == 2) {
                     DLPath D{&S, R, P.smp, P.lam};

@@ -75,10 +75,8 @@ def test_shape_uvs():
 def test_mirroring_transformation_rewinds_uvs_with_the_triangles():
     p = scenery.Parallelogram((0, 0, 0), (1, 0, 0), (0, 1, 0))
     p.shader = shaders.Lambert(tx.CheckerBoard(0.1, 0.9))
-    with pytest.warns(UserWarning, match="bilinear"):
-        tx.CheckerBoard._warned = False
-        m = scenery.Transformation(p, [[-1, 0, 0, 0], [0, 1, 0, 0], [0, 0, 1, 0], [0, 0, 0, 1]])
-        flat = R.flatten(m)
+    m = scenery.Transformation(p, [[-1, 0, 0, 0], [0, 1, 0, 0], [0, 0, 1, 0], [0, 0, 0, 1]])
+    flat = R.flatten(m)
     uv = flat.triangle_uvs.reshape(-1, 3, 2)
     np.testing.assert_array_equal(uv, p.corner_uvs()[:, [0, 2, 1]])
     assert (flat.triangles == np.array([[0, 2, 1], [0, 3, 2]])).all()
@@ -167,22 +165,28 @@ def test_image_texture_is_flattened_into_the_pixel_pool(tmp_path):
     T = list(flat.textures)
     ia = T[flat.materials[0].tex[0]]
     ib = T[T[flat.materials[1].tex[0]].a]
+    # each image: its mip table (a header and one entry per level; from_xyz has no mip levels),
+    # then the pixels
     assert (ia.type, ia.a, ia.b, ia.pixels, ia.p[0]) == (R.TEX_IMAGE, 3, 2, 0, 0.0)
-    assert (ib.type, ib.a, ib.b, ib.pixels, ib.p[0]) == (R.TEX_IMAGE, 1, 2, 6, 1.0)
-    assert flat.texture_pixels.shape == (8, 4)
-    np.testing.assert_array_equal(flat.texture_pixels[:6, 1], np.float32([0.2, 0.4, 0.3, 0.6, 0.8, 0.5]))
+    assert (ib.type, ib.a, ib.b, ib.pixels, ib.p[0]) == (R.TEX_IMAGE, 1, 2, 8, 1.0)
+    assert flat.texture_pixels.shape == (12, 4)
+    head = flat.texture_pixels[:2].view(np.int32)
+    assert list(head[0]) == [1, 1, 0, 0] and list(head[1]) == [2, 0, 3, 2]
+    np.testing.assert_array_equal(flat.texture_pixels[2:8, 1], np.float32([0.2, 0.4, 0.3, 0.6, 0.8, 0.5]))
     # a file is read in its codec's colour space
     img = output.Image(str(tmp_path / "t.pfm"), (3, 2))
     img.exposureStops = 0.0
     xyza = np.concatenate([_grey_xyz([[0.2, 0.4, 0.3], [0.6, 0.8, 0.5]]), np.ones((2, 3, 1), np.float32)], -1)
     img.write(xyza, None)
     t = tx.Image(str(tmp_path / "t.pfm"))
-    assert t.resolution == (3, 2) and t.antiAliasing == "trilinear" and t.rgbSpace.gamma == 1.0
+    assert t.resolution == (3, 2) and t.antiAliasing == "trilinear" and t.mipMapping == "anisotropic"
+    assert t.rgbSpace.gamma == 1.0
     np.testing.assert_allclose(t.xyz, xyza[..., :3], rtol=1e-5, atol=1e-6)
-    with pytest.warns(UserWarning, match="trilinear"):
-        tx.Image._warned = False
-        p.shader = shaders.Lambert(t)
-        R.flatten(p)
+    p.shader = shaders.Lambert(t)
+    f2 = R.flatten(p)
+    # anisotropic levels of a 3 x 2 image: 2 along u (3, 1 wide) x 2 along v (2, 1 high)
+    assert f2.textures[f2.materials[0].tex[0]].p[0] == 2.0
+    assert list(f2.texture_pixels[:1].view(np.int32)[0]) == [2, 2, 2, 0]
 
 
 @pytest.mark.parametrize("filter", ["none", "bilinear"])
@@ -305,3 +309,65 @@ def test_pcg_extension_table_advances_like_an_inside_out_generator():
     g._advance_table()
     st = (tx._rxs_m_xs_32_inverse(before[0]) * tx._PCG_MUL32 + tx._PCG_INC32 + 2) & 0xFFFFFFFF
     assert g.table[0] == tx._rxs_m_xs_32(st)
+
+
+def test_mip_levels_follow_the_references_construction():
+    """Image::makeMipMaps (image.cpp:365-560): even sizes average pairs; odd sizes 2n+1 weigh three
+    neighbours by (n - k, n, k + 1) / (2n + 1), except that the vectorised build (the reference's
+    default) multiplies the middle pixel along x by itself; anisotropic tables halve y per row and x
+    per column, isotropic levels halve both."""
+    rng = np.random.default_rng(4)
+    img = rng.uniform(0.1, 0.9, size=(6, 5, 4)).astype(np.float32)
+    nu, nv, lv = tx.mip_levels(img, "anisotropic")
+    assert (nu, nv, len(lv)) == (3, 3, 9)
+    assert [x.shape[:2] for x in lv[:3]] == [(6, 5), (6, 2), (6, 1)]
+    assert [x.shape[:2] for x in lv[3::3]] == [(3, 5), (1, 5)]
+    # x: 5 -> 2 (odd): w0 = (2 - k) / 5, middle squared, w2 = (k + 1) / 5
+    w = np.float32(1) / np.float32(5)
+    k0 = (w * np.float32(2)) * img[:, 0] + img[:, 1] * img[:, 1] + (w * np.float32(1)) * img[:, 2]
+    np.testing.assert_allclose(lv[1][:, 0], k0, rtol=1e-6)
+    # y: 6 -> 3 (even): pairs averaged
+    np.testing.assert_allclose(lv[3][1], (img[2] + img[3]) * np.float32(0.5), rtol=1e-6)
+    # y: 3 -> 1 (odd): the middle row weighed by 1/3
+    w3 = np.float32(1) / np.float32(3)
+    np.testing.assert_allclose(lv[6][0], (w3 * lv[3][0] + w3 * lv[3][1]) + w3 * lv[3][2], rtol=1e-6)
+    nu, nv, lv = tx.mip_levels(img, "isotropic")
+    assert (nu, nv) == (3, 1) and [x.shape[:2] for x in lv] == [(6, 5), (3, 2), (1, 1)]
+    assert tx.mip_levels(img, "none")[:2] == (1, 1)
+
+
+def test_oracle_checker_board_anti_aliasing_averages_the_footprint():
+    """A board of many checkers per pixel: with bilinear anti-aliasing each camera hit sees the
+    share of A over its footprint (CheckerBoard::integrate), so the pixels are near the average of
+    A and B and vary far less than with point lookups ("none")."""
+    res = {}
+    for aa in ("none", "bilinear"):
+        board = tx.CheckerBoard(0.9, 0.1)
+        board.antiAliasing = aa
+        tex = tx.TransformationUv(board, [[200, 0, 0], [0, 200, 0], [0, 0, 1]])
+        scene, cam = _board_scene(tex)
+        t = tracers.DirectLighting()
+        t.maxRayGeneration = 1
+        img, _ = R.resolve(oracle.RenderScene(R.flatten(scene)).render(R.render_desc(cam, 24, 24, 16, t, seed=5)))
+        res[aa] = img[..., 1]
+    assert abs(res["bilinear"].mean() - 0.5) < 0.05
+    assert res["bilinear"].std() < 0.5 * res["none"].std()
+
+
+def test_oracle_fbm_octaves_follow_the_footprint():
+    """FBm keeps every octave where the footprint is zero (past the camera vertex) and fewer at a
+    camera hit whose footprint is wide: the camera image of a distant FBm plane is smoother than
+    the same texture looked up without a footprint."""
+    from liar_b200 import cameras
+    plane = scenery.Parallelogram((-50, 0, -50), (100, 0, 0), (0, 0, 100))
+    plane.shader = shaders.Lambert(tx.Sum(tx.Product(tx.FBm(8, 0.5), 0.3), 0.5))
+    cam = cameras.PerspectiveCamera()
+    cam.position = (0, 30, -40)
+    cam.sky = (0, 1, 0)
+    cam.lookAt((0, 0, 0))
+    scene = scenery.List([plane, scenery.LightSky(tx.Constant(1.0))])
+    flat = R.flatten(scene)
+    t = tracers.DirectLighting()
+    t.maxRayGeneration = 1
+    img, _ = R.resolve(oracle.RenderScene(flat).render(R.render_desc(cam, 32, 32, 1, t, seed=2)))
+    assert np.isfinite(img).all() and img[..., 1].mean() > 0.1

@@ -157,3 +157,69 @@ def test_upload_refuses_bad_texture_trees():
     p.shader = shaders.Lambert(deep)
     with pytest.raises(LiarGpuError):
         _upload(R.flatten(p))
+
+
+def _filtered_scene():
+    """The reference's default filtering: CheckerBoard with bilinear anti-aliasing, Image with
+    trilinear lookups over anisotropic (and, on a second panel, isotropic) mip levels, FBm whose
+    octaves follow the footprint; a receding floor so that footprints grow across the image, and
+    a thin-lens camera, whose differential rays start at the lens sample."""
+    fine = tx.CheckerBoard(tx.Constant(0.9), tx.Constant(0.1))     # antiAliasing: the default, bilinear
+    floor = scenery.Parallelogram((-3, 0, -2), (6, 0, 0), (0, 0, 30))
+    floor.shader = shaders.Lambert(tx.TransformationUv(fine, [[12, 0, 0], [0, 60, 0], [0, 0, 1]]))
+    rng = np.random.default_rng(3)
+    pix = rng.uniform(0.05, 0.9, size=(37, 53, 3)).astype(np.float32)   # odd sizes: odd mip reductions
+    aniso = tx.Image.from_xyz(sRGB.linearSpace().toXYZlinear(pix), antiAliasing="trilinear", mipMapping="anisotropic")
+    back = scenery.Parallelogram((-3, 0, 6), (6, 0, 0), (0, 3, 0))
+    back.shader = shaders.Lambert(tx.TransformationUv(aniso, [[6, 0, 0], [0, 2, 0], [0, 0, 1]]))
+    iso = tx.Image.from_xyz(sRGB.linearSpace().toXYZlinear(pix[:16, :16]), antiAliasing="trilinear",
+                            mipMapping="isotropic")
+    side = scenery.Parallelogram((2.9, 0, -1), (0, 0, 8), (0, 2.5, 0))
+    side.shader = shaders.Lambert(tx.TransformationUv(iso, [[5, 0, 0], [0, 3, 0], [0, 0, 1]]))
+    ball = scenery.Sphere((-1.0, 0.7, 1.5), 0.7)
+    ball.shader = shaders.Lambert(tx.Sum(0.25, tx.Product(0.5, tx.Abs(tx.FBm(8, 0.6)))))
+    sky = scenery.LightSky(tx.Constant(0.7))
+    lamp = scenery.LightArea(scenery.Parallelogram((-0.5, 3.5, 0.5), (1, 0, 0), (0, 0, 1)))
+    lamp.radiance = spectra.BlackBody(5000, 10)
+    cam = cameras.PerspectiveCamera()
+    cam.position = (0, 1.2, -2.5)
+    cam.lookAt((0, 0.6, 2.0))
+    cam.lensRadius = 0.02
+    cam.focusDistance = 4.0
+    return scenery.List([floor, back, side, ball, sky, lamp]), cam
+
+
+@pytest.mark.parametrize("kind", ["path", "direct"])
+def test_filtered_textures_match_oracle(kind):
+    scene, cam = _filtered_scene()
+    flat = R.flatten(scene)
+    assert flat.textures[flat.materials[0].tex[0]].type == R.TEX_UV_TRANSFORM
+    gs = R.GpuScene(default_context(), flat)
+    t = tracers.AdjointPhotonTracer() if kind == "path" else tracers.DirectLighting()
+    t.maxRayGeneration = 3
+    d = R.render_desc(cam, 64, 48, 9, t, seed=8)
+    g = gs.render(d)
+    c = oracle.RenderScene(flat).render(d)
+    mg, _ = _within_3_sigma(g, c)
+    # far down the floor the checkers are averaged: the top rows of the floor are near grey
+    assert mg[..., 1].mean() > 0.05
+    gs.close()
+
+
+def test_filtered_textures_batch_matches_single_render():
+    scene, cam = _filtered_scene()
+    gs = R.GpuScene(default_context(), R.flatten(scene))
+    t = tracers.AdjointPhotonTracer()
+    t.maxRayGeneration = 3
+    t.maxDepth = 8
+    d = R.render_desc(cam, 40, 30, 4, t, seed=2)
+    film = torch.zeros((d.height, d.width, 8), dtype=torch.float32, device="cuda:0")
+    gs.render_device(d, film.data_ptr())
+    br = B.BatchRenderer(default_context(), [(gs, d)], B.make_config(hero=1))
+    br.launch()
+    torch.cuda.synchronize()
+    a, b = br.films[0].cpu().numpy(), film.cpu().numpy()
+    scale = max(float(np.abs(b[..., :7]).max()), 1e-6)
+    np.testing.assert_allclose(a[..., :7], b[..., :7], rtol=2e-5, atol=2e-6 * scale)
+    br.close()
+    gs.close()
