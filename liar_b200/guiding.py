@@ -95,6 +95,13 @@ class Guide:
                                                                 _ptr(out), _stream(stream)))
         return out
 
+    def train_device(self, records, apply: bool = True, loss=None, stream=None) -> None:
+        """One training step over records ((n, 13) float32 cuda tensor) queued on `stream`, without a
+        synchronize; the batch's loss is written to `loss` (a one-element cuda tensor) when given."""
+        self.ctx.check(self.ctx._lib.liar_gpu_guide_train_device(
+            self.ctx.handle, self.handle, _ptr(records), records.shape[0], int(apply), C.c_void_p(0),
+            C.c_void_p(_ptr(loss) if loss is not None else 0), _stream(stream)))
+
     def train_step(self, records, apply: bool = True, want_grad: bool = False, stream=None):
         """records: (n, 13) float32 cuda tensor. Returns (loss, gradient or None) after a synchronize."""
         import torch
