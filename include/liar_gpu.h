@@ -303,7 +303,9 @@ typedef struct liar_photon_mapper_desc {
     int32_t final_gather_rays;      /* numFinalGatherRays, used with traced direct light (0 = no final gather) */
     int32_t secondary_gather_rays;  /* numSecondaryGatherRays: 0 = the reference's 1, -1 = none */
     float ratio_precomputed_irradiance; /* ratioPrecomputedIrradiance: 0 = the reference's 0.25, < 0 = none */
-    int32_t reserved;
+    float caustics_quality;         /* causticsQuality (photon_mapper.cpp:165-175, 1455-1462): 0 = the
+                                       reference's 1, < 0 = 0 (no caustic photons); the storage
+                                       probabilities of liar_photon_desc */
 } liar_photon_mapper_desc;
 
 typedef struct liar_render_desc {
@@ -503,7 +505,11 @@ typedef struct liar_photon_desc {
     uint64_t max_emitted;        /* maxNumberOfPhotons */
     uint64_t wave;               /* photons emitted per wave, 0 = automatic */
     int32_t final_gather;        /* 1: every diffuse hit goes to the global map (hasFinalGather) */
-    int32_t reserved;
+    /* causticsQuality q (0 = the reference's 1, < 0 = 0): a diffuse hit enters the global map with
+     * probability 1 / max(q, 1) and the caustic map with probability q / max(q, 1), by Russian
+     * roulette (photon_mapper.cpp:733-745, 1455-1462); a stored photon keeps its power, and the maps
+     * are scaled by the inverse probabilities when they are built */
+    float caustics_quality;
 } liar_photon_desc;
 typedef struct liar_photon_buffers {  /* device arrays of `capacity` photons */
     float* position;   /* x 3 */

@@ -232,8 +232,13 @@ int build_maps(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_render
     pd.wave = std::min<uint64_t>(std::max<uint64_t>(2 * target, 1u << 14), 1u << 21);
     const bool fg = D.ray_trace_direct >= 0 && D.final_gather_rays > 0;  // hasFinalGather
     pd.final_gather = fg ? 1 : 0;
+    pd.caustics_quality = D.caustics_quality;
+    float p_store[2];  // storage probabilities of the global and caustic maps
+    storage_probabilities(D.caustics_quality, p_store[kPmGlobal], p_store[kPmCaustic]);
+    // a global map filled at probability p takes about 1 / p more emissions (and their caustics)
+    const uint64_t more = (uint64_t)std::ceil(1.0 / std::max(p_store[kPmGlobal], 1e-6f));
     Traced T;
-    int rc = trace(ctx, scene, pd, (target + pd.wave) * 4, st, T);
+    int rc = trace(ctx, scene, pd, (target * more + pd.wave) * 4, st, T);
     if (rc) return rc;
     // the reference's buffer order: by emission, then by bounce (the generation is in tag >> 8)
     std::vector<uint32_t> order(T.stored);
@@ -287,7 +292,7 @@ int build_maps(liar_gpu_ctx* ctx, const liar_gpu_scene* scene, const liar_render
             for (int c = 0; c < 3; ++c) {
                 host[3 * j + c] = T.position[3 * i + c];
                 host[3 * n + 3 * j + c] = T.omega[3 * i + c];
-                host[6 * n + 3 * j + c] = T.power[3 * i + c] * scale;
+                host[6 * n + 3 * j + c] = T.power[3 * i + c] * (scale / p_store[m]);  // russianRoulette's power / p
             }
         }
         float radius = D.estimation_radius[m];

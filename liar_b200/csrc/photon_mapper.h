@@ -11,6 +11,15 @@ namespace liar_gpu {
 
 enum PmMapKind { kPmGlobal = 0, kPmCaustic = 1 };
 
+// PhotonMapper's storage probabilities (photon_mapper.cpp:1455-1462) of causticsQuality q (0: the
+// reference's 1, negative: 0): the global map 1 / max(q, 1), the caustic map q / max(q, 1)
+inline void storage_probabilities(float quality, float& p_global, float& p_caustic) {
+    const float q = quality == 0.0f ? 1.0f : (quality > 0.0f ? quality : 0.0f);
+    const float m = q > 1.0f ? q : 1.0f;
+    p_global = 1.0f / m;
+    p_caustic = q / m;
+}
+
 // one photon map on the device: the photons in the reference's buffer order (emission, then
 // bounce), their power scaled by 1 / photons emitted, and each power's spectral blend
 struct PmMap {

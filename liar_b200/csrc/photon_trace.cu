@@ -12,11 +12,14 @@
 // round-off can re-hit the surface it just left.
 #include <cuda_runtime.h>
 
+#include <cmath>
+
 #include <algorithm>
 #include <new>
 
 #include "../../include/liar_gpu.h"
 #include "ctx.h"
+#include "photon_mapper.h"
 #include "render_dev.cuh"
 
 using namespace liar_gpu;
@@ -33,7 +36,10 @@ int scene_device(const liar_gpu_scene* s);
 namespace {
 
 // photon sample dimensions (plain hashes: the photon sampler is not stratified per pixel)
-enum : uint32_t { P_LIGHT = 0, P_A = 1, P_B = 3, P_LAMBDA = 5, P_GEN0 = 8, P_PER_GEN = 8, P_BSDF = 0, P_COMP = 2, P_RR = 3 };
+enum : uint32_t {
+    P_LIGHT = 0, P_A = 1, P_B = 3, P_LAMBDA = 5, P_GEN0 = 8, P_PER_GEN = 8, P_BSDF = 0, P_COMP = 2, P_RR = 3,
+    P_STORE_CAUSTIC = 4, P_STORE_GLOBAL = 5
+};
 
 struct PState {
     float* lam;
@@ -54,7 +60,9 @@ struct PParams {
     int max_gen;
     int rt_direct;
     int final_gather;  // every diffuse hit is a global photon
+    float p_global, p_caustic;  // storage probabilities (causticsQuality)
 };
+
 
 __device__ __forceinline__ float psample(const PParams& P, uint64_t path, uint32_t dim) {
     SampleKey k;
@@ -171,9 +179,13 @@ __global__ void __launch_bounds__(128) k_photon_shade(DScene S, PParams P, PStat
             } else {
                 const liar_material M = S.mats[mi];
                 if (M.type == LIAR_MAT_LAMBERT) {
-                    // Shader::hasCaps(diffuse): store (photon_mapper.cpp:733-748)
-                    const bool to_caustic = caustic;
-                    const bool to_global = ((gen > 0 || !P.rt_direct) && !caustic) || P.final_gather;
+                    // Shader::hasCaps(diffuse): store (photon_mapper.cpp:733-748), each map by Russian
+                    // roulette with its storage probability (kept when u <= p)
+                    const uint32_t sbase = P_GEN0 + P_PER_GEN * (uint32_t)gen;
+                    const bool to_caustic =
+                        caustic && (P.p_caustic >= 1.0f || !(psample(P, path, sbase + P_STORE_CAUSTIC) > P.p_caustic));
+                    const bool to_global = (((gen > 0 || !P.rt_direct) && !caustic) || P.final_gather) &&
+                                           (P.p_global >= 1.0f || !(psample(P, path, sbase + P_STORE_GLOBAL) > P.p_global));
                     if (to_caustic || to_global) {
                         const unsigned long long s = atomicAdd(counters + 0, 1ull);
                         if (s < B.capacity) {
@@ -333,6 +345,8 @@ extern "C" int liar_gpu_photon_trace(liar_gpu_ctx* ctx, const liar_gpu_scene* sc
     P.max_gen = desc->max_ray_generation;
     P.rt_direct = desc->ray_traced_direct;
     P.final_gather = desc->final_gather ? 1 : 0;
+    if (!std::isfinite(desc->caustics_quality)) return ctx_fail(ctx, LIAR_ERR_INVALID, "caustics quality is not finite");
+    storage_probabilities(desc->caustics_quality, P.p_global, P.p_caustic);
     uint64_t emitted = 0;
     counts->stored = counts->global = counts->caustic = 0;
     while (emitted < desc->max_emitted && counts->global < desc->global_target) {

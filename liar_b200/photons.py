@@ -83,7 +83,7 @@ class PhotonMap:
 class PhotonDesc(C.Structure):
     _fields_ = [("max_ray_generation", C.c_int32), ("ray_traced_direct", C.c_int32), ("seed", C.c_uint64),
                 ("global_target", C.c_uint64), ("max_emitted", C.c_uint64), ("wave", C.c_uint64),
-                ("final_gather", C.c_int32), ("reserved", C.c_int32)]
+                ("final_gather", C.c_int32), ("caustics_quality", C.c_float)]
 
 
 class PhotonBuffers(C.Structure):
@@ -99,8 +99,14 @@ GLOBAL, CAUSTIC = 1, 2
 
 
 def photon_desc(global_target: int, max_emitted: int = 100_000_000, max_ray_generation: int = 8, seed: int = 0,
-                wave: int = 0, ray_traced_direct: bool = True, final_gather: bool = False) -> PhotonDesc:
+                wave: int = 0, ray_traced_direct: bool = True, final_gather: bool = False,
+                caustics_quality: float = 1.0) -> PhotonDesc:
+    """liar_photon_desc; caustics_quality is PhotonMapper.causticsQuality (storage probabilities
+    1 / max(q, 1) for the global map and q / max(q, 1) for the caustic map; stored powers are not
+    divided by them)."""
     d = PhotonDesc()
+    q = max(float(caustics_quality), 0.0)
+    d.caustics_quality = q if q > 0.0 else -1.0
     d.max_ray_generation = int(max_ray_generation)
     d.ray_traced_direct = int(bool(ray_traced_direct))
     d.seed = int(seed)

@@ -69,7 +69,7 @@ class CPhotonMapperDesc(C.Structure):
                 ("estimation_radius", C.c_float * 2), ("estimation_tolerance", C.c_float * 2),
                 ("estimation_size", C.c_int32 * 2), ("ray_trace_direct", C.c_int32), ("visualize", C.c_int32),
                 ("final_gather_rays", C.c_int32), ("secondary_gather_rays", C.c_int32),
-                ("ratio_precomputed_irradiance", C.c_float), ("reserved", C.c_int32)]
+                ("ratio_precomputed_irradiance", C.c_float), ("caustics_quality", C.c_float)]
 
 
 class CRenderDesc(C.Structure):
@@ -557,9 +557,9 @@ def render_desc(camera, width: int, height: int, spp: int, tracer, seed: int = 0
     r.secondary_light_samples = int(getattr(tracer, "numberOfSecondaryLightSamples", 1))
     r.trace_glossy = 1 if getattr(tracer, "traceGlossy", True) else -1
     if r.tracer == 2:
-        if float(getattr(tracer, "causticsQuality", 1.0)) != 1.0:
-            raise NotImplementedError("PhotonMapper causticsQuality other than 1 is not on the GPU path")
         pm = r.photon_mapper
+        q = max(float(getattr(tracer, "causticsQuality", 1.0)), 0.0)   # setCausticsQuality clamps at 0
+        pm.caustics_quality = q if q > 0.0 else -1.0
         pm.max_photons = int(tracer.maxNumberOfPhotons)
         pm.global_map_size = int(tracer.globalMapSize)
         for m in range(2):

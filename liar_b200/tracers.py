@@ -36,8 +36,9 @@ class PhotonMapper(DirectLighting):
     BSDF-sampled rays, evaluated at their hits from the precomputed irradiance map
     (ratioPrecomputedIrradiance of the global photons), with numSecondaryGatherRays more rays where a
     hit lies closer than the estimation radius. Defaults as the reference's
-    (photon_mapper.cpp:108-142). Volumetric maps and causticsQuality other than 1 (its storage
-    probabilities) are not on the GPU path."""
+    (photon_mapper.cpp:108-142); causticsQuality sets the storage probabilities of the two maps
+    (1 / max(q, 1) global, q / max(q, 1) caustic, :1455-1462). Volumetric maps are not on the GPU
+    path (participating media are out of scope)."""
     kind = 2
     MAP_TYPES = {"global": 0, "caustic": 1, "caustics": 1}
 

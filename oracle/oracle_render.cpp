@@ -115,7 +115,7 @@ struct RenderIn {
     int32_t pm_size[2], pm_ray_trace_direct, pm_visualize;
     int32_t pm_final_gather_rays, pm_secondary_gather_rays;
     float pm_ratio_precomputed_irradiance;
-    int32_t pm_reserved;
+    float pm_caustics_quality;
     int32_t sampler;  // LIAR_SAMPLER_* bits
 };
 
@@ -1915,7 +1915,8 @@ uint64_t oracle_mix64(uint64_t z) { return mix64(z); }
 struct PhotonIn {
     int32_t max_ray_generation, ray_traced_direct;
     uint64_t seed, global_target, max_emitted, wave;
-    int32_t final_gather, reserved;
+    int32_t final_gather;
+    float caustics_quality;
 };
 static_assert(sizeof(PhotonIn) == sizeof(liar_photon_desc), "oracle mirror out of step with include/liar_gpu.h");
 struct PhotonRec {
@@ -1940,9 +1941,16 @@ static void trace_photon_rec(const Scene& S, const PhotonIn& D, const Sampler& s
     if (S.in.materials[mi].type == M_NONE) return;  // a shader without a BSDF absorbs the photon
     const Material& M = S.in.materials[mi];
     if (M.type == M_LAMBERT) {
-        const bool to_caustic = caustic;
+        // storage by Russian roulette with the maps' probabilities (photon_mapper.cpp:733-745,
+        // 1455-1462): 1 / max(q, 1) global, q / max(q, 1) caustic; the power stays, the map builder
+        // divides by the probability
+        const float q = D.caustics_quality == 0 ? 1.0f : std::max(D.caustics_quality, 0.0f);
+        const float pg = 1.0f / std::max(q, 1.0f), pc = q / std::max(q, 1.0f);
+        const uint32_t sbase = 8 + 8 * (uint32_t)gen;
+        const bool to_caustic = caustic && (pc >= 1 || !(smp.get(sbase + 4, false) > pc));
         // photon_mapper.cpp:742: with final gathering every diffuse hit is a global photon
-        const bool to_global = ((gen > 0 || !D.ray_traced_direct) && !caustic) || D.final_gather;
+        const bool to_global = (((gen > 0 || !D.ray_traced_direct) && !caustic) || D.final_gather) &&
+                               (pg >= 1 || !(smp.get(sbase + 5, false) > pg));
         if (to_caustic || to_global) {
             PhotonRec r;
             r.pos[0] = hit.x;

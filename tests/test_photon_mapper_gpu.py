@@ -194,12 +194,24 @@ def test_final_gathering_agrees_with_path_tracing_on_average():
     assert abs(ya / yb - 1) < 0.1, (ya, yb)
 
 
+def test_caustics_quality_matches_oracle():
+    """causticsQuality 4: the global map is filled at storage probability 1/4 (four times the
+    emissions), every caustic photon is kept, and the maps' powers are divided by their
+    probabilities; the render agrees with the oracle over the same maps, and its global map is the
+    requested size."""
+    t = _pm(global_size=8_000)
+    t.causticsQuality = 4.0
+    g, c, st, maps = _run(t, w=32, h=32, spp=4, seed=6)
+    _close(g, c)
+    assert st["global"] == 8_000
+    t1 = _pm(global_size=8_000)
+    _, _, st1, _ = _run(t1, w=8, h=8, spp=1, seed=6)
+    assert st["emitted"] > 2.5 * st1["emitted"]
+    assert st["caustic"] > 2.0 * st1["caustic"]
+
+
 def test_unsupported_settings_fail_loudly():
-    t = _pm()
-    t.causticsQuality = 2.0
     scene, cam = _scene()
-    with pytest.raises(NotImplementedError):
-        R.render_desc(cam, 8, 8, 1, t)
     t = _pm()
     t.setEstimationSize("caustic", 100)
     gs = R.GpuScene(default_context(), R.flatten(scene))

@@ -11,20 +11,25 @@ from liar_b200.kernel import default_context
 pytestmark = pytest.mark.gpu
 
 
-def _both(global_target, rt_direct, wave=8192, max_emitted=400_000):
+def _both(global_target, rt_direct, wave=8192, max_emitted=400_000, quality=1.0):
     scene, _ = scenes_render.photon_scene()
     flat = R.flatten(scene)
     gs = R.GpuScene(default_context(), flat)
-    d = photons.photon_desc(global_target, max_emitted=max_emitted, wave=wave, ray_traced_direct=rt_direct, seed=4)
+    d = photons.photon_desc(global_target, max_emitted=max_emitted, wave=wave, ray_traced_direct=rt_direct, seed=4,
+                            caustics_quality=quality)
     g, gc = photons.trace_photons(gs, d, capacity=400_000)
     c, cc = oracle.photon_trace(oracle.RenderScene(flat), d, 400_000)
     g = {k: v.cpu().numpy() for k, v in g.items()}
     return g, gc, c, cc
 
 
-@pytest.mark.parametrize("rt_direct", [True, False])
-def test_photon_trace_matches_oracle(rt_direct):
-    g, gc, c, cc = _both(3000, rt_direct)
+@pytest.mark.parametrize("rt_direct,quality", [(True, 1.0), (False, 1.0), (False, 4.0), (True, 0.0)])
+def test_photon_trace_matches_oracle(rt_direct, quality):
+    """quality: causticsQuality, whose storage probabilities (1 / 4 global, 1 caustic at 4; no
+    caustic photons at 0) decide by Russian roulette which diffuse hits are stored."""
+    g, gc, c, cc = _both(3000, rt_direct, quality=quality)
+    if quality == 0.0:
+        assert gc["caustic"] == 0 and cc["caustic"] == 0
     assert gc["emitted"] == cc["emitted"]
     for k in ("stored", "global", "caustic"):
         assert abs(gc[k] - cc[k]) <= max(3, 0.01 * cc[k]), (k, gc, cc)
