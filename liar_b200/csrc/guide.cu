@@ -6,9 +6,10 @@
 // (neural importance sampling, Mueller et al. 2019): for records (x, w, F/p) the loss is
 //   L = -(1/B) sum_i min((F_i/p_i) / mean(F/p), 20) * log q(w_i | x_i),
 // q = sum_l pi_l vMF(w; mu_l, kappa_l), pi = softmax(logits), mu = m / |m|, kappa = e^{clamp(s)}.
-// One step: forward (stores the bf16 activations and the output gradient, fused) -> backward
-// (stores the bf16 layer deltas) -> weight gradients as split-K GEMMs over the records ->
-// Adam on the f32 master weights -> repack the bf16 fragments.
+// One step, every GEMM on the 5th-generation tensor cores (tcgen05): forward (stores the bf16
+// activations and the output gradient, fused) -> backward (stores the bf16 layer deltas) -> weight
+// gradients over the records, accumulated in tensor memory -> Adam on the f32 master weights ->
+// repack the bf16 operand images.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -33,12 +34,10 @@ struct liar_gpu_guide {
     float* adam_m = nullptr;
     float* adam_v = nullptr;
     uint32_t* step = nullptr;  // Adam step count (device)
-    uint2* frag_fwd = nullptr;
-    uint2* frag_bwd = nullptr;
-    unsigned char* umma_w = nullptr;  // B-operand images of the six layers for the tcgen05 inference
+    unsigned char* umma_w = nullptr;   // forward B-operand images of the six layers (inference, training)
+    unsigned char* umma_wb = nullptr;  // backward B-operand images of W1..W5 (training)
     // training scratch, sized for cap records
     size_t cap = 0;
-    __nv_bfloat16* enc = nullptr;    // h_0 (the encodings): [cap][256]
     __nv_bfloat16* act = nullptr;    // h_1..h_5: [5][cap][64]
     __nv_bfloat16* delta = nullptr;  // delta_1..delta_5: [5][cap][64]
     __nv_bfloat16* gout = nullptr;   // [cap][48]
@@ -51,7 +50,6 @@ struct liar_gpu_guide {
 namespace liar_gpu {
 namespace guide {
 // used by the guided renderer (guided.cu)
-const uint2* guide_frag_fwd(const liar_gpu_guide* g) { return g->frag_fwd; }
 const liar_guide_config& guide_config(const liar_gpu_guide* g) { return g->cfg; }
 int guide_device(const liar_gpu_guide* g) { return g->device; }
 unsigned long long guide_steps(const liar_gpu_guide* g) { return g->steps_done; }
@@ -67,16 +65,10 @@ int guide_train(liar_gpu_ctx* ctx, liar_gpu_guide* g, const float* d_records, co
 
 namespace {
 
-constexpr int kThreads = 128;  // 4 warps
 constexpr int kRecordFloats = 13;
 // normalised record weights are clipped here: radiance estimates are heavy-tailed and a handful of
 // records would otherwise set the whole gradient (the renderer stays unbiased whatever the guide)
 constexpr float kWeightClip = 20.0f;
-constexpr int kFwdWarps = 8;  // forward kernels: 8 warps share one copy of the weights
-constexpr int kFwdThreads = 32 * kFwdWarps;
-// per warp: the encodings of its 32 rows; the raw outputs reuse the same bytes afterwards
-static_assert((size_t)32 * kOutStride * sizeof(float) <= kEncWarpBytes, "output scratch fits the encodings");
-constexpr size_t kEvalSmem = kFwdBytes + kFwdWarps * kEncWarpBytes;
 
 __device__ __forceinline__ void normalise_input(const float* raw, const float* lo, const float* inv_ext, float* x) {
     for (int c = 0; c < 3; ++c) x[c] = (raw[c] - lo[c]) * inv_ext[c];
@@ -97,45 +89,13 @@ Box make_box(const liar_guide_config& c) {
     return b;
 }
 
-// ---- fragments
-
-__global__ void k_pack(const float* __restrict__ P, uint2* __restrict__ fwd, uint2* __restrict__ bwd,
-                       uint32_t* step, int bump) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int lane = i & 31, g = lane >> 2, t = lane & 3;
-    const int tile = i >> 5;
-    if (i == 0 && bump) *step += 1;
-    auto bf = [](float v) { return __float2bfloat16_rn(v); };
-    auto pk = [&](float a, float b) {
-        __nv_bfloat162 v;
-        v.x = bf(a);
-        v.y = bf(b);
-        return *reinterpret_cast<uint32_t*>(&v);
-    };
-    if (tile < kFwdTiles) {
-        int l = 0;
-        while (l < 5 && tile >= fwd_tile_offset(l + 1)) ++l;
-        const int loc = tile - fwd_tile_offset(l), N = layer_n(l);
-        const int kk = loc / (N / 8), nt = loc % (N / 8);
-        const int k0 = 16 * kk + 2 * t, n = 8 * nt + g;
-        const float* W = P + param_offset(l);
-        fwd[i] = make_uint2(pk(W[k0 * N + n], W[(k0 + 1) * N + n]), pk(W[(k0 + 8) * N + n], W[(k0 + 9) * N + n]));
-    } else if (tile < kFwdTiles + kBwdTiles) {
-        const int bt = tile - kFwdTiles;
-        int l = 1;
-        while (l < 5 && bt >= bwd_tile_offset(l + 1)) ++l;
-        const int loc = bt - bwd_tile_offset(l), N = layer_n(l);
-        const int kk = loc / 8, nt = loc % 8;
-        const int k0 = 16 * kk + 2 * t, n = 8 * nt + g;  // k over the out features, n over the in features
-        const float* W = P + param_offset(l);
-        bwd[(size_t)bt * 32 + lane] =
-            make_uint2(pk(W[n * N + k0], W[n * N + k0 + 1]), pk(W[n * N + k0 + 8], W[n * N + k0 + 9]));
-    }
-}
+// ---- operand images
 
 // the tcgen05 B operands: layer l's element (n, k) = W_l[k][n] at umma_offset(n, k, K_l)
-__global__ void k_pack_umma(const float* __restrict__ P, unsigned char* __restrict__ img) {
+// (bump: count the Adam step just taken)
+__global__ void k_pack_umma(const float* __restrict__ P, unsigned char* __restrict__ img, uint32_t* step, int bump) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;  // one parameter (k, n) per thread
+    if (i == 0 && bump) *step += 1;
     if (i >= kParams) return;
     int l = 0;
     while (l < 5 && i >= param_offset(l + 1)) ++l;
@@ -143,20 +103,6 @@ __global__ void k_pack_umma(const float* __restrict__ P, unsigned char* __restri
     const int k = loc / N, n = loc % N;
     *reinterpret_cast<__nv_bfloat16*>(img + umma_w_offset(l) + umma_offset((uint32_t)n, (uint32_t)k, (uint32_t)K)) =
         __float2bfloat16_rn(P[i]);
-}
-
-int launch_pack(liar_gpu_guide* G, cudaStream_t st, int bump) {
-    const int total = (kFwdTiles + kBwdTiles) * 32;
-    k_pack<<<(total + 255) / 256, 256, 0, st>>>(G->params, G->frag_fwd, G->frag_bwd, G->step, bump);
-    k_pack_umma<<<(kParams + 255) / 256, 256, 0, st>>>(G->params, G->umma_w);
-    return cudaGetLastError() == cudaSuccess ? LIAR_OK : LIAR_ERR_CUDA;
-}
-
-__device__ __forceinline__ void load_frags(uint2* dst, const uint2* __restrict__ src, size_t bytes) {
-    const uint4* s = reinterpret_cast<const uint4*>(src);
-    uint4* d = reinterpret_cast<uint4*>(dst);
-    for (size_t i = threadIdx.x; i < bytes / 16; i += blockDim.x) d[i] = s[i];
-    __syncthreads();
 }
 
 // ---- inference on tcgen05: two slots of 128 rows per CTA (guide_umma.cuh)
@@ -326,234 +272,465 @@ __device__ float record_gradient(const float* o, float wx, float wy, float wz, f
     return -weight * lq;
 }
 
-// forward over a batch of records with the activations stored, then the output gradient
-__global__ void __launch_bounds__(kFwdThreads) k_train_forward(const uint2* __restrict__ frag, const float* __restrict__ rec,
-                                                               const uint32_t* __restrict__ n_dev, size_t n_max, Box box,
-                                                               const float* __restrict__ scalars_in,
-                                                               __nv_bfloat16* __restrict__ enc_out,
-                                                               __nv_bfloat16* __restrict__ act,
-                                                               __nv_bfloat16* __restrict__ gout, float* __restrict__ loss) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    uint2* wf = reinterpret_cast<uint2*>(smem);
-    load_frags(wf, frag, kFwdBytes);
+// ---- training on tcgen05 (guide_umma.cuh's operand layouts and instruction forms)
+//
+// forward  k_train_fwd_tc: the inference kernel's two 4-warp slots of 128 records; after every
+//          hidden layer its ReLU'd bf16 activations also go to global memory (h_1..h_5, for the
+//          backward masks and the weight gradients), and after the last layer each thread turns
+//          its row's 40 raw outputs into the loss and its gradient (record_gradient), stored bf16
+// backward k_train_bwd_tc: delta_l = (delta_{l+1} W_l^T) * [h_l > 0] for l = 5..1 (delta_6 =
+//          the output gradient), one UMMA chain per 128-record tile with the weights as B
+//          operands element (n, k) = W_l[n][k] (n an input, k an output of layer l); each delta
+//          is stored bf16 and written back as the next A operand
+// weights  k_train_dw_tc: dW_l = H_l^T D_l summed over the records (H_0 the encodings, recomputed;
+//          H_l = h_l; D_l = delta_{l+1}, D_5 the output gradient): the records are the K
+//          dimension, so each 64-record stage is staged row-major and transposed into K-major
+//          operands (A: features x records, B: outputs x records); a CTA accumulates all six
+//          weight gradients of its records in tensor memory (448 of 512 columns; the 64-feature
+//          layers use the lower half of M = 128, the upper half zero) and adds them to the
+//          global gradient once
+// Every mbarrier wait is bounded (max_tries polls): a wait that runs out records kStatusTimeout,
+// waits once more (bounded) for the commit it gave up on, and the CTA frees its tensor memory.
+// issue_mma = 0 (the fault test) issues no MMA or commit, so the first wait runs out.
+
+// backward B images: layer l (1..5) element (n, k) = W_l[n][k] at umma_offset(n, k, N_l)
+__host__ __device__ constexpr uint32_t umma_wb_offset(int l) { return 8192u * (uint32_t)(l - 1); }
+constexpr uint32_t kUmmaWbBytes = 4u * 8192u + 6144u;  // W1..W4 64 x 64, W5 64 x 48
+
+__global__ void k_pack_umma_bwd(const float* __restrict__ P, unsigned char* __restrict__ img) {
+    const int i = param_offset(1) + blockIdx.x * blockDim.x + threadIdx.x;  // the parameters of W1..W5
+    if (i >= kParams) return;
+    int l = 1;
+    while (l < 5 && i >= param_offset(l + 1)) ++l;
+    const int loc = i - param_offset(l), N = layer_n(l);
+    const int in = loc / N, out = loc % N;
+    *reinterpret_cast<__nv_bfloat16*>(img + umma_wb_offset(l) + umma_offset((uint32_t)in, (uint32_t)out, (uint32_t)N)) =
+        __float2bfloat16_rn(P[i]);
+}
+
+__device__ __forceinline__ void store_row_bf16(__nv_bfloat16* dst, const float* v, int n, bool relu) {
+    uint4* d = reinterpret_cast<uint4*>(dst);
+    for (int c = 0; c < n / 8; ++c) {
+        const float* q = v + 8 * c;
+        auto f = [&](float x) { return relu ? fmaxf(x, 0.0f) : x; };
+        d[c] = make_uint4(pack_bf16(f(q[0]), f(q[1])), pack_bf16(f(q[2]), f(q[3])), pack_bf16(f(q[4]), f(q[5])),
+                          pack_bf16(f(q[6]), f(q[7])));
+    }
+}
+
+// the shared prologue of the two per-tile kernels: weights to shared memory, mbarriers, TMEM
+struct TcTile {
+    uint64_t* mbar_all;
+    uint32_t* tmem_slot;
+    volatile uint32_t* failed;
+};
+__device__ __forceinline__ TcTile tc_setup(unsigned char* smem, size_t w_bytes, size_t buf_bytes,
+                                           const unsigned char* __restrict__ w_img) {
+    TcTile T;
+    T.mbar_all = reinterpret_cast<uint64_t*>(smem + w_bytes + (size_t)kTcSlots * buf_bytes);
+    T.tmem_slot = reinterpret_cast<uint32_t*>(T.mbar_all + kTcSlots);
+    T.failed = T.tmem_slot + 1;
+    const uint32_t tid = threadIdx.x;
+    const uint4* s = reinterpret_cast<const uint4*>(w_img);
+    uint4* d = reinterpret_cast<uint4*>(smem);
+    for (uint32_t i = tid; i < w_bytes / 16; i += kTcThreads) d[i] = s[i];
+    if (tid == 0) {
+        for (int k = 0; k < kTcSlots; ++k)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(T.mbar_all + k)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        T.failed[0] = T.failed[1] = 0u;
+    }
+    if ((tid >> 5) == 0) {
+        const uint32_t sa = (uint32_t)__cvta_generic_to_shared(T.tmem_slot);
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sa), "r"(kTcTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    return T;
+}
+
+__device__ __forceinline__ void tc_teardown(const TcTile& T, uint32_t* status) {
+    tc_fence_before();
+    __syncthreads();
+    if ((threadIdx.x >> 5) == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*T.tmem_slot), "r"(kTcTmemCols));
+    if (threadIdx.x == 0 && (T.failed[0] | T.failed[1])) atomicOr(status, kStatusTimeout);
+}
+
+// one layer of a slot: K / 16 MMAs by the slot's thread 0, committed to the slot's mbarrier, then a
+// bounded wait; false when the wait ran out (after the drain wait)
+__device__ __forceinline__ bool tc_layer(uint32_t r, uint32_t tmem, uint32_t a_addr, uint32_t b_addr, uint32_t K,
+                                         uint32_t N, uint32_t mbar_addr, uint32_t& phase, uint32_t slot,
+                                         volatile uint32_t* failed, uint32_t max_tries, int issue_mma) {
+    fence_async_smem();
+    tc_fence_before();
+    asm volatile("bar.sync %0, 128;" ::"r"(1u + slot) : "memory");
+    tc_fence_after();
+    if (r == 0 && issue_mma) {
+        const uint32_t idesc = umma_idesc(N);
+        for (uint32_t j = 0; j < K / 16; ++j)
+            umma_bf16(tmem, umma_smem_desc(a_addr + 256u * j, (K / 8) * 128u), umma_smem_desc(b_addr + 256u * j, (K / 8) * 128u),
+                      idesc, j > 0 ? 1u : 0u);
+        umma_commit(mbar_addr);
+    }
+    if (!mbar_wait(mbar_addr, phase, max_tries)) failed[slot] = 1u;
+    asm volatile("bar.sync %0, 128;" ::"r"(1u + slot) : "memory");
+    if (failed[slot]) {
+        if (issue_mma) mbar_wait(mbar_addr, phase, max_tries);
+        return false;
+    }
+    phase ^= 1u;
+    tc_fence_after();
+    return true;
+}
+
+constexpr size_t kFwdTcSmem = 1024 + kUmmaWBytes + (size_t)kTcSlots * kUmmaA0Bytes + 128;
+
+__global__ void __launch_bounds__(kTcThreads, 1) k_train_fwd_tc(const unsigned char* __restrict__ w_img,
+                                                                const float* __restrict__ rec,
+                                                                const uint32_t* __restrict__ n_dev, size_t n_max, Box box,
+                                                                const float* __restrict__ scalars_in,
+                                                                __nv_bfloat16* __restrict__ act,
+                                                                __nv_bfloat16* __restrict__ gout, float* __restrict__ loss,
+                                                                uint32_t* __restrict__ status, uint32_t max_tries,
+                                                                int issue_mma) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    const TcTile T = tc_setup(smem, kUmmaWBytes, kUmmaA0Bytes, w_img);
     const size_t n = n_dev ? min((size_t)*n_dev, n_max) : n_max;
     const float wsum = scalars_in[0];
     const float inv_mean = (wsum > 0.0f && n > 0) ? (float)n / wsum : 0.0f;
     const float inv_b = n > 0 ? 1.0f / (float)n : 0.0f;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    __nv_bfloat16* enc = reinterpret_cast<__nv_bfloat16*>(smem + kFwdBytes + warp * kEncWarpBytes);
-    float* os = reinterpret_cast<float*>(enc);
-    const size_t n_tiles = (n + 31) / 32;
+    const uint32_t tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t slot = tid >> 7, r = tid & 127u;
+    unsigned char* buf = smem + kUmmaWBytes + slot * kUmmaA0Bytes;
+    const uint32_t tmem = *T.tmem_slot + 64u * slot;
+    const uint32_t taddr = tmem + ((32u * (warp & 3u)) << 16);
+    const uint32_t mbar_addr = (uint32_t)__cvta_generic_to_shared(T.mbar_all + slot);
+    const uint32_t sw_addr = (uint32_t)__cvta_generic_to_shared(smem);
+    const uint32_t buf_addr = (uint32_t)__cvta_generic_to_shared(buf);
+    uint32_t phase = 0;
     float lsum = 0.0f;
-    for (size_t tile = (size_t)blockIdx.x * kFwdWarps + warp; tile < n_tiles; tile += (size_t)gridDim.x * kFwdWarps) {
-        const size_t row = tile * 32 + lane;
+    const size_t n_tiles = (n + kTcRows - 1) / kTcRows;
+    bool ok = true;
+    for (size_t tile = (size_t)blockIdx.x * kTcSlots + slot; ok && tile < n_tiles; tile += (size_t)gridDim.x * kTcSlots) {
+        const size_t row = tile * kTcRows + r;
         float x[kIn];
-        float wx = 0, wy = 0, wz = 1, weight = 0;
+        float wx = 0.0f, wy = 0.0f, wz = 1.0f, weight = 0.0f;
         if (row < n) {
-            const float* r = rec + row * kRecordFloats;
-            normalise_input(r, box.lo, box.inv_ext, x);
-            wx = r[9];
-            wy = r[10];
-            wz = r[11];
-            weight = r[12];
+            const float* rr = rec + row * kRecordFloats;
+            normalise_input(rr, box.lo, box.inv_ext, x);
+            wx = rr[9];
+            wy = rr[10];
+            wz = rr[11];
+            weight = rr[12];
             if (!(weight > 0.0f) || !isfinite(weight)) weight = 0.0f;
         } else {
             for (int c = 0; c < kIn; ++c) x[c] = 0.0f;
         }
-        encode_row(x, enc + lane * kEncLd);
-        __syncwarp();
-        const uint32_t valid = (uint32_t)min((size_t)32, n - tile * 32);
-        // h_0 for the weight gradient of W0: the warp writes its rows, 512 contiguous bytes each
-        for (uint32_t r = 0; r < valid; ++r)
-            reinterpret_cast<uint4*>(enc_out + (tile * 32 + r) * kEnc)[lane] =
-                reinterpret_cast<const uint4*>(enc + r * kEncLd)[lane];
-        float out[2][6][4];
-        mlp_forward_warp(enc, wf, out, ActStore{act, n_max * kWidth, (uint32_t)(tile * 32), valid});
-        __syncwarp();
-        scatter_out(out, os);
-        __syncwarp();
+        encode_row_umma(x, buf, r);
+        float v[64];
+        for (int l = 0; l < kLayers && ok; ++l) {
+            ok = tc_layer(r, tmem, buf_addr, sw_addr + umma_w_offset(l), (uint32_t)layer_k(l), (uint32_t)layer_n(l), mbar_addr,
+                          phase, slot, T.failed, max_tries, issue_mma);
+            if (!ok) break;
+            tmem_ld_x64(taddr, v);
+            if (l < kLayers - 1) {
+                // h_{l+1}: ReLU, bf16, to global memory and as the next A operand
+                if (row < n) store_row_bf16(act + (size_t)l * n_max * kWidth + row * kWidth, v, kWidth, true);
+                unsigned char* dst = buf + (r >> 3) * (kWidth / 8) * 128u + (r & 7u) * 16u;
+#pragma unroll
+                for (int c = 0; c < kWidth / 8; ++c) {
+                    const float* q = v + 8 * c;
+                    *reinterpret_cast<uint4*>(dst + c * 128u) =
+                        make_uint4(pack_bf16(fmaxf(q[0], 0.0f), fmaxf(q[1], 0.0f)), pack_bf16(fmaxf(q[2], 0.0f), fmaxf(q[3], 0.0f)),
+                                   pack_bf16(fmaxf(q[4], 0.0f), fmaxf(q[5], 0.0f)), pack_bf16(fmaxf(q[6], 0.0f), fmaxf(q[7], 0.0f)));
+                }
+            }
+        }
+        if (!ok) break;
         if (row < n) {
             float d[kOut];
             for (int c = kOutUsed; c < kOut; ++c) d[c] = 0.0f;
             const float wn = fminf(weight * inv_mean, kWeightClip);
-            lsum += record_gradient(os + lane * kOutStride, wx, wy, wz, wn, inv_b, d);
-            uint32_t* dst = reinterpret_cast<uint32_t*>(gout + row * kOut);
-            for (int c = 0; c < kOut / 2; ++c) dst[c] = pack_bf16(d[2 * c], d[2 * c + 1]);
+            lsum += record_gradient(v, wx, wy, wz, wn, inv_b, d);
+            store_row_bf16(gout + row * kOut, d, kOut, false);
         }
-        __syncwarp();
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) lsum += __shfl_down_sync(0xffffffffu, lsum, o);
-    if (lane == 0 && lsum != 0.0f) atomicAdd(loss, lsum * inv_b);
+    if ((tid & 31u) == 0 && lsum != 0.0f) atomicAdd(loss, lsum * inv_b);
+    tc_teardown(T, status);
 }
 
-// backward: delta_5 = (g_out W5^T) * [h_5 > 0], ..., delta_1 = (delta_2 W1^T) * [h_1 > 0]
-__global__ void __launch_bounds__(kThreads) k_train_backward(const uint2* __restrict__ frag_bwd,
+constexpr uint32_t kBwdBuf = (uint32_t)kTcRows * kWidth * 2;  // a slot's A operand: 128 x 64 bf16
+constexpr size_t kBwdTcSmem = 1024 + kUmmaWbBytes + (size_t)kTcSlots * kBwdBuf + 128;
+
+__global__ void __launch_bounds__(kTcThreads) k_train_bwd_tc(const unsigned char* __restrict__ wb_img,
                                                              const uint32_t* __restrict__ n_dev, size_t n_max,
                                                              const __nv_bfloat16* __restrict__ act,
                                                              const __nv_bfloat16* __restrict__ gout,
-                                                             __nv_bfloat16* __restrict__ delta) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    uint2* wb = reinterpret_cast<uint2*>(smem);
-    load_frags(wb, frag_bwd, kBwdBytes);
+                                                             __nv_bfloat16* __restrict__ delta,
+                                                             uint32_t* __restrict__ status, uint32_t max_tries,
+                                                             int issue_mma) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    const TcTile T = tc_setup(smem, kUmmaWbBytes, kBwdBuf, wb_img);
     const size_t n = n_dev ? min((size_t)*n_dev, n_max) : n_max;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    const size_t n_tiles = (n + 31) / 32;
-    for (size_t tile = (size_t)blockIdx.x * 4 + warp; tile < n_tiles; tile += (size_t)gridDim.x * 4) {
-        const size_t r0 = tile * 32;
-        auto ld32 = [&](const __nv_bfloat16* base, size_t ld, size_t row, int col) -> uint32_t {
-            return row < n ? *reinterpret_cast<const uint32_t*>(base + row * ld + col) : 0u;
-        };
-        // A fragments of g_out (3 k tiles of 16 over the 48 outputs)
-        uint32_t a[2][4][4];
+    const uint32_t tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t slot = tid >> 7, r = tid & 127u;
+    unsigned char* buf = smem + kUmmaWbBytes + slot * kBwdBuf;
+    const uint32_t tmem = *T.tmem_slot + 64u * slot;
+    const uint32_t taddr = tmem + ((32u * (warp & 3u)) << 16);
+    const uint32_t mbar_addr = (uint32_t)__cvta_generic_to_shared(T.mbar_all + slot);
+    const uint32_t sw_addr = (uint32_t)__cvta_generic_to_shared(smem);
+    const uint32_t buf_addr = (uint32_t)__cvta_generic_to_shared(buf);
+    uint32_t phase = 0;
+    const size_t n_tiles = (n + kTcRows - 1) / kTcRows;
+    bool ok = true;
+    for (size_t tile = (size_t)blockIdx.x * kTcSlots + slot; ok && tile < n_tiles; tile += (size_t)gridDim.x * kTcSlots) {
+        const size_t row = tile * kTcRows + r;
+        // the output gradient (48 wide) as the first A operand
+        {
+            const uint4* src = reinterpret_cast<const uint4*>(gout + row * kOut);
+            unsigned char* dst = buf + (r >> 3) * (kOut / 8) * 128u + (r & 7u) * 16u;
 #pragma unroll
-        for (int mt = 0; mt < 2; ++mt)
+            for (int c = 0; c < kOut / 8; ++c)
+                *reinterpret_cast<uint4*>(dst + c * 128u) = row < n ? src[c] : make_uint4(0u, 0u, 0u, 0u);
+        }
+        for (int l = kLayers - 1; l >= 1 && ok; --l) {
+            ok = tc_layer(r, tmem, buf_addr, sw_addr + umma_wb_offset(l), (uint32_t)layer_n(l), (uint32_t)kWidth, mbar_addr,
+                          phase, slot, T.failed, max_tries, issue_mma);
+            if (!ok) break;
+            float v[64];
+            tmem_ld_x64(taddr, v);
+            // mask by h_l > 0 (the ReLU of layer l - 1's output), store delta_l, next A operand
+            if (row < n) {
+                const uint4* hp = reinterpret_cast<const uint4*>(act + (size_t)(l - 1) * n_max * kWidth + row * kWidth);
 #pragma unroll
-            for (int kk = 0; kk < 3; ++kk) {
-                const size_t ra = r0 + 16 * mt + g;
-                a[mt][kk][0] = ld32(gout, kOut, ra, 16 * kk + 2 * t);
-                a[mt][kk][1] = ld32(gout, kOut, ra + 8, 16 * kk + 2 * t);
-                a[mt][kk][2] = ld32(gout, kOut, ra, 16 * kk + 8 + 2 * t);
-                a[mt][kk][3] = ld32(gout, kOut, ra + 8, 16 * kk + 8 + 2 * t);
-            }
-#pragma unroll 1
-        for (int l = 5; l >= 1; --l) {
-            const int n_kk = layer_n(l) / 16;  // 3 for W5, 4 otherwise
-            float acc[2][8][4];
+                for (int c = 0; c < kWidth / 8; ++c) {
+                    const uint4 h = hp[c];
+                    const uint32_t hw[4] = {h.x, h.y, h.z, h.w};
 #pragma unroll
-            for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-                for (int nt = 0; nt < 8; ++nt)
-#pragma unroll
-                    for (int r = 0; r < 4; ++r) acc[mt][nt][r] = 0.0f;
-            const uint2* wl = wb + (size_t)bwd_tile_offset(l) * 32 + lane;
-#pragma unroll
-            for (int kk = 0; kk < 4; ++kk) {
-                if (kk < n_kk) {
-#pragma unroll
-                    for (int nt = 0; nt < 8; ++nt) {
-                        const uint2 b = wl[(kk * 8 + nt) * 32];
-                        mma_bf16(acc[0][nt], a[0][kk], b);
-                        mma_bf16(acc[1][nt], a[1][kk], b);
+                    for (int e = 0; e < 4; ++e) {
+                        if (!(bf16_lo(hw[e]) > 0.0f)) v[8 * c + 2 * e] = 0.0f;
+                        if (!(bf16_hi(hw[e]) > 0.0f)) v[8 * c + 2 * e + 1] = 0.0f;
                     }
                 }
+                store_row_bf16(delta + (size_t)(l - 1) * n_max * kWidth + row * kWidth, v, kWidth, false);
+            } else {
+                for (int c = 0; c < 64; ++c) v[c] = 0.0f;
             }
-            // mask by h_l > 0, store delta_l, regroup as A fragments for the next layer down
-            const __nv_bfloat16* h = act + (size_t)(l - 1) * n_max * kWidth;
-            __nv_bfloat16* dl = delta + (size_t)(l - 1) * n_max * kWidth;
+            if (l > 1) {
+                unsigned char* dst = buf + (r >> 3) * (kWidth / 8) * 128u + (r & 7u) * 16u;
 #pragma unroll
-            for (int mt = 0; mt < 2; ++mt) {
-                const size_t ra = r0 + 16 * mt + g, rb = ra + 8;
-#pragma unroll
-                for (int nt = 0; nt < 8; ++nt) {
-                    const int c = 8 * nt + 2 * t;
-                    const uint32_t ha = ld32(h, kWidth, ra, c), hb = ld32(h, kWidth, rb, c);
-                    float* v = acc[mt][nt];
-                    if (!(bf16_lo(ha) > 0.0f)) v[0] = 0.0f;
-                    if (!(bf16_hi(ha) > 0.0f)) v[1] = 0.0f;
-                    if (!(bf16_lo(hb) > 0.0f)) v[2] = 0.0f;
-                    if (!(bf16_hi(hb) > 0.0f)) v[3] = 0.0f;
-                    const uint32_t pa = pack_bf16(v[0], v[1]), pb = pack_bf16(v[2], v[3]);
-                    if (ra < n) *reinterpret_cast<uint32_t*>(dl + ra * kWidth + c) = pa;
-                    if (rb < n) *reinterpret_cast<uint32_t*>(dl + rb * kWidth + c) = pb;
-                    const int kk = nt >> 1;
-                    if ((nt & 1) == 0) {
-                        a[mt][kk][0] = pa;
-                        a[mt][kk][1] = pb;
-                    } else {
-                        a[mt][kk][2] = pa;
-                        a[mt][kk][3] = pb;
-                    }
+                for (int c = 0; c < kWidth / 8; ++c) {
+                    const float* q = v + 8 * c;
+                    *reinterpret_cast<uint4*>(dst + c * 128u) = make_uint4(pack_bf16(q[0], q[1]), pack_bf16(q[2], q[3]),
+                                                                           pack_bf16(q[4], q[5]), pack_bf16(q[6], q[7]));
                 }
             }
         }
+    }
+    tc_teardown(T, status);
+}
+
+// weight gradients: shared-memory plan of one CTA (bytes from the 1024-aligned base)
+constexpr int kDwRecords = 64;                            // records per stage (the UMMA K of a stage)
+constexpr uint32_t kDwA = 128u * kDwRecords * 2;          // an A operand: 128 features x 64 records
+constexpr uint32_t kDwB = 64u * kDwRecords * 2;           // a B operand: 64 outputs x 64 records
+constexpr uint32_t kDwOffA0 = 0, kDwOffB0 = 2 * kDwA, kDwOffA1 = kDwOffB0 + kDwB, kDwOffB1 = kDwOffA1 + 2 * kDwA;
+constexpr uint32_t kDwOffH = kDwOffB1 + 2 * kDwB;         // staging: 64 records x up to 256 features, row-major
+constexpr uint32_t kDwOffD = kDwOffH + kDwRecords * kEnc * 2;  // staging: 64 records x up to 64 outputs
+constexpr uint32_t kDwOffBar = kDwOffD + kDwRecords * kWidth * 2;
+constexpr size_t kDwTcSmem = 1024 + kDwOffBar + 64;
+constexpr int kDwThreads = 256;
+constexpr uint32_t kDwTmemCols = 512;  // dW0 (two M blocks), dW1..dW4, dW5: 7 x 64 columns
+
+// stage rows [s0, s0 + 64) of a [n][ld] bf16 matrix into a row-major [64][ld] tile (zeros past n)
+__device__ __forceinline__ void dw_stage(unsigned char* dst, const __nv_bfloat16* __restrict__ src, size_t s0, size_t n,
+                                         int ld) {
+    const int chunks = ld / 8;
+    for (int i = threadIdx.x; i < kDwRecords * chunks; i += kDwThreads) {
+        const int rr = i / chunks, c = i % chunks;
+        const size_t row = s0 + rr;
+        reinterpret_cast<uint4*>(dst)[i] =
+            row < n ? reinterpret_cast<const uint4*>(src + row * ld)[c] : make_uint4(0u, 0u, 0u, 0u);
     }
 }
 
-// weight gradients: dW_l = H_l^T D_l summed over the records, split over record chunks.
-// job 0..3: W0 rows [64 j, 64 j + 64) (H = the encoding, D = delta_1); job 4..7: W1..W4
-// (H = h_l, D = delta_{l+1}); job 8: W5 (H = h_5, D = g_out, 48 wide).
-constexpr int kDwChunk = 2048;
-constexpr int kDwStage = 64;
-constexpr int kDwLd = 72;  // padded bf16 row stride of the staged tiles
+// the transpose of a staged [64][ld] tile, columns [c0, c0 + rows): operand row m = column c0 + m,
+// K = the 64 records, in the K-major layout (umma_offset(m, k, 64))
+__device__ __forceinline__ void dw_transpose(unsigned char* op, const unsigned char* tile, int ld, int c0, int rows) {
+    const uint16_t* t = reinterpret_cast<const uint16_t*>(tile);
+    for (int i = threadIdx.x; i < rows * (kDwRecords / 8); i += kDwThreads) {
+        const int m = i % rows, g = i / rows;  // consecutive threads: consecutive columns (conflict-free reads)
+        uint32_t w[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const uint32_t lo = t[(size_t)(8 * g + 2 * e) * ld + c0 + m];
+            const uint32_t hi = t[(size_t)(8 * g + 2 * e + 1) * ld + c0 + m];
+            w[e] = lo | (hi << 16);
+        }
+        *reinterpret_cast<uint4*>(op + umma_offset((uint32_t)m, (uint32_t)(8 * g), (uint32_t)kDwRecords)) =
+            make_uint4(w[0], w[1], w[2], w[3]);
+    }
+}
 
-__global__ void __launch_bounds__(kThreads) k_train_dw(const uint32_t* __restrict__ n_dev, size_t n_max,
-                                                       const __nv_bfloat16* __restrict__ enc,
-                                                       const __nv_bfloat16* __restrict__ act,
-                                                       const __nv_bfloat16* __restrict__ delta,
-                                                       const __nv_bfloat16* __restrict__ gout, float* __restrict__ grads) {
-    __shared__ __align__(16) uint16_t Hs[kDwStage * kDwLd];
-    __shared__ __align__(16) uint16_t Ds[kDwStage * kDwLd];
+__global__ void __launch_bounds__(kDwThreads, 1) k_train_dw_tc(const float* __restrict__ rec,
+                                                               const uint32_t* __restrict__ n_dev, size_t n_max, Box box,
+                                                               const __nv_bfloat16* __restrict__ act,
+                                                               const __nv_bfloat16* __restrict__ delta,
+                                                               const __nv_bfloat16* __restrict__ gout,
+                                                               float* __restrict__ grads, size_t per_cta,
+                                                               uint32_t* __restrict__ status, uint32_t max_tries,
+                                                               int issue_mma) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + kDwOffBar);  // [0] W0, [1], [2] the two W1..W5 buffers
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 3);
+    volatile uint32_t* failed = tmem_slot + 1;
+    const uint32_t tid = threadIdx.x, warp = tid >> 5;
     const size_t n = n_dev ? min((size_t)*n_dev, n_max) : n_max;
-    const int job = blockIdx.y;
-    const size_t c0 = (size_t)blockIdx.x * kDwChunk;
-    if (c0 >= n) return;
-    const size_t c1 = min(n, c0 + kDwChunk);
-    const int layer = job < 4 ? 0 : job - 3;
-    const int N = layer_n(layer);  // 48 or 64
-    const __nv_bfloat16* H = layer == 0 ? nullptr : act + (size_t)(layer - 1) * n_max * kWidth;
-    const __nv_bfloat16* D = layer == 5 ? gout : delta + (size_t)layer * n_max * kWidth;  // delta_{l+1} at index l
-    const int ldD = layer == 5 ? kOut : kWidth;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    float acc[8][4];
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt)
-#pragma unroll
-        for (int r = 0; r < 4; ++r) acc[nt][r] = 0.0f;
-    for (size_t s0 = c0; s0 < c1; s0 += kDwStage) {
+    const size_t c0 = (size_t)blockIdx.x * per_cta, c1 = min(n, c0 + per_cta);
+    // the upper halves (features 64..127) of the W1..W5 A operands stay zero
+    for (uint32_t i = tid; i < 2 * (kDwA / 2) / 16; i += kDwThreads) {
+        const uint32_t b = i / ((kDwA / 2) / 16), j = i % ((kDwA / 2) / 16);
+        reinterpret_cast<uint4*>(smem + kDwOffA1 + b * kDwA + kDwA / 2)[j] = make_uint4(0u, 0u, 0u, 0u);
+    }
+    if (tid == 0) {
+        for (int k = 0; k < 3; ++k)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(mbar + k)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        *failed = 0u;
+    }
+    if (warp == 0) {
+        const uint32_t sa = (uint32_t)__cvta_generic_to_shared(tmem_slot);
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sa), "r"(kDwTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t base = (uint32_t)__cvta_generic_to_shared(smem);
+    uint32_t phase[3] = {0u, 0u, 0u};
+    bool pending[3] = {false, false, false};
+    bool issued_any = false;  // an MMA has written the accumulators (the first ones overwrite)
+    bool ok = true;
+    // every thread waits for the commit of barrier b before its buffers are refilled
+    auto wait_bar = [&](int b) {
+        if (!pending[b]) return;
+        const uint32_t addr = (uint32_t)__cvta_generic_to_shared(mbar + b);
+        if (!mbar_wait(addr, phase[b], max_tries)) *failed = 1u;
         __syncthreads();
-        // stage H (64 records x 64 features; for W0 the job's 64 columns of the encodings) and D
-        const __nv_bfloat16* Hs_src = layer == 0 ? enc + 64 * job : H;
-        const int ldH = layer == 0 ? kEnc : kWidth;
-        for (int i = threadIdx.x; i < kDwStage * 8; i += kThreads) {
-            const int r = i >> 3, ch = i & 7;
-            const size_t row = s0 + r;
-            uint4 v = make_uint4(0, 0, 0, 0);
-            if (row < c1) v = *reinterpret_cast<const uint4*>(Hs_src + row * ldH + ch * 8);
-            *reinterpret_cast<uint4*>(&Hs[r * kDwLd + ch * 8]) = v;
+        if (*failed) {
+            ok = false;
+            return;
         }
-        const int chunks = ldD / 8;
-        for (int i = threadIdx.x; i < kDwStage * chunks; i += kThreads) {
-            const int r = i / chunks, ch = i % chunks;
-            const size_t row = s0 + r;
-            uint4 v = make_uint4(0, 0, 0, 0);
-            if (row < c1) v = *reinterpret_cast<const uint4*>(D + row * ldD + ch * 8);
-            *reinterpret_cast<uint4*>(&Ds[r * kDwLd + ch * 8]) = v;
+        phase[b] ^= 1u;
+        pending[b] = false;
+        tc_fence_after();
+    };
+    auto issue = [&](int b, uint32_t d_col, uint32_t a_off, uint32_t b_off, uint32_t N, bool acc0) {
+        if (tid == 0 && issue_mma) {
+            const uint32_t idesc = umma_idesc(N);
+            for (uint32_t j = 0; j < (uint32_t)kDwRecords / 16; ++j)
+                umma_bf16(tmem + d_col, umma_smem_desc(base + a_off + 256u * j, (kDwRecords / 8) * 128u),
+                          umma_smem_desc(base + b_off + 256u * j, (kDwRecords / 8) * 128u), idesc,
+                          (acc0 || j > 0) ? 1u : 0u);
         }
+    };
+    auto commit = [&](int b) {
+        if (tid == 0 && issue_mma) umma_commit((uint32_t)__cvta_generic_to_shared(mbar + b));
+        pending[b] = true;
+    };
+    for (size_t s0 = c0; ok && s0 < c1; s0 += kDwRecords) {
+        const bool acc = issued_any;
+        // ---- W0: the encodings of the stage's records (the forward's, recomputed) and delta_1
+        wait_bar(0);
+        if (!ok) break;
+        for (int i = tid; i < kDwRecords; i += kDwThreads) {
+            const size_t row = s0 + i;
+            float x[kIn];
+            if (row < c1) normalise_input(rec + row * kRecordFloats, box.lo, box.inv_ext, x);
+            __nv_bfloat16* dst = reinterpret_cast<__nv_bfloat16*>(smem + kDwOffH) + (size_t)i * kEnc;
+            if (row < c1) {
+                encode_row(x, dst);
+            } else {
+                for (int c = 0; c < kEnc / 8; ++c) reinterpret_cast<uint4*>(dst)[c] = make_uint4(0u, 0u, 0u, 0u);
+            }
+        }
+        dw_stage(smem + kDwOffD, delta, s0, c1, kWidth);
         __syncthreads();
-        const int m = 16 * warp + g;
-#pragma unroll
-        for (int k0 = 0; k0 < kDwStage; k0 += 16) {
-            auto hp = [&](int k, int mm) { return (uint32_t)Hs[k * kDwLd + mm]; };
-            uint32_t a[4];
-            a[0] = hp(k0 + 2 * t, m) | (hp(k0 + 2 * t + 1, m) << 16);
-            a[1] = hp(k0 + 2 * t, m + 8) | (hp(k0 + 2 * t + 1, m + 8) << 16);
-            a[2] = hp(k0 + 2 * t + 8, m) | (hp(k0 + 2 * t + 9, m) << 16);
-            a[3] = hp(k0 + 2 * t + 8, m + 8) | (hp(k0 + 2 * t + 9, m + 8) << 16);
-#pragma unroll
-            for (int nt = 0; nt < 8; ++nt) {
-                if (nt < N / 8) {
-                    const int nn = 8 * nt + g;
-                    uint2 b;
-                    b.x = (uint32_t)Ds[(k0 + 2 * t) * kDwLd + nn] | ((uint32_t)Ds[(k0 + 2 * t + 1) * kDwLd + nn] << 16);
-                    b.y = (uint32_t)Ds[(k0 + 2 * t + 8) * kDwLd + nn] | ((uint32_t)Ds[(k0 + 2 * t + 9) * kDwLd + nn] << 16);
-                    mma_bf16(acc[nt], a, b);
-                }
+        dw_transpose(smem + kDwOffA0, smem + kDwOffH, kEnc, 0, 128);
+        dw_transpose(smem + kDwOffA0 + kDwA, smem + kDwOffH, kEnc, 128, 128);
+        dw_transpose(smem + kDwOffB0, smem + kDwOffD, kWidth, 0, kWidth);
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        issue(0, 0u, kDwOffA0, kDwOffB0, 64u, acc);
+        issue(0, 64u, kDwOffA0 + kDwA, kDwOffB0, 64u, acc);
+        commit(0);
+        // ---- W1..W5: h_l and delta_{l+1} (the output gradient for W5), alternating buffers
+        for (int l = 1; l <= 5 && ok; ++l) {
+            const int b = 1 + ((l - 1) & 1);
+            wait_bar(b);
+            if (!ok) break;
+            const int N = layer_n(l);
+            dw_stage(smem + kDwOffH, act + (size_t)(l - 1) * n_max * kWidth, s0, c1, kWidth);
+            if (l < 5) dw_stage(smem + kDwOffD, delta + (size_t)l * n_max * kWidth, s0, c1, kWidth);
+            else dw_stage(smem + kDwOffD, gout, s0, c1, kOut);
+            __syncthreads();
+            const uint32_t a_off = kDwOffA1 + (uint32_t)(b - 1) * kDwA, b_off = kDwOffB1 + (uint32_t)(b - 1) * kDwB;
+            dw_transpose(smem + a_off, smem + kDwOffH, kWidth, 0, kWidth);
+            dw_transpose(smem + b_off, smem + kDwOffD, N, 0, N);
+            fence_async_smem();
+            tc_fence_before();
+            __syncthreads();
+            tc_fence_after();
+            issue(b, 128u + 64u * (uint32_t)(l - 1), a_off, b_off, (uint32_t)N, acc);
+            commit(b);
+        }
+        issued_any = true;
+    }
+    // drain: every outstanding commit (bounded), then the accumulators out
+    for (int b = 0; b < 3; ++b) {
+        if (!pending[b]) continue;
+        const uint32_t addr = (uint32_t)__cvta_generic_to_shared(mbar + b);
+        if (!mbar_wait(addr, phase[b], max_tries)) *failed = 1u;
+    }
+    __syncthreads();
+    tc_fence_after();
+    if (!*failed && issued_any) {
+        // warp w reads lane quarter w % 4 (features 32 (w % 4) ..); warps 0-3 take dW0 and dW1, 4-7
+        // dW2..dW5
+        const uint32_t q = warp & 3u, m = 32u * q + (tid & 31u);
+        const uint32_t lane_base = (32u * q) << 16;
+        for (int acc_i = (warp < 4 ? 0 : 3); acc_i < (warp < 4 ? 3 : 7); ++acc_i) {
+            float v[64];
+            tmem_ld_x64(tmem + lane_base + 64u * (uint32_t)acc_i, v);
+            if (acc_i <= 1) {  // dW0: features m (block 0) or 128 + m (block 1), 64 outputs
+                float* G = grads + param_offset(0) + (size_t)(m + 128u * (uint32_t)acc_i) * kWidth;
+                for (int c = 0; c < kWidth; ++c)
+                    if (v[c] != 0.0f) atomicAdd(G + c, v[c]);
+            } else if (m < (uint32_t)kWidth) {  // dW_l, l = acc_i - 1: features m < 64
+                const int l = acc_i - 1, N = layer_n(l);
+                float* G = grads + param_offset(l) + (size_t)m * N;
+                for (int c = 0; c < N; ++c)
+                    if (v[c] != 0.0f) atomicAdd(G + c, v[c]);
             }
         }
     }
-    float* G = grads + param_offset(layer);
-    const int mrow = (layer == 0 ? 64 * job : 0) + 16 * warp + g;
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt) {
-        if (nt < N / 8) {
-            const int c = 8 * nt + 2 * t;
-            atomicAdd(G + (size_t)mrow * N + c, acc[nt][0]);
-            atomicAdd(G + (size_t)mrow * N + c + 1, acc[nt][1]);
-            atomicAdd(G + (size_t)(mrow + 8) * N + c, acc[nt][2]);
-            atomicAdd(G + (size_t)(mrow + 8) * N + c + 1, acc[nt][3]);
-        }
-    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kDwTmemCols));
+    if (tid == 0 && *failed) atomicOr(status, kStatusTimeout);
 }
 
 __global__ void k_adam(float* __restrict__ P, float* __restrict__ Gr, float* __restrict__ M, float* __restrict__ V,
@@ -573,6 +750,12 @@ __global__ void k_adam(float* __restrict__ P, float* __restrict__ Gr, float* __r
     P[i] -= lr * mh / (sqrtf(vh) + eps);
 }
 
+int launch_pack(liar_gpu_guide* G, cudaStream_t st, int bump) {
+    k_pack_umma<<<(kParams + 255) / 256, 256, 0, st>>>(G->params, G->umma_w, G->step, bump);
+    k_pack_umma_bwd<<<(kParams - param_offset(1) + 255) / 256, 256, 0, st>>>(G->params, G->umma_wb);
+    return cudaGetLastError() == cudaSuccess ? LIAR_OK : LIAR_ERR_CUDA;
+}
+
 int g_alloc(liar_gpu_ctx* ctx, liar_gpu_guide* G, size_t bytes, void** p, const char* what) {
     cudaError_t e = cudaMalloc(p, std::max<size_t>(bytes, 16));
     if (e != cudaSuccess) {
@@ -586,18 +769,15 @@ int g_alloc(liar_gpu_ctx* ctx, liar_gpu_guide* G, size_t bytes, void** p, const 
 
 int ensure_train_buffers(liar_gpu_ctx* ctx, liar_gpu_guide* G, size_t n) {
     if (G->cap >= n) return LIAR_OK;
-    for (void* p : {(void*)G->enc, (void*)G->act, (void*)G->delta, (void*)G->gout}) {
+    for (void* p : {(void*)G->act, (void*)G->delta, (void*)G->gout}) {
         if (!p) continue;
         cudaFree(p);
         G->buffers.erase(std::remove(G->buffers.begin(), G->buffers.end(), p), G->buffers.end());
     }
-    G->enc = G->act = G->delta = G->gout = nullptr;
+    G->act = G->delta = G->gout = nullptr;
     G->cap = 0;
     void* p = nullptr;
-    int rc = g_alloc(ctx, G, n * kEnc * 2, &p, "guide encodings");
-    if (rc) return rc;
-    G->enc = static_cast<__nv_bfloat16*>(p);
-    rc = g_alloc(ctx, G, n * 5 * kWidth * 2, &p, "guide activations");
+    int rc = g_alloc(ctx, G, n * 5 * kWidth * 2, &p, "guide activations");
     if (rc) return rc;
     G->act = static_cast<__nv_bfloat16*>(p);
     rc = g_alloc(ctx, G, n * 5 * kWidth * 2, &p, "guide deltas");
@@ -613,9 +793,11 @@ int ensure_train_buffers(liar_gpu_ctx* ctx, liar_gpu_guide* G, size_t n) {
 int smem_attrs(liar_gpu_ctx* ctx) {
     static int done_device = -1;
     if (done_device == ctx->device) return LIAR_OK;
-    cudaError_t e = cudaFuncSetAttribute(k_train_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEvalSmem);
+    cudaError_t e = cudaFuncSetAttribute(k_train_fwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwdTcSmem);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_train_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBwdBytes);
+        e = cudaFuncSetAttribute(k_train_bwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBwdTcSmem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_train_dw_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDwTcSmem);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_eval_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUmmaSmem);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "guide kernel attributes");
@@ -661,15 +843,25 @@ int guide_train(liar_gpu_ctx* ctx, liar_gpu_guide* G, const float* d_records, co
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "guide scalars");
     const int sms = ctx->num_sms;
     k_weight_sum<<<sms * 4, 256, 0, st>>>(d_records, d_count, n_max, G->scalars);
-    const unsigned tiles = (unsigned)((n_max + 31) / 32);
-    const unsigned fgrid = std::max(1u, std::min<unsigned>((tiles + kFwdWarps - 1) / kFwdWarps, (unsigned)sms));
-    const unsigned grid = std::max(1u, std::min<unsigned>((tiles + 3) / 4, (unsigned)sms * 2));
-    k_train_forward<<<fgrid, kFwdThreads, kEvalSmem, st>>>(G->frag_fwd, d_records, d_count, n_max, box, G->scalars, G->enc,
-                                                           G->act,
-                                                        G->gout, G->scalars + 1);
-    k_train_backward<<<grid, kThreads, kBwdBytes, st>>>(G->frag_bwd, d_count, n_max, G->act, G->gout, G->delta);
-    const dim3 dwg((unsigned)((n_max + kDwChunk - 1) / kDwChunk), 9);
-    k_train_dw<<<dwg, kThreads, 0, st>>>(d_count, n_max, G->enc, G->act, G->delta, G->gout, G->grads);
+    // the bounded waits of the tensor-core kernels (the fault test: no MMA, a short limit)
+    const bool wait_test = ctx->fault_test == LIAR_FAULT_TEST_GUIDE_WAIT;
+    const uint32_t tries = wait_test ? 1u << 16 : 1u << 24;
+    const int mma = wait_test ? 0 : 1;
+    uint32_t* status = ctx->d_scratch + kStatusWord;
+    const size_t tiles = (n_max + kTcRows - 1) / kTcRows;
+    const unsigned tgrid = (unsigned)std::max<size_t>(1, std::min<size_t>((tiles + kTcSlots - 1) / kTcSlots, (size_t)sms));
+    k_train_fwd_tc<<<tgrid, kTcThreads, kFwdTcSmem, st>>>(G->umma_w, d_records, d_count, n_max, box, G->scalars, G->act,
+                                                         G->gout, G->scalars + 1, status, tries, mma);
+    const unsigned bgrid =
+        (unsigned)std::max<size_t>(1, std::min<size_t>((tiles + kTcSlots - 1) / kTcSlots, (size_t)sms * 3));
+    k_train_bwd_tc<<<bgrid, kTcThreads, kBwdTcSmem, st>>>(G->umma_wb, d_count, n_max, G->act, G->gout, G->delta, status,
+                                                         tries, mma);
+    // weight gradients: one CTA per SM, each over a contiguous run of whole 64-record stages
+    const size_t stages = (n_max + kDwRecords - 1) / kDwRecords;
+    const size_t per_cta = ((stages + sms - 1) / sms) * kDwRecords;
+    const unsigned dgrid = (unsigned)std::max<size_t>(1, (n_max + per_cta - 1) / per_cta);
+    k_train_dw_tc<<<dgrid, kDwThreads, kDwTcSmem, st>>>(d_records, d_count, n_max, box, G->act, G->delta, G->gout,
+                                                       G->grads, per_cta, status, tries, mma);
     const float lr = apply ? (G->cfg.learning_rate > 0 ? G->cfg.learning_rate : 5e-3f) : 0.0f;
     k_adam<<<(kParams + 255) / 256, 256, 0, st>>>(G->params, G->grads, G->adam_m, G->adam_v, G->step, lr, 0.9f, 0.99f,
                                                   1e-8f, d_grad_out);
@@ -721,12 +913,10 @@ extern "C" int liar_gpu_guide_create(liar_gpu_ctx* ctx, const liar_guide_config*
         G->step = reinterpret_cast<uint32_t*>(f + 4 * kParams);
         G->scalars = f + 4 * kParams + 4;
     }
-    if (!rc) rc = g_alloc(ctx, G, kFwdBytes, &p, "guide fragments");
-    if (!rc) G->frag_fwd = static_cast<uint2*>(p);
-    if (!rc) rc = g_alloc(ctx, G, kBwdBytes, &p, "guide fragments");
-    if (!rc) G->frag_bwd = static_cast<uint2*>(p);
     if (!rc) rc = g_alloc(ctx, G, kUmmaWBytes, &p, "guide operand images");
     if (!rc) G->umma_w = static_cast<unsigned char*>(p);
+    if (!rc) rc = g_alloc(ctx, G, kUmmaWbBytes, &p, "guide operand images");
+    if (!rc) G->umma_wb = static_cast<unsigned char*>(p);
     if (!rc) {
         std::vector<float> P;
         init_params(P, cfg->seed);

@@ -4,16 +4,11 @@
 // previous vertex) -> frequency encoding (per input: sin and cos of pi * 2^(f/2) * x, f = 0..11, then
 // the 9 raw inputs; 225 features, padded to 256) -> 5 ReLU layers of 64 -> 48 outputs (40 used):
 // 8 von Mises-Fisher lobes, each (mean direction m 3, log concentration 1, logit 1). No biases.
-// Weights are bf16, accumulation f32. Inference runs on tcgen05 (guide_umma.cuh); the training
-// forward and backward here run per warp on mma.sync m16n8k16, with the activations in registers
-// between layers: the f32 accumulator fragment of two adjacent 8-column tiles is, element for
-// element, the A fragment of the next layer's 16-column k tile (no shared-memory round trip), and
-// the bf16 activations are stored for the backward pass.
+// Weights are bf16, accumulation f32. Inference and training run on tcgen05 (guide_umma.cuh,
+// guide.cu).
 //
-// Parameters (f32 master copy, row-major [in][out]): W0 256x64, W1..W4 64x64, W5 64x48.
-// For the kernels they are repacked as bf16 B fragments in lane order ("fwd": B = W_l,
-// "bwd": B = W_l^T for l = 1..5), one uint2 per lane per 16x8 tile, so a warp loads a tile
-// with one conflict-free 64-bit shared-memory access.
+// Parameters (f32 master copy, row-major [in][out]): W0 256x64, W1..W4 64x64, W5 64x48. For the
+// kernels they are repacked as bf16 tcgen05 B-operand images (guide.cu k_pack_umma, k_pack_umma_bwd).
 #pragma once
 #include <cuda_bf16.h>
 #include <stdint.h>
@@ -38,22 +33,6 @@ __host__ __device__ constexpr int param_offset(int l) {
 }
 constexpr int kParams = param_offset(6);  // 35840
 
-// fragment tile counts and offsets (in tiles of 32 uint2): W0 has 16 x 8 tiles, W1..W4 4 x 8, W5 4 x 6
-__host__ __device__ constexpr int fwd_tiles(int l) { return (layer_k(l) / 16) * (layer_n(l) / 8); }
-__host__ __device__ constexpr int fwd_tile_offset(int l) {
-    return l == 0 ? 0 : (l <= 5 ? 128 + 32 * (l - 1) : 128 + 32 * 4 + 24);
-}
-constexpr int kFwdTiles = fwd_tile_offset(6);  // 280
-// backward: B = W_l^T (k = out features of W_l, n = its 64 in features), l = 1..5: 4 x 8 tiles
-// for W1..W4, 3 x 8 for W5
-__host__ __device__ constexpr int bwd_tiles(int l) { return (layer_n(l) / 16) * (kWidth / 8); }
-__host__ __device__ constexpr int bwd_tile_offset(int l) { return l <= 5 ? 32 * (l - 1) : 32 * 4 + 24; }
-constexpr int kBwdTiles = bwd_tile_offset(6);  // 152
-static_assert(fwd_tile_offset(5) + fwd_tiles(5) == kFwdTiles, "forward fragment table");
-static_assert(bwd_tile_offset(5) + bwd_tiles(5) == kBwdTiles, "backward fragment table");
-constexpr size_t kFwdBytes = (size_t)kFwdTiles * 32 * 8;
-constexpr size_t kBwdBytes = (size_t)kBwdTiles * 32 * 8;
-
 #ifdef __CUDACC__
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
@@ -64,21 +43,11 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
 __device__ __forceinline__ float bf16_lo(uint32_t v) { return __uint_as_float(v << 16); }
 __device__ __forceinline__ float bf16_hi(uint32_t v) { return __uint_as_float(v & 0xffff0000u); }
 
-__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint2 b) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};\n"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b.x), "r"(b.y));
-}
-
-// The encoding of one row, written by its lane into the warp's shared buffer (row stride kEncLd
-// bf16, padded so that the eight 16-byte rows an ldmatrix reads fall on distinct banks). Per input
-// two sincospif calls (pi x and pi x sqrt(2)); the other frequencies by the doubling formulas
-// sin 2a = 2 sin a cos a, cos 2a = cos^2 a - sin^2 a (x fl(sqrt 2) 2^k is exactly fl(x fl(sqrt 2)) 2^k,
-// so these are the angles of the definition; the recurrence adds ~1e-6 absolute error, far below bf16).
-constexpr int kEncLd = kEnc + 8;
-constexpr size_t kEncWarpBytes = (size_t)32 * kEncLd * 2;
+// The encoding of one row as 256 bf16 in a row-major buffer (encode_row_umma of guide_umma.cuh
+// writes the same values into the K-major operand layout). Per input two sincospif calls (pi x and
+// pi x sqrt(2)); the other frequencies by the doubling formulas sin 2a = 2 sin a cos a,
+// cos 2a = cos^2 a - sin^2 a (x fl(sqrt 2) 2^k is exactly fl(x fl(sqrt 2)) 2^k, so these are the
+// angles of the definition; the recurrence adds ~1e-6 absolute error, far below bf16).
 
 __device__ __forceinline__ void encode_row(const float* x, __nv_bfloat16* row) {
     uint32_t* dst = reinterpret_cast<uint32_t*>(row);
@@ -106,120 +75,6 @@ __device__ __forceinline__ void encode_row(const float* x, __nv_bfloat16* row) {
     raw[4] = pack_bf16(x[8], 0.0f);
 #pragma unroll
     for (int c = 5; c < (kEnc - kIn * 2 * kFreq) / 2; ++c) raw[c] = 0u;
-}
-
-__device__ __forceinline__ void ldmatrix_x4(uint32_t (&r)[4], const void* smem_ptr) {
-    const uint32_t a = (uint32_t)__cvta_generic_to_shared(smem_ptr);
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(a));
-}
-
-// one warp, 32 rows = two m16 tiles. enc: the warp's [32][kEncLd] bf16 encodings (encode_row).
-// Returns the output-layer accumulators out[mt][nt][4] (6 n tiles of 8). If S.base is set, stores
-// the bf16 activations h_1..h_5 at S.base[(l-1) * ld_layer + row * 64 + col] for valid rows.
-struct ActStore {
-    __nv_bfloat16* base;  // null: no store
-    size_t ld_layer;      // elements between layers
-    uint32_t row0;        // first row of this warp in the store
-    uint32_t n_valid;     // rows of this warp that exist
-};
-
-__device__ __forceinline__ void store_frag_row(const ActStore& S, int layer, uint32_t row, int col, uint32_t v) {
-    if (S.base && row < S.n_valid)
-        *reinterpret_cast<uint32_t*>(S.base + (size_t)(layer - 1) * S.ld_layer + (size_t)(S.row0 + row) * kWidth + col) = v;
-}
-
-__device__ __forceinline__ void mlp_forward_warp(const __nv_bfloat16* enc, const uint2* __restrict__ wf,
-                                                 float (&out)[2][6][4], const ActStore& S) {
-    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    float acc[2][8][4];
-    uint32_t a[2][4][4];  // next layer's A fragments [mt][kk][reg]
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-        for (int nt = 0; nt < 8; ++nt)
-#pragma unroll
-            for (int r = 0; r < 4; ++r) acc[mt][nt][r] = 0.0f;
-    // layer 0: A fragments by ldmatrix from the encodings (lane l addresses row l % 16, column
-    // half 8 (l / 16) of the 16 x 16 tile)
-    const __nv_bfloat16* arow = enc + (lane & 15) * kEncLd + 8 * (lane >> 4);
-#pragma unroll 2
-    for (int kk = 0; kk < kEnc / 16; ++kk) {
-        uint32_t a0[2][4];
-        ldmatrix_x4(a0[0], arow + 16 * kk);
-        ldmatrix_x4(a0[1], arow + 16 * kEncLd + 16 * kk);
-        const uint2* wt = wf + (size_t)(kk * 8) * 32 + lane;
-#pragma unroll
-        for (int nt = 0; nt < 8; ++nt) {
-            const uint2 b = wt[nt * 32];
-            mma_bf16(acc[0][nt], a0[0], b);
-            mma_bf16(acc[1][nt], a0[1], b);
-        }
-    }
-    // hidden layers 1..4 and the output layer 5
-#pragma unroll 1
-    for (int l = 1; l <= 5; ++l) {
-        // ReLU, round to bf16, regroup as A fragments (and store h_l)
-#pragma unroll
-        for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-            for (int kk = 0; kk < 4; ++kk) {
-                const float* e = acc[mt][2 * kk];
-                const float* o = acc[mt][2 * kk + 1];
-                a[mt][kk][0] = pack_bf16(fmaxf(e[0], 0.0f), fmaxf(e[1], 0.0f));
-                a[mt][kk][1] = pack_bf16(fmaxf(e[2], 0.0f), fmaxf(e[3], 0.0f));
-                a[mt][kk][2] = pack_bf16(fmaxf(o[0], 0.0f), fmaxf(o[1], 0.0f));
-                a[mt][kk][3] = pack_bf16(fmaxf(o[2], 0.0f), fmaxf(o[3], 0.0f));
-                if (S.base) {
-                    const uint32_t r0 = 16 * mt + g;
-                    store_frag_row(S, l, r0, 16 * kk + 2 * t, a[mt][kk][0]);
-                    store_frag_row(S, l, r0 + 8, 16 * kk + 2 * t, a[mt][kk][1]);
-                    store_frag_row(S, l, r0, 16 * kk + 8 + 2 * t, a[mt][kk][2]);
-                    store_frag_row(S, l, r0 + 8, 16 * kk + 8 + 2 * t, a[mt][kk][3]);
-                }
-            }
-        const int n_nt = l == 5 ? kOut / 8 : 8;
-#pragma unroll
-        for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-            for (int nt = 0; nt < 8; ++nt)
-#pragma unroll
-                for (int r = 0; r < 4; ++r) acc[mt][nt][r] = 0.0f;
-        const uint2* wl = wf + (size_t)fwd_tile_offset(l) * 32 + lane;
-#pragma unroll
-        for (int kk = 0; kk < 4; ++kk)
-#pragma unroll
-            for (int nt = 0; nt < 8; ++nt) {
-                if (nt < n_nt) {
-                    const uint2 b = wl[(kk * n_nt + nt) * 32];
-                    mma_bf16(acc[0][nt], a[0][kk], b);
-                    mma_bf16(acc[1][nt], a[1][kk], b);
-                }
-            }
-    }
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-        for (int nt = 0; nt < 6; ++nt)
-#pragma unroll
-            for (int r = 0; r < 4; ++r) out[mt][nt][r] = acc[mt][nt][r];
-}
-
-// writes the warp's raw outputs to a per-warp [32][kOutStride] f32 scratch
-constexpr int kOutStride = kOut + 1;
-__device__ __forceinline__ void scatter_out(const float (&out)[2][6][4], float* s) {
-    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-        for (int nt = 0; nt < 6; ++nt) {
-            const int r = 16 * mt + g, c = 8 * nt + 2 * t;
-            s[r * kOutStride + c] = out[mt][nt][0];
-            s[r * kOutStride + c + 1] = out[mt][nt][1];
-            s[(r + 8) * kOutStride + c] = out[mt][nt][2];
-            s[(r + 8) * kOutStride + c + 1] = out[mt][nt][3];
-        }
 }
 
 #endif  // __CUDACC__

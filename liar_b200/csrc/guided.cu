@@ -39,7 +39,6 @@ const liar_gpu_mesh* scene_mesh(const liar_gpu_scene* s);
 int scene_device(const liar_gpu_scene* s);
 }  // namespace rt
 namespace guide {
-const uint2* guide_frag_fwd(const liar_gpu_guide* g);
 const liar_guide_config& guide_config(const liar_gpu_guide* g);
 int guide_device(const liar_gpu_guide* g);
 int guide_train(liar_gpu_ctx* ctx, liar_gpu_guide* g, const float* d_records, const uint32_t* d_count, size_t n_max,
