@@ -105,12 +105,14 @@ __global__ void k_pack_umma(const float* __restrict__ P, unsigned char* __restri
         __float2bfloat16_rn(P[i]);
 }
 
-// ---- inference on tcgen05: two slots of 128 rows per CTA (guide_umma.cuh)
+// ---- inference on tcgen05: four slots of 128 rows per CTA (guide_umma.cuh)
+// Layer 0 runs as four K-chunks over the two halves of the slot's buffer, each chunk committed to
+// the half's own mbarrier; a half is rewritten only after the commit of the chunk that read it.
 // Every mbarrier wait is bounded by max_tries polls. A wait that runs out records the timeout,
-// waits once more (bounded again) for the commit it was waiting for, so that no MMA still writes
+// waits once more (bounded again) for every commit still outstanding, so that no MMA still writes
 // the accumulator, and the CTA frees its TMEM and leaves. issue_mma = 0 is the timeout test: no
 // MMA and no commit are issued, so the first wait runs out with nothing in flight.
-__global__ void __launch_bounds__(kTcThreads, 1) k_eval_tc(const unsigned char* __restrict__ w_img,
+__global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* __restrict__ w_img,
                                                            const float* __restrict__ in, size_t n, Box box,
                                                            float* __restrict__ mix, int stride,
                                                            uint32_t* __restrict__ status, uint32_t max_tries,
@@ -118,110 +120,161 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_eval_tc(const unsigned char* 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     unsigned char* sw = smem;
-    uint64_t* mbar_all = reinterpret_cast<uint64_t*>(sw + kUmmaWBytes + (size_t)kTcSlots * kUmmaA0Bytes);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar_all + kTcSlots);
+    uint64_t* mbar_all = reinterpret_cast<uint64_t*>(sw + kUmmaWBytes + (size_t)kEvSlots * (kEvBuf + kEvIn));
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar_all + 2 * kEvSlots);
     volatile uint32_t* failed = tmem_slot + 1;  // one flag per slot
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
     const uint32_t slot = tid >> 7, r = tid & 127u;  // this thread's slot and row within the slot's tile
-    unsigned char* buf = sw + kUmmaWBytes + slot * kUmmaA0Bytes;
+    unsigned char* buf = sw + kUmmaWBytes + slot * kEvBuf;
+    float* stage_in = reinterpret_cast<float*>(sw + kUmmaWBytes + (size_t)kEvSlots * kEvBuf + slot * kEvIn);
     {
         const uint4* s = reinterpret_cast<const uint4*>(w_img);
         uint4* d = reinterpret_cast<uint4*>(sw);
-        for (uint32_t i = tid; i < kUmmaWBytes / 16; i += kTcThreads) d[i] = s[i];
+        for (uint32_t i = tid; i < kUmmaWBytes / 16; i += kEvThreads) d[i] = s[i];
     }
     if (tid == 0) {
-        for (int k = 0; k < kTcSlots; ++k)
+        for (int k = 0; k < 2 * kEvSlots; ++k)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(mbar_all + k)));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        failed[0] = failed[1] = 0u;
+        for (int k = 0; k < kEvSlots; ++k) failed[k] = 0u;
     }
     if (warp == 0) {
         const uint32_t sa = (uint32_t)__cvta_generic_to_shared(tmem_slot);
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sa), "r"(kTcTmemCols));
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sa), "r"(kEvTmemCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     fence_async_smem();
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    const uint32_t tmem = *tmem_slot + 64u * slot;                 // the slot's accumulator columns
-    const uint32_t taddr = tmem + ((32u * (warp & 3u)) << 16);     // the warp's lane quarter
-    const uint32_t mbar_addr = (uint32_t)__cvta_generic_to_shared(mbar_all + slot);
+    const uint32_t tmem = *tmem_slot + 64u * slot;              // the slot's accumulator columns
+    const uint32_t taddr = tmem + ((32u * (warp & 3u)) << 16);  // the warp's lane quarter
+    const uint32_t mb[2] = {(uint32_t)__cvta_generic_to_shared(mbar_all + 2 * slot),
+                            (uint32_t)__cvta_generic_to_shared(mbar_all + 2 * slot + 1)};
     const uint32_t sw_addr = (uint32_t)__cvta_generic_to_shared(sw);
     const uint32_t buf_addr = (uint32_t)__cvta_generic_to_shared(buf);
     auto slot_sync = [&]() { asm volatile("bar.sync %0, 128;" ::"r"(1u + slot) : "memory"); };
-    uint32_t phase = 0;
+    uint32_t phase[2] = {0u, 0u};
+    bool pending[2] = {false, false};  // a commit to the half's mbarrier not yet waited for
+    // wait for half h's outstanding commit; false (for the whole slot) when any thread gave up
+    auto wait_half = [&](int h) -> bool {
+        if (!mbar_wait(mb[h], phase[h], max_tries)) failed[slot] = 1u;
+        slot_sync();
+        if (failed[slot]) return false;
+        phase[h] ^= 1u;
+        pending[h] = false;
+        return true;
+    };
+    // hand the slot's operand to the tensor core (the writes of every thread are visible to the
+    // async proxy and the accumulator reads are done) and, from thread 0, issue K / 16 MMAs
+    auto issue = [&](uint32_t a_addr, uint32_t a_sbo, uint32_t b_addr, uint32_t b_sbo, uint32_t ksteps, uint32_t N,
+                     bool acc0, int h) {
+        fence_async_smem();
+        tc_fence_before();
+        slot_sync();
+        tc_fence_after();
+        if (r == 0 && issue_mma) {
+            const uint32_t idesc = umma_idesc(N);
+            for (uint32_t j = 0; j < ksteps; ++j)
+                umma_bf16(tmem, umma_smem_desc(a_addr + 256u * j, a_sbo), umma_smem_desc(b_addr + 256u * j, b_sbo), idesc,
+                          (acc0 || j > 0) ? 1u : 0u);
+            umma_commit(mb[h]);
+        }
+        pending[h] = true;
+    };
     const size_t n_tiles = (n + kTcRows - 1) / kTcRows;
-    for (size_t tile = (size_t)blockIdx.x * kTcSlots + slot; tile < n_tiles; tile += (size_t)gridDim.x * kTcSlots) {
-        const size_t row = tile * kTcRows + r;
+    bool ok = true;
+    for (size_t tile = (size_t)blockIdx.x * kEvSlots + slot; ok && tile < n_tiles; tile += (size_t)gridDim.x * kEvSlots) {
+        const size_t row0 = tile * kTcRows;
+        const uint32_t rows = n - row0 < (size_t)kTcRows ? (uint32_t)(n - row0) : (uint32_t)kTcRows;
+        // the tile's inputs, coalesced, through shared memory (the previous tile's readers have passed
+        // the slot barriers since)
+        for (uint32_t i = r; i < rows * kIn; i += 128u) stage_in[i] = __ldg(in + row0 * kIn + i);
+        slot_sync();
         float x[kIn];
-        if (row < n) normalise_input(in + row * kIn, box.lo, box.inv_ext, x);
+        if (r < rows) normalise_input(stage_in + r * kIn, box.lo, box.inv_ext, x);
         else
             for (int c = 0; c < kIn; ++c) x[c] = 0.0f;
-        encode_row_umma(x, buf, r);
-        float v[64];
-        bool ok = true;
-        for (int l = 0; l < kLayers; ++l) {
-            // the layer's A operand is in shared memory and the slot's last accumulator reads are
-            // done: hand the operand to the tensor core
-            fence_async_smem();
-            tc_fence_before();
-            slot_sync();
-            tc_fence_after();
-            if (r == 0 && issue_mma) {
-                const uint32_t K = (uint32_t)layer_k(l), N = (uint32_t)layer_n(l);
-                const uint32_t b_base = sw_addr + umma_w_offset(l);
-                const uint32_t idesc = umma_idesc(N);
-                for (uint32_t j = 0; j < K / 16; ++j)
-                    umma_bf16(tmem, umma_smem_desc(buf_addr + 256u * j, (K / 8) * 128u),
-                              umma_smem_desc(b_base + 256u * j, (K / 8) * 128u), idesc, j > 0 ? 1u : 0u);
-                umma_commit(mbar_addr);
-            }
-            if (!mbar_wait(mbar_addr, phase, max_tries)) failed[slot] = 1u;
-            slot_sync();  // the slot agrees on completion before anyone reads the accumulator
-            if (failed[slot]) {
-                // drain: the commit this slot gave up on, if any, before the TMEM is freed
-                if (issue_mma) mbar_wait(mbar_addr, phase, max_tries);
+        // layer 0: chunk c's encodings into half c % 2 once the chunk before last has been consumed
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int h = c & 1;
+            if (c >= 2 && !wait_half(h)) {
                 ok = false;
                 break;
             }
-            phase ^= 1u;
+            encode_chunk_umma(x, buf + h * kEvHalf, r, c);
+            issue(buf_addr + h * kEvHalf, 1024u, sw_addr + umma_w_offset(0) + 1024u * c, (kEnc / 8) * 128u, 4u, kWidth,
+                  c > 0, h);
+        }
+        if (ok) ok = wait_half(0) && wait_half(1);
+        // hidden layers and the output layer from half 0; v holds the accumulator 32 columns at a time
+        for (int l = 1; ok && l <= kLayers; ++l) {
             tc_fence_after();
-            tmem_ld_x64(taddr, v);
-            if (l < kLayers - 1) {
-                // ReLU, bf16, the next layer's A operand (row r, 8 chunks of 8 columns) in the slot's
-                // buffer, whose encodings the finished layer-0 MMA no longer needs
-                unsigned char* dst = buf + (r >> 3) * (kWidth / 8) * 128u + (r & 7u) * 16u;
+            unsigned char* dst = buf + (r >> 3) * (kWidth / 8) * 128u + (r & 7u) * 16u;
+            if (l < kLayers) {
+                // ReLU, bf16, the next layer's A operand (row r, 8 chunks of 8 columns)
 #pragma unroll
-                for (int c = 0; c < kWidth / 8; ++c) {
-                    const float* q = v + 8 * c;
-                    *reinterpret_cast<uint4*>(dst + c * 128u) =
-                        make_uint4(pack_bf16(fmaxf(q[0], 0.0f), fmaxf(q[1], 0.0f)), pack_bf16(fmaxf(q[2], 0.0f), fmaxf(q[3], 0.0f)),
-                                   pack_bf16(fmaxf(q[4], 0.0f), fmaxf(q[5], 0.0f)), pack_bf16(fmaxf(q[6], 0.0f), fmaxf(q[7], 0.0f)));
+                for (int half = 0; half < 2; ++half) {
+                    float v[32];
+                    tmem_ld_32x32b<32>(taddr + 32u * half, v);
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        const float* q = v + 8 * c;
+                        *reinterpret_cast<uint4*>(dst + (4 * half + c) * 128u) = make_uint4(
+                            pack_bf16(fmaxf(q[0], 0.0f), fmaxf(q[1], 0.0f)), pack_bf16(fmaxf(q[2], 0.0f), fmaxf(q[3], 0.0f)),
+                            pack_bf16(fmaxf(q[4], 0.0f), fmaxf(q[5], 0.0f)), pack_bf16(fmaxf(q[6], 0.0f), fmaxf(q[7], 0.0f)));
+                    }
+                }
+                issue(buf_addr, (kWidth / 8) * 128u, sw_addr + umma_w_offset(l), (kWidth / 8) * 128u, kWidth / 16,
+                      (uint32_t)layer_n(l), false, 0);
+                ok = wait_half(0);
+            } else {
+                // the mixture of row r into the staging rows (pitch stride + 4 floats), then the
+                // slot's rows leave as one contiguous, coalesced block
+                float o[kOutUsed];
+                tmem_ld_32x32b<32>(taddr, o);
+                tmem_ld_32x32b<8>(taddr + 32u, o + 32);
+                const uint32_t pitch = (uint32_t)stride + 4u;
+                float* srow = reinterpret_cast<float*>(buf) + r * pitch;
+                Lobe lobes[kLobes];
+                float w[kLobes];
+                mixture_from_raw(o, lobes, w);
+#pragma unroll
+                for (int k = 0; k < kLobes; ++k)
+                    *reinterpret_cast<float4*>(srow + 4 * k) = make_float4(lobes[k].mx, lobes[k].my, lobes[k].mz, lobes[k].kappa);
+                *reinterpret_cast<float4*>(srow + 32) = make_float4(w[0], w[1], w[2], w[3]);
+                *reinterpret_cast<float4*>(srow + 36) = make_float4(w[4], w[5], w[6], w[7]);
+                if (stride == kMixRender) {
+                    float a[kLobes];
+#pragma unroll
+                    for (int k = 0; k < kLobes; ++k) a[k] = w[k] * vmf_norm(lobes[k].kappa);
+                    *reinterpret_cast<float4*>(srow + 40) = make_float4(a[0], a[1], a[2], a[3]);
+                    *reinterpret_cast<float4*>(srow + 44) = make_float4(a[4], a[5], a[6], a[7]);
+                }
+                slot_sync();
+                const uint32_t per_row = (uint32_t)stride / 4u, total = rows * per_row;
+                float4* gdst = reinterpret_cast<float4*>(mix + row0 * (size_t)stride);
+                for (uint32_t i = r; i < total; i += 128u) {
+                    const uint32_t q = i / per_row, c4 = i - q * per_row;
+                    gdst[i] = *reinterpret_cast<const float4*>(reinterpret_cast<const float*>(buf) + q * pitch + 4u * c4);
                 }
             }
         }
-        if (!ok) break;
-        if (row < n) {
-            Lobe lobes[kLobes];
-            float w[kLobes];
-            mixture_from_raw(v, lobes, w);
-            float4* dst = reinterpret_cast<float4*>(mix + row * (size_t)stride);
-            for (int l = 0; l < kLobes; ++l) dst[l] = make_float4(lobes[l].mx, lobes[l].my, lobes[l].mz, lobes[l].kappa);
-            dst[8] = make_float4(w[0], w[1], w[2], w[3]);
-            dst[9] = make_float4(w[4], w[5], w[6], w[7]);
-            if (stride == kMixRender) {
-                float a[kLobes];
-                for (int l = 0; l < kLobes; ++l) a[l] = w[l] * vmf_norm(lobes[l].kappa);
-                dst[10] = make_float4(a[0], a[1], a[2], a[3]);
-                dst[11] = make_float4(a[4], a[5], a[6], a[7]);
-            }
-        }
+    }
+    if (!ok && issue_mma) {
+        // drain: the commits this slot gave up on, before the TMEM is freed
+        for (int h = 0; h < 2; ++h)
+            if (pending[h]) mbar_wait(mb[h], phase[h], max_tries);
     }
     tc_fence_before();
     __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tmem_slot), "r"(kTcTmemCols));
-    if (tid == 0 && (failed[0] | failed[1])) atomicOr(status, kStatusTimeout);
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tmem_slot), "r"(kEvTmemCols));
+    if (tid == 0) {
+        uint32_t f = 0;
+        for (int k = 0; k < kEvSlots; ++k) f |= failed[k];
+        if (f) atomicOr(status, kStatusTimeout);
+    }
 }
 
 // ---- training
@@ -799,7 +852,7 @@ int smem_attrs(liar_gpu_ctx* ctx) {
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_train_dw_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDwTcSmem);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_eval_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUmmaSmem);
+        e = cudaFuncSetAttribute(k_eval_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEvSmem);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "guide kernel attributes");
     done_device = ctx->device;
     return LIAR_OK;
@@ -998,11 +1051,12 @@ int liar_gpu::guide::guide_eval(liar_gpu_ctx* ctx, const liar_gpu_guide* G, cons
     if (rc) return rc;
     if (stride != kOutUsed && stride != kMixRender) return ctx_fail(ctx, LIAR_ERR_INVALID, "mixture stride %d", stride);
     const size_t tiles = (n + kTcRows - 1) / kTcRows;
-    const unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>((tiles + kTcSlots - 1) / kTcSlots, (size_t)ctx->num_sms));
+    if ((uintptr_t)d_mixture & 15u) return ctx_fail(ctx, LIAR_ERR_INVALID, "mixture output not 16-byte aligned");
+    const unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>((tiles + kEvSlots - 1) / kEvSlots, (size_t)ctx->num_sms));
     // the bounded waits' limit: 2^24 polls, far beyond a layer's MMAs; the timeout test
     // (liar_gpu_set_fault_test) issues no MMA and gives up after 2^16 polls
     const bool wait_test = ctx->fault_test == LIAR_FAULT_TEST_GUIDE_WAIT;
-    k_eval_tc<<<grid, kTcThreads, kUmmaSmem, st>>>(G->umma_w, d_inputs, n, make_box(G->cfg), d_mixture, stride,
+    k_eval_tc<<<grid, kEvThreads, kEvSmem, st>>>(G->umma_w, d_inputs, n, make_box(G->cfg), d_mixture, stride,
                                                    ctx->d_scratch + kStatusWord, wait_test ? 1u << 16 : 1u << 24,
                                                    wait_test ? 0 : 1);
     return ctx_cuda(ctx, cudaGetLastError(), "guide evaluation");

@@ -1,14 +1,15 @@
 // guide_umma.cuh -- the guide network's inference on the 5th-generation tensor cores (tcgen05).
 //
-// A CTA runs two independent 4-warp slots, each evaluating 128 rows at a time (M = 128; thread r
-// of the slot owns row r), so that one slot's SIMT work overlaps the other's tensor-core work.
+// A CTA runs independent 4-warp slots (four for inference, two in training), each evaluating 128
+// rows at a time (M = 128; thread r of the slot owns row r), so that one slot's SIMT work overlaps
+// the others' tensor-core work.
 //   * the weights live in shared memory as the B operands of every layer, bf16, K-major, in the
 //     canonical no-swizzle layout: element (n, k) of a layer with K inputs at
 //     (n / 8) * (K / 8) * 128 + (k / 8) * 128 + (n % 8) * 16 + (k % 8) * 2 bytes, i.e. 8x16-byte core
 //     matrices with the K-adjacent ones 128 B apart (leading byte offset) and the 8-row groups
 //     (K / 8) * 128 B apart (stride byte offset);
-//   * the activations (A operands) use the same layout: 128 x 256 for the encodings, 128 x 64 for
-//     the hidden layers;
+//   * the activations (A operands) use the same layout: 128 x 256 for the encodings (inference
+//     streams them as four 128 x 64 K-chunks), 128 x 64 for the hidden layers;
 //   * a slot's accumulator is 128 lanes x 64 f32 columns of tensor memory; its thread 0 issues each layer
 //     as K / 16 tcgen05.mma (kind::f16, bf16 inputs, f32 accumulation) and commits them to an
 //     mbarrier; every warp then reads its 32 lanes (tcgen05.ld 32x32b.x64), applies ReLU, and
@@ -36,9 +37,19 @@ __host__ __device__ constexpr uint32_t umma_w_offset(int l) {
 constexpr uint32_t kUmmaWBytes = umma_w_offset(6);  // 71680
 constexpr uint32_t kUmmaA0Bytes = (uint32_t)kTcRows * kEnc * 2;    // 65536
 constexpr uint32_t kUmmaA1Bytes = (uint32_t)kTcRows * kWidth * 2;  // 16384
-// per slot one operand buffer: the encodings for layer 0, then (once layer 0 has finished) the
-// hidden activations in its first kUmmaA1Bytes
-constexpr size_t kUmmaSmem = 1024 + kUmmaWBytes + (size_t)kTcSlots * kUmmaA0Bytes + 128;
+
+// Inference runs four slots per CTA (16 warps per SM). A slot's operand buffer holds two 128 x 64
+// halves: layer 0's K = 256 is fed to the tensor core in four K-chunks of 64 encodings, chunk c in
+// half c % 2 (the encodings of chunk c + 1 are written while chunk c's MMAs run), and the hidden
+// activations use half 0. After the last layer the buffer stages the slot's 128 output rows (row
+// pitch padded by 4 floats) for coalesced stores; a second area stages the 128 input rows.
+constexpr int kEvSlots = 4;
+constexpr int kEvThreads = 128 * kEvSlots;
+constexpr uint32_t kEvTmemCols = 64 * kEvSlots;
+constexpr uint32_t kEvHalf = (uint32_t)kTcRows * 64 * 2;  // 16384
+constexpr uint32_t kEvBuf = 2 * kEvHalf;                   // 32768
+constexpr uint32_t kEvIn = (uint32_t)kTcRows * kIn * 4;     // 4608
+constexpr size_t kEvSmem = 1024 + kUmmaWBytes + (size_t)kEvSlots * (kEvBuf + kEvIn) + 128;
 
 // byte offset of element (row, k) in a K-major no-swizzle operand with K columns
 __host__ __device__ __forceinline__ uint32_t umma_offset(uint32_t row, uint32_t k, uint32_t K) {
@@ -115,6 +126,38 @@ __device__ __forceinline__ void tmem_ld_x64(uint32_t taddr, float (&v)[64]) {
     for (int i = 0; i < 64; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+template <int N>
+__device__ __forceinline__ void tmem_ld_32x32b(uint32_t taddr, float* v);
+
+// columns [c, c + 32) and [c, c + 8) of the warp's 32 lanes
+template <>
+__device__ __forceinline__ void tmem_ld_32x32b<32>(uint32_t taddr, float* v) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+template <>
+__device__ __forceinline__ void tmem_ld_32x32b<8>(uint32_t taddr, float* v) {
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -149,6 +192,47 @@ __device__ __forceinline__ void encode_row_umma(const float* x, unsigned char* a
     *reinterpret_cast<uint4*>(row + 28 * 128u) = make_uint4(pack_bf16(x[8], 0.0f), 0u, 0u, 0u);
 #pragma unroll
     for (int c = 29; c < kEnc / 8; ++c) *reinterpret_cast<uint4*>(row + c * 128u) = make_uint4(0u, 0u, 0u, 0u);
+}
+
+// The K-chunk c (encoding columns 64 c .. 64 c + 63) of row r, written into a 128 x 64 K-major
+// operand buffer (the same values as encode_row_umma): the inputs whose 24 columns (3 core
+// columns 3 d .. 3 d + 2) meet the chunk are encoded (an input that straddles two chunks is
+// encoded in both), chunk 3 also holds the raw inputs and the zero padding.
+__device__ __forceinline__ void encode_chunk_umma(const float* x, unsigned char* a, uint32_t r, int c) {
+    unsigned char* row = a + (r >> 3) * 8u * 128u + (r & 7u) * 16u;
+    const int lo = 8 * c, hi = 8 * c + 7;  // the chunk's core columns
+#pragma unroll
+    for (int d = 0; d < kIn; ++d) {
+        if (3 * d + 2 < lo || 3 * d > hi) continue;
+        float s0, c0, s1, c1;
+        sincospif(x[d], &s0, &c0);
+        sincospif(x[d] * 1.41421356237309515f, &s1, &c1);
+        uint32_t w[12];
+#pragma unroll
+        for (int k = 0; k < kFreq / 2; ++k) {
+            w[2 * k] = pack_bf16(s0, c0);
+            w[2 * k + 1] = pack_bf16(s1, c1);
+            const float ns0 = 2.0f * s0 * c0, nc0 = c0 * c0 - s0 * s0;
+            const float ns1 = 2.0f * s1 * c1, nc1 = c1 * c1 - s1 * s1;
+            s0 = ns0;
+            c0 = nc0;
+            s1 = ns1;
+            c1 = nc1;
+        }
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const int col = 3 * d + q;
+            if (col >= lo && col <= hi)
+                *reinterpret_cast<uint4*>(row + (col - lo) * 128) = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+        }
+    }
+    if (c == 3) {
+        *reinterpret_cast<uint4*>(row + (27 - lo) * 128) =
+            make_uint4(pack_bf16(x[0], x[1]), pack_bf16(x[2], x[3]), pack_bf16(x[4], x[5]), pack_bf16(x[6], x[7]));
+        *reinterpret_cast<uint4*>(row + (28 - lo) * 128) = make_uint4(pack_bf16(x[8], 0.0f), 0u, 0u, 0u);
+#pragma unroll
+        for (int col = 29; col < kEnc / 8; ++col) *reinterpret_cast<uint4*>(row + (col - lo) * 128) = make_uint4(0u, 0u, 0u, 0u);
+    }
 }
 
 #endif  // __CUDACC__
