@@ -228,46 +228,55 @@ __global__ void __launch_bounds__(128) k_shade(DScene S, WaveParams W, Paths P, 
                 const float strategy_pdf = (has_caps(B.caps, CAP_DIFF) || has_caps(B.caps, CAP_GLOSSY)) ? 0.5f : 1.0f;
                 BsdfSample out{mk(0, 0, 0), 0.0f, 0.0f};
                 bool ok = false;
-                if (sample_dim(key, base + OFF_STRATEGY, strat) < strategy_pdf) {
-                    out = bsdf_sample(B, wi, sample_dim(key, base + OFF_BSDF, strat),
-                                      sample_dim(key, base + OFF_BSDF + 1, strat),
+                // the strategy's own direction (divergent: BSDF sample or light sample), then the
+                // other lights' emission densities along it in one loop every lane runs together,
+                // then the strategy's weight (the sums keep the light order of both branches)
+                const bool by_bsdf = sample_dim(key, base + OFF_STRATEGY, strat) < strategy_pdf;
+                bool have = false;
+                int k = -1;
+                float3 dir = mk(0, 0, 1);
+                float acc = 0.0f;
+                if (by_bsdf) {
+                    out = bsdf_sample(B, wi, sample_dim(key, base + OFF_BSDF, strat), sample_dim(key, base + OFF_BSDF + 1, strat),
                                       sample_dim(key, base + OFF_COMPONENT, strat), CAP_ALL);
                     if (out.ok()) {
                         out.pdf *= strategy_pdf;
-                        const float3 wd = out.wo.x * u + out.wo.y * v + out.wo.z * N;
-                        float pl = 0.0f;
-                        for (int l = 0; l < S.n_lights; ++l) {
-                            const LightEmission e = light_emission(S, l, target, wd, lam);
-                            if (e.pdf > 0.0f) pl += light_choice_pdf(S, l) * e.pdf;
-                        }
-                        pl *= (1.0f - strategy_pdf);
-                        out.value *= power_heuristic(out.pdf, pl);
-                        ok = out.ok();
+                        dir = out.wo.x * u + out.wo.y * v + out.wo.z * N;
+                        have = true;
                     }
                 } else if (S.n_lights > 0) {
                     const float uc = sample_dim(key, base + OFF_LIGHT_CHOICE, strat);
-                    int k = lower_bound_f(S.light_cdf, S.n_lights, uc);
+                    k = lower_bound_f(S.light_cdf, S.n_lights, uc);
                     if (k > S.n_lights - 1) k = S.n_lights - 1;
                     const float pc = light_choice_pdf(S, k);
                     if (pc > 0.0f) {
                         const LightSample ls = light_sample(S, k, target, sample_dim(key, base + OFF_LIGHT, strat),
                                                             sample_dim(key, base + OFF_LIGHT + 1, strat), lam);
                         if (ls.pdf > 0.0f) {
-                            float pdf = pc * ls.pdf;
-                            for (int l = 0; l < S.n_lights; ++l) {
-                                if (l == k) continue;
-                                const LightEmission e = light_emission(S, l, target, ls.dir, lam);
-                                if (e.pdf > 0.0f) pdf += light_choice_pdf(S, l) * e.pdf;
-                            }
-                            pdf *= (1.0f - strategy_pdf);
-                            const float3 wo = mk(dot(ls.dir, u), dot(ls.dir, v), dot(ls.dir, N));
-                            const BsdfOut be = bsdf_evaluate(B, wi, wo, CAP_ALL);
-                            if (be.pdf > 0.0f && be.value != 0.0f) {
-                                out.wo = wo;
-                                out.value = be.value * power_heuristic(pdf, be.pdf * strategy_pdf);
-                                out.pdf = pdf;
-                                ok = out.ok();
-                            }
+                            acc = pc * ls.pdf;
+                            dir = ls.dir;
+                            have = true;
+                        }
+                    }
+                }
+                if (have) {
+                    for (int l = 0; l < S.n_lights; ++l) {
+                        if (l == k) continue;
+                        const LightEmission e = light_emission(S, l, target, dir, lam);
+                        if (e.pdf > 0.0f) acc += light_choice_pdf(S, l) * e.pdf;
+                    }
+                    acc *= (1.0f - strategy_pdf);
+                    if (by_bsdf) {
+                        out.value *= power_heuristic(out.pdf, acc);
+                        ok = out.ok();
+                    } else {
+                        const float3 wo = mk(dot(dir, u), dot(dir, v), dot(dir, N));
+                        const BsdfOut be = bsdf_evaluate(B, wi, wo, CAP_ALL);
+                        if (be.pdf > 0.0f && be.value != 0.0f) {
+                            out.wo = wo;
+                            out.value = be.value * power_heuristic(acc, be.pdf * strategy_pdf);
+                            out.pdf = acc;
+                            ok = out.ok();
                         }
                     }
                 }

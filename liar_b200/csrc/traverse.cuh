@@ -129,103 +129,110 @@ struct LaneStack {
     }
 };
 
-// Traverses from st.node until one leaf has been tested (or the ray is finished).
-// Returns true when the ray is finished.
+// One inner node: st.node >= 0 on entry. Its hit children are ordered by entry distance, the
+// farther ones pushed; on exit st.node is the nearest hit child (inner node or leaf), or kNodeNone
+// when no child is hit.
 template <bool ANY, int S, int BLOCK, bool COUNT>
-__device__ __forceinline__ bool trace_step(const QNode* __restrict__ nodes, const QTri* __restrict__ tris, RayState& st,
-                                           LaneStack<S, BLOCK>& stack, uint64_t pol_tree, uint32_t& status,
-                                           uint32_t& n_nodes, uint32_t& n_tris) {
+__device__ __forceinline__ void visit_node(const QNode* __restrict__ nodes, RayState& st, LaneStack<S, BLOCK>& stack,
+                                           uint64_t pol_tree, uint32_t& status, uint32_t& n_nodes) {
     const bool nx = st.dx < 0.0f, ny = st.dy < 0.0f, nz = st.dz < 0.0f;
-    // ---- descend through inner nodes until the nearest candidate is a leaf
-    while (st.node >= 0) {
-        if (COUNT) ++n_nodes;
-        const QNode* q = nodes + st.node;
-        const float4 lx = ld_hint(&q->lo_x, pol_tree), hx = ld_hint(&q->hi_x, pol_tree);
-        const float4 ly = ld_hint(&q->lo_y, pol_tree), hy = ld_hint(&q->hi_y, pol_tree);
-        const float4 lz = ld_hint(&q->lo_z, pol_tree), hz = ld_hint(&q->hi_z, pol_tree);
-        const int4 ch = ld_hint_i(&q->child, pol_tree);
-        const float4 nxp = nx ? hx : lx, fxp = nx ? lx : hx;
-        const float4 nyp = ny ? hy : ly, fyp = ny ? ly : hy;
-        const float4 nzp = nz ? hz : lz, fzp = nz ? lz : hz;
-        float tn[4], tf[4];
-        tn[0] = max4f(fmaf(nxp.x, st.idx, -st.oix), fmaf(nyp.x, st.idy, -st.oiy), fmaf(nzp.x, st.idz, -st.oiz), st.tmin);
-        tn[1] = max4f(fmaf(nxp.y, st.idx, -st.oix), fmaf(nyp.y, st.idy, -st.oiy), fmaf(nzp.y, st.idz, -st.oiz), st.tmin);
-        tn[2] = max4f(fmaf(nxp.z, st.idx, -st.oix), fmaf(nyp.z, st.idy, -st.oiy), fmaf(nzp.z, st.idz, -st.oiz), st.tmin);
-        tn[3] = max4f(fmaf(nxp.w, st.idx, -st.oix), fmaf(nyp.w, st.idy, -st.oiy), fmaf(nzp.w, st.idz, -st.oiz), st.tmin);
-        tf[0] = min4f(fmaf(fxp.x, st.idx, -st.oix), fmaf(fyp.x, st.idy, -st.oiy), fmaf(fzp.x, st.idz, -st.oiz), st.tbest);
-        tf[1] = min4f(fmaf(fxp.y, st.idx, -st.oix), fmaf(fyp.y, st.idy, -st.oiy), fmaf(fzp.y, st.idz, -st.oiz), st.tbest);
-        tf[2] = min4f(fmaf(fxp.z, st.idx, -st.oix), fmaf(fyp.z, st.idy, -st.oiy), fmaf(fzp.z, st.idz, -st.oiz), st.tbest);
-        tf[3] = min4f(fmaf(fxp.w, st.idx, -st.oix), fmaf(fyp.w, st.idy, -st.oiy), fmaf(fzp.w, st.idz, -st.oiz), st.tbest);
-        // sortable keys: entry distance bits (tn >= tmin >= 0 for valid rays) with the slot in
-        // the two low bits; misses become 0xffffffff
-        uint32_t key[4];
+    if (COUNT) ++n_nodes;
+    const QNode* q = nodes + st.node;
+    const float4 lx = ld_hint(&q->lo_x, pol_tree), hx = ld_hint(&q->hi_x, pol_tree);
+    const float4 ly = ld_hint(&q->lo_y, pol_tree), hy = ld_hint(&q->hi_y, pol_tree);
+    const float4 lz = ld_hint(&q->lo_z, pol_tree), hz = ld_hint(&q->hi_z, pol_tree);
+    const int4 ch = ld_hint_i(&q->child, pol_tree);
+    const float4 nxp = nx ? hx : lx, fxp = nx ? lx : hx;
+    const float4 nyp = ny ? hy : ly, fyp = ny ? ly : hy;
+    const float4 nzp = nz ? hz : lz, fzp = nz ? lz : hz;
+    float tn[4], tf[4];
+    tn[0] = max4f(fmaf(nxp.x, st.idx, -st.oix), fmaf(nyp.x, st.idy, -st.oiy), fmaf(nzp.x, st.idz, -st.oiz), st.tmin);
+    tn[1] = max4f(fmaf(nxp.y, st.idx, -st.oix), fmaf(nyp.y, st.idy, -st.oiy), fmaf(nzp.y, st.idz, -st.oiz), st.tmin);
+    tn[2] = max4f(fmaf(nxp.z, st.idx, -st.oix), fmaf(nyp.z, st.idy, -st.oiy), fmaf(nzp.z, st.idz, -st.oiz), st.tmin);
+    tn[3] = max4f(fmaf(nxp.w, st.idx, -st.oix), fmaf(nyp.w, st.idy, -st.oiy), fmaf(nzp.w, st.idz, -st.oiz), st.tmin);
+    tf[0] = min4f(fmaf(fxp.x, st.idx, -st.oix), fmaf(fyp.x, st.idy, -st.oiy), fmaf(fzp.x, st.idz, -st.oiz), st.tbest);
+    tf[1] = min4f(fmaf(fxp.y, st.idx, -st.oix), fmaf(fyp.y, st.idy, -st.oiy), fmaf(fzp.y, st.idz, -st.oiz), st.tbest);
+    tf[2] = min4f(fmaf(fxp.z, st.idx, -st.oix), fmaf(fyp.z, st.idy, -st.oiy), fmaf(fzp.z, st.idz, -st.oiz), st.tbest);
+    tf[3] = min4f(fmaf(fxp.w, st.idx, -st.oix), fmaf(fyp.w, st.idy, -st.oiy), fmaf(fzp.w, st.idz, -st.oiz), st.tbest);
+    // sortable keys: entry distance bits (tn >= tmin >= 0 for valid rays) with the slot in
+    // the two low bits; misses become 0xffffffff
+    uint32_t key[4];
 #pragma unroll
-        for (int c = 0; c < 4; ++c)
-            key[c] = tn[c] <= tf[c] ? ((__float_as_uint(fmaxf(tn[c], 0.0f)) & ~3u) | (uint32_t)c) : 0xffffffffu;
-        if (!ANY) {
-            cswap(key[0], key[1]);
-            cswap(key[2], key[3]);
-            cswap(key[0], key[2]);
-            cswap(key[1], key[3]);
-            cswap(key[1], key[2]);
-        }
-        const int first = key[0] != 0xffffffffu ? 0 : key[1] != 0xffffffffu ? 1 : key[2] != 0xffffffffu ? 2
-                                                                        : key[3] != 0xffffffffu ? 3 : -1;
-        if (first < 0) {
-            st.node = kNodeNone;  // nothing hit below this node
-            break;
-        }
-        // push the other hit children, farthest first
-#pragma unroll
-        for (int c = 3; c >= 0; --c) {
-            if (c == first || key[c] == 0xffffffffu) continue;
-            const uint32_t slot = key[c] & 3u;
-            if (st.sp >= kTraceStackTotal) {
-                status |= STATUS_STACK_OVERFLOW;
-                continue;
-            }
-            stack.push(st.sp, sel4i(ch, slot), sel4f(tn[0], tn[1], tn[2], tn[3], slot));
-            ++st.sp;
-        }
-        const uint32_t kf = first == 0 ? key[0] : first == 1 ? key[1] : first == 2 ? key[2] : key[3];
-        st.node = sel4i(ch, kf & 3u);
+    for (int c = 0; c < 4; ++c)
+        key[c] = tn[c] <= tf[c] ? ((__float_as_uint(fmaxf(tn[c], 0.0f)) & ~3u) | (uint32_t)c) : 0xffffffffu;
+    if (!ANY) {
+        cswap(key[0], key[1]);
+        cswap(key[2], key[3]);
+        cswap(key[0], key[2]);
+        cswap(key[1], key[3]);
+        cswap(key[1], key[2]);
     }
-    // ---- test the leaf, if one was reached: packed 0x80000000 | count << 27 | first
-    if (st.node != kNodeNone) {
-        const uint32_t packed = (uint32_t)st.node;
-        const uint32_t count = (packed >> 27) & 15u;
-        const uint32_t first = packed & 0x07ffffffu;
-        for (uint32_t k = 0; k < count; ++k) {
-            if (COUNT) ++n_tris;
-            const QTri* tp = tris + first + k;
-            const float4 a = ld_hint(&tp->v0, pol_tree), e1 = ld_hint(&tp->e1, pol_tree), e2 = ld_hint(&tp->e2, pol_tree);
-            float t, u, v;
-            bool hit;
-            if (e1.w != 0.0f) {
-                // a sphere: its nearer root beyond tmin, else the farther one
-                float t1;
-                hit = sphere_intersect_exact(st.ox, st.oy, st.oz, st.dx, st.dy, st.dz, a.x, a.y, a.z, e1.x, t, t1);
-                if (hit && !(t > st.tmin)) t = t1;
-            } else {
-                hit = tri_intersect_exact(st.ox, st.oy, st.oz, st.dx, st.dy, st.dz, a.x, a.y, a.z, e1.x, e1.y, e1.z,
-                                          e2.x, e2.y, e2.z, t, u, v);
-            }
-            if (hit) {
-                const int prim = __float_as_int(a.w);
-                if (ANY) {
-                    if (t > st.tmin && t < st.tmax) {
-                        st.best = prim;
-                        st.tbest = t;
-                        return true;
-                    }
-                } else if (t > st.tmin && (t < st.tbest || (t == st.tbest && prim < st.best))) {
-                    st.tbest = t;
+    const int first = key[0] != 0xffffffffu ? 0 : key[1] != 0xffffffffu ? 1 : key[2] != 0xffffffffu ? 2
+                                                                    : key[3] != 0xffffffffu ? 3 : -1;
+    if (first < 0) {
+        st.node = kNodeNone;  // nothing hit below this node
+        return;
+    }
+    // push the other hit children, farthest first
+#pragma unroll
+    for (int c = 3; c >= 0; --c) {
+        if (c == first || key[c] == 0xffffffffu) continue;
+        const uint32_t slot = key[c] & 3u;
+        if (st.sp >= kTraceStackTotal) {
+            status |= STATUS_STACK_OVERFLOW;
+            continue;
+        }
+        stack.push(st.sp, sel4i(ch, slot), sel4f(tn[0], tn[1], tn[2], tn[3], slot));
+        ++st.sp;
+    }
+    const uint32_t kf = first == 0 ? key[0] : first == 1 ? key[1] : first == 2 ? key[2] : key[3];
+    st.node = sel4i(ch, kf & 3u);
+}
+
+// Tests the leaf st.node (packed 0x80000000 | count << 27 | first). True when an any-hit ray is
+// finished by it.
+template <bool ANY, bool COUNT>
+__device__ __forceinline__ bool test_leaf(const QTri* __restrict__ tris, RayState& st, uint64_t pol_tree,
+                                          uint32_t& n_tris) {
+    const uint32_t packed = (uint32_t)st.node;
+    const uint32_t count = (packed >> 27) & 15u;
+    const uint32_t first = packed & 0x07ffffffu;
+    for (uint32_t k = 0; k < count; ++k) {
+        if (COUNT) ++n_tris;
+        const QTri* tp = tris + first + k;
+        const float4 a = ld_hint(&tp->v0, pol_tree), e1 = ld_hint(&tp->e1, pol_tree), e2 = ld_hint(&tp->e2, pol_tree);
+        float t, u, v;
+        bool hit;
+        if (e1.w != 0.0f) {
+            // a sphere: its nearer root beyond tmin, else the farther one
+            float t1;
+            hit = sphere_intersect_exact(st.ox, st.oy, st.oz, st.dx, st.dy, st.dz, a.x, a.y, a.z, e1.x, t, t1);
+            if (hit && !(t > st.tmin)) t = t1;
+        } else {
+            hit = tri_intersect_exact(st.ox, st.oy, st.oz, st.dx, st.dy, st.dz, a.x, a.y, a.z, e1.x, e1.y, e1.z, e2.x,
+                                      e2.y, e2.z, t, u, v);
+        }
+        if (hit) {
+            const int prim = __float_as_int(a.w);
+            if (ANY) {
+                if (t > st.tmin && t < st.tmax) {
                     st.best = prim;
+                    st.tbest = t;
+                    return true;
                 }
+            } else if (t > st.tmin && (t < st.tbest || (t == st.tbest && prim < st.best))) {
+                st.tbest = t;
+                st.best = prim;
             }
         }
     }
-    // ---- pop the next entry that can still hold a closer hit
+    return false;
+}
+
+// Pops the next entry that can still hold a closer hit into st.node; true when there is none (the
+// ray is finished).
+template <bool ANY, int S, int BLOCK>
+__device__ __forceinline__ bool pop_next(RayState& st, const LaneStack<S, BLOCK>& stack) {
     while (st.sp > 0) {
         --st.sp;
         int nd;
@@ -239,6 +246,17 @@ __device__ __forceinline__ bool trace_step(const QNode* __restrict__ nodes, cons
     return true;
 }
 
+// Traverses from st.node until one leaf has been tested (or the ray is finished).
+// Returns true when the ray is finished.
+template <bool ANY, int S, int BLOCK, bool COUNT>
+__device__ __forceinline__ bool trace_step(const QNode* __restrict__ nodes, const QTri* __restrict__ tris, RayState& st,
+                                           LaneStack<S, BLOCK>& stack, uint64_t pol_tree, uint32_t& status,
+                                           uint32_t& n_nodes, uint32_t& n_tris) {
+    while (st.node >= 0) visit_node<ANY, S, BLOCK, COUNT>(nodes, st, stack, pol_tree, status, n_nodes);
+    if (st.node != kNodeNone && test_leaf<ANY, COUNT>(tris, st, pol_tree, n_tris)) return true;
+    return pop_next<ANY, S, BLOCK>(st, stack);
+}
+
 // rays per warp fetch: the n rays spread evenly over the launch's warps, rounded up to a multiple
 // of 32 and kept within [32, 256] (fewer fetches for large waves, full occupancy for small ones)
 __host__ __device__ __forceinline__ uint32_t trace_batch(uint32_t n, uint32_t warps) {
@@ -247,8 +265,10 @@ __host__ __device__ __forceinline__ uint32_t trace_batch(uint32_t n, uint32_t wa
     return b < 32u ? 32u : (b > 256u ? 256u : b);
 }
 
-template <bool ANY, int S, int BLOCK, bool COUNT>
-__global__ void __launch_bounds__(BLOCK) trace_kernel(const QNode* __restrict__ nodes, const QTri* __restrict__ tris,
+// REFILL: idle lanes that trigger a refill; LEAF_AT: lanes waiting at a leaf that start the leaf
+// phase (see below); MINB: resident blocks the register allocation must allow
+template <bool ANY, int S, int BLOCK, bool COUNT, int REFILL = 4, int LEAF_AT = 8, int MINB = 1>
+__global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const QNode* __restrict__ nodes, const QTri* __restrict__ tris,
                                                       const liar_ray* __restrict__ rays, liar_hit* __restrict__ hits,
                                                       uint32_t n_rays, uint32_t* __restrict__ work_counter,
                                                       uint32_t* __restrict__ status_word,
@@ -262,7 +282,6 @@ __global__ void __launch_bounds__(BLOCK) trace_kernel(const QNode* __restrict__ 
         n_rays = min(*n_dev, n_rays);
         BATCH = trace_batch(n_rays, gridDim.x * (BLOCK / 32));
     }
-    constexpr int REFILL = 8;         // refill once this many lanes are idle
     extern __shared__ int trace_smem[];  // S * BLOCK node entries, then S * BLOCK distances
     LaneStack<S, BLOCK> stack;
     stack.s_node = trace_smem;
@@ -326,17 +345,35 @@ __global__ void __launch_bounds__(BLOCK) trace_kernel(const QNode* __restrict__ 
                 w_next += min(avail, (uint32_t)__popc(idle));
             }
         }
+        // node phase: every descending lane visits one node; a lane whose node hit nothing pops at
+        // once (a ray turned away near the root finishes here and is replaced next turn)
+        bool done = false;
         if (rid >= 0) {
-            const bool done = st.node == kNodeNone ||
-                              trace_step<ANY, S, BLOCK, COUNT>(nodes, tris, st, stack, pol_tree, status, n_nodes, n_tris);
-            if (done) {
-                int prim = st.best;
-                float t = st.tbest;
-                if (!ANY && prim >= 0 && !(t > range_near(st.tmin))) prim = -1;  // BoundedRay::inRange near side
-                if (prim < 0) t = INFINITY;
-                st_hint(hits + rid, prim, __float_as_int(t), pol_stream);
-                rid = -1;
+            if (st.node >= 0) {
+                visit_node<ANY, S, BLOCK, COUNT>(nodes, st, stack, pol_tree, status, n_nodes);
+                if (st.node == kNodeNone) done = pop_next<ANY, S, BLOCK>(st, stack);
+            } else if (st.node == kNodeNone) {
+                done = true;  // a ray with non-finite components, retired untraced
             }
+        }
+        // leaf phase: lanes that reached a leaf wait until LEAF_AT of them have (or no lane is
+        // descending any more), then test their leaves together and pop
+        const bool at_leaf = rid >= 0 && !done && st.node < 0;
+        const uint32_t leafw = __ballot_sync(0xffffffffu, at_leaf);
+        if (leafw) {
+            const uint32_t desc = __ballot_sync(0xffffffffu, rid >= 0 && !done && st.node >= 0);
+            if ((uint32_t)__popc(leafw) >= (uint32_t)LEAF_AT || desc == 0u) {
+                if (at_leaf)
+                    done = test_leaf<ANY, COUNT>(tris, st, pol_tree, n_tris) || pop_next<ANY, S, BLOCK>(st, stack);
+            }
+        }
+        if (done) {
+            int prim = st.best;
+            float t = st.tbest;
+            if (!ANY && prim >= 0 && !(t > range_near(st.tmin))) prim = -1;  // BoundedRay::inRange near side
+            if (prim < 0) t = INFINITY;
+            st_hint(hits + rid, prim, __float_as_int(t), pol_stream);
+            rid = -1;
         }
     }
     if (status) atomicOr(status_word, status);
