@@ -11,7 +11,13 @@
 //     REFILL lanes have finished their ray, those lanes load the next rays of the batch, so short
 //     rays (most random rays miss the mesh after a node or two) do not leave lanes idle while a
 //     long ray of the same warp is still traversing (dynamic fetch, Aila & Laine 2009);
-//   * one loop turn per lane = descend through inner nodes to the next leaf, then test that leaf;
+//   * one loop turn = a node phase and a leaf phase: every lane still descending visits one node
+//     (a lane whose node hit nothing pops its next entry at once), and lanes that have reached a
+//     leaf wait until LEAF_AT of them have (or none descends any more), then test their leaves
+//     together and pop; refills are checked every turn. Compared with running each lane down to
+//     its next leaf per turn, lanes idle far less (random rays of very different lengths): on the
+//     1.31M-triangle icosphere with 16.7M random rays, 5.76 against 4.20 Grays/s closest hit and
+//     6.36 against 4.76 any hit, hits identical;
 //   * a node is one 128-byte line read with seven 16-byte loads that carry an L2 evict-last
 //     policy; rays and hits stream with evict-first, so the 512 MiB ray stream does not push the
 //     tree out of L2;
@@ -246,17 +252,6 @@ __device__ __forceinline__ bool pop_next(RayState& st, const LaneStack<S, BLOCK>
     return true;
 }
 
-// Traverses from st.node until one leaf has been tested (or the ray is finished).
-// Returns true when the ray is finished.
-template <bool ANY, int S, int BLOCK, bool COUNT>
-__device__ __forceinline__ bool trace_step(const QNode* __restrict__ nodes, const QTri* __restrict__ tris, RayState& st,
-                                           LaneStack<S, BLOCK>& stack, uint64_t pol_tree, uint32_t& status,
-                                           uint32_t& n_nodes, uint32_t& n_tris) {
-    while (st.node >= 0) visit_node<ANY, S, BLOCK, COUNT>(nodes, st, stack, pol_tree, status, n_nodes);
-    if (st.node != kNodeNone && test_leaf<ANY, COUNT>(tris, st, pol_tree, n_tris)) return true;
-    return pop_next<ANY, S, BLOCK>(st, stack);
-}
-
 // rays per warp fetch: the n rays spread evenly over the launch's warps, rounded up to a multiple
 // of 32 and kept within [32, 256] (fewer fetches for large waves, full occupancy for small ones)
 __host__ __device__ __forceinline__ uint32_t trace_batch(uint32_t n, uint32_t warps) {
@@ -267,7 +262,7 @@ __host__ __device__ __forceinline__ uint32_t trace_batch(uint32_t n, uint32_t wa
 
 // REFILL: idle lanes that trigger a refill; LEAF_AT: lanes waiting at a leaf that start the leaf
 // phase (see below); MINB: resident blocks the register allocation must allow
-template <bool ANY, int S, int BLOCK, bool COUNT, int REFILL = 4, int LEAF_AT = 8, int MINB = 1>
+template <bool ANY, int S, int BLOCK, bool COUNT, int REFILL = 8, int LEAF_AT = 8, int MINB = 1>
 __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const QNode* __restrict__ nodes, const QTri* __restrict__ tris,
                                                       const liar_ray* __restrict__ rays, liar_hit* __restrict__ hits,
                                                       uint32_t n_rays, uint32_t* __restrict__ work_counter,
@@ -406,7 +401,7 @@ __global__ void __launch_bounds__(BLOCK) trace_multi_kernel(const TreeRoot* __re
                                                             liar_hit* __restrict__ hits, const uint32_t* __restrict__ n_dev,
                                                             uint32_t* __restrict__ work_counter,
                                                             uint32_t* __restrict__ status_word) {
-    constexpr int REFILL = 8;
+    constexpr int REFILL = 8, LEAF_AT = 8;  // as trace_kernel
     extern __shared__ int trace_smem[];
     LaneStack<S, BLOCK> stack;
     stack.s_node = trace_smem;
@@ -474,17 +469,31 @@ __global__ void __launch_bounds__(BLOCK) trace_multi_kernel(const TreeRoot* __re
                 w_next += min(avail, (uint32_t)__popc(idle));
             }
         }
+        // the node and leaf phases of trace_kernel
+        bool done = false;
         if (rid >= 0) {
-            const bool done = st.node == kNodeNone ||
-                              trace_step<false, S, BLOCK, false>(nodes, tris, st, stack, pol_tree, status, n_nodes, n_tris);
-            if (done) {
-                int prim = st.best;
-                float t = st.tbest;
-                if (prim >= 0 && !(t > range_near(st.tmin))) prim = -1;
-                if (prim < 0) t = INFINITY;
-                st_hint(hits + rid, prim, __float_as_int(t), pol_stream);
-                rid = -1;
+            if (st.node >= 0) {
+                visit_node<false, S, BLOCK, false>(nodes, st, stack, pol_tree, status, n_nodes);
+                if (st.node == kNodeNone) done = pop_next<false, S, BLOCK>(st, stack);
+            } else if (st.node == kNodeNone) {
+                done = true;
             }
+        }
+        const bool at_leaf = rid >= 0 && !done && st.node < 0;
+        const uint32_t leafw = __ballot_sync(0xffffffffu, at_leaf);
+        if (leafw) {
+            const uint32_t desc = __ballot_sync(0xffffffffu, rid >= 0 && !done && st.node >= 0);
+            if ((uint32_t)__popc(leafw) >= (uint32_t)LEAF_AT || desc == 0u) {
+                if (at_leaf) done = test_leaf<false, false>(tris, st, pol_tree, n_tris) || pop_next<false, S, BLOCK>(st, stack);
+            }
+        }
+        if (done) {
+            int prim = st.best;
+            float t = st.tbest;
+            if (prim >= 0 && !(t > range_near(st.tmin))) prim = -1;
+            if (prim < 0) t = INFINITY;
+            st_hint(hits + rid, prim, __float_as_int(t), pol_stream);
+            rid = -1;
         }
     }
     if (status) atomicOr(status_word, status);

@@ -212,7 +212,12 @@ def test_workload_scenes_through_the_batch_match_the_oracle():
         ma, mc = _mean_within(g, c, min_fraction=0.98)
         np.testing.assert_array_equal(g[..., 7], c[..., 7])
         assert mc[..., 1].mean() > 0.01
-        assert abs(ma[..., 1].mean() / mc[..., 1].mean() - 1) < 0.03
+        # the image means of Y agree within 4 standard errors (pixels are independent estimates: the
+        # variance of the image mean is the sum of the pixels' variances of their means / npix^2)
+        _, va = R.resolve(g)
+        _, vc = R.resolve(c)
+        se = np.sqrt((va[..., 1].sum() + vc[..., 1].sum())) / va[..., 1].size
+        assert abs(ma[..., 1].mean() - mc[..., 1].mean()) <= 4.0 * se, (ma[..., 1].mean(), mc[..., 1].mean(), se)
         gs.close()
     br.close()
 
