@@ -734,7 +734,8 @@ def run_case(name: str) -> None:
     """Small single-kernel workloads for profiling captures (ncu -k ... python bench.py --case NAME):
     guide-eval (the guide network over 1M random vertices, 3 launches), direct (DirectLighting on
     the Cornell frame, 256^2 x 4 spp, twice), shade (the Cornell path-tracing frame, twice),
-    gather (k = 64 over 4M uniform photons for 256k uniform queries, twice), guided (the slit
+    gather (k = 64 over 4M uniform photons for 256k uniform queries, twice), gather-photon (the
+    photon workload's gather: 10M photons, the 1080p camera queries, k = 64, twice), guided (the slit
     room at 256^2: 4 training passes, then 16 guided samples per pixel), pm (the PhotonMapper on
     the photon scene, 1M global photons, 480 x 270, two frames)."""
     import torch
@@ -796,6 +797,27 @@ def run_case(name: str) -> None:
         film = torch.zeros((270, 480, 8), device="cuda")
         for k in range(2):
             gs.render_device(R.render_desc(cam, 480, 270, 1, t, seed=0, first_sample=k), film.data_ptr())
+    elif name == "gather-photon":
+        # the photon workload's gather: 10M global photons of the photon scene, the 1920 x 1080
+        # camera queries on diffuse surfaces, k = 64, twice
+        from liar_b200 import photons as PH, render as R, scenes_render
+        scene, cam = scenes_render.photon_scene()
+        flat = R.flatten(scene)
+        gs = R.GpuScene(ctx, flat)
+        desc = PH.photon_desc(10_000_000, max_emitted=(1 << 32) - 1, ray_traced_direct=False, wave=1 << 22)
+        ph, counts = PH.trace_photons(gs, desc, capacity=10_000_000 + (3 << 22))
+        glob = (ph["tag"] & PH.GLOBAL) != 0
+        pos = ph["position"][glob][:10_000_000].contiguous()
+        r = PH.automatic_radius(ph["power"][glob][:10_000_000].cpu().numpy(), counts["emitted"], 64)
+        q, _ = camera_queries(flat, cam, 1920, 1080)
+        m = PH.PhotonMap(ctx, device_ptr=pos.data_ptr(), n=pos.shape[0], r_max=r)
+        dq = torch.from_numpy(q).cuda()
+        nq = q.shape[0]
+        di = torch.empty((nq, 64), dtype=torch.int32, device="cuda")
+        dd = torch.empty((nq, 64), dtype=torch.float32, device="cuda")
+        dc = torch.empty(nq, dtype=torch.int32, device="cuda")
+        for _ in range(2):
+            m.gather_device(dq.data_ptr(), nq, 64, di.data_ptr(), dd.data_ptr(), dc.data_ptr(), 0)
     elif name == "gather":
         from liar_b200 import photons as PH
         rng = np.random.default_rng(0)

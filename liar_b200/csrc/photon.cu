@@ -6,8 +6,9 @@
 // nearest to a point, all closer than r_max, the farthest first in the reference's heap.
 //
 // Build (spatial hashing, Teschner et al. 2003): a bounding-box reduction fixes the grid origin;
-// cells are r_max / kRefine wide, cell = floor((p - origin) / cell_size), bucket =
-// hash(cell) mod 2^m; a counting sort (histogram, exclusive scan, scatter) orders the photons by
+// the cell width follows the photons' density (map_build_impl: about seven photons per cell on
+// surfaces, two and a half in volumes, between r_max and r_max / 12), cell = floor((p - origin) /
+// cell_size), bucket = hash(cell) mod 2^m; a counting sort (histogram, exclusive scan, scatter) orders the photons by
 // bucket into float4 (x, y, z, original index) records, each with its packed cell key beside it.
 // Gather: one warp per query visits the cells around the query in rings of growing Chebyshev
 // distance R and stops after ring R as soon as the current k-th distance is at most R cell
@@ -122,6 +123,18 @@ __global__ void k_bucket_count(const float* __restrict__ pos, uint32_t n, BuildP
     const uint32_t b = bucket_of(cell_coord(x, P.ox, P.inv), cell_coord(y, P.oy, P.inv), cell_coord(z, P.oz, P.inv), P.mask);
     keys[i] = b;
     atomicAdd(counts + b, 1u);
+}
+
+// sum over buckets of count^2 (the photon-weighted bucket occupancy times n)
+__global__ void k_sumsq(const uint32_t* __restrict__ counts, uint32_t nb, unsigned long long* __restrict__ out) {
+    unsigned long long s = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
+        const unsigned long long c = counts[i];
+        s += c * c;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31u) == 0 && s) atomicAdd(out, s);
 }
 
 // exclusive scan of `counts` (n_buckets + 1 entries written to `start`), one block per 1024 x 4 entries
@@ -498,6 +511,18 @@ int map_build_impl(liar_gpu_ctx* ctx, liar_gpu_photon_map* m, const float* d_pos
     // grid origin and extent from the photons' bounding box
     m->origin[0] = m->origin[1] = m->origin[2] = 0.0f;
     m->extent = 0.0f;
+    m->cell = m->r_max / kRefine;
+    float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    // one cell of margin below the lowest photon keeps every cell index positive
+    auto set_grid = [&](float cell) -> bool {
+        m->cell = cell;
+        m->extent = 0.0f;
+        for (int a = 0; a < 3; ++a) {
+            m->origin[a] = lo[a] - cell;
+            m->extent = std::max(m->extent, hi[a] - m->origin[a]);
+        }
+        return m->extent / cell <= (float)(kCellLimit - 4);
+    };
     if (n) {
         const uint32_t init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
         e = cudaMemcpyAsync(bounds, init, sizeof(init), cudaMemcpyHostToDevice, st);
@@ -509,13 +534,45 @@ int map_build_impl(liar_gpu_ctx* ctx, liar_gpu_photon_map* m, const float* d_pos
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return ctx_cuda(ctx, e, "photon bounds");
         for (int a = 0; a < 3; ++a) {
-            const float lo = fkey_inv(hb[a]), hi = fkey_inv(hb[3 + a]);
-            if (!std::isfinite(lo) || !std::isfinite(hi)) return ctx_fail(ctx, LIAR_ERR_INVALID, "photon position is not finite");
-            // one cell of margin below the lowest photon keeps every cell index positive
-            m->origin[a] = lo - m->cell;
-            m->extent = std::max(m->extent, hi - m->origin[a]);
+            lo[a] = fkey_inv(hb[a]);
+            hi[a] = fkey_inv(hb[3 + a]);
+            if (!std::isfinite(lo[a]) || !std::isfinite(hi[a]))
+                return ctx_fail(ctx, LIAR_ERR_INVALID, "photon position is not finite");
         }
-        if (m->extent / m->cell > (float)(kCellLimit - 4))
+        // the cell width from the photons' density: the photon-weighted number of other photons
+        // sharing a photon's cell, lambda(c) (a bucket's count squared summed over the buckets, over
+        // n, less the photon itself and the expected share of colliding cells n / nb), at r_max / 2
+        // and r_max / 4 gives the local dimension D = log2(lambda1 / lambda2) (2 for photons on
+        // surfaces, 3 in volumes) and the width at which lambda = T(D): 7 on surfaces, 2.5 in
+        // volumes -- the k = 64 neighbours then lie within about two cells, which balances the
+        // bucket lookups of the ring walk against the candidates it tests (cells r_max / 1 ..
+        // r_max / 12)
+        if (n >= 1024) {
+            double lam[2] = {0.0, 0.0};
+            unsigned long long* d_sum = reinterpret_cast<unsigned long long*>(bounds + 8);
+            for (int t = 0; t < 2 && e == cudaSuccess; ++t) {
+                if (!set_grid(m->r_max / (t == 0 ? 2.0f : 4.0f))) break;
+                const BuildParams T{m->origin[0], m->origin[1], m->origin[2], 1.0f / m->cell, (uint32_t)(nb - 1)};
+                e = cudaMemsetAsync(counts, 0, nb * 4, st);
+                if (e == cudaSuccess) e = cudaMemsetAsync(d_sum, 0, 8, st);
+                if (e != cudaSuccess) break;
+                k_bucket_count<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_pos, (uint32_t)n, T, keys, counts);
+                k_sumsq<<<(unsigned)ctx->num_sms * 4, 256, 0, st>>>(counts, (uint32_t)nb, d_sum);
+                unsigned long long hs = 0;
+                e = cudaMemcpyAsync(&hs, d_sum, 8, cudaMemcpyDeviceToHost, st);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+                lam[t] = (double)hs / (double)n - 1.0 - (double)n / (double)nb;
+            }
+            if (e != cudaSuccess) return ctx_cuda(ctx, e, "photon density");
+            float refine = kRefine;
+            if (lam[0] > 0.0 && lam[1] > 0.0) {
+                const double D = std::min(3.0, std::max(1.5, std::log2(lam[0] / lam[1])));
+                const double target = 7.0 * std::pow(2.5 / 7.0, D - 2.0);
+                refine = (float)std::min(12.0, std::max(1.0, 2.0 * std::pow(lam[0] / target, 1.0 / D)));
+            }
+            while (!set_grid(m->r_max / refine) && refine > 1.0f) refine = std::max(1.0f, refine * 0.5f);
+        }
+        if (!set_grid(m->cell))
             return ctx_fail(ctx, LIAR_ERR_UNSUPPORTED, "photons span more than %d grid cells per axis; raise r_max",
                             kCellLimit - 4);
     }
