@@ -275,6 +275,35 @@ __device__ __forceinline__ uint64_t reverse_lanes(uint64_t v) {
     return __shfl_sync(0xffffffffu, (unsigned long long)v, 31 - (threadIdx.x & 31u));
 }
 
+// i / d for 0 <= i < 2^22, 0 < d, through a float reciprocal with one correction step
+__device__ __forceinline__ int div_small(int i, int d, float inv_d) {
+    int q = (int)(((float)i + 0.5f) * inv_d);
+    if (q * d > i) --q;
+    else if ((q + 1) * d <= i) ++q;
+    return q;
+}
+
+// cell i of the shell at Chebyshev distance R >= 1 around a cell ((2R+1)^3 - (2R-1)^3 cells): the
+// two z faces, then the square rings of the levels between them
+__device__ __forceinline__ void shell_cell(int i, int R, int& dx, int& dy, int& dz) {
+    const int side = 2 * R + 1, face = side * side;
+    if (i < 2 * face) {
+        const int j = i < face ? i : i - face;
+        dz = i < face ? -R : R;
+        const int y = div_small(j, side, 1.0f / (float)side);
+        dy = y - R;
+        dx = j - y * side - R;
+    } else {
+        const int per = 8 * R, i2 = i - 2 * face;
+        const int level = div_small(i2, per, 1.0f / (float)per);
+        dz = level - R + 1;
+        const int p = i2 - level * per;
+        const int k = div_small(p, 2 * R, 1.0f / (float)(2 * R)), t = p - k * 2 * R;
+        dx = k == 0 ? -R + t : k == 1 ? R : k == 2 ? R - t : -R;
+        dy = k == 0 ? -R : k == 1 ? -R + t : k == 2 ? R : R - t;
+    }
+}
+
 struct GatherParams {
     BuildParams B;
     float r2max;
@@ -319,19 +348,13 @@ __global__ void __launch_bounds__(256) k_gather(const float4* __restrict__ sorte
         uint64_t lo = INF, hi = INF;
         uint64_t kth = INF;  // key of the current k-th (64th) nearest
         for (int R = 0; R <= G.max_ring; ++R) {
-            const int side = 2 * R + 1;
-            const int cube = side * side * side;
-            for (int c0 = 0; c0 < cube; c0 += 32) {
-                // lane: one cell of the cube around the query; keep the shell cells (Chebyshev = R)
+            // the cells at Chebyshev distance R, 32 at a time (lane: one cell)
+            const int shell = R == 0 ? 1 : (2 * R + 1) * (2 * R + 1) * (2 * R + 1) - (2 * R - 1) * (2 * R - 1) * (2 * R - 1);
+            for (int c0 = 0; c0 < shell; c0 += 32) {
                 const int c = c0 + (int)lane;
                 int dx = 0, dy = 0, dz = 0;
-                bool mine = false;
-                if (c < cube) {
-                    dx = c % side - R;
-                    dy = (c / side) % side - R;
-                    dz = c / (side * side) - R;
-                    mine = max(abs(dx), max(abs(dy), abs(dz))) == R;
-                }
+                bool mine = c < shell;
+                if (mine && R > 0) shell_cell(c, R, dx, dy, dz);
                 const int ix = cx + dx, iy = cy + dy, iz = cz + dz;
                 mine = mine && ix >= 0 && iy >= 0 && iz >= 0 && ix <= kCellLimit && iy <= kCellLimit && iz <= kCellLimit;
                 uint32_t s0 = 0, s1 = 0;
