@@ -603,18 +603,6 @@ constexpr size_t kDwTcSmem = 1024 + kDwOffBar + 64;
 constexpr int kDwThreads = 256;
 constexpr uint32_t kDwTmemCols = 512;  // dW0 (two M blocks), dW1..dW4, dW5: 7 x 64 columns
 
-// stage rows [s0, s0 + 64) of a [n][ld] bf16 matrix into a row-major [64][ld] tile (zeros past n)
-__device__ __forceinline__ void dw_stage(unsigned char* dst, const __nv_bfloat16* __restrict__ src, size_t s0, size_t n,
-                                         int ld) {
-    const int chunks = ld / 8;
-    for (int i = threadIdx.x; i < kDwRecords * chunks; i += kDwThreads) {
-        const int rr = i / chunks, c = i % chunks;
-        const size_t row = s0 + rr;
-        reinterpret_cast<uint4*>(dst)[i] =
-            row < n ? reinterpret_cast<const uint4*>(src + row * ld)[c] : make_uint4(0u, 0u, 0u, 0u);
-    }
-}
-
 // the transpose of a staged [64][ld] tile, columns [c0, c0 + rows): operand row m = column c0 + m,
 // K = the 64 records, in the K-major layout (umma_offset(m, k, 64))
 __device__ __forceinline__ void dw_transpose(unsigned char* op, const unsigned char* tile, int ld, int c0, int rows) {
@@ -702,23 +690,69 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw_tc(const float* __re
         if (tid == 0 && issue_mma) umma_commit((uint32_t)__cvta_generic_to_shared(mbar + b));
         pending[b] = true;
     };
+    // the staging loads of one layer step into registers, so that the next step's global reads are
+    // in flight while this step's transposes and MMAs run: step 0 = delta_1 (with the encodings),
+    // step l = h_l and delta_{l+1} (the output gradient for l = 5); 512 uint4 per 64 x 64 matrix
+    uint4 pre_h[2], pre_d[2];
+    auto prefetch = [&](size_t s0, int l) {
+        const __nv_bfloat16* hsrc = l >= 1 ? act + (size_t)(l - 1) * n_max * kWidth : nullptr;
+        const __nv_bfloat16* dsrc = l < 5 ? delta + (size_t)l * n_max * kWidth : gout;
+        const int dld = l < 5 ? kWidth : kOut;
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const int i = tid + j * kDwThreads;
+            const size_t row = s0 + (size_t)(i >> 3);
+            const int c = i & 7;
+            pre_h[j] = (hsrc && row < c1) ? reinterpret_cast<const uint4*>(hsrc + row * kWidth)[c] : make_uint4(0u, 0u, 0u, 0u);
+            const int dc = dld / 8;
+            const int di = tid + j * kDwThreads;
+            const size_t drow = s0 + (size_t)(di / dc);
+            pre_d[j] = (di < kDwRecords * dc && drow < c1) ? reinterpret_cast<const uint4*>(dsrc + drow * dld)[di % dc]
+                                                            : make_uint4(0u, 0u, 0u, 0u);
+        }
+    };
+    auto store_pre = [&](int l) {
+        const int dc = (l < 5 ? kWidth : kOut) / 8;
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const int i = tid + j * kDwThreads;
+            if (l >= 1) reinterpret_cast<uint4*>(smem + kDwOffH)[i] = pre_h[j];
+            if (i < kDwRecords * dc) reinterpret_cast<uint4*>(smem + kDwOffD)[i] = pre_d[j];
+        }
+    };
+    if (c0 < c1) prefetch(c0, 0);
     for (size_t s0 = c0; ok && s0 < c1; s0 += kDwRecords) {
         const bool acc = issued_any;
-        // ---- W0: the encodings of the stage's records (the forward's, recomputed) and delta_1
-        wait_bar(0);
-        if (!ok) break;
-        for (int i = tid; i < kDwRecords; i += kDwThreads) {
+        // ---- W0: the encodings of the stage's records (the forward's, recomputed) and delta_1;
+        // four threads per record, each encoding the inputs d = part, part + 4, ... (part 3 also
+        // writes the raw inputs and the zero padding)
+        {
+            const int i = tid & (kDwRecords - 1), part = tid >> 6;
             const size_t row = s0 + i;
+            uint32_t* dst = reinterpret_cast<uint32_t*>(smem + kDwOffH + (size_t)i * kEnc * 2);
             float x[kIn];
             if (row < c1) normalise_input(rec + row * kRecordFloats, box.lo, box.inv_ext, x);
-            __nv_bfloat16* dst = reinterpret_cast<__nv_bfloat16*>(smem + kDwOffH) + (size_t)i * kEnc;
-            if (row < c1) {
-                encode_row(x, dst);
-            } else {
-                for (int c = 0; c < kEnc / 8; ++c) reinterpret_cast<uint4*>(dst)[c] = make_uint4(0u, 0u, 0u, 0u);
+            else
+                for (int c = 0; c < kIn; ++c) x[c] = 0.0f;
+            const bool live = row < c1;
+            for (int d = part; d < kIn; d += 4) {
+                if (live) encode_input(x[d], dst + d * kFreq);
+                else
+                    for (int k = 0; k < kFreq; ++k) dst[d * kFreq + k] = 0u;
+            }
+            if (part == 3) {
+                uint32_t* raw = dst + kIn * kFreq;  // columns 216..255
+#pragma unroll
+                for (int c = 0; c < 4; ++c) raw[c] = pack_bf16(x[2 * c], x[2 * c + 1]);
+                raw[4] = pack_bf16(x[8], 0.0f);
+#pragma unroll
+                for (int c = 5; c < (kEnc - kIn * 2 * kFreq) / 2; ++c) raw[c] = 0u;
             }
         }
-        dw_stage(smem + kDwOffD, delta, s0, c1, kWidth);
+        store_pre(0);
+        prefetch(s0, 1);
+        wait_bar(0);  // (its barrier also orders the staging writes before the transposes)
+        if (!ok) break;
         __syncthreads();
         dw_transpose(smem + kDwOffA0, smem + kDwOffH, kEnc, 0, 128);
         dw_transpose(smem + kDwOffA0 + kDwA, smem + kDwOffH, kEnc, 128, 128);
@@ -733,12 +767,12 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw_tc(const float* __re
         // ---- W1..W5: h_l and delta_{l+1} (the output gradient for W5), alternating buffers
         for (int l = 1; l <= 5 && ok; ++l) {
             const int b = 1 + ((l - 1) & 1);
+            const int N = layer_n(l);
+            store_pre(l);
+            if (l < 5) prefetch(s0, l + 1);
+            else if (s0 + kDwRecords < c1) prefetch(s0 + kDwRecords, 0);
             wait_bar(b);
             if (!ok) break;
-            const int N = layer_n(l);
-            dw_stage(smem + kDwOffH, act + (size_t)(l - 1) * n_max * kWidth, s0, c1, kWidth);
-            if (l < 5) dw_stage(smem + kDwOffD, delta + (size_t)l * n_max * kWidth, s0, c1, kWidth);
-            else dw_stage(smem + kDwOffD, gout, s0, c1, kOut);
             __syncthreads();
             const uint32_t a_off = kDwOffA1 + (uint32_t)(b - 1) * kDwA, b_off = kDwOffB1 + (uint32_t)(b - 1) * kDwB;
             dw_transpose(smem + a_off, smem + kDwOffH, kWidth, 0, kWidth);

@@ -49,6 +49,24 @@ __device__ __forceinline__ float bf16_hi(uint32_t v) { return __uint_as_float(v 
 // cos 2a = cos^2 a - sin^2 a (x fl(sqrt 2) 2^k is exactly fl(x fl(sqrt 2)) 2^k, so these are the
 // angles of the definition; the recurrence adds ~1e-6 absolute error, far below bf16).
 
+// the 12 words (24 bf16: sin/cos pairs of the 12 frequencies) of input value xd, as encode_row
+__device__ __forceinline__ void encode_input(float xd, uint32_t* w) {
+    float s0, c0, s1, c1;
+    sincospif(xd, &s0, &c0);
+    sincospif(xd * 1.41421356237309515f, &s1, &c1);
+#pragma unroll
+    for (int k = 0; k < kFreq / 2; ++k) {
+        w[2 * k] = pack_bf16(s0, c0);
+        w[2 * k + 1] = pack_bf16(s1, c1);
+        const float ns0 = 2.0f * s0 * c0, nc0 = c0 * c0 - s0 * s0;
+        const float ns1 = 2.0f * s1 * c1, nc1 = c1 * c1 - s1 * s1;
+        s0 = ns0;
+        c0 = nc0;
+        s1 = ns1;
+        c1 = nc1;
+    }
+}
+
 __device__ __forceinline__ void encode_row(const float* x, __nv_bfloat16* row) {
     uint32_t* dst = reinterpret_cast<uint32_t*>(row);
 #pragma unroll
