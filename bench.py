@@ -757,7 +757,8 @@ def run_case(name: str) -> None:
             torch.rand((65536, 1), device="cuda", generator=gen)], 1).contiguous()
         g.train_step(rec)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        st = torch.cuda.current_stream()
+        st = torch.cuda.Stream()  # a stream of its own: the events must see the training kernels
+        torch.cuda.synchronize()
         e0.record(st)
         for _ in range(3):
             g.train_device(rec, stream=st.cuda_stream)
