@@ -6,9 +6,9 @@
 // nearest to a point, all closer than r_max, the farthest first in the reference's heap.
 //
 // Build (spatial hashing, Teschner et al. 2003): a bounding-box reduction fixes the grid origin;
-// the cell width follows the photons' density (map_build_impl: about seven photons per cell on
-// surfaces, two and a half in volumes, between r_max and r_max / 12), cell = floor((p - origin) /
-// cell_size), bucket = hash(cell) mod 2^m; a counting sort (histogram, exclusive scan, scatter) orders the photons by
+// the cell width follows the photons' density (map_build_impl: about 60 photons per cell on
+// surfaces, 4 in volumes, between r_max and r_max / 8), cell = floor((p - origin) / cell_size),
+// bucket = hash(cell) mod 2^m; a counting sort (histogram, exclusive scan, scatter) orders the photons by
 // bucket into float4 (x, y, z, original index) records, each with its packed cell key beside it.
 // Gather: one warp per query visits the cells around the query in rings of growing Chebyshev
 // distance R and stops after ring R as soon as the current k-th distance is at most R cell
@@ -304,6 +304,25 @@ __device__ __forceinline__ void shell_cell(int i, int R, int& dx, int& dy, int& 
     }
 }
 
+// inserts key x into the ascending 64-list (lo: slots 0..31, hi: 32..63, one of each per lane),
+// dropping the largest; every lane takes part (the branches are warp-uniform)
+constexpr int kInsertMax = 8;  // batches with more keys below the k-th take the bitonic merge
+__device__ __forceinline__ void insert_key(uint64_t x, uint64_t& lo, uint64_t& hi) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const int p = __popc(__ballot_sync(0xffffffffu, lo < x));  // lo is ascending: the entries below x lead
+    const uint64_t lo_up = __shfl_up_sync(0xffffffffu, (unsigned long long)lo, 1);
+    const uint64_t lo_last = __shfl_sync(0xffffffffu, (unsigned long long)lo, 31);
+    const uint64_t hi_up = __shfl_up_sync(0xffffffffu, (unsigned long long)hi, 1);
+    if (p < 32) {
+        // x at slot p; lo[31] becomes hi[0]; hi moves up one slot
+        lo = (int)lane < p ? lo : ((int)lane == p ? x : lo_up);
+        hi = lane == 0 ? lo_last : hi_up;
+    } else {
+        const int q = __popc(__ballot_sync(0xffffffffu, hi < x));
+        if (q < 32) hi = (int)lane < q ? hi : ((int)lane == q ? x : hi_up);
+    }
+}
+
 struct GatherParams {
     BuildParams B;
     float r2max;
@@ -403,7 +422,19 @@ __global__ void __launch_bounds__(256) k_gather(const float4* __restrict__ sorte
                             if (d2 < G.r2max) key = ((uint64_t)__float_as_uint(d2) << 32) | (uint64_t)__float_as_uint(p.w);
                         }
                     }
-                    if (__ballot_sync(0xffffffffu, key < kth) == 0u) continue;
+                    const uint32_t better = __ballot_sync(0xffffffffu, key < kth);
+                    if (better == 0u) continue;
+                    if (__popc(better) <= kInsertMax) {
+                        // a few keys below the k-th: insert them one at a time
+                        uint32_t m = better;
+                        while (m) {
+                            const int src = __ffs(m) - 1;
+                            m &= m - 1;
+                            insert_key(__shfl_sync(0xffffffffu, (unsigned long long)key, src), lo, hi);
+                        }
+                        kth = __shfl_sync(0xffffffffu, (unsigned long long)hi, 31);
+                        continue;
+                    }
                     const uint64_t bsort = warp_sort32(key);
                     // smallest 32 of hi and the batch: half-cleaner against the reversed batch
                     // (every shuffle is executed by all 32 lanes, outside lane-dependent branches)
@@ -566,10 +597,10 @@ int map_build_impl(liar_gpu_ctx* ctx, liar_gpu_photon_map* m, const float* d_pos
         // sharing a photon's cell, lambda(c) (a bucket's count squared summed over the buckets, over
         // n, less the photon itself and the expected share of colliding cells n / nb), at r_max / 2
         // and r_max / 4 gives the local dimension D = log2(lambda1 / lambda2) (2 for photons on
-        // surfaces, 3 in volumes) and the width at which lambda = T(D): 7 on surfaces, 2.5 in
-        // volumes -- the k = 64 neighbours then lie within about two cells, which balances the
-        // bucket lookups of the ring walk against the candidates it tests (cells r_max / 1 ..
-        // r_max / 12)
+        // surfaces, 3 in volumes) and the width at which lambda = T(D), 60 on surfaces and 4 in
+        // volumes (geometric in between), measured optima of the ring walk's cost: the bucket
+        // lookups of the cells visited (queries with fewer than k photons within r_max visit all
+        // of them) against the candidates tested; cells r_max / 1 .. r_max / 8
         if (n >= 1024) {
             double lam[2] = {0.0, 0.0};
             unsigned long long* d_sum = reinterpret_cast<unsigned long long*>(bounds + 8);
@@ -590,8 +621,8 @@ int map_build_impl(liar_gpu_ctx* ctx, liar_gpu_photon_map* m, const float* d_pos
             float refine = kRefine;
             if (lam[0] > 0.0 && lam[1] > 0.0) {
                 const double D = std::min(3.0, std::max(1.5, std::log2(lam[0] / lam[1])));
-                const double target = 7.0 * std::pow(2.5 / 7.0, D - 2.0);
-                refine = (float)std::min(12.0, std::max(1.0, 2.0 * std::pow(lam[0] / target, 1.0 / D)));
+                const double target = 60.0 * std::pow(4.0 / 60.0, D - 2.0);
+                refine = (float)std::min(8.0, std::max(1.0, 2.0 * std::pow(lam[0] / target, 1.0 / D)));
             }
             while (!set_grid(m->r_max / refine) && refine > 1.0f) refine = std::max(1.0f, refine * 0.5f);
         }
