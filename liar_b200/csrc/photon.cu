@@ -374,8 +374,31 @@ __global__ void __launch_bounds__(256) k_gather(const float4* __restrict__ sorte
                 int dx = 0, dy = 0, dz = 0;
                 bool mine = c < shell;
                 if (mine && R > 0) shell_cell(c, R, dx, dy, dz);
-                const int ix = cx + dx, iy = cy + dy, iz = cz + dz;
+                int ix = cx + dx, iy = cy + dy, iz = cz + dz;
                 mine = mine && ix >= 0 && iy >= 0 && iz >= 0 && ix <= kCellLimit && iy <= kCellLimit && iz <= kCellLimit;
+                if (R > 0) {
+                    // the query's distance to the cell's box, less the cell-assignment round-off: a
+                    // cell farther than the current k-th (or r_max) cannot contribute and is skipped;
+                    // the others are taken nearest first, so that the k-th falls early and later
+                    // candidates fail the batch test instead of entering the list
+                    float md2 = 0.0f;
+                    if (mine) {
+                        const float bx = P.ox + (float)ix * G.cell, by = P.oy + (float)iy * G.cell, bz = P.oz + (float)iz * G.cell;
+                        const float ex = fmaxf(fmaxf(bx - qx, qx - (bx + G.cell)), 0.0f);
+                        const float ey = fmaxf(fmaxf(by - qy, qy - (by + G.cell)), 0.0f);
+                        const float ez = fmaxf(fmaxf(bz - qz, qz - (bz + G.cell)), 0.0f);
+                        const float md = fmaxf(sqrtf(ex * ex + ey * ey + ez * ez) - G.slack, 0.0f);
+                        md2 = md * md;
+                        const float bound = kth != INF ? fminf(__uint_as_float((uint32_t)(kth >> 32)), G.r2max) : G.r2max;
+                        mine = md2 <= bound;
+                    }
+                    const uint64_t ck = warp_sort32(mine ? ((uint64_t)__float_as_uint(md2) << 32) | (uint64_t)lane : INF);
+                    const int src = (int)(ck & 31u);
+                    mine = ck != INF;
+                    ix = __shfl_sync(0xffffffffu, ix, src);
+                    iy = __shfl_sync(0xffffffffu, iy, src);
+                    iz = __shfl_sync(0xffffffffu, iz, src);
+                }
                 uint32_t s0 = 0, s1 = 0;
                 if (mine) {
                     const uint32_t b = bucket_of(ix, iy, iz, P.mask);
