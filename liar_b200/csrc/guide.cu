@@ -596,30 +596,29 @@ constexpr int kDwRecords = 64;                            // records per stage (
 constexpr uint32_t kDwA = 128u * kDwRecords * 2;          // an A operand: 128 features x 64 records
 constexpr uint32_t kDwB = 64u * kDwRecords * 2;           // a B operand: 64 outputs x 64 records
 constexpr uint32_t kDwOffA0 = 0, kDwOffB0 = 2 * kDwA, kDwOffA1 = kDwOffB0 + kDwB, kDwOffB1 = kDwOffA1 + 2 * kDwA;
-constexpr uint32_t kDwOffH = kDwOffB1 + 2 * kDwB;         // staging: 64 records x up to 256 features, row-major
-constexpr uint32_t kDwOffD = kDwOffH + kDwRecords * kEnc * 2;  // staging: 64 records x up to 64 outputs
-constexpr uint32_t kDwOffBar = kDwOffD + kDwRecords * kWidth * 2;
-constexpr size_t kDwTcSmem = 1024 + kDwOffBar + 64;
+constexpr uint32_t kDwOffBar = kDwOffB1 + 2 * kDwB;
+// (at least 120 KB: one CTA per SM, since each holds all 512 tensor-memory columns)
+constexpr size_t kDwTcSmem = (1024 + kDwOffBar + 64) > 122880 ? (1024 + kDwOffBar + 64) : 122880;
 constexpr int kDwThreads = 256;
 constexpr uint32_t kDwTmemCols = 512;  // dW0 (two M blocks), dW1..dW4, dW5: 7 x 64 columns
-
-// the transpose of a staged [64][ld] tile, columns [c0, c0 + rows): operand row m = column c0 + m,
-// K = the 64 records, in the K-major layout (umma_offset(m, k, 64))
-__device__ __forceinline__ void dw_transpose(unsigned char* op, const unsigned char* tile, int ld, int c0, int rows) {
-    const uint16_t* t = reinterpret_cast<const uint16_t*>(tile);
-    for (int i = threadIdx.x; i < rows * (kDwRecords / 8); i += kDwThreads) {
-        const int m = i % rows, g = i / rows;  // consecutive threads: consecutive columns (conflict-free reads)
-        uint32_t w[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const uint32_t lo = t[(size_t)(8 * g + 2 * e) * ld + c0 + m];
-            const uint32_t hi = t[(size_t)(8 * g + 2 * e + 1) * ld + c0 + m];
-            w[e] = lo | (hi << 16);
-        }
-        *reinterpret_cast<uint4*>(op + umma_offset((uint32_t)m, (uint32_t)(8 * g), (uint32_t)kDwRecords)) =
-            make_uint4(w[0], w[1], w[2], w[3]);
-    }
+// The weight-gradient operands are MN-major (the records, the UMMA K, are the rows of the stored
+// activations, the features or outputs contiguous in each): core matrix = 8 records x 8 features
+// (16 B per record, 128 B per core matrix); K-adjacent core matrices 128 B apart (leading byte
+// offset), MN-adjacent ones 1024 B apart (stride byte offset, 8 record groups of a stage). A row
+// of 8 features of record k therefore lands at (feature / 8) * 1024 + (k / 8) * 128 + (k % 8) * 16,
+// straight from its 16-byte global load: no transposition.
+constexpr uint32_t kDwLbo = 128u, kDwSbo = (uint32_t)(kDwRecords / 8) * 128u;
+__device__ __forceinline__ uint32_t dw_offset(uint32_t group, uint32_t k) {
+    return group * kDwSbo + (k >> 3) * kDwLbo + (k & 7u) * 16u;
 }
+// MN-major shared-memory descriptor (no swizzle): leading byte offset = the K stride, stride byte
+// offset = the MN stride
+__device__ __forceinline__ uint64_t umma_desc_mn(uint32_t smem_addr) {
+    return (uint64_t)((smem_addr >> 4) & 0x3FFFu) | ((uint64_t)(kDwLbo >> 4) << 16) |
+           ((uint64_t)((kDwSbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+// kind::f16 with both operands MN-major (bits 15 and 16)
+__host__ __device__ constexpr uint32_t umma_idesc_mn(uint32_t n) { return umma_idesc(n) | (1u << 15) | (1u << 16); }
 
 __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw_tc(const float* __restrict__ rec,
                                                                const uint32_t* __restrict__ n_dev, size_t n_max, Box box,
@@ -677,111 +676,105 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw_tc(const float* __re
         pending[b] = false;
         tc_fence_after();
     };
-    auto issue = [&](int b, uint32_t d_col, uint32_t a_off, uint32_t b_off, uint32_t N, bool acc0) {
+    auto issue = [&](uint32_t d_col, uint32_t a_off, uint32_t b_off, uint32_t N, bool acc0) {
         if (tid == 0 && issue_mma) {
-            const uint32_t idesc = umma_idesc(N);
+            const uint32_t idesc = umma_idesc_mn(N);
             for (uint32_t j = 0; j < (uint32_t)kDwRecords / 16; ++j)
-                umma_bf16(tmem + d_col, umma_smem_desc(base + a_off + 256u * j, (kDwRecords / 8) * 128u),
-                          umma_smem_desc(base + b_off + 256u * j, (kDwRecords / 8) * 128u), idesc,
-                          (acc0 || j > 0) ? 1u : 0u);
+                umma_bf16(tmem + d_col, umma_desc_mn(base + a_off + 2u * kDwLbo * j),
+                          umma_desc_mn(base + b_off + 2u * kDwLbo * j), idesc, (acc0 || j > 0) ? 1u : 0u);
         }
     };
     auto commit = [&](int b) {
         if (tid == 0 && issue_mma) umma_commit((uint32_t)__cvta_generic_to_shared(mbar + b));
         pending[b] = true;
     };
-    // the staging loads of one layer step into registers, so that the next step's global reads are
-    // in flight while this step's transposes and MMAs run: step 0 = delta_1 (with the encodings),
-    // step l = h_l and delta_{l+1} (the output gradient for l = 5); 512 uint4 per 64 x 64 matrix
+    // the 16-byte rows of one layer step, loaded into registers one step ahead: thread i takes
+    // record i / 8, 8-feature group i % 8 (two per thread), of h_l and of delta_{l+1} (the output
+    // gradient, 6 groups, for l = 5); step 0 loads delta_1 alone (the encodings are computed)
     uint4 pre_h[2], pre_d[2];
     auto prefetch = [&](size_t s0, int l) {
         const __nv_bfloat16* hsrc = l >= 1 ? act + (size_t)(l - 1) * n_max * kWidth : nullptr;
         const __nv_bfloat16* dsrc = l < 5 ? delta + (size_t)l * n_max * kWidth : gout;
-        const int dld = l < 5 ? kWidth : kOut;
+        const int dld = l < 5 ? kWidth : kOut, dc = dld / 8;
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
             const int i = tid + j * kDwThreads;
             const size_t row = s0 + (size_t)(i >> 3);
-            const int c = i & 7;
-            pre_h[j] = (hsrc && row < c1) ? reinterpret_cast<const uint4*>(hsrc + row * kWidth)[c] : make_uint4(0u, 0u, 0u, 0u);
-            const int dc = dld / 8;
-            const int di = tid + j * kDwThreads;
-            const size_t drow = s0 + (size_t)(di / dc);
-            pre_d[j] = (di < kDwRecords * dc && drow < c1) ? reinterpret_cast<const uint4*>(dsrc + drow * dld)[di % dc]
-                                                            : make_uint4(0u, 0u, 0u, 0u);
+            pre_h[j] = (hsrc && row < c1) ? reinterpret_cast<const uint4*>(hsrc + row * kWidth)[i & 7] : make_uint4(0u, 0u, 0u, 0u);
+            const size_t drow = s0 + (size_t)(i / dc);
+            pre_d[j] = (i < kDwRecords * dc && drow < c1) ? reinterpret_cast<const uint4*>(dsrc + drow * dld)[i % dc]
+                                                          : make_uint4(0u, 0u, 0u, 0u);
         }
     };
-    auto store_pre = [&](int l) {
+    // the prefetched rows into the operand buffers at (a_off, b_off)
+    auto place = [&](int l, uint32_t a_off, uint32_t b_off) {
         const int dc = (l < 5 ? kWidth : kOut) / 8;
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
             const int i = tid + j * kDwThreads;
-            if (l >= 1) reinterpret_cast<uint4*>(smem + kDwOffH)[i] = pre_h[j];
-            if (i < kDwRecords * dc) reinterpret_cast<uint4*>(smem + kDwOffD)[i] = pre_d[j];
+            if (l >= 1) *reinterpret_cast<uint4*>(smem + a_off + dw_offset((uint32_t)(i & 7), (uint32_t)(i >> 3))) = pre_h[j];
+            if (i < kDwRecords * dc)
+                *reinterpret_cast<uint4*>(smem + b_off + dw_offset((uint32_t)(i % dc), (uint32_t)(i / dc))) = pre_d[j];
         }
     };
     if (c0 < c1) prefetch(c0, 0);
     for (size_t s0 = c0; ok && s0 < c1; s0 += kDwRecords) {
         const bool acc = issued_any;
-        // ---- W0: the encodings of the stage's records (the forward's, recomputed) and delta_1;
-        // four threads per record, each encoding the inputs d = part, part + 4, ... (part 3 also
-        // writes the raw inputs and the zero padding)
+        // ---- W0: the encodings of the stage's records (the forward's, recomputed) and delta_1
+        wait_bar(0);
+        if (!ok) break;
         {
+            // four threads per record, each encoding the inputs d = part, part + 4, ... (part 3
+            // also writes the raw inputs and the zero padding); encoding column group g (8
+            // features) of record i goes to A block g / 16, group g % 16
             const int i = tid & (kDwRecords - 1), part = tid >> 6;
             const size_t row = s0 + i;
-            uint32_t* dst = reinterpret_cast<uint32_t*>(smem + kDwOffH + (size_t)i * kEnc * 2);
             float x[kIn];
-            if (row < c1) normalise_input(rec + row * kRecordFloats, box.lo, box.inv_ext, x);
+            const bool live = row < c1;
+            if (live) normalise_input(rec + row * kRecordFloats, box.lo, box.inv_ext, x);
             else
                 for (int c = 0; c < kIn; ++c) x[c] = 0.0f;
-            const bool live = row < c1;
+            auto put = [&](int g, uint4 v) {
+                *reinterpret_cast<uint4*>(smem + kDwOffA0 + (uint32_t)(g >> 4) * kDwA + dw_offset((uint32_t)(g & 15), (uint32_t)i)) = v;
+            };
             for (int d = part; d < kIn; d += 4) {
-                if (live) encode_input(x[d], dst + d * kFreq);
+                uint32_t w[kFreq];
+                if (live) encode_input(x[d], w);
                 else
-                    for (int k = 0; k < kFreq; ++k) dst[d * kFreq + k] = 0u;
+                    for (int k = 0; k < kFreq; ++k) w[k] = 0u;
+#pragma unroll
+                for (int q = 0; q < 3; ++q) put(3 * d + q, make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]));
             }
             if (part == 3) {
-                uint32_t* raw = dst + kIn * kFreq;  // columns 216..255
-#pragma unroll
-                for (int c = 0; c < 4; ++c) raw[c] = pack_bf16(x[2 * c], x[2 * c + 1]);
-                raw[4] = pack_bf16(x[8], 0.0f);
-#pragma unroll
-                for (int c = 5; c < (kEnc - kIn * 2 * kFreq) / 2; ++c) raw[c] = 0u;
+                put(27, make_uint4(pack_bf16(x[0], x[1]), pack_bf16(x[2], x[3]), pack_bf16(x[4], x[5]), pack_bf16(x[6], x[7])));
+                put(28, make_uint4(pack_bf16(x[8], 0.0f), 0u, 0u, 0u));
+                for (int g = 29; g < kEnc / 8; ++g) put(g, make_uint4(0u, 0u, 0u, 0u));
             }
         }
-        store_pre(0);
+        place(0, 0, kDwOffB0);
         prefetch(s0, 1);
-        wait_bar(0);  // (its barrier also orders the staging writes before the transposes)
-        if (!ok) break;
-        __syncthreads();
-        dw_transpose(smem + kDwOffA0, smem + kDwOffH, kEnc, 0, 128);
-        dw_transpose(smem + kDwOffA0 + kDwA, smem + kDwOffH, kEnc, 128, 128);
-        dw_transpose(smem + kDwOffB0, smem + kDwOffD, kWidth, 0, kWidth);
         fence_async_smem();
         tc_fence_before();
         __syncthreads();
         tc_fence_after();
-        issue(0, 0u, kDwOffA0, kDwOffB0, 64u, acc);
-        issue(0, 64u, kDwOffA0 + kDwA, kDwOffB0, 64u, acc);
+        issue(0u, kDwOffA0, kDwOffB0, 64u, acc);
+        issue(64u, kDwOffA0 + kDwA, kDwOffB0, 64u, acc);
         commit(0);
         // ---- W1..W5: h_l and delta_{l+1} (the output gradient for W5), alternating buffers
         for (int l = 1; l <= 5 && ok; ++l) {
             const int b = 1 + ((l - 1) & 1);
             const int N = layer_n(l);
-            store_pre(l);
-            if (l < 5) prefetch(s0, l + 1);
-            else if (s0 + kDwRecords < c1) prefetch(s0 + kDwRecords, 0);
             wait_bar(b);
             if (!ok) break;
-            __syncthreads();
             const uint32_t a_off = kDwOffA1 + (uint32_t)(b - 1) * kDwA, b_off = kDwOffB1 + (uint32_t)(b - 1) * kDwB;
-            dw_transpose(smem + a_off, smem + kDwOffH, kWidth, 0, kWidth);
-            dw_transpose(smem + b_off, smem + kDwOffD, N, 0, N);
+            place(l, a_off, b_off);
+            if (l < 5) prefetch(s0, l + 1);
+            else if (s0 + kDwRecords < c1) prefetch(s0 + kDwRecords, 0);
             fence_async_smem();
             tc_fence_before();
             __syncthreads();
             tc_fence_after();
-            issue(b, 128u + 64u * (uint32_t)(l - 1), a_off, b_off, (uint32_t)N, acc);
+            issue(128u + 64u * (uint32_t)(l - 1), a_off, b_off, (uint32_t)N, acc);
             commit(b);
         }
         issued_any = true;
