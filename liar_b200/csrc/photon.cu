@@ -376,6 +376,7 @@ __global__ void __launch_bounds__(256) k_gather(const float4* __restrict__ sorte
                 if (mine && R > 0) shell_cell(c, R, dx, dy, dz);
                 int ix = cx + dx, iy = cy + dy, iz = cz + dz;
                 mine = mine && ix >= 0 && iy >= 0 && iz >= 0 && ix <= kCellLimit && iy <= kCellLimit && iz <= kCellLimit;
+                float cell_d2 = 0.0f;  // after the sort: lane j's cell's distance bound (ascending in j)
                 if (R > 0) {
                     // the query's distance to the cell's box, less the cell-assignment round-off: a
                     // cell farther than the current k-th (or r_max) cannot contribute and is skipped;
@@ -395,6 +396,7 @@ __global__ void __launch_bounds__(256) k_gather(const float4* __restrict__ sorte
                     const uint64_t ck = warp_sort32(mine ? ((uint64_t)__float_as_uint(md2) << 32) | (uint64_t)lane : INF);
                     const int src = (int)(ck & 31u);
                     mine = ck != INF;
+                    cell_d2 = __uint_as_float((uint32_t)(ck >> 32));
                     ix = __shfl_sync(0xffffffffu, ix, src);
                     iy = __shfl_sync(0xffffffffu, iy, src);
                     iz = __shfl_sync(0xffffffffu, iz, src);
@@ -432,6 +434,12 @@ __global__ void __launch_bounds__(256) k_gather(const float4* __restrict__ sorte
                     for (uint32_t step = 16; step > 0; step >>= 1) {
                         const uint64_t e = __shfl_sync(0xffffffffu, (unsigned long long)excl, (int)(owner + step));
                         if (e <= item) owner += step;
+                    }
+                    // the cells are in ascending distance order: once the batch's first cell lies
+                    // beyond the current k-th, so do all that follow
+                    if (R > 0 && kth != INF) {
+                        const float first_d2 = __shfl_sync(0xffffffffu, cell_d2, (int)__shfl_sync(0xffffffffu, owner, 0));
+                        if (first_d2 > __uint_as_float((uint32_t)(kth >> 32))) break;
                     }
                     const uint32_t o_s0 = __shfl_sync(0xffffffffu, s0, (int)owner);
                     const uint64_t o_excl = __shfl_sync(0xffffffffu, (unsigned long long)excl, (int)owner);
