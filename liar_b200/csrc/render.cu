@@ -374,8 +374,9 @@ int ensure_render_buffers(liar_gpu_ctx* ctx, RenderBuffers* rb, size_t n) {
     if (rb->mem) cudaFree(rb->mem);
     rb->mem = nullptr;
     rb->cap = 0;
-    // per path: 6 state words; per queue slot (x2): 32 B ray + 4 B path; hits 8 B; 2 counters
-    const size_t bytes = n * (6 * 4 + 2 * (32 + 4) + 8) + 1024;
+    // per path: 6 state words; per queue slot (x2): 32 B ray + 4 B path; hits 8 B; 2 counters;
+    // plus the 256-byte rounding of each of the 13 pieces
+    const size_t bytes = n * (6 * 4 + 2 * (32 + 4) + 8) + 13 * 256;
     cudaError_t e = cudaMalloc(&rb->mem, bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
