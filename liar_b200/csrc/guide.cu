@@ -595,10 +595,13 @@ __global__ void __launch_bounds__(kTcThreads) k_train_bwd_tc(const unsigned char
 constexpr int kDwRecords = 64;                            // records per stage (the UMMA K of a stage)
 constexpr uint32_t kDwA = 128u * kDwRecords * 2;          // an A operand: 128 features x 64 records
 constexpr uint32_t kDwB = 64u * kDwRecords * 2;           // a B operand: 64 outputs x 64 records
-constexpr uint32_t kDwOffA0 = 0, kDwOffB0 = 2 * kDwA, kDwOffA1 = kDwOffB0 + kDwB, kDwOffB1 = kDwOffA1 + 2 * kDwA;
-constexpr uint32_t kDwOffBar = kDwOffB1 + 2 * kDwB;
-// (at least 120 KB: one CTA per SM, since each holds all 512 tensor-memory columns)
-constexpr size_t kDwTcSmem = (1024 + kDwOffBar + 64) > 122880 ? (1024 + kDwOffBar + 64) : 122880;
+// one stage's operands all at once: W0 (two 128-feature blocks of encodings, delta_1), then
+// W1..W5 (h_l, upper 64 features zero; delta_{l+1} or the output gradient)
+constexpr uint32_t kDwOffA0 = 0, kDwOffB0 = 2 * kDwA;
+__host__ __device__ constexpr uint32_t dw_off_a(int l) { return kDwOffB0 + kDwB + (uint32_t)(l - 1) * (kDwA + kDwB); }
+__host__ __device__ constexpr uint32_t dw_off_b(int l) { return dw_off_a(l) + kDwA; }
+constexpr uint32_t kDwOffBar = dw_off_a(6);                // 160 KB
+constexpr size_t kDwTcSmem = 1024 + kDwOffBar + 64;
 constexpr int kDwThreads = 256;
 constexpr uint32_t kDwTmemCols = 512;  // dW0 (two M blocks), dW1..dW4, dW5: 7 x 64 columns
 // The weight-gradient operands are MN-major (the records, the UMMA K, are the rows of the stored
@@ -620,6 +623,10 @@ __device__ __forceinline__ uint64_t umma_desc_mn(uint32_t smem_addr) {
 // kind::f16 with both operands MN-major (bits 15 and 16)
 __host__ __device__ constexpr uint32_t umma_idesc_mn(uint32_t n) { return umma_idesc(n) | (1u << 15) | (1u << 16); }
 
+// Per stage of 64 records: every operand of the six weight gradients is written into shared memory
+// (the encodings computed, the other rows from registers loaded during the previous stage), one
+// barrier, 28 MMAs from one thread, one commit; the next stage's rows are then loaded into
+// registers while the MMAs run, so that a stage waits on global memory only once.
 __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw_tc(const float* __restrict__ rec,
                                                                const uint32_t* __restrict__ n_dev, size_t n_max, Box box,
                                                                const __nv_bfloat16* __restrict__ act,
@@ -630,17 +637,16 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw_tc(const float* __re
                                                                int issue_mma) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + kDwOffBar);  // [0] W0, [1], [2] the two W1..W5 buffers
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + kDwOffBar);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 3);
     volatile uint32_t* failed = tmem_slot + 1;
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
     const size_t n = n_dev ? min((size_t)*n_dev, n_max) : n_max;
     const size_t c0 = (size_t)blockIdx.x * per_cta, c1 = min(n, c0 + per_cta);
     // the upper halves (features 64..127) of the W1..W5 A operands stay zero
-    for (uint32_t i = tid; i < 2 * (kDwA / 2) / 16; i += kDwThreads) {
-        const uint32_t b = i / ((kDwA / 2) / 16), j = i % ((kDwA / 2) / 16);
-        reinterpret_cast<uint4*>(smem + kDwOffA1 + b * kDwA + kDwA / 2)[j] = make_uint4(0u, 0u, 0u, 0u);
-    }
+    for (int l = 1; l <= 5; ++l)
+        for (uint32_t i = tid; i < (kDwA / 2) / 16; i += kDwThreads)
+            reinterpret_cast<uint4*>(smem + dw_off_a(l) + kDwA / 2)[i] = make_uint4(0u, 0u, 0u, 0u);
     if (tid == 0) {
         for (int k = 0; k < 3; ++k)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(mbar + k)));
@@ -659,23 +665,9 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw_tc(const float* __re
     const uint32_t tmem = *tmem_slot;
     const uint32_t base = (uint32_t)__cvta_generic_to_shared(smem);
     uint32_t phase[3] = {0u, 0u, 0u};
-    bool pending[3] = {false, false, false};
+    bool pending[3] = {false, false, false};  // only barrier 0 is used; the drain below checks all
     bool issued_any = false;  // an MMA has written the accumulators (the first ones overwrite)
     bool ok = true;
-    // every thread waits for the commit of barrier b before its buffers are refilled
-    auto wait_bar = [&](int b) {
-        if (!pending[b]) return;
-        const uint32_t addr = (uint32_t)__cvta_generic_to_shared(mbar + b);
-        if (!mbar_wait(addr, phase[b], max_tries)) *failed = 1u;
-        __syncthreads();
-        if (*failed) {
-            ok = false;
-            return;
-        }
-        phase[b] ^= 1u;
-        pending[b] = false;
-        tc_fence_after();
-    };
     auto issue = [&](uint32_t d_col, uint32_t a_off, uint32_t b_off, uint32_t N, bool acc0) {
         if (tid == 0 && issue_mma) {
             const uint32_t idesc = umma_idesc_mn(N);
@@ -684,54 +676,57 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw_tc(const float* __re
                           umma_desc_mn(base + b_off + 2u * kDwLbo * j), idesc, (acc0 || j > 0) ? 1u : 0u);
         }
     };
-    auto commit = [&](int b) {
-        if (tid == 0 && issue_mma) umma_commit((uint32_t)__cvta_generic_to_shared(mbar + b));
-        pending[b] = true;
-    };
-    // the 16-byte rows of one layer step, loaded into registers one step ahead: thread i takes
-    // record i / 8, 8-feature group i % 8 (two per thread), of h_l and of delta_{l+1} (the output
-    // gradient, 6 groups, for l = 5); step 0 loads delta_1 alone (the encodings are computed)
-    uint4 pre_h[2], pre_d[2];
-    auto prefetch = [&](size_t s0, int l) {
-        const __nv_bfloat16* hsrc = l >= 1 ? act + (size_t)(l - 1) * n_max * kWidth : nullptr;
-        const __nv_bfloat16* dsrc = l < 5 ? delta + (size_t)l * n_max * kWidth : gout;
-        const int dld = l < 5 ? kWidth : kOut, dc = dld / 8;
+    // the stage's rows in registers: thread i takes record i / 8, 8-feature group i % 8 (two per
+    // thread) of h_1..h_5, of delta_1..delta_5 and of the output gradient (6 groups), and the raw
+    // inputs of record tid % 64
+    uint4 ph[5][2], pd[6][2];
+    float px[kIn];
+    auto load_stage = [&](size_t s0) {
 #pragma unroll
-        for (int j = 0; j < 2; ++j) {
-            const int i = tid + j * kDwThreads;
-            const size_t row = s0 + (size_t)(i >> 3);
-            pre_h[j] = (hsrc && row < c1) ? reinterpret_cast<const uint4*>(hsrc + row * kWidth)[i & 7] : make_uint4(0u, 0u, 0u, 0u);
-            const size_t drow = s0 + (size_t)(i / dc);
-            pre_d[j] = (i < kDwRecords * dc && drow < c1) ? reinterpret_cast<const uint4*>(dsrc + drow * dld)[i % dc]
-                                                          : make_uint4(0u, 0u, 0u, 0u);
-        }
-    };
-    // the prefetched rows into the operand buffers at (a_off, b_off)
-    auto place = [&](int l, uint32_t a_off, uint32_t b_off) {
-        const int dc = (l < 5 ? kWidth : kOut) / 8;
+        for (int l = 0; l < 6; ++l) {
+            const int dld = l < 5 ? kWidth : kOut, dc = dld / 8;
+            const __nv_bfloat16* dsrc = l < 5 ? delta + (size_t)l * n_max * kWidth : gout;
 #pragma unroll
-        for (int j = 0; j < 2; ++j) {
-            const int i = tid + j * kDwThreads;
-            if (l >= 1) *reinterpret_cast<uint4*>(smem + a_off + dw_offset((uint32_t)(i & 7), (uint32_t)(i >> 3))) = pre_h[j];
-            if (i < kDwRecords * dc)
-                *reinterpret_cast<uint4*>(smem + b_off + dw_offset((uint32_t)(i % dc), (uint32_t)(i / dc))) = pre_d[j];
+            for (int j = 0; j < 2; ++j) {
+                const int i = tid + j * kDwThreads;
+                if (l < 5) {
+                    const size_t row = s0 + (size_t)(i >> 3);
+                    ph[l][j] = row < c1 ? reinterpret_cast<const uint4*>(act + (size_t)l * n_max * kWidth + row * kWidth)[i & 7]
+                                        : make_uint4(0u, 0u, 0u, 0u);
+                }
+                const size_t drow = s0 + (size_t)(i / dc);
+                pd[l][j] = (i < kDwRecords * dc && drow < c1) ? reinterpret_cast<const uint4*>(dsrc + drow * dld)[i % dc]
+                                                              : make_uint4(0u, 0u, 0u, 0u);
+            }
         }
+        const size_t row = s0 + (tid & (kDwRecords - 1));
+#pragma unroll
+        for (int c = 0; c < kIn; ++c) px[c] = row < c1 ? rec[row * kRecordFloats + c] : 0.0f;
     };
-    if (c0 < c1) prefetch(c0, 0);
+    if (c0 < c1) load_stage(c0);
     for (size_t s0 = c0; ok && s0 < c1; s0 += kDwRecords) {
         const bool acc = issued_any;
-        // ---- W0: the encodings of the stage's records (the forward's, recomputed) and delta_1
-        wait_bar(0);
-        if (!ok) break;
+        // the previous stage's MMAs have read every operand buffer
+        if (pending[0]) {
+            const uint32_t addr = (uint32_t)__cvta_generic_to_shared(mbar);
+            if (!mbar_wait(addr, phase[0], max_tries)) *failed = 1u;
+            __syncthreads();
+            if (*failed) {
+                ok = false;
+                break;
+            }
+            phase[0] ^= 1u;
+            pending[0] = false;
+            tc_fence_after();
+        }
         {
-            // four threads per record, each encoding the inputs d = part, part + 4, ... (part 3
-            // also writes the raw inputs and the zero padding); encoding column group g (8
-            // features) of record i goes to A block g / 16, group g % 16
+            // the encodings: four threads per record, each encoding the inputs d = part, part +
+            // 4, ... (part 3 also writes the raw inputs and the zero padding); encoding column
+            // group g (8 features) of record i goes to A block g / 16, group g % 16
             const int i = tid & (kDwRecords - 1), part = tid >> 6;
-            const size_t row = s0 + i;
+            const bool live = s0 + i < c1;
             float x[kIn];
-            const bool live = row < c1;
-            if (live) normalise_input(rec + row * kRecordFloats, box.lo, box.inv_ext, x);
+            if (live) normalise_input(px, box.lo, box.inv_ext, x);
             else
                 for (int c = 0; c < kIn; ++c) x[c] = 0.0f;
             auto put = [&](int g, uint4 v) {
@@ -751,33 +746,31 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw_tc(const float* __re
                 for (int g = 29; g < kEnc / 8; ++g) put(g, make_uint4(0u, 0u, 0u, 0u));
             }
         }
-        place(0, 0, kDwOffB0);
-        prefetch(s0, 1);
+        // the loaded rows: B of W0 = delta_1; A of W_l = h_l, B of W_l = delta_{l+1} (W5: gradient)
+#pragma unroll
+        for (int l = 0; l < 6; ++l) {
+            const int dc = (l < 5 ? kWidth : kOut) / 8;
+            const uint32_t b_off = l == 0 ? kDwOffB0 : dw_off_b(l);
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const int i = tid + j * kDwThreads;
+                if (l >= 1)
+                    *reinterpret_cast<uint4*>(smem + dw_off_a(l) + dw_offset((uint32_t)(i & 7), (uint32_t)(i >> 3))) = ph[l - 1][j];
+                if (i < kDwRecords * dc)
+                    *reinterpret_cast<uint4*>(smem + b_off + dw_offset((uint32_t)(i % dc), (uint32_t)(i / dc))) = pd[l][j];
+            }
+        }
         fence_async_smem();
         tc_fence_before();
         __syncthreads();
         tc_fence_after();
         issue(0u, kDwOffA0, kDwOffB0, 64u, acc);
         issue(64u, kDwOffA0 + kDwA, kDwOffB0, 64u, acc);
-        commit(0);
-        // ---- W1..W5: h_l and delta_{l+1} (the output gradient for W5), alternating buffers
-        for (int l = 1; l <= 5 && ok; ++l) {
-            const int b = 1 + ((l - 1) & 1);
-            const int N = layer_n(l);
-            wait_bar(b);
-            if (!ok) break;
-            const uint32_t a_off = kDwOffA1 + (uint32_t)(b - 1) * kDwA, b_off = kDwOffB1 + (uint32_t)(b - 1) * kDwB;
-            place(l, a_off, b_off);
-            if (l < 5) prefetch(s0, l + 1);
-            else if (s0 + kDwRecords < c1) prefetch(s0 + kDwRecords, 0);
-            fence_async_smem();
-            tc_fence_before();
-            __syncthreads();
-            tc_fence_after();
-            issue(128u + 64u * (uint32_t)(l - 1), a_off, b_off, (uint32_t)N, acc);
-            commit(b);
-        }
+        for (int l = 1; l <= 5; ++l) issue(128u + 64u * (uint32_t)(l - 1), dw_off_a(l), dw_off_b(l), (uint32_t)layer_n(l), acc);
+        if (tid == 0 && issue_mma) umma_commit((uint32_t)__cvta_generic_to_shared(mbar));
+        pending[0] = true;
         issued_any = true;
+        if (s0 + kDwRecords < c1) load_stage(s0 + kDwRecords);
     }
     // drain: every outstanding commit (bounded), then the accumulators out
     for (int b = 0; b < 3; ++b) {
