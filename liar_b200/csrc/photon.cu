@@ -255,6 +255,22 @@ __device__ __forceinline__ uint64_t cmpx(uint64_t v, int j, bool up) {
     const bool take_min = lower == up;
     return take_min ? (v < o ? v : o) : (v > o ? v : o);
 }
+// the same on 32-bit keys
+__device__ __forceinline__ uint32_t warp_sort32u(uint32_t v) {
+    const uint32_t lane = threadIdx.x & 31u;
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const uint32_t o = __shfl_xor_sync(0xffffffffu, v, j);
+            const bool lower = (lane & (uint32_t)j) == 0u;
+            const bool take_min = lower == ((lane & (uint32_t)k) == 0u);
+            v = take_min ? min(v, o) : max(v, o);
+        }
+    }
+    return v;
+}
+
 // full ascending bitonic sort of one key per lane
 __device__ __forceinline__ uint64_t warp_sort32(uint64_t v) {
     const uint32_t lane = threadIdx.x & 31u;
@@ -393,13 +409,28 @@ __global__ void __launch_bounds__(256) k_gather(const float4* __restrict__ sorte
                         const float bound = kth != INF ? fminf(__uint_as_float((uint32_t)(kth >> 32)), G.r2max) : G.r2max;
                         mine = md2 <= bound;
                     }
-                    const uint64_t ck = warp_sort32(mine ? ((uint64_t)__float_as_uint(md2) << 32) | (uint64_t)lane : INF);
-                    const int src = (int)(ck & 31u);
-                    mine = ck != INF;
-                    cell_d2 = __uint_as_float((uint32_t)(ck >> 32));
-                    ix = __shfl_sync(0xffffffffu, ix, src);
-                    iy = __shfl_sync(0xffffffffu, iy, src);
-                    iz = __shfl_sync(0xffffffffu, iz, src);
+                    const uint32_t live = __ballot_sync(0xffffffffu, mine);
+                    if (live == 0u) continue;  // nothing in this chunk can come within the k-th
+                    if (live & (live - 1u)) {
+                        // 32-bit sort keys: the bound with its 5 low bits cleared (a lower bound
+                        // still, so that the order stays ascending in the bound the batches test)
+                        // and the lane in those bits
+                        const uint32_t ck = warp_sort32u(mine ? ((__float_as_uint(md2) & ~31u) | lane) : 0xffffffffu);
+                        const int src = (int)(ck & 31u);
+                        mine = ck != 0xffffffffu;
+                        cell_d2 = __uint_as_float(ck & ~31u);
+                        ix = __shfl_sync(0xffffffffu, ix, src);
+                        iy = __shfl_sync(0xffffffffu, iy, src);
+                        iz = __shfl_sync(0xffffffffu, iz, src);
+                    } else {
+                        // one cell: lane 0 takes it
+                        const int src = __ffs(live) - 1;
+                        cell_d2 = __uint_as_float(__float_as_uint(__shfl_sync(0xffffffffu, md2, src)) & ~31u);
+                        ix = __shfl_sync(0xffffffffu, ix, src);
+                        iy = __shfl_sync(0xffffffffu, iy, src);
+                        iz = __shfl_sync(0xffffffffu, iz, src);
+                        mine = lane == 0;
+                    }
                 }
                 uint32_t s0 = 0, s1 = 0;
                 if (mine) {

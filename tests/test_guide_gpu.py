@@ -71,9 +71,12 @@ def test_eval_matches_oracle(n):
     np.testing.assert_allclose(mu[..., 3], mur[..., 3], rtol=2e-2)
 
 
-def test_gradient_matches_oracle():
+@pytest.mark.parametrize("n", [5000, 40000])
+def test_gradient_matches_oracle(n):
+    """5,000 records: one 64-record stage of the weight-gradient kernel per CTA; 40,000: several
+    stages per CTA, accumulated in tensor memory."""
     g = _guide(seed=7)
-    rec = _records(5000, seed=2)
+    rec = _records(n, seed=2)
     loss, grad = g.train_step(_cuda(rec), apply=False, want_grad=True)
     ref, ref_loss = oracle.guide_grad(g.params, rec, LO, HI, emulate=True)
     assert abs(loss - ref_loss) < 1e-3 * abs(ref_loss) + 1e-6
