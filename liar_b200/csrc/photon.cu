@@ -244,6 +244,24 @@ __global__ void k_scatter(const float* __restrict__ pos, uint32_t n, BuildParams
     cell_key[slot] = pack_cell(cell_coord(x, P.ox, P.inv), cell_coord(y, P.oy, P.inv), cell_coord(z, P.oz, P.inv));
 }
 
+// bit 31 of a bucket's start marks a bucket that holds photons of more than one cell (hash
+// collisions): the photons of a bucket are contiguous, so two neighbours in the same bucket with
+// different cell keys mark it; the gather checks the cell keys of such buckets photon by photon
+// and those of the other buckets once
+constexpr uint32_t kBucketMixed = 0x80000000u;
+__device__ __forceinline__ uint32_t bucket_of_key(uint64_t k, uint32_t mask) {
+    const uint32_t m = (1u << kCellBits) - 1u;
+    return bucket_of((int)(uint32_t)(k >> (2 * kCellBits)), (int)((uint32_t)(k >> kCellBits) & m), (int)((uint32_t)k & m), mask);
+}
+__global__ void k_mark_mixed(const uint64_t* __restrict__ cell_key, uint32_t n, uint32_t mask, uint32_t* __restrict__ start) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0 || i >= n) return;
+    const uint64_t a = cell_key[i - 1], b = cell_key[i];
+    if (a == b) return;
+    const uint32_t ba = bucket_of_key(a, mask), bb = bucket_of_key(b, mask);
+    if (ba == bb) atomicOr(start + bb, kBucketMixed);
+}
+
 // ---- warp sorting helpers on 64-bit keys
 __device__ __forceinline__ uint64_t shfl_xor64(uint64_t v, int m) {
     return __shfl_xor_sync(0xffffffffu, (unsigned long long)v, m);
@@ -433,16 +451,22 @@ __global__ void __launch_bounds__(256) k_gather(const float4* __restrict__ sorte
                     }
                 }
                 uint32_t s0 = 0, s1 = 0;
+                uint64_t my_key = pack_cell(ix, iy, iz);
                 if (mine) {
                     const uint32_t b = bucket_of(ix, iy, iz, P.mask);
-                    s0 = __ldg(start + b);
-                    s1 = __ldg(start + b + 1);
+                    const uint32_t r0 = __ldg(start + b);
+                    s0 = r0 & ~kBucketMixed;
+                    s1 = __ldg(start + b + 1) & ~kBucketMixed;
                     if (s0 > s1 || s1 > G.n_photons) {  // corrupt bucket range: record it, skip the cell
                         atomicOr(status, kStatusBadBucket);
                         s0 = s1 = 0;
                     }
+                    if (s1 > s0 && !(r0 & kBucketMixed)) {
+                        // a single-cell bucket: its first key tells whether it is this cell's
+                        if (__ldg(reinterpret_cast<const unsigned long long*>(cell_key) + s0) != my_key) s1 = s0;
+                        else my_key |= 1ull << 63;  // every photon of the range belongs to the cell
+                    }
                 }
-                const uint64_t my_key = pack_cell(ix, iy, iz);
                 // the chunk's photons as one list: lane j's cell owns items [excl_j, excl_j + cnt_j)
                 // of it, so that a batch of 32 candidates spans as many cells as it takes (cells
                 // hold a photon or two on average; one batch per cell would leave most lanes idle)
@@ -478,8 +502,10 @@ __global__ void __launch_bounds__(256) k_gather(const float4* __restrict__ sorte
                     uint64_t key = INF;
                     if (item < total) {
                         const uint32_t i = o_s0 + (uint32_t)(item - o_excl);
-                        if (__ldg(reinterpret_cast<const unsigned long long*>(cell_key) + i) == target) {
-                            const float4 p = __ldg(sorted + i);
+                        const float4 p = __ldg(sorted + i);
+                        const bool in_cell = (target >> 63) != 0ull ||
+                                             __ldg(reinterpret_cast<const unsigned long long*>(cell_key) + i) == target;
+                        if (in_cell) {
                             const float d2 = dist2_exact(p.x, p.y, p.z, qx, qy, qz);
                             if (d2 < G.r2max) key = ((uint64_t)__float_as_uint(d2) << 32) | (uint64_t)__float_as_uint(p.w);
                         }
@@ -706,9 +732,11 @@ int map_build_impl(liar_gpu_ctx* ctx, liar_gpu_photon_map* m, const float* d_pos
     }
     e = cudaMemcpyAsync(cursor, m->bucket_start, (nb + 1) * 4, cudaMemcpyDeviceToDevice, st);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "photon map cursor");
-    if (n)
+    if (n) {
         k_scatter<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_pos, (uint32_t)n, P, keys, cursor, m->sorted,
                                                               m->cell_key, ctx->d_scratch + kStatusWord);
+        k_mark_mixed<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(m->cell_key, (uint32_t)n, (uint32_t)(nb - 1), m->bucket_start);
+    }
     m->n = n;
     return ctx_cuda(ctx, cudaGetLastError(), "photon map build");
 }
