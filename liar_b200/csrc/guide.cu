@@ -371,31 +371,33 @@ __device__ __forceinline__ void store_row_bf16(__nv_bfloat16* dst, const float* 
     }
 }
 
-// the shared prologue of the two per-tile kernels: weights to shared memory, mbarriers, TMEM
+// the shared prologue of the per-tile kernels (SLOTS 4-warp slots): weights to shared memory,
+// mbarriers, TMEM (64 columns per slot)
 struct TcTile {
     uint64_t* mbar_all;
     uint32_t* tmem_slot;
     volatile uint32_t* failed;
 };
+template <int SLOTS = kTcSlots>
 __device__ __forceinline__ TcTile tc_setup(unsigned char* smem, size_t w_bytes, size_t buf_bytes,
                                            const unsigned char* __restrict__ w_img) {
     TcTile T;
-    T.mbar_all = reinterpret_cast<uint64_t*>(smem + w_bytes + (size_t)kTcSlots * buf_bytes);
-    T.tmem_slot = reinterpret_cast<uint32_t*>(T.mbar_all + kTcSlots);
+    T.mbar_all = reinterpret_cast<uint64_t*>(smem + w_bytes + (size_t)SLOTS * buf_bytes);
+    T.tmem_slot = reinterpret_cast<uint32_t*>(T.mbar_all + SLOTS);
     T.failed = T.tmem_slot + 1;
     const uint32_t tid = threadIdx.x;
     const uint4* s = reinterpret_cast<const uint4*>(w_img);
     uint4* d = reinterpret_cast<uint4*>(smem);
-    for (uint32_t i = tid; i < w_bytes / 16; i += kTcThreads) d[i] = s[i];
+    for (uint32_t i = tid; i < w_bytes / 16; i += 128u * SLOTS) d[i] = s[i];
     if (tid == 0) {
-        for (int k = 0; k < kTcSlots; ++k)
+        for (int k = 0; k < SLOTS; ++k)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(T.mbar_all + k)));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        T.failed[0] = T.failed[1] = 0u;
+        for (int k = 0; k < SLOTS; ++k) T.failed[k] = 0u;
     }
     if ((tid >> 5) == 0) {
         const uint32_t sa = (uint32_t)__cvta_generic_to_shared(T.tmem_slot);
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sa), "r"(kTcTmemCols));
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sa), "r"(64u * SLOTS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     fence_async_smem();
@@ -405,12 +407,17 @@ __device__ __forceinline__ TcTile tc_setup(unsigned char* smem, size_t w_bytes, 
     return T;
 }
 
+template <int SLOTS = kTcSlots>
 __device__ __forceinline__ void tc_teardown(const TcTile& T, uint32_t* status) {
     tc_fence_before();
     __syncthreads();
     if ((threadIdx.x >> 5) == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*T.tmem_slot), "r"(kTcTmemCols));
-    if (threadIdx.x == 0 && (T.failed[0] | T.failed[1])) atomicOr(status, kStatusTimeout);
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*T.tmem_slot), "r"(64u * SLOTS));
+    if (threadIdx.x == 0) {
+        uint32_t f = 0;
+        for (int k = 0; k < SLOTS; ++k) f |= T.failed[k];
+        if (f) atomicOr(status, kStatusTimeout);
+    }
 }
 
 // one layer of a slot: K / 16 MMAs by the slot's thread 0, committed to the slot's mbarrier, then a
@@ -520,18 +527,22 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_train_fwd_tc(const unsigned c
 }
 
 constexpr uint32_t kBwdBuf = (uint32_t)kTcRows * kWidth * 2;  // a slot's A operand: 128 x 64 bf16
-constexpr size_t kBwdTcSmem = 1024 + kUmmaWbBytes + (size_t)kTcSlots * kBwdBuf + 128;
+constexpr int kBwdSlots = 4;
+constexpr int kBwdThreads = 128 * kBwdSlots;
+constexpr size_t kBwdTcSmem = 1024 + kUmmaWbBytes + (size_t)kBwdSlots * kBwdBuf + 128;
 
-__global__ void __launch_bounds__(kTcThreads) k_train_bwd_tc(const unsigned char* __restrict__ wb_img,
-                                                             const uint32_t* __restrict__ n_dev, size_t n_max,
-                                                             const __nv_bfloat16* __restrict__ act,
-                                                             const __nv_bfloat16* __restrict__ gout,
-                                                             __nv_bfloat16* __restrict__ delta,
-                                                             uint32_t* __restrict__ status, uint32_t max_tries,
-                                                             int issue_mma) {
+// Four slots of 128 records; per layer the record's h_l row (the ReLU mask) is loaded before the
+// layer's MMAs are waited for, and the accumulator is read 32 columns at a time.
+__global__ void __launch_bounds__(kBwdThreads, 1) k_train_bwd_tc(const unsigned char* __restrict__ wb_img,
+                                                                 const uint32_t* __restrict__ n_dev, size_t n_max,
+                                                                 const __nv_bfloat16* __restrict__ act,
+                                                                 const __nv_bfloat16* __restrict__ gout,
+                                                                 __nv_bfloat16* __restrict__ delta,
+                                                                 uint32_t* __restrict__ status, uint32_t max_tries,
+                                                                 int issue_mma) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    const TcTile T = tc_setup(smem, kUmmaWbBytes, kBwdBuf, wb_img);
+    const TcTile T = tc_setup<kBwdSlots>(smem, kUmmaWbBytes, kBwdBuf, wb_img);
     const size_t n = n_dev ? min((size_t)*n_dev, n_max) : n_max;
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
     const uint32_t slot = tid >> 7, r = tid & 127u;
@@ -544,51 +555,52 @@ __global__ void __launch_bounds__(kTcThreads) k_train_bwd_tc(const unsigned char
     uint32_t phase = 0;
     const size_t n_tiles = (n + kTcRows - 1) / kTcRows;
     bool ok = true;
-    for (size_t tile = (size_t)blockIdx.x * kTcSlots + slot; ok && tile < n_tiles; tile += (size_t)gridDim.x * kTcSlots) {
+    for (size_t tile = (size_t)blockIdx.x * kBwdSlots + slot; ok && tile < n_tiles; tile += (size_t)gridDim.x * kBwdSlots) {
         const size_t row = tile * kTcRows + r;
+        const bool live = row < n;
         // the output gradient (48 wide) as the first A operand
         {
             const uint4* src = reinterpret_cast<const uint4*>(gout + row * kOut);
             unsigned char* dst = buf + (r >> 3) * (kOut / 8) * 128u + (r & 7u) * 16u;
 #pragma unroll
             for (int c = 0; c < kOut / 8; ++c)
-                *reinterpret_cast<uint4*>(dst + c * 128u) = row < n ? src[c] : make_uint4(0u, 0u, 0u, 0u);
+                *reinterpret_cast<uint4*>(dst + c * 128u) = live ? src[c] : make_uint4(0u, 0u, 0u, 0u);
         }
         for (int l = kLayers - 1; l >= 1 && ok; --l) {
+            // h_l (the mask) on its way while the layer's MMAs run
+            uint4 h[kWidth / 8];
+            const uint4* hp = reinterpret_cast<const uint4*>(act + (size_t)(l - 1) * n_max * kWidth + row * kWidth);
+#pragma unroll
+            for (int c = 0; c < kWidth / 8; ++c) h[c] = live ? hp[c] : make_uint4(0u, 0u, 0u, 0u);
             ok = tc_layer(r, tmem, buf_addr, sw_addr + umma_wb_offset(l), (uint32_t)layer_n(l), (uint32_t)kWidth, mbar_addr,
                           phase, slot, T.failed, max_tries, issue_mma);
             if (!ok) break;
-            float v[64];
-            tmem_ld_x64(taddr, v);
             // mask by h_l > 0 (the ReLU of layer l - 1's output), store delta_l, next A operand
-            if (row < n) {
-                const uint4* hp = reinterpret_cast<const uint4*>(act + (size_t)(l - 1) * n_max * kWidth + row * kWidth);
+            unsigned char* dst = buf + (r >> 3) * (kWidth / 8) * 128u + (r & 7u) * 16u;
+            uint4* drow = reinterpret_cast<uint4*>(delta + (size_t)(l - 1) * n_max * kWidth + row * kWidth);
 #pragma unroll
-                for (int c = 0; c < kWidth / 8; ++c) {
-                    const uint4 h = hp[c];
-                    const uint32_t hw[4] = {h.x, h.y, h.z, h.w};
+            for (int half = 0; half < 2; ++half) {
+                float v[32];
+                tmem_ld_32x32b<32>(taddr + 32u * half, v);
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const uint4 hh = h[4 * half + c];
+                    const uint32_t hw[4] = {hh.x, hh.y, hh.z, hh.w};
+                    uint32_t o[4];
 #pragma unroll
                     for (int e = 0; e < 4; ++e) {
-                        if (!(bf16_lo(hw[e]) > 0.0f)) v[8 * c + 2 * e] = 0.0f;
-                        if (!(bf16_hi(hw[e]) > 0.0f)) v[8 * c + 2 * e + 1] = 0.0f;
+                        const float a = bf16_lo(hw[e]) > 0.0f ? v[8 * c + 2 * e] : 0.0f;
+                        const float b = bf16_hi(hw[e]) > 0.0f ? v[8 * c + 2 * e + 1] : 0.0f;
+                        o[e] = pack_bf16(a, b);
                     }
-                }
-                store_row_bf16(delta + (size_t)(l - 1) * n_max * kWidth + row * kWidth, v, kWidth, false);
-            } else {
-                for (int c = 0; c < 64; ++c) v[c] = 0.0f;
-            }
-            if (l > 1) {
-                unsigned char* dst = buf + (r >> 3) * (kWidth / 8) * 128u + (r & 7u) * 16u;
-#pragma unroll
-                for (int c = 0; c < kWidth / 8; ++c) {
-                    const float* q = v + 8 * c;
-                    *reinterpret_cast<uint4*>(dst + c * 128u) = make_uint4(pack_bf16(q[0], q[1]), pack_bf16(q[2], q[3]),
-                                                                           pack_bf16(q[4], q[5]), pack_bf16(q[6], q[7]));
+                    const uint4 packed = make_uint4(o[0], o[1], o[2], o[3]);
+                    if (live) drow[4 * half + c] = packed;
+                    if (l > 1) *reinterpret_cast<uint4*>(dst + (4 * half + c) * 128u) = packed;
                 }
             }
         }
     }
-    tc_teardown(T, status);
+    tc_teardown<kBwdSlots>(T, status);
 }
 
 // weight gradients: shared-memory plan of one CTA (bytes from the 1024-aligned base)
@@ -926,8 +938,8 @@ int guide_train(liar_gpu_ctx* ctx, liar_gpu_guide* G, const float* d_records, co
     k_train_fwd_tc<<<tgrid, kTcThreads, kFwdTcSmem, st>>>(G->umma_w, d_records, d_count, n_max, box, G->scalars, G->act,
                                                          G->gout, G->scalars + 1, status, tries, mma);
     const unsigned bgrid =
-        (unsigned)std::max<size_t>(1, std::min<size_t>((tiles + kTcSlots - 1) / kTcSlots, (size_t)sms * 3));
-    k_train_bwd_tc<<<bgrid, kTcThreads, kBwdTcSmem, st>>>(G->umma_wb, d_count, n_max, G->act, G->gout, G->delta, status,
+        (unsigned)std::max<size_t>(1, std::min<size_t>((tiles + kBwdSlots - 1) / kBwdSlots, (size_t)sms));
+    k_train_bwd_tc<<<bgrid, kBwdThreads, kBwdTcSmem, st>>>(G->umma_wb, d_count, n_max, G->act, G->gout, G->delta, status,
                                                          tries, mma);
     // weight gradients: one CTA per SM, each over a contiguous run of whole 64-record stages
     const size_t stages = (n_max + kDwRecords - 1) / kDwRecords;
