@@ -245,27 +245,30 @@ def test_guided_render_is_unbiased():
 def test_slit_room_guide_learns_the_slit():
     """After online training in the slit room, the guide at points of the wall facing the slit puts
     far more density toward the slit than a uniform hemisphere would: it has learned where the
-    light comes from. Guided images keep the plain image's mean."""
+    light comes from."""
     scene, cam = scenes_guiding.slit_room(n_triangles=20_000)
     flat = R.flatten(scene)
     gs = R.GpuScene(default_context(), flat)
     g = GD.Guide(default_context(), GD.scene_bounds(flat), guide_probability=0.3, learning_rate=5e-3,
                  steps_per_pass=8, batch_records=65536, seed=0)
-    # 64 training passes: online training from path records is noisy (records arrive in atomic
-    # order), so the test trains long enough for every run to find the slit
-    train_d = R.render_desc(cam, 256, 256, 64, _tracer(), seed=7, wave_paths=256 * 256)
-    g.render(gs, train_d, _film(train_d).data_ptr(), train=True)
-    assert g.stats()["records"] > 20000
+    # online training from path records is noisy run to run (records arrive in atomic order, so
+    # batches differ): the guide gets up to three rounds of 64 training passes to find the slit
     rng = np.random.default_rng(0)
     n = 256
     pts = np.stack([np.full(n, -4.99), rng.uniform(1.6, 2.4, n), rng.uniform(-0.8, 0.8, n)], 1)
     to_slit = np.array([5.0, 2.0, 0.0]) - pts
     to_slit /= np.linalg.norm(to_slit, axis=1, keepdims=True)
     x = np.concatenate([pts, np.tile([1.0, 0, 0], (n, 1)), np.tile([1.0, 0, 0], (n, 1))], 1).astype(np.float32)
-    mix = g.eval(torch.from_numpy(x).cuda()).cpu().numpy()
-    q = oracle.vmf_pdf(mix, to_slit.astype(np.float32))
-    ratio = np.median(q) * 2 * np.pi  # against a uniform density over the hemisphere
-    print(f"slit room: guide density toward the slit / uniform hemisphere = {ratio:.1f}")
+    for round_ in range(3):
+        train_d = R.render_desc(cam, 256, 256, 64, _tracer(), seed=7 + round_, wave_paths=256 * 256)
+        g.render(gs, train_d, _film(train_d).data_ptr(), train=True)
+        assert g.stats()["records"] > 20000
+        mix = g.eval(torch.from_numpy(x).cuda()).cpu().numpy()
+        q = oracle.vmf_pdf(mix, to_slit.astype(np.float32))
+        ratio = np.median(q) * 2 * np.pi  # against a uniform density over the hemisphere
+        print(f"slit room, round {round_ + 1}: guide density toward the slit / uniform hemisphere = {ratio:.1f}")
+        if ratio > 5.0:
+            break
     assert ratio > 5.0
 
 
