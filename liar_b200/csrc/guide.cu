@@ -41,6 +41,7 @@ struct liar_gpu_guide {
     __nv_bfloat16* act = nullptr;    // h_1..h_5: [5][cap][64]
     __nv_bfloat16* delta = nullptr;  // delta_1..delta_5: [5][cap][64]
     __nv_bfloat16* gout = nullptr;   // [cap][48]
+    float* raw_out = nullptr;        // [cap][40]: the forward's raw outputs
     float* scalars = nullptr;        // [0] weight sum [1] loss sum
     std::vector<void*> buffers;
     unsigned long long steps_done = 0;
@@ -112,11 +113,19 @@ __global__ void k_pack_umma(const float* __restrict__ P, unsigned char* __restri
 // waits once more (bounded again) for every commit still outstanding, so that no MMA still writes
 // the accumulator, and the CTA frees its TMEM and leaves. issue_mma = 0 is the timeout test: no
 // MMA and no commit are issued, so the first wait runs out with nothing in flight.
+// TRAIN (the training forward): the inputs are training records (13 floats, the first 9 the
+// network's inputs), the row count may come from device memory (n_dev, at most n), every hidden
+// layer's bf16 activations h_1..h_5 also go to act ([5][n_max][64]) and the 40 raw outputs of each
+// row go to mix (stride 40) for the loss kernel instead of the mixture.
+template <bool TRAIN>
 __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* __restrict__ w_img,
                                                            const float* __restrict__ in, size_t n, Box box,
                                                            float* __restrict__ mix, int stride,
                                                            uint32_t* __restrict__ status, uint32_t max_tries,
-                                                           int issue_mma) {
+                                                           int issue_mma, const uint32_t* __restrict__ n_dev,
+                                                           __nv_bfloat16* __restrict__ act, size_t n_max) {
+    constexpr int IN = TRAIN ? kRecordFloats : kIn;
+    if (TRAIN && n_dev) n = min((size_t)*n_dev, n);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     unsigned char* sw = smem;
@@ -189,10 +198,10 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
         const uint32_t rows = n - row0 < (size_t)kTcRows ? (uint32_t)(n - row0) : (uint32_t)kTcRows;
         // the tile's inputs, coalesced, through shared memory (the previous tile's readers have passed
         // the slot barriers since)
-        for (uint32_t i = r; i < rows * kIn; i += 128u) stage_in[i] = __ldg(in + row0 * kIn + i);
+        for (uint32_t i = r; i < rows * IN; i += 128u) stage_in[i] = __ldg(in + row0 * IN + i);
         slot_sync();
         float x[kIn];
-        if (r < rows) normalise_input(stage_in + r * kIn, box.lo, box.inv_ext, x);
+        if (r < rows) normalise_input(stage_in + r * IN, box.lo, box.inv_ext, x);
         else
             for (int c = 0; c < kIn; ++c) x[c] = 0.0f;
         // layer 0: chunk c's encodings into half c % 2 once the chunk before last has been consumed
@@ -221,9 +230,12 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
 #pragma unroll
                     for (int c = 0; c < 4; ++c) {
                         const float* q = v + 8 * c;
-                        *reinterpret_cast<uint4*>(dst + (4 * half + c) * 128u) = make_uint4(
+                        const uint4 hq = make_uint4(
                             pack_bf16(fmaxf(q[0], 0.0f), fmaxf(q[1], 0.0f)), pack_bf16(fmaxf(q[2], 0.0f), fmaxf(q[3], 0.0f)),
                             pack_bf16(fmaxf(q[4], 0.0f), fmaxf(q[5], 0.0f)), pack_bf16(fmaxf(q[6], 0.0f), fmaxf(q[7], 0.0f)));
+                        *reinterpret_cast<uint4*>(dst + (4 * half + c) * 128u) = hq;
+                        if (TRAIN && r < rows)
+                            reinterpret_cast<uint4*>(act + (size_t)(l - 1) * n_max * kWidth + (row0 + r) * kWidth)[4 * half + c] = hq;
                     }
                 }
                 issue(buf_addr, (kWidth / 8) * 128u, sw_addr + umma_w_offset(l), (kWidth / 8) * 128u, kWidth / 16,
@@ -237,6 +249,11 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
                 tmem_ld_32x32b<8>(taddr + 32u, o + 32);
                 const uint32_t pitch = (uint32_t)stride + 4u;
                 float* srow = reinterpret_cast<float*>(buf) + r * pitch;
+                if (TRAIN) {
+#pragma unroll
+                    for (int k = 0; k < kOutUsed / 4; ++k)
+                        *reinterpret_cast<float4*>(srow + 4 * k) = make_float4(o[4 * k], o[4 * k + 1], o[4 * k + 2], o[4 * k + 3]);
+                } else {
                 Lobe lobes[kLobes];
                 float w[kLobes];
                 mixture_from_raw(o, lobes, w);
@@ -251,6 +268,7 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
                     for (int k = 0; k < kLobes; ++k) a[k] = w[k] * vmf_norm(lobes[k].kappa);
                     *reinterpret_cast<float4*>(srow + 40) = make_float4(a[0], a[1], a[2], a[3]);
                     *reinterpret_cast<float4*>(srow + 44) = make_float4(a[4], a[5], a[6], a[7]);
+                }
                 }
                 slot_sync();
                 const uint32_t per_row = (uint32_t)stride / 4u, total = rows * per_row;
@@ -327,10 +345,10 @@ __device__ float record_gradient(const float* o, float wx, float wy, float wz, f
 
 // ---- training on tcgen05 (guide_umma.cuh's operand layouts and instruction forms)
 //
-// forward  k_train_fwd_tc: the inference kernel's two 4-warp slots of 128 records; after every
+// forward  k_eval_tc<true>: the inference kernel's four 4-warp slots of 128 records; after every
 //          hidden layer its ReLU'd bf16 activations also go to global memory (h_1..h_5, for the
-//          backward masks and the weight gradients), and after the last layer each thread turns
-//          its row's 40 raw outputs into the loss and its gradient (record_gradient), stored bf16
+//          backward masks and the weight gradients) and the 40 raw outputs of each row follow;
+//          k_train_head turns them into the loss and its gradient (record_gradient), stored bf16
 // backward k_train_bwd_tc: delta_l = (delta_{l+1} W_l^T) * [h_l > 0] for l = 5..1 (delta_6 =
 //          the output gradient), one UMMA chain per 128-record tile with the weights as B
 //          operands element (n, k) = W_l[n][k] (n an input, k an output of layer l); each delta
@@ -447,83 +465,40 @@ __device__ __forceinline__ bool tc_layer(uint32_t r, uint32_t tmem, uint32_t a_a
     return true;
 }
 
-constexpr size_t kFwdTcSmem = 1024 + kUmmaWBytes + (size_t)kTcSlots * kUmmaA0Bytes + 128;
-
-__global__ void __launch_bounds__(kTcThreads, 1) k_train_fwd_tc(const unsigned char* __restrict__ w_img,
-                                                                const float* __restrict__ rec,
-                                                                const uint32_t* __restrict__ n_dev, size_t n_max, Box box,
-                                                                const float* __restrict__ scalars_in,
-                                                                __nv_bfloat16* __restrict__ act,
-                                                                __nv_bfloat16* __restrict__ gout, float* __restrict__ loss,
-                                                                uint32_t* __restrict__ status, uint32_t max_tries,
-                                                                int issue_mma) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    const TcTile T = tc_setup(smem, kUmmaWBytes, kUmmaA0Bytes, w_img);
+// the loss and its output gradient per record, from the training forward's raw outputs (one thread
+// per record): weights normalised by their batch mean and clipped at kWeightClip, gradient stored
+// bf16 (48 wide, the padding zero), the loss summed over the batch
+__global__ void __launch_bounds__(256) k_train_head(const float* __restrict__ raw, const float* __restrict__ rec,
+                                                    const uint32_t* __restrict__ n_dev, size_t n_max,
+                                                    const float* __restrict__ scalars_in,
+                                                    __nv_bfloat16* __restrict__ gout, float* __restrict__ loss) {
     const size_t n = n_dev ? min((size_t)*n_dev, n_max) : n_max;
     const float wsum = scalars_in[0];
     const float inv_mean = (wsum > 0.0f && n > 0) ? (float)n / wsum : 0.0f;
     const float inv_b = n > 0 ? 1.0f / (float)n : 0.0f;
-    const uint32_t tid = threadIdx.x, warp = tid >> 5;
-    const uint32_t slot = tid >> 7, r = tid & 127u;
-    unsigned char* buf = smem + kUmmaWBytes + slot * kUmmaA0Bytes;
-    const uint32_t tmem = *T.tmem_slot + 64u * slot;
-    const uint32_t taddr = tmem + ((32u * (warp & 3u)) << 16);
-    const uint32_t mbar_addr = (uint32_t)__cvta_generic_to_shared(T.mbar_all + slot);
-    const uint32_t sw_addr = (uint32_t)__cvta_generic_to_shared(smem);
-    const uint32_t buf_addr = (uint32_t)__cvta_generic_to_shared(buf);
-    uint32_t phase = 0;
     float lsum = 0.0f;
-    const size_t n_tiles = (n + kTcRows - 1) / kTcRows;
-    bool ok = true;
-    for (size_t tile = (size_t)blockIdx.x * kTcSlots + slot; ok && tile < n_tiles; tile += (size_t)gridDim.x * kTcSlots) {
-        const size_t row = tile * kTcRows + r;
-        float x[kIn];
-        float wx = 0.0f, wy = 0.0f, wz = 1.0f, weight = 0.0f;
-        if (row < n) {
-            const float* rr = rec + row * kRecordFloats;
-            normalise_input(rr, box.lo, box.inv_ext, x);
-            wx = rr[9];
-            wy = rr[10];
-            wz = rr[11];
-            weight = rr[12];
-            if (!(weight > 0.0f) || !isfinite(weight)) weight = 0.0f;
-        } else {
-            for (int c = 0; c < kIn; ++c) x[c] = 0.0f;
-        }
-        encode_row_umma(x, buf, r);
-        float v[64];
-        for (int l = 0; l < kLayers && ok; ++l) {
-            ok = tc_layer(r, tmem, buf_addr, sw_addr + umma_w_offset(l), (uint32_t)layer_k(l), (uint32_t)layer_n(l), mbar_addr,
-                          phase, slot, T.failed, max_tries, issue_mma);
-            if (!ok) break;
-            tmem_ld_x64(taddr, v);
-            if (l < kLayers - 1) {
-                // h_{l+1}: ReLU, bf16, to global memory and as the next A operand
-                if (row < n) store_row_bf16(act + (size_t)l * n_max * kWidth + row * kWidth, v, kWidth, true);
-                unsigned char* dst = buf + (r >> 3) * (kWidth / 8) * 128u + (r & 7u) * 16u;
+    for (size_t row = (size_t)blockIdx.x * blockDim.x + threadIdx.x; row < n; row += (size_t)gridDim.x * blockDim.x) {
+        const float* rr = rec + row * kRecordFloats;
+        float weight = rr[12];
+        if (!(weight > 0.0f) || !isfinite(weight)) weight = 0.0f;
+        float o[kOutUsed];
 #pragma unroll
-                for (int c = 0; c < kWidth / 8; ++c) {
-                    const float* q = v + 8 * c;
-                    *reinterpret_cast<uint4*>(dst + c * 128u) =
-                        make_uint4(pack_bf16(fmaxf(q[0], 0.0f), fmaxf(q[1], 0.0f)), pack_bf16(fmaxf(q[2], 0.0f), fmaxf(q[3], 0.0f)),
-                                   pack_bf16(fmaxf(q[4], 0.0f), fmaxf(q[5], 0.0f)), pack_bf16(fmaxf(q[6], 0.0f), fmaxf(q[7], 0.0f)));
-                }
-            }
+        for (int k = 0; k < kOutUsed / 4; ++k) {
+            const float4 q = reinterpret_cast<const float4*>(raw + row * kOutUsed)[k];
+            o[4 * k] = q.x;
+            o[4 * k + 1] = q.y;
+            o[4 * k + 2] = q.z;
+            o[4 * k + 3] = q.w;
         }
-        if (!ok) break;
-        if (row < n) {
-            float d[kOut];
-            for (int c = kOutUsed; c < kOut; ++c) d[c] = 0.0f;
-            const float wn = fminf(weight * inv_mean, kWeightClip);
-            lsum += record_gradient(v, wx, wy, wz, wn, inv_b, d);
-            store_row_bf16(gout + row * kOut, d, kOut, false);
-        }
+        float d[kOut];
+        for (int c = kOutUsed; c < kOut; ++c) d[c] = 0.0f;
+        const float wn = fminf(weight * inv_mean, kWeightClip);
+        lsum += record_gradient(o, rr[9], rr[10], rr[11], wn, inv_b, d);
+        store_row_bf16(gout + row * kOut, d, kOut, false);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) lsum += __shfl_down_sync(0xffffffffu, lsum, o);
-    if ((tid & 31u) == 0 && lsum != 0.0f) atomicAdd(loss, lsum * inv_b);
-    tc_teardown(T, status);
+    if ((threadIdx.x & 31u) == 0 && lsum != 0.0f) atomicAdd(loss, lsum * inv_b);
 }
 
 constexpr uint32_t kBwdBuf = (uint32_t)kTcRows * kWidth * 2;  // a slot's A operand: 128 x 64 bf16
@@ -854,12 +829,13 @@ int g_alloc(liar_gpu_ctx* ctx, liar_gpu_guide* G, size_t bytes, void** p, const 
 
 int ensure_train_buffers(liar_gpu_ctx* ctx, liar_gpu_guide* G, size_t n) {
     if (G->cap >= n) return LIAR_OK;
-    for (void* p : {(void*)G->act, (void*)G->delta, (void*)G->gout}) {
+    for (void* p : {(void*)G->act, (void*)G->delta, (void*)G->gout, (void*)G->raw_out}) {
         if (!p) continue;
         cudaFree(p);
         G->buffers.erase(std::remove(G->buffers.begin(), G->buffers.end(), p), G->buffers.end());
     }
     G->act = G->delta = G->gout = nullptr;
+    G->raw_out = nullptr;
     G->cap = 0;
     void* p = nullptr;
     int rc = g_alloc(ctx, G, n * 5 * kWidth * 2, &p, "guide activations");
@@ -871,6 +847,9 @@ int ensure_train_buffers(liar_gpu_ctx* ctx, liar_gpu_guide* G, size_t n) {
     rc = g_alloc(ctx, G, n * kOut * 2, &p, "guide output gradients");
     if (rc) return rc;
     G->gout = static_cast<__nv_bfloat16*>(p);
+    rc = g_alloc(ctx, G, n * kOutUsed * 4, &p, "guide raw outputs");
+    if (rc) return rc;
+    G->raw_out = static_cast<float*>(p);
     G->cap = n;
     return LIAR_OK;
 }
@@ -878,13 +857,13 @@ int ensure_train_buffers(liar_gpu_ctx* ctx, liar_gpu_guide* G, size_t n) {
 int smem_attrs(liar_gpu_ctx* ctx) {
     static int done_device = -1;
     if (done_device == ctx->device) return LIAR_OK;
-    cudaError_t e = cudaFuncSetAttribute(k_train_fwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwdTcSmem);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_train_bwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBwdTcSmem);
+    cudaError_t e = cudaFuncSetAttribute(k_train_bwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBwdTcSmem);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_train_dw_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDwTcSmem);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_eval_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEvSmem);
+        e = cudaFuncSetAttribute(k_eval_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEvSmem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_eval_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEvSmem);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "guide kernel attributes");
     done_device = ctx->device;
     return LIAR_OK;
@@ -934,9 +913,13 @@ int guide_train(liar_gpu_ctx* ctx, liar_gpu_guide* G, const float* d_records, co
     const int mma = wait_test ? 0 : 1;
     uint32_t* status = ctx->d_scratch + kStatusWord;
     const size_t tiles = (n_max + kTcRows - 1) / kTcRows;
-    const unsigned tgrid = (unsigned)std::max<size_t>(1, std::min<size_t>((tiles + kTcSlots - 1) / kTcSlots, (size_t)sms));
-    k_train_fwd_tc<<<tgrid, kTcThreads, kFwdTcSmem, st>>>(G->umma_w, d_records, d_count, n_max, box, G->scalars, G->act,
-                                                         G->gout, G->scalars + 1, status, tries, mma);
+    // forward: the inference kernel's four slots storing h_1..h_5 and the raw outputs, then the
+    // loss and output gradient per record
+    const unsigned tgrid = (unsigned)std::max<size_t>(1, std::min<size_t>((tiles + kEvSlots - 1) / kEvSlots, (size_t)sms));
+    k_eval_tc<true><<<tgrid, kEvThreads, kEvSmem, st>>>(G->umma_w, d_records, n_max, box, G->raw_out, kOutUsed, status,
+                                                         tries, mma, d_count, G->act, n_max);
+    k_train_head<<<(unsigned)std::max<size_t>(1, std::min<size_t>((n_max + 255) / 256, (size_t)sms * 8)), 256, 0, st>>>(
+        G->raw_out, d_records, d_count, n_max, G->scalars, G->gout, G->scalars + 1);
     const unsigned bgrid =
         (unsigned)std::max<size_t>(1, std::min<size_t>((tiles + kBwdSlots - 1) / kBwdSlots, (size_t)sms));
     k_train_bwd_tc<<<bgrid, kBwdThreads, kBwdTcSmem, st>>>(G->umma_wb, d_count, n_max, G->act, G->gout, G->delta, status,
@@ -1088,9 +1071,9 @@ int liar_gpu::guide::guide_eval(liar_gpu_ctx* ctx, const liar_gpu_guide* G, cons
     // the bounded waits' limit: 2^24 polls, far beyond a layer's MMAs; the timeout test
     // (liar_gpu_set_fault_test) issues no MMA and gives up after 2^16 polls
     const bool wait_test = ctx->fault_test == LIAR_FAULT_TEST_GUIDE_WAIT;
-    k_eval_tc<<<grid, kEvThreads, kEvSmem, st>>>(G->umma_w, d_inputs, n, make_box(G->cfg), d_mixture, stride,
-                                                   ctx->d_scratch + kStatusWord, wait_test ? 1u << 16 : 1u << 24,
-                                                   wait_test ? 0 : 1);
+    k_eval_tc<false><<<grid, kEvThreads, kEvSmem, st>>>(G->umma_w, d_inputs, n, make_box(G->cfg), d_mixture, stride,
+                                                          ctx->d_scratch + kStatusWord, wait_test ? 1u << 16 : 1u << 24,
+                                                          wait_test ? 0 : 1, nullptr, nullptr, 0);
     return ctx_cuda(ctx, cudaGetLastError(), "guide evaluation");
 }
 

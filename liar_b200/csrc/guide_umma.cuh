@@ -48,7 +48,7 @@ constexpr int kEvThreads = 128 * kEvSlots;
 constexpr uint32_t kEvTmemCols = 64 * kEvSlots;
 constexpr uint32_t kEvHalf = (uint32_t)kTcRows * 64 * 2;  // 16384
 constexpr uint32_t kEvBuf = 2 * kEvHalf;                   // 32768
-constexpr uint32_t kEvIn = (uint32_t)kTcRows * kIn * 4;     // 4608
+constexpr uint32_t kEvIn = (uint32_t)kTcRows * 13 * 4;     // 6656: 128 training records of 13 floats
 constexpr size_t kEvSmem = 1024 + kUmmaWBytes + (size_t)kEvSlots * (kEvBuf + kEvIn) + 128;
 
 // byte offset of element (row, k) in a K-major no-swizzle operand with K columns
