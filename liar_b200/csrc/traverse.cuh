@@ -138,9 +138,12 @@ struct LaneStack {
 // One inner node: st.node >= 0 on entry. Its hit children are ordered by entry distance, the
 // farther ones pushed; on exit st.node is the nearest hit child (inner node or leaf), or kNodeNone
 // when no child is hit.
-template <bool ANY, int S, int BLOCK, bool COUNT>
+// PF: 1 = prefetch the next node's line into L1 once it is known, 2 = also the first triangle line
+// of a leaf reached (the loads of the next turn then find it there)
+template <bool ANY, int S, int BLOCK, bool COUNT, int PF = 0>
 __device__ __forceinline__ void visit_node(const QNode* __restrict__ nodes, RayState& st, LaneStack<S, BLOCK>& stack,
-                                           uint64_t pol_tree, uint32_t& status, uint32_t& n_nodes) {
+                                           uint64_t pol_tree, uint32_t& status, uint32_t& n_nodes,
+                                           const QTri* __restrict__ tris = nullptr) {
     const bool nx = st.dx < 0.0f, ny = st.dy < 0.0f, nz = st.dz < 0.0f;
     if (COUNT) ++n_nodes;
     const QNode* q = nodes + st.node;
@@ -193,6 +196,11 @@ __device__ __forceinline__ void visit_node(const QNode* __restrict__ nodes, RayS
     }
     const uint32_t kf = first == 0 ? key[0] : first == 1 ? key[1] : first == 2 ? key[2] : key[3];
     st.node = sel4i(ch, kf & 3u);
+    if (PF >= 1 && st.node >= 0) {
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(nodes + st.node));
+    } else if (PF >= 2 && st.node != kNodeNone) {
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(tris + ((uint32_t)st.node & 0x07ffffffu)));
+    }
 }
 
 // Tests the leaf st.node (packed 0x80000000 | count << 27 | first). True when an any-hit ray is
@@ -262,7 +270,7 @@ __host__ __device__ __forceinline__ uint32_t trace_batch(uint32_t n, uint32_t wa
 
 // REFILL: idle lanes that trigger a refill; LEAF_AT: lanes waiting at a leaf that start the leaf
 // phase (see below); MINB: resident blocks the register allocation must allow
-template <bool ANY, int S, int BLOCK, bool COUNT, int REFILL = 8, int LEAF_AT = 8, int MINB = 1>
+template <bool ANY, int S, int BLOCK, bool COUNT, int REFILL = 8, int LEAF_AT = 8, int MINB = 1, int PF = 0>
 __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const QNode* __restrict__ nodes, const QTri* __restrict__ tris,
                                                       const liar_ray* __restrict__ rays, liar_hit* __restrict__ hits,
                                                       uint32_t n_rays, uint32_t* __restrict__ work_counter,
@@ -345,7 +353,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) trace_kernel(const QNode* __restr
         bool done = false;
         if (rid >= 0) {
             if (st.node >= 0) {
-                visit_node<ANY, S, BLOCK, COUNT>(nodes, st, stack, pol_tree, status, n_nodes);
+                visit_node<ANY, S, BLOCK, COUNT, PF>(nodes, st, stack, pol_tree, status, n_nodes, tris);
                 if (st.node == kNodeNone) done = pop_next<ANY, S, BLOCK>(st, stack);
             } else if (st.node == kNodeNone) {
                 done = true;  // a ray with non-finite components, retired untraced
