@@ -44,16 +44,46 @@ __device__ __forceinline__ float bf16_lo(uint32_t v) { return __uint_as_float(v 
 __device__ __forceinline__ float bf16_hi(uint32_t v) { return __uint_as_float(v & 0xffff0000u); }
 
 // The encoding of one row as 256 bf16 in a row-major buffer (encode_row_umma of guide_umma.cuh
-// writes the same values into the K-major operand layout). Per input two sincospif calls (pi x and
+// writes the same values into the K-major operand layout). Per input two sincospi_enc calls (pi x and
 // pi x sqrt(2)); the other frequencies by the doubling formulas sin 2a = 2 sin a cos a,
 // cos 2a = cos^2 a - sin^2 a (x fl(sqrt 2) 2^k is exactly fl(x fl(sqrt 2)) 2^k, so these are the
 // angles of the definition; the recurrence adds ~1e-6 absolute error, far below bf16).
 
+// sin(pi x) and cos(pi x) for the encodings (|x| < 2^21): x = n / 2 + r with n the nearest integer
+// to 2x (found by adding 1.5 * 2^23, whose low mantissa bits then hold n) and |r| <= 1/4, so that
+// r = x - n / 2 is exact; the Taylor polynomials of sin and cos about 0 up to the 11th and 10th
+// degree on |pi r| <= pi / 4 (truncation below 2e-9 and 1e-8), then the quarter-turn n mod 4
+// rotates (sin, cos). Absolute error a few 1e-8, far below the bf16 rounding of the encodings.
+__device__ __forceinline__ void sincospi_enc(float x, float* sp, float* cp) {
+    const float t = x + x;
+    const float big = t + 12582912.0f;  // 1.5 * 2^23
+    const int n = __float_as_int(big) - 0x4B400000;
+    const float nf = big - 12582912.0f;
+    const float r = fmaf(nf, -0.5f, x);
+    const float a = r * 3.14159265358979323846f;
+    const float a2 = a * a;
+    float ps = fmaf(a2, -2.50521083854417188e-8f, 2.75573192239858907e-6f);  // -1/11!, 1/9!
+    ps = fmaf(a2, ps, -1.98412698412698413e-4f);                             // -1/7!
+    ps = fmaf(a2, ps, 8.33333333333333333e-3f);                              // 1/5!
+    ps = fmaf(a2, ps, -1.66666666666666667e-1f);                             // -1/3!
+    const float sn = fmaf(a * a2, ps, a);
+    float pc = fmaf(a2, 2.08767569878680990e-9f, -2.75573192239858907e-7f);  // 1/12!, -1/10!
+    pc = fmaf(a2, pc, 2.48015873015873016e-5f);                              // 1/8!
+    pc = fmaf(a2, pc, -1.38888888888888889e-3f);                             // -1/6!
+    pc = fmaf(a2, pc, 4.16666666666666667e-2f);                              // 1/4!
+    pc = fmaf(a2, pc, -0.5f);                                                // -1/2!
+    const float cs = fmaf(a2, pc, 1.0f);
+    const int q = n & 3;
+    const float s_ = (q & 1) ? cs : sn, c_ = (q & 1) ? sn : cs;
+    *sp = (q & 2) ? -s_ : s_;
+    *cp = ((q + 1) & 2) ? -c_ : c_;
+}
+
 // the 12 words (24 bf16: sin/cos pairs of the 12 frequencies) of input value xd, as encode_row
 __device__ __forceinline__ void encode_input(float xd, uint32_t* w) {
     float s0, c0, s1, c1;
-    sincospif(xd, &s0, &c0);
-    sincospif(xd * 1.41421356237309515f, &s1, &c1);
+    sincospi_enc(xd, &s0, &c0);
+    sincospi_enc(xd * 1.41421356237309515f, &s1, &c1);
 #pragma unroll
     for (int k = 0; k < kFreq / 2; ++k) {
         w[2 * k] = pack_bf16(s0, c0);
@@ -72,8 +102,8 @@ __device__ __forceinline__ void encode_row(const float* x, __nv_bfloat16* row) {
 #pragma unroll
     for (int d = 0; d < kIn; ++d) {
         float s0, c0, s1, c1;
-        sincospif(x[d], &s0, &c0);
-        sincospif(x[d] * 1.41421356237309515f, &s1, &c1);
+        sincospi_enc(x[d], &s0, &c0);
+        sincospi_enc(x[d] * 1.41421356237309515f, &s1, &c1);
         uint32_t* w = dst + d * kFreq;  // pair index (d * 24 + 2 f) / 2
 #pragma unroll
         for (int k = 0; k < kFreq / 2; ++k) {

@@ -169,8 +169,8 @@ __device__ __forceinline__ void encode_row_umma(const float* x, unsigned char* a
 #pragma unroll
     for (int d = 0; d < kIn; ++d) {
         float s0, c0, s1, c1;
-        sincospif(x[d], &s0, &c0);
-        sincospif(x[d] * 1.41421356237309515f, &s1, &c1);
+        sincospi_enc(x[d], &s0, &c0);
+        sincospi_enc(x[d] * 1.41421356237309515f, &s1, &c1);
         uint32_t w[12];
 #pragma unroll
         for (int k = 0; k < kFreq / 2; ++k) {
@@ -205,8 +205,8 @@ __device__ __forceinline__ void encode_chunk_umma(const float* x, unsigned char*
     for (int d = 0; d < kIn; ++d) {
         if (3 * d + 2 < lo || 3 * d > hi) continue;
         float s0, c0, s1, c1;
-        sincospif(x[d], &s0, &c0);
-        sincospif(x[d] * 1.41421356237309515f, &s1, &c1);
+        sincospi_enc(x[d], &s0, &c0);
+        sincospi_enc(x[d] * 1.41421356237309515f, &s1, &c1);
         uint32_t w[12];
 #pragma unroll
         for (int k = 0; k < kFreq / 2; ++k) {
