@@ -363,11 +363,14 @@ def batch_bench(ctx, stream, args, world, dist, local, cpu: bool, n_scenes: int 
     return out
 
 
-def guided_bench(ctx, stream, args, world, dist, local, cpu: bool) -> dict:
+def guided_bench(ctx, stream, args, world, dist, local, cpu: bool, plain_curve: bool = False) -> dict:
     """Learned path guiding on the slit room (200k clutter triangles, 1024^2): time for guided
     rendering (online training included) to reach the error of a plain 1024-spp render, against a
     plain reference at args.guided_ref_spp (the reference's own variance is subtracted from each MSE).
-    Also the guide network's tensor-core throughput (inference and one training step)."""
+    Also the guide network's tensor-core throughput (inference and one training step).
+    plain_curve: also render the plain tracer in 16-spp chunks up to 1024 spp (outside the timed
+    plain render) and record its MSE after every power-of-two spp, the plain half of the MSE-vs-time
+    comparison."""
     import torch
     from liar_b200 import guiding as GD, render as R, scenes_guiding as SG
     res, ref_spp, plain_spp, chunk = args.guided_res, args.guided_ref_spp, 1024, 16
@@ -411,6 +414,19 @@ def guided_bench(ctx, stream, args, world, dist, local, cpu: bool) -> dict:
     plain_s = e0.elapsed_time(e1) * 1e-3
     plain_mse = mse(plain)
     plain_stats = gs.stats()
+    pcurve = []
+    if plain_curve:
+        pf, t_cum, spp = film(), 0.0, 0
+        while spp < plain_spp:
+            e0.record(stream)
+            gs.render_device(R.render_desc(cam, res, res, chunk, tracer, seed=9, first_sample=spp), pf.data_ptr(), st)
+            e1.record(stream)
+            stream.synchronize()
+            t_cum += e0.elapsed_time(e1) * 1e-3
+            spp += chunk
+            if spp & (spp - 1) == 0:
+                pcurve.append((round(t_cum, 4), spp, mse(pf)))
+        del pf
     # guided: chunks of 16 spp; during the first train_chunks chunks the guide trains after every
     # pass over the image (4 Adam steps of 16,384 records)
     c_guide, lp_guide, train_chunks = 0.4, 0.1, 4
@@ -471,6 +487,7 @@ def guided_bench(ctx, stream, args, world, dist, local, cpu: bool) -> dict:
                       "training_chunks": train_chunks, "chunk_spp": chunk, "adam_steps": gstats["steps"],
                       "batch_records": 16384, "guide_probability": c_guide, "light_probability": lp_guide,
                       "curve_t_spp_mse": curve[:: max(1, len(curve) // 24)]},
+           **({"plain_curve_t_spp_mse": pcurve} if plain_curve else {}),
            "time_ratio_guided_over_plain": (t_hit / plain_s) if t_hit else None,
            "network": {"inference_queries_per_s": (1 << 20) / eval_s,
                        "inference_tflops": flop_fwd * (1 << 20) / eval_s / 1e12,
@@ -487,13 +504,14 @@ def guided_bench(ctx, stream, args, world, dist, local, cpu: bool) -> dict:
         d = R.render_desc(cam, cres, cres, 16, tracer, seed=3)
         cfilm = np.zeros((cres, cres, 8), np.float32)
         rows, t0 = 0, time.perf_counter()
-        while time.perf_counter() - t0 < 8.0 and rows < cres:
-            rs.render(d, cfilm, pixels=(rows * cres, (rows + 4) * cres))
+        while time.perf_counter() - t0 < 2.0:  # whole 16-spp frames, repeated, for at least 2 s
+            r0 = rows % cres
+            rs.render(d, cfilm, pixels=(r0 * cres, (r0 + 4) * cres))
             rows += 4
         dt = time.perf_counter() - t0
         out["cpu_baseline"] = {"value": rows * cres * 16 / dt, "unit": "samples/s", "cores": oracle.hardware_threads(),
-                               "kind": "port", "sample": f"plain path tracing, {rows} rows of a {cres}^2 16-spp "
-                                                         f"render of the slit room, {dt:.1f} s"}
+                               "kind": "port", "sample": f"plain path tracing, {rows} rows (in passes over a {cres}^2 "
+                                                         f"16-spp render) of the slit room, {dt:.1f} s"}
     g.close()
     gs.close()
     return out
@@ -736,7 +754,8 @@ def run_case(name: str) -> None:
     the Cornell frame, 256^2 x 4 spp, twice), shade (the Cornell path-tracing frame, twice),
     gather (k = 64 over 4M uniform photons for 256k uniform queries, twice), gather-photon (the
     photon workload's gather: 10M photons, the 1080p camera queries, k = 64, twice), guided (the slit
-    room at 256^2: 4 training passes, then 16 guided samples per pixel), pm (the PhotonMapper on
+    room at 256^2: 4 training passes, then 16 guided samples per pixel), guided-crossing (the guiding
+    workload against a 65,536-spp plain reference, both MSE curves), pm (the PhotonMapper on
     the photon scene, 1M global photons, 480 x 270, two frames)."""
     import torch
     from liar_b200.kernel import default_context
@@ -774,6 +793,13 @@ def run_case(name: str) -> None:
              else R.render_desc(e.camera, 256, 256, 16, e.tracer))
         for _ in range(2):
             gs.render_device(d, film.data_ptr())
+    elif name == "guided-crossing":
+        # the guiding workload measured against its stated reference: a plain 65,536-spp render of
+        # the slit room at 1024^2 (about 2.5 minutes), the plain MSE-vs-time curve beside the guided one
+        stream = torch.cuda.Stream()
+        args = argparse.Namespace(guided_res=1024, guided_ref_spp=65536)
+        out = guided_bench(ctx, stream, args, 1, None, 0, cpu=False, plain_curve=True)
+        print(json.dumps({"case": name, "guided": out}), flush=True)
     elif name == "guided":
         from liar_b200 import guiding as GD, render as R, scenes_guiding as SG
         scene, cam = SG.slit_room(200_000)
