@@ -30,7 +30,6 @@ struct liar_gpu_guide {
     int device = -1;
     liar_guide_config cfg{};
     float* params = nullptr;   // f32 master weights
-    float* grads = nullptr;
     float* adam_m = nullptr;
     float* adam_v = nullptr;
     uint32_t* step = nullptr;  // Adam step count (device)
@@ -41,7 +40,8 @@ struct liar_gpu_guide {
     __nv_bfloat16* act = nullptr;    // h_1..h_5: [5][cap][64]
     __nv_bfloat16* delta = nullptr;  // delta_1..delta_5: [5][cap][64]
     __nv_bfloat16* gout = nullptr;   // [cap][48]
-    float* raw_out = nullptr;        // [cap][40]: the forward's raw outputs
+    float* grad_part = nullptr;      // [part_cap][kParams]: the weight-gradient CTAs' partial sums
+    int part_cap = 0;
     float* scalars = nullptr;        // [0] weight sum [1] loss sum
     std::vector<void*> buffers;
     unsigned long long steps_done = 0;
@@ -92,9 +92,16 @@ Box make_box(const liar_guide_config& c) {
 
 // ---- operand images
 
-// the tcgen05 B operands: layer l's element (n, k) = W_l[k][n] at umma_offset(n, k, K_l)
-// (bump: count the Adam step just taken)
-__global__ void k_pack_umma(const float* __restrict__ P, unsigned char* __restrict__ img, uint32_t* step, int bump) {
+// backward B images: layer l (1..5) element (n, k) = W_l[n][k] at umma_offset(n, k, N_l)
+__host__ __device__ constexpr uint32_t umma_wb_offset(int l) { return 8192u * (uint32_t)(l - 1); }
+constexpr uint32_t kUmmaWbBytes = 4u * 8192u + 6144u;  // W1..W4 64 x 64, W5 64 x 48
+
+
+// the tcgen05 B operands: layer l's element (n, k) = W_l[k][n] at umma_offset(n, k, K_l) in img
+// (the forward), and for l >= 1 element (k, n) at umma_offset(k, n, N_l) in img_b (the backward,
+// W_l transposed); bump: count the Adam step just taken
+__global__ void k_pack_umma(const float* __restrict__ P, unsigned char* __restrict__ img,
+                            unsigned char* __restrict__ img_b, uint32_t* step, int bump) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;  // one parameter (k, n) per thread
     if (i == 0 && bump) *step += 1;
     if (i >= kParams) return;
@@ -102,8 +109,43 @@ __global__ void k_pack_umma(const float* __restrict__ P, unsigned char* __restri
     while (l < 5 && i >= param_offset(l + 1)) ++l;
     const int loc = i - param_offset(l), N = layer_n(l), K = layer_k(l);
     const int k = loc / N, n = loc % N;
-    *reinterpret_cast<__nv_bfloat16*>(img + umma_w_offset(l) + umma_offset((uint32_t)n, (uint32_t)k, (uint32_t)K)) =
-        __float2bfloat16_rn(P[i]);
+    const __nv_bfloat16 w = __float2bfloat16_rn(P[i]);
+    *reinterpret_cast<__nv_bfloat16*>(img + umma_w_offset(l) + umma_offset((uint32_t)n, (uint32_t)k, (uint32_t)K)) = w;
+    if (l >= 1)
+        *reinterpret_cast<__nv_bfloat16*>(img_b + umma_wb_offset(l) + umma_offset((uint32_t)k, (uint32_t)n, (uint32_t)N)) = w;
+}
+
+// the loss gradient of one record with respect to the 40 raw outputs (scaled by `scale`)
+__device__ float record_gradient(const float* o, float wx, float wy, float wz, float weight, float scale, float* d) {
+    Lobe L[kLobes];
+    float pi[kLobes], la[kLobes], cs[kLobes];
+    mixture_from_raw(o, L, pi);
+    float mx = -3.0e38f;
+    for (int l = 0; l < kLobes; ++l) {
+        cs[l] = L[l].mx * wx + L[l].my * wy + L[l].mz * wz;
+        la[l] = logf(pi[l]) + vmf_log_pdf(L[l].kappa, cs[l]);
+        mx = fmaxf(mx, la[l]);
+    }
+    float s = 0.0f;
+    for (int l = 0; l < kLobes; ++l) s += expf(la[l] - mx);
+    const float lq = mx + logf(s);
+    const float ws = weight * scale;
+    for (int l = 0; l < kLobes; ++l) {
+        const float r = expf(la[l] - lq);
+        const float k = L[l].kappa;
+        const float c = -ws * r;
+        d[5 * l + 4] = -ws * (r - pi[l]);
+        const float sk = o[5 * l + 3];
+        d[5 * l + 3] = (sk > kLogKappaMin && sk < kLogKappaMax) ? c * k * (1.0f / k - 2.0f / expm1f(2.0f * k) + cs[l] - 1.0f)
+                                                                 : 0.0f;
+        // d mu / d m = (I - mu mu^T) / |m|
+        const float nm = sqrtf(o[5 * l] * o[5 * l] + o[5 * l + 1] * o[5 * l + 1] + o[5 * l + 2] * o[5 * l + 2]);
+        const float f = c * k / fmaxf(nm, kMeanNormMin);
+        d[5 * l + 0] = f * (wx - cs[l] * L[l].mx);
+        d[5 * l + 1] = f * (wy - cs[l] * L[l].my);
+        d[5 * l + 2] = f * (wz - cs[l] * L[l].mz);
+    }
+    return -weight * lq;
 }
 
 // ---- inference on tcgen05: four slots of 128 rows per CTA (guide_umma.cuh)
@@ -115,17 +157,26 @@ __global__ void k_pack_umma(const float* __restrict__ P, unsigned char* __restri
 // MMA and no commit are issued, so the first wait runs out with nothing in flight.
 // TRAIN (the training forward): the inputs are training records (13 floats, the first 9 the
 // network's inputs), the row count may come from device memory (n_dev, at most n), every hidden
-// layer's bf16 activations h_1..h_5 also go to act ([5][n_max][64]) and the 40 raw outputs of each
-// row go to mix (stride 40) for the loss kernel instead of the mixture.
+// layer's bf16 activations h_1..h_5 also go to act ([5][n_max][64]), and the output layer ends in
+// the loss head instead of the mixture: each row's loss gradient with respect to its 40 raw outputs
+// (record_gradient, weights normalised by the batch mean train[0] from k_weight_sum and clipped)
+// goes to gout as 48 bf16 (the last 8 zero), the batch loss is added to train[1].
 template <bool TRAIN>
 __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* __restrict__ w_img,
                                                            const float* __restrict__ in, size_t n, Box box,
                                                            float* __restrict__ mix, int stride,
                                                            uint32_t* __restrict__ status, uint32_t max_tries,
                                                            int issue_mma, const uint32_t* __restrict__ n_dev,
-                                                           __nv_bfloat16* __restrict__ act, size_t n_max) {
+                                                           __nv_bfloat16* __restrict__ act, size_t n_max,
+                                                           float* __restrict__ train, __nv_bfloat16* __restrict__ gout) {
     constexpr int IN = TRAIN ? kRecordFloats : kIn;
     if (TRAIN && n_dev) n = min((size_t)*n_dev, n);
+    float inv_mean = 0.0f, inv_b = 0.0f;  // TRAIN: 1 / mean record weight, 1 / batch size
+    if (TRAIN) {
+        const float wsum = train[0];
+        inv_mean = (wsum > 0.0f && n > 0) ? (float)n / wsum : 0.0f;
+        inv_b = n > 0 ? 1.0f / (float)n : 0.0f;
+    }
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     unsigned char* sw = smem;
@@ -247,13 +298,34 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
                 float o[kOutUsed];
                 tmem_ld_32x32b<32>(taddr, o);
                 tmem_ld_32x32b<8>(taddr + 32u, o + 32);
+                if (TRAIN) {
+                    // the loss head: row r's gradient as 48 bf16 (96 B) into the staging rows, the
+                    // loss summed per warp, then the slot's gradient rows leave as one coalesced block
+                    float lsum = 0.0f;
+                    if (r < rows) {
+                        const float* rr = stage_in + r * IN;
+                        float weight = rr[12];
+                        if (!(weight > 0.0f) || !isfinite(weight)) weight = 0.0f;
+                        float d[kOut];
+#pragma unroll
+                        for (int c = kOutUsed; c < kOut; ++c) d[c] = 0.0f;
+                        lsum = record_gradient(o, rr[9], rr[10], rr[11], fminf(weight * inv_mean, kWeightClip), inv_b, d);
+                        uint4* grow = reinterpret_cast<uint4*>(buf + r * (kOut * 2));
+#pragma unroll
+                        for (int c = 0; c < kOut / 8; ++c)
+                            grow[c] = make_uint4(pack_bf16(d[8 * c], d[8 * c + 1]), pack_bf16(d[8 * c + 2], d[8 * c + 3]),
+                                                 pack_bf16(d[8 * c + 4], d[8 * c + 5]), pack_bf16(d[8 * c + 6], d[8 * c + 7]));
+                    }
+#pragma unroll
+                    for (int s = 16; s > 0; s >>= 1) lsum += __shfl_down_sync(0xffffffffu, lsum, s);
+                    if ((tid & 31u) == 0 && lsum != 0.0f) atomicAdd(train + 1, lsum * inv_b);
+                    slot_sync();
+                    const uint4* srows = reinterpret_cast<const uint4*>(buf);
+                    uint4* gdst = reinterpret_cast<uint4*>(gout + row0 * kOut);
+                    for (uint32_t i = r; i < rows * (kOut * 2 / 16); i += 128u) gdst[i] = srows[i];
+                } else {
                 const uint32_t pitch = (uint32_t)stride + 4u;
                 float* srow = reinterpret_cast<float*>(buf) + r * pitch;
-                if (TRAIN) {
-#pragma unroll
-                    for (int k = 0; k < kOutUsed / 4; ++k)
-                        *reinterpret_cast<float4*>(srow + 4 * k) = make_float4(o[4 * k], o[4 * k + 1], o[4 * k + 2], o[4 * k + 3]);
-                } else {
                 Lobe lobes[kLobes];
                 float w[kLobes];
                 mixture_from_raw(o, lobes, w);
@@ -269,13 +341,13 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
                     *reinterpret_cast<float4*>(srow + 40) = make_float4(a[0], a[1], a[2], a[3]);
                     *reinterpret_cast<float4*>(srow + 44) = make_float4(a[4], a[5], a[6], a[7]);
                 }
-                }
                 slot_sync();
                 const uint32_t per_row = (uint32_t)stride / 4u, total = rows * per_row;
                 float4* gdst = reinterpret_cast<float4*>(mix + row0 * (size_t)stride);
                 for (uint32_t i = r; i < total; i += 128u) {
                     const uint32_t q = i / per_row, c4 = i - q * per_row;
                     gdst[i] = *reinterpret_cast<const float4*>(reinterpret_cast<const float*>(buf) + q * pitch + 4u * c4);
+                }
                 }
             }
         }
@@ -310,45 +382,13 @@ __global__ void k_weight_sum(const float* __restrict__ rec, const uint32_t* __re
     if ((threadIdx.x & 31) == 0 && s != 0.0f) atomicAdd(scalars, s);
 }
 
-// the loss gradient of one record with respect to the 40 raw outputs (scaled by `scale`)
-__device__ float record_gradient(const float* o, float wx, float wy, float wz, float weight, float scale, float* d) {
-    Lobe L[kLobes];
-    float pi[kLobes], la[kLobes], cs[kLobes];
-    mixture_from_raw(o, L, pi);
-    float mx = -3.0e38f;
-    for (int l = 0; l < kLobes; ++l) {
-        cs[l] = L[l].mx * wx + L[l].my * wy + L[l].mz * wz;
-        la[l] = logf(pi[l]) + vmf_log_pdf(L[l].kappa, cs[l]);
-        mx = fmaxf(mx, la[l]);
-    }
-    float s = 0.0f;
-    for (int l = 0; l < kLobes; ++l) s += expf(la[l] - mx);
-    const float lq = mx + logf(s);
-    const float ws = weight * scale;
-    for (int l = 0; l < kLobes; ++l) {
-        const float r = expf(la[l] - lq);
-        const float k = L[l].kappa;
-        const float c = -ws * r;
-        d[5 * l + 4] = -ws * (r - pi[l]);
-        const float sk = o[5 * l + 3];
-        d[5 * l + 3] = (sk > kLogKappaMin && sk < kLogKappaMax) ? c * k * (1.0f / k - 2.0f / expm1f(2.0f * k) + cs[l] - 1.0f)
-                                                                 : 0.0f;
-        // d mu / d m = (I - mu mu^T) / |m|
-        const float nm = sqrtf(o[5 * l] * o[5 * l] + o[5 * l + 1] * o[5 * l + 1] + o[5 * l + 2] * o[5 * l + 2]);
-        const float f = c * k / fmaxf(nm, kMeanNormMin);
-        d[5 * l + 0] = f * (wx - cs[l] * L[l].mx);
-        d[5 * l + 1] = f * (wy - cs[l] * L[l].my);
-        d[5 * l + 2] = f * (wz - cs[l] * L[l].mz);
-    }
-    return -weight * lq;
-}
 
 // ---- training on tcgen05 (guide_umma.cuh's operand layouts and instruction forms)
 //
 // forward  k_eval_tc<true>: the inference kernel's four 4-warp slots of 128 records; after every
 //          hidden layer its ReLU'd bf16 activations also go to global memory (h_1..h_5, for the
-//          backward masks and the weight gradients) and the 40 raw outputs of each row follow;
-//          k_train_head turns them into the loss and its gradient (record_gradient), stored bf16
+//          backward masks and the weight gradients); its output layer ends in the loss head (the
+//          loss and its gradient per record, record_gradient), stored bf16
 // backward k_train_bwd_tc: delta_l = (delta_{l+1} W_l^T) * [h_l > 0] for l = 5..1 (delta_6 =
 //          the output gradient), one UMMA chain per 128-record tile with the weights as B
 //          operands element (n, k) = W_l[n][k] (n an input, k an output of layer l); each delta
@@ -363,31 +403,6 @@ __device__ float record_gradient(const float* o, float wx, float wy, float wz, f
 // Every mbarrier wait is bounded (max_tries polls): a wait that runs out records kStatusTimeout,
 // waits once more (bounded) for the commit it gave up on, and the CTA frees its tensor memory.
 // issue_mma = 0 (the fault test) issues no MMA or commit, so the first wait runs out.
-
-// backward B images: layer l (1..5) element (n, k) = W_l[n][k] at umma_offset(n, k, N_l)
-__host__ __device__ constexpr uint32_t umma_wb_offset(int l) { return 8192u * (uint32_t)(l - 1); }
-constexpr uint32_t kUmmaWbBytes = 4u * 8192u + 6144u;  // W1..W4 64 x 64, W5 64 x 48
-
-__global__ void k_pack_umma_bwd(const float* __restrict__ P, unsigned char* __restrict__ img) {
-    const int i = param_offset(1) + blockIdx.x * blockDim.x + threadIdx.x;  // the parameters of W1..W5
-    if (i >= kParams) return;
-    int l = 1;
-    while (l < 5 && i >= param_offset(l + 1)) ++l;
-    const int loc = i - param_offset(l), N = layer_n(l);
-    const int in = loc / N, out = loc % N;
-    *reinterpret_cast<__nv_bfloat16*>(img + umma_wb_offset(l) + umma_offset((uint32_t)in, (uint32_t)out, (uint32_t)N)) =
-        __float2bfloat16_rn(P[i]);
-}
-
-__device__ __forceinline__ void store_row_bf16(__nv_bfloat16* dst, const float* v, int n, bool relu) {
-    uint4* d = reinterpret_cast<uint4*>(dst);
-    for (int c = 0; c < n / 8; ++c) {
-        const float* q = v + 8 * c;
-        auto f = [&](float x) { return relu ? fmaxf(x, 0.0f) : x; };
-        d[c] = make_uint4(pack_bf16(f(q[0]), f(q[1])), pack_bf16(f(q[2]), f(q[3])), pack_bf16(f(q[4]), f(q[5])),
-                          pack_bf16(f(q[6]), f(q[7])));
-    }
-}
 
 // the shared prologue of the per-tile kernels (SLOTS 4-warp slots): weights to shared memory,
 // mbarriers, TMEM (64 columns per slot)
@@ -468,38 +483,6 @@ __device__ __forceinline__ bool tc_layer(uint32_t r, uint32_t tmem, uint32_t a_a
 // the loss and its output gradient per record, from the training forward's raw outputs (one thread
 // per record): weights normalised by their batch mean and clipped at kWeightClip, gradient stored
 // bf16 (48 wide, the padding zero), the loss summed over the batch
-__global__ void __launch_bounds__(256) k_train_head(const float* __restrict__ raw, const float* __restrict__ rec,
-                                                    const uint32_t* __restrict__ n_dev, size_t n_max,
-                                                    const float* __restrict__ scalars_in,
-                                                    __nv_bfloat16* __restrict__ gout, float* __restrict__ loss) {
-    const size_t n = n_dev ? min((size_t)*n_dev, n_max) : n_max;
-    const float wsum = scalars_in[0];
-    const float inv_mean = (wsum > 0.0f && n > 0) ? (float)n / wsum : 0.0f;
-    const float inv_b = n > 0 ? 1.0f / (float)n : 0.0f;
-    float lsum = 0.0f;
-    for (size_t row = (size_t)blockIdx.x * blockDim.x + threadIdx.x; row < n; row += (size_t)gridDim.x * blockDim.x) {
-        const float* rr = rec + row * kRecordFloats;
-        float weight = rr[12];
-        if (!(weight > 0.0f) || !isfinite(weight)) weight = 0.0f;
-        float o[kOutUsed];
-#pragma unroll
-        for (int k = 0; k < kOutUsed / 4; ++k) {
-            const float4 q = reinterpret_cast<const float4*>(raw + row * kOutUsed)[k];
-            o[4 * k] = q.x;
-            o[4 * k + 1] = q.y;
-            o[4 * k + 2] = q.z;
-            o[4 * k + 3] = q.w;
-        }
-        float d[kOut];
-        for (int c = kOutUsed; c < kOut; ++c) d[c] = 0.0f;
-        const float wn = fminf(weight * inv_mean, kWeightClip);
-        lsum += record_gradient(o, rr[9], rr[10], rr[11], wn, inv_b, d);
-        store_row_bf16(gout + row * kOut, d, kOut, false);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) lsum += __shfl_down_sync(0xffffffffu, lsum, o);
-    if ((threadIdx.x & 31u) == 0 && lsum != 0.0f) atomicAdd(loss, lsum * inv_b);
-}
 
 constexpr uint32_t kBwdBuf = (uint32_t)kTcRows * kWidth * 2;  // a slot's A operand: 128 x 64 bf16
 constexpr int kBwdSlots = 4;
@@ -619,7 +602,7 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw_tc(const float* __re
                                                                const __nv_bfloat16* __restrict__ act,
                                                                const __nv_bfloat16* __restrict__ delta,
                                                                const __nv_bfloat16* __restrict__ gout,
-                                                               float* __restrict__ grads, size_t per_cta,
+                                                               float* __restrict__ part, size_t per_cta,
                                                                uint32_t* __restrict__ status, uint32_t max_tries,
                                                                int issue_mma) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -767,24 +750,27 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw_tc(const float* __re
     }
     __syncthreads();
     tc_fence_after();
-    if (!*failed && issued_any) {
-        // warp w reads lane quarter w % 4 (features 32 (w % 4) ..); warps 0-3 take dW0 and dW1, 4-7
-        // dW2..dW5
+    // the CTA's partial sums of all six weight gradients to its own slice of part (every entry
+    // written, zero when it had no records or gave up), in the parameters' layout; k_adam_reduce
+    // adds the slices. Warp w reads lane quarter w % 4 (features 32 (w % 4) ..); warps 0-3 take
+    // dW0 and dW1, 4-7 dW2..dW5; a thread's row leaves as float4 stores.
+    {
+        const bool have = !*failed && issued_any;  // uniform over the CTA
+        float* P = part + (size_t)blockIdx.x * kParams;
         const uint32_t q = warp & 3u, m = 32u * q + (tid & 31u);
         const uint32_t lane_base = (32u * q) << 16;
         for (int acc_i = (warp < 4 ? 0 : 3); acc_i < (warp < 4 ? 3 : 7); ++acc_i) {
+            if (acc_i >= 2 && q >= 2) continue;  // dW1..dW5 have 64 features: lane quarters 0 and 1
             float v[64];
-            tmem_ld_x64(tmem + lane_base + 64u * (uint32_t)acc_i, v);
-            if (acc_i <= 1) {  // dW0: features m (block 0) or 128 + m (block 1), 64 outputs
-                float* G = grads + param_offset(0) + (size_t)(m + 128u * (uint32_t)acc_i) * kWidth;
-                for (int c = 0; c < kWidth; ++c)
-                    if (v[c] != 0.0f) atomicAdd(G + c, v[c]);
-            } else if (m < (uint32_t)kWidth) {  // dW_l, l = acc_i - 1: features m < 64
-                const int l = acc_i - 1, N = layer_n(l);
-                float* G = grads + param_offset(l) + (size_t)m * N;
-                for (int c = 0; c < N; ++c)
-                    if (v[c] != 0.0f) atomicAdd(G + c, v[c]);
-            }
+            if (have) tmem_ld_x64(tmem + lane_base + 64u * (uint32_t)acc_i, v);
+            else
+                for (int c = 0; c < 64; ++c) v[c] = 0.0f;
+            const int l = acc_i <= 1 ? 0 : acc_i - 1, N = layer_n(l);
+            const uint32_t row = acc_i <= 1 ? m + 128u * (uint32_t)acc_i : m;  // dW0: block 1 holds features 128..255
+            float4* G = reinterpret_cast<float4*>(P + param_offset(l) + (size_t)row * N);
+#pragma unroll
+            for (int c = 0; c < 16; ++c)
+                if (4 * c < N) G[c] = make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
         }
     }
     tc_fence_before();
@@ -793,26 +779,56 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw_tc(const float* __re
     if (tid == 0 && *failed) atomicOr(status, kStatusTimeout);
 }
 
-__global__ void k_adam(float* __restrict__ P, float* __restrict__ Gr, float* __restrict__ M, float* __restrict__ V,
-                       const uint32_t* __restrict__ step, float lr, float b1, float b2, float eps, float* grad_out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= kParams) return;
-    const float g = Gr[i];
-    if (grad_out) grad_out[i] = g;
-    Gr[i] = 0.0f;
+// The weight gradient (the sum of the nparts partial slices of k_train_dw_tc, in a fixed order, so
+// that a step is reproducible) and Adam on the f32 master weights. A block covers 32 float4
+// columns of parameters; its 8 warps sum every 8th slice each, then warp 0 adds the 8 sums.
+constexpr int kReduceCols = 32, kReduceGroups = 8;
+__global__ void __launch_bounds__(kReduceCols * kReduceGroups) k_adam_reduce(
+    const float* __restrict__ part, int nparts, float* __restrict__ P, float* __restrict__ M, float* __restrict__ V,
+    const uint32_t* __restrict__ step, float lr, float b1, float b2, float eps, float* __restrict__ grad_out) {
+    __shared__ float4 sums[kReduceGroups][kReduceCols];
+    const int lane = threadIdx.x % kReduceCols, grp = threadIdx.x / kReduceCols;
+    const int c4 = blockIdx.x * kReduceCols + lane;
+    const bool live = c4 < kParams / 4;
+    float4 acc = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (live) {
+#pragma unroll 4
+        for (int p = grp; p < nparts; p += kReduceGroups) {
+            const float4 x = __ldcs(reinterpret_cast<const float4*>(part + (size_t)p * kParams) + c4);
+            acc.x += x.x;
+            acc.y += x.y;
+            acc.z += x.z;
+            acc.w += x.w;
+        }
+    }
+    sums[grp][lane] = acc;
+    __syncthreads();
+    if (grp != 0 || !live) return;
+    float g[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    for (int k = 0; k < kReduceGroups; ++k) {
+        g[0] += sums[k][lane].x;
+        g[1] += sums[k][lane].y;
+        g[2] += sums[k][lane].z;
+        g[3] += sums[k][lane].w;
+    }
+    if (grad_out) reinterpret_cast<float4*>(grad_out)[c4] = make_float4(g[0], g[1], g[2], g[3]);
     if (lr <= 0.0f) return;  // gradients only
     const float t = (float)(*step + 1);
-    const float m = b1 * M[i] + (1.0f - b1) * g;
-    const float v = b2 * V[i] + (1.0f - b2) * g * g;
-    M[i] = m;
-    V[i] = v;
-    const float mh = m / (1.0f - powf(b1, t)), vh = v / (1.0f - powf(b2, t));
-    P[i] -= lr * mh / (sqrtf(vh) + eps);
+    const float c1 = 1.0f - powf(b1, t), c2 = 1.0f - powf(b2, t);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int i = 4 * c4 + j;
+        const float m = b1 * M[i] + (1.0f - b1) * g[j];
+        const float v = b2 * V[i] + (1.0f - b2) * g[j] * g[j];
+        M[i] = m;
+        V[i] = v;
+        const float mh = m / c1, vh = v / c2;
+        P[i] -= lr * mh / (sqrtf(vh) + eps);
+    }
 }
 
 int launch_pack(liar_gpu_guide* G, cudaStream_t st, int bump) {
-    k_pack_umma<<<(kParams + 255) / 256, 256, 0, st>>>(G->params, G->umma_w, G->step, bump);
-    k_pack_umma_bwd<<<(kParams - param_offset(1) + 255) / 256, 256, 0, st>>>(G->params, G->umma_wb);
+    k_pack_umma<<<(kParams + 255) / 256, 256, 0, st>>>(G->params, G->umma_w, G->umma_wb, G->step, bump);
     return cudaGetLastError() == cudaSuccess ? LIAR_OK : LIAR_ERR_CUDA;
 }
 
@@ -828,16 +844,27 @@ int g_alloc(liar_gpu_ctx* ctx, liar_gpu_guide* G, size_t bytes, void** p, const 
 }
 
 int ensure_train_buffers(liar_gpu_ctx* ctx, liar_gpu_guide* G, size_t n) {
+    void* p = nullptr;
+    if (G->part_cap < ctx->num_sms) {
+        if (G->grad_part) {
+            cudaFree(G->grad_part);
+            G->buffers.erase(std::remove(G->buffers.begin(), G->buffers.end(), (void*)G->grad_part), G->buffers.end());
+        }
+        G->grad_part = nullptr;
+        G->part_cap = 0;
+        int rc = g_alloc(ctx, G, (size_t)ctx->num_sms * kParams * sizeof(float), &p, "guide gradient partial sums");
+        if (rc) return rc;
+        G->grad_part = static_cast<float*>(p);
+        G->part_cap = ctx->num_sms;
+    }
     if (G->cap >= n) return LIAR_OK;
-    for (void* p : {(void*)G->act, (void*)G->delta, (void*)G->gout, (void*)G->raw_out}) {
-        if (!p) continue;
-        cudaFree(p);
-        G->buffers.erase(std::remove(G->buffers.begin(), G->buffers.end(), p), G->buffers.end());
+    for (void* q : {(void*)G->act, (void*)G->delta, (void*)G->gout}) {
+        if (!q) continue;
+        cudaFree(q);
+        G->buffers.erase(std::remove(G->buffers.begin(), G->buffers.end(), q), G->buffers.end());
     }
     G->act = G->delta = G->gout = nullptr;
-    G->raw_out = nullptr;
     G->cap = 0;
-    void* p = nullptr;
     int rc = g_alloc(ctx, G, n * 5 * kWidth * 2, &p, "guide activations");
     if (rc) return rc;
     G->act = static_cast<__nv_bfloat16*>(p);
@@ -847,9 +874,6 @@ int ensure_train_buffers(liar_gpu_ctx* ctx, liar_gpu_guide* G, size_t n) {
     rc = g_alloc(ctx, G, n * kOut * 2, &p, "guide output gradients");
     if (rc) return rc;
     G->gout = static_cast<__nv_bfloat16*>(p);
-    rc = g_alloc(ctx, G, n * kOutUsed * 4, &p, "guide raw outputs");
-    if (rc) return rc;
-    G->raw_out = static_cast<float*>(p);
     G->cap = n;
     return LIAR_OK;
 }
@@ -913,13 +937,11 @@ int guide_train(liar_gpu_ctx* ctx, liar_gpu_guide* G, const float* d_records, co
     const int mma = wait_test ? 0 : 1;
     uint32_t* status = ctx->d_scratch + kStatusWord;
     const size_t tiles = (n_max + kTcRows - 1) / kTcRows;
-    // forward: the inference kernel's four slots storing h_1..h_5 and the raw outputs, then the
-    // loss and output gradient per record
+    // forward: the inference kernel's four slots storing h_1..h_5, the loss and the output
+    // gradient per record
     const unsigned tgrid = (unsigned)std::max<size_t>(1, std::min<size_t>((tiles + kEvSlots - 1) / kEvSlots, (size_t)sms));
-    k_eval_tc<true><<<tgrid, kEvThreads, kEvSmem, st>>>(G->umma_w, d_records, n_max, box, G->raw_out, kOutUsed, status,
-                                                         tries, mma, d_count, G->act, n_max);
-    k_train_head<<<(unsigned)std::max<size_t>(1, std::min<size_t>((n_max + 255) / 256, (size_t)sms * 8)), 256, 0, st>>>(
-        G->raw_out, d_records, d_count, n_max, G->scalars, G->gout, G->scalars + 1);
+    k_eval_tc<true><<<tgrid, kEvThreads, kEvSmem, st>>>(G->umma_w, d_records, n_max, box, nullptr, 0, status, tries,
+                                                         mma, d_count, G->act, n_max, G->scalars, G->gout);
     const unsigned bgrid =
         (unsigned)std::max<size_t>(1, std::min<size_t>((tiles + kBwdSlots - 1) / kBwdSlots, (size_t)sms));
     k_train_bwd_tc<<<bgrid, kBwdThreads, kBwdTcSmem, st>>>(G->umma_wb, d_count, n_max, G->act, G->gout, G->delta, status,
@@ -929,10 +951,10 @@ int guide_train(liar_gpu_ctx* ctx, liar_gpu_guide* G, const float* d_records, co
     const size_t per_cta = ((stages + sms - 1) / sms) * kDwRecords;
     const unsigned dgrid = (unsigned)std::max<size_t>(1, (n_max + per_cta - 1) / per_cta);
     k_train_dw_tc<<<dgrid, kDwThreads, kDwTcSmem, st>>>(d_records, d_count, n_max, box, G->act, G->delta, G->gout,
-                                                       G->grads, per_cta, status, tries, mma);
+                                                       G->grad_part, per_cta, status, tries, mma);
     const float lr = apply ? (G->cfg.learning_rate > 0 ? G->cfg.learning_rate : 5e-3f) : 0.0f;
-    k_adam<<<(kParams + 255) / 256, 256, 0, st>>>(G->params, G->grads, G->adam_m, G->adam_v, G->step, lr, 0.9f, 0.99f,
-                                                  1e-8f, d_grad_out);
+    k_adam_reduce<<<(kParams / 4 + kReduceCols - 1) / kReduceCols, kReduceCols * kReduceGroups, 0, st>>>(
+        G->grad_part, (int)dgrid, G->params, G->adam_m, G->adam_v, G->step, lr, 0.9f, 0.99f, 1e-8f, d_grad_out);
     if (apply) {
         rc = launch_pack(G, st, 1);
         if (rc) return ctx_cuda(ctx, cudaGetLastError(), "guide pack");
@@ -971,15 +993,14 @@ extern "C" int liar_gpu_guide_create(liar_gpu_ctx* ctx, const liar_guide_config*
     G->device = ctx->device;
     G->cfg = *cfg;
     void* p = nullptr;
-    rc = g_alloc(ctx, G, 4 * (size_t)kParams * sizeof(float) + 256, &p, "guide parameters");
+    rc = g_alloc(ctx, G, 3 * (size_t)kParams * sizeof(float) + 256, &p, "guide parameters");
     if (!rc) {
         float* f = static_cast<float*>(p);
         G->params = f;
-        G->grads = f + kParams;
-        G->adam_m = f + 2 * kParams;
-        G->adam_v = f + 3 * kParams;
-        G->step = reinterpret_cast<uint32_t*>(f + 4 * kParams);
-        G->scalars = f + 4 * kParams + 4;
+        G->adam_m = f + kParams;
+        G->adam_v = f + 2 * kParams;
+        G->step = reinterpret_cast<uint32_t*>(f + 3 * kParams);
+        G->scalars = f + 3 * kParams + 4;
     }
     if (!rc) rc = g_alloc(ctx, G, kUmmaWBytes, &p, "guide operand images");
     if (!rc) G->umma_w = static_cast<unsigned char*>(p);
@@ -989,7 +1010,7 @@ extern "C" int liar_gpu_guide_create(liar_gpu_ctx* ctx, const liar_guide_config*
         std::vector<float> P;
         init_params(P, cfg->seed);
         cudaError_t e = cudaMemcpy(G->params, P.data(), kParams * sizeof(float), cudaMemcpyHostToDevice);
-        if (e == cudaSuccess) e = cudaMemset(G->grads, 0, 3 * (size_t)kParams * sizeof(float) + 256);
+        if (e == cudaSuccess) e = cudaMemset(G->adam_m, 0, 2 * (size_t)kParams * sizeof(float) + 256);
         if (e != cudaSuccess) rc = ctx_cuda(ctx, e, "guide initialisation");
     }
     if (!rc && launch_pack(G, ctx->stream, 0)) rc = ctx_cuda(ctx, cudaGetLastError(), "guide pack");
@@ -1031,7 +1052,7 @@ extern "C" int liar_gpu_guide_set_params(liar_gpu_ctx* ctx, liar_gpu_guide* G, c
     if (rc) return rc;
     cudaError_t e = cudaStreamSynchronize(ctx->stream);
     if (e == cudaSuccess) e = cudaMemcpy(G->params, host, n * sizeof(float), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemset(G->grads, 0, 3 * (size_t)kParams * sizeof(float) + 256);  // grads, Adam, step
+    if (e == cudaSuccess) e = cudaMemset(G->adam_m, 0, 2 * (size_t)kParams * sizeof(float) + 256);  // Adam, step
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "guide parameters");
     if (launch_pack(G, ctx->stream, 0)) return ctx_cuda(ctx, cudaGetLastError(), "guide pack");
     G->steps_done = 0;
@@ -1073,7 +1094,7 @@ int liar_gpu::guide::guide_eval(liar_gpu_ctx* ctx, const liar_gpu_guide* G, cons
     const bool wait_test = ctx->fault_test == LIAR_FAULT_TEST_GUIDE_WAIT;
     k_eval_tc<false><<<grid, kEvThreads, kEvSmem, st>>>(G->umma_w, d_inputs, n, make_box(G->cfg), d_mixture, stride,
                                                           ctx->d_scratch + kStatusWord, wait_test ? 1u << 16 : 1u << 24,
-                                                          wait_test ? 0 : 1, nullptr, nullptr, 0);
+                                                          wait_test ? 0 : 1, nullptr, nullptr, 0, nullptr, nullptr);
     return ctx_cuda(ctx, cudaGetLastError(), "guide evaluation");
 }
 
