@@ -764,8 +764,19 @@ def run_case(name: str) -> None:
         from liar_b200 import guiding as GD
         g = GD.Guide(ctx, (np.array([-1, -1, -1], np.float32), np.array([1, 1, 1], np.float32)))
         x = torch.rand((1 << 20, 9), device="cuda", generator=torch.Generator("cuda").manual_seed(0)) * 2 - 1
+        st = torch.cuda.Stream()  # a stream of its own: the events must see the network's kernels
         for _ in range(3):
-            g.eval(x)
+            g.eval(x, stream=st.cuda_stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        for _ in range(5):
+            g.eval(x, stream=st.cuda_stream)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 5
+        flop = 2 * (225 * 64 + 4 * 64 * 64 + 64 * 40) * (1 << 20)
+        print(json.dumps({"case": name, "eval_device_ms_1M": ms, "tflops": flop / (ms * 1e-3) / 1e12}))
     elif name == "guide-train":
         # three Adam steps over 65,536 random records, device-timed
         from liar_b200 import guiding as GD

@@ -102,6 +102,8 @@ constexpr uint32_t kUmmaWbBytes = 4u * 8192u + 6144u;  // W1..W4 64 x 64, W5 64 
 // W_l transposed); bump: count the Adam step just taken
 __global__ void k_pack_umma(const float* __restrict__ P, unsigned char* __restrict__ img,
                             unsigned char* __restrict__ img_b, uint32_t* step, int bump) {
+    grid_dependency_wait();  // the Adam update, when it precedes
+    launch_dependents();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;  // one parameter (k, n) per thread
     if (i == 0 && bump) *step += 1;
     if (i >= kParams) return;
@@ -148,6 +150,39 @@ __device__ float record_gradient(const float* o, float wx, float wy, float wz, f
     return -weight * lq;
 }
 
+// The inference head: mixture_from_raw with the hardware's approximate reciprocal square root,
+// exponential and division (relative errors of a few 1e-7, far below the bf16 rounding of the
+// network), and each lobe's weight times its vMF normalisation for the renderer's copy.
+__device__ __forceinline__ void mixture_head_fast(const float* o, Lobe* lobes, float* w) {
+    float mx = -3.0e38f;
+#pragma unroll
+    for (int l = 0; l < kLobes; ++l) mx = fmaxf(mx, o[5 * l + 4]);
+    float sum = 0.0f;
+#pragma unroll
+    for (int l = 0; l < kLobes; ++l) {
+        const float x = o[5 * l], y = o[5 * l + 1], z = o[5 * l + 2];
+        const float n2 = x * x + y * y + z * z;
+        if (n2 > 0.0f) {
+            const float inv = rsqrtf(n2);
+            lobes[l].mx = x * inv;
+            lobes[l].my = y * inv;
+            lobes[l].mz = z * inv;
+        } else {
+            lobes[l].mx = lobes[l].my = 0.0f;
+            lobes[l].mz = 1.0f;
+        }
+        lobes[l].kappa = __expf(fminf(fmaxf(o[5 * l + 3], kLogKappaMin), kLogKappaMax));
+        w[l] = __expf(o[5 * l + 4] - mx);
+        sum += w[l];
+    }
+    const float inv_sum = __fdividef(1.0f, sum);
+#pragma unroll
+    for (int l = 0; l < kLobes; ++l) w[l] *= inv_sum;
+}
+__device__ __forceinline__ float vmf_norm_fast(float kappa) {
+    return __fdividef(kappa, 6.283185307179586f * -expm1f(-2.0f * kappa));
+}
+
 // ---- inference on tcgen05: four slots of 128 rows per CTA (guide_umma.cuh)
 // Layer 0 runs as four K-chunks over the two halves of the slot's buffer, each chunk committed to
 // the half's own mbarrier; a half is rewritten only after the commit of the chunk that read it.
@@ -171,12 +206,6 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
                                                            float* __restrict__ train, __nv_bfloat16* __restrict__ gout) {
     constexpr int IN = TRAIN ? kRecordFloats : kIn;
     if (TRAIN && n_dev) n = min((size_t)*n_dev, n);
-    float inv_mean = 0.0f, inv_b = 0.0f;  // TRAIN: 1 / mean record weight, 1 / batch size
-    if (TRAIN) {
-        const float wsum = train[0];
-        inv_mean = (wsum > 0.0f && n > 0) ? (float)n / wsum : 0.0f;
-        inv_b = n > 0 ? 1.0f / (float)n : 0.0f;
-    }
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     unsigned char* sw = smem;
@@ -207,6 +236,16 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
+    // the training forward follows k_weight_sum (programmatic launch): the prologue above ran
+    // beside it, its weight sum is read after the wait
+    grid_dependency_wait();
+    launch_dependents();
+    float inv_mean = 0.0f, inv_b = 0.0f;  // TRAIN: 1 / mean record weight, 1 / batch size
+    if (TRAIN) {
+        const float wsum = train[0];
+        inv_mean = (wsum > 0.0f && n > 0) ? (float)n / wsum : 0.0f;
+        inv_b = n > 0 ? 1.0f / (float)n : 0.0f;
+    }
     const uint32_t tmem = *tmem_slot + 64u * slot;              // the slot's accumulator columns
     const uint32_t taddr = tmem + ((32u * (warp & 3u)) << 16);  // the warp's lane quarter
     const uint32_t mb[2] = {(uint32_t)__cvta_generic_to_shared(mbar_all + 2 * slot),
@@ -243,19 +282,35 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
         pending[h] = true;
     };
     const size_t n_tiles = (n + kTcRows - 1) / kTcRows;
+    const size_t tile_step = (size_t)gridDim.x * kEvSlots;
     bool ok = true;
-    for (size_t tile = (size_t)blockIdx.x * kEvSlots + slot; ok && tile < n_tiles; tile += (size_t)gridDim.x * kEvSlots) {
+    // the inputs of a tile, coalesced: thread r holds elements r + 128 j (j < IN) of the tile's
+    // rows * IN floats; the next tile's are loaded while the current one runs
+    float pre[IN];
+    auto prefetch = [&](size_t t) {
+        const size_t base = t * kTcRows * (size_t)IN, end = min(n * (size_t)IN, base + (size_t)kTcRows * IN);
+#pragma unroll
+        for (int j = 0; j < IN; ++j) {
+            const size_t i = base + r + 128u * (uint32_t)j;
+            pre[j] = (t < n_tiles && i < end) ? __ldg(in + i) : 0.0f;
+        }
+    };
+    prefetch((size_t)blockIdx.x * kEvSlots + slot);
+    for (size_t tile = (size_t)blockIdx.x * kEvSlots + slot; ok && tile < n_tiles; tile += tile_step) {
         const size_t row0 = tile * kTcRows;
         const uint32_t rows = n - row0 < (size_t)kTcRows ? (uint32_t)(n - row0) : (uint32_t)kTcRows;
-        // the tile's inputs, coalesced, through shared memory (the previous tile's readers have passed
-        // the slot barriers since)
-        for (uint32_t i = r; i < rows * IN; i += 128u) stage_in[i] = __ldg(in + row0 * IN + i);
+        // the tile's inputs through shared memory (the previous tile's readers have passed the slot
+        // barriers since), then the next tile's loads go out
+#pragma unroll
+        for (int j = 0; j < IN; ++j) stage_in[r + 128u * (uint32_t)j] = pre[j];
+        prefetch(tile + tile_step);
         slot_sync();
         float x[kIn];
         if (r < rows) normalise_input(stage_in + r * IN, box.lo, box.inv_ext, x);
         else
             for (int c = 0; c < kIn; ++c) x[c] = 0.0f;
         // layer 0: chunk c's encodings into half c % 2 once the chunk before last has been consumed
+        uint32_t carry[8];
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             const int h = c & 1;
@@ -263,7 +318,7 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
                 ok = false;
                 break;
             }
-            encode_chunk_umma(x, buf + h * kEvHalf, r, c);
+            encode_chunk_carry(x, buf + h * kEvHalf, r, c, carry);
             issue(buf_addr + h * kEvHalf, 1024u, sw_addr + umma_w_offset(0) + 1024u * c, (kEnc / 8) * 128u, 4u, kWidth,
                   c > 0, h);
         }
@@ -281,9 +336,8 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
 #pragma unroll
                     for (int c = 0; c < 4; ++c) {
                         const float* q = v + 8 * c;
-                        const uint4 hq = make_uint4(
-                            pack_bf16(fmaxf(q[0], 0.0f), fmaxf(q[1], 0.0f)), pack_bf16(fmaxf(q[2], 0.0f), fmaxf(q[3], 0.0f)),
-                            pack_bf16(fmaxf(q[4], 0.0f), fmaxf(q[5], 0.0f)), pack_bf16(fmaxf(q[6], 0.0f), fmaxf(q[7], 0.0f)));
+                        const uint4 hq = make_uint4(pack_bf16_relu(q[0], q[1]), pack_bf16_relu(q[2], q[3]),
+                                                    pack_bf16_relu(q[4], q[5]), pack_bf16_relu(q[6], q[7]));
                         *reinterpret_cast<uint4*>(dst + (4 * half + c) * 128u) = hq;
                         if (TRAIN && r < rows)
                             reinterpret_cast<uint4*>(act + (size_t)(l - 1) * n_max * kWidth + (row0 + r) * kWidth)[4 * half + c] = hq;
@@ -328,7 +382,7 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
                 float* srow = reinterpret_cast<float*>(buf) + r * pitch;
                 Lobe lobes[kLobes];
                 float w[kLobes];
-                mixture_from_raw(o, lobes, w);
+                mixture_head_fast(o, lobes, w);
 #pragma unroll
                 for (int k = 0; k < kLobes; ++k)
                     *reinterpret_cast<float4*>(srow + 4 * k) = make_float4(lobes[k].mx, lobes[k].my, lobes[k].mz, lobes[k].kappa);
@@ -337,7 +391,7 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
                 if (stride == kMixRender) {
                     float a[kLobes];
 #pragma unroll
-                    for (int k = 0; k < kLobes; ++k) a[k] = w[k] * vmf_norm(lobes[k].kappa);
+                    for (int k = 0; k < kLobes; ++k) a[k] = w[k] * vmf_norm_fast(lobes[k].kappa);
                     *reinterpret_cast<float4*>(srow + 40) = make_float4(a[0], a[1], a[2], a[3]);
                     *reinterpret_cast<float4*>(srow + 44) = make_float4(a[4], a[5], a[6], a[7]);
                 }
@@ -371,6 +425,7 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
 
 __global__ void k_weight_sum(const float* __restrict__ rec, const uint32_t* __restrict__ n_dev, size_t n_max,
                              float* scalars) {
+    launch_dependents();  // the training forward's prologue reads nothing written here
     const size_t n = n_dev ? min((size_t)*n_dev, n_max) : n_max;
     float s = 0.0f;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -501,6 +556,8 @@ __global__ void __launch_bounds__(kBwdThreads, 1) k_train_bwd_tc(const unsigned 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     const TcTile T = tc_setup<kBwdSlots>(smem, kUmmaWbBytes, kBwdBuf, wb_img);
+    grid_dependency_wait();  // the forward's activations and output gradients
+    launch_dependents();
     const size_t n = n_dev ? min((size_t)*n_dev, n_max) : n_max;
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
     const uint32_t slot = tid >> 7, r = tid & 127u;
@@ -632,6 +689,8 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw_tc(const float* __re
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
+    grid_dependency_wait();  // the backward's deltas
+    launch_dependents();
     const uint32_t tmem = *tmem_slot;
     const uint32_t base = (uint32_t)__cvta_generic_to_shared(smem);
     uint32_t phase[3] = {0u, 0u, 0u};
@@ -646,32 +705,37 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw_tc(const float* __re
                           umma_desc_mn(base + b_off + 2u * kDwLbo * j), idesc, (acc0 || j > 0) ? 1u : 0u);
         }
     };
-    // the stage's rows in registers: thread i takes record i / 8, 8-feature group i % 8 (two per
-    // thread) of h_1..h_5, of delta_1..delta_5 and of the output gradient (6 groups), and the raw
-    // inputs of record tid % 64
+    // the stage's rows in registers: warp w takes records 8w .. 8w + 7 (lane % 8) and, in its two
+    // loads, 8-feature groups lane / 8 and 4 + lane / 8 of h_1..h_5, of delta_1..delta_5 and of the
+    // output gradient (6 groups). A warp's 16-byte pieces then cover 8 records x 4 groups, whose
+    // places in the MN-major operands fall on distinct bank quarters (4 wavefronts per store, no
+    // conflicts), while its global loads still use every byte of the sectors they touch. The raw
+    // inputs: thread tid encodes record tid % 64, inputs d = tid / 64 + 4 m (the fourth part also
+    // writes all nine raw inputs), and loads only those.
+    const uint32_t my_rec = 8u * warp + (tid & 7u), my_grp = (tid >> 3) & 3u, enc_part = tid >> 6;
     uint4 ph[5][2], pd[6][2];
     float px[kIn];
     auto load_stage = [&](size_t s0) {
+        const size_t row = s0 + my_rec;
+        const bool live = row < c1;
 #pragma unroll
         for (int l = 0; l < 6; ++l) {
             const int dld = l < 5 ? kWidth : kOut, dc = dld / 8;
             const __nv_bfloat16* dsrc = l < 5 ? delta + (size_t)l * n_max * kWidth : gout;
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
-                const int i = tid + j * kDwThreads;
-                if (l < 5) {
-                    const size_t row = s0 + (size_t)(i >> 3);
-                    ph[l][j] = row < c1 ? reinterpret_cast<const uint4*>(act + (size_t)l * n_max * kWidth + row * kWidth)[i & 7]
-                                        : make_uint4(0u, 0u, 0u, 0u);
-                }
-                const size_t drow = s0 + (size_t)(i / dc);
-                pd[l][j] = (i < kDwRecords * dc && drow < c1) ? reinterpret_cast<const uint4*>(dsrc + drow * dld)[i % dc]
-                                                              : make_uint4(0u, 0u, 0u, 0u);
+                const uint32_t g = my_grp + 4u * (uint32_t)j;
+                if (l < 5)
+                    ph[l][j] = live ? reinterpret_cast<const uint4*>(act + (size_t)l * n_max * kWidth + row * kWidth)[g]
+                                    : make_uint4(0u, 0u, 0u, 0u);
+                pd[l][j] = (live && g < (uint32_t)dc) ? reinterpret_cast<const uint4*>(dsrc + row * dld)[g]
+                                                      : make_uint4(0u, 0u, 0u, 0u);
             }
         }
-        const size_t row = s0 + (tid & (kDwRecords - 1));
+        const size_t xrow = s0 + (tid & (kDwRecords - 1));
 #pragma unroll
-        for (int c = 0; c < kIn; ++c) px[c] = row < c1 ? rec[row * kRecordFloats + c] : 0.0f;
+        for (int c = 0; c < kIn; ++c)
+            px[c] = (xrow < c1 && (enc_part == 3u || (uint32_t)(c & 3) == enc_part)) ? rec[xrow * kRecordFloats + c] : 0.0f;
     };
     if (c0 < c1) load_stage(c0);
     for (size_t s0 = c0; ok && s0 < c1; s0 += kDwRecords) {
@@ -693,7 +757,7 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw_tc(const float* __re
             // the encodings: four threads per record, each encoding the inputs d = part, part +
             // 4, ... (part 3 also writes the raw inputs and the zero padding); encoding column
             // group g (8 features) of record i goes to A block g / 16, group g % 16
-            const int i = tid & (kDwRecords - 1), part = tid >> 6;
+            const int i = tid & (kDwRecords - 1);
             const bool live = s0 + i < c1;
             float x[kIn];
             if (live) normalise_input(px, box.lo, box.inv_ext, x);
@@ -702,7 +766,7 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw_tc(const float* __re
             auto put = [&](int g, uint4 v) {
                 *reinterpret_cast<uint4*>(smem + kDwOffA0 + (uint32_t)(g >> 4) * kDwA + dw_offset((uint32_t)(g & 15), (uint32_t)i)) = v;
             };
-            for (int d = part; d < kIn; d += 4) {
+            for (int d = (int)enc_part; d < kIn; d += 4) {
                 uint32_t w[kFreq];
                 if (live) encode_input(x[d], w);
                 else
@@ -710,7 +774,7 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw_tc(const float* __re
 #pragma unroll
                 for (int q = 0; q < 3; ++q) put(3 * d + q, make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]));
             }
-            if (part == 3) {
+            if (enc_part == 3u) {
                 put(27, make_uint4(pack_bf16(x[0], x[1]), pack_bf16(x[2], x[3]), pack_bf16(x[4], x[5]), pack_bf16(x[6], x[7])));
                 put(28, make_uint4(pack_bf16(x[8], 0.0f), 0u, 0u, 0u));
                 for (int g = 29; g < kEnc / 8; ++g) put(g, make_uint4(0u, 0u, 0u, 0u));
@@ -723,11 +787,9 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw_tc(const float* __re
             const uint32_t b_off = l == 0 ? kDwOffB0 : dw_off_b(l);
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
-                const int i = tid + j * kDwThreads;
-                if (l >= 1)
-                    *reinterpret_cast<uint4*>(smem + dw_off_a(l) + dw_offset((uint32_t)(i & 7), (uint32_t)(i >> 3))) = ph[l - 1][j];
-                if (i < kDwRecords * dc)
-                    *reinterpret_cast<uint4*>(smem + b_off + dw_offset((uint32_t)(i % dc), (uint32_t)(i / dc))) = pd[l][j];
+                const uint32_t g = my_grp + 4u * (uint32_t)j;
+                if (l >= 1) *reinterpret_cast<uint4*>(smem + dw_off_a(l) + dw_offset(g, my_rec)) = ph[l - 1][j];
+                if (g < (uint32_t)dc) *reinterpret_cast<uint4*>(smem + b_off + dw_offset(g, my_rec)) = pd[l][j];
             }
         }
         fence_async_smem();
@@ -787,6 +849,8 @@ __global__ void __launch_bounds__(kReduceCols * kReduceGroups) k_adam_reduce(
     const float* __restrict__ part, int nparts, float* __restrict__ P, float* __restrict__ M, float* __restrict__ V,
     const uint32_t* __restrict__ step, float lr, float b1, float b2, float eps, float* __restrict__ grad_out) {
     __shared__ float4 sums[kReduceGroups][kReduceCols];
+    grid_dependency_wait();  // the weight-gradient partial sums
+    launch_dependents();
     const int lane = threadIdx.x % kReduceCols, grp = threadIdx.x / kReduceCols;
     const int c4 = blockIdx.x * kReduceCols + lane;
     const bool live = c4 < kParams / 4;
@@ -827,8 +891,30 @@ __global__ void __launch_bounds__(kReduceCols * kReduceGroups) k_adam_reduce(
     }
 }
 
-int launch_pack(liar_gpu_guide* G, cudaStream_t st, int bump) {
-    k_pack_umma<<<(kParams + 255) / 256, 256, 0, st>>>(G->params, G->umma_w, G->umma_wb, G->step, bump);
+// launches kernel with programmatic stream serialization (grid_dependency_wait): its CTAs may
+// start, and run the part before their wait, while the previous kernel of the stream finishes
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t st,
+                       Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
+// pdl: the pack follows the Adam kernel of a training step (programmatic launch)
+int launch_pack(liar_gpu_guide* G, cudaStream_t st, int bump, bool pdl = false) {
+    const unsigned grid = (kParams + 255) / 256;
+    if (pdl) return launch_pdl(k_pack_umma, grid, 256, 0, st, G->params, G->umma_w, G->umma_wb, G->step, bump) == cudaSuccess
+                        ? LIAR_OK : LIAR_ERR_CUDA;
+    k_pack_umma<<<grid, 256, 0, st>>>(G->params, G->umma_w, G->umma_wb, G->step, bump);
     return cudaGetLastError() == cudaSuccess ? LIAR_OK : LIAR_ERR_CUDA;
 }
 
@@ -940,23 +1026,30 @@ int guide_train(liar_gpu_ctx* ctx, liar_gpu_guide* G, const float* d_records, co
     // forward: the inference kernel's four slots storing h_1..h_5, the loss and the output
     // gradient per record
     const unsigned tgrid = (unsigned)std::max<size_t>(1, std::min<size_t>((tiles + kEvSlots - 1) / kEvSlots, (size_t)sms));
-    k_eval_tc<true><<<tgrid, kEvThreads, kEvSmem, st>>>(G->umma_w, d_records, n_max, box, nullptr, 0, status, tries,
-                                                         mma, d_count, G->act, n_max, G->scalars, G->gout);
+    // the kernels after k_weight_sum start programmatically: each one's prologue (weights to shared
+    // memory, barriers, tensor memory) overlaps the end of the kernel before it
+    e = launch_pdl(k_eval_tc<true>, tgrid, kEvThreads, kEvSmem, st, G->umma_w, d_records, n_max, box, (float*)nullptr, 0,
+                   status, tries, mma, d_count, G->act, n_max, G->scalars, G->gout);
+    if (e != cudaSuccess) return ctx_cuda(ctx, e, "guide training forward");
     const unsigned bgrid =
         (unsigned)std::max<size_t>(1, std::min<size_t>((tiles + kBwdSlots - 1) / kBwdSlots, (size_t)sms));
-    k_train_bwd_tc<<<bgrid, kBwdThreads, kBwdTcSmem, st>>>(G->umma_wb, d_count, n_max, G->act, G->gout, G->delta, status,
-                                                         tries, mma);
+    e = launch_pdl(k_train_bwd_tc, bgrid, kBwdThreads, kBwdTcSmem, st, G->umma_wb, d_count, n_max, G->act, G->gout,
+                   G->delta, status, tries, mma);
+    if (e != cudaSuccess) return ctx_cuda(ctx, e, "guide training backward");
     // weight gradients: one CTA per SM, each over a contiguous run of whole 64-record stages
     const size_t stages = (n_max + kDwRecords - 1) / kDwRecords;
     const size_t per_cta = ((stages + sms - 1) / sms) * kDwRecords;
     const unsigned dgrid = (unsigned)std::max<size_t>(1, (n_max + per_cta - 1) / per_cta);
-    k_train_dw_tc<<<dgrid, kDwThreads, kDwTcSmem, st>>>(d_records, d_count, n_max, box, G->act, G->delta, G->gout,
-                                                       G->grad_part, per_cta, status, tries, mma);
+    e = launch_pdl(k_train_dw_tc, dgrid, kDwThreads, kDwTcSmem, st, d_records, d_count, n_max, box, G->act, G->delta,
+                   G->gout, G->grad_part, per_cta, status, tries, mma);
+    if (e != cudaSuccess) return ctx_cuda(ctx, e, "guide weight gradients");
     const float lr = apply ? (G->cfg.learning_rate > 0 ? G->cfg.learning_rate : 5e-3f) : 0.0f;
-    k_adam_reduce<<<(kParams / 4 + kReduceCols - 1) / kReduceCols, kReduceCols * kReduceGroups, 0, st>>>(
-        G->grad_part, (int)dgrid, G->params, G->adam_m, G->adam_v, G->step, lr, 0.9f, 0.99f, 1e-8f, d_grad_out);
+    e = launch_pdl(k_adam_reduce, (kParams / 4 + kReduceCols - 1) / kReduceCols, kReduceCols * kReduceGroups, 0, st,
+                   G->grad_part, (int)dgrid, G->params, G->adam_m, G->adam_v, G->step, lr, 0.9f, 0.99f, 1e-8f,
+                   d_grad_out);
+    if (e != cudaSuccess) return ctx_cuda(ctx, e, "guide Adam step");
     if (apply) {
-        rc = launch_pack(G, st, 1);
+        rc = launch_pack(G, st, 1, true);
         if (rc) return ctx_cuda(ctx, cudaGetLastError(), "guide pack");
         G->steps_done += 1;
     }

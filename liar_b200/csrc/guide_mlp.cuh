@@ -40,6 +40,15 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
     return *reinterpret_cast<const uint32_t*>(&v);
 }
 
+// max(lo, 0) and max(hi, 0) as a bf16 pair in one conversion (cvt.rn.relu: rounded to nearest
+// even, negative results clamped to zero); equal to pack_bf16(fmaxf(lo, 0), fmaxf(hi, 0)) for
+// every input but NaN
+__device__ __forceinline__ uint32_t pack_bf16_relu(float lo, float hi) {
+    uint32_t d;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+    return d;
+}
+
 __device__ __forceinline__ float bf16_lo(uint32_t v) { return __uint_as_float(v << 16); }
 __device__ __forceinline__ float bf16_hi(uint32_t v) { return __uint_as_float(v & 0xffff0000u); }
 

@@ -162,6 +162,15 @@ __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.a
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
+// Programmatic dependent launch: a kernel launched with programmatic stream serialization may start
+// before the previous kernel of its stream has finished. grid_dependency_wait() blocks until that
+// kernel has completed and its memory is visible (a no-op for a normally launched kernel); every
+// read of its results, and every write it could still read, comes after. launch_dependents() lets
+// the next such kernel start its own prologue; the kernels here call it only after their own wait,
+// so a prologue never overlaps more than one kernel back.
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // the encodings of row r into the 128 x 256 A operand: per input 12 sin/cos pairs = 3 chunks of
 // 16 bytes (angle doubling as encode_row), then the raw inputs and zero padding
 __device__ __forceinline__ void encode_row_umma(const float* x, unsigned char* a0, uint32_t r) {
@@ -198,6 +207,48 @@ __device__ __forceinline__ void encode_row_umma(const float* x, unsigned char* a
 // operand buffer (the same values as encode_row_umma): the inputs whose 24 columns (3 core
 // columns 3 d .. 3 d + 2) meet the chunk are encoded (an input that straddles two chunks is
 // encoded in both), chunk 3 also holds the raw inputs and the zero padding.
+// The same encodings for the K-chunks of 8 core columns as encode_chunk_umma, every input encoded
+// once: input d fills core columns 3d .. 3d + 2, so inputs 2 (columns 6, 7 | 8) and 5 (15 | 16,
+// 17) straddle a chunk boundary; their columns of the next chunk wait in carry (two columns of four
+// words) and are written by the next call. Calls run for c = 0, 1, 2, 3 in order.
+__device__ __forceinline__ void encode_chunk_carry(const float* x, unsigned char* a, uint32_t r, int c,
+                                                   uint32_t (&carry)[8]) {
+    unsigned char* row = a + (r >> 3) * 8u * 128u + (r & 7u) * 16u;
+    const int lo = 8 * c, hi = 8 * c + 7;  // the chunk's core columns
+    // the columns carried over from the previous chunk: 8 (c = 1), 16 and 17 (c = 2)
+    if (c == 1) *reinterpret_cast<uint4*>(row) = make_uint4(carry[0], carry[1], carry[2], carry[3]);
+    if (c == 2) {
+        *reinterpret_cast<uint4*>(row) = make_uint4(carry[0], carry[1], carry[2], carry[3]);
+        *reinterpret_cast<uint4*>(row + 128) = make_uint4(carry[4], carry[5], carry[6], carry[7]);
+    }
+#pragma unroll
+    for (int d = 0; d < kIn; ++d) {
+        if (3 * d < lo || 3 * d > hi) continue;  // an input belongs to the chunk of its first column
+        uint32_t w[12];
+        encode_input(x[d], w);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const int col = 3 * d + q;
+            if (col <= hi) {
+                *reinterpret_cast<uint4*>(row + (col - lo) * 128) = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+            } else {
+                const int k = col - hi - 1;  // 0 or 1: its slot in the carry
+                carry[4 * k] = w[4 * q];
+                carry[4 * k + 1] = w[4 * q + 1];
+                carry[4 * k + 2] = w[4 * q + 2];
+                carry[4 * k + 3] = w[4 * q + 3];
+            }
+        }
+    }
+    if (c == 3) {
+        *reinterpret_cast<uint4*>(row + (27 - lo) * 128) =
+            make_uint4(pack_bf16(x[0], x[1]), pack_bf16(x[2], x[3]), pack_bf16(x[4], x[5]), pack_bf16(x[6], x[7]));
+        *reinterpret_cast<uint4*>(row + (28 - lo) * 128) = make_uint4(pack_bf16(x[8], 0.0f), 0u, 0u, 0u);
+#pragma unroll
+        for (int col = 29; col < kEnc / 8; ++col) *reinterpret_cast<uint4*>(row + (col - lo) * 128) = make_uint4(0u, 0u, 0u, 0u);
+    }
+}
+
 __device__ __forceinline__ void encode_chunk_umma(const float* x, unsigned char* a, uint32_t r, int c) {
     unsigned char* row = a + (r >> 3) * 8u * 128u + (r & 7u) * 16u;
     const int lo = 8 * c, hi = 8 * c + 7;  // the chunk's core columns
