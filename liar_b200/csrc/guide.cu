@@ -255,23 +255,27 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
     auto slot_sync = [&]() { asm volatile("bar.sync %0, 128;" ::"r"(1u + slot) : "memory"); };
     uint32_t phase[2] = {0u, 0u};
     bool pending[2] = {false, false};  // a commit to the half's mbarrier not yet waited for
-    // wait for half h's outstanding commit; false (for the whole slot) when any thread gave up
-    auto wait_half = [&](int h) -> bool {
-        if (!mbar_wait(mb[h], phase[h], max_tries)) failed[slot] = 1u;
-        slot_sync();
-        if (failed[slot]) return false;
-        phase[h] ^= 1u;
-        pending[h] = false;
-        return true;
+    // wait for half h's outstanding commit. Every thread polls the mbarrier itself, so no barrier
+    // follows: a thread that gives up marks the slot failed and keeps the commit pending (the drain
+    // waits for it again), and the whole slot sees the mark at the barrier of its next issue
+    auto wait_half = [&](int h) {
+        if (mbar_wait(mb[h], phase[h], max_tries)) {
+            phase[h] ^= 1u;
+            pending[h] = false;
+        } else {
+            failed[slot] = 1u;
+        }
     };
     // hand the slot's operand to the tensor core (the writes of every thread are visible to the
-    // async proxy and the accumulator reads are done) and, from thread 0, issue K / 16 MMAs
+    // async proxy and the accumulator reads are done) and, from thread 0, issue K / 16 MMAs; false
+    // (for the whole slot, nothing issued) once a wait of the slot has given up
     auto issue = [&](uint32_t a_addr, uint32_t a_sbo, uint32_t b_addr, uint32_t b_sbo, uint32_t ksteps, uint32_t N,
-                     bool acc0, int h) {
+                     bool acc0, int h) -> bool {
         fence_async_smem();
         tc_fence_before();
         slot_sync();
         tc_fence_after();
+        if (failed[slot]) return false;
         if (r == 0 && issue_mma) {
             const uint32_t idesc = umma_idesc(N);
             for (uint32_t j = 0; j < ksteps; ++j)
@@ -280,6 +284,7 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
             umma_commit(mb[h]);
         }
         pending[h] = true;
+        return true;
     };
     const size_t n_tiles = (n + kTcRows - 1) / kTcRows;
     const size_t tile_step = (size_t)gridDim.x * kEvSlots;
@@ -314,38 +319,43 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             const int h = c & 1;
-            if (c >= 2 && !wait_half(h)) {
+            if (c >= 2) wait_half(h);
+            encode_chunk_carry(x, buf + h * kEvHalf, r, c, carry);
+            if (!issue(buf_addr + h * kEvHalf, 1024u, sw_addr + umma_w_offset(0) + 1024u * c, (kEnc / 8) * 128u, 4u,
+                       kWidth, c > 0, h)) {
                 ok = false;
                 break;
             }
-            encode_chunk_carry(x, buf + h * kEvHalf, r, c, carry);
-            issue(buf_addr + h * kEvHalf, 1024u, sw_addr + umma_w_offset(0) + 1024u * c, (kEnc / 8) * 128u, 4u, kWidth,
-                  c > 0, h);
         }
-        if (ok) ok = wait_half(0) && wait_half(1);
-        // hidden layers and the output layer from half 0; v holds the accumulator 32 columns at a time
+        if (ok) {
+            wait_half(0);
+            wait_half(1);
+        }
+        // hidden layers and the output layer from half 0
         for (int l = 1; ok && l <= kLayers; ++l) {
             tc_fence_after();
             unsigned char* dst = buf + (r >> 3) * (kWidth / 8) * 128u + (r & 7u) * 16u;
             if (l < kLayers) {
                 // ReLU, bf16, the next layer's A operand (row r, 8 chunks of 8 columns)
+                {
+                    float v[64];
+                    tmem_ld_x64(taddr, v);
 #pragma unroll
-                for (int half = 0; half < 2; ++half) {
-                    float v[32];
-                    tmem_ld_32x32b<32>(taddr + 32u * half, v);
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) {
+                    for (int c = 0; c < 8; ++c) {
                         const float* q = v + 8 * c;
                         const uint4 hq = make_uint4(pack_bf16_relu(q[0], q[1]), pack_bf16_relu(q[2], q[3]),
                                                     pack_bf16_relu(q[4], q[5]), pack_bf16_relu(q[6], q[7]));
-                        *reinterpret_cast<uint4*>(dst + (4 * half + c) * 128u) = hq;
+                        *reinterpret_cast<uint4*>(dst + c * 128u) = hq;
                         if (TRAIN && r < rows)
-                            reinterpret_cast<uint4*>(act + (size_t)(l - 1) * n_max * kWidth + (row0 + r) * kWidth)[4 * half + c] = hq;
+                            reinterpret_cast<uint4*>(act + (size_t)(l - 1) * n_max * kWidth + (row0 + r) * kWidth)[c] = hq;
                     }
                 }
-                issue(buf_addr, (kWidth / 8) * 128u, sw_addr + umma_w_offset(l), (kWidth / 8) * 128u, kWidth / 16,
-                      (uint32_t)layer_n(l), false, 0);
-                ok = wait_half(0);
+                if (!issue(buf_addr, (kWidth / 8) * 128u, sw_addr + umma_w_offset(l), (kWidth / 8) * 128u, kWidth / 16,
+                           (uint32_t)layer_n(l), false, 0)) {
+                    ok = false;
+                    break;
+                }
+                wait_half(0);
             } else {
                 // the mixture of row r into the staging rows (pitch stride + 4 floats), then the
                 // slot's rows leave as one contiguous, coalesced block
@@ -374,6 +384,10 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
                     for (int s = 16; s > 0; s >>= 1) lsum += __shfl_down_sync(0xffffffffu, lsum, s);
                     if ((tid & 31u) == 0 && lsum != 0.0f) atomicAdd(train + 1, lsum * inv_b);
                     slot_sync();
+                    if (failed[slot]) {  // the last layer's wait gave up: nothing leaves
+                        ok = false;
+                        break;
+                    }
                     const uint4* srows = reinterpret_cast<const uint4*>(buf);
                     uint4* gdst = reinterpret_cast<uint4*>(gout + row0 * kOut);
                     for (uint32_t i = r; i < rows * (kOut * 2 / 16); i += 128u) gdst[i] = srows[i];
@@ -396,6 +410,10 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
                     *reinterpret_cast<float4*>(srow + 44) = make_float4(a[4], a[5], a[6], a[7]);
                 }
                 slot_sync();
+                if (failed[slot]) {  // the last layer's wait gave up: nothing leaves
+                    ok = false;
+                    break;
+                }
                 const uint32_t per_row = (uint32_t)stride / 4u, total = rows * per_row;
                 float4* gdst = reinterpret_cast<float4*>(mix + row0 * (size_t)stride);
                 for (uint32_t i = r; i < total; i += 128u) {
