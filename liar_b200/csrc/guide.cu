@@ -10,6 +10,8 @@
 // activations and the output gradient, fused) -> backward (stores the bf16 layer deltas) -> weight
 // gradients over the records, accumulated in tensor memory -> Adam on the f32 master weights ->
 // repack the bf16 operand images.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -43,6 +45,10 @@ struct liar_gpu_guide {
     float* grad_part = nullptr;      // [part_cap][kParams]: the weight-gradient CTAs' partial sums
     int part_cap = 0;
     float* scalars = nullptr;        // [0] weight sum [1] loss sum
+    // TMA descriptors of act, delta and gout for the weight-gradient kernel, for tm_rows records
+    CUtensorMap tm_act{}, tm_delta{}, tm_gout{};
+    const void* tm_base = nullptr;
+    size_t tm_rows = 0;
     std::vector<void*> buffers;
     unsigned long long steps_done = 0;
     unsigned long long records = 0, guided = 0, passes = 0;
@@ -346,8 +352,11 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
                         const uint4 hq = make_uint4(pack_bf16_relu(q[0], q[1]), pack_bf16_relu(q[2], q[3]),
                                                     pack_bf16_relu(q[4], q[5]), pack_bf16_relu(q[6], q[7]));
                         *reinterpret_cast<uint4*>(dst + c * 128u) = hq;
-                        if (TRAIN && r < rows)
-                            reinterpret_cast<uint4*>(act + (size_t)(l - 1) * n_max * kWidth + (row0 + r) * kWidth)[c] = hq;
+                        // rows past the record count (to the tile's end) are stored as zeros: the
+                        // weight-gradient kernel reads whole 32-record stages
+                        if (TRAIN && row0 + r < n_max)
+                            reinterpret_cast<uint4*>(act + (size_t)(l - 1) * n_max * kWidth + (row0 + r) * kWidth)[c] =
+                                r < rows ? hq : make_uint4(0u, 0u, 0u, 0u);
                     }
                 }
                 if (!issue(buf_addr, (kWidth / 8) * 128u, sw_addr + umma_w_offset(l), (kWidth / 8) * 128u, kWidth / 16,
@@ -366,7 +375,11 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
                     // the loss head: row r's gradient as 48 bf16 (96 B) into the staging rows, the
                     // loss summed per warp, then the slot's gradient rows leave as one coalesced block
                     float lsum = 0.0f;
-                    if (r < rows) {
+                    uint4* grow = reinterpret_cast<uint4*>(buf + r * (kOut * 2));
+                    if (r >= rows) {  // zero gradient rows to the tile's end (whole weight-gradient stages)
+#pragma unroll
+                        for (int c = 0; c < kOut / 8; ++c) grow[c] = make_uint4(0u, 0u, 0u, 0u);
+                    } else {
                         const float* rr = stage_in + r * IN;
                         float weight = rr[12];
                         if (!(weight > 0.0f) || !isfinite(weight)) weight = 0.0f;
@@ -374,7 +387,6 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
 #pragma unroll
                         for (int c = kOutUsed; c < kOut; ++c) d[c] = 0.0f;
                         lsum = record_gradient(o, rr[9], rr[10], rr[11], fminf(weight * inv_mean, kWeightClip), inv_b, d);
-                        uint4* grow = reinterpret_cast<uint4*>(buf + r * (kOut * 2));
 #pragma unroll
                         for (int c = 0; c < kOut / 8; ++c)
                             grow[c] = make_uint4(pack_bf16(d[8 * c], d[8 * c + 1]), pack_bf16(d[8 * c + 2], d[8 * c + 3]),
@@ -390,7 +402,8 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
                     }
                     const uint4* srows = reinterpret_cast<const uint4*>(buf);
                     uint4* gdst = reinterpret_cast<uint4*>(gout + row0 * kOut);
-                    for (uint32_t i = r; i < rows * (kOut * 2 / 16); i += 128u) gdst[i] = srows[i];
+                    const uint32_t rows_out = (uint32_t)min((size_t)kTcRows, n_max - row0);
+                    for (uint32_t i = r; i < rows_out * (kOut * 2 / 16); i += 128u) gdst[i] = srows[i];
                 } else {
                 const uint32_t pitch = (uint32_t)stride + 4u;
                 float* srow = reinterpret_cast<float*>(buf) + r * pitch;
@@ -627,7 +640,7 @@ __global__ void __launch_bounds__(kBwdThreads, 1) k_train_bwd_tc(const unsigned 
                         o[e] = pack_bf16(a, b);
                     }
                     const uint4 packed = make_uint4(o[0], o[1], o[2], o[3]);
-                    if (live) drow[4 * half + c] = packed;
+                    if (row < n_max) drow[4 * half + c] = packed;  // zero past the record count
                     if (l > 1) *reinterpret_cast<uint4*>(dst + (4 * half + c) * 128u) = packed;
                 }
             }
@@ -636,25 +649,39 @@ __global__ void __launch_bounds__(kBwdThreads, 1) k_train_bwd_tc(const unsigned 
     tc_teardown<kBwdSlots>(T, status);
 }
 
-// weight gradients: shared-memory plan of one CTA (bytes from the 1024-aligned base)
-constexpr int kDwRecords = 64;                            // records per stage (the UMMA K of a stage)
-constexpr uint32_t kDwA = 128u * kDwRecords * 2;          // an A operand: 128 features x 64 records
-constexpr uint32_t kDwB = 64u * kDwRecords * 2;           // a B operand: 64 outputs x 64 records
-// one stage's operands all at once: W0 (two 128-feature blocks of encodings, delta_1), then
-// W1..W5 (h_l, upper 64 features zero; delta_{l+1} or the output gradient)
-constexpr uint32_t kDwOffA0 = 0, kDwOffB0 = 2 * kDwA;
-__host__ __device__ constexpr uint32_t dw_off_a(int l) { return kDwOffB0 + kDwB + (uint32_t)(l - 1) * (kDwA + kDwB); }
-__host__ __device__ constexpr uint32_t dw_off_b(int l) { return dw_off_a(l) + kDwA; }
-constexpr uint32_t kDwOffBar = dw_off_a(6);                // 160 KB
-constexpr size_t kDwTcSmem = 1024 + kDwOffBar + 64;
-constexpr int kDwThreads = 256;
+// weight gradients: shared-memory plan of one CTA (bytes from the 1024-aligned base): three
+// buffers of one 32-record stage each, so that the loads and encodings of the next two stages
+// overlap a stage's MMAs
+constexpr int kDwRecords = 32;                                 // records per stage (the UMMA K of a stage)
+constexpr uint32_t kDwGroup = (uint32_t)kDwRecords * 16u;      // 8 features of the stage's records: 512 B
+constexpr uint32_t kDwA = 16u * kDwGroup;                      // an M = 128 A operand: 128 features x 32 records
+constexpr uint32_t kDwLayer = 8u * kDwGroup;                   // 64 features (or outputs) x 32 records: 4 KB
+// a buffer: A0 = the encodings (two 128-feature blocks); H = h_1..h_5 back to back; D = delta_1..
+// delta_5 back to back; G = the output gradient (6 groups). W_l's A operand (l >= 1) is the M = 128
+// window starting at h_l: its upper 64 rows read the next 4 KB (h_{l+1}, or delta_1 after h_5),
+// whose products land in accumulator rows 64..127, which are never read.
+constexpr uint32_t kDwOffA0 = 0, kDwOffH = 2 * kDwA, kDwOffD = kDwOffH + 5 * kDwLayer, kDwOffG = kDwOffD + 5 * kDwLayer;
+constexpr uint32_t kDwBuf = 60u * 1024u;                       // 59 KB used, rounded to 1 KB
+static_assert(kDwOffG + 6 * kDwGroup <= kDwBuf, "weight-gradient buffer overflow");
+__host__ __device__ constexpr uint32_t dw_off_a(int l) { return kDwOffH + (uint32_t)(l - 1) * kDwLayer; }
+// the B operand of W_l: delta_{l+1} (W0..W4), the output gradient (W5)
+__host__ __device__ constexpr uint32_t dw_off_b(int l) { return l < 5 ? kDwOffD + (uint32_t)l * kDwLayer : kDwOffG; }
+constexpr int kDwBufs = 3;
+constexpr uint32_t kDwOffBar = kDwBufs * kDwBuf;               // 180 KB
+constexpr size_t kDwTcSmem = 1024 + kDwOffBar + 128;
+constexpr int kDwEncWarps = 9;                                 // warp p encodes input p of the stage's 32 records
+constexpr int kDwThreads = 32 * (kDwEncWarps + 1);             // + the load/MMA warp
 constexpr uint32_t kDwTmemCols = 512;  // dW0 (two M blocks), dW1..dW4, dW5: 7 x 64 columns
+// bytes one stage's three TMA loads bring: h_1..h_5, delta_1..delta_5, the output gradient
+constexpr uint32_t kDwStageTx = (5u * 8u + 5u * 8u + 6u) * kDwGroup;
 // The weight-gradient operands are MN-major (the records, the UMMA K, are the rows of the stored
 // activations, the features or outputs contiguous in each): core matrix = 8 records x 8 features
 // (16 B per record, 128 B per core matrix); K-adjacent core matrices 128 B apart (leading byte
-// offset), MN-adjacent ones 1024 B apart (stride byte offset, 8 record groups of a stage). A row
-// of 8 features of record k therefore lands at (feature / 8) * 1024 + (k / 8) * 128 + (k % 8) * 16,
-// straight from its 16-byte global load: no transposition.
+// offset), MN-adjacent ones 512 B apart (stride byte offset, the 4 record groups of a stage). The 8
+// features of group g for all 32 records are therefore one contiguous 512-byte block at g * 512,
+// record k at k * 16. A TMA box of {8 features, 32 records, 8 groups, 5 layers} over the stored
+// [layer][record][64 features] rows (the group dimension's stride 16 B, the record's 128 B) lands in
+// exactly this order, all five layers back to back.
 constexpr uint32_t kDwLbo = 128u, kDwSbo = (uint32_t)(kDwRecords / 8) * 128u;
 __device__ __forceinline__ uint32_t dw_offset(uint32_t group, uint32_t k) {
     return group * kDwSbo + (k >> 3) * kDwLbo + (k & 7u) * 16u;
@@ -668,33 +695,55 @@ __device__ __forceinline__ uint64_t umma_desc_mn(uint32_t smem_addr) {
 // kind::f16 with both operands MN-major (bits 15 and 16)
 __host__ __device__ constexpr uint32_t umma_idesc_mn(uint32_t n) { return umma_idesc(n) | (1u << 15) | (1u << 16); }
 
-// Per stage of 64 records: every operand of the six weight gradients is written into shared memory
-// (the encodings computed, the other rows from registers loaded during the previous stage), one
-// barrier, 28 MMAs from one thread, one commit; the next stage's rows are then loaded into
-// registers while the MMAs run, so that a stage waits on global memory only once.
-__global__ void __launch_bounds__(kDwThreads, 1) k_train_dw_tc(const float* __restrict__ rec,
-                                                               const uint32_t* __restrict__ n_dev, size_t n_max, Box box,
-                                                               const __nv_bfloat16* __restrict__ act,
-                                                               const __nv_bfloat16* __restrict__ delta,
-                                                               const __nv_bfloat16* __restrict__ gout,
-                                                               float* __restrict__ part, size_t per_cta,
-                                                               uint32_t* __restrict__ status, uint32_t max_tries,
-                                                               int issue_mma) {
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const void* tmap, int x, int y, int z, int w, uint32_t mbar_addr) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(
+            dst),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(z), "r"(w), "r"(mbar_addr)
+        : "memory");
+}
+// mbar_wait that also gives up once another thread of the CTA has marked it failed
+__device__ __forceinline__ bool mbar_wait_or_fail(uint32_t addr, uint32_t phase, uint32_t max_tries,
+                                                  volatile uint32_t* failed) {
+    for (uint32_t i = 0; i < max_tries; i += 256u) {
+        if (mbar_wait(addr, phase, 256u)) return true;
+        if (*failed) return false;
+    }
+    return false;
+}
+
+// Per CTA a contiguous run of whole 32-record stages, three buffers. Warp 9 (one thread) loads each
+// stage's h_1..h_5, delta_1..delta_5 and output gradient by TMA straight into the MN-major operand
+// layout (three loads per stage) and issues the stage's 14 MMAs with one commit; warps 0..8 write the stage's layer-0 encodings (warp p: input p of the 32 records; warp 8
+// also the raw inputs and the zero padding). Per buffer three mbarriers: tma_full (the loads
+// landed), enc_full (the 9 encoder warps arrived), empty (the stage's MMAs completed, so the buffer
+// may be refilled). The CTA accumulates all six weight gradients of its records in tensor memory
+// (448 of 512 columns; the 64-feature layers use the lower half of M = 128, the upper half zero)
+// and writes them as its partial sums. Rows past the record count read as zero: the forward and
+// the backward write zero rows up to the end of their last tile, and the TMA fills rows past the
+// buffers' extent with zeros.
+__global__ void __launch_bounds__(kDwThreads, 1) k_train_dw_tc(
+    const __grid_constant__ CUtensorMap tm_act, const __grid_constant__ CUtensorMap tm_delta,
+    const __grid_constant__ CUtensorMap tm_gout, const float* __restrict__ rec, const uint32_t* __restrict__ n_dev,
+    size_t n_max, Box box, float* __restrict__ part, size_t per_cta, uint32_t* __restrict__ status, uint32_t max_tries,
+    int issue_mma) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + kDwOffBar);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 3);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kDwOffBar + 3 * kDwBufs * 8);
     volatile uint32_t* failed = tmem_slot + 1;
-    const uint32_t tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
     const size_t n = n_dev ? min((size_t)*n_dev, n_max) : n_max;
     const size_t c0 = (size_t)blockIdx.x * per_cta, c1 = min(n, c0 + per_cta);
-    // the upper halves (features 64..127) of the W1..W5 A operands stay zero
-    for (int l = 1; l <= 5; ++l)
-        for (uint32_t i = tid; i < (kDwA / 2) / 16; i += kDwThreads)
-            reinterpret_cast<uint4*>(smem + dw_off_a(l) + kDwA / 2)[i] = make_uint4(0u, 0u, 0u, 0u);
+    const int S = c1 > c0 ? (int)((c1 - c0 + kDwRecords - 1) / kDwRecords) : 0;
+    const uint32_t base = (uint32_t)__cvta_generic_to_shared(smem);
+    // kind 0: tma_full, 1: enc_full, 2: empty
+    auto bar = [&](int kind, int b) { return base + kDwOffBar + 8u * (uint32_t)(kDwBufs * kind + b); };
     if (tid == 0) {
-        for (int k = 0; k < 3; ++k)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(mbar + k)));
+        for (int b = 0; b < kDwBufs; ++b) {
+            mbar_init(bar(0, b), 1);
+            mbar_init(bar(1, b), kDwEncWarps);
+            mbar_init(bar(2, b), 1);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         *failed = 0u;
     }
@@ -707,137 +756,129 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw_tc(const float* __re
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    grid_dependency_wait();  // the backward's deltas
+    grid_dependency_wait();  // the backward's deltas (and, before it, the forward's activations)
     launch_dependents();
     const uint32_t tmem = *tmem_slot;
-    const uint32_t base = (uint32_t)__cvta_generic_to_shared(smem);
-    uint32_t phase[3] = {0u, 0u, 0u};
-    bool pending[3] = {false, false, false};  // only barrier 0 is used; the drain below checks all
-    bool issued_any = false;  // an MMA has written the accumulators (the first ones overwrite)
-    bool ok = true;
-    auto issue = [&](uint32_t d_col, uint32_t a_off, uint32_t b_off, uint32_t N, bool acc0) {
-        if (tid == 0 && issue_mma) {
-            const uint32_t idesc = umma_idesc_mn(N);
-            for (uint32_t j = 0; j < (uint32_t)kDwRecords / 16; ++j)
-                umma_bf16(tmem + d_col, umma_desc_mn(base + a_off + 2u * kDwLbo * j),
-                          umma_desc_mn(base + b_off + 2u * kDwLbo * j), idesc, (acc0 || j > 0) ? 1u : 0u);
-        }
-    };
-    // the stage's rows in registers: warp w takes records 8w .. 8w + 7 (lane % 8) and, in its two
-    // loads, 8-feature groups lane / 8 and 4 + lane / 8 of h_1..h_5, of delta_1..delta_5 and of the
-    // output gradient (6 groups). A warp's 16-byte pieces then cover 8 records x 4 groups, whose
-    // places in the MN-major operands fall on distinct bank quarters (4 wavefronts per store, no
-    // conflicts), while its global loads still use every byte of the sectors they touch. The raw
-    // inputs: thread tid encodes record tid % 64, inputs d = tid / 64 + 4 m (the fourth part also
-    // writes all nine raw inputs), and loads only those.
-    const uint32_t my_rec = 8u * warp + (tid & 7u), my_grp = (tid >> 3) & 3u, enc_part = tid >> 6;
-    uint4 ph[5][2], pd[6][2];
-    float px[kIn];
-    auto load_stage = [&](size_t s0) {
-        const size_t row = s0 + my_rec;
-        const bool live = row < c1;
-#pragma unroll
-        for (int l = 0; l < 6; ++l) {
-            const int dld = l < 5 ? kWidth : kOut, dc = dld / 8;
-            const __nv_bfloat16* dsrc = l < 5 ? delta + (size_t)l * n_max * kWidth : gout;
-#pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                const uint32_t g = my_grp + 4u * (uint32_t)j;
-                if (l < 5)
-                    ph[l][j] = live ? reinterpret_cast<const uint4*>(act + (size_t)l * n_max * kWidth + row * kWidth)[g]
-                                    : make_uint4(0u, 0u, 0u, 0u);
-                pd[l][j] = (live && g < (uint32_t)dc) ? reinterpret_cast<const uint4*>(dsrc + row * dld)[g]
-                                                      : make_uint4(0u, 0u, 0u, 0u);
+    if (warp == (uint32_t)kDwEncWarps) {
+        if (lane == 0) {
+            // the TMA loads of stage s into buffer s % 3
+            auto load_stage = [&](int s) {
+                const int b = s % kDwBufs;
+                const uint32_t buf = base + (uint32_t)b * kDwBuf, fb = bar(0, b);
+                const int y = (int)(c0 + (size_t)s * kDwRecords);
+                mbar_arrive_expect_tx(fb, kDwStageTx);
+                tma_load_4d(buf + kDwOffH, &tm_act, 0, y, 0, 0, fb);
+                tma_load_4d(buf + kDwOffD, &tm_delta, 0, y, 0, 0, fb);
+                tma_load_3d(buf + kDwOffG, &tm_gout, 0, y, 0, fb);
+            };
+            auto issue = [&](uint32_t d_col, uint32_t a, uint32_t bb, uint32_t N, bool acc0) {
+                const uint32_t idesc = umma_idesc_mn(N);
+                for (uint32_t j = 0; j < (uint32_t)kDwRecords / 16; ++j)
+                    umma_bf16(tmem + d_col, umma_desc_mn(a + 2u * kDwLbo * j), umma_desc_mn(bb + 2u * kDwLbo * j), idesc,
+                              (acc0 || j > 0) ? 1u : 0u);
+            };
+            int loaded = 0, landed = 0, committed = 0;  // stages whose loads were issued / waited for / MMAs committed
+            if (issue_mma)  // the timeout test issues nothing, so that the first wait runs out
+                for (; loaded < min(S, kDwBufs); ++loaded) load_stage(loaded);
+            for (int s = 0; s < S; ++s) {
+                const int b = s % kDwBufs;
+                const uint32_t par = (uint32_t)(s / kDwBufs) & 1u;
+                if (!mbar_wait_or_fail(bar(0, b), par, max_tries, failed)) {
+                    *failed = 1u;
+                    break;
+                }
+                landed = s + 1;
+                if (!mbar_wait_or_fail(bar(1, b), par, max_tries, failed)) {
+                    *failed = 1u;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t buf = base + (uint32_t)b * kDwBuf;
+                const bool acc = s > 0;
+                issue(0u, buf + kDwOffA0, buf + dw_off_b(0), 64u, acc);
+                issue(64u, buf + kDwOffA0 + kDwA, buf + dw_off_b(0), 64u, acc);
+                for (int l = 1; l <= 5; ++l)
+                    issue(128u + 64u * (uint32_t)(l - 1), buf + dw_off_a(l), buf + dw_off_b(l), (uint32_t)layer_n(l), acc);
+                umma_commit(bar(2, b));
+                committed = s + 1;
+                if (s >= 1 && s - 1 + kDwBufs < S) {
+                    // refill stage s - 1's buffer with stage s + 2 once stage s - 1's MMAs are done
+                    if (!mbar_wait_or_fail(bar(2, (s - 1) % kDwBufs), (uint32_t)((s - 1) / kDwBufs) & 1u, max_tries, failed)) {
+                        *failed = 1u;
+                        break;
+                    }
+                    load_stage(s - 1 + kDwBufs);
+                    loaded = s - 1 + kDwBufs + 1;
+                }
+            }
+            // every MMA done (the last commit follows all of them); after a failure, also every
+            // load still in flight, so that nothing writes this CTA's memory once it has left
+            if (!*failed) {
+                if (committed > 0 && !mbar_wait_or_fail(bar(2, (committed - 1) % kDwBufs),
+                                                        (uint32_t)((committed - 1) / kDwBufs) & 1u, max_tries, failed))
+                    *failed = 1u;
+            }
+            if (*failed) {
+                for (int s = landed; s < loaded; ++s) mbar_wait(bar(0, s % kDwBufs), (uint32_t)(s / kDwBufs) & 1u, max_tries);
+                if (committed > 0)
+                    mbar_wait(bar(2, (committed - 1) % kDwBufs), (uint32_t)((committed - 1) / kDwBufs) & 1u, max_tries);
             }
         }
-        const size_t xrow = s0 + (tid & (kDwRecords - 1));
+    } else {
+        // encoder warp p: input p of record `lane` of each stage into the stage buffer's A0 (column
+        // groups 3p .. 3p + 2); warp 8 also the raw inputs (groups 27, 28) and the zero padding
+        const int p = (int)warp;
+        float xr[kIn];  // raw inputs of the next stage's record (only those this warp needs)
+        auto load_x = [&](int s) {
+            const size_t row = c0 + (size_t)s * kDwRecords + lane;
+            const bool live = s < S && row < c1;
 #pragma unroll
-        for (int c = 0; c < kIn; ++c)
-            px[c] = (xrow < c1 && (enc_part == 3u || (uint32_t)(c & 3) == enc_part)) ? rec[xrow * kRecordFloats + c] : 0.0f;
-    };
-    if (c0 < c1) load_stage(c0);
-    for (size_t s0 = c0; ok && s0 < c1; s0 += kDwRecords) {
-        const bool acc = issued_any;
-        // the previous stage's MMAs have read every operand buffer
-        if (pending[0]) {
-            const uint32_t addr = (uint32_t)__cvta_generic_to_shared(mbar);
-            if (!mbar_wait(addr, phase[0], max_tries)) *failed = 1u;
-            __syncthreads();
-            if (*failed) {
-                ok = false;
+            for (int c = 0; c < kIn; ++c) xr[c] = (live && (p == kIn - 1 || c == p)) ? rec[row * kRecordFloats + c] : 0.0f;
+        };
+        load_x(0);
+        for (int s = 0; s < S; ++s) {
+            const int b = s % kDwBufs;
+            // the buffer's previous stage (s - 3) has been consumed by its MMAs
+            if (s >= kDwBufs && !mbar_wait_or_fail(bar(2, b), (uint32_t)(s / kDwBufs - 1) & 1u, max_tries, failed)) {
+                *failed = 1u;
                 break;
             }
-            phase[0] ^= 1u;
-            pending[0] = false;
-            tc_fence_after();
-        }
-        {
-            // the encodings: four threads per record, each encoding the inputs d = part, part +
-            // 4, ... (part 3 also writes the raw inputs and the zero padding); encoding column
-            // group g (8 features) of record i goes to A block g / 16, group g % 16
-            const int i = tid & (kDwRecords - 1);
-            const bool live = s0 + i < c1;
+            const bool live = c0 + (size_t)s * kDwRecords + lane < c1;
             float x[kIn];
-            if (live) normalise_input(px, box.lo, box.inv_ext, x);
+            if (live) normalise_input(xr, box.lo, box.inv_ext, x);
             else
                 for (int c = 0; c < kIn; ++c) x[c] = 0.0f;
+            load_x(s + 1);
+            unsigned char* a0 = smem + (uint32_t)b * kDwBuf + kDwOffA0;
             auto put = [&](int g, uint4 v) {
-                *reinterpret_cast<uint4*>(smem + kDwOffA0 + (uint32_t)(g >> 4) * kDwA + dw_offset((uint32_t)(g & 15), (uint32_t)i)) = v;
+                *reinterpret_cast<uint4*>(a0 + (uint32_t)(g >> 4) * kDwA + dw_offset((uint32_t)(g & 15), lane)) = v;
             };
-            for (int d = (int)enc_part; d < kIn; d += 4) {
-                uint32_t w[kFreq];
-                if (live) encode_input(x[d], w);
-                else
-                    for (int k = 0; k < kFreq; ++k) w[k] = 0u;
+            uint32_t w[kFreq];
+            if (live) encode_input(x[p], w);
+            else
+                for (int k = 0; k < kFreq; ++k) w[k] = 0u;
 #pragma unroll
-                for (int q = 0; q < 3; ++q) put(3 * d + q, make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]));
-            }
-            if (enc_part == 3u) {
+            for (int q = 0; q < 3; ++q) put(3 * p + q, make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]));
+            if (p == kIn - 1) {
                 put(27, make_uint4(pack_bf16(x[0], x[1]), pack_bf16(x[2], x[3]), pack_bf16(x[4], x[5]), pack_bf16(x[6], x[7])));
                 put(28, make_uint4(pack_bf16(x[8], 0.0f), 0u, 0u, 0u));
                 for (int g = 29; g < kEnc / 8; ++g) put(g, make_uint4(0u, 0u, 0u, 0u));
             }
+            fence_async_smem();  // the generic-proxy stores, visible to the tensor core
+            __syncwarp();
+            if (lane == 0) mbar_arrive(bar(1, b));
         }
-        // the loaded rows: B of W0 = delta_1; A of W_l = h_l, B of W_l = delta_{l+1} (W5: gradient)
-#pragma unroll
-        for (int l = 0; l < 6; ++l) {
-            const int dc = (l < 5 ? kWidth : kOut) / 8;
-            const uint32_t b_off = l == 0 ? kDwOffB0 : dw_off_b(l);
-#pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                const uint32_t g = my_grp + 4u * (uint32_t)j;
-                if (l >= 1) *reinterpret_cast<uint4*>(smem + dw_off_a(l) + dw_offset(g, my_rec)) = ph[l - 1][j];
-                if (g < (uint32_t)dc) *reinterpret_cast<uint4*>(smem + b_off + dw_offset(g, my_rec)) = pd[l][j];
-            }
-        }
-        fence_async_smem();
-        tc_fence_before();
-        __syncthreads();
-        tc_fence_after();
-        issue(0u, kDwOffA0, kDwOffB0, 64u, acc);
-        issue(64u, kDwOffA0 + kDwA, kDwOffB0, 64u, acc);
-        for (int l = 1; l <= 5; ++l) issue(128u + 64u * (uint32_t)(l - 1), dw_off_a(l), dw_off_b(l), (uint32_t)layer_n(l), acc);
-        if (tid == 0 && issue_mma) umma_commit((uint32_t)__cvta_generic_to_shared(mbar));
-        pending[0] = true;
-        issued_any = true;
-        if (s0 + kDwRecords < c1) load_stage(s0 + kDwRecords);
-    }
-    // drain: every outstanding commit (bounded), then the accumulators out
-    for (int b = 0; b < 3; ++b) {
-        if (!pending[b]) continue;
-        const uint32_t addr = (uint32_t)__cvta_generic_to_shared(mbar + b);
-        if (!mbar_wait(addr, phase[b], max_tries)) *failed = 1u;
     }
     __syncthreads();
     tc_fence_after();
     // the CTA's partial sums of all six weight gradients to its own slice of part (every entry
     // written, zero when it had no records or gave up), in the parameters' layout; k_adam_reduce
-    // adds the slices. Warp w reads lane quarter w % 4 (features 32 (w % 4) ..); warps 0-3 take
+    // adds the slices. Warp w < 8 reads lane quarter w % 4 (features 32 (w % 4) ..); warps 0-3 take
     // dW0 and dW1, 4-7 dW2..dW5; a thread's row leaves as float4 stores.
-    {
-        const bool have = !*failed && issued_any;  // uniform over the CTA
+    if (warp < 8) {
+        const bool have = !*failed && S > 0 && issue_mma;  // uniform over the CTA
         float* P = part + (size_t)blockIdx.x * kParams;
-        const uint32_t q = warp & 3u, m = 32u * q + (tid & 31u);
+        const uint32_t q = warp & 3u, m = 32u * q + lane;
         const uint32_t lane_base = (32u * q) << 16;
         for (int acc_i = (warp < 4 ? 0 : 3); acc_i < (warp < 4 ? 3 : 7); ++acc_i) {
             if (acc_i >= 2 && q >= 2) continue;  // dW1..dW5 have 64 features: lane quarters 0 and 1
@@ -978,7 +1019,63 @@ int ensure_train_buffers(liar_gpu_ctx* ctx, liar_gpu_guide* G, size_t n) {
     rc = g_alloc(ctx, G, n * kOut * 2, &p, "guide output gradients");
     if (rc) return rc;
     G->gout = static_cast<__nv_bfloat16*>(p);
+    // rows past a step's record count are read as zero operands; start them at zero
+    cudaError_t e = cudaMemset(G->act, 0, n * 5 * kWidth * 2);
+    if (e == cudaSuccess) e = cudaMemset(G->delta, 0, n * 5 * kWidth * 2);
+    if (e == cudaSuccess) e = cudaMemset(G->gout, 0, n * kOut * 2);
+    if (e != cudaSuccess) return ctx_cuda(ctx, e, "guide training buffers");
+    G->tm_base = nullptr;
     G->cap = n;
+    return LIAR_OK;
+}
+
+// cuTensorMapEncodeTiled from the driver, through the runtime (the library links no driver stub)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+// The weight-gradient kernel's TMA descriptors for n_max records: act and delta ([5][n_max][64]
+// bf16) as 4D tensors {8 features, n_max records (stride 128 B), 8 feature groups (stride 16 B),
+// 5 layers}, boxes {8, 32, 8, 5}; the output gradient ([n_max][48]) as {8, n_max (stride 96 B),
+// 6 groups (stride 16 B)}, boxes {8, 32, 6}. The boxes land as [layer][group][record][8 features],
+// the MN-major operand layout; no swizzle; rows past n_max read as zero. Re-encoded when the buffers or the record count change.
+int ensure_tensor_maps(liar_gpu_ctx* ctx, liar_gpu_guide* G, size_t n_max) {
+    if (G->tm_base == G->act && G->tm_rows == n_max) return LIAR_OK;
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return ctx_fail(ctx, LIAR_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    const cuuint32_t box4[4] = {8, (cuuint32_t)kDwRecords, 8, 5}, box3[3] = {8, (cuuint32_t)kDwRecords, 6};
+    const cuuint32_t unit[4] = {1, 1, 1, 1};
+    const cuuint64_t dims4[4] = {8, (cuuint64_t)n_max, 8, 5};
+    const cuuint64_t strides4[3] = {(cuuint64_t)kWidth * 2, 16, (cuuint64_t)n_max * kWidth * 2};
+    const cuuint64_t dims3[3] = {8, (cuuint64_t)n_max, 6};
+    const cuuint64_t strides3[2] = {(cuuint64_t)kOut * 2, 16};
+    CUresult r = enc(&G->tm_act, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, G->act, dims4, strides4, box4, unit,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r == CUDA_SUCCESS)
+        r = enc(&G->tm_delta, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, G->delta, dims4, strides4, box4, unit,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r == CUDA_SUCCESS)
+        r = enc(&G->tm_gout, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, G->gout, dims3, strides3, box3, unit,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        G->tm_base = nullptr;
+        return ctx_fail(ctx, LIAR_ERR_CUDA, "TMA descriptor encoding failed (CUresult %d)", (int)r);
+    }
+    G->tm_base = G->act;
+    G->tm_rows = n_max;
     return LIAR_OK;
 }
 
@@ -1054,12 +1151,14 @@ int guide_train(liar_gpu_ctx* ctx, liar_gpu_guide* G, const float* d_records, co
     e = launch_pdl(k_train_bwd_tc, bgrid, kBwdThreads, kBwdTcSmem, st, G->umma_wb, d_count, n_max, G->act, G->gout,
                    G->delta, status, tries, mma);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "guide training backward");
-    // weight gradients: one CTA per SM, each over a contiguous run of whole 64-record stages
+    // weight gradients: one CTA per SM, each over a contiguous run of whole 32-record stages
+    rc = ensure_tensor_maps(ctx, G, n_max);
+    if (rc) return rc;
     const size_t stages = (n_max + kDwRecords - 1) / kDwRecords;
     const size_t per_cta = ((stages + sms - 1) / sms) * kDwRecords;
     const unsigned dgrid = (unsigned)std::max<size_t>(1, (n_max + per_cta - 1) / per_cta);
-    e = launch_pdl(k_train_dw_tc, dgrid, kDwThreads, kDwTcSmem, st, d_records, d_count, n_max, box, G->act, G->delta,
-                   G->gout, G->grad_part, per_cta, status, tries, mma);
+    e = launch_pdl(k_train_dw_tc, dgrid, kDwThreads, kDwTcSmem, st, G->tm_act, G->tm_delta, G->tm_gout, d_records,
+                   d_count, n_max, box, G->grad_part, per_cta, status, tries, mma);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "guide weight gradients");
     const float lr = apply ? (G->cfg.learning_rate > 0 ? G->cfg.learning_rate : 5e-3f) : 0.0f;
     e = launch_pdl(k_adam_reduce, (kParams / 4 + kReduceCols - 1) / kReduceCols, kReduceCols * kReduceGroups, 0, st,

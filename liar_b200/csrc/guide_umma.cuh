@@ -86,6 +86,34 @@ __device__ __forceinline__ void umma_commit(uint32_t mbar_addr) {
                  : "memory");
 }
 
+// ---- TMA (tensor memory access) loads into this CTA's shared memory, completing on an mbarrier's
+// transaction count; no cluster multicast (the source is always this GPU's own global memory)
+__device__ __forceinline__ void mbar_init(uint32_t mbar_addr, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar_addr), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar_addr) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar_addr) : "memory");
+}
+// one arrival that also announces `bytes` of TMA transactions still to land on the barrier
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t mbar_addr, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar_addr), "r"(bytes) : "memory");
+}
+// box of a 2D / 3D tensor map at (x, y[, z]) -> shared memory; x * element size must be a multiple of
+// 16 bytes (the innermost coordinate's alignment rule), rows past the tensor's extent read as zero
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const void* tmap, int x, int y, uint32_t mbar_addr) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(mbar_addr)
+        : "memory");
+}
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const void* tmap, int x, int y, int z, uint32_t mbar_addr) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+            dst),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(z), "r"(mbar_addr)
+        : "memory");
+}
+
 // bounded wait for the mbarrier phase: true when it completed
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar_addr, uint32_t phase, uint32_t max_tries) {
     for (uint32_t i = 0; i < max_tries; ++i) {
