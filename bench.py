@@ -778,7 +778,7 @@ def run_case(name: str) -> None:
         flop = 2 * (225 * 64 + 4 * 64 * 64 + 64 * 40) * (1 << 20)
         print(json.dumps({"case": name, "eval_device_ms_1M": ms, "tflops": flop / (ms * 1e-3) / 1e12}))
     elif name == "guide-train":
-        # three Adam steps over 65,536 random records, device-timed
+        # twenty Adam steps over 65,536 random records, device-timed
         from liar_b200 import guiding as GD
         g = GD.Guide(ctx, (np.array([-1, -1, -1], np.float32), np.array([1, 1, 1], np.float32)))
         gen = torch.Generator("cuda").manual_seed(0)
@@ -790,11 +790,11 @@ def run_case(name: str) -> None:
         st = torch.cuda.Stream()  # a stream of its own: the events must see the training kernels
         torch.cuda.synchronize()
         e0.record(st)
-        for _ in range(3):
+        for _ in range(20):
             g.train_device(rec, stream=st.cuda_stream)
         e1.record(st)
         torch.cuda.synchronize()
-        print(json.dumps({"case": name, "train_step_device_ms": e0.elapsed_time(e1) / 3}))
+        print(json.dumps({"case": name, "train_step_device_ms": e0.elapsed_time(e1) / 20}))
     elif name in ("direct", "shade"):
         from liar_b200 import render as R, scenes_render, tracers
         e = scenes_render.cornell_engine(256, 256, 16)

@@ -679,15 +679,25 @@ constexpr uint32_t kDwStageTx = (5u * 8u + 5u * 8u + 6u) * kDwGroup;
 // (16 B per record, 128 B per core matrix); K-adjacent core matrices 128 B apart (leading byte
 // offset), MN-adjacent ones 512 B apart (stride byte offset, the 4 record groups of a stage). The 8
 // features of group g for all 32 records are therefore one contiguous 512-byte block at g * 512,
-// record k at k * 16. A TMA box of {8 features, 32 records, 8 groups, 5 layers} over the stored
-// [layer][record][64 features] rows (the group dimension's stride 16 B, the record's 128 B) lands in
-// exactly this order, all five layers back to back.
+// record k at k * 16. This interleaved layout is kept for the output gradient (48 wide, the B
+// operand of W5), loaded as a TMA box {8 features, 32 records, 6 groups} (the group dimension's
+// stride 16 B, the record's 96 B); the other operands use the 128-byte swizzle below.
 constexpr uint32_t kDwLbo = 128u, kDwSbo = (uint32_t)(kDwRecords / 8) * 128u;
 __device__ __forceinline__ uint32_t dw_offset(uint32_t group, uint32_t k) {
     return group * kDwSbo + (k >> 3) * kDwLbo + (k & 7u) * 16u;
 }
 // MN-major shared-memory descriptor (no swizzle): leading byte offset = the K stride, stride byte
 // offset = the MN stride
+// MN-major with the 128-byte swizzle (the layout a TMA box of 64 features x 32 records writes with
+// CU_TENSOR_MAP_SWIZZLE_128B): rows of 64 features (128 B, 16-byte chunks XOR-permuted by the row's
+// index within its 8-row group), 8 records per 1024-byte group; leading byte offset = the stride
+// between 64-feature atoms along MN (4 KB: 32 records), stride byte offset = the 8-record stride
+// (1 KB); layout type 2 (128B) in bits 61-63
+constexpr uint32_t kDwSwAtom = 4096u, kDwSwGroup = 1024u;
+__device__ __forceinline__ uint64_t umma_desc_mn_sw128(uint32_t smem_addr) {
+    return (uint64_t)((smem_addr >> 4) & 0x3FFFu) | ((uint64_t)(kDwSwAtom >> 4) << 16) |
+           ((uint64_t)(kDwSwGroup >> 4) << 32) | (1ull << 46) | (2ull << 61);
+}
 __device__ __forceinline__ uint64_t umma_desc_mn(uint32_t smem_addr) {
     return (uint64_t)((smem_addr >> 4) & 0x3FFFu) | ((uint64_t)(kDwLbo >> 4) << 16) |
            ((uint64_t)((kDwSbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
@@ -767,14 +777,17 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw_tc(
                 const uint32_t buf = base + (uint32_t)b * kDwBuf, fb = bar(0, b);
                 const int y = (int)(c0 + (size_t)s * kDwRecords);
                 mbar_arrive_expect_tx(fb, kDwStageTx);
-                tma_load_4d(buf + kDwOffH, &tm_act, 0, y, 0, 0, fb);
-                tma_load_4d(buf + kDwOffD, &tm_delta, 0, y, 0, 0, fb);
+                tma_load_3d(buf + kDwOffH, &tm_act, 0, y, 0, fb);
+                tma_load_3d(buf + kDwOffD, &tm_delta, 0, y, 0, fb);
                 tma_load_3d(buf + kDwOffG, &tm_gout, 0, y, 0, fb);
             };
-            auto issue = [&](uint32_t d_col, uint32_t a, uint32_t bb, uint32_t N, bool acc0) {
+            // A and B swizzled (128B), except the output gradient (B of W5), interleaved; a K step of
+            // 16 records is two 8-record groups: 2 KB swizzled, 256 B interleaved
+            auto issue = [&](uint32_t d_col, uint32_t a, uint32_t bb, uint32_t N, bool acc0, bool b_sw) {
                 const uint32_t idesc = umma_idesc_mn(N);
                 for (uint32_t j = 0; j < (uint32_t)kDwRecords / 16; ++j)
-                    umma_bf16(tmem + d_col, umma_desc_mn(a + 2u * kDwLbo * j), umma_desc_mn(bb + 2u * kDwLbo * j), idesc,
+                    umma_bf16(tmem + d_col, umma_desc_mn_sw128(a + 2u * kDwSwGroup * j),
+                              b_sw ? umma_desc_mn_sw128(bb + 2u * kDwSwGroup * j) : umma_desc_mn(bb + 2u * kDwLbo * j), idesc,
                               (acc0 || j > 0) ? 1u : 0u);
             };
             int loaded = 0, landed = 0, committed = 0;  // stages whose loads were issued / waited for / MMAs committed
@@ -795,10 +808,10 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw_tc(
                 tc_fence_after();
                 const uint32_t buf = base + (uint32_t)b * kDwBuf;
                 const bool acc = s > 0;
-                issue(0u, buf + kDwOffA0, buf + dw_off_b(0), 64u, acc);
-                issue(64u, buf + kDwOffA0 + kDwA, buf + dw_off_b(0), 64u, acc);
+                issue(0u, buf + kDwOffA0, buf + dw_off_b(0), 64u, acc, true);
+                issue(64u, buf + kDwOffA0 + kDwA, buf + dw_off_b(0), 64u, acc, true);
                 for (int l = 1; l <= 5; ++l)
-                    issue(128u + 64u * (uint32_t)(l - 1), buf + dw_off_a(l), buf + dw_off_b(l), (uint32_t)layer_n(l), acc);
+                    issue(128u + 64u * (uint32_t)(l - 1), buf + dw_off_a(l), buf + dw_off_b(l), (uint32_t)layer_n(l), acc, l < 5);
                 umma_commit(bar(2, b));
                 committed = s + 1;
                 if (s >= 1 && s - 1 + kDwBufs < S) {
@@ -851,7 +864,9 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw_tc(
             load_x(s + 1);
             unsigned char* a0 = smem + (uint32_t)b * kDwBuf + kDwOffA0;
             auto put = [&](int g, uint4 v) {
-                *reinterpret_cast<uint4*>(a0 + (uint32_t)(g >> 4) * kDwA + dw_offset((uint32_t)(g & 15), lane)) = v;
+                const uint32_t r8 = lane & 7u;
+                *reinterpret_cast<uint4*>(a0 + (uint32_t)(g >> 3) * kDwSwAtom + (lane >> 3) * kDwSwGroup + r8 * 128u +
+                                          (((uint32_t)(g & 7) ^ r8) << 4)) = v;
             };
             uint32_t w[kFreq];
             if (live) encode_input(x[p], w);
@@ -1045,26 +1060,27 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 }
 
 // The weight-gradient kernel's TMA descriptors for n_max records: act and delta ([5][n_max][64]
-// bf16) as 4D tensors {8 features, n_max records (stride 128 B), 8 feature groups (stride 16 B),
-// 5 layers}, boxes {8, 32, 8, 5}; the output gradient ([n_max][48]) as {8, n_max (stride 96 B),
-// 6 groups (stride 16 B)}, boxes {8, 32, 6}. The boxes land as [layer][group][record][8 features],
-// the MN-major operand layout; no swizzle; rows past n_max read as zero. Re-encoded when the buffers or the record count change.
+// bf16) as 3D tensors {64 features, n_max records, 5 layers}, boxes {64, 32, 5} with the 128-byte
+// swizzle (the MN-major swizzled operand layout, five layers back to back); the output gradient
+// ([n_max][48]) as {8 features, n_max records (stride 96 B), 6 groups (stride 16 B)}, boxes
+// {8, 32, 6}, unswizzled (the interleaved MN-major layout). Rows past n_max read as zero.
+// Re-encoded when the buffers or the record count change.
 int ensure_tensor_maps(liar_gpu_ctx* ctx, liar_gpu_guide* G, size_t n_max) {
     if (G->tm_base == G->act && G->tm_rows == n_max) return LIAR_OK;
     PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
     if (!enc) return ctx_fail(ctx, LIAR_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
-    const cuuint32_t box4[4] = {8, (cuuint32_t)kDwRecords, 8, 5}, box3[3] = {8, (cuuint32_t)kDwRecords, 6};
+    const cuuint32_t box4[3] = {(cuuint32_t)kWidth, (cuuint32_t)kDwRecords, 5}, box3[3] = {8, (cuuint32_t)kDwRecords, 6};
     const cuuint32_t unit[4] = {1, 1, 1, 1};
-    const cuuint64_t dims4[4] = {8, (cuuint64_t)n_max, 8, 5};
-    const cuuint64_t strides4[3] = {(cuuint64_t)kWidth * 2, 16, (cuuint64_t)n_max * kWidth * 2};
+    const cuuint64_t dims4[3] = {(cuuint64_t)kWidth, (cuuint64_t)n_max, 5};
+    const cuuint64_t strides4[2] = {(cuuint64_t)kWidth * 2, (cuuint64_t)n_max * kWidth * 2};
     const cuuint64_t dims3[3] = {8, (cuuint64_t)n_max, 6};
     const cuuint64_t strides3[2] = {(cuuint64_t)kOut * 2, 16};
-    CUresult r = enc(&G->tm_act, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, G->act, dims4, strides4, box4, unit,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+    CUresult r = enc(&G->tm_act, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, G->act, dims4, strides4, box4, unit,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r == CUDA_SUCCESS)
-        r = enc(&G->tm_delta, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, G->delta, dims4, strides4, box4, unit,
-                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+        r = enc(&G->tm_delta, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, G->delta, dims4, strides4, box4, unit,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r == CUDA_SUCCESS)
         r = enc(&G->tm_gout, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, G->gout, dims3, strides3, box3, unit,
