@@ -123,38 +123,12 @@ __global__ void k_pack_umma(const float* __restrict__ P, unsigned char* __restri
         *reinterpret_cast<__nv_bfloat16*>(img_b + umma_wb_offset(l) + umma_offset((uint32_t)k, (uint32_t)n, (uint32_t)N)) = w;
 }
 
-// the loss gradient of one record with respect to the 40 raw outputs (scaled by `scale`)
-__device__ float record_gradient(const float* o, float wx, float wy, float wz, float weight, float scale, float* d) {
-    Lobe L[kLobes];
-    float pi[kLobes], la[kLobes], cs[kLobes];
-    mixture_from_raw(o, L, pi);
-    float mx = -3.0e38f;
-    for (int l = 0; l < kLobes; ++l) {
-        cs[l] = L[l].mx * wx + L[l].my * wy + L[l].mz * wz;
-        la[l] = logf(pi[l]) + vmf_log_pdf(L[l].kappa, cs[l]);
-        mx = fmaxf(mx, la[l]);
-    }
-    float s = 0.0f;
-    for (int l = 0; l < kLobes; ++l) s += expf(la[l] - mx);
-    const float lq = mx + logf(s);
-    const float ws = weight * scale;
-    for (int l = 0; l < kLobes; ++l) {
-        const float r = expf(la[l] - lq);
-        const float k = L[l].kappa;
-        const float c = -ws * r;
-        d[5 * l + 4] = -ws * (r - pi[l]);
-        const float sk = o[5 * l + 3];
-        d[5 * l + 3] = (sk > kLogKappaMin && sk < kLogKappaMax) ? c * k * (1.0f / k - 2.0f / expm1f(2.0f * k) + cs[l] - 1.0f)
-                                                                 : 0.0f;
-        // d mu / d m = (I - mu mu^T) / |m|
-        const float nm = sqrtf(o[5 * l] * o[5 * l] + o[5 * l + 1] * o[5 * l + 1] + o[5 * l + 2] * o[5 * l + 2]);
-        const float f = c * k / fmaxf(nm, kMeanNormMin);
-        d[5 * l + 0] = f * (wx - cs[l] * L[l].mx);
-        d[5 * l + 1] = f * (wy - cs[l] * L[l].my);
-        d[5 * l + 2] = f * (wz - cs[l] * L[l].mz);
-    }
-    return -weight * lq;
-}
+// the loss gradient of one record with respect to the 40 raw outputs (scaled by `scale`); the
+// mixture from mixture_head_fast, the hardware's approximate exponential, logarithm and division
+// (relative errors of a few 1e-7, far below the bf16 rounding of the gradient), expm1f where
+// 1 - e^{-2 kappa} cancels
+__device__ float record_gradient(const float* o, float wx, float wy, float wz, float weight, float scale, float* d);
+
 
 // The inference head: mixture_from_raw with the hardware's approximate reciprocal square root,
 // exponential and division (relative errors of a few 1e-7, far below the bf16 rounding of the
@@ -187,6 +161,39 @@ __device__ __forceinline__ void mixture_head_fast(const float* o, Lobe* lobes, f
 }
 __device__ __forceinline__ float vmf_norm_fast(float kappa) {
     return __fdividef(kappa, 6.283185307179586f * -expm1f(-2.0f * kappa));
+}
+
+__device__ float record_gradient(const float* o, float wx, float wy, float wz, float weight, float scale, float* d) {
+    Lobe L[kLobes];
+    float pi[kLobes], la[kLobes], cs[kLobes];
+    mixture_head_fast(o, L, pi);
+    float mx = -3.0e38f;
+    for (int l = 0; l < kLobes; ++l) {
+        cs[l] = L[l].mx * wx + L[l].my * wy + L[l].mz * wz;
+        la[l] = __logf(pi[l]) + __logf(__fdividef(L[l].kappa, -expm1f(-2.0f * L[l].kappa))) -
+                1.8378770664093453f /* log 2 pi */ + L[l].kappa * (cs[l] - 1.0f);
+        mx = fmaxf(mx, la[l]);
+    }
+    float s = 0.0f;
+    for (int l = 0; l < kLobes; ++l) s += __expf(la[l] - mx);
+    const float lq = mx + __logf(s);
+    const float ws = weight * scale;
+    for (int l = 0; l < kLobes; ++l) {
+        const float r = __expf(la[l] - lq);
+        const float k = L[l].kappa;
+        const float c = -ws * r;
+        d[5 * l + 4] = -ws * (r - pi[l]);
+        const float sk = o[5 * l + 3];
+        d[5 * l + 3] = (sk > kLogKappaMin && sk < kLogKappaMax) ? c * k * (__fdividef(1.0f, k) - __fdividef(2.0f, expm1f(2.0f * k)) + cs[l] - 1.0f)
+                                                                 : 0.0f;
+        // d mu / d m = (I - mu mu^T) / |m|
+        const float nm = sqrtf(o[5 * l] * o[5 * l] + o[5 * l + 1] * o[5 * l + 1] + o[5 * l + 2] * o[5 * l + 2]);
+        const float f = __fdividef(c * k, fmaxf(nm, kMeanNormMin));
+        d[5 * l + 0] = f * (wx - cs[l] * L[l].mx);
+        d[5 * l + 1] = f * (wy - cs[l] * L[l].my);
+        d[5 * l + 2] = f * (wz - cs[l] * L[l].mz);
+    }
+    return -weight * lq;
 }
 
 // ---- inference on tcgen05: four slots of 128 rows per CTA (guide_umma.cuh)
@@ -465,7 +472,14 @@ __global__ void k_weight_sum(const float* __restrict__ rec, const uint32_t* __re
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if ((threadIdx.x & 31) == 0 && s != 0.0f) atomicAdd(scalars, s);
+    __shared__ float warp_sum[32];
+    if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {  // one atomic per block
+        float b = 0.0f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) b += warp_sum[w];
+        if (b != 0.0f) atomicAdd(scalars, b);
+    }
 }
 
 
@@ -683,9 +697,6 @@ constexpr uint32_t kDwStageTx = (5u * 8u + 5u * 8u + 6u) * kDwGroup;
 // operand of W5), loaded as a TMA box {8 features, 32 records, 6 groups} (the group dimension's
 // stride 16 B, the record's 96 B); the other operands use the 128-byte swizzle below.
 constexpr uint32_t kDwLbo = 128u, kDwSbo = (uint32_t)(kDwRecords / 8) * 128u;
-__device__ __forceinline__ uint32_t dw_offset(uint32_t group, uint32_t k) {
-    return group * kDwSbo + (k >> 3) * kDwLbo + (k & 7u) * 16u;
-}
 // MN-major shared-memory descriptor (no swizzle): leading byte offset = the K stride, stride byte
 // offset = the MN stride
 // MN-major with the 128-byte swizzle (the layout a TMA box of 64 features x 32 records writes with
@@ -705,13 +716,6 @@ __device__ __forceinline__ uint64_t umma_desc_mn(uint32_t smem_addr) {
 // kind::f16 with both operands MN-major (bits 15 and 16)
 __host__ __device__ constexpr uint32_t umma_idesc_mn(uint32_t n) { return umma_idesc(n) | (1u << 15) | (1u << 16); }
 
-__device__ __forceinline__ void tma_load_4d(uint32_t dst, const void* tmap, int x, int y, int z, int w, uint32_t mbar_addr) {
-    asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(
-            dst),
-        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(z), "r"(w), "r"(mbar_addr)
-        : "memory");
-}
 // mbar_wait that also gives up once another thread of the CTA has marked it failed
 __device__ __forceinline__ bool mbar_wait_or_fail(uint32_t addr, uint32_t phase, uint32_t max_tries,
                                                   volatile uint32_t* failed) {
@@ -917,8 +921,9 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw_tc(
 
 // The weight gradient (the sum of the nparts partial slices of k_train_dw_tc, in a fixed order, so
 // that a step is reproducible) and Adam on the f32 master weights. A block covers 32 float4
-// columns of parameters; its 8 warps sum every 8th slice each, then warp 0 adds the 8 sums.
-constexpr int kReduceCols = 32, kReduceGroups = 8;
+// columns of parameters; its 32 warps sum every 32nd slice each (at most 5 loads, all in flight
+// together), then warp 0 adds the 32 sums.
+constexpr int kReduceCols = 32, kReduceGroups = 32, kReduceMaxParts = 160;
 __global__ void __launch_bounds__(kReduceCols * kReduceGroups) k_adam_reduce(
     const float* __restrict__ part, int nparts, float* __restrict__ P, float* __restrict__ M, float* __restrict__ V,
     const uint32_t* __restrict__ step, float lr, float b1, float b2, float eps, float* __restrict__ grad_out) {
@@ -930,13 +935,19 @@ __global__ void __launch_bounds__(kReduceCols * kReduceGroups) k_adam_reduce(
     const bool live = c4 < kParams / 4;
     float4 acc = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     if (live) {
-#pragma unroll 4
-        for (int p = grp; p < nparts; p += kReduceGroups) {
-            const float4 x = __ldcs(reinterpret_cast<const float4*>(part + (size_t)p * kParams) + c4);
-            acc.x += x.x;
-            acc.y += x.y;
-            acc.z += x.z;
-            acc.w += x.w;
+        float4 x[kReduceMaxParts / kReduceGroups];
+#pragma unroll
+        for (int k = 0; k < kReduceMaxParts / kReduceGroups; ++k) {
+            const int p = grp + k * kReduceGroups;
+            x[k] = p < nparts ? __ldcs(reinterpret_cast<const float4*>(part + (size_t)p * kParams) + c4)
+                              : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+#pragma unroll
+        for (int k = 0; k < kReduceMaxParts / kReduceGroups; ++k) {
+            acc.x += x[k].x;
+            acc.y += x[k].y;
+            acc.z += x[k].z;
+            acc.w += x[k].w;
         }
     }
     sums[grp][lane] = acc;
@@ -1147,7 +1158,8 @@ int guide_train(liar_gpu_ctx* ctx, liar_gpu_guide* G, const float* d_records, co
     cudaError_t e = cudaMemsetAsync(G->scalars, 0, 2 * sizeof(float), st);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "guide scalars");
     const int sms = ctx->num_sms;
-    k_weight_sum<<<sms * 4, 256, 0, st>>>(d_records, d_count, n_max, G->scalars);
+    k_weight_sum<<<(unsigned)std::max<size_t>(1, std::min<size_t>((n_max + 255) / 256, (size_t)sms * 4)), 256, 0, st>>>(
+        d_records, d_count, n_max, G->scalars);
     // the bounded waits of the tensor-core kernels (the fault test: no MMA, a short limit)
     const bool wait_test = ctx->fault_test == LIAR_FAULT_TEST_GUIDE_WAIT;
     const uint32_t tries = wait_test ? 1u << 16 : 1u << 24;
@@ -1171,7 +1183,8 @@ int guide_train(liar_gpu_ctx* ctx, liar_gpu_guide* G, const float* d_records, co
     rc = ensure_tensor_maps(ctx, G, n_max);
     if (rc) return rc;
     const size_t stages = (n_max + kDwRecords - 1) / kDwRecords;
-    const size_t per_cta = ((stages + sms - 1) / sms) * kDwRecords;
+    const size_t ctas = (size_t)std::min(sms, kReduceMaxParts);  // partial slices k_adam_reduce can add
+    const size_t per_cta = ((stages + ctas - 1) / ctas) * kDwRecords;
     const unsigned dgrid = (unsigned)std::max<size_t>(1, (n_max + per_cta - 1) / per_cta);
     e = launch_pdl(k_train_dw_tc, dgrid, kDwThreads, kDwTcSmem, st, G->tm_act, G->tm_delta, G->tm_gout, d_records,
                    d_count, n_max, box, G->grad_part, per_cta, status, tries, mma);
