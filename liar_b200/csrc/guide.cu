@@ -8,8 +8,8 @@
 // q = sum_l pi_l vMF(w; mu_l, kappa_l), pi = softmax(logits), mu = m / |m|, kappa = e^{clamp(s)}.
 // One step, every GEMM on the 5th-generation tensor cores (tcgen05): forward (stores the bf16
 // activations and the output gradient, fused) -> backward (stores the bf16 layer deltas) -> weight
-// gradients over the records, accumulated in tensor memory -> Adam on the f32 master weights ->
-// repack the bf16 operand images.
+// gradients over the records (TMA-fed), accumulated in tensor memory as per-CTA partial sums ->
+// their sum, Adam on the f32 master weights and the repacked bf16 operand images, one kernel.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
@@ -34,7 +34,6 @@ struct liar_gpu_guide {
     float* params = nullptr;   // f32 master weights
     float* adam_m = nullptr;
     float* adam_v = nullptr;
-    uint32_t* step = nullptr;  // Adam step count (device)
     unsigned char* umma_w = nullptr;   // forward B-operand images of the six layers (inference, training)
     unsigned char* umma_wb = nullptr;  // backward B-operand images of W1..W5 (training)
     // training scratch, sized for cap records
@@ -105,22 +104,21 @@ constexpr uint32_t kUmmaWbBytes = 4u * 8192u + 6144u;  // W1..W4 64 x 64, W5 64 
 
 // the tcgen05 B operands: layer l's element (n, k) = W_l[k][n] at umma_offset(n, k, K_l) in img
 // (the forward), and for l >= 1 element (k, n) at umma_offset(k, n, N_l) in img_b (the backward,
-// W_l transposed); bump: count the Adam step just taken
-__global__ void k_pack_umma(const float* __restrict__ P, unsigned char* __restrict__ img,
-                            unsigned char* __restrict__ img_b, uint32_t* step, int bump) {
-    grid_dependency_wait();  // the Adam update, when it precedes
-    launch_dependents();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;  // one parameter (k, n) per thread
-    if (i == 0 && bump) *step += 1;
-    if (i >= kParams) return;
+// W_l transposed): parameter i (row-major [in][out] within its layer) as bf16 into both
+__device__ __forceinline__ void pack_param(int i, float value, unsigned char* __restrict__ img,
+                                           unsigned char* __restrict__ img_b) {
     int l = 0;
     while (l < 5 && i >= param_offset(l + 1)) ++l;
     const int loc = i - param_offset(l), N = layer_n(l), K = layer_k(l);
     const int k = loc / N, n = loc % N;
-    const __nv_bfloat16 w = __float2bfloat16_rn(P[i]);
+    const __nv_bfloat16 w = __float2bfloat16_rn(value);
     *reinterpret_cast<__nv_bfloat16*>(img + umma_w_offset(l) + umma_offset((uint32_t)n, (uint32_t)k, (uint32_t)K)) = w;
     if (l >= 1)
         *reinterpret_cast<__nv_bfloat16*>(img_b + umma_wb_offset(l) + umma_offset((uint32_t)k, (uint32_t)n, (uint32_t)N)) = w;
+}
+__global__ void k_pack_umma(const float* __restrict__ P, unsigned char* __restrict__ img, unsigned char* __restrict__ img_b) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;  // one parameter (k, n) per thread
+    if (i < kParams) pack_param(i, P[i], img, img_b);
 }
 
 // the loss gradient of one record with respect to the 40 raw outputs (scaled by `scale`); the
@@ -647,12 +645,12 @@ __global__ void __launch_bounds__(kBwdThreads, 1) k_train_bwd_tc(const unsigned 
                     const uint4 hh = h[4 * half + c];
                     const uint32_t hw[4] = {hh.x, hh.y, hh.z, hh.w};
                     uint32_t o[4];
+                    // h_l is a ReLU output (a zero or positive), so h > 0 is "its 15 magnitude bits
+                    // are not zero": the bf16 pair of the accumulator masked by a per-half compare
+                    // (the same bits as converting the selected values, a masked half being +0)
 #pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        const float a = bf16_lo(hw[e]) > 0.0f ? v[8 * c + 2 * e] : 0.0f;
-                        const float b = bf16_hi(hw[e]) > 0.0f ? v[8 * c + 2 * e + 1] : 0.0f;
-                        o[e] = pack_bf16(a, b);
-                    }
+                    for (int e = 0; e < 4; ++e)
+                        o[e] = pack_bf16(v[8 * c + 2 * e], v[8 * c + 2 * e + 1]) & __vcmpne2(hw[e] & 0x7fff7fffu, 0u);
                     const uint4 packed = make_uint4(o[0], o[1], o[2], o[3]);
                     if (row < n_max) drow[4 * half + c] = packed;  // zero past the record count
                     if (l > 1) *reinterpret_cast<uint4*>(dst + (4 * half + c) * 128u) = packed;
@@ -920,13 +918,15 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw_tc(
 }
 
 // The weight gradient (the sum of the nparts partial slices of k_train_dw_tc, in a fixed order, so
-// that a step is reproducible) and Adam on the f32 master weights. A block covers 32 float4
+// that a step is reproducible) and Adam on the f32 master weights, each new weight also packed
+// into the bf16 operand images. A block covers 32 float4
 // columns of parameters; its 32 warps sum every 32nd slice each (at most 5 loads, all in flight
 // together), then warp 0 adds the 32 sums.
 constexpr int kReduceCols = 32, kReduceGroups = 32, kReduceMaxParts = 160;
 __global__ void __launch_bounds__(kReduceCols * kReduceGroups) k_adam_reduce(
     const float* __restrict__ part, int nparts, float* __restrict__ P, float* __restrict__ M, float* __restrict__ V,
-    const uint32_t* __restrict__ step, float lr, float b1, float b2, float eps, float* __restrict__ grad_out) {
+    float t, float lr, float b1, float b2, float eps, float* __restrict__ grad_out, unsigned char* __restrict__ img,
+    unsigned char* __restrict__ img_b) {
     __shared__ float4 sums[kReduceGroups][kReduceCols];
     grid_dependency_wait();  // the weight-gradient partial sums
     launch_dependents();
@@ -962,8 +962,7 @@ __global__ void __launch_bounds__(kReduceCols * kReduceGroups) k_adam_reduce(
     }
     if (grad_out) reinterpret_cast<float4*>(grad_out)[c4] = make_float4(g[0], g[1], g[2], g[3]);
     if (lr <= 0.0f) return;  // gradients only
-    const float t = (float)(*step + 1);
-    const float c1 = 1.0f - powf(b1, t), c2 = 1.0f - powf(b2, t);
+    const float c1 = 1.0f - powf(b1, t), c2 = 1.0f - powf(b2, t);  // t: the step being taken, from 1
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         const int i = 4 * c4 + j;
@@ -972,7 +971,9 @@ __global__ void __launch_bounds__(kReduceCols * kReduceGroups) k_adam_reduce(
         M[i] = m;
         V[i] = v;
         const float mh = m / c1, vh = v / c2;
-        P[i] -= lr * mh / (sqrtf(vh) + eps);
+        const float p = P[i] - lr * mh / (sqrtf(vh) + eps);
+        P[i] = p;
+        pack_param(i, p, img, img_b);  // the new weight into both bf16 operand images
     }
 }
 
@@ -994,12 +995,8 @@ cudaError_t launch_pdl(void (*kernel)(KArgs...), unsigned grid, unsigned block, 
     return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
 }
 
-// pdl: the pack follows the Adam kernel of a training step (programmatic launch)
-int launch_pack(liar_gpu_guide* G, cudaStream_t st, int bump, bool pdl = false) {
-    const unsigned grid = (kParams + 255) / 256;
-    if (pdl) return launch_pdl(k_pack_umma, grid, 256, 0, st, G->params, G->umma_w, G->umma_wb, G->step, bump) == cudaSuccess
-                        ? LIAR_OK : LIAR_ERR_CUDA;
-    k_pack_umma<<<grid, 256, 0, st>>>(G->params, G->umma_w, G->umma_wb, G->step, bump);
+int launch_pack(liar_gpu_guide* G, cudaStream_t st) {
+    k_pack_umma<<<(kParams + 255) / 256, 256, 0, st>>>(G->params, G->umma_w, G->umma_wb);
     return cudaGetLastError() == cudaSuccess ? LIAR_OK : LIAR_ERR_CUDA;
 }
 
@@ -1191,14 +1188,10 @@ int guide_train(liar_gpu_ctx* ctx, liar_gpu_guide* G, const float* d_records, co
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "guide weight gradients");
     const float lr = apply ? (G->cfg.learning_rate > 0 ? G->cfg.learning_rate : 5e-3f) : 0.0f;
     e = launch_pdl(k_adam_reduce, (kParams / 4 + kReduceCols - 1) / kReduceCols, kReduceCols * kReduceGroups, 0, st,
-                   G->grad_part, (int)dgrid, G->params, G->adam_m, G->adam_v, G->step, lr, 0.9f, 0.99f, 1e-8f,
-                   d_grad_out);
+                   G->grad_part, (int)dgrid, G->params, G->adam_m, G->adam_v, (float)(G->steps_done + 1), lr, 0.9f,
+                   0.99f, 1e-8f, d_grad_out, G->umma_w, G->umma_wb);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "guide Adam step");
-    if (apply) {
-        rc = launch_pack(G, st, 1, true);
-        if (rc) return ctx_cuda(ctx, cudaGetLastError(), "guide pack");
-        G->steps_done += 1;
-    }
+    if (apply) G->steps_done += 1;
     if (d_loss_out) {
         e = cudaMemcpyAsync(d_loss_out, G->scalars + 1, sizeof(float), cudaMemcpyDeviceToDevice, st);
         if (e != cudaSuccess) return ctx_cuda(ctx, e, "guide loss");
@@ -1238,8 +1231,7 @@ extern "C" int liar_gpu_guide_create(liar_gpu_ctx* ctx, const liar_guide_config*
         G->params = f;
         G->adam_m = f + kParams;
         G->adam_v = f + 2 * kParams;
-        G->step = reinterpret_cast<uint32_t*>(f + 3 * kParams);
-        G->scalars = f + 3 * kParams + 4;
+        G->scalars = f + 3 * kParams + 4;  // after 4 spare floats
     }
     if (!rc) rc = g_alloc(ctx, G, kUmmaWBytes, &p, "guide operand images");
     if (!rc) G->umma_w = static_cast<unsigned char*>(p);
@@ -1252,7 +1244,7 @@ extern "C" int liar_gpu_guide_create(liar_gpu_ctx* ctx, const liar_guide_config*
         if (e == cudaSuccess) e = cudaMemset(G->adam_m, 0, 2 * (size_t)kParams * sizeof(float) + 256);
         if (e != cudaSuccess) rc = ctx_cuda(ctx, e, "guide initialisation");
     }
-    if (!rc && launch_pack(G, ctx->stream, 0)) rc = ctx_cuda(ctx, cudaGetLastError(), "guide pack");
+    if (!rc && launch_pack(G, ctx->stream)) rc = ctx_cuda(ctx, cudaGetLastError(), "guide pack");
     if (!rc) rc = ctx_cuda(ctx, cudaStreamSynchronize(ctx->stream), "guide initialisation");
     if (rc) {
         liar_gpu_guide_destroy(G);
@@ -1291,9 +1283,9 @@ extern "C" int liar_gpu_guide_set_params(liar_gpu_ctx* ctx, liar_gpu_guide* G, c
     if (rc) return rc;
     cudaError_t e = cudaStreamSynchronize(ctx->stream);
     if (e == cudaSuccess) e = cudaMemcpy(G->params, host, n * sizeof(float), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemset(G->adam_m, 0, 2 * (size_t)kParams * sizeof(float) + 256);  // Adam, step
+    if (e == cudaSuccess) e = cudaMemset(G->adam_m, 0, 2 * (size_t)kParams * sizeof(float) + 256);  // Adam moments
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "guide parameters");
-    if (launch_pack(G, ctx->stream, 0)) return ctx_cuda(ctx, cudaGetLastError(), "guide pack");
+    if (launch_pack(G, ctx->stream)) return ctx_cuda(ctx, cudaGetLastError(), "guide pack");
     G->steps_done = 0;
     G->records = G->guided = G->passes = 0;
     return ctx_cuda(ctx, cudaStreamSynchronize(ctx->stream), "guide parameters");
