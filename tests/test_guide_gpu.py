@@ -297,3 +297,28 @@ def test_bounded_wait_times_out_and_the_context_stays_usable():
     ctx.synchronize()
     torch.testing.assert_close(again, ref, rtol=0, atol=0)
     g.close()
+
+
+def test_training_waits_time_out_and_training_recovers():
+    """The training kernels' bounded waits (the forward and backward MMA chains, and the
+    weight-gradient pipeline's TMA, encoder and commit barriers): under the fault test mode nothing
+    is issued to the tensor core or the TMA unit, so the first wait of every kernel runs out; the
+    step records a timeout, liar_gpu_synchronize reports LIAR_ERR_TIMEOUT, and afterwards the same
+    guide computes the same gradient as before (the partial sums are added in a fixed order)."""
+    import ctypes as C
+    from liar_b200._native import LiarGpuError
+    ctx = default_context()
+    g = _guide(seed=7)
+    rec = _cuda(_records(5000, seed=2))
+    _, ref = g.train_step(rec, apply=False, want_grad=True)
+    ctx.check(ctx._lib.liar_gpu_set_fault_test(ctx.handle, C.c_int(1)))
+    try:
+        g.train_device(rec, apply=False)
+        with pytest.raises(LiarGpuError) as err:
+            ctx.synchronize()
+        assert err.value.code == -6  # LIAR_ERR_TIMEOUT
+    finally:
+        ctx.check(ctx._lib.liar_gpu_set_fault_test(ctx.handle, C.c_int(0)))
+    _, grad = g.train_step(rec, apply=False, want_grad=True)
+    np.testing.assert_allclose(grad, ref, rtol=1e-5, atol=1e-9)
+    g.close()
