@@ -8,7 +8,8 @@
 // guide.cu).
 //
 // Parameters (f32 master copy, row-major [in][out]): W0 256x64, W1..W4 64x64, W5 64x48. For the
-// kernels they are repacked as bf16 tcgen05 B-operand images (guide.cu k_pack_umma, k_pack_umma_bwd).
+// kernels they are packed as bf16 tcgen05 B-operand images, forward and transposed (guide.cu
+// pack_param).
 #pragma once
 #include <cuda_bf16.h>
 #include <stdint.h>
