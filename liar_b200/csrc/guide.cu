@@ -42,6 +42,7 @@ struct liar_gpu_guide {
     __nv_bfloat16* delta = nullptr;  // delta_1..delta_5: [5][cap][64]
     __nv_bfloat16* gout = nullptr;   // [cap][48]
     float* grad_part = nullptr;      // [part_cap][kParams]: the weight-gradient CTAs' partial sums
+    float* wpart = nullptr;          // [kWeightParts]: k_weight_sum's block sums
     int part_cap = 0;
     float* scalars = nullptr;        // [0] weight sum [1] loss sum
     // TMA descriptors of act, delta and gout for the weight-gradient kernel, for tm_rows records
@@ -75,6 +76,7 @@ constexpr int kRecordFloats = 13;
 // normalised record weights are clipped here: radiance estimates are heavy-tailed and a handful of
 // records would otherwise set the whole gradient (the renderer stays unbiased whatever the guide)
 constexpr float kWeightClip = 20.0f;
+constexpr int kWeightParts = 1024;  // most blocks of k_weight_sum (one sum each)
 
 __device__ __forceinline__ void normalise_input(const float* raw, const float* lo, const float* inv_ext, float* x) {
     for (int c = 0; c < 3; ++c) x[c] = (raw[c] - lo[c]) * inv_ext[c];
@@ -205,7 +207,7 @@ __device__ float record_gradient(const float* o, float wx, float wy, float wz, f
 // network's inputs), the row count may come from device memory (n_dev, at most n), every hidden
 // layer's bf16 activations h_1..h_5 also go to act ([5][n_max][64]), and the output layer ends in
 // the loss head instead of the mixture: each row's loss gradient with respect to its 40 raw outputs
-// (record_gradient, weights normalised by the batch mean train[0] from k_weight_sum and clipped)
+// (record_gradient, weights normalised by the batch mean from k_weight_sum's block sums, clipped)
 // goes to gout as 48 bf16 (the last 8 zero), the batch loss is added to train[1].
 template <bool TRAIN>
 __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* __restrict__ w_img,
@@ -214,7 +216,8 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
                                                            uint32_t* __restrict__ status, uint32_t max_tries,
                                                            int issue_mma, const uint32_t* __restrict__ n_dev,
                                                            __nv_bfloat16* __restrict__ act, size_t n_max,
-                                                           float* __restrict__ train, __nv_bfloat16* __restrict__ gout) {
+                                                           float* __restrict__ train, __nv_bfloat16* __restrict__ gout,
+                                                           const float* __restrict__ wpart, int n_wpart) {
     constexpr int IN = TRAIN ? kRecordFloats : kIn;
     if (TRAIN && n_dev) n = min((size_t)*n_dev, n);
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -253,7 +256,14 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
     launch_dependents();
     float inv_mean = 0.0f, inv_b = 0.0f;  // TRAIN: 1 / mean record weight, 1 / batch size
     if (TRAIN) {
-        const float wsum = train[0];
+        // the weight sum: k_weight_sum's block sums added in one fixed order (lane j takes every
+        // 32nd, then a shuffle tree), lane 0's result broadcast, so every thread of every CTA has
+        // the same bits
+        float wsum = 0.0f;
+        for (int j = (int)(tid & 31u); j < n_wpart; j += 32) wsum += wpart[j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) wsum += __shfl_down_sync(0xffffffffu, wsum, o);
+        wsum = __shfl_sync(0xffffffffu, wsum, 0);
         inv_mean = (wsum > 0.0f && n > 0) ? (float)n / wsum : 0.0f;
         inv_b = n > 0 ? 1.0f / (float)n : 0.0f;
     }
@@ -459,8 +469,10 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
 
 // ---- training
 
+// the batch's record weights (positive and finite ones), one sum per block into wpart; the
+// training forward adds the block sums in a fixed order, so that a step is reproducible
 __global__ void k_weight_sum(const float* __restrict__ rec, const uint32_t* __restrict__ n_dev, size_t n_max,
-                             float* scalars) {
+                             float* __restrict__ wpart) {
     launch_dependents();  // the training forward's prologue reads nothing written here
     const size_t n = n_dev ? min((size_t)*n_dev, n_max) : n_max;
     float s = 0.0f;
@@ -473,10 +485,10 @@ __global__ void k_weight_sum(const float* __restrict__ rec, const uint32_t* __re
     __shared__ float warp_sum[32];
     if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = s;
     __syncthreads();
-    if (threadIdx.x == 0) {  // one atomic per block
+    if (threadIdx.x == 0) {
         float b = 0.0f;
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) b += warp_sum[w];
-        if (b != 0.0f) atomicAdd(scalars, b);
+        wpart[blockIdx.x] = b;
     }
 }
 
@@ -582,13 +594,20 @@ __device__ __forceinline__ bool tc_layer(uint32_t r, uint32_t tmem, uint32_t a_a
 // per record): weights normalised by their batch mean and clipped at kWeightClip, gradient stored
 // bf16 (48 wide, the padding zero), the loss summed over the batch
 
-constexpr uint32_t kBwdBuf = (uint32_t)kTcRows * kWidth * 2;  // a slot's A operand: 128 x 64 bf16
+constexpr uint32_t kBwdBuf = (uint32_t)kTcRows * kWidth * 2;    // a slot's A operand: 128 x 64 bf16
+constexpr uint32_t kBwdStage = (uint32_t)kTcRows * kWidth * 2;  // a slot's h rows: 128 x 64 bf16
 constexpr int kBwdSlots = 4;
 constexpr int kBwdThreads = 128 * kBwdSlots;
-constexpr size_t kBwdTcSmem = 1024 + kUmmaWbBytes + (size_t)kBwdSlots * kBwdBuf + 128;
+constexpr size_t kBwdTcSmem = 1024 + kUmmaWbBytes + (size_t)kBwdSlots * (kBwdBuf + kBwdStage) + 128;
 
-// Four slots of 128 records; per layer the record's h_l row (the ReLU mask) is loaded before the
-// layer's MMAs are waited for, and the accumulator is read 32 columns at a time.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+
+// Four slots of 128 records. Each thread copies its record's h_l row (the ReLU mask of the next
+// layer) asynchronously into the slot's staging rows (16-byte chunks XOR-permuted by the row, so
+// that a warp's accesses spread over all banks) one layer ahead, so the copy overlaps the layer
+// before; the accumulator is read 32 columns at a time.
 __global__ void __launch_bounds__(kBwdThreads, 1) k_train_bwd_tc(const unsigned char* __restrict__ wb_img,
                                                                  const uint32_t* __restrict__ n_dev, size_t n_max,
                                                                  const __nv_bfloat16* __restrict__ act,
@@ -598,13 +617,14 @@ __global__ void __launch_bounds__(kBwdThreads, 1) k_train_bwd_tc(const unsigned 
                                                                  int issue_mma) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    const TcTile T = tc_setup<kBwdSlots>(smem, kUmmaWbBytes, kBwdBuf, wb_img);
+    const TcTile T = tc_setup<kBwdSlots>(smem, kUmmaWbBytes, kBwdBuf + kBwdStage, wb_img);
     grid_dependency_wait();  // the forward's activations and output gradients
     launch_dependents();
     const size_t n = n_dev ? min((size_t)*n_dev, n_max) : n_max;
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
     const uint32_t slot = tid >> 7, r = tid & 127u;
-    unsigned char* buf = smem + kUmmaWbBytes + slot * kBwdBuf;
+    unsigned char* buf = smem + kUmmaWbBytes + slot * (kBwdBuf + kBwdStage);
+    const uint32_t stage_row = (uint32_t)__cvta_generic_to_shared(buf + kBwdBuf) + r * 128u;  // this row's h
     const uint32_t tmem = *T.tmem_slot + 64u * slot;
     const uint32_t taddr = tmem + ((32u * (warp & 3u)) << 16);
     const uint32_t mbar_addr = (uint32_t)__cvta_generic_to_shared(T.mbar_all + slot);
@@ -616,6 +636,15 @@ __global__ void __launch_bounds__(kBwdThreads, 1) k_train_bwd_tc(const unsigned 
     for (size_t tile = (size_t)blockIdx.x * kBwdSlots + slot; ok && tile < n_tiles; tile += (size_t)gridDim.x * kBwdSlots) {
         const size_t row = tile * kTcRows + r;
         const bool live = row < n;
+        // h_l of this row into the staging row (zeros past the record count), one commit group
+        auto fetch_h = [&](int l) {
+            const unsigned char* src = reinterpret_cast<const unsigned char*>(act + (size_t)(l - 1) * n_max * kWidth +
+                                                                              (live ? row : 0) * kWidth);
+#pragma unroll
+            for (uint32_t c = 0; c < 8u; ++c) cp_async16(stage_row + ((c ^ (r & 7u)) << 4), src + 16u * c, live ? 16u : 0u);
+            asm volatile("cp.async.commit_group;" ::: "memory");
+        };
+        fetch_h(kLayers - 1);
         // the output gradient (48 wide) as the first A operand
         {
             const uint4* src = reinterpret_cast<const uint4*>(gout + row * kOut);
@@ -625,14 +654,21 @@ __global__ void __launch_bounds__(kBwdThreads, 1) k_train_bwd_tc(const unsigned 
                 *reinterpret_cast<uint4*>(dst + c * 128u) = live ? src[c] : make_uint4(0u, 0u, 0u, 0u);
         }
         for (int l = kLayers - 1; l >= 1 && ok; --l) {
-            // h_l (the mask) on its way while the layer's MMAs run
-            uint4 h[kWidth / 8];
-            const uint4* hp = reinterpret_cast<const uint4*>(act + (size_t)(l - 1) * n_max * kWidth + row * kWidth);
-#pragma unroll
-            for (int c = 0; c < kWidth / 8; ++c) h[c] = live ? hp[c] : make_uint4(0u, 0u, 0u, 0u);
             ok = tc_layer(r, tmem, buf_addr, sw_addr + umma_wb_offset(l), (uint32_t)layer_n(l), (uint32_t)kWidth, mbar_addr,
                           phase, slot, T.failed, max_tries, issue_mma);
             if (!ok) break;
+            // h_l (its copy was issued a layer earlier) into registers, then h_{l-1} on its way
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+            uint4 h[kWidth / 8];
+#pragma unroll
+            for (uint32_t c = 0; c < 8u; ++c) {
+                uint4 q;
+                asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+                             : "=r"(q.x), "=r"(q.y), "=r"(q.z), "=r"(q.w)
+                             : "r"(stage_row + ((c ^ (r & 7u)) << 4)));
+                h[c] = q;
+            }
+            if (l > 1) fetch_h(l - 1);
             // mask by h_l > 0 (the ReLU of layer l - 1's output), store delta_l, next A operand
             unsigned char* dst = buf + (r >> 3) * (kWidth / 8) * 128u + (r & 7u) * 16u;
             uint4* drow = reinterpret_cast<uint4*>(delta + (size_t)(l - 1) * n_max * kWidth + row * kWidth);
@@ -658,6 +694,7 @@ __global__ void __launch_bounds__(kBwdThreads, 1) k_train_bwd_tc(const unsigned 
             }
         }
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");  // no copy into this CTA's memory outlives it
     tc_teardown<kBwdSlots>(T, status);
 }
 
@@ -1025,6 +1062,11 @@ int ensure_train_buffers(liar_gpu_ctx* ctx, liar_gpu_guide* G, size_t n) {
         G->grad_part = static_cast<float*>(p);
         G->part_cap = ctx->num_sms;
     }
+    if (!G->wpart) {
+        int rc = g_alloc(ctx, G, kWeightParts * sizeof(float), &p, "guide weight sums");
+        if (rc) return rc;
+        G->wpart = static_cast<float*>(p);
+    }
     if (G->cap >= n) return LIAR_OK;
     for (void* q : {(void*)G->act, (void*)G->delta, (void*)G->gout}) {
         if (!q) continue;
@@ -1155,8 +1197,8 @@ int guide_train(liar_gpu_ctx* ctx, liar_gpu_guide* G, const float* d_records, co
     cudaError_t e = cudaMemsetAsync(G->scalars, 0, 2 * sizeof(float), st);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "guide scalars");
     const int sms = ctx->num_sms;
-    k_weight_sum<<<(unsigned)std::max<size_t>(1, std::min<size_t>((n_max + 255) / 256, (size_t)sms * 4)), 256, 0, st>>>(
-        d_records, d_count, n_max, G->scalars);
+    const unsigned wgrid = (unsigned)std::max<size_t>(1, std::min<size_t>((n_max + 255) / 256, (size_t)kWeightParts));
+    k_weight_sum<<<wgrid, 256, 0, st>>>(d_records, d_count, n_max, G->wpart);
     // the bounded waits of the tensor-core kernels (the fault test: no MMA, a short limit)
     const bool wait_test = ctx->fault_test == LIAR_FAULT_TEST_GUIDE_WAIT;
     const uint32_t tries = wait_test ? 1u << 16 : 1u << 24;
@@ -1169,7 +1211,7 @@ int guide_train(liar_gpu_ctx* ctx, liar_gpu_guide* G, const float* d_records, co
     // the kernels after k_weight_sum start programmatically: each one's prologue (weights to shared
     // memory, barriers, tensor memory) overlaps the end of the kernel before it
     e = launch_pdl(k_eval_tc<true>, tgrid, kEvThreads, kEvSmem, st, G->umma_w, d_records, n_max, box, (float*)nullptr, 0,
-                   status, tries, mma, d_count, G->act, n_max, G->scalars, G->gout);
+                   status, tries, mma, d_count, G->act, n_max, G->scalars, G->gout, (const float*)G->wpart, (int)wgrid);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "guide training forward");
     const unsigned bgrid =
         (unsigned)std::max<size_t>(1, std::min<size_t>((tiles + kBwdSlots - 1) / kBwdSlots, (size_t)sms));
@@ -1325,7 +1367,7 @@ int liar_gpu::guide::guide_eval(liar_gpu_ctx* ctx, const liar_gpu_guide* G, cons
     const bool wait_test = ctx->fault_test == LIAR_FAULT_TEST_GUIDE_WAIT;
     k_eval_tc<false><<<grid, kEvThreads, kEvSmem, st>>>(G->umma_w, d_inputs, n, make_box(G->cfg), d_mixture, stride,
                                                           ctx->d_scratch + kStatusWord, wait_test ? 1u << 16 : 1u << 24,
-                                                          wait_test ? 0 : 1, nullptr, nullptr, 0, nullptr, nullptr);
+                                                          wait_test ? 0 : 1, nullptr, nullptr, 0, nullptr, nullptr, nullptr, 0);
     return ctx_cuda(ctx, cudaGetLastError(), "guide evaluation");
 }
 

@@ -71,10 +71,12 @@ def test_eval_matches_oracle(n):
     np.testing.assert_allclose(mu[..., 3], mur[..., 3], rtol=2e-2)
 
 
-@pytest.mark.parametrize("n", [5000, 40000])
+@pytest.mark.parametrize("n", [1, 33, 5000, 40000])
 def test_gradient_matches_oracle(n):
-    """5,000 records: one 64-record stage of the weight-gradient kernel per CTA; 40,000: several
-    stages per CTA, accumulated in tensor memory."""
+    """1 and 33 records: one CTA with a partial 32-record stage (the rows past the count read as
+    zeros; the single record of n = 1 has weight zero, so its gradient is exactly zero); 5,000
+    records: one or two stages per CTA of the weight-gradient kernel; 40,000: nine stages per CTA
+    over its three stage buffers, accumulated in tensor memory."""
     g = _guide(seed=7)
     rec = _records(n, seed=2)
     loss, grad = g.train_step(_cuda(rec), apply=False, want_grad=True)
@@ -82,6 +84,9 @@ def test_gradient_matches_oracle(n):
     assert abs(loss - ref_loss) < 1e-3 * abs(ref_loss) + 1e-6
     for l in range(6):
         a, b = grad[OFFS[l]:OFFS[l + 1]].astype(np.float64), ref[OFFS[l]:OFFS[l + 1]]
+        if not np.any(b):
+            assert not np.any(a), l
+            continue
         cos = a @ b / (np.linalg.norm(a) * np.linalg.norm(b))
         rel = np.linalg.norm(a - b) / np.linalg.norm(b)
         assert cos > 0.9995 and rel < 0.03, (l, cos, rel)
@@ -304,7 +309,8 @@ def test_training_waits_time_out_and_training_recovers():
     weight-gradient pipeline's TMA, encoder and commit barriers): under the fault test mode nothing
     is issued to the tensor core or the TMA unit, so the first wait of every kernel runs out; the
     step records a timeout, liar_gpu_synchronize reports LIAR_ERR_TIMEOUT, and afterwards the same
-    guide computes the same gradient as before (the partial sums are added in a fixed order)."""
+    guide computes the same gradient as before, bit for bit (the weight sum and the weight
+    gradients' partial sums are added in fixed orders, so a step is reproducible)."""
     import ctypes as C
     from liar_b200._native import LiarGpuError
     ctx = default_context()
@@ -320,5 +326,5 @@ def test_training_waits_time_out_and_training_recovers():
     finally:
         ctx.check(ctx._lib.liar_gpu_set_fault_test(ctx.handle, C.c_int(0)))
     _, grad = g.train_step(rec, apply=False, want_grad=True)
-    np.testing.assert_allclose(grad, ref, rtol=1e-5, atol=1e-9)
+    np.testing.assert_array_equal(grad, ref)
     g.close()
