@@ -196,6 +196,26 @@ __device__ float record_gradient(const float* o, float wx, float wy, float wz, f
     return -weight * lq;
 }
 
+// The rows of a slot's 128 x 64 bf16 A operand (K-major core matrices: row r, 8-feature chunk c
+// at (r / 8) * 1024 + (r % 8) * 16 + c * 128) to row-major global rows dst[row][64] for
+// row < limit, rows >= valid stored as zeros; thread t of the slot moves pieces t + 128 i. A warp's
+// sixteen-byte pieces cover 8 rows x 4 chunks: distinct banks in shared memory (4 wavefronts) and
+// 64 contiguous bytes per row in global memory, where one thread per row storing its own 16-byte
+// pieces touched 32 rows per instruction.
+__device__ __forceinline__ void store_tile_rows(const unsigned char* a, __nv_bfloat16* dst, uint32_t valid,
+                                                uint32_t limit, uint32_t t) {
+#pragma unroll
+    for (uint32_t i = 0; i < 8u; ++i) {
+        const uint32_t p = i * 128u + t;
+        const uint32_t row = (p & 7u) + 8u * (p >> 6), c = (p >> 3) & 7u;
+        if (row < limit) {
+            const uint4 v = row < valid ? *reinterpret_cast<const uint4*>(a + (row >> 3) * 1024u + (row & 7u) * 16u + c * 128u)
+                                        : make_uint4(0u, 0u, 0u, 0u);
+            reinterpret_cast<uint4*>(dst + (size_t)row * kWidth)[c] = v;
+        }
+    }
+}
+
 // ---- inference on tcgen05: four slots of 128 rows per CTA (guide_umma.cuh)
 // Layer 0 runs as four K-chunks over the two halves of the slot's buffer, each chunk committed to
 // the half's own mbarrier; a half is rewritten only after the commit of the chunk that read it.
@@ -367,11 +387,6 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
                         const uint4 hq = make_uint4(pack_bf16_relu(q[0], q[1]), pack_bf16_relu(q[2], q[3]),
                                                     pack_bf16_relu(q[4], q[5]), pack_bf16_relu(q[6], q[7]));
                         *reinterpret_cast<uint4*>(dst + c * 128u) = hq;
-                        // rows past the record count (to the tile's end) are stored as zeros: the
-                        // weight-gradient kernel reads whole 32-record stages
-                        if (TRAIN && row0 + r < n_max)
-                            reinterpret_cast<uint4*>(act + (size_t)(l - 1) * n_max * kWidth + (row0 + r) * kWidth)[c] =
-                                r < rows ? hq : make_uint4(0u, 0u, 0u, 0u);
                     }
                 }
                 if (!issue(buf_addr, (kWidth / 8) * 128u, sw_addr + umma_w_offset(l), (kWidth / 8) * 128u, kWidth / 16,
@@ -379,7 +394,15 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
                     ok = false;
                     break;
                 }
+                // training: h_l leaves from the operand while the layer's MMAs read it, rows past the
+                // record count (to the tile's end) as zeros, since the weight-gradient kernel reads
+                // whole 32-record stages; the slot barrier after the wait keeps the operand until
+                // every thread has moved its pieces
+                if (TRAIN)
+                    store_tile_rows(buf, act + (size_t)(l - 1) * n_max * kWidth + row0 * kWidth, rows,
+                                    (uint32_t)min((size_t)kTcRows, n_max - row0), r);
                 wait_half(0);
+                if (TRAIN) slot_sync();
             } else {
                 // the mixture of row r into the staging rows (pitch stride + 4 floats), then the
                 // slot's rows leave as one contiguous, coalesced block
@@ -565,9 +588,12 @@ __device__ __forceinline__ void tc_teardown(const TcTile& T, uint32_t* status) {
 
 // one layer of a slot: K / 16 MMAs by the slot's thread 0, committed to the slot's mbarrier, then a
 // bounded wait; false when the wait ran out (after the drain wait)
+// `between` runs on every thread of the slot after the MMAs are issued and before they are waited
+// for (the operand is stable then: written before the first barrier, rewritten after the second)
+template <typename F>
 __device__ __forceinline__ bool tc_layer(uint32_t r, uint32_t tmem, uint32_t a_addr, uint32_t b_addr, uint32_t K,
                                          uint32_t N, uint32_t mbar_addr, uint32_t& phase, uint32_t slot,
-                                         volatile uint32_t* failed, uint32_t max_tries, int issue_mma) {
+                                         volatile uint32_t* failed, uint32_t max_tries, int issue_mma, F&& between) {
     fence_async_smem();
     tc_fence_before();
     asm volatile("bar.sync %0, 128;" ::"r"(1u + slot) : "memory");
@@ -579,6 +605,7 @@ __device__ __forceinline__ bool tc_layer(uint32_t r, uint32_t tmem, uint32_t a_a
                       idesc, j > 0 ? 1u : 0u);
         umma_commit(mbar_addr);
     }
+    between();
     if (!mbar_wait(mbar_addr, phase, max_tries)) failed[slot] = 1u;
     asm volatile("bar.sync %0, 128;" ::"r"(1u + slot) : "memory");
     if (failed[slot]) {
@@ -589,10 +616,6 @@ __device__ __forceinline__ bool tc_layer(uint32_t r, uint32_t tmem, uint32_t a_a
     tc_fence_after();
     return true;
 }
-
-// the loss and its output gradient per record, from the training forward's raw outputs (one thread
-// per record): weights normalised by their batch mean and clipped at kWeightClip, gradient stored
-// bf16 (48 wide, the padding zero), the loss summed over the batch
 
 constexpr uint32_t kBwdBuf = (uint32_t)kTcRows * kWidth * 2;    // a slot's A operand: 128 x 64 bf16
 constexpr uint32_t kBwdStage = (uint32_t)kTcRows * kWidth * 2;  // a slot's h rows: 128 x 64 bf16
@@ -653,9 +676,18 @@ __global__ void __launch_bounds__(kBwdThreads, 1) k_train_bwd_tc(const unsigned 
             for (int c = 0; c < kOut / 8; ++c)
                 *reinterpret_cast<uint4*>(dst + c * 128u) = live ? src[c] : make_uint4(0u, 0u, 0u, 0u);
         }
+        // delta rows of the tile: rows past the record count are zeros (their masks are), rows past
+        // n_max are not stored
+        const uint32_t limit = (uint32_t)min((size_t)kTcRows, n_max - tile * kTcRows);
         for (int l = kLayers - 1; l >= 1 && ok; --l) {
+            // the operand holds delta_{l+1} (the output gradient for l = 5): it leaves while the
+            // layer's MMAs read it
             ok = tc_layer(r, tmem, buf_addr, sw_addr + umma_wb_offset(l), (uint32_t)layer_n(l), (uint32_t)kWidth, mbar_addr,
-                          phase, slot, T.failed, max_tries, issue_mma);
+                          phase, slot, T.failed, max_tries, issue_mma, [&]() {
+                              if (l < kLayers - 1)
+                                  store_tile_rows(buf, delta + (size_t)l * n_max * kWidth + tile * kTcRows * kWidth, limit,
+                                                  limit, r);
+                          });
             if (!ok) break;
             // h_l (its copy was issued a layer earlier) into registers, then h_{l-1} on its way
             asm volatile("cp.async.wait_group 0;" ::: "memory");
@@ -671,7 +703,6 @@ __global__ void __launch_bounds__(kBwdThreads, 1) k_train_bwd_tc(const unsigned 
             if (l > 1) fetch_h(l - 1);
             // mask by h_l > 0 (the ReLU of layer l - 1's output), store delta_l, next A operand
             unsigned char* dst = buf + (r >> 3) * (kWidth / 8) * 128u + (r & 7u) * 16u;
-            uint4* drow = reinterpret_cast<uint4*>(delta + (size_t)(l - 1) * n_max * kWidth + row * kWidth);
 #pragma unroll
             for (int half = 0; half < 2; ++half) {
                 float v[32];
@@ -687,11 +718,16 @@ __global__ void __launch_bounds__(kBwdThreads, 1) k_train_bwd_tc(const unsigned 
 #pragma unroll
                     for (int e = 0; e < 4; ++e)
                         o[e] = pack_bf16(v[8 * c + 2 * e], v[8 * c + 2 * e + 1]) & __vcmpne2(hw[e] & 0x7fff7fffu, 0u);
-                    const uint4 packed = make_uint4(o[0], o[1], o[2], o[3]);
-                    if (row < n_max) drow[4 * half + c] = packed;  // zero past the record count
-                    if (l > 1) *reinterpret_cast<uint4*>(dst + (4 * half + c) * 128u) = packed;
+                    *reinterpret_cast<uint4*>(dst + (4 * half + c) * 128u) = make_uint4(o[0], o[1], o[2], o[3]);
                 }
             }
+        }
+        if (ok) {
+            // delta_1 leaves once every thread has written its row, and before the next tile's
+            // output gradient takes the operand's place
+            asm volatile("bar.sync %0, 128;" ::"r"(1u + slot) : "memory");
+            store_tile_rows(buf, delta + tile * kTcRows * kWidth, limit, limit, r);
+            asm volatile("bar.sync %0, 128;" ::"r"(1u + slot) : "memory");
         }
     }
     asm volatile("cp.async.wait_all;" ::: "memory");  // no copy into this CTA's memory outlives it
