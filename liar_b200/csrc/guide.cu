@@ -47,6 +47,8 @@ struct liar_gpu_guide {
     float* scalars = nullptr;        // [0] weight sum [1] loss sum
     // TMA descriptors of act, delta and gout for the weight-gradient kernel, for tm_rows records
     CUtensorMap tm_act{}, tm_delta{}, tm_gout{};
+    // TMA descriptors through which the forward and backward store their activation / delta tiles
+    CUtensorMap tm_act_st{}, tm_delta_st{};
     const void* tm_base = nullptr;
     size_t tm_rows = 0;
     std::vector<void*> buffers;
@@ -77,6 +79,9 @@ constexpr int kRecordFloats = 13;
 // records would otherwise set the whole gradient (the renderer stays unbiased whatever the guide)
 constexpr float kWeightClip = 20.0f;
 constexpr int kWeightParts = 1024;  // most blocks of k_weight_sum (one sum each)
+// rows per layer of the training activations and deltas ([5][act_rows(n)][64] bf16): n rounded up
+// to whole 8-row groups, the unit the tile stores write
+__host__ __device__ __forceinline__ size_t act_rows(size_t n) { return (n + 7) & ~(size_t)7; }
 
 __device__ __forceinline__ void normalise_input(const float* raw, const float* lo, const float* inv_ext, float* x) {
     for (int c = 0; c < 3; ++c) x[c] = (raw[c] - lo[c]) * inv_ext[c];
@@ -196,26 +201,6 @@ __device__ float record_gradient(const float* o, float wx, float wy, float wz, f
     return -weight * lq;
 }
 
-// The rows of a slot's 128 x 64 bf16 A operand (K-major core matrices: row r, 8-feature chunk c
-// at (r / 8) * 1024 + (r % 8) * 16 + c * 128) to row-major global rows dst[row][64] for
-// row < limit, rows >= valid stored as zeros; thread t of the slot moves pieces t + 128 i. A warp's
-// sixteen-byte pieces cover 8 rows x 4 chunks: distinct banks in shared memory (4 wavefronts) and
-// 64 contiguous bytes per row in global memory, where one thread per row storing its own 16-byte
-// pieces touched 32 rows per instruction.
-__device__ __forceinline__ void store_tile_rows(const unsigned char* a, __nv_bfloat16* dst, uint32_t valid,
-                                                uint32_t limit, uint32_t t) {
-#pragma unroll
-    for (uint32_t i = 0; i < 8u; ++i) {
-        const uint32_t p = i * 128u + t;
-        const uint32_t row = (p & 7u) + 8u * (p >> 6), c = (p >> 3) & 7u;
-        if (row < limit) {
-            const uint4 v = row < valid ? *reinterpret_cast<const uint4*>(a + (row >> 3) * 1024u + (row & 7u) * 16u + c * 128u)
-                                        : make_uint4(0u, 0u, 0u, 0u);
-            reinterpret_cast<uint4*>(dst + (size_t)row * kWidth)[c] = v;
-        }
-    }
-}
-
 // ---- inference on tcgen05: four slots of 128 rows per CTA (guide_umma.cuh)
 // Layer 0 runs as four K-chunks over the two halves of the slot's buffer, each chunk committed to
 // the half's own mbarrier; a half is rewritten only after the commit of the chunk that read it.
@@ -237,7 +222,8 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
                                                            int issue_mma, const uint32_t* __restrict__ n_dev,
                                                            __nv_bfloat16* __restrict__ act, size_t n_max,
                                                            float* __restrict__ train, __nv_bfloat16* __restrict__ gout,
-                                                           const float* __restrict__ wpart, int n_wpart) {
+                                                           const float* __restrict__ wpart, int n_wpart,
+                                                           const __grid_constant__ CUtensorMap tm_act_store) {
     constexpr int IN = TRAIN ? kRecordFloats : kIn;
     if (TRAIN && n_dev) n = min((size_t)*n_dev, n);
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -384,8 +370,12 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
 #pragma unroll
                     for (int c = 0; c < 8; ++c) {
                         const float* q = v + 8 * c;
-                        const uint4 hq = make_uint4(pack_bf16_relu(q[0], q[1]), pack_bf16_relu(q[2], q[3]),
-                                                    pack_bf16_relu(q[4], q[5]), pack_bf16_relu(q[6], q[7]));
+                        // training: rows past the record count hold zeros (they leave with the tile;
+                        // their MMA outputs are never read)
+                        const uint4 hq = (!TRAIN || r < rows)
+                                             ? make_uint4(pack_bf16_relu(q[0], q[1]), pack_bf16_relu(q[2], q[3]),
+                                                          pack_bf16_relu(q[4], q[5]), pack_bf16_relu(q[6], q[7]))
+                                             : make_uint4(0u, 0u, 0u, 0u);
                         *reinterpret_cast<uint4*>(dst + c * 128u) = hq;
                     }
                 }
@@ -394,13 +384,14 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
                     ok = false;
                     break;
                 }
-                // training: h_l leaves from the operand while the layer's MMAs read it, rows past the
-                // record count (to the tile's end) as zeros, since the weight-gradient kernel reads
-                // whole 32-record stages; the slot barrier after the wait keeps the operand until
-                // every thread has moved its pieces
-                if (TRAIN)
-                    store_tile_rows(buf, act + (size_t)(l - 1) * n_max * kWidth + row0 * kWidth, rows,
-                                    (uint32_t)min((size_t)kTcRows, n_max - row0), r);
+                // training: h_l leaves the operand by one TMA store while the layer's MMAs read it (the
+                // tile's 16 8-row groups, rows past the record count as zeros: the weight-gradient
+                // kernel reads whole 32-record stages); its issuer waits until the store has read the
+                // operand, and the slot barrier after the MMA wait keeps the operand until then
+                if (TRAIN && r == 0) {
+                    tma_store_5d(&tm_act_store, 0, 0, 0, (int)(row0 >> 3), l - 1, buf_addr);
+                    bulk_wait_read();
+                }
                 wait_half(0);
                 if (TRAIN) slot_sync();
             } else {
@@ -480,6 +471,7 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
         for (int h = 0; h < 2; ++h)
             if (pending[h]) mbar_wait(mb[h], phase[h], max_tries);
     }
+    if (TRAIN && r == 0) bulk_wait_all();  // the activation stores are complete before the grid ends
     tc_fence_before();
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tmem_slot), "r"(kEvTmemCols));
@@ -637,7 +629,8 @@ __global__ void __launch_bounds__(kBwdThreads, 1) k_train_bwd_tc(const unsigned 
                                                                  const __nv_bfloat16* __restrict__ gout,
                                                                  __nv_bfloat16* __restrict__ delta,
                                                                  uint32_t* __restrict__ status, uint32_t max_tries,
-                                                                 int issue_mma) {
+                                                                 int issue_mma,
+                                                                 const __grid_constant__ CUtensorMap tm_delta_store) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     const TcTile T = tc_setup<kBwdSlots>(smem, kUmmaWbBytes, kBwdBuf + kBwdStage, wb_img);
@@ -661,7 +654,7 @@ __global__ void __launch_bounds__(kBwdThreads, 1) k_train_bwd_tc(const unsigned 
         const bool live = row < n;
         // h_l of this row into the staging row (zeros past the record count), one commit group
         auto fetch_h = [&](int l) {
-            const unsigned char* src = reinterpret_cast<const unsigned char*>(act + (size_t)(l - 1) * n_max * kWidth +
+            const unsigned char* src = reinterpret_cast<const unsigned char*>(act + (size_t)(l - 1) * act_rows(n_max) * kWidth +
                                                                               (live ? row : 0) * kWidth);
 #pragma unroll
             for (uint32_t c = 0; c < 8u; ++c) cp_async16(stage_row + ((c ^ (r & 7u)) << 4), src + 16u * c, live ? 16u : 0u);
@@ -676,17 +669,17 @@ __global__ void __launch_bounds__(kBwdThreads, 1) k_train_bwd_tc(const unsigned 
             for (int c = 0; c < kOut / 8; ++c)
                 *reinterpret_cast<uint4*>(dst + c * 128u) = live ? src[c] : make_uint4(0u, 0u, 0u, 0u);
         }
-        // delta rows of the tile: rows past the record count are zeros (their masks are), rows past
-        // n_max are not stored
-        const uint32_t limit = (uint32_t)min((size_t)kTcRows, n_max - tile * kTcRows);
+        // delta rows of the tile leave by one TMA store of the operand (rows past the record count
+        // are zeros, their masks being zero; whole 8-row groups up to act_rows(n_max))
         for (int l = kLayers - 1; l >= 1 && ok; --l) {
             // the operand holds delta_{l+1} (the output gradient for l = 5): it leaves while the
-            // layer's MMAs read it
+            // layer's MMAs read it, and its issuer waits until the store has read it
             ok = tc_layer(r, tmem, buf_addr, sw_addr + umma_wb_offset(l), (uint32_t)layer_n(l), (uint32_t)kWidth, mbar_addr,
                           phase, slot, T.failed, max_tries, issue_mma, [&]() {
-                              if (l < kLayers - 1)
-                                  store_tile_rows(buf, delta + (size_t)l * n_max * kWidth + tile * kTcRows * kWidth, limit,
-                                                  limit, r);
+                              if (l < kLayers - 1 && r == 0) {
+                                  tma_store_5d(&tm_delta_store, 0, 0, 0, (int)(tile * (kTcRows / 8)), l, buf_addr);
+                                  bulk_wait_read();
+                              }
                           });
             if (!ok) break;
             // h_l (its copy was issued a layer earlier) into registers, then h_{l-1} on its way
@@ -725,12 +718,17 @@ __global__ void __launch_bounds__(kBwdThreads, 1) k_train_bwd_tc(const unsigned 
         if (ok) {
             // delta_1 leaves once every thread has written its row, and before the next tile's
             // output gradient takes the operand's place
+            fence_async_smem();
             asm volatile("bar.sync %0, 128;" ::"r"(1u + slot) : "memory");
-            store_tile_rows(buf, delta + tile * kTcRows * kWidth, limit, limit, r);
+            if (r == 0) {
+                tma_store_5d(&tm_delta_store, 0, 0, 0, (int)(tile * (kTcRows / 8)), 0, buf_addr);
+                bulk_wait_read();
+            }
             asm volatile("bar.sync %0, 128;" ::"r"(1u + slot) : "memory");
         }
     }
     asm volatile("cp.async.wait_all;" ::: "memory");  // no copy into this CTA's memory outlives it
+    if (r == 0) bulk_wait_all();                        // the delta stores are complete before the grid ends
     tc_teardown<kBwdSlots>(T, status);
 }
 
@@ -1111,18 +1109,18 @@ int ensure_train_buffers(liar_gpu_ctx* ctx, liar_gpu_guide* G, size_t n) {
     }
     G->act = G->delta = G->gout = nullptr;
     G->cap = 0;
-    int rc = g_alloc(ctx, G, n * 5 * kWidth * 2, &p, "guide activations");
+    int rc = g_alloc(ctx, G, act_rows(n) * 5 * kWidth * 2, &p, "guide activations");
     if (rc) return rc;
     G->act = static_cast<__nv_bfloat16*>(p);
-    rc = g_alloc(ctx, G, n * 5 * kWidth * 2, &p, "guide deltas");
+    rc = g_alloc(ctx, G, act_rows(n) * 5 * kWidth * 2, &p, "guide deltas");
     if (rc) return rc;
     G->delta = static_cast<__nv_bfloat16*>(p);
     rc = g_alloc(ctx, G, n * kOut * 2, &p, "guide output gradients");
     if (rc) return rc;
     G->gout = static_cast<__nv_bfloat16*>(p);
     // rows past a step's record count are read as zero operands; start them at zero
-    cudaError_t e = cudaMemset(G->act, 0, n * 5 * kWidth * 2);
-    if (e == cudaSuccess) e = cudaMemset(G->delta, 0, n * 5 * kWidth * 2);
+    cudaError_t e = cudaMemset(G->act, 0, act_rows(n) * 5 * kWidth * 2);
+    if (e == cudaSuccess) e = cudaMemset(G->delta, 0, act_rows(n) * 5 * kWidth * 2);
     if (e == cudaSuccess) e = cudaMemset(G->gout, 0, n * kOut * 2);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "guide training buffers");
     G->tm_base = nullptr;
@@ -1151,6 +1149,9 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 // ([n_max][48]) as {8 features, n_max records (stride 96 B), 6 groups (stride 16 B)}, boxes
 // {8, 32, 6}, unswizzled (the interleaved MN-major layout). Rows past n_max read as zero.
 // Re-encoded when the buffers or the record count change.
+// the inference launches' unused tile-store descriptor
+const CUtensorMap kNoTensorMap{};
+
 int ensure_tensor_maps(liar_gpu_ctx* ctx, liar_gpu_guide* G, size_t n_max) {
     if (G->tm_base == G->act && G->tm_rows == n_max) return LIAR_OK;
     PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
@@ -1158,7 +1159,7 @@ int ensure_tensor_maps(liar_gpu_ctx* ctx, liar_gpu_guide* G, size_t n_max) {
     const cuuint32_t box4[3] = {(cuuint32_t)kWidth, (cuuint32_t)kDwRecords, 5}, box3[3] = {8, (cuuint32_t)kDwRecords, 6};
     const cuuint32_t unit[4] = {1, 1, 1, 1};
     const cuuint64_t dims4[3] = {(cuuint64_t)kWidth, (cuuint64_t)n_max, 5};
-    const cuuint64_t strides4[2] = {(cuuint64_t)kWidth * 2, (cuuint64_t)n_max * kWidth * 2};
+    const cuuint64_t strides4[2] = {(cuuint64_t)kWidth * 2, (cuuint64_t)act_rows(n_max) * kWidth * 2};
     const cuuint64_t dims3[3] = {8, (cuuint64_t)n_max, 6};
     const cuuint64_t strides3[2] = {(cuuint64_t)kOut * 2, 16};
     CUresult r = enc(&G->tm_act, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, G->act, dims4, strides4, box4, unit,
@@ -1170,6 +1171,21 @@ int ensure_tensor_maps(liar_gpu_ctx* ctx, liar_gpu_guide* G, size_t n_max) {
                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r == CUDA_SUCCESS)
         r = enc(&G->tm_gout, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, G->gout, dims3, strides3, box3, unit,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    // the tile stores: {8 features, 8 rows (stride 128 B), 8 chunks (stride 16 B), row groups
+    // (stride 1 KB), 5 layers}, boxes of one 128-row tile {8, 8, 8, 16, 1} read from the K-major
+    // core-matrix layout of a slot's operand (row r, chunk c at (r / 8) * 1024 + c * 128 + (r % 8) * 16)
+    const cuuint64_t rows_pad = act_rows(n_max);
+    const cuuint64_t dims5[5] = {8, 8, 8, rows_pad / 8, 5};
+    const cuuint64_t strides5[4] = {(cuuint64_t)kWidth * 2, 16, 8 * (cuuint64_t)kWidth * 2, rows_pad * kWidth * 2};
+    const cuuint32_t box5[5] = {8, 8, 8, (cuuint32_t)kTcRows / 8, 1}, unit5[5] = {1, 1, 1, 1, 1};
+    if (r == CUDA_SUCCESS)
+        r = enc(&G->tm_act_st, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, G->act, dims5, strides5, box5, unit5,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r == CUDA_SUCCESS)
+        r = enc(&G->tm_delta_st, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, G->delta, dims5, strides5, box5, unit5,
                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
@@ -1244,19 +1260,20 @@ int guide_train(liar_gpu_ctx* ctx, liar_gpu_guide* G, const float* d_records, co
     // forward: the inference kernel's four slots storing h_1..h_5, the loss and the output
     // gradient per record
     const unsigned tgrid = (unsigned)std::max<size_t>(1, std::min<size_t>((tiles + kEvSlots - 1) / kEvSlots, (size_t)sms));
+    rc = ensure_tensor_maps(ctx, G, n_max);
+    if (rc) return rc;
     // the kernels after k_weight_sum start programmatically: each one's prologue (weights to shared
     // memory, barriers, tensor memory) overlaps the end of the kernel before it
     e = launch_pdl(k_eval_tc<true>, tgrid, kEvThreads, kEvSmem, st, G->umma_w, d_records, n_max, box, (float*)nullptr, 0,
-                   status, tries, mma, d_count, G->act, n_max, G->scalars, G->gout, (const float*)G->wpart, (int)wgrid);
+                   status, tries, mma, d_count, G->act, n_max, G->scalars, G->gout, (const float*)G->wpart, (int)wgrid,
+                   G->tm_act_st);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "guide training forward");
     const unsigned bgrid =
         (unsigned)std::max<size_t>(1, std::min<size_t>((tiles + kBwdSlots - 1) / kBwdSlots, (size_t)sms));
     e = launch_pdl(k_train_bwd_tc, bgrid, kBwdThreads, kBwdTcSmem, st, G->umma_wb, d_count, n_max, G->act, G->gout,
-                   G->delta, status, tries, mma);
+                   G->delta, status, tries, mma, G->tm_delta_st);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "guide training backward");
     // weight gradients: one CTA per SM, each over a contiguous run of whole 32-record stages
-    rc = ensure_tensor_maps(ctx, G, n_max);
-    if (rc) return rc;
     const size_t stages = (n_max + kDwRecords - 1) / kDwRecords;
     const size_t ctas = (size_t)std::min(sms, kReduceMaxParts);  // partial slices k_adam_reduce can add
     const size_t per_cta = ((stages + ctas - 1) / ctas) * kDwRecords;
@@ -1403,7 +1420,8 @@ int liar_gpu::guide::guide_eval(liar_gpu_ctx* ctx, const liar_gpu_guide* G, cons
     const bool wait_test = ctx->fault_test == LIAR_FAULT_TEST_GUIDE_WAIT;
     k_eval_tc<false><<<grid, kEvThreads, kEvSmem, st>>>(G->umma_w, d_inputs, n, make_box(G->cfg), d_mixture, stride,
                                                           ctx->d_scratch + kStatusWord, wait_test ? 1u << 16 : 1u << 24,
-                                                          wait_test ? 0 : 1, nullptr, nullptr, 0, nullptr, nullptr, nullptr, 0);
+                                                          wait_test ? 0 : 1, nullptr, nullptr, 0, nullptr, nullptr, nullptr, 0,
+                                                          kNoTensorMap);
     return ctx_cuda(ctx, cudaGetLastError(), "guide evaluation");
 }
 

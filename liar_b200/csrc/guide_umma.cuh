@@ -114,6 +114,20 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const void* tmap, int 
         : "memory");
 }
 
+// shared memory -> a 5D box of a tensor map in global memory (bulk async group of the issuing
+// thread; rows past the tensor's extent are not written)
+__device__ __forceinline__ void tma_store_5d(const void* tmap, int c0, int c1, int c2, int c3, int c4, uint32_t src) {
+    asm volatile("cp.async.bulk.tensor.5d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4, %5}], [%6];" ::"l"(
+                     reinterpret_cast<uint64_t>(tmap)),
+                 "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(src)
+                 : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+// the issuing thread's bulk stores have read their shared memory (it may be rewritten)
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// the issuing thread's bulk stores are complete
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
 // bounded wait for the mbarrier phase: true when it completed
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar_addr, uint32_t phase, uint32_t max_tries) {
     for (uint32_t i = 0; i < max_tries; ++i) {
