@@ -336,6 +336,7 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
 #pragma unroll
         for (int j = 0; j < IN; ++j) stage_in[r + 128u * (uint32_t)j] = pre[j];
         prefetch(tile + tile_step);
+        if (TRAIN && r == 0) bulk_wait_read();  // the previous tile's last store has read its half
         slot_sync();
         float x[kIn];
         if (r < rows) normalise_input(stage_in + r * IN, box.lo, box.inv_ext, x);
@@ -361,7 +362,10 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
         // hidden layers and the output layer from half 0
         for (int l = 1; ok && l <= kLayers; ++l) {
             tc_fence_after();
-            unsigned char* dst = buf + (r >> 3) * (kWidth / 8) * 128u + (r & 7u) * 16u;
+            // training alternates the hidden layers between the halves (h_l in half l % 2), so that
+            // the TMA store of one layer's operand runs on while the next layer's is written
+            const uint32_t hh = TRAIN ? (uint32_t)(l & 1) * kEvHalf : 0u;
+            unsigned char* dst = buf + hh + (r >> 3) * (kWidth / 8) * 128u + (r & 7u) * 16u;
             if (l < kLayers) {
                 // ReLU, bf16, the next layer's A operand (row r, 8 chunks of 8 columns)
                 {
@@ -379,21 +383,19 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
                         *reinterpret_cast<uint4*>(dst + c * 128u) = hq;
                     }
                 }
-                if (!issue(buf_addr, (kWidth / 8) * 128u, sw_addr + umma_w_offset(l), (kWidth / 8) * 128u, kWidth / 16,
+                // training: the previous layer's store has read the other half before the barrier,
+                // after which that half may be rewritten (by layer l + 1, or by the loss head's rows)
+                if (TRAIN && r == 0) bulk_wait_read();
+                if (!issue(buf_addr + hh, (kWidth / 8) * 128u, sw_addr + umma_w_offset(l), (kWidth / 8) * 128u, kWidth / 16,
                            (uint32_t)layer_n(l), false, 0)) {
                     ok = false;
                     break;
                 }
                 // training: h_l leaves the operand by one TMA store while the layer's MMAs read it (the
                 // tile's 16 8-row groups, rows past the record count as zeros: the weight-gradient
-                // kernel reads whole 32-record stages); its issuer waits until the store has read the
-                // operand, and the slot barrier after the MMA wait keeps the operand until then
-                if (TRAIN && r == 0) {
-                    tma_store_5d(&tm_act_store, 0, 0, 0, (int)(row0 >> 3), l - 1, buf_addr);
-                    bulk_wait_read();
-                }
+                // kernel reads whole 32-record stages)
+                if (TRAIN && r == 0) tma_store_5d(&tm_act_store, 0, 0, 0, (int)(row0 >> 3), l - 1, buf_addr + hh);
                 wait_half(0);
-                if (TRAIN) slot_sync();
             } else {
                 // the mixture of row r into the staging rows (pitch stride + 4 floats), then the
                 // slot's rows leave as one contiguous, coalesced block
@@ -599,6 +601,7 @@ __device__ __forceinline__ bool tc_layer(uint32_t r, uint32_t tmem, uint32_t a_a
     }
     between();
     if (!mbar_wait(mbar_addr, phase, max_tries)) failed[slot] = 1u;
+    if (r == 0) bulk_wait_read();  // a store issued by `between` has read the operand before it is rewritten
     asm volatile("bar.sync %0, 128;" ::"r"(1u + slot) : "memory");
     if (failed[slot]) {
         if (issue_mma) mbar_wait(mbar_addr, phase, max_tries);
@@ -676,10 +679,8 @@ __global__ void __launch_bounds__(kBwdThreads, 1) k_train_bwd_tc(const unsigned 
             // layer's MMAs read it, and its issuer waits until the store has read it
             ok = tc_layer(r, tmem, buf_addr, sw_addr + umma_wb_offset(l), (uint32_t)layer_n(l), (uint32_t)kWidth, mbar_addr,
                           phase, slot, T.failed, max_tries, issue_mma, [&]() {
-                              if (l < kLayers - 1 && r == 0) {
+                              if (l < kLayers - 1 && r == 0)
                                   tma_store_5d(&tm_delta_store, 0, 0, 0, (int)(tile * (kTcRows / 8)), l, buf_addr);
-                                  bulk_wait_read();
-                              }
                           });
             if (!ok) break;
             // h_l (its copy was issued a layer earlier) into registers, then h_{l-1} on its way
