@@ -601,7 +601,9 @@ __device__ __forceinline__ bool tc_layer(uint32_t r, uint32_t tmem, uint32_t a_a
     }
     between();
     if (!mbar_wait(mbar_addr, phase, max_tries)) failed[slot] = 1u;
-    if (r == 0) bulk_wait_read();  // a store issued by `between` has read the operand before it is rewritten
+    // every store but the newest (issued by `between`) has read its operand: the buffer this
+    // layer's result is written into is free
+    if (r == 0) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
     asm volatile("bar.sync %0, 128;" ::"r"(1u + slot) : "memory");
     if (failed[slot]) {
         if (issue_mma) mbar_wait(mbar_addr, phase, max_tries);
@@ -612,91 +614,70 @@ __device__ __forceinline__ bool tc_layer(uint32_t r, uint32_t tmem, uint32_t a_a
     return true;
 }
 
-constexpr uint32_t kBwdBuf = (uint32_t)kTcRows * kWidth * 2;    // a slot's A operand: 128 x 64 bf16
-constexpr uint32_t kBwdStage = (uint32_t)kTcRows * kWidth * 2;  // a slot's h rows: 128 x 64 bf16
+constexpr uint32_t kBwdBuf = (uint32_t)kTcRows * kWidth * 2;  // one A operand: 128 x 64 bf16
 constexpr int kBwdSlots = 4;
 constexpr int kBwdThreads = 128 * kBwdSlots;
-constexpr size_t kBwdTcSmem = 1024 + kUmmaWbBytes + (size_t)kBwdSlots * (kBwdBuf + kBwdStage) + 128;
+constexpr size_t kBwdTcSmem = 1024 + kUmmaWbBytes + (size_t)kBwdSlots * 2 * kBwdBuf + 128;
 
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
-}
-
-// Four slots of 128 records. Each thread copies its record's h_l row (the ReLU mask of the next
-// layer) asynchronously into the slot's staging rows (16-byte chunks XOR-permuted by the row, so
-// that a warp's accesses spread over all banks) one layer ahead, so the copy overlaps the layer
-// before; the accumulator is read 32 columns at a time.
+// Four slots of 128 records, each with two operand buffers: layer l's A operand (delta_{l+1}, the
+// output gradient for l = 5) is buffer l % 2, and delta_l is written into the other one, so that
+// the TMA store of one layer's deltas runs on while the next layer's are computed. Each layer's
+// mask row h_l is loaded into registers before the layer's MMAs are waited for; the accumulator is
+// read 32 columns at a time.
 __global__ void __launch_bounds__(kBwdThreads, 1) k_train_bwd_tc(const unsigned char* __restrict__ wb_img,
                                                                  const uint32_t* __restrict__ n_dev, size_t n_max,
                                                                  const __nv_bfloat16* __restrict__ act,
                                                                  const __nv_bfloat16* __restrict__ gout,
-                                                                 __nv_bfloat16* __restrict__ delta,
                                                                  uint32_t* __restrict__ status, uint32_t max_tries,
                                                                  int issue_mma,
                                                                  const __grid_constant__ CUtensorMap tm_delta_store) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    const TcTile T = tc_setup<kBwdSlots>(smem, kUmmaWbBytes, kBwdBuf + kBwdStage, wb_img);
+    const TcTile T = tc_setup<kBwdSlots>(smem, kUmmaWbBytes, 2 * kBwdBuf, wb_img);
     grid_dependency_wait();  // the forward's activations and output gradients
     launch_dependents();
     const size_t n = n_dev ? min((size_t)*n_dev, n_max) : n_max;
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
     const uint32_t slot = tid >> 7, r = tid & 127u;
-    unsigned char* buf = smem + kUmmaWbBytes + slot * (kBwdBuf + kBwdStage);
-    const uint32_t stage_row = (uint32_t)__cvta_generic_to_shared(buf + kBwdBuf) + r * 128u;  // this row's h
+    unsigned char* bufs = smem + kUmmaWbBytes + slot * 2 * kBwdBuf;
     const uint32_t tmem = *T.tmem_slot + 64u * slot;
     const uint32_t taddr = tmem + ((32u * (warp & 3u)) << 16);
     const uint32_t mbar_addr = (uint32_t)__cvta_generic_to_shared(T.mbar_all + slot);
     const uint32_t sw_addr = (uint32_t)__cvta_generic_to_shared(smem);
-    const uint32_t buf_addr = (uint32_t)__cvta_generic_to_shared(buf);
+    const uint32_t bufs_addr = (uint32_t)__cvta_generic_to_shared(bufs);
+    const size_t rows_pad = act_rows(n_max);
     uint32_t phase = 0;
     const size_t n_tiles = (n + kTcRows - 1) / kTcRows;
     bool ok = true;
     for (size_t tile = (size_t)blockIdx.x * kBwdSlots + slot; ok && tile < n_tiles; tile += (size_t)gridDim.x * kBwdSlots) {
         const size_t row = tile * kTcRows + r;
         const bool live = row < n;
-        // h_l of this row into the staging row (zeros past the record count), one commit group
-        auto fetch_h = [&](int l) {
-            const unsigned char* src = reinterpret_cast<const unsigned char*>(act + (size_t)(l - 1) * act_rows(n_max) * kWidth +
-                                                                              (live ? row : 0) * kWidth);
-#pragma unroll
-            for (uint32_t c = 0; c < 8u; ++c) cp_async16(stage_row + ((c ^ (r & 7u)) << 4), src + 16u * c, live ? 16u : 0u);
-            asm volatile("cp.async.commit_group;" ::: "memory");
-        };
-        fetch_h(kLayers - 1);
-        // the output gradient (48 wide) as the first A operand
+        const int g0 = (int)(tile * (kTcRows / 8));  // the tile's first 8-row group
+        // the output gradient (48 wide) as the first A operand, in buffer 1
         {
             const uint4* src = reinterpret_cast<const uint4*>(gout + row * kOut);
-            unsigned char* dst = buf + (r >> 3) * (kOut / 8) * 128u + (r & 7u) * 16u;
+            unsigned char* dst = bufs + kBwdBuf + (r >> 3) * (kOut / 8) * 128u + (r & 7u) * 16u;
 #pragma unroll
             for (int c = 0; c < kOut / 8; ++c)
                 *reinterpret_cast<uint4*>(dst + c * 128u) = live ? src[c] : make_uint4(0u, 0u, 0u, 0u);
         }
-        // delta rows of the tile leave by one TMA store of the operand (rows past the record count
-        // are zeros, their masks being zero; whole 8-row groups up to act_rows(n_max))
         for (int l = kLayers - 1; l >= 1 && ok; --l) {
-            // the operand holds delta_{l+1} (the output gradient for l = 5): it leaves while the
-            // layer's MMAs read it, and its issuer waits until the store has read it
-            ok = tc_layer(r, tmem, buf_addr, sw_addr + umma_wb_offset(l), (uint32_t)layer_n(l), (uint32_t)kWidth, mbar_addr,
-                          phase, slot, T.failed, max_tries, issue_mma, [&]() {
-                              if (l < kLayers - 1 && r == 0)
-                                  tma_store_5d(&tm_delta_store, 0, 0, 0, (int)(tile * (kTcRows / 8)), l, buf_addr);
+            const uint32_t a_off = (uint32_t)(l & 1) * kBwdBuf;  // this layer's operand; delta_l goes to the other
+            // h_l (the mask) on its way while the layer's MMAs run
+            uint4 h[kWidth / 8];
+            const uint4* hp = reinterpret_cast<const uint4*>(act + (size_t)(l - 1) * rows_pad * kWidth + row * kWidth);
+#pragma unroll
+            for (int c = 0; c < kWidth / 8; ++c) h[c] = live ? hp[c] : make_uint4(0u, 0u, 0u, 0u);
+            // the operand holds delta_{l+1} (l < 5): it leaves by one TMA store while the layer's
+            // MMAs read it (rows past the record count are zeros, their masks being zero; whole
+            // 8-row groups up to act_rows(n_max))
+            ok = tc_layer(r, tmem, bufs_addr + a_off, sw_addr + umma_wb_offset(l), (uint32_t)layer_n(l), (uint32_t)kWidth,
+                          mbar_addr, phase, slot, T.failed, max_tries, issue_mma, [&]() {
+                              if (l < kLayers - 1 && r == 0) tma_store_5d(&tm_delta_store, 0, 0, 0, g0, l, bufs_addr + a_off);
                           });
             if (!ok) break;
-            // h_l (its copy was issued a layer earlier) into registers, then h_{l-1} on its way
-            asm volatile("cp.async.wait_group 0;" ::: "memory");
-            uint4 h[kWidth / 8];
-#pragma unroll
-            for (uint32_t c = 0; c < 8u; ++c) {
-                uint4 q;
-                asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
-                             : "=r"(q.x), "=r"(q.y), "=r"(q.z), "=r"(q.w)
-                             : "r"(stage_row + ((c ^ (r & 7u)) << 4)));
-                h[c] = q;
-            }
-            if (l > 1) fetch_h(l - 1);
-            // mask by h_l > 0 (the ReLU of layer l - 1's output), store delta_l, next A operand
-            unsigned char* dst = buf + (r >> 3) * (kWidth / 8) * 128u + (r & 7u) * 16u;
+            // mask by h_l > 0 (the ReLU of layer l - 1's output): delta_l, the next A operand
+            unsigned char* dst = bufs + (kBwdBuf - a_off) + (r >> 3) * (kWidth / 8) * 128u + (r & 7u) * 16u;
 #pragma unroll
             for (int half = 0; half < 2; ++half) {
                 float v[32];
@@ -717,19 +698,18 @@ __global__ void __launch_bounds__(kBwdThreads, 1) k_train_bwd_tc(const unsigned 
             }
         }
         if (ok) {
-            // delta_1 leaves once every thread has written its row, and before the next tile's
-            // output gradient takes the operand's place
+            // delta_1 (in buffer 0) leaves once every thread has written its row; every store of
+            // the tile has read its operand before the next tile writes the buffers
             fence_async_smem();
             asm volatile("bar.sync %0, 128;" ::"r"(1u + slot) : "memory");
             if (r == 0) {
-                tma_store_5d(&tm_delta_store, 0, 0, 0, (int)(tile * (kTcRows / 8)), 0, buf_addr);
+                tma_store_5d(&tm_delta_store, 0, 0, 0, g0, 0, bufs_addr);
                 bulk_wait_read();
             }
             asm volatile("bar.sync %0, 128;" ::"r"(1u + slot) : "memory");
         }
     }
-    asm volatile("cp.async.wait_all;" ::: "memory");  // no copy into this CTA's memory outlives it
-    if (r == 0) bulk_wait_all();                        // the delta stores are complete before the grid ends
+    if (r == 0) bulk_wait_all();  // the delta stores are complete before the grid ends
     tc_teardown<kBwdSlots>(T, status);
 }
 
@@ -1272,7 +1252,7 @@ int guide_train(liar_gpu_ctx* ctx, liar_gpu_guide* G, const float* d_records, co
     const unsigned bgrid =
         (unsigned)std::max<size_t>(1, std::min<size_t>((tiles + kBwdSlots - 1) / kBwdSlots, (size_t)sms));
     e = launch_pdl(k_train_bwd_tc, bgrid, kBwdThreads, kBwdTcSmem, st, G->umma_wb, d_count, n_max, G->act, G->gout,
-                   G->delta, status, tries, mma, G->tm_delta_st);
+                   status, tries, mma, G->tm_delta_st);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "guide training backward");
     // weight gradients: one CTA per SM, each over a contiguous run of whole 32-record stages
     const size_t stages = (n_max + kDwRecords - 1) / kDwRecords;
