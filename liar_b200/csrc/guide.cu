@@ -489,8 +489,10 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
 // the batch's record weights (positive and finite ones), one sum per block into wpart; the
 // training forward adds the block sums in a fixed order, so that a step is reproducible
 __global__ void k_weight_sum(const float* __restrict__ rec, const uint32_t* __restrict__ n_dev, size_t n_max,
-                             float* __restrict__ wpart) {
-    launch_dependents();  // the training forward's prologue reads nothing written here
+                             float* __restrict__ wpart, float* __restrict__ loss) {
+    grid_dependency_wait();  // the records and the previous step are complete
+    launch_dependents();     // the training forward's prologue reads nothing written here
+    if (blockIdx.x == 0 && threadIdx.x == 0) *loss = 0.0f;  // the forward adds the batch's loss after its wait
     const size_t n = n_dev ? min((size_t)*n_dev, n_max) : n_max;
     float s = 0.0f;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -1227,11 +1229,12 @@ int guide_train(liar_gpu_ctx* ctx, liar_gpu_guide* G, const float* d_records, co
     rc = smem_attrs(ctx);
     if (rc) return rc;
     const Box box = make_box(G->cfg);
-    cudaError_t e = cudaMemsetAsync(G->scalars, 0, 2 * sizeof(float), st);
-    if (e != cudaSuccess) return ctx_cuda(ctx, e, "guide scalars");
     const int sms = ctx->num_sms;
     const unsigned wgrid = (unsigned)std::max<size_t>(1, std::min<size_t>((n_max + 255) / 256, (size_t)kWeightParts));
-    k_weight_sum<<<wgrid, 256, 0, st>>>(d_records, d_count, n_max, G->wpart);
+    // launched programmatically as well (it waits for the kernel before it, a previous step's Adam
+    // kernel or whatever wrote the records, before reading anything), and it clears the loss sum
+    cudaError_t e = launch_pdl(k_weight_sum, wgrid, 256, 0, st, d_records, d_count, n_max, G->wpart, G->scalars + 1);
+    if (e != cudaSuccess) return ctx_cuda(ctx, e, "guide weight sum");
     // the bounded waits of the tensor-core kernels (the fault test: no MMA, a short limit)
     const bool wait_test = ctx->fault_test == LIAR_FAULT_TEST_GUIDE_WAIT;
     const uint32_t tries = wait_test ? 1u << 16 : 1u << 24;
