@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
                                                            __nv_bfloat16* __restrict__ act, size_t n_max,
                                                            float* __restrict__ train, __nv_bfloat16* __restrict__ gout,
                                                            const float* __restrict__ wpart, int n_wpart,
-                                                           const __grid_constant__ CUtensorMap tm_act_store) {
+                                                           const __grid_constant__ CUtensorMap tm_store) {
     constexpr int IN = TRAIN ? kRecordFloats : kIn;
     if (TRAIN && n_dev) n = min((size_t)*n_dev, n);
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -336,7 +336,7 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
 #pragma unroll
         for (int j = 0; j < IN; ++j) stage_in[r + 128u * (uint32_t)j] = pre[j];
         prefetch(tile + tile_step);
-        if (TRAIN && r == 0) bulk_wait_read();  // the previous tile's last store has read its half
+        if (r == 0) bulk_wait_read();  // the previous tile's last store has read its buffer
         slot_sync();
         float x[kIn];
         if (r < rows) normalise_input(stage_in + r * IN, box.lo, box.inv_ext, x);
@@ -394,11 +394,9 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
                 // training: h_l leaves the operand by one TMA store while the layer's MMAs read it (the
                 // tile's 16 8-row groups, rows past the record count as zeros: the weight-gradient
                 // kernel reads whole 32-record stages)
-                if (TRAIN && r == 0) tma_store_5d(&tm_act_store, 0, 0, 0, (int)(row0 >> 3), l - 1, buf_addr + hh);
+                if (TRAIN && r == 0) tma_store_5d(&tm_store, 0, 0, 0, (int)(row0 >> 3), l - 1, buf_addr + hh);
                 wait_half(0);
             } else {
-                // the mixture of row r into the staging rows (pitch stride + 4 floats), then the
-                // slot's rows leave as one contiguous, coalesced block
                 float o[kOutUsed];
                 tmem_ld_32x32b<32>(taddr, o);
                 tmem_ld_32x32b<8>(taddr + 32u, o + 32);
@@ -436,8 +434,9 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
                     const uint32_t rows_out = (uint32_t)min((size_t)kTcRows, n_max - row0);
                     for (uint32_t i = r; i < rows_out * (kOut * 2 / 16); i += 128u) gdst[i] = srows[i];
                 } else {
-                const uint32_t pitch = (uint32_t)stride + 4u;
-                float* srow = reinterpret_cast<float*>(buf) + r * pitch;
+                // the mixture of row r into the staging rows (dense, stride floats per row), then the
+                // slot's rows leave by one TMA store of the block (rows past n are not written)
+                float* srow = reinterpret_cast<float*>(buf) + r * (uint32_t)stride;
                 Lobe lobes[kLobes];
                 float w[kLobes];
                 mixture_head_fast(o, lobes, w);
@@ -453,17 +452,13 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
                     *reinterpret_cast<float4*>(srow + 40) = make_float4(a[0], a[1], a[2], a[3]);
                     *reinterpret_cast<float4*>(srow + 44) = make_float4(a[4], a[5], a[6], a[7]);
                 }
+                fence_async_smem();
                 slot_sync();
                 if (failed[slot]) {  // the last layer's wait gave up: nothing leaves
                     ok = false;
                     break;
                 }
-                const uint32_t per_row = (uint32_t)stride / 4u, total = rows * per_row;
-                float4* gdst = reinterpret_cast<float4*>(mix + row0 * (size_t)stride);
-                for (uint32_t i = r; i < total; i += 128u) {
-                    const uint32_t q = i / per_row, c4 = i - q * per_row;
-                    gdst[i] = *reinterpret_cast<const float4*>(reinterpret_cast<const float*>(buf) + q * pitch + 4u * c4);
-                }
+                if (r == 0) tma_store_2d(&tm_store, 0, (int)row0, buf_addr);
                 }
             }
         }
@@ -473,7 +468,7 @@ __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* 
         for (int h = 0; h < 2; ++h)
             if (pending[h]) mbar_wait(mb[h], phase[h], max_tries);
     }
-    if (TRAIN && r == 0) bulk_wait_all();  // the activation stores are complete before the grid ends
+    if (r == 0) bulk_wait_all();  // the tile stores are complete before the grid ends
     tc_fence_before();
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tmem_slot), "r"(kEvTmemCols));
@@ -1132,9 +1127,6 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 // ([n_max][48]) as {8 features, n_max records (stride 96 B), 6 groups (stride 16 B)}, boxes
 // {8, 32, 6}, unswizzled (the interleaved MN-major layout). Rows past n_max read as zero.
 // Re-encoded when the buffers or the record count change.
-// the inference launches' unused tile-store descriptor
-const CUtensorMap kNoTensorMap{};
-
 int ensure_tensor_maps(liar_gpu_ctx* ctx, liar_gpu_guide* G, size_t n_max) {
     if (G->tm_base == G->act && G->tm_rows == n_max) return LIAR_OK;
     PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
@@ -1399,13 +1391,24 @@ int liar_gpu::guide::guide_eval(liar_gpu_ctx* ctx, const liar_gpu_guide* G, cons
     const size_t tiles = (n + kTcRows - 1) / kTcRows;
     if ((uintptr_t)d_mixture & 15u) return ctx_fail(ctx, LIAR_ERR_INVALID, "mixture output not 16-byte aligned");
     const unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>((tiles + kEvSlots - 1) / kEvSlots, (size_t)ctx->num_sms));
+    // the mixtures leave each slot as one TMA store: a 2D map over [n][stride] floats, boxes of
+    // 128 rows (rows past n are not written)
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return ctx_fail(ctx, LIAR_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    CUtensorMap tm_mix;
+    const cuuint64_t dims[2] = {(cuuint64_t)stride, (cuuint64_t)n}, strides[1] = {(cuuint64_t)stride * 4};
+    const cuuint32_t box[2] = {(cuuint32_t)stride, (cuuint32_t)kTcRows}, unit[2] = {1, 1};
+    const CUresult cr = enc(&tm_mix, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, d_mixture, dims, strides, box, unit,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (cr != CUDA_SUCCESS) return ctx_fail(ctx, LIAR_ERR_CUDA, "TMA descriptor encoding failed (CUresult %d)", (int)cr);
     // the bounded waits' limit: 2^24 polls, far beyond a layer's MMAs; the timeout test
     // (liar_gpu_set_fault_test) issues no MMA and gives up after 2^16 polls
     const bool wait_test = ctx->fault_test == LIAR_FAULT_TEST_GUIDE_WAIT;
     k_eval_tc<false><<<grid, kEvThreads, kEvSmem, st>>>(G->umma_w, d_inputs, n, make_box(G->cfg), d_mixture, stride,
                                                           ctx->d_scratch + kStatusWord, wait_test ? 1u << 16 : 1u << 24,
                                                           wait_test ? 0 : 1, nullptr, nullptr, 0, nullptr, nullptr, nullptr, 0,
-                                                          kNoTensorMap);
+                                                          tm_mix);
     return ctx_cuda(ctx, cudaGetLastError(), "guide evaluation");
 }
 

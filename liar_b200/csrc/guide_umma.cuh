@@ -123,6 +123,14 @@ __device__ __forceinline__ void tma_store_5d(const void* tmap, int c0, int c1, i
                  : "memory");
     asm volatile("cp.async.bulk.commit_group;" ::: "memory");
 }
+// shared memory -> a 2D box of a tensor map in global memory (bulk async group of the issuing thread)
+__device__ __forceinline__ void tma_store_2d(const void* tmap, int x, int y, uint32_t src) {
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                     reinterpret_cast<uint64_t>(tmap)),
+                 "r"(x), "r"(y), "r"(src)
+                 : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
 // the issuing thread's bulk stores have read their shared memory (it may be rewritten)
 __device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 // the issuing thread's bulk stores are complete
