@@ -208,20 +208,22 @@ __device__ float record_gradient(const float* o, float wx, float wy, float wz, f
 // waits once more (bounded again) for every commit still outstanding, so that no MMA still writes
 // the accumulator, and the CTA frees its TMEM and leaves. issue_mma = 0 is the timeout test: no
 // MMA and no commit are issued, so the first wait runs out with nothing in flight.
-// TRAIN (the training forward): the inputs are training records (13 floats, the first 9 the
-// network's inputs), the row count may come from device memory (n_dev, at most n), every hidden
-// layer's bf16 activations h_1..h_5 also go to act ([5][n_max][64]), and the output layer ends in
-// the loss head instead of the mixture: each row's loss gradient with respect to its 40 raw outputs
-// (record_gradient, weights normalised by the batch mean from k_weight_sum's block sums, clipped)
-// goes to gout as 48 bf16 (the last 8 zero), the batch loss is added to train[1].
+// Inference writes each row's mixture (stride floats) through tm_store, a 2D map over the
+// [n][stride] output. TRAIN (the training forward): the inputs are training records (13 floats, the
+// first 9 the network's inputs), the row count may come from device memory (n_dev, at most n),
+// every hidden layer's bf16 activations h_1..h_5 also go to the activation buffer
+// ([5][act_rows(n_max)][64]) through tm_store (then a 5D map of the tile stores), and the output layer ends in the loss head instead
+// of the mixture: each row's loss gradient with respect to its 40 raw outputs (record_gradient,
+// weights normalised by the batch mean from k_weight_sum's block sums, clipped) goes to gout as
+// 48 bf16 (the last 8 zero), the batch loss is added to train[1].
 template <bool TRAIN>
 __global__ void __launch_bounds__(kEvThreads, 1) k_eval_tc(const unsigned char* __restrict__ w_img,
                                                            const float* __restrict__ in, size_t n, Box box,
-                                                           float* __restrict__ mix, int stride,
+                                                           int stride,
                                                            uint32_t* __restrict__ status, uint32_t max_tries,
                                                            int issue_mma, const uint32_t* __restrict__ n_dev,
-                                                           __nv_bfloat16* __restrict__ act, size_t n_max,
-                                                           float* __restrict__ train, __nv_bfloat16* __restrict__ gout,
+                                                           size_t n_max, float* __restrict__ train,
+                                                           __nv_bfloat16* __restrict__ gout,
                                                            const float* __restrict__ wpart, int n_wpart,
                                                            const __grid_constant__ CUtensorMap tm_store) {
     constexpr int IN = TRAIN ? kRecordFloats : kIn;
@@ -1240,8 +1242,8 @@ int guide_train(liar_gpu_ctx* ctx, liar_gpu_guide* G, const float* d_records, co
     if (rc) return rc;
     // the kernels after k_weight_sum start programmatically: each one's prologue (weights to shared
     // memory, barriers, tensor memory) overlaps the end of the kernel before it
-    e = launch_pdl(k_eval_tc<true>, tgrid, kEvThreads, kEvSmem, st, G->umma_w, d_records, n_max, box, (float*)nullptr, 0,
-                   status, tries, mma, d_count, G->act, n_max, G->scalars, G->gout, (const float*)G->wpart, (int)wgrid,
+    e = launch_pdl(k_eval_tc<true>, tgrid, kEvThreads, kEvSmem, st, G->umma_w, d_records, n_max, box, 0,
+                   status, tries, mma, d_count, n_max, G->scalars, G->gout, (const float*)G->wpart, (int)wgrid,
                    G->tm_act_st);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "guide training forward");
     const unsigned bgrid =
@@ -1405,9 +1407,9 @@ int liar_gpu::guide::guide_eval(liar_gpu_ctx* ctx, const liar_gpu_guide* G, cons
     // the bounded waits' limit: 2^24 polls, far beyond a layer's MMAs; the timeout test
     // (liar_gpu_set_fault_test) issues no MMA and gives up after 2^16 polls
     const bool wait_test = ctx->fault_test == LIAR_FAULT_TEST_GUIDE_WAIT;
-    k_eval_tc<false><<<grid, kEvThreads, kEvSmem, st>>>(G->umma_w, d_inputs, n, make_box(G->cfg), d_mixture, stride,
+    k_eval_tc<false><<<grid, kEvThreads, kEvSmem, st>>>(G->umma_w, d_inputs, n, make_box(G->cfg), stride,
                                                           ctx->d_scratch + kStatusWord, wait_test ? 1u << 16 : 1u << 24,
-                                                          wait_test ? 0 : 1, nullptr, nullptr, 0, nullptr, nullptr, nullptr, 0,
+                                                          wait_test ? 0 : 1, nullptr, 0, nullptr, nullptr, nullptr, 0,
                                                           tm_mix);
     return ctx_cuda(ctx, cudaGetLastError(), "guide evaluation");
 }
