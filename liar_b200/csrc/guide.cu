@@ -537,7 +537,7 @@ struct TcTile {
     uint32_t* tmem_slot;
     volatile uint32_t* failed;
 };
-template <int SLOTS = kTcSlots>
+template <int SLOTS>
 __device__ __forceinline__ TcTile tc_setup(unsigned char* smem, size_t w_bytes, size_t buf_bytes,
                                            const unsigned char* __restrict__ w_img) {
     TcTile T;
@@ -566,7 +566,7 @@ __device__ __forceinline__ TcTile tc_setup(unsigned char* smem, size_t w_bytes, 
     return T;
 }
 
-template <int SLOTS = kTcSlots>
+template <int SLOTS>
 __device__ __forceinline__ void tc_teardown(const TcTile& T, uint32_t* status) {
     tc_fence_before();
     __syncthreads();

@@ -1,8 +1,8 @@
 // guide_umma.cuh -- the guide network's inference on the 5th-generation tensor cores (tcgen05).
 //
-// A CTA runs independent 4-warp slots (four for inference, two in training), each evaluating 128
-// rows at a time (M = 128; thread r of the slot owns row r), so that one slot's SIMT work overlaps
-// the others' tensor-core work.
+// A CTA runs four independent 4-warp slots (inference, the training forward and backward), each
+// evaluating 128 rows at a time (M = 128; thread r of the slot owns row r), so that one slot's SIMT
+// work overlaps the others' tensor-core work.
 //   * the weights live in shared memory as the B operands of every layer, bf16, K-major, in the
 //     canonical no-swizzle layout: element (n, k) of a layer with K inputs at
 //     (n / 8) * (K / 8) * 128 + (k / 8) * 128 + (n % 8) * 16 + (k % 8) * 2 bytes, i.e. 8x16-byte core
@@ -26,9 +26,6 @@ namespace liar_gpu {
 namespace guide {
 
 constexpr int kTcRows = 128;
-constexpr int kTcSlots = 2;                    // tiles in flight per CTA, one per 4-warp slot
-constexpr int kTcThreads = 128 * kTcSlots;
-constexpr uint32_t kTcTmemCols = 64 * kTcSlots;  // slot s accumulates in columns [64 s, 64 s + 64)
 
 // B-operand images of the six layers (bytes from the start of the image)
 __host__ __device__ constexpr uint32_t umma_w_offset(int l) {
