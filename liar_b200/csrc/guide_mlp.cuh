@@ -89,21 +89,79 @@ __device__ __forceinline__ void sincospi_enc(float x, float* sp, float* cp) {
     *cp = ((q + 1) & 2) ? -c_ : c_;
 }
 
-// the 12 words (24 bf16: sin/cos pairs of the 12 frequencies) of input value xd, as encode_row
+// packed pairs of f32 (Blackwell's two-wide FP32 instructions): every lane rounds exactly as the
+// scalar operation would
+__device__ __forceinline__ uint64_t f2_make(float lo, float hi) {
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void f2_split(uint64_t v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ uint64_t f2_fma(uint64_t a, uint64_t b, uint64_t c) {
+    uint64_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ uint64_t f2_mul(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t f2_add(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t f2_splat(float a) { return f2_make(a, a); }
+
+// the 12 words (24 bf16: sin/cos pairs of the 12 frequencies) of input value xd, as encode_row:
+// the two angle chains (pi x and pi x sqrt 2) run side by side as f32x2 pairs, each lane with the
+// operations and roundings of sincospi_enc and the doubling formulas
 __device__ __forceinline__ void encode_input(float xd, uint32_t* w) {
-    float s0, c0, s1, c1;
-    sincospi_enc(xd, &s0, &c0);
-    sincospi_enc(xd * 1.41421356237309515f, &s1, &c1);
+    const float x0 = xd, x1 = xd * 1.41421356237309515f;
+    // x = n / 2 + r, |r| <= 1/4, as in sincospi_enc (the integer quadrants per lane)
+    const float b0 = (x0 + x0) + 12582912.0f, b1 = (x1 + x1) + 12582912.0f;
+    const int q0 = (__float_as_int(b0) - 0x4B400000) & 3, q1 = (__float_as_int(b1) - 0x4B400000) & 3;
+    const uint64_t X = f2_make(x0, x1);
+    const uint64_t NF = f2_make(b0 - 12582912.0f, b1 - 12582912.0f);
+    const uint64_t R = f2_fma(NF, f2_splat(-0.5f), X);
+    const uint64_t A = f2_mul(R, f2_splat(3.14159265358979323846f));
+    const uint64_t A2 = f2_mul(A, A);
+    uint64_t ps = f2_fma(A2, f2_splat(-2.50521083854417188e-8f), f2_splat(2.75573192239858907e-6f));
+    ps = f2_fma(A2, ps, f2_splat(-1.98412698412698413e-4f));
+    ps = f2_fma(A2, ps, f2_splat(8.33333333333333333e-3f));
+    ps = f2_fma(A2, ps, f2_splat(-1.66666666666666667e-1f));
+    const uint64_t SN = f2_fma(f2_mul(A, A2), ps, A);
+    uint64_t pc = f2_fma(A2, f2_splat(2.08767569878680990e-9f), f2_splat(-2.75573192239858907e-7f));
+    pc = f2_fma(A2, pc, f2_splat(2.48015873015873016e-5f));
+    pc = f2_fma(A2, pc, f2_splat(-1.38888888888888889e-3f));
+    pc = f2_fma(A2, pc, f2_splat(4.16666666666666667e-2f));
+    pc = f2_fma(A2, pc, f2_splat(-0.5f));
+    const uint64_t CS = f2_fma(A2, pc, f2_splat(1.0f));
+    float sn0, sn1, cs0, cs1;
+    f2_split(SN, sn0, sn1);
+    f2_split(CS, cs0, cs1);
+    // the quarter-turn n mod 4 of each lane
+    const float t0 = (q0 & 1) ? cs0 : sn0, u0 = (q0 & 1) ? sn0 : cs0;
+    const float t1 = (q1 & 1) ? cs1 : sn1, u1 = (q1 & 1) ? sn1 : cs1;
+    uint64_t S = f2_make((q0 & 2) ? -t0 : t0, (q1 & 2) ? -t1 : t1);
+    uint64_t C = f2_make(((q0 + 1) & 2) ? -u0 : u0, ((q1 + 1) & 2) ? -u1 : u1);
 #pragma unroll
     for (int k = 0; k < kFreq / 2; ++k) {
+        float s0, s1, c0, c1;
+        f2_split(S, s0, s1);
+        f2_split(C, c0, c1);
         w[2 * k] = pack_bf16(s0, c0);
         w[2 * k + 1] = pack_bf16(s1, c1);
-        const float ns0 = 2.0f * s0 * c0, nc0 = c0 * c0 - s0 * s0;
-        const float ns1 = 2.0f * s1 * c1, nc1 = c1 * c1 - s1 * s1;
-        s0 = ns0;
-        c0 = nc0;
-        s1 = ns1;
-        c1 = nc1;
+        // sin 2a = (2 sin a) cos a, cos 2a = cos a cos a - sin a sin a
+        const uint64_t NS = f2_mul(f2_add(S, S), C);
+        const uint64_t SS = f2_mul(S, S);
+        float ss0, ss1;
+        f2_split(SS, ss0, ss1);
+        C = f2_fma(C, C, f2_make(-ss0, -ss1));
+        S = NS;
     }
 }
 
