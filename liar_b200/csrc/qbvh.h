@@ -39,6 +39,10 @@ struct alignas(128) QNode {
     I4 count;                               // leaf triangle count per child, 0 for inner/empty
 };
 static_assert(sizeof(QNode) == 128, "QNode must be one 128-byte line");
+// the traversal selects a child row's near or far plane by these offsets (hi_* = lo_* + 16 bytes)
+static_assert(offsetof(QNode, lo_x) == 0 && offsetof(QNode, hi_x) == 16 && offsetof(QNode, lo_y) == 32 &&
+                  offsetof(QNode, hi_y) == 48 && offsetof(QNode, lo_z) == 64 && offsetof(QNode, hi_z) == 80,
+              "QNode plane rows");
 
 struct alignas(16) QTri {
     F4 v0;   // v0.xyz, w = original triangle index (int bits)

@@ -147,13 +147,15 @@ __device__ __forceinline__ void visit_node(const QNode* __restrict__ nodes, RayS
     const bool nx = st.dx < 0.0f, ny = st.dy < 0.0f, nz = st.dz < 0.0f;
     if (COUNT) ++n_nodes;
     const QNode* q = nodes + st.node;
-    const float4 lx = ld_hint(&q->lo_x, pol_tree), hx = ld_hint(&q->hi_x, pol_tree);
-    const float4 ly = ld_hint(&q->lo_y, pol_tree), hy = ld_hint(&q->hi_y, pol_tree);
-    const float4 lz = ld_hint(&q->lo_z, pol_tree), hz = ld_hint(&q->hi_z, pol_tree);
+    // the planes a ray meets first along each axis (lo for a positive direction, hi for a negative
+    // one; hi_* follows lo_* by 16 bytes) selected by address rather than by value, so the four
+    // children's near and far rows arrive in place of the six rows and their 24 selects
+    const char* qb = reinterpret_cast<const char*>(q);
+    const uint32_t onx = nx ? 16u : 0u, ony = ny ? 48u : 32u, onz = nz ? 80u : 64u;
+    const float4 nxp = ld_hint(qb + onx, pol_tree), fxp = ld_hint(qb + (onx ^ 16u), pol_tree);
+    const float4 nyp = ld_hint(qb + ony, pol_tree), fyp = ld_hint(qb + (ony ^ 16u), pol_tree);
+    const float4 nzp = ld_hint(qb + onz, pol_tree), fzp = ld_hint(qb + (onz ^ 16u), pol_tree);
     const int4 ch = ld_hint_i(&q->child, pol_tree);
-    const float4 nxp = nx ? hx : lx, fxp = nx ? lx : hx;
-    const float4 nyp = ny ? hy : ly, fyp = ny ? ly : hy;
-    const float4 nzp = nz ? hz : lz, fzp = nz ? lz : hz;
     float tn[4], tf[4];
     tn[0] = max4f(fmaf(nxp.x, st.idx, -st.oix), fmaf(nyp.x, st.idy, -st.oiy), fmaf(nzp.x, st.idz, -st.oiz), st.tmin);
     tn[1] = max4f(fmaf(nxp.y, st.idx, -st.oix), fmaf(nyp.y, st.idy, -st.oiy), fmaf(nzp.y, st.idz, -st.oiz), st.tmin);
