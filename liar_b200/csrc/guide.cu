@@ -44,7 +44,7 @@ struct liar_gpu_guide {
     float* grad_part = nullptr;      // [part_cap][kParams]: the weight-gradient CTAs' partial sums
     float* wpart = nullptr;          // [kWeightParts]: k_weight_sum's block sums
     int part_cap = 0;
-    float* scalars = nullptr;        // [0] weight sum [1] loss sum
+    float* scalars = nullptr;        // [1] the step's loss sum ([0] unused)
     // TMA descriptors of act, delta and gout for the weight-gradient kernel, for tm_rows records
     CUtensorMap tm_act{}, tm_delta{}, tm_gout{};
     // TMA descriptors through which the forward and backward store their activation / delta tiles
